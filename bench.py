@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Throughput of the CRKSPH particle step on B200: particle-steps/s.
+
+Workload: the 2D Sedov-Taylor blast of the CRKSPH hot path -- 512 x 512 = 262,144
+particles on the periodic unit square, rho = 1, p = 1e-6, gamma = 5/3, E = 1
+deposited kernel-weighted at the centre, Wendland C4 with 32 neighbours,
+Cullen-Dehnen switch, Heun RK2 with compatible energy, CFL 0.3 time step computed
+on the device every step.  One "step" = one full integrator step (two right-hand
+sides, neighbour search, finalize, dt).  Inputs are synthetic (seedless lattice).
+
+Arms
+  default            the GPU path (libwarpsph_b200) through the reference's API
+  --impl reference   the reference's CPU implementation of the path -- here the C
+                     oracle that restates it (the reference itself needs NVIDIA Warp
+                     and two sibling packages that are not available), timed on the
+                     host cores with all threads.
+Multi-GPU (torchrun): the path does not shard (one simulation per GPU), so N ranks
+run N independent replicas; value = total particle-steps/s, time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s on 1 B200; DFSPH time-to-tolerance, learned warm-start vs plain"
+UNIT = "particle-steps/s"
+WORKLOAD = "Sedov 2D CRKSPH 512x512 (262,144 particles), Wendland C4, 32 neighbours, Cullen-Dehnen, RK2, compatible energy"
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nx", type=int, default=512)
+    ap.add_argument("--cpu-steps", type=int, default=1, help="steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--breakdown", action="store_true", help="print a per-kernel time breakdown to stderr")
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                                          "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------- byte model
+def bytes_accel_dudt(d: int, K: float) -> float:
+    """Algorithmic bytes per particle of the fused CRK accel + du/dt pass (FP32):
+    per-particle inputs x, v, B, gradA (4d each), H, m, rho, V, A, c, P (+3 words of
+    padding-free scalars) = 16d + 40, DvDx and gradB (4d^2 each) = 8d^2; outputs
+    dv/dt (4d) and du/dt (4); per interacting pair a 4-byte index and the pairwise
+    ap_ij, av_ij the reference's API returns (8d)."""
+    return (16 * d + 40 + 8 * d * d) + 4 * d + 4 + K * (4 + 8 * d)
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return dict(json.loads(p.read_text()), source="measured")
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+# ---------------------------------------------------------------------------- CPU arm
+def cpu_setup(nx: int):
+    """Sedov initial state built by the oracle on the host (never the GPU engine)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    from oracle.cases import sedov_state
+    from oracle.steps import CRKSPHOracle, SWITCH_CULLEN
+    import warpsph_b200 as ws
+    cfg, _ = ws.buildConfig(dim=2, domain=ws.buildDomainDescription(1.0, 2, True, "cpu"), kernel=ws.KernelFunctions.Wendland4,
+                            targetNeighbors=32, device="cpu")
+    sch = ws.CRKSPHConfig()
+    sch.gamma = 5 / 3
+    sch.viscositySwitchParams.scheme = ws.ViscositySwitch.CullenDehnen2010
+    params = ws.make_params(cfg, sch)
+    st = sedov_state(params, nx, 2, target_neighbors=32.0)
+    orc = CRKSPHOracle(params, "f32", switch=SWITCH_CULLEN)
+    dt = orc.o.cfl_dt(params, st["supports"], st["internalEnergies"])
+    return orc, st, dt
+
+
+def cpu_time_steps(orc, st, dt, steps: int):
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        st, _, _ = orc.step(st, dt, "rungeKutta2")
+    return st, time.perf_counter() - t0
+
+
+def cpu_baseline(nx: int, steps: int) -> dict:
+    """The oracle (C restatement of the reference, all host threads) on a bounded
+    sample: `steps` full RK2 steps of the same Sedov workload."""
+    orc, st, dt = cpu_setup(nx)
+    n = st["masses"].shape[0]
+    st, sec = cpu_time_steps(orc, st, dt, steps)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": n * steps / sec, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} RK2 step(s) of the {nx}x{nx} Sedov CRKSPH workload ({n} particles), FP32 oracle, {sec:.2f} s"}
+
+
+def reference_arm(args, rank: int):
+    """Each step is one RK2 step of the full workload on the host cores."""
+    if rank != 0:
+        return 0
+    t0 = time.perf_counter()
+    orc, st, dt = cpu_setup(args.nx)
+    n = st["masses"].shape[0]
+    st, _ = cpu_time_steps(orc, st, dt, min(args.warmup, 1))
+    per = []
+    for _ in range(args.steps):
+        st, sec = cpu_time_steps(orc, st, dt, 1)
+        per.append(sec)
+    total = sum(per)
+    val = n * args.steps / total
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    cb = {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+          "sample": f"{args.steps} RK2 steps of the {args.nx}x{args.nx} Sedov CRKSPH workload ({n} particles), FP32 oracle"}
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD + " -- CPU oracle restating the reference", "particles": n},
+            "cpu_baseline": cb, "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t0}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------- GPU arm
+def build_workload(nx, dev):
+    import warpsph_b200 as ws
+    cfg, integrator = ws.buildConfig(dim=2, domain=ws.buildDomainDescription(1.0, 2, True, dev), kernel=ws.KernelFunctions.Wendland4,
+                                     targetNeighbors=32, integrationScheme=ws.IntegrationSchemeType.rungeKutta2, cflFactor=0.3,
+                                     device=dev)
+    System, State, Config, Update, step, *_ = ws.buildScheme("crkSPH")
+    sch = Config()
+    sch.gamma = 5 / 3
+    sch.viscositySwitchParams.scheme = ws.ViscositySwitch.CullenDehnen2010
+    system = ws.buildSedov(System, State, cfg, nx=nx, dim=2, domainExtent=1.0, E0=1.0, p0=1e-6, gamma=5 / 3,
+                           kernel=ws.KernelFunctions.Wendland4, targetNeighbors=32, device=dev)
+    return cfg, sch, integrator, step, system
+
+
+def gpu_arm(args, rank: int, world: int):
+    import torch
+    import torch.distributed as dist
+    import warpsph_b200 as ws
+    from warpsph_b200 import _capi, ops
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    cfg, sch, integ, step, system = build_workload(args.nx, dev)
+    params = ws.make_params(cfg, sch)
+    n = system.state.masses.shape[0]
+    L = _capi.lib()
+
+    state = {"system": system, "dt": torch.tensor([cfg.dt], device=dev, dtype=torch.float32)}
+
+    def one_step():
+        S = state["system"].state
+        dt = ops.cfl_dt(params, S.supports, S.internalEnergies, dt_prev=state["dt"])
+        state["dt"] = dt
+        state["system"] = integ.function(state=state["system"], f=step, dt=dt, config=cfg, compParams=sch).state
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 0)):
+        one_step()
+    torch.cuda.synchronize()
+
+    # ------------------------------------------------ device-resident timed region
+    timer = ops.KernelTimer(names={"crk_accel_dudt"})
+    clocks = ClockSampler(dev.index)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = L.sph_launch_count()
+    ops.TIMER = timer
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        one_step()
+    ev1.record()
+    torch.cuda.synchronize()
+    ops.TIMER = None
+    launches = L.sph_launch_count() - launches0
+    barrier()
+    clock_info = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = n * args.steps * world / (ms_max / 1e3)
+    ksum = timer.summary().get("crk_accel_dudt", {"launches": 0, "avg_ms": float("nan")})
+
+    # roofline of the dominant kernel
+    S = state["system"].state
+    adj = state["system"].adjacency
+    dvec = S.positions[adj.i] - S.positions[adj.j]
+    r = torch.linalg.norm(dvec - torch.round(dvec), dim=1)   # unit periodic box: minimum image
+    Hmax = torch.maximum(S.supports[adj.i], S.supports[adj.j])
+    K_meas = float((r < Hmax).sum().item()) / n
+    nnz_per = adj.nnz / n
+    per_particle = bytes_accel_dudt(2, 32.0)
+    peaks = load_peaks()
+    achieved = per_particle * n / (ksum["avg_ms"] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": "k_crk_accel_dudt",
+                "algorithmic_bytes_per_particle": per_particle, "model_K": 32, "measured_interacting_per_particle": K_meas,
+                "verlet_entries_per_particle": nnz_per, "avg_launch_ms": ksum["avg_ms"], "launches_timed": ksum["launches"],
+                "peak_source": peaks.get("source")}
+
+    breakdown = None
+    if args.breakdown:
+        bt = ops.KernelTimer()
+        ops.TIMER = bt
+        for _ in range(3):
+            one_step()
+        torch.cuda.synchronize()
+        ops.TIMER = None
+        breakdown = bt.summary()
+
+    # ------------------------------------------------ end-to-end through the API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        fields = ["positions", "velocities", "internalEnergies", "supports", "masses", "densities", "alpha0s", "alphas", "divergence"]
+        S = state["system"].state
+        host_in = {f: getattr(S, f).detach().cpu().pin_memory() for f in fields}
+        host_out = {f: torch.empty_like(host_in[f]).pin_memory() for f in fields}
+        h2d = sum(t.numel() * t.element_size() for t in host_in.values())
+        d2h = h2d
+        e2e_steps = max(3, args.steps // 2)
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(e2e_steps):
+            S = state["system"].state
+            for f in fields:
+                setattr(S, f, host_in[f].to(dev, non_blocking=True))
+            one_step()
+            S = state["system"].state
+            for f in fields:
+                host_out[f].copy_(getattr(S, f), non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+        e1.record()
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        te = torch.tensor([ems], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": n * e2e_steps * world / (float(te.item()) / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": e2e_steps}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(args.nx, args.cpu_steps)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "particles": n, "nx": args.nx, "parallelism": f"replicas x{world}",
+                           "l2": "working set larger than L2 (pair arrays ~0.7 GB per step), no flush needed"},
+                "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info}
+        if breakdown is not None:
+            line["breakdown_ms"] = {k: round(v["total_ms"] / 3, 4) for k, v in breakdown.items()}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    try:
+        return gpu_arm(args, rank, world)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

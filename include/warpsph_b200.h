@@ -1,0 +1,306 @@
+/*
+ * warpsph_b200.h -- C ABI of libwarpsph_b200.so, the sm_100a implementation of the
+ * warpSPH per-step particle hot path (neighbour search, SPH pair interactions,
+ * DFSPH Jacobi solves, integrator update and CFL time step).
+ *
+ * Conventions shared by every entry point
+ *   - All array arguments are DEVICE pointers (allocated by the caller, e.g. torch).
+ *     The library never allocates in these calls and never frees caller memory.
+ *   - Positions and other per-particle vectors are row-major [n, dim] float arrays,
+ *     per-particle matrices are row-major [n, dim, dim]; M[a][b] = d(field^a)/dx^b.
+ *   - Neighbour lists are CSR: neighbor_offsets[n], num_neighbors[n] (int32) and
+ *     neighbor_list[nnz] (int32, original particle indices).  Row i lists every j
+ *     with |x_i - x_j| < verlet_scale * max(H_i, H_j) (i itself included), in
+ *     ascending order of j's position in the cell-sorted order.
+ *   - `stream` is a cudaStream_t passed as void*; work is enqueued asynchronously.
+ *   - Scalars that change every step (dt) are read from DEVICE memory so a step can
+ *     be captured in a CUDA graph without host round trips.
+ *   - Return value: SPH_OK (0) or a negative SPH_ERR_* code; sph_last_error_string()
+ *     describes the last failure of the calling thread.
+ *   - Every entry point accepts n == 0 and then does nothing.
+ *
+ * Reference interface: wi-re/warpSPH (Python + NVIDIA Warp).  Each declaration names
+ * the reference function it replaces, relative to the reference's project root.
+ */
+#ifndef WARPSPH_B200_H
+#define WARPSPH_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+#define SPH_OK                  0
+#define SPH_ERR_BAD_ARG        -1   /* null pointer, bad enum, misaligned array, n < 0 */
+#define SPH_ERR_WORKSPACE      -2   /* caller workspace smaller than *_workspace_size */
+#define SPH_ERR_CAPACITY       -3   /* neighbour list capacity exceeded (device flag) */
+#define SPH_ERR_CUDA           -4   /* a CUDA launch failed */
+#define SPH_ERR_NOT_CONVERGED  -5   /* Jacobi solve hit its iteration cap */
+#define SPH_ERR_TIMEOUT        -6   /* a bounded device wait gave up */
+#define SPH_ERR_NONFINITE      -7   /* NaN/Inf detected in a reduction */
+#define SPH_ERR_UNSUPPORTED    -8   /* option not implemented on this path */
+
+/* device status word bits (written by kernels into a caller-provided int32) */
+#define SPH_STATUS_LIST_OVERFLOW   0x1
+#define SPH_STATUS_NONFINITE       0x2
+#define SPH_STATUS_NOT_CONVERGED   0x4
+#define SPH_STATUS_TIMEOUT         0x8
+
+/* ---------------------------------------------------------------- enumerations */
+/* Kernel functions (warpSPHCore KernelFunctions; names as used in
+ * configurations/simulationConfig.py:25). */
+#define SPH_KERNEL_WENDLAND2 1
+#define SPH_KERNEL_WENDLAND4 2
+#define SPH_KERNEL_WENDLAND6 3
+
+/* Support schemes (warpSPHCore SupportScheme): h used for the pair kernel value. */
+#define SPH_SUPPORT_GATHER               0   /* H_i */
+#define SPH_SUPPORT_SCATTER              1   /* H_j */
+#define SPH_SUPPORT_SYMMETRIC            2   /* W(r, (H_i+H_j)/2) */
+#define SPH_SUPPORT_SUPERSYMMETRIC       3   /* W(r, max(H_i, H_j)) */
+#define SPH_SUPPORT_KERNELMEANSYMMETRIC  4   /* (W(r,H_i) + W(r,H_j)) / 2 */
+
+/* Energy partition schemes (enumTypes.py:5-11, same values). */
+#define SPH_ENERGY_EQUALWORK   0
+#define SPH_ENERGY_PDV         1
+#define SPH_ENERGY_DIMINISHING 2
+#define SPH_ENERGY_MONOTONIC   3
+#define SPH_ENERGY_HYBRID      4
+#define SPH_ENERGY_CRK         5
+
+/* Artificial viscosity terms (configurations/moduleConfigurations/diffusionParameters.py:8-20). */
+#define SPH_VISC_DEFAULT              0
+#define SPH_VISC_MONAGHANGINGOLD1983  1
+#define SPH_VISC_CLEARY1998           2
+#define SPH_VISC_MONAGHAN1992         3
+#define SPH_VISC_MONAGHAN1997A        4
+#define SPH_VISC_MONAGHAN1997B        5
+#define SPH_VISC_DUKOWICZ             6
+#define SPH_VISC_PRICE2012_98         7
+#define SPH_VISC_PRICE2012            8
+#define SPH_VISC_PRICE2008            9
+#define SPH_VISC_WADSLEY2008         10
+#define SPH_VISC_DELTASPH            11
+
+/* ---------------------------------------------------------------- parameters */
+/* Plain-old-data parameter block.  Doubles first so the layout has no padding
+ * surprises for ctypes; the GPU path rounds them to float at launch. */
+typedef struct SphParams {
+    /* domain (utils/domain.py:7-22 DomainDescription) */
+    double domain_min[3];
+    double domain_max[3];
+    double verlet_scale;              /* simulationConfig.py:24 */
+    /* DiffusionParameters (configurations/moduleConfigurations/diffusionParameters.py:22-37) */
+    double C_l, C_q, Cu_l, Cu_q, K;
+    /* CRKViscosity (configurations/crkSPH.py:16-25) */
+    double eta_crit, eta_fold;
+    /* compressible scheme (configurations/compressibleConfig.py:16-30) */
+    double gamma;
+    /* ViscositySwitchConfig (configurations/moduleConfigurations/viscositySwitchParameters.py:11-26) */
+    double alpha_min, alpha_max, beta_xi;
+    /* adaptive support and time step (simulationConfig.py:28-38) */
+    double target_neighbors;
+    double cfl, min_dt, max_dt, dt_growth;
+    double reserved_d[8];
+    /* integers */
+    int32_t dim;                      /* 1, 2 or 3 */
+    int32_t kernel;                   /* SPH_KERNEL_* */
+    int32_t periodic[3];
+    int32_t viscosity_term;           /* SPH_VISC_* */
+    int32_t monaghan_switch, correct_xi, scale_beta;
+    int32_t enable_crk_limiter, enable_vanleer_limiter, force_vanleer_off, force_vanleer_on;
+    int32_t energy_scheme;            /* SPH_ENERGY_* */
+    int32_t limit_xi;
+    int32_t kahan;                    /* 1: compensated accumulation of dv/dt and du/dt */
+    int32_t reserved_i[8];
+} SphParams;
+
+/* ---------------------------------------------------------------- library */
+const char* sph_version(void);
+const char* sph_last_error_string(void);
+/* Number of CUDA kernels this library has launched in the process (all threads). */
+int64_t sph_launch_count(void);
+/* Kernel-function constants used by the library (normalisation C_d, kernel scale
+ * H/h = 1/(2 sigma), Dehnen & Aly 2012 Table 1). Host-only, no GPU needed. */
+int sph_kernel_constants(int32_t kernel, int32_t dim, double* norm_out, double* scale_out);
+
+/* ---------------------------------------------------------------- (a) neighbour search */
+/* Workspace bytes for sph_neighbors_build with `cell_capacity` dense cells. */
+int sph_neighbors_workspace_size(const SphParams* p, int64_t n, int64_t cell_capacity,
+                                 int64_t* bytes_out);
+
+/* Replaces warpSPHCore buildVerletList (called at schemes/crkSPH.py:54-58,
+ * schemes/compSPH.py:42-46, schemes/dfsph.py:29-33): Morton-keyed dense cell grid
+ * of cell size >= verlet_scale*max(H), counting sort by (cell key, index), cell
+ * offset table, then count -> scan -> fill of the CSR Verlet list.
+ * Outputs: sort_index[n] (original index of the k-th sorted particle),
+ * sorted_keys[n] (its Morton cell key), cell_begin/cell_end[cell_capacity],
+ * CSR arrays, *nnz_out (device int64).  If nnz > list_capacity the list is not
+ * filled, SPH_STATUS_LIST_OVERFLOW is or-ed into *status (device int32) and
+ * *nnz_out still holds the required size. grid_out (device, 8 int32): grid dims,
+ * bits per axis, and the cell size as float bits. */
+int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const float* H,
+                        void* workspace, int64_t workspace_bytes, int64_t cell_capacity,
+                        int32_t* sort_index, uint32_t* sorted_keys,
+                        int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
+                        int32_t* neighbor_offsets, int32_t* num_neighbors,
+                        int32_t* neighbor_list, int64_t list_capacity,
+                        int64_t* nnz_out, int32_t* status, void* stream);
+
+/* Expands CSR rows into the reference's AdjacencyList.i / .j int64 arrays
+ * (io.py:8-20 field names). */
+int sph_neighbors_expand(int64_t n, const int32_t* neighbor_offsets, const int32_t* num_neighbors,
+                         const int32_t* neighbor_list, int64_t nnz,
+                         int64_t* i_out, int64_t* j_out, void* stream);
+
+/* ---------------------------------------------------------------- (b) pair interactions */
+/* Density summation rho_i = sum_j m_j W(r_ij, h_ij) with the given support scheme.
+ * Replaces warpOperation(Density) (modules/density/density.py:16-28). */
+int sph_density_gather(const SphParams* p, int64_t n, int32_t support_mode,
+                       const float* x, const float* H, const float* m,
+                       const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                       float* rho_out, void* stream);
+
+/* One Monaghan Newton iteration of the adaptive support
+ * (modules/adaptiveSupport/optimalSupportMonaghan.py:87-125 with the Omega kernel
+ * modules/adaptiveSupport/wp_omega.py:10-60): gather density, Omega = dF/dh,
+ * H_new = clamp(H - F/(Omega+1e-6), hbounds[0]/4, 4*hbounds[1]).
+ * hbounds (device float[2]) holds min/max of H on entry; ratio_out[n] = H_new/(H+1e-6). */
+int sph_adaptive_h_iter(const SphParams* p, int64_t n, int32_t support_mode,
+                        const float* x, const float* H, const float* m,
+                        const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                        const float* hbounds, float* rho_out, float* H_out, float* ratio_out,
+                        void* stream);
+
+/* min and max of a device array into out2[0], out2[1] (device). */
+int sph_minmax(int64_t n, const float* a, float* out2, void* stream);
+
+/* CRK apparent volume V_i = 1 / sum_j W(r_ij, H_j)  (warpSPHCore crk_volume,
+ * called through computeCRKFactors at schemes/crkSPH.py:61). */
+int sph_crk_volume(const SphParams* p, int64_t n, const float* x, const float* H,
+                   const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                   float* V_out, void* stream);
+
+/* CRK correction coefficients A, B, gradA, gradB (Frontiere, Raskin & Owen 2017)
+ * from the moments m0, m1, m2 and their gradients, solved in FP64, and the CRK
+ * density rho_i = sum_j m_j A_i (1 + B_i.x_ij) W(r_ij, H_j)  (warpSPHCore
+ * crk_moments / crk_density via computeCRKFactors, schemes/crkSPH.py:61). */
+int sph_crk_factors(const SphParams* p, int64_t n, const float* x, const float* H,
+                    const float* m, const float* V,
+                    const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                    float* A, float* B, float* gradA, float* gradB, float* rho_out,
+                    void* stream);
+
+/* Ideal-gas EOS (modules/eos/idealGas.py:6-38 with u and rho given). */
+int sph_eos_ideal_gas(const SphParams* p, int64_t n, const float* u, const float* rho,
+                      float* A_out, float* P_out, float* c_out, void* stream);
+
+/* CRK velocity gradient DvDx[i][a][b] = sum_j V_j (v_j^a - v_i^a) dW^R_ij/dx^b
+ * (scatter support, difference form; schemes/crkSPH.py:158-172 incl. the .mT),
+ * drhodt = -tr(DvDx) rho.  When div_out/vsig_out are non-null the same pass also
+ * computes the Cullen-Dehnen divergence (super-symmetric, m_j/rho_j volumes;
+ * modules/shockCapturing/CullenDehnen2010.py:246-257) and the signal velocity
+ * max_j (c_bar - mu_ij) (modules/shockCapturing/wp_vsig.py:11-90). */
+int sph_grad_v(const SphParams* p, int64_t n, const float* x, const float* H, const float* m,
+               const float* rho, const float* V, const float* A, const float* B,
+               const float* gradA, const float* gradB, const float* v, const float* c,
+               const int32_t* offs, const int32_t* cnt, const int32_t* list,
+               float* DvDx_out, float* drhodt_out, float* div_out, float* vsig_out,
+               void* stream);
+
+/* Cullen & Dehnen 2010 switch (modules/shockCapturing/CullenDehnen2010.py:218-331):
+ * R pass (gather interpolation of m_j sgn(div_j)), Xi limiter, A_i, alpha_loc,
+ * and the alpha0 relaxation with tau = h/(2*0.05*v_sig*xi).  div_prev is the
+ * state's previous divergence, alpha0_prev the state's alpha0s.  Outputs the
+ * new alphas (the reference returns alpha0s as alphas, crkSPH.py:195-200). */
+int sph_switch_cullen(const SphParams* p, int64_t n, const float* x, const float* H,
+                      const float* m, const float* rho, const float* div, const float* div_prev,
+                      const float* vsig, const float* alpha0_prev, const float* dt,
+                      const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                      float* alpha_out, float* R_out, void* stream);
+
+/* Balsara 1995 switch alpha = clamp(|div v| / (|div v| + |curl v| + 1e-4 c), 0, 1)
+ * with CRK difference-form divergence and curl (formula restated from the comment
+ * at schemes/crkSPH.py:132-133; the reference dispatcher rejects it,
+ * modules/shockCapturing/wrapper.py:25-32). DvDx from sph_grad_v. */
+int sph_switch_balsara(const SphParams* p, int64_t n, const float* DvDx, const float* c,
+                       float* alpha_out, void* stream);
+
+/* CRKSPH momentum and energy RHS in one pair pass:
+ * modules/crk/accel.py:15-250 (dv/dt and the pairwise ap_ij, av_ij [nnz, dim]) and
+ * modules/crk/dudt.py:15-229 (du/dt).  Any of dvdt_out, dudt_out, ap_ij, av_ij may
+ * be null.  With p->kahan the per-particle sums are Neumaier-compensated. */
+int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
+                       const float* m, const float* rho, const float* V,
+                       const float* A, const float* B, const float* gradA, const float* gradB,
+                       const float* v, const float* c, const float* P, const float* DvDx,
+                       const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                       float* dvdt_out, float* dudt_out, float* ap_ij, float* av_ij,
+                       void* stream);
+/* Same pass, separate names for callers that bind the reference's two wrappers
+ * computeCrkSPHAccelWarp (modules/crk/accel.py:391) and computeCrkSPHdudtWarp
+ * (modules/crk/dudt.py:364). */
+int sph_crk_accel(const SphParams* p, int64_t n, const float* x, const float* H,
+                  const float* m, const float* rho, const float* V,
+                  const float* A, const float* B, const float* gradA, const float* gradB,
+                  const float* v, const float* c, const float* P, const float* DvDx,
+                  const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                  float* dvdt_out, float* ap_ij, float* av_ij, void* stream);
+int sph_crk_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
+                 const float* m, const float* rho, const float* V,
+                 const float* A, const float* B, const float* gradA, const float* gradB,
+                 const float* v, const float* c, const float* P, const float* DvDx,
+                 const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                 float* dudt_out, void* stream);
+
+/* Pairwise energy-partition fraction f_ij (modules/compSPH/balance.py:17-154) for
+ * the six energy schemes, evaluated at v_half = v + dt/2 dvdt (schemes/crkSPH.py:341-363). */
+int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const float* rho,
+                        const float* P, const float* u, const float* v, const float* dvdt,
+                        const float* dt, const int32_t* offs, const int32_t* cnt,
+                        const int32_t* list, const float* ap_ij, const float* av_ij,
+                        float* f_ij_out, void* stream);
+
+/* ---------------------------------------------------------------- (d) integrator and dt */
+/* CFL time step (modules/timestep/compressible.py:12-61): dt = min_i cfl*min(H)/(c_i xi),
+ * clamped to [min_dt, max_dt] and, when dt_prev != null, to <= dt_growth*dt_prev.
+ * c is computed from u by the ideal-gas EOS.  dt_out is device memory of at least
+ * 4 floats: dt_out[0] receives dt, dt_out[1..2] are reduction scratch. */
+int sph_cfl_dt(const SphParams* p, int64_t n, const float* H, const float* u, const float* rho,
+               const float* dt_prev, float* dt_out, void* stream);
+
+/* Runge-Kutta stage combination y = y0 + dt * sum_k w_k K_k for `nk` derivative
+ * arrays (each [count] floats), optional periodic wrap of positions into the domain
+ * when wrap_dim > 0 (count = n*wrap_dim).  Weights are host doubles, dt is device. */
+int sph_rk_combine(const SphParams* p, int64_t count, const float* y0, int32_t nk,
+                   const float* const* k_ptrs, const double* weights, const float* dt,
+                   int32_t wrap_dim, float* y_out, void* stream);
+
+/* Compatible-energy finalize (systems/compSPH.py:100-111 and
+ * modules/compSPH/multistep.py:52-94): v_half = v0 + dt/2 sum_s b_s dvdt_s,
+ * du_i = sum_s b_s sum_j f_ij^s (v_half_j - v_half_i).(ap_ij^s + av_ij^s)
+ * (PdV: f_ij ap + 1/2 av), u = u0 + du*dt.  Per-stage arrays are passed as arrays
+ * of device pointers (host arrays of length nstages).  du_out must hold
+ * n*(1+dim) floats: du in the first n, the half-step velocity as scratch after it. */
+int sph_finalize_compatible_energy(const SphParams* p, int64_t n, int32_t nstages,
+                                   const double* weights, const float* dt,
+                                   const float* v0, const float* u0,
+                                   const float* const* dvdt_s,
+                                   const int32_t* const* offs_s, const int32_t* const* cnt_s,
+                                   const int32_t* const* list_s,
+                                   const float* const* f_ij_s, const float* const* ap_ij_s,
+                                   const float* const* av_ij_s,
+                                   float* u_out, float* du_out, void* stream);
+
+/* Mass, momentum, kinetic, internal and total energy sums in FP64 (device double[6+dim]):
+ * [M, KE, IE, E, px, py, pz]; used for conservation checks. */
+int sph_conservation_sums(const SphParams* p, int64_t n, const float* m, const float* v,
+                          const float* u, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WARPSPH_B200_H */

@@ -1,0 +1,237 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+The oracle restates the reference's algorithms in plain C (``sph_oracle.c``); this
+module exposes it on numpy arrays.  Only ``tests/``, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` import it: the product (``warpsph_b200``) never
+does, and never falls back to it.
+
+Two precisions are available: ``Oracle('f32')`` computes every float operation in
+single precision (tight parity with the GPU), ``Oracle('f64')`` in double (the
+"all-FP64 oracle" for error and drift measurements).  The neighbour search always
+runs in single precision in both, so both produce the GPU's exact lists.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+BUILD = HERE / "_build"
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+def build(force: bool = False) -> None:
+    """Compiles liboracle32.so / liboracle64.so with the committed Makefile."""
+    args = ["make", "-C", str(HERE)]
+    if force:
+        args.append("-B")
+    r = subprocess.run(args, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
+
+
+def _nullable(arrtype):
+    """ndpointer that also accepts None (passed as NULL)."""
+    class _N(arrtype):  # type: ignore[misc, valid-type]
+        @classmethod
+        def from_param(cls, obj):
+            if obj is None:
+                return None
+            return super().from_param(obj)
+    return _N
+
+
+class Oracle:
+    def __init__(self, precision: str = "f64"):
+        if precision not in ("f32", "f64"):
+            raise ValueError("precision must be 'f32' or 'f64'")
+        lib_path = BUILD / ("liboracle32.so" if precision == "f32" else "liboracle64.so")
+        if not lib_path.exists():
+            build()
+        self.lib = C.CDLL(str(lib_path))
+        self.precision = precision
+        self.dtype = np.float32 if precision == "f32" else np.float64
+        rp = _f32p if precision == "f32" else _f64p
+        rpn = _nullable(rp)
+        self._rp = rp
+        L = self.lib
+        L.oracle_real_size.restype = C.c_int
+        assert L.oracle_real_size() == np.dtype(self.dtype).itemsize
+        P = C.c_void_p
+        i64 = C.c_int64
+        L.oracle_neighbors_build.argtypes = [P, i64, _f32p, _f32p, i64, _i32p, _u32p, _i32p, _i32p, _i32p,
+                                             _nullable(_i32p), i64, C.POINTER(C.c_int64)]
+        L.oracle_density.argtypes = [P, i64, C.c_int, rp, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_adaptive_h_iter.argtypes = [P, i64, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rpn]
+        L.oracle_crk_volume.argtypes = [P, i64, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_crk_factors.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rp, rpn]
+        L.oracle_eos_ideal_gas.argtypes = [P, i64, rp, rp, rpn, rpn, rpn]
+        L.oracle_grad_v.argtypes = [P, i64, rp, rp, rpn, rp, rp, rp, rp, rp, rp, rp, rpn, _i32p, _i32p, _i32p,
+                                    rp, rpn, rpn, rpn]
+        real_c = C.c_float if precision == "f32" else C.c_double
+        self._real_c = real_c
+        L.oracle_switch_cullen.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, rp, rp, real_c, _i32p, _i32p, _i32p, rp, rpn]
+        L.oracle_switch_balsara.argtypes = [P, i64, rp, rp, rp]
+        L.oracle_crk_accel_dudt.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, rp, rp, rp, rp, rp, rp, rp,
+                                            _i32p, _i32p, _i32p, rpn, rpn, rpn, rpn]
+        L.oracle_compsph_balance.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, real_c, _i32p, _i32p, _i32p, rp, rp, rp]
+        L.oracle_cfl_dt.argtypes = [P, i64, rp, rp, real_c, C.c_int]
+        L.oracle_cfl_dt.restype = real_c
+        L.oracle_finalize_compatible_energy.argtypes = [P, i64, C.c_int, P, real_c, rp, rp, P, P, P, P, P, P, P, rp, rpn]
+        L.oracle_kernel_eval.argtypes = [C.c_int, C.c_int, i64, rp, real_c, rp, rp, rp]
+
+    # ------------------------------------------------------------------ helpers
+    def arr(self, a) -> np.ndarray:
+        return np.ascontiguousarray(np.asarray(a), dtype=self.dtype)
+
+    @staticmethod
+    def _p(params) -> C.c_void_p:
+        return C.c_void_p(C.addressof(params))
+
+    # ------------------------------------------------------------------ neighbour search
+    def neighbors(self, params, x, H, cell_capacity: int, list_capacity: int | None = None) -> dict:
+        x32 = np.ascontiguousarray(np.asarray(x), dtype=np.float32)
+        H32 = np.ascontiguousarray(np.asarray(H), dtype=np.float32)
+        n = H32.shape[0]
+        si = np.zeros(n, np.int32); sk = np.zeros(n, np.uint32); grid = np.zeros(8, np.int32)
+        offs = np.zeros(n, np.int32); cnt = np.zeros(n, np.int32)
+        nnz = C.c_int64(0)
+        # count first
+        self.lib.oracle_neighbors_build(self._p(params), n, x32, H32, cell_capacity, si, sk, grid, offs, cnt, None, 0, C.byref(nnz))
+        cap = nnz.value if list_capacity is None else list_capacity
+        lst = np.zeros(max(cap, 1), np.int32)
+        self.lib.oracle_neighbors_build(self._p(params), n, x32, H32, cell_capacity, si, sk, grid, offs, cnt, lst, cap, C.byref(nnz))
+        return dict(sort_index=si, sorted_keys=sk, grid=grid, offsets=offs, counts=cnt, list=lst[: nnz.value], nnz=nnz.value)
+
+    # ------------------------------------------------------------------ pair operations
+    def density(self, params, mode, x, H, m, nb) -> np.ndarray:
+        n = len(H)
+        out = np.zeros(n, self.dtype)
+        self.lib.oracle_density(self._p(params), n, mode, self.arr(x), self.arr(H), self.arr(m), nb["offsets"], nb["counts"], nb["list"], out)
+        return out
+
+    def adaptive_h_iter(self, params, x, H, m, nb, hb):
+        n = len(H)
+        rho = np.zeros(n, self.dtype); Hn = np.zeros(n, self.dtype); ratio = np.zeros(n, self.dtype)
+        self.lib.oracle_adaptive_h_iter(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), nb["offsets"], nb["counts"], nb["list"],
+                                        self.arr(hb), rho, Hn, ratio)
+        return rho, Hn, ratio
+
+    def crk_volume(self, params, x, H, nb):
+        n = len(H)
+        V = np.zeros(n, self.dtype)
+        self.lib.oracle_crk_volume(self._p(params), n, self.arr(x), self.arr(H), nb["offsets"], nb["counts"], nb["list"], V)
+        return V
+
+    def crk_factors(self, params, x, H, m, V, nb):
+        n, d = len(H), params.dim
+        A = np.zeros(n, self.dtype); B = np.zeros((n, d), self.dtype); gA = np.zeros((n, d), self.dtype)
+        gB = np.zeros((n, d, d), self.dtype); rho = np.zeros(n, self.dtype)
+        self.lib.oracle_crk_factors(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(V), nb["offsets"], nb["counts"],
+                                    nb["list"], A, B, gA, gB, rho)
+        return A, B, gA, gB, rho
+
+    def eos(self, params, u, rho):
+        n = len(u)
+        A = np.zeros(n, self.dtype); P = np.zeros(n, self.dtype); c = np.zeros(n, self.dtype)
+        self.lib.oracle_eos_ideal_gas(self._p(params), n, self.arr(u), self.arr(rho), A, P, c)
+        return A, P, c
+
+    def grad_v(self, params, x, H, m, rho, V, A, B, gA, gB, v, c, nb, cullen: bool = True):
+        n, d = len(H), params.dim
+        G = np.zeros((n, d, d), self.dtype); drho = np.zeros(n, self.dtype)
+        div = np.zeros(n, self.dtype) if cullen else None
+        vs = np.zeros(n, self.dtype) if cullen else None
+        self.lib.oracle_grad_v(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(V), self.arr(A),
+                               self.arr(B), self.arr(gA), self.arr(gB), self.arr(v), self.arr(c), nb["offsets"], nb["counts"], nb["list"],
+                               G, drho, div, vs)
+        return G, drho, div, vs
+
+    def switch_cullen(self, params, x, H, m, rho, div, div_prev, vsig, alpha0, dt, nb):
+        n = len(H)
+        al = np.zeros(n, self.dtype); R = np.zeros(n, self.dtype)
+        self.lib.oracle_switch_cullen(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(div),
+                                      self.arr(div_prev), self.arr(vsig), self.arr(alpha0), float(dt), nb["offsets"], nb["counts"],
+                                      nb["list"], al, R)
+        return al, R
+
+    def switch_balsara(self, params, G, c):
+        n = len(c)
+        al = np.zeros(n, self.dtype)
+        self.lib.oracle_switch_balsara(self._p(params), n, self.arr(G), self.arr(c), al)
+        return al
+
+    def crk_accel_dudt(self, params, x, H, m, rho, V, A, B, gA, gB, v, c, P, G, nb):
+        n, d = len(H), params.dim
+        nnz = int(nb["list"].shape[0])
+        dvdt = np.zeros((n, d), self.dtype); dudt = np.zeros(n, self.dtype)
+        ap = np.zeros((max(nnz, 1), d), self.dtype); av = np.zeros((max(nnz, 1), d), self.dtype)
+        self.lib.oracle_crk_accel_dudt(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(V), self.arr(A),
+                                       self.arr(B), self.arr(gA), self.arr(gB), self.arr(v), self.arr(c), self.arr(P), self.arr(G),
+                                       nb["offsets"], nb["counts"], nb["list"], dvdt, dudt, ap, av)
+        return dvdt, dudt, ap[:nnz], av[:nnz]
+
+    def balance(self, params, m, rho, P, u, v, dvdt, dt, nb, ap, av):
+        n = len(m)
+        nnz = int(nb["list"].shape[0])
+        f = np.zeros(max(nnz, 1), self.dtype)
+        self.lib.oracle_compsph_balance(self._p(params), n, self.arr(m), self.arr(rho), self.arr(P), self.arr(u), self.arr(v), self.arr(dvdt),
+                                        float(dt), nb["offsets"], nb["counts"], nb["list"], self.arr(ap).reshape(-1), self.arr(av).reshape(-1), f)
+        return f[:nnz]
+
+    def cfl_dt(self, params, H, u, dt_prev=None) -> float:
+        return float(self.lib.oracle_cfl_dt(self._p(params), len(H), self.arr(H), self.arr(u), float(dt_prev or 0.0), 1 if dt_prev else 0))
+
+    def finalize(self, params, weights, dt, v0, u0, stages):
+        """stages: list of dicts with dvdt, nb, f, ap, av (numpy)."""
+        n = len(u0)
+        ns = len(stages)
+        keep = []
+
+        def ptrs(arrs):
+            a = (C.c_void_p * ns)(*[x.ctypes.data for x in arrs])
+            keep.append(a)
+            keep.extend(arrs)
+            return C.cast(a, C.c_void_p)
+
+        dv = [self.arr(s["dvdt"]) for s in stages]
+        offs = [np.ascontiguousarray(s["nb"]["offsets"]) for s in stages]
+        cnt = [np.ascontiguousarray(s["nb"]["counts"]) for s in stages]
+        lst = [np.ascontiguousarray(s["nb"]["list"]) for s in stages]
+        f = [self.arr(s["f"]) for s in stages]
+        ap = [self.arr(s["ap"]) for s in stages]
+        av = [self.arr(s["av"]) for s in stages]
+        w = (C.c_double * ns)(*weights)
+        u = np.zeros(n, self.dtype); du = np.zeros(n, self.dtype)
+        self.lib.oracle_finalize_compatible_energy(self._p(params), n, ns, C.cast(w, C.c_void_p), float(dt), self.arr(v0), self.arr(u0),
+                                                   ptrs(dv), ptrs(offs), ptrs(cnt), ptrs(lst), ptrs(f), ptrs(ap), ptrs(av), u, du)
+        return u, du
+
+    def kernel_eval(self, kernel, dim, r, H):
+        r = self.arr(r)
+        W = np.zeros_like(r); dWdr = np.zeros_like(r); dWdH = np.zeros_like(r)
+        self.lib.oracle_kernel_eval(kernel, dim, len(r), r, float(H), W, dWdr, dWdH)
+        return W, dWdr, dWdH
+
+
+_cache: dict[str, Oracle] = {}
+
+
+def get(precision: str = "f64") -> Oracle:
+    if precision not in _cache:
+        _cache[precision] = Oracle(precision)
+    return _cache[precision]
+
+
+if __name__ == "__main__":  # pragma: no cover
+    build(force=bool(os.environ.get("FORCE")))
+    print("oracle built:", sorted(p.name for p in BUILD.glob("*.so")))

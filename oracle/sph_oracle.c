@@ -1,0 +1,893 @@
+/*
+ * sph_oracle.c -- CPU oracle for the warpSPH per-step hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file restates, in plain C, the algorithms of the
+ * reference (wi-re/warpSPH) that the CUDA library implements, so that tests can
+ * check the GPU results.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg may load it; the product path never does.
+ *
+ * Precision: compiled twice, with REAL=float (liboracle32.so) and REAL=double
+ * (liboracle64.so).  The neighbour search always runs in float with explicitly
+ * ordered operations (no FMA contraction: built with -ffp-contract=off), so its
+ * permutation and CSR lists are bit-identical to the GPU's.
+ *
+ * Parity status: the reference-resident arithmetic (pair bodies of
+ * modules/crk/accel.py, modules/crk/dudt.py, modules/crk/limiter.py,
+ * modules/compSPH/balance.py, modules/shockCapturing (CullenDehnen2010.py, wp_vsig.py), modules/eos/idealGas.py,
+ * modules/timestep/compressible.py, modules/compSPH/multistep.py) is pinned by the
+ * golden vectors in tests/golden (generated by executing the reference's own
+ * Python source, see tests/golden/make_golden.py).  The parts that live in the
+ * absent warpSPHCore / warpSPHIntegrators packages (kernel functions, neighbour
+ * search, CRK coefficients, generic SPH operators, Runge-Kutta bookkeeping) are
+ * restated from the published methods; for those, parity with the reference is
+ * unpinned.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include "../include/warpsph_b200.h"
+
+#ifndef REAL
+#define REAL double
+#endif
+typedef REAL real;
+
+#define PI_R ((real)3.14159265358979323846)
+
+static inline real wmin(real a, real b) { return a < b ? a : b; }   /* Warp builtin min */
+static inline real wmax(real a, real b) { return a > b ? a : b; }   /* Warp builtin max */
+static inline real rsqrt_safe(real x) { return (real)sqrt((double)(x > 0 ? x : 0)); }
+#if defined(ORACLE_FLOAT)
+#define SQRT sqrtf
+#define EXP expf
+#define POW powf
+#define FABS fabsf
+#define FLOOR floorf
+#else
+#define SQRT sqrt
+#define EXP exp
+#define POW pow
+#define FABS fabs
+#define FLOOR floor
+#endif
+
+/* ------------------------------------------------------------------ parameters */
+typedef struct {
+    int dim, kernel;
+    real dmin[3], dmax[3], L[3], halfL[3];
+    int periodic[3];
+    real vs;
+    real C_l, C_q;
+    real eta_crit, eta_fold;
+    int crk_lim, vl, vl_off, vl_on;
+    real gamma;
+    int energy_scheme, limit_xi, kahan;
+    real alpha_min, alpha_max, beta_xi;
+    real target_neighbors;
+    real cfl, min_dt, max_dt, dt_growth;
+    real kscale, kxi;
+} OP;
+
+static double kscale_tab(int kernel, int dim) {
+    static const double t[3][3] = {{1.620185175, 1.897366596, 1.936491673},
+                                   {1.936491673, 2.171240593, 2.207940217},
+                                   {2.207940217, 2.415229458, 2.449489743}};
+    return t[kernel - 1][dim - 1];
+}
+
+static OP op_from(const SphParams* p) {
+    OP o;
+    memset(&o, 0, sizeof(o));
+    o.dim = p->dim; o.kernel = p->kernel;
+    for (int a = 0; a < 3; ++a) {
+        /* float first: identical domain constants to the GPU's float parameters */
+        float mn = (float)p->domain_min[a], mx = (float)p->domain_max[a], L = (float)(p->domain_max[a] - p->domain_min[a]);
+        o.dmin[a] = (real)mn; o.dmax[a] = (real)mx; o.L[a] = (real)L; o.halfL[a] = (real)(0.5f * L);
+        o.periodic[a] = p->periodic[a] ? 1 : 0;
+    }
+    o.vs = (real)p->verlet_scale;
+    o.C_l = (real)p->C_l; o.C_q = (real)p->C_q;
+    o.eta_crit = (real)p->eta_crit; o.eta_fold = (real)p->eta_fold;
+    o.crk_lim = p->enable_crk_limiter; o.vl = p->enable_vanleer_limiter; o.vl_off = p->force_vanleer_off; o.vl_on = p->force_vanleer_on;
+    o.gamma = (real)p->gamma; o.energy_scheme = p->energy_scheme; o.limit_xi = p->limit_xi; o.kahan = p->kahan;
+    o.alpha_min = (real)p->alpha_min; o.alpha_max = (real)p->alpha_max; o.beta_xi = (real)p->beta_xi;
+    o.target_neighbors = (real)p->target_neighbors;
+    o.cfl = (real)p->cfl; o.min_dt = (real)p->min_dt; o.max_dt = (real)p->max_dt; o.dt_growth = (real)p->dt_growth;
+    o.kscale = (real)kscale_tab(p->kernel, p->dim);
+    o.kxi = o.kscale;
+    return o;
+}
+
+/* ------------------------------------------------------------------ kernels
+ * Wendland (1995) functions with support radius H, q = r/H, normalisations C_d
+ * (Dehnen & Aly 2012):  W = C_d/H^d k(q),  dk/dq = -q p(q). */
+static real kernel_C(int K, int D) {
+    if (K == 1) return D == 1 ? (real)1.25 : (D == 2 ? (real)(7.0 / 3.14159265358979323846) : (real)(21.0 / (2.0 * 3.14159265358979323846)));
+    if (K == 2) return D == 1 ? (real)1.5 : (D == 2 ? (real)(9.0 / 3.14159265358979323846) : (real)(495.0 / (32.0 * 3.14159265358979323846)));
+    return D == 1 ? (real)1.71875 : (D == 2 ? (real)(78.0 / (7.0 * 3.14159265358979323846)) : (real)(1365.0 / (64.0 * 3.14159265358979323846)));
+}
+static void kernel_kp(int K, int D, real q, real* k, real* p) {
+    real t = 1 - q;
+    if (K == 1) {
+        if (D == 1) { real t2 = t * t; *k = t2 * t * (1 + 3 * q); *p = 12 * t2; }
+        else { real t3 = t * t * t; *k = t3 * t * (1 + 4 * q); *p = 20 * t3; }
+    } else if (K == 2) {
+        if (D == 1) { real t4 = (t * t) * (t * t); *k = t4 * t * (1 + 5 * q + 8 * q * q); *p = 14 * (1 + 4 * q) * t4; }
+        else { real t5 = (t * t) * (t * t) * t; *k = t5 * t * (1 + 6 * q + ((real)35 / (real)3) * q * q); *p = ((real)56 / (real)3) * (1 + 5 * q) * t5; }
+    } else {
+        if (D == 1) { real t6 = (t * t) * (t * t) * (t * t); *k = t6 * t * (1 + 7 * q + 19 * q * q + 21 * q * q * q); *p = 6 * (3 + 18 * q + 35 * q * q) * t6; }
+        else { real t7 = (t * t) * (t * t) * (t * t) * t; *k = t7 * t * (1 + 8 * q + 25 * q * q + 32 * q * q * q); *p = 22 * (1 + 7 * q + 16 * q * q) * t7; }
+    }
+}
+static real ipowD(real h, int D) { return D == 1 ? h : (D == 2 ? h * h : h * h * h); }
+
+static real kW(const OP* o, real r, real H) {
+    real q = r / H;
+    if (!(q < 1)) return 0;
+    real k, p; kernel_kp(o->kernel, o->dim, q, &k, &p);
+    return kernel_C(o->kernel, o->dim) / ipowD(H, o->dim) * k;
+}
+static void kWG(const OP* o, const real* x, real r, real H, real* W, real* g) {
+    real q = r / H;
+    int D = o->dim;
+    if (!(q < 1)) { *W = 0; for (int a = 0; a < D; ++a) g[a] = 0; return; }
+    real k, p; kernel_kp(o->kernel, D, q, &k, &p);
+    real cH = kernel_C(o->kernel, D) / ipowD(H, D);
+    *W = cH * k;
+    real s = -cH * p / (H * H);
+    for (int a = 0; a < D; ++a) g[a] = s * x[a];
+}
+static void kWdH(const OP* o, real r, real H, real* W, real* dWdH) {
+    real q = r / H;
+    int D = o->dim;
+    if (!(q < 1)) { *W = 0; *dWdH = 0; return; }
+    real k, p; kernel_kp(o->kernel, D, q, &k, &p);
+    real cH = kernel_C(o->kernel, D) / ipowD(H, D);
+    *W = cH * k;
+    *dWdH = -cH / H * ((real)D * k - q * q * p);
+}
+static real kW_mode(const OP* o, real r, real Hi, real Hj, int mode) {
+    switch (mode) {
+        case SPH_SUPPORT_GATHER: return kW(o, r, Hi);
+        case SPH_SUPPORT_SCATTER: return kW(o, r, Hj);
+        case SPH_SUPPORT_SYMMETRIC: return kW(o, r, (real)0.5 * (Hi + Hj));
+        case SPH_SUPPORT_SUPERSYMMETRIC: return kW(o, r, wmax(Hi, Hj));
+        default: return (real)0.5 * (kW(o, r, Hi) + kW(o, r, Hj));
+    }
+}
+
+/* minimum-image x_ij = x_i - x_j (warpSPHCore computeDistanceVec, restated) */
+static void dist_vec(const OP* o, const real* xi, const real* xj, real* d) {
+    for (int a = 0; a < o->dim; ++a) {
+        real v = xi[a] - xj[a];
+        if (o->periodic[a]) {
+            if (v > o->halfL[a]) v = v - o->L[a];
+            else if (v < -o->halfL[a]) v = v + o->L[a];
+        }
+        d[a] = v;
+    }
+}
+static real dotD(const real* a, const real* b, int D) { real s = a[0] * b[0]; for (int k = 1; k < D; ++k) s += a[k] * b[k]; return s; }
+
+/* CRK corrected gradient (Frontiere, Raskin & Owen 2017); gB[a*D+g] = dB^a/dx^g */
+static void crk_grad(int D, const real* x, real W, const real* gW, real A, const real* B, const real* gA, const real* gB, real* out) {
+    real bx = 1 + dotD(B, x, D);
+    for (int g = 0; g < D; ++g) {
+        real gbx = gB[0 * D + g] * x[0];
+        for (int a = 1; a < D; ++a) gbx += gB[a * D + g] * x[a];
+        out[g] = A * bx * gW[g] + A * B[g] * W + gA[g] * bx * W + A * gbx * W;
+    }
+}
+
+/* ------------------------------------------------------------------ neighbour search (float) */
+static uint32_t spread2(uint32_t x) {
+    x &= 0x0000ffffu; x = (x | (x << 8)) & 0x00ff00ffu; x = (x | (x << 4)) & 0x0f0f0f0fu;
+    x = (x | (x << 2)) & 0x33333333u; x = (x | (x << 1)) & 0x55555555u; return x;
+}
+static uint32_t spread3(uint32_t x) {
+    x &= 0x000003ffu; x = (x | (x << 16)) & 0x030000ffu; x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u; x = (x | (x << 2)) & 0x09249249u; return x;
+}
+static uint32_t morton(int D, const int* c) {
+    if (D == 1) return (uint32_t)c[0];
+    if (D == 2) return spread2((uint32_t)c[0]) | (spread2((uint32_t)c[1]) << 1);
+    return spread3((uint32_t)c[0]) | (spread3((uint32_t)c[1]) << 1) | (spread3((uint32_t)c[2]) << 2);
+}
+static int max_bits_for(int dim, int64_t cap) {
+    int lb = 0;
+    while (((int64_t)1 << (lb + 1)) <= cap) ++lb;
+    int mb = lb / dim;
+    int lim = dim == 1 ? 30 : (dim == 2 ? 16 : 10);
+    return mb > lim ? lim : mb;
+}
+
+typedef struct { int G[3]; float inv[3]; float dmin[3], L[3], halfL[3]; int periodic[3]; } NGrid;
+
+static void cell_coords_f(const NGrid* g, int D, const float* x, int* c) {
+    for (int a = 0; a < D; ++a) {
+        float t = (x[a] - g->dmin[a]) * g->inv[a];
+        int ci = (int)floorf(t);
+        c[a] = ci < 0 ? 0 : (ci >= g->G[a] ? g->G[a] - 1 : ci);
+    }
+}
+
+/* Verlet list, same definition and canonical order as the GPU (see header). */
+int oracle_neighbors_build(const SphParams* p, int64_t n, const float* x, const float* H, int64_t cell_capacity,
+                           int32_t* sort_index, uint32_t* sorted_keys, int32_t* grid_out,
+                           int32_t* offsets, int32_t* counts, int32_t* list, int64_t list_capacity, int64_t* nnz_out) {
+    int D = p->dim;
+    NGrid g;
+    memset(&g, 0, sizeof(g));
+    float Lmax = 0.f, hmax = 0.f;
+    for (int a = 0; a < 3; ++a) {
+        g.dmin[a] = (float)p->domain_min[a];
+        g.L[a] = (float)(p->domain_max[a] - p->domain_min[a]);
+        g.halfL[a] = 0.5f * g.L[a];
+        g.periodic[a] = p->periodic[a] ? 1 : 0;
+        g.G[a] = 1;
+    }
+    for (int a = 0; a < D; ++a) Lmax = fmaxf(Lmax, g.L[a]);
+    for (int64_t i = 0; i < n; ++i) hmax = fmaxf(hmax, H[i]);
+    float vs = (float)p->verlet_scale;
+    float cell = (vs * hmax) * 1.001f + Lmax * 1e-6f;
+    int mb = max_bits_for(D, cell_capacity);
+    int bits[3] = {0, 0, 0};
+    for (int a = 0; a < D; ++a) {
+        float f = floorf(g.L[a] / cell);
+        int gmax = 1 << mb;
+        int gi = (f >= (float)gmax) ? gmax : (f < 1.f ? 1 : (int)f);
+        int b = 0;
+        while ((1 << b) < gi) ++b;
+        g.G[a] = gi; bits[a] = b;
+        g.inv[a] = (float)gi / g.L[a];
+    }
+    if (grid_out) {
+        for (int a = 0; a < 3; ++a) { grid_out[a] = g.G[a]; grid_out[3 + a] = bits[a]; }
+        memcpy(&grid_out[6], &cell, 4);
+        grid_out[7] = D;
+    }
+    int64_t ncells = (int64_t)1 << (mb * D);
+    uint32_t* keys = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+    int32_t* begin = (int32_t*)calloc((size_t)ncells + 1, sizeof(int32_t));
+    for (int64_t i = 0; i < n; ++i) {
+        int c[3];
+        cell_coords_f(&g, D, x + i * D, c);
+        keys[i] = morton(D, c);
+        begin[keys[i] + 1]++;
+    }
+    for (int64_t c = 0; c < ncells; ++c) begin[c + 1] += begin[c];
+    int32_t* cur = (int32_t*)malloc(sizeof(int32_t) * (size_t)ncells);
+    memcpy(cur, begin, sizeof(int32_t) * (size_t)ncells);
+    for (int64_t i = 0; i < n; ++i) sort_index[cur[keys[i]]++] = (int32_t)i;   /* stable */
+    for (int64_t k = 0; k < n; ++k) sorted_keys[k] = keys[sort_index[k]];
+
+    int64_t total = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+            total = 0;
+            for (int64_t i = 0; i < n; ++i) { offsets[i] = (int32_t)total; total += counts[i]; }
+            *nnz_out = total;
+            if (total > list_capacity) break;
+        }
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) {
+            const float* xi = x + i * D;
+            float Hi = H[i];
+            int c[3];
+            cell_coords_f(&g, D, xi, c);
+            uint32_t sk[27];
+            int nk = 0;
+            int NS = D == 1 ? 3 : (D == 2 ? 9 : 27);
+            for (int s = 0; s < NS; ++s) {
+                int o[3] = {s % 3 - 1, (s / 3) % 3 - 1, (s / 9) % 3 - 1};
+                int cc[3];
+                int ok = 1;
+                for (int a = 0; a < D; ++a) {
+                    int v = c[a] + o[a];
+                    if (v < 0 || v >= g.G[a]) {
+                        if (g.periodic[a]) v = (v + g.G[a]) % g.G[a]; else ok = 0;
+                    }
+                    cc[a] = v;
+                }
+                if (!ok) continue;
+                uint32_t kk = morton(D, cc);
+                int dup = 0;
+                for (int q = 0; q < nk; ++q) if (sk[q] == kk) { dup = 1; break; }
+                if (dup) continue;
+                int m = nk - 1;
+                while (m >= 0 && sk[m] > kk) { sk[m + 1] = sk[m]; --m; }
+                sk[m + 1] = kk;
+                ++nk;
+            }
+            int cntv = 0;
+            int32_t base = pass ? offsets[i] : 0;
+            for (int q = 0; q < nk; ++q) {
+                for (int32_t k = begin[sk[q]]; k < begin[sk[q] + 1]; ++k) {
+                    int32_t j = sort_index[k];
+                    const float* xj = x + (int64_t)j * D;
+                    float R = vs * fmaxf(Hi, H[j]);
+                    float r2 = 0.f;
+                    for (int a = 0; a < D; ++a) {
+                        float d = xi[a] - xj[a];
+                        if (g.periodic[a]) {
+                            if (d > g.halfL[a]) d = d - g.L[a];
+                            else if (d < -g.halfL[a]) d = d + g.L[a];
+                        }
+                        r2 = a == 0 ? d * d : r2 + d * d;
+                    }
+                    if (r2 < R * R) {
+                        if (pass) list[base + cntv] = j;
+                        ++cntv;
+                    }
+                }
+            }
+            if (!pass) counts[i] = cntv;
+        }
+    }
+    free(keys); free(begin); free(cur);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ density (modules/density/density.py:16-28) */
+int oracle_density(const SphParams* p, int64_t n, int mode, const real* x, const real* H, const real* m,
+                   const int32_t* offs, const int32_t* cnt, const int32_t* list, real* rho) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real s = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            s += m[j] * kW_mode(&o, rsqrt_safe(dotD(d, d, D)), H[i], H[j], mode);
+        }
+        rho[i] = s;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ adaptive support
+ * modules/adaptiveSupport/optimalSupportMonaghan.py:52-59 (computeH/F) and :87-125 (Newton step),
+ * modules/adaptiveSupport/wp_omega.py:40-60 (Omega = 1 - sum dh/drho m_j dW/dh),
+ * utils/support.py:24-44 (volumeToSupportHelper). */
+static real volume_to_support(real V, real nH, int D) {
+    if (D == 1) return nH * V / 2;
+    if (D == 2) return SQRT(nH * V / PI_R);
+    return POW(nH * V / PI_R * 3 / 4, (real)1 / (real)3);
+}
+int oracle_adaptive_h_iter(const SphParams* p, int64_t n, const real* x, const real* H, const real* m,
+                           const int32_t* offs, const int32_t* cnt, const int32_t* list, const real* hb,
+                           real* rho_out, real* H_out, real* ratio) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real rs = 0, ds = 0, Hi = H[i];
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real W, dWdH;
+            kWdH(&o, rsqrt_safe(dotD(d, d, D)), Hi, &W, &dWdH);
+            rs += m[j] * W;
+            ds += m[j] * dWdH;
+        }
+        real rho = rs;
+        real safe_rho = isfinite(rho) ? (rho > (real)1e-12 ? rho : (real)1e-12) : 1;
+        real F = Hi - volume_to_support(m[i] / safe_rho, o.target_neighbors, D);
+        real dh_drho = -Hi / (rho * (real)D);
+        real omega = 1 - dh_drho * ds;
+        if (!isfinite(omega)) omega = 0;
+        real step = F / (omega + (real)1e-6);
+        if (!isfinite(step)) step = 0;
+        real hn = Hi - step;
+        if (!isfinite(hn)) hn = Hi;
+        real lo = hb[0] * (real)0.25, hi = hb[1] * 4;
+        hn = hn < lo ? lo : (hn > hi ? hi : hn);
+        rho_out[i] = rho; H_out[i] = hn;
+        if (ratio) ratio[i] = hn / (Hi + (real)1e-6);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ CRK volume and coefficients
+ * warpSPHCore crk_volume / crk_moments / crk_density (called via computeCRKFactors,
+ * schemes/crkSPH.py:61), restated from Frontiere, Raskin & Owen 2017. */
+int oracle_crk_volume(const SphParams* p, int64_t n, const real* x, const real* H, const int32_t* offs, const int32_t* cnt,
+                      const int32_t* list, real* V) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real s = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            s += kW(&o, rsqrt_safe(dotD(d, d, D)), H[j]);
+        }
+        V[i] = 1 / s;
+    }
+    return 0;
+}
+
+static double inv_sym(int D, const double* a, double* r) {
+    if (D == 1) { r[0] = 1.0 / a[0]; return a[0]; }
+    if (D == 2) {
+        double det = a[0] * a[3] - a[1] * a[2], id = 1.0 / det;
+        r[0] = a[3] * id; r[3] = a[0] * id; r[1] = -a[1] * id; r[2] = -a[2] * id;
+        return det;
+    }
+    double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+    double det = a[0] * c00 + a[1] * c01 + a[2] * c02, id = 1.0 / det;
+    r[0] = c00 * id; r[1] = (a[2] * a[7] - a[1] * a[8]) * id; r[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    r[3] = c01 * id; r[4] = (a[0] * a[8] - a[2] * a[6]) * id; r[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    r[6] = c02 * id; r[7] = (a[1] * a[6] - a[0] * a[7]) * id; r[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+    return det;
+}
+
+int oracle_crk_factors(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* V,
+                       const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                       real* Aout, real* Bout, real* gAout, real* gBout, real* rho_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real m0 = 0, s0 = 0, m1[3] = {0}, s1[3] = {0}, m2[9] = {0}, dm0[3] = {0}, dm1[9] = {0}, dm2[27] = {0};
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], gW[3], W;
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG(&o, d, rsqrt_safe(dotD(d, d, D)), H[j], &W, gW);
+            if (W == 0) continue;
+            real Vj = V[j], VW = Vj * W;
+            m0 += VW; s0 += m[j] * W;
+            for (int a = 0; a < D; ++a) {
+                m1[a] += VW * d[a];
+                s1[a] += m[j] * W * d[a];
+                dm0[a] += Vj * gW[a];
+                for (int c = 0; c < D; ++c) {
+                    m2[a * D + c] += VW * d[a] * d[c];
+                    dm1[a * D + c] += Vj * (d[a] * gW[c] + (a == c ? W : 0));
+                }
+            }
+            for (int a = 0; a < D; ++a)
+                for (int c = a; c < D; ++c)
+                    for (int g2 = 0; g2 < D; ++g2)
+                        dm2[(a * D + c) * D + g2] += Vj * (d[a] * d[c] * gW[g2] + ((a == g2 ? d[c] : 0) + (c == g2 ? d[a] : 0)) * W);
+        }
+        double M2[9], Mi[9], tr = 0;
+        for (int a = 0; a < D; ++a) { for (int c = 0; c < D; ++c) M2[a * D + c] = (double)(a <= c ? m2[a * D + c] : m2[c * D + a]); tr += M2[a * D + a]; }
+        double det = inv_sym(D, M2, Mi);
+        double sc = tr / D, sD = sc;
+        for (int a = 1; a < D; ++a) sD *= sc;
+        int ok = isfinite(det) && fabs(det) > 1e-10 * fabs(sD) && m0 > 0;
+        double A, Bv[3], gA[3], gB[9];
+        if (ok) {
+            double mb = (double)m0;
+            for (int a = 0; a < D; ++a) { double t = 0; for (int c = 0; c < D; ++c) t -= Mi[a * D + c] * (double)m1[c]; Bv[a] = t; }
+            for (int a = 0; a < D; ++a) mb += (double)m1[a] * Bv[a];
+            A = 1.0 / mb;
+            for (int g2 = 0; g2 < D; ++g2) {
+                double rhs[3];
+                for (int a = 0; a < D; ++a) {
+                    double t = (double)dm1[a * D + g2];
+                    for (int c = 0; c < D; ++c) t += (double)(a <= c ? dm2[(a * D + c) * D + g2] : dm2[(c * D + a) * D + g2]) * Bv[c];
+                    rhs[a] = t;
+                }
+                for (int a = 0; a < D; ++a) { double t = 0; for (int c = 0; c < D; ++c) t -= Mi[a * D + c] * rhs[c]; gB[a * D + g2] = t; }
+            }
+            for (int g2 = 0; g2 < D; ++g2) {
+                double t = (double)dm0[g2];
+                for (int a = 0; a < D; ++a) t += (double)dm1[a * D + g2] * Bv[a] + (double)m1[a] * gB[a * D + g2];
+                gA[g2] = -A * A * t;
+            }
+        } else {
+            double m0d = (double)m0;
+            A = 1.0 / m0d;
+            for (int a = 0; a < D; ++a) { Bv[a] = 0; gA[a] = -(double)dm0[a] / (m0d * m0d); for (int c = 0; c < D; ++c) gB[a * D + c] = 0; }
+        }
+        double rho = (double)s0;
+        for (int a = 0; a < D; ++a) rho += Bv[a] * (double)s1[a];
+        rho *= A;
+        Aout[i] = (real)A;
+        for (int a = 0; a < D; ++a) {
+            Bout[i * D + a] = (real)Bv[a]; gAout[i * D + a] = (real)gA[a];
+            for (int c = 0; c < D; ++c) gBout[i * D * D + a * D + c] = (real)gB[a * D + c];
+        }
+        if (rho_out) rho_out[i] = (real)rho;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ EOS (modules/eos/idealGas.py:16-36, u and rho given) */
+int oracle_eos_ideal_gas(const SphParams* p, int64_t n, const real* u, const real* rho, real* A, real* P, real* c) {
+    real g = (real)p->gamma;
+    for (int64_t i = 0; i < n; ++i) {
+        if (c) c[i] = SQRT(FABS(u[i]) * g * (g - 1));
+        if (P) P[i] = (g - 1) * rho[i] * u[i];
+        if (A) A[i] = u[i] * (g - 1) * POW(rho[i], 1 - g);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ velocity gradient, Cullen div, v_sig
+ * schemes/crkSPH.py:158-172 (CRK difference gradient, scatter, then .mT),
+ * modules/shockCapturing/CullenDehnen2010.py:246-257 (divergence, super-symmetric),
+ * modules/shockCapturing/wp_vsig.py:55-90 (signal velocity max-reduction). */
+int oracle_grad_v(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                  const real* V, const real* A, const real* B, const real* gA, const real* gB, const real* v, const real* c,
+                  const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                  real* DvDx, real* drhodt, real* div_out, real* vsig_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real G[9] = {0}, div = 0, vsig = 0;
+        const real* vi = v + i * D;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], gW[3], W, gR[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real r = rsqrt_safe(dotD(d, d, D));
+            const real* vj = v + (int64_t)j * D;
+            kWG(&o, d, r, H[j], &W, gW);
+            if (W != 0) {
+                crk_grad(D, d, W, gW, A[i], B + i * D, gA + i * D, gB + i * D * D, gR);
+                for (int a = 0; a < D; ++a) {
+                    real dv = V[j] * (vj[a] - vi[a]);
+                    for (int g2 = 0; g2 < D; ++g2) G[a * D + g2] += dv * gR[g2];
+                }
+            }
+            if (div_out) {
+                real Hs = wmax(H[i], H[j]);
+                if (r < Hs) {
+                    real W2, g2v[3];
+                    kWG(&o, d, r, Hs, &W2, g2v);
+                    real vol = m[j] / rho[j], s = 0;
+                    for (int a = 0; a < D; ++a) s += (vj[a] - vi[a]) * g2v[a];
+                    div += vol * s;
+                }
+                if (r < o.vs * Hs) {
+                    real mu = 0;
+                    for (int a = 0; a < D; ++a) mu += (vi[a] - vj[a]) * d[a];
+                    mu = mu / (r + (real)1e-14 * H[i]);
+                    real vsv = (real)0.5 * (c[i] + c[j]) - mu;
+                    if (mu > 0) vsv = 0;
+                    vsig = wmax(vsig, vsv);
+                }
+            }
+        }
+        for (int q = 0; q < D * D; ++q) DvDx[i * D * D + q] = G[q];
+        if (drhodt) { real tr = 0; for (int a = 0; a < D; ++a) tr += G[a * D + a]; drhodt[i] = -tr * rho[i]; }
+        if (div_out) { div_out[i] = div; if (vsig_out) vsig_out[i] = FABS(vsig); }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ Cullen & Dehnen switch
+ * modules/shockCapturing/CullenDehnen2010.py:121-164 (R), :166-191 (Xi), :281-314 (alpha update). */
+int oracle_switch_cullen(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                         const real* div, const real* div_prev, const real* vsig, const real* alpha0_prev, real dt,
+                         const int32_t* offs, const int32_t* cnt, const int32_t* list, real* alpha_out, real* R_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real s = 0, Hi = H[i];
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real W = kW(&o, rsqrt_safe(dotD(d, d, D)), Hi);
+            if (W == 0) continue;
+            real sg = div[j] > 0 ? 1 : (div[j] < 0 ? -1 : 0);
+            s += m[j] / rho[j] * (rho[j] * sg) * W;
+        }
+        real R = 1 / rho[i] * s;
+        real omr = 1 - R, omr2 = omr * omr;
+        real nom = o.beta_xi * (omr2 * omr2) * div[i];
+        real Xi = o.limit_xi ? (nom * nom + (real)1e-14 * Hi) / (nom * nom + 0 + (real)1e-14 * Hi)
+                             : (nom * nom) / (nom * nom + 0 + (real)1e-14 * Hi);
+        real ddiv = (div[i] - div_prev[i]) / dt;
+        real Ai = Xi * (-ddiv > 0 ? -ddiv : 0);
+        real vs = vsig[i];
+        real scaling = Hi * Hi * Ai / (vs * vs + Hi * Hi * Ai + (real)1e-14 * Hi);
+        real al = o.alpha_max * scaling;
+        al = al < o.alpha_min ? o.alpha_min : (al > o.alpha_max ? o.alpha_max : al);
+        real a0 = alpha0_prev[i];
+        real tau = Hi * (1 / o.kxi) / (2 * (real)0.05 * vs);
+        real adot = (al - a0) / tau;
+        a0 = al > a0 ? al : a0;
+        a0 = al < a0 ? a0 + adot * dt : a0;
+        a0 = a0 < o.alpha_min ? o.alpha_min : (a0 > o.alpha_max ? o.alpha_max : a0);
+        alpha_out[i] = a0;
+        if (R_out) R_out[i] = R;
+    }
+    return 0;
+}
+
+/* Balsara (commented formula at schemes/crkSPH.py:132-133) */
+int oracle_switch_balsara(const SphParams* p, int64_t n, const real* DvDx, const real* c, real* alpha) {
+    int D = p->dim;
+    for (int64_t i = 0; i < n; ++i) {
+        const real* G = DvDx + i * D * D;
+        real dv = 0, curl2 = 0;
+        for (int a = 0; a < D; ++a) dv += G[a * D + a];
+        if (D == 2) { real w = G[2] - G[1]; curl2 = w * w; }
+        if (D == 3) { real w0 = G[7] - G[5], w1 = G[2] - G[6], w2 = G[3] - G[1]; curl2 = w0 * w0 + w1 * w1 + w2 * w2; }
+        real ad = FABS(dv);
+        real b = ad / (ad + SQRT(curl2) + (real)1e-4 * c[i]);
+        alpha[i] = b < 0 ? 0 : (b > 1 ? 1 : b);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ CRK accel / dudt
+ * modules/crk/limiter.py:10-16 (limiterVL), :27-86 (computeVanLeer), :89-128 (crkLimiter);
+ * modules/crk/accel.py:65-250 (computeCrkSPHAccel_Func_i);
+ * modules/crk/dudt.py:62-229 (computeCrkSPHdudt_Func_i). */
+static real limiter_vl(real x) {
+    if (x <= 0) return 0;
+    real vL = 2 / (1 + x);
+    return x * vL * vL;
+}
+static real sgn_pos(real x) { return x >= 0 ? 1 : -1; }
+static real van_leer(int D, const real* xij_, const real* Gi, const real* Gj) {
+    real h[3], ci[3], cj[3];
+    for (int a = 0; a < D; ++a) h[a] = (real)0.5 * xij_[a];
+    for (int a = 0; a < D; ++a) {
+        ci[a] = Gi[a * D] * h[0]; cj[a] = Gj[a * D] * h[0];
+        for (int b = 1; b < D; ++b) { ci[a] += Gi[a * D + b] * h[b]; cj[a] += Gj[a * D + b] * h[b]; }
+    }
+    real gi = dotD(ci, h, D), gj = dotD(cj, h, D);
+    real ri = gi / (sgn_pos(gj) * FABS(gj));
+    real rj = gj / (sgn_pos(gi) * FABS(gi));
+    if (ri != ri) ri = 1;
+    if (rj != rj) rj = 1;
+    return limiter_vl(wmin(ri, rj));
+}
+static real crk_limiter(int D, const real* xij, real hi, real hj, real eta_crit, real eta_fold) {
+    real ni = 0, nj = 0;
+    for (int a = 0; a < D; ++a) { real ei = xij[a] / hi, ej = xij[a] / hj; ni += ei * ei; nj += ej * ej; }
+    real eta = wmin(rsqrt_safe(ni), rsqrt_safe(nj));
+    real f = 1;
+    if (eta < eta_crit) { real t = (eta - eta_crit) / eta_fold; f = EXP(-(t * t)); }
+    return f;
+}
+static void kahan_add(real* s, real* c, real x, int comp) {
+    if (!comp) { *s += x; return; }
+    real t = *s + x;
+    if (FABS(*s) >= FABS(x)) *c += (*s - t) + x; else *c += (x - t) + *s;
+    *s = t;
+}
+
+int oracle_crk_accel_dudt(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                          const real* V, const real* A, const real* B, const real* gA, const real* gB, const real* v,
+                          const real* c, const real* Pr, const real* DvDx,
+                          const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                          real* dvdt, real* dudt, real* ap, real* av) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        const real *xi = x + i * D, *vi = v + i * D, *Gi = DvDx + i * D * D;
+        real Hi = H[i], mi = m[i], rhoi = rho[i], Vi = V[i], ci = c[i], Pi = Pr[i];
+        real smooth_i = Hi / o.kscale;
+        real acc[3] = {0, 0, 0}, accc[3] = {0, 0, 0}, du = 0, duc = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, xi, x + (int64_t)j * D, d);
+            real r2 = dotD(d, d, D);
+            real Hj = H[j], Hm = wmax(Hi, Hj);
+            if (!(r2 < Hm * Hm)) {
+                if (ap) for (int a = 0; a < D; ++a) ap[(int64_t)k * D + a] = 0;
+                if (av) for (int a = 0; a < D; ++a) av[(int64_t)k * D + a] = 0;
+                continue;
+            }
+            real r = rsqrt_safe(r2);
+            const real *vj = v + (int64_t)j * D, *Gj = DvDx + (int64_t)j * D * D;
+            real rhoj = rho[j], Vj = V[j], cj = c[j], Pj = Pr[j];
+            real factor = 1;
+            if (o.crk_lim) factor = crk_limiter(D, d, Hi, Hj, o.eta_crit, o.eta_fold);
+            real phi = 0;
+            if (o.vl) phi = van_leer(D, d, Gi, Gj) * factor;
+            if (o.vl_off) phi = 0;
+            if (o.vl_on) phi = 1;
+            phi = wmax(wmin(phi, 1), 0);
+            real Gix[3], Gjx[3];
+            for (int a = 0; a < D; ++a) {
+                Gix[a] = Gi[a * D] * d[0]; Gjx[a] = Gj[a * D] * d[0];
+                for (int b = 1; b < D; ++b) { Gix[a] += Gi[a * D + b] * d[b]; Gjx[a] += Gj[a * D + b] * d[b]; }
+            }
+            real hp = phi / 2, vdi[3], vdja[3], vdjd[3];
+            for (int a = 0; a < D; ++a) {
+                vdi[a] = vi[a] - hp * Gix[a];
+                vdja[a] = vj[a] + hp * Gjx[a];
+                vdjd[a] = vj[a] + hp * (-Gjx[a]);
+            }
+            real Wi, gWi[3], gri[3], Wj, gWj[3], grj[3], xji[3], gij[3];
+            kWG(&o, d, r, Hj, &Wi, gWi);
+            crk_grad(D, d, Wi, gWi, A[i], B + i * D, gA + i * D, gB + i * D * D, gri);
+            for (int a = 0; a < D; ++a) xji[a] = -d[a];
+            kWG(&o, xji, r, Hi, &Wj, gWj);
+            crk_grad(D, xji, Wj, gWj, A[j], B + (int64_t)j * D, gA + (int64_t)j * D, gB + (int64_t)j * D * D, grj);
+            for (int a = 0; a < D; ++a) gij[a] = (real)0.5 * (gri[a] - grj[a]);
+            real smooth_j = Hj / o.kscale;
+            real ee_i = 0, ee_j = 0, mia = 0, mja = 0, mid = 0, mjd = 0;
+            for (int a = 0; a < D; ++a) {
+                real ei = d[a] / smooth_i, ej = d[a] / smooth_j;
+                ee_i += ei * ei; ee_j += ej * ej;
+                real da = vdi[a] - vdja[a], dd = vdi[a] - vdjd[a];
+                mia += da * ei; mja += da * ej; mid += dd * ei; mjd += dd * ej;
+            }
+            real den_i = ee_i + (real)1.0e-7 * smooth_i * smooth_i, den_j = ee_j + (real)1.0e-7 * smooth_j * smooth_j;
+            mia = wmin(0, mia / den_i); mja = wmin(0, mja / den_j);
+            mid = wmin(0, mid / den_i); mjd = wmin(0, mjd / den_j);
+            real Qia = rhoi * (-o.C_l * ci * mia + o.C_q * mia * mia), Qja = rhoj * (-o.C_l * cj * mja + o.C_q * mja * mja);
+            real Qid = rhoi * (-o.C_l * ci * mid + o.C_q * mid * mid), Qjd = rhoj * (-o.C_l * cj * mjd + o.C_q * mjd * mjd);
+            real dotu = 0;
+            for (int a = 0; a < D; ++a) {
+                real pt = -(Pi + Pj) * gij[a] * Vi * Vj / mi;
+                real vt = -(Qia + Qja) * Vj * 1 * gij[a] * Vi / mi;
+                if (ap) ap[(int64_t)k * D + a] = pt;
+                if (av) av[(int64_t)k * D + a] = vt;
+                kahan_add(&acc[a], &accc[a], pt + vt, o.kahan);
+                dotu += (vi[a] - vj[a]) * gij[a];
+            }
+            real pTerm = Pj * dotu * Vi * Vj / mi;
+            real vTerm = (real)0.5 * (Qid + Qjd) * 1 * dotu * Vi * Vj / mi;
+            kahan_add(&du, &duc, pTerm + vTerm, o.kahan);
+        }
+        if (dvdt) for (int a = 0; a < D; ++a) dvdt[i * D + a] = acc[a] + accc[a];
+        if (dudt) dudt[i] = du + duc;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ energy partition (modules/compSPH/balance.py:62-154) */
+static real sgn0(real x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
+int oracle_compsph_balance(const SphParams* p, int64_t n, const real* m, const real* rho, const real* Pr, const real* u,
+                           const real* v, const real* dvdt, real dt, const int32_t* offs, const int32_t* cnt,
+                           const int32_t* list, const real* ap, const real* av, real* fout) {
+    OP o = op_from(p);
+    int D = o.dim;
+    real hdt = (real)0.5 * dt;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real vi[3];
+        for (int a = 0; a < D; ++a) vi[a] = v[i * D + a] + hdt * dvdt[i * D + a];
+        real mi = m[i], rhoi = rho[i], Pi = Pr[i], ui = u[i];
+        real si = o.energy_scheme == SPH_ENERGY_CRK ? Pi / POW(rhoi, o.gamma) : 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real mj = m[j], rhoj = rho[j], Pj = Pr[j], uj = u[j];
+            real dE = 0;
+            for (int a = 0; a < D; ++a)
+                dE += ((v[(int64_t)j * D + a] + hdt * dvdt[(int64_t)j * D + a]) - vi[a]) * (ap[(int64_t)k * D + a] + av[(int64_t)k * D + a]);
+            dE = mi * dE * dt;
+            real uji = uj - ui, f = (real)0.5;
+            int sch = o.energy_scheme;
+            if (sch == SPH_ENERGY_EQUALWORK) f = (real)0.5;
+            else if (sch == SPH_ENERGY_PDV) f = (Pi / (rhoi * rhoi)) / (Pi / (rhoi * rhoi) + Pj / (rhoj * rhoj));
+            else if (sch == SPH_ENERGY_DIMINISHING) { real un = FABS(uji); f = (real)0.5 * (1 + (uji * sgn0(dE)) / (un + 1 / (1 + un))); }
+            else if (sch == SPH_ENERGY_MONOTONIC || sch == SPH_ENERGY_HYBRID) {
+                real Aq = dE / (uji + (real)1.0e-14);
+                real Bq = Aq >= 0 ? Aq / mi : Aq / mj;
+                real t1 = wmax(0, sgn0(Bq));
+                real t2 = mi / (dE + (real)1.0e-14) * ((dE + mi * ui + mj * uj) / (mi + mj) - ui);
+                real fm = FABS(Bq) <= 1 ? t1 : t2;
+                if (sch == SPH_ENERGY_MONOTONIC) f = fm;
+                else {
+                    real un = FABS(uji);
+                    real fsm = (real)0.5 * (1 + (uji * sgn0(dE)) / (un + 1 / (1 + un)));
+                    real chi = FABS(uji) / (FABS(ui) + FABS(uj) + (real)1.0e-14);
+                    f = chi * fm + (1 - chi) * fsm;
+                }
+            } else if (sch == SPH_ENERGY_CRK) {
+                real sj = Pj / POW(rhoj, o.gamma);
+                real smin = wmin(FABS(si), FABS(sj)), smax = wmax(FABS(si), FABS(sj));
+                int mA = FABS(si - sj) == 0;
+                int mB = (dE >= 0 && si >= sj) || (dE < 0 && si < sj);
+                int mC = (dE >= 0 && si < sj) || (dE < 0 && si >= sj);
+                f = (real)0.5;
+                if (mA) f = (real)0.5;
+                if (!mA && mB) f = smin / (smin + smax + (real)1.0e-14);
+                if (!mA && !mB && mC) f = smax / (smin + smax + (real)1.0e-14);
+                f = wmax(0, wmin(1, f));
+            }
+            fout[k] = f;
+        }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ CFL (modules/timestep/compressible.py:18-61) */
+real oracle_cfl_dt(const SphParams* p, int64_t n, const real* H, const real* u, real dt_prev, int has_prev) {
+    OP o = op_from(p);
+    real hmin = H[0], best = 0;
+    for (int64_t i = 1; i < n; ++i) hmin = H[i] < hmin ? H[i] : hmin;
+    for (int64_t i = 0; i < n; ++i) {
+        real cs = SQRT(FABS(u[i]) * o.gamma * (o.gamma - 1));
+        real dt = o.cfl * hmin / (cs * o.kxi);
+        if (i == 0 || dt < best) best = dt;
+    }
+    best = best < o.min_dt ? o.min_dt : (best > o.max_dt ? o.max_dt : best);
+    if (has_prev && best > dt_prev) best = best < o.dt_growth * dt_prev ? best : o.dt_growth * dt_prev;
+    return best;
+}
+
+/* ------------------------------------------------------------------ compatible energy
+ * modules/compSPH/multistep.py:52-94 and systems/compSPH.py:100-111. */
+int oracle_finalize_compatible_energy(const SphParams* p, int64_t n, int ns, const double* w, real dt, const real* v0,
+                                      const real* u0, const real* const* dvdt_s, const int32_t* const* offs_s,
+                                      const int32_t* const* cnt_s, const int32_t* const* list_s, const real* const* f_s,
+                                      const real* const* ap_s, const real* const* av_s, real* u_out, real* du_out) {
+    int D = p->dim;
+    int pdv = p->energy_scheme == SPH_ENERGY_PDV;
+    real* vh = (real*)malloc(sizeof(real) * (size_t)(n * D > 0 ? n * D : 1));
+    for (int64_t q = 0; q < n * D; ++q) {
+        real fa = 0;
+        for (int s = 0; s < ns; ++s) fa += (real)w[s] * dvdt_s[s][q];
+        vh[q] = v0[q] + (real)0.5 * fa * dt;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real du = 0;
+        for (int s = 0; s < ns; ++s) {
+            real acc = 0, ws = (real)w[s];
+            for (int32_t k = offs_s[s][i]; k < offs_s[s][i] + cnt_s[s][i]; ++k) {
+                int32_t j = list_s[s][k];
+                real d1 = 0, d2 = 0;
+                for (int a = 0; a < D; ++a) {
+                    real vji = vh[(int64_t)j * D + a] - vh[i * D + a];
+                    d1 += vji * ap_s[s][(int64_t)k * D + a];
+                    d2 += vji * av_s[s][(int64_t)k * D + a];
+                }
+                real fk = f_s[s][k];
+                acc += pdv ? (ws * fk * d1 + ws * (real)0.5 * d2) : (ws * fk * (d1 + d2));
+            }
+            du += acc;
+        }
+        if (du_out) du_out[i] = du;
+        u_out[i] = u0[i] + du * dt;
+    }
+    free(vh);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ helpers exported for tests */
+int oracle_real_size(void) { return (int)sizeof(real); }
+int oracle_kernel_eval(int kernel, int dim, int64_t n, const real* r, real H, real* W, real* dWdr, real* dWdH) {
+    SphParams p;
+    memset(&p, 0, sizeof(p));
+    p.kernel = kernel; p.dim = dim;
+    OP o = op_from(&p);
+    for (int64_t i = 0; i < n; ++i) {
+        real q = r[i] / H;
+        if (!(q < 1)) { W[i] = 0; dWdr[i] = 0; dWdH[i] = 0; continue; }
+        real k, pq; kernel_kp(kernel, dim, q, &k, &pq);
+        real cH = kernel_C(kernel, dim) / ipowD(H, dim);
+        W[i] = cH * k;
+        dWdr[i] = -cH / H * q * pq;
+        real Wd, dh; kWdH(&o, r[i], H, &Wd, &dh);
+        dWdH[i] = dh;
+    }
+    return 0;
+}
+
+/* sizeof / offsetof probes so tests can check the ctypes mirror of SphParams */
+#include <stddef.h>
+int64_t oracle_params_layout(int which) {
+    switch (which) {
+        case 0: return (int64_t)sizeof(SphParams);
+        case 1: return (int64_t)offsetof(SphParams, dim);
+        case 2: return (int64_t)offsetof(SphParams, kahan);
+        case 3: return (int64_t)offsetof(SphParams, target_neighbors);
+        case 4: return (int64_t)offsetof(SphParams, energy_scheme);
+        default: return -1;
+    }
+}

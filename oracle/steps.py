@@ -1,0 +1,152 @@
+"""CPU oracle of the full CRKSPH step (test infrastructure only).
+
+Mirrors, on numpy arrays and the C oracle kernels, the reference's step order:
+schemes/crkSPH.py:19-366 (one right-hand-side evaluation),
+modules/adaptiveSupport/optimalSupportMonaghan.py:62-150 (adaptive support),
+systems/compSPH.py:87-129 + modules/compSPH/multistep.py:52-94 (finalize with
+compatible energy), and explicit Runge-Kutta staging (Heun RK2 / classic RK4; the
+reference's integrator package is absent, so the tableaux are restated).
+
+A state is a dict of numpy arrays with the reference's field names.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import oracle as _oracle
+
+TABLEAUX = {
+    "explicitEuler": ([[]], [1.0], [0.0]),
+    "rungeKutta2": ([[], [1.0]], [0.5, 0.5], [0.0, 1.0]),
+    "rungeKutta4": ([[], [0.5], [0.0, 0.5], [0.0, 0.0, 1.0]], [1 / 6, 1 / 3, 1 / 3, 1 / 6], [0.0, 0.5, 0.5, 1.0]),
+}
+
+SWITCH_NONE, SWITCH_CULLEN, SWITCH_BALSARA = 0, 1, 2
+
+
+def cell_capacity_for(n: int, dim: int) -> int:
+    want = max(1024, n * (1 << dim))
+    cap = 1
+    while cap < want:
+        cap <<= 1
+    return min(cap, 1 << 24)
+
+
+class CRKSPHOracle:
+    def __init__(self, params, precision: str = "f32", adaptive_iterations: int = 1, adaptive_threshold: float = 1e-3,
+                 switch: int = SWITCH_CULLEN, compatible_energy: bool = True, adaptive: bool = True):
+        self.o = _oracle.get(precision)
+        self.p = params
+        self.dt_ = self.o.dtype
+        self.iters = adaptive_iterations
+        self.thr = adaptive_threshold
+        self.switch = switch
+        self.compatible = compatible_energy
+        self.adaptive = adaptive
+        self.dim = int(params.dim)
+
+    # --------------------------------------------------------------- helpers
+    def nb(self, x, H):
+        return self.o.neighbors(self.p, x.astype(np.float32), H.astype(np.float32), cell_capacity_for(len(H), self.dim))
+
+    def wrap(self, x):
+        p = self.p
+        x = x.copy()
+        for a in range(self.dim):
+            if p.periodic[a]:
+                mn, mx = np.float32(p.domain_min[a]), np.float32(p.domain_max[a])
+                L = np.float32(p.domain_max[a] - p.domain_min[a])
+                col = x[:, a]
+                hi = col >= mx
+                lo = col < mn
+                col[hi] = col[hi] - L.astype(self.dt_)
+                col[lo] = col[lo] + L.astype(self.dt_)
+        return x
+
+    def combine(self, y0, ks, ws, dt, wrap=False):
+        f = self.dt_
+        s = np.zeros_like(y0, dtype=f)
+        for k, w in zip(ks, ws):
+            if w == 0.0:
+                continue
+            s = (s + (f(w) * k.astype(f)).astype(f)).astype(f)
+        y = (y0.astype(f) + (f(dt) * s).astype(f)).astype(f)
+        return self.wrap(y) if wrap else y
+
+    # --------------------------------------------------------------- adaptive support
+    def optimal_support(self, st):
+        o, p = self.o, self.p
+        x, H, m = st["positions"], st["supports"], st["masses"]
+        hb = np.array([H.min(), H.max()], dtype=self.dt_)
+        for it in range(self.iters):
+            nb = self.nb(x, H)
+            rho, Hn, ratio = o.adaptive_h_iter(p, x, H, m, nb, hb)
+            hb = np.array([Hn.min(), Hn.max()], dtype=self.dt_)
+            H = Hn
+            if it < self.iters - 1 and np.abs(ratio - 1).max() < self.thr:
+                break
+        nb = self.nb(x, H)
+        rho = o.density(p, 0, x, H, m, nb)
+        return rho, H
+
+    # --------------------------------------------------------------- one RHS evaluation
+    def rhs(self, st, dt):
+        o, p = self.o, self.p
+        st = dict(st)
+        if self.adaptive:
+            st["densities"], st["supports"] = self.optimal_support(st)
+        x, H, m, v, u = st["positions"], st["supports"], st["masses"], st["velocities"], st["internalEnergies"]
+        nb = self.nb(x, H)
+        V = o.crk_volume(p, x, H, nb)
+        A, B, gA, gB, rho = o.crk_factors(p, x, H, m, V, nb)
+        st["densities"] = rho
+        st["entropies"], st["pressures"], st["soundspeeds"] = o.eos(p, u, rho)
+        c, P = st["soundspeeds"], st["pressures"]
+        cullen = self.switch == SWITCH_CULLEN
+        G, drho, div, vs = o.grad_v(p, x, H, m, rho, V, A, B, gA, gB, v, c, nb, cullen=cullen)
+        if cullen:
+            st["alphas"], _ = o.switch_cullen(p, x, H, m, rho, div, st["divergence"], vs, st["alpha0s"], dt, nb)
+        elif self.switch == SWITCH_BALSARA:
+            st["alphas"] = o.switch_balsara(p, G, c)
+        dvdt, dudt, ap, av = o.crk_accel_dudt(p, x, H, m, rho, V, A, B, gA, gB, v, c, P, G, nb)
+        st["divergence"] = (-drho / rho).astype(self.dt_)
+        st["ap_ij"], st["av_ij"] = ap, av
+        st["f_ij"] = o.balance(p, m, rho, P, u, v, dvdt, dt, nb, ap, av)
+        upd = dict(dxdt=v, dvdt=dvdt, dudt=dudt, drhodt=drho)
+        extras = dict(V=V, A=A, B=B, gradA=gA, gradB=gB, DvDx=G, div_cd=div, vsig=vs)
+        return upd, nb, st, extras
+
+    # --------------------------------------------------------------- integrator step
+    def step(self, st0, dt, scheme: str = "rungeKutta2"):
+        a, b, _c = TABLEAUX[scheme]
+        updates, rvs = [], []
+        prev = dict(st0)
+        for s in range(len(b)):
+            Ss = dict(prev)
+            if s > 0:
+                Ss["positions"] = self.combine(st0["positions"], [u["dxdt"] for u in updates], a[s], dt, wrap=True)
+                Ss["velocities"] = self.combine(st0["velocities"], [u["dvdt"] for u in updates], a[s], dt)
+                Ss["internalEnergies"] = self.combine(st0["internalEnergies"], [u["dudt"] for u in updates], a[s], dt)
+            upd, nb, Sout, _ = self.rhs(Ss, dt)
+            updates.append(upd)
+            rvs.append((nb, Sout))
+            prev = Sout
+        Sf = dict(prev)
+        Sf["positions"] = self.combine(st0["positions"], [u["dxdt"] for u in updates], b, dt, wrap=True)
+        Sf["velocities"] = self.combine(st0["velocities"], [u["dvdt"] for u in updates], b, dt)
+        Sf["internalEnergies"] = self.combine(st0["internalEnergies"], [u["dudt"] for u in updates], b, dt)
+        if self.compatible:
+            stages = [dict(dvdt=u["dvdt"], nb=nb, f=S["f_ij"], ap=S["ap_ij"], av=S["av_ij"]) for u, (nb, S) in zip(updates, rvs)]
+            Sf["internalEnergies"], _ = self.o.finalize(self.p, b, dt, st0["velocities"], st0["internalEnergies"], stages)
+        return Sf, updates, rvs
+
+
+def state_to_numpy(state, dtype=np.float32) -> dict:
+    """Copies the tensors of a CompSPHState-like object into numpy arrays."""
+    out = {}
+    for name in ("positions", "velocities", "supports", "masses", "densities", "internalEnergies", "pressures", "soundspeeds",
+                 "divergence", "alpha0s", "alphas", "entropies"):
+        t = getattr(state, name, None)
+        if t is not None:
+            out[name] = t.detach().cpu().numpy().astype(dtype)
+    return out

@@ -1,0 +1,189 @@
+"""GPU kernels (through the C ABI) against the CPU oracle on identical seeded inputs.
+
+Integer/indexing work is compared bit for bit; floating-point outputs with the
+tolerances written at each assertion (FP32 GPU vs FP32 oracle: differences come
+only from FMA contraction and operation order; vs the FP64 oracle: FP32 rounding)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle
+from oracle.steps import cell_capacity_for
+from tests.cases import assert_close, make_params, make_particles
+from warpsph_b200 import core, ops
+from warpsph_b200.enumTypes import EnergyScheme
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(1, 400), (2, 40), (3, 14)]
+
+
+def to_gpu(P, dev):
+    return {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in P.items()}
+
+
+def nb_numpy(adj):
+    return dict(offsets=adj.neighborOffsets.cpu().numpy(), counts=adj.numNeighbors.cpu().numpy(),
+                list=adj.neighborList.cpu().numpy())
+
+
+@pytest.mark.parametrize("dim,n_side", CASES)
+@pytest.mark.parametrize("periodic", [True, False])
+def test_neighbors_bit_exact(cuda, dim, n_side, periodic):
+    cfg, sch, p = make_params(dim, periodic=periodic)
+    P = make_particles(dim, n_side, periodic=periodic, seed=10 + dim)
+    G = to_gpu(P, cuda)
+    adj = ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale)
+    ref = oracle.get("f32").neighbors(p, P["positions"], P["supports"], cell_capacity_for(len(P["supports"]), dim))
+    assert adj.nnz == ref["nnz"]
+    assert np.array_equal(adj.sortIndex.cpu().numpy(), ref["sort_index"])
+    assert np.array_equal(adj.sortedKeys.cpu().numpy().view(np.uint32), ref["sorted_keys"])
+    assert np.array_equal(adj.grid.cpu().numpy(), ref["grid"])
+    assert np.array_equal(adj.neighborOffsets.cpu().numpy(), ref["offsets"])
+    assert np.array_equal(adj.numNeighbors.cpu().numpy(), ref["counts"])
+    assert np.array_equal(adj.neighborList.cpu().numpy(), ref["list"])
+    i, j = adj.i.cpu().numpy(), adj.j.cpu().numpy()
+    assert np.array_equal(j, ref["list"]) and np.array_equal(np.bincount(i, minlength=len(ref["counts"])), ref["counts"])
+
+
+def test_neighbors_capacity_overflow_is_recovered(cuda):
+    cfg, sch, p = make_params(2)
+    P = make_particles(2, 30, seed=5)
+    G = to_gpu(P, cuda)
+    from warpsph_b200 import ops as _ops
+    _ops._nb_cache.cap_hint[(cuda.index or 0, 900, 2)] = 16   # force an overflow on the first attempt
+    adj = ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale)
+    ref = oracle.get("f32").neighbors(p, P["positions"], P["supports"], cell_capacity_for(900, 2))
+    assert adj.nnz == ref["nnz"] and np.array_equal(adj.neighborList.cpu().numpy(), ref["list"])
+
+
+def test_neighbors_reject_nonpositive_support(cuda):
+    cfg, sch, p = make_params(2)
+    P = make_particles(2, 10, seed=5)
+    G = to_gpu(P, cuda)
+    H = G["supports"].clone()
+    H[3] = 0.0
+    with pytest.raises(RuntimeError, match="finite and positive"):
+        ops.buildVerletList(G["positions"], H, p, p.verlet_scale)
+
+
+def test_neighbors_reuse_unchanged_prior(cuda):
+    cfg, sch, p = make_params(2)
+    G = to_gpu(make_particles(2, 12, seed=1), cuda)
+    a = ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale)
+    assert ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale, a) is a
+    x2 = G["positions"].clone()
+    assert ops.buildVerletList(x2, G["supports"], p, p.verlet_scale, a) is not a
+
+
+def pipeline_inputs(dim, n_side, dev, seed=0, kernel=core.KernelFunctions.Wendland4, periodic=True, **kw):
+    cfg, sch, p = make_params(dim, kernel=kernel, periodic=periodic, **kw)
+    P = make_particles(dim, n_side, periodic=periodic, seed=seed)
+    G = to_gpu(P, dev)
+    adj = ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale)
+    return cfg, sch, p, P, G, adj
+
+
+@pytest.mark.parametrize("dim,n_side", CASES)
+@pytest.mark.parametrize("kernel", [core.KernelFunctions.Wendland2, core.KernelFunctions.Wendland4])
+def test_density_and_adaptive_support(cuda, dim, n_side, kernel):
+    cfg, sch, p, P, G, adj = pipeline_inputs(dim, n_side, cuda, kernel=kernel)
+    nb = nb_numpy(adj)
+    for precision, tol in (("f32", 2e-6), ("f64", 2e-6)):
+        o = oracle.get(precision)
+        for mode in (core.SupportScheme.Gather, core.SupportScheme.Scatter, core.SupportScheme.SuperSymmetric,
+                     core.SupportScheme.KernelMeanSymmetric, core.SupportScheme.Symmetric):
+            rho = ops.density(p, G["positions"], G["supports"], G["masses"], adj, mode).cpu().numpy()
+            ref = o.density(p, ops._SUPPORT[mode], P["positions"], P["supports"], P["masses"], nb)
+            assert_close(rho, ref, tol, tol, f"density {mode} {precision}")
+    hb = ops.minmax(G["supports"])
+    rho, Hn, ratio = ops.adaptive_h_iter(p, G["positions"], G["supports"], G["masses"], adj, hb)
+    r_rho, r_H, r_ratio = oracle.get("f32").adaptive_h_iter(p, P["positions"], P["supports"], P["masses"], nb, hb.cpu().numpy())
+    assert_close(rho.cpu().numpy(), r_rho, 2e-6, 2e-6, "adaptive rho")
+    assert_close(Hn.cpu().numpy(), r_H, 1e-5, 1e-5, "adaptive H")
+    assert np.array_equal(hb.cpu().numpy(), np.array([P["supports"].min(), P["supports"].max()], np.float32))
+
+
+@pytest.mark.parametrize("dim,n_side", CASES)
+def test_crk_pipeline(cuda, dim, n_side):
+    cfg, sch, p, P, G, adj = pipeline_inputs(dim, n_side, cuda, seed=3)
+    nb = nb_numpy(adj)
+    o32, o64 = oracle.get("f32"), oracle.get("f64")
+    x, H, m, v, u = (P[k] for k in ("positions", "supports", "masses", "velocities", "internalEnergies"))
+    # CRK volume and coefficients
+    V = ops.crk_volume(p, G["positions"], G["supports"], adj)
+    assert_close(V.cpu().numpy(), o32.crk_volume(p, x, H, nb), 2e-6, 2e-6, "V")
+    Vn = V.cpu().numpy()
+    crk, rho = ops.crk_factors(p, G["positions"], G["supports"], G["masses"], V, adj)
+    rA, rB, rgA, rgB, rrho = o64.crk_factors(p, x, H, m, Vn, nb)
+    assert_close(crk.A.cpu().numpy(), rA, 1e-4, 1e-4, "A")
+    assert_close(crk.B.cpu().numpy(), rB, 1e-3, 1e-3, "B")
+    assert_close(crk.gradA.cpu().numpy(), rgA, 1e-3, 1e-3, "gradA")
+    assert_close(crk.gradB.cpu().numpy(), rgB, 2e-3, 2e-3, "gradB")
+    assert_close(rho.cpu().numpy(), rrho, 1e-5, 1e-5, "CRK rho")
+    # EOS
+    A_, Pr, c = ops.eos_ideal_gas(p, G["internalEnergies"], rho)
+    rA_, rP, rc = o32.eos(p, u, rho.cpu().numpy())
+    assert_close(Pr.cpu().numpy(), rP, 1e-6, 1e-6, "P")
+    assert_close(c.cpu().numpy(), rc, 1e-6, 1e-6, "c")
+    assert_close(A_.cpu().numpy(), rA_, 1e-5, 1e-5, "A(entropy)")
+    # velocity gradient + Cullen divergence + v_sig (inputs from the GPU so errors do not compound)
+    cn = {k: t.cpu().numpy() for k, t in dict(A=crk.A, B=crk.B, gA=crk.gradA, gB=crk.gradB, rho=rho, c=c, P=Pr).items()}
+    Gv, drho, div, vs = ops.grad_v(p, G["positions"], G["supports"], G["masses"], rho, V, crk, G["velocities"], c, adj, True)
+    rG, rdrho, rdiv, rvs = o32.grad_v(p, x, H, m, cn["rho"], Vn, cn["A"], cn["B"], cn["gA"], cn["gB"], v, cn["c"], nb, True)
+    assert_close(Gv.cpu().numpy(), rG, 1e-4, 1e-4, "DvDx")
+    assert_close(drho.cpu().numpy(), rdrho, 1e-4, 1e-4, "drhodt")
+    assert_close(div.cpu().numpy(), rdiv, 1e-4, 1e-4, "Cullen div")
+    assert_close(vs.cpu().numpy(), rvs, 1e-6, 1e-6, "v_sig")
+    # Cullen switch
+    div_prev = torch.from_numpy(rdiv * 0.9 + 0.01).to(cuda)
+    a0 = torch.full_like(rho, 0.5)
+    al, R = ops.switch_cullen(p, G["positions"], G["supports"], G["masses"], rho, div, div_prev, vs, a0, 1e-3, adj, want_R=True)
+    ral, rR = o32.switch_cullen(p, x, H, m, cn["rho"], div.cpu().numpy(), div_prev.cpu().numpy(), vs.cpu().numpy(),
+                                np.full(len(H), 0.5, np.float32), 1e-3, nb)
+    assert_close(R.cpu().numpy(), rR, 1e-5, 1e-5, "R")
+    assert_close(al.cpu().numpy(), ral, 1e-4, 1e-4, "alphas")
+    bal = ops.switch_balsara(p, Gv, c)
+    assert_close(bal.cpu().numpy(), o32.switch_balsara(p, Gv.cpu().numpy(), cn["c"]), 1e-5, 1e-5, "Balsara")
+    # fused accel + dudt with pair arrays
+    Gn = Gv.cpu().numpy()
+    dvdt, dudt, ap, av = ops.crk_accel_dudt(p, G["positions"], G["supports"], G["masses"], rho, V, crk, G["velocities"], c, Pr,
+                                            Gv, adj)
+    rdv, rdu, rap, rav = o32.crk_accel_dudt(p, x, H, m, cn["rho"], Vn, cn["A"], cn["B"], cn["gA"], cn["gB"], v, cn["c"], cn["P"],
+                                            Gn, nb)
+    assert_close(ap.cpu().numpy(), rap, 1e-4, 1e-4, "ap_ij")
+    assert_close(av.cpu().numpy(), rav, 1e-3, 1e-3, "av_ij")
+    assert_close(dvdt.cpu().numpy(), rdv, 1e-3, 1e-3, "dvdt")
+    assert_close(dudt.cpu().numpy(), rdu, 1e-3, 1e-3, "dudt")
+    # against the FP64 oracle too (FP32 rounding only)
+    r64 = o64.crk_accel_dudt(p, x, H, m, cn["rho"], Vn, cn["A"], cn["B"], cn["gA"], cn["gB"], v, cn["c"], cn["P"], Gn, nb)
+    assert_close(dvdt.cpu().numpy(), r64[0], 2e-3, 2e-3, "dvdt vs f64")
+    # balance, all energy schemes
+    for es in EnergyScheme:
+        p.energy_scheme = es.value
+        f = ops.compsph_balance(p, G["masses"], rho, Pr, G["internalEnergies"], G["velocities"], dvdt, 1e-3, adj, ap, av)
+        rf = o32.balance(p, m, cn["rho"], cn["P"], u, v, dvdt.cpu().numpy(), 1e-3, nb, ap.cpu().numpy(), av.cpu().numpy())
+        fg = f.cpu().numpy()
+        mism = np.mean(np.abs(fg - rf) > 1e-4)
+        # the partition is discontinuous in sign(dE); entries where dE rounds across zero may flip
+        assert mism < 2e-3, (es, mism)
+
+
+def test_kahan_option_matches(cuda):
+    cfg, sch, p, P, G, adj = pipeline_inputs(2, 32, cuda, seed=9, kahan=True)
+    V = ops.crk_volume(p, G["positions"], G["supports"], adj)
+    crk, rho = ops.crk_factors(p, G["positions"], G["supports"], G["masses"], V, adj)
+    _, Pr, c = ops.eos_ideal_gas(p, G["internalEnergies"], rho)
+    Gv, *_ = ops.grad_v(p, G["positions"], G["supports"], G["masses"], rho, V, crk, G["velocities"], c, adj, False)
+    dv_k, du_k, _, _ = ops.crk_accel_dudt(p, G["positions"], G["supports"], G["masses"], rho, V, crk, G["velocities"], c, Pr, Gv, adj,
+                                          pair_arrays=False)
+    p.kahan = 0
+    dv, du, _, _ = ops.crk_accel_dudt(p, G["positions"], G["supports"], G["masses"], rho, V, crk, G["velocities"], c, Pr, Gv, adj,
+                                      pair_arrays=False)
+    nb = nb_numpy(adj)
+    cn = {k: t.cpu().numpy() for k, t in dict(A=crk.A, B=crk.B, gA=crk.gradA, gB=crk.gradB, rho=rho, c=c, P=Pr, G=Gv, V=V).items()}
+    r64 = oracle.get("f64").crk_accel_dudt(p, P["positions"], P["supports"], P["masses"], cn["rho"], cn["V"], cn["A"], cn["B"],
+                                           cn["gA"], cn["gB"], P["velocities"], cn["c"], cn["P"], cn["G"], nb)
+    e_k = np.abs(dv_k.cpu().numpy() - r64[0]).max()
+    e_p = np.abs(dv.cpu().numpy() - r64[0]).max()
+    assert e_k <= e_p * 1.5 + 1e-7

@@ -1,0 +1,161 @@
+"""ctypes layer over libwarpsph_b200.so (declared in include/warpsph_b200.h).
+
+Loads the in-tree shared library and exposes each C entry point with argument
+types.  There is no fallback: if the library is missing, or a call is made on
+tensors that are not CUDA float32, a RuntimeError is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import torch
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libwarpsph_b200.so"
+
+SPH_OK = 0
+STATUS_LIST_OVERFLOW = 0x1
+STATUS_NONFINITE = 0x2
+STATUS_NOT_CONVERGED = 0x4
+STATUS_TIMEOUT = 0x8
+
+SUPPORT_GATHER = 0
+SUPPORT_SCATTER = 1
+SUPPORT_SYMMETRIC = 2
+SUPPORT_SUPERSYMMETRIC = 3
+SUPPORT_KERNELMEANSYMMETRIC = 4
+
+
+class SphParams(C.Structure):
+    """Mirror of the C struct SphParams (include/warpsph_b200.h)."""
+
+    _fields_ = [
+        ("domain_min", C.c_double * 3),
+        ("domain_max", C.c_double * 3),
+        ("verlet_scale", C.c_double),
+        ("C_l", C.c_double), ("C_q", C.c_double), ("Cu_l", C.c_double), ("Cu_q", C.c_double), ("K", C.c_double),
+        ("eta_crit", C.c_double), ("eta_fold", C.c_double),
+        ("gamma", C.c_double),
+        ("alpha_min", C.c_double), ("alpha_max", C.c_double), ("beta_xi", C.c_double),
+        ("target_neighbors", C.c_double),
+        ("cfl", C.c_double), ("min_dt", C.c_double), ("max_dt", C.c_double), ("dt_growth", C.c_double),
+        ("reserved_d", C.c_double * 8),
+        ("dim", C.c_int32),
+        ("kernel", C.c_int32),
+        ("periodic", C.c_int32 * 3),
+        ("viscosity_term", C.c_int32),
+        ("monaghan_switch", C.c_int32), ("correct_xi", C.c_int32), ("scale_beta", C.c_int32),
+        ("enable_crk_limiter", C.c_int32), ("enable_vanleer_limiter", C.c_int32),
+        ("force_vanleer_off", C.c_int32), ("force_vanleer_on", C.c_int32),
+        ("energy_scheme", C.c_int32),
+        ("limit_xi", C.c_int32),
+        ("kahan", C.c_int32),
+        ("reserved_i", C.c_int32 * 8),
+    ]
+
+
+_P = C.c_void_p
+_I64 = C.c_int64
+_I32 = C.c_int32
+
+# name -> argtypes (restype is int unless listed in _RESTYPE)
+_PROTOS = {
+    "sph_version": [],
+    "sph_last_error_string": [],
+    "sph_launch_count": [],
+    "sph_kernel_constants": [_I32, _I32, _P, _P],
+    "sph_neighbors_workspace_size": [_P, _I64, _I64, _P],
+    "sph_neighbors_build": [_P, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _P, _P, _P],
+    "sph_neighbors_expand": [_I64, _P, _P, _P, _I64, _P, _P, _P],
+    "sph_density_gather": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P],
+    "sph_adaptive_h_iter": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "sph_minmax": [_I64, _P, _P, _P],
+    "sph_crk_volume": [_P, _I64, _P, _P, _P, _P, _P, _P, _P],
+    "sph_crk_factors": [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "sph_eos_ideal_gas": [_P, _I64, _P, _P, _P, _P, _P, _P],
+    "sph_grad_v": [_P, _I64] + [_P] * 19,
+    "sph_switch_cullen": [_P, _I64] + [_P] * 15,
+    "sph_switch_balsara": [_P, _I64, _P, _P, _P, _P],
+    "sph_crk_accel_dudt": [_P, _I64] + [_P] * 21,
+    "sph_crk_accel": [_P, _I64] + [_P] * 20,
+    "sph_crk_dudt": [_P, _I64] + [_P] * 18,
+    "sph_compsph_balance": [_P, _I64] + [_P] * 14,
+    "sph_cfl_dt": [_P, _I64, _P, _P, _P, _P, _P, _P],
+    "sph_rk_combine": [_P, _I64, _P, _I32, _P, _P, _P, _I32, _P, _P],
+    "sph_finalize_compatible_energy": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "sph_conservation_sums": [_P, _I64, _P, _P, _P, _P, _P],
+}
+_RESTYPE = {"sph_version": C.c_char_p, "sph_last_error_string": C.c_char_p, "sph_launch_count": C.c_int64}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libwarpsph_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(os.environ.get("WARPSPH_B200_LIB", LIB_PATH))
+    if not path.exists():
+        raise RuntimeError(
+            f"libwarpsph_b200.so not found at {path}; build it with `python -m warpsph_b200.build` "
+            "(there is no CPU fallback)")
+    L = C.CDLL(str(path))
+    for name, args in _PROTOS.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPE.get(name, C.c_int)
+    _lib = L
+    return L
+
+
+def declared_functions() -> list[str]:
+    return list(_PROTOS)
+
+
+def last_error() -> str:
+    return lib().sph_last_error_string().decode()
+
+
+def check(rc: int, what: str) -> None:
+    if rc != SPH_OK:
+        raise RuntimeError(f"{what} failed ({rc}): {last_error()}")
+
+
+def ptr(t) -> int | None:
+    """Device pointer of a CUDA tensor (None for None)."""
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"expected a torch.Tensor, got {type(t)}")
+    if not t.is_cuda:
+        raise RuntimeError("warpsph_b200 operates on CUDA tensors only (no CPU fallback)")
+    if not t.is_contiguous():
+        raise RuntimeError("warpsph_b200 requires contiguous tensors")
+    return t.data_ptr()
+
+
+def fptr(t) -> int | None:
+    if t is not None and t.dtype != torch.float32:
+        raise RuntimeError(f"expected float32 tensor, got {t.dtype}")
+    return ptr(t)
+
+
+def iptr(t) -> int | None:
+    if t is not None and t.dtype != torch.int32:
+        raise RuntimeError(f"expected int32 tensor, got {t.dtype}")
+    return ptr(t)
+
+
+def stream_ptr(device=None) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def ptr_array(ptrs) -> C.Array:
+    return (C.c_void_p * len(ptrs))(*ptrs)
+
+
+def double_array(vals) -> C.Array:
+    return (C.c_double * len(vals))(*[float(v) for v in vals])

@@ -1,0 +1,360 @@
+"""Configuration dataclasses with the reference's names, fields and defaults.
+
+Mirrors src/warpSPH/configurations/: SimulationConfig / buildConfig
+(simulationConfig.py:15-121), DiffusionParameters and ViscosityTerms
+(moduleConfigurations/diffusionParameters.py:8-37, a Warp struct in the reference,
+a plain dataclass here), ViscositySwitchConfig (moduleConfigurations/viscositySwitchParameters.py:11-26),
+CompressibleSPHConfig (compressibleConfig.py:16-30), CompSPHConfig (compSPHConfig.py:32-40),
+CRKViscosity / CRKSPHConfig (crkSPH.py:16-80), with the *ToDict / dictTo* round trips.
+``make_params`` packs a configuration into the C ABI's SphParams block.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from enum import Enum
+from typing import Any, Dict, List, Optional
+
+import torch
+
+from . import _capi
+from .core import (DomainDescription, GradientScheme, IntegrationSchemeType, KernelFunctions, LaplacianScheme,
+                   SamplingScheme, SupportScheme, buildDomainDescription, n_h_to_nH)
+from .enumTypes import AdaptiveSupportScheme, EnergyScheme, ViscositySwitch
+
+
+# ------------------------------------------------------------------ simulation config
+@dataclass
+class SimulationConfig:
+    device: torch.device = field(default_factory=lambda: torch.device("cuda:0") if torch.cuda.is_available() else torch.device("cpu"))
+    dtype: torch.dtype = torch.float32
+    domain: DomainDescription = field(default_factory=lambda: buildDomainDescription(l=2, dim=2, periodic=True))
+    dim: int = 2
+    verletScale: float = 2.0 ** 0.5
+    kernel: KernelFunctions = KernelFunctions.Wendland2
+    integrationScheme: IntegrationSchemeType = IntegrationSchemeType.rungeKutta4
+    cflFactor: float = 0.3
+    dt: Optional[float] = None
+    minDt: Optional[float] = 1e-6
+    maxDt: Optional[float] = 1e-2
+    dtGrowthFactor: Optional[float] = 1.1
+    adaptiveDt: bool = True
+    dx: Optional[float] = None
+    nx: Optional[int] = None
+    targetNeighbors: float = field(default_factory=lambda: n_h_to_nH(4, 2))
+    supportMode: SupportScheme = SupportScheme.SuperSymmetric
+    gradientMode: GradientScheme = GradientScheme.Difference
+    laplacianMode: LaplacianScheme = LaplacianScheme.Brookshaw
+    samplingScheme: SamplingScheme = SamplingScheme.regular
+
+
+def buildConfig(device=None, dtype=None, domain=None, dim=None, verletScale=None, kernel=None, integrationScheme=None,
+                cflFactor=None, dt=None, minDt=None, maxDt=None, dtGrowthFactor=None, adaptiveDt=None,
+                targetNeighbors=None, supportMode=None, gradientMode=None, laplacianMode=None, samplingScheme=None):
+    """simulationConfig.py:47-121: fills defaults and returns (config, integrator)."""
+    from .integrators import getIntegrator
+    if device is None:
+        device = torch.device("cuda:0") if torch.cuda.is_available() else torch.device("cpu")
+    dtype = torch.float32 if dtype is None else dtype
+    dim = 2 if dim is None else dim
+    domain = buildDomainDescription(l=2, dim=dim, periodic=True) if domain is None else domain
+    verletScale = 2.0 ** (1 / dim) if verletScale is None else verletScale
+    kernel = KernelFunctions.Wendland2 if kernel is None else kernel
+    integrationScheme = IntegrationSchemeType.rungeKutta2 if integrationScheme is None else integrationScheme
+    cflFactor = 0.3 if cflFactor is None else cflFactor
+    adaptiveDt = True if adaptiveDt is None else adaptiveDt
+    targetNeighbors = n_h_to_nH(4, dim) if targetNeighbors is None else targetNeighbors
+    supportMode = SupportScheme.SuperSymmetric if supportMode is None else supportMode
+    gradientMode = GradientScheme.Difference if gradientMode is None else gradientMode
+    laplacianMode = LaplacianScheme.Brookshaw if laplacianMode is None else laplacianMode
+    samplingScheme = SamplingScheme.regular if samplingScheme is None else samplingScheme
+    minDt = 1e-6 if minDt is None else minDt
+    maxDt = 1e-2 if maxDt is None else maxDt
+    dtGrowthFactor = 1.1 if dtGrowthFactor is None else dtGrowthFactor
+    cfg = SimulationConfig(device=device, dtype=dtype, domain=domain, dim=dim, verletScale=verletScale, kernel=kernel,
+                           integrationScheme=integrationScheme, cflFactor=cflFactor, dt=dt, minDt=minDt, maxDt=maxDt,
+                           dtGrowthFactor=dtGrowthFactor, adaptiveDt=adaptiveDt, targetNeighbors=targetNeighbors,
+                           supportMode=supportMode, gradientMode=gradientMode, laplacianMode=laplacianMode,
+                           samplingScheme=samplingScheme)
+    return cfg, getIntegrator(integrationScheme)
+
+
+def configurationToDict(config: SimulationConfig) -> Dict[str, Any]:
+    dmin, dmax, per = config.domain.host()
+    return {
+        "device": str(config.device), "dtype": str(config.dtype),
+        "domain": {"min": dmin, "max": dmax, "periodic": per, "dim": config.domain.dim},
+        "dim": config.dim, "verletScale": config.verletScale, "kernel": config.kernel.name,
+        "integrationScheme": config.integrationScheme.name, "cflFactor": config.cflFactor,
+        "dt": float(config.dt) if config.dt is not None else None, "minDt": config.minDt, "maxDt": config.maxDt,
+        "dtGrowthFactor": config.dtGrowthFactor, "adaptiveDt": config.adaptiveDt,
+        "targetNeighbors": config.targetNeighbors, "supportMode": config.supportMode.name,
+        "gradientMode": config.gradientMode.name, "laplacianMode": config.laplacianMode.name,
+        "samplingScheme": config.samplingScheme.name,
+    }
+
+
+def dictToConfig(d: Dict[str, Any]) -> SimulationConfig:
+    device = torch.device(d["device"])
+    dtype = getattr(torch, d["dtype"].split(".")[-1])
+    dd = d["domain"]
+    domain = DomainDescription(torch.tensor(dd["min"], device=device, dtype=dtype), torch.tensor(dd["max"], device=device, dtype=dtype),
+                               torch.tensor(dd["periodic"], device=device, dtype=torch.bool), dd["dim"])
+    return SimulationConfig(device=device, dtype=dtype, domain=domain, dim=int(d["dim"]), verletScale=float(d["verletScale"]),
+                            kernel=KernelFunctions[d["kernel"]], integrationScheme=IntegrationSchemeType[d["integrationScheme"]],
+                            cflFactor=float(d["cflFactor"]), dt=None if d["dt"] is None else float(d["dt"]),
+                            minDt=float(d["minDt"]), maxDt=float(d["maxDt"]), dtGrowthFactor=float(d["dtGrowthFactor"]),
+                            adaptiveDt=bool(d["adaptiveDt"]), targetNeighbors=float(d["targetNeighbors"]),
+                            supportMode=SupportScheme[d["supportMode"]], gradientMode=GradientScheme[d["gradientMode"]],
+                            laplacianMode=LaplacianScheme[d["laplacianMode"]], samplingScheme=SamplingScheme[d["samplingScheme"]])
+
+
+# ------------------------------------------------------------------ module parameters
+class ViscosityTerms(Enum):
+    Default = 0
+    MonaghanGingold1983 = 1
+    Cleary1998 = 2
+    Monaghan1992 = 3
+    Monaghan1997a = 4
+    Monaghan1997b = 5
+    Dukowicz = 6
+    Price2012_98 = 7
+    Price2012 = 8
+    Price2008 = 9
+    Wadsley2008 = 10
+    DeltaSPH = 11
+
+
+@dataclass
+class DiffusionParameters:
+    c_s: float = 1.0
+    C_l: float = 1.0
+    C_q: float = 2.0
+    Cu_l: float = 1.0
+    Cu_q: float = 2.0
+    K: float = 1.0
+    thermalConductivity: float = 0.5
+    viscosityTerm: int = ViscosityTerms.Price2012_98.value
+    thermalConducitiyTerm: int = ViscosityTerms.Price2012_98.value
+    scaleBeta: bool = False
+    monaghanSwitch: bool = True
+    correctXi: bool = True
+
+
+def buildDefaultDiffusionParamsCompressibleSPH() -> DiffusionParameters:
+    return DiffusionParameters(c_s=1, C_l=1, C_q=0, Cu_l=1, Cu_q=0, K=1.0, thermalConductivity=0.5,
+                               viscosityTerm=ViscosityTerms.Price2012_98.value, thermalConducitiyTerm=ViscosityTerms.Price2008.value,
+                               scaleBeta=False, monaghanSwitch=True, correctXi=True)
+
+
+def buildDefaultDiffusionParamsCRKSPH() -> DiffusionParameters:
+    return DiffusionParameters(c_s=1, C_l=1, C_q=1, Cu_l=1, Cu_q=1, K=1.0, thermalConductivity=0.5,
+                               viscosityTerm=ViscosityTerms.Monaghan1992.value, thermalConducitiyTerm=ViscosityTerms.Price2012_98.value,
+                               scaleBeta=False, monaghanSwitch=True, correctXi=True)
+
+
+def buildDefaultDiffusionParamsCompSPH() -> DiffusionParameters:
+    return DiffusionParameters(c_s=1, C_l=1, C_q=2, Cu_l=1, Cu_q=2, K=1.0, thermalConductivity=0.5,
+                               viscosityTerm=ViscosityTerms.Monaghan1992.value, thermalConducitiyTerm=ViscosityTerms.Price2012_98.value,
+                               scaleBeta=False, monaghanSwitch=True, correctXi=True)
+
+
+def _term_value(t) -> int:
+    return t.value if isinstance(t, ViscosityTerms) else int(t)
+
+
+def diffusionParamsToDict(p: DiffusionParameters) -> Dict[str, Any]:
+    return {"c_s": p.c_s, "C_l": p.C_l, "C_q": p.C_q, "Cu_l": p.Cu_l, "Cu_q": p.Cu_q, "K": p.K,
+            "thermalConductivity": p.thermalConductivity, "viscosityTerm": ViscosityTerms(_term_value(p.viscosityTerm)).name,
+            "thermalConducitiyTerm": ViscosityTerms(_term_value(p.thermalConducitiyTerm)).name, "scaleBeta": p.scaleBeta,
+            "monaghanSwitch": p.monaghanSwitch, "correctXi": p.correctXi}
+
+
+def dictToDiffusionParams(d: Dict[str, Any]) -> DiffusionParameters:
+    vt = d["viscosityTerm"]
+    tt = d["thermalConducitiyTerm"]
+    return DiffusionParameters(c_s=d["c_s"], C_l=d["C_l"], C_q=d["C_q"], Cu_l=d["Cu_l"], Cu_q=d["Cu_q"], K=d["K"],
+                               thermalConductivity=d["thermalConductivity"],
+                               viscosityTerm=ViscosityTerms[vt].value if isinstance(vt, str) else vt,
+                               thermalConducitiyTerm=ViscosityTerms[tt].value if isinstance(tt, str) else tt,
+                               scaleBeta=d["scaleBeta"], monaghanSwitch=d["monaghanSwitch"], correctXi=d["correctXi"])
+
+
+@dataclass
+class ViscositySwitchConfig:
+    scheme: ViscositySwitch = ViscositySwitch.NoneSwitch
+    correctVelocityGradient: bool = False
+    divergenceScheme: Optional[str] = "naive"
+    alpha_min: float = 0.02
+    alpha_max: float = 2.0
+    beta_c: float = 0.7
+    beta_d: float = 0.05
+    beta_xi: float = 2.0
+    limitXi: bool = True   # the reference declares the field twice; the later default (True) is the effective one
+
+
+def viscositySwitchConfigToDict(c: ViscositySwitchConfig) -> Dict[str, Any]:
+    return {"scheme": c.scheme.name, "limitXi": c.limitXi, "correctVelocityGradient": c.correctVelocityGradient,
+            "divergenceScheme": c.divergenceScheme, "alpha_min": c.alpha_min, "alpha_max": c.alpha_max,
+            "beta_c": c.beta_c, "beta_d": c.beta_d, "beta_xi": c.beta_xi}
+
+
+def dictToViscositySwitchConfig(d: Dict[str, Any]) -> ViscositySwitchConfig:
+    s = d["scheme"]
+    return ViscositySwitchConfig(scheme=ViscositySwitch[s] if isinstance(s, str) else s, limitXi=d["limitXi"],
+                                 correctVelocityGradient=d["correctVelocityGradient"], divergenceScheme=d["divergenceScheme"],
+                                 alpha_min=d["alpha_min"], alpha_max=d["alpha_max"], beta_c=d["beta_c"], beta_d=d["beta_d"],
+                                 beta_xi=d["beta_xi"])
+
+
+@dataclass
+class CRKViscosity:
+    eta_fold: float = 0.2
+    eta_crit: float = 0.3333333
+    enableCRKLimiter: bool = True
+    enableVanLeerLimiter: bool = True
+    forceVanLeerOff: bool = False
+    forceVanLeerOn: bool = False
+
+
+def buildDefaultCRKViscosityParams() -> CRKViscosity:
+    return CRKViscosity()
+
+
+# ------------------------------------------------------------------ scheme configs
+@dataclass
+class CompressibleSPHConfig:
+    gamma: float = 1.4
+    backgroundPressure: float = 0.0
+    rho0: float = 1.0
+    adaptiveSupportScheme: AdaptiveSupportScheme = AdaptiveSupportScheme.Monaghan
+    adaptiveSupportIterations: int = 1
+    adaptiveSupportThreshold: float = 1e-3
+    adaptiveSupportCorrections: bool = True
+    diffusionParams: DiffusionParameters = field(default_factory=buildDefaultDiffusionParamsCompressibleSPH)
+    viscositySwitchParams: ViscositySwitchConfig = field(default_factory=ViscositySwitchConfig)
+    schemeName: str = "Compressible SPH"
+    boundaryConditions: List[Any] = field(default_factory=list)
+    # B200 build option: Neumaier-compensated accumulation of dv/dt and du/dt
+    compensatedSums: bool = False
+
+
+def compressibleConfigToDict(c: CompressibleSPHConfig) -> Dict[str, Any]:
+    if c.boundaryConditions:
+        raise NotImplementedError("boundary conditions are outside the GPU hot path")
+    return {"gamma": c.gamma, "backgroundPressure": c.backgroundPressure, "rho0": c.rho0,
+            "adaptiveSupportScheme": c.adaptiveSupportScheme.name, "adaptiveSupportIterations": c.adaptiveSupportIterations,
+            "adaptiveSupportThreshold": c.adaptiveSupportThreshold, "adaptiveSupportCorrections": c.adaptiveSupportCorrections,
+            "diffusionParams": diffusionParamsToDict(c.diffusionParams),
+            "viscositySwitchParams": viscositySwitchConfigToDict(c.viscositySwitchParams), "schemeName": c.schemeName,
+            "boundaryConditions": [], "compensatedSums": c.compensatedSums}
+
+
+def dictToCompressibleConfig(d: Dict[str, Any]) -> CompressibleSPHConfig:
+    a = d["adaptiveSupportScheme"]
+    return CompressibleSPHConfig(gamma=d["gamma"], backgroundPressure=d["backgroundPressure"], rho0=d["rho0"],
+                                 adaptiveSupportScheme=AdaptiveSupportScheme[a] if isinstance(a, str) else a,
+                                 adaptiveSupportIterations=d["adaptiveSupportIterations"],
+                                 adaptiveSupportThreshold=d["adaptiveSupportThreshold"],
+                                 adaptiveSupportCorrections=d["adaptiveSupportCorrections"],
+                                 diffusionParams=dictToDiffusionParams(d["diffusionParams"]),
+                                 viscositySwitchParams=dictToViscositySwitchConfig(d["viscositySwitchParams"]),
+                                 schemeName=d["schemeName"], boundaryConditions=[],
+                                 compensatedSums=bool(d.get("compensatedSums", False)))
+
+
+@dataclass
+class CompSPHConfig(CompressibleSPHConfig):
+    energyScheme: EnergyScheme = EnergyScheme.CRK
+    diffusionParams: DiffusionParameters = field(default_factory=buildDefaultDiffusionParamsCompSPH)
+    schemeName: str = "CompSPH"
+    compatibleEnergy: bool = True
+
+
+def compSPHConfigToDict(c: CompSPHConfig) -> Dict[str, Any]:
+    d = compressibleConfigToDict(c)
+    d.update({"energyScheme": c.energyScheme.name, "compatibleEnergy": c.compatibleEnergy})
+    return d
+
+
+def dictToCompSPHConfig(d: Dict[str, Any]) -> CompSPHConfig:
+    base = dictToCompressibleConfig(d)
+    c = CompSPHConfig(**base.__dict__)
+    e = d["energyScheme"]
+    c.energyScheme = EnergyScheme[e] if isinstance(e, str) else e
+    c.compatibleEnergy = d["compatibleEnergy"]
+    return c
+
+
+@dataclass
+class CRKSPHConfig(CompressibleSPHConfig):
+    energyScheme: EnergyScheme = EnergyScheme.CRK
+    diffusionParams: DiffusionParameters = field(default_factory=buildDefaultDiffusionParamsCRKSPH)
+    crkViscosityParams: CRKViscosity = field(default_factory=buildDefaultCRKViscosityParams)
+    schemeName: str = "CRKSPH"
+    compatibleEnergy: bool = True
+
+
+def crkSPHConfigToDict(c: CRKSPHConfig) -> Dict[str, Any]:
+    d = compressibleConfigToDict(c)
+    v = c.crkViscosityParams
+    d.update({"energyScheme": c.energyScheme.name, "compatibleEnergy": c.compatibleEnergy,
+              "crkViscosityParams": {"eta_fold": v.eta_fold, "eta_crit": v.eta_crit, "enableCRKLimiter": v.enableCRKLimiter,
+                                     "enableVanLeerLimiter": v.enableVanLeerLimiter, "forceVanLeerOff": v.forceVanLeerOff,
+                                     "forceVanLeerOn": v.forceVanLeerOn}})
+    return d
+
+
+def dictToCRKSPHConfig(d: Dict[str, Any]) -> CRKSPHConfig:
+    base = dictToCompressibleConfig(d)
+    c = CRKSPHConfig(**base.__dict__)
+    e = d["energyScheme"]
+    c.energyScheme = EnergyScheme[e] if isinstance(e, str) else e
+    c.compatibleEnergy = d["compatibleEnergy"]
+    v = d["crkViscosityParams"]
+    c.crkViscosityParams = CRKViscosity(eta_fold=v["eta_fold"], eta_crit=v["eta_crit"], enableCRKLimiter=v["enableCRKLimiter"],
+                                        enableVanLeerLimiter=v["enableVanLeerLimiter"], forceVanLeerOff=v["forceVanLeerOff"],
+                                        forceVanLeerOn=v["forceVanLeerOn"])
+    return c
+
+
+# ------------------------------------------------------------------ C ABI parameter block
+def make_params(config: SimulationConfig, scheme: Optional[CompressibleSPHConfig] = None) -> _capi.SphParams:
+    """Packs the configuration into the C ABI's SphParams (host-side, no device sync
+    beyond a cached read of the domain tensors)."""
+    p = _capi.SphParams()
+    dmin, dmax, per = config.domain.host()
+    dim = int(config.dim)
+    for a in range(3):
+        p.domain_min[a] = dmin[a] if a < dim else 0.0
+        p.domain_max[a] = dmax[a] if a < dim else 1.0
+        p.periodic[a] = int(per[a]) if a < dim else 0
+    p.dim = dim
+    p.kernel = int(config.kernel.value)
+    p.verlet_scale = float(config.verletScale)
+    p.target_neighbors = float(config.targetNeighbors)
+    p.cfl = float(config.cflFactor)
+    p.min_dt = float(config.minDt if config.minDt is not None else 0.0)
+    p.max_dt = float(config.maxDt if config.maxDt is not None else 1e30)
+    p.dt_growth = float(config.dtGrowthFactor if config.dtGrowthFactor is not None else 1e30)
+    if scheme is not None:
+        dp = scheme.diffusionParams
+        p.C_l, p.C_q, p.Cu_l, p.Cu_q, p.K = float(dp.C_l), float(dp.C_q), float(dp.Cu_l), float(dp.Cu_q), float(dp.K)
+        p.viscosity_term = _term_value(dp.viscosityTerm)
+        p.monaghan_switch = int(bool(dp.monaghanSwitch))
+        p.correct_xi = int(bool(dp.correctXi))
+        p.scale_beta = int(bool(dp.scaleBeta))
+        p.gamma = float(scheme.gamma)
+        sw = scheme.viscositySwitchParams
+        p.alpha_min, p.alpha_max, p.beta_xi = float(sw.alpha_min), float(sw.alpha_max), float(sw.beta_xi)
+        p.limit_xi = int(bool(sw.limitXi))
+        p.kahan = int(bool(getattr(scheme, "compensatedSums", False)))
+        es = getattr(scheme, "energyScheme", EnergyScheme.CRK)
+        p.energy_scheme = int(es.value)
+        cv = getattr(scheme, "crkViscosityParams", None)
+        if cv is not None:
+            p.eta_crit, p.eta_fold = float(cv.eta_crit), float(cv.eta_fold)
+            p.enable_crk_limiter = int(bool(cv.enableCRKLimiter))
+            p.enable_vanleer_limiter = int(bool(cv.enableVanLeerLimiter))
+            p.force_vanleer_off = int(bool(cv.forceVanLeerOff))
+            p.force_vanleer_on = int(bool(cv.forceVanLeerOn))
+    return p

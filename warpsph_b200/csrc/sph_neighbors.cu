@@ -1,0 +1,594 @@
+// Neighbour search for libwarpsph_b200 and the library's host utilities.
+//
+// Replaces warpSPHCore's buildVerletList (compact hash + CUB radix sort in the
+// reference, called at schemes/crkSPH.py:54-58).  Design:
+//   1. cell size c >= verlet_scale * max(H) (device max-reduction, no host sync);
+//      dense grid of G_d = floor(L_d / c) cells per axis, keyed by the Morton code
+//      of the cell coordinate so that spatially close cells are close in memory.
+//   2. counting sort by key: histogram (atomics), exclusive scan -> cell_begin,
+//      atomic scatter, then a per-cell insertion sort by particle index, so the
+//      permutation equals a stable sort by (key, index) -- deterministic and
+//      bit-identical to the CPU oracle.
+//   3. Verlet list as CSR: count pass, exclusive scan, fill pass.  Each thread owns
+//      one particle (taken in sorted order for locality), visits the 3^d stencil
+//      cells in ascending key order, and keeps j when
+//      |x_i - x_j|^2 < (verlet_scale * max(H_i, H_j))^2 (computed with explicit
+//      round-to-nearest operations so the oracle reproduces it exactly).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+#include <cuda_runtime.h>
+#include "sph_common.cuh"
+
+namespace wsph {
+
+// ---------------------------------------------------------------- error handling
+static thread_local char g_err[512] = "no error";
+
+int set_error(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+int check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(SPH_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return SPH_OK;
+}
+
+double kernel_norm(int kernel, int dim) {
+    const double pi = 3.14159265358979323846;
+    if (kernel == SPH_KERNEL_WENDLAND2) return dim == 1 ? 1.25 : (dim == 2 ? 7.0 / pi : 21.0 / (2.0 * pi));
+    if (kernel == SPH_KERNEL_WENDLAND4) return dim == 1 ? 1.5 : (dim == 2 ? 9.0 / pi : 495.0 / (32.0 * pi));
+    if (kernel == SPH_KERNEL_WENDLAND6) return dim == 1 ? 1.71875 : (dim == 2 ? 78.0 / (7.0 * pi) : 1365.0 / (64.0 * pi));
+    return 0.0;
+}
+
+// H / h with h = 2 sigma, sigma^2 = (1/d) int |x|^2 W dx (Dehnen & Aly 2012, Table 1).
+double kernel_scale(int kernel, int dim) {
+    static const double t[3][3] = {
+        {1.620185175, 1.897366596, 1.936491673},
+        {1.936491673, 2.171240593, 2.207940217},
+        {2.207940217, 2.415229458, 2.449489743}};
+    if (kernel < 1 || kernel > 3 || dim < 1 || dim > 3) return 0.0;
+    return t[kernel - 1][dim - 1];
+}
+
+int params_to_dev(const SphParams* p, DevParams* o) {
+    if (!p) return set_error(SPH_ERR_BAD_ARG, "null SphParams");
+    if (p->dim < 1 || p->dim > 3) return set_error(SPH_ERR_BAD_ARG, "dim must be 1..3 (got %d)", p->dim);
+    if (p->kernel < SPH_KERNEL_WENDLAND2 || p->kernel > SPH_KERNEL_WENDLAND6)
+        return set_error(SPH_ERR_BAD_ARG, "unsupported kernel id %d", p->kernel);
+    memset(o, 0, sizeof(*o));
+    o->dim = p->dim;
+    o->kernel = p->kernel;
+    for (int a = 0; a < 3; ++a) {
+        o->dom.min[a] = (float)p->domain_min[a];
+        o->dom.max[a] = (float)p->domain_max[a];
+        o->dom.L[a] = (float)(p->domain_max[a] - p->domain_min[a]);
+        o->dom.halfL[a] = 0.5f * o->dom.L[a];
+        o->dom.periodic[a] = p->periodic[a] ? 1 : 0;
+        if (a < p->dim && !(o->dom.L[a] > 0.f)) return set_error(SPH_ERR_BAD_ARG, "domain extent along axis %d must be > 0", a);
+    }
+    o->verlet_scale = (float)p->verlet_scale;
+    if (!(o->verlet_scale >= 1.f)) return set_error(SPH_ERR_BAD_ARG, "verlet_scale must be >= 1");
+    o->C_l = (float)p->C_l; o->C_q = (float)p->C_q; o->Cu_l = (float)p->Cu_l; o->Cu_q = (float)p->Cu_q; o->K = (float)p->K;
+    o->viscosity_term = p->viscosity_term;
+    o->monaghan_switch = p->monaghan_switch; o->correct_xi = p->correct_xi; o->scale_beta = p->scale_beta;
+    o->eta_crit = (float)p->eta_crit; o->eta_fold = (float)p->eta_fold;
+    o->enable_crk_limiter = p->enable_crk_limiter; o->enable_vanleer = p->enable_vanleer_limiter;
+    o->force_vl_off = p->force_vanleer_off; o->force_vl_on = p->force_vanleer_on;
+    o->gamma = (float)p->gamma;
+    o->energy_scheme = p->energy_scheme; o->limit_xi = p->limit_xi; o->kahan = p->kahan;
+    o->alpha_min = (float)p->alpha_min; o->alpha_max = (float)p->alpha_max; o->beta_xi = (float)p->beta_xi;
+    o->target_neighbors = (float)p->target_neighbors;
+    o->cfl = (float)p->cfl; o->min_dt = (float)p->min_dt; o->max_dt = (float)p->max_dt; o->dt_growth = (float)p->dt_growth;
+    o->kscale = (float)kernel_scale(p->kernel, p->dim);
+    o->kxi = o->kscale;
+    return SPH_OK;
+}
+
+// ---------------------------------------------------------------- scan
+// Exclusive scan of int32 values with an int64 grand total.  Block-level scans of
+// 2048 items (256 threads x 8), recursive over block sums.
+static constexpr int SCAN_THREADS = 256;
+static constexpr int SCAN_ITEMS = 8;
+static constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ long long block_exclusive_scan(long long v, long long* smem_warp, long long& total) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long x = v;
+    #pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) smem_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        long long w = (lane < SCAN_THREADS / 32) ? smem_warp[lane] : 0;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            long long y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < SCAN_THREADS / 32) smem_warp[lane] = w;
+    }
+    __syncthreads();
+    long long warp_off = warp > 0 ? smem_warp[warp - 1] : 0;
+    total = smem_warp[SCAN_THREADS / 32 - 1];
+    __syncthreads();
+    return warp_off + x - v;
+}
+
+// in -> out (exclusive, local to tile), tile totals -> sums
+__global__ void k_scan_tiles(const int32_t* __restrict__ in, int64_t n, long long* __restrict__ out_ll,
+                             int32_t* __restrict__ out32, long long* __restrict__ sums) {
+    __shared__ long long sw[SCAN_THREADS / 32];
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    long long vals[SCAN_ITEMS];
+    long long local = 0;
+    #pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        int64_t idx = base + k;
+        vals[k] = idx < n ? (long long)in[idx] : 0;
+        local += vals[k];
+    }
+    long long total;
+    long long off = block_exclusive_scan(local, sw, total);
+    #pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        int64_t idx = base + k;
+        if (idx < n) {
+            if (out_ll) out_ll[idx] = off; else out32[idx] = (int32_t)off;
+        }
+        off += vals[k];
+    }
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+// in and out may alias (in-place scan of tile sums): no __restrict__ here.
+__global__ void k_scan_tiles_ll(const long long* in, int64_t n, long long* out, long long* __restrict__ sums) {
+    __shared__ long long sw[SCAN_THREADS / 32];
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    long long vals[SCAN_ITEMS];
+    long long local = 0;
+    #pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        int64_t idx = base + k;
+        vals[k] = idx < n ? in[idx] : 0;
+        local += vals[k];
+    }
+    long long total;
+    long long off = block_exclusive_scan(local, sw, total);
+    #pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        int64_t idx = base + k;
+        if (idx < n) out[idx] = off;
+        off += vals[k];
+    }
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+__global__ void k_scan_add(long long* __restrict__ out_ll, int32_t* __restrict__ out32, int64_t n,
+                           const long long* __restrict__ tile_off) {
+    int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    long long o = tile_off[idx / SCAN_TILE];
+    if (out_ll) out_ll[idx] += o; else out32[idx] = (int32_t)((long long)out32[idx] + o);
+}
+
+// Workspace: for each level the tile sums and their scanned offsets.
+static int64_t scan_ws_bytes(int64_t n) {
+    int64_t bytes = 0;
+    int64_t m = n;
+    do {
+        int64_t tiles = (m + SCAN_TILE - 1) / SCAN_TILE;
+        if (tiles < 1) tiles = 1;
+        bytes += 2 * ((tiles * 8 + 255) / 256) * 256;
+        m = tiles;
+    } while (m > 1);
+    return bytes + 256;
+}
+
+// Scans a level of long long values in place (exclusive) and writes the total to *total.
+static void scan_ll_inplace(long long* data, int64_t n, char* ws, long long* total, cudaStream_t s) {
+    int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (tiles < 1) tiles = 1;
+    long long* sums = reinterpret_cast<long long*>(ws);
+    char* next = ws + ((tiles * 8 + 255) / 256) * 256 * 2;
+    wsph::count_launch(); k_scan_tiles_ll<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(data, n, data, sums);
+    if (tiles == 1) {
+        cudaMemcpyAsync(total, sums, sizeof(long long), cudaMemcpyDeviceToDevice, s);
+        return;
+    }
+    scan_ll_inplace(sums, tiles, next, total, s);
+    wsph::count_launch(); k_scan_add<<<grid_for(n, 256), 256, 0, s>>>(data, nullptr, n, sums);
+}
+
+// Exclusive scan int32 -> int32, total (int64, device).
+static void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, char* ws, long long* total, cudaStream_t s) {
+    int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (tiles < 1) tiles = 1;
+    long long* sums = reinterpret_cast<long long*>(ws);
+    char* next = ws + ((tiles * 8 + 255) / 256) * 256 * 2;
+    wsph::count_launch(); k_scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, nullptr, out, sums);
+    if (tiles == 1) {
+        cudaMemcpyAsync(total, sums, sizeof(long long), cudaMemcpyDeviceToDevice, s);
+        return;
+    }
+    scan_ll_inplace(sums, tiles, next, total, s);
+    wsph::count_launch(); k_scan_add<<<grid_for(n, 256), 256, 0, s>>>(nullptr, out, n, sums);
+}
+
+// ---------------------------------------------------------------- min / max
+__global__ void k_minmax_init(float* out2) { out2[0] = __int_as_float(0x7f800000); out2[1] = -__int_as_float(0x7f800000); }
+
+__device__ __forceinline__ void atomic_min_float(float* addr, float v) {
+    // ordered-int trick valid for non-NaN floats of any sign
+    if (v >= 0.f) atomicMin(reinterpret_cast<int*>(addr), __float_as_int(v));
+    else atomicMax(reinterpret_cast<unsigned int*>(addr), __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_float(float* addr, float v) {
+    if (v >= 0.f) atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
+    else atomicMin(reinterpret_cast<unsigned int*>(addr), __float_as_uint(v));
+}
+
+__global__ void k_minmax(const float* __restrict__ a, int64_t n, float* out2) {
+    float lo = __int_as_float(0x7f800000), hi = -lo;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float v = a[i];
+        lo = fminf(lo, v); hi = fmaxf(hi, v);
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) { atomic_min_float(out2, lo); atomic_max_float(out2 + 1, hi); }
+}
+
+int launch_minmax(int64_t n, const float* a, float* out2, cudaStream_t s) {
+    wsph::count_launch(); k_minmax_init<<<1, 1, 0, s>>>(out2);
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    wsph::count_launch(); k_minmax<<<blocks, 256, 0, s>>>(a, n, out2);
+    return check_launch("sph_minmax");
+}
+
+// ---------------------------------------------------------------- grid
+struct GridDev {
+    int G[3];
+    int bits[3];
+    float inv[3];   // G_d / L_d
+    float cell;     // requested cell size (>= verlet_scale * max H)
+};
+
+__device__ __forceinline__ uint32_t spread2(uint32_t x) {  // 16 bits -> even positions
+    x &= 0x0000ffffu;
+    x = (x | (x << 8)) & 0x00ff00ffu;
+    x = (x | (x << 4)) & 0x0f0f0f0fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    x = (x | (x << 1)) & 0x55555555u;
+    return x;
+}
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {  // 10 bits -> every third position
+    x &= 0x000003ffu;
+    x = (x | (x << 16)) & 0x030000ffu;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+template <int D> __device__ __forceinline__ uint32_t morton(const int* c) {
+    if constexpr (D == 1) return (uint32_t)c[0];
+    else if constexpr (D == 2) return spread2((uint32_t)c[0]) | (spread2((uint32_t)c[1]) << 1);
+    else return spread3((uint32_t)c[0]) | (spread3((uint32_t)c[1]) << 1) | (spread3((uint32_t)c[2]) << 2);
+}
+
+template <int D> __device__ __forceinline__ void cell_coords(const Vec<D>& x, const GridDev& g, const DomainF& dom, int* c) {
+    #pragma unroll
+    for (int a = 0; a < D; ++a) {
+        float t = __fmul_rn(__fsub_rn(x.v[a], dom.min[a]), g.inv[a]);
+        int ci = (int)floorf(t);
+        ci = ci < 0 ? 0 : (ci >= g.G[a] ? g.G[a] - 1 : ci);
+        c[a] = ci;
+    }
+}
+
+__global__ void k_hmax(const float* __restrict__ H, int64_t n, float* out, int32_t* status) {
+    float hi = 0.f;
+    bool bad = false;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float h = H[i];
+        if (!(h > 0.f) || isinf(h)) bad = true; else hi = fmaxf(hi, h);
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int*>(out), __float_as_int(hi));
+    if (bad) atomicOr(status, SPH_STATUS_NONFINITE);
+}
+
+// One thread: derive the grid from max H and the cell-table capacity.
+template <int D>
+__global__ void k_grid(const float* hmax, DevParams P, int max_bits, GridDev* g, int32_t* grid_out) {
+    float h = *hmax;
+    float Lmax = 0.f;
+    for (int a = 0; a < D; ++a) Lmax = fmaxf(Lmax, P.dom.L[a]);
+    // margin keeps the 3^d stencil exact despite rounding of the cell coordinate
+    float cell = __fadd_rn(__fmul_rn(__fmul_rn(P.verlet_scale, h), 1.001f), __fmul_rn(Lmax, 1e-6f));
+    GridDev G;
+    for (int a = 0; a < 3; ++a) { G.G[a] = 1; G.bits[a] = 0; G.inv[a] = 0.f; }
+    for (int a = 0; a < D; ++a) {
+        float f = floorf(P.dom.L[a] / cell);
+        int gmax = 1 << max_bits;
+        int gi = (f >= (float)gmax) ? gmax : (f < 1.f ? 1 : (int)f);
+        int b = 0;
+        while ((1 << b) < gi) ++b;
+        G.G[a] = gi;
+        G.bits[a] = b;
+        G.inv[a] = __fdiv_rn((float)gi, P.dom.L[a]);
+    }
+    G.cell = cell;
+    *g = G;
+    for (int a = 0; a < 3; ++a) { grid_out[a] = G.G[a]; grid_out[3 + a] = G.bits[a]; }
+    grid_out[6] = __float_as_int(cell);
+    grid_out[7] = D;
+}
+
+template <int D>
+__global__ void k_keys(const float* __restrict__ x, int n, const GridDev* __restrict__ gp, DomainF dom,
+                       uint32_t* __restrict__ keys, int32_t* __restrict__ counts) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    GridDev g = *gp;
+    int c[3];
+    cell_coords<D>(load_vec<D>(x, i), g, dom, c);
+    uint32_t key = morton<D>(c);
+    keys[i] = key;
+    atomicAdd(counts + key, 1);
+}
+
+__global__ void k_scatter(const uint32_t* __restrict__ keys, int n, int32_t* __restrict__ cursor, int32_t* __restrict__ sort_index) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int pos = atomicAdd(cursor + keys[i], 1);
+    sort_index[pos] = i;
+}
+
+// Canonical order inside a cell: ascending particle index.
+__global__ void k_cell_sort(const int32_t* __restrict__ begin, const int32_t* __restrict__ end, int64_t ncells,
+                            int32_t* __restrict__ sort_index) {
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    int b = begin[c], e = end[c];
+    for (int k = b + 1; k < e; ++k) {
+        int v = sort_index[k];
+        int m = k - 1;
+        while (m >= b && sort_index[m] > v) { sort_index[m + 1] = sort_index[m]; --m; }
+        sort_index[m + 1] = v;
+    }
+}
+
+__global__ void k_sorted_keys(const uint32_t* __restrict__ keys, const int32_t* __restrict__ sort_index, int n,
+                              uint32_t* __restrict__ sorted_keys) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    sorted_keys[k] = keys[sort_index[k]];
+}
+
+// Stencil of neighbour cell keys for a particle, ascending and de-duplicated.
+template <int D>
+__device__ __forceinline__ int stencil_keys(const int* c, const GridDev& g, const DomainF& dom, uint32_t* out) {
+    int cnt = 0;
+    constexpr int NS = D == 1 ? 3 : (D == 2 ? 9 : 27);
+    for (int s = 0; s < NS; ++s) {
+        int o[3] = {s % 3 - 1, (s / 3) % 3 - 1, (s / 9) % 3 - 1};
+        int cc[3];
+        bool ok = true;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) {
+            int v = c[a] + o[a];
+            if (v < 0 || v >= g.G[a]) {
+                if (dom.periodic[a]) v = (v + g.G[a]) % g.G[a];
+                else ok = false;
+            }
+            cc[a] = v;
+        }
+        if (!ok) continue;
+        uint32_t k = morton<D>(cc);
+        // insertion into the sorted list, skipping duplicates
+        int m = cnt - 1;
+        bool dup = false;
+        for (int q = 0; q < cnt; ++q) if (out[q] == k) { dup = true; break; }
+        if (dup) continue;
+        while (m >= 0 && out[m] > k) { out[m + 1] = out[m]; --m; }
+        out[m + 1] = k;
+        ++cnt;
+    }
+    return cnt;
+}
+
+template <int D, bool FILL>
+__global__ void __launch_bounds__(128)
+k_verlet(const float* __restrict__ x, const float* __restrict__ H, int n, const GridDev* __restrict__ gp, DevParams P,
+         const int32_t* __restrict__ sort_index, const int32_t* __restrict__ cell_begin, const int32_t* __restrict__ cell_end,
+         int32_t* __restrict__ counts, const int32_t* __restrict__ offsets, int32_t* __restrict__ list,
+         const long long* __restrict__ nnz, long long capacity) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    if (FILL && *nnz > capacity) return;
+    GridDev g = *gp;
+    int i = sort_index[t];
+    Vec<D> xi = load_vec<D>(x, i);
+    float Hi = H[i];
+    int c[3];
+    cell_coords<D>(xi, g, P.dom, c);
+    uint32_t keys[D == 1 ? 3 : (D == 2 ? 9 : 27)];
+    int nk = stencil_keys<D>(c, g, P.dom, keys);
+    int cnt = 0;
+    int base = FILL ? offsets[i] : 0;
+    for (int q = 0; q < nk; ++q) {
+        int b = cell_begin[keys[q]], e = cell_end[keys[q]];
+        for (int k = b; k < e; ++k) {
+            int j = sort_index[k];
+            Vec<D> xj = load_vec<D>(x, j);
+            float R = __fmul_rn(P.verlet_scale, fmaxf(Hi, __ldg(H + j)));
+            float r2 = dist2_rn<D>(dist_vec<D>(xi, xj, P.dom));
+            if (r2 < __fmul_rn(R, R)) {
+                if (FILL) list[base + cnt] = j;
+                ++cnt;
+            }
+        }
+    }
+    if (!FILL) counts[i] = cnt;
+}
+
+__global__ void k_check_capacity(const long long* nnz, long long capacity, int32_t* status) {
+    if (*nnz > capacity) atomicOr(status, SPH_STATUS_LIST_OVERFLOW);
+}
+
+__global__ void k_expand(const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+                         int n, int64_t* __restrict__ iout, int64_t* __restrict__ jout) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int b = offs[i], c = cnt[i];
+    for (int k = 0; k < c; ++k) {
+        if (iout) iout[b + k] = i;
+        if (jout) jout[b + k] = list[b + k];
+    }
+}
+
+// workspace carve-up
+struct NbWs {
+    float* hmax;
+    GridDev* grid;
+    long long* total;
+    uint32_t* keys;
+    int32_t* counts;
+    char* scan;
+    int64_t bytes;
+};
+static int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
+static NbWs carve(char* base, int64_t n, int64_t cap) {
+    NbWs w;
+    int64_t off = 0;
+    w.hmax = reinterpret_cast<float*>(base + off); off += 256;
+    w.grid = reinterpret_cast<GridDev*>(base + off); off += align256(sizeof(GridDev));
+    w.total = reinterpret_cast<long long*>(base + off); off += 256;
+    w.keys = reinterpret_cast<uint32_t*>(base + off); off += align256(n * 4);
+    w.counts = reinterpret_cast<int32_t*>(base + off); off += align256(cap * 4);
+    w.scan = base + off;
+    int64_t sb = scan_ws_bytes(cap > n ? cap : n);
+    off += align256(sb);
+    w.bytes = off;
+    return w;
+}
+
+static int max_bits_for(int dim, int64_t cap) {
+    int lb = 0;
+    while (((int64_t)1 << (lb + 1)) <= cap) ++lb;  // floor(log2 cap)
+    int mb = lb / dim;
+    int lim = dim == 1 ? 30 : (dim == 2 ? 16 : 10);
+    return mb > lim ? lim : mb;
+}
+
+}  // namespace wsph
+
+using namespace wsph;
+
+extern "C" {
+
+const char* sph_version(void) { return "warpsph_b200 0.1.0 (sm_100a)"; }
+const char* sph_last_error_string(void) { return g_err; }
+int64_t sph_launch_count(void) { return g_launches.load(); }
+
+int sph_kernel_constants(int32_t kernel, int32_t dim, double* norm_out, double* scale_out) {
+    double c = kernel_norm(kernel, dim), s = kernel_scale(kernel, dim);
+    if (c == 0.0 || s == 0.0) return set_error(SPH_ERR_BAD_ARG, "unknown kernel %d / dim %d", kernel, dim);
+    if (norm_out) *norm_out = c;
+    if (scale_out) *scale_out = s;
+    return SPH_OK;
+}
+
+int sph_minmax(int64_t n, const float* a, float* out2, void* stream) {
+    if (n < 0) return set_error(SPH_ERR_BAD_ARG, "sph_minmax: n < 0");
+    WSPH_CHECK_PTR(out2);
+    if (n > 0) WSPH_CHECK_PTR(a);
+    return launch_minmax(n, a, out2, WSPH_STREAM(stream));
+}
+
+int sph_neighbors_workspace_size(const SphParams* p, int64_t n, int64_t cell_capacity, int64_t* bytes_out) {
+    WSPH_CHECK_PTR(p); WSPH_CHECK_PTR(bytes_out);
+    if (n < 0 || cell_capacity < 1) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_workspace_size: bad sizes");
+    NbWs w = carve(nullptr, n, cell_capacity);
+    *bytes_out = w.bytes;
+    return SPH_OK;
+}
+
+int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const float* H,
+                        void* workspace, int64_t workspace_bytes, int64_t cell_capacity,
+                        int32_t* sort_index, uint32_t* sorted_keys,
+                        int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
+                        int32_t* neighbor_offsets, int32_t* num_neighbors,
+                        int32_t* neighbor_list, int64_t list_capacity,
+                        int64_t* nnz_out, int32_t* status, void* stream) {
+    DevParams P;
+    int rc = params_to_dev(p, &P);
+    if (rc) return rc;
+    if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_build: n out of range");
+    if (cell_capacity < 1) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_build: cell_capacity < 1");
+    WSPH_CHECK_PTR(nnz_out); WSPH_CHECK_PTR(status); WSPH_CHECK_PTR(grid_out);
+    cudaStream_t s = WSPH_STREAM(stream);
+    if (n == 0) {
+        cudaMemsetAsync(nnz_out, 0, sizeof(int64_t), s);
+        return check_launch("sph_neighbors_build");
+    }
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(workspace); WSPH_CHECK_PTR(sort_index);
+    WSPH_CHECK_PTR(sorted_keys); WSPH_CHECK_PTR(cell_begin); WSPH_CHECK_PTR(cell_end);
+    WSPH_CHECK_PTR(neighbor_offsets); WSPH_CHECK_PTR(num_neighbors);
+    if (list_capacity > 0) WSPH_CHECK_PTR(neighbor_list);
+    if (P.dim == 2 && (reinterpret_cast<uintptr_t>(x) & 7)) return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
+    NbWs w = carve(reinterpret_cast<char*>(workspace), n, cell_capacity);
+    if (workspace_bytes < w.bytes) return set_error(SPH_ERR_WORKSPACE, "neighbour workspace too small: %lld < %lld", (long long)workspace_bytes, (long long)w.bytes);
+    int mb = max_bits_for(P.dim, cell_capacity);
+    int64_t ncells = (int64_t)1 << (mb * P.dim);
+
+    cudaMemsetAsync(w.hmax, 0, sizeof(float), s);
+    int rblocks = grid_for(n, 256);
+    if (rblocks > 148 * 8) rblocks = 148 * 8;
+    wsph::count_launch(); k_hmax<<<rblocks, 256, 0, s>>>(H, n, w.hmax, status);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, k_grid<D><<<1, 1, 0, s>>>(w.hmax, P, mb, w.grid, grid_out));
+    cudaMemsetAsync(w.counts, 0, ncells * sizeof(int32_t), s);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, k_keys<D><<<grid_for(n, 256), 256, 0, s>>>(x, (int)n, w.grid, P.dom, w.keys, w.counts));
+    exclusive_scan_i32(w.counts, cell_begin, ncells, w.scan, w.total, s);
+    cudaMemcpyAsync(cell_end, cell_begin, ncells * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+    wsph::count_launch(); k_scatter<<<grid_for(n, 256), 256, 0, s>>>(w.keys, (int)n, cell_end, sort_index);
+    wsph::count_launch(); k_cell_sort<<<grid_for(ncells, 256), 256, 0, s>>>(cell_begin, cell_end, ncells, sort_index);
+    wsph::count_launch(); k_sorted_keys<<<grid_for(n, 256), 256, 0, s>>>(w.keys, sort_index, (int)n, sorted_keys);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, false><<<grid_for(n, 128), 128, 0, s>>>(x, H, (int)n, w.grid, P, sort_index, cell_begin, cell_end,
+                                                                                 num_neighbors, nullptr, nullptr, nullptr, 0)));
+    exclusive_scan_i32(num_neighbors, neighbor_offsets, n, w.scan, reinterpret_cast<long long*>(nnz_out), s);
+    wsph::count_launch(); k_check_capacity<<<1, 1, 0, s>>>(reinterpret_cast<long long*>(nnz_out), list_capacity, status);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, true><<<grid_for(n, 128), 128, 0, s>>>(x, H, (int)n, w.grid, P, sort_index, cell_begin, cell_end,
+                                                                                nullptr, neighbor_offsets, neighbor_list,
+                                                                                reinterpret_cast<long long*>(nnz_out), list_capacity)));
+    return check_launch("sph_neighbors_build");
+}
+
+int sph_neighbors_expand(int64_t n, const int32_t* neighbor_offsets, const int32_t* num_neighbors,
+                         const int32_t* neighbor_list, int64_t nnz, int64_t* i_out, int64_t* j_out, void* stream) {
+    if (n < 0 || nnz < 0) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_expand: negative size");
+    if (n == 0) return SPH_OK;
+    WSPH_CHECK_PTR(neighbor_offsets); WSPH_CHECK_PTR(num_neighbors); WSPH_CHECK_PTR(neighbor_list);
+    wsph::count_launch(); k_expand<<<grid_for(n, 256), 256, 0, WSPH_STREAM(stream)>>>(neighbor_offsets, num_neighbors, neighbor_list, (int)n, i_out, j_out);
+    return check_launch("sph_neighbors_expand");
+}
+
+}  // extern "C"

@@ -1,0 +1,1022 @@
+// SPH pair-interaction kernels of the compressible (CRKSPH / CompSPH) hot path.
+//
+// Every pair kernel walks the CSR Verlet list of one particle per thread in list
+// order.  Entries whose distance exceeds the kernel support contribute exact zeros
+// (as in the reference, where Verlet entries beyond the support give W = 0), so
+// those entries only cost the distance test.
+#include <cuda_runtime.h>
+#include "sph_common.cuh"
+
+namespace wsph {
+
+constexpr int PAIR_BLOCK = 128;
+
+// Neumaier-compensated accumulator (used when DevParams::kahan is set).
+struct KSum {
+    float s, c;
+    __device__ __forceinline__ void init() { s = 0.f; c = 0.f; }
+    __device__ __forceinline__ void add(float x, bool comp) {
+        if (!comp) { s += x; return; }
+        float t = s + x;
+        if (fabsf(s) >= fabsf(x)) c += (s - t) + x; else c += (x - t) + s;
+        s = t;
+    }
+    __device__ __forceinline__ float value() const { return s + c; }
+};
+
+// ---------------------------------------------------------------- density
+template <int KF, int D>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_density(int n, int mode, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+          const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+          float* __restrict__ rho) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec<D> xi = load_vec<D>(x, i);
+    float Hi = H[i];
+    int b = offs[i], e = b + cnt[i];
+    float s = 0.f;
+    for (int k = b; k < e; ++k) {
+        int j = __ldg(list + k);
+        Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+        float r = safe_sqrt(dot<D>(xij, xij));
+        s += __ldg(m + j) * kernelW_mode<KF, D>(r, Hi, __ldg(H + j), mode);
+    }
+    rho[i] = s;
+}
+
+// ---------------------------------------------------------------- adaptive support (Monaghan Newton)
+// h(V) from utils/support.py:24-44 (volumeToSupportHelper)
+template <int D> __device__ __forceinline__ float volume_to_support(float V, float nH) {
+    if constexpr (D == 1) return nH * V / 2.f;
+    else if constexpr (D == 2) return sqrtf(nH * V / 3.14159265358979f);
+    else return powf(nH * V / 3.14159265358979f * 3.f / 4.f, 1.f / 3.f);
+}
+
+template <int KF, int D>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_adaptive_h(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+             const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+             const float* __restrict__ hb, float* __restrict__ rho_out, float* __restrict__ H_out, float* __restrict__ ratio) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec<D> xi = load_vec<D>(x, i);
+    float Hi = H[i];
+    int b = offs[i], e = b + cnt[i];
+    float rs = 0.f, ds = 0.f;
+    for (int k = b; k < e; ++k) {
+        int j = __ldg(list + k);
+        Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+        float r = safe_sqrt(dot<D>(xij, xij));
+        float W, dWdH;
+        kernelWdH<KF, D>(r, Hi, W, dWdH);   // gather support
+        float mj = __ldg(m + j);
+        rs += mj * W;
+        ds += mj * dWdH;
+    }
+    // optimalSupportMonaghan.py:104-117
+    float rho = rs;
+    float safe_rho = isfinite(rho) ? fmaxf(rho, 1e-12f) : 1.f;
+    float Fv = Hi - volume_to_support<D>(m[i] / safe_rho, P.target_neighbors);
+    float dh_drho = -Hi / (rho * (float)D);
+    float omega = 1.f - dh_drho * ds;           // wp_omega.py: 1 - sum dh_drho m_j dW/dh
+    if (!isfinite(omega)) omega = 0.f;
+    float step = Fv / (omega + 1e-6f);
+    if (!isfinite(step)) step = 0.f;
+    float hn = Hi - step;
+    if (!isfinite(hn)) hn = Hi;
+    float lo = hb[0] * 0.25f, hi = hb[1] * 4.f;
+    hn = fminf(fmaxf(hn, lo), hi);
+    rho_out[i] = rho;
+    H_out[i] = hn;
+    if (ratio) ratio[i] = hn / (Hi + 1e-6f);
+}
+
+// ---------------------------------------------------------------- CRK volume and factors
+template <int KF, int D>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_crk_volume(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H,
+             const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+             float* __restrict__ V) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec<D> xi = load_vec<D>(x, i);
+    int b = offs[i], e = b + cnt[i];
+    float s = 0.f;
+    for (int k = b; k < e; ++k) {
+        int j = __ldg(list + k);
+        Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+        float r = safe_sqrt(dot<D>(xij, xij));
+        s += kernelW<KF, D>(r, __ldg(H + j));
+    }
+    V[i] = 1.f / s;
+}
+
+// Inverse of a symmetric DxD matrix in double; returns the determinant.
+template <int D> __device__ __forceinline__ double inv_sym(const double (&a)[D][D], double (&r)[D][D]) {
+    if constexpr (D == 1) {
+        double det = a[0][0];
+        r[0][0] = 1.0 / det;
+        return det;
+    } else if constexpr (D == 2) {
+        double det = a[0][0] * a[1][1] - a[0][1] * a[1][0];
+        double id = 1.0 / det;
+        r[0][0] = a[1][1] * id; r[1][1] = a[0][0] * id;
+        r[0][1] = -a[0][1] * id; r[1][0] = -a[1][0] * id;
+        return det;
+    } else {
+        double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+        double c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
+        double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+        double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+        double id = 1.0 / det;
+        r[0][0] = c00 * id;
+        r[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) * id;
+        r[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) * id;
+        r[1][0] = c01 * id;
+        r[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) * id;
+        r[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) * id;
+        r[2][0] = c02 * id;
+        r[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) * id;
+        r[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) * id;
+        return det;
+    }
+}
+
+// Moments (FP32 sums over the list, W_ij = W(r_ij, H_j)), FP64 solve for A, B, gradA,
+// gradB (Frontiere, Raskin & Owen 2017, linear reproducing conditions), and the
+// CRK density sum_j m_j W^R_ij.  Fallback to zeroth-order correction when the
+// second moment is singular (fewer than D+1 effective neighbours).
+template <int KF, int D>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_crk_factors(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+              const float* __restrict__ V, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
+              const int32_t* __restrict__ list, float* __restrict__ Aout, float* __restrict__ Bout,
+              float* __restrict__ gAout, float* __restrict__ gBout, float* __restrict__ rho_out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec<D> xi = load_vec<D>(x, i);
+    int b = offs[i], e = b + cnt[i];
+    float m0 = 0.f, m1[D], m2[D][D], dm0[D], dm1[D][D], dm2[D][D][D], s0 = 0.f, s1[D];
+    #pragma unroll
+    for (int a = 0; a < D; ++a) {
+        m1[a] = 0.f; dm0[a] = 0.f; s1[a] = 0.f;
+        #pragma unroll
+        for (int c = 0; c < D; ++c) { m2[a][c] = 0.f; dm1[a][c] = 0.f;
+            #pragma unroll
+            for (int g = 0; g < D; ++g) dm2[a][c][g] = 0.f; }
+    }
+    for (int k = b; k < e; ++k) {
+        int j = __ldg(list + k);
+        Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+        float r = safe_sqrt(dot<D>(xij, xij));
+        float W; Vec<D> gW;
+        kernelWG<KF, D>(xij, r, __ldg(H + j), W, gW);
+        if (W == 0.f) continue;
+        float Vj = __ldg(V + j), mj = __ldg(m + j);
+        float VW = Vj * W;
+        m0 += VW;
+        s0 += mj * W;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) {
+            m1[a] += VW * xij.v[a];
+            s1[a] += mj * W * xij.v[a];
+            dm0[a] += Vj * gW.v[a];
+            #pragma unroll
+            for (int c = 0; c < D; ++c) {
+                m2[a][c] += VW * xij.v[a] * xij.v[c];
+                // d/dx^c of (x^a W): x^a dW/dx^c + delta_ac W
+                dm1[a][c] += Vj * (xij.v[a] * gW.v[c] + (a == c ? W : 0.f));
+            }
+        }
+        #pragma unroll
+        for (int a = 0; a < D; ++a)
+            #pragma unroll
+            for (int c = a; c < D; ++c)
+                #pragma unroll
+                for (int g = 0; g < D; ++g)
+                    dm2[a][c][g] += Vj * (xij.v[a] * xij.v[c] * gW.v[g] + ((a == g ? xij.v[c] : 0.f) + (c == g ? xij.v[a] : 0.f)) * W);
+    }
+    // FP64 solve
+    double M2[D][D], Mi[D][D];
+    double tr = 0.0;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) {
+        #pragma unroll
+        for (int c = 0; c < D; ++c) M2[a][c] = (double)(a <= c ? m2[a][c] : m2[c][a]);
+        tr += M2[a][a];
+    }
+    double det = inv_sym<D>(M2, Mi);
+    double scale = tr / D;
+    double sD = scale; for (int a = 1; a < D; ++a) sD *= scale;
+    bool ok = isfinite(det) && fabs(det) > 1e-10 * fabs(sD) && m0 > 0.f;
+    double A, Bv[D], gA[D], gB[D][D];
+    if (ok) {
+        // B = -M2^-1 m1 ; A = 1/(m0 + m1.B)
+        double mb = m0;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) {
+            double t = 0.0;
+            #pragma unroll
+            for (int c = 0; c < D; ++c) t -= Mi[a][c] * (double)m1[c];
+            Bv[a] = t;
+        }
+        #pragma unroll
+        for (int a = 0; a < D; ++a) mb += (double)m1[a] * Bv[a];
+        A = 1.0 / mb;
+        // dB/dx^g = -M2^-1 (dm1[:,g] + dm2[:,:,g] B)
+        #pragma unroll
+        for (int g = 0; g < D; ++g) {
+            double rhs[D];
+            #pragma unroll
+            for (int a = 0; a < D; ++a) {
+                double t = (double)dm1[a][g];
+                #pragma unroll
+                for (int c = 0; c < D; ++c) t += (double)(a <= c ? dm2[a][c][g] : dm2[c][a][g]) * Bv[c];
+                rhs[a] = t;
+            }
+            #pragma unroll
+            for (int a = 0; a < D; ++a) {
+                double t = 0.0;
+                #pragma unroll
+                for (int c = 0; c < D; ++c) t -= Mi[a][c] * rhs[c];
+                gB[a][g] = t;
+            }
+        }
+        // dA/dx^g = -A^2 (dm0_g + dm1[:,g].B + m1.dB[:,g])
+        #pragma unroll
+        for (int g = 0; g < D; ++g) {
+            double t = (double)dm0[g];
+            #pragma unroll
+            for (int a = 0; a < D; ++a) t += (double)dm1[a][g] * Bv[a] + (double)m1[a] * gB[a][g];
+            gA[g] = -A * A * t;
+        }
+    } else {
+        double m0d = (double)m0;
+        A = 1.0 / m0d;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) {
+            Bv[a] = 0.0;
+            gA[a] = -(double)dm0[a] / (m0d * m0d);
+            #pragma unroll
+            for (int c = 0; c < D; ++c) gB[a][c] = 0.0;
+        }
+    }
+    double rho = (double)s0;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) rho += Bv[a] * (double)s1[a];
+    rho *= A;
+    Aout[i] = (float)A;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) {
+        Bout[(size_t)i * D + a] = (float)Bv[a];
+        gAout[(size_t)i * D + a] = (float)gA[a];
+        #pragma unroll
+        for (int c = 0; c < D; ++c) gBout[(size_t)i * D * D + a * D + c] = (float)gB[a][c];
+    }
+    if (rho_out) rho_out[i] = (float)rho;
+}
+
+// ---------------------------------------------------------------- EOS
+__global__ void k_eos(int n, float gamma, const float* __restrict__ u, const float* __restrict__ rho,
+                      float* __restrict__ Aout, float* __restrict__ Pout, float* __restrict__ cout) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float ui = u[i], r = rho[i];
+    if (cout) cout[i] = sqrtf(fabsf(ui) * gamma * (gamma - 1.f));
+    if (Pout) Pout[i] = (gamma - 1.f) * r * ui;
+    if (Aout) Aout[i] = ui * (gamma - 1.f) * powf(r, 1.f - gamma);
+}
+
+// ---------------------------------------------------------------- CRK velocity gradient (+ Cullen div, v_sig)
+template <int KF, int D>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_grad_v(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+         const float* __restrict__ rho, const float* __restrict__ V, const float* __restrict__ A, const float* __restrict__ B,
+         const float* __restrict__ gA, const float* __restrict__ gB, const float* __restrict__ v, const float* __restrict__ c,
+         const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+         float* __restrict__ DvDx, float* __restrict__ drhodt, float* __restrict__ div_out, float* __restrict__ vsig_out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
+    float Hi = H[i];
+    float Ai = A[i];
+    Vec<D> Bi = load_vec<D>(B, i), gAi = load_vec<D>(gA, i);
+    Mat<D> gBi = load_mat<D>(gB, i);
+    bool want_cd = div_out != nullptr;
+    float ci = want_cd ? c[i] : 0.f;
+    Mat<D> G = mzero<D>();
+    float div = 0.f, vsig = 0.f;
+    float vs2 = P.verlet_scale;
+    int b = offs[i], e = b + cnt[i];
+    for (int k = b; k < e; ++k) {
+        int j = __ldg(list + k);
+        Vec<D> xj = load_vec<D>(x, j);
+        Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
+        float r = safe_sqrt(dot<D>(xij, xij));
+        float Hj = __ldg(H + j);
+        Vec<D> vj = load_vec<D>(v, j);
+        float W; Vec<D> gW;
+        kernelWG<KF, D>(xij, r, Hj, W, gW);
+        if (W != 0.f) {
+            Vec<D> gR = crk_grad<D>(xij, W, gW, Ai, Bi, gAi, gBi);
+            float Vj = __ldg(V + j);
+            #pragma unroll
+            for (int a = 0; a < D; ++a) {
+                float dv = Vj * (vj.v[a] - vi.v[a]);
+                #pragma unroll
+                for (int g = 0; g < D; ++g) G.m[a][g] += dv * gR.v[g];
+            }
+        }
+        if (want_cd) {
+            float Hs = wmax(Hi, Hj);
+            if (r < Hs) {
+                float W2; Vec<D> g2;
+                kernelWG<KF, D>(xij, r, Hs, W2, g2);
+                float vol = __ldg(m + j) / __ldg(rho + j);
+                float s = 0.f;
+                #pragma unroll
+                for (int a = 0; a < D; ++a) s += (vj.v[a] - vi.v[a]) * g2.v[a];
+                div += vol * s;
+            }
+            // signal velocity over the Verlet set r < verlet_scale*max(H_i, H_j)
+            if (r < vs2 * Hs) {
+                float mu = 0.f;
+                #pragma unroll
+                for (int a = 0; a < D; ++a) mu += (vi.v[a] - vj.v[a]) * xij.v[a];
+                mu = mu / (r + 1e-14f * Hi);
+                float vsv = 0.5f * (ci + __ldg(c + j)) - mu;
+                if (mu > 0.f) vsv = 0.f;
+                vsig = wmax(vsig, vsv);
+            }
+        }
+    }
+    store_mat<D>(DvDx, i, G);
+    if (drhodt) {
+        float tr = G.m[0][0];
+        #pragma unroll
+        for (int a = 1; a < D; ++a) tr += G.m[a][a];
+        drhodt[i] = -tr * rho[i];
+    }
+    if (want_cd) { div_out[i] = div; if (vsig_out) vsig_out[i] = fabsf(vsig); }
+}
+
+// ---------------------------------------------------------------- Cullen-Dehnen R pass + switch algebra
+template <int KF, int D>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+         const float* __restrict__ rho, const float* __restrict__ div, const float* __restrict__ div_prev,
+         const float* __restrict__ vsig, const float* __restrict__ alpha0_prev, const float* __restrict__ dtp,
+         const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+         float* __restrict__ alpha_out, float* __restrict__ R_out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec<D> xi = load_vec<D>(x, i);
+    float Hi = H[i];
+    int b = offs[i], e = b + cnt[i];
+    float s = 0.f;
+    for (int k = b; k < e; ++k) {
+        int j = __ldg(list + k);
+        Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+        float r = safe_sqrt(dot<D>(xij, xij));
+        float W = kernelW<KF, D>(r, Hi);   // gather
+        if (W == 0.f) continue;
+        float dj = __ldg(div + j);
+        float sg = dj > 0.f ? 1.f : (dj < 0.f ? -1.f : 0.f);
+        float rj = __ldg(rho + j);
+        s += __ldg(m + j) / rj * (rj * sg) * W;
+    }
+    float rhoi = rho[i];
+    float R = 1.f / rhoi * s;
+    float dv = div[i];
+    float dt = *dtp;
+    // CullenDehnen2010.py:183-191 (S = None -> trace 0)
+    float omr = 1.f - R;
+    float omr2 = omr * omr;
+    float nom = P.beta_xi * (omr2 * omr2) * dv;
+    float Xi = P.limit_xi ? (nom * nom + 1e-14f * Hi) / (nom * nom + 0.f + 1e-14f * Hi)
+                          : (nom * nom) / (nom * nom + 0.f + 1e-14f * Hi);
+    float ddiv = (dv - div_prev[i]) / dt;
+    float Ai = Xi * fmaxf(-ddiv, 0.f);
+    float vs = vsig[i];
+    float scaling = Hi * Hi * Ai / (vs * vs + Hi * Hi * Ai + 1e-14f * Hi);
+    float alphas = P.alpha_max * scaling;
+    alphas = fminf(fmaxf(alphas, P.alpha_min), P.alpha_max);
+    float a0 = alpha0_prev[i];
+    float fk = 1.f / P.kxi;
+    float tau = Hi * fk / (2.f * 0.05f * vs);
+    float adot = (alphas - a0) / tau;
+    a0 = alphas > a0 ? alphas : a0;
+    a0 = alphas < a0 ? a0 + adot * dt : a0;
+    a0 = fminf(fmaxf(a0, P.alpha_min), P.alpha_max);
+    alpha_out[i] = a0;
+    if (R_out) R_out[i] = R;
+}
+
+// Balsara switch from the velocity gradient.
+template <int D>
+__global__ void k_balsara(int n, const float* __restrict__ DvDx, const float* __restrict__ c, float* __restrict__ alpha) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Mat<D> G = load_mat<D>(DvDx, i);
+    float dv = G.m[0][0];
+    for (int a = 1; a < D; ++a) dv += G.m[a][a];
+    float curl2 = 0.f;
+    if constexpr (D == 2) { float w = G.m[1][0] - G.m[0][1]; curl2 = w * w; }
+    if constexpr (D == 3) {
+        float w0 = G.m[2][1] - G.m[1][2], w1 = G.m[0][2] - G.m[2][0], w2 = G.m[1][0] - G.m[0][1];
+        curl2 = w0 * w0 + w1 * w1 + w2 * w2;
+    }
+    float ad = fabsf(dv);
+    float bal = ad / (ad + sqrtf(curl2) + 1e-4f * c[i]);
+    alpha[i] = fminf(fmaxf(bal, 0.f), 1.f);
+}
+
+// ---------------------------------------------------------------- CRK accel + dudt
+// modules/crk/limiter.py:10-16
+__device__ __forceinline__ float limiter_vl(float x) {
+    if (x <= 0.f) return 0.f;
+    float vL = 2.f / (1.f + x);
+    return x * vL * vL;
+}
+__device__ __forceinline__ float sgn_pos(float x) { return x >= 0.f ? 1.f : -1.f; }
+
+// modules/crk/limiter.py:27-86 (quadratic-form Van Leer)
+template <int D>
+__device__ __forceinline__ float van_leer(const Vec<D>& xij_, const Mat<D>& Gi, const Mat<D>& Gj) {
+    Vec<D> h;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) h.v[a] = 0.5f * xij_.v[a];
+    float gi = dot<D>(matvec<D>(Gi, h), h);
+    float gj = dot<D>(matvec<D>(Gj, h), h);
+    float ri = gi / (sgn_pos(gj) * fabsf(gj));
+    float rj = gj / (sgn_pos(gi) * fabsf(gi));
+    if (ri != ri) ri = 1.f;
+    if (rj != rj) rj = 1.f;
+    return limiter_vl(wmin(ri, rj));
+}
+// modules/crk/limiter.py:89-128 (eta measured in supports H)
+template <int D>
+__device__ __forceinline__ float crk_limiter(const Vec<D>& xij, float hi, float hj, float eta_crit, float eta_fold) {
+    float ni = 0.f, nj = 0.f;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) { float ei = xij.v[a] / hi, ej = xij.v[a] / hj; ni += ei * ei; nj += ej * ej; }
+    float eta = wmin(safe_sqrt(ni), safe_sqrt(nj));
+    float f = 1.f;
+    if (eta < eta_crit) { float t = (eta - eta_crit) / eta_fold; f = expf(-(t * t)); }
+    return f;
+}
+
+template <int KF, int D>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+                 const float* __restrict__ rho, const float* __restrict__ V, const float* __restrict__ A,
+                 const float* __restrict__ B, const float* __restrict__ gA, const float* __restrict__ gB,
+                 const float* __restrict__ v, const float* __restrict__ c, const float* __restrict__ Pr,
+                 const float* __restrict__ DvDx, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
+                 const int32_t* __restrict__ list, float* __restrict__ dvdt, float* __restrict__ dudt,
+                 float* __restrict__ ap, float* __restrict__ av) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
+    float Hi = H[i], mi = m[i], rhoi = rho[i], Vi = V[i], ci = c[i], Pi = Pr[i];
+    float Ai = A[i];
+    Vec<D> Bi = load_vec<D>(B, i), gAi = load_vec<D>(gA, i);
+    Mat<D> gBi = load_mat<D>(gB, i), Gi = load_mat<D>(DvDx, i);
+    const float ks = P.kscale;
+    const float smooth_i = Hi / ks;
+    const bool comp = P.kahan != 0;
+    KSum acc[D], du;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) acc[a].init();
+    du.init();
+    int b = offs[i], e = b + cnt[i];
+    for (int k = b; k < e; ++k) {
+        int j = __ldg(list + k);
+        Vec<D> xj = load_vec<D>(x, j);
+        Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
+        float r2 = dot<D>(xij, xij);
+        float Hj = __ldg(H + j);
+        float Hm = wmax(Hi, Hj);
+        if (!(r2 < Hm * Hm)) {
+            if (ap) store_vec<D>(ap, k, vzero<D>());
+            if (av) store_vec<D>(av, k, vzero<D>());
+            continue;
+        }
+        float r = safe_sqrt(r2);
+        Vec<D> vj = load_vec<D>(v, j);
+        float rhoj = __ldg(rho + j), Vj = __ldg(V + j), cj = __ldg(c + j), Pj = __ldg(Pr + j);
+        Mat<D> Gj = load_mat<D>(DvDx, j);
+        // limiters
+        float factor = 1.f;
+        if (P.enable_crk_limiter) factor = crk_limiter<D>(xij, Hi, Hj, P.eta_crit, P.eta_fold);
+        float phi = 0.f;
+        if (P.enable_vanleer) phi = van_leer<D>(xij, Gi, Gj) * factor;
+        if (P.force_vl_off) phi = 0.f;
+        if (P.force_vl_on) phi = 1.f;
+        phi = wmax(wmin(phi, 1.f), 0.f);
+        Vec<D> Gix = matvec<D>(Gi, xij), Gjx = matvec<D>(Gj, xij);
+        float hp = phi / 2.f;
+        Vec<D> vdi, vdj_a, vdj_d;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) {
+            vdi.v[a] = vi.v[a] - hp * Gix.v[a];
+            vdj_a.v[a] = vj.v[a] + hp * Gjx.v[a];        // accel.py:138
+            vdj_d.v[a] = vj.v[a] + hp * (-Gjx.v[a]);     // dudt.py:123 (matmul(gradV_j, -x_ij))
+        }
+        // corrected gradients
+        float Wi; Vec<D> gWi;
+        kernelWG<KF, D>(xij, r, Hj, Wi, gWi);
+        Vec<D> gradw_i = crk_grad<D>(xij, Wi, gWi, Ai, Bi, gAi, gBi);
+        float Aj = __ldg(A + j);
+        Vec<D> Bj = load_vec<D>(B, j), gAj = load_vec<D>(gA, j);
+        Mat<D> gBj = load_mat<D>(gB, j);
+        Vec<D> xji;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) xji.v[a] = -xij.v[a];
+        float Wj; Vec<D> gWj;
+        kernelWG<KF, D>(xji, r, Hi, Wj, gWj);
+        Vec<D> gradw_j = crk_grad<D>(xji, Wj, gWj, Aj, Bj, gAj, gBj);
+        Vec<D> gij;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) gij.v[a] = 0.5f * (gradw_i.v[a] - gradw_j.v[a]);
+        // viscous Q (accel.py:189-206 / dudt.py:174-191)
+        float smooth_j = Hj / ks;
+        float ee_i = 0.f, ee_j = 0.f, mi_a = 0.f, mj_a = 0.f, mi_d = 0.f, mj_d = 0.f;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) {
+            float ei = xij.v[a] / smooth_i, ej = xij.v[a] / smooth_j;
+            ee_i += ei * ei; ee_j += ej * ej;
+            float da = vdi.v[a] - vdj_a.v[a], dd = vdi.v[a] - vdj_d.v[a];
+            mi_a += da * ei; mj_a += da * ej;
+            mi_d += dd * ei; mj_d += dd * ej;
+        }
+        float den_i = ee_i + 1.0e-7f * smooth_i * smooth_i, den_j = ee_j + 1.0e-7f * smooth_j * smooth_j;
+        mi_a = wmin(0.f, mi_a / den_i); mj_a = wmin(0.f, mj_a / den_j);
+        mi_d = wmin(0.f, mi_d / den_i); mj_d = wmin(0.f, mj_d / den_j);
+        float Qi_a = rhoi * (-P.C_l * ci * mi_a + P.C_q * mi_a * mi_a);
+        float Qj_a = rhoj * (-P.C_l * cj * mj_a + P.C_q * mj_a * mj_a);
+        float Qi_d = rhoi * (-P.C_l * ci * mi_d + P.C_q * mi_d * mi_d);
+        float Qj_d = rhoj * (-P.C_l * cj * mj_d + P.C_q * mj_d * mj_d);
+        // accel.py:228-249
+        Vec<D> pt, vt;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) {
+            pt.v[a] = -(Pi + Pj) * gij.v[a] * Vi * Vj / mi;
+            vt.v[a] = -(Qi_a + Qj_a) * Vj * 1.f * gij.v[a] * Vi / mi;
+            acc[a].add(pt.v[a] + vt.v[a], comp);
+        }
+        if (ap) store_vec<D>(ap, k, pt);
+        if (av) store_vec<D>(av, k, vt);
+        // dudt.py:208-226
+        float dotu = 0.f;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) dotu += (vi.v[a] - vj.v[a]) * gij.v[a];
+        float pTerm = Pj * dotu * Vi * Vj / mi;
+        float vTerm = 0.5f * (Qi_d + Qj_d) * 1.f * dotu * Vi * Vj / mi;
+        du.add(pTerm + vTerm, comp);
+    }
+    if (dvdt) {
+        Vec<D> o;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) o.v[a] = acc[a].value();
+        store_vec<D>(dvdt, i, o);
+    }
+    if (dudt) dudt[i] = du.value();
+}
+
+// ---------------------------------------------------------------- energy partition f_ij
+__device__ __forceinline__ float sgn0(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
+
+template <int D>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restrict__ rho, const float* __restrict__ Pr,
+          const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ dvdt, const float* __restrict__ dtp,
+          const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+          const float* __restrict__ ap, const float* __restrict__ av, float* __restrict__ fout) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float dt = *dtp;
+    float hdt = 0.5f * dt;
+    Vec<D> vi = load_vec<D>(v, i), ai = load_vec<D>(dvdt, i);
+    #pragma unroll
+    for (int a = 0; a < D; ++a) vi.v[a] = vi.v[a] + hdt * ai.v[a];
+    float mi = m[i], rhoi = rho[i], Pi = Pr[i], ui = u[i];
+    const int scheme = P.energy_scheme;
+    float si = 0.f;
+    if (scheme == SPH_ENERGY_CRK) si = Pi / powf(rhoi, P.gamma);
+    int b = offs[i], e = b + cnt[i];
+    for (int k = b; k < e; ++k) {
+        int j = __ldg(list + k);
+        Vec<D> vj = load_vec<D>(v, j), aj = load_vec<D>(dvdt, j);
+        Vec<D> apk = load_vec<D>(ap, k), avk = load_vec<D>(av, k);
+        float mj = __ldg(m + j), rhoj = __ldg(rho + j), Pj = __ldg(Pr + j), uj = __ldg(u + j);
+        float dE = 0.f;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) dE += ((vj.v[a] + hdt * aj.v[a]) - vi.v[a]) * (apk.v[a] + avk.v[a]);
+        dE = mi * dE * dt;
+        float uji = uj - ui;
+        float f = 0.5f;
+        if (scheme == SPH_ENERGY_EQUALWORK) {
+            f = 0.5f;
+        } else if (scheme == SPH_ENERGY_PDV) {
+            f = (Pi / (rhoi * rhoi)) / (Pi / (rhoi * rhoi) + Pj / (rhoj * rhoj));
+        } else if (scheme == SPH_ENERGY_DIMINISHING) {
+            float un = fabsf(uji);
+            f = 0.5f * (1.f + (uji * sgn0(dE)) / (un + 1.f / (1.f + un)));
+        } else if (scheme == SPH_ENERGY_MONOTONIC || scheme == SPH_ENERGY_HYBRID) {
+            float Aq = dE / (uji + 1.0e-14f);
+            float Bq = Aq >= 0.f ? Aq / mi : Aq / mj;
+            float t1 = wmax(0.f, sgn0(Bq));
+            float t2 = mi / (dE + 1.0e-14f) * ((dE + mi * ui + mj * uj) / (mi + mj) - ui);
+            float fm = fabsf(Bq) <= 1.f ? t1 : t2;
+            if (scheme == SPH_ENERGY_MONOTONIC) f = fm;
+            else {
+                float un = fabsf(uji);
+                float fsm = 0.5f * (1.f + (uji * sgn0(dE)) / (un + 1.f / (1.f + un)));
+                float chi = fabsf(uji) / (fabsf(ui) + fabsf(uj) + 1.0e-14f);
+                f = chi * fm + (1.f - chi) * fsm;
+            }
+        } else if (scheme == SPH_ENERGY_CRK) {
+            float sj = Pj / powf(rhoj, P.gamma);
+            float smin = wmin(fabsf(si), fabsf(sj)), smax = wmax(fabsf(si), fabsf(sj));
+            bool mA = fabsf(si - sj) == 0.f;
+            bool mB = (dE >= 0.f && si >= sj) || (dE < 0.f && si < sj);
+            bool mC = (dE >= 0.f && si < sj) || (dE < 0.f && si >= sj);
+            f = 0.5f;
+            if (mA) f = 0.5f;
+            if (!mA && mB) f = smin / (smin + smax + 1.0e-14f);
+            if (!mA && !mB && mC) f = smax / (smin + smax + 1.0e-14f);
+            f = wmax(0.f, wmin(1.f, f));
+        }
+        fout[k] = f;
+    }
+}
+
+// ---------------------------------------------------------------- CFL dt
+__global__ void k_cfl_reduce(int n, float gamma, const float* __restrict__ H, const float* __restrict__ u,
+                             float* __restrict__ red /* [0]=min H, [1]=max c */) {
+    float hmin = __int_as_float(0x7f800000), cmax = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        hmin = fminf(hmin, H[i]);
+        cmax = fmaxf(cmax, sqrtf(fabsf(u[i]) * gamma * (gamma - 1.f)));
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        hmin = fminf(hmin, __shfl_xor_sync(0xffffffffu, hmin, o));
+        cmax = fmaxf(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(reinterpret_cast<int*>(red), __float_as_int(hmin));
+        atomicMax(reinterpret_cast<int*>(red + 1), __float_as_int(cmax));
+    }
+}
+__global__ void k_cfl_init(float* red) { red[0] = __int_as_float(0x7f800000); red[1] = 0.f; }
+__global__ void k_cfl_final(DevParams P, const float* __restrict__ red, const float* __restrict__ dt_prev, float* __restrict__ dt_out) {
+    // compressible.py:49-61 ; min_i cfl*h/(c_i*xi) is attained at max_i c_i
+    float dt = P.cfl * red[0] / (red[1] * P.kxi);
+    dt = fminf(fmaxf(dt, P.min_dt), P.max_dt);
+    if (dt_prev) {
+        float prev = *dt_prev;
+        if (dt > prev) dt = fminf(dt, P.dt_growth * prev);
+    }
+    *dt_out = dt;
+}
+
+// ---------------------------------------------------------------- RK stage combination
+struct KPtrs { const float* k[8]; float w[8]; };
+__global__ void k_rk_combine(int64_t count, const float* __restrict__ y0, int nk, KPtrs K, const float* __restrict__ dtp,
+                             int wrap_dim, DomainF dom, float* __restrict__ y) {
+    int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= count) return;
+    float dt = *dtp;
+    // explicitly rounded (no FMA) so the CPU oracle reproduces the stage states bit for bit
+    float s = 0.f;
+    for (int q = 0; q < nk; ++q) s = __fadd_rn(s, __fmul_rn(K.w[q], K.k[q][idx]));
+    float val = __fadd_rn(y0[idx], __fmul_rn(dt, s));
+    if (wrap_dim > 0) {
+        int a = (int)(idx % wrap_dim);
+        if (dom.periodic[a]) {
+            if (val >= dom.max[a]) val = __fsub_rn(val, dom.L[a]);
+            else if (val < dom.min[a]) val = __fadd_rn(val, dom.L[a]);
+        }
+    }
+    y[idx] = val;
+}
+
+// ---------------------------------------------------------------- compatible energy
+struct StagePtrs {
+    const float* dvdt[8];
+    const int32_t* offs[8];
+    const int32_t* cnt[8];
+    const int32_t* list[8];
+    const float* f[8];
+    const float* ap[8];
+    const float* av[8];
+    float w[8];
+};
+template <int D>
+__global__ void k_vhalf(int n, int ns, StagePtrs S, const float* __restrict__ dtp, const float* __restrict__ v0, float* __restrict__ vh) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float dt = *dtp;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) {
+        float fa = 0.f;
+        for (int s = 0; s < ns; ++s) fa += S.w[s] * S.dvdt[s][(size_t)i * D + a];
+        vh[(size_t)i * D + a] = v0[(size_t)i * D + a] + 0.5f * fa * dt;
+    }
+}
+template <int D>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_finalize(int n, int ns, StagePtrs S, int pdv, const float* __restrict__ dtp, const float* __restrict__ vh,
+           const float* __restrict__ u0, float* __restrict__ u_out, float* __restrict__ du_out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec<D> vi = load_vec<D>(vh, i);
+    float du = 0.f;
+    for (int s = 0; s < ns; ++s) {
+        const int32_t* __restrict__ lst = S.list[s];
+        const float* __restrict__ f = S.f[s];
+        const float* __restrict__ ap = S.ap[s];
+        const float* __restrict__ av = S.av[s];
+        int b = S.offs[s][i], e = b + S.cnt[s][i];
+        float w = S.w[s];
+        float acc = 0.f;
+        for (int k = b; k < e; ++k) {
+            int j = __ldg(lst + k);
+            Vec<D> vj = load_vec<D>(vh, j);
+            Vec<D> a1 = load_vec<D>(ap, k), a2 = load_vec<D>(av, k);
+            float fk = __ldg(f + k);
+            float d1 = 0.f, d2 = 0.f;
+            #pragma unroll
+            for (int a = 0; a < D; ++a) { float vji = vj.v[a] - vi.v[a]; d1 += vji * a1.v[a]; d2 += vji * a2.v[a]; }
+            float term = pdv ? (w * fk * d1 + w * 0.5f * d2) : (w * fk * (d1 + d2));
+            acc += term;
+        }
+        du += acc;
+    }
+    float dt = *dtp;
+    if (du_out) du_out[i] = du;
+    u_out[i] = u0[i] + du * dt;
+}
+
+// ---------------------------------------------------------------- conservation
+template <int D>
+__global__ void k_cons(int n, const float* __restrict__ m, const float* __restrict__ v, const float* __restrict__ u, double* out) {
+    double M = 0, KE = 0, IE = 0, p[3] = {0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double mi = m[i];
+        double v2 = 0;
+        for (int a = 0; a < D; ++a) { double va = v[(size_t)i * D + a]; v2 += va * va; p[a] += mi * va; }
+        M += mi; KE += 0.5 * mi * v2; IE += mi * (double)u[i];
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        M += __shfl_xor_sync(0xffffffffu, M, o); KE += __shfl_xor_sync(0xffffffffu, KE, o); IE += __shfl_xor_sync(0xffffffffu, IE, o);
+        for (int a = 0; a < 3; ++a) p[a] += __shfl_xor_sync(0xffffffffu, p[a], o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out + 0, M); atomicAdd(out + 1, KE); atomicAdd(out + 2, IE); atomicAdd(out + 3, KE + IE);
+        for (int a = 0; a < D; ++a) atomicAdd(out + 4 + a, p[a]);
+    }
+}
+
+}  // namespace wsph
+
+using namespace wsph;
+
+#define PAIR_PRELUDE()                                                        \
+    DevParams P;                                                              \
+    int rc = params_to_dev(p, &P);                                            \
+    if (rc) return rc;                                                        \
+    if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "%s: n out of range", __func__); \
+    if (n == 0) return SPH_OK;                                                \
+    cudaStream_t s = WSPH_STREAM(stream);                                     \
+    (void)s;
+
+#define CHECK_CSR() do { WSPH_CHECK_PTR(offs); WSPH_CHECK_PTR(cnt); WSPH_CHECK_PTR(list); } while (0)
+
+static int check_align_vec(const DevParams& P, const void* ptr, const char* name) {
+    if (P.dim == 2 && ptr && (reinterpret_cast<uintptr_t>(ptr) & 7))
+        return set_error(SPH_ERR_BAD_ARG, "%s must be 8-byte aligned for dim 2", name);
+    return SPH_OK;
+}
+
+extern "C" {
+
+int sph_density_gather(const SphParams* p, int64_t n, int32_t support_mode, const float* x, const float* H, const float* m,
+                       const int32_t* offs, const int32_t* cnt, const int32_t* list, float* rho_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho_out); CHECK_CSR();
+    if (support_mode < 0 || support_mode > 4) return set_error(SPH_ERR_BAD_ARG, "bad support mode %d", support_mode);
+    if ((rc = check_align_vec(P, x, "x"))) return rc;
+    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_density<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, support_mode, P, x, H, m, offs, cnt, list, rho_out)));
+    return check_launch("sph_density_gather");
+}
+
+int sph_adaptive_h_iter(const SphParams* p, int64_t n, int32_t support_mode, const float* x, const float* H, const float* m,
+                        const int32_t* offs, const int32_t* cnt, const int32_t* list, const float* hbounds,
+                        float* rho_out, float* H_out, float* ratio_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(hbounds); WSPH_CHECK_PTR(rho_out); WSPH_CHECK_PTR(H_out); CHECK_CSR();
+    if (support_mode != SPH_SUPPORT_GATHER) return set_error(SPH_ERR_UNSUPPORTED, "adaptive support: only the gather scheme is implemented");
+    if ((rc = check_align_vec(P, x, "x"))) return rc;
+    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_adaptive_h<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, offs, cnt, list, hbounds, rho_out, H_out, ratio_out)));
+    return check_launch("sph_adaptive_h_iter");
+}
+
+int sph_crk_volume(const SphParams* p, int64_t n, const float* x, const float* H, const int32_t* offs, const int32_t* cnt,
+                   const int32_t* list, float* V_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(V_out); CHECK_CSR();
+    if ((rc = check_align_vec(P, x, "x"))) return rc;
+    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_crk_volume<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, offs, cnt, list, V_out)));
+    return check_launch("sph_crk_volume");
+}
+
+int sph_crk_factors(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* V,
+                    const int32_t* offs, const int32_t* cnt, const int32_t* list, float* A, float* B, float* gradA,
+                    float* gradB, float* rho_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(V);
+    WSPH_CHECK_PTR(A); WSPH_CHECK_PTR(B); WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); CHECK_CSR();
+    if ((rc = check_align_vec(P, x, "x"))) return rc;
+    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_crk_factors<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out)));
+    return check_launch("sph_crk_factors");
+}
+
+int sph_eos_ideal_gas(const SphParams* p, int64_t n, const float* u, const float* rho, float* A_out, float* P_out,
+                      float* c_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(u); WSPH_CHECK_PTR(rho);
+    wsph::count_launch(); k_eos<<<grid_for(n, 256), 256, 0, s>>>((int)n, P.gamma, u, rho, A_out, P_out, c_out);
+    return check_launch("sph_eos_ideal_gas");
+}
+
+int sph_grad_v(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
+               const float* V, const float* A, const float* B, const float* gradA, const float* gradB, const float* v,
+               const float* c, const int32_t* offs, const int32_t* cnt, const int32_t* list, float* DvDx_out,
+               float* drhodt_out, float* div_out, float* vsig_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(V); WSPH_CHECK_PTR(A); WSPH_CHECK_PTR(B);
+    WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(DvDx_out); CHECK_CSR();
+    if (div_out) { WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(c); }
+    if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v")) || (rc = check_align_vec(P, B, "B")) ||
+        (rc = check_align_vec(P, gradA, "gradA")))
+        return rc;
+    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_grad_v<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
+                                                                                                  offs, cnt, list, DvDx_out, drhodt_out, div_out, vsig_out)));
+    return check_launch("sph_grad_v");
+}
+
+int sph_switch_cullen(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
+                      const float* div, const float* div_prev, const float* vsig, const float* alpha0_prev, const float* dt,
+                      const int32_t* offs, const int32_t* cnt, const int32_t* list, float* alpha_out, float* R_out,
+                      void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(div); WSPH_CHECK_PTR(div_prev);
+    WSPH_CHECK_PTR(vsig); WSPH_CHECK_PTR(alpha0_prev); WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(alpha_out); CHECK_CSR();
+    if ((rc = check_align_vec(P, x, "x"))) return rc;
+    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_cullen<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div, div_prev, vsig, alpha0_prev, dt,
+                                                                                                  offs, cnt, list, alpha_out, R_out)));
+    return check_launch("sph_switch_cullen");
+}
+
+int sph_switch_balsara(const SphParams* p, int64_t n, const float* DvDx, const float* c, float* alpha_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(DvDx); WSPH_CHECK_PTR(c); WSPH_CHECK_PTR(alpha_out);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_balsara<D><<<grid_for(n, 256), 256, 0, s>>>((int)n, DvDx, c, alpha_out)));
+    return check_launch("sph_switch_balsara");
+}
+
+int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
+                       const float* V, const float* A, const float* B, const float* gradA, const float* gradB,
+                       const float* v, const float* c, const float* Pr, const float* DvDx, const int32_t* offs,
+                       const int32_t* cnt, const int32_t* list, float* dvdt_out, float* dudt_out, float* ap_ij,
+                       float* av_ij, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(V); WSPH_CHECK_PTR(A);
+    WSPH_CHECK_PTR(B); WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(c); WSPH_CHECK_PTR(Pr);
+    WSPH_CHECK_PTR(DvDx); CHECK_CSR();
+    if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v")) || (rc = check_align_vec(P, B, "B")) ||
+        (rc = check_align_vec(P, gradA, "gradA")) || (rc = check_align_vec(P, dvdt_out, "dvdt")) ||
+        (rc = check_align_vec(P, ap_ij, "ap_ij")) || (rc = check_align_vec(P, av_ij, "av_ij")))
+        return rc;
+    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_crk_accel_dudt<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
+                                                                                                          Pr, DvDx, offs, cnt, list, dvdt_out, dudt_out, ap_ij, av_ij)));
+    return check_launch("sph_crk_accel_dudt");
+}
+
+int sph_crk_accel(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
+                  const float* V, const float* A, const float* B, const float* gradA, const float* gradB, const float* v,
+                  const float* c, const float* P, const float* DvDx, const int32_t* offs, const int32_t* cnt,
+                  const int32_t* list, float* dvdt_out, float* ap_ij, float* av_ij, void* stream) {
+    return sph_crk_accel_dudt(p, n, x, H, m, rho, V, A, B, gradA, gradB, v, c, P, DvDx, offs, cnt, list, dvdt_out, nullptr,
+                              ap_ij, av_ij, stream);
+}
+
+int sph_crk_dudt(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
+                 const float* V, const float* A, const float* B, const float* gradA, const float* gradB, const float* v,
+                 const float* c, const float* P, const float* DvDx, const int32_t* offs, const int32_t* cnt,
+                 const int32_t* list, float* dudt_out, void* stream) {
+    return sph_crk_accel_dudt(p, n, x, H, m, rho, V, A, B, gradA, gradB, v, c, P, DvDx, offs, cnt, list, nullptr, dudt_out,
+                              nullptr, nullptr, stream);
+}
+
+int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const float* rho, const float* Pr, const float* u,
+                        const float* v, const float* dvdt, const float* dt, const int32_t* offs, const int32_t* cnt,
+                        const int32_t* list, const float* ap_ij, const float* av_ij, float* f_ij_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(Pr); WSPH_CHECK_PTR(u); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(dvdt);
+    WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(ap_ij); WSPH_CHECK_PTR(av_ij); WSPH_CHECK_PTR(f_ij_out); CHECK_CSR();
+    if (P.energy_scheme < 0 || P.energy_scheme > 5) return set_error(SPH_ERR_BAD_ARG, "bad energy scheme %d", P.energy_scheme);
+    if ((rc = check_align_vec(P, v, "v")) || (rc = check_align_vec(P, dvdt, "dvdt")) || (rc = check_align_vec(P, ap_ij, "ap_ij")) ||
+        (rc = check_align_vec(P, av_ij, "av_ij")))
+        return rc;
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_balance<D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, m, rho, Pr, u, v, dvdt, dt, offs, cnt, list, ap_ij, av_ij, f_ij_out)));
+    return check_launch("sph_compsph_balance");
+}
+
+int sph_cfl_dt(const SphParams* p, int64_t n, const float* H, const float* u, const float* rho, const float* dt_prev,
+               float* dt_out, void* stream) {
+    DevParams P;
+    int rc = params_to_dev(p, &P);
+    if (rc) return rc;
+    if (n <= 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "sph_cfl_dt: n must be in [1, 2^31)");
+    WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(u); WSPH_CHECK_PTR(dt_out);
+    (void)rho;
+    cudaStream_t s = WSPH_STREAM(stream);
+    // dt_out doubles as the reduction scratch: [dt, hmin, cmax] need 3 floats -> use a static per-call layout
+    // in the caller's dt_out buffer (must hold 4 floats).
+    float* red = dt_out + 1;
+    wsph::count_launch(); k_cfl_init<<<1, 1, 0, s>>>(red);
+    int blocks = grid_for(n, 256);
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    wsph::count_launch(); k_cfl_reduce<<<blocks, 256, 0, s>>>((int)n, P.gamma, H, u, red);
+    wsph::count_launch(); k_cfl_final<<<1, 1, 0, s>>>(P, red, dt_prev, dt_out);
+    return check_launch("sph_cfl_dt");
+}
+
+int sph_rk_combine(const SphParams* p, int64_t count, const float* y0, int32_t nk, const float* const* k_ptrs,
+                   const double* weights, const float* dt, int32_t wrap_dim, float* y_out, void* stream) {
+    DevParams P;
+    int rc = params_to_dev(p, &P);
+    if (rc) return rc;
+    if (count < 0) return set_error(SPH_ERR_BAD_ARG, "sph_rk_combine: count < 0");
+    if (count == 0) return SPH_OK;
+    if (nk < 0 || nk > 8) return set_error(SPH_ERR_BAD_ARG, "sph_rk_combine: nk must be in [0, 8]");
+    WSPH_CHECK_PTR(y0); WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(y_out);
+    KPtrs K;
+    for (int q = 0; q < 8; ++q) { K.k[q] = nullptr; K.w[q] = 0.f; }
+    for (int q = 0; q < nk; ++q) {
+        if (!k_ptrs || !k_ptrs[q] || !weights) return set_error(SPH_ERR_BAD_ARG, "sph_rk_combine: null derivative %d", q);
+        K.k[q] = k_ptrs[q]; K.w[q] = (float)weights[q];
+    }
+    wsph::count_launch(); k_rk_combine<<<grid_for(count, 256), 256, 0, WSPH_STREAM(stream)>>>(count, y0, nk, K, dt, wrap_dim, P.dom, y_out);
+    return check_launch("sph_rk_combine");
+}
+
+int sph_finalize_compatible_energy(const SphParams* p, int64_t n, int32_t nstages, const double* weights, const float* dt,
+                                   const float* v0, const float* u0, const float* const* dvdt_s,
+                                   const int32_t* const* offs_s, const int32_t* const* cnt_s, const int32_t* const* list_s,
+                                   const float* const* f_ij_s, const float* const* ap_ij_s, const float* const* av_ij_s,
+                                   float* u_out, float* du_out, void* stream) {
+    PAIR_PRELUDE();
+    if (nstages < 1 || nstages > 8) return set_error(SPH_ERR_BAD_ARG, "nstages must be in [1, 8]");
+    WSPH_CHECK_PTR(weights); WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(v0); WSPH_CHECK_PTR(u0); WSPH_CHECK_PTR(u_out);
+    WSPH_CHECK_PTR(dvdt_s); WSPH_CHECK_PTR(offs_s); WSPH_CHECK_PTR(cnt_s); WSPH_CHECK_PTR(list_s);
+    WSPH_CHECK_PTR(f_ij_s); WSPH_CHECK_PTR(ap_ij_s); WSPH_CHECK_PTR(av_ij_s);
+    StagePtrs S;
+    for (int q = 0; q < nstages; ++q) {
+        if (!dvdt_s[q] || !offs_s[q] || !cnt_s[q] || !list_s[q] || !f_ij_s[q] || !ap_ij_s[q] || !av_ij_s[q])
+            return set_error(SPH_ERR_BAD_ARG, "finalize: null array for stage %d", q);
+        S.dvdt[q] = dvdt_s[q]; S.offs[q] = offs_s[q]; S.cnt[q] = cnt_s[q]; S.list[q] = list_s[q];
+        S.f[q] = f_ij_s[q]; S.ap[q] = ap_ij_s[q]; S.av[q] = av_ij_s[q]; S.w[q] = (float)weights[q];
+    }
+    // the half-step velocity goes into du_out's companion scratch: caller passes du_out with room for n*(1+dim) floats
+    if (!du_out) return set_error(SPH_ERR_BAD_ARG, "finalize: du_out must hold n*(1+dim) floats (du and v_half scratch)");
+    float* vh = du_out + n;
+    int pdv = P.energy_scheme == SPH_ENERGY_PDV;
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_vhalf<D><<<grid_for(n, 256), 256, 0, s>>>((int)n, nstages, S, dt, v0, vh)));
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_finalize<D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, nstages, S, pdv, dt, vh, u0, u_out, du_out)));
+    return check_launch("sph_finalize_compatible_energy");
+}
+
+int sph_conservation_sums(const SphParams* p, int64_t n, const float* m, const float* v, const float* u, double* out,
+                          void* stream) {
+    DevParams P;
+    int rc = params_to_dev(p, &P);
+    if (rc) return rc;
+    WSPH_CHECK_PTR(out);
+    cudaStream_t s = WSPH_STREAM(stream);
+    cudaMemsetAsync(out, 0, sizeof(double) * 7, s);
+    if (n <= 0) return check_launch("sph_conservation_sums");
+    WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(u);
+    int blocks = grid_for(n, 256);
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_cons<D><<<blocks, 256, 0, s>>>((int)n, m, v, u, out)));
+    return check_launch("sph_conservation_sums");
+}
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+"""Explicit Runge-Kutta integrators with the call shape of the reference's absent
+warpSPHIntegrators package: ``getIntegrator(type).function(state=system, f=step_fn,
+dt=..., config=..., compParams=...)`` returning an object with ``.state`` and
+``.stages`` (call site examples/compressible/01-sod-shock-tube-1d.py:196-210).
+
+Tableaux (restated; the package's own choice is not visible):
+  explicitEuler       c=[0],          b=[1]
+  rungeKutta2 (Heun)  c=[0,1],        a21=1,                    b=[1/2,1/2]
+  rungeKutta4         c=[0,1/2,1/2,1], a21=a32=1/2, a43=1,       b=[1/6,1/3,1/3,1/6]
+Stage s starts from a copy of stage s-1's state (so non-integrated fields such as
+the supports carry over), with positions, velocities and internal energies set to
+y0 + dt * sum_k a_sk K_k; periodic positions are wrapped into the domain.  After
+the last stage the integrated fields are y0 + dt * sum_s b_s K_s and the system's
+``finalize`` runs (compatible energy).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Any, List
+
+import torch
+
+from . import ops
+from .core import IntegrationSchemeType
+
+
+@dataclass
+class StageRecord:
+    update: Any
+    aux: Any
+
+
+@dataclass
+class IntegrationResult:
+    state: Any
+    stages: List[StageRecord] = field(default_factory=list)
+
+
+_TABLEAUX = {
+    IntegrationSchemeType.explicitEuler: ([[]], [1.0], [0.0]),
+    IntegrationSchemeType.rungeKutta2: ([[], [1.0]], [0.5, 0.5], [0.0, 1.0]),
+    IntegrationSchemeType.rungeKutta4: ([[], [0.5], [0.0, 0.5], [0.0, 0.0, 1.0]], [1 / 6, 1 / 3, 1 / 3, 1 / 6], [0.0, 0.5, 0.5, 1.0]),
+}
+
+
+class RungeKuttaIntegrator:
+    def __init__(self, scheme: IntegrationSchemeType):
+        if scheme not in _TABLEAUX:
+            raise ValueError(f"integration scheme {scheme} is not available on this path")
+        self.scheme = scheme
+        self.a, self.b, self.c = _TABLEAUX[scheme]
+
+    def _combine(self, params, y0, ks, ws, dt, wrap_dim):
+        pairs = [(k, w) for k, w in zip(ks, ws) if w != 0.0]
+        return ops.rk_combine(params, y0, [k for k, _ in pairs], [w for _, w in pairs], dt, wrap_dim)
+
+    def function(self, state, f, dt, config, compParams, verbose=False, **kwargs) -> IntegrationResult:
+        from .configurations import make_params
+        params = make_params(config, compParams)
+        sys0 = state
+        S0 = sys0.state
+        dim = int(config.dim)
+        updates, returnValues = [], []
+        prev = S0
+        adjacency = sys0.adjacency
+        for s in range(len(self.b)):
+            Ss = prev.initializeNewState()
+            if s > 0:
+                aw = self.a[s]
+                Ss.positions = self._combine(params, S0.positions, [u.dxdt for u in updates], aw, dt, dim)
+                Ss.velocities = self._combine(params, S0.velocities, [u.dvdt for u in updates], aw, dt, 0)
+                Ss.internalEnergies = self._combine(params, S0.internalEnergies, [u.dudt for u in updates], aw, dt, 0)
+            t_s = sys0.t + self.c[s] * (float(dt) if not isinstance(dt, torch.Tensor) else 0.0)
+            sys_s = type(sys0)(state=Ss, adjacency=adjacency, domain=sys0.domain, t=t_s)
+            update, adjacency, Sout = f(sys_s, dt, config, compParams, verbose=verbose)
+            updates.append(update)
+            returnValues.append((adjacency, Sout))
+            prev = Sout
+        Sf = prev.initializeNewState()
+        Sf.positions = self._combine(params, S0.positions, [u.dxdt for u in updates], self.b, dt, dim)
+        Sf.velocities = self._combine(params, S0.velocities, [u.dvdt for u in updates], self.b, dt, 0)
+        Sf.internalEnergies = self._combine(params, S0.internalEnergies, [u.dudt for u in updates], self.b, dt, 0)
+        new_sys = type(sys0)(state=Sf, adjacency=adjacency, domain=sys0.domain, t=sys0.t)
+        new_sys.finalize(sys0, dt, returnValues, updates, self.b, config, compParams)
+        new_sys.t = sys0.t + (float(dt) if not isinstance(dt, torch.Tensor) else 0.0)
+        if isinstance(dt, torch.Tensor):
+            new_sys.t_device = getattr(sys0, "t_device", 0.0) + dt
+        stages = [StageRecord(update=u, aux=rv) for u, rv in zip(updates, returnValues)]
+        return IntegrationResult(state=new_sys, stages=stages)
+
+
+def getIntegrator(scheme: IntegrationSchemeType) -> RungeKuttaIntegrator:
+    return RungeKuttaIntegrator(scheme)

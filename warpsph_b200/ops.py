@@ -1,0 +1,351 @@
+"""Torch-tensor wrappers of the C ABI (one function per entry point).
+
+Every function takes CUDA float32 / int32 tensors, allocates its outputs with torch
+on the same device, and enqueues the CUDA kernels on the current torch stream.
+Errors from the library raise RuntimeError; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import torch
+
+from . import _capi
+from ._capi import check, fptr, iptr, ptr, stream_ptr
+from .core import AdjacencyList, CRKState, SupportScheme
+
+
+class KernelTimer:
+    """Records CUDA events around selected library calls on the launching stream.
+
+    ``names`` is the set of wrapper names to time (None = all).  Durations are read
+    with ``summary()`` after a synchronize."""
+
+    def __init__(self, names=None):
+        self.names = None if names is None else set(names)
+        self.events = []
+
+    def wants(self, name: str) -> bool:
+        return self.names is None or name in self.names
+
+    def summary(self) -> dict:
+        out = {}
+        for name, a, b in self.events:
+            t = out.setdefault(name, [0, 0.0])
+            t[0] += 1
+            t[1] += a.elapsed_time(b)
+        return {k: {"launches": v[0], "total_ms": v[1], "avg_ms": v[1] / max(v[0], 1)} for k, v in out.items()}
+
+
+TIMER: Optional[KernelTimer] = None
+
+
+class _timed:
+    def __init__(self, name: str):
+        self.name = name
+
+    def __enter__(self):
+        t = TIMER
+        self.ev = None
+        if t is not None and t.wants(self.name):
+            self.ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            self.ev[0].record()
+        return self
+
+    def __exit__(self, *exc):
+        if self.ev is not None:
+            self.ev[1].record()
+            TIMER.events.append((self.name, self.ev[0], self.ev[1]))
+        return False
+
+
+_SUPPORT = {SupportScheme.Gather: 0, SupportScheme.Scatter: 1, SupportScheme.Symmetric: 2,
+            SupportScheme.SuperSymmetric: 3, SupportScheme.KernelMeanSymmetric: 4}
+
+
+def _p(params) -> C.c_void_p:
+    return C.cast(C.pointer(params), C.c_void_p)
+
+
+def _f32(t: torch.Tensor) -> torch.Tensor:
+    if not t.is_cuda:
+        raise RuntimeError("warpsph_b200 operates on CUDA tensors only (no CPU fallback)")
+    if t.dtype != torch.float32:
+        raise RuntimeError(f"expected float32 tensor, got {t.dtype}")
+    return t.contiguous()
+
+
+def _empty(shape, like: torch.Tensor, dtype=torch.float32) -> torch.Tensor:
+    return torch.empty(shape, device=like.device, dtype=dtype)
+
+
+_dt_cache: dict = {}
+
+
+def dt_tensor(dt, device) -> torch.Tensor:
+    """Device float32 scalar (shape [1]) holding dt; accepts floats or tensors."""
+    if isinstance(dt, torch.Tensor):
+        t = dt.reshape(-1)[:1]
+        if t.device != torch.device(device) or t.dtype != torch.float32:
+            t = t.to(device=device, dtype=torch.float32)
+        return t.contiguous()
+    key = (str(device), float(dt))
+    t = _dt_cache.get(key)
+    if t is None:
+        if len(_dt_cache) > 64:
+            _dt_cache.clear()
+        t = torch.tensor([float(dt)], device=device, dtype=torch.float32)
+        _dt_cache[key] = t
+    return t
+
+
+# ------------------------------------------------------------------ neighbour search
+def _version(t: torch.Tensor) -> tuple:
+    return (id(t), t._version, t.data_ptr(), tuple(t.shape))
+
+
+class _NbCache:
+    def __init__(self):
+        self.ws = {}
+        self.cap_hint = {}
+
+
+_nb_cache = _NbCache()
+
+
+def cell_capacity_for(n: int, dim: int) -> int:
+    want = max(1024, n * (1 << dim))
+    cap = 1
+    while cap < want:
+        cap <<= 1
+    return min(cap, 1 << 24)
+
+
+def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float,
+                    priorNeighborhood: Optional[AdjacencyList] = None, keep_sort: bool = True) -> AdjacencyList:
+    """Replaces warpSPHCore buildVerletList (schemes/crkSPH.py:54-58).
+
+    An unchanged prior list (same position and support tensors, same version) is
+    returned as is; otherwise the list is rebuilt on the GPU."""
+    x = _f32(x)
+    H = _f32(H)
+    if priorNeighborhood is not None and priorNeighborhood._x_version == _version(x) and \
+            priorNeighborhood._h_version == _version(H) and priorNeighborhood.verletScale == float(verletScale):
+        return priorNeighborhood
+    n = int(H.shape[0])
+    dim = int(params.dim)
+    params.verlet_scale = float(verletScale)
+    dev = x.device
+    L = _capi.lib()
+    cap = cell_capacity_for(n, dim)
+    wsb = C.c_int64(0)
+    check(L.sph_neighbors_workspace_size(_p(params), n, cap, C.byref(wsb)), "sph_neighbors_workspace_size")
+    key = (dev.index, wsb.value)
+    ws = _nb_cache.ws.get(key)
+    if ws is None:
+        _nb_cache.ws.clear()
+        ws = torch.empty(wsb.value, dtype=torch.uint8, device=dev)
+        _nb_cache.ws[key] = ws
+    offs = torch.empty(n, dtype=torch.int32, device=dev)
+    cnt = torch.empty(n, dtype=torch.int32, device=dev)
+    si = torch.empty(n, dtype=torch.int32, device=dev)
+    sk = torch.empty(n, dtype=torch.int32, device=dev)
+    cb = torch.empty(cap, dtype=torch.int32, device=dev)
+    ce = torch.empty(cap, dtype=torch.int32, device=dev)
+    grid = torch.empty(8, dtype=torch.int32, device=dev)
+    flags = torch.zeros(2, dtype=torch.int64, device=dev)   # [nnz, status(int32 in the low half)]
+    list_cap = _nb_cache.cap_hint.get((dev.index, n, dim), max(n * 64, 1024))
+    for attempt in range(2):
+        lst = torch.empty(max(list_cap, 1), dtype=torch.int32, device=dev)
+        flags.zero_()
+        with _timed("neighbors_build"):
+            rc = L.sph_neighbors_build(_p(params), n, ptr(x), ptr(H), ptr(ws), wsb.value, cap, ptr(si), ptr(sk), ptr(cb), ptr(ce),
+                                       ptr(grid), ptr(offs), ptr(cnt), ptr(lst), list_cap, flags.data_ptr(), flags.data_ptr() + 8,
+                                       stream_ptr(dev))
+        check(rc, "sph_neighbors_build")
+        f = flags.cpu()
+        nnz, status = int(f[0]), int(f[1]) & 0xffffffff
+        if status & _capi.STATUS_NONFINITE:
+            raise RuntimeError("buildVerletList: supports must be finite and positive")
+        if status & _capi.STATUS_LIST_OVERFLOW:
+            list_cap = int(nnz * 1.15) + 1024
+            continue
+        break
+    else:  # pragma: no cover
+        raise RuntimeError("buildVerletList: list capacity could not be satisfied")
+    _nb_cache.cap_hint[(dev.index, n, dim)] = int(nnz * 1.15) + 1024
+    adj = AdjacencyList(neighborOffsets=offs, numNeighbors=cnt, neighborList=lst[:nnz], numRows=n, numCols=n, nnz=nnz,
+                        sortIndex=si if keep_sort else None, sortedKeys=sk if keep_sort else None, grid=grid,
+                        queryPositions=x, querySupports=H, verletScale=float(verletScale))
+    adj._x_version = _version(x)
+    adj._h_version = _version(H)
+    return adj
+
+
+def expand_adjacency(adj: AdjacencyList):
+    dev = adj.neighborList.device
+    i = torch.empty(adj.nnz, dtype=torch.int64, device=dev)
+    j = torch.empty(adj.nnz, dtype=torch.int64, device=dev)
+    check(_capi.lib().sph_neighbors_expand(adj.numRows, ptr(adj.neighborOffsets), ptr(adj.numNeighbors),
+                                           ptr(adj.neighborList), adj.nnz, ptr(i), ptr(j), stream_ptr(dev)),
+          "sph_neighbors_expand")
+    return i, j
+
+
+def _csr(adj: AdjacencyList):
+    return iptr(adj.neighborOffsets), iptr(adj.numNeighbors), iptr(adj.neighborList)
+
+
+# ------------------------------------------------------------------ pair operations
+def density(params, x, H, m, adj: AdjacencyList, supportMode: SupportScheme = SupportScheme.Gather) -> torch.Tensor:
+    n = H.shape[0]
+    rho = _empty(n, H)
+    with _timed("density"):
+        check(_capi.lib().sph_density_gather(_p(params), n, _SUPPORT[supportMode], fptr(x), fptr(H), fptr(m), *_csr(adj), ptr(rho),
+                                             stream_ptr(H.device)), "sph_density_gather")
+    return rho
+
+
+def minmax(a: torch.Tensor) -> torch.Tensor:
+    out = _empty(2, a)
+    with _timed("minmax"):
+        check(_capi.lib().sph_minmax(a.shape[0], fptr(a), ptr(out), stream_ptr(a.device)), "sph_minmax")
+    return out
+
+
+def adaptive_h_iter(params, x, H, m, adj: AdjacencyList, hbounds: torch.Tensor):
+    n = H.shape[0]
+    rho, Hn, ratio = _empty(n, H), _empty(n, H), _empty(n, H)
+    with _timed("adaptive_h_iter"):
+        check(_capi.lib().sph_adaptive_h_iter(_p(params), n, 0, fptr(x), fptr(H), fptr(m), *_csr(adj), fptr(hbounds), ptr(rho), ptr(Hn),
+                                              ptr(ratio), stream_ptr(H.device)), "sph_adaptive_h_iter")
+    return rho, Hn, ratio
+
+
+def crk_volume(params, x, H, adj: AdjacencyList) -> torch.Tensor:
+    n = H.shape[0]
+    V = _empty(n, H)
+    with _timed("crk_volume"):
+        check(_capi.lib().sph_crk_volume(_p(params), n, fptr(x), fptr(H), *_csr(adj), ptr(V), stream_ptr(H.device)), "sph_crk_volume")
+    return V
+
+
+def crk_factors(params, x, H, m, V, adj: AdjacencyList):
+    n, d = H.shape[0], int(params.dim)
+    A, B, gA, gB, rho = _empty(n, H), _empty((n, d), H), _empty((n, d), H), _empty((n, d, d), H), _empty(n, H)
+    with _timed("crk_factors"):
+        check(_capi.lib().sph_crk_factors(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(V), *_csr(adj), ptr(A), ptr(B), ptr(gA), ptr(gB),
+                                          ptr(rho), stream_ptr(H.device)), "sph_crk_factors")
+    return CRKState(A=A, B=B, gradA=gA, gradB=gB), rho
+
+
+def eos_ideal_gas(params, u, rho):
+    n = u.shape[0]
+    A, P, c = _empty(n, u), _empty(n, u), _empty(n, u)
+    with _timed("eos_ideal_gas"):
+        check(_capi.lib().sph_eos_ideal_gas(_p(params), n, fptr(u), fptr(rho), ptr(A), ptr(P), ptr(c), stream_ptr(u.device)),
+              "sph_eos_ideal_gas")
+    return A, P, c
+
+
+def grad_v(params, x, H, m, rho, V, crk: CRKState, v, c, adj: AdjacencyList, cullen: bool):
+    n, d = H.shape[0], int(params.dim)
+    G, drho = _empty((n, d, d), H), _empty(n, H)
+    div = _empty(n, H) if cullen else None
+    vs = _empty(n, H) if cullen else None
+    with _timed("grad_v"):
+        check(_capi.lib().sph_grad_v(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(V), fptr(crk.A), fptr(crk.B), fptr(crk.gradA),
+                                     fptr(crk.gradB), fptr(v), fptr(c), *_csr(adj), ptr(G), ptr(drho), ptr(div), ptr(vs),
+                                     stream_ptr(H.device)), "sph_grad_v")
+    return G, drho, div, vs
+
+
+def switch_cullen(params, x, H, m, rho, div, div_prev, vsig, alpha0, dt, adj: AdjacencyList, want_R: bool = False):
+    n = H.shape[0]
+    al = _empty(n, H)
+    R = _empty(n, H) if want_R else None
+    with _timed("switch_cullen"):
+        check(_capi.lib().sph_switch_cullen(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(div), fptr(_f32(div_prev)), fptr(vsig),
+                                            fptr(_f32(alpha0)), fptr(dt_tensor(dt, H.device)), *_csr(adj), ptr(al), ptr(R),
+                                            stream_ptr(H.device)), "sph_switch_cullen")
+    return al, R
+
+
+def switch_balsara(params, DvDx, c):
+    n = c.shape[0]
+    al = _empty(n, c)
+    check(_capi.lib().sph_switch_balsara(_p(params), n, fptr(DvDx), fptr(c), ptr(al), stream_ptr(c.device)), "sph_switch_balsara")
+    return al
+
+
+def crk_accel_dudt(params, x, H, m, rho, V, crk: CRKState, v, c, P, DvDx, adj: AdjacencyList, pair_arrays: bool = True):
+    n, d = H.shape[0], int(params.dim)
+    dvdt, dudt = _empty((n, d), H), _empty(n, H)
+    ap = _empty((adj.nnz, d), H) if pair_arrays else None
+    av = _empty((adj.nnz, d), H) if pair_arrays else None
+    with _timed("crk_accel_dudt"):
+        check(_capi.lib().sph_crk_accel_dudt(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(V), fptr(crk.A), fptr(crk.B),
+                                             fptr(crk.gradA), fptr(crk.gradB), fptr(v), fptr(c), fptr(P), fptr(DvDx), *_csr(adj),
+                                             ptr(dvdt), ptr(dudt), ptr(ap), ptr(av), stream_ptr(H.device)), "sph_crk_accel_dudt")
+    return dvdt, dudt, ap, av
+
+
+def compsph_balance(params, m, rho, P, u, v, dvdt, dt, adj: AdjacencyList, ap, av):
+    f = _empty(adj.nnz, m)
+    with _timed("compsph_balance"):
+        check(_capi.lib().sph_compsph_balance(_p(params), m.shape[0], fptr(m), fptr(rho), fptr(P), fptr(u), fptr(v), fptr(dvdt),
+                                              fptr(dt_tensor(dt, m.device)), *_csr(adj), fptr(ap), fptr(av), ptr(f),
+                                              stream_ptr(m.device)), "sph_compsph_balance")
+    return f
+
+
+def cfl_dt(params, H, u, rho=None, dt_prev=None) -> torch.Tensor:
+    """Device-side CFL time step (returns a [1] float32 tensor; no host sync)."""
+    buf = _empty(4, H)
+    prev = None if dt_prev is None else dt_tensor(dt_prev, H.device)
+    with _timed("cfl_dt"):
+        check(_capi.lib().sph_cfl_dt(_p(params), H.shape[0], fptr(H), fptr(u), None, ptr(prev), ptr(buf), stream_ptr(H.device)),
+              "sph_cfl_dt")
+    return buf[:1]
+
+
+def rk_combine(params, y0: torch.Tensor, ks, weights, dt, wrap_dim: int = 0, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    y0 = _f32(y0)
+    y = torch.empty_like(y0) if out is None else out
+    kp = [fptr(_f32(k)) for k in ks]
+    arr = _capi.ptr_array(kp) if kp else None
+    w = _capi.double_array(weights) if kp else None
+    with _timed("rk_combine"):
+        check(_capi.lib().sph_rk_combine(_p(params), y0.numel(), ptr(y0), len(kp), C.cast(arr, C.c_void_p) if arr is not None else None,
+                                         C.cast(w, C.c_void_p) if w is not None else None, fptr(dt_tensor(dt, y0.device)), wrap_dim,
+                                         ptr(y), stream_ptr(y0.device)), "sph_rk_combine")
+    return y
+
+
+def finalize_compatible_energy(params, weights, dt, v0, u0, stages):
+    """stages: list of (dvdt, adjacency, f_ij, ap_ij, av_ij)."""
+    n, d = u0.shape[0], int(params.dim)
+    u = _empty(n, u0)
+    scratch = _empty(n * (1 + d), u0)
+    ns = len(stages)
+    arrs = [_capi.ptr_array([fptr(s[0]) for s in stages]),
+            _capi.ptr_array([iptr(s[1].neighborOffsets) for s in stages]),
+            _capi.ptr_array([iptr(s[1].numNeighbors) for s in stages]),
+            _capi.ptr_array([iptr(s[1].neighborList) for s in stages]),
+            _capi.ptr_array([fptr(s[2]) for s in stages]),
+            _capi.ptr_array([fptr(s[3]) for s in stages]),
+            _capi.ptr_array([fptr(s[4]) for s in stages])]
+    w = _capi.double_array(weights)
+    with _timed("finalize_compatible_energy"):
+        check(_capi.lib().sph_finalize_compatible_energy(_p(params), n, ns, C.cast(w, C.c_void_p), fptr(dt_tensor(dt, u0.device)),
+                                                         fptr(_f32(v0)), fptr(_f32(u0)), *[C.cast(a, C.c_void_p) for a in arrs],
+                                                         ptr(u), ptr(scratch), stream_ptr(u0.device)), "sph_finalize_compatible_energy")
+    return u, scratch[:n]
+
+
+def conservation_sums(params, m, v, u) -> torch.Tensor:
+    out = torch.empty(7, device=m.device, dtype=torch.float64)
+    check(_capi.lib().sph_conservation_sums(_p(params), m.shape[0], fptr(m), fptr(v), fptr(u), ptr(out), stream_ptr(m.device)),
+          "sph_conservation_sums")
+    return out

@@ -1,0 +1,155 @@
+"""Step functions and scheme dispatch.
+
+``buildScheme`` returns the reference's 7-tuple (src/warpSPH/schemes/builder.py:11-36).
+``crkSPH_step`` follows src/warpSPH/schemes/crkSPH.py:19-366 call for call, with
+every SPH operation executed by libwarpsph_b200 kernels:
+
+  adaptive support (Monaghan Newton)  crkSPH.py:40  -> sph_adaptive_h_iter + sph_density_gather
+  Verlet list                         crkSPH.py:54  -> sph_neighbors_build (unchanged prior reused)
+  CRK volume / coefficients / rho     crkSPH.py:61  -> sph_crk_volume + sph_crk_factors
+  ideal-gas EOS                       crkSPH.py:95  -> sph_eos_ideal_gas
+  CRK velocity gradient               crkSPH.py:158 -> sph_grad_v (also Cullen div and v_sig)
+  viscosity switch                    crkSPH.py:195 -> sph_switch_cullen / sph_switch_balsara
+  momentum + energy RHS               crkSPH.py:241,263 -> sph_crk_accel_dudt (one fused pass)
+  energy partition f_ij               crkSPH.py:343 -> sph_compsph_balance
+"""
+from __future__ import annotations
+
+from typing import Optional, Union
+
+import torch
+
+from . import ops
+from .configurations import (CompSPHConfig, CompressibleSPHConfig, CRKSPHConfig, SimulationConfig, compSPHConfigToDict,
+                             crkSPHConfigToDict, dictToCompSPHConfig, dictToCRKSPHConfig, make_params)
+from .core import AdjacencyList, SupportScheme, sphKernel_xi, volumeToSupportHelper
+from .enumTypes import AdaptiveSupportScheme, CompressibleSPHScheme, ViscositySwitch
+from .systems import CompressibleSystemUpdate, CompSPHState, CompSPHSystem
+
+
+# ------------------------------------------------------------------ adaptive support
+def evaluateOptimalSupport(particleState, config: SimulationConfig, compParams: CompressibleSPHConfig,
+                           supportScheme: SupportScheme = SupportScheme.Scatter, adjacency: Optional[AdjacencyList] = None,
+                           iterations: Optional[int] = None, threshold: Optional[float] = None):
+    """modules/adaptiveSupport/optimalSupport.py:12-43 and optimalSupportMonaghan.py:62-150.
+
+    Returns (densities, supports, adjacency, None, None).  The Owen LUT scheme is not
+    on this path; NoScheme returns the state unchanged."""
+    scheme = compParams.adaptiveSupportScheme
+    if scheme == AdaptiveSupportScheme.NoScheme:
+        return particleState.densities, particleState.supports, adjacency, None, None
+    if scheme == AdaptiveSupportScheme.Owen:
+        raise NotImplementedError("the Owen LUT adaptive-support scheme is not implemented on the GPU path; use Monaghan")
+    if supportScheme != SupportScheme.Gather:
+        raise NotImplementedError("adaptive support is implemented for the gather support scheme")
+    params = make_params(config, compParams)
+    nIter = compParams.adaptiveSupportIterations if iterations is None else iterations
+    hThreshold = compParams.adaptiveSupportThreshold if threshold is None else threshold
+    S = particleState
+    hb = ops.minmax(S.supports)
+    for it in range(nIter):
+        adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, adjacency)
+        rho, h_new, ratio = ops.adaptive_h_iter(params, S.positions, S.supports, S.masses, adjacency, hb)
+        S.densities = rho
+        hb = ops.minmax(h_new)
+        S.supports = h_new
+        if it < nIter - 1 and float((ratio - 1).abs().max()) < hThreshold:
+            break
+    adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, adjacency)
+    densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
+    return densities, S.supports, adjacency, None, None
+
+
+def computeCRKFactors(particleState, config: SimulationConfig, adjacency: AdjacencyList, params=None):
+    """warpSPHCore computeCRKFactors (schemes/crkSPH.py:61): (apparentVolume, densities, crkState)."""
+    params = make_params(config) if params is None else params
+    S = particleState
+    V = ops.crk_volume(params, S.positions, S.supports, adjacency)
+    crk, rho = ops.crk_factors(params, S.positions, S.supports, S.masses, V, adjacency)
+    return V, rho, crk
+
+
+def idealGasEOS(A, u, P, rho, gamma):
+    """modules/eos/idealGas.py:6-38 for the (u, rho) case used by the step functions.
+    Returns (A, u, P, c)."""
+    if A is not None or P is not None or u is None:
+        raise NotImplementedError("only the (u, rho) form of the ideal-gas EOS is on the GPU path")
+    from ._capi import SphParams
+    p = SphParams()
+    p.dim, p.kernel, p.verlet_scale, p.gamma = 1, 1, 1.0, float(gamma)
+    p.domain_max[0] = 1.0
+    A_, P_, c_ = ops.eos_ideal_gas(p, u, rho)
+    return A_, u, P_, c_
+
+
+def computeTimestep(system, config: SimulationConfig, compParams: CompressibleSPHConfig, dt=None, device_result: bool = False):
+    """modules/timestep/compressible.py:12-66: CFL dt = min_i cfl*min(H)/(c_i xi), clamped
+    to [minDt, maxDt] and to dtGrowthFactor*config.dt when dt is given.  With
+    device_result=True the value stays on the GPU (no host sync)."""
+    if not config.adaptiveDt:
+        if dt is not None:
+            return dt
+        raise ValueError("dt must be provided if adaptiveDt is False")
+    params = make_params(config, compParams)
+    prev = config.dt if (dt is not None and config.dt is not None) else None
+    S = system.state
+    t = ops.cfl_dt(params, S.supports, S.internalEnergies, dt_prev=prev)
+    return t if device_result else float(t.item())
+
+
+# ------------------------------------------------------------------ CRKSPH step
+def crkSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams: CRKSPHConfig, verbose: bool = False):
+    """schemes/crkSPH.py:19-366 on the GPU.  Returns (update, adjacency, state)."""
+    if compParams.boundaryConditions:
+        raise NotImplementedError("boundary conditions are outside the GPU hot path")
+    params = make_params(config, compParams)
+    S = system.state
+    # crkSPH.py:40-42
+    rho_opt, h_opt, system.adjacency, *_ = evaluateOptimalSupport(S, config, compParams, SupportScheme.Gather, system.adjacency)
+    S.supports = h_opt
+    S.densities = rho_opt
+    # crkSPH.py:54-59
+    adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, system.adjacency)
+    system.adjacency = adjacency
+    # crkSPH.py:61
+    V, S.densities, crk = computeCRKFactors(S, config, adjacency, params)
+    if S.divergence is None:
+        S.divergence = torch.zeros_like(S.densities)
+    # crkSPH.py:95-101
+    S.entropies, S.pressures, S.soundspeeds = ops.eos_ideal_gas(params, S.internalEnergies, S.densities)
+    switch = compParams.viscositySwitchParams.scheme
+    cullen = switch == ViscositySwitch.CullenDehnen2010
+    # crkSPH.py:158-172 (+ the Cullen divergence and v_sig in the same pass)
+    DvDx, drhodt, div_cd, vsig = ops.grad_v(params, S.positions, S.supports, S.masses, S.densities, V, crk, S.velocities,
+                                            S.soundspeeds, adjacency, cullen)
+    # crkSPH.py:195-200
+    if cullen:
+        S.alphas, _ = ops.switch_cullen(params, S.positions, S.supports, S.masses, S.densities, div_cd, S.divergence, vsig,
+                                        S.alpha0s, dt, adjacency)
+    elif switch == ViscositySwitch.Balsara1995:
+        S.alphas = ops.switch_balsara(params, DvDx, S.soundspeeds)
+    elif switch != ViscositySwitch.NoneSwitch:
+        raise ValueError(f"Unsupported viscosity switch scheme: {switch}")
+    # crkSPH.py:241-284
+    dvdt, dudt, S.ap_ij, S.av_ij = ops.crk_accel_dudt(params, S.positions, S.supports, S.masses, S.densities, V, crk, S.velocities,
+                                                      S.soundspeeds, S.pressures, DvDx, adjacency)
+    # crkSPH.py:324-337
+    S.divergence = -drhodt / S.densities
+    dEdt = S.masses * torch.einsum("ij,ij->i", S.velocities, dvdt) + S.masses * dudt
+    update = CompressibleSystemUpdate(dxdt=S.velocities, dvdt=dvdt, dudt=dudt, drhodt=drhodt, dEdt=dEdt, passive=None)
+    # crkSPH.py:341-363
+    S.f_ij = ops.compsph_balance(params, S.masses, S.densities, S.pressures, S.internalEnergies, S.velocities, dvdt, dt, adjacency,
+                                 S.ap_ij, S.av_ij)
+    return update, adjacency, S
+
+
+def buildScheme(schemeName: Union[str, CompressibleSPHScheme]):
+    """schemes/builder.py:11-36: (System, State, SchemeConfig, Update, step_fn, export_fn, import_fn)."""
+    if (isinstance(schemeName, str) and schemeName == "crkSPH") or schemeName == CompressibleSPHScheme.CRKSPH:
+        return (CompSPHSystem, CompSPHState, CRKSPHConfig, CompressibleSystemUpdate, crkSPH_step, crkSPHConfigToDict,
+                dictToCRKSPHConfig)
+    if (isinstance(schemeName, str) and schemeName == "compSPH") or schemeName == CompressibleSPHScheme.CompSPH:
+        from .compsph import compSPH_step
+        return (CompSPHSystem, CompSPHState, CompSPHConfig, CompressibleSystemUpdate, compSPH_step, compSPHConfigToDict,
+                dictToCompSPHConfig)
+    raise ValueError(f"Scheme {schemeName} not recognized.")
