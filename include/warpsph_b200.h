@@ -10,8 +10,9 @@
  *     per-particle matrices are row-major [n, dim, dim]; M[a][b] = d(field^a)/dx^b.
  *   - Neighbour lists are CSR: neighbor_offsets[n], num_neighbors[n] (int32) and
  *     neighbor_list[nnz] (int32, original particle indices).  Row i lists every j
- *     with |x_i - x_j| < verlet_scale * max(H_i, H_j) (i itself included), in
- *     ascending order of j's position in the cell-sorted order.
+ *     with |x_i - x_j| < verlet_scale * max(H_i, H_j) (i itself included), ordered
+ *     by stencil cell (offsets -1, 0, +1 per axis, x fastest) and, inside a cell, by
+ *     ascending position in the cell-sorted order.
  *   - `stream` is a cudaStream_t passed as void*; work is enqueued asynchronously.
  *   - Scalars that change every step (dt) are read from DEVICE memory so a step can
  *     be captured in a CUDA graph without host round trips.
@@ -114,7 +115,12 @@ typedef struct SphParams {
     int32_t energy_scheme;            /* SPH_ENERGY_* */
     int32_t limit_xi;
     int32_t kahan;                    /* 1: compensated accumulation of dv/dt and du/dt */
-    int32_t reserved_i[8];
+    /* Layout of the `list` argument of the pair entry points: 1 (or 0) = Verlet list of
+     * neighbour indices j; 2 = interacting list of (j, Verlet entry index) int32 pairs
+     * from sph_neighbors_build.  Pairwise outputs/inputs (ap_ij, av_ij, f_ij) are always
+     * indexed by the Verlet entry. */
+    int32_t list_stride;
+    int32_t reserved_i[7];
 } SphParams;
 
 /* ---------------------------------------------------------------- library */
@@ -133,21 +139,31 @@ int sph_neighbors_workspace_size(const SphParams* p, int64_t n, int64_t cell_cap
 
 /* Replaces warpSPHCore buildVerletList (called at schemes/crkSPH.py:54-58,
  * schemes/compSPH.py:42-46, schemes/dfsph.py:29-33): Morton-keyed dense cell grid
- * of cell size >= verlet_scale*max(H), counting sort by (cell key, index), cell
- * offset table, then count -> scan -> fill of the CSR Verlet list.
+ * of cell size >= verlet_scale*max(H), counting sort by (cell key, index) (atomic
+ * scatter + in-cell rank), cell offset table, then count -> scan -> fill of the CSR
+ * Verlet list over position/support records gathered in sorted order.
  * Outputs: sort_index[n] (original index of the k-th sorted particle),
  * sorted_keys[n] (its Morton cell key), cell_begin/cell_end[cell_capacity],
- * CSR arrays, *nnz_out (device int64).  If nnz > list_capacity the list is not
- * filled, SPH_STATUS_LIST_OVERFLOW is or-ed into *status (device int32) and
- * *nnz_out still holds the required size. grid_out (device, 8 int32): grid dims,
- * bits per axis, and the cell size as float bits. */
+ * CSR arrays, *nnz_out (device int64).
+ * Optional interacting list (all inter_* non-null): the subset of entries with
+ * r/max(H_i,H_j) < 1 -- every pair any support scheme gives a non-zero kernel
+ * value -- as (j, index of the entry in neighbor_list) int32 pairs, stored inside
+ * each row's own Verlet range: inter_offsets[i] == neighbor_offsets[i], the first
+ * inter_counts[i] pairs of the range are valid.  inter_list holds 2*inter_capacity
+ * int32 (8-byte aligned, inter_capacity >= list_capacity); *inter_nnz_out receives
+ * the number of valid pairs.  If the Verlet list exceeds list_capacity nothing is
+ * filled, SPH_STATUS_LIST_OVERFLOW is or-ed into *status (device int32) and *nnz_out
+ * holds the required size.
+ * grid_out (device, 8 int32): grid dims, bits per axis, cell size as float bits, dim. */
 int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const float* H,
                         void* workspace, int64_t workspace_bytes, int64_t cell_capacity,
                         int32_t* sort_index, uint32_t* sorted_keys,
                         int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
                         int32_t* neighbor_offsets, int32_t* num_neighbors,
-                        int32_t* neighbor_list, int64_t list_capacity,
-                        int64_t* nnz_out, int32_t* status, void* stream);
+                        int32_t* neighbor_list, int64_t list_capacity, int64_t* nnz_out,
+                        int32_t* inter_offsets, int32_t* inter_counts, int32_t* inter_list,
+                        int64_t inter_capacity, int64_t* inter_nnz_out,
+                        int32_t* status, void* stream);
 
 /* Expands CSR rows into the reference's AdjacencyList.i / .j int64 arrays
  * (io.py:8-20 field names). */
@@ -213,13 +229,17 @@ int sph_grad_v(const SphParams* p, int64_t n, const float* x, const float* H, co
 /* Cullen & Dehnen 2010 switch (modules/shockCapturing/CullenDehnen2010.py:218-331):
  * R pass (gather interpolation of m_j sgn(div_j)), Xi limiter, A_i, alpha_loc,
  * and the alpha0 relaxation with tau = h/(2*0.05*v_sig*xi).  div_prev is the
- * state's previous divergence, alpha0_prev the state's alpha0s.  Outputs the
- * new alphas (the reference returns alpha0s as alphas, crkSPH.py:195-200). */
+ * state's previous divergence, alpha0_prev the state's alpha0s.  When vsig is
+ * NULL the signal velocity max_j (c_bar - mu_ij) (modules/shockCapturing/wp_vsig.py:11-90)
+ * is computed in the same pass from v and c over the Verlet set -- `list` must then
+ * be the Verlet list (stride 1) -- and written to vsig_out when non-null.
+ * Outputs the new alphas (the reference returns alpha0s as alphas, crkSPH.py:195-200). */
 int sph_switch_cullen(const SphParams* p, int64_t n, const float* x, const float* H,
                       const float* m, const float* rho, const float* div, const float* div_prev,
-                      const float* vsig, const float* alpha0_prev, const float* dt,
+                      const float* vsig, const float* v, const float* c,
+                      const float* alpha0_prev, const float* dt,
                       const int32_t* offs, const int32_t* cnt, const int32_t* list,
-                      float* alpha_out, float* R_out, void* stream);
+                      float* alpha_out, float* R_out, float* vsig_out, void* stream);
 
 /* Balsara 1995 switch alpha = clamp(|div v| / (|div v| + |curl v| + 1e-4 c), 0, 1)
  * with CRK difference-form divergence and curl (formula restated from the comment
@@ -231,7 +251,9 @@ int sph_switch_balsara(const SphParams* p, int64_t n, const float* DvDx, const f
 /* CRKSPH momentum and energy RHS in one pair pass:
  * modules/crk/accel.py:15-250 (dv/dt and the pairwise ap_ij, av_ij [nnz, dim]) and
  * modules/crk/dudt.py:15-229 (du/dt).  Any of dvdt_out, dudt_out, ap_ij, av_ij may
- * be null.  With p->kahan the per-particle sums are Neumaier-compensated. */
+ * be null.  With p->kahan the per-particle sums are Neumaier-compensated.  With the
+ * interacting list (list_stride 2) only interacting entries of ap_ij / av_ij are
+ * written; the caller passes zero-filled arrays. */
 int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
                        const float* m, const float* rho, const float* V,
                        const float* A, const float* B, const float* gradA, const float* gradB,
@@ -256,12 +278,14 @@ int sph_crk_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
                  float* dudt_out, void* stream);
 
 /* Pairwise energy-partition fraction f_ij (modules/compSPH/balance.py:17-154) for
- * the six energy schemes, evaluated at v_half = v + dt/2 dvdt (schemes/crkSPH.py:341-363). */
+ * the six energy schemes, evaluated at v_half = v + dt/2 dvdt (schemes/crkSPH.py:341-363).
+ * scratch: device memory of n*(dim+1) floats (half-step velocities and P/rho^gamma).
+ * f_ij is written for every entry of `list` (pass the Verlet list to fill all of it). */
 int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const float* rho,
                         const float* P, const float* u, const float* v, const float* dvdt,
                         const float* dt, const int32_t* offs, const int32_t* cnt,
                         const int32_t* list, const float* ap_ij, const float* av_ij,
-                        float* f_ij_out, void* stream);
+                        float* scratch, float* f_ij_out, void* stream);
 
 /* ---------------------------------------------------------------- (d) integrator and dt */
 /* CFL time step (modules/timestep/compressible.py:12-61): dt = min_i cfl*min(H)/(c_i xi),

@@ -276,6 +276,8 @@ int oracle_neighbors_build(const SphParams* p, int64_t n, const float* x, const 
             float Hi = H[i];
             int c[3];
             cell_coords_f(&g, D, xi, c);
+            /* stencil cells in offset order (x fastest), duplicates (grids with fewer
+             * than three cells along a periodic axis) visited once */
             uint32_t sk[27];
             int nk = 0;
             int NS = D == 1 ? 3 : (D == 2 ? 9 : 27);
@@ -295,10 +297,7 @@ int oracle_neighbors_build(const SphParams* p, int64_t n, const float* x, const 
                 int dup = 0;
                 for (int q = 0; q < nk; ++q) if (sk[q] == kk) { dup = 1; break; }
                 if (dup) continue;
-                int m = nk - 1;
-                while (m >= 0 && sk[m] > kk) { sk[m + 1] = sk[m]; --m; }
-                sk[m + 1] = kk;
-                ++nk;
+                sk[nk++] = kk;
             }
             int cntv = 0;
             int32_t base = pass ? offsets[i] : 0;

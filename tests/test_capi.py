@@ -69,7 +69,7 @@ def test_argument_validation_happens_on_the_host():
     # a workspace smaller than required is refused
     dummy = 256  # never dereferenced: the size check fails first
     rc = lib.sph_neighbors_build(pp, 1000, dummy, dummy, dummy, 16, 4096, dummy, dummy, dummy, dummy, dummy, dummy, dummy,
-                                 dummy, 10, dummy, dummy, None)
+                                 dummy, 10, dummy, None, None, None, 0, None, dummy, None)
     assert rc == -2
 
 

@@ -46,6 +46,35 @@ def test_neighbors_bit_exact(cuda, dim, n_side, periodic):
     assert np.array_equal(j, ref["list"]) and np.array_equal(np.bincount(i, minlength=len(ref["counts"])), ref["counts"])
 
 
+@pytest.mark.parametrize("dim,n_side", CASES)
+def test_interacting_list_is_exact_subset(cuda, dim, n_side):
+    """The interacting list holds exactly the Verlet entries with fl(sqrt(r^2))/max(H_i,H_j) < 1
+    (same float operations as the list builder), in Verlet order, with their entry index."""
+    cfg, sch, p = make_params(dim)
+    P = make_particles(dim, n_side, seed=20 + dim)
+    G = to_gpu(P, cuda)
+    adj = ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale)
+    x, H = P["positions"], P["supports"]
+    offs, cnt, lst = (a.cpu().numpy() for a in (adj.neighborOffsets, adj.numNeighbors, adj.neighborList))
+    i = np.repeat(np.arange(len(H)), cnt)
+    d = (x[i] - x[lst]).astype(np.float32)
+    hl = np.float32(0.5)
+    d = np.where(d > hl, d - np.float32(1.0), np.where(d < -hl, d + np.float32(1.0), d)).astype(np.float32)
+    r2 = np.zeros(len(lst), np.float32)
+    for a in range(dim):
+        r2 = (r2 + d[:, a] * d[:, a]).astype(np.float32)
+    Hm = np.maximum(H[i], H[lst])
+    keep = (np.sqrt(r2).astype(np.float32) / Hm).astype(np.float32) < np.float32(1.0)
+    il = adj.interList.cpu().numpy().reshape(-1, 2)
+    ioffs, icnt = adj.interOffsets.cpu().numpy(), adj.interCounts.cpu().numpy()
+    assert np.array_equal(ioffs, offs)
+    assert adj.interNnz == int(keep.sum()) == int(icnt.sum())
+    assert np.array_equal(icnt, np.bincount(i[keep], minlength=len(H)))
+    valid = np.concatenate([np.arange(o, o + c) for o, c in zip(ioffs, icnt)])
+    assert np.array_equal(il[valid, 1], np.nonzero(keep)[0])
+    assert np.array_equal(il[valid, 0], lst[keep])
+
+
 def test_neighbors_capacity_overflow_is_recovered(cuda):
     cfg, sch, p = make_params(2)
     P = make_particles(2, 30, seed=5)
@@ -129,7 +158,8 @@ def test_crk_pipeline(cuda, dim, n_side):
     assert_close(A_.cpu().numpy(), rA_, 1e-5, 1e-5, "A(entropy)")
     # velocity gradient + Cullen divergence + v_sig (inputs from the GPU so errors do not compound)
     cn = {k: t.cpu().numpy() for k, t in dict(A=crk.A, B=crk.B, gA=crk.gradA, gB=crk.gradB, rho=rho, c=c, P=Pr).items()}
-    Gv, drho, div, vs = ops.grad_v(p, G["positions"], G["supports"], G["masses"], rho, V, crk, G["velocities"], c, adj, True)
+    Gv, drho, div, vs = ops.grad_v(p, G["positions"], G["supports"], G["masses"], rho, V, crk, G["velocities"], c, adj, True,
+                                   want_vsig=True)
     rG, rdrho, rdiv, rvs = o32.grad_v(p, x, H, m, cn["rho"], Vn, cn["A"], cn["B"], cn["gA"], cn["gB"], v, cn["c"], nb, True)
     assert_close(Gv.cpu().numpy(), rG, 1e-4, 1e-4, "DvDx")
     assert_close(drho.cpu().numpy(), rdrho, 1e-4, 1e-4, "drhodt")
@@ -138,7 +168,12 @@ def test_crk_pipeline(cuda, dim, n_side):
     # Cullen switch
     div_prev = torch.from_numpy(rdiv * 0.9 + 0.01).to(cuda)
     a0 = torch.full_like(rho, 0.5)
-    al, R = ops.switch_cullen(p, G["positions"], G["supports"], G["masses"], rho, div, div_prev, vs, a0, 1e-3, adj, want_R=True)
+    al, R, _ = ops.switch_cullen(p, G["positions"], G["supports"], G["masses"], rho, div, div_prev, vs, a0, 1e-3, adj, want_R=True)
+    # the same switch computing v_sig itself over the Verlet list
+    al2, R2, vs2 = ops.switch_cullen(p, G["positions"], G["supports"], G["masses"], rho, div, div_prev, None, a0, 1e-3, adj,
+                                     want_R=True, v=G["velocities"], c=c, want_vsig=True)
+    assert_close(vs2.cpu().numpy(), rvs, 1e-6, 1e-6, "v_sig in the Cullen pass")
+    assert_close(al2.cpu().numpy(), al.cpu().numpy(), 1e-6, 1e-6, "alphas with internal v_sig")
     ral, rR = o32.switch_cullen(p, x, H, m, cn["rho"], div.cpu().numpy(), div_prev.cpu().numpy(), vs.cpu().numpy(),
                                 np.full(len(H), 0.5, np.float32), 1e-3, nb)
     assert_close(R.cpu().numpy(), rR, 1e-5, 1e-5, "R")

@@ -74,7 +74,12 @@ def test_neighbor_list_matches_brute_force(o32, dim, n_side, periodic):
     for i in range(len(H)):
         row = nb["list"][nb["offsets"][i]: nb["offsets"][i] + nb["counts"][i]]
         assert set(row.tolist()) == set(np.nonzero(ref[i])[0].tolist()), i
-        assert np.all(np.diff(pos[row]) > 0), "rows are in ascending sorted order"
+        # canonical order: cells contiguous, ascending sorted position inside a cell
+        ck = nb["sorted_keys"][pos[row]]
+        change = np.nonzero(np.diff(ck.astype(np.int64)))[0]
+        assert len(set(ck.tolist())) == len(change) + 1, "each stencil cell appears once"
+        for seg in np.split(pos[row], change + 1):
+            assert np.all(np.diff(seg) > 0)
         assert i in row
     # super-symmetric lists are symmetric
     assert ref.sum() == nb["nnz"]

@@ -52,7 +52,8 @@ class SphParams(C.Structure):
         ("energy_scheme", C.c_int32),
         ("limit_xi", C.c_int32),
         ("kahan", C.c_int32),
-        ("reserved_i", C.c_int32 * 8),
+        ("list_stride", C.c_int32),
+        ("reserved_i", C.c_int32 * 7),
     ]
 
 
@@ -67,7 +68,8 @@ _PROTOS = {
     "sph_launch_count": [],
     "sph_kernel_constants": [_I32, _I32, _P, _P],
     "sph_neighbors_workspace_size": [_P, _I64, _I64, _P],
-    "sph_neighbors_build": [_P, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _P, _P, _P],
+    "sph_neighbors_build": [_P, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _P,
+                            _P, _P, _P, _I64, _P, _P, _P],
     "sph_neighbors_expand": [_I64, _P, _P, _P, _I64, _P, _P, _P],
     "sph_density_gather": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_adaptive_h_iter": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
@@ -76,12 +78,12 @@ _PROTOS = {
     "sph_crk_factors": [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_eos_ideal_gas": [_P, _I64, _P, _P, _P, _P, _P, _P],
     "sph_grad_v": [_P, _I64] + [_P] * 19,
-    "sph_switch_cullen": [_P, _I64] + [_P] * 15,
+    "sph_switch_cullen": [_P, _I64] + [_P] * 18,
     "sph_switch_balsara": [_P, _I64, _P, _P, _P, _P],
     "sph_crk_accel_dudt": [_P, _I64] + [_P] * 21,
     "sph_crk_accel": [_P, _I64] + [_P] * 20,
     "sph_crk_dudt": [_P, _I64] + [_P] * 18,
-    "sph_compsph_balance": [_P, _I64] + [_P] * 14,
+    "sph_compsph_balance": [_P, _I64] + [_P] * 15,
     "sph_cfl_dt": [_P, _I64, _P, _P, _P, _P, _P, _P],
     "sph_rk_combine": [_P, _I64, _P, _I32, _P, _P, _P, _I32, _P, _P],
     "sph_finalize_compatible_energy": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],

@@ -155,6 +155,12 @@ class AdjacencyList:
     queryPositions: Optional[torch.Tensor] = None
     querySupports: Optional[torch.Tensor] = None
     verletScale: float = 1.0
+    # interacting subset (r < max(H_i, H_j)): (j, entry index) int32 pairs stored in each
+    # row's own Verlet range (interOffsets == neighborOffsets, first interCounts[i] valid)
+    interOffsets: Optional[torch.Tensor] = None
+    interCounts: Optional[torch.Tensor] = None
+    interList: Optional[torch.Tensor] = None
+    interNnz: int = 0
     _x_version: Optional[tuple] = field(default=None, repr=False)
     _h_version: Optional[tuple] = field(default=None, repr=False)
     _ij: Optional[tuple] = field(default=None, repr=False)

@@ -91,13 +91,14 @@ __device__ __forceinline__ float safe_sqrt(float x) { return sqrtf(x > 0.f ? x :
 // ---------------------------------------------------------------- domain
 // Minimum-image x_ij = x_i - x_j. Positions live inside the periodic box, so one
 // conditional shift per periodic axis is exact.
+// Written with selects rather than branches (same result as the if / else-if form).
 template <int D> __device__ __forceinline__ Vec<D> dist_vec(const Vec<D>& xi, const Vec<D>& xj, const DomainF& dom) {
     Vec<D> r;
     _Pragma("unroll") for (int a = 0; a < D; ++a) {
         float d = __fsub_rn(xi.v[a], xj.v[a]);
         if (dom.periodic[a]) {
-            if (d > dom.halfL[a]) d = __fsub_rn(d, dom.L[a]);
-            else if (d < -dom.halfL[a]) d = __fadd_rn(d, dom.L[a]);
+            const float dp = __fsub_rn(d, dom.L[a]), dm = __fadd_rn(d, dom.L[a]);
+            d = d > dom.halfL[a] ? dp : (d < -dom.halfL[a] ? dm : d);
         }
         r.v[a] = d;
     }

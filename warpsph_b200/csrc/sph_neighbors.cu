@@ -9,11 +9,12 @@
 //      atomic scatter, then a per-cell insertion sort by particle index, so the
 //      permutation equals a stable sort by (key, index) -- deterministic and
 //      bit-identical to the CPU oracle.
-//   3. Verlet list as CSR: count pass, exclusive scan, fill pass.  Each thread owns
-//      one particle (taken in sorted order for locality), visits the 3^d stencil
-//      cells in ascending key order, and keeps j when
-//      |x_i - x_j|^2 < (verlet_scale * max(H_i, H_j))^2 (computed with explicit
-//      round-to-nearest operations so the oracle reproduces it exactly).
+//   3. Verlet list as CSR: count pass, exclusive scan, fill pass.  One warp per
+//      particle (in sorted order, over position/support records gathered in sorted
+//      order) visits the 3^d stencil cells in offset order with lanes over the
+//      candidates, keeps j when |x_i - x_j|^2 < (verlet_scale * max(H_i, H_j))^2
+//      (explicit round-to-nearest operations, so the oracle reproduces it exactly)
+//      and writes each row with ballot-compacted, coalesced stores.
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -362,92 +363,226 @@ __global__ void k_scatter(const uint32_t* __restrict__ keys, int n, int32_t* __r
     sort_index[pos] = i;
 }
 
-// Canonical order inside a cell: ascending particle index.
-__global__ void k_cell_sort(const int32_t* __restrict__ begin, const int32_t* __restrict__ end, int64_t ncells,
-                            int32_t* __restrict__ sort_index) {
-    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncells) return;
-    int b = begin[c], e = end[c];
-    for (int k = b + 1; k < e; ++k) {
-        int v = sort_index[k];
-        int m = k - 1;
-        while (m >= b && sort_index[m] > v) { sort_index[m + 1] = sort_index[m]; --m; }
-        sort_index[m + 1] = v;
-    }
-}
-
-__global__ void k_sorted_keys(const uint32_t* __restrict__ keys, const int32_t* __restrict__ sort_index, int n,
-                              uint32_t* __restrict__ sorted_keys) {
+// Canonical order inside a cell: ascending particle index.  After the atomic
+// scatter each cell holds its particles in arbitrary order; every particle's final
+// slot is begin[cell] + (number of cell members with a smaller index).  The pass
+// also writes the sorted keys and packs (x, H) into sorted float4 records that the
+// Verlet walk reads contiguously.
+template <int D>
+__global__ void k_rank_sort(const int32_t* __restrict__ tmp, const uint32_t* __restrict__ keys,
+                            const int32_t* __restrict__ begin, const int32_t* __restrict__ end, int n,
+                            const float* __restrict__ x, const float* __restrict__ H,
+                            int32_t* __restrict__ sort_index, uint32_t* __restrict__ sorted_keys, float4* __restrict__ recs,
+                            int32_t* __restrict__ tasks, int32_t* __restrict__ ntasks) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    sorted_keys[k] = keys[sort_index[k]];
+    int i = tmp[k];
+    uint32_t c = keys[i];
+    int b = begin[c], e = end[c];
+    int rank = 0;
+    for (int m = b; m < e; ++m) rank += tmp[m] < i;
+    int slot = b + rank;
+    if (rank == 0) {   // the cell's first particle appends its work items (chunks of <= 32 sorted positions)
+        int nch = (e - b + 31) >> 5;
+        int t0 = atomicAdd(ntasks, nch);
+        for (int q = 0; q < nch; ++q) tasks[t0 + q] = b + 32 * q;
+    }
+    sort_index[slot] = i;
+    sorted_keys[slot] = c;
+    Vec<D> xi = load_vec<D>(x, i);
+    float4 r = make_float4(xi.v[0], D > 1 ? xi.v[D > 1 ? 1 : 0] : 0.f, D > 2 ? xi.v[D > 2 ? 2 : 0] : 0.f, H[i]);
+    recs[slot] = r;
 }
 
-// Stencil of neighbour cell keys for a particle, ascending and de-duplicated.
+template <int D> __device__ __forceinline__ Vec<D> rec_pos(const float4& r) {
+    Vec<D> v;
+    v.v[0] = r.x;
+    if constexpr (D > 1) v.v[1] = r.y;
+    if constexpr (D > 2) v.v[2] = r.z;
+    return v;
+}
+
+// Stencil of neighbour cell keys in offset order (x fastest, offsets -1, 0, +1 per
+// axis), periodic axes wrapped, cells outside a non-periodic grid skipped, and a cell
+// reached twice (fewer than three cells along a periodic axis) kept only once.
+// shift[q*3+a] is the periodic image offset of stencil cell q along axis a (-L, 0, +L):
+// x_i - x_j - shift is the minimum-image difference for every pair within one cell
+// width, bit-identical to the per-pair test of dist_vec (x - 0 = x exactly).
 template <int D>
-__device__ __forceinline__ int stencil_keys(const int* c, const GridDev& g, const DomainF& dom, uint32_t* out) {
+__device__ __forceinline__ int stencil_keys(const int* c, const GridDev& g, const DomainF& dom, uint32_t* out, float* shift) {
     int cnt = 0;
     constexpr int NS = D == 1 ? 3 : (D == 2 ? 9 : 27);
+    bool dedupe = false;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) dedupe |= g.G[a] < 3;
+    #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        int o[3] = {s % 3 - 1, (s / 3) % 3 - 1, (s / 9) % 3 - 1};
+        const int o[3] = {s % 3 - 1, (s / 3) % 3 - 1, (s / 9) % 3 - 1};
         int cc[3];
+        float sh[3] = {0.f, 0.f, 0.f};
         bool ok = true;
         #pragma unroll
         for (int a = 0; a < D; ++a) {
             int v = c[a] + o[a];
-            if (v < 0 || v >= g.G[a]) {
-                if (dom.periodic[a]) v = (v + g.G[a]) % g.G[a];
-                else ok = false;
+            if (v < 0) {
+                if (dom.periodic[a]) { v += g.G[a]; sh[a] = -dom.L[a]; } else ok = false;
+            } else if (v >= g.G[a]) {
+                if (dom.periodic[a]) { v -= g.G[a]; sh[a] = dom.L[a]; } else ok = false;
             }
             cc[a] = v;
         }
-        if (!ok) continue;
         uint32_t k = morton<D>(cc);
-        // insertion into the sorted list, skipping duplicates
-        int m = cnt - 1;
-        bool dup = false;
-        for (int q = 0; q < cnt; ++q) if (out[q] == k) { dup = true; break; }
-        if (dup) continue;
-        while (m >= 0 && out[m] > k) { out[m + 1] = out[m]; --m; }
-        out[m + 1] = k;
-        ++cnt;
+        if (ok && dedupe) {
+            for (int q = 0; q < cnt; ++q) ok = ok && out[q] != k;
+        }
+        if (ok) {
+            #pragma unroll
+            for (int a = 0; a < 3; ++a) shift[cnt * 3 + a] = sh[a];
+            out[cnt++] = k;
+        }
     }
     return cnt;
 }
 
-template <int D, bool FILL>
-__global__ void __launch_bounds__(128)
-k_verlet(const float* __restrict__ x, const float* __restrict__ H, int n, const GridDev* __restrict__ gp, DevParams P,
-         const int32_t* __restrict__ sort_index, const int32_t* __restrict__ cell_begin, const int32_t* __restrict__ cell_end,
-         int32_t* __restrict__ counts, const int32_t* __restrict__ offsets, int32_t* __restrict__ list,
-         const long long* __restrict__ nnz, long long capacity) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    if (FILL && *nnz > capacity) return;
-    GridDev g = *gp;
-    int i = sort_index[t];
-    Vec<D> xi = load_vec<D>(x, i);
-    float Hi = H[i];
-    int c[3];
-    cell_coords<D>(xi, g, P.dom, c);
-    uint32_t keys[D == 1 ? 3 : (D == 2 ? 9 : 27)];
-    int nk = stencil_keys<D>(c, g, P.dom, keys);
-    int cnt = 0;
-    int base = FILL ? offsets[i] : 0;
-    for (int q = 0; q < nk; ++q) {
-        int b = cell_begin[keys[q]], e = cell_end[keys[q]];
-        for (int k = b; k < e; ++k) {
-            int j = sort_index[k];
-            Vec<D> xj = load_vec<D>(x, j);
-            float R = __fmul_rn(P.verlet_scale, fmaxf(Hi, __ldg(H + j)));
-            float r2 = dist2_rn<D>(dist_vec<D>(xi, xj, P.dom));
-            if (r2 < __fmul_rn(R, R)) {
-                if (FILL) list[base + cnt] = j;
-                ++cnt;
-            }
+// Verlet list walk, one warp per work item: up to 32 particles of one cell, lane l
+// owning sorted position start+l.  All lanes share the cell and hence the 3^d stencil
+// and every loop bound (no divergence).  Candidate records of each stencil cell are
+// staged through shared memory 32 at a time (one coalesced load, broadcast reads).
+// A Verlet entry needs r^2 < (verlet_scale*max(H_i,H_j))^2.  The fill pass also
+// marks the interacting subset used by the pair kernels -- fl(sqrt(r^2))/max(H_i,H_j)
+// < 1, exactly when some support scheme gives W != 0 (band test on r^2, exact
+// evaluation only inside the band) -- storing it inside the row's own Verlet range.
+// Rows are staged in shared memory (VS entries per lane) and flushed by the warp
+// cooperatively (VS lanes per row segment), so they are written with contiguous
+// stores.  Row order: stencil cells in offset order, candidates by sorted position.
+constexpr int VW_WARPS = 4;
+constexpr int VW_BLOCK = 32 * VW_WARPS;
+constexpr int VS = 16;
+
+__device__ __forceinline__ void verlet_flush(int lane, int wib, int& nb, int& nib, int& written, int& iwritten, int row,
+                                             int32_t (*sbuf)[32][VS], int2 (*sibuf)[32][VS],
+                                             int32_t* __restrict__ list, int2* __restrict__ ilist, bool want_inter) {
+    __syncwarp();
+    const int half = lane >> 4, e = lane & 15;
+    #pragma unroll 4
+    for (int r = 0; r < 32; r += 2) {
+        const int owner = r + half;
+        const int n_o = __shfl_sync(0xffffffffu, nb, owner);
+        const int b_o = __shfl_sync(0xffffffffu, row + written, owner);
+        if (e < n_o) list[b_o + e] = sbuf[wib][owner][e];
+        if (want_inter) {
+            const int ni_o = __shfl_sync(0xffffffffu, nib, owner);
+            const int ib_o = __shfl_sync(0xffffffffu, row + iwritten, owner);
+            if (e < ni_o) ilist[ib_o + e] = sibuf[wib][owner][e];
         }
     }
-    if (!FILL) counts[i] = cnt;
+    __syncwarp();
+    written += nb; iwritten += nib;
+    nb = 0; nib = 0;
+}
+
+template <int D, bool FILL>
+__global__ void __launch_bounds__(VW_BLOCK)
+k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_keys, const int32_t* __restrict__ tasks,
+         const int32_t* __restrict__ ntasks, const GridDev* __restrict__ gp, DevParams P,
+         const int32_t* __restrict__ sort_index, const int32_t* __restrict__ cell_begin, const int32_t* __restrict__ cell_end,
+         int32_t* __restrict__ counts, const int32_t* __restrict__ offsets, int32_t* __restrict__ ioffsets,
+         int32_t* __restrict__ icounts, int32_t* __restrict__ list, int2* __restrict__ ilist, long long* __restrict__ innz,
+         const long long* __restrict__ nnz, long long capacity) {
+    __shared__ float4 srec[VW_WARPS][32];
+    __shared__ int32_t sidx[FILL ? VW_WARPS : 1][32];
+    __shared__ int32_t sbuf[FILL ? VW_WARPS : 1][32][VS];
+    __shared__ int2 sibuf[FILL ? VW_WARPS : 1][32][VS];
+    const bool want_inter = FILL && ilist != nullptr;
+    if (FILL && *nnz > capacity) return;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int nt = *ntasks;
+    const GridDev g = *gp;
+    const DomainF dom = P.dom;
+    const float vs = P.verlet_scale;
+    for (int task = warp; task < nt; task += nwarps) {
+        const int start = tasks[task];
+        const uint32_t ckey = sorted_keys[start];
+        const int stop = min(start + 32, cell_end[ckey]);
+        const int t = start + lane;
+        const bool active = t < stop;
+        const float4 ri = recs[active ? t : start];
+        const Vec<D> xi = rec_pos<D>(ri);
+        const float Hi = ri.w;
+        int c[3];
+        cell_coords<D>(rec_pos<D>(recs[start]), g, dom, c);
+        uint32_t keys[D == 1 ? 3 : (D == 2 ? 9 : 27)];
+        float shifts[3 * (D == 1 ? 3 : (D == 2 ? 9 : 27))];
+        const int nk = stencil_keys<D>(c, g, dom, keys, shifts);
+        const int i = active ? sort_index[t] : 0;
+        int cnt = 0;
+        int row = 0, nb = 0, nib = 0, written = 0, iwritten = 0;
+        if (FILL && active) row = offsets[i];
+        for (int q = 0; q < nk; ++q) {
+            const int b = cell_begin[keys[q]], e = cell_end[keys[q]];
+            float sh[3] = {shifts[3 * q], shifts[3 * q + 1], shifts[3 * q + 2]};
+            for (int k0 = b; k0 < e; k0 += 32) {
+                __syncwarp();
+                if (k0 + lane < e) {
+                    srec[wib][lane] = recs[k0 + lane];
+                    if (FILL) sidx[wib][lane] = sort_index[k0 + lane];
+                }
+                __syncwarp();
+                const int mcount = min(32, e - k0);
+                for (int u0 = 0; u0 < mcount; u0 += 8) {
+                    // room for the next 8 candidates in every lane's buffer
+                    if (FILL && __any_sync(0xffffffffu, nb > VS - 8))
+                        verlet_flush(lane, wib, nb, nib, written, iwritten, row, sbuf, sibuf, list, ilist, want_inter);
+                    #pragma unroll
+                    for (int du = 0; du < 8; ++du) {
+                        const int u = u0 + du;
+                        const float4 rj = srec[wib][u < mcount ? u : 0];
+                        const float Hm = fmaxf(Hi, rj.w);
+                        const float R = __fmul_rn(vs, Hm);
+                        Vec<D> dv;
+                        #pragma unroll
+                        for (int a = 0; a < D; ++a)
+                            dv.v[a] = __fsub_rn(__fsub_rn(xi.v[a], a == 0 ? rj.x : (a == 1 ? rj.y : rj.z)), sh[a]);
+                        const float r2 = dist2_rn<D>(dv);
+                        const bool hit = active & (u < mcount) & (r2 < __fmul_rn(R, R));
+                        if (FILL) {
+                            bool inter = false;
+                            if (want_inter) {
+                                const float h2 = Hm * Hm;
+                                inter = hit & (r2 < 0.9998f * h2);
+                                const bool band = hit & !inter & (r2 < 1.0002f * h2);
+                                if (__any_sync(0xffffffffu, band)) {     // rare: exact test near r = H
+                                    if (band) inter = __fdiv_rn(sqrtf(r2), Hm) < 1.f;
+                                }
+                            }
+                            if (hit) {
+                                const int j = sidx[wib][u];
+                                if (inter) sibuf[wib][lane][nib++] = make_int2(j, row + written + nb);
+                                sbuf[wib][lane][nb++] = j;
+                            }
+                        } else {
+                            cnt += hit;
+                        }
+                    }
+                }
+            }
+        }
+        if (FILL) {
+            if (__any_sync(0xffffffffu, nb > 0 || nib > 0))
+                verlet_flush(lane, wib, nb, nib, written, iwritten, row, sbuf, sibuf, list, ilist, want_inter);
+            if (want_inter) {
+                if (active) { ioffsets[i] = row; icounts[i] = iwritten; }
+                int tot = active ? iwritten : 0;
+                #pragma unroll
+                for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+                if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long*>(innz), (unsigned long long)tot);
+            }
+        } else if (active) {
+            counts[i] = cnt;
+        }
+    }
 }
 
 __global__ void k_check_capacity(const long long* nnz, long long capacity, int32_t* status) {
@@ -472,6 +607,10 @@ struct NbWs {
     long long* total;
     uint32_t* keys;
     int32_t* counts;
+    int32_t* tmp;
+    float4* recs;
+    int32_t* tasks;
+    int32_t* ntasks;
     char* scan;
     int64_t bytes;
 };
@@ -484,6 +623,10 @@ static NbWs carve(char* base, int64_t n, int64_t cap) {
     w.total = reinterpret_cast<long long*>(base + off); off += 256;
     w.keys = reinterpret_cast<uint32_t*>(base + off); off += align256(n * 4);
     w.counts = reinterpret_cast<int32_t*>(base + off); off += align256(cap * 4);
+    w.tmp = reinterpret_cast<int32_t*>(base + off); off += align256(n * 4);
+    w.recs = reinterpret_cast<float4*>(base + off); off += align256(n * 16);
+    w.tasks = reinterpret_cast<int32_t*>(base + off); off += align256(n * 4);
+    w.ntasks = reinterpret_cast<int32_t*>(base + off); off += 256;
     w.scan = base + off;
     int64_t sb = scan_ws_bytes(cap > n ? cap : n);
     off += align256(sb);
@@ -537,28 +680,38 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
                         int32_t* sort_index, uint32_t* sorted_keys,
                         int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
                         int32_t* neighbor_offsets, int32_t* num_neighbors,
-                        int32_t* neighbor_list, int64_t list_capacity,
-                        int64_t* nnz_out, int32_t* status, void* stream) {
+                        int32_t* neighbor_list, int64_t list_capacity, int64_t* nnz_out,
+                        int32_t* inter_offsets, int32_t* inter_counts, int32_t* inter_list,
+                        int64_t inter_capacity, int64_t* inter_nnz_out,
+                        int32_t* status, void* stream) {
     DevParams P;
     int rc = params_to_dev(p, &P);
     if (rc) return rc;
     if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_build: n out of range");
     if (cell_capacity < 1) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_build: cell_capacity < 1");
     WSPH_CHECK_PTR(nnz_out); WSPH_CHECK_PTR(status); WSPH_CHECK_PTR(grid_out);
+    const bool inter = inter_list != nullptr || inter_counts != nullptr;
+    if (inter) { WSPH_CHECK_PTR(inter_offsets); WSPH_CHECK_PTR(inter_counts); WSPH_CHECK_PTR(inter_nnz_out); }
     cudaStream_t s = WSPH_STREAM(stream);
     if (n == 0) {
         cudaMemsetAsync(nnz_out, 0, sizeof(int64_t), s);
+        if (inter) cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
         return check_launch("sph_neighbors_build");
     }
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(workspace); WSPH_CHECK_PTR(sort_index);
     WSPH_CHECK_PTR(sorted_keys); WSPH_CHECK_PTR(cell_begin); WSPH_CHECK_PTR(cell_end);
     WSPH_CHECK_PTR(neighbor_offsets); WSPH_CHECK_PTR(num_neighbors);
     if (list_capacity > 0) WSPH_CHECK_PTR(neighbor_list);
+    if (inter && inter_capacity > 0) WSPH_CHECK_PTR(inter_list);
     if (P.dim == 2 && (reinterpret_cast<uintptr_t>(x) & 7)) return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
+    if (inter && (reinterpret_cast<uintptr_t>(inter_list) & 7)) return set_error(SPH_ERR_BAD_ARG, "inter_list must be 8-byte aligned");
+    if (inter && inter_capacity < list_capacity)
+        return set_error(SPH_ERR_BAD_ARG, "inter_capacity (%lld pairs) must be >= list_capacity (%lld)", (long long)inter_capacity, (long long)list_capacity);
     NbWs w = carve(reinterpret_cast<char*>(workspace), n, cell_capacity);
     if (workspace_bytes < w.bytes) return set_error(SPH_ERR_WORKSPACE, "neighbour workspace too small: %lld < %lld", (long long)workspace_bytes, (long long)w.bytes);
     int mb = max_bits_for(P.dim, cell_capacity);
     int64_t ncells = (int64_t)1 << (mb * P.dim);
+    long long* innz = inter ? reinterpret_cast<long long*>(inter_nnz_out) : nullptr;
 
     cudaMemsetAsync(w.hmax, 0, sizeof(float), s);
     int rblocks = grid_for(n, 256);
@@ -569,16 +722,23 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, k_keys<D><<<grid_for(n, 256), 256, 0, s>>>(x, (int)n, w.grid, P.dom, w.keys, w.counts));
     exclusive_scan_i32(w.counts, cell_begin, ncells, w.scan, w.total, s);
     cudaMemcpyAsync(cell_end, cell_begin, ncells * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
-    wsph::count_launch(); k_scatter<<<grid_for(n, 256), 256, 0, s>>>(w.keys, (int)n, cell_end, sort_index);
-    wsph::count_launch(); k_cell_sort<<<grid_for(ncells, 256), 256, 0, s>>>(cell_begin, cell_end, ncells, sort_index);
-    wsph::count_launch(); k_sorted_keys<<<grid_for(n, 256), 256, 0, s>>>(w.keys, sort_index, (int)n, sorted_keys);
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, false><<<grid_for(n, 128), 128, 0, s>>>(x, H, (int)n, w.grid, P, sort_index, cell_begin, cell_end,
-                                                                                 num_neighbors, nullptr, nullptr, nullptr, 0)));
+    wsph::count_launch(); k_scatter<<<grid_for(n, 256), 256, 0, s>>>(w.keys, (int)n, cell_end, w.tmp);
+    cudaMemsetAsync(w.ntasks, 0, sizeof(int32_t), s);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_rank_sort<D><<<grid_for(n, 256), 256, 0, s>>>(w.tmp, w.keys, cell_begin, cell_end, (int)n, x, H,
+                                                                                                 sort_index, sorted_keys, w.recs, w.tasks, w.ntasks)));
+    int vblocks = grid_for(n, VW_BLOCK);          // >= one warp per 32 particles; warps stride over the work items
+    if (vblocks > 148 * 32) vblocks = 148 * 32;
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, false><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
+                                                                                 cell_begin, cell_end, num_neighbors, nullptr, nullptr, nullptr,
+                                                                                 nullptr, nullptr, nullptr, nullptr, 0)));
     exclusive_scan_i32(num_neighbors, neighbor_offsets, n, w.scan, reinterpret_cast<long long*>(nnz_out), s);
     wsph::count_launch(); k_check_capacity<<<1, 1, 0, s>>>(reinterpret_cast<long long*>(nnz_out), list_capacity, status);
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, true><<<grid_for(n, 128), 128, 0, s>>>(x, H, (int)n, w.grid, P, sort_index, cell_begin, cell_end,
-                                                                                nullptr, neighbor_offsets, neighbor_list,
-                                                                                reinterpret_cast<long long*>(nnz_out), list_capacity)));
+    if (inter) cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, true><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
+                                                                                cell_begin, cell_end, nullptr, neighbor_offsets,
+                                                                                inter ? inter_offsets : nullptr, inter ? inter_counts : nullptr,
+                                                                                neighbor_list, inter ? reinterpret_cast<int2*>(inter_list) : nullptr,
+                                                                                innz, reinterpret_cast<long long*>(nnz_out), list_capacity)));
     return check_launch("sph_neighbors_build");
 }
 

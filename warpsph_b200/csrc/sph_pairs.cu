@@ -1,9 +1,17 @@
 // SPH pair-interaction kernels of the compressible (CRKSPH / CompSPH) hot path.
 //
-// Every pair kernel walks the CSR Verlet list of one particle per thread in list
-// order.  Entries whose distance exceeds the kernel support contribute exact zeros
-// (as in the reference, where Verlet entries beyond the support give W = 0), so
-// those entries only cost the distance test.
+// Layout: G lanes of a warp cooperate on one particle i.  Lane l walks the entries
+// b+l, b+l+G, ... of i's neighbour row, so the G lanes read G consecutive entries
+// (coalesced index loads and pair-array stores), accumulate per-lane partial sums,
+// and reduce them with warp shuffles inside the group.  Rows are either the Verlet
+// list (stride 1, entry index = position in the list) or the interacting list
+// (stride 2, (j, Verlet entry index) pairs holding only r < max(H_i, H_j)), which
+// removes the beyond-support entries -- about half of a Verlet row -- from every
+// pass that only needs W != 0.
+//
+// Arithmetic restates the reference (file:line at each kernel); divisions by the
+// same quantity are replaced by multiplications with a reciprocal, so results
+// differ from the CPU oracle by rounding only.
 #include <cuda_runtime.h>
 #include "sph_common.cuh"
 
@@ -11,7 +19,56 @@ namespace wsph {
 
 constexpr int PAIR_BLOCK = 128;
 
-// Neumaier-compensated accumulator (used when DevParams::kahan is set).
+// ---------------------------------------------------------------- group helpers
+template <int G> struct Grp {
+    int i, lane;
+    bool valid;
+    __device__ __forceinline__ explicit Grp(int n) {
+        int t = blockIdx.x * blockDim.x + threadIdx.x;
+        i = t / G;
+        lane = threadIdx.x & (G - 1);
+        valid = i < n;
+    }
+};
+template <int G> __device__ __forceinline__ float gsum(float v) {
+    #pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+template <int G> __device__ __forceinline__ float gmaxw(float v) {
+    #pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v = wmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+template <int ST> __device__ __forceinline__ void entry(const int32_t* __restrict__ list, int q, int& j, int& k) {
+    if constexpr (ST == 2) {
+        int2 e = __ldg(reinterpret_cast<const int2*>(list) + q);
+        j = e.x; k = e.y;
+    } else {
+        j = __ldg(list + q); k = q;
+    }
+}
+template <int G> __host__ __forceinline__ int grid_g(int64_t n) { return (int)((n * G + PAIR_BLOCK - 1) / PAIR_BLOCK); }
+
+// W and grad_i W with a precomputed 1/H.
+template <int KF, int D> __device__ __forceinline__ float kW_inv(float r, float invH) {
+    float q = r * invH;
+    if (!(q < 1.f)) return 0.f;
+    float k, p; kernel_kp<KF, D>(q, k, p);
+    return KernelTraits<KF, D>::C * ipow<D>(invH) * k;
+}
+template <int KF, int D> __device__ __forceinline__ void kWG_inv(const Vec<D>& x, float r, float invH, float& W, Vec<D>& g) {
+    float q = r * invH;
+    if (!(q < 1.f)) { W = 0.f; g = vzero<D>(); return; }
+    float k, p; kernel_kp<KF, D>(q, k, p);
+    float cH = KernelTraits<KF, D>::C * ipow<D>(invH);
+    W = cH * k;
+    float s = -cH * p * (invH * invH);
+    #pragma unroll
+    for (int a = 0; a < D; ++a) g.v[a] = s * x.v[a];
+}
+
+// Neumaier-compensated accumulator (DevParams::kahan).
 struct KSum {
     float s, c;
     __device__ __forceinline__ void init() { s = 0.f; c = 0.f; }
@@ -21,103 +78,109 @@ struct KSum {
         if (fabsf(s) >= fabsf(x)) c += (s - t) + x; else c += (x - t) + s;
         s = t;
     }
-    __device__ __forceinline__ float value() const { return s + c; }
 };
 
-// ---------------------------------------------------------------- density
-template <int KF, int D>
+// ---------------------------------------------------------------- density (modules/density/density.py:16-28)
+template <int KF, int D, int G, int ST>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_density(int n, int mode, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
           const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
           float* __restrict__ rho) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Vec<D> xi = load_vec<D>(x, i);
-    float Hi = H[i];
-    int b = offs[i], e = b + cnt[i];
+    Grp<G> g(n);
     float s = 0.f;
-    for (int k = b; k < e; ++k) {
-        int j = __ldg(list + k);
-        Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
-        float r = safe_sqrt(dot<D>(xij, xij));
-        s += __ldg(m + j) * kernelW_mode<KF, D>(r, Hi, __ldg(H + j), mode);
+    if (g.valid) {
+        Vec<D> xi = load_vec<D>(x, g.i);
+        float Hi = H[g.i];
+        int b = offs[g.i], e = b + cnt[g.i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry<ST>(list, q, j, k);
+            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float r = safe_sqrt(dot<D>(xij, xij));
+            s += __ldg(m + j) * kernelW_mode<KF, D>(r, Hi, __ldg(H + j), mode);
+        }
     }
-    rho[i] = s;
+    s = gsum<G>(s);
+    if (g.valid && g.lane == 0) rho[g.i] = s;
 }
 
-// ---------------------------------------------------------------- adaptive support (Monaghan Newton)
-// h(V) from utils/support.py:24-44 (volumeToSupportHelper)
+// ---------------------------------------------------------------- adaptive support
+// h(V) of utils/support.py:24-44 (volumeToSupportHelper)
 template <int D> __device__ __forceinline__ float volume_to_support(float V, float nH) {
     if constexpr (D == 1) return nH * V / 2.f;
     else if constexpr (D == 2) return sqrtf(nH * V / 3.14159265358979f);
     else return powf(nH * V / 3.14159265358979f * 3.f / 4.f, 1.f / 3.f);
 }
 
-template <int KF, int D>
+// One Newton iteration of modules/adaptiveSupport/optimalSupportMonaghan.py:87-125
+// with Omega of modules/adaptiveSupport/wp_omega.py:40-60 (gather support).
+template <int KF, int D, int G, int ST>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_adaptive_h(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
              const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
              const float* __restrict__ hb, float* __restrict__ rho_out, float* __restrict__ H_out, float* __restrict__ ratio) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Vec<D> xi = load_vec<D>(x, i);
-    float Hi = H[i];
-    int b = offs[i], e = b + cnt[i];
-    float rs = 0.f, ds = 0.f;
-    for (int k = b; k < e; ++k) {
-        int j = __ldg(list + k);
-        Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
-        float r = safe_sqrt(dot<D>(xij, xij));
-        float W, dWdH;
-        kernelWdH<KF, D>(r, Hi, W, dWdH);   // gather support
-        float mj = __ldg(m + j);
-        rs += mj * W;
-        ds += mj * dWdH;
+    Grp<G> g(n);
+    float rs = 0.f, ds = 0.f, Hi = 1.f;
+    if (g.valid) {
+        Vec<D> xi = load_vec<D>(x, g.i);
+        Hi = H[g.i];
+        int b = offs[g.i], e = b + cnt[g.i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry<ST>(list, q, j, k);
+            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float r = safe_sqrt(dot<D>(xij, xij));
+            float W, dWdH;
+            kernelWdH<KF, D>(r, Hi, W, dWdH);
+            float mj = __ldg(m + j);
+            rs += mj * W;
+            ds += mj * dWdH;
+        }
     }
-    // optimalSupportMonaghan.py:104-117
+    rs = gsum<G>(rs);
+    ds = gsum<G>(ds);
+    if (!g.valid || g.lane != 0) return;
     float rho = rs;
     float safe_rho = isfinite(rho) ? fmaxf(rho, 1e-12f) : 1.f;
-    float Fv = Hi - volume_to_support<D>(m[i] / safe_rho, P.target_neighbors);
+    float Fv = Hi - volume_to_support<D>(m[g.i] / safe_rho, P.target_neighbors);
     float dh_drho = -Hi / (rho * (float)D);
-    float omega = 1.f - dh_drho * ds;           // wp_omega.py: 1 - sum dh_drho m_j dW/dh
+    float omega = 1.f - dh_drho * ds;
     if (!isfinite(omega)) omega = 0.f;
     float step = Fv / (omega + 1e-6f);
     if (!isfinite(step)) step = 0.f;
     float hn = Hi - step;
     if (!isfinite(hn)) hn = Hi;
-    float lo = hb[0] * 0.25f, hi = hb[1] * 4.f;
-    hn = fminf(fmaxf(hn, lo), hi);
-    rho_out[i] = rho;
-    H_out[i] = hn;
-    if (ratio) ratio[i] = hn / (Hi + 1e-6f);
+    hn = fminf(fmaxf(hn, hb[0] * 0.25f), hb[1] * 4.f);
+    rho_out[g.i] = rho;
+    H_out[g.i] = hn;
+    if (ratio) ratio[g.i] = hn / (Hi + 1e-6f);
 }
 
-// ---------------------------------------------------------------- CRK volume and factors
-template <int KF, int D>
+// ---------------------------------------------------------------- CRK volume (scatter support)
+template <int KF, int D, int G, int ST>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_crk_volume(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H,
              const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
              float* __restrict__ V) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Vec<D> xi = load_vec<D>(x, i);
-    int b = offs[i], e = b + cnt[i];
+    Grp<G> g(n);
     float s = 0.f;
-    for (int k = b; k < e; ++k) {
-        int j = __ldg(list + k);
-        Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
-        float r = safe_sqrt(dot<D>(xij, xij));
-        s += kernelW<KF, D>(r, __ldg(H + j));
+    if (g.valid) {
+        Vec<D> xi = load_vec<D>(x, g.i);
+        int b = offs[g.i], e = b + cnt[g.i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry<ST>(list, q, j, k);
+            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float r = safe_sqrt(dot<D>(xij, xij));
+            s += kW_inv<KF, D>(r, 1.f / __ldg(H + j));
+        }
     }
-    V[i] = 1.f / s;
+    s = gsum<G>(s);
+    if (g.valid && g.lane == 0) V[g.i] = 1.f / s;
 }
 
 // Inverse of a symmetric DxD matrix in double; returns the determinant.
 template <int D> __device__ __forceinline__ double inv_sym(const double (&a)[D][D], double (&r)[D][D]) {
     if constexpr (D == 1) {
-        double det = a[0][0];
-        r[0][0] = 1.0 / det;
-        return det;
+        r[0][0] = 1.0 / a[0][0];
+        return a[0][0];
     } else if constexpr (D == 2) {
         double det = a[0][0] * a[1][1] - a[0][1] * a[1][0];
         double id = 1.0 / det;
@@ -143,141 +206,144 @@ template <int D> __device__ __forceinline__ double inv_sym(const double (&a)[D][
     }
 }
 
-// Moments (FP32 sums over the list, W_ij = W(r_ij, H_j)), FP64 solve for A, B, gradA,
-// gradB (Frontiere, Raskin & Owen 2017, linear reproducing conditions), and the
-// CRK density sum_j m_j W^R_ij.  Fallback to zeroth-order correction when the
-// second moment is singular (fewer than D+1 effective neighbours).
-template <int KF, int D>
+// CRK moments (FP32 sums, W_ij = W(r_ij, H_j)), FP64 solve for A, B, gradA, gradB
+// (Frontiere, Raskin & Owen 2017: linear reproducing conditions) and the CRK density
+// sum_j m_j W^R_ij.  A singular second moment (fewer than D+1 effective neighbours)
+// falls back to the zeroth-order correction.
+template <int D> struct CrkAcc {
+    float m0, s0, m1[D], s1[D], dm0[D], m2[D][D], dm1[D][D], dm2[D][D][D];
+};
+template <int KF, int D, int G, int ST>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_crk_factors(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
               const float* __restrict__ V, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
               const int32_t* __restrict__ list, float* __restrict__ Aout, float* __restrict__ Bout,
               float* __restrict__ gAout, float* __restrict__ gBout, float* __restrict__ rho_out) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Vec<D> xi = load_vec<D>(x, i);
-    int b = offs[i], e = b + cnt[i];
-    float m0 = 0.f, m1[D], m2[D][D], dm0[D], dm1[D][D], dm2[D][D][D], s0 = 0.f, s1[D];
-    #pragma unroll
-    for (int a = 0; a < D; ++a) {
-        m1[a] = 0.f; dm0[a] = 0.f; s1[a] = 0.f;
+    Grp<G> g(n);
+    CrkAcc<D> a;
+    {
+        float* f = reinterpret_cast<float*>(&a);
         #pragma unroll
-        for (int c = 0; c < D; ++c) { m2[a][c] = 0.f; dm1[a][c] = 0.f;
-            #pragma unroll
-            for (int g = 0; g < D; ++g) dm2[a][c][g] = 0.f; }
+        for (int q = 0; q < (int)(sizeof(CrkAcc<D>) / 4); ++q) f[q] = 0.f;
     }
-    for (int k = b; k < e; ++k) {
-        int j = __ldg(list + k);
-        Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
-        float r = safe_sqrt(dot<D>(xij, xij));
-        float W; Vec<D> gW;
-        kernelWG<KF, D>(xij, r, __ldg(H + j), W, gW);
-        if (W == 0.f) continue;
-        float Vj = __ldg(V + j), mj = __ldg(m + j);
-        float VW = Vj * W;
-        m0 += VW;
-        s0 += mj * W;
-        #pragma unroll
-        for (int a = 0; a < D; ++a) {
-            m1[a] += VW * xij.v[a];
-            s1[a] += mj * W * xij.v[a];
-            dm0[a] += Vj * gW.v[a];
+    if (g.valid) {
+        Vec<D> xi = load_vec<D>(x, g.i);
+        int b = offs[g.i], e = b + cnt[g.i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry<ST>(list, q, j, k);
+            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float r = safe_sqrt(dot<D>(xij, xij));
+            float W; Vec<D> gW;
+            kWG_inv<KF, D>(xij, r, 1.f / __ldg(H + j), W, gW);
+            if (W == 0.f) continue;
+            float Vj = __ldg(V + j), mj = __ldg(m + j);
+            float VW = Vj * W, mW = mj * W;
+            a.m0 += VW;
+            a.s0 += mW;
             #pragma unroll
-            for (int c = 0; c < D; ++c) {
-                m2[a][c] += VW * xij.v[a] * xij.v[c];
-                // d/dx^c of (x^a W): x^a dW/dx^c + delta_ac W
-                dm1[a][c] += Vj * (xij.v[a] * gW.v[c] + (a == c ? W : 0.f));
-            }
-        }
-        #pragma unroll
-        for (int a = 0; a < D; ++a)
-            #pragma unroll
-            for (int c = a; c < D; ++c)
+            for (int u = 0; u < D; ++u) {
+                a.m1[u] += VW * xij.v[u];
+                a.s1[u] += mW * xij.v[u];
+                a.dm0[u] += Vj * gW.v[u];
                 #pragma unroll
-                for (int g = 0; g < D; ++g)
-                    dm2[a][c][g] += Vj * (xij.v[a] * xij.v[c] * gW.v[g] + ((a == g ? xij.v[c] : 0.f) + (c == g ? xij.v[a] : 0.f)) * W);
+                for (int c = 0; c < D; ++c) {
+                    a.m2[u][c] += VW * xij.v[u] * xij.v[c];
+                    a.dm1[u][c] += Vj * (xij.v[u] * gW.v[c] + (u == c ? W : 0.f));
+                }
+            }
+            #pragma unroll
+            for (int u = 0; u < D; ++u)
+                #pragma unroll
+                for (int c = u; c < D; ++c)
+                    #pragma unroll
+                    for (int w = 0; w < D; ++w)
+                        a.dm2[u][c][w] += Vj * (xij.v[u] * xij.v[c] * gW.v[w] + ((u == w ? xij.v[c] : 0.f) + (c == w ? xij.v[u] : 0.f)) * W);
+        }
     }
-    // FP64 solve
-    double M2[D][D], Mi[D][D];
-    double tr = 0.0;
-    #pragma unroll
-    for (int a = 0; a < D; ++a) {
+    {
+        float* f = reinterpret_cast<float*>(&a);
         #pragma unroll
-        for (int c = 0; c < D; ++c) M2[a][c] = (double)(a <= c ? m2[a][c] : m2[c][a]);
-        tr += M2[a][a];
+        for (int q = 0; q < (int)(sizeof(CrkAcc<D>) / 4); ++q) f[q] = gsum<G>(f[q]);
+    }
+    if (!g.valid || g.lane != 0) return;
+    const int i = g.i;
+    double M2[D][D], Mi[D][D], tr = 0.0;
+    #pragma unroll
+    for (int u = 0; u < D; ++u) {
+        #pragma unroll
+        for (int c = 0; c < D; ++c) M2[u][c] = (double)(u <= c ? a.m2[u][c] : a.m2[c][u]);
+        tr += M2[u][u];
     }
     double det = inv_sym<D>(M2, Mi);
-    double scale = tr / D;
-    double sD = scale; for (int a = 1; a < D; ++a) sD *= scale;
-    bool ok = isfinite(det) && fabs(det) > 1e-10 * fabs(sD) && m0 > 0.f;
+    double sc = tr / D, sD = sc;
+    #pragma unroll
+    for (int u = 1; u < D; ++u) sD *= sc;
+    bool ok = isfinite(det) && fabs(det) > 1e-10 * fabs(sD) && a.m0 > 0.f;
     double A, Bv[D], gA[D], gB[D][D];
     if (ok) {
-        // B = -M2^-1 m1 ; A = 1/(m0 + m1.B)
-        double mb = m0;
+        double mb = a.m0;
         #pragma unroll
-        for (int a = 0; a < D; ++a) {
+        for (int u = 0; u < D; ++u) {
             double t = 0.0;
             #pragma unroll
-            for (int c = 0; c < D; ++c) t -= Mi[a][c] * (double)m1[c];
-            Bv[a] = t;
+            for (int c = 0; c < D; ++c) t -= Mi[u][c] * (double)a.m1[c];
+            Bv[u] = t;
         }
         #pragma unroll
-        for (int a = 0; a < D; ++a) mb += (double)m1[a] * Bv[a];
+        for (int u = 0; u < D; ++u) mb += (double)a.m1[u] * Bv[u];
         A = 1.0 / mb;
-        // dB/dx^g = -M2^-1 (dm1[:,g] + dm2[:,:,g] B)
         #pragma unroll
-        for (int g = 0; g < D; ++g) {
+        for (int w = 0; w < D; ++w) {
             double rhs[D];
             #pragma unroll
-            for (int a = 0; a < D; ++a) {
-                double t = (double)dm1[a][g];
+            for (int u = 0; u < D; ++u) {
+                double t = (double)a.dm1[u][w];
                 #pragma unroll
-                for (int c = 0; c < D; ++c) t += (double)(a <= c ? dm2[a][c][g] : dm2[c][a][g]) * Bv[c];
-                rhs[a] = t;
+                for (int c = 0; c < D; ++c) t += (double)(u <= c ? a.dm2[u][c][w] : a.dm2[c][u][w]) * Bv[c];
+                rhs[u] = t;
             }
             #pragma unroll
-            for (int a = 0; a < D; ++a) {
+            for (int u = 0; u < D; ++u) {
                 double t = 0.0;
                 #pragma unroll
-                for (int c = 0; c < D; ++c) t -= Mi[a][c] * rhs[c];
-                gB[a][g] = t;
+                for (int c = 0; c < D; ++c) t -= Mi[u][c] * rhs[c];
+                gB[u][w] = t;
             }
         }
-        // dA/dx^g = -A^2 (dm0_g + dm1[:,g].B + m1.dB[:,g])
         #pragma unroll
-        for (int g = 0; g < D; ++g) {
-            double t = (double)dm0[g];
+        for (int w = 0; w < D; ++w) {
+            double t = (double)a.dm0[w];
             #pragma unroll
-            for (int a = 0; a < D; ++a) t += (double)dm1[a][g] * Bv[a] + (double)m1[a] * gB[a][g];
-            gA[g] = -A * A * t;
+            for (int u = 0; u < D; ++u) t += (double)a.dm1[u][w] * Bv[u] + (double)a.m1[u] * gB[u][w];
+            gA[w] = -A * A * t;
         }
     } else {
-        double m0d = (double)m0;
+        double m0d = (double)a.m0;
         A = 1.0 / m0d;
         #pragma unroll
-        for (int a = 0; a < D; ++a) {
-            Bv[a] = 0.0;
-            gA[a] = -(double)dm0[a] / (m0d * m0d);
+        for (int u = 0; u < D; ++u) {
+            Bv[u] = 0.0;
+            gA[u] = -(double)a.dm0[u] / (m0d * m0d);
             #pragma unroll
-            for (int c = 0; c < D; ++c) gB[a][c] = 0.0;
+            for (int c = 0; c < D; ++c) gB[u][c] = 0.0;
         }
     }
-    double rho = (double)s0;
+    double rho = (double)a.s0;
     #pragma unroll
-    for (int a = 0; a < D; ++a) rho += Bv[a] * (double)s1[a];
+    for (int u = 0; u < D; ++u) rho += Bv[u] * (double)a.s1[u];
     rho *= A;
     Aout[i] = (float)A;
     #pragma unroll
-    for (int a = 0; a < D; ++a) {
-        Bout[(size_t)i * D + a] = (float)Bv[a];
-        gAout[(size_t)i * D + a] = (float)gA[a];
+    for (int u = 0; u < D; ++u) {
+        Bout[(size_t)i * D + u] = (float)Bv[u];
+        gAout[(size_t)i * D + u] = (float)gA[u];
         #pragma unroll
-        for (int c = 0; c < D; ++c) gBout[(size_t)i * D * D + a * D + c] = (float)gB[a][c];
+        for (int c = 0; c < D; ++c) gBout[(size_t)i * D * D + u * D + c] = (float)gB[u][c];
     }
     if (rho_out) rho_out[i] = (float)rho;
 }
 
-// ---------------------------------------------------------------- EOS
+// ---------------------------------------------------------------- EOS (modules/eos/idealGas.py:16-36)
 __global__ void k_eos(int n, float gamma, const float* __restrict__ u, const float* __restrict__ rho,
                       float* __restrict__ Aout, float* __restrict__ Pout, float* __restrict__ cout) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -289,58 +355,56 @@ __global__ void k_eos(int n, float gamma, const float* __restrict__ u, const flo
 }
 
 // ---------------------------------------------------------------- CRK velocity gradient (+ Cullen div, v_sig)
-template <int KF, int D>
+// schemes/crkSPH.py:158-172 (difference form, scatter support, CRK kernel, .mT),
+// CullenDehnen2010.py:246-257 (super-symmetric divergence), wp_vsig.py:55-90.
+template <int KF, int D, int G, int ST>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_grad_v(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
          const float* __restrict__ rho, const float* __restrict__ V, const float* __restrict__ A, const float* __restrict__ B,
          const float* __restrict__ gA, const float* __restrict__ gB, const float* __restrict__ v, const float* __restrict__ c,
          const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
          float* __restrict__ DvDx, float* __restrict__ drhodt, float* __restrict__ div_out, float* __restrict__ vsig_out) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
-    float Hi = H[i];
-    float Ai = A[i];
-    Vec<D> Bi = load_vec<D>(B, i), gAi = load_vec<D>(gA, i);
-    Mat<D> gBi = load_mat<D>(gB, i);
-    bool want_cd = div_out != nullptr;
-    float ci = want_cd ? c[i] : 0.f;
-    Mat<D> G = mzero<D>();
+    Grp<G> g(n);
+    const bool want_div = div_out != nullptr, want_vs = vsig_out != nullptr;
+    Mat<D> Gm = mzero<D>();
     float div = 0.f, vsig = 0.f;
-    float vs2 = P.verlet_scale;
-    int b = offs[i], e = b + cnt[i];
-    for (int k = b; k < e; ++k) {
-        int j = __ldg(list + k);
-        Vec<D> xj = load_vec<D>(x, j);
-        Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
-        float r = safe_sqrt(dot<D>(xij, xij));
-        float Hj = __ldg(H + j);
-        Vec<D> vj = load_vec<D>(v, j);
-        float W; Vec<D> gW;
-        kernelWG<KF, D>(xij, r, Hj, W, gW);
-        if (W != 0.f) {
-            Vec<D> gR = crk_grad<D>(xij, W, gW, Ai, Bi, gAi, gBi);
-            float Vj = __ldg(V + j);
-            #pragma unroll
-            for (int a = 0; a < D; ++a) {
-                float dv = Vj * (vj.v[a] - vi.v[a]);
+    if (g.valid) {
+        const int i = g.i;
+        Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
+        float Hi = H[i], Ai = A[i];
+        Vec<D> Bi = load_vec<D>(B, i), gAi = load_vec<D>(gA, i);
+        Mat<D> gBi = load_mat<D>(gB, i);
+        float ci = want_vs ? c[i] : 0.f;
+        int b = offs[i], e = b + cnt[i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry<ST>(list, q, j, k);
+            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float r = safe_sqrt(dot<D>(xij, xij));
+            float Hj = __ldg(H + j);
+            Vec<D> vj = load_vec<D>(v, j);
+            float W; Vec<D> gW;
+            kWG_inv<KF, D>(xij, r, 1.f / Hj, W, gW);
+            if (W != 0.f) {
+                Vec<D> gR = crk_grad<D>(xij, W, gW, Ai, Bi, gAi, gBi);
+                float Vj = __ldg(V + j);
                 #pragma unroll
-                for (int g = 0; g < D; ++g) G.m[a][g] += dv * gR.v[g];
+                for (int a = 0; a < D; ++a) {
+                    float dv = Vj * (vj.v[a] - vi.v[a]);
+                    #pragma unroll
+                    for (int w = 0; w < D; ++w) Gm.m[a][w] += dv * gR.v[w];
+                }
             }
-        }
-        if (want_cd) {
             float Hs = wmax(Hi, Hj);
-            if (r < Hs) {
+            if (want_div && r < Hs) {
                 float W2; Vec<D> g2;
-                kernelWG<KF, D>(xij, r, Hs, W2, g2);
+                kWG_inv<KF, D>(xij, r, 1.f / Hs, W2, g2);
                 float vol = __ldg(m + j) / __ldg(rho + j);
                 float s = 0.f;
                 #pragma unroll
                 for (int a = 0; a < D; ++a) s += (vj.v[a] - vi.v[a]) * g2.v[a];
                 div += vol * s;
             }
-            // signal velocity over the Verlet set r < verlet_scale*max(H_i, H_j)
-            if (r < vs2 * Hs) {
+            if (want_vs && r < P.verlet_scale * Hs) {
                 float mu = 0.f;
                 #pragma unroll
                 for (int a = 0; a < D; ++a) mu += (vi.v[a] - vj.v[a]) * xij.v[a];
@@ -351,46 +415,83 @@ k_grad_v(int n, DevParams P, const float* __restrict__ x, const float* __restric
             }
         }
     }
-    store_mat<D>(DvDx, i, G);
-    if (drhodt) {
-        float tr = G.m[0][0];
+    #pragma unroll
+    for (int a = 0; a < D; ++a)
         #pragma unroll
-        for (int a = 1; a < D; ++a) tr += G.m[a][a];
-        drhodt[i] = -tr * rho[i];
+        for (int w = 0; w < D; ++w) Gm.m[a][w] = gsum<G>(Gm.m[a][w]);
+    if (want_div) div = gsum<G>(div);
+    if (want_vs) vsig = gmaxw<G>(vsig);
+    if (!g.valid || g.lane != 0) return;
+    store_mat<D>(DvDx, g.i, Gm);
+    if (drhodt) {
+        float tr = Gm.m[0][0];
+        #pragma unroll
+        for (int a = 1; a < D; ++a) tr += Gm.m[a][a];
+        drhodt[g.i] = -tr * rho[g.i];
     }
-    if (want_cd) { div_out[i] = div; if (vsig_out) vsig_out[i] = fabsf(vsig); }
+    if (want_div) div_out[g.i] = div;
+    if (want_vs) vsig_out[g.i] = fabsf(vsig);
 }
 
-// ---------------------------------------------------------------- Cullen-Dehnen R pass + switch algebra
-template <int KF, int D>
+// ---------------------------------------------------------------- Cullen-Dehnen switch
+// R (CullenDehnen2010.py:121-164, gather interpolation of rho_j sgn(div_j) / rho_j * m_j),
+// v_sig over the Verlet set when not supplied (wp_vsig.py:55-90), Xi (:166-191) and the
+// alpha / alpha0 update (:281-314).
+template <int KF, int D, int G, int ST>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
          const float* __restrict__ rho, const float* __restrict__ div, const float* __restrict__ div_prev,
-         const float* __restrict__ vsig, const float* __restrict__ alpha0_prev, const float* __restrict__ dtp,
+         const float* __restrict__ vsig_in, const float* __restrict__ v, const float* __restrict__ c,
+         const float* __restrict__ alpha0_prev, const float* __restrict__ dtp,
          const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
-         float* __restrict__ alpha_out, float* __restrict__ R_out) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Vec<D> xi = load_vec<D>(x, i);
-    float Hi = H[i];
-    int b = offs[i], e = b + cnt[i];
-    float s = 0.f;
-    for (int k = b; k < e; ++k) {
-        int j = __ldg(list + k);
-        Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
-        float r = safe_sqrt(dot<D>(xij, xij));
-        float W = kernelW<KF, D>(r, Hi);   // gather
-        if (W == 0.f) continue;
-        float dj = __ldg(div + j);
-        float sg = dj > 0.f ? 1.f : (dj < 0.f ? -1.f : 0.f);
-        float rj = __ldg(rho + j);
-        s += __ldg(m + j) / rj * (rj * sg) * W;
+         float* __restrict__ alpha_out, float* __restrict__ R_out, float* __restrict__ vsig_out) {
+    Grp<G> g(n);
+    const bool want_vs = vsig_in == nullptr;
+    float s = 0.f, vsig = 0.f;
+    float Hi = 1.f;
+    if (g.valid) {
+        const int i = g.i;
+        Vec<D> xi = load_vec<D>(x, i);
+        Hi = H[i];
+        const float invHi = 1.f / Hi;
+        Vec<D> vi = want_vs ? load_vec<D>(v, i) : vzero<D>();
+        float ci = want_vs ? c[i] : 0.f;
+        int b = offs[i], e = b + cnt[i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry<ST>(list, q, j, k);
+            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float r = safe_sqrt(dot<D>(xij, xij));
+            float W = kW_inv<KF, D>(r, invHi);   // gather support
+            if (W != 0.f) {
+                float dj = __ldg(div + j);
+                float sg = dj > 0.f ? 1.f : (dj < 0.f ? -1.f : 0.f);
+                s += __ldg(m + j) * sg * W;
+            }
+            if (want_vs) {
+                float Hs = wmax(Hi, __ldg(H + j));
+                if (r < P.verlet_scale * Hs) {
+                    Vec<D> vj = load_vec<D>(v, j);
+                    float mu = 0.f;
+                    #pragma unroll
+                    for (int a = 0; a < D; ++a) mu += (vi.v[a] - vj.v[a]) * xij.v[a];
+                    mu = mu / (r + 1e-14f * Hi);
+                    float vsv = 0.5f * (ci + __ldg(c + j)) - mu;
+                    if (mu > 0.f) vsv = 0.f;
+                    vsig = wmax(vsig, vsv);
+                }
+            }
+        }
     }
+    s = gsum<G>(s);
+    if (want_vs) vsig = gmaxw<G>(vsig);
+    if (!g.valid || g.lane != 0) return;
+    const int i = g.i;
+    float vs = want_vs ? fabsf(vsig) : vsig_in[i];
+    if (want_vs && vsig_out) vsig_out[i] = vs;
     float rhoi = rho[i];
     float R = 1.f / rhoi * s;
     float dv = div[i];
     float dt = *dtp;
-    // CullenDehnen2010.py:183-191 (S = None -> trace 0)
     float omr = 1.f - R;
     float omr2 = omr * omr;
     float nom = P.beta_xi * (omr2 * omr2) * dv;
@@ -398,33 +499,29 @@ k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restric
                           : (nom * nom) / (nom * nom + 0.f + 1e-14f * Hi);
     float ddiv = (dv - div_prev[i]) / dt;
     float Ai = Xi * fmaxf(-ddiv, 0.f);
-    float vs = vsig[i];
     float scaling = Hi * Hi * Ai / (vs * vs + Hi * Hi * Ai + 1e-14f * Hi);
-    float alphas = P.alpha_max * scaling;
-    alphas = fminf(fmaxf(alphas, P.alpha_min), P.alpha_max);
+    float alphas = fminf(fmaxf(P.alpha_max * scaling, P.alpha_min), P.alpha_max);
     float a0 = alpha0_prev[i];
-    float fk = 1.f / P.kxi;
-    float tau = Hi * fk / (2.f * 0.05f * vs);
+    float tau = Hi * (1.f / P.kxi) / (2.f * 0.05f * vs);
     float adot = (alphas - a0) / tau;
     a0 = alphas > a0 ? alphas : a0;
     a0 = alphas < a0 ? a0 + adot * dt : a0;
-    a0 = fminf(fmaxf(a0, P.alpha_min), P.alpha_max);
-    alpha_out[i] = a0;
+    alpha_out[i] = fminf(fmaxf(a0, P.alpha_min), P.alpha_max);
     if (R_out) R_out[i] = R;
 }
 
-// Balsara switch from the velocity gradient.
+// Balsara switch from the velocity gradient (schemes/crkSPH.py:132-133 comment).
 template <int D>
 __global__ void k_balsara(int n, const float* __restrict__ DvDx, const float* __restrict__ c, float* __restrict__ alpha) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    Mat<D> G = load_mat<D>(DvDx, i);
-    float dv = G.m[0][0];
-    for (int a = 1; a < D; ++a) dv += G.m[a][a];
+    Mat<D> Gm = load_mat<D>(DvDx, i);
+    float dv = Gm.m[0][0];
+    for (int a = 1; a < D; ++a) dv += Gm.m[a][a];
     float curl2 = 0.f;
-    if constexpr (D == 2) { float w = G.m[1][0] - G.m[0][1]; curl2 = w * w; }
+    if constexpr (D == 2) { float w = Gm.m[1][0] - Gm.m[0][1]; curl2 = w * w; }
     if constexpr (D == 3) {
-        float w0 = G.m[2][1] - G.m[1][2], w1 = G.m[0][2] - G.m[2][0], w2 = G.m[1][0] - G.m[0][1];
+        float w0 = Gm.m[2][1] - Gm.m[1][2], w1 = Gm.m[0][2] - Gm.m[2][0], w2 = Gm.m[1][0] - Gm.m[0][1];
         curl2 = w0 * w0 + w1 * w1 + w2 * w2;
     }
     float ad = fabsf(dv);
@@ -455,19 +552,13 @@ __device__ __forceinline__ float van_leer(const Vec<D>& xij_, const Mat<D>& Gi, 
     if (rj != rj) rj = 1.f;
     return limiter_vl(wmin(ri, rj));
 }
-// modules/crk/limiter.py:89-128 (eta measured in supports H)
-template <int D>
-__device__ __forceinline__ float crk_limiter(const Vec<D>& xij, float hi, float hj, float eta_crit, float eta_fold) {
-    float ni = 0.f, nj = 0.f;
-    #pragma unroll
-    for (int a = 0; a < D; ++a) { float ei = xij.v[a] / hi, ej = xij.v[a] / hj; ni += ei * ei; nj += ej * ej; }
-    float eta = wmin(safe_sqrt(ni), safe_sqrt(nj));
-    float f = 1.f;
-    if (eta < eta_crit) { float t = (eta - eta_crit) / eta_fold; f = expf(-(t * t)); }
-    return f;
-}
 
-template <int KF, int D>
+// modules/crk/accel.py:65-250 and modules/crk/dudt.py:62-229 in one pass.  The
+// unused computePi_actual calls of the reference (accel.py:143-168, dudt.py:128-153)
+// have no effect on the outputs and are not evaluated.  With the interacting list
+// (stride 2) the ap_ij / av_ij entries of non-interacting Verlet pairs are not
+// written (the caller provides zero-filled arrays).
+template <int KF, int D, int G, int ST>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
                  const float* __restrict__ rho, const float* __restrict__ V, const float* __restrict__ A,
@@ -476,155 +567,184 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
                  const float* __restrict__ DvDx, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
                  const int32_t* __restrict__ list, float* __restrict__ dvdt, float* __restrict__ dudt,
                  float* __restrict__ ap, float* __restrict__ av) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
-    float Hi = H[i], mi = m[i], rhoi = rho[i], Vi = V[i], ci = c[i], Pi = Pr[i];
-    float Ai = A[i];
-    Vec<D> Bi = load_vec<D>(B, i), gAi = load_vec<D>(gA, i);
-    Mat<D> gBi = load_mat<D>(gB, i), Gi = load_mat<D>(DvDx, i);
-    const float ks = P.kscale;
-    const float smooth_i = Hi / ks;
+    Grp<G> g(n);
     const bool comp = P.kahan != 0;
     KSum acc[D], du;
     #pragma unroll
     for (int a = 0; a < D; ++a) acc[a].init();
     du.init();
-    int b = offs[i], e = b + cnt[i];
-    for (int k = b; k < e; ++k) {
-        int j = __ldg(list + k);
-        Vec<D> xj = load_vec<D>(x, j);
-        Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
-        float r2 = dot<D>(xij, xij);
-        float Hj = __ldg(H + j);
-        float Hm = wmax(Hi, Hj);
-        if (!(r2 < Hm * Hm)) {
-            if (ap) store_vec<D>(ap, k, vzero<D>());
-            if (av) store_vec<D>(av, k, vzero<D>());
-            continue;
+    if (g.valid) {
+        const int i = g.i;
+        Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
+        const float Hi = H[i], rhoi = rho[i], ci = c[i], Pi = Pr[i];
+        const float invHi = 1.f / Hi;
+        const float Vi_m = V[i] / m[i];          // V_i / m_i
+        const float Ai = A[i];
+        Vec<D> Bi = load_vec<D>(B, i), gAi = load_vec<D>(gA, i);
+        Mat<D> gBi = load_mat<D>(gB, i), Gi = load_mat<D>(DvDx, i);
+        const float ks = P.kscale;
+        const float inv_smooth_i = ks * invHi;   // 1 / (H_i / ks)
+        const float sm_i = Hi / ks;
+        const float eps_i = 1.0e-7f * sm_i * sm_i;
+        int b = offs[i], e = b + cnt[i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry<ST>(list, q, j, k);
+            Vec<D> xj = load_vec<D>(x, j);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
+            float r2 = dot<D>(xij, xij);
+            float Hj = __ldg(H + j);
+            float Hm = wmax(Hi, Hj);
+            if (!(r2 < Hm * Hm)) {
+                if (ST == 1) {
+                    if (ap) store_vec<D>(ap, k, vzero<D>());
+                    if (av) store_vec<D>(av, k, vzero<D>());
+                }
+                continue;
+            }
+            float r = safe_sqrt(r2);
+            const float invHj = 1.f / Hj;
+            Vec<D> vj = load_vec<D>(v, j);
+            float rhoj = __ldg(rho + j), Vj = __ldg(V + j), cj = __ldg(c + j), Pj = __ldg(Pr + j);
+            Mat<D> Gj = load_mat<D>(DvDx, j);
+            // CRK limiter (limiter.py:89-128), eta measured in supports
+            float factor = 1.f;
+            if (P.enable_crk_limiter) {
+                float eta = r * wmin(invHi, invHj);
+                if (eta < P.eta_crit) { float t = (eta - P.eta_crit) / P.eta_fold; factor = expf(-(t * t)); }
+            }
+            float phi = 0.f;
+            if (P.enable_vanleer) phi = van_leer<D>(xij, Gi, Gj) * factor;
+            if (P.force_vl_off) phi = 0.f;
+            if (P.force_vl_on) phi = 1.f;
+            phi = wmax(wmin(phi, 1.f), 0.f);
+            Vec<D> Gix = matvec<D>(Gi, xij), Gjx = matvec<D>(Gj, xij);
+            float hp = 0.5f * phi;
+            // v_dot_i - v_dot_j (accel.py:137-141; dudt.py:122-126 uses gradV_j . (-x_ij))
+            Vec<D> da, dd;
+            #pragma unroll
+            for (int a = 0; a < D; ++a) {
+                float vdi = vi.v[a] - hp * Gix.v[a];
+                da.v[a] = vdi - (vj.v[a] + hp * Gjx.v[a]);
+                dd.v[a] = vdi - (vj.v[a] - hp * Gjx.v[a]);
+            }
+            // corrected gradients (accel.py:170-187, dudt.py:155-170)
+            float Wi; Vec<D> gWi;
+            kWG_inv<KF, D>(xij, r, invHj, Wi, gWi);
+            Vec<D> gradw_i = crk_grad<D>(xij, Wi, gWi, Ai, Bi, gAi, gBi);
+            float Aj = __ldg(A + j);
+            Vec<D> Bj = load_vec<D>(B, j), gAj = load_vec<D>(gA, j);
+            Mat<D> gBj = load_mat<D>(gB, j);
+            Vec<D> xji;
+            #pragma unroll
+            for (int a = 0; a < D; ++a) xji.v[a] = -xij.v[a];
+            float Wj; Vec<D> gWj;
+            kWG_inv<KF, D>(xji, r, invHi, Wj, gWj);
+            Vec<D> gradw_j = crk_grad<D>(xji, Wj, gWj, Aj, Bj, gAj, gBj);
+            Vec<D> gij;
+            #pragma unroll
+            for (int a = 0; a < D; ++a) gij.v[a] = 0.5f * (gradw_i.v[a] - gradw_j.v[a]);
+            // mu_ij, mu_ji and Q (accel.py:189-206): eta = x_ij / smoothing length
+            const float inv_smooth_j = ks * invHj;
+            const float sm_j = Hj / ks;
+            const float eps_j = 1.0e-7f * sm_j * sm_j;
+            float den_i = r2 * (inv_smooth_i * inv_smooth_i) + eps_i;
+            float den_j = r2 * (inv_smooth_j * inv_smooth_j) + eps_j;
+            float xa = dot<D>(da, xij), xd = dot<D>(dd, xij);
+            float idi = inv_smooth_i / den_i, idj = inv_smooth_j / den_j;
+            float mia = wmin(0.f, xa * idi), mja = wmin(0.f, xa * idj);
+            float mid = wmin(0.f, xd * idi), mjd = wmin(0.f, xd * idj);
+            float Qa = rhoi * (-P.C_l * ci * mia + P.C_q * mia * mia) + rhoj * (-P.C_l * cj * mja + P.C_q * mja * mja);
+            float Qd = rhoi * (-P.C_l * ci * mid + P.C_q * mid * mid) + rhoj * (-P.C_l * cj * mjd + P.C_q * mjd * mjd);
+            // accel.py:228-249 (mu_ij = 1 there)
+            const float w = Vj * Vi_m;   // V_i V_j / m_i
+            Vec<D> pt, vt;
+            float dotu = 0.f;
+            #pragma unroll
+            for (int a = 0; a < D; ++a) {
+                pt.v[a] = -(Pi + Pj) * gij.v[a] * w;
+                vt.v[a] = -Qa * gij.v[a] * w;
+                acc[a].add(pt.v[a] + vt.v[a], comp);
+                dotu += (vi.v[a] - vj.v[a]) * gij.v[a];
+            }
+            if (ap) store_vec<D>(ap, k, pt);
+            if (av) store_vec<D>(av, k, vt);
+            // dudt.py:208-226
+            du.add((Pj + 0.5f * Qd) * dotu * w, comp);
         }
-        float r = safe_sqrt(r2);
-        Vec<D> vj = load_vec<D>(v, j);
-        float rhoj = __ldg(rho + j), Vj = __ldg(V + j), cj = __ldg(c + j), Pj = __ldg(Pr + j);
-        Mat<D> Gj = load_mat<D>(DvDx, j);
-        // limiters
-        float factor = 1.f;
-        if (P.enable_crk_limiter) factor = crk_limiter<D>(xij, Hi, Hj, P.eta_crit, P.eta_fold);
-        float phi = 0.f;
-        if (P.enable_vanleer) phi = van_leer<D>(xij, Gi, Gj) * factor;
-        if (P.force_vl_off) phi = 0.f;
-        if (P.force_vl_on) phi = 1.f;
-        phi = wmax(wmin(phi, 1.f), 0.f);
-        Vec<D> Gix = matvec<D>(Gi, xij), Gjx = matvec<D>(Gj, xij);
-        float hp = phi / 2.f;
-        Vec<D> vdi, vdj_a, vdj_d;
-        #pragma unroll
-        for (int a = 0; a < D; ++a) {
-            vdi.v[a] = vi.v[a] - hp * Gix.v[a];
-            vdj_a.v[a] = vj.v[a] + hp * Gjx.v[a];        // accel.py:138
-            vdj_d.v[a] = vj.v[a] + hp * (-Gjx.v[a]);     // dudt.py:123 (matmul(gradV_j, -x_ij))
-        }
-        // corrected gradients
-        float Wi; Vec<D> gWi;
-        kernelWG<KF, D>(xij, r, Hj, Wi, gWi);
-        Vec<D> gradw_i = crk_grad<D>(xij, Wi, gWi, Ai, Bi, gAi, gBi);
-        float Aj = __ldg(A + j);
-        Vec<D> Bj = load_vec<D>(B, j), gAj = load_vec<D>(gA, j);
-        Mat<D> gBj = load_mat<D>(gB, j);
-        Vec<D> xji;
-        #pragma unroll
-        for (int a = 0; a < D; ++a) xji.v[a] = -xij.v[a];
-        float Wj; Vec<D> gWj;
-        kernelWG<KF, D>(xji, r, Hi, Wj, gWj);
-        Vec<D> gradw_j = crk_grad<D>(xji, Wj, gWj, Aj, Bj, gAj, gBj);
-        Vec<D> gij;
-        #pragma unroll
-        for (int a = 0; a < D; ++a) gij.v[a] = 0.5f * (gradw_i.v[a] - gradw_j.v[a]);
-        // viscous Q (accel.py:189-206 / dudt.py:174-191)
-        float smooth_j = Hj / ks;
-        float ee_i = 0.f, ee_j = 0.f, mi_a = 0.f, mj_a = 0.f, mi_d = 0.f, mj_d = 0.f;
-        #pragma unroll
-        for (int a = 0; a < D; ++a) {
-            float ei = xij.v[a] / smooth_i, ej = xij.v[a] / smooth_j;
-            ee_i += ei * ei; ee_j += ej * ej;
-            float da = vdi.v[a] - vdj_a.v[a], dd = vdi.v[a] - vdj_d.v[a];
-            mi_a += da * ei; mj_a += da * ej;
-            mi_d += dd * ei; mj_d += dd * ej;
-        }
-        float den_i = ee_i + 1.0e-7f * smooth_i * smooth_i, den_j = ee_j + 1.0e-7f * smooth_j * smooth_j;
-        mi_a = wmin(0.f, mi_a / den_i); mj_a = wmin(0.f, mj_a / den_j);
-        mi_d = wmin(0.f, mi_d / den_i); mj_d = wmin(0.f, mj_d / den_j);
-        float Qi_a = rhoi * (-P.C_l * ci * mi_a + P.C_q * mi_a * mi_a);
-        float Qj_a = rhoj * (-P.C_l * cj * mj_a + P.C_q * mj_a * mj_a);
-        float Qi_d = rhoi * (-P.C_l * ci * mi_d + P.C_q * mi_d * mi_d);
-        float Qj_d = rhoj * (-P.C_l * cj * mj_d + P.C_q * mj_d * mj_d);
-        // accel.py:228-249
-        Vec<D> pt, vt;
-        #pragma unroll
-        for (int a = 0; a < D; ++a) {
-            pt.v[a] = -(Pi + Pj) * gij.v[a] * Vi * Vj / mi;
-            vt.v[a] = -(Qi_a + Qj_a) * Vj * 1.f * gij.v[a] * Vi / mi;
-            acc[a].add(pt.v[a] + vt.v[a], comp);
-        }
-        if (ap) store_vec<D>(ap, k, pt);
-        if (av) store_vec<D>(av, k, vt);
-        // dudt.py:208-226
-        float dotu = 0.f;
-        #pragma unroll
-        for (int a = 0; a < D; ++a) dotu += (vi.v[a] - vj.v[a]) * gij.v[a];
-        float pTerm = Pj * dotu * Vi * Vj / mi;
-        float vTerm = 0.5f * (Qi_d + Qj_d) * 1.f * dotu * Vi * Vj / mi;
-        du.add(pTerm + vTerm, comp);
     }
+    float o[D], od;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) o[a] = gsum<G>(acc[a].s) + gsum<G>(acc[a].c);
+    od = gsum<G>(du.s) + gsum<G>(du.c);
+    if (!g.valid || g.lane != 0) return;
     if (dvdt) {
-        Vec<D> o;
+        Vec<D> ov;
         #pragma unroll
-        for (int a = 0; a < D; ++a) o.v[a] = acc[a].value();
-        store_vec<D>(dvdt, i, o);
+        for (int a = 0; a < D; ++a) ov.v[a] = o[a];
+        store_vec<D>(dvdt, g.i, ov);
     }
-    if (dudt) dudt[i] = du.value();
+    if (dudt) dudt[g.i] = od;
 }
 
-// ---------------------------------------------------------------- energy partition f_ij
+// ---------------------------------------------------------------- energy partition f_ij (modules/compSPH/balance.py:62-154)
 __device__ __forceinline__ float sgn0(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
 
+// Per-particle prologue: half-step velocity v + dt/2 dv/dt (schemes/crkSPH.py:341) and
+// the CRK entropy P / rho^gamma (balance.py:126-127).
 template <int D>
-__global__ void __launch_bounds__(PAIR_BLOCK)
-k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restrict__ rho, const float* __restrict__ Pr,
-          const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ dvdt, const float* __restrict__ dtp,
-          const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
-          const float* __restrict__ ap, const float* __restrict__ av, float* __restrict__ fout) {
+__global__ void k_balance_prep(int n, DevParams P, const float* __restrict__ rho, const float* __restrict__ Pr,
+                               const float* __restrict__ v, const float* __restrict__ dvdt, const float* __restrict__ dtp,
+                               float* __restrict__ vh, float* __restrict__ sarr) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    float dt = *dtp;
-    float hdt = 0.5f * dt;
+    float hdt = 0.5f * (*dtp);
     Vec<D> vi = load_vec<D>(v, i), ai = load_vec<D>(dvdt, i);
     #pragma unroll
     for (int a = 0; a < D; ++a) vi.v[a] = vi.v[a] + hdt * ai.v[a];
-    float mi = m[i], rhoi = rho[i], Pi = Pr[i], ui = u[i];
+    store_vec<D>(vh, i, vi);
+    sarr[i] = Pr[i] / powf(rho[i], P.gamma);
+}
+
+template <int D, int G, int ST>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restrict__ rho, const float* __restrict__ Pr,
+          const float* __restrict__ u, const float* __restrict__ vh, const float* __restrict__ sarr, const float* __restrict__ dtp,
+          const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+          const float* __restrict__ ap, const float* __restrict__ av, float* __restrict__ fout) {
+    Grp<G> g(n);
+    if (!g.valid) return;
+    const int i = g.i;
+    const float dt = *dtp;
+    Vec<D> vi = load_vec<D>(vh, i);
+    const float mi = m[i], rhoi = rho[i], Pi = Pr[i], ui = u[i], si = sarr[i];
     const int scheme = P.energy_scheme;
-    float si = 0.f;
-    if (scheme == SPH_ENERGY_CRK) si = Pi / powf(rhoi, P.gamma);
     int b = offs[i], e = b + cnt[i];
-    for (int k = b; k < e; ++k) {
-        int j = __ldg(list + k);
-        Vec<D> vj = load_vec<D>(v, j), aj = load_vec<D>(dvdt, j);
+    for (int q = b + g.lane; q < e; q += G) {
+        int j, k; entry<ST>(list, q, j, k);
+        Vec<D> vj = load_vec<D>(vh, j);
         Vec<D> apk = load_vec<D>(ap, k), avk = load_vec<D>(av, k);
-        float mj = __ldg(m + j), rhoj = __ldg(rho + j), Pj = __ldg(Pr + j), uj = __ldg(u + j);
         float dE = 0.f;
         #pragma unroll
-        for (int a = 0; a < D; ++a) dE += ((vj.v[a] + hdt * aj.v[a]) - vi.v[a]) * (apk.v[a] + avk.v[a]);
+        for (int a = 0; a < D; ++a) dE += (vj.v[a] - vi.v[a]) * (apk.v[a] + avk.v[a]);
         dE = mi * dE * dt;
-        float uji = uj - ui;
         float f = 0.5f;
-        if (scheme == SPH_ENERGY_EQUALWORK) {
-            f = 0.5f;
+        if (scheme == SPH_ENERGY_CRK) {
+            float sj = __ldg(sarr + j);
+            float smin = wmin(fabsf(si), fabsf(sj)), smax = wmax(fabsf(si), fabsf(sj));
+            bool mA = fabsf(si - sj) == 0.f;
+            bool mB = (dE >= 0.f && si >= sj) || (dE < 0.f && si < sj);
+            bool mC = (dE >= 0.f && si < sj) || (dE < 0.f && si >= sj);
+            if (!mA && mB) f = smin / (smin + smax + 1.0e-14f);
+            if (!mA && !mB && mC) f = smax / (smin + smax + 1.0e-14f);
+            f = wmax(0.f, wmin(1.f, f));
         } else if (scheme == SPH_ENERGY_PDV) {
+            float rhoj = __ldg(rho + j), Pj = __ldg(Pr + j);
             f = (Pi / (rhoi * rhoi)) / (Pi / (rhoi * rhoi) + Pj / (rhoj * rhoj));
         } else if (scheme == SPH_ENERGY_DIMINISHING) {
-            float un = fabsf(uji);
+            float uji = __ldg(u + j) - ui, un = fabsf(uji);
             f = 0.5f * (1.f + (uji * sgn0(dE)) / (un + 1.f / (1.f + un)));
         } else if (scheme == SPH_ENERGY_MONOTONIC || scheme == SPH_ENERGY_HYBRID) {
+            float mj = __ldg(m + j), uj = __ldg(u + j), uji = uj - ui;
             float Aq = dE / (uji + 1.0e-14f);
             float Bq = Aq >= 0.f ? Aq / mi : Aq / mj;
             float t1 = wmax(0.f, sgn0(Bq));
@@ -637,23 +757,12 @@ k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restri
                 float chi = fabsf(uji) / (fabsf(ui) + fabsf(uj) + 1.0e-14f);
                 f = chi * fm + (1.f - chi) * fsm;
             }
-        } else if (scheme == SPH_ENERGY_CRK) {
-            float sj = Pj / powf(rhoj, P.gamma);
-            float smin = wmin(fabsf(si), fabsf(sj)), smax = wmax(fabsf(si), fabsf(sj));
-            bool mA = fabsf(si - sj) == 0.f;
-            bool mB = (dE >= 0.f && si >= sj) || (dE < 0.f && si < sj);
-            bool mC = (dE >= 0.f && si < sj) || (dE < 0.f && si >= sj);
-            f = 0.5f;
-            if (mA) f = 0.5f;
-            if (!mA && mB) f = smin / (smin + smax + 1.0e-14f);
-            if (!mA && !mB && mC) f = smax / (smin + smax + 1.0e-14f);
-            f = wmax(0.f, wmin(1.f, f));
         }
         fout[k] = f;
     }
 }
 
-// ---------------------------------------------------------------- CFL dt
+// ---------------------------------------------------------------- CFL dt (modules/timestep/compressible.py:18-61)
 __global__ void k_cfl_reduce(int n, float gamma, const float* __restrict__ H, const float* __restrict__ u,
                              float* __restrict__ red /* [0]=min H, [1]=max c */) {
     float hmin = __int_as_float(0x7f800000), cmax = 0.f;
@@ -673,7 +782,7 @@ __global__ void k_cfl_reduce(int n, float gamma, const float* __restrict__ H, co
 }
 __global__ void k_cfl_init(float* red) { red[0] = __int_as_float(0x7f800000); red[1] = 0.f; }
 __global__ void k_cfl_final(DevParams P, const float* __restrict__ red, const float* __restrict__ dt_prev, float* __restrict__ dt_out) {
-    // compressible.py:49-61 ; min_i cfl*h/(c_i*xi) is attained at max_i c_i
+    // min_i cfl*h/(c_i*xi) is attained at max_i c_i (the map c -> cfl*h/(c*xi) is monotone)
     float dt = P.cfl * red[0] / (red[1] * P.kxi);
     dt = fminf(fmaxf(dt, P.min_dt), P.max_dt);
     if (dt_prev) {
@@ -705,6 +814,7 @@ __global__ void k_rk_combine(int64_t count, const float* __restrict__ y0, int nk
 }
 
 // ---------------------------------------------------------------- compatible energy
+// modules/compSPH/multistep.py:52-94 and systems/compSPH.py:100-111
 struct StagePtrs {
     const float* dvdt[8];
     const int32_t* offs[8];
@@ -727,41 +837,43 @@ __global__ void k_vhalf(int n, int ns, StagePtrs S, const float* __restrict__ dt
         vh[(size_t)i * D + a] = v0[(size_t)i * D + a] + 0.5f * fa * dt;
     }
 }
-template <int D>
+template <int D, int G, int ST>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_finalize(int n, int ns, StagePtrs S, int pdv, const float* __restrict__ dtp, const float* __restrict__ vh,
            const float* __restrict__ u0, float* __restrict__ u_out, float* __restrict__ du_out) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Vec<D> vi = load_vec<D>(vh, i);
+    Grp<G> g(n);
     float du = 0.f;
-    for (int s = 0; s < ns; ++s) {
-        const int32_t* __restrict__ lst = S.list[s];
-        const float* __restrict__ f = S.f[s];
-        const float* __restrict__ ap = S.ap[s];
-        const float* __restrict__ av = S.av[s];
-        int b = S.offs[s][i], e = b + S.cnt[s][i];
-        float w = S.w[s];
-        float acc = 0.f;
-        for (int k = b; k < e; ++k) {
-            int j = __ldg(lst + k);
-            Vec<D> vj = load_vec<D>(vh, j);
-            Vec<D> a1 = load_vec<D>(ap, k), a2 = load_vec<D>(av, k);
-            float fk = __ldg(f + k);
-            float d1 = 0.f, d2 = 0.f;
-            #pragma unroll
-            for (int a = 0; a < D; ++a) { float vji = vj.v[a] - vi.v[a]; d1 += vji * a1.v[a]; d2 += vji * a2.v[a]; }
-            float term = pdv ? (w * fk * d1 + w * 0.5f * d2) : (w * fk * (d1 + d2));
-            acc += term;
+    if (g.valid) {
+        Vec<D> vi = load_vec<D>(vh, g.i);
+        for (int s = 0; s < ns; ++s) {
+            const int32_t* __restrict__ lst = S.list[s];
+            const float* __restrict__ f = S.f[s];
+            const float* __restrict__ ap = S.ap[s];
+            const float* __restrict__ av = S.av[s];
+            const float w = S.w[s];
+            int b = S.offs[s][g.i], e = b + S.cnt[s][g.i];
+            float acc = 0.f;
+            for (int q = b + g.lane; q < e; q += G) {
+                int j, k; entry<ST>(lst, q, j, k);
+                Vec<D> vj = load_vec<D>(vh, j);
+                Vec<D> a1 = load_vec<D>(ap, k), a2 = load_vec<D>(av, k);
+                float fk = __ldg(f + k);
+                float d1 = 0.f, d2 = 0.f;
+                #pragma unroll
+                for (int a = 0; a < D; ++a) { float vji = vj.v[a] - vi.v[a]; d1 += vji * a1.v[a]; d2 += vji * a2.v[a]; }
+                acc += pdv ? (w * fk * d1 + w * 0.5f * d2) : (w * fk * (d1 + d2));
+            }
+            du += acc;
         }
-        du += acc;
     }
+    du = gsum<G>(du);
+    if (!g.valid || g.lane != 0) return;
     float dt = *dtp;
-    if (du_out) du_out[i] = du;
-    u_out[i] = u0[i] + du * dt;
+    if (du_out) du_out[g.i] = du;
+    u_out[g.i] = u0[g.i] + du * dt;
 }
 
-// ---------------------------------------------------------------- conservation
+// ---------------------------------------------------------------- conservation sums (FP64)
 template <int D>
 __global__ void k_cons(int n, const float* __restrict__ m, const float* __restrict__ v, const float* __restrict__ u, double* out) {
     double M = 0, KE = 0, IE = 0, p[3] = {0, 0, 0};
@@ -786,16 +898,30 @@ __global__ void k_cons(int n, const float* __restrict__ m, const float* __restri
 
 using namespace wsph;
 
+// group sizes (lanes per particle) of the pair passes
+#define G_LIGHT 8
+#define G_HEAVY 8
+#define G_CRK 4
+
+#define WSPH_DISPATCH_KDS(params, ...)                                                    \
+    if ((params).list_stride == 2) { constexpr int ST = 2; WSPH_DISPATCH_KD(P.kernel, P.dim, __VA_ARGS__) } \
+    else { constexpr int ST = 1; WSPH_DISPATCH_KD(P.kernel, P.dim, __VA_ARGS__) }
+#define WSPH_DISPATCH_DS(params, ...)                                                     \
+    if ((params).list_stride == 2) { constexpr int ST = 2; WSPH_DISPATCH_DIM(P.dim, __VA_ARGS__) } \
+    else { constexpr int ST = 1; WSPH_DISPATCH_DIM(P.dim, __VA_ARGS__) }
+
 #define PAIR_PRELUDE()                                                        \
     DevParams P;                                                              \
     int rc = params_to_dev(p, &P);                                            \
     if (rc) return rc;                                                        \
-    if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "%s: n out of range", __func__); \
+    if (n < 0 || n > 0x3fffffff) return set_error(SPH_ERR_BAD_ARG, "%s: n out of range", __func__); \
+    if (p->list_stride < 0 || p->list_stride > 2) return set_error(SPH_ERR_BAD_ARG, "%s: list_stride must be 1 or 2", __func__); \
     if (n == 0) return SPH_OK;                                                \
     cudaStream_t s = WSPH_STREAM(stream);                                     \
     (void)s;
 
-#define CHECK_CSR() do { WSPH_CHECK_PTR(offs); WSPH_CHECK_PTR(cnt); WSPH_CHECK_PTR(list); } while (0)
+#define CHECK_CSR() do { WSPH_CHECK_PTR(offs); WSPH_CHECK_PTR(cnt); WSPH_CHECK_PTR(list); \
+    if (p->list_stride == 2 && (reinterpret_cast<uintptr_t>(list) & 7)) return set_error(SPH_ERR_BAD_ARG, "%s: interacting list must be 8-byte aligned", __func__); } while (0)
 
 static int check_align_vec(const DevParams& P, const void* ptr, const char* name) {
     if (P.dim == 2 && ptr && (reinterpret_cast<uintptr_t>(ptr) & 7))
@@ -811,7 +937,8 @@ int sph_density_gather(const SphParams* p, int64_t n, int32_t support_mode, cons
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho_out); CHECK_CSR();
     if (support_mode < 0 || support_mode > 4) return set_error(SPH_ERR_BAD_ARG, "bad support mode %d", support_mode);
     if ((rc = check_align_vec(P, x, "x"))) return rc;
-    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_density<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, support_mode, P, x, H, m, offs, cnt, list, rho_out)));
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_density<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, support_mode, P, x, H, m, offs, cnt, list, rho_out)));
     return check_launch("sph_density_gather");
 }
 
@@ -822,7 +949,8 @@ int sph_adaptive_h_iter(const SphParams* p, int64_t n, int32_t support_mode, con
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(hbounds); WSPH_CHECK_PTR(rho_out); WSPH_CHECK_PTR(H_out); CHECK_CSR();
     if (support_mode != SPH_SUPPORT_GATHER) return set_error(SPH_ERR_UNSUPPORTED, "adaptive support: only the gather scheme is implemented");
     if ((rc = check_align_vec(P, x, "x"))) return rc;
-    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_adaptive_h<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, offs, cnt, list, hbounds, rho_out, H_out, ratio_out)));
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_adaptive_h<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, offs, cnt, list, hbounds, rho_out, H_out, ratio_out)));
     return check_launch("sph_adaptive_h_iter");
 }
 
@@ -831,7 +959,8 @@ int sph_crk_volume(const SphParams* p, int64_t n, const float* x, const float* H
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(V_out); CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x"))) return rc;
-    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_crk_volume<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, offs, cnt, list, V_out)));
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_crk_volume<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, offs, cnt, list, V_out)));
     return check_launch("sph_crk_volume");
 }
 
@@ -842,7 +971,8 @@ int sph_crk_factors(const SphParams* p, int64_t n, const float* x, const float* 
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(V);
     WSPH_CHECK_PTR(A); WSPH_CHECK_PTR(B); WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x"))) return rc;
-    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_crk_factors<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out)));
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_crk_factors<KF, D, G_CRK, ST><<<grid_g<G_CRK>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out)));
     return check_launch("sph_crk_factors");
 }
 
@@ -861,25 +991,32 @@ int sph_grad_v(const SphParams* p, int64_t n, const float* x, const float* H, co
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(V); WSPH_CHECK_PTR(A); WSPH_CHECK_PTR(B);
     WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(DvDx_out); CHECK_CSR();
-    if (div_out) { WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(c); }
+    if (div_out) WSPH_CHECK_PTR(m);
+    if (vsig_out) WSPH_CHECK_PTR(c);
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v")) || (rc = check_align_vec(P, B, "B")) ||
         (rc = check_align_vec(P, gradA, "gradA")))
         return rc;
-    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_grad_v<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_grad_v<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
                                                                                                   offs, cnt, list, DvDx_out, drhodt_out, div_out, vsig_out)));
     return check_launch("sph_grad_v");
 }
 
 int sph_switch_cullen(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
-                      const float* div, const float* div_prev, const float* vsig, const float* alpha0_prev, const float* dt,
-                      const int32_t* offs, const int32_t* cnt, const int32_t* list, float* alpha_out, float* R_out,
-                      void* stream) {
+                      const float* div, const float* div_prev, const float* vsig, const float* v, const float* c,
+                      const float* alpha0_prev, const float* dt, const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                      float* alpha_out, float* R_out, float* vsig_out, void* stream) {
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(div); WSPH_CHECK_PTR(div_prev);
-    WSPH_CHECK_PTR(vsig); WSPH_CHECK_PTR(alpha0_prev); WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(alpha_out); CHECK_CSR();
-    if ((rc = check_align_vec(P, x, "x"))) return rc;
-    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_cullen<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div, div_prev, vsig, alpha0_prev, dt,
-                                                                                                  offs, cnt, list, alpha_out, R_out)));
+    WSPH_CHECK_PTR(alpha0_prev); WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(alpha_out); CHECK_CSR();
+    if (!vsig) {
+        WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(c);
+        if (p->list_stride == 2) return set_error(SPH_ERR_BAD_ARG, "sph_switch_cullen: computing v_sig needs the Verlet list (stride 1)");
+    }
+    if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v"))) return rc;
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_cullen<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div, div_prev, vsig, v, c,
+                                                                                                  alpha0_prev, dt, offs, cnt, list, alpha_out, R_out, vsig_out)));
     return check_launch("sph_switch_cullen");
 }
 
@@ -903,7 +1040,8 @@ int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const floa
         (rc = check_align_vec(P, gradA, "gradA")) || (rc = check_align_vec(P, dvdt_out, "dvdt")) ||
         (rc = check_align_vec(P, ap_ij, "ap_ij")) || (rc = check_align_vec(P, av_ij, "av_ij")))
         return rc;
-    wsph::count_launch(); WSPH_DISPATCH_KD(P.kernel, P.dim, (k_crk_accel_dudt<KF, D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_crk_accel_dudt<KF, D, G_HEAVY, ST><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
                                                                                                           Pr, DvDx, offs, cnt, list, dvdt_out, dudt_out, ap_ij, av_ij)));
     return check_launch("sph_crk_accel_dudt");
 }
@@ -926,15 +1064,20 @@ int sph_crk_dudt(const SphParams* p, int64_t n, const float* x, const float* H, 
 
 int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const float* rho, const float* Pr, const float* u,
                         const float* v, const float* dvdt, const float* dt, const int32_t* offs, const int32_t* cnt,
-                        const int32_t* list, const float* ap_ij, const float* av_ij, float* f_ij_out, void* stream) {
+                        const int32_t* list, const float* ap_ij, const float* av_ij, float* scratch, float* f_ij_out,
+                        void* stream) {
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(Pr); WSPH_CHECK_PTR(u); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(dvdt);
-    WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(ap_ij); WSPH_CHECK_PTR(av_ij); WSPH_CHECK_PTR(f_ij_out); CHECK_CSR();
+    WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(ap_ij); WSPH_CHECK_PTR(av_ij); WSPH_CHECK_PTR(scratch); WSPH_CHECK_PTR(f_ij_out); CHECK_CSR();
     if (P.energy_scheme < 0 || P.energy_scheme > 5) return set_error(SPH_ERR_BAD_ARG, "bad energy scheme %d", P.energy_scheme);
     if ((rc = check_align_vec(P, v, "v")) || (rc = check_align_vec(P, dvdt, "dvdt")) || (rc = check_align_vec(P, ap_ij, "ap_ij")) ||
-        (rc = check_align_vec(P, av_ij, "av_ij")))
+        (rc = check_align_vec(P, av_ij, "av_ij")) || (rc = check_align_vec(P, scratch, "scratch")))
         return rc;
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_balance<D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, P, m, rho, Pr, u, v, dvdt, dt, offs, cnt, list, ap_ij, av_ij, f_ij_out)));
+    float* vh = scratch;
+    float* sarr = scratch + n * P.dim;
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_balance_prep<D><<<grid_for(n, 256), 256, 0, s>>>((int)n, P, rho, Pr, v, dvdt, dt, vh, sarr)));
+    wsph::count_launch();
+    WSPH_DISPATCH_DS(*p, (k_balance<D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, m, rho, Pr, u, vh, sarr, dt, offs, cnt, list, ap_ij, av_ij, f_ij_out)));
     return check_launch("sph_compsph_balance");
 }
 
@@ -947,8 +1090,6 @@ int sph_cfl_dt(const SphParams* p, int64_t n, const float* H, const float* u, co
     WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(u); WSPH_CHECK_PTR(dt_out);
     (void)rho;
     cudaStream_t s = WSPH_STREAM(stream);
-    // dt_out doubles as the reduction scratch: [dt, hmin, cmax] need 3 floats -> use a static per-call layout
-    // in the caller's dt_out buffer (must hold 4 floats).
     float* red = dt_out + 1;
     wsph::count_launch(); k_cfl_init<<<1, 1, 0, s>>>(red);
     int blocks = grid_for(n, 256);
@@ -991,15 +1132,17 @@ int sph_finalize_compatible_energy(const SphParams* p, int64_t n, int32_t nstage
     for (int q = 0; q < nstages; ++q) {
         if (!dvdt_s[q] || !offs_s[q] || !cnt_s[q] || !list_s[q] || !f_ij_s[q] || !ap_ij_s[q] || !av_ij_s[q])
             return set_error(SPH_ERR_BAD_ARG, "finalize: null array for stage %d", q);
+        if (p->list_stride == 2 && (reinterpret_cast<uintptr_t>(list_s[q]) & 7))
+            return set_error(SPH_ERR_BAD_ARG, "finalize: interacting list of stage %d must be 8-byte aligned", q);
         S.dvdt[q] = dvdt_s[q]; S.offs[q] = offs_s[q]; S.cnt[q] = cnt_s[q]; S.list[q] = list_s[q];
         S.f[q] = f_ij_s[q]; S.ap[q] = ap_ij_s[q]; S.av[q] = av_ij_s[q]; S.w[q] = (float)weights[q];
     }
-    // the half-step velocity goes into du_out's companion scratch: caller passes du_out with room for n*(1+dim) floats
     if (!du_out) return set_error(SPH_ERR_BAD_ARG, "finalize: du_out must hold n*(1+dim) floats (du and v_half scratch)");
     float* vh = du_out + n;
     int pdv = P.energy_scheme == SPH_ENERGY_PDV;
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_vhalf<D><<<grid_for(n, 256), 256, 0, s>>>((int)n, nstages, S, dt, v0, vh)));
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_finalize<D><<<grid_for(n, PAIR_BLOCK), PAIR_BLOCK, 0, s>>>((int)n, nstages, S, pdv, dt, vh, u0, u_out, du_out)));
+    wsph::count_launch();
+    WSPH_DISPATCH_DS(*p, (k_finalize<D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, nstages, S, pdv, dt, vh, u0, u_out, du_out)));
     return check_launch("sph_finalize_compatible_energy");
 }
 

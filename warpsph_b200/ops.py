@@ -154,22 +154,28 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
     cb = torch.empty(cap, dtype=torch.int32, device=dev)
     ce = torch.empty(cap, dtype=torch.int32, device=dev)
     grid = torch.empty(8, dtype=torch.int32, device=dev)
-    flags = torch.zeros(2, dtype=torch.int64, device=dev)   # [nnz, status(int32 in the low half)]
-    list_cap = _nb_cache.cap_hint.get((dev.index, n, dim), max(n * 64, 1024))
+    ioffs = torch.empty(n, dtype=torch.int32, device=dev)
+    icnt = torch.empty(n, dtype=torch.int32, device=dev)
+    flags = torch.zeros(3, dtype=torch.int64, device=dev)   # [nnz, status (int32 in the low half), interacting nnz]
+    hint = _nb_cache.cap_hint.get((dev.index, n, dim))
+    list_cap = hint if hint is not None else max(n * 64, 1024)
     for attempt in range(2):
         lst = torch.empty(max(list_cap, 1), dtype=torch.int32, device=dev)
+        ilst = torch.empty(2 * max(list_cap, 1), dtype=torch.int32, device=dev)
+        inter_cap = list_cap
         flags.zero_()
         with _timed("neighbors_build"):
             rc = L.sph_neighbors_build(_p(params), n, ptr(x), ptr(H), ptr(ws), wsb.value, cap, ptr(si), ptr(sk), ptr(cb), ptr(ce),
-                                       ptr(grid), ptr(offs), ptr(cnt), ptr(lst), list_cap, flags.data_ptr(), flags.data_ptr() + 8,
-                                       stream_ptr(dev))
+                                       ptr(grid), ptr(offs), ptr(cnt), ptr(lst), list_cap, flags.data_ptr(),
+                                       ptr(ioffs), ptr(icnt), ptr(ilst), inter_cap, flags.data_ptr() + 16,
+                                       flags.data_ptr() + 8, stream_ptr(dev))
         check(rc, "sph_neighbors_build")
         f = flags.cpu()
-        nnz, status = int(f[0]), int(f[1]) & 0xffffffff
+        nnz, status, innz = int(f[0]), int(f[1]) & 0xffffffff, int(f[2])
         if status & _capi.STATUS_NONFINITE:
             raise RuntimeError("buildVerletList: supports must be finite and positive")
         if status & _capi.STATUS_LIST_OVERFLOW:
-            list_cap = int(nnz * 1.15) + 1024
+            list_cap = max(list_cap, int(nnz * 1.15) + 1024)
             continue
         break
     else:  # pragma: no cover
@@ -177,7 +183,8 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
     _nb_cache.cap_hint[(dev.index, n, dim)] = int(nnz * 1.15) + 1024
     adj = AdjacencyList(neighborOffsets=offs, numNeighbors=cnt, neighborList=lst[:nnz], numRows=n, numCols=n, nnz=nnz,
                         sortIndex=si if keep_sort else None, sortedKeys=sk if keep_sort else None, grid=grid,
-                        queryPositions=x, querySupports=H, verletScale=float(verletScale))
+                        queryPositions=x, querySupports=H, verletScale=float(verletScale),
+                        interOffsets=ioffs, interCounts=icnt, interList=ilst[:2 * nnz], interNnz=innz)
     adj._x_version = _version(x)
     adj._h_version = _version(H)
     return adj
@@ -197,12 +204,22 @@ def _csr(adj: AdjacencyList):
     return iptr(adj.neighborOffsets), iptr(adj.numNeighbors), iptr(adj.neighborList)
 
 
+def _lists(params, adj: AdjacencyList, interacting: bool):
+    """Selects the row lists a pass walks: the interacting subset (r < max(H_i, H_j),
+    stride 2) when available and sufficient, else the Verlet list (stride 1)."""
+    if interacting and adj.interList is not None:
+        params.list_stride = 2
+        return iptr(adj.interOffsets), iptr(adj.interCounts), iptr(adj.interList)
+    params.list_stride = 1
+    return _csr(adj)
+
+
 # ------------------------------------------------------------------ pair operations
 def density(params, x, H, m, adj: AdjacencyList, supportMode: SupportScheme = SupportScheme.Gather) -> torch.Tensor:
     n = H.shape[0]
     rho = _empty(n, H)
     with _timed("density"):
-        check(_capi.lib().sph_density_gather(_p(params), n, _SUPPORT[supportMode], fptr(x), fptr(H), fptr(m), *_csr(adj), ptr(rho),
+        check(_capi.lib().sph_density_gather(_p(params), n, _SUPPORT[supportMode], fptr(x), fptr(H), fptr(m), *_lists(params, adj, True), ptr(rho),
                                              stream_ptr(H.device)), "sph_density_gather")
     return rho
 
@@ -218,7 +235,7 @@ def adaptive_h_iter(params, x, H, m, adj: AdjacencyList, hbounds: torch.Tensor):
     n = H.shape[0]
     rho, Hn, ratio = _empty(n, H), _empty(n, H), _empty(n, H)
     with _timed("adaptive_h_iter"):
-        check(_capi.lib().sph_adaptive_h_iter(_p(params), n, 0, fptr(x), fptr(H), fptr(m), *_csr(adj), fptr(hbounds), ptr(rho), ptr(Hn),
+        check(_capi.lib().sph_adaptive_h_iter(_p(params), n, 0, fptr(x), fptr(H), fptr(m), *_lists(params, adj, True), fptr(hbounds), ptr(rho), ptr(Hn),
                                               ptr(ratio), stream_ptr(H.device)), "sph_adaptive_h_iter")
     return rho, Hn, ratio
 
@@ -227,7 +244,7 @@ def crk_volume(params, x, H, adj: AdjacencyList) -> torch.Tensor:
     n = H.shape[0]
     V = _empty(n, H)
     with _timed("crk_volume"):
-        check(_capi.lib().sph_crk_volume(_p(params), n, fptr(x), fptr(H), *_csr(adj), ptr(V), stream_ptr(H.device)), "sph_crk_volume")
+        check(_capi.lib().sph_crk_volume(_p(params), n, fptr(x), fptr(H), *_lists(params, adj, True), ptr(V), stream_ptr(H.device)), "sph_crk_volume")
     return V
 
 
@@ -235,7 +252,7 @@ def crk_factors(params, x, H, m, V, adj: AdjacencyList):
     n, d = H.shape[0], int(params.dim)
     A, B, gA, gB, rho = _empty(n, H), _empty((n, d), H), _empty((n, d), H), _empty((n, d, d), H), _empty(n, H)
     with _timed("crk_factors"):
-        check(_capi.lib().sph_crk_factors(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(V), *_csr(adj), ptr(A), ptr(B), ptr(gA), ptr(gB),
+        check(_capi.lib().sph_crk_factors(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(V), *_lists(params, adj, True), ptr(A), ptr(B), ptr(gA), ptr(gB),
                                           ptr(rho), stream_ptr(H.device)), "sph_crk_factors")
     return CRKState(A=A, B=B, gradA=gA, gradB=gB), rho
 
@@ -249,27 +266,34 @@ def eos_ideal_gas(params, u, rho):
     return A, P, c
 
 
-def grad_v(params, x, H, m, rho, V, crk: CRKState, v, c, adj: AdjacencyList, cullen: bool):
+def grad_v(params, x, H, m, rho, V, crk: CRKState, v, c, adj: AdjacencyList, cullen: bool, want_vsig: bool = False):
+    """CRK velocity gradient (+ the Cullen divergence when `cullen`).  v_sig needs the
+    Verlet set; the step computes it in the Cullen pass, tests may ask for it here."""
     n, d = H.shape[0], int(params.dim)
     G, drho = _empty((n, d, d), H), _empty(n, H)
     div = _empty(n, H) if cullen else None
-    vs = _empty(n, H) if cullen else None
+    vs = _empty(n, H) if want_vsig else None
     with _timed("grad_v"):
         check(_capi.lib().sph_grad_v(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(V), fptr(crk.A), fptr(crk.B), fptr(crk.gradA),
-                                     fptr(crk.gradB), fptr(v), fptr(c), *_csr(adj), ptr(G), ptr(drho), ptr(div), ptr(vs),
-                                     stream_ptr(H.device)), "sph_grad_v")
+                                     fptr(crk.gradB), fptr(v), fptr(c), *_lists(params, adj, not want_vsig), ptr(G), ptr(drho), ptr(div),
+                                     ptr(vs), stream_ptr(H.device)), "sph_grad_v")
     return G, drho, div, vs
 
 
-def switch_cullen(params, x, H, m, rho, div, div_prev, vsig, alpha0, dt, adj: AdjacencyList, want_R: bool = False):
+def switch_cullen(params, x, H, m, rho, div, div_prev, vsig, alpha0, dt, adj: AdjacencyList, want_R: bool = False,
+                  v=None, c=None, want_vsig: bool = False):
+    """Cullen-Dehnen switch.  With vsig=None the signal velocity is computed in the same
+    pass from v and c over the Verlet list (returned third when want_vsig)."""
     n = H.shape[0]
     al = _empty(n, H)
     R = _empty(n, H) if want_R else None
+    vs_out = _empty(n, H) if (vsig is None and want_vsig) else None
     with _timed("switch_cullen"):
-        check(_capi.lib().sph_switch_cullen(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(div), fptr(_f32(div_prev)), fptr(vsig),
-                                            fptr(_f32(alpha0)), fptr(dt_tensor(dt, H.device)), *_csr(adj), ptr(al), ptr(R),
+        check(_capi.lib().sph_switch_cullen(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(div), fptr(_f32(div_prev)),
+                                            fptr(vsig), fptr(v), fptr(c), fptr(_f32(alpha0)), fptr(dt_tensor(dt, H.device)),
+                                            *_lists(params, adj, vsig is not None), ptr(al), ptr(R), ptr(vs_out),
                                             stream_ptr(H.device)), "sph_switch_cullen")
-    return al, R
+    return al, R, vs_out
 
 
 def switch_balsara(params, DvDx, c):
@@ -280,23 +304,31 @@ def switch_balsara(params, DvDx, c):
 
 
 def crk_accel_dudt(params, x, H, m, rho, V, crk: CRKState, v, c, P, DvDx, adj: AdjacencyList, pair_arrays: bool = True):
+    """Fused CRK momentum and energy RHS over the interacting list; the pairwise
+    accelerations are returned in Verlet-entry order (zeros beyond the support)."""
     n, d = H.shape[0], int(params.dim)
     dvdt, dudt = _empty((n, d), H), _empty(n, H)
-    ap = _empty((adj.nnz, d), H) if pair_arrays else None
-    av = _empty((adj.nnz, d), H) if pair_arrays else None
+    inter = adj.interList is not None
+    alloc = torch.zeros if inter else torch.empty
+    ap = alloc((adj.nnz, d), device=H.device, dtype=torch.float32) if pair_arrays else None
+    av = alloc((adj.nnz, d), device=H.device, dtype=torch.float32) if pair_arrays else None
     with _timed("crk_accel_dudt"):
         check(_capi.lib().sph_crk_accel_dudt(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(V), fptr(crk.A), fptr(crk.B),
-                                             fptr(crk.gradA), fptr(crk.gradB), fptr(v), fptr(c), fptr(P), fptr(DvDx), *_csr(adj),
-                                             ptr(dvdt), ptr(dudt), ptr(ap), ptr(av), stream_ptr(H.device)), "sph_crk_accel_dudt")
+                                             fptr(crk.gradA), fptr(crk.gradB), fptr(v), fptr(c), fptr(P), fptr(DvDx),
+                                             *_lists(params, adj, True), ptr(dvdt), ptr(dudt), ptr(ap), ptr(av),
+                                             stream_ptr(H.device)), "sph_crk_accel_dudt")
     return dvdt, dudt, ap, av
 
 
 def compsph_balance(params, m, rho, P, u, v, dvdt, dt, adj: AdjacencyList, ap, av):
+    """Energy partition f_ij for every Verlet entry."""
+    n, d = m.shape[0], int(params.dim)
     f = _empty(adj.nnz, m)
+    scratch = _empty(n * (d + 1), m)
     with _timed("compsph_balance"):
-        check(_capi.lib().sph_compsph_balance(_p(params), m.shape[0], fptr(m), fptr(rho), fptr(P), fptr(u), fptr(v), fptr(dvdt),
-                                              fptr(dt_tensor(dt, m.device)), *_csr(adj), fptr(ap), fptr(av), ptr(f),
-                                              stream_ptr(m.device)), "sph_compsph_balance")
+        check(_capi.lib().sph_compsph_balance(_p(params), n, fptr(m), fptr(rho), fptr(P), fptr(u), fptr(v), fptr(dvdt),
+                                              fptr(dt_tensor(dt, m.device)), *_lists(params, adj, False), fptr(ap), fptr(av),
+                                              ptr(scratch), ptr(f), stream_ptr(m.device)), "sph_compsph_balance")
     return f
 
 
@@ -329,10 +361,12 @@ def finalize_compatible_energy(params, weights, dt, v0, u0, stages):
     u = _empty(n, u0)
     scratch = _empty(n * (1 + d), u0)
     ns = len(stages)
+    inter = all(s[1].interList is not None for s in stages)
+    params.list_stride = 2 if inter else 1
     arrs = [_capi.ptr_array([fptr(s[0]) for s in stages]),
-            _capi.ptr_array([iptr(s[1].neighborOffsets) for s in stages]),
-            _capi.ptr_array([iptr(s[1].numNeighbors) for s in stages]),
-            _capi.ptr_array([iptr(s[1].neighborList) for s in stages]),
+            _capi.ptr_array([iptr(s[1].interOffsets if inter else s[1].neighborOffsets) for s in stages]),
+            _capi.ptr_array([iptr(s[1].interCounts if inter else s[1].numNeighbors) for s in stages]),
+            _capi.ptr_array([iptr(s[1].interList if inter else s[1].neighborList) for s in stages]),
             _capi.ptr_array([fptr(s[2]) for s in stages]),
             _capi.ptr_array([fptr(s[3]) for s in stages]),
             _capi.ptr_array([fptr(s[4]) for s in stages])]

@@ -8,8 +8,8 @@ every SPH operation executed by libwarpsph_b200 kernels:
   Verlet list                         crkSPH.py:54  -> sph_neighbors_build (unchanged prior reused)
   CRK volume / coefficients / rho     crkSPH.py:61  -> sph_crk_volume + sph_crk_factors
   ideal-gas EOS                       crkSPH.py:95  -> sph_eos_ideal_gas
-  CRK velocity gradient               crkSPH.py:158 -> sph_grad_v (also Cullen div and v_sig)
-  viscosity switch                    crkSPH.py:195 -> sph_switch_cullen / sph_switch_balsara
+  CRK velocity gradient               crkSPH.py:158 -> sph_grad_v (also the Cullen divergence)
+  viscosity switch                    crkSPH.py:195 -> sph_switch_cullen (R and v_sig) / sph_switch_balsara
   momentum + energy RHS               crkSPH.py:241,263 -> sph_crk_accel_dudt (one fused pass)
   energy partition f_ij               crkSPH.py:343 -> sph_compsph_balance
 """
@@ -119,13 +119,13 @@ def crkSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams:
     S.entropies, S.pressures, S.soundspeeds = ops.eos_ideal_gas(params, S.internalEnergies, S.densities)
     switch = compParams.viscositySwitchParams.scheme
     cullen = switch == ViscositySwitch.CullenDehnen2010
-    # crkSPH.py:158-172 (+ the Cullen divergence and v_sig in the same pass)
-    DvDx, drhodt, div_cd, vsig = ops.grad_v(params, S.positions, S.supports, S.masses, S.densities, V, crk, S.velocities,
-                                            S.soundspeeds, adjacency, cullen)
-    # crkSPH.py:195-200
+    # crkSPH.py:158-172 (+ the Cullen divergence in the same pass)
+    DvDx, drhodt, div_cd, _ = ops.grad_v(params, S.positions, S.supports, S.masses, S.densities, V, crk, S.velocities,
+                                         S.soundspeeds, adjacency, cullen)
+    # crkSPH.py:195-200 (v_sig over the Verlet set is computed inside the switch pass)
     if cullen:
-        S.alphas, _ = ops.switch_cullen(params, S.positions, S.supports, S.masses, S.densities, div_cd, S.divergence, vsig,
-                                        S.alpha0s, dt, adjacency)
+        S.alphas, _, _ = ops.switch_cullen(params, S.positions, S.supports, S.masses, S.densities, div_cd, S.divergence, None,
+                                           S.alpha0s, dt, adjacency, v=S.velocities, c=S.soundspeeds)
     elif switch == ViscositySwitch.Balsara1995:
         S.alphas = ops.switch_balsara(params, DvDx, S.soundspeeds)
     elif switch != ViscositySwitch.NoneSwitch:
