@@ -1,0 +1,444 @@
+"""Generates the golden vectors in tests/golden/ by executing the reference's own
+Python source (wi-re/warpSPH, read from /root/reference at generation time only).
+
+The hot-path arithmetic that lives in the reference repository is plain Python:
+Warp @wp.func bodies (modules/crk/accel.py, modules/crk/dudt.py, modules/crk/limiter.py,
+modules/compSPH/balance.py, modules/shockCapturing/wp_vsig.py, modules/dissipation/pi.py,
+modules/dissipation/util.py) and torch code (modules/eos/idealGas.py,
+modules/compSPH/multistep.py, modules/shockCapturing/CullenDehnen2010.py,
+modules/timestep/compressible.py, modules/adaptiveSupport/optimalSupportMonaghan.py).
+This script runs those function bodies unmodified, with
+  * a numpy stand-in for the Warp builtins they call (wp.dot, wp.min/max with Warp's
+    `a < b ? a : b` semantics, wp.exp, wp.pow, ...; decorators are identities), all
+    arithmetic in numpy float32 scalars and arrays;
+  * the pieces the reference imports from its absent sibling package warpSPHCore
+    (minimum-image distance, Wendland kernel and gradient, the CRK-corrected gradient,
+    particle accessors, generic interpolation) supplied by this project's restatement,
+    operation for operation as in oracle/sph_oracle.c.
+Inputs that come from warpSPHCore in the reference (CRK coefficients, volumes,
+densities) are computed by the FP32 oracle and stored with the outputs, so a test
+can feed identical inputs to the oracle or the GPU and compare with the reference's
+own results.
+
+Usage (in a container that has the reference checkout):
+    python tests/golden/make_golden.py [--reference /root/reference]
+"""
+from __future__ import annotations
+
+import argparse
+import inspect
+import re
+import sys
+import types
+from dataclasses import dataclass, field
+from enum import Enum
+from pathlib import Path
+from typing import Any, List, Optional, Tuple, Union
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+F = np.float32
+
+
+# ---------------------------------------------------------------- Warp stand-in
+def _ident(*a, **k):
+    if len(a) == 1 and callable(a[0]) and not k:
+        return a[0]
+    return lambda f: f
+
+
+wp = types.SimpleNamespace(
+    func=_ident, kernel=_ident, struct=_ident, static=lambda x: x,
+    dot=lambda a, b: F(np.dot(np.asarray(a, F), np.asarray(b, F))),
+    min=lambda a, b: a if a < b else b, max=lambda a, b: a if a > b else b,
+    abs=lambda x: abs(x), exp=lambda x: F(np.exp(F(x))), pow=lambda a, b: F(np.power(F(a), F(b))),
+    sqrt=lambda x: F(np.sqrt(F(x))),
+    int32=int, int64=int, bool=bool, float32=F, array=lambda *a, **k: None, tid=lambda: 0,
+)
+vector = matrix = lambda *a, **k: None
+
+
+# ---------------------------------------------------------------- warpSPHCore restatement (ours)
+class OperationDirection(Enum):
+    TrueAllToToAll = 0
+
+
+KSCALE = {(1, 1): 1.620185175, (1, 2): 1.897366596, (1, 3): 1.936491673,
+          (2, 1): 1.936491673, (2, 2): 2.171240593, (2, 3): 2.207940217,
+          (3, 1): 2.207940217, (3, 2): 2.415229458, (3, 3): 2.449489743}
+
+
+def kernel_C(K, D):
+    pi = 3.14159265358979323846
+    if K == 1:
+        return F(1.25) if D == 1 else (F(7.0 / pi) if D == 2 else F(21.0 / (2.0 * pi)))
+    if K == 2:
+        return F(1.5) if D == 1 else (F(9.0 / pi) if D == 2 else F(495.0 / (32.0 * pi)))
+    return F(1.71875) if D == 1 else (F(78.0 / (7.0 * pi)) if D == 2 else F(1365.0 / (64.0 * pi)))
+
+
+def kernel_kp(K, D, q):
+    t = F(1) - q
+    if K == 1:
+        if D == 1:
+            t2 = t * t
+            return t2 * t * (F(1) + F(3) * q), F(12) * t2
+        t3 = t * t * t
+        return t3 * t * (F(1) + F(4) * q), F(20) * t3
+    if K == 2:
+        if D == 1:
+            t4 = (t * t) * (t * t)
+            return t4 * t * (F(1) + F(5) * q + F(8) * q * q), F(14) * (F(1) + F(4) * q) * t4
+        t5 = (t * t) * (t * t) * t
+        return t5 * t * (F(1) + F(6) * q + (F(35) / F(3)) * q * q), (F(56) / F(3)) * (F(1) + F(5) * q) * t5
+    if D == 1:
+        t6 = (t * t) * (t * t) * (t * t)
+        return t6 * t * (F(1) + F(7) * q + F(19) * q * q + F(21) * q * q * q), F(6) * (F(3) + F(18) * q + F(35) * q * q) * t6
+    t7 = (t * t) * (t * t) * (t * t) * t
+    return t7 * t * (F(1) + F(8) * q + F(25) * q * q + F(32) * q * q * q), F(22) * (F(1) + F(7) * q + F(16) * q * q) * t7
+
+
+def ipowD(h, D):
+    return h if D == 1 else (h * h if D == 2 else h * h * h)
+
+
+class Ctx:
+    kernel = 2
+    dim = 2
+    L = F(1.0)
+    halfL = F(0.5)
+    periodic = True
+
+
+def computeDistanceVec(xi, xj, domainState=None):
+    d = (np.asarray(xi, F) - np.asarray(xj, F)).astype(F)
+    if Ctx.periodic:
+        d = np.where(d > Ctx.halfL, (d - Ctx.L).astype(F), np.where(d < -Ctx.halfL, (d + Ctx.L).astype(F), d)).astype(F)
+    return d
+
+
+def safe_sqrt(x):
+    return F(np.sqrt(F(x if x > 0 else 0)))
+
+
+def kWG(x, r, H):
+    K, D = Ctx.kernel, Ctx.dim
+    q = F(r) / F(H)
+    if not (q < F(1)):
+        return F(0), np.zeros(D, F)
+    k, p = kernel_kp(K, D, q)
+    cH = kernel_C(K, D) / ipowD(F(H), D)
+    W = cH * k
+    s = -cH * p / (F(H) * F(H))
+    return F(W), (F(s) * np.asarray(x, F)).astype(F)
+
+
+def computeKernelGradientCRK(xi, xj, hi, hj, kernelProperties, domainState, useCRK, A, B, gradA, gradB):
+    # W evaluated with hj (the two supports are equal at every reference call site)
+    D = Ctx.dim
+    x = computeDistanceVec(xi, xj, domainState)
+    r = safe_sqrt(wp.dot(x, x))
+    W, gW = kWG(x, r, hj)
+    B = np.asarray(B, F)
+    bx = F(1) + wp.dot(B, x)
+    out = np.zeros(D, F)
+    for g in range(D):
+        gbx = F(gradB[0][g]) * x[0]
+        for a in range(1, D):
+            gbx = gbx + F(gradB[a][g]) * x[a]
+        out[g] = F(A) * bx * gW[g] + F(A) * B[g] * W + F(gradA[g]) * bx * W + F(A) * gbx * W
+    return out
+
+
+def sphKernelScale(kernel, dim):
+    return F(KSCALE[(int(kernel), int(dim))])
+
+
+sphKernel_xi = sphKernelScale
+
+
+def zero_like_warp(v):
+    return np.zeros_like(np.asarray(v, F)) if np.ndim(v) else F(0)
+
+
+def matmul(M, x):
+    M = np.asarray(M, F)
+    x = np.asarray(x, F)
+    D = len(x)
+    out = np.zeros(D, F)
+    for a in range(D):
+        s = M[a, 0] * x[0]
+        for b in range(1, D):
+            s = s + M[a, b] * x[b]
+        out[a] = s
+    return out
+
+
+class SoA:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+def getParticle(state, j):
+    return state.positions[j], F(state.supports[j]), F(state.masses[j]), F(state.densities[j]), int(state.kinds[j])
+
+
+def getVolume_j(cd, j):
+    return True, F(cd.V[j])
+
+
+def getCRK_j(cd, j):
+    return True, F(cd.A[j]), cd.B[j], cd.gA[j], cd.gB[j]
+
+
+def checkDirectionality_j(k, mode):
+    return True
+
+
+CORE = dict(scalar_t=F, vector=vector, matrix=matrix, Any=Any, OperationDirection=OperationDirection,
+            computeDistanceVec=computeDistanceVec, safe_sqrt=safe_sqrt, computeKernelGradientCRK=computeKernelGradientCRK,
+            sphKernelScale=sphKernelScale, sphKernel_xi=sphKernel_xi, zero_like_warp=zero_like_warp, matmul=matmul,
+            getParticle=getParticle, getVolume_j=getVolume_j, getCRK_j=getCRK_j, checkDirectionality_j=checkDirectionality_j,
+            domainData=None, kernelState=None, adjacencyData=None, gridData=None)
+
+
+# ---------------------------------------------------------------- loading reference files
+def load(ref: Path, rel: str, extra: dict | None = None) -> dict:
+    src = (ref / "src" / "warpSPH" / rel).read_text()
+    lines = src.split("\n")
+    out, skip = [], False
+    for ln in lines:
+        if skip:
+            out.append("")
+            skip = "(" in ln and ")" not in ln or (skip and ")" not in ln)
+            continue
+        if re.match(r"^(from|import)\s", ln):
+            out.append("")
+            skip = "(" in ln and ")" not in ln
+        else:
+            out.append(ln)
+    ns = dict(CORE)
+    ns.update(wp=wp, torch=torch, np=np, Optional=Optional, Union=Union, Tuple=Tuple, List=List, dataclass=dataclass, field=field,
+              Enum=Enum, record_function=torch.profiler.record_function, __name__="ref_" + rel.replace("/", "_"))
+    if extra:
+        ns.update(extra)
+    exec(compile("\n".join(out), str(ref / "src" / "warpSPH" / rel), "exec"), ns)
+    return ns
+
+
+def call(fn, **values):
+    names = list(inspect.signature(fn).parameters)
+    missing = [n for n in names if n not in values]
+    if missing:
+        raise KeyError(f"{fn.__name__}: no value for {missing}")
+    return fn(*[values[n] for n in names])
+
+
+# ---------------------------------------------------------------- inputs
+def make_case(seed=0, n_side=14):
+    from oracle import oracle
+    from oracle.steps import cell_capacity_for
+    from tests.cases import make_params, make_particles
+    import warpsph_b200 as ws
+    cfg, sch, p = make_params(2, kernel=ws.KernelFunctions.Wendland4)
+    P = make_particles(2, n_side, seed=seed, jitter=0.4, flow=1.0)
+    n = len(P["masses"])
+    rng = np.random.default_rng(seed + 100)
+    x, H, m, v = P["positions"], P["supports"], P["masses"], P["velocities"]
+    # compressive + shearing flow so the limiters and the viscosity are exercised
+    v = (v - 2.0 * x + 0.3 * rng.standard_normal(x.shape)).astype(F)
+    u = (1.0 + 3.0 * rng.random(n)).astype(F)
+    o = oracle.get("f32")
+    nb = o.neighbors(p, x, H, cell_capacity_for(n, 2))
+    V = o.crk_volume(p, x, H, nb)
+    A, B, gA, gB, rho = o.crk_factors(p, x, H, m, V, nb)
+    Aent, Pr, c = o.eos(p, u, rho)
+    G, drho, div, vsig = o.grad_v(p, x, H, m, rho, V, A, B, gA, gB, v, c, nb, cullen=True)
+    dvdt_guess = (0.5 * rng.standard_normal(x.shape)).astype(F)
+    return dict(params=p, x=x, H=H, m=m, v=v, u=u, V=V, A=A, B=B, gA=gA, gB=gB, rho=rho, P=Pr, c=c, G=G, drho=drho, div=div,
+                vsig=vsig, nb=nb, dvdt_guess=dvdt_guess, n=n)
+
+
+def run_reference(ref: Path, case: dict) -> dict:
+    import warpsph_b200 as ws
+    p = case["params"]
+    n = case["n"]
+    nb = case["nb"]
+    offs, cnt, lst = nb["offsets"], nb["counts"], nb["list"].astype(np.int64)
+    nnz = len(lst)
+    state = SoA(positions=case["x"], supports=case["H"], masses=case["m"], densities=case["rho"], kinds=np.zeros(n, np.int32))
+    cd = SoA(V=case["V"], A=case["A"], B=case["B"], gA=case["gA"], gB=case["gB"])
+    dp = ws.configurations.buildDefaultDiffusionParamsCRKSPH()
+    visc = SoA(C_l=F(dp.C_l), C_q=F(dp.C_q), Cu_l=F(dp.Cu_l), Cu_q=F(dp.Cu_q), K=F(dp.K), viscosityTerm=dp.viscosityTerm,
+               thermalConducitiyTerm=dp.thermalConducitiyTerm, scaleBeta=dp.scaleBeta, monaghanSwitch=dp.monaghanSwitch,
+               correctXi=dp.correctXi)
+    crkv = SoA(eta_fold=F(0.2), eta_crit=F(0.3333333), enableCRKLimiter=True, enableVanLeerLimiter=True,
+               forceVanLeerOff=False, forceVanLeerOn=False)
+    kp = SoA(operationMode=OperationDirection.TrueAllToToAll.value, kernelFunction=int(p.kernel))
+    dom = SoA(dim=2)
+    diff = load(ref, "configurations/moduleConfigurations/diffusionParameters.py")
+    util = load(ref, "modules/dissipation/util.py", {"ViscosityTerms": diff["ViscosityTerms"]})
+    pi = load(ref, "modules/dissipation/pi.py", {"ViscosityTerms": diff["ViscosityTerms"], "DiffusionParameters": None,
+                                               "compute_mu_ij": util["compute_mu_ij"], "compute_bars": util["compute_bars"]})
+    lim = load(ref, "modules/crk/limiter.py")
+    common = dict(CRKViscosity=None, DiffusionParameters=None, computePi_actual=pi["computePi_actual"],
+                  computeVanLeer=lim["computeVanLeer"], crkLimiter=lim["crkLimiter"])
+    acc = load(ref, "modules/crk/accel.py", common)
+    dud = load(ref, "modules/crk/dudt.py", common)
+    out = {}
+    ap = np.zeros((nnz, 2), F)
+    av = np.zeros((nnz, 2), F)
+    accel = np.zeros((n, 2), F)
+    dudt = np.zeros(n, F)
+    with np.errstate(all="ignore"):
+        for i in range(n):
+            vals = dict(i=i, dim=2, xi=case["x"][i], hi=F(case["H"][i]), mi=F(case["m"][i]), rhoi=F(case["rho"][i]),
+                        referenceState=state, correctionData=cd, domainState=dom, kernelProperties=kp,
+                        beginIndex=int(offs[i]), numIndices=int(cnt[i]), offsetArray=lst, ki=0, referenceKinds=state.kinds,
+                        useGradientRenormalization=False, Li=None, useGradHTerms=False, omega_i=F(1), useVolume=True,
+                        Vi=F(case["V"][i]), useCRK=True, Ai=F(case["A"][i]), Bi=case["B"][i], gradAi=case["gA"][i],
+                        gradBi=case["gB"][i], vel_i=case["v"][i], referenceVelocities=case["v"], u_i=F(case["u"][i]),
+                        referenceEnergies=case["u"], cs_i=F(case["c"][i]), referenceCs=case["c"], viscositySwitch=True,
+                        alpha_i=F(1), referenceAlphas=np.ones(n, F), P_i=F(case["P"][i]), referencePressures=case["P"],
+                        viscosityParams=visc, crkViscosityParams=crkv, gradV_i=case["G"][i],
+                        referenceVelocityTensor=case["G"], pressureAccel_ij=ap, viscosityAccel_ij=av)
+            accel[i] = call(acc["computeCrkSPHAccel_Func_i"], **vals)
+            dudt[i] = call(dud["computeCrkSPHdudt_Func_i"], **vals)
+    out.update(accel=accel, dudt=dudt, ap=ap, av=av)
+
+    # energy partition f_ij for the six schemes (modules/compSPH/balance.py)
+    bal = load(ref, "modules/compSPH/balance.py", {"EnergyScheme": ws.EnergyScheme})
+    dt = F(1e-3)
+    vh = (case["v"] + F(0.5) * dt * case["dvdt_guess"]).astype(F)
+    fs = np.zeros((6, nnz), F)
+    with np.errstate(all="ignore"):
+        for es in ws.EnergyScheme:
+            f_ij = np.zeros(nnz, F)
+            for i in range(n):
+                call(bal["computeCompSPHBalanceTerm_Func_i"], i=i, dim=2, xi=case["x"][i], hi=F(case["H"][i]), mi=F(case["m"][i]),
+                     rhoi=F(case["rho"][i]), referenceState=state, domainState=dom, kernelProperties=kp,
+                     beginIndex=int(offs[i]), numIndices=int(cnt[i]), offsetArray=lst, ki=0, referenceKinds=state.kinds,
+                     useGradientRenormalization=False, Li=None, useGradHTerms=False, omega_i=F(1), referenceOmegas=None,
+                     useVolume=True, Vi=F(case["V"][i]), referenceVolumes=case["V"], useCRK=True, Ai=F(case["A"][i]),
+                     Bi=case["B"][i], gradAi=case["gA"][i], gradBi=case["gB"][i], vel_i=vh[i], referenceVelocities=vh,
+                     u_i=F(case["u"][i]), referenceEnergies=case["u"], P_i=F(case["P"][i]), referencePressures=case["P"],
+                     ap_ij=ap, av_ij=av, energyScheme_int=es.value, dt=dt, gamma=F(p.gamma), f_ij=f_ij)
+            fs[es.value] = f_ij
+    out.update(f_ij=fs, balance_dt=np.array([dt], F), dvdt_guess=case["dvdt_guess"])
+
+    # signal velocity (modules/shockCapturing/wp_vsig.py)
+    vs_ns = load(ref, "modules/shockCapturing/wp_vsig.py")
+    vsig = np.zeros(n, F)
+    with np.errstate(all="ignore"):
+        for i in range(n):
+            vsig[i] = call(vs_ns["computeVsig_Func_i"], i=i, dim=2, xi=case["x"][i], hi=F(case["H"][i]), mi=F(case["m"][i]),
+                           rhoi=F(case["rho"][i]), referenceState=state, domainState=dom, kernelProperties=kp,
+                           beginIndex=int(offs[i]), numIndices=int(cnt[i]), offsetArray=lst, ki=0, referenceKinds=state.kinds,
+                           useGradientRenormalization=False, Li=None, useGradHTerms=False, Viscosity_i=F(1),
+                           referenceViscositys=None, useVolume=False, Vi=F(0), referenceVolumes=None, useCRK=False, Ai=F(1),
+                           Bi=None, gradAi=None, gradBi=None, vel_i=case["v"][i], referenceVelocities=case["v"],
+                           individual_cs=True, cs_i=F(case["c"][i]), referenceCs=case["c"], outputValue=F(0))
+    out["vsig"] = np.abs(vsig)
+
+    # ideal-gas EOS (modules/eos/idealGas.py)
+    eos = load(ref, "modules/eos/idealGas.py")
+    Aent, _, Pt, ct = eos["idealGasEOS"](A=None, u=torch.from_numpy(case["u"]), P=None, rho=torch.from_numpy(case["rho"]),
+                                           gamma=float(p.gamma))
+    out.update(eos_A=Aent.numpy(), eos_P=Pt.numpy(), eos_c=ct.numpy())
+
+    # Cullen-Dehnen switch algebra (modules/shockCapturing/CullenDehnen2010.py:218-331) with the
+    # generic SPH operations (warpSPHCore warpOperation) restated here in numpy
+    H, m, rho, x = case["H"], case["m"], case["rho"], case["x"]
+
+    def warpOperation(state, props, domain=None, adjacency=None, queryValues=None, **kw):
+        op = props.operation
+        if op == "Divergence":
+            return torch.from_numpy(case["div"])
+        if op == "Interpolate":
+            qv = queryValues.numpy() if isinstance(queryValues, torch.Tensor) else queryValues
+            outv = np.zeros(n, F)
+            for i in range(n):
+                s = F(0)
+                for k in range(offs[i], offs[i] + cnt[i]):
+                    j = lst[k]
+                    d = computeDistanceVec(x[i], x[j])
+                    W, _ = kWG(d, safe_sqrt(wp.dot(d, d)), H[i])
+                    s = s + m[j] / rho[j] * qv[j] * W
+                outv[i] = s
+            return torch.from_numpy(outv)
+        raise NotImplementedError(op)
+
+    class OperationProperties:
+        def __init__(self, kernel=None, operation=None, supportMode=None, gradientMode=None):
+            self.operation = operation
+
+    WarpOperation = types.SimpleNamespace(Divergence="Divergence", Interpolate="Interpolate", Gradient="Gradient")
+    cd_ns = load(ref, "modules/shockCapturing/CullenDehnen2010.py", dict(
+        warpOperation=warpOperation, OperationProperties=OperationProperties, WarpOperation=WarpOperation,
+        GradientScheme=types.SimpleNamespace(Difference=1), SupportScheme=types.SimpleNamespace(Gather=0, SuperSymmetric=3),
+        ViscositySwitchState=lambda **kw: SoA(**kw), CompressibleState=None, SimulationConfig=None, CompressibleSPHConfig=None,
+        AdjacencyList=None, CompactHashMap=None, computeM=None,
+        computeVsigWarp=lambda *a, **k: torch.from_numpy(out["vsig"])))
+    div_prev = (case["div"] * 0.7 + 0.05).astype(F)
+    alpha0 = np.full(n, 0.6, F)
+    ps = SoA(positions=torch.from_numpy(x), supports=torch.from_numpy(H), densities=torch.from_numpy(rho),
+             divergence=torch.from_numpy(div_prev), alpha0s=torch.from_numpy(alpha0), velocities=torch.from_numpy(case["v"]),
+             soundspeeds=torch.from_numpy(case["c"]))
+    swc = SoA(alpha_min=0.02, alpha_max=2.0, beta_xi=2.0, limitXi=True, correctVelocityGradient=False)
+    sim = SoA(kernel=types.SimpleNamespace(value=int(p.kernel)), supportMode=3, domain=None)
+    a0s, sst = cd_ns["computeCullenTerms"](1e-3, ps, sim, SoA(viscositySwitchParams=swc), None, None)
+    out.update(cullen_alpha=a0s.numpy().astype(F), cullen_R=sst.R.numpy().astype(F), cullen_div_prev=div_prev,
+               cullen_alpha0=alpha0)
+
+    # compatible energy (modules/compSPH/multistep.py:52-94), two stages
+    ms = load(ref, "modules/compSPH/multistep.py", {"EnergyScheme": ws.EnergyScheme, "CompressibleSystemUpdate": None,
+                                                     "CompSPHConfig": None, "SimulationConfig": None})
+    i_idx = torch.from_numpy(np.repeat(np.arange(n), cnt).astype(np.int64))
+    j_idx = torch.from_numpy(lst)
+    rng = np.random.default_rng(7)
+    stages, updates = [], []
+    f_stage = [fs[5], fs[0]]
+    for s in range(2):
+        dv = (case["dvdt_guess"] * (1 + 0.3 * s)).astype(F)
+        stages.append((SoA(i=i_idx, j=j_idx), SoA(f_ij=torch.from_numpy(f_stage[s]), ap_ij=torch.from_numpy(ap * F(1 + 0.1 * s)),
+                                                   av_ij=torch.from_numpy(av * F(1 - 0.1 * s)))))
+        updates.append(SoA(dvdt=torch.from_numpy(dv)))
+    init = SoA(velocities=torch.from_numpy(case["v"]), internalEnergies=torch.from_numpy(case["u"]), positions=torch.from_numpy(x))
+    for es in (ws.EnergyScheme.CRK, ws.EnergyScheme.PdV):
+        du = ms["compSPH_deltaU_multistep"](float(dt), init, stages, updates, np.array([0.5, 0.5]), None, SoA(energyScheme=es))
+        out[f"multistep_du_{es.name}"] = du.numpy().astype(F)
+    out["multistep_dvdt"] = np.stack([u.dvdt.numpy() for u in updates])
+
+    # CFL time step (modules/timestep/compressible.py:12-61)
+    ts = load(ref, "modules/timestep/compressible.py", {"idealGasEOS": eos["idealGasEOS"], "volumeToSupportHelper": lambda *a: 0.0,
+                                                        "CompressibleState": None, "CompressibleSystem": None,
+                                                        "CompressibleSPHConfig": None, "SimulationConfig": None})
+    sysobj = SoA(state=SoA(internalEnergies=torch.from_numpy(case["u"]), densities=torch.from_numpy(rho), supports=torch.from_numpy(H)))
+    conf = SoA(adaptiveDt=True, cflFactor=0.3, dx=1.0, targetNeighbors=32, dim=2, kernel=types.SimpleNamespace(value=int(p.kernel)),
+               minDt=1e-6, maxDt=1e-2, dt=1e-4, dtGrowthFactor=1.1)
+    out["cfl_dt_grow"] = np.array([ts["computeTimestep"](sysobj, conf, SoA(gamma=float(p.gamma)), dt=1e-4)], np.float64)
+    out["cfl_dt_first"] = np.array([ts["computeTimestep"](sysobj, conf, SoA(gamma=float(p.gamma)), dt=None)], np.float64)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    a = ap.parse_args()
+    ref = Path(a.reference)
+    case = make_case()
+    out = run_reference(ref, case)
+    nb = case["nb"]
+    np.savez_compressed(Path(__file__).parent / "crk_pair_golden.npz",
+                        x=case["x"], H=case["H"], m=case["m"], v=case["v"], u=case["u"], V=case["V"], A=case["A"], B=case["B"],
+                        gA=case["gA"], gB=case["gB"], rho=case["rho"], P=case["P"], c=case["c"], G=case["G"], div=case["div"],
+                        offsets=nb["offsets"], counts=nb["counts"], list=nb["list"], **out)
+    print("wrote", Path(__file__).parent / "crk_pair_golden.npz", "particles", case["n"], "pairs", len(nb["list"]))
+
+
+if __name__ == "__main__":
+    main()
