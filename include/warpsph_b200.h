@@ -287,6 +287,21 @@ int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const flo
                         const int32_t* list, const float* ap_ij, const float* av_ij,
                         float* scratch, float* f_ij_out, void* stream);
 
+/* sph_compsph_balance without a scratch argument: no counterpart in the reference,
+ * which allocates its temporaries through torch.  For callers that cannot allocate
+ * device memory on the step path (an FFI host with no caching allocator, or a timed
+ * loop where cudaMalloc/cudaFree would synchronise the device).  The scratch is a
+ * fixed per-device array of SPH_BALANCE_NOALLOC_MAX_FLOATS floats, so n*(dim+1) must
+ * not exceed it (SPH_ERR_BAD_ARG otherwise).  The first call on a device resolves the
+ * array's address; make it before any stream capture.  Calls in flight at the same
+ * time on one device share the array and race: serialise them on one stream. */
+#define SPH_BALANCE_NOALLOC_MAX_FLOATS (1 << 22)
+int sph_compsph_balance_noalloc(const SphParams* p, int64_t n, const float* m, const float* rho,
+                                const float* P, const float* u, const float* v, const float* dvdt,
+                                const float* dt, const int32_t* offs, const int32_t* cnt,
+                                const int32_t* list, const float* ap_ij, const float* av_ij,
+                                float* f_ij_out, void* stream);
+
 /* ---------------------------------------------------------------- (d) integrator and dt */
 /* CFL time step (modules/timestep/compressible.py:12-61): dt = min_i cfl*min(H)/(c_i xi),
  * clamped to [min_dt, max_dt] and, when dt_prev != null, to <= dt_growth*dt_prev.

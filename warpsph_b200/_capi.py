@@ -16,6 +16,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libwarpsph_b200.so"
 
 SPH_OK = 0
+SPH_ERR_BAD_ARG = -1
 STATUS_LIST_OVERFLOW = 0x1
 STATUS_NONFINITE = 0x2
 STATUS_NOT_CONVERGED = 0x4
@@ -84,6 +85,7 @@ _PROTOS = {
     "sph_crk_accel": [_P, _I64] + [_P] * 20,
     "sph_crk_dudt": [_P, _I64] + [_P] * 18,
     "sph_compsph_balance": [_P, _I64] + [_P] * 15,
+    "sph_compsph_balance_noalloc": [_P, _I64] + [_P] * 14,
     "sph_cfl_dt": [_P, _I64, _P, _P, _P, _P, _P, _P],
     "sph_rk_combine": [_P, _I64, _P, _I32, _P, _P, _P, _I32, _P, _P],
     "sph_finalize_compatible_energy": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],

@@ -13,6 +13,8 @@
 // same quantity are replaced by multiplications with a reciprocal, so results
 // differ from the CPU oracle by rounding only.
 #include <cuda_runtime.h>
+#include <atomic>
+#include <mutex>
 #include "sph_common.cuh"
 
 namespace wsph {
@@ -929,6 +931,42 @@ static int check_align_vec(const DevParams& P, const void* ptr, const char* name
     return SPH_OK;
 }
 
+// Fixed scratch for sph_compsph_balance_noalloc: n*(dim+1) floats (half-step
+// velocities, then P/rho^gamma).  One copy per device, placed by the module loader,
+// so the entry point that uses it never calls an allocator.  Every element the
+// balance kernel reads is written first by the prep kernel of the same call, so
+// nothing in it has to start at zero.
+static __device__ __align__(256) float g_balance_scratch[SPH_BALANCE_NOALLOC_MAX_FLOATS];
+
+constexpr int kMaxDevices = 64;
+static std::atomic<float*> g_balance_scratch_ptr[kMaxDevices];
+static std::mutex g_balance_scratch_mu;
+
+// Address of g_balance_scratch on the current device, resolved once per device with
+// cudaGetSymbolAddress while that device is current.
+static int balance_scratch_on_current_device(float** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error(SPH_ERR_CUDA, "sph_compsph_balance_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return set_error(SPH_ERR_BAD_ARG, "sph_compsph_balance_noalloc: device %d >= %d", dev, kMaxDevices);
+    float* ptr = g_balance_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (!ptr) {
+        std::lock_guard<std::mutex> lock(g_balance_scratch_mu);
+        ptr = g_balance_scratch_ptr[dev].load(std::memory_order_relaxed);
+        if (!ptr) {
+            void* sym = nullptr;
+            e = cudaGetSymbolAddress(&sym, g_balance_scratch);
+            if (e != cudaSuccess || !sym)
+                return set_error(SPH_ERR_CUDA, "sph_compsph_balance_noalloc: cudaGetSymbolAddress on device %d: %s", dev,
+                                 cudaGetErrorString(e));
+            ptr = static_cast<float*>(sym);
+            g_balance_scratch_ptr[dev].store(ptr, std::memory_order_release);
+        }
+    }
+    *out = ptr;
+    return SPH_OK;
+}
+
 extern "C" {
 
 int sph_density_gather(const SphParams* p, int64_t n, int32_t support_mode, const float* x, const float* H, const float* m,
@@ -1079,6 +1117,29 @@ int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const flo
     wsph::count_launch();
     WSPH_DISPATCH_DS(*p, (k_balance<D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, m, rho, Pr, u, vh, sarr, dt, offs, cnt, list, ap_ij, av_ij, f_ij_out)));
     return check_launch("sph_compsph_balance");
+}
+
+// sph_compsph_balance with its scratch taken from g_balance_scratch instead of the
+// caller.  For callers that cannot allocate device memory on the step path: a plain C
+// or Fortran host code bound through the FFI with no caching allocator of its own, or
+// a timed inner loop, where cudaMalloc/cudaFree would synchronise the whole device.
+// The first call on each device resolves the scratch address (cudaGetSymbolAddress);
+// make that first call before any stream capture.  Calls in flight at the same time on
+// one device (different streams, or different host threads) share the scratch and race.
+int sph_compsph_balance_noalloc(const SphParams* p, int64_t n, const float* m, const float* rho, const float* Pr,
+                                const float* u, const float* v, const float* dvdt, const float* dt, const int32_t* offs,
+                                const int32_t* cnt, const int32_t* list, const float* ap_ij, const float* av_ij,
+                                float* f_ij_out, void* stream) {
+    if (!p) return set_error(SPH_ERR_BAD_ARG, "sph_compsph_balance_noalloc: null params");
+    if (p->dim < 1 || p->dim > 3) return set_error(SPH_ERR_BAD_ARG, "sph_compsph_balance_noalloc: dim must be 1, 2 or 3");
+    if (n > 0 && n * (int64_t)(p->dim + 1) > (int64_t)SPH_BALANCE_NOALLOC_MAX_FLOATS)
+        return set_error(SPH_ERR_BAD_ARG, "sph_compsph_balance_noalloc: n*(dim+1) = %lld exceeds the fixed scratch of %d floats",
+                         (long long)(n * (p->dim + 1)), SPH_BALANCE_NOALLOC_MAX_FLOATS);
+    if (n <= 0) return sph_compsph_balance(p, n, m, rho, Pr, u, v, dvdt, dt, offs, cnt, list, ap_ij, av_ij, nullptr, f_ij_out, stream);
+    float* scratch = nullptr;
+    int rc = balance_scratch_on_current_device(&scratch);
+    if (rc) return rc;
+    return sph_compsph_balance(p, n, m, rho, Pr, u, v, dvdt, dt, offs, cnt, list, ap_ij, av_ij, scratch, f_ij_out, stream);
 }
 
 int sph_cfl_dt(const SphParams* p, int64_t n, const float* H, const float* u, const float* rho, const float* dt_prev,
