@@ -302,6 +302,87 @@ int sph_compsph_balance_noalloc(const SphParams* p, int64_t n, const float* m, c
                                 const int32_t* list, const float* ap_ij, const float* av_ij,
                                 float* f_ij_out, void* stream);
 
+/* ---------------------------------------------------------------- (c) incompressible (DFSPH) */
+/* Relaxed Jacobi solver settings (configurations/moduleConfigurations/solver.py:8-28
+ * RelaxedJacobiSolverConfig) plus the rest density (fluidProperties.restDensity). */
+typedef struct SphJacobiConfig {
+    double rest_density;              /* rho0 */
+    double tolerance;                 /* divergence-free default 2.5e-3, density 5e-4 */
+    double relaxation;                /* omega: 0.3 for both default solvers */
+    int32_t min_iterations;           /* 2 */
+    int32_t max_iterations;           /* divergence-free 32, density 64 */
+    /* 0: the reference's initial pressure (divergence-free: 0.75 * p_init,
+     *    divergenceFree.py:72; density: 0, incompressible.py:79);
+     * 1: p_init is used as given (a learned warm start). */
+    int32_t init_mode;
+    int32_t reserved_i[3];
+} SphJacobiConfig;
+
+/* DFSPH diagonal, the value computeAlpha returns (modules/incompressible/wp_alpha.py:35-118,
+ * :294-313): alpha_out_i = -( (V_i/m_i) |sum_j V_j gradW_ij|^2 + V_i sum_j V_j^2/m_j |gradW_ij|^2 )
+ * with V = m/rho and the gather kernel gradient gradW(x_i - x_j, H_i). */
+int sph_dfsph_alpha(const SphParams* p, int64_t n, const float* x, const float* H, const float* m,
+                    const float* rho, const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                    float* alpha_out, void* stream);
+
+/* computeMomentumIncompressible (modules/momentum/incompressible.py:9-34) of the
+ * predicted velocity v* = v + dt*dvdt (dvdt may be null: v* = v):
+ * div_out_i = -rho0 * sum_j V_j (v*_j - v*_i) . gradW(x_ij, H_j). */
+int sph_incompressible_divergence(const SphParams* p, int64_t n, double rest_density,
+                                  const float* x, const float* H, const float* m, const float* rho,
+                                  const float* v, const float* dvdt, const float* dt,
+                                  const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                                  float* div_out, void* stream);
+
+/* computePressureAccelIISPH (modules/pressure/iisph.py:7-24), scatter support:
+ * a_i = -(rho_i sum_j m_j (p_i/rho_i^2 + p_j/rho_j^2) gradW(x_ij, H_j)) / rho_i. */
+int sph_pressure_accel_iisph(const SphParams* p, int64_t n, const float* x, const float* H,
+                             const float* m, const float* rho, const float* pressure,
+                             const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                             float* accel_out, void* stream);
+
+/* computePressureShiftIISPH (modules/incompressible/drift.py:38-57):
+ * s_i = -sum_j V_j (a_j - a_i) . gradW(x_ij, H_j). */
+int sph_pressure_shift_iisph(const SphParams* p, int64_t n, const float* x, const float* H,
+                             const float* m, const float* rho, const float* accel,
+                             const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                             float* shift_out, void* stream);
+
+/* Workspace bytes of sph_dfsph_div_solve / sph_dfsph_density_solve. */
+int64_t sph_dfsph_workspace_size(int64_t n, int32_t dim);
+
+/* solveDivergenceFree (modules/incompressible/divergenceFree.py:23-139) as ONE
+ * persistent cooperative kernel: source = -div(v + dt dvdt) (above, times -1),
+ * diag = dt*alpha, p0 from p_init (init_mode), then per iteration
+ * a = pressure_accel(p), r = source - dt*pressure_shift(a), p += omega r/diag,
+ * p -= mean(p), error = mean|r|, stop when it >= min_iterations and error < tolerance.
+ * The final pressure acceleration is computed from the last pressure.
+ * Outputs: p_out [n], accel_out [n*dim], history [max_iterations*4] floats
+ * (per iteration: error, min p, max p, mean p after the gauge, as the reference's
+ * `errors` and `pressures` lists), *iterations (device int32) and *status (device
+ * int32; SPH_STATUS_NOT_CONVERGED when the cap was hit, SPH_STATUS_NONFINITE,
+ * SPH_STATUS_TIMEOUT if a grid barrier gave up).  No host synchronisation inside. */
+int sph_dfsph_div_solve(const SphParams* p, const SphJacobiConfig* cfg, int64_t n,
+                        const float* x, const float* H, const float* m, const float* rho,
+                        const float* v, const float* dvdt, const float* p_init, const float* dt,
+                        const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                        void* workspace, int64_t workspace_bytes,
+                        float* p_out, float* accel_out, float* history, int32_t* iterations,
+                        int32_t* status, void* stream);
+
+/* solveIncompressible (modules/incompressible/incompressible.py:21-143), same
+ * structure: rho* = max(rho + dt*div, 0.9), source = rho0 - rho*,
+ * diag = min(dt^2 alpha, -1e-6), p0 = 0 (init_mode 0), per iteration
+ * r = source - dt^2*pressure_shift(a), p = max(p + omega r/diag, 0),
+ * error = mean(max(-r, -tolerance)). */
+int sph_dfsph_density_solve(const SphParams* p, const SphJacobiConfig* cfg, int64_t n,
+                            const float* x, const float* H, const float* m, const float* rho,
+                            const float* v, const float* dvdt, const float* p_init, const float* dt,
+                            const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                            void* workspace, int64_t workspace_bytes,
+                            float* p_out, float* accel_out, float* history, int32_t* iterations,
+                            int32_t* status, void* stream);
+
 /* ---------------------------------------------------------------- (d) integrator and dt */
 /* CFL time step (modules/timestep/compressible.py:12-61): dt = min_i cfl*min(H)/(c_i xi),
  * clamped to [min_dt, max_dt] and, when dt_prev != null, to <= dt_growth*dt_prev.

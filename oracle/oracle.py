@@ -88,6 +88,12 @@ class Oracle:
         L.oracle_cfl_dt.restype = real_c
         L.oracle_finalize_compatible_energy.argtypes = [P, i64, C.c_int, P, real_c, rp, rp, P, P, P, P, P, P, P, rp, rpn]
         L.oracle_kernel_eval.argtypes = [C.c_int, C.c_int, i64, rp, real_c, rp, rp, rp]
+        L.oracle_incompressible_divergence.argtypes = [P, i64, C.c_double, rp, rp, rp, rp, rp, rpn, real_c, _i32p, _i32p, _i32p, rp]
+        L.oracle_dfsph_alpha.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_pressure_accel_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_pressure_shift_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_jacobi_solve.argtypes = [P, C.c_int, P, i64, rp, rp, rp, rp, rp, rpn, rp, real_c, _i32p, _i32p, _i32p, rp, rp,
+                                          _f64p, C.POINTER(C.c_int)]
 
     # ------------------------------------------------------------------ helpers
     def arr(self, a) -> np.ndarray:
@@ -215,6 +221,44 @@ class Oracle:
         self.lib.oracle_finalize_compatible_energy(self._p(params), n, ns, C.cast(w, C.c_void_p), float(dt), self.arr(v0), self.arr(u0),
                                                    ptrs(dv), ptrs(offs), ptrs(cnt), ptrs(lst), ptrs(f), ptrs(ap), ptrs(av), u, du)
         return u, du
+
+    # ------------------------------------------------------------------ incompressible (DFSPH)
+    def incompressible_divergence(self, params, rho0, x, H, m, rho, v, dvdt, dt, nb):
+        out = np.zeros(len(H), self.dtype)
+        self.lib.oracle_incompressible_divergence(self._p(params), len(H), float(rho0), self.arr(x), self.arr(H), self.arr(m),
+                                                  self.arr(rho), self.arr(v), None if dvdt is None else self.arr(dvdt), float(dt),
+                                                  nb["offsets"], nb["counts"], nb["list"], out)
+        return out
+
+    def dfsph_alpha(self, params, x, H, m, rho, nb):
+        out = np.zeros(len(H), self.dtype)
+        self.lib.oracle_dfsph_alpha(self._p(params), len(H), self.arr(x), self.arr(H), self.arr(m), self.arr(rho), nb["offsets"],
+                                    nb["counts"], nb["list"], out)
+        return out
+
+    def pressure_accel_iisph(self, params, x, H, m, rho, pr, nb):
+        out = np.zeros((len(H), params.dim), self.dtype)
+        self.lib.oracle_pressure_accel_iisph(self._p(params), len(H), self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(pr),
+                                             nb["offsets"], nb["counts"], nb["list"], out)
+        return out
+
+    def pressure_shift_iisph(self, params, x, H, m, rho, acc, nb):
+        out = np.zeros(len(H), self.dtype)
+        self.lib.oracle_pressure_shift_iisph(self._p(params), len(H), self.arr(x), self.arr(H), self.arr(m), self.arr(rho),
+                                             self.arr(acc), nb["offsets"], nb["counts"], nb["list"], out)
+        return out
+
+    def jacobi_solve(self, params, mode, cfg, x, H, m, rho, v, dvdt, p_init, dt, nb):
+        """mode 0: solveDivergenceFree, mode 1: solveIncompressible.  cfg is a
+        warpsph_b200._capi.SphJacobiConfig.  Returns (p, accel, history[iters, 4], iters)."""
+        n, d = len(H), params.dim
+        p = np.zeros(n, self.dtype); acc = np.zeros((n, d), self.dtype)
+        hist = np.zeros((max(cfg.max_iterations, 1), 4), np.float64)
+        it = C.c_int(0)
+        self.lib.oracle_jacobi_solve(self._p(params), int(mode), C.c_void_p(C.addressof(cfg)), n, self.arr(x), self.arr(H), self.arr(m),
+                                     self.arr(rho), self.arr(v), None if dvdt is None else self.arr(dvdt), self.arr(p_init), float(dt),
+                                     nb["offsets"], nb["counts"], nb["list"], p, acc, hist, C.byref(it))
+        return p, acc, hist[: it.value], it.value
 
     def kernel_eval(self, kernel, dim, r, H):
         r = self.arr(r)

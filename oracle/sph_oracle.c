@@ -858,6 +858,187 @@ int oracle_finalize_compatible_energy(const SphParams* p, int64_t n, int ns, con
     return 0;
 }
 
+/* ------------------------------------------------------------------ incompressible (DFSPH)
+ * The generic warpSPHCore operations these modules call are restated with the
+ * standard SPH forms (parity with the reference unpinned for those operators):
+ *   Divergence, Difference, consistentDivergence=False:  sum_j V_j (q_j - q_i) . gradW_ij
+ *   Gradient, Symmetric:  rho_i sum_j m_j (q_i/rho_i^2 + q_j/rho_j^2) gradW_ij
+ * with V_j = m_j/rho_j and gradW_ij = grad_i W(x_i - x_j, H) (H_j for scatter, H_i
+ * for gather support). */
+static void kWG_mode(const OP* o, const real* x, real r, real Hi, real Hj, int mode, real* W, real* g) {
+    if (mode == SPH_SUPPORT_GATHER) kWG(o, x, r, Hi, W, g);
+    else kWG(o, x, r, Hj, W, g);
+}
+
+/* modules/momentum/incompressible.py:9-34 with v* = v + dt*dvdt (divergenceFree.py:32) */
+int oracle_incompressible_divergence(const SphParams* p, int64_t n, double rho0, const real* x, const real* H, const real* m,
+                                     const real* rho, const real* v, const real* dvdt, real dt, const int32_t* offs,
+                                     const int32_t* cnt, const int32_t* list, real* div) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real vi[3], s = 0;
+        for (int a = 0; a < D; ++a) vi[a] = dvdt ? v[i * D + a] + dt * dvdt[i * D + a] : v[i * D + a];
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG_mode(&o, d, rsqrt_safe(dotD(d, d, D)), H[i], H[j], SPH_SUPPORT_SCATTER, &W, g);
+            real Vj = m[j] / rho[j], t = 0;
+            for (int a = 0; a < D; ++a) {
+                real vj = dvdt ? v[(int64_t)j * D + a] + dt * dvdt[(int64_t)j * D + a] : v[(int64_t)j * D + a];
+                t += (vj - vi[a]) * g[a];
+            }
+            s += Vj * t;
+        }
+        div[i] = -(real)rho0 * s;
+    }
+    return 0;
+}
+
+/* modules/incompressible/wp_alpha.py:35-118 (gather support, areaI = m_i/rho_i) and
+ * :294-313 (the returned value is -alpha) */
+int oracle_dfsph_alpha(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                       const int32_t* offs, const int32_t* cnt, const int32_t* list, real* alpha) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real sA[3] = {0, 0, 0}, sB = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG_mode(&o, d, rsqrt_safe(dotD(d, d, D)), H[i], H[j], SPH_SUPPORT_GATHER, &W, g);
+            real Vj = m[j] / rho[j];
+            for (int a = 0; a < D; ++a) sA[a] += Vj * g[a];
+            sB += Vj * Vj / m[j] * dotD(g, g, D);
+        }
+        real Ai = m[i] / rho[i];
+        alpha[i] = -(Ai / m[i] * dotD(sA, sA, D) + Ai * sB);
+    }
+    return 0;
+}
+
+/* modules/pressure/iisph.py:7-24 (scatter support) */
+int oracle_pressure_accel_iisph(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                                const real* pr, const int32_t* offs, const int32_t* cnt, const int32_t* list, real* acc) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real s[3] = {0, 0, 0};
+        real qi = pr[i] / (rho[i] * rho[i]);
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG_mode(&o, d, rsqrt_safe(dotD(d, d, D)), H[i], H[j], SPH_SUPPORT_SCATTER, &W, g);
+            real c = m[j] * (qi + pr[j] / (rho[j] * rho[j]));
+            for (int a = 0; a < D; ++a) s[a] += c * g[a];
+        }
+        for (int a = 0; a < D; ++a) acc[i * D + a] = -(rho[i] * s[a]) / rho[i];
+    }
+    return 0;
+}
+
+/* modules/incompressible/drift.py:38-57 */
+int oracle_pressure_shift_iisph(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                                const real* acc, const int32_t* offs, const int32_t* cnt, const int32_t* list, real* shift) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real s = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG_mode(&o, d, rsqrt_safe(dotD(d, d, D)), H[i], H[j], SPH_SUPPORT_SCATTER, &W, g);
+            real t = 0;
+            for (int a = 0; a < D; ++a) t += (acc[(int64_t)j * D + a] - acc[i * D + a]) * g[a];
+            s += m[j] / rho[j] * t;
+        }
+        shift[i] = -s;
+    }
+    return 0;
+}
+
+/* The two relaxed Jacobi solves:
+ *   mode 0: solveDivergenceFree (modules/incompressible/divergenceFree.py:23-139)
+ *   mode 1: solveIncompressible (modules/incompressible/incompressible.py:21-143)
+ * hist[it*4 + {0,1,2,3}] = error, min p, max p, mean p (after the update of iteration it). */
+int oracle_jacobi_solve(const SphParams* p, int mode, const SphJacobiConfig* cfg, int64_t n, const real* x, const real* H,
+                        const real* m, const real* rho, const real* v, const real* dvdt, const real* p_init, real dt,
+                        const int32_t* offs, const int32_t* cnt, const int32_t* list, real* p_out, real* acc_out,
+                        double* hist, int* iters) {
+    int D = p->dim;
+    size_t nn = (size_t)(n > 0 ? n : 1);
+    real* src = (real*)malloc(sizeof(real) * nn);
+    real* diag = (real*)malloc(sizeof(real) * nn);
+    real* pa = (real*)malloc(sizeof(real) * nn);
+    real* sh = (real*)malloc(sizeof(real) * nn);
+    real* acc = (real*)malloc(sizeof(real) * nn * D);
+    real dtf = mode == 0 ? dt : dt * dt;
+    real omega = (real)cfg->relaxation, tol = (real)cfg->tolerance;
+    oracle_incompressible_divergence(p, n, cfg->rest_density, x, H, m, rho, v, dvdt, dt, offs, cnt, list, src);
+    oracle_dfsph_alpha(p, n, x, H, m, rho, offs, cnt, list, diag);
+    for (int64_t i = 0; i < n; ++i) {
+        if (mode == 0) {
+            src[i] = -src[i];                                   /* divergenceFree.py:54 */
+            diag[i] = dt * diag[i];                             /* :62 */
+            p_out[i] = cfg->init_mode ? p_init[i] : p_init[i] * (real)0.75;   /* :72 */
+        } else {
+            real rs = rho[i] + dt * src[i];                     /* incompressible.py:54-56 */
+            rs = rs < (real)0.9 ? (real)0.9 : rs;
+            src[i] = (real)cfg->rest_density - rs;              /* :59 */
+            real a = dt * dt * diag[i];                         /* :68 */
+            diag[i] = a > (real)-1e-6 ? (real)-1e-6 : a;        /* :76 */
+            p_out[i] = cfg->init_mode ? p_init[i] : (real)0;    /* :79 */
+        }
+    }
+    int it = 0;
+    for (it = 0; it < cfg->max_iterations; ++it) {
+        for (int64_t i = 0; i < n; ++i) pa[i] = p_out[i];
+        oracle_pressure_accel_iisph(p, n, x, H, m, rho, pa, offs, cnt, list, acc);
+        oracle_pressure_shift_iisph(p, n, x, H, m, rho, acc, offs, cnt, list, sh);
+        double esum = 0, psum = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            real r = src[i] - dtf * sh[i];
+            real pb = pa[i] + omega * r / diag[i];
+            if (mode == 1) {
+                pb = pb < 0 ? 0 : pb;                           /* incompressible.py:108 */
+                real e = -r < -tol ? -tol : -r;                 /* :111 */
+                esum += (double)e;
+            } else {
+                esum += fabs((double)r);                        /* divergenceFree.py:112 */
+            }
+            p_out[i] = pb;
+            psum += (double)pb;
+        }
+        real mu = mode == 0 && n > 0 ? (real)(psum / (double)n) : 0;
+        real pmin = 0, pmax = 0;
+        double msum = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            if (mode == 0) p_out[i] = p_out[i] - mu;            /* divergenceFree.py:104 */
+            if (i == 0 || p_out[i] < pmin) pmin = p_out[i];
+            if (i == 0 || p_out[i] > pmax) pmax = p_out[i];
+            msum += (double)p_out[i];
+        }
+        double err = n > 0 ? esum / (double)n : 0;
+        hist[it * 4 + 0] = err;
+        hist[it * 4 + 1] = pmin;
+        hist[it * 4 + 2] = pmax;
+        hist[it * 4 + 3] = n > 0 ? msum / (double)n : 0;
+        if (it >= cfg->min_iterations && err < cfg->tolerance) { ++it; break; }
+    }
+    *iters = it < cfg->max_iterations ? it : cfg->max_iterations;
+    oracle_pressure_accel_iisph(p, n, x, H, m, rho, p_out, offs, cnt, list, acc_out);
+    free(src); free(diag); free(pa); free(sh); free(acc);
+    return 0;
+}
+
 /* ------------------------------------------------------------------ helpers exported for tests */
 int oracle_real_size(void) { return (int)sizeof(real); }
 int oracle_kernel_eval(int kernel, int dim, int64_t n, const real* r, real H, real* W, real* dWdr, real* dWdH) {

@@ -425,19 +425,162 @@ def run_reference(ref: Path, case: dict) -> dict:
     return out
 
 
+# ---------------------------------------------------------------- DFSPH pressure solves
+def make_dfsph_case(seed=3, n_side=16):
+    """Periodic unit box, rest density 1, uniform support, a divergent velocity field,
+    gravity plus noise as the non-pressure acceleration and a positive previous pressure."""
+    from oracle import oracle
+    from oracle.steps import cell_capacity_for
+    from tests.cases import make_params, make_particles
+    import warpsph_b200 as ws
+    cfg, sch, p = make_params(2, kernel=ws.KernelFunctions.Wendland4)
+    P = make_particles(2, n_side, seed=seed, jitter=0.3, flow=1.0, h_spread=0.0)
+    n = len(P["masses"])
+    rng = np.random.default_rng(seed + 200)
+    x, H, m = P["positions"], P["supports"], P["masses"]
+    v = (P["velocities"] + 0.5 * x + 0.1 * rng.standard_normal(x.shape)).astype(F)
+    dvdt = (np.array([0.0, -1.0]) + 0.2 * rng.standard_normal(x.shape)).astype(F)
+    p_prev = (0.1 + 0.05 * rng.random(n)).astype(F)
+    o = oracle.get("f32")
+    nb = o.neighbors(p, x, H, cell_capacity_for(n, 2))
+    rho = o.density(p, 0, x, H, m, nb)
+    return dict(params=p, x=x, H=H, m=m, v=v, dvdt=dvdt, p_prev=p_prev, rho=rho, nb=nb, n=n, dt=F(2e-3))
+
+
+def run_reference_dfsph(ref: Path, case: dict) -> dict:
+    """Runs solveDivergenceFree (modules/incompressible/divergenceFree.py) and
+    solveIncompressible (modules/incompressible/incompressible.py) unmodified, with
+    computeAlpha from modules/incompressible/wp_alpha.py (its Warp function body run
+    per particle), computeMomentumIncompressible (modules/momentum/incompressible.py),
+    computePressureAccelIISPH (modules/pressure/iisph.py) and computePressureShiftIISPH
+    (modules/incompressible/drift.py).  The generic operations those call
+    (warpSPHCore warpOperation: symmetric gradient, difference divergence, scatter
+    support) are this project's restatement, in float32 with the oracle's order."""
+    n = case["n"]
+    nb = case["nb"]
+    offs, cnt, lst = nb["offsets"], nb["counts"], nb["list"].astype(np.int64)
+    x, H, m, rho = case["x"], case["H"], case["m"], case["rho"]
+    i_idx = np.repeat(np.arange(n), cnt)
+    # per-pair scatter gradients (H_j) in the oracle's operation order; H is uniform so
+    # the gather gradient of computeAlpha is the same field
+    gS = np.zeros((len(lst), 2), F)
+    for k in range(len(lst)):
+        i, j = i_idx[k], lst[k]
+        d = computeDistanceVec(x[i], x[j])
+        _, g = kWG(d, safe_sqrt(wp.dot(d, d)), H[j])
+        gS[k] = g
+
+    def seg_sum(vals):
+        """Row sums accumulated in list order (float32, like the oracle's loop)."""
+        out = np.zeros((n,) + vals.shape[1:], F)
+        for k in range(len(lst)):
+            out[i_idx[k]] = (out[i_idx[k]] + vals[k]).astype(F)
+        return out
+
+    def warpOperation(state, props, queryValues=None, domain=None, adjacency=None, consistentDivergence=True, **kw):
+        q = queryValues.numpy().astype(F)
+        rj = rho[lst]
+        if props.operation == "Gradient" and props.gradientMode == "Symmetric":
+            qi = (q / (rho * rho)).astype(F)
+            c = (m[lst] * (qi[i_idx] + (q[lst] / (rj * rj)).astype(F))).astype(F)
+            s = seg_sum((c[:, None] * gS).astype(F))
+            return torch.from_numpy((rho[:, None] * s).astype(F))
+        if props.operation == "Divergence" and props.gradientMode == "Difference" and not consistentDivergence:
+            dq = (q[lst] - q[i_idx]).astype(F)
+            t = (dq[:, 0] * gS[:, 0]).astype(F)
+            for a in range(1, dq.shape[1]):
+                t = (t + dq[:, a] * gS[:, a]).astype(F)
+            return torch.from_numpy(seg_sum(((m[lst] / rj).astype(F) * t).astype(F)))
+        raise NotImplementedError((props.operation, props.gradientMode, consistentDivergence))
+
+    class OperationProperties:
+        def __init__(self, kernel=None, operation=None, gradientMode=None, supportMode=None, **kw):
+            self.operation, self.gradientMode = operation, gradientMode
+
+    names = dict(warpOperation=warpOperation, OperationProperties=OperationProperties,
+                 WarpOperation=types.SimpleNamespace(Gradient="Gradient", Divergence="Divergence", Density="Density"),
+                 GradientScheme=types.SimpleNamespace(Symmetric="Symmetric", Difference="Difference"),
+                 SupportScheme=types.SimpleNamespace(Scatter=1, Gather=0), CompressibleState=None, SimulationConfig=None,
+                 AdjacencyList=None, CompactHashMap=None, ParticleState=None, DomainDescription=None, CRKState=None,
+                 GradHState=None, RenormalizationState=None)
+    mom = load(ref, "modules/momentum/incompressible.py", names)
+    iis = load(ref, "modules/pressure/iisph.py", names)
+    dri = load(ref, "modules/incompressible/drift.py", names)
+    state = SoA(positions=x, supports=H, masses=m, densities=rho, kinds=np.zeros(n, np.int32))
+
+    def computeAlphaWarp(queryParticles=None, operationProperties=None, domain=None, adjacency=None, queryApparentAreas=None, **kw):
+        A = queryApparentAreas.numpy().astype(F)
+        out = np.zeros(n, F)
+        for i in range(n):
+            out[i] = alpha_ns["computeAlpha_Func_i_first"](
+                i, 2, x[i], F(H[i]), F(m[i]), F(rho[i]), state, None, SoA(operationMode=0, kernelFunction=2),
+                int(offs[i]), int(cnt[i]), lst, 0, None, False, None, False, F(0), None, False, F(0), None,
+                False, F(1), np.zeros(2, F), np.zeros(2, F), np.zeros((2, 2), F), F(A[i]), A)
+        return torch.from_numpy(out)
+
+    alpha_names = dict(names, computeAlphaWarp=computeAlphaWarp, warpWrapper2=None, launch_kernel=None,
+                       castTorchToWarpAsBuiltins=None, getL_i=None, getGradH_i=None, getVolume_i=None, getCRK_i=None,
+                       checkDirectionality_i=None, checkOffset=None, particleDataSoA=None)
+    alpha_ns = load(ref, "modules/incompressible/wp_alpha.py", alpha_names)
+    alpha_ns["computeAlphaWarp"] = computeAlphaWarp   # the Warp launch wrapper; its per-particle body runs as is
+    solver_names = dict(names, computeAlpha=alpha_ns["computeAlpha"], computeMomentumIncompressible=mom["computeMomentumIncompressible"],
+                        computePressureAccelIISPH=iis["computePressureAccelIISPH"],
+                        computePressureShiftIISPH=dri["computePressureShiftIISPH"])
+    dfs = load(ref, "modules/incompressible/divergenceFree.py", solver_names)
+    inc = load(ref, "modules/incompressible/incompressible.py", solver_names)
+    particles = SoA(positions=torch.from_numpy(x), supports=torch.from_numpy(H), masses=torch.from_numpy(m),
+                    densities=torch.from_numpy(rho), velocities=torch.from_numpy(case["v"]), pressures=torch.from_numpy(case["p_prev"]))
+    conf = SoA(kernel=SoA(value=2), domain=None, dt=float(case["dt"]))
+    out = {}
+    mom_div = mom["computeMomentumIncompressible"](particles, conf, SoA(fluid=SoA(restDensity=1.0)), None, torch.from_numpy(case["v"]))
+    out["alpha"] = alpha_ns["computeAlpha"](particles, conf, None, None, torch.from_numpy((m / rho).astype(F))).numpy()
+    out["divergence"] = mom_div.numpy()
+    pr = torch.from_numpy(case["p_prev"])
+    acc = iis["computePressureAccelIISPH"](particles, pr, conf, 1, None)
+    out["accel_iisph"] = acc.numpy()
+    out["shift_iisph"] = dri["computePressureShiftIISPH"](particles, conf, acc, 1, None).numpy()
+    runs = {"df_fixed": ("divergenceFreeSolver", dfs["solveDivergenceFree"], 2, 6, 0.0, 0.3),
+            "df_default": ("divergenceFreeSolver", dfs["solveDivergenceFree"], 2, 32, 2.5e-3, 0.3),
+            "rho_fixed": ("pressureSolver", inc["solveIncompressible"], 2, 6, 0.0, 0.3),
+            "rho_default": ("pressureSolver", inc["solveIncompressible"], 2, 64, 5e-4, 0.3)}
+    for name, (key, fn, mn, mx, tol, om) in runs.items():
+        solver = SoA(minIterations=mn, maxIterations=mx, tolerance=tol, relaxationFactor=om)
+        sc = SoA(fluid=SoA(restDensity=1.0), solverConfig=SoA(**{key: solver}))
+        with np.errstate(all="ignore"):
+            a_p, pB, errors, pressures = fn(particles, conf, sc, None, torch.from_numpy(case["dvdt"]), float(case["dt"]))
+        out[f"{name}_accel"] = a_p.numpy().astype(F)
+        out[f"{name}_p"] = pB.numpy().astype(F)
+        out[f"{name}_errors"] = np.array(errors, np.float64)
+        out[f"{name}_pressures"] = np.array(pressures, np.float64).reshape(-1, 3)
+        out[f"{name}_config"] = np.array([mn, mx, tol, om], np.float64)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--which", choices=["all", "crk", "dfsph"], default="all")
     a = ap.parse_args()
     ref = Path(a.reference)
-    case = make_case()
-    out = run_reference(ref, case)
-    nb = case["nb"]
-    np.savez_compressed(Path(__file__).parent / "crk_pair_golden.npz",
-                        x=case["x"], H=case["H"], m=case["m"], v=case["v"], u=case["u"], V=case["V"], A=case["A"], B=case["B"],
-                        gA=case["gA"], gB=case["gB"], rho=case["rho"], P=case["P"], c=case["c"], G=case["G"], div=case["div"],
-                        offsets=nb["offsets"], counts=nb["counts"], list=nb["list"], **out)
-    print("wrote", Path(__file__).parent / "crk_pair_golden.npz", "particles", case["n"], "pairs", len(nb["list"]))
+    if a.which in ("all", "crk"):
+        case = make_case()
+        out = run_reference(ref, case)
+        nb = case["nb"]
+        np.savez_compressed(Path(__file__).parent / "crk_pair_golden.npz",
+                            x=case["x"], H=case["H"], m=case["m"], v=case["v"], u=case["u"], V=case["V"], A=case["A"], B=case["B"],
+                            gA=case["gA"], gB=case["gB"], rho=case["rho"], P=case["P"], c=case["c"], G=case["G"], div=case["div"],
+                            offsets=nb["offsets"], counts=nb["counts"], list=nb["list"], **out)
+        print("wrote", Path(__file__).parent / "crk_pair_golden.npz", "particles", case["n"], "pairs", len(nb["list"]))
+    if a.which in ("all", "dfsph"):
+        case = make_dfsph_case()
+        out = run_reference_dfsph(ref, case)
+        nb = case["nb"]
+        np.savez_compressed(Path(__file__).parent / "dfsph_golden.npz",
+                            x=case["x"], H=case["H"], m=case["m"], v=case["v"], dvdt=case["dvdt"], p_prev=case["p_prev"],
+                            rho=case["rho"], dt=np.array([case["dt"]], F), offsets=nb["offsets"], counts=nb["counts"], list=nb["list"],
+                            **out)
+        print("wrote", Path(__file__).parent / "dfsph_golden.npz", "particles", case["n"], "pairs", len(nb["list"]),
+              {k: len(out[k]) for k in out if k.endswith("_errors")})
 
 
 if __name__ == "__main__":

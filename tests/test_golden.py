@@ -82,3 +82,55 @@ def test_golden_compatible_energy(gold, setup, scheme):
                    av=g["av"] * np.float32(1 - 0.1 * s)) for s in range(2)]
     u, du = oracle.get("f32").finalize(p, [0.5, 0.5], float(g["balance_dt"][0]), g["v"], g["u"], stages)
     assert_close(du, g[f"multistep_du_{scheme.name}"], 1e-5, 1e-6, f"du vs reference multistep.py ({scheme.name})")
+
+
+# ---------------------------------------------------------------- DFSPH (tests/golden/dfsph_golden.npz)
+DF_GOLD = Path(__file__).resolve().parent / "golden" / "dfsph_golden.npz"
+
+
+@pytest.fixture(scope="module")
+def dgold():
+    return dict(np.load(DF_GOLD))
+
+
+def jacobi_cfg(g, name):
+    from warpsph_b200._capi import SphJacobiConfig
+    mn, mx, tol, om = g[name + "_config"]
+    c = SphJacobiConfig()
+    c.rest_density, c.tolerance, c.relaxation = 1.0, float(tol), float(om)
+    c.min_iterations, c.max_iterations = int(mn), int(mx)
+    return c
+
+
+def test_golden_dfsph_operators(dgold):
+    """computeAlpha (wp_alpha.py), computeMomentumIncompressible, computePressureAccelIISPH and
+    computePressureShiftIISPH: identical float32 operation order, so exact."""
+    g = dgold
+    cfg, sch, p = make_params(2, kernel=core.KernelFunctions.Wendland4)
+    nb = dict(offsets=g["offsets"], counts=g["counts"], list=g["list"])
+    o = oracle.get("f32")
+    assert_close(o.dfsph_alpha(p, g["x"], g["H"], g["m"], g["rho"], nb), g["alpha"], 1e-6, 1e-7, "computeAlpha")
+    assert_close(o.incompressible_divergence(p, 1.0, g["x"], g["H"], g["m"], g["rho"], g["v"], None, 0.0, nb), g["divergence"],
+                 1e-6, 1e-7, "computeMomentumIncompressible")
+    assert_close(o.pressure_accel_iisph(p, g["x"], g["H"], g["m"], g["rho"], g["p_prev"], nb), g["accel_iisph"], 1e-6, 1e-7,
+                 "computePressureAccelIISPH")
+    assert_close(o.pressure_shift_iisph(p, g["x"], g["H"], g["m"], g["rho"], g["accel_iisph"], nb), g["shift_iisph"], 1e-6, 1e-7,
+                 "computePressureShiftIISPH")
+
+
+@pytest.mark.parametrize("name,mode", [("df_fixed", 0), ("df_default", 0), ("rho_fixed", 1), ("rho_default", 1)])
+def test_golden_dfsph_solves(dgold, name, mode):
+    """solveDivergenceFree / solveIncompressible run from the reference source: the
+    iteration count, the per-iteration errors and pressure statistics, the final
+    pressure and acceleration.  The divergence-free gauge subtracts a mean that torch
+    sums in float32 and the oracle in double: 1e-6 relative."""
+    g = dgold
+    cfg, sch, p = make_params(2, kernel=core.KernelFunctions.Wendland4)
+    nb = dict(offsets=g["offsets"], counts=g["counts"], list=g["list"])
+    pr, acc, hist, it = oracle.get("f32").jacobi_solve(p, mode, jacobi_cfg(g, name), g["x"], g["H"], g["m"], g["rho"], g["v"],
+                                                       g["dvdt"], g["p_prev"], float(g["dt"][0]), nb)
+    assert it == len(g[name + "_errors"])
+    assert_close(hist[:, 0], g[name + "_errors"], 1e-6, 1e-7, f"{name} errors")
+    assert_close(hist[:, 1:], g[name + "_pressures"], 1e-6, 1e-6, f"{name} pressures")
+    assert_close(pr, g[name + "_p"], 1e-6, 1e-6, f"{name} pressure")
+    assert_close(acc, g[name + "_accel"], 1e-6, 1e-6, f"{name} acceleration")

@@ -58,6 +58,20 @@ class SphParams(C.Structure):
     ]
 
 
+class SphJacobiConfig(C.Structure):
+    """Mirror of the C struct SphJacobiConfig (include/warpsph_b200.h)."""
+
+    _fields_ = [
+        ("rest_density", C.c_double),
+        ("tolerance", C.c_double),
+        ("relaxation", C.c_double),
+        ("min_iterations", C.c_int32),
+        ("max_iterations", C.c_int32),
+        ("init_mode", C.c_int32),
+        ("reserved_i", C.c_int32 * 3),
+    ]
+
+
 _P = C.c_void_p
 _I64 = C.c_int64
 _I32 = C.c_int32
@@ -90,8 +104,16 @@ _PROTOS = {
     "sph_rk_combine": [_P, _I64, _P, _I32, _P, _P, _P, _I32, _P, _P],
     "sph_finalize_compatible_energy": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_conservation_sums": [_P, _I64, _P, _P, _P, _P, _P],
+    "sph_dfsph_alpha": [_P, _I64] + [_P] * 9,
+    "sph_incompressible_divergence": [_P, _I64, C.c_double] + [_P] * 12,
+    "sph_pressure_accel_iisph": [_P, _I64] + [_P] * 10,
+    "sph_pressure_shift_iisph": [_P, _I64] + [_P] * 10,
+    "sph_dfsph_workspace_size": [_I64, _I32],
+    "sph_dfsph_div_solve": [_P, _P, _I64] + [_P] * 12 + [_I64] + [_P] * 6,
+    "sph_dfsph_density_solve": [_P, _P, _I64] + [_P] * 12 + [_I64] + [_P] * 6,
 }
-_RESTYPE = {"sph_version": C.c_char_p, "sph_last_error_string": C.c_char_p, "sph_launch_count": C.c_int64}
+_RESTYPE = {"sph_version": C.c_char_p, "sph_last_error_string": C.c_char_p, "sph_launch_count": C.c_int64,
+            "sph_dfsph_workspace_size": C.c_int64}
 
 _lib = None
 

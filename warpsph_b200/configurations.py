@@ -317,6 +317,72 @@ def dictToCRKSPHConfig(d: Dict[str, Any]) -> CRKSPHConfig:
     return c
 
 
+# ------------------------------------------------------------------ incompressible (DFSPH)
+@dataclass
+class RelaxedJacobiSolverConfig:
+    """configurations/moduleConfigurations/solver.py:7-12 (same defaults)."""
+    minIterations: int = 1
+    maxIterations: int = 10
+    tolerance: float = 1e-3
+    relaxationFactor: float = 0.5
+
+
+def buildDefaultPSConfig() -> RelaxedJacobiSolverConfig:
+    """solver.py:15-21: the density (pressure) solver."""
+    return RelaxedJacobiSolverConfig(minIterations=2, maxIterations=64, tolerance=5e-4, relaxationFactor=0.3)
+
+
+def buildDefaultDFConfig() -> RelaxedJacobiSolverConfig:
+    """solver.py:22-28: the divergence-free solver."""
+    return RelaxedJacobiSolverConfig(minIterations=2, maxIterations=32, tolerance=2.5e-3, relaxationFactor=0.3)
+
+
+@dataclass
+class IncompressibleSolverConfig:
+    """solver.py:31-35."""
+    pressureSolver: RelaxedJacobiSolverConfig = field(default_factory=buildDefaultPSConfig)
+    divergenceFreeSolver: RelaxedJacobiSolverConfig = field(default_factory=buildDefaultDFConfig)
+    integrateRho: bool = False
+
+
+def buildDefaultIncompressibleSolverConfig() -> IncompressibleSolverConfig:
+    return IncompressibleSolverConfig(pressureSolver=buildDefaultPSConfig(), divergenceFreeSolver=buildDefaultDFConfig(),
+                                      integrateRho=False)
+
+
+@dataclass
+class fluidProperties:
+    """moduleConfigurations/fluidProperties.py:9-30 (the fields the solves read)."""
+    restDensity: float = 1.0
+    polytropicExponent: Optional[float] = 7.0
+    kappa: Optional[float] = 1.3
+    fixedSoundSpeed: Optional[float] = 10.0
+
+
+def buildDefaultFluidProperties() -> fluidProperties:
+    return fluidProperties(restDensity=1.0, polytropicExponent=7.0, kappa=1.3, fixedSoundSpeed=10.0)
+
+
+@dataclass
+class IncompressibleSPHConfig:
+    """configurations/incompressible.py:32-68, restricted to the fields the pressure
+    solves use (fluid, solverConfig)."""
+    fluid: fluidProperties = field(default_factory=buildDefaultFluidProperties)
+    solverConfig: IncompressibleSolverConfig = field(default_factory=buildDefaultIncompressibleSolverConfig)
+
+
+def jacobi_config(solver: RelaxedJacobiSolverConfig, restDensity: float, learned_init: bool = False) -> _capi.SphJacobiConfig:
+    """Packs a RelaxedJacobiSolverConfig into the C ABI's SphJacobiConfig."""
+    c = _capi.SphJacobiConfig()
+    c.rest_density = float(restDensity)
+    c.tolerance = float(solver.tolerance)
+    c.relaxation = float(solver.relaxationFactor)
+    c.min_iterations = int(solver.minIterations)
+    c.max_iterations = int(solver.maxIterations)
+    c.init_mode = 1 if learned_init else 0
+    return c
+
+
 # ------------------------------------------------------------------ C ABI parameter block
 def make_params(config: SimulationConfig, scheme: Optional[CompressibleSPHConfig] = None) -> _capi.SphParams:
     """Packs the configuration into the C ABI's SphParams (host-side, no device sync

@@ -1,0 +1,105 @@
+// Shared pieces of the pair passes: G lanes of a warp per particle, row-entry
+// decoding for the Verlet (stride 1) and interacting (stride 2) lists, kernel
+// evaluation with a precomputed 1/H, group reductions, and the host-side argument
+// checks and template dispatch of the pair entry points.
+#pragma once
+#include <cuda_runtime.h>
+#include "sph_common.cuh"
+
+namespace wsph {
+
+constexpr int PAIR_BLOCK = 128;
+
+// ---------------------------------------------------------------- group helpers
+template <int G> struct Grp {
+    int i, lane;
+    bool valid;
+    __device__ __forceinline__ explicit Grp(int n) {
+        int t = blockIdx.x * blockDim.x + threadIdx.x;
+        i = t / G;
+        lane = threadIdx.x & (G - 1);
+        valid = i < n;
+    }
+};
+template <int G> __device__ __forceinline__ float gsum(float v) {
+    #pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+template <int G> __device__ __forceinline__ float gmaxw(float v) {
+    #pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v = wmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+template <int ST> __device__ __forceinline__ void entry(const int32_t* __restrict__ list, int q, int& j, int& k) {
+    if constexpr (ST == 2) {
+        int2 e = __ldg(reinterpret_cast<const int2*>(list) + q);
+        j = e.x; k = e.y;
+    } else {
+        j = __ldg(list + q); k = q;
+    }
+}
+template <int G> __host__ __forceinline__ int grid_g(int64_t n) { return (int)((n * G + PAIR_BLOCK - 1) / PAIR_BLOCK); }
+
+// W and grad_i W with a precomputed 1/H.
+template <int KF, int D> __device__ __forceinline__ float kW_inv(float r, float invH) {
+    float q = r * invH;
+    if (!(q < 1.f)) return 0.f;
+    float k, p; kernel_kp<KF, D>(q, k, p);
+    return KernelTraits<KF, D>::C * ipow<D>(invH) * k;
+}
+template <int KF, int D> __device__ __forceinline__ void kWG_inv(const Vec<D>& x, float r, float invH, float& W, Vec<D>& g) {
+    float q = r * invH;
+    if (!(q < 1.f)) { W = 0.f; g = vzero<D>(); return; }
+    float k, p; kernel_kp<KF, D>(q, k, p);
+    float cH = KernelTraits<KF, D>::C * ipow<D>(invH);
+    W = cH * k;
+    float s = -cH * p * (invH * invH);
+    #pragma unroll
+    for (int a = 0; a < D; ++a) g.v[a] = s * x.v[a];
+}
+
+// Neumaier-compensated accumulator (DevParams::kahan).
+struct KSum {
+    float s, c;
+    __device__ __forceinline__ void init() { s = 0.f; c = 0.f; }
+    __device__ __forceinline__ void add(float x, bool comp) {
+        if (!comp) { s += x; return; }
+        float t = s + x;
+        if (fabsf(s) >= fabsf(x)) c += (s - t) + x; else c += (x - t) + s;
+        s = t;
+    }
+};
+
+// group sizes (lanes per particle) of the pair passes
+#define G_LIGHT 8
+#define G_HEAVY 8
+#define G_CRK 4
+
+#define WSPH_DISPATCH_KDS(params, ...)                                                    \
+    if ((params).list_stride == 2) { constexpr int ST = 2; WSPH_DISPATCH_KD(P.kernel, P.dim, __VA_ARGS__) } \
+    else { constexpr int ST = 1; WSPH_DISPATCH_KD(P.kernel, P.dim, __VA_ARGS__) }
+#define WSPH_DISPATCH_DS(params, ...)                                                     \
+    if ((params).list_stride == 2) { constexpr int ST = 2; WSPH_DISPATCH_DIM(P.dim, __VA_ARGS__) } \
+    else { constexpr int ST = 1; WSPH_DISPATCH_DIM(P.dim, __VA_ARGS__) }
+
+#define PAIR_PRELUDE()                                                        \
+    DevParams P;                                                              \
+    int rc = params_to_dev(p, &P);                                            \
+    if (rc) return rc;                                                        \
+    if (n < 0 || n > 0x3fffffff) return set_error(SPH_ERR_BAD_ARG, "%s: n out of range", __func__); \
+    if (p->list_stride < 0 || p->list_stride > 2) return set_error(SPH_ERR_BAD_ARG, "%s: list_stride must be 1 or 2", __func__); \
+    if (n == 0) return SPH_OK;                                                \
+    cudaStream_t s = WSPH_STREAM(stream);                                     \
+    (void)s;
+
+#define CHECK_CSR() do { WSPH_CHECK_PTR(offs); WSPH_CHECK_PTR(cnt); WSPH_CHECK_PTR(list); \
+    if (p->list_stride == 2 && (reinterpret_cast<uintptr_t>(list) & 7)) return set_error(SPH_ERR_BAD_ARG, "%s: interacting list must be 8-byte aligned", __func__); } while (0)
+
+inline int check_align_vec(const DevParams& P, const void* ptr, const char* name) {
+    if (P.dim == 2 && ptr && (reinterpret_cast<uintptr_t>(ptr) & 7))
+        return set_error(SPH_ERR_BAD_ARG, "%s must be 8-byte aligned for dim 2", name);
+    return SPH_OK;
+}
+
+}  // namespace wsph

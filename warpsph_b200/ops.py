@@ -383,3 +383,77 @@ def conservation_sums(params, m, v, u) -> torch.Tensor:
     check(_capi.lib().sph_conservation_sums(_p(params), m.shape[0], fptr(m), fptr(v), fptr(u), ptr(out), stream_ptr(m.device)),
           "sph_conservation_sums")
     return out
+
+
+# ------------------------------------------------------------------ incompressible (DFSPH)
+def dfsph_alpha(params, x, H, m, rho, adj: AdjacencyList) -> torch.Tensor:
+    """computeAlpha (modules/incompressible/wp_alpha.py:294-313): the negative DFSPH diagonal."""
+    out = _empty(m.shape[0], m)
+    with _timed("dfsph_alpha"):
+        check(_capi.lib().sph_dfsph_alpha(_p(params), m.shape[0], fptr(x), fptr(H), fptr(m), fptr(rho), *_lists(params, adj, True),
+                                          ptr(out), stream_ptr(m.device)), "sph_dfsph_alpha")
+    return out
+
+
+def incompressible_divergence(params, rho0, x, H, m, rho, v, adj: AdjacencyList, dvdt=None, dt=None) -> torch.Tensor:
+    """computeMomentumIncompressible (modules/momentum/incompressible.py:9-34) of v + dt*dvdt."""
+    out = _empty(m.shape[0], m)
+    dtt = None if dvdt is None else dt_tensor(dt, m.device)
+    with _timed("incompressible_divergence"):
+        check(_capi.lib().sph_incompressible_divergence(_p(params), m.shape[0], float(rho0), fptr(x), fptr(H), fptr(m), fptr(rho),
+                                                        fptr(v), fptr(dvdt), ptr(dtt), *_lists(params, adj, True), ptr(out),
+                                                        stream_ptr(m.device)), "sph_incompressible_divergence")
+    return out
+
+
+def pressure_accel_iisph(params, x, H, m, rho, pressure, adj: AdjacencyList) -> torch.Tensor:
+    """computePressureAccelIISPH (modules/pressure/iisph.py:7-24)."""
+    out = _empty((m.shape[0], int(params.dim)), m)
+    with _timed("pressure_accel_iisph"):
+        check(_capi.lib().sph_pressure_accel_iisph(_p(params), m.shape[0], fptr(x), fptr(H), fptr(m), fptr(rho), fptr(pressure),
+                                                   *_lists(params, adj, True), ptr(out), stream_ptr(m.device)),
+              "sph_pressure_accel_iisph")
+    return out
+
+
+def pressure_shift_iisph(params, x, H, m, rho, accel, adj: AdjacencyList) -> torch.Tensor:
+    """computePressureShiftIISPH (modules/incompressible/drift.py:38-57)."""
+    out = _empty(m.shape[0], m)
+    with _timed("pressure_shift_iisph"):
+        check(_capi.lib().sph_pressure_shift_iisph(_p(params), m.shape[0], fptr(x), fptr(H), fptr(m), fptr(rho), fptr(accel),
+                                                   *_lists(params, adj, True), ptr(out), stream_ptr(m.device)),
+              "sph_pressure_shift_iisph")
+    return out
+
+
+_jacobi_ws: dict = {}
+
+DIVERGENCE_FREE = 0
+DENSITY = 1
+
+
+def jacobi_solve(params, mode: int, cfg, x, H, m, rho, v, dvdt, p_init, dt, adj: AdjacencyList):
+    """One persistent-kernel relaxed Jacobi solve (mode DIVERGENCE_FREE or DENSITY).
+
+    cfg is a _capi.SphJacobiConfig.  Returns device tensors
+    (pressure [n], accel [n, dim], history [max_iterations, 4], iterations [1] int32,
+    status [1] int32); nothing is synchronised."""
+    n, d = m.shape[0], int(params.dim)
+    key = (m.device.index, n)
+    ws = _jacobi_ws.get(key)
+    need = int(_capi.lib().sph_dfsph_workspace_size(n, d))
+    if ws is None or ws.numel() < need:
+        if len(_jacobi_ws) > 8:
+            _jacobi_ws.clear()
+        ws = torch.empty(need, dtype=torch.uint8, device=m.device)
+        _jacobi_ws[key] = ws
+    pr = _empty(n, m)
+    acc = _empty((n, d), m)
+    hist = torch.zeros((max(int(cfg.max_iterations), 1), 4), device=m.device, dtype=torch.float32)
+    flags = torch.zeros(2, device=m.device, dtype=torch.int32)
+    fn = _capi.lib().sph_dfsph_div_solve if mode == DIVERGENCE_FREE else _capi.lib().sph_dfsph_density_solve
+    with _timed("dfsph_div_solve" if mode == DIVERGENCE_FREE else "dfsph_density_solve"):
+        check(fn(_p(params), C.cast(C.pointer(cfg), C.c_void_p), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(v), fptr(dvdt),
+                 fptr(p_init), ptr(dt_tensor(dt, m.device)), *_lists(params, adj, True), ptr(ws), int(ws.numel()), ptr(pr), ptr(acc),
+                 ptr(hist), ptr(flags), ptr(flags[1:]), stream_ptr(m.device)), "jacobi solve")
+    return pr, acc, hist, flags[:1], flags[1:]
