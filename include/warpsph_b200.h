@@ -48,6 +48,7 @@ extern "C" {
 #define SPH_STATUS_NONFINITE       0x2
 #define SPH_STATUS_NOT_CONVERGED   0x4
 #define SPH_STATUS_TIMEOUT         0x8
+#define SPH_STATUS_LIST_STALE      0x10
 
 /* ---------------------------------------------------------------- enumerations */
 /* Kernel functions (warpSPHCore KernelFunctions; names as used in
@@ -164,6 +165,21 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
                         int32_t* inter_offsets, int32_t* inter_counts, int32_t* inter_list,
                         int64_t inter_capacity, int64_t* inter_nnz_out,
                         int32_t* status, void* stream);
+
+/* Prior-list reuse (the validity check warpSPHCore buildVerletList performs before
+ * rebuilding; its rule is restated here): a list built at (x0, H0) with verlet_scale vs
+ * still holds every pair with |x_i - x_j| < max(H_i, H_j) at (x, H) when
+ * max_k (H_k - vs H0_k) + 2 max_k |x_k - x0_k| <= 0 (a 1e-5 relative margin is kept
+ * for rounding).  When that holds, the interacting sublist for (x, H) is written to
+ * inter_* (same layout as sph_neighbors_build) and *inter_nnz_out receives its size;
+ * otherwise SPH_STATUS_LIST_STALE is or-ed into *status and the caller rebuilds.
+ * scratch: device memory of 4 uint32 words. */
+int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const float* H,
+                          const float* x0, const float* H0,
+                          const int32_t* neighbor_offsets, const int32_t* num_neighbors,
+                          const int32_t* neighbor_list,
+                          int32_t* inter_offsets, int32_t* inter_counts, int32_t* inter_list,
+                          uint32_t* scratch, int64_t* inter_nnz_out, int32_t* status, void* stream);
 
 /* Expands CSR rows into the reference's AdjacencyList.i / .j int64 arrays
  * (io.py:8-20 field names). */

@@ -222,3 +222,41 @@ def test_kahan_option_matches(cuda):
     e_k = np.abs(dv_k.cpu().numpy() - r64[0]).max()
     e_p = np.abs(dv.cpu().numpy() - r64[0]).max()
     assert e_k <= e_p * 1.5 + 1e-7
+
+
+@pytest.mark.parametrize("dim,n_side", CASES)
+def test_prior_list_refresh(cuda, dim, n_side):
+    """A still-valid prior list (small displacement and support change) is kept and its
+    interacting sublist recomputed: per row the same j set as a fresh build, with entry
+    indices pointing at those j in the prior Verlet rows.  A large displacement rebuilds
+    (the result then equals the oracle's list bit for bit)."""
+    cfg, sch, p = make_params(dim)
+    P = make_particles(dim, n_side, seed=90 + dim)
+    G = to_gpu(P, cuda)
+    adj0 = ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale)
+    rng = np.random.default_rng(5)
+    H = P["supports"]
+    x1 = (P["positions"] + (0.02 * H[:, None] * rng.standard_normal(P["positions"].shape)).astype(np.float32)).astype(np.float32)
+    x1 = ((x1 + 0.5) % 1.0 - 0.5).astype(np.float32)
+    H1 = (H * (1 + 0.05 * (rng.random(len(H)) - 0.5))).astype(np.float32)
+    adj1 = ops.buildVerletList(torch.from_numpy(x1).to(cuda), torch.from_numpy(H1).to(cuda), p, p.verlet_scale, adj0)
+    assert adj1.neighborList.data_ptr() == adj0.neighborList.data_ptr(), "valid prior list must be kept"
+    fresh = ops.buildVerletList(torch.from_numpy(x1).to(cuda), torch.from_numpy(H1).to(cuda), p, p.verlet_scale)
+    lst0 = adj0.neighborList.cpu().numpy()
+    il1 = adj1.interList.cpu().numpy().reshape(-1, 2)
+    o1, c1 = adj1.interOffsets.cpu().numpy(), adj1.interCounts.cpu().numpy()
+    il2 = fresh.interList.cpu().numpy().reshape(-1, 2)
+    o2, c2 = fresh.interOffsets.cpu().numpy(), fresh.interCounts.cpu().numpy()
+    assert adj1.interNnz == fresh.interNnz == int(c1.sum())
+    for i in range(len(H)):
+        r1 = il1[o1[i]: o1[i] + c1[i]]
+        r2 = il2[o2[i]: o2[i] + c2[i]]
+        assert set(r1[:, 0].tolist()) == set(r2[:, 0].tolist()), i
+        assert np.array_equal(lst0[r1[:, 1]], r1[:, 0])
+        assert np.all(np.diff(r1[:, 1]) > 0)
+    # beyond the skin: rebuilt, identical to the oracle
+    x2 = (((P["positions"] + 0.5 * H.max()) + 0.5) % 1.0 - 0.5).astype(np.float32)
+    adj2 = ops.buildVerletList(torch.from_numpy(x2).to(cuda), G["supports"], p, p.verlet_scale, adj0)
+    assert adj2.neighborList.data_ptr() != adj0.neighborList.data_ptr()
+    ref = oracle.get("f32").neighbors(p, x2, H, cell_capacity_for(len(H), dim))
+    assert np.array_equal(adj2.neighborList.cpu().numpy(), ref["list"])

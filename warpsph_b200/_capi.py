@@ -21,6 +21,7 @@ STATUS_LIST_OVERFLOW = 0x1
 STATUS_NONFINITE = 0x2
 STATUS_NOT_CONVERGED = 0x4
 STATUS_TIMEOUT = 0x8
+STATUS_LIST_STALE = 0x10
 
 SUPPORT_GATHER = 0
 SUPPORT_SCATTER = 1
@@ -85,6 +86,7 @@ _PROTOS = {
     "sph_neighbors_workspace_size": [_P, _I64, _I64, _P],
     "sph_neighbors_build": [_P, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _P,
                             _P, _P, _P, _I64, _P, _P, _P],
+    "sph_neighbors_refresh": [_P, _I64] + [_P] * 14,
     "sph_neighbors_expand": [_I64, _P, _P, _P, _I64, _P, _P, _P],
     "sph_density_gather": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_adaptive_h_iter": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],

@@ -164,6 +164,10 @@ class AdjacencyList:
     _x_version: Optional[tuple] = field(default=None, repr=False)
     _h_version: Optional[tuple] = field(default=None, repr=False)
     _ij: Optional[tuple] = field(default=None, repr=False)
+    # positions / supports the Verlet rows were built from (for the validity check)
+    _x0: Optional[torch.Tensor] = field(default=None, repr=False)
+    _h0: Optional[torch.Tensor] = field(default=None, repr=False)
+    _dim: int = field(default=0, repr=False)
 
     @property
     def edgeOffsets(self) -> torch.Tensor:

@@ -642,6 +642,90 @@ static int max_bits_for(int dim, int64_t cap) {
     return mb > lim ? lim : mb;
 }
 
+// ---------------------------------------------------------------- prior-list refresh
+// Validity of a Verlet list built at (x0, H0): every pair with |x_i - x_j| < max(H_i, H_j)
+// at (x, H) is in the list when, for every particle k,
+//     H_k + 2 max_l |x_l - x0_l| <= vs H0_k
+// (triangle inequality: r0 <= r + |dx_i| + |dx_j| < H_i + 2 dmax <= vs H0_i <= vs max(H0_i, H0_j)).
+// k_refresh_check reduces max_k |x_k - x0_k|, max_k (H_k - vs H0_k) and max_k vs H0_k into
+// three ordered-encoded words; k_refilter evaluates the criterion (with a relative
+// margin for rounding) and, when it holds, rebuilds the interacting sublist in place of
+// a full neighbour search.
+__device__ __forceinline__ unsigned int ord_enc(float f) {
+    const unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord_dec(unsigned int o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+
+template <int D>
+__global__ void k_refresh_check(const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ x0,
+                                const float* __restrict__ H0, int n, DevParams P, unsigned int* __restrict__ acc3) {
+    float dmax = 0.f, amax = -__int_as_float(0x7f800000), hmax = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Vec<D> d = dist_vec<D>(load_vec<D>(x, i), load_vec<D>(x0, i), P.dom);
+        const float disp = sqrtf(dist2_rn<D>(d));
+        const float h = H[i], h0 = P.verlet_scale * H0[i];
+        // a NaN keeps itself (both comparisons fail afterwards) and forces a rebuild
+        dmax = (disp > dmax || disp != disp) ? disp : dmax;
+        amax = (h - h0 > amax || h != h) ? h - h0 : amax;
+        hmax = h0 > hmax ? h0 : hmax;
+    }
+    unsigned int e0 = ord_enc(dmax), e1 = ord_enc(amax), e2 = ord_enc(hmax);
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        e0 = max(e0, __shfl_xor_sync(0xffffffffu, e0, o));
+        e1 = max(e1, __shfl_xor_sync(0xffffffffu, e1, o));
+        e2 = max(e2, __shfl_xor_sync(0xffffffffu, e2, o));
+    }
+    if ((threadIdx.x & 31) == 0) { atomicMax(acc3 + 0, e0); atomicMax(acc3 + 1, e1); atomicMax(acc3 + 2, e2); }
+}
+
+__device__ __forceinline__ bool refresh_valid(const unsigned int* acc3) {
+    const float dmax = ord_dec(acc3[0]), amax = ord_dec(acc3[1]), hmax = ord_dec(acc3[2]);
+    return amax + 2.0002f * dmax + 1e-5f * hmax <= 0.f;   // false for NaN
+}
+
+// One warp per row: the interacting entries (fl(sqrt(r^2)) / max(H_i, H_j) < 1, the test the
+// list builder applies) of the row's Verlet range, compacted in Verlet order as (j, entry).
+template <int D>
+__global__ void k_refilter(const float* __restrict__ x, const float* __restrict__ H, int n, DevParams P,
+                           const unsigned int* __restrict__ acc3, const int32_t* __restrict__ offs,
+                           const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+                           int32_t* __restrict__ ioffs, int32_t* __restrict__ icnt, int2* __restrict__ ilist,
+                           unsigned long long* __restrict__ innz, int32_t* __restrict__ status) {
+    if (!refresh_valid(acc3)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, SPH_STATUS_LIST_STALE);
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const unsigned int lt = (1u << lane) - 1u;
+    unsigned long long total = 0;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
+        const Vec<D> xi = load_vec<D>(x, i);
+        const float Hi = H[i];
+        const int b = offs[i], c = cnt[i];
+        int w = 0;
+        for (int base = 0; base < c; base += 32) {
+            const int k = b + base + lane;
+            bool keep = false;
+            int j = 0;
+            if (base + lane < c) {
+                j = list[k];
+                const Vec<D> d = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+                const float Hm = fmaxf(Hi, __ldg(H + j));
+                keep = __fdiv_rn(sqrtf(dist2_rn<D>(d)), Hm) < 1.f;
+            }
+            const unsigned int bal = __ballot_sync(0xffffffffu, keep);
+            if (keep) ilist[b + w + __popc(bal & lt)] = make_int2(j, k);
+            w += __popc(bal);
+        }
+        if (lane == 0) { ioffs[i] = b; icnt[i] = w; total += (unsigned long long)w; }
+    }
+    if (lane == 0 && total) atomicAdd(innz, total);
+}
+
 }  // namespace wsph
 
 using namespace wsph;
@@ -740,6 +824,39 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
                                                                                 neighbor_list, inter ? reinterpret_cast<int2*>(inter_list) : nullptr,
                                                                                 innz, reinterpret_cast<long long*>(nnz_out), list_capacity)));
     return check_launch("sph_neighbors_build");
+}
+
+int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const float* H, const float* x0, const float* H0,
+                          const int32_t* neighbor_offsets, const int32_t* num_neighbors, const int32_t* neighbor_list,
+                          int32_t* inter_offsets, int32_t* inter_counts, int32_t* inter_list, uint32_t* scratch,
+                          int64_t* inter_nnz_out, int32_t* status, void* stream) {
+    DevParams P;
+    int rc = params_to_dev(p, &P);
+    if (rc) return rc;
+    if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_refresh: n out of range");
+    WSPH_CHECK_PTR(scratch); WSPH_CHECK_PTR(inter_nnz_out); WSPH_CHECK_PTR(status);
+    cudaStream_t s = WSPH_STREAM(stream);
+    cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
+    if (n == 0) return check_launch("sph_neighbors_refresh");
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(x0); WSPH_CHECK_PTR(H0); WSPH_CHECK_PTR(neighbor_offsets);
+    WSPH_CHECK_PTR(num_neighbors); WSPH_CHECK_PTR(neighbor_list); WSPH_CHECK_PTR(inter_offsets); WSPH_CHECK_PTR(inter_counts);
+    WSPH_CHECK_PTR(inter_list);
+    if (P.dim == 2 && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(x0)) & 7))
+        return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
+    if (reinterpret_cast<uintptr_t>(inter_list) & 7) return set_error(SPH_ERR_BAD_ARG, "inter_list must be 8-byte aligned");
+    cudaMemsetAsync(scratch, 0, 3 * sizeof(uint32_t), s);
+    int cblocks = grid_for(n, 256);
+    if (cblocks > 148 * 8) cblocks = 148 * 8;
+    wsph::count_launch();
+    WSPH_DISPATCH_DIM(P.dim, (k_refresh_check<D><<<cblocks, 256, 0, s>>>(x, H, x0, H0, (int)n, P, scratch)));
+    int64_t rblocks = (n + 7) / 8;                 // one warp per row, 8 warps per block
+    if (rblocks > 148 * 32) rblocks = 148 * 32;
+    wsph::count_launch();
+    WSPH_DISPATCH_DIM(P.dim, (k_refilter<D><<<(int)rblocks, 256, 0, s>>>(x, H, (int)n, P, scratch, neighbor_offsets, num_neighbors,
+                                                                        neighbor_list, inter_offsets, inter_counts,
+                                                                        reinterpret_cast<int2*>(inter_list),
+                                                                        reinterpret_cast<unsigned long long*>(inter_nnz_out), status)));
+    return check_launch("sph_neighbors_refresh");
 }
 
 int sph_neighbors_expand(int64_t n, const int32_t* neighbor_offsets, const int32_t* num_neighbors,

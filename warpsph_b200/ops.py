@@ -122,12 +122,19 @@ def cell_capacity_for(n: int, dim: int) -> int:
     return min(cap, 1 << 24)
 
 
+# Reuse still-valid prior lists (sph_neighbors_refresh) instead of rebuilding them.
+REUSE_PRIOR = True
+
+
 def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float,
                     priorNeighborhood: Optional[AdjacencyList] = None, keep_sort: bool = True) -> AdjacencyList:
     """Replaces warpSPHCore buildVerletList (schemes/crkSPH.py:54-58).
 
     An unchanged prior list (same position and support tensors, same version) is
-    returned as is; otherwise the list is rebuilt on the GPU."""
+    returned as is.  A prior list that is still valid for the new positions and
+    supports (sph_neighbors_refresh: no particle moved or grew its support far enough
+    to leave the Verlet skin) keeps its Verlet rows and gets a fresh interacting
+    sublist; otherwise the list is rebuilt on the GPU."""
     x = _f32(x)
     H = _f32(H)
     if priorNeighborhood is not None and priorNeighborhood._x_version == _version(x) and \
@@ -138,6 +145,28 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
     params.verlet_scale = float(verletScale)
     dev = x.device
     L = _capi.lib()
+    prior = priorNeighborhood
+    if REUSE_PRIOR and prior is not None and prior._x0 is not None and prior.numRows == n and \
+            prior.verletScale == float(verletScale) and prior._x0.device == dev and prior._dim == dim:
+        ioffs = torch.empty(n, dtype=torch.int32, device=dev)
+        icnt = torch.empty(n, dtype=torch.int32, device=dev)
+        ilst = torch.empty(2 * max(prior.nnz, 1), dtype=torch.int32, device=dev)
+        flags = torch.zeros(4, dtype=torch.int64, device=dev)   # [inter nnz, status (low half), scratch (2 words)]
+        with _timed("neighbors_refresh"):
+            check(L.sph_neighbors_refresh(_p(params), n, ptr(x), ptr(H), ptr(prior._x0), ptr(prior._h0), ptr(prior.neighborOffsets),
+                                          ptr(prior.numNeighbors), ptr(prior.neighborList), ptr(ioffs), ptr(icnt), ptr(ilst),
+                                          flags.data_ptr() + 16, flags.data_ptr(), flags.data_ptr() + 8, stream_ptr(dev)),
+                  "sph_neighbors_refresh")
+        f = flags[:2].cpu()
+        if not (int(f[1]) & 0xffffffff) & _capi.STATUS_LIST_STALE:
+            adj = AdjacencyList(neighborOffsets=prior.neighborOffsets, numNeighbors=prior.numNeighbors,
+                                neighborList=prior.neighborList, numRows=n, numCols=n, nnz=prior.nnz, sortIndex=prior.sortIndex,
+                                sortedKeys=prior.sortedKeys, grid=prior.grid, queryPositions=x, querySupports=H,
+                                verletScale=float(verletScale), interOffsets=ioffs, interCounts=icnt, interList=ilst[:2 * prior.nnz],
+                                interNnz=int(f[0]))
+            adj._x_version, adj._h_version = _version(x), _version(H)
+            adj._x0, adj._h0, adj._dim = prior._x0, prior._h0, dim
+            return adj
     cap = cell_capacity_for(n, dim)
     wsb = C.c_int64(0)
     check(L.sph_neighbors_workspace_size(_p(params), n, cap, C.byref(wsb)), "sph_neighbors_workspace_size")
@@ -187,6 +216,7 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
                         interOffsets=ioffs, interCounts=icnt, interList=ilst[:2 * nnz], interNnz=innz)
     adj._x_version = _version(x)
     adj._h_version = _version(H)
+    adj._x0, adj._h0, adj._dim = x.clone(), H.clone(), dim   # build-time state for the validity check
     return adj
 
 
