@@ -687,8 +687,10 @@ __device__ __forceinline__ bool refresh_valid(const unsigned int* acc3) {
     return amax + 2.0002f * dmax + 1e-5f * hmax <= 0.f;   // false for NaN
 }
 
-// One warp per row: the interacting entries (fl(sqrt(r^2)) / max(H_i, H_j) < 1, the test the
-// list builder applies) of the row's Verlet range, compacted in Verlet order as (j, entry).
+// Eight lanes per row, four rows per warp: the interacting entries
+// (fl(sqrt(r^2)) / max(H_i, H_j) < 1, the test the list builder applies) of the row's
+// Verlet range, compacted in Verlet order as (j, entry) with a ballot per 8-entry chunk.
+constexpr int RF_G = 8;
 template <int D>
 __global__ void k_refilter(const float* __restrict__ x, const float* __restrict__ H, int n, DevParams P,
                            const unsigned int* __restrict__ acc3, const int32_t* __restrict__ offs,
@@ -700,30 +702,35 @@ __global__ void k_refilter(const float* __restrict__ x, const float* __restrict_
         return;
     }
     const int lane = threadIdx.x & 31;
-    const unsigned int lt = (1u << lane) - 1u;
-    unsigned long long total = 0;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
-        const Vec<D> xi = load_vec<D>(x, i);
-        const float Hi = H[i];
-        const int b = offs[i], c = cnt[i];
-        int w = 0;
-        for (int base = 0; base < c; base += 32) {
-            const int k = b + base + lane;
-            bool keep = false;
-            int j = 0;
-            if (base + lane < c) {
-                j = list[k];
-                const Vec<D> d = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
-                const float Hm = fmaxf(Hi, __ldg(H + j));
-                keep = __fdiv_rn(sqrtf(dist2_rn<D>(d)), Hm) < 1.f;
-            }
-            const unsigned int bal = __ballot_sync(0xffffffffu, keep);
-            if (keep) ilist[b + w + __popc(bal & lt)] = make_int2(j, k);
-            w += __popc(bal);
+    const int sub = lane & (RF_G - 1);
+    const int gshift = lane & ~(RF_G - 1);                 // first lane of this row's group
+    const int64_t ii = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / RF_G;
+    const bool valid = ii < n;
+    const int i = valid ? (int)ii : 0;
+    Vec<D> xi;
+    float Hi = 1.f;
+    int b = 0, c = 0;
+    if (valid) { xi = load_vec<D>(x, i); Hi = H[i]; b = offs[i]; c = cnt[i]; }
+    int w = 0;
+    for (int base = 0; __any_sync(0xffffffffu, base < c); base += RF_G) {
+        const int k = b + base + sub;
+        bool keep = false;
+        int j = 0;
+        if (base + sub < c) {
+            j = list[k];
+            const Vec<D> d = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            const float Hm = fmaxf(Hi, __ldg(H + j));
+            keep = __fdiv_rn(sqrtf(dist2_rn<D>(d)), Hm) < 1.f;
         }
-        if (lane == 0) { ioffs[i] = b; icnt[i] = w; total += (unsigned long long)w; }
+        const unsigned int bits = (__ballot_sync(0xffffffffu, keep) >> gshift) & ((1u << RF_G) - 1u);
+        if (keep) ilist[b + w + __popc(bits & ((1u << sub) - 1u))] = make_int2(j, k);
+        w += __popc(bits);
     }
-    if (lane == 0 && total) atomicAdd(innz, total);
+    unsigned long long t = (valid && sub == 0) ? (unsigned long long)w : 0ull;
+    if (valid && sub == 0) { ioffs[i] = b; icnt[i] = w; }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0 && t) atomicAdd(innz, t);
 }
 
 }  // namespace wsph
@@ -849,8 +856,7 @@ int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const f
     if (cblocks > 148 * 8) cblocks = 148 * 8;
     wsph::count_launch();
     WSPH_DISPATCH_DIM(P.dim, (k_refresh_check<D><<<cblocks, 256, 0, s>>>(x, H, x0, H0, (int)n, P, scratch)));
-    int64_t rblocks = (n + 7) / 8;                 // one warp per row, 8 warps per block
-    if (rblocks > 148 * 32) rblocks = 148 * 32;
+    const int64_t rblocks = (n * RF_G + 255) / 256;   // RF_G lanes per row, 256 threads per block
     wsph::count_launch();
     WSPH_DISPATCH_DIM(P.dim, (k_refilter<D><<<(int)rblocks, 256, 0, s>>>(x, H, (int)n, P, scratch, neighbor_offsets, num_neighbors,
                                                                         neighbor_list, inter_offsets, inter_counts,

@@ -135,7 +135,8 @@ def crkSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams:
                                                       S.soundspeeds, S.pressures, DvDx, adjacency)
     # crkSPH.py:324-337
     S.divergence = -drhodt / S.densities
-    dEdt = S.masses * torch.einsum("ij,ij->i", S.velocities, dvdt) + S.masses * dudt
+    # the reference's einsum("ij,ij->i", v, dvdt) as a fused row dot (einsum lowers to a GEMV here)
+    dEdt = S.masses * (S.velocities * dvdt).sum(-1) + S.masses * dudt
     update = CompressibleSystemUpdate(dxdt=S.velocities, dvdt=dvdt, dudt=dudt, drhodt=drhodt, dEdt=dEdt, passive=None)
     # crkSPH.py:341-363
     S.f_ij = ops.compsph_balance(params, S.masses, S.densities, S.pressures, S.internalEnergies, S.velocities, dvdt, dt, adjacency,
