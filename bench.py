@@ -115,6 +115,12 @@ def bytes_accel_dudt(d: int, K: float) -> float:
     return (16 * d + 40 + 8 * d * d) + 4 * d + 4 + K * (4 + 8 * d)
 
 
+# DRAM bytes (read + write) of one k_crk_accel_dudt launch from an ncu capture of the
+# 384^2 case (profiles/k_crk_accel_dudt_sedov2d_384.md), scaled to a launch of n
+# particles by particle count (the pass is per particle, so traffic grows with n).
+ACCEL_TRAFFIC_BYTES_PER_PARTICLE = 292.2e6 / 147456
+
+
 def load_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -268,7 +274,9 @@ def gpu_arm(args, rank: int, world: int):
     peaks = load_peaks()
     achieved = per_particle * n / (ksum["avg_ms"] / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": "k_crk_accel_dudt",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": ACCEL_TRAFFIC_BYTES_PER_PARTICLE * n / 1e9,
+                "traffic_unit": "GB per launch (ncu dram__bytes_read+write, 384^2 capture scaled by particle count)",
+                "kernel": "k_crk_accel_dudt",
                 "algorithmic_bytes_per_particle": per_particle, "model_K": 32, "measured_interacting_per_particle": K_meas,
                 "verlet_entries_per_particle": nnz_per, "avg_launch_ms": ksum["avg_ms"], "launches_timed": ksum["launches"],
                 "peak_source": peaks.get("source")}
