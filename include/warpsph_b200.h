@@ -399,6 +399,42 @@ int sph_dfsph_density_solve(const SphParams* p, const SphJacobiConfig* cfg, int6
                             float* p_out, float* accel_out, float* history, int32_t* iterations,
                             int32_t* status, void* stream);
 
+/* ---------------------------------------------------------------- learned warm start
+ * No counterpart in the reference: a per-particle MLP predicts the initial pressure of
+ * the Jacobi solves (replacing 0.75 p_prev at divergenceFree.py:72 and 0 at
+ * incompressible.py:79); the solve then iterates to the same tolerance (init_mode 1).
+ * Network: 8 -> 64 -> 64 -> 64 -> 1, ReLU; FP32 master parameters
+ *   W1[64][8] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4[1]
+ * BF16 weights and activations into the tensor cores, FP32 accumulation. */
+#define SPH_MLP_PARAM_COUNT 8961
+int64_t sph_mlp_param_count(void);
+
+/* Input features of the solve `mode` (0 divergence-free, 1 density) for the state:
+ * feats_out [n][8] (16-byte aligned): p_jac/P, smoothed p_jac/P, p_prev/P, smoothed
+ * p_prev/P, 100 (rho/rho0 - 1), Shepard deficit, relative neighbour count, relative
+ * diagonal, with p_jac = source/diagonal of that solve and P = mean |p_jac|
+ * (scale_out[0]).  workspace: sph_dfsph_workspace_size(n) bytes, 256-byte aligned. */
+int sph_dfsph_features(const SphParams* p, const SphJacobiConfig* cfg, int32_t mode, int64_t n,
+                       const float* x, const float* H, const float* m, const float* rho,
+                       const float* v, const float* dvdt, const float* p_prev, const float* dt,
+                       const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                       void* workspace, int64_t workspace_bytes,
+                       float* feats_out, float* scale_out, void* stream);
+
+/* out[i] = MLP(feats[i]) * (*scale) (scale may be null: 1). */
+int sph_mlp_forward(const float* params, int64_t n, const float* feats, const float* scale,
+                    float* out, void* stream);
+
+/* Gradient of the mean squared error (1/n) sum_i (MLP(feats_i) - target_i)^2 with
+ * respect to the parameters: grad [SPH_MLP_PARAM_COUNT] is overwritten, *loss receives
+ * sum_i (MLP(feats_i) - target_i)^2 (device double). */
+int sph_mlp_grad(const float* params, int64_t n, const float* feats, const float* target,
+                 float* grad, double* loss, void* stream);
+
+/* One Adam step (Kingma & Ba 2015, bias-corrected; step counts from 1). */
+int sph_mlp_adam(float* params, const float* grad, float* m1, float* m2, int64_t count,
+                 float lr, float beta1, float beta2, float eps, int64_t step, void* stream);
+
 /* ---------------------------------------------------------------- (d) integrator and dt */
 /* CFL time step (modules/timestep/compressible.py:12-61): dt = min_i cfl*min(H)/(c_i xi),
  * clamped to [min_dt, max_dt] and, when dt_prev != null, to <= dt_growth*dt_prev.

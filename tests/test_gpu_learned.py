@@ -1,0 +1,160 @@
+"""Learned warm start on the GPU: the BF16 tensor-core MLP kernels against the CPU
+oracle (forward, the gradient of the mean squared error, Adam), the feature kernel
+against its numpy restatement, training, and what the trained network gains over the
+plain initial pressure on held-out dam-break geometries.
+
+Tolerances: the oracle rounds to BF16 at the same points as the kernels, and the
+remaining differences are FP32 against FP64 accumulation order.  A rounding boundary
+can flip for a few activations, so the comparisons are relative to each block's scale:
+1e-2 for forward outputs and gradients, 1e-5 for the Adam update and 1e-4 for its
+second moment (elementwise FP32; the GPU contracts b2 m + (1 - b2) g^2 into an FMA)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp as omlp
+from oracle import oracle
+from tests.cases import assert_close, make_params, make_particles
+from warpsph_b200 import _capi, core, learned, ops
+from warpsph_b200.core import AdjacencyList
+
+pytestmark = pytest.mark.gpu
+BLOCKS = [("W1", 0, 512), ("b1", 512, 576), ("W2", 576, 4672), ("b2", 4672, 4736), ("W3", 4736, 8832), ("b3", 8832, 8896),
+          ("w4", 8896, 8960), ("b4", 8960, 8961)]
+
+
+def random_net(seed):
+    rng = np.random.default_rng(seed)
+    th = omlp.init_params(seed)
+    th[512:576] = 0.1 * rng.standard_normal(64)       # nonzero biases so every path is exercised
+    th[4672:4736] = 0.1 * rng.standard_normal(64)
+    th[8832:8896] = 0.1 * rng.standard_normal(64)
+    th[8960] = 0.2
+    return th.astype(np.float32)
+
+
+@pytest.mark.parametrize("n", [1, 37, 1000, 20000])
+def test_mlp_forward_matches_oracle(cuda, n):
+    rng = np.random.default_rng(n)
+    th = random_net(1)
+    x = rng.standard_normal((n, 8)).astype(np.float32)
+    ref, _ = omlp.forward(th, x)
+    out = ops.mlp_forward(torch.from_numpy(th).to(cuda), torch.from_numpy(x).to(cuda))
+    assert_close(out.cpu().numpy(), ref, 1e-2, 1e-2, "MLP forward vs oracle")
+    assert np.median(np.abs(out.cpu().numpy() - ref)) <= 1e-3 * np.abs(ref).max()
+    sc = torch.tensor([2.5], device=cuda)
+    out2 = ops.mlp_forward(torch.from_numpy(th).to(cuda), torch.from_numpy(x).to(cuda), sc)
+    assert torch.allclose(out2, 2.5 * out, rtol=1e-6, atol=0)
+
+
+@pytest.mark.parametrize("n", [16, 333, 5000])
+def test_mlp_gradient_matches_oracle(cuda, n):
+    """The gradient check: every parameter block of the kernel's MSE gradient against the
+    oracle's analytic gradient (itself checked against finite differences on the CPU)."""
+    rng = np.random.default_rng(10 + n)
+    th = random_net(2)
+    x = rng.standard_normal((n, 8)).astype(np.float32)
+    t = rng.standard_normal(n).astype(np.float32)
+    gref, lref = omlp.grad(th, x, t)
+    g, loss = ops.mlp_grad(torch.from_numpy(th).to(cuda), torch.from_numpy(x).to(cuda), torch.from_numpy(t).to(cuda))
+    g = g.cpu().numpy()
+    assert abs(float(loss.item()) - lref) <= 1e-2 * lref
+    for name, a, b in BLOCKS:
+        assert_close(g[a:b], gref[a:b], 2e-2, 2e-2, f"d loss / d {name}")
+
+
+def test_mlp_adam_matches_oracle(cuda):
+    rng = np.random.default_rng(3)
+    th = random_net(3)
+    m1 = np.zeros_like(th); m2 = np.zeros_like(th)
+    T, M1, M2 = (torch.from_numpy(a.copy()).to(cuda) for a in (th, m1, m2))
+    for step in range(1, 4):
+        g = (1e-2 * rng.standard_normal(th.shape)).astype(np.float32)
+        th, m1, m2 = omlp.adam(th, g, m1, m2, step, 1e-3)
+        ops.mlp_adam(T, torch.from_numpy(g).to(cuda), M1, M2, step, 1e-3)
+    assert_close(T.cpu().numpy(), th, 1e-5, 1e-6, "Adam parameters")
+    assert_close(M2.cpu().numpy(), m2, 1e-4, 1e-6, "Adam second moment (FMA-contracted on the GPU)")
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_dfsph_features_match_numpy(cuda, mode):
+    """The eight features restated in numpy on the oracle's divergence, alpha and kernel."""
+    cfg, sch, p = make_params(2, kernel=core.KernelFunctions.Wendland4)
+    P = make_particles(2, 20, seed=7, jitter=0.3, h_spread=0.1)
+    rng = np.random.default_rng(8)
+    n = len(P["masses"])
+    x, H, m, v = P["positions"], P["supports"], P["masses"], P["velocities"]
+    dvdt = (0.3 * rng.standard_normal(x.shape)).astype(np.float32)
+    pprev = (0.2 + 0.1 * rng.random(n)).astype(np.float32)
+    o = oracle.get("f32")
+    nb = o.neighbors(p, x, H, 1 << 14)
+    rho = o.density(p, 0, x, H, m, nb)
+    dt, rho0 = np.float32(2e-3), 1.0
+    div = o.incompressible_divergence(p, rho0, x, H, m, rho, v, dvdt, dt, nb)
+    al = o.dfsph_alpha(p, x, H, m, rho, nb)
+    if mode == 0:
+        src, diag = -div, dt * al
+    else:
+        src = np.float32(rho0) - np.maximum(rho + dt * div, np.float32(0.9))
+        diag = np.minimum((dt * dt) * al, np.float32(-1e-6))
+    pj = (src / diag).astype(np.float64)
+    Pref = np.abs(pj).mean()
+    S = np.zeros((n, 3))
+    for i in range(n):
+        row = nb["list"][nb["offsets"][i]: nb["offsets"][i] + nb["counts"][i]]
+        d = x[i] - x[row]
+        d = np.where(d > 0.5, d - 1, np.where(d < -0.5, d + 1, d))
+        W, _, _ = o.kernel_eval(p.kernel, 2, np.linalg.norm(d, axis=1), float(H[i]))
+        w = m[row] / rho[row] * W
+        S[i] = [w.sum(), (w * pj[row]).sum(), (w * pprev[row]).sum()]
+    cnt = nb["counts"].astype(np.float64)
+    ref = np.stack([pj / Pref, S[:, 1] / Pref, pprev / Pref, S[:, 2] / Pref, 100 * (rho / rho0 - 1), S[:, 0] - 1,
+                    cnt / cnt.mean() - 1, diag / diag.mean() - 1], 1)
+    t = {k: torch.from_numpy(np.ascontiguousarray(a)).to(cuda) for k, a in dict(x=x, H=H, m=m, rho=rho, v=v, dvdt=dvdt, pp=pprev).items()}
+    adj = AdjacencyList(neighborOffsets=torch.from_numpy(nb["offsets"]).to(cuda), numNeighbors=torch.from_numpy(nb["counts"]).to(cuda),
+                        neighborList=torch.from_numpy(nb["list"]).to(cuda), numRows=n, numCols=n, nnz=int(nb["nnz"]))
+    c = _capi.SphJacobiConfig()
+    c.rest_density = rho0
+    f, sc = ops.dfsph_features(p, mode, c, t["x"], t["H"], t["m"], t["rho"], t["v"], t["dvdt"], t["pp"], float(dt), adj)
+    assert abs(float(sc.item()) - Pref) <= 1e-4 * Pref
+    for k in range(8):
+        assert_close(f.cpu().numpy()[:, k], ref[:, k], 1e-4, 1e-4, f"feature {k}")
+
+
+def test_training_reduces_loss(cuda):
+    """Adam on the kernels' gradient fits a smooth function of the features."""
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal((20000, 8)).astype(np.float32)
+    y = (np.sin(x[:, 0]) + 0.5 * x[:, 1] * x[:, 2] - 0.3 * np.abs(x[:, 3])).astype(np.float32)
+    X, Y = torch.from_numpy(x).to(cuda), torch.from_numpy(y).to(cuda)
+    net = learned.WarmStartMLP(cuda, seed=0)
+    l0 = net.loss(X, Y)
+    losses = net.fit(X, Y, epochs=25, batch=2048, lr=3e-3)
+    assert losses[-1] < 0.1 * l0 and losses[-1] < losses[0]
+
+
+def test_learned_warm_start_gain(cuda):
+    """What the trained network gains: on dam-break column sizes it was not trained on,
+    the density solve reaches the 0.01 % tolerance in at most 0.7 of the plain solve's
+    iterations, and the divergence-free solve ends the reference's 32-iteration budget
+    with a lower error; both solves still iterate to the same stopping rule.  (With the
+    reference's density error, mean(max(-r, -tol)), a free-surface column often meets
+    the tolerance within a few iterations, so the margin is stated on iterations; wall
+    time is measured by bench.py on larger columns.)"""
+    rng = np.random.default_rng(0)
+    geos = [(float(rng.uniform(0.3, 0.7)), float(rng.uniform(0.6, 1.0)), s) for s in range(6)]
+    data = learned.generate_samples(geos, steps=10, device=cuda, dx=0.02)
+    nets = []
+    for mode in (1, 0):
+        f, tg = data[mode]
+        net = learned.WarmStartMLP(cuda, seed=mode)
+        losses = net.fit(f, tg, epochs=25, batch=4096, lr=2e-3)
+        assert losses[-1] < 0.5 * float(tg.var())
+        nets.append(net)
+    tot = learned.compare_warm_starts([(0.45, 0.85, 100), (0.62, 0.72, 101)], steps=8, nets=(nets[0], nets[1]), device=cuda, dx=0.02)
+    d, df = tot["density"], tot["divergence_free"]
+    assert d["learned"][2] == 0 and d["plain"][2] == 0, d
+    assert d["learned"][0] <= 0.7 * d["plain"][0], d
+    assert df["learned"][0] < df["plain"][0], df

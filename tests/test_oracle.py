@@ -164,3 +164,31 @@ def test_full_step_conserves_mass_momentum_energy(o64):
         st, _, _ = orc.step(st, 2e-4, "rungeKutta2")
     assert abs(E(st) - E0) / E0 < 1e-12
     assert np.max(np.abs(mom(st) - p0)) < 1e-12 * np.sum(st["masses"])
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The MLP oracle's analytic gradient (float64, no BF16 rounding) against central
+    differences of its loss, on every parameter block."""
+    from oracle import mlp
+    rng = np.random.default_rng(1)
+    theta = mlp.init_params(3).astype(np.float64)
+    theta[mlp.NPARAM - 1] = 0.3
+    x = rng.standard_normal((40, 8))
+    t = rng.standard_normal(40)
+    g, _ = mlp.grad(theta, x, t, bf=False)
+    loss = lambda th: np.mean((mlp.forward(th, x, bf=False)[0] - t) ** 2)
+    idx = np.concatenate([rng.choice(np.arange(a, b), 12, replace=False) for a, b in
+                          [(0, 512), (512, 576), (576, 4672), (4672, 4736), (4736, 8832), (8832, 8896), (8896, 8960)]] + [[8960]])
+    for k in idx:
+        e = np.zeros_like(theta)
+        e[k] = 1e-6
+        fd = (loss(theta + e) - loss(theta - e)) / 2e-6
+        assert abs(fd - g[k]) <= 1e-6 + 1e-5 * abs(fd), (k, fd, g[k])
+
+
+def test_mlp_oracle_bf16_rounding():
+    from oracle import mlp
+    a = np.array([1.0, 1.00390625, 1.005859375, -2.5e-3, 3.0e38], np.float32)
+    b = mlp.bf16(a)
+    assert b[0] == 1.0 and b[1] == 1.0 and b[2] == np.float32(1.0078125)   # ties to even, then round up
+    assert np.all(np.abs(b - a) <= np.abs(a) * 2 ** -8)

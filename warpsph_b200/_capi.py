@@ -111,11 +111,17 @@ _PROTOS = {
     "sph_pressure_accel_iisph": [_P, _I64] + [_P] * 10,
     "sph_pressure_shift_iisph": [_P, _I64] + [_P] * 10,
     "sph_dfsph_workspace_size": [_I64, _I32],
+    "sph_dfsph_features": [_P, _P, _I32, _I64] + [_P] * 12 + [_I64] + [_P] * 3,
+    "sph_mlp_param_count": [],
+    "sph_mlp_forward": [_P, _I64, _P, _P, _P, _P],
+    "sph_mlp_grad": [_P, _I64, _P, _P, _P, _P, _P],
+    "sph_mlp_adam": [_P, _P, _P, _P, _I64, C.c_float, C.c_float, C.c_float, C.c_float, _I64, _P],
     "sph_dfsph_div_solve": [_P, _P, _I64] + [_P] * 12 + [_I64] + [_P] * 6,
     "sph_dfsph_density_solve": [_P, _P, _I64] + [_P] * 12 + [_I64] + [_P] * 6,
 }
 _RESTYPE = {"sph_version": C.c_char_p, "sph_last_error_string": C.c_char_p, "sph_launch_count": C.c_int64,
-            "sph_dfsph_workspace_size": C.c_int64}
+            "sph_dfsph_workspace_size": C.c_int64,
+            "sph_mlp_param_count": C.c_int64}
 
 _lib = None
 

@@ -508,6 +508,77 @@ static int dfsph_solve(int mode, const SphParams* p, const SphJacobiConfig* cfg,
     return rc;
 }
 
+// ---------------------------------------------------------------- learned warm start: input features
+// Sums over particles of |src/diag|, the row count and diag (FP64, into the control block).
+__global__ void k_feature_sums(int n, const float* __restrict__ src, const float* __restrict__ diag, const int32_t* __restrict__ cnt,
+                               double* __restrict__ sums3) {
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        a += fabs((double)src[i] / (double)diag[i]);
+        b += (double)cnt[i];
+        c += (double)diag[i];
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o); b += __shfl_xor_sync(0xffffffffu, b, o); c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if ((threadIdx.x & 31) == 0) { atomicAdd(sums3, a); atomicAdd(sums3 + 1, b); atomicAdd(sums3 + 2, c); }
+}
+
+// Eight per-particle features (gather support W(r, H_i), V_j = m_j / rho_j):
+//   0  p_jac_i / P           p_jac = src / diag, the diagonal (one-iteration) Jacobi estimate
+//   1  sum_j V_j W_ij p_jac_j / P
+//   2  p_prev_i / P
+//   3  sum_j V_j W_ij p_prev_j / P
+//   4  100 (rho_i / rho0 - 1)
+//   5  sum_j V_j W_ij - 1    (Shepard deficit: free surface)
+//   6  cnt_i / mean(cnt) - 1
+//   7  diag_i / mean(diag) - 1
+// with P = mean_i |p_jac_i| (written to scale_out[0]); a network output y maps to p = y P.
+template <int KF, int D, int G, int ST>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_features(int n, DevParams P, float rho0, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+           const float* __restrict__ rho, const float* __restrict__ src, const float* __restrict__ diag,
+           const float* __restrict__ p_prev, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
+           const int32_t* __restrict__ list, const double* __restrict__ sums3, float* __restrict__ feats,
+           float* __restrict__ scale_out) {
+    Grp<G> g(n);
+    const float Pref = (float)(sums3[0] / (double)n);
+    const float inv_P = Pref > 0.f ? 1.f / Pref : 0.f;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    if (g.valid) {
+        const int i = g.i;
+        const Vec<D> xi = load_vec<D>(x, i);
+        const float Hi = H[i];
+        const int b = offs[i], e = b + cnt[i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry<ST>(list, q, j, k);
+            const Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            const float w = __ldg(m + j) / __ldg(rho + j) * kernelW<KF, D>(safe_sqrt(dot<D>(xij, xij)), Hi);
+            s0 += w;
+            s1 += w * (__ldg(src + j) / __ldg(diag + j));
+            s2 += w * __ldg(p_prev + j);
+        }
+    }
+    s0 = gsum<G>(s0); s1 = gsum<G>(s1); s2 = gsum<G>(s2);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && scale_out) scale_out[0] = Pref;
+    if (!g.valid || g.lane != 0) return;
+    const int i = g.i;
+    const float mean_cnt = (float)(sums3[1] / (double)n), mean_diag = (float)(sums3[2] / (double)n);
+    float f[8];
+    f[0] = src[i] / diag[i] * inv_P;
+    f[1] = s1 * inv_P;
+    f[2] = p_prev[i] * inv_P;
+    f[3] = s2 * inv_P;
+    f[4] = 100.f * (rho[i] / rho0 - 1.f);
+    f[5] = s0 - 1.f;
+    f[6] = mean_cnt > 0.f ? (float)cnt[i] / mean_cnt - 1.f : 0.f;
+    f[7] = mean_diag != 0.f ? diag[i] / mean_diag - 1.f : 0.f;
+    float4* o = reinterpret_cast<float4*>(feats + (size_t)i * 8);
+    o[0] = make_float4(f[0], f[1], f[2], f[3]);
+    o[1] = make_float4(f[4], f[5], f[6], f[7]);
+}
+
 }  // namespace wsph
 
 using namespace wsph;
@@ -564,6 +635,40 @@ int sph_pressure_shift_iisph(const SphParams* p, int64_t n, const float* x, cons
     WSPH_DISPATCH_KDS(*p, (k_iisph_shift<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
         (int)n, P, x, H, m, rho, accel, offs, cnt, list, shift_out)));
     return check_launch("sph_pressure_shift_iisph");
+}
+
+int sph_dfsph_features(const SphParams* p, const SphJacobiConfig* cfg, int32_t mode, int64_t n, const float* x, const float* H,
+                       const float* m, const float* rho, const float* v, const float* dvdt, const float* p_prev, const float* dt,
+                       const int32_t* offs, const int32_t* cnt, const int32_t* list, void* workspace, int64_t workspace_bytes,
+                       float* feats_out, float* scale_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(cfg); WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(v);
+    WSPH_CHECK_PTR(p_prev); WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(workspace); WSPH_CHECK_PTR(feats_out); WSPH_CHECK_PTR(scale_out);
+    CHECK_CSR();
+    if (mode != 0 && mode != 1) return set_error(SPH_ERR_BAD_ARG, "sph_dfsph_features: mode must be 0 or 1");
+    if (workspace_bytes < dfsph_ws_bytes(n)) return set_error(SPH_ERR_WORKSPACE, "sph_dfsph_features: workspace too small");
+    if (reinterpret_cast<uintptr_t>(workspace) & 255) return set_error(SPH_ERR_BAD_ARG, "sph_dfsph_features: workspace must be 256-byte aligned");
+    if (reinterpret_cast<uintptr_t>(feats_out) & 15) return set_error(SPH_ERR_BAD_ARG, "sph_dfsph_features: feats_out must be 16-byte aligned");
+    if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v")) || (rc = check_align_vec(P, dvdt, "dvdt"))) return rc;
+    char* w = static_cast<char*>(workspace);
+    const size_t nb = align256((size_t)n * sizeof(float));
+    double* sums3 = reinterpret_cast<double*>(w);
+    float* p0 = reinterpret_cast<float*>(w + kCtlBytes);
+    float* src = reinterpret_cast<float*>(w + kCtlBytes + nb);
+    float* diag = reinterpret_cast<float*>(w + kCtlBytes + 2 * nb);
+    cudaError_t e = cudaMemsetAsync(sums3, 0, 3 * sizeof(double), s);
+    if (e != cudaSuccess) return set_error(SPH_ERR_CUDA, "sph_dfsph_features: memset: %s", cudaGetErrorString(e));
+    count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_dfsph_prep<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
+        (int)n, P, mode, (float)cfg->rest_density, x, H, m, rho, v, dvdt, dt, offs, cnt, list, nullptr, nullptr, p_prev, 1, src, diag, p0)));
+    int rb = grid_for(n, 256);
+    if (rb > 148 * 4) rb = 148 * 4;
+    count_launch();
+    k_feature_sums<<<rb, 256, 0, s>>>((int)n, src, diag, cnt, sums3);
+    count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_features<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
+        (int)n, P, (float)cfg->rest_density, x, H, m, rho, src, diag, p_prev, offs, cnt, list, sums3, feats_out, scale_out)));
+    return check_launch("sph_dfsph_features");
 }
 
 int64_t sph_dfsph_workspace_size(int64_t n, int32_t dim) {

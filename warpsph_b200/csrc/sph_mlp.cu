@@ -1,0 +1,405 @@
+// Learned warm start for the DFSPH pressure solves: a per-particle MLP
+//   8 features -> 64 -> 64 -> 64 -> 1, ReLU hidden layers,
+// with FP32 master parameters, BF16 weights and activations into the tensor cores and
+// FP32 accumulation.  No counterpart in the reference: it replaces the initial pressure
+// guess of modules/incompressible/divergenceFree.py:72 (0.75 p_prev) and
+// modules/incompressible/incompressible.py:79 (0).
+//
+// Tensor-core tiles: mma.sync m16n8k16 (BF16 x BF16 -> FP32).  One warp owns 16 samples;
+// a hidden layer is 8 n-tiles x (K/16) k-steps.  The FP32 accumulator fragment of one
+// layer maps onto the BF16 A fragment of the next without leaving registers:
+//   A(k-block kb) = { C(n-tile 2kb)[0:2], C(2kb)[2:4], C(2kb+1)[0:2], C(2kb+1)[2:4] }.
+// The weight-gradient GEMMs dW_l = dZ_l^T H_{l-1} contract over the 16 samples of the warp;
+// their operands are staged transposed in per-warp shared memory.
+//
+// Parameter vector (FP32, SPH_MLP_PARAM_COUNT floats):
+//   W1[64][8] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4[1]
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+#include <mutex>
+#include "sph_common.cuh"
+
+namespace wsph {
+
+constexpr int MLP_IN = 8, MLP_H = 64;
+constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + MLP_H * MLP_IN, OFF_W2 = OFF_B1 + MLP_H, OFF_B2 = OFF_W2 + MLP_H * MLP_H,
+              OFF_W3 = OFF_B2 + MLP_H, OFF_B3 = OFF_W3 + MLP_H * MLP_H, OFF_W4 = OFF_B3 + MLP_H, OFF_B4 = OFF_W4 + MLP_H,
+              MLP_NPARAM = OFF_B4 + 1;
+static_assert(MLP_NPARAM == SPH_MLP_PARAM_COUNT, "parameter layout");
+constexpr int MLP_WARPS = 4;
+constexpr int MLP_THREADS = 32 * MLP_WARPS;
+constexpr int K1 = 16;   // layer-1 K padded to one mma k-step
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ uint32_t lds32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+// Weights staged in shared memory as BF16.  W1s is [64][16] (K zero padded); WT are the
+// transposes used by the backward data GEMMs.
+struct MlpSmemW {
+    __nv_bfloat16 W1[MLP_H * K1];
+    __nv_bfloat16 W2[MLP_H * MLP_H];
+    __nv_bfloat16 W3[MLP_H * MLP_H];
+    float b1[MLP_H], b2[MLP_H], b3[MLP_H], w4[MLP_H];
+    float b4;
+};
+
+__device__ void stage_weights(const float* __restrict__ prm, MlpSmemW& s, __nv_bfloat16* W2T, __nv_bfloat16* W3T) {
+    for (int t = threadIdx.x; t < MLP_H * K1; t += blockDim.x) {
+        const int nrow = t / K1, k = t % K1;
+        s.W1[t] = __float2bfloat16_rn(k < MLP_IN ? prm[OFF_W1 + nrow * MLP_IN + k] : 0.f);
+    }
+    for (int t = threadIdx.x; t < MLP_H * MLP_H; t += blockDim.x) {
+        const int r = t / MLP_H, c = t % MLP_H;
+        const __nv_bfloat16 w2 = __float2bfloat16_rn(prm[OFF_W2 + t]), w3 = __float2bfloat16_rn(prm[OFF_W3 + t]);
+        s.W2[t] = w2;
+        s.W3[t] = w3;
+        if (W2T) { W2T[c * MLP_H + r] = w2; W3T[c * MLP_H + r] = w3; }
+    }
+    for (int t = threadIdx.x; t < MLP_H; t += blockDim.x) {
+        s.b1[t] = prm[OFF_B1 + t]; s.b2[t] = prm[OFF_B2 + t]; s.b3[t] = prm[OFF_B3 + t]; s.w4[t] = prm[OFF_W4 + t];
+    }
+    if (threadIdx.x == 0) s.b4 = prm[OFF_B4];
+}
+
+// One hidden layer with K = 64: C[nt] = A x W^T (W row-major [64 out][64 in]) + bias, ReLU.
+__device__ __forceinline__ void hidden_layer(const uint32_t (&A)[4][4], const __nv_bfloat16* W, const float* bias, int g, int t,
+                                             float (&h)[8][4]) {
+    #pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        const __nv_bfloat16* wr = W + (nt * 8 + g) * MLP_H + 2 * t;
+        #pragma unroll
+        for (int ks = 0; ks < 4; ++ks) mma_bf16(c, A[ks][0], A[ks][1], A[ks][2], A[ks][3], lds32(wr + ks * 16), lds32(wr + ks * 16 + 8));
+        const float bb0 = bias[nt * 8 + 2 * t], bb1 = bias[nt * 8 + 2 * t + 1];
+        h[nt][0] = fmaxf(c[0] + bb0, 0.f); h[nt][1] = fmaxf(c[1] + bb1, 0.f);
+        h[nt][2] = fmaxf(c[2] + bb0, 0.f); h[nt][3] = fmaxf(c[3] + bb1, 0.f);
+    }
+}
+__device__ __forceinline__ void c_to_a(const float (&h)[8][4], uint32_t (&A)[4][4]) {
+    #pragma unroll
+    for (int kb = 0; kb < 4; ++kb) {
+        A[kb][0] = pack_bf16(h[2 * kb][0], h[2 * kb][1]);
+        A[kb][1] = pack_bf16(h[2 * kb][2], h[2 * kb][3]);
+        A[kb][2] = pack_bf16(h[2 * kb + 1][0], h[2 * kb + 1][1]);
+        A[kb][3] = pack_bf16(h[2 * kb + 1][2], h[2 * kb + 1][3]);
+    }
+}
+__device__ __forceinline__ void layer1(const float* __restrict__ feats, int64_t n, int64_t r0, int g, int t, const MlpSmemW& s,
+                                       uint32_t (&A0)[4], float (&h1)[8][4]) {
+    const int64_t ra = r0 + g, rb = r0 + g + 8;
+    float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
+    if (ra < n) { x0 = feats[ra * MLP_IN + 2 * t]; x1 = feats[ra * MLP_IN + 2 * t + 1]; }
+    if (rb < n) { x2 = feats[rb * MLP_IN + 2 * t]; x3 = feats[rb * MLP_IN + 2 * t + 1]; }
+    A0[0] = pack_bf16(x0, x1); A0[1] = pack_bf16(x2, x3); A0[2] = 0u; A0[3] = 0u;
+    #pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        const __nv_bfloat16* wr = s.W1 + (nt * 8 + g) * K1 + 2 * t;
+        mma_bf16(c, A0[0], A0[1], A0[2], A0[3], lds32(wr), lds32(wr + 8));
+        const float bb0 = s.b1[nt * 8 + 2 * t], bb1 = s.b1[nt * 8 + 2 * t + 1];
+        h1[nt][0] = fmaxf(c[0] + bb0, 0.f); h1[nt][1] = fmaxf(c[1] + bb1, 0.f);
+        h1[nt][2] = fmaxf(c[2] + bb0, 0.f); h1[nt][3] = fmaxf(c[3] + bb1, 0.f);
+    }
+}
+// y for rows g (out[0]) and g+8 (out[1]) of the warp tile, valid in lanes with t == 0.
+__device__ __forceinline__ void output_layer(const float (&h3)[8][4], const MlpSmemW& s, int t, float& ya, float& yb) {
+    float pa = 0.f, pb = 0.f;
+    #pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const float w0 = s.w4[nt * 8 + 2 * t], w1 = s.w4[nt * 8 + 2 * t + 1];
+        pa += h3[nt][0] * w0 + h3[nt][1] * w1;
+        pb += h3[nt][2] * w0 + h3[nt][3] * w1;
+    }
+    pa += __shfl_xor_sync(0xffffffffu, pa, 1); pa += __shfl_xor_sync(0xffffffffu, pa, 2);
+    pb += __shfl_xor_sync(0xffffffffu, pb, 1); pb += __shfl_xor_sync(0xffffffffu, pb, 2);
+    ya = pa + s.b4;
+    yb = pb + s.b4;
+}
+
+// ---------------------------------------------------------------- inference
+__global__ void __launch_bounds__(MLP_THREADS)
+k_mlp_forward(const float* __restrict__ prm, int64_t n, const float* __restrict__ feats, const float* __restrict__ scale,
+              float* __restrict__ out) {
+    __shared__ MlpSmemW s;
+    stage_weights(prm, s, nullptr, nullptr);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const float sc = scale ? *scale : 1.f;
+    for (int64_t r0 = ((int64_t)blockIdx.x * MLP_WARPS + warp) * 16; r0 < n; r0 += (int64_t)gridDim.x * MLP_WARPS * 16) {
+        uint32_t A0[4], A[4][4];
+        float h[8][4];
+        layer1(feats, n, r0, g, t, s, A0, h);
+        c_to_a(h, A);
+        hidden_layer(A, s.W2, s.b2, g, t, h);
+        c_to_a(h, A);
+        hidden_layer(A, s.W3, s.b3, g, t, h);
+        float ya, yb;
+        output_layer(h, s, t, ya, yb);
+        if (t == 0) {
+            if (r0 + g < n) out[r0 + g] = ya * sc;
+            if (r0 + g + 8 < n) out[r0 + g + 8] = yb * sc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- training: forward + backward
+// Per warp: transposed BF16 copies of the layer inputs and of dZ for the weight GEMMs.
+struct MlpWarpScratch {
+    __nv_bfloat16 xT[K1 * 16];        // [k][r]
+    __nv_bfloat16 h1T[MLP_H * 16];    // [c][r]
+    __nv_bfloat16 h2T[MLP_H * 16];
+    __nv_bfloat16 dzT[MLP_H * 16];
+};
+struct MlpSmemTrain {
+    MlpSmemW w;
+    __nv_bfloat16 W2T[MLP_H * MLP_H];
+    __nv_bfloat16 W3T[MLP_H * MLP_H];
+    float grad[MLP_NPARAM];
+    MlpWarpScratch ws[MLP_WARPS];
+    double loss[MLP_WARPS];
+};
+
+// Writes the fragment h (rows g, g+8; cols nt*8+2t, +1) transposed into dstT[c][r] as BF16.
+__device__ __forceinline__ void store_T(const float (&h)[8][4], __nv_bfloat16* dstT, int g, int t) {
+    #pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const int c = nt * 8 + 2 * t;
+        dstT[c * 16 + g] = __float2bfloat16_rn(h[nt][0]);
+        dstT[(c + 1) * 16 + g] = __float2bfloat16_rn(h[nt][1]);
+        dstT[c * 16 + g + 8] = __float2bfloat16_rn(h[nt][2]);
+        dstT[(c + 1) * 16 + g + 8] = __float2bfloat16_rn(h[nt][3]);
+    }
+}
+// grad[off + c*K + k] += sum_r dZT[c][r] * HT[k][r] over the warp's 16 samples, c < 64, k < kdim
+// (kdim multiple of 8; HT rows beyond kdim are not read).
+__device__ __forceinline__ void weight_grad(const __nv_bfloat16* dzT, const __nv_bfloat16* HT, int kdim, float* grad, int g, int t) {
+    #pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+        const __nv_bfloat16* ar = dzT + (mt * 16 + g) * 16 + 2 * t;
+        const uint32_t a0 = lds32(ar), a1 = lds32(ar + 8 * 16), a2 = lds32(ar + 8), a3 = lds32(ar + 8 * 16 + 8);
+        for (int nt = 0; nt < kdim / 8; ++nt) {
+            const __nv_bfloat16* br = HT + (nt * 8 + g) * 16 + 2 * t;
+            float c[4] = {0.f, 0.f, 0.f, 0.f};
+            mma_bf16(c, a0, a1, a2, a3, lds32(br), lds32(br + 8));
+            const int row = mt * 16 + g, col = nt * 8 + 2 * t;
+            atomicAdd(grad + row * kdim + col, c[0]);
+            atomicAdd(grad + row * kdim + col + 1, c[1]);
+            atomicAdd(grad + (row + 8) * kdim + col, c[2]);
+            atomicAdd(grad + (row + 8) * kdim + col + 1, c[3]);
+        }
+    }
+}
+// Bias gradient: sum over the 16 rows of the dz fragment (rows g, g+8 in each lane).
+__device__ __forceinline__ void bias_grad(const float (&dz)[8][4], float* gb, int g, int t) {
+    #pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        float s0 = dz[nt][0] + dz[nt][2], s1 = dz[nt][1] + dz[nt][3];
+        #pragma unroll
+        for (int o = 4; o < 32; o <<= 1) { s0 += __shfl_xor_sync(0xffffffffu, s0, o); s1 += __shfl_xor_sync(0xffffffffu, s1, o); }
+        if (g == 0) { atomicAdd(gb + nt * 8 + 2 * t, s0); atomicAdd(gb + nt * 8 + 2 * t + 1, s1); }
+    }
+}
+// dH = dZ x W (W row-major [out][in], WT = its transpose [in][out]): M = 16 samples, N = 64 in, K = 64 out.
+__device__ __forceinline__ void data_grad(const uint32_t (&A)[4][4], const __nv_bfloat16* WT, int g, int t, float (&dh)[8][4]) {
+    #pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        const __nv_bfloat16* br = WT + (nt * 8 + g) * MLP_H + 2 * t;
+        #pragma unroll
+        for (int ks = 0; ks < 4; ++ks) mma_bf16(c, A[ks][0], A[ks][1], A[ks][2], A[ks][3], lds32(br + ks * 16), lds32(br + ks * 16 + 8));
+        dh[nt][0] = c[0]; dh[nt][1] = c[1]; dh[nt][2] = c[2]; dh[nt][3] = c[3];
+    }
+}
+// dz = dh * relu'(z), with z > 0 read back from the BF16 activation hT[c][r].
+__device__ __forceinline__ void relu_mask(float (&dh)[8][4], const __nv_bfloat16* hT, int g, int t) {
+    #pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const int c = nt * 8 + 2 * t;
+        if (!(__bfloat162float(hT[c * 16 + g]) > 0.f)) dh[nt][0] = 0.f;
+        if (!(__bfloat162float(hT[(c + 1) * 16 + g]) > 0.f)) dh[nt][1] = 0.f;
+        if (!(__bfloat162float(hT[c * 16 + g + 8]) > 0.f)) dh[nt][2] = 0.f;
+        if (!(__bfloat162float(hT[(c + 1) * 16 + g + 8]) > 0.f)) dh[nt][3] = 0.f;
+    }
+}
+
+// Mean-squared-error gradient over n samples: grad (FP32, MLP_NPARAM) += d/dtheta of
+// (1/n) sum_r (y_r - target_r)^2, and *loss += sum_r (y_r - target_r)^2 (FP64).
+__global__ void __launch_bounds__(MLP_THREADS)
+k_mlp_grad(const float* __restrict__ prm, int64_t n, const float* __restrict__ feats, const float* __restrict__ target,
+           float* __restrict__ grad, double* __restrict__ loss) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MlpSmemTrain& S = *reinterpret_cast<MlpSmemTrain*>(smem_raw);
+    stage_weights(prm, S.w, S.W2T, S.W3T);
+    for (int q = threadIdx.x; q < MLP_NPARAM; q += blockDim.x) S.grad[q] = 0.f;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    MlpWarpScratch& W = S.ws[warp];
+    const float inv_n = 1.f / (float)n;
+    double lsum = 0.0;
+    for (int64_t r0 = ((int64_t)blockIdx.x * MLP_WARPS + warp) * 16; r0 < n; r0 += (int64_t)gridDim.x * MLP_WARPS * 16) {
+        const int64_t ra = r0 + g, rb = r0 + g + 8;
+        // ---- forward (keeps h3 in FP32, h1/h2/x transposed in BF16)
+        uint32_t A0[4], A[4][4];
+        float h1[8][4], h2[8][4], h3[8][4];
+        layer1(feats, n, r0, g, t, S.w, A0, h1);
+        {   // x^T for dW1 (cols 0..7 real, 8..15 zero)
+            float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
+            if (ra < n) { x0 = feats[ra * MLP_IN + 2 * t]; x1 = feats[ra * MLP_IN + 2 * t + 1]; }
+            if (rb < n) { x2 = feats[rb * MLP_IN + 2 * t]; x3 = feats[rb * MLP_IN + 2 * t + 1]; }
+            W.xT[(2 * t) * 16 + g] = __float2bfloat16_rn(x0);
+            W.xT[(2 * t + 1) * 16 + g] = __float2bfloat16_rn(x1);
+            W.xT[(2 * t) * 16 + g + 8] = __float2bfloat16_rn(x2);
+            W.xT[(2 * t + 1) * 16 + g + 8] = __float2bfloat16_rn(x3);
+        }
+        store_T(h1, W.h1T, g, t);
+        c_to_a(h1, A);
+        hidden_layer(A, S.w.W2, S.w.b2, g, t, h2);
+        store_T(h2, W.h2T, g, t);
+        c_to_a(h2, A);
+        hidden_layer(A, S.w.W3, S.w.b3, g, t, h3);
+        float ya, yb;
+        output_layer(h3, S.w, t, ya, yb);
+        // ---- loss and dy (same value in the four lanes of a row group)
+        const float ta = ra < n ? target[ra] : ya, tb = rb < n ? target[rb] : yb;
+        const float ea = ra < n ? ya - ta : 0.f, eb = rb < n ? yb - tb : 0.f;
+        if (t == 0) lsum += (double)ea * ea + (double)eb * eb;
+        const float dya = 2.f * ea * inv_n, dyb = 2.f * eb * inv_n;
+        // ---- layer 4: dW4 = sum dy h3, db4 = sum dy; dz3 = dy w4 * relu'(z3)
+        float dz[8][4];
+        #pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            const int c = nt * 8 + 2 * t;
+            float s0 = dya * h3[nt][0] + dyb * h3[nt][2], s1 = dya * h3[nt][1] + dyb * h3[nt][3];
+            #pragma unroll
+            for (int o = 4; o < 32; o <<= 1) { s0 += __shfl_xor_sync(0xffffffffu, s0, o); s1 += __shfl_xor_sync(0xffffffffu, s1, o); }
+            if (g == 0) { atomicAdd(S.grad + OFF_W4 + c, s0); atomicAdd(S.grad + OFF_W4 + c + 1, s1); }
+            const float w0 = S.w.w4[c], w1 = S.w.w4[c + 1];
+            dz[nt][0] = h3[nt][0] > 0.f ? dya * w0 : 0.f;
+            dz[nt][1] = h3[nt][1] > 0.f ? dya * w1 : 0.f;
+            dz[nt][2] = h3[nt][2] > 0.f ? dyb * w0 : 0.f;
+            dz[nt][3] = h3[nt][3] > 0.f ? dyb * w1 : 0.f;
+        }
+        {
+            float sd = dya + dyb;
+            #pragma unroll
+            for (int o = 4; o < 32; o <<= 1) sd += __shfl_xor_sync(0xffffffffu, sd, o);
+            if (lane == 0) atomicAdd(S.grad + OFF_B4, sd);
+        }
+        // ---- layer 3
+        bias_grad(dz, S.grad + OFF_B3, g, t);
+        store_T(dz, W.dzT, g, t);
+        __syncwarp();
+        weight_grad(W.dzT, W.h2T, MLP_H, S.grad + OFF_W3, g, t);
+        c_to_a(dz, A);
+        data_grad(A, S.W3T, g, t, dz);       // dz <- dh2
+        relu_mask(dz, W.h2T, g, t);          // dz2
+        __syncwarp();
+        // ---- layer 2
+        bias_grad(dz, S.grad + OFF_B2, g, t);
+        store_T(dz, W.dzT, g, t);
+        __syncwarp();
+        weight_grad(W.dzT, W.h1T, MLP_H, S.grad + OFF_W2, g, t);
+        c_to_a(dz, A);
+        data_grad(A, S.W2T, g, t, dz);       // dh1
+        relu_mask(dz, W.h1T, g, t);          // dz1
+        __syncwarp();
+        // ---- layer 1 (K = 8 real inputs)
+        bias_grad(dz, S.grad + OFF_B1, g, t);
+        store_T(dz, W.dzT, g, t);
+        __syncwarp();
+        weight_grad(W.dzT, W.xT, MLP_IN, S.grad + OFF_W1, g, t);
+        __syncwarp();
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    if (lane == 0) S.loss[warp] = lsum;
+    __syncthreads();
+    for (int q = threadIdx.x; q < MLP_NPARAM; q += blockDim.x) {
+        const float v = S.grad[q];
+        if (v != 0.f) atomicAdd(grad + q, v);
+    }
+    if (threadIdx.x == 0) {
+        double l = 0.0;
+        for (int w = 0; w < MLP_WARPS; ++w) l += S.loss[w];
+        atomicAdd(loss, l);
+    }
+}
+
+// Adam (Kingma & Ba 2015) with bias correction, elementwise over the parameter vector.
+__global__ void k_mlp_adam(float* __restrict__ prm, const float* __restrict__ grad, float* __restrict__ m1, float* __restrict__ m2,
+                           int64_t count, float lr, float beta1, float beta2, float eps, float c1, float c2) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x) {
+        const float gq = grad[q];
+        const float a = beta1 * m1[q] + (1.f - beta1) * gq;
+        const float b = beta2 * m2[q] + (1.f - beta2) * gq * gq;
+        m1[q] = a;
+        m2[q] = b;
+        prm[q] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
+    }
+}
+
+static int train_smem_bytes() { return (int)sizeof(MlpSmemTrain); }
+
+}  // namespace wsph
+
+using namespace wsph;
+
+extern "C" {
+
+int64_t sph_mlp_param_count(void) { return MLP_NPARAM; }
+
+int sph_mlp_forward(const float* params, int64_t n, const float* feats, const float* scale, float* out, void* stream) {
+    if (n < 0) return set_error(SPH_ERR_BAD_ARG, "sph_mlp_forward: n < 0");
+    if (n == 0) return SPH_OK;
+    WSPH_CHECK_PTR(params); WSPH_CHECK_PTR(feats); WSPH_CHECK_PTR(out);
+    if (reinterpret_cast<uintptr_t>(feats) & 7) return set_error(SPH_ERR_BAD_ARG, "sph_mlp_forward: feats must be 8-byte aligned");
+    const int64_t tiles = (n + 16 * MLP_WARPS - 1) / (16 * MLP_WARPS);
+    const int grid = (int)(tiles < 148 * 16 ? tiles : 148 * 16);
+    count_launch();
+    k_mlp_forward<<<grid, MLP_THREADS, 0, WSPH_STREAM(stream)>>>(params, n, feats, scale, out);
+    return check_launch("sph_mlp_forward");
+}
+
+int sph_mlp_grad(const float* params, int64_t n, const float* feats, const float* target, float* grad, double* loss, void* stream) {
+    if (n < 0) return set_error(SPH_ERR_BAD_ARG, "sph_mlp_grad: n < 0");
+    WSPH_CHECK_PTR(params); WSPH_CHECK_PTR(grad); WSPH_CHECK_PTR(loss);
+    cudaStream_t s = WSPH_STREAM(stream);
+    cudaMemsetAsync(grad, 0, sizeof(float) * MLP_NPARAM, s);
+    cudaMemsetAsync(loss, 0, sizeof(double), s);
+    if (n == 0) return check_launch("sph_mlp_grad");
+    WSPH_CHECK_PTR(feats); WSPH_CHECK_PTR(target);
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, train_smem_bytes());
+    });
+    if (attr_err != cudaSuccess) return set_error(SPH_ERR_CUDA, "sph_mlp_grad: shared memory opt-in: %s", cudaGetErrorString(attr_err));
+    const int64_t tiles = (n + 16 * MLP_WARPS - 1) / (16 * MLP_WARPS);
+    const int grid = (int)(tiles < 148 * 2 ? tiles : 148 * 2);
+    count_launch();
+    k_mlp_grad<<<grid, MLP_THREADS, train_smem_bytes(), s>>>(params, n, feats, target, grad, loss);
+    return check_launch("sph_mlp_grad");
+}
+
+int sph_mlp_adam(float* params, const float* grad, float* m1, float* m2, int64_t count, float lr, float beta1, float beta2, float eps,
+                 int64_t step, void* stream) {
+    if (count < 0 || step < 1) return set_error(SPH_ERR_BAD_ARG, "sph_mlp_adam: count < 0 or step < 1");
+    if (count == 0) return SPH_OK;
+    WSPH_CHECK_PTR(params); WSPH_CHECK_PTR(grad); WSPH_CHECK_PTR(m1); WSPH_CHECK_PTR(m2);
+    const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+    count_launch();
+    k_mlp_adam<<<grid_for(count, 256), 256, 0, WSPH_STREAM(stream)>>>(params, grad, m1, m2, count, lr, beta1, beta2, eps, c1, c2);
+    return check_launch("sph_mlp_adam");
+}
+
+}  // extern "C"

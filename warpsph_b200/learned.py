@@ -1,0 +1,309 @@
+"""Learned warm start for the DFSPH pressure solves, and the dam-break case that trains
+and judges it.
+
+The plain solves start from the reference's guesses: 0.75 p_prev for the
+divergence-free solve (modules/incompressible/divergenceFree.py:72) and 0 for the
+density solve (modules/incompressible/incompressible.py:79).  ``WarmStartMLP``
+predicts the initial pressure per particle from eight local features
+(``sph_dfsph_features``).  The prediction is an 8 -> 64 -> 64 -> 64 -> 1 ReLU network
+trained by the library's own BF16 tensor-core kernels: ``sph_mlp_grad`` for the
+gradient and ``sph_mlp_adam`` for the update.  The solve then iterates from that guess
+to the same tolerance, so it remains both the fallback and the judge of the network's
+error (init_mode 1 of the solver).
+
+``DamBreak2D`` is a small incompressible dam break run entirely by the library's
+kernels. Its parts:
+  * Fluid column: the column sits in a tank lined with three layers of fixed boundary
+    particles. These take part in every sum and are solved like fluid, but never move.
+  * Step: the density solve, then the divergence-free solve on the predicted
+    velocity, then symplectic Euler.
+  * Training data: its trajectories over randomised column sizes give the
+    (features, converged pressure) pairs.
+  * Evaluation: it measures iterations and GPU time to tolerance, plain against learned.
+
+There is no counterpart of either in the reference.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from . import _capi, ops
+from .configurations import RelaxedJacobiSolverConfig, jacobi_config, make_params
+from .core import AdjacencyList, DomainDescription, KernelFunctions, volumeToSupportHelper
+
+N_FEATURES = 8
+HIDDEN = 64
+PARAM_COUNT = 8961
+# (name, shape, fan-in) in the parameter vector's order; names starting with "b" are biases
+_SIZES = [("W1", (HIDDEN, N_FEATURES), N_FEATURES), ("b1", (HIDDEN,), 0), ("W2", (HIDDEN, HIDDEN), HIDDEN), ("b2", (HIDDEN,), 0),
+          ("W3", (HIDDEN, HIDDEN), HIDDEN), ("b3", (HIDDEN,), 0), ("w4", (HIDDEN,), HIDDEN), ("b4", (1,), 0)]
+
+
+class WarmStartMLP:
+    """FP32 master parameters plus Adam moments on one device."""
+
+    def __init__(self, device, seed: int = 0):
+        assert int(_capi.lib().sph_mlp_param_count()) == PARAM_COUNT
+        gen = torch.Generator().manual_seed(seed)
+        parts = []
+        for name, shape, fan_in in _SIZES:
+            if name.startswith("b"):
+                parts.append(torch.zeros(shape))
+            else:
+                lim = math.sqrt(6.0 / fan_in)                          # He-uniform
+                parts.append((torch.rand(shape, generator=gen) * 2 - 1) * lim)
+        self.theta = torch.cat([p.reshape(-1) for p in parts]).to(device=device, dtype=torch.float32).contiguous()
+        self.m1 = torch.zeros_like(self.theta)
+        self.m2 = torch.zeros_like(self.theta)
+        self.step = 0
+
+    # -------------------------------------------------------------- training
+    def fit(self, feats: torch.Tensor, targets: torch.Tensor, epochs: int = 30, batch: int = 4096, lr: float = 2e-3,
+            seed: int = 0, lr_decay: float = 0.97) -> List[float]:
+        """Minibatch Adam on the mean squared error; returns the mean loss per epoch."""
+        n = feats.shape[0]
+        gen = torch.Generator(device=feats.device).manual_seed(seed)
+        losses = []
+        for ep in range(epochs):
+            perm = torch.randperm(n, generator=gen, device=feats.device)
+            tot = torch.zeros(1, device=feats.device, dtype=torch.float64)
+            for b0 in range(0, n, batch):
+                idx = perm[b0:b0 + batch]
+                g, l = ops.mlp_grad(self.theta, feats[idx].contiguous(), targets[idx].contiguous())
+                self.step += 1
+                ops.mlp_adam(self.theta, g, self.m1, self.m2, self.step, lr * lr_decay ** ep)
+                tot += l
+            losses.append(float(tot.item()) / n)
+        return losses
+
+    def loss(self, feats, targets) -> float:
+        _, l = ops.mlp_grad(self.theta, feats.contiguous(), targets.contiguous())
+        return float(l.item()) / feats.shape[0]
+
+    # -------------------------------------------------------------- inference
+    def initial_pressure(self, params, mode: int, cfg, x, H, m, rho, v, dvdt, p_prev, dt, adj: AdjacencyList) -> torch.Tensor:
+        feats, scale = ops.dfsph_features(params, mode, cfg, x, H, m, rho, v, dvdt, p_prev, dt, adj)
+        return ops.mlp_forward(self.theta, feats, scale)
+
+    def state_dict(self) -> dict:
+        return {"theta": self.theta.detach().cpu(), "step": self.step}
+
+    def load_state_dict(self, d: dict):
+        self.theta.copy_(d["theta"].to(self.theta.device))
+        self.step = int(d.get("step", 0))
+
+
+# ------------------------------------------------------------------ dam break
+@dataclass
+class SolveStats:
+    mode: int
+    iterations: int
+    ms: float          # GPU time of the solve, including the learned guess when used
+    error: float       # final error in the reference's definition
+    converged: bool
+
+
+@dataclass
+class DamBreak2D:
+    """Fluid column width x height (m) in a tank_w x tank_h tank, spacing dx, gravity g;
+    boundary: three layers of fixed particles under the floor and outside both walls.
+
+    The reference's solves balance a source in density units (rho0 - rho*, or
+    rho0 div v*) against dt^2 div a_p, which carries no density factor: they are
+    consistent for the reference's default restDensity = 1 (configurations/
+    moduleConfigurations/fluidProperties.py:12) and nothing else, so the case runs with
+    rho0 = 1 (pressure in units of rho0 m^2/s^2).  The particle mass makes the kernel
+    sum on the interior lattice equal rho0 exactly, so the column starts at rest density."""
+    width: float = 0.5
+    height: float = 1.0
+    tank_w: float = 1.6
+    tank_h: float = 1.2
+    dx: float = 0.01
+    rho0: float = 1.0
+    g: float = -9.81
+    dt: float = 1e-3
+    target_neighbors: float = 20.0
+    device: str = "cuda"
+    kernel: KernelFunctions = KernelFunctions.Wendland2
+    layers: int = 3
+    seed: int = 0
+    state: dict = field(default_factory=dict)
+
+    def __post_init__(self):
+        dev = torch.device(self.device)
+        dx = self.dx
+        rng = np.random.default_rng(self.seed)
+        nfx, nfy = int(round(self.width / dx)), int(round(self.height / dx))
+        fx, fy = np.meshgrid((np.arange(nfx) + 0.5) * dx, (np.arange(nfy) + 0.5) * dx, indexing="xy")
+        fluid = np.stack([fx.ravel(), fy.ravel()], 1)
+        fluid += 0.02 * dx * (rng.random(fluid.shape) - 0.5)     # break the lattice symmetry slightly
+        bnd = []
+        nbx = int(round(self.tank_w / dx))
+        for k in range(self.layers):
+            xs = (np.arange(-self.layers, nbx + self.layers) + 0.5) * dx
+            bnd.append(np.stack([xs, np.full_like(xs, -(k + 0.5) * dx)], 1))
+            ys = (np.arange(int(round(self.tank_h / dx))) + 0.5) * dx
+            bnd.append(np.stack([np.full_like(ys, -(k + 0.5) * dx), ys], 1))
+            bnd.append(np.stack([np.full_like(ys, self.tank_w + (k + 0.5) * dx), ys], 1))
+        bnd = np.concatenate(bnd, 0)
+        x = np.concatenate([fluid, bnd], 0).astype(np.float32)
+        self.n_fluid, self.n = fluid.shape[0], x.shape[0]
+        pad = (self.layers + 2) * dx
+        self.domain = DomainDescription(torch.tensor([-pad, -pad], device=dev), torch.tensor([self.tank_w + pad, self.tank_h + pad], device=dev),
+                                        torch.tensor([False, False], device=dev), 2)
+        from .configurations import SimulationConfig
+        self.config = SimulationConfig(device=dev, domain=self.domain, dim=2, kernel=self.kernel, verletScale=2.0 ** 0.5,
+                                       targetNeighbors=self.target_neighbors)
+        self.params = make_params(self.config)
+        H = float(volumeToSupportHelper(dx * dx, self.target_neighbors, 2))
+        S = self.state
+        S["x"] = torch.from_numpy(x).to(dev)
+        S["H"] = torch.full((self.n,), H, device=dev)
+        S["m"] = torch.ones(self.n, device=dev)
+        adj = ops.buildVerletList(S["x"], S["H"], self.params, self.config.verletScale)
+        rho_unit = ops.density(self.params, S["x"], S["H"], S["m"], adj)
+        interior = self._interior_index(fluid)
+        S["m"] *= self.rho0 / float(rho_unit[interior].item())
+        S["v"] = torch.zeros((self.n, 2), device=dev)
+        S["p_rho"] = torch.zeros(self.n, device=dev)
+        S["p_df"] = torch.zeros(self.n, device=dev)
+        self.fluid = torch.zeros(self.n, dtype=torch.bool, device=dev)
+        self.fluid[: self.n_fluid] = True
+        self.gvec = torch.zeros((self.n, 2), device=dev)
+        self.gvec[: self.n_fluid, 1] = self.g
+        self.adj = None
+        self.t = 0.0
+
+    def _interior_index(self, fluid: np.ndarray) -> int:
+        """A fluid particle at least three supports away from every free surface and wall."""
+        c = np.array([0.5 * self.width, 0.5 * self.height])
+        return int(np.argmin(np.linalg.norm(fluid - c, axis=1)))
+
+    def _solve(self, mode, cfg, v, dvdt, p_init, rho):
+        S = self.state
+        return ops.jacobi_solve(self.params, mode, cfg, S["x"], S["H"], S["m"], rho, v, dvdt, p_init, self.dt, self.adj)
+
+    def _arm(self, mode, solver: RelaxedJacobiSolverConfig, v, dvdt, p_prev, rho, net: Optional[WarmStartMLP]) -> SolveStats:
+        """One solve of the current state from the plain guess (net None: the reference's
+        rule) or the learned guess, timed on the GPU including the guess."""
+        S = self.state
+        cfg = jacobi_config(solver, self.rho0, learned_init=net is not None)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        p0 = p_prev
+        if net is not None:
+            p0 = net.initial_pressure(self.params, mode, cfg, S["x"], S["H"], S["m"], rho, v, dvdt, p_prev, self.dt, self.adj)
+        pr, acc, hist, it, st = self._solve(mode, cfg, v, dvdt, p0, rho)
+        ev1.record()
+        torch.cuda.synchronize()
+        k = int(it.item())
+        err = float(hist[k - 1, 0].item()) if k > 0 else float("nan")
+        return SolveStats(mode, k, ev0.elapsed_time(ev1), err, (int(st.item()) & _capi.STATUS_NOT_CONVERGED) == 0)
+
+    def step(self, driver: tuple, collect: Optional[dict] = None, compare: Optional[dict] = None):
+        """One DFSPH step: density solve, predicted velocity, divergence-free solve on it,
+        symplectic Euler for the fluid.  ``driver`` = (density, divergence-free)
+        RelaxedJacobiSolverConfig of the solves that advance the state; they start from
+        the previous step's pressure.  ``collect`` (dict of lists) receives the features
+        and the driver's pressures divided by the feature scale (training targets).
+        ``compare`` = {"solvers": (density, div-free configs), "nets": (net_rho, net_df),
+        "stats": list}: before each driver solve the same state is also solved from the
+        plain and the learned guess, and their SolveStats are appended to stats."""
+        S = self.state
+        self.adj = ops.buildVerletList(S["x"], S["H"], self.params, self.config.verletScale, self.adj)
+        rho = ops.density(self.params, S["x"], S["H"], S["m"], self.adj)
+        zero = torch.zeros_like(S["v"])
+        out = {}
+        for mode, v, dvdt, key in ((ops.DENSITY, S["v"], self.gvec, "p_rho"), (ops.DIVERGENCE_FREE, None, zero, "p_df")):
+            if mode == ops.DIVERGENCE_FREE:
+                v = torch.where(self.fluid[:, None], S["v"] + self.dt * (self.gvec + out[ops.DENSITY]), zero).contiguous()
+                vstar = v
+            solver = driver[0] if mode == ops.DENSITY else driver[1]
+            dcfg = jacobi_config(solver, self.rho0, learned_init=True)
+            if compare is not None:
+                ev = compare["solvers"][0] if mode == ops.DENSITY else compare["solvers"][1]
+                net = compare["nets"][0] if mode == ops.DENSITY else compare["nets"][1]
+                compare["stats"].append(("plain", self._arm(mode, ev, v, dvdt, S[key], rho, None)))
+                compare["stats"].append(("learned", self._arm(mode, ev, v, dvdt, S[key], rho, net)))
+            if collect is not None:
+                f, sc = ops.dfsph_features(self.params, mode, dcfg, S["x"], S["H"], S["m"], rho, v, dvdt, S[key], self.dt, self.adj)
+            pr, acc, hist, it, st = self._solve(mode, dcfg, v, dvdt, S[key], rho)
+            out[mode] = acc
+            if collect is not None:
+                collect.setdefault(("feats", mode), []).append(f)
+                collect.setdefault(("target", mode), []).append(pr / sc)
+            S[key] = pr
+        v = torch.where(self.fluid[:, None], vstar + self.dt * out[ops.DIVERGENCE_FREE], zero)
+        S["x"] = (S["x"] + self.dt * v).contiguous()
+        S["v"] = v.contiguous()
+        self.t += self.dt
+
+
+def solver_configs(rho0: float, density_tol_frac: float = 1e-4, div_tol_frac: float = 1e-3, max_iterations: int = 400):
+    """The reference's relaxed-Jacobi settings (solver.py:15-28) with the tolerances of
+    a 0.01 % density error and a 0.1 % divergence error, both normalised by rho0."""
+    return (RelaxedJacobiSolverConfig(minIterations=2, maxIterations=max_iterations, tolerance=density_tol_frac * rho0,
+                                      relaxationFactor=0.3),
+            RelaxedJacobiSolverConfig(minIterations=2, maxIterations=max_iterations, tolerance=div_tol_frac * rho0,
+                                      relaxationFactor=0.3))
+
+
+def driver_configs(rho0: float):
+    """Solves that advance the dam break, warm-started from the previous pressure: the
+    density solve to a tenth of the evaluation tolerance (3000 iterations at most), so
+    its pressures are converged targets; the divergence-free solve for 1000 iterations
+    (in a free-surface column it stalls above 0.1 %, the reference having no free-surface
+    treatment in that solve, so its targets are the pressure after 1000 iterations)."""
+    rho, df = solver_configs(rho0, 1e-5, 1e-4, 3000)
+    df.maxIterations = 1000
+    return rho, df
+
+
+def generate_samples(geometries, steps: int, device="cuda", dx: float = 0.02, dt: float = 1e-3):
+    """(features, targets) per solve mode from dam-break trajectories; ``geometries`` is a
+    list of (width, height, seed)."""
+    collect: dict = {}
+    for (w, h, seed) in geometries:
+        case = DamBreak2D(width=w, height=h, dx=dx, dt=dt, device=device, seed=seed)
+        drv = driver_configs(case.rho0)
+        for _ in range(steps):
+            case.step(drv, collect=collect)
+    out = {}
+    for mode in (0, 1):
+        out[mode] = (torch.cat(collect[("feats", mode)]).contiguous(), torch.cat(collect[("target", mode)]).contiguous())
+    return out
+
+
+def compare_warm_starts(geometries, steps: int, nets, device="cuda", dx: float = 0.02, dt: float = 1e-3, skip: int = 2,
+                        max_iterations: int = 2000, df_budget: int = 32):
+    """Plain against learned initial pressure on the same states, after the first ``skip``
+    steps of each trajectory:
+      density solve: summed iterations and GPU ms to the 0.01 % tolerance (cap
+        ``max_iterations``), and how many solves missed it;
+      divergence-free solve: the error after the reference's budget of ``df_budget``
+        iterations (solver.py:22-28, maxIterations 32), summed, and the GPU ms."""
+    tot = {"density": {"plain": [0, 0.0, 0], "learned": [0, 0.0, 0]},
+           "divergence_free": {"plain": [0.0, 0.0, 0], "learned": [0.0, 0.0, 0]}}
+    for (w, h, seed) in geometries:
+        case = DamBreak2D(width=w, height=h, dx=dx, dt=dt, device=device, seed=seed)
+        drv = driver_configs(case.rho0)
+        rho_ev, df_ev = solver_configs(case.rho0, max_iterations=max_iterations)
+        df_ev = RelaxedJacobiSolverConfig(minIterations=df_budget, maxIterations=df_budget, tolerance=0.0,
+                                          relaxationFactor=df_ev.relaxationFactor)
+        for k in range(steps):
+            cmp = {"solvers": (rho_ev, df_ev), "nets": nets, "stats": []} if k >= skip else None
+            case.step(drv, compare=cmp)
+            if cmp is not None:
+                for arm, st in cmp["stats"]:
+                    if st.mode == ops.DENSITY:
+                        t = tot["density"][arm]
+                        t[0] += st.iterations; t[1] += st.ms; t[2] += int(not st.converged)
+                    else:
+                        t = tot["divergence_free"][arm]
+                        t[0] += st.error; t[1] += st.ms; t[2] += 1
+    return tot

@@ -469,14 +469,7 @@ def jacobi_solve(params, mode: int, cfg, x, H, m, rho, v, dvdt, p_init, dt, adj:
     (pressure [n], accel [n, dim], history [max_iterations, 4], iterations [1] int32,
     status [1] int32); nothing is synchronised."""
     n, d = m.shape[0], int(params.dim)
-    key = (m.device.index, n)
-    ws = _jacobi_ws.get(key)
-    need = int(_capi.lib().sph_dfsph_workspace_size(n, d))
-    if ws is None or ws.numel() < need:
-        if len(_jacobi_ws) > 8:
-            _jacobi_ws.clear()
-        ws = torch.empty(need, dtype=torch.uint8, device=m.device)
-        _jacobi_ws[key] = ws
+    ws = _jacobi_workspace(n, d, m.device)
     pr = _empty(n, m)
     acc = _empty((n, d), m)
     hist = torch.zeros((max(int(cfg.max_iterations), 1), 4), device=m.device, dtype=torch.float32)
@@ -487,3 +480,54 @@ def jacobi_solve(params, mode: int, cfg, x, H, m, rho, v, dvdt, p_init, dt, adj:
                  fptr(p_init), ptr(dt_tensor(dt, m.device)), *_lists(params, adj, True), ptr(ws), int(ws.numel()), ptr(pr), ptr(acc),
                  ptr(hist), ptr(flags), ptr(flags[1:]), stream_ptr(m.device)), "jacobi solve")
     return pr, acc, hist, flags[:1], flags[1:]
+
+
+def _jacobi_workspace(n: int, d: int, device) -> torch.Tensor:
+    key = (device.index, n)
+    ws = _jacobi_ws.get(key)
+    need = int(_capi.lib().sph_dfsph_workspace_size(n, d))
+    if ws is None or ws.numel() < need:
+        if len(_jacobi_ws) > 8:
+            _jacobi_ws.clear()
+        ws = torch.empty(need, dtype=torch.uint8, device=device)
+        _jacobi_ws[key] = ws
+    return ws
+
+
+# ------------------------------------------------------------------ learned warm start
+def dfsph_features(params, mode: int, cfg, x, H, m, rho, v, dvdt, p_prev, dt, adj: AdjacencyList):
+    """The eight warm-start features of solve `mode` and the pressure scale P
+    (feats [n, 8], scale [1]; device tensors, no sync)."""
+    n, d = m.shape[0], int(params.dim)
+    ws = _jacobi_workspace(n, d, m.device)
+    feats = torch.empty((n, 8), device=m.device, dtype=torch.float32)
+    scale = torch.empty(1, device=m.device, dtype=torch.float32)
+    with _timed("dfsph_features"):
+        check(_capi.lib().sph_dfsph_features(_p(params), C.cast(C.pointer(cfg), C.c_void_p), int(mode), n, fptr(x), fptr(H), fptr(m),
+                                             fptr(rho), fptr(v), fptr(dvdt), fptr(p_prev), ptr(dt_tensor(dt, m.device)),
+                                             *_lists(params, adj, True), ptr(ws), int(ws.numel()), ptr(feats), ptr(scale),
+                                             stream_ptr(m.device)), "sph_dfsph_features")
+    return feats, scale
+
+
+def mlp_forward(theta, feats, scale=None) -> torch.Tensor:
+    out = torch.empty(feats.shape[0], device=feats.device, dtype=torch.float32)
+    with _timed("mlp_forward"):
+        check(_capi.lib().sph_mlp_forward(fptr(theta), feats.shape[0], fptr(feats.contiguous()), ptr(scale), ptr(out),
+                                          stream_ptr(feats.device)), "sph_mlp_forward")
+    return out
+
+
+def mlp_grad(theta, feats, target):
+    """(grad [P] float32, loss [1] float64 = sum of squared errors) of the MSE."""
+    g = torch.empty_like(theta)
+    loss = torch.empty(1, device=theta.device, dtype=torch.float64)
+    with _timed("mlp_grad"):
+        check(_capi.lib().sph_mlp_grad(fptr(theta), feats.shape[0], fptr(feats.contiguous()), fptr(target.contiguous()), ptr(g),
+                                       ptr(loss), stream_ptr(theta.device)), "sph_mlp_grad")
+    return g, loss
+
+
+def mlp_adam(theta, grad, m1, m2, step: int, lr: float, beta1=0.9, beta2=0.999, eps=1e-8):
+    check(_capi.lib().sph_mlp_adam(fptr(theta), fptr(grad), fptr(m1), fptr(m2), theta.numel(), float(lr), float(beta1),
+                                   float(beta2), float(eps), int(step), stream_ptr(theta.device)), "sph_mlp_adam")
