@@ -49,12 +49,16 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--breakdown", action="store_true", help="print a per-kernel time breakdown to stderr")
+    ap.add_argument("--no-dfsph", action="store_true", help="skip the DFSPH warm-start comparison")
     return ap.parse_args(argv)
 
 
 # ---------------------------------------------------------------------------- clocks
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    """nvidia-smi samples every 50 ms from start() to stop(); summarise() keeps the samples
+    whose own timestamps fall inside a given wall-clock window (the timed region), so the
+    process start-up happens before the window."""
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
@@ -65,7 +69,7 @@ class ClockSampler:
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "50",
                                           "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, ValueError):
             self.proc = None
@@ -77,9 +81,9 @@ class ClockSampler:
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
 
-    def stop(self) -> dict:
+    def stop(self):
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -87,22 +91,34 @@ class ClockSampler:
             self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
-        sm, smax, reasons = [], [], set()
+
+    def summarise(self, t0: float, t1: float) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        from datetime import datetime
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
+                ts = datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(parts[2]), float(parts[3]), parts[6:10]))
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+        inside = [r for r in rows if t0 - 0.06 <= r[0] <= t1 + 0.06]
+        if not inside and rows:   # a window shorter than the sampling period: the nearest sample after its start
+            after = [r for r in rows if r[0] >= t0]
+            inside = after[:1] if after else rows[-1:]
+        reasons = set()
+        for r in inside:
+            for nm, v in zip(names, r[3]):
                 if v.lower() == "active":
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [r[1] for r in inside]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(r[2] for r in inside) if inside else None,
+                "reasons": sorted(reasons), "samples": len(inside)}
 
 
 # ---------------------------------------------------------------------------- byte model
@@ -192,6 +208,51 @@ def reference_arm(args, rank: int):
     return 0
 
 
+# ---------------------------------------------------------------------------- DFSPH warm start
+def dfsph_warm_start(dev) -> dict:
+    """DFSPH time-to-tolerance, learned warm start against the plain initial pressure.
+
+    2D dam break (tank 1.6 x 1.2 m, three boundary layers, dx = 0.01 m, dt = 1 ms,
+    rho0 = 1, g = -9.81).  The networks are trained by the library's kernels on eight
+    seeded column sizes (0.3-0.7 m wide, 0.6-1.0 m tall, ten steps each), then both
+    initial pressures solve the same states of two held-out columns (steps 3-10) to the
+    0.01 % density tolerance, and for the reference's 32-iteration budget of the
+    divergence-free solve.  Times are CUDA-event GPU ms per solve including the
+    learned guess (features + network)."""
+    import numpy as np
+    import torch
+    from warpsph_b200 import learned
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(0)
+    geos = [(float(rng.uniform(0.3, 0.7)), float(rng.uniform(0.6, 1.0)), s) for s in range(8)]
+    data = learned.generate_samples(geos, steps=10, device=dev, dx=0.01)
+    nets, fit = [], {}
+    for mode in (1, 0):
+        f, tg = data[mode]
+        net = learned.WarmStartMLP(dev, seed=mode)
+        losses = net.fit(f, tg, epochs=25, batch=4096, lr=2e-3)
+        fit[mode] = {"samples": int(f.shape[0]), "final_mse": losses[-1], "target_variance": float(tg.var())}
+        nets.append(net)
+    held = [(0.45, 0.85, 100), (0.62, 0.72, 101)]
+    tot = learned.compare_warm_starts(held, steps=10, nets=(nets[0], nets[1]), device=dev, dx=0.01)
+    d, df = tot["density"], tot["divergence_free"]
+    nsolve = 2 * 8
+    return {
+        "case": "2D dam break, dx 0.01 m (5,000 fluid + 1,218 boundary particles at 0.5 x 1.0 m), 2 held-out columns x 8 steps",
+        "density_solve": {"tolerance": "0.01 % of rho0 (reference error definition)",
+                          "plain": {"iterations_per_solve": d["plain"][0] / nsolve, "ms_per_solve": d["plain"][1] / nsolve,
+                                    "missed_tolerance": d["plain"][2]},
+                          "learned": {"iterations_per_solve": d["learned"][0] / nsolve, "ms_per_solve": d["learned"][1] / nsolve,
+                                      "missed_tolerance": d["learned"][2]},
+                          "time_speedup": d["plain"][1] / max(d["learned"][1], 1e-9)},
+        "divergence_free_solve": {"budget_iterations": 32,
+                                  "plain": {"final_error_mean": df["plain"][0] / nsolve, "ms_per_solve": df["plain"][1] / nsolve},
+                                  "learned": {"final_error_mean": df["learned"][0] / nsolve, "ms_per_solve": df["learned"][1] / nsolve}},
+        "training": {"density": fit[1], "divergence_free": fit[0]},
+        "wall_s": time.perf_counter() - t0,
+    }
+
+
 # ---------------------------------------------------------------------------- GPU arm
 def build_workload(nx, dev):
     import warpsph_b200 as ws
@@ -232,16 +293,17 @@ def gpu_arm(args, rank: int, world: int):
         if world > 1:
             dist.barrier()
 
+    clocks = ClockSampler(dev.index)
+    clocks.start()
     for _ in range(max(args.warmup, 0)):
         one_step()
     torch.cuda.synchronize()
 
     # ------------------------------------------------ device-resident timed region
     timer = ops.KernelTimer(names={"crk_accel_dudt"})
-    clocks = ClockSampler(dev.index)
     barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    tw0 = time.time()
     launches0 = L.sph_launch_count()
     ops.TIMER = timer
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -252,8 +314,10 @@ def gpu_arm(args, rank: int, world: int):
     torch.cuda.synchronize()
     ops.TIMER = None
     launches = L.sph_launch_count() - launches0
+    tw1 = time.time()
     barrier()
-    clock_info = clocks.stop()
+    clocks.stop()
+    clock_info = clocks.summarise(tw0, tw1)
     ms = ev0.elapsed_time(ev1)
     t = torch.tensor([ms], device=dev, dtype=torch.float64)
     if world > 1:
@@ -323,6 +387,10 @@ def gpu_arm(args, rank: int, world: int):
         e2e = {"value": n * e2e_steps * world / (float(te.item()) / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "steps": e2e_steps}
 
+    dfsph = None
+    if rank == 0 and world == 1 and not args.no_dfsph:
+        dfsph = dfsph_warm_start(dev)
+
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(args.nx, args.cpu_steps)
@@ -333,7 +401,8 @@ def gpu_arm(args, rank: int, world: int):
                 "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "particles": n, "nx": args.nx, "parallelism": f"replicas x{world}",
                            "l2": "working set larger than L2 (pair arrays ~0.7 GB per step), no flush needed"},
-                "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info}
+                "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
+                "dfsph_warm_start": dfsph}
         if breakdown is not None:
             line["breakdown_ms"] = {k: round(v["total_ms"] / 3, 4) for k, v in breakdown.items()}
         print(json.dumps(line), flush=True)
