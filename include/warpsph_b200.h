@@ -173,7 +173,8 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
  * for rounding).  When that holds, the interacting sublist for (x, H) is written to
  * inter_* (same layout as sph_neighbors_build) and *inter_nnz_out receives its size;
  * otherwise SPH_STATUS_LIST_STALE is or-ed into *status and the caller rebuilds.
- * scratch: device memory of 4 uint32 words. */
+ * With inter_list == NULL only the verdict is computed (the sublist can be filtered by
+ * a later call, when a pass needs it).  scratch: device memory of 4 uint32 words. */
 int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const float* H,
                           const float* x0, const float* H0,
                           const int32_t* neighbor_offsets, const int32_t* num_neighbors,

@@ -242,12 +242,14 @@ def test_prior_list_refresh(cuda, dim, n_side):
     adj1 = ops.buildVerletList(torch.from_numpy(x1).to(cuda), torch.from_numpy(H1).to(cuda), p, p.verlet_scale, adj0)
     assert adj1.neighborList.data_ptr() == adj0.neighborList.data_ptr(), "valid prior list must be kept"
     fresh = ops.buildVerletList(torch.from_numpy(x1).to(cuda), torch.from_numpy(H1).to(cuda), p, p.verlet_scale)
+    assert adj1.interList is None                      # filtered on first use by a pass
+    ops._lists(p, adj1, True)
     lst0 = adj0.neighborList.cpu().numpy()
     il1 = adj1.interList.cpu().numpy().reshape(-1, 2)
     o1, c1 = adj1.interOffsets.cpu().numpy(), adj1.interCounts.cpu().numpy()
     il2 = fresh.interList.cpu().numpy().reshape(-1, 2)
     o2, c2 = fresh.interOffsets.cpu().numpy(), fresh.interCounts.cpu().numpy()
-    assert adj1.interNnz == fresh.interNnz == int(c1.sum())
+    assert int(adj1._inter_nnz_dev.item()) == fresh.interNnz == int(c1.sum())
     for i in range(len(H)):
         r1 = il1[o1[i]: o1[i] + c1[i]]
         r2 = il2[o2[i]: o2[i] + c2[i]]

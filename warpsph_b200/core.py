@@ -168,6 +168,9 @@ class AdjacencyList:
     _x0: Optional[torch.Tensor] = field(default=None, repr=False)
     _h0: Optional[torch.Tensor] = field(default=None, repr=False)
     _dim: int = field(default=0, repr=False)
+    # SphParams of a kept prior list whose interacting subset is filtered on first use
+    _pending: Optional[object] = field(default=None, repr=False)
+    _inter_nnz_dev: Optional[torch.Tensor] = field(default=None, repr=False)
 
     @property
     def edgeOffsets(self) -> torch.Tensor:

@@ -841,24 +841,32 @@ int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const f
     int rc = params_to_dev(p, &P);
     if (rc) return rc;
     if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_refresh: n out of range");
-    WSPH_CHECK_PTR(scratch); WSPH_CHECK_PTR(inter_nnz_out); WSPH_CHECK_PTR(status);
+    WSPH_CHECK_PTR(scratch); WSPH_CHECK_PTR(status);
+    const bool filter = inter_list != nullptr;
     cudaStream_t s = WSPH_STREAM(stream);
-    cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
+    if (filter) {
+        WSPH_CHECK_PTR(inter_nnz_out);
+        cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
+    }
     if (n == 0) return check_launch("sph_neighbors_refresh");
-    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(x0); WSPH_CHECK_PTR(H0); WSPH_CHECK_PTR(neighbor_offsets);
-    WSPH_CHECK_PTR(num_neighbors); WSPH_CHECK_PTR(neighbor_list); WSPH_CHECK_PTR(inter_offsets); WSPH_CHECK_PTR(inter_counts);
-    WSPH_CHECK_PTR(inter_list);
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(x0); WSPH_CHECK_PTR(H0);
+    if (filter) {
+        WSPH_CHECK_PTR(neighbor_offsets); WSPH_CHECK_PTR(num_neighbors); WSPH_CHECK_PTR(neighbor_list);
+        WSPH_CHECK_PTR(inter_offsets); WSPH_CHECK_PTR(inter_counts);
+        if (reinterpret_cast<uintptr_t>(inter_list) & 7) return set_error(SPH_ERR_BAD_ARG, "inter_list must be 8-byte aligned");
+    }
     if (P.dim == 2 && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(x0)) & 7))
         return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
-    if (reinterpret_cast<uintptr_t>(inter_list) & 7) return set_error(SPH_ERR_BAD_ARG, "inter_list must be 8-byte aligned");
     cudaMemsetAsync(scratch, 0, 3 * sizeof(uint32_t), s);
     int cblocks = grid_for(n, 256);
     if (cblocks > 148 * 8) cblocks = 148 * 8;
     wsph::count_launch();
     WSPH_DISPATCH_DIM(P.dim, (k_refresh_check<D><<<cblocks, 256, 0, s>>>(x, H, x0, H0, (int)n, P, scratch)));
-    const int64_t rblocks = (n * RF_G + 255) / 256;   // RF_G lanes per row, 256 threads per block
+    // without list buffers only the verdict is written (no rows are filtered)
+    const int64_t rows = filter ? n : 0;
+    const int64_t rblocks = filter ? (n * RF_G + 255) / 256 : 1;   // RF_G lanes per row, 256 threads per block
     wsph::count_launch();
-    WSPH_DISPATCH_DIM(P.dim, (k_refilter<D><<<(int)rblocks, 256, 0, s>>>(x, H, (int)n, P, scratch, neighbor_offsets, num_neighbors,
+    WSPH_DISPATCH_DIM(P.dim, (k_refilter<D><<<(int)rblocks, 256, 0, s>>>(x, H, (int)rows, P, scratch, neighbor_offsets, num_neighbors,
                                                                         neighbor_list, inter_offsets, inter_counts,
                                                                         reinterpret_cast<int2*>(inter_list),
                                                                         reinterpret_cast<unsigned long long*>(inter_nnz_out), status)));

@@ -148,24 +148,19 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
     prior = priorNeighborhood
     if REUSE_PRIOR and prior is not None and prior._x0 is not None and prior.numRows == n and \
             prior.verletScale == float(verletScale) and prior._x0.device == dev and prior._dim == dim:
-        ioffs = torch.empty(n, dtype=torch.int32, device=dev)
-        icnt = torch.empty(n, dtype=torch.int32, device=dev)
-        ilst = torch.empty(2 * max(prior.nnz, 1), dtype=torch.int32, device=dev)
-        flags = torch.zeros(4, dtype=torch.int64, device=dev)   # [inter nnz, status (low half), scratch (2 words)]
+        flags = torch.zeros(4, dtype=torch.int64, device=dev)   # [-, status (low half), scratch (2 words)]
         with _timed("neighbors_refresh"):
-            check(L.sph_neighbors_refresh(_p(params), n, ptr(x), ptr(H), ptr(prior._x0), ptr(prior._h0), ptr(prior.neighborOffsets),
-                                          ptr(prior.numNeighbors), ptr(prior.neighborList), ptr(ioffs), ptr(icnt), ptr(ilst),
-                                          flags.data_ptr() + 16, flags.data_ptr(), flags.data_ptr() + 8, stream_ptr(dev)),
+            check(L.sph_neighbors_refresh(_p(params), n, ptr(x), ptr(H), ptr(prior._x0), ptr(prior._h0), None, None, None, None,
+                                          None, None, flags.data_ptr() + 16, None, flags.data_ptr() + 8, stream_ptr(dev)),
                   "sph_neighbors_refresh")
-        f = flags[:2].cpu()
-        if not (int(f[1]) & 0xffffffff) & _capi.STATUS_LIST_STALE:
+        if not (int(flags[1].item()) & 0xffffffff) & _capi.STATUS_LIST_STALE:
             adj = AdjacencyList(neighborOffsets=prior.neighborOffsets, numNeighbors=prior.numNeighbors,
                                 neighborList=prior.neighborList, numRows=n, numCols=n, nnz=prior.nnz, sortIndex=prior.sortIndex,
                                 sortedKeys=prior.sortedKeys, grid=prior.grid, queryPositions=x, querySupports=H,
-                                verletScale=float(verletScale), interOffsets=ioffs, interCounts=icnt, interList=ilst[:2 * prior.nnz],
-                                interNnz=int(f[0]))
+                                verletScale=float(verletScale))
             adj._x_version, adj._h_version = _version(x), _version(H)
             adj._x0, adj._h0, adj._dim = prior._x0, prior._h0, dim
+            adj._pending = _capi.SphParams.from_buffer_copy(params)   # interacting sublist filtered on first use
             return adj
     cap = cell_capacity_for(n, dim)
     wsb = C.c_int64(0)
@@ -234,9 +229,30 @@ def _csr(adj: AdjacencyList):
     return iptr(adj.neighborOffsets), iptr(adj.numNeighbors), iptr(adj.neighborList)
 
 
+def _materialize_inter(adj: AdjacencyList) -> None:
+    """Filters the interacting sublist of a kept prior list (sph_neighbors_refresh)."""
+    params = adj._pending
+    n, dev = adj.numRows, adj.neighborList.device
+    ioffs = torch.empty(n, dtype=torch.int32, device=dev)
+    icnt = torch.empty(n, dtype=torch.int32, device=dev)
+    ilst = torch.empty(2 * max(adj.nnz, 1), dtype=torch.int32, device=dev)
+    flags = torch.zeros(4, dtype=torch.int64, device=dev)   # [inter nnz, status (low half), scratch (2 words)]
+    with _timed("neighbors_refresh"):
+        check(_capi.lib().sph_neighbors_refresh(_p(params), n, ptr(adj.queryPositions), ptr(adj.querySupports), ptr(adj._x0),
+                                                ptr(adj._h0), ptr(adj.neighborOffsets), ptr(adj.numNeighbors), ptr(adj.neighborList),
+                                                ptr(ioffs), ptr(icnt), ptr(ilst), flags.data_ptr() + 16, flags.data_ptr(),
+                                                flags.data_ptr() + 8, stream_ptr(dev)), "sph_neighbors_refresh")
+    adj.interOffsets, adj.interCounts, adj.interList = ioffs, icnt, ilst[:2 * adj.nnz]
+    adj._inter_nnz_dev = flags[:1]
+    adj._pending = None
+
+
 def _lists(params, adj: AdjacencyList, interacting: bool):
     """Selects the row lists a pass walks: the interacting subset (r < max(H_i, H_j),
-    stride 2) when available and sufficient, else the Verlet list (stride 1)."""
+    stride 2) when available and sufficient, else the Verlet list (stride 1).  A kept
+    prior list filters its interacting subset here, on first use."""
+    if interacting and adj._pending is not None:
+        _materialize_inter(adj)
     if interacting and adj.interList is not None:
         params.list_stride = 2
         return iptr(adj.interOffsets), iptr(adj.interCounts), iptr(adj.interList)
@@ -265,7 +281,10 @@ def adaptive_h_iter(params, x, H, m, adj: AdjacencyList, hbounds: torch.Tensor):
     n = H.shape[0]
     rho, Hn, ratio = _empty(n, H), _empty(n, H), _empty(n, H)
     with _timed("adaptive_h_iter"):
-        check(_capi.lib().sph_adaptive_h_iter(_p(params), n, 0, fptr(x), fptr(H), fptr(m), *_lists(params, adj, True), fptr(hbounds), ptr(rho), ptr(Hn),
+        # the supports change right after this pass: a kept list that has not filtered its
+        # interacting subset yet is walked over its Verlet rows (W = 0 beyond the support)
+        check(_capi.lib().sph_adaptive_h_iter(_p(params), n, 0, fptr(x), fptr(H), fptr(m), *_lists(params, adj, adj._pending is None),
+                                              fptr(hbounds), ptr(rho), ptr(Hn),
                                               ptr(ratio), stream_ptr(H.device)), "sph_adaptive_h_iter")
     return rho, Hn, ratio
 
