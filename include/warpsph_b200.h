@@ -400,6 +400,86 @@ int sph_dfsph_density_solve(const SphParams* p, const SphJacobiConfig* cfg, int6
                             float* p_out, float* accel_out, float* history, int32_t* iterations,
                             int32_t* status, void* stream);
 
+/* ---------------------------------------------------------------- weakly compressible (delta-SPH) */
+/* EOS (modules/eos/weaklyCompressible.py:4-44), density diffusion terms
+ * (enumTypes.py:53-58, DensityDiffusionScheme) and pressure terms (enumTypes.py:60-66). */
+#define SPH_EOS_STIFF_TAIT   0
+#define SPH_EOS_TAIT         1
+#define SPH_EOS_ISOTHERMAL   2
+#define SPH_EOS_POLYTROPIC   3
+#define SPH_EOS_MURNAGHAN    4
+#define SPH_DENSITY_DIFFUSION_DELTA         0
+#define SPH_DENSITY_DIFFUSION_DENSITY_ONLY  2
+#define SPH_DENSITY_DIFFUSION_DELTA_ONLY    3
+#define SPH_PRESSURE_CONSERVATIVE     0
+#define SPH_PRESSURE_NONCONSERVATIVE  1
+#define SPH_PRESSURE_ANTUONO          2
+#define SPH_PRESSURE_I                3
+#define SPH_PRESSURE_J                4
+#define SPH_PRESSURE_SYMMETRIC        5
+
+/* fluidProperties (configurations/moduleConfigurations/fluidProperties.py:9-19) and
+ * WeaklyCompressibleDiffusionParams (weaklyCompressibleDiffusionParams.py:10-17). */
+typedef struct SphWcParams {
+    double rest_density;          /* rho0 */
+    double sound_speed;           /* fixedSoundSpeed c0 */
+    double polytropic_exponent;   /* 7 */
+    double kappa;
+    double density_delta;         /* delta, 0.1 */
+    double viscosity_nu;          /* viscidNu, 1e-3 */
+    double inviscid_alpha;        /* 0.01 */
+    int32_t inviscid;             /* 1: alpha c0 H / xi; 0: 2 (d + 2) nu */
+    int32_t density_scheme;       /* SPH_DENSITY_DIFFUSION_* */
+    int32_t pressure_term;        /* SPH_PRESSURE_* (the reference default is Antuono) */
+    int32_t eos;                  /* SPH_EOS_* */
+    int32_t reserved_i[4];
+} SphWcParams;
+
+/* One delta-SPH right-hand side (schemes/deltaSPH.py:97-171 for a periodic fluid with
+ * no boundaries, forcing or surface detection): pass A computes the renormalised
+ * density gradient (modules/density/gradRhoL.py) and the EOS pressure into scratch
+ * [n*(dim+1)] floats; pass B writes dvdt [n, dim] = pressure force
+ * (modules/pressure/wp_surfaceAware.py) + velocity diffusion (wp_viscosityDelta.py) and
+ * drhodt [n] = continuity (modules/momentum/inconsistent.py) + density diffusion
+ * (modules/deltaSPH/densityDiffusion.py).  Kernel support max(H_i, H_j). */
+int sph_deltasph_rhs(const SphParams* p, const SphWcParams* wc, int64_t n, const float* x,
+                     const float* H, const float* m, const float* rho, const float* v,
+                     const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                     float* scratch, float* dvdt_out, float* drhodt_out, void* stream);
+
+/* Batched ensemble of independent periodic boxes (no counterpart in the reference, which
+ * runs one simulation per process).  Particles of every box share one set of arrays;
+ * box_of[n] gives each particle's box.  Box b has a grid of box_grid[b]^dim cells over
+ * the periodic domain of `p` (cell size L / box_grid[b] >= verlet_scale * max H of the
+ * box, box_grid[b] >= 3), whose keys start at box_cell_base[b]; total_cells is the sum
+ * of box_grid[b]^dim.  The Verlet rows (same row rule and order conventions as
+ * sph_neighbors_build, per box) never pair particles of different boxes. */
+int64_t sph_ensemble_neighbors_workspace_size(int64_t n, int64_t total_cells);
+int sph_ensemble_neighbors_build(const SphParams* p, int64_t n, int32_t nbox, const int32_t* box_of,
+                                 const int32_t* box_grid, const int32_t* box_cell_base,
+                                 int64_t total_cells, const float* x, const float* H,
+                                 void* workspace, int64_t workspace_bytes,
+                                 int32_t* offs, int32_t* cnt, int32_t* list, int64_t list_capacity,
+                                 int64_t* nnz_out, int32_t* status, void* stream);
+
+/* One Heun RK2 step of every box in ONE cooperative persistent launch: delta-SPH
+ * right-hand side (sph_deltasph_rhs) at y0 and y1 = y0 + dt k1, then
+ * y = y0 + dt/2 (k1 + k2) for x (wrapped into the periodic domain), v and rho; dt is
+ * box_dt[box_of[i]].  x, v, rho are updated in place.  *disp_max receives the largest
+ * |x - x_build| / H since x_build (ordered-float encoding, atomicMax: zero it after a
+ * rebuild); the rows stay valid while 2 disp_max < verlet_scale - 1.  lanes (4, 8, 16)
+ * and block (128, 256) select the tile shape (the autotuner's choice).  workspace:
+ * sph_ensemble_step_workspace_size(n, dim) bytes, 256-byte aligned. */
+int64_t sph_ensemble_step_workspace_size(int64_t n, int32_t dim);
+int sph_ensemble_step(const SphParams* p, const SphWcParams* wc, int64_t n, const int32_t* box_of,
+                      const float* box_dt, const float* H, const float* m, float* x, float* v,
+                      float* rho, const float* x_build, const int32_t* offs, const int32_t* cnt,
+                      const int32_t* list, void* workspace, int64_t workspace_bytes,
+                      int32_t lanes, int32_t block, uint32_t* disp_max, int32_t* status, void* stream);
+
+/* weaklyCompressibleEOS (modules/eos/weaklyCompressible.py:21-44). */
+int sph_wc_eos(const SphWcParams* wc, int64_t n, const float* rho, float* P_out, void* stream);
+
 /* ---------------------------------------------------------------- learned warm start
  * No counterpart in the reference: a per-particle MLP predicts the initial pressure of
  * the Jacobi solves (replacing 0.75 p_prev at divergenceFree.py:72 and 0 at

@@ -92,6 +92,7 @@ class Oracle:
         L.oracle_dfsph_alpha.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pressure_accel_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pressure_shift_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_deltasph_rhs.argtypes = [P, P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rp]
         L.oracle_jacobi_solve.argtypes = [P, C.c_int, P, i64, rp, rp, rp, rp, rp, rpn, rp, real_c, _i32p, _i32p, _i32p, rp, rp,
                                           _f64p, C.POINTER(C.c_int)]
 
@@ -259,6 +260,16 @@ class Oracle:
                                      self.arr(rho), self.arr(v), None if dvdt is None else self.arr(dvdt), self.arr(p_init), float(dt),
                                      nb["offsets"], nb["counts"], nb["list"], p, acc, hist, C.byref(it))
         return p, acc, hist[: it.value], it.value
+
+    # ------------------------------------------------------------------ weakly compressible delta-SPH
+    def deltasph_rhs(self, params, wc, x, H, m, rho, v, nb):
+        """(dvdt, drhodt, gradRhoL, P); wc is a warpsph_b200._capi.SphWcParams."""
+        n, d = len(H), params.dim
+        gL = np.zeros((n, d), self.dtype); P = np.zeros(n, self.dtype)
+        dv = np.zeros((n, d), self.dtype); dr = np.zeros(n, self.dtype)
+        self.lib.oracle_deltasph_rhs(self._p(params), C.c_void_p(C.addressof(wc)), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho),
+                                     self.arr(v), nb["offsets"], nb["counts"], nb["list"], gL, P, dv, dr)
+        return dv, dr, gL, P
 
     def kernel_eval(self, kernel, dim, r, H):
         r = self.arr(r)

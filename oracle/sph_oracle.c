@@ -1039,6 +1039,112 @@ int oracle_jacobi_solve(const SphParams* p, int mode, const SphJacobiConfig* cfg
     return 0;
 }
 
+/* ------------------------------------------------------------------ weakly compressible delta-SPH
+ * modules/eos/weaklyCompressible.py:4-44; the renormalised density gradient of
+ * modules/density/gradRhoL.py:33-56 with L = (sum_j V_j gradW (x) (x_j - x_i))^-1
+ * (warpSPHCore's renormalisation, restated); modules/momentum/inconsistent.py:16-31;
+ * modules/deltaSPH/wp_densityDelta.py:14-118 with densityDiffusion.py:17-35;
+ * modules/pressure/wp_surfaceAware.py:10-64, :207; modules/deltaSPH/wp_viscosityDelta.py:14-108.
+ * Kernel support max(H_i, H_j) (super-symmetric). */
+static real wc_eos(const SphWcParams* w, real rho) {
+    real r0 = (real)w->rest_density, c = (real)w->sound_speed, g = (real)w->polytropic_exponent, k = (real)w->kappa;
+    switch (w->eos) {
+        case SPH_EOS_STIFF_TAIT: return r0 * c * c / g * (POW(rho / r0, g) - 1);
+        case SPH_EOS_TAIT: return k * (rho - r0);
+        case SPH_EOS_ISOTHERMAL: return c * c * (rho - r0);
+        case SPH_EOS_POLYTROPIC: return k * POW(rho, g);
+        default: return k / g * (POW(rho / r0, g) - 1);
+    }
+}
+
+int oracle_deltasph_rhs(const SphParams* p, const SphWcParams* w, int64_t n, const real* x, const real* H, const real* m,
+                        const real* rho, const real* v, const int32_t* offs, const int32_t* cnt, const int32_t* list, real* gL,
+                        real* Pr, real* dvdt, real* drhodt) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real M[3][3] = {{0}}, g[3] = {0, 0, 0};
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, gw[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG(&o, d, rsqrt_safe(dotD(d, d, D)), wmax(H[i], H[j]), &W, gw);
+            real Vj = m[j] / rho[j], dr = rho[j] - rho[i];
+            for (int a = 0; a < D; ++a) {
+                g[a] += Vj * dr * gw[a];
+                for (int c = 0; c < D; ++c) M[a][c] += Vj * gw[a] * (-d[c]);
+            }
+        }
+        real r[3] = {g[0], g[1], g[2]};
+        if (D == 1) {
+            if (FABS(M[0][0]) > (real)1e-6) r[0] = g[0] / M[0][0];
+        } else if (D == 2) {
+            real det = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+            if (FABS(det) > (real)1e-6) {
+                real id = 1 / det;
+                r[0] = id * (M[1][1] * g[0] - M[0][1] * g[1]);
+                r[1] = id * (-M[1][0] * g[0] + M[0][0] * g[1]);
+            }
+        } else {
+            double a[9], inv[9];
+            for (int q = 0; q < 9; ++q) a[q] = (double)M[q / 3][q % 3];
+            double det = inv_sym(3, a, inv);   /* general 3x3 inverse */
+            if (fabs(det) > 1e-6)
+                for (int q = 0; q < 3; ++q) r[q] = (real)(inv[q * 3 + 0] * g[0] + inv[q * 3 + 1] * g[1] + inv[q * 3 + 2] * g[2]);
+        }
+        for (int a = 0; a < D; ++a) gL[i * D + a] = r[a];
+        Pr[i] = wc_eos(w, rho[i]);
+    }
+    real xi = o.kxi;
+    real visc_nu = (real)2 * (real)(D + 2) * (real)w->viscosity_nu;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real cont = 0, dd = 0, pf[3] = {0, 0, 0}, vs[3] = {0, 0, 0};
+        real Hi = H[i], rhoi = rho[i], Pi = Pr[i], eps = (real)1.0e-14 * Hi;
+        real factor = w->inviscid ? (real)w->inviscid_alpha * (real)w->sound_speed * Hi / xi : visc_nu;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, gw[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real r2 = dotD(d, d, D), rr = rsqrt_safe(r2);
+            kWG(&o, d, rr, wmax(Hi, H[j]), &W, gw);
+            real rj = rho[j], Vj = m[j] / rj;
+            real t = 0;
+            for (int a = 0; a < D; ++a) t += (v[(int64_t)j * D + a] - v[i * D + a]) * gw[a];
+            cont += Vj * t;
+            real inv = 1 / (rr + eps), s = (real)2 * (rj - rhoi) * inv * inv, pd = 0;
+            for (int a = 0; a < D; ++a) {
+                real psi;
+                if (w->density_scheme == SPH_DENSITY_DIFFUSION_DELTA) psi = (gL[i * D + a] + gL[(int64_t)j * D + a]) - s * d[a];
+                else if (w->density_scheme == SPH_DENSITY_DIFFUSION_DENSITY_ONLY) psi = -(s * d[a]);
+                else psi = gL[i * D + a] + gL[(int64_t)j * D + a];
+                pd += psi * gw[a];
+            }
+            dd += Vj * pd;
+            real Pj = Pr[j], pij;
+            switch (w->pressure_term) {
+                case SPH_PRESSURE_CONSERVATIVE: pij = Pj - Pi; break;
+                case SPH_PRESSURE_NONCONSERVATIVE: pij = Pj + Pi; break;
+                case SPH_PRESSURE_ANTUONO: pij = (Pi >= 0 || Pj >= 0) ? Pj + Pi : Pj - Pi; break;
+                case SPH_PRESSURE_I: pij = Pi; break;
+                case SPH_PRESSURE_J: pij = Pj; break;
+                default: pij = (Pj / (rj * rj) + Pi / (rhoi * rhoi)) * rj; break;
+            }
+            for (int a = 0; a < D; ++a) pf[a] += Vj * pij * gw[a];
+            real vx = 0;
+            for (int a = 0; a < D; ++a) vx += (v[i * D + a] - v[(int64_t)j * D + a]) * d[a];
+            real mu = vx / (r2 + eps * Hi);
+            mu = mu > 0 ? 0 : mu;
+            real ww = Vj * mu * factor / ((rj + rhoi) / 2);
+            for (int a = 0; a < D; ++a) vs[a] += ww * gw[a];
+        }
+        drhodt[i] = -rhoi * cont + (real)w->density_delta * Hi / xi * (real)w->sound_speed * dd;
+        for (int a = 0; a < D; ++a) dvdt[i * D + a] = -pf[a] + vs[a];
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------------------ helpers exported for tests */
 int oracle_real_size(void) { return (int)sizeof(real); }
 int oracle_kernel_eval(int kernel, int dim, int64_t n, const real* r, real H, real* W, real* dWdr, real* dWdH) {

@@ -91,3 +91,18 @@ def test_tensors_must_be_cuda():
     x = torch.zeros(4, 2)
     with pytest.raises(RuntimeError, match="CUDA"):
         ops.crk_volume(p, x, torch.ones(4), None)
+
+
+def test_ctypes_prototypes_match_header_arity():
+    """Every ctypes prototype has as many arguments as its C declaration."""
+    import re
+    from pathlib import Path
+    from warpsph_b200 import _capi
+    h = (Path(__file__).resolve().parents[1] / "include" / "warpsph_b200.h").read_text()
+    h = re.sub(r"/\*.*?\*/", "", h, flags=re.S)
+    for name, args in _capi._PROTOS.items():
+        m = re.search(r"\b" + name + r"\s*\(([^;]*?)\)\s*;", h, re.S)
+        assert m, name
+        params = m.group(1).strip()
+        n = 0 if params in ("", "void") else len(params.split(","))
+        assert n == len(args), (name, n, len(args))

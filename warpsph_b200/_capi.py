@@ -73,6 +73,17 @@ class SphJacobiConfig(C.Structure):
     ]
 
 
+class SphWcParams(C.Structure):
+    """Mirror of the C struct SphWcParams (include/warpsph_b200.h)."""
+
+    _fields_ = [
+        ("rest_density", C.c_double), ("sound_speed", C.c_double), ("polytropic_exponent", C.c_double), ("kappa", C.c_double),
+        ("density_delta", C.c_double), ("viscosity_nu", C.c_double), ("inviscid_alpha", C.c_double),
+        ("inviscid", C.c_int32), ("density_scheme", C.c_int32), ("pressure_term", C.c_int32), ("eos", C.c_int32),
+        ("reserved_i", C.c_int32 * 4),
+    ]
+
+
 _P = C.c_void_p
 _I64 = C.c_int64
 _I32 = C.c_int32
@@ -113,6 +124,12 @@ _PROTOS = {
     "sph_dfsph_workspace_size": [_I64, _I32],
     "sph_dfsph_features": [_P, _P, _I32, _I64] + [_P] * 12 + [_I64] + [_P] * 3,
     "sph_mlp_param_count": [],
+    "sph_deltasph_rhs": [_P, _P, _I64] + [_P] * 12,
+    "sph_wc_eos": [_P, _I64, _P, _P, _P],
+    "sph_ensemble_neighbors_workspace_size": [_I64, _I64],
+    "sph_ensemble_neighbors_build": [_P, _I64, _I32, _P, _P, _P, _I64, _P, _P, _P, _I64, _P, _P, _P, _I64, _P, _P, _P],
+    "sph_ensemble_step_workspace_size": [_I64, _I32],
+    "sph_ensemble_step": [_P, _P, _I64] + [_P] * 12 + [_I64, _I32, _I32, _P, _P, _P],
     "sph_mlp_forward": [_P, _I64, _P, _P, _P, _P],
     "sph_mlp_grad": [_P, _I64, _P, _P, _P, _P, _P],
     "sph_mlp_adam": [_P, _P, _P, _P, _I64, C.c_float, C.c_float, C.c_float, C.c_float, _I64, _P],
@@ -121,7 +138,8 @@ _PROTOS = {
 }
 _RESTYPE = {"sph_version": C.c_char_p, "sph_last_error_string": C.c_char_p, "sph_launch_count": C.c_int64,
             "sph_dfsph_workspace_size": C.c_int64,
-            "sph_mlp_param_count": C.c_int64}
+            "sph_mlp_param_count": C.c_int64, "sph_ensemble_neighbors_workspace_size": C.c_int64,
+            "sph_ensemble_step_workspace_size": C.c_int64}
 
 _lib = None
 

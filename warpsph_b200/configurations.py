@@ -383,6 +383,47 @@ def jacobi_config(solver: RelaxedJacobiSolverConfig, restDensity: float, learned
     return c
 
 
+# ------------------------------------------------------------------ weakly compressible (delta-SPH)
+@dataclass
+class WeaklyCompressibleDiffusionParams:
+    """configurations/moduleConfigurations/weaklyCompressibleDiffusionParams.py:10-26."""
+    inviscid: bool = True
+    inviscidAlpha: float = 0.01
+    viscidNu: float = 1e-3
+    densityDelta: float = 0.1
+    densityDiffusionTerm: str = "deltaSPH"
+
+
+@dataclass
+class WeaklyCompressibleSPHConfig:
+    """configurations/weaklyCompressible.py:35-57, restricted to the fields of the periodic
+    delta-SPH right-hand side (fluid, diffusionParams, pressureForceTerm)."""
+    fluid: fluidProperties = field(default_factory=lambda: fluidProperties(restDensity=1.0, polytropicExponent=7.0, kappa=1.3,
+                                                                           fixedSoundSpeed=10.0))
+    eosType: str = "stiffTait"
+    diffusionParams: WeaklyCompressibleDiffusionParams = field(default_factory=WeaklyCompressibleDiffusionParams)
+    pressureForceTerm: str = "Antuono"
+
+
+_EOS = {"stiffTait": 0, "Tait": 1, "isoThermal": 2, "polytropic": 3, "murnaghan": 4}
+_DDIFF = {"deltaSPH": 0, "densityOnly": 2, "deltaOnly": 3}
+_PTERM = {"conservative": 0, "nonConservative": 1, "Antuono": 2, "i": 3, "j": 4, "symmetric": 5}
+
+
+def wc_params(cfg: WeaklyCompressibleSPHConfig) -> _capi.SphWcParams:
+    """Packs a WeaklyCompressibleSPHConfig into the C ABI's SphWcParams."""
+    w = _capi.SphWcParams()
+    f, d = cfg.fluid, cfg.diffusionParams
+    w.rest_density, w.sound_speed = float(f.restDensity), float(f.fixedSoundSpeed)
+    w.polytropic_exponent, w.kappa = float(f.polytropicExponent), float(f.kappa)
+    w.density_delta, w.viscosity_nu, w.inviscid_alpha = float(d.densityDelta), float(d.viscidNu), float(d.inviscidAlpha)
+    w.inviscid = int(bool(d.inviscid))
+    w.density_scheme = _DDIFF[d.densityDiffusionTerm]
+    w.pressure_term = _PTERM[cfg.pressureForceTerm]
+    w.eos = _EOS[cfg.eosType]
+    return w
+
+
 # ------------------------------------------------------------------ C ABI parameter block
 def make_params(config: SimulationConfig, scheme: Optional[CompressibleSPHConfig] = None) -> _capi.SphParams:
     """Packs the configuration into the C ABI's SphParams (host-side, no device sync

@@ -245,6 +245,11 @@ double kernel_scale(int kernel, int dim);
 
 inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
 
+// Exclusive scan of int32 values with a device int64 total (sph_neighbors.cu), and the
+// bytes of workspace it needs for n values.
+void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, char* ws, long long* total, cudaStream_t s);
+int64_t scan_ws_bytes(int64_t n);
+
 }  // namespace wsph
 
 #define WSPH_CHECK_PTR(ptr) do { if (!(ptr)) return wsph::set_error(SPH_ERR_BAD_ARG, "%s: null pointer '%s'", __func__, #ptr); } while (0)

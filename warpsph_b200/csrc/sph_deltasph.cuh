@@ -1,0 +1,250 @@
+// Pair bodies of the weakly compressible delta-SPH right-hand side, shared by the
+// single-list entry point (sph_deltasph.cu) and the batched ensemble (sph_ensemble.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstring>
+#include "sph_pair_common.cuh"
+
+namespace wsph {
+
+struct WcDev {
+    float rho0, c0, gamma, kappa, delta, nu, alpha;
+    int inviscid, density_scheme, pressure_term, eos;
+    float xi;           // kernel xi (= kernel scale H/h)
+    float visc_nu;      // 2 (d + 2) nu, the viscous factor of wp_viscosityDelta.py:97
+};
+
+inline int wc_to_dev(const SphWcParams* w, const DevParams& P, WcDev* o) {
+    memset(o, 0, sizeof(*o));
+    o->rho0 = (float)w->rest_density; o->c0 = (float)w->sound_speed; o->gamma = (float)w->polytropic_exponent;
+    o->kappa = (float)w->kappa; o->delta = (float)w->density_delta; o->nu = (float)w->viscosity_nu; o->alpha = (float)w->inviscid_alpha;
+    o->inviscid = w->inviscid; o->density_scheme = w->density_scheme; o->pressure_term = w->pressure_term; o->eos = w->eos;
+    o->xi = P.kscale;
+    o->visc_nu = 2.f * (float)(P.dim + 2) * o->nu;
+    if (o->eos < SPH_EOS_STIFF_TAIT || o->eos > SPH_EOS_MURNAGHAN) return set_error(SPH_ERR_BAD_ARG, "unknown EOS %d", o->eos);
+    if (o->density_scheme != SPH_DENSITY_DIFFUSION_DELTA && o->density_scheme != SPH_DENSITY_DIFFUSION_DENSITY_ONLY &&
+        o->density_scheme != SPH_DENSITY_DIFFUSION_DELTA_ONLY)
+        return set_error(SPH_ERR_UNSUPPORTED, "density diffusion scheme %d is not on this path", o->density_scheme);
+    if (o->pressure_term < 0 || o->pressure_term > 5) return set_error(SPH_ERR_BAD_ARG, "unknown pressure term %d", o->pressure_term);
+    if (!(o->rho0 > 0.f)) return set_error(SPH_ERR_BAD_ARG, "rest density must be > 0");
+    return SPH_OK;
+}
+
+// modules/eos/weaklyCompressible.py:4-44
+__device__ __forceinline__ float wc_eos(const WcDev& W, float rho) {
+    switch (W.eos) {
+        case SPH_EOS_STIFF_TAIT: return W.rho0 * W.c0 * W.c0 / W.gamma * (powf(rho / W.rho0, W.gamma) - 1.f);
+        case SPH_EOS_TAIT: return W.kappa * (rho - W.rho0);
+        case SPH_EOS_ISOTHERMAL: return W.c0 * W.c0 * (rho - W.rho0);
+        case SPH_EOS_POLYTROPIC: return W.kappa * powf(rho, W.gamma);
+        default: return W.kappa / W.gamma * (powf(rho / W.rho0, W.gamma) - 1.f);
+    }
+}
+
+static __global__ void k_wc_eos(int n, WcDev W, const float* __restrict__ rho, float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = wc_eos(W, rho[i]);
+}
+
+// Loads of the pair passes.  CG: ld.global.cg (L2, coherent across blocks) for arrays
+// that other blocks rewrite inside one persistent launch; otherwise the read-only path.
+template <bool CG> __device__ __forceinline__ float ldf(const float* p) { return CG ? __ldcg(p) : __ldg(p); }
+template <int D, bool CG> __device__ __forceinline__ Vec<D> ldv(const float* p, int i) {
+    Vec<D> r;
+    if constexpr (D == 2) {
+        const float2 t = CG ? __ldcg(reinterpret_cast<const float2*>(p) + i) : __ldg(reinterpret_cast<const float2*>(p) + i);
+        r.v[0] = t.x; r.v[1] = t.y;
+    } else {
+        #pragma unroll
+        for (int a = 0; a < D; ++a) r.v[a] = ldf<CG>(p + (size_t)i * D + a);
+    }
+    return r;
+}
+
+// Renormalisation of pass A: L = M^-1 with M_ab = sum_j V_j gradW_a (x_j - x_i)_b; a
+// (near-)singular M (isolated particle) leaves the gradient unrenormalised.
+template <int D> __device__ __forceinline__ Vec<D> renormalise(const Mat<D>& M, const Vec<D>& g) {
+    Vec<D> r = g;
+    if constexpr (D == 1) {
+        if (fabsf(M.m[0][0]) > 1e-6f) r.v[0] = g.v[0] / M.m[0][0];
+    } else if constexpr (D == 2) {
+        const float det = M.m[0][0] * M.m[1][1] - M.m[0][1] * M.m[1][0];
+        if (fabsf(det) > 1e-6f) {
+            const float id = 1.f / det;
+            r.v[0] = id * (M.m[1][1] * g.v[0] - M.m[0][1] * g.v[1]);
+            r.v[1] = id * (-M.m[1][0] * g.v[0] + M.m[0][0] * g.v[1]);
+        }
+    } else {
+        const float c00 = M.m[1][1] * M.m[2][2] - M.m[1][2] * M.m[2][1];
+        const float c01 = M.m[1][2] * M.m[2][0] - M.m[1][0] * M.m[2][2];
+        const float c02 = M.m[1][0] * M.m[2][1] - M.m[1][1] * M.m[2][0];
+        const float det = M.m[0][0] * c00 + M.m[0][1] * c01 + M.m[0][2] * c02;
+        if (fabsf(det) > 1e-6f) {
+            const float id = 1.f / det;
+            const float i00 = c00, i01 = M.m[0][2] * M.m[2][1] - M.m[0][1] * M.m[2][2], i02 = M.m[0][1] * M.m[1][2] - M.m[0][2] * M.m[1][1];
+            const float i10 = c01, i11 = M.m[0][0] * M.m[2][2] - M.m[0][2] * M.m[2][0], i12 = M.m[0][2] * M.m[1][0] - M.m[0][0] * M.m[1][2];
+            const float i20 = c02, i21 = M.m[0][1] * M.m[2][0] - M.m[0][0] * M.m[2][1], i22 = M.m[0][0] * M.m[1][1] - M.m[0][1] * M.m[1][0];
+            r.v[0] = id * (i00 * g.v[0] + i01 * g.v[1] + i02 * g.v[2]);
+            r.v[1] = id * (i10 * g.v[0] + i11 * g.v[1] + i12 * g.v[2]);
+            r.v[2] = id * (i20 * g.v[0] + i21 * g.v[1] + i22 * g.v[2]);
+        }
+    }
+    return r;
+}
+
+// Per-lane partial sums of pass A for particle i.
+template <int KF, int D, int G, int ST, bool CG = false>
+__device__ __forceinline__ void passA_partial(int i, int lane, const DevParams& P, const float* x,
+                                              const float* __restrict__ H, const float* __restrict__ m,
+                                              const float* rho, const int32_t* __restrict__ offs,
+                                              const int32_t* __restrict__ cnt, const int32_t* __restrict__ list, Mat<D>& M,
+                                              Vec<D>& g) {
+    const Vec<D> xi = ldv<D, CG>(x, i);
+    const float Hi = H[i], rhoi = ldf<CG>(rho + i);
+    const int b = offs[i], e = b + cnt[i];
+    for (int q = b + lane; q < e; q += G) {
+        int j, k; entry<ST>(list, q, j, k);
+        const Vec<D> xij = dist_vec<D>(xi, ldv<D, CG>(x, j), P.dom);
+        const float r = safe_sqrt(dot<D>(xij, xij));
+        float W; Vec<D> gW;
+        kernelWG<KF, D>(xij, r, wmax(Hi, __ldg(H + j)), W, gW);
+        const float rj = ldf<CG>(rho + j);
+        const float Vj = __ldg(m + j) / rj;
+        const float dr = rj - rhoi;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) {
+            g.v[a] += Vj * dr * gW.v[a];
+            #pragma unroll
+            for (int c = 0; c < D; ++c) M.m[a][c] += Vj * gW.v[a] * (-xij.v[c]);
+        }
+    }
+}
+
+template <int D, int G> __device__ __forceinline__ void passA_reduce(Mat<D>& M, Vec<D>& g) {
+    #pragma unroll
+    for (int a = 0; a < D; ++a) {
+        g.v[a] = gsum<G>(g.v[a]);
+        #pragma unroll
+        for (int c = 0; c < D; ++c) M.m[a][c] = gsum<G>(M.m[a][c]);
+    }
+}
+
+// Per-lane partial sums of pass B for particle i: cont = sum V (v_j - v_i).gW,
+// dd = sum V psi.gW, pf = sum V p_ij gW, visc = sum V mu f gW / rho_bar.
+template <int KF, int D, int G, int ST, bool CG = false>
+__device__ __forceinline__ void passB_partial(int i, int lane, const DevParams& P, const WcDev& W, const float* x,
+                                              const float* __restrict__ H, const float* __restrict__ m, const float* rho,
+                                              const float* v, const float* gL, const float* Pr,
+                                              const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
+                                              const int32_t* __restrict__ list, float& cont, float& dd, Vec<D>& pf, Vec<D>& visc) {
+    const Vec<D> xi = ldv<D, CG>(x, i), vi = ldv<D, CG>(v, i), gLi = ldv<D, CG>(gL, i);
+    const float Hi = H[i], rhoi = ldf<CG>(rho + i), Pi = ldf<CG>(Pr + i);
+    const float eps = 1.0e-14f * Hi;
+    const float factor = W.inviscid ? W.alpha * W.c0 * Hi / W.xi : W.visc_nu;
+    const int b = offs[i], e = b + cnt[i];
+    for (int q = b + lane; q < e; q += G) {
+        int j, k; entry<ST>(list, q, j, k);
+        const Vec<D> xij = dist_vec<D>(xi, ldv<D, CG>(x, j), P.dom);
+        const float r2 = dot<D>(xij, xij);
+        const float r = safe_sqrt(r2);
+        float Wv; Vec<D> gW;
+        kernelWG<KF, D>(xij, r, wmax(Hi, __ldg(H + j)), Wv, gW);
+        const float rj = ldf<CG>(rho + j);
+        const float Vj = __ldg(m + j) / rj;
+        const Vec<D> vj = ldv<D, CG>(v, j);
+        // continuity (inconsistent.py:19-31): V_j (v_j - v_i).gW
+        float t = 0.f;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) t += (vj.v[a] - vi.v[a]) * gW.v[a];
+        cont += Vj * t;
+        // density diffusion (wp_densityDelta.py:88-117)
+        {
+            const Vec<D> gLj = ldv<D, CG>(gL, j);
+            const float inv = 1.f / (r + eps);
+            const float s = 2.f * (rj - rhoi) * inv * inv;      // 2 (rho_j - rho_i) n_ij / (r + eps), n_ij = x_ij / (r + eps)
+            float pd = 0.f;
+            #pragma unroll
+            for (int a = 0; a < D; ++a) {
+                float psi;
+                if (W.density_scheme == SPH_DENSITY_DIFFUSION_DELTA) psi = (gLi.v[a] + gLj.v[a]) - s * xij.v[a];
+                else if (W.density_scheme == SPH_DENSITY_DIFFUSION_DENSITY_ONLY) psi = -(s * xij.v[a]);
+                else psi = gLi.v[a] + gLj.v[a];
+                pd += psi * gW.v[a];
+            }
+            dd += Vj * pd;
+        }
+        // pressure (wp_surfaceAware.py:48-63); no free-surface mask on this path
+        {
+            const float Pj = ldf<CG>(Pr + j);
+            float pij;
+            switch (W.pressure_term) {
+                case SPH_PRESSURE_CONSERVATIVE: pij = Pj - Pi; break;
+                case SPH_PRESSURE_NONCONSERVATIVE: pij = Pj + Pi; break;
+                case SPH_PRESSURE_ANTUONO: pij = (Pi >= 0.f || Pj >= 0.f) ? Pj + Pi : Pj - Pi; break;
+                case SPH_PRESSURE_I: pij = Pi; break;
+                case SPH_PRESSURE_J: pij = Pj; break;
+                default: pij = (Pj / (rj * rj) + Pi / (rhoi * rhoi)) * rj; break;
+            }
+            #pragma unroll
+            for (int a = 0; a < D; ++a) pf.v[a] += Vj * pij * gW.v[a];
+        }
+        // velocity diffusion (wp_viscosityDelta.py:86-106)
+        {
+            float vx = 0.f;
+            #pragma unroll
+            for (int a = 0; a < D; ++a) vx += (vi.v[a] - vj.v[a]) * xij.v[a];
+            float mu = vx / (r2 + eps * Hi);
+            mu = mu > 0.f ? 0.f : mu;
+            const float w = Vj * mu * factor / ((rj + rhoi) / 2.f);
+            #pragma unroll
+            for (int a = 0; a < D; ++a) visc.v[a] += w * gW.v[a];
+        }
+    }
+}
+
+// pass B output: drhodt = -rho cont + delta (H / xi) c0 dd, dvdt = -pf + visc.
+template <int D> __device__ __forceinline__ void passB_finish(const WcDev& W, float rhoi, float Hi, float cont, float dd, const Vec<D>& pf,
+                                                               const Vec<D>& visc, float& drho, Vec<D>& dv) {
+    drho = -rhoi * cont + W.delta * Hi / W.xi * W.c0 * dd;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) dv.v[a] = -pf.v[a] + visc.v[a];
+}
+
+// Pass A: gradRhoL [n, D] and the EOS pressure P [n].
+template <int KF, int D, int G, int ST>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_ds_passA(int n, DevParams P, WcDev W, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+           const float* __restrict__ rho, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
+           const int32_t* __restrict__ list, float* __restrict__ gL, float* __restrict__ Pr) {
+    Grp<G> g(n);
+    Mat<D> M = mzero<D>();
+    Vec<D> s = vzero<D>();
+    if (g.valid) passA_partial<KF, D, G, ST>(g.i, g.lane, P, x, H, m, rho, offs, cnt, list, M, s);
+    passA_reduce<D, G>(M, s);
+    if (g.valid && g.lane == 0) {
+        store_vec<D>(gL, g.i, renormalise<D>(M, s));
+        Pr[g.i] = wc_eos(W, rho[g.i]);
+    }
+}
+
+template <int KF, int D, int G, int ST>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_ds_passB(int n, DevParams P, WcDev W, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+           const float* __restrict__ rho, const float* __restrict__ v, const float* __restrict__ gL, const float* __restrict__ Pr,
+           const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+           float* __restrict__ dvdt, float* __restrict__ drhodt) {
+    Grp<G> g(n);
+    float cont = 0.f, dd = 0.f;
+    Vec<D> pf = vzero<D>(), visc = vzero<D>();
+    if (g.valid) passB_partial<KF, D, G, ST>(g.i, g.lane, P, W, x, H, m, rho, v, gL, Pr, offs, cnt, list, cont, dd, pf, visc);
+    cont = gsum<G>(cont); dd = gsum<G>(dd);
+    #pragma unroll
+    for (int a = 0; a < D; ++a) { pf.v[a] = gsum<G>(pf.v[a]); visc.v[a] = gsum<G>(visc.v[a]); }
+    if (!g.valid || g.lane != 0) return;
+    float dr; Vec<D> dv;
+    passB_finish<D>(W, rho[g.i], H[g.i], cont, dd, pf, visc, dr, dv);
+    drhodt[g.i] = dr;
+    store_vec<D>(dvdt, g.i, dv);
+}
+
+}  // namespace wsph

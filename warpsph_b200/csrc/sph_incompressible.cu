@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <mutex>
 #include "sph_pair_common.cuh"
+#include "sph_persistent.cuh"
 
 namespace wsph {
 
@@ -36,10 +37,7 @@ constexpr int JAC_G = 8;
 constexpr int JAC_PPB = JAC_BLOCK / JAC_G;   // particles per block and round
 
 struct JacobiCtl {
-    unsigned int count;        // barrier arrivals
-    unsigned int gen;          // barrier generation
-    int status;                // SPH_STATUS_* bits
-    int pad;
+    BarrierCtl bar;            // grid barrier and SPH_STATUS_* bits
     double sum[3][2];          // [slot][0] = sum p, [slot][1] = sum of the error term
     unsigned int mm[3][2];     // [slot][0] = min p, [slot][1] = max p (ordered encoding)
 };
@@ -51,53 +49,12 @@ __device__ __forceinline__ unsigned int f2o(float f) {
 __device__ __forceinline__ float o2f(unsigned int o) {
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
 }
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
 
 template <int D> __device__ __forceinline__ Vec<D> load_vec_cg(const float* p, int i) {
     Vec<D> r;
     #pragma unroll
     for (int a = 0; a < D; ++a) r.v[a] = __ldcg(p + (size_t)i * D + a);
     return r;
-}
-
-// Bounded grid-wide barrier for a cooperative launch.  Returns false when any
-// block gave up (SPH_STATUS_TIMEOUT), in which case the caller returns.
-__device__ bool grid_barrier(JacobiCtl* c) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int* vgen = &c->gen;
-        volatile int* vstat = &c->status;
-        const unsigned int g = *vgen;
-        int good = 1;
-        __threadfence();
-        const unsigned int arrived = atomicAdd(&c->count, 1u) + 1u;
-        if (arrived == gridDim.x) {
-            atomicExch(&c->count, 0u);
-            __threadfence();
-            atomicAdd(&c->gen, 1u);
-        } else {
-            const unsigned long long t0 = global_ns();
-            unsigned int spins = 0;
-            while (*vgen == g) {
-                if (*vstat & SPH_STATUS_TIMEOUT) { good = 0; break; }
-                if (++spins > (1u << 26) || global_ns() - t0 > 2000000000ull) {
-                    atomicOr(&c->status, SPH_STATUS_TIMEOUT);
-                    good = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        ok = good;
-    }
-    __syncthreads();
-    return ok != 0;
 }
 
 // ---------------------------------------------------------------- per-lane partial sums
@@ -343,7 +300,7 @@ k_jacobi(JacobiArgs a) {
             }
         }
         if (converged || it >= a.max_it) break;
-        if (!grid_barrier(c)) { if (threadIdx.x == 0) atomicOr(a.status_out, SPH_STATUS_TIMEOUT); return; }
+        if (!grid_barrier(&c->bar)) { if (threadIdx.x == 0) atomicOr(a.status_out, SPH_STATUS_TIMEOUT); return; }
 
         // ------------------------------------------------ phase B: shift, residual, update
         double psum = 0.0, esum = 0.0;
@@ -387,7 +344,7 @@ k_jacobi(JacobiArgs a) {
             atomicMin(&c->mm[sl][0], lo);
             atomicMax(&c->mm[sl][1], hi);
         }
-        if (!grid_barrier(c)) { if (threadIdx.x == 0) atomicOr(a.status_out, SPH_STATUS_TIMEOUT); return; }
+        if (!grid_barrier(&c->bar)) { if (threadIdx.x == 0) atomicOr(a.status_out, SPH_STATUS_TIMEOUT); return; }
 
         // ------------------------------------------------ decide (identical in every block)
         const int sl = it % 3;
@@ -405,12 +362,12 @@ k_jacobi(JacobiArgs a) {
             a.hist[it * 4 + 3] = (float)(mean - (double)mu);
         }
         const bool finite = isfinite(err);
-        if (!finite) { if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(&c->status, SPH_STATUS_NONFINITE); }
+        if (!finite) { if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(&c->bar.status, SPH_STATUS_NONFINITE); }
         converged = (it >= a.min_it && err < (double)a.tol) || !finite;
         ++it;
     }
     if (threadIdx.x == 0) {
-        int st = *(volatile int*)&c->status;
+        int st = *(volatile int*)&c->bar.status;
         if (blockIdx.x == 0) {
             if (!converged && a.max_it > 0) st |= SPH_STATUS_NOT_CONVERGED;
             *a.iters_out = it;

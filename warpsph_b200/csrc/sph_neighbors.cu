@@ -185,7 +185,7 @@ __global__ void k_scan_add(long long* __restrict__ out_ll, int32_t* __restrict__
 }
 
 // Workspace: for each level the tile sums and their scanned offsets.
-static int64_t scan_ws_bytes(int64_t n) {
+int64_t scan_ws_bytes(int64_t n) {
     int64_t bytes = 0;
     int64_t m = n;
     do {
@@ -213,7 +213,7 @@ static void scan_ll_inplace(long long* data, int64_t n, char* ws, long long* tot
 }
 
 // Exclusive scan int32 -> int32, total (int64, device).
-static void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, char* ws, long long* total, cudaStream_t s) {
+void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, char* ws, long long* total, cudaStream_t s) {
     int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (tiles < 1) tiles = 1;
     long long* sums = reinterpret_cast<long long*>(ws);

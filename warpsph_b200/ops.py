@@ -550,3 +550,23 @@ def mlp_grad(theta, feats, target):
 def mlp_adam(theta, grad, m1, m2, step: int, lr: float, beta1=0.9, beta2=0.999, eps=1e-8):
     check(_capi.lib().sph_mlp_adam(fptr(theta), fptr(grad), fptr(m1), fptr(m2), theta.numel(), float(lr), float(beta1),
                                    float(beta2), float(eps), int(step), stream_ptr(theta.device)), "sph_mlp_adam")
+
+
+# ------------------------------------------------------------------ weakly compressible delta-SPH
+def deltasph_rhs(params, wc, x, H, m, rho, v, adj: AdjacencyList):
+    """One delta-SPH right-hand side: (dvdt [n, dim], drhodt [n], gradRhoL [n, dim], P [n])."""
+    n, d = m.shape[0], int(params.dim)
+    scratch = _empty(n * (d + 1), m)
+    dvdt, drhodt = _empty((n, d), m), _empty(n, m)
+    with _timed("deltasph_rhs"):
+        check(_capi.lib().sph_deltasph_rhs(_p(params), C.cast(C.pointer(wc), C.c_void_p), n, fptr(x), fptr(H), fptr(m), fptr(rho),
+                                           fptr(v), *_lists(params, adj, True), ptr(scratch), ptr(dvdt), ptr(drhodt),
+                                           stream_ptr(m.device)), "sph_deltasph_rhs")
+    return dvdt, drhodt, scratch[: n * d].view(n, d), scratch[n * d:]
+
+
+def wc_eos(wc, rho) -> torch.Tensor:
+    out = torch.empty_like(rho)
+    check(_capi.lib().sph_wc_eos(C.cast(C.pointer(wc), C.c_void_p), rho.shape[0], fptr(rho), ptr(out), stream_ptr(rho.device)),
+          "sph_wc_eos")
+    return out
