@@ -50,6 +50,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--breakdown", action="store_true", help="print a per-kernel time breakdown to stderr")
     ap.add_argument("--no-dfsph", action="store_true", help="skip the DFSPH warm-start comparison")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched delta-SPH ensemble")
     return ap.parse_args(argv)
 
 
@@ -253,6 +254,37 @@ def dfsph_warm_start(dev) -> dict:
     }
 
 
+# ---------------------------------------------------------------------------- batched ensemble
+def ensemble_throughput(dev, chunks: int = 6) -> dict:
+    """The batched weakly compressible delta-SPH ensemble: 256 periodic 2D unit boxes with
+    particle counts log-uniform in [4096, 65536] (seed 0), divergence-free E(k) ~ k^-5/3
+    velocity fields at U_max = 1, stiff Tait EOS c0 = 10, delta = 0.1, nu = 1e-3, Wendland
+    C2 with the reference's default 50 neighbours, Heun RK2 at dt = 0.3 h / c0 per box.
+    One cooperative launch per step for all boxes, steps replayed from a CUDA graph,
+    lists rebuilt when the Verlet skin requires it (included in the time)."""
+    import torch
+    from warpsph_b200.ensemble import Ensemble, build_boxes
+    t0 = time.perf_counter()
+    E = Ensemble(build_boxes(256, seed=0), dev)
+    tune = E.autotune(steps=2)
+    E.advance(1 + E.graph_steps)
+    torch.cuda.synchronize()
+    r0 = E.rebuilds
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    done = E.advance(chunks * E.graph_steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"workload": "256 periodic 2D delta-SPH boxes, N_b log-uniform [4096, 65536], RK2, CUDA graph",
+            "particles": E.n, "boxes": len(E.sizes), "verlet_entries_per_particle": E.nnz / E.n,
+            "steps": done, "ms_per_step": ms / done, "value": E.n * done / (ms / 1e3), "unit": "particle-steps/s",
+            "launches_per_step": "1 cooperative step kernel (+ list rebuilds)", "rebuilds": E.rebuilds - r0,
+            "tile": {"lanes": E.tile[0], "block": E.tile[1]},
+            "autotune_ms_per_step": {f"{k[0]}x{k[1]}": round(v, 3) for k, v in tune.items()},
+            "status": E.status(), "wall_s": time.perf_counter() - t0}
+
+
 # ---------------------------------------------------------------------------- GPU arm
 def build_workload(nx, dev):
     import warpsph_b200 as ws
@@ -390,6 +422,9 @@ def gpu_arm(args, rank: int, world: int):
     dfsph = None
     if rank == 0 and world == 1 and not args.no_dfsph:
         dfsph = dfsph_warm_start(dev)
+    ens = None
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        ens = ensemble_throughput(dev)
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -402,7 +437,7 @@ def gpu_arm(args, rank: int, world: int):
                 "config": {"workload": WORKLOAD, "particles": n, "nx": args.nx, "parallelism": f"replicas x{world}",
                            "l2": "working set larger than L2 (pair arrays ~0.7 GB per step), no flush needed"},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
-                "dfsph_warm_start": dfsph}
+                "dfsph_warm_start": dfsph, "ensemble": ens}
         if breakdown is not None:
             line["breakdown_ms"] = {k: round(v["total_ms"] / 3, 4) for k, v in breakdown.items()}
         print(json.dumps(line), flush=True)

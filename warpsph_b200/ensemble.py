@@ -170,6 +170,7 @@ class Ensemble:
             raise RuntimeError(f"ensemble list capacity {self.capacity} < {self.nnz} entries")
         self.x_build.copy_(self.x)
         self.flags[2].zero_()
+        self._used_at_check = 0.0
         self.rebuilds += 1
 
     def skin_used(self) -> float:
@@ -217,12 +218,16 @@ class Ensemble:
                     self._launch()
             done += self.graph_steps
             self.steps_done += self.graph_steps
-            # the rows must hold until the next check: rebuild once half the skin is used
+            # the rows must hold until the next check: rebuild when the last chunk's growth
+            # of the used skin, with a 1.5x margin, would exhaust it before then
             used = 2.0 * self.skin_used()
-            if used >= self.config.verletScale - 1.0:
+            skin = self.config.verletScale - 1.0
+            if used >= skin:
                 raise RuntimeError("ensemble: particles left the Verlet skin between two checks")
-            if used > 0.5 * (self.config.verletScale - 1.0):
+            if used + 1.5 * (used - self._used_at_check) >= skin:
                 self.rebuild()
+                used = 0.0
+            self._used_at_check = used
         return done
 
     def status(self) -> int:
@@ -246,6 +251,6 @@ class Ensemble:
             torch.cuda.synchronize(self.device)
             res[tile] = e0.elapsed_time(e1) / steps
         self.tile = min(res, key=res.get)
-        self.flags[2].zero_()
+        self.rebuild()          # the candidates moved copies; restart the skin from the state
         self.graph = None
         return res
