@@ -105,7 +105,10 @@ typedef struct SphParams {
     /* adaptive support and time step (simulationConfig.py:28-38) */
     double target_neighbors;
     double cfl, min_dt, max_dt, dt_growth;
-    double reserved_d[8];
+    /* DiffusionParameters.c_s: the sound speed of the viscosity terms when no per-particle
+     * sound speeds are passed (diffusionParameters.py:24) */
+    double c_s;
+    double reserved_d[7];
     /* integers */
     int32_t dim;                      /* 1, 2 or 3 */
     int32_t kernel;                   /* SPH_KERNEL_* */
@@ -121,7 +124,10 @@ typedef struct SphParams {
      * from sph_neighbors_build.  Pairwise outputs/inputs (ap_ij, av_ij, f_ij) are always
      * indexed by the Verlet entry. */
     int32_t list_stride;
-    int32_t reserved_i[7];
+    /* DiffusionParameters.thermalConducitiyTerm (SPH_VISC_*): the signal-velocity form of
+     * the artificial conductivity (diffusionParameters.py:33, pi.py:63) */
+    int32_t conductivity_term;
+    int32_t reserved_i[6];
 } SphParams;
 
 /* ---------------------------------------------------------------- library */
@@ -293,6 +299,73 @@ int sph_crk_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
                  const float* v, const float* c, const float* P, const float* DvDx,
                  const int32_t* offs, const int32_t* cnt, const int32_t* list,
                  float* dudt_out, void* stream);
+
+/* ---------------------------------------------------------------- CompSPH / Monaghan schemes */
+/* One walk of each row for three of the reference's passes (schemes/compSPH.py:89-97,
+ * :105-110 and :162-169; schemes/monaghan.py:59-101):
+ *   omega_out  grad-h Omega_i = 1 - sum_j (-H_i/(rho_i d)) m_j dW/dH(r_ij, H_i), gather
+ *              support -- replaces computeOmegaWarp (modules/adaptiveSupport/wp_omega.py:175);
+ *   div_out    difference divergence sum_j m_j/rho_j (v_j - v_i).grad W(r_ij, max(H_i,H_j)) of
+ *              the Cullen switch (modules/shockCapturing/CullenDehnen2010.py:246-257);
+ *   drhodt_out consistent continuity -(1/Omega_i) sum_j m_j (v_j - v_i).grad W(r_ij, max(H_i,H_j))
+ *              -- replaces computeMomentumConsistent_warp (modules/momentum/consistent.py:8-35);
+ *              Omega = 1 when omega_out is null (no grad-h corrections).
+ * Any output may be null; v may be null when only omega_out is requested. */
+int sph_compsph_prep(const SphParams* p, int64_t n, const float* x, const float* H,
+                     const float* m, const float* rho, const float* v,
+                     const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                     float* omega_out, float* div_out, float* drhodt_out, void* stream);
+/* Omega alone, for callers that bind computeOmegaWarp (wp_omega.py:175). */
+int sph_grad_h_omega(const SphParams* p, int64_t n, const float* x, const float* H,
+                     const float* m, const float* rho,
+                     const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                     float* omega_out, void* stream);
+
+/* CompSPH momentum and energy right-hand sides in one pass -- replaces
+ * computeCompSPHAccelWarp (modules/compSPH/accel.py:284) and computeCompSPHdudtWarp
+ * (modules/compSPH/dudt.py:224): per pair the kernel-mean gradient, grad-h pressure
+ * terms P/(rho^2 Omega), and the artificial viscosity Pi of computePi_actual
+ * (modules/dissipation/pi.py:11-161, the p->viscosity_term form) scaled by rho_bar/rho;
+ * du/dt with the gather gradient.  c, alpha and omega may be null (c_s, 1 and 1, as the
+ * reference does without sound speeds, switch or grad-h state).  Outputs:
+ * dvdt [n*dim], dudt [n], dEdt [n] = m v.dvdt + m dudt (schemes/compSPH.py:170), pairwise
+ * pressure / viscous accelerations ap_ij, av_ij [nnz*dim] by Verlet entry; any may be null.
+ * With the interacting list (list_stride 2) only interacting entries of ap_ij / av_ij are
+ * written; the caller passes zero-filled arrays. */
+int sph_compsph_accel_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
+                           const float* m, const float* rho, const float* v, const float* c,
+                           const float* alpha, const float* P, const float* omega,
+                           const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                           float* dvdt_out, float* dudt_out, float* dEdt_out,
+                           float* ap_ij, float* av_ij, void* stream);
+/* The same pass under the reference's two wrapper names. */
+int sph_compsph_accel(const SphParams* p, int64_t n, const float* x, const float* H,
+                      const float* m, const float* rho, const float* v, const float* c,
+                      const float* alpha, const float* P, const float* omega,
+                      const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                      float* dvdt_out, float* ap_ij, float* av_ij, void* stream);
+int sph_compsph_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
+                     const float* m, const float* rho, const float* v, const float* c,
+                     const float* alpha, const float* P, const float* omega,
+                     const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                     float* dudt_out, void* stream);
+
+/* Monaghan-scheme right-hand side (schemes/monaghan.py:77-143) in one pass with the
+ * kernel-mean support: symmetric grad-h pressure force (computePressureForceSymmetric,
+ * modules/pressure/symmetricForce.py:7), PdV work (computeDudtMonaghan,
+ * modules/internalEnergy/dudt.py:7), artificial viscosity (computeViscosityWarp,
+ * modules/dissipation/wp_diffusion.py:246), conductivity with p->conductivity_term and
+ * Cu_l / Cu_q (computeConductivityWarp, wp_conductivity.py:246) and viscous heating
+ * (computeThermalDissipationWarp, wp_dissipation.py:249).  Outputs (any may be null):
+ * dvdt = pressure + viscosity, dudt = PdV + conductivity + heating, dEdt = m v.dvdt +
+ * m (PdV + conductivity) (monaghan.py:143), and each term on its own. */
+int sph_monaghan_rhs(const SphParams* p, int64_t n, const float* x, const float* H,
+                     const float* m, const float* rho, const float* v, const float* u,
+                     const float* c, const float* alpha, const float* P, const float* omega,
+                     const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                     float* dvdt_out, float* dudt_out, float* dEdt_out,
+                     float* dvdt_pressure, float* dvdt_viscosity, float* dudt_pdv,
+                     float* dudt_conductivity, float* dudt_heating, void* stream);
 
 /* Pairwise energy-partition fraction f_ij (modules/compSPH/balance.py:17-154) for
  * the six energy schemes, evaluated at v_half = v + dt/2 dvdt (schemes/crkSPH.py:341-363).

@@ -93,6 +93,13 @@ class Oracle:
         L.oracle_pressure_accel_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pressure_shift_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_deltasph_rhs.argtypes = [P, P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rp]
+        L.oracle_vsig.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_pi_pairs.argtypes = [P, i64, rp, rp, rp, rp, rpn, rpn, rp, _i32p, _i32p, _i32p, C.c_int, C.c_int, rp]
+        L.oracle_compsph_prep.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rpn, rpn, rpn]
+        L.oracle_compsph_accel_dudt.argtypes = [P, i64, rp, rp, rp, rp, rp, rpn, rpn, rp, rpn, _i32p, _i32p, _i32p,
+                                                rpn, rpn, rpn, rpn, rpn]
+        L.oracle_monaghan_rhs.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, rpn, rpn, rp, rpn, _i32p, _i32p, _i32p,
+                                          rpn, rpn, rpn, rpn]
         L.oracle_jacobi_solve.argtypes = [P, C.c_int, P, i64, rp, rp, rp, rp, rp, rpn, rp, real_c, _i32p, _i32p, _i32p, rp, rp,
                                           _f64p, C.POINTER(C.c_int)]
 
@@ -270,6 +277,54 @@ class Oracle:
         self.lib.oracle_deltasph_rhs(self._p(params), C.c_void_p(C.addressof(wc)), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho),
                                      self.arr(v), nb["offsets"], nb["counts"], nb["list"], gL, P, dv, dr)
         return dv, dr, gL, P
+
+    def vsig(self, params, x, H, v, c, nb):
+        out = np.zeros(len(H), self.dtype)
+        self.lib.oracle_vsig(self._p(params), len(H), self.arr(x), self.arr(H), self.arr(v), self.arr(c), nb["offsets"], nb["counts"],
+                             nb["list"], out)
+        return out
+
+    def _opt(self, a):
+        return None if a is None else self.arr(a)
+
+    def pi_pairs(self, params, x, H, rho, v, c, alpha, P, nb, useJ: bool = False, thermal: bool = False):
+        """Pi_ij * rho_j of computePi_actual for every Verlet entry."""
+        out = np.zeros(len(nb["list"]), self.dtype)
+        self.lib.oracle_pi_pairs(self._p(params), len(H), self.arr(x), self.arr(H), self.arr(rho), self.arr(v), self._opt(c),
+                                 self._opt(alpha), self.arr(P), nb["offsets"], nb["counts"], nb["list"], int(useJ), int(thermal), out)
+        return out
+
+    def compsph_prep(self, params, x, H, m, rho, v, nb, grad_h: bool = True):
+        """(omega or None, div, drhodt)"""
+        n = len(H)
+        om = np.zeros(n, self.dtype) if grad_h else None
+        div = np.zeros(n, self.dtype); dr = np.zeros(n, self.dtype)
+        self.lib.oracle_compsph_prep(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(v),
+                                     nb["offsets"], nb["counts"], nb["list"], om, div, dr)
+        return om, div, dr
+
+    def compsph_accel_dudt(self, params, x, H, m, rho, v, c, alpha, P, omega, nb):
+        """(dvdt, dudt, dEdt, ap_ij, av_ij)"""
+        n, d = len(H), params.dim
+        nnz = len(nb["list"])
+        dv = np.zeros((n, d), self.dtype); du = np.zeros(n, self.dtype); dE = np.zeros(n, self.dtype)
+        ap = np.zeros((nnz, d), self.dtype); av = np.zeros((nnz, d), self.dtype)
+        self.lib.oracle_compsph_accel_dudt(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(v),
+                                           self._opt(c), self._opt(alpha), self.arr(P), self._opt(omega), nb["offsets"], nb["counts"],
+                                           nb["list"], dv, du, dE, ap, av)
+        return dv, du, dE, ap, av
+
+    def monaghan_rhs(self, params, x, H, m, rho, v, u, c, alpha, P, omega, nb):
+        """(dvdt, dudt, dEdt, terms) with terms = dict(pressure, viscosity, pdv, conductivity, heating)."""
+        n, d = len(H), params.dim
+        dv = np.zeros((n, d), self.dtype); du = np.zeros(n, self.dtype); dE = np.zeros(n, self.dtype)
+        o5 = np.zeros((n, 2 * d + 3), self.dtype)
+        self.lib.oracle_monaghan_rhs(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(v), self.arr(u),
+                                     self._opt(c), self._opt(alpha), self.arr(P), self._opt(omega), nb["offsets"], nb["counts"],
+                                     nb["list"], dv, du, dE, o5)
+        terms = dict(pressure=o5[:, :d], viscosity=o5[:, d:2 * d], pdv=o5[:, 2 * d], conductivity=o5[:, 2 * d + 1],
+                     heating=o5[:, 2 * d + 2])
+        return dv, du, dE, terms
 
     def kernel_eval(self, kernel, dim, r, H):
         r = self.arr(r)

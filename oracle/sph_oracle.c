@@ -67,6 +67,8 @@ typedef struct {
     real target_neighbors;
     real cfl, min_dt, max_dt, dt_growth;
     real kscale, kxi;
+    real Cu_l, Cu_q, c_s;
+    int visc_term, cond_term, mswitch, correct_xi, scale_beta;
 } OP;
 
 static double kscale_tab(int kernel, int dim) {
@@ -96,6 +98,9 @@ static OP op_from(const SphParams* p) {
     o.cfl = (real)p->cfl; o.min_dt = (real)p->min_dt; o.max_dt = (real)p->max_dt; o.dt_growth = (real)p->dt_growth;
     o.kscale = (real)kscale_tab(p->kernel, p->dim);
     o.kxi = o.kscale;
+    o.Cu_l = (real)p->Cu_l; o.Cu_q = (real)p->Cu_q; o.c_s = (real)p->c_s;
+    o.visc_term = p->viscosity_term; o.cond_term = p->conductivity_term;
+    o.mswitch = p->monaghan_switch; o.correct_xi = p->correct_xi; o.scale_beta = p->scale_beta;
     return o;
 }
 
@@ -604,6 +609,33 @@ int oracle_switch_cullen(const SphParams* p, int64_t n, const real* x, const rea
         a0 = a0 < o.alpha_min ? o.alpha_min : (a0 > o.alpha_max ? o.alpha_max : a0);
         alpha_out[i] = a0;
         if (R_out) R_out[i] = R;
+    }
+    return 0;
+}
+
+/* Signal velocity over the Verlet set (modules/shockCapturing/wp_vsig.py:11-90): max_j of
+ * c_bar - mu_ij for approaching pairs with r < verletScale * max(H_i, H_j), absolute value. */
+int oracle_vsig(const SphParams* p, int64_t n, const real* x, const real* H, const real* v, const real* c,
+                const int32_t* offs, const int32_t* cnt, const int32_t* list, real* vsig_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real vsig = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real r = rsqrt_safe(dotD(d, d, D));
+            if (!(r < o.vs * wmax(H[i], H[j]))) continue;
+            real mu = 0;
+            for (int a = 0; a < D; ++a) mu += (v[i * D + a] - v[(int64_t)j * D + a]) * d[a];
+            mu = mu / (r + (real)1e-14 * H[i]);
+            real vsv = (real)0.5 * (c[i] + c[j]) - mu;
+            if (mu > 0) vsv = 0;
+            vsig = wmax(vsig, vsv);
+        }
+        vsig_out[i] = FABS(vsig);
     }
     return 0;
 }
@@ -1141,6 +1173,250 @@ int oracle_deltasph_rhs(const SphParams* p, const SphWcParams* w, int64_t n, con
         }
         drhodt[i] = -rhoi * cont + (real)w->density_delta * Hi / xi * (real)w->sound_speed * dd;
         for (int a = 0; a < D; ++a) dvdt[i * D + a] = -pf[a] + vs[a];
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ artificial viscosity Pi_ij
+ * modules/dissipation/pi.py:11-161 (computePi_actual) with util.py:6-38 (compute_mu_ij) and
+ * util.py:42-134 (compute_bars).  ux = (v_i - v_j).x_ij, x_ij = x_i - x_j.  Returns Pi_ij
+ * times rho_j, as the reference does (pi.py:8-9). */
+static real oracle_pi(const OP* o, real r, real ux, real hi, real hj, real rhoi, real rhoj, real Pi_, real Pj_,
+                      real ci, real cj, real ai, real aj, int useJ, int thermal) {
+    real rho_bar = (real)1 / (real)2 * (rhoi + rhoj);
+    real c_bar = (real)1 / (real)2 * (ci + cj);
+    real h_bar = (real)1 / (real)2 * (hi + hj);
+    real xi = o->correct_xi ? o->kxi : (real)1;
+    real Cl_ = thermal ? o->Cu_l : o->C_l, Cq_ = thermal ? o->Cu_q : o->C_q;
+    real C_l = (real)1 / (real)2 * (ai + aj) * Cl_;
+    real C_q = (real)1 / (real)2 * (ai + aj) * Cq_;
+    if (o->scale_beta) C_q = C_q * C_l;
+    int term = thermal ? o->cond_term : o->visc_term;
+    /* compute_mu_ij */
+    real mu0 = ux / (r + (real)1e-14 * h_bar);
+    real sfac = h_bar / xi / (r + (real)1e-14 * h_bar);
+    real mu, sf;
+    if (term == SPH_VISC_MONAGHAN1992) { mu = mu0 * sfac; sf = (real)1 * sfac; }
+    else if (term == SPH_VISC_DEFAULT || term == SPH_VISC_MONAGHANGINGOLD1983 || term == SPH_VISC_DELTASPH || term > SPH_VISC_DELTASPH) {
+        mu = mu0 * sfac; sf = h_bar / xi;
+    } else { mu = mu0; sf = 1; }
+    /* compute_bars */
+    int brho = 1, bc = 1, bh = 1;
+    if (term == SPH_VISC_CLEARY1998) { brho = 0; bc = 0; bh = 0; }
+    else if (term == SPH_VISC_MONAGHAN1992) bc = 0;
+    else if (term == SPH_VISC_DELTASPH) brho = 0;
+    real rho = brho ? rho_bar : (useJ ? rhoj : rhoi);
+    real c = bc ? c_bar : (useJ ? cj : ci);
+    real h = bh ? h_bar : (useJ ? hj : hi);
+    real v_sig = 0;
+    switch (term) {
+        case SPH_VISC_MONAGHANGINGOLD1983: v_sig = c; break;
+        case SPH_VISC_CLEARY1998: {
+            real f = (real)1 / ((real)2 * ((real)o->dim + (real)2));
+            real mi_ = f * ai * C_l * hi * ci * rhoi / xi, mj_ = f * aj * C_l * hj * cj * rhoj / xi;
+            v_sig = (real)19.8 * mi_ * mj_ / (rhoi * rhoj * (mi_ + mj_)) / (r + (real)1e-14 * h);
+            break;
+        }
+        case SPH_VISC_MONAGHAN1997B:
+            v_sig = rsqrt_safe(ci * ci + C_q * mu * mu) + rsqrt_safe(cj * cj + C_q * mu * mu) - mu; break;
+        case SPH_VISC_DUKOWICZ: v_sig = C_l * c - (real)3 / (real)4 * C_q * mu; break;
+        case SPH_VISC_PRICE2012: v_sig = C_l * c - C_q / (real)2 * mu; break;
+        case SPH_VISC_PRICE2008: {
+            real rb = (rhoi + rhoj) / (real)2;
+            v_sig = C_l * rsqrt_safe(FABS(Pi_ - Pj_) / (rb + (real)1e-14 * h));
+            break;
+        }
+        case SPH_VISC_WADSLEY2008: v_sig = C_l * FABS(mu); break;
+        default: v_sig = C_l * c - C_q * mu; break;   /* Monaghan1992, 1997a, Price2012_98, DeltaSPH, Default */
+    }
+    real val = rhoj * (real)1 / rho * v_sig * sf;
+    if (o->mswitch && !thermal && ux > 0) val = 0;
+    return val;
+}
+
+/* Pi_ij for every Verlet entry (tests compare it with the reference's computePi_actual). */
+int oracle_pi_pairs(const SphParams* p, int64_t n, const real* x, const real* H, const real* rho, const real* v, const real* c,
+                    const real* alpha, const real* Pr, const int32_t* offs, const int32_t* cnt, const int32_t* list, int useJ,
+                    int thermal, real* out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real r = rsqrt_safe(dotD(d, d, D)), ux = 0;
+            for (int a = 0; a < D; ++a) ux += (v[i * D + a] - v[(int64_t)j * D + a]) * d[a];
+            out[k] = oracle_pi(&o, r, ux, H[i], H[j], rho[i], rho[j], Pr[i], Pr[j], c ? c[i] : o.c_s, c ? c[j] : o.c_s,
+                               alpha ? alpha[i] : 1, alpha ? alpha[j] : 1, useJ, thermal);
+        }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ CompSPH / Monaghan schemes
+ * Omega: modules/adaptiveSupport/wp_omega.py:11-78, :140 (gather support).
+ * Cullen divergence: difference divergence, super-symmetric support, V_j = m_j/rho_j
+ * (CullenDehnen2010.py:246-257).  Consistent continuity (modules/momentum/consistent.py:
+ * 8-35): -(rho_i/Omega_i) * (1/rho_i) sum_j m_j (v_j - v_i).gradW(max(H_i,H_j)) -- the
+ * consistentDivergence operator of warpSPHCore is restated as the divergence weighted
+ * by m_j/rho_i (parity unpinned for that operator). */
+int oracle_compsph_prep(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                        const real* v, const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                        real* omega, real* div, real* drhodt) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real Hi = H[i], dh_drho = -Hi / (rho[i] * (real)D), om = 0, sdiv = 0, scon = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real r = rsqrt_safe(dotD(d, d, D));
+            real W, dWdh;
+            kWdH(&o, r, Hi, &W, &dWdh);
+            om += dh_drho * m[j] * dWdh;
+            if (div || drhodt) {
+                real g[3], W2, s = 0;
+                kWG(&o, d, r, wmax(Hi, H[j]), &W2, g);
+                for (int a = 0; a < D; ++a) s += (v[(int64_t)j * D + a] - v[i * D + a]) * g[a];
+                sdiv += m[j] / rho[j] * s;
+                scon += m[j] * s;
+            }
+        }
+        real Om = omega ? (real)1 - om : (real)1;
+        if (omega) omega[i] = Om;
+        if (div) div[i] = sdiv;
+        if (drhodt) drhodt[i] = -(rho[i] / Om) * (scon / rho[i]);
+    }
+    return 0;
+}
+
+/* modules/compSPH/accel.py:60-154 and modules/compSPH/dudt.py:60-139 (see the GPU pass). */
+int oracle_compsph_accel_dudt(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                              const real* v, const real* c, const real* alpha, const real* Pr, const real* omega,
+                              const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                              real* dvdt, real* dudt, real* dEdt, real* ap, real* av) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        const real *xi = x + i * D, *vi = v + i * D;
+        real Hi = H[i], rhoi = rho[i], Pi = Pr[i];
+        real ci = c ? c[i] : o.c_s, ai = alpha ? alpha[i] : 1, omi = omega ? omega[i] : 1;
+        real pTi = Pi / (rhoi * rhoi) / omi;
+        real acc[3] = {0, 0, 0}, accc[3] = {0, 0, 0}, du = 0, duc = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            const real* vj = v + (int64_t)j * D;
+            real d[3];
+            dist_vec(&o, xi, x + (int64_t)j * D, d);
+            real r = rsqrt_safe(dotD(d, d, D));
+            real Hj = H[j], mj = m[j], rhoj = rho[j], Pj = Pr[j];
+            real cj = c ? c[j] : o.c_s, aj = alpha ? alpha[j] : 1, omj = omega ? omega[j] : 1;
+            real Vj = mj / rhoj;
+            real rho_bar = (real)0.5 * (rhoi + rhoj);
+            real ux = 0, uxr = 0;
+            for (int a = 0; a < D; ++a) { ux += (vi[a] - vj[a]) * d[a]; uxr += (vj[a] - vi[a]) * d[a]; }
+            real pi_i = oracle_pi(&o, r, ux, Hi, Hj, rhoi, rhoj, Pi, Pj, ci, cj, ai, aj, 0, 0) * (rho_bar / rhoi);
+            real pi_j = oracle_pi(&o, r, ux, Hi, Hj, rhoi, rhoj, Pi, Pj, ci, cj, ai, aj, 1, 0) * (rho_bar / rhoj);
+            real Wi, Wj, gi[3], gj[3], gw[3];
+            kWG(&o, d, r, Hi, &Wi, gi);
+            kWG(&o, d, r, Hj, &Wj, gj);
+            for (int a = 0; a < D; ++a) gw[a] = (real)0.5 * (gi[a] + gj[a]);
+            real pTj = Pj / (rhoj * rhoj) / omj;
+            real mu = uxr / (r + (real)1.0e-14 * Hi);
+            real dotg = 0;
+            for (int a = 0; a < D; ++a) {
+                real pt = -(pTi * gw[a] + pTj * gw[a]) * mj;
+                real vt = -(real)0.5 * (pi_i * gw[a] + pi_j * gw[a]) * Vj * mu;
+                if (ap) ap[(int64_t)k * D + a] = pt;
+                if (av) av[(int64_t)k * D + a] = vt;
+                kahan_add(&acc[a], &accc[a], pt + vt, o.kahan);
+                dotg += (vj[a] - vi[a]) * gi[a];
+            }
+            real pTerm = -Vj * pTi * rhoj * dotg;
+            real vTerm = -(real)0.5 * Vj * pi_i * mu * dotg;
+            kahan_add(&du, &duc, pTerm + vTerm, o.kahan);
+        }
+        real a_[3], vdot = 0;
+        for (int a = 0; a < D; ++a) { a_[a] = acc[a] + accc[a]; vdot += vi[a] * a_[a]; }
+        if (dvdt) for (int a = 0; a < D; ++a) dvdt[i * D + a] = a_[a];
+        if (dudt) dudt[i] = du + duc;
+        if (dEdt) dEdt[i] = m[i] * vdot + m[i] * (du + duc);
+    }
+    return 0;
+}
+
+/* Monaghan scheme (schemes/monaghan.py:77-143), kernel-mean support.  The symmetric
+ * pressure gradient with grad-h terms is the warpSPHCore operator restated as
+ * rho_i sum_j m_j (P_i/(Omega_i rho_i^2) + P_j/(Omega_j rho_j^2)) gradW (parity unpinned);
+ * the viscosity, conductivity and heating pair bodies are wp_diffusion.py:71-107,
+ * wp_conductivity.py:59-115 and wp_dissipation.py:59-119.  out5 (nullable) receives the
+ * five terms: [pressure (D), viscosity (D), PdV, conductivity, heating] per particle. */
+int oracle_monaghan_rhs(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                        const real* v, const real* u, const real* c, const real* alpha, const real* Pr, const real* omega,
+                        const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                        real* dvdt, real* dudt, real* dEdt, real* out5) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        const real *xi = x + i * D, *vi = v + i * D;
+        real Hi = H[i], rhoi = rho[i], Pi = Pr[i], ui = u[i];
+        real ci = c ? c[i] : o.c_s, ai = alpha ? alpha[i] : 1, omi = omega ? omega[i] : 1;
+        real pTi = Pi / (rhoi * rhoi) / omi;
+        real sp[3] = {0, 0, 0}, spc[3] = {0, 0, 0}, sv[3] = {0, 0, 0}, svc[3] = {0, 0, 0};
+        real pdv = 0, pdvc = 0, cond = 0, condc = 0, heat = 0, heatc = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            const real* vj = v + (int64_t)j * D;
+            real d[3];
+            dist_vec(&o, xi, x + (int64_t)j * D, d);
+            real r = rsqrt_safe(dotD(d, d, D));
+            real Hj = H[j], mj = m[j], rhoj = rho[j], Pj = Pr[j];
+            real cj = c ? c[j] : o.c_s, aj = alpha ? alpha[j] : 1, omj = omega ? omega[j] : 1;
+            real Vj = mj / rhoj;
+            real ux = 0, uxr = 0;
+            for (int a = 0; a < D; ++a) { ux += (vi[a] - vj[a]) * d[a]; uxr += (vj[a] - vi[a]) * d[a]; }
+            real pi_v = oracle_pi(&o, r, ux, Hi, Hj, rhoi, rhoj, Pi, Pj, ci, cj, ai, aj, 0, 0);
+            real pi_u = oracle_pi(&o, r, ux, Hi, Hj, rhoi, rhoj, Pi, Pj, ci, cj, ai, aj, 0, 1);
+            real Wi, Wj, gi[3], gj[3], gk[3];
+            kWG(&o, d, r, Hi, &Wi, gi);
+            kWG(&o, d, r, Hj, &Wj, gj);
+            for (int a = 0; a < D; ++a) gk[a] = (real)0.5 * (gi[a] + gj[a]);
+            real pTj = Pj / (rhoj * rhoj) / omj;
+            real den = r + (real)1.0e-14 * Hi;
+            real mu = ux / den, mup = uxr / den;
+            real dvg = 0, lap = 0;
+            for (int a = 0; a < D; ++a) {
+                kahan_add(&sp[a], &spc[a], mj * (pTi + pTj) * gk[a], o.kahan);
+                kahan_add(&sv[a], &svc[a], Vj * pi_v * gk[a] * mu, o.kahan);
+                dvg += (vj[a] - vi[a]) * gk[a];
+                lap += gk[a] * (d[a] / den);
+            }
+            kahan_add(&pdv, &pdvc, mj * dvg, o.kahan);
+            kahan_add(&cond, &condc, -(real)0.5 * Vj * pi_u * (u[j] - ui) * lap, o.kahan);
+            kahan_add(&heat, &heatc, -Vj * pi_v * (mup * mup) * lap, o.kahan);
+        }
+        real ap_[3], av_[3], vdot = 0;
+        for (int a = 0; a < D; ++a) {
+            ap_[a] = -(rhoi * (sp[a] + spc[a])) / rhoi;
+            av_[a] = sv[a] + svc[a];
+            vdot += vi[a] * (ap_[a] + av_[a]);
+        }
+        real du_pdv = -(Pi / rhoi / omi) * ((pdv + pdvc) / rhoi);
+        real du_cond = cond + condc, du_heat = heat + heatc;
+        if (dvdt) for (int a = 0; a < D; ++a) dvdt[i * D + a] = ap_[a] + av_[a];
+        if (dudt) dudt[i] = du_pdv + du_cond + du_heat;
+        if (dEdt) dEdt[i] = m[i] * vdot + m[i] * (du_pdv + du_cond);
+        if (out5) {
+            real* q = out5 + i * (2 * D + 3);
+            for (int a = 0; a < D; ++a) { q[a] = ap_[a]; q[D + a] = av_[a]; }
+            q[2 * D] = du_pdv; q[2 * D + 1] = du_cond; q[2 * D + 2] = du_heat;
+        }
     }
     return 0;
 }

@@ -141,6 +141,69 @@ class CRKSPHOracle:
         return Sf, updates, rvs
 
 
+class CompSPHOracle(CRKSPHOracle):
+    """One right-hand-side evaluation of schemes/compSPH.py:22-215 on the C oracle
+    (gather density, grad-h Omega, Cullen switch, CompSPH accel/dudt, energy partition);
+    staging and compatible-energy finalize as in CRKSPHOracle."""
+
+    def __init__(self, params, precision: str = "f32", grad_h: bool = True, **kw):
+        super().__init__(params, precision, **kw)
+        self.grad_h = grad_h
+
+    def rhs(self, st, dt):
+        o, p = self.o, self.p
+        st = dict(st)
+        if self.adaptive:
+            st["densities"], st["supports"] = self.optimal_support(st)
+        x, H, m, v, u = st["positions"], st["supports"], st["masses"], st["velocities"], st["internalEnergies"]
+        nb = self.nb(x, H)
+        rho = o.density(p, 0, x, H, m, nb)
+        st["densities"] = rho
+        if st.get("divergence") is None:
+            st["divergence"] = o.compsph_prep(p, x, H, m, rho, v, nb, grad_h=False)[2]
+        st["entropies"], st["pressures"], st["soundspeeds"] = o.eos(p, u, rho)
+        c, P = st["soundspeeds"], st["pressures"]
+        om, div, drho = o.compsph_prep(p, x, H, m, rho, v, nb, grad_h=self.grad_h)
+        if self.switch == SWITCH_CULLEN:
+            vs = o.vsig(p, x, H, v, c, nb)
+            st["alphas"], _ = o.switch_cullen(p, x, H, m, rho, div, st["divergence"], vs, st["alpha0s"], dt, nb)
+        dvdt, dudt, dEdt, ap, av = o.compsph_accel_dudt(p, x, H, m, rho, v, c, st.get("alphas"), P, om, nb)
+        if self.switch == SWITCH_CULLEN:
+            st["alpha0s"] = st["alphas"]
+        st["divergence"] = (-drho / rho).astype(self.dt_)
+        st["ap_ij"], st["av_ij"] = ap, av
+        st["f_ij"] = o.balance(p, m, rho, P, u, v, dvdt, dt, nb, ap, av)
+        upd = dict(dxdt=v, dvdt=dvdt, dudt=dudt, drhodt=drho, dEdt=dEdt)
+        return upd, nb, st, dict(omega=om, div_cd=div)
+
+
+class MonaghanOracle(CRKSPHOracle):
+    """One right-hand-side evaluation of schemes/monaghan.py:13-158 on the C oracle;
+    no compatible-energy finalize (the scheme integrates u directly)."""
+
+    def __init__(self, params, precision: str = "f32", grad_h: bool = True, density_mode: int = 3, **kw):
+        kw.setdefault("compatible_energy", False)
+        kw.setdefault("switch", SWITCH_NONE)
+        super().__init__(params, precision, **kw)
+        self.grad_h = grad_h
+        self.density_mode = density_mode
+
+    def rhs(self, st, dt):
+        o, p = self.o, self.p
+        st = dict(st)
+        if self.adaptive:
+            st["densities"], st["supports"] = self.optimal_support(st)
+        x, H, m, v, u = st["positions"], st["supports"], st["masses"], st["velocities"], st["internalEnergies"]
+        nb = self.nb(x, H)
+        rho = o.density(p, self.density_mode, x, H, m, nb)
+        st["densities"] = rho
+        st["entropies"], st["pressures"], st["soundspeeds"] = o.eos(p, u, rho)
+        om, _, drho = o.compsph_prep(p, x, H, m, rho, v, nb, grad_h=self.grad_h)
+        dvdt, dudt, dEdt, _ = o.monaghan_rhs(p, x, H, m, rho, v, u, st["soundspeeds"], st.get("alphas"), st["pressures"], om, nb)
+        upd = dict(dxdt=v, dvdt=dvdt, dudt=dudt, drhodt=drho, dEdt=dEdt)
+        return upd, nb, st, dict(omega=om)
+
+
 def state_to_numpy(state, dtype=np.float32) -> dict:
     """Copies the tensors of a CompSPHState-like object into numpy arrays."""
     out = {}

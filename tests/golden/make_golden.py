@@ -137,12 +137,34 @@ def kWG(x, r, H):
     return F(W), (F(s) * np.asarray(x, F)).astype(F)
 
 
+def kWdH(r, H):
+    K, D = Ctx.kernel, Ctx.dim
+    q = F(r) / F(H)
+    if not (q < F(1)):
+        return F(0), F(0)
+    k, p = kernel_kp(K, D, q)
+    cH = kernel_C(K, D) / ipowD(F(H), D)
+    return F(cH * k), F(-cH / F(H) * (F(D) * k - q * q * p))
+
+
 def computeKernelGradientCRK(xi, xj, hi, hj, kernelProperties, domainState, useCRK, A, B, gradA, gradB):
-    # W evaluated with hj (the two supports are equal at every reference call site)
+    # The CRK call sites pass equal supports; the CompSPH / Monaghan call sites pass
+    # (H_i, H_j) and the operation's support scheme picks the gradient: gather uses H_i,
+    # the kernel-mean scheme averages the two gradients.
     D = Ctx.dim
     x = computeDistanceVec(xi, xj, domainState)
     r = safe_sqrt(wp.dot(x, x))
-    W, gW = kWG(x, r, hj)
+    mode = getattr(kernelProperties, "supportMode", None)
+    if mode == "gather":
+        W, gW = kWG(x, r, hi)
+    elif mode == "kernelMeanSymmetric":
+        Wi, gi = kWG(x, r, hi)
+        Wj, gj = kWG(x, r, hj)
+        W, gW = F(F(0.5) * (Wi + Wj)), (F(0.5) * (gi + gj)).astype(F)
+    else:
+        W, gW = kWG(x, r, hj)
+    if not useCRK:
+        return gW
     B = np.asarray(B, F)
     bx = F(1) + wp.dot(B, x)
     out = np.zeros(D, F)
@@ -151,6 +173,19 @@ def computeKernelGradientCRK(xi, xj, hi, hj, kernelProperties, domainState, useC
         for a in range(1, D):
             gbx = gbx + F(gradB[a][g]) * x[a]
         out[g] = F(A) * bx * gW[g] + F(A) * B[g] * W + F(gradA[g]) * bx * W + F(A) * gbx * W
+    return out
+
+
+def sphKernelDkDh(xi, xj, hi, hj, kernelProperties, domainState):
+    # gather support (the only call site, wp_omega.py:71, runs under SupportScheme.Gather)
+    x = computeDistanceVec(xi, xj, domainState)
+    return kWdH(safe_sqrt(wp.dot(x, x)), hi)[1]
+
+
+def iPow(x, n):
+    out = F(x)
+    for _ in range(int(n) - 1):
+        out = F(out * F(x))
     return out
 
 
@@ -203,6 +238,7 @@ CORE = dict(scalar_t=F, vector=vector, matrix=matrix, Any=Any, OperationDirectio
             computeDistanceVec=computeDistanceVec, safe_sqrt=safe_sqrt, computeKernelGradientCRK=computeKernelGradientCRK,
             sphKernelScale=sphKernelScale, sphKernel_xi=sphKernel_xi, zero_like_warp=zero_like_warp, matmul=matmul,
             getParticle=getParticle, getVolume_j=getVolume_j, getCRK_j=getCRK_j, checkDirectionality_j=checkDirectionality_j,
+            sphKernelDkDh=sphKernelDkDh, iPow=iPow,
             domainData=None, kernelState=None, adjacencyData=None, gridData=None)
 
 
@@ -556,10 +592,152 @@ def run_reference_dfsph(ref: Path, case: dict) -> dict:
     return out
 
 
+# ---------------------------------------------------------------- CompSPH and Monaghan-scheme pair bodies
+PI_VARIANTS = np.array([[1, 0, 1], [0, 1, 0]], np.int32)   # (monaghanSwitch, scaleBeta, correctXi)
+PI_COEFFS = np.array([1.0, 2.0, 0.7, 1.3, 1.0], np.float64)  # C_l, C_q, Cu_l, Cu_q, c_s
+
+
+def make_compsph_case(seed=5, n_side=14):
+    """Periodic unit box, varied supports, compressive + shearing flow, gather density,
+    ideal-gas pressure and sound speed, a spread of switch values."""
+    from oracle import oracle
+    from oracle.steps import cell_capacity_for
+    from tests.cases import make_params, make_particles
+    import warpsph_b200 as ws
+    cfg, sch, p = make_params(2, kernel=ws.KernelFunctions.Wendland4)
+    P = make_particles(2, n_side, seed=seed, jitter=0.4, flow=1.0, h_spread=0.15)
+    n = len(P["masses"])
+    rng = np.random.default_rng(seed + 300)
+    x, H, m = P["positions"], P["supports"], P["masses"]
+    v = (P["velocities"] - 1.5 * x + 0.3 * rng.standard_normal(x.shape)).astype(F)
+    u = (1.0 + 3.0 * rng.random(n)).astype(F)
+    alpha = (0.2 + 1.3 * rng.random(n)).astype(F)
+    o = oracle.get("f32")
+    nb = o.neighbors(p, x, H, cell_capacity_for(n, 2))
+    rho = o.density(p, 0, x, H, m, nb)
+    _, Pr, c = o.eos(p, u, rho)
+    sel = np.sort(rng.choice(len(nb["list"]), 512, replace=False)).astype(np.int64)
+    return dict(params=p, x=x, H=H, m=m, v=v, u=u, alpha=alpha, rho=rho, P=Pr, c=c, nb=nb, n=n, pi_sel=sel)
+
+
+def run_reference_compsph(ref: Path, case: dict) -> dict:
+    """Executes, per particle and unmodified: computeOmega_Func_i (wp_omega.py), the
+    CompSPH pair bodies computeCompSPHAccel_Func_i / computeCompSPHdudt_Func_i
+    (modules/compSPH/accel.py, dudt.py) for every ViscosityTerms form, computePi_actual
+    (modules/dissipation/pi.py) on a sample of pairs for every form and two flag
+    settings, and the Monaghan-scheme dissipation bodies (wp_diffusion.py,
+    wp_conductivity.py, wp_dissipation.py) under the kernel-mean support."""
+    p = case["params"]
+    n, nb = case["n"], case["nb"]
+    offs, cnt, lst = nb["offsets"], nb["counts"], nb["list"].astype(np.int64)
+    nnz = len(lst)
+    row = np.repeat(np.arange(n), cnt)
+    x, H, m, v, u, rho, Pr, c, alpha = (case[k] for k in ("x", "H", "m", "v", "u", "rho", "P", "c", "alpha"))
+    state = SoA(positions=x, supports=H, masses=m, densities=rho, kinds=np.zeros(n, np.int32))
+    dom = SoA(dim=2)
+    diff = load(ref, "configurations/moduleConfigurations/diffusionParameters.py")
+    util = load(ref, "modules/dissipation/util.py", {"ViscosityTerms": diff["ViscosityTerms"]})
+    pi = load(ref, "modules/dissipation/pi.py", {"ViscosityTerms": diff["ViscosityTerms"], "DiffusionParameters": None,
+                                               "compute_mu_ij": util["compute_mu_ij"], "compute_bars": util["compute_bars"]})
+    common = dict(DiffusionParameters=None, computePi_actual=pi["computePi_actual"])
+    om_ns = load(ref, "modules/adaptiveSupport/wp_omega.py")
+    acc = load(ref, "modules/compSPH/accel.py", common)
+    dud = load(ref, "modules/compSPH/dudt.py", common)
+    vis = load(ref, "modules/dissipation/wp_diffusion.py", common)
+    con = load(ref, "modules/dissipation/wp_conductivity.py", common)
+    dis = load(ref, "modules/dissipation/wp_dissipation.py", common)
+    C_l, C_q, Cu_l, Cu_q, c_s = (F(a) for a in PI_COEFFS)
+
+    def visc_params(term, cterm, sw=True, sb=False, cx=True):
+        return SoA(c_s=c_s, C_l=C_l, C_q=C_q, Cu_l=Cu_l, Cu_q=Cu_q, K=F(1), thermalConductivity=F(0.5), viscosityTerm=int(term),
+                   thermalConducitiyTerm=int(cterm), scaleBeta=bool(sb), monaghanSwitch=bool(sw), correctXi=bool(cx))
+
+    def base(i, kp, vp):
+        return dict(i=i, dim=2, xi=x[i], hi=F(H[i]), mi=F(m[i]), rhoi=F(rho[i]), referenceState=state, domainState=dom,
+                    kernelProperties=kp, beginIndex=int(offs[i]), numIndices=int(cnt[i]), offsetArray=lst, ki=0,
+                    referenceKinds=state.kinds, useGradientRenormalization=False, Li=None, useGradHTerms=True,
+                    omega_i=F(omega[i]) if omega is not None else F(1), referenceOmegas=omega, Viscosity_i=F(1),
+                    referenceViscositys=None, useVolume=False, Vi=F(0), referenceVolumes=None, useCRK=False, Ai=F(1),
+                    Bi=np.zeros(2, F), gradAi=np.zeros(2, F), gradBi=np.zeros((2, 2), F), vel_i=v[i], referenceVelocities=v,
+                    u_i=F(u[i]), referenceEnergies=u, individual_cs=True, cs_i=F(c[i]), referenceCs=c, viscositySwitch=True,
+                    alpha_i=F(alpha[i]), referenceAlphas=alpha, explicitPressure=True, P_i=F(Pr[i]), referencePressures=Pr,
+                    viscosityParams=vp, outputValue=F(0))
+
+    out = {}
+    omega = None
+    kp_g = SoA(operationMode=0, kernelFunction=int(p.kernel), supportMode="gather")
+    om = np.zeros(n, F)
+    with np.errstate(all="ignore"):
+        for i in range(n):
+            vals = base(i, kp_g, None)
+            vals["useGradHTerms"] = False
+            s = call(om_ns["computeOmega_Func_i"], **vals)
+            om[i] = F(1) - s
+    out["omega"] = om
+    omega = om
+
+    # computePi_actual on the sampled pairs: [variant, term, (i, j, thermal), pair]
+    sel = case["pi_sel"]
+    pis = np.zeros((len(PI_VARIANTS), 12, 3, len(sel)), F)
+    with np.errstate(all="ignore"):
+        for vi_, (sw, sb, cx) in enumerate(PI_VARIANTS):
+            for t in range(12):
+                vp = visc_params(t, t, sw, sb, cx)
+                for q, k in enumerate(sel):
+                    i, j = row[k], lst[k]
+                    args = (x[i], x[j], F(H[i]), F(H[j]), F(m[i]), F(m[j]), F(rho[i]), F(rho[j]), True, F(Pr[i]), F(Pr[j]),
+                            v[i], v[j], dom, int(p.kernel), F(c[i]), F(c[j]), F(alpha[i]), F(alpha[j]), vp)
+                    pis[vi_, t, 0, q] = pi["computePi_actual"](*args, False, False)
+                    pis[vi_, t, 1, q] = pi["computePi_actual"](*args, True, False)
+                    pis[vi_, t, 2, q] = pi["computePi_actual"](*args, False, True)
+    out["pi"] = pis
+
+    # CompSPH accel (kernel-mean via explicit (H_i,H_i) / (H_j,H_j) calls) and dudt (gather)
+    kp_a = SoA(operationMode=0, kernelFunction=int(p.kernel), supportMode=None)
+    acc_t = np.zeros((12, n, 2), F)
+    dud_t = np.zeros((12, n), F)
+    ap = np.zeros((nnz, 2), F)
+    av = np.zeros((nnz, 2), F)
+    with np.errstate(all="ignore"):
+        for t in range(12):
+            vp = visc_params(t, t)
+            ap_t = np.zeros((nnz, 2), F)
+            av_t = np.zeros((nnz, 2), F)
+            for i in range(n):
+                vals = base(i, kp_a, vp)
+                vals.update(pressureAccel_ij=ap_t, viscosityAccel_ij=av_t)
+                acc_t[t, i] = call(acc["computeCompSPHAccel_Func_i"], **vals)
+                vals["kernelProperties"] = kp_g
+                dud_t[t, i] = call(dud["computeCompSPHdudt_Func_i"], **vals)
+            if t == 3:      # Monaghan1992, the CompSPH default
+                ap[:], av[:] = ap_t, av_t
+    out.update(compsph_accel=acc_t, compsph_dudt=dud_t, compsph_ap=ap, compsph_av=av)
+
+    # Monaghan-scheme dissipation bodies, kernel-mean support, two parameter sets
+    kp_k = SoA(operationMode=0, kernelFunction=int(p.kernel), supportMode="kernelMeanSymmetric")
+    sets = np.array([[7, 9], [3, 7]], np.int32)   # (viscosityTerm, thermalConducitiyTerm)
+    visc_o = np.zeros((len(sets), n, 2), F)
+    cond_o = np.zeros((len(sets), n), F)
+    heat_o = np.zeros((len(sets), n), F)
+    with np.errstate(all="ignore"):
+        for si, (t, ct) in enumerate(sets):
+            vp = visc_params(t, ct)
+            for i in range(n):
+                vals = base(i, kp_k, vp)
+                vals["useGradHTerms"] = False
+                vals["outputValue"] = np.zeros(2, F)
+                visc_o[si, i] = call(vis["computeViscosity_Func_i"], **vals)
+                vals["outputValue"] = F(0)
+                cond_o[si, i] = call(con["computeConductivity_Func_i"], **vals)
+                heat_o[si, i] = call(dis["computeThermalDissipation_Func_i"], **vals)
+    out.update(monaghan_sets=sets, monaghan_viscosity=visc_o, monaghan_conductivity=cond_o, monaghan_heating=heat_o)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--which", choices=["all", "crk", "dfsph"], default="all")
+    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph"], default="all")
     a = ap.parse_args()
     ref = Path(a.reference)
     if a.which in ("all", "crk"):
@@ -581,6 +759,15 @@ def main():
                             **out)
         print("wrote", Path(__file__).parent / "dfsph_golden.npz", "particles", case["n"], "pairs", len(nb["list"]),
               {k: len(out[k]) for k in out if k.endswith("_errors")})
+    if a.which in ("all", "compsph"):
+        case = make_compsph_case()
+        out = run_reference_compsph(ref, case)
+        nb = case["nb"]
+        np.savez_compressed(Path(__file__).parent / "compsph_golden.npz",
+                            x=case["x"], H=case["H"], m=case["m"], v=case["v"], u=case["u"], alpha=case["alpha"], rho=case["rho"],
+                            P=case["P"], c=case["c"], offsets=nb["offsets"], counts=nb["counts"], list=nb["list"],
+                            pi_sel=case["pi_sel"], pi_variants=PI_VARIANTS, pi_coeffs=PI_COEFFS, **out)
+        print("wrote", Path(__file__).parent / "compsph_golden.npz", "particles", case["n"], "pairs", len(nb["list"]))
 
 
 if __name__ == "__main__":

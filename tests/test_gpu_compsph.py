@@ -1,0 +1,224 @@
+"""CompSPH and Monaghan-scheme CUDA passes (through the C ABI) against the golden
+vectors of the reference's own pair bodies and against the CPU oracle; full CompSPH and
+Monaghan integrator steps against the oracle's steps; conservation of the CompSPH step
+with compatible energy.
+
+The GPU replaces repeated divisions by reciprocal multiplications and sums each row in
+G interleaved partial sums, so tolerances are relative to each field's scale (stated at
+each assertion)."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+import warpsph_b200 as ws
+from oracle import oracle
+from oracle.steps import SWITCH_CULLEN, SWITCH_NONE, CompSPHOracle, MonaghanOracle, cell_capacity_for, state_to_numpy
+from tests.cases import assert_close, make_params, make_particles
+from warpsph_b200 import core, ops
+from warpsph_b200.core import AdjacencyList
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden" / "compsph_golden.npz"
+
+
+def params_for(g, term=3, cterm=None, dim=2, kernel=core.KernelFunctions.Wendland4, kahan=False):
+    cfg, sch, p = make_params(dim, kernel=kernel, kahan=kahan)
+    p.C_l, p.C_q, p.Cu_l, p.Cu_q, p.c_s = (float(a) for a in g["pi_coeffs"]) if g is not None else (1.0, 2.0, 0.7, 1.3, 1.0)
+    p.viscosity_term = int(term)
+    p.conductivity_term = int(term if cterm is None else cterm)
+    p.monaghan_switch, p.scale_beta, p.correct_xi = 1, 0, 1
+    return p
+
+
+@pytest.fixture(scope="module")
+def G(cuda):
+    g = dict(np.load(GOLD))
+    return {k: torch.from_numpy(np.ascontiguousarray(v)).to(cuda) for k, v in g.items()}, g
+
+
+def verlet_adjacency(t):
+    n = t["offsets"].shape[0]
+    return AdjacencyList(neighborOffsets=t["offsets"], numNeighbors=t["counts"], neighborList=t["list"], numRows=n, numCols=n,
+                         nnz=int(t["list"].shape[0]))
+
+
+def built_adjacency(p, x, H):
+    """The library's own list (Verlet + interacting subset); equal to the oracle's list."""
+    return ops.buildVerletList(x, H, p, float(p.verlet_scale))
+
+
+def test_gpu_golden_omega_and_pi_forms(G):
+    """Omega against wp_omega.py; every ViscosityTerms form through the fused CompSPH pass
+    against the reference's accel.py / dudt.py bodies."""
+    t, g = G
+    adj = verlet_adjacency(t)
+    om, _, _ = ops.compsph_prep(params_for(g), t["x"], t["H"], t["m"], t["rho"], t["v"], adj, want_div=False, want_drhodt=False)
+    assert_close(om.cpu().numpy(), g["omega"], 1e-5, 1e-6, "Omega vs reference wp_omega.py (GPU)")
+    for term in range(12):
+        p = params_for(g, term)
+        dvdt, dudt, dEdt, ap, av = ops.compsph_accel_dudt(p, t["x"], t["H"], t["m"], t["rho"], t["v"], t["c"], t["alpha"], t["P"],
+                                                          t["omega"], adj)
+        assert_close(dvdt.cpu().numpy(), g["compsph_accel"][term], 1e-4, 1e-5, f"dv/dt vs reference compSPH/accel.py term {term} (GPU)")
+        assert_close(dudt.cpu().numpy(), g["compsph_dudt"][term], 1e-4, 1e-5, f"du/dt vs reference compSPH/dudt.py term {term} (GPU)")
+        if term == 3:
+            assert_close(ap.cpu().numpy(), g["compsph_ap"], 1e-4, 1e-5, "ap_ij vs reference (GPU)")
+            assert_close(av.cpu().numpy(), g["compsph_av"], 1e-4, 1e-5, "av_ij vs reference (GPU)")
+
+
+def test_gpu_golden_interacting_list(G):
+    """The same golden results through the library's own list and its interacting subset
+    (stride-2 rows; pairwise arrays still indexed by Verlet entry)."""
+    t, g = G
+    p = params_for(g)
+    adj = built_adjacency(p, t["x"], t["H"])
+    assert adj.interList is not None
+    assert adj.nnz == t["list"].shape[0]
+    assert torch.equal(adj.neighborList[: adj.nnz], t["list"].to(adj.neighborList.dtype)), "library list differs from the oracle's"
+    dvdt, dudt, dEdt, ap, av = ops.compsph_accel_dudt(p, t["x"], t["H"], t["m"], t["rho"], t["v"], t["c"], t["alpha"], t["P"],
+                                                      t["omega"], adj)
+    assert_close(dvdt.cpu().numpy(), g["compsph_accel"][3], 1e-4, 1e-5, "dv/dt (interacting list)")
+    assert_close(dudt.cpu().numpy(), g["compsph_dudt"][3], 1e-4, 1e-5, "du/dt (interacting list)")
+    assert_close(ap.cpu().numpy(), g["compsph_ap"], 1e-4, 1e-5, "ap_ij (interacting list)")
+    assert_close(av.cpu().numpy(), g["compsph_av"], 1e-4, 1e-5, "av_ij (interacting list)")
+    for which in range(2):
+        tt, ct = g["monaghan_sets"][which]
+        pm = params_for(g, tt, ct)
+        for a in (adj, verlet_adjacency(t)):
+            dv, du, dE, T = ops.monaghan_rhs(pm, t["x"], t["H"], t["m"], t["rho"], t["v"], t["u"], t["c"], t["alpha"], t["P"],
+                                             t["omega"], a, terms=True)
+            assert_close(T["viscosity"].cpu().numpy(), g["monaghan_viscosity"][which], 1e-4, 1e-5, "viscosity vs wp_diffusion.py (GPU)")
+            assert_close(T["conductivity"].cpu().numpy(), g["monaghan_conductivity"][which], 1e-4, 1e-5,
+                         "conductivity vs wp_conductivity.py (GPU)")
+            assert_close(T["heating"].cpu().numpy(), g["monaghan_heating"][which], 1e-4, 1e-5, "heating vs wp_dissipation.py (GPU)")
+
+
+CASES = [(2, 40, core.KernelFunctions.Wendland4, False), (2, 32, core.KernelFunctions.Wendland2, True),
+         (3, 10, core.KernelFunctions.Wendland6, False), (1, 200, core.KernelFunctions.Wendland4, False)]
+
+
+def case_inputs(dim, n_side, kernel, kahan, cuda, seed=11):
+    P = make_particles(dim, n_side, seed=seed, jitter=0.4, h_spread=0.15)
+    p = params_for(None, dim=dim, kernel=kernel, kahan=kahan)
+    rng = np.random.default_rng(seed)
+    n = len(P["masses"])
+    x, H, m = P["positions"], P["supports"], P["masses"]
+    v = (P["velocities"] - 1.5 * x + 0.2 * rng.standard_normal(x.shape)).astype(np.float32)
+    u = P["internalEnergies"]
+    alpha = (0.2 + rng.random(n)).astype(np.float32)
+    o = oracle.get("f32")
+    nb = o.neighbors(p, x, H, cell_capacity_for(n, dim))
+    rho = o.density(p, 0, x, H, m, nb)
+    _, Pr, c = o.eos(p, u, rho)
+    host = dict(x=x, H=H, m=m, v=v, u=u, alpha=alpha, rho=rho, P=Pr, c=c)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(a)).to(cuda) for k, a in host.items()}
+    return p, nb, host, dev
+
+
+@pytest.mark.parametrize("dim,n_side,kernel,kahan", CASES)
+def test_gpu_prep_accel_monaghan_match_oracle(cuda, dim, n_side, kernel, kahan):
+    p, nb, h, d = case_inputs(dim, n_side, kernel, kahan, cuda)
+    o = oracle.get("f32")
+    adj = built_adjacency(p, d["x"], d["H"])
+    assert adj.nnz == len(nb["list"])
+    om, div, dr = ops.compsph_prep(p, d["x"], d["H"], d["m"], d["rho"], d["v"], adj)
+    rom, rdiv, rdr = o.compsph_prep(p, h["x"], h["H"], h["m"], h["rho"], h["v"], nb)
+    assert_close(om.cpu().numpy(), rom, 1e-5, 1e-6, "Omega")
+    assert_close(div.cpu().numpy(), rdiv, 1e-4, 1e-5, "Cullen divergence")
+    assert_close(dr.cpu().numpy(), rdr, 1e-4, 1e-5, "consistent d rho/dt")
+    for c_, a_, w_ in ((True, True, True), (False, False, False)):
+        cc, aa, ww = (d["c"] if c_ else None), (d["alpha"] if a_ else None), (om if w_ else None)
+        dv, du, dE, ap, av = ops.compsph_accel_dudt(p, d["x"], d["H"], d["m"], d["rho"], d["v"], cc, aa, d["P"], ww, adj)
+        rdv, rdu, rdE, rap, rav = o.compsph_accel_dudt(p, h["x"], h["H"], h["m"], h["rho"], h["v"], h["c"] if c_ else None,
+                                                       h["alpha"] if a_ else None, h["P"], rom if w_ else None, nb)
+        tag = f"dim {dim} c/alpha/omega {c_}"
+        assert_close(dv.cpu().numpy(), rdv, 2e-4, 2e-5, f"CompSPH dv/dt {tag}")
+        assert_close(du.cpu().numpy(), rdu, 2e-4, 2e-5, f"CompSPH du/dt {tag}")
+        assert_close(dE.cpu().numpy(), rdE, 2e-4, 2e-5, f"CompSPH dE/dt {tag}")
+        assert_close(ap.cpu().numpy(), rap, 2e-4, 2e-5, f"ap_ij {tag}")
+        assert_close(av.cpu().numpy(), rav, 2e-4, 2e-5, f"av_ij {tag}")
+    dv, du, dE, T = ops.monaghan_rhs(p, d["x"], d["H"], d["m"], d["rho"], d["v"], d["u"], d["c"], d["alpha"], d["P"], om, adj,
+                                     terms=True)
+    rdv, rdu, rdE, rT = o.monaghan_rhs(p, h["x"], h["H"], h["m"], h["rho"], h["v"], h["u"], h["c"], h["alpha"], h["P"], rom, nb)
+    assert_close(dv.cpu().numpy(), rdv, 2e-4, 2e-5, "Monaghan dv/dt")
+    assert_close(du.cpu().numpy(), rdu, 2e-4, 2e-5, "Monaghan du/dt")
+    assert_close(dE.cpu().numpy(), rdE, 2e-4, 2e-5, "Monaghan dE/dt")
+    for k in ("pressure", "viscosity", "pdv", "conductivity", "heating"):
+        assert_close(T[k].cpu().numpy(), rT[k], 2e-4, 2e-5, f"Monaghan {k}")
+
+
+def test_gpu_compsph_momentum_is_conserved(cuda):
+    """Pairwise antisymmetry: sum_i m_i dv_i/dt = 0 (the pressure and viscous pair
+    accelerations are equal and opposite)."""
+    p, nb, h, d = case_inputs(2, 48, core.KernelFunctions.Wendland4, True, cuda)
+    adj = built_adjacency(p, d["x"], d["H"])
+    om, _, _ = ops.compsph_prep(p, d["x"], d["H"], d["m"], d["rho"], d["v"], adj, want_div=False, want_drhodt=False)
+    dv, *_ = ops.compsph_accel_dudt(p, d["x"], d["H"], d["m"], d["rho"], d["v"], d["c"], d["alpha"], d["P"], om, adj)
+    mom = (d["m"].double()[:, None] * dv.double()).sum(0).abs().max().item()
+    scale = (d["m"].double()[:, None] * dv.double()).abs().sum().item()
+    assert mom < 1e-5 * scale, (mom, scale)
+
+
+def sedov(nx, dev, scheme_name="compSPH", switch=ws.ViscositySwitch.CullenDehnen2010):
+    cfg, integrator = ws.buildConfig(dim=2, domain=ws.buildDomainDescription(1.0, 2, True, dev), kernel=ws.KernelFunctions.Wendland4,
+                                     targetNeighbors=32, integrationScheme=ws.IntegrationSchemeType.rungeKutta2, device=dev)
+    System, State, Config, Update, step, *_ = ws.buildScheme(scheme_name)
+    sch = Config()
+    sch.gamma = 5 / 3
+    sch.viscositySwitchParams.scheme = switch
+    system = ws.buildSedov(System, State, cfg, nx=nx, dim=2, domainExtent=1.0, E0=1.0, p0=1e-6, gamma=5 / 3,
+                           kernel=ws.KernelFunctions.Wendland4, targetNeighbors=32, device=dev)
+    return cfg, sch, integrator, step, system
+
+
+@pytest.mark.parametrize("switch", [ws.ViscositySwitch.CullenDehnen2010, ws.ViscositySwitch.NoneSwitch])
+def test_compsph_step_matches_oracle(cuda, switch):
+    cfg, sch, integ, step, system = sedov(32, cuda, "compSPH", switch)
+    dt = 2e-4
+    st = state_to_numpy(system.state)
+    orc = CompSPHOracle(ws.make_params(cfg, sch), "f32", switch=SWITCH_CULLEN if switch == ws.ViscositySwitch.CullenDehnen2010
+                        else SWITCH_NONE)
+    for k in range(3):
+        system = integ.function(state=system, f=step, dt=dt, config=cfg, compParams=sch).state
+        st, _, _ = orc.step(st, dt, "rungeKutta2")
+        S = system.state
+        tol = 2e-4 * (k + 1)
+        assert_close(S.positions.cpu().numpy(), st["positions"], 1e-6, 1e-6, f"x step {k}")
+        assert_close(S.velocities.cpu().numpy(), st["velocities"], tol, tol, f"v step {k}")
+        assert_close(S.internalEnergies.cpu().numpy(), st["internalEnergies"], tol, tol, f"u step {k}")
+        assert_close(S.densities.cpu().numpy(), st["densities"], 1e-5, 1e-5, f"rho step {k}")
+        assert_close(S.alphas.cpu().numpy(), st["alphas"], 1e-3, 1e-3, f"alpha step {k}")
+    assert np.abs(st["velocities"]).max() > 0.1
+
+
+def test_monaghan_step_matches_oracle(cuda):
+    cfg, sch, integ, step, system = sedov(32, cuda, "MonaghanCompressibleSPH", ws.ViscositySwitch.NoneSwitch)
+    dt = 2e-4
+    st = state_to_numpy(system.state)
+    orc = MonaghanOracle(ws.make_params(cfg, sch), "f32", density_mode=int(cfg.supportMode.value))
+    for k in range(3):
+        system = integ.function(state=system, f=step, dt=dt, config=cfg, compParams=sch).state
+        st, _, _ = orc.step(st, dt, "rungeKutta2")
+        S = system.state
+        tol = 2e-4 * (k + 1)
+        assert_close(S.velocities.cpu().numpy(), st["velocities"], tol, tol, f"v step {k}")
+        assert_close(S.internalEnergies.cpu().numpy(), st["internalEnergies"], tol, tol, f"u step {k}")
+        assert_close(S.densities.cpu().numpy(), st["densities"], 1e-5, 1e-5, f"rho step {k}")
+    assert np.abs(st["velocities"]).max() > 0.1
+
+
+def test_compsph_energy_conservation(cuda):
+    """Compatible energy: total energy is conserved to FP32 summation error over 5 steps."""
+    cfg, sch, integ, step, system = sedov(128, cuda, "compSPH")
+    sch.compensatedSums = True
+    p = ws.make_params(cfg, sch)
+    S = system.state
+    c0 = ops.conservation_sums(p, S.masses, S.velocities, S.internalEnergies).cpu().numpy()
+    dt = ws.computeTimestep(system, cfg, sch, dt=None)
+    for _ in range(5):
+        system = integ.function(state=system, f=step, dt=dt, config=cfg, compParams=sch).state
+    S = system.state
+    c1 = ops.conservation_sums(p, S.masses, S.velocities, S.internalEnergies).cpu().numpy()
+    assert abs(c1[3] - c0[3]) / c0[3] < 2e-6, ("total energy drift", c0[3], c1[3])
+    assert np.max(np.abs(c1[4:6])) < 1e-6 * np.sqrt(2 * c1[1] * c1[0]) + 1e-12

@@ -46,6 +46,30 @@ def test_neighbors_bit_exact(cuda, dim, n_side, periodic):
     assert np.array_equal(j, ref["list"]) and np.array_equal(np.bincount(i, minlength=len(ref["counts"])), ref["counts"])
 
 
+@pytest.mark.parametrize("dim,n_side", [(1, 12), (1, 20), (2, 9), (2, 12), (3, 8)])
+def test_neighbors_bit_exact_small_periodic_grids(cuda, dim, n_side):
+    """One or two cells along a periodic axis: a cell is reached through two periodic
+    images, and every pair must still be tested at its minimum image."""
+    cfg, sch, p = make_params(dim)
+    P = make_particles(dim, n_side, seed=30 + dim, jitter=0.4, h_spread=0.15)
+    G = to_gpu(P, cuda)
+    adj = ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale)
+    ref = oracle.get("f32").neighbors(p, P["positions"], P["supports"], cell_capacity_for(len(P["supports"]), dim))
+    assert ref["grid"][:dim].min() < 3, ref["grid"]
+    assert np.array_equal(adj.grid.cpu().numpy(), ref["grid"])
+    assert adj.nnz == ref["nnz"]
+    assert np.array_equal(adj.neighborOffsets.cpu().numpy(), ref["offsets"])
+    assert np.array_equal(adj.numNeighbors.cpu().numpy(), ref["counts"])
+    assert np.array_equal(adj.neighborList[: adj.nnz].cpu().numpy(), ref["list"])
+    # brute force: every pair within verlet_scale * max(H_i, H_j) at its minimum image
+    x, H = P["positions"], P["supports"]
+    d = x[:, None, :] - x[None, :, :]
+    d = np.where(d > 0.5, d - 1.0, np.where(d < -0.5, d + 1.0, d)).astype(np.float32)
+    r2 = (d.astype(np.float64) ** 2).sum(-1)
+    R = float(p.verlet_scale) * np.maximum(H[:, None], H[None, :]).astype(np.float64)
+    assert abs(int((r2 < R * R).sum()) - adj.nnz) <= 4   # FP32 rounding at r = R
+
+
 @pytest.mark.parametrize("dim,n_side", CASES)
 def test_interacting_list_is_exact_subset(cuda, dim, n_side):
     """The interacting list holds exactly the Verlet entries with fl(sqrt(r^2))/max(H_i,H_j) < 1

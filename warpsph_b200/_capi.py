@@ -43,7 +43,8 @@ class SphParams(C.Structure):
         ("alpha_min", C.c_double), ("alpha_max", C.c_double), ("beta_xi", C.c_double),
         ("target_neighbors", C.c_double),
         ("cfl", C.c_double), ("min_dt", C.c_double), ("max_dt", C.c_double), ("dt_growth", C.c_double),
-        ("reserved_d", C.c_double * 8),
+        ("c_s", C.c_double),
+        ("reserved_d", C.c_double * 7),
         ("dim", C.c_int32),
         ("kernel", C.c_int32),
         ("periodic", C.c_int32 * 3),
@@ -55,7 +56,8 @@ class SphParams(C.Structure):
         ("limit_xi", C.c_int32),
         ("kahan", C.c_int32),
         ("list_stride", C.c_int32),
-        ("reserved_i", C.c_int32 * 7),
+        ("conductivity_term", C.c_int32),
+        ("reserved_i", C.c_int32 * 6),
     ]
 
 
@@ -111,6 +113,12 @@ _PROTOS = {
     "sph_crk_accel_dudt": [_P, _I64] + [_P] * 21,
     "sph_crk_accel": [_P, _I64] + [_P] * 20,
     "sph_crk_dudt": [_P, _I64] + [_P] * 18,
+    "sph_compsph_prep": [_P, _I64] + [_P] * 12,
+    "sph_grad_h_omega": [_P, _I64] + [_P] * 9,
+    "sph_compsph_accel_dudt": [_P, _I64] + [_P] * 18,
+    "sph_compsph_accel": [_P, _I64] + [_P] * 16,
+    "sph_compsph_dudt": [_P, _I64] + [_P] * 14,
+    "sph_monaghan_rhs": [_P, _I64] + [_P] * 22,
     "sph_compsph_balance": [_P, _I64] + [_P] * 15,
     "sph_compsph_balance_noalloc": [_P, _I64] + [_P] * 14,
     "sph_cfl_dt": [_P, _I64, _P, _P, _P, _P, _P, _P],

@@ -447,6 +447,8 @@ def make_params(config: SimulationConfig, scheme: Optional[CompressibleSPHConfig
         dp = scheme.diffusionParams
         p.C_l, p.C_q, p.Cu_l, p.Cu_q, p.K = float(dp.C_l), float(dp.C_q), float(dp.Cu_l), float(dp.Cu_q), float(dp.K)
         p.viscosity_term = _term_value(dp.viscosityTerm)
+        p.conductivity_term = _term_value(dp.thermalConducitiyTerm)
+        p.c_s = float(dp.c_s)
         p.monaghan_switch = int(bool(dp.monaghanSwitch))
         p.correct_xi = int(bool(dp.correctXi))
         p.scale_beta = int(bool(dp.scaleBeta))

@@ -29,6 +29,8 @@ struct DevParams {
     float alpha_min, alpha_max, beta_xi;
     float target_neighbors;
     float cfl, min_dt, max_dt, dt_growth;
+    float c_s;      // sound speed of the viscosity terms without per-particle sound speeds
+    int conductivity_term;
     float kscale;   // H / h  (kernel scale)
     float kxi;      // the kernel "xi" used by CFL, viscosity and switches
 };

@@ -91,6 +91,12 @@ int params_to_dev(const SphParams* p, DevParams* o) {
     o->alpha_min = (float)p->alpha_min; o->alpha_max = (float)p->alpha_max; o->beta_xi = (float)p->beta_xi;
     o->target_neighbors = (float)p->target_neighbors;
     o->cfl = (float)p->cfl; o->min_dt = (float)p->min_dt; o->max_dt = (float)p->max_dt; o->dt_growth = (float)p->dt_growth;
+    o->c_s = (float)p->c_s;
+    o->conductivity_term = p->conductivity_term;
+    if (p->viscosity_term < SPH_VISC_DEFAULT || p->viscosity_term > SPH_VISC_DELTASPH)
+        return set_error(SPH_ERR_BAD_ARG, "viscosity_term %d out of range", p->viscosity_term);
+    if (p->conductivity_term < SPH_VISC_DEFAULT || p->conductivity_term > SPH_VISC_DELTASPH)
+        return set_error(SPH_ERR_BAD_ARG, "conductivity_term %d out of range", p->conductivity_term);
     o->kscale = (float)kernel_scale(p->kernel, p->dim);
     o->kxi = o->kscale;
     return SPH_OK;
@@ -406,8 +412,19 @@ template <int D> __device__ __forceinline__ Vec<D> rec_pos(const float4& r) {
 // axis), periodic axes wrapped, cells outside a non-periodic grid skipped, and a cell
 // reached twice (fewer than three cells along a periodic axis) kept only once.
 // shift[q*3+a] is the periodic image offset of stencil cell q along axis a (-L, 0, +L):
-// x_i - x_j - shift is the minimum-image difference for every pair within one cell
-// width, bit-identical to the per-pair test of dist_vec (x - 0 = x exactly).
+// with at least three cells per axis, x_i - x_j - shift is the minimum-image
+// difference for every pair within one cell width, bit-identical to the per-pair test
+// of dist_vec (x - 0 = x exactly).  With fewer than three cells along an axis one cell
+// is reached through two images and a single shift cannot serve every pair in it; the
+// walk then takes the minimum image pair by pair (see grid_needs_min_image).
+template <int D>
+__device__ __forceinline__ bool grid_needs_min_image(const GridDev& g, const DomainF& dom) {
+    bool r = false;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) r |= dom.periodic[a] && g.G[a] < 3;
+    return r;
+}
+
 template <int D>
 __device__ __forceinline__ int stencil_keys(const int* c, const GridDev& g, const DomainF& dom, uint32_t* out, float* shift) {
     int cnt = 0;
@@ -516,6 +533,7 @@ k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_ke
         uint32_t keys[D == 1 ? 3 : (D == 2 ? 9 : 27)];
         float shifts[3 * (D == 1 ? 3 : (D == 2 ? 9 : 27))];
         const int nk = stencil_keys<D>(c, g, dom, keys, shifts);
+        const bool min_image = grid_needs_min_image<D>(g, dom);     // uniform over the grid
         const int i = active ? sort_index[t] : 0;
         int cnt = 0;
         int row = 0, nb = 0, nib = 0, written = 0, iwritten = 0;
@@ -543,8 +561,19 @@ k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_ke
                         const float R = __fmul_rn(vs, Hm);
                         Vec<D> dv;
                         #pragma unroll
-                        for (int a = 0; a < D; ++a)
-                            dv.v[a] = __fsub_rn(__fsub_rn(xi.v[a], a == 0 ? rj.x : (a == 1 ? rj.y : rj.z)), sh[a]);
+                        for (int a = 0; a < D; ++a) {
+                            const float xj = a == 0 ? rj.x : (a == 1 ? rj.y : rj.z);
+                            if (min_image) {
+                                float d = __fsub_rn(xi.v[a], xj);
+                                if (dom.periodic[a]) {
+                                    if (d > dom.halfL[a]) d = __fsub_rn(d, dom.L[a]);
+                                    else if (d < -dom.halfL[a]) d = __fadd_rn(d, dom.L[a]);
+                                }
+                                dv.v[a] = d;
+                            } else {
+                                dv.v[a] = __fsub_rn(__fsub_rn(xi.v[a], xj), sh[a]);
+                            }
+                        }
                         const float r2 = dist2_rn<D>(dv);
                         const bool hit = active & (u < mcount) & (r2 < __fmul_rn(R, R));
                         if (FILL) {

@@ -369,6 +369,55 @@ def crk_accel_dudt(params, x, H, m, rho, V, crk: CRKState, v, c, P, DvDx, adj: A
     return dvdt, dudt, ap, av
 
 
+def compsph_prep(params, x, H, m, rho, v, adj: AdjacencyList, grad_h: bool = True, want_div: bool = True,
+                 want_drhodt: bool = True):
+    """Grad-h Omega, the super-symmetric velocity divergence and the consistent
+    continuity d rho/dt from one pass (each None when not requested)."""
+    n = H.shape[0]
+    om = _empty(n, H) if grad_h else None
+    div = _empty(n, H) if want_div else None
+    dr = _empty(n, H) if want_drhodt else None
+    with _timed("compsph_prep"):
+        check(_capi.lib().sph_compsph_prep(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(v), *_lists(params, adj, True),
+                                           ptr(om), ptr(div), ptr(dr), stream_ptr(H.device)), "sph_compsph_prep")
+    return om, div, dr
+
+
+def compsph_accel_dudt(params, x, H, m, rho, v, c, alpha, P, omega, adj: AdjacencyList, pair_arrays: bool = True,
+                       want_dEdt: bool = True):
+    """Fused CompSPH momentum and energy RHS; returns (dvdt, dudt, dEdt, ap_ij, av_ij) with
+    the pairwise accelerations in Verlet-entry order (zeros beyond the support)."""
+    n, d = H.shape[0], int(params.dim)
+    dvdt, dudt = _empty((n, d), H), _empty(n, H)
+    dEdt = _empty(n, H) if want_dEdt else None
+    alloc = torch.zeros if adj.interList is not None else torch.empty
+    ap = alloc((adj.nnz, d), device=H.device, dtype=torch.float32) if pair_arrays else None
+    av = alloc((adj.nnz, d), device=H.device, dtype=torch.float32) if pair_arrays else None
+    with _timed("compsph_accel_dudt"):
+        check(_capi.lib().sph_compsph_accel_dudt(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(v), fptr(c), fptr(alpha),
+                                                 fptr(P), fptr(omega), *_lists(params, adj, True), ptr(dvdt), ptr(dudt), ptr(dEdt),
+                                                 ptr(ap), ptr(av), stream_ptr(H.device)), "sph_compsph_accel_dudt")
+    return dvdt, dudt, dEdt, ap, av
+
+
+def monaghan_rhs(params, x, H, m, rho, v, u, c, alpha, P, omega, adj: AdjacencyList, terms: bool = False):
+    """Monaghan-scheme RHS: (dvdt, dudt, dEdt, parts) with parts = dict(pressure, viscosity,
+    pdv, conductivity, heating) when `terms`, else None."""
+    n, d = H.shape[0], int(params.dim)
+    dvdt, dudt, dEdt = _empty((n, d), H), _empty(n, H), _empty(n, H)
+    parts = None
+    if terms:
+        parts = dict(pressure=_empty((n, d), H), viscosity=_empty((n, d), H), pdv=_empty(n, H), conductivity=_empty(n, H),
+                     heating=_empty(n, H))
+    q = parts or {}
+    with _timed("monaghan_rhs"):
+        check(_capi.lib().sph_monaghan_rhs(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(v), fptr(u), fptr(c), fptr(alpha),
+                                           fptr(P), fptr(omega), *_lists(params, adj, True), ptr(dvdt), ptr(dudt), ptr(dEdt),
+                                           ptr(q.get("pressure")), ptr(q.get("viscosity")), ptr(q.get("pdv")),
+                                           ptr(q.get("conductivity")), ptr(q.get("heating")), stream_ptr(H.device)), "sph_monaghan_rhs")
+    return dvdt, dudt, dEdt, parts
+
+
 def compsph_balance(params, m, rho, P, u, v, dvdt, dt, adj: AdjacencyList, ap, av):
     """Energy partition f_ij for every Verlet entry."""
     n, d = m.shape[0], int(params.dim)

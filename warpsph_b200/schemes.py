@@ -20,11 +20,12 @@ from typing import Optional, Union
 import torch
 
 from . import ops
-from .configurations import (CompSPHConfig, CompressibleSPHConfig, CRKSPHConfig, SimulationConfig, compSPHConfigToDict,
-                             crkSPHConfigToDict, dictToCompSPHConfig, dictToCRKSPHConfig, make_params)
+from .configurations import (CompSPHConfig, CompressibleSPHConfig, CRKSPHConfig, SimulationConfig, compressibleConfigToDict,
+                             compSPHConfigToDict, crkSPHConfigToDict, dictToCompressibleConfig, dictToCompSPHConfig,
+                             dictToCRKSPHConfig, make_params)
 from .core import AdjacencyList, SupportScheme, sphKernel_xi, volumeToSupportHelper
 from .enumTypes import AdaptiveSupportScheme, CompressibleSPHScheme, ViscositySwitch
-from .systems import CompressibleSystemUpdate, CompSPHState, CompSPHSystem
+from .systems import CompressibleState, CompressibleSystem, CompressibleSystemUpdate, CompSPHState, CompSPHSystem
 
 
 # ------------------------------------------------------------------ adaptive support
@@ -153,4 +154,8 @@ def buildScheme(schemeName: Union[str, CompressibleSPHScheme]):
         from .compsph import compSPH_step
         return (CompSPHSystem, CompSPHState, CompSPHConfig, CompressibleSystemUpdate, compSPH_step, compSPHConfigToDict,
                 dictToCompSPHConfig)
+    if (isinstance(schemeName, str) and schemeName == "MonaghanCompressibleSPH") or schemeName == CompressibleSPHScheme.Monaghan:
+        from .compsph import compressibleSPH_Monaghan
+        return (CompressibleSystem, CompressibleState, CompressibleSPHConfig, CompressibleSystemUpdate, compressibleSPH_Monaghan,
+                compressibleConfigToDict, dictToCompressibleConfig)
     raise ValueError(f"Scheme {schemeName} not recognized.")
