@@ -51,6 +51,8 @@ def parse_args(argv=None):
     ap.add_argument("--breakdown", action="store_true", help="print a per-kernel time breakdown to stderr")
     ap.add_argument("--no-dfsph", action="store_true", help="skip the DFSPH warm-start comparison")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched delta-SPH ensemble")
+    ap.add_argument("--no-compsph", action="store_true", help="skip the CompSPH Sedov 2D throughput")
+    ap.add_argument("--no-sedov3d", action="store_true", help="skip the CRKSPH Sedov 3D (128^3) throughput")
     return ap.parse_args(argv)
 
 
@@ -285,6 +287,68 @@ def ensemble_throughput(dev, chunks: int = 6) -> dict:
             "status": E.status(), "wall_s": time.perf_counter() - t0}
 
 
+def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, steps: int, warmup: int, kahan: bool = False,
+                      timed_kernel: str = None, bytes_per_particle: float = None) -> dict:
+    """particle-steps/s of one compressible scheme on the Sedov blast (device-resident,
+    CUDA events, CFL dt on the device every step), the total-energy drift over the timed
+    steps from the FP64 conservation sums, and the dominant pair kernel's average launch
+    against the measured HBM peak."""
+    import torch
+    import warpsph_b200 as ws
+    from warpsph_b200 import ops
+    t0 = time.perf_counter()
+    cfg, integ = ws.buildConfig(dim=dim, domain=ws.buildDomainDescription(1.0, dim, True, dev), kernel=ws.KernelFunctions.Wendland4,
+                                targetNeighbors=neighbours, integrationScheme=ws.IntegrationSchemeType.rungeKutta2, cflFactor=0.3,
+                                device=dev)
+    System, State, Config, Update, step, *_ = ws.buildScheme(scheme)
+    sch = Config()
+    sch.gamma = 5 / 3
+    sch.viscositySwitchParams.scheme = ws.ViscositySwitch.CullenDehnen2010
+    sch.compensatedSums = kahan
+    system = ws.buildSedov(System, State, cfg, nx=nx, dim=dim, domainExtent=1.0, E0=1.0, p0=1e-6, gamma=5 / 3,
+                           kernel=ws.KernelFunctions.Wendland4, targetNeighbors=neighbours, device=dev)
+    params = ws.make_params(cfg, sch)
+    n = system.state.masses.shape[0]
+    box = {"system": system, "dt": torch.tensor([cfg.dt], device=dev, dtype=torch.float32)}
+
+    def one_step():
+        S = box["system"].state
+        box["dt"] = ops.cfl_dt(params, S.supports, S.internalEnergies, dt_prev=box["dt"])
+        box["system"] = integ.function(state=box["system"], f=step, dt=box["dt"], config=cfg, compParams=sch).state
+
+    for _ in range(warmup):
+        one_step()
+    torch.cuda.synchronize()
+    S = box["system"].state
+    c0 = ops.conservation_sums(params, S.masses, S.velocities, S.internalEnergies).cpu().numpy()
+    timer = ops.KernelTimer(names={timed_kernel}) if timed_kernel else None
+    ops.TIMER = timer
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        one_step()
+    e1.record()
+    torch.cuda.synchronize()
+    ops.TIMER = None
+    ms = e0.elapsed_time(e1)
+    S = box["system"].state
+    c1 = ops.conservation_sums(params, S.masses, S.velocities, S.internalEnergies).cpu().numpy()
+    out = {"particles": int(n), "neighbours": neighbours, "steps": steps, "ms_per_step": ms / steps,
+           "value": n * steps / (ms / 1e3), "unit": UNIT, "compensated_sums": kahan,
+           "energy_drift_timed_steps": float(abs(c1[3] - c0[3]) / c0[3]),
+           "verlet_entries_per_particle": box["system"].adjacency.nnz / n}
+    if timer is not None:
+        k = timer.summary().get(timed_kernel)
+        if k:
+            peaks = load_peaks()
+            ach = bytes_per_particle * n / (k["avg_ms"] / 1e3) / 1e9
+            out["kernel"] = {"name": timed_kernel, "avg_launch_ms": k["avg_ms"], "launches": k["launches"],
+                             "algorithmic_bytes_per_particle": bytes_per_particle, "achieved_gbs": ach,
+                             "frac_of_measured_hbm": ach / peaks["hbm_gbs"]}
+    out["wall_s"] = time.perf_counter() - t0
+    return out
+
+
 # ---------------------------------------------------------------------------- GPU arm
 def build_workload(nx, dev):
     import warpsph_b200 as ws
@@ -426,6 +490,18 @@ def gpu_arm(args, rank: int, world: int):
     if rank == 0 and world == 1 and not args.no_ensemble:
         ens = ensemble_throughput(dev)
 
+    comp = None
+    if rank == 0 and world == 1 and not args.no_compsph:
+        d, K = 2, 32.0
+        comp = scheme_throughput(dev, "compSPH", 2, args.nx, 32, steps=args.steps, warmup=args.warmup,
+                                 timed_kernel="compsph_accel_dudt", bytes_per_particle=(8 * d + 28) + (4 * d + 8) + K * (4 + 8 * d))
+        comp["workload"] = f"Sedov 2D CompSPH {args.nx}x{args.nx}, Wendland C4, 32 neighbours, Cullen-Dehnen, RK2, compatible energy"
+    s3 = None
+    if rank == 0 and world == 1 and not args.no_sedov3d:
+        s3 = scheme_throughput(dev, "crkSPH", 3, 128, 128, steps=3, warmup=2, kahan=True, timed_kernel="crk_accel_dudt",
+                               bytes_per_particle=bytes_accel_dudt(3, 128.0))
+        s3["workload"] = "Sedov 3D CRKSPH 128^3 (2,097,152 particles), Wendland C4, 128 neighbours, Cullen-Dehnen, RK2, Kahan sums"
+
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(args.nx, args.cpu_steps)
@@ -437,7 +513,7 @@ def gpu_arm(args, rank: int, world: int):
                 "config": {"workload": WORKLOAD, "particles": n, "nx": args.nx, "parallelism": f"replicas x{world}",
                            "l2": "working set larger than L2 (pair arrays ~0.7 GB per step), no flush needed"},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
-                "dfsph_warm_start": dfsph, "ensemble": ens}
+                "dfsph_warm_start": dfsph, "ensemble": ens, "compsph": comp, "sedov3d": s3}
         if breakdown is not None:
             line["breakdown_ms"] = {k: round(v["total_ms"] / 3, 4) for k, v in breakdown.items()}
         print(json.dumps(line), flush=True)

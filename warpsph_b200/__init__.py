@@ -17,6 +17,6 @@ from .configurations import (CompressibleSPHConfig, CompSPHConfig, CRKSPHConfig,
 from .systems import CompressibleState, CompressibleSystem, CompressibleSystemUpdate, CompSPHState, CompSPHSystem
 from .integrators import IntegrationResult, getIntegrator
 from .schemes import buildScheme, computeCRKFactors, computeTimestep, crkSPH_step, evaluateOptimalSupport, idealGasEOS
-from .cases import buildPointCloud, buildSedov
+from .cases import buildPointCloud, buildSedov, buildSod1D, sodInitialState
 
 __version__ = "0.1.0"

@@ -1,5 +1,11 @@
 """Case builders for the synthetic benchmark workloads.
 
+``buildSod1D`` follows src/warpSPH/caseUtils/compressible/sod/sod.py:21-236: the
+mirrored periodic layout on [-1, 1] (dense left state for |x| < 1/2, the right state
+with samplingRatio-times coarser spacing and equal masses outside), supports from 16
+gather Newton iterations, the ideal-gas state from the prescribed density, and the
+logistic ramp of the internal energy across both interfaces when ``smoothIC``.
+
 ``buildPointCloud`` follows src/warpSPH/sample/regular.py:6-50 (cell-centred lattice
 for periodic axes, 'xy' meshgrid order).  ``buildSedov`` follows
 src/warpSPH/caseUtils/compressible/sedov/initial.py:24-218, including the 'hat'
@@ -11,6 +17,7 @@ sum to one, on top of the background pressure p0.
 from __future__ import annotations
 
 import math
+from typing import NamedTuple
 
 import torch
 
@@ -105,4 +112,75 @@ def buildSedov(SimulationSystem, SimulationState, config: SimulationConfig, nx: 
     config.dx = float(area)
     if computeDt:
         config.dt = computeTimestep(system, config, setup, dt=config.dt)
+    return system
+
+
+class sodInitialState(NamedTuple):
+    p: float
+    rho: float
+    v: float
+
+
+def buildSod1D(SimulationSystem, SimulationState, samplingRatio: int, leftState: sodInitialState, rightState: sodInitialState,
+               gamma: float, config: SimulationConfig, smoothIC: bool = False,
+               adaptiveSupportScheme: AdaptiveSupportScheme = AdaptiveSupportScheme.Monaghan, smoothingSpacings: float = 0.5):
+    """caseUtils/compressible/sod/sod.py:21-236.  config.nx dense particles on |x| < 1/2 and
+    config.nx // samplingRatio coarse ones on 1/2 < |x| < 1 in the periodic domain
+    config.domain = [-1, 1]; each half is a tube with reflecting walls at its ends.
+    ``smoothingSpacings`` is the logistic ramp's scale in dense spacings (the reference's
+    0.5, sod.py:173-174)."""
+    nx = int(config.nx)
+    dev, dtype = config.device, config.dtype
+    actualRatio = nx / (nx // samplingRatio)
+    unit = buildDomainDescription(1, config.dim, periodic=True, device=dev, dtype=dtype)
+    pos_l, H_l, area_l, _ = buildPointCloud(nx, unit, config.targetNeighbors, device=dev, dtype=dtype)
+    pos_r, H_r, area_r, _ = buildPointCloud(nx // samplingRatio, unit, config.targetNeighbors, device=dev, dtype=dtype)
+    pos_r = pos_r.clone()
+    neg = pos_r[:, 0] < 0
+    pos_r[neg, 0] -= 0.5
+    pos_r[~neg & (pos_r[:, 0] > 0), 0] += 0.5
+    pos = torch.cat([pos_l, pos_r], 0).contiguous()
+    nl, nr = pos_l.shape[0], pos_r.shape[0]
+    tags = torch.cat([torch.zeros(nl, dtype=torch.int32, device=dev), torch.ones(nr, dtype=torch.int32, device=dev)])
+    left = tags == 0
+    leftMass = float(area_l) * leftState.rho
+    rightMass = float(area_l) * rightState.rho * actualRatio
+    masses = torch.where(left, leftMass, rightMass).to(dtype)
+    supports = torch.where(left, float(H_l.min()), float(H_r.min())).to(dtype)
+    densities = torch.where(left, leftState.rho, rightState.rho).to(dtype)
+    velocities = torch.where(left[:, None], float(leftState.v), float(rightState.v)).to(dtype).contiguous()
+    UIDs = torch.cat([torch.arange(nl, dtype=torch.int32, device=dev), torch.arange(nr, dtype=torch.int32, device=dev)])
+    state = SimulationState(positions=pos, velocities=velocities, supports=supports, masses=masses, densities=densities,
+                            kinds=torch.zeros_like(tags), materials=tags, UIDs=UIDs, UIDcounter=int(UIDs.max()) + 1,
+                            divergence=torch.zeros_like(densities), alpha0s=torch.ones_like(densities),
+                            alphas=torch.ones_like(densities))
+    prescribed = densities.clone()
+    compParams = CompressibleSPHConfig(gamma=gamma, adaptiveSupportCorrections=True, adaptiveSupportIterations=16,
+                                       adaptiveSupportThreshold=1e-3, adaptiveSupportScheme=adaptiveSupportScheme)
+    rho_opt, h_opt, adjacency, *_ = evaluateOptimalSupport(state, config, compParams, SupportScheme.Gather)
+    state.supports = h_opt
+    eosRho = rho_opt if smoothIC else prescribed
+    P_initial = torch.where(left, leftState.p, rightState.p).to(dtype)
+    u = 1 / (gamma - 1) * (P_initial / eosRho)
+    if smoothIC:
+        dx = float(pos_l[1, 0] - pos_l[0, 0]) * smoothingSpacings
+
+        def ramped(a, b, x):
+            return (a - b) / (torch.exp(x / dx) + 1) + b
+
+        left_u = 1 / (gamma - 1) * (leftState.p / leftState.rho)
+        right_u = 1 / (gamma - 1) * (rightState.p / rightState.rho)
+        x = state.positions[:, 0]
+        u = torch.where(x > 0.0, ramped(left_u, right_u, x - 0.5), u)
+        u = torch.where(x < 0.0, ramped(right_u, left_u, x + 0.5), u).to(dtype)
+    state.densities = eosRho.contiguous()
+    state.internalEnergies = u.contiguous()
+    state.entropies, state.pressures, state.soundspeeds = ops.eos_ideal_gas(make_params(config, compParams), state.internalEnergies,
+                                                                            state.densities)
+    state.totalEnergies = (state.internalEnergies + 0.5 * (state.velocities ** 2).sum(-1)) * state.masses
+    adjacency = ops.buildVerletList(state.positions, state.supports, make_params(config), 2 ** (1 / config.dim))
+    system = SimulationSystem(state=state, adjacency=adjacency, domain=config.domain)
+    compParams.gamma = gamma
+    config.dx = float(masses.min())
+    config.dt = computeTimestep(system, config, compParams, dt=None)
     return system
