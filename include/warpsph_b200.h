@@ -119,10 +119,10 @@ typedef struct SphParams {
     int32_t energy_scheme;            /* SPH_ENERGY_* */
     int32_t limit_xi;
     int32_t kahan;                    /* 1: compensated accumulation of dv/dt and du/dt */
-    /* Layout of the `list` argument of the pair entry points: 1 (or 0) = Verlet list of
-     * neighbour indices j; 2 = interacting list of (j, Verlet entry index) int32 pairs
-     * from sph_neighbors_build.  Pairwise outputs/inputs (ap_ij, av_ij, f_ij) are always
-     * indexed by the Verlet entry. */
+    /* Layout of the `list` argument of the pair entry points: 1 (or 0), rows of int32
+     * neighbour indices j.  A pass walks whole Verlet rows (cnt = Verlet counts) or their
+     * interacting prefixes (cnt = interacting counts from sph_neighbors_build); pairwise
+     * outputs/inputs (ap_ij, av_ij, f_ij) are indexed by the Verlet entry either way. */
     int32_t list_stride;
     /* DiffusionParameters.thermalConducitiyTerm (SPH_VISC_*): the signal-velocity form of
      * the artificial conductivity (diffusionParameters.py:33, pi.py:63) */
@@ -152,15 +152,14 @@ int sph_neighbors_workspace_size(const SphParams* p, int64_t n, int64_t cell_cap
  * Outputs: sort_index[n] (original index of the k-th sorted particle),
  * sorted_keys[n] (its Morton cell key), cell_begin/cell_end[cell_capacity],
  * CSR arrays, *nnz_out (device int64).
- * Optional interacting list (all inter_* non-null): the subset of entries with
- * r/max(H_i,H_j) < 1 -- every pair any support scheme gives a non-zero kernel
- * value -- as (j, index of the entry in neighbor_list) int32 pairs, stored inside
- * each row's own Verlet range: inter_offsets[i] == neighbor_offsets[i], the first
- * inter_counts[i] pairs of the range are valid.  inter_list holds 2*inter_capacity
- * int32 (8-byte aligned, inter_capacity >= list_capacity); *inter_nnz_out receives
- * the number of valid pairs.  If the Verlet list exceeds list_capacity nothing is
- * filled, SPH_STATUS_LIST_OVERFLOW is or-ed into *status (device int32) and *nnz_out
- * holds the required size.
+ * Interacting prefix (inter_counts non-null): each row holds first the entries with
+ * fl(sqrt(r^2))/max(H_i,H_j) < 1 -- every pair any support scheme gives a non-zero
+ * kernel value -- then the rest of its Verlet entries, both parts in walk order
+ * (stencil cells in offset order, candidates by sorted position); inter_counts[i] is the
+ * length of the prefix and *inter_nnz_out their sum.  Without inter_counts the rows are
+ * in walk order.  If the Verlet list exceeds list_capacity nothing is filled,
+ * SPH_STATUS_LIST_OVERFLOW is or-ed into *status (device int32) and *nnz_out holds the
+ * required size.
  * grid_out (device, 8 int32): grid dims, bits per axis, cell size as float bits, dim. */
 int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const float* H,
                         void* workspace, int64_t workspace_bytes, int64_t cell_capacity,
@@ -168,24 +167,25 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
                         int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
                         int32_t* neighbor_offsets, int32_t* num_neighbors,
                         int32_t* neighbor_list, int64_t list_capacity, int64_t* nnz_out,
-                        int32_t* inter_offsets, int32_t* inter_counts, int32_t* inter_list,
-                        int64_t inter_capacity, int64_t* inter_nnz_out,
+                        int32_t* inter_counts, int64_t* inter_nnz_out,
                         int32_t* status, void* stream);
 
 /* Prior-list reuse (the validity check warpSPHCore buildVerletList performs before
  * rebuilding; its rule is restated here): a list built at (x0, H0) with verlet_scale vs
  * still holds every pair with |x_i - x_j| < max(H_i, H_j) at (x, H) when
  * max_k (H_k - vs H0_k) + 2 max_k |x_k - x0_k| <= 0 (a 1e-5 relative margin is kept
- * for rounding).  When that holds, the interacting sublist for (x, H) is written to
- * inter_* (same layout as sph_neighbors_build) and *inter_nnz_out receives its size;
- * otherwise SPH_STATUS_LIST_STALE is or-ed into *status and the caller rebuilds.
- * With inter_list == NULL only the verdict is computed (the sublist can be filtered by
- * a later call, when a pass needs it).  scratch: device memory of 4 uint32 words. */
+ * for rounding).  When that holds, every row of neighbor_list is rewritten into
+ * list_out (same offsets and counts; list_out must not alias neighbor_list, which
+ * earlier stages may still reference) with its interacting entries for (x, H) first,
+ * in the kept order, and the rest after them in reverse kept order; inter_counts and
+ * *inter_nnz_out receive the prefix lengths and their sum.  Otherwise
+ * SPH_STATUS_LIST_STALE is or-ed into *status and the caller rebuilds.  With
+ * list_out == NULL only the verdict is computed (the rows can be rewritten by a later
+ * call, when a pass needs them).  scratch: device memory of 4 uint32 words. */
 int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const float* H,
                           const float* x0, const float* H0,
                           const int32_t* neighbor_offsets, const int32_t* num_neighbors,
-                          const int32_t* neighbor_list,
-                          int32_t* inter_offsets, int32_t* inter_counts, int32_t* inter_list,
+                          const int32_t* neighbor_list, int32_t* list_out, int32_t* inter_counts,
                           uint32_t* scratch, int64_t* inter_nnz_out, int32_t* status, void* stream);
 
 /* Expands CSR rows into the reference's AdjacencyList.i / .j int64 arrays
@@ -273,17 +273,19 @@ int sph_switch_balsara(const SphParams* p, int64_t n, const float* DvDx, const f
 
 /* CRKSPH momentum and energy RHS in one pair pass:
  * modules/crk/accel.py:15-250 (dv/dt and the pairwise ap_ij, av_ij [nnz, dim]) and
- * modules/crk/dudt.py:15-229 (du/dt).  Any of dvdt_out, dudt_out, ap_ij, av_ij may
- * be null.  With p->kahan the per-particle sums are Neumaier-compensated.  With the
- * interacting list (list_stride 2) only interacting entries of ap_ij / av_ij are
- * written; the caller passes zero-filled arrays. */
+ * modules/crk/dudt.py:15-229 (du/dt), with dEdt [n] = m v.dv/dt + m du/dt
+ * (schemes/crkSPH.py:330).  Any of dvdt_out, dudt_out, dEdt_out, ap_ij, av_ij may be
+ * null.  With p->kahan the per-particle sums are Neumaier-compensated.  Walking the
+ * interacting prefixes (cnt = interacting counts), pass verlet_cnt = the Verlet counts
+ * and the rest of each row of ap_ij / av_ij is written as zeros; with verlet_cnt NULL
+ * only the walked entries are written. */
 int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
                        const float* m, const float* rho, const float* V,
                        const float* A, const float* B, const float* gradA, const float* gradB,
                        const float* v, const float* c, const float* P, const float* DvDx,
                        const int32_t* offs, const int32_t* cnt, const int32_t* list,
-                       float* dvdt_out, float* dudt_out, float* ap_ij, float* av_ij,
-                       void* stream);
+                       const int32_t* verlet_cnt, float* dvdt_out, float* dudt_out,
+                       float* dEdt_out, float* ap_ij, float* av_ij, void* stream);
 /* Same pass, separate names for callers that bind the reference's two wrappers
  * computeCrkSPHAccelWarp (modules/crk/accel.py:391) and computeCrkSPHdudtWarp
  * (modules/crk/dudt.py:364). */
@@ -292,7 +294,8 @@ int sph_crk_accel(const SphParams* p, int64_t n, const float* x, const float* H,
                   const float* A, const float* B, const float* gradA, const float* gradB,
                   const float* v, const float* c, const float* P, const float* DvDx,
                   const int32_t* offs, const int32_t* cnt, const int32_t* list,
-                  float* dvdt_out, float* ap_ij, float* av_ij, void* stream);
+                  const int32_t* verlet_cnt, float* dvdt_out, float* ap_ij, float* av_ij,
+                  void* stream);
 int sph_crk_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
                  const float* m, const float* rho, const float* V,
                  const float* A, const float* B, const float* gradA, const float* gradB,
@@ -330,20 +333,20 @@ int sph_grad_h_omega(const SphParams* p, int64_t n, const float* x, const float*
  * reference does without sound speeds, switch or grad-h state).  Outputs:
  * dvdt [n*dim], dudt [n], dEdt [n] = m v.dvdt + m dudt (schemes/compSPH.py:170), pairwise
  * pressure / viscous accelerations ap_ij, av_ij [nnz*dim] by Verlet entry; any may be null.
- * With the interacting list (list_stride 2) only interacting entries of ap_ij / av_ij are
- * written; the caller passes zero-filled arrays. */
+ * verlet_cnt as for sph_crk_accel_dudt (zeros for the rest of each walked row). */
 int sph_compsph_accel_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
                            const float* m, const float* rho, const float* v, const float* c,
                            const float* alpha, const float* P, const float* omega,
                            const int32_t* offs, const int32_t* cnt, const int32_t* list,
-                           float* dvdt_out, float* dudt_out, float* dEdt_out,
-                           float* ap_ij, float* av_ij, void* stream);
+                           const int32_t* verlet_cnt, float* dvdt_out, float* dudt_out,
+                           float* dEdt_out, float* ap_ij, float* av_ij, void* stream);
 /* The same pass under the reference's two wrapper names. */
 int sph_compsph_accel(const SphParams* p, int64_t n, const float* x, const float* H,
                       const float* m, const float* rho, const float* v, const float* c,
                       const float* alpha, const float* P, const float* omega,
                       const int32_t* offs, const int32_t* cnt, const int32_t* list,
-                      float* dvdt_out, float* ap_ij, float* av_ij, void* stream);
+                      const int32_t* verlet_cnt, float* dvdt_out, float* ap_ij, float* av_ij,
+                      void* stream);
 int sph_compsph_dudt(const SphParams* p, int64_t n, const float* x, const float* H,
                      const float* m, const float* rho, const float* v, const float* c,
                      const float* alpha, const float* P, const float* omega,

@@ -68,7 +68,7 @@ class Oracle:
         assert L.oracle_real_size() == np.dtype(self.dtype).itemsize
         P = C.c_void_p
         i64 = C.c_int64
-        L.oracle_neighbors_build.argtypes = [P, i64, _f32p, _f32p, i64, _i32p, _u32p, _i32p, _i32p, _i32p,
+        L.oracle_neighbors_build.argtypes = [P, i64, _f32p, _f32p, i64, _i32p, _u32p, _i32p, _i32p, _i32p, _nullable(_i32p),
                                              _nullable(_i32p), i64, C.POINTER(C.c_int64)]
         L.oracle_density.argtypes = [P, i64, C.c_int, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_adaptive_h_iter.argtypes = [P, i64, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rpn]
@@ -112,19 +112,27 @@ class Oracle:
         return C.c_void_p(C.addressof(params))
 
     # ------------------------------------------------------------------ neighbour search
-    def neighbors(self, params, x, H, cell_capacity: int, list_capacity: int | None = None) -> dict:
+    def neighbors(self, params, x, H, cell_capacity: int, list_capacity: int | None = None, partition: bool = True) -> dict:
+        """Verlet list in the library's layout: with ``partition`` (the library's default)
+        each row holds its interacting entries first (``inter_counts`` of them)."""
         x32 = np.ascontiguousarray(np.asarray(x), dtype=np.float32)
         H32 = np.ascontiguousarray(np.asarray(H), dtype=np.float32)
         n = H32.shape[0]
         si = np.zeros(n, np.int32); sk = np.zeros(n, np.uint32); grid = np.zeros(8, np.int32)
         offs = np.zeros(n, np.int32); cnt = np.zeros(n, np.int32)
+        icnt = np.zeros(n, np.int32) if partition else None
         nnz = C.c_int64(0)
         # count first
-        self.lib.oracle_neighbors_build(self._p(params), n, x32, H32, cell_capacity, si, sk, grid, offs, cnt, None, 0, C.byref(nnz))
+        self.lib.oracle_neighbors_build(self._p(params), n, x32, H32, cell_capacity, si, sk, grid, offs, cnt, icnt, None, 0,
+                                        C.byref(nnz))
         cap = nnz.value if list_capacity is None else list_capacity
         lst = np.zeros(max(cap, 1), np.int32)
-        self.lib.oracle_neighbors_build(self._p(params), n, x32, H32, cell_capacity, si, sk, grid, offs, cnt, lst, cap, C.byref(nnz))
-        return dict(sort_index=si, sorted_keys=sk, grid=grid, offsets=offs, counts=cnt, list=lst[: nnz.value], nnz=nnz.value)
+        self.lib.oracle_neighbors_build(self._p(params), n, x32, H32, cell_capacity, si, sk, grid, offs, cnt, icnt, lst, cap,
+                                        C.byref(nnz))
+        out = dict(sort_index=si, sorted_keys=sk, grid=grid, offsets=offs, counts=cnt, list=lst[: nnz.value], nnz=nnz.value)
+        if partition:
+            out["inter_counts"] = icnt
+        return out
 
     # ------------------------------------------------------------------ pair operations
     def density(self, params, mode, x, H, m, nb) -> np.ndarray:

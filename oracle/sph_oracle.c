@@ -217,10 +217,13 @@ static void cell_coords_f(const NGrid* g, int D, const float* x, int* c) {
     }
 }
 
-/* Verlet list, same definition and canonical order as the GPU (see header). */
+/* Verlet list, same definition and canonical order as the GPU (see header).  With
+ * inter_counts, each row holds its interacting entries (fl(sqrt(r^2))/max(H_i,H_j) < 1)
+ * first and the rest after them, both in walk order; inter_counts[i] is the prefix length. */
 int oracle_neighbors_build(const SphParams* p, int64_t n, const float* x, const float* H, int64_t cell_capacity,
                            int32_t* sort_index, uint32_t* sorted_keys, int32_t* grid_out,
-                           int32_t* offsets, int32_t* counts, int32_t* list, int64_t list_capacity, int64_t* nnz_out) {
+                           int32_t* offsets, int32_t* counts, int32_t* inter_counts, int32_t* list, int64_t list_capacity,
+                           int64_t* nnz_out) {
     int D = p->dim;
     NGrid g;
     memset(&g, 0, sizeof(g));
@@ -304,13 +307,15 @@ int oracle_neighbors_build(const SphParams* p, int64_t n, const float* x, const 
                 if (dup) continue;
                 sk[nk++] = kk;
             }
-            int cntv = 0;
+            int cntv = 0, icntv = 0, restv = 0;
             int32_t base = pass ? offsets[i] : 0;
+            int32_t tail = (pass && inter_counts) ? base + inter_counts[i] : base;
             for (int q = 0; q < nk; ++q) {
                 for (int32_t k = begin[sk[q]]; k < begin[sk[q] + 1]; ++k) {
                     int32_t j = sort_index[k];
                     const float* xj = x + (int64_t)j * D;
-                    float R = vs * fmaxf(Hi, H[j]);
+                    float Hm = fmaxf(Hi, H[j]);
+                    float R = vs * Hm;
                     float r2 = 0.f;
                     for (int a = 0; a < D; ++a) {
                         float d = xi[a] - xj[a];
@@ -321,12 +326,18 @@ int oracle_neighbors_build(const SphParams* p, int64_t n, const float* x, const 
                         r2 = a == 0 ? d * d : r2 + d * d;
                     }
                     if (r2 < R * R) {
-                        if (pass) list[base + cntv] = j;
+                        int inter = inter_counts && (sqrtf(r2) / Hm < 1.0f);
+                        if (pass) {
+                            if (inter) list[base + icntv] = j;
+                            else list[tail + restv] = j;
+                        }
+                        icntv += inter;
+                        restv += !inter;
                         ++cntv;
                     }
                 }
             }
-            if (!pass) counts[i] = cntv;
+            if (!pass) { counts[i] = cntv; if (inter_counts) inter_counts[i] = icntv; }
         }
     }
     free(keys); free(begin); free(cur);

@@ -69,7 +69,7 @@ def test_argument_validation_happens_on_the_host():
     # a workspace smaller than required is refused
     dummy = 256  # never dereferenced: the size check fails first
     rc = lib.sph_neighbors_build(pp, 1000, dummy, dummy, dummy, 16, 4096, dummy, dummy, dummy, dummy, dummy, dummy, dummy,
-                                 dummy, 10, dummy, None, None, None, 0, None, dummy, None)
+                                 dummy, 10, dummy, None, None, dummy, None)
     assert rc == -2
 
 
@@ -106,3 +106,35 @@ def test_ctypes_prototypes_match_header_arity():
         params = m.group(1).strip()
         n = 0 if params in ("", "void") else len(params.split(","))
         assert n == len(args), (name, n, len(args))
+
+
+def test_python_call_sites_pass_every_argument():
+    """Every call of a C entry point in the package passes exactly the declared number of
+    arguments (``*_lists(...)``, ``*_csr(...)`` and ``*rows`` expand to the three CSR
+    pointers).  Runs on the source, so it needs no GPU."""
+    import ast
+    import pathlib
+    root = pathlib.Path(_capi.__file__).resolve().parent
+    protos = dict(_capi._PROTOS)
+    checked = 0
+    for path in sorted(root.glob("*.py")):
+        tree = ast.parse(path.read_text())
+        for node in ast.walk(tree):
+            if not (isinstance(node, ast.Call) and isinstance(node.func, ast.Attribute) and node.func.attr in protos):
+                continue
+            n, known = 0, True
+            for a in node.args:
+                if isinstance(a, ast.Starred):
+                    v = a.value
+                    if isinstance(v, ast.Call) and isinstance(v.func, ast.Name) and v.func.id in ("_lists", "_csr"):
+                        n += 3
+                    elif isinstance(v, ast.Name) and v.id == "rows":
+                        n += 3
+                    else:
+                        known = False
+                else:
+                    n += 1
+            if known:
+                assert n == len(protos[node.func.attr]), f"{path.name}:{node.lineno} {node.func.attr}: {n} != {len(protos[node.func.attr])}"
+                checked += 1
+    assert checked > 30

@@ -67,21 +67,34 @@ def test_gpu_golden_omega_and_pi_forms(G):
             assert_close(av.cpu().numpy(), g["compsph_av"], 1e-4, 1e-5, "av_ij vs reference (GPU)")
 
 
+def verlet_permutation(g, adj):
+    """Index of each of the library's Verlet entries in the golden (walk-order) list."""
+    offs, cnt = g["offsets"], g["counts"]
+    lst = adj.neighborList.cpu().numpy()
+    perm = np.empty(adj.nnz, np.int64)
+    for i in range(len(cnt)):
+        row = g["list"][offs[i]: offs[i] + cnt[i]]
+        where = {j: offs[i] + k for k, j in enumerate(row.tolist())}
+        perm[offs[i]: offs[i] + cnt[i]] = [where[j] for j in lst[offs[i]: offs[i] + cnt[i]].tolist()]
+    return perm
+
+
 def test_gpu_golden_interacting_list(G):
-    """The same golden results through the library's own list and its interacting subset
-    (stride-2 rows; pairwise arrays still indexed by Verlet entry)."""
+    """The same golden results through the library's own list, walking the interacting
+    prefix of each row (pairwise arrays indexed by the library's Verlet entries, zeros
+    for the rest of each row)."""
     t, g = G
     p = params_for(g)
     adj = built_adjacency(p, t["x"], t["H"])
-    assert adj.interList is not None
-    assert adj.nnz == t["list"].shape[0]
-    assert torch.equal(adj.neighborList[: adj.nnz], t["list"].to(adj.neighborList.dtype)), "library list differs from the oracle's"
+    assert adj.interCounts is not None and adj.nnz == t["list"].shape[0]
+    assert np.array_equal(adj.numNeighbors.cpu().numpy(), g["counts"])
+    perm = verlet_permutation(g, adj)
     dvdt, dudt, dEdt, ap, av = ops.compsph_accel_dudt(p, t["x"], t["H"], t["m"], t["rho"], t["v"], t["c"], t["alpha"], t["P"],
                                                       t["omega"], adj)
-    assert_close(dvdt.cpu().numpy(), g["compsph_accel"][3], 1e-4, 1e-5, "dv/dt (interacting list)")
-    assert_close(dudt.cpu().numpy(), g["compsph_dudt"][3], 1e-4, 1e-5, "du/dt (interacting list)")
-    assert_close(ap.cpu().numpy(), g["compsph_ap"], 1e-4, 1e-5, "ap_ij (interacting list)")
-    assert_close(av.cpu().numpy(), g["compsph_av"], 1e-4, 1e-5, "av_ij (interacting list)")
+    assert_close(dvdt.cpu().numpy(), g["compsph_accel"][3], 1e-4, 1e-5, "dv/dt (interacting prefixes)")
+    assert_close(dudt.cpu().numpy(), g["compsph_dudt"][3], 1e-4, 1e-5, "du/dt (interacting prefixes)")
+    assert_close(ap.cpu().numpy(), g["compsph_ap"][perm], 1e-4, 1e-5, "ap_ij (interacting prefixes)")
+    assert_close(av.cpu().numpy(), g["compsph_av"][perm], 1e-4, 1e-5, "av_ij (interacting prefixes)")
     for which in range(2):
         tt, ct = g["monaghan_sets"][which]
         pm = params_for(g, tt, ct)

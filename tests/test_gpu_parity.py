@@ -89,14 +89,12 @@ def test_interacting_list_is_exact_subset(cuda, dim, n_side):
         r2 = (r2 + d[:, a] * d[:, a]).astype(np.float32)
     Hm = np.maximum(H[i], H[lst])
     keep = (np.sqrt(r2).astype(np.float32) / Hm).astype(np.float32) < np.float32(1.0)
-    il = adj.interList.cpu().numpy().reshape(-1, 2)
-    ioffs, icnt = adj.interOffsets.cpu().numpy(), adj.interCounts.cpu().numpy()
-    assert np.array_equal(ioffs, offs)
+    icnt = adj.interCounts.cpu().numpy()
     assert adj.interNnz == int(keep.sum()) == int(icnt.sum())
     assert np.array_equal(icnt, np.bincount(i[keep], minlength=len(H)))
-    valid = np.concatenate([np.arange(o, o + c) for o, c in zip(ioffs, icnt)])
-    assert np.array_equal(il[valid, 1], np.nonzero(keep)[0])
-    assert np.array_equal(il[valid, 0], lst[keep])
+    # every row: its interacting entries first, the rest after them
+    pos_in_row = np.arange(len(lst)) - np.repeat(offs, cnt)
+    assert np.array_equal(keep, pos_in_row < np.repeat(icnt, cnt))
 
 
 def test_neighbors_capacity_overflow_is_recovered(cuda):
@@ -108,6 +106,7 @@ def test_neighbors_capacity_overflow_is_recovered(cuda):
     adj = ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale)
     ref = oracle.get("f32").neighbors(p, P["positions"], P["supports"], cell_capacity_for(900, 2))
     assert adj.nnz == ref["nnz"] and np.array_equal(adj.neighborList.cpu().numpy(), ref["list"])
+    assert np.array_equal(adj.interCounts.cpu().numpy(), ref["inter_counts"])
 
 
 def test_neighbors_reject_nonpositive_support(cuda):
@@ -251,9 +250,9 @@ def test_kahan_option_matches(cuda):
 @pytest.mark.parametrize("dim,n_side", CASES)
 def test_prior_list_refresh(cuda, dim, n_side):
     """A still-valid prior list (small displacement and support change) is kept and its
-    interacting sublist recomputed: per row the same j set as a fresh build, with entry
-    indices pointing at those j in the prior Verlet rows.  A large displacement rebuilds
-    (the result then equals the oracle's list bit for bit)."""
+    rows reordered for the new positions: per row the same Verlet set as before, its
+    interacting prefix the same j set as a fresh build's, in the prior row order.  A large
+    displacement rebuilds (the result then equals the oracle's list bit for bit)."""
     cfg, sch, p = make_params(dim)
     P = make_particles(dim, n_side, seed=90 + dim)
     G = to_gpu(P, cuda)
@@ -266,23 +265,28 @@ def test_prior_list_refresh(cuda, dim, n_side):
     adj1 = ops.buildVerletList(torch.from_numpy(x1).to(cuda), torch.from_numpy(H1).to(cuda), p, p.verlet_scale, adj0)
     assert adj1.neighborList.data_ptr() == adj0.neighborList.data_ptr(), "valid prior list must be kept"
     fresh = ops.buildVerletList(torch.from_numpy(x1).to(cuda), torch.from_numpy(H1).to(cuda), p, p.verlet_scale)
-    assert adj1.interList is None                      # filtered on first use by a pass
+    assert adj1.interCounts is None                    # rows reordered on first use by a pass
+    lst0 = adj0.neighborList.cpu().numpy().copy()
     ops._lists(p, adj1, True)
-    lst0 = adj0.neighborList.cpu().numpy()
-    il1 = adj1.interList.cpu().numpy().reshape(-1, 2)
-    o1, c1 = adj1.interOffsets.cpu().numpy(), adj1.interCounts.cpu().numpy()
-    il2 = fresh.interList.cpu().numpy().reshape(-1, 2)
-    o2, c2 = fresh.interOffsets.cpu().numpy(), fresh.interCounts.cpu().numpy()
+    assert adj1.neighborList.data_ptr() != adj0.neighborList.data_ptr(), "the prior rows must stay untouched"
+    assert np.array_equal(adj0.neighborList.cpu().numpy(), lst0)
+    o, cnt = adj1.neighborOffsets.cpu().numpy(), adj1.numNeighbors.cpu().numpy()
+    l1, c1 = adj1.neighborList.cpu().numpy(), adj1.interCounts.cpu().numpy()
+    l2, c2 = fresh.neighborList.cpu().numpy(), fresh.interCounts.cpu().numpy()
+    o2 = fresh.neighborOffsets.cpu().numpy()
     assert int(adj1._inter_nnz_dev.item()) == fresh.interNnz == int(c1.sum())
     for i in range(len(H)):
-        r1 = il1[o1[i]: o1[i] + c1[i]]
-        r2 = il2[o2[i]: o2[i] + c2[i]]
-        assert set(r1[:, 0].tolist()) == set(r2[:, 0].tolist()), i
-        assert np.array_equal(lst0[r1[:, 1]], r1[:, 0])
-        assert np.all(np.diff(r1[:, 1]) > 0)
+        row0 = lst0[o[i]: o[i] + cnt[i]]
+        row1 = l1[o[i]: o[i] + cnt[i]]
+        assert sorted(row1.tolist()) == sorted(row0.tolist()), i
+        pre1, pre2 = row1[: c1[i]], l2[o2[i]: o2[i] + c2[i]]
+        assert set(pre1.tolist()) == set(pre2.tolist()), i
+        where = {j: k for k, j in enumerate(row0.tolist())}
+        assert np.all(np.diff([where[j] for j in pre1.tolist()]) > 0)          # prior order kept in the prefix
     # beyond the skin: rebuilt, identical to the oracle
     x2 = (((P["positions"] + 0.5 * H.max()) + 0.5) % 1.0 - 0.5).astype(np.float32)
     adj2 = ops.buildVerletList(torch.from_numpy(x2).to(cuda), G["supports"], p, p.verlet_scale, adj0)
     assert adj2.neighborList.data_ptr() != adj0.neighborList.data_ptr()
     ref = oracle.get("f32").neighbors(p, x2, H, cell_capacity_for(len(H), dim))
     assert np.array_equal(adj2.neighborList.cpu().numpy(), ref["list"])
+    assert np.array_equal(adj2.interCounts.cpu().numpy(), ref["inter_counts"])

@@ -63,7 +63,7 @@ def test_neighbor_list_matches_brute_force(o32, dim, n_side, periodic):
     cfg, sch, p = make_params(dim, periodic=periodic)
     P = make_particles(dim, n_side, periodic=periodic, seed=dim)
     x, H = P["positions"], P["supports"]
-    nb = o32.neighbors(p, x, H, 1 << 16)
+    nb = o32.neighbors(p, x, H, 1 << 16, partition=False)
     ref = brute_force(x, H, p.verlet_scale, 1.0, periodic)
     pos = np.argsort(nb["sort_index"])
     assert np.array_equal(np.sort(nb["sort_index"]), np.arange(len(H)))
@@ -83,6 +83,23 @@ def test_neighbor_list_matches_brute_force(o32, dim, n_side, periodic):
         assert i in row
     # super-symmetric lists are symmetric
     assert ref.sum() == nb["nnz"]
+    # the library's layout: every row a stable partition of the walk-order row, the
+    # entries with fl(sqrt(r^2)) / max(H_i, H_j) < 1 first
+    part = o32.neighbors(p, x, H, 1 << 16)
+    assert np.array_equal(part["offsets"], nb["offsets"]) and np.array_equal(part["counts"], nb["counts"])
+    for i in range(len(H)):
+        row = nb["list"][nb["offsets"][i]: nb["offsets"][i] + nb["counts"][i]]
+        d = (x[i] - x[row]).astype(np.float32)
+        if periodic:
+            d = np.where(d > 0.5, d - np.float32(1.0), np.where(d < -0.5, d + np.float32(1.0), d)).astype(np.float32)
+        r2 = d[:, 0] * d[:, 0]
+        for a in range(1, dim):
+            r2 = (r2 + d[:, a] * d[:, a]).astype(np.float32)
+        inter = (np.sqrt(r2, dtype=np.float32) / np.maximum(H[i], H[row])) < np.float32(1.0)
+        want = np.concatenate([row[inter], row[~inter]])
+        got = part["list"][part["offsets"][i]: part["offsets"][i] + part["counts"][i]]
+        assert np.array_equal(got, want), i
+        assert part["inter_counts"][i] == inter.sum()
 
 
 def test_neighbor_small_periodic_grid_deduplicates(o32):

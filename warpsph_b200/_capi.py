@@ -98,8 +98,8 @@ _PROTOS = {
     "sph_kernel_constants": [_I32, _I32, _P, _P],
     "sph_neighbors_workspace_size": [_P, _I64, _I64, _P],
     "sph_neighbors_build": [_P, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _P,
-                            _P, _P, _P, _I64, _P, _P, _P],
-    "sph_neighbors_refresh": [_P, _I64] + [_P] * 14,
+                            _P, _P, _P, _P],
+    "sph_neighbors_refresh": [_P, _I64] + [_P] * 13,
     "sph_neighbors_expand": [_I64, _P, _P, _P, _I64, _P, _P, _P],
     "sph_density_gather": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_adaptive_h_iter": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
@@ -110,13 +110,13 @@ _PROTOS = {
     "sph_grad_v": [_P, _I64] + [_P] * 19,
     "sph_switch_cullen": [_P, _I64] + [_P] * 18,
     "sph_switch_balsara": [_P, _I64, _P, _P, _P, _P],
-    "sph_crk_accel_dudt": [_P, _I64] + [_P] * 21,
-    "sph_crk_accel": [_P, _I64] + [_P] * 20,
+    "sph_crk_accel_dudt": [_P, _I64] + [_P] * 23,
+    "sph_crk_accel": [_P, _I64] + [_P] * 21,
     "sph_crk_dudt": [_P, _I64] + [_P] * 18,
     "sph_compsph_prep": [_P, _I64] + [_P] * 12,
     "sph_grad_h_omega": [_P, _I64] + [_P] * 9,
-    "sph_compsph_accel_dudt": [_P, _I64] + [_P] * 18,
-    "sph_compsph_accel": [_P, _I64] + [_P] * 16,
+    "sph_compsph_accel_dudt": [_P, _I64] + [_P] * 19,
+    "sph_compsph_accel": [_P, _I64] + [_P] * 17,
     "sph_compsph_dudt": [_P, _I64] + [_P] * 14,
     "sph_monaghan_rhs": [_P, _I64] + [_P] * 22,
     "sph_compsph_balance": [_P, _I64] + [_P] * 15,
@@ -167,8 +167,25 @@ def lib() -> C.CDLL:
         fn = getattr(L, name)
         fn.argtypes = args
         fn.restype = _RESTYPE.get(name, C.c_int)
+        setattr(L, name, _Strict(fn, name, len(args)))
     _lib = L
     return L
+
+
+class _Strict:
+    """A C entry point that refuses a call with the wrong number of arguments (ctypes
+    passes surplus arguments on silently, which would shift every argument after a
+    forgotten or extra one)."""
+
+    __slots__ = ("fn", "name", "nargs")
+
+    def __init__(self, fn, name: str, nargs: int):
+        self.fn, self.name, self.nargs = fn, name, nargs
+
+    def __call__(self, *args):
+        if len(args) != self.nargs:
+            raise TypeError(f"{self.name} takes {self.nargs} arguments ({len(args)} given)")
+        return self.fn(*args)
 
 
 def declared_functions() -> list[str]:

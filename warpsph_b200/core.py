@@ -142,7 +142,8 @@ class AdjacencyList:
 
     neighborOffsets / numNeighbors are int32 [N]; neighborList is int32 [nnz] (the
     reference stores int64; ``i``/``j`` give the expanded int64 row/column arrays the
-    reference's torch code indexes with)."""
+    reference's torch code indexes with).  Each row lists its interacting neighbours
+    first (``interCounts``); pairwise arrays are indexed by position in neighborList."""
     neighborOffsets: torch.Tensor
     numNeighbors: torch.Tensor
     neighborList: torch.Tensor
@@ -155,11 +156,9 @@ class AdjacencyList:
     queryPositions: Optional[torch.Tensor] = None
     querySupports: Optional[torch.Tensor] = None
     verletScale: float = 1.0
-    # interacting subset (r < max(H_i, H_j)): (j, entry index) int32 pairs stored in each
-    # row's own Verlet range (interOffsets == neighborOffsets, first interCounts[i] valid)
-    interOffsets: Optional[torch.Tensor] = None
+    # interacting prefix: row i holds its entries with r < max(H_i, H_j) first, so the
+    # pair passes walk neighborList[off_i : off_i + interCounts[i]]
     interCounts: Optional[torch.Tensor] = None
-    interList: Optional[torch.Tensor] = None
     interNnz: int = 0
     _x_version: Optional[tuple] = field(default=None, repr=False)
     _h_version: Optional[tuple] = field(default=None, repr=False)

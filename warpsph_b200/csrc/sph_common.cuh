@@ -88,6 +88,28 @@ template <int D> __device__ __forceinline__ Vec<D> matvec(const Mat<D>& M, const
 // Warp's builtin min/max: `a < b ? a : b` / `a > b ? a : b` (NaN propagates from b).
 __device__ __forceinline__ float wmin(float a, float b) { return a < b ? a : b; }
 __device__ __forceinline__ float wmax(float a, float b) { return a > b ? a : b; }
+
+// Block-wide reduction (blockDim.x a multiple of 32, at most 1024 threads); the result is
+// valid in thread 0.  Every thread of the block must call it (it synchronises).  Used by
+// the global reductions so that each block issues one atomic instead of one per warp.
+template <typename T, typename Op>
+__device__ __forceinline__ T block_reduce(T v, T identity, Op op) {
+    __shared__ T part[32];
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();                              // earlier readers of part[] are done
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : identity;
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+struct OpMinF { __device__ __forceinline__ float operator()(float a, float b) const { return fminf(a, b); } };
+struct OpMaxF { __device__ __forceinline__ float operator()(float a, float b) const { return fmaxf(a, b); } };
+struct OpMaxU { __device__ __forceinline__ unsigned int operator()(unsigned int a, unsigned int b) const { return a > b ? a : b; } };
 __device__ __forceinline__ float safe_sqrt(float x) { return sqrtf(x > 0.f ? x : 0.f); }
 
 // ---------------------------------------------------------------- domain

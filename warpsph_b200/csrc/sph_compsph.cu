@@ -1,6 +1,6 @@
 // Pair passes of the CompSPH (grad-h, compatibly differenced) and Monaghan compressible
-// schemes.  Same lane layout as the CRK passes: G lanes of a warp per particle, rows
-// of the Verlet list (stride 1) or of its interacting subset (stride 2, r < max(H_i, H_j)).
+// schemes.  Same lane layout as the CRK passes: G lanes of a warp per particle, over
+// Verlet rows or their interacting prefixes (r < max(H_i, H_j)).
 //
 //   k_compsph_prep        Omega (grad-h, gather), the super-symmetric velocity divergence
 //                         of the Cullen switch and the consistent continuity d rho/dt,
@@ -25,7 +25,7 @@ namespace wsph {
 // d rho_i/dt = -(rho_i / Omega_i) (1 / rho_i) sum_j m_j (v_j - v_i) . grad W(r_ij, max(H_i, H_j))
 //   (modules/momentum/consistent.py:8-35, the consistent divergence weighting each
 //   neighbour by m_j / rho_i, so that rho_i cancels).
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_compsph_prep(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
                const float* __restrict__ rho, const float* __restrict__ v,
@@ -41,7 +41,7 @@ k_compsph_prep(int n, DevParams P, const float* __restrict__ x, const float* __r
         const float Hi = H[i];
         int b = offs[i], e = b + cnt[i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             float r2 = dot<D>(xij, xij);
             float Hs = wmax(Hi, __ldg(H + j));
@@ -86,16 +86,17 @@ k_compsph_prep(int n, DevParams P, const float* __restrict__ x, const float* __r
 // and modules/compSPH/dudt.py:60-139 (gather gradient grad W(H_i)) in one pass; dE/dt of
 // schemes/compSPH.py:170 per particle.  Without Omega the grad-h terms are 1, without
 // alpha the switch is 1 and without c the sound speed is DiffusionParameters.c_s
-// (accel.py:195-198).  With the interacting list (stride 2) the ap_ij / av_ij entries of
-// non-interacting Verlet pairs are not written (the caller provides zero-filled arrays).
-template <int KF, int D, int G, int ST>
+// (accel.py:195-198).  Walking the interacting prefix of each Verlet row (cnt =
+// interacting counts) with vcnt = the Verlet counts, the ap_ij / av_ij entries of the
+// rest of the row are written as zeros.
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
                      const float* __restrict__ rho, const float* __restrict__ v, const float* __restrict__ c,
                      const float* __restrict__ alpha, const float* __restrict__ Pr, const float* __restrict__ omega,
                      const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
-                     float* __restrict__ dvdt, float* __restrict__ dudt, float* __restrict__ dEdt,
-                     float* __restrict__ ap, float* __restrict__ av) {
+                     const int32_t* __restrict__ vcnt, float* __restrict__ dvdt, float* __restrict__ dudt,
+                     float* __restrict__ dEdt, float* __restrict__ ap, float* __restrict__ av) {
     Grp<G> g(n);
     const bool comp = P.kahan != 0;
     KSum acc[D], du;
@@ -111,16 +112,14 @@ k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const floa
         const float pTi = Pi / (rhoi * rhoi) / omi;
         int b = offs[i], e = b + cnt[i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             float r2 = dot<D>(xij, xij);
             float Hj = __ldg(H + j);
             float Hm = wmax(Hi, Hj);
             if (!(r2 < Hm * Hm)) {
-                if (ST == 1) {
-                    if (ap) store_vec<D>(ap, k, vzero<D>());
-                    if (av) store_vec<D>(av, k, vzero<D>());
-                }
+                if (ap) store_vec<D>(ap, k, vzero<D>());
+                if (av) store_vec<D>(av, k, vzero<D>());
                 continue;
             }
             float r = safe_sqrt(r2);
@@ -156,6 +155,13 @@ k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const floa
             const float vTerm = -0.5f * Vj * pi_i * mu * dotg;
             du.add(pTerm + vTerm, comp);
         }
+        if (vcnt && (ap || av)) {
+            const int te = b + __ldg(vcnt + i);
+            for (int q = e + g.lane; q < te; q += G) {
+                if (ap) store_vec<D>(ap, q, vzero<D>());
+                if (av) store_vec<D>(av, q, vzero<D>());
+            }
+        }
     }
     float o[D], od;
     #pragma unroll
@@ -189,7 +195,7 @@ k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const floa
 //              (dissipation/wp_dissipation.py:59-119)
 // dv/dt = pressure + viscosity; du/dt = PdV + conduction + heating;
 // dE/dt = m_i v_i . dv/dt + m_i (PdV + conduction) (monaghan.py:143).
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_monaghan_rhs(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
                const float* __restrict__ rho, const float* __restrict__ v, const float* __restrict__ u,
@@ -214,7 +220,7 @@ k_monaghan_rhs(int n, DevParams P, const float* __restrict__ x, const float* __r
         const float pTi = Pi / (rhoi * rhoi) / omi;
         int b = offs[i], e = b + cnt[i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             float r2 = dot<D>(xij, xij);
             float Hj = __ldg(H + j);
@@ -298,7 +304,7 @@ int sph_compsph_prep(const SphParams* p, int64_t n, const float* x, const float*
     if (!omega_out && !div_out && !drhodt_out) return SPH_OK;
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_compsph_prep<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, v, offs, cnt, list,
+    WSPH_DISPATCH_KDS(*p, (k_compsph_prep<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, v, offs, cnt, list,
                                                                                                         omega_out, div_out, drhodt_out)));
     return check_launch("sph_compsph_prep");
 }
@@ -311,8 +317,8 @@ int sph_grad_h_omega(const SphParams* p, int64_t n, const float* x, const float*
 
 int sph_compsph_accel_dudt(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
                            const float* v, const float* c, const float* alpha, const float* Pr, const float* omega,
-                           const int32_t* offs, const int32_t* cnt, const int32_t* list, float* dvdt_out, float* dudt_out,
-                           float* dEdt_out, float* ap_ij, float* av_ij, void* stream) {
+                           const int32_t* offs, const int32_t* cnt, const int32_t* list, const int32_t* verlet_cnt,
+                           float* dvdt_out, float* dudt_out, float* dEdt_out, float* ap_ij, float* av_ij, void* stream) {
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(Pr);
     CHECK_CSR();
@@ -320,24 +326,25 @@ int sph_compsph_accel_dudt(const SphParams* p, int64_t n, const float* x, const 
         (rc = check_align_vec(P, ap_ij, "ap_ij")) || (rc = check_align_vec(P, av_ij, "av_ij")))
         return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_compsph_accel_dudt<KF, D, G_HEAVY, ST><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>(
-                              (int)n, P, x, H, m, rho, v, c, alpha, Pr, omega, offs, cnt, list, dvdt_out, dudt_out, dEdt_out, ap_ij, av_ij)));
+    WSPH_DISPATCH_KDS(*p, (k_compsph_accel_dudt<KF, D, G_HEAVY><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>(
+                              (int)n, P, x, H, m, rho, v, c, alpha, Pr, omega, offs, cnt, list, verlet_cnt, dvdt_out, dudt_out, dEdt_out,
+                              ap_ij, av_ij)));
     return check_launch("sph_compsph_accel_dudt");
 }
 
 int sph_compsph_accel(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
                       const float* v, const float* c, const float* alpha, const float* P, const float* omega,
-                      const int32_t* offs, const int32_t* cnt, const int32_t* list, float* dvdt_out, float* ap_ij,
-                      float* av_ij, void* stream) {
-    return sph_compsph_accel_dudt(p, n, x, H, m, rho, v, c, alpha, P, omega, offs, cnt, list, dvdt_out, nullptr, nullptr, ap_ij,
-                                  av_ij, stream);
+                      const int32_t* offs, const int32_t* cnt, const int32_t* list, const int32_t* verlet_cnt,
+                      float* dvdt_out, float* ap_ij, float* av_ij, void* stream) {
+    return sph_compsph_accel_dudt(p, n, x, H, m, rho, v, c, alpha, P, omega, offs, cnt, list, verlet_cnt, dvdt_out, nullptr, nullptr,
+                                  ap_ij, av_ij, stream);
 }
 
 int sph_compsph_dudt(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
                      const float* v, const float* c, const float* alpha, const float* P, const float* omega,
                      const int32_t* offs, const int32_t* cnt, const int32_t* list, float* dudt_out, void* stream) {
-    return sph_compsph_accel_dudt(p, n, x, H, m, rho, v, c, alpha, P, omega, offs, cnt, list, nullptr, dudt_out, nullptr, nullptr,
-                                  nullptr, stream);
+    return sph_compsph_accel_dudt(p, n, x, H, m, rho, v, c, alpha, P, omega, offs, cnt, list, nullptr, nullptr, dudt_out, nullptr,
+                                  nullptr, nullptr, stream);
 }
 
 int sph_monaghan_rhs(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
@@ -352,7 +359,7 @@ int sph_monaghan_rhs(const SphParams* p, int64_t n, const float* x, const float*
         (rc = check_align_vec(P, dvdt_pressure, "dvdt_pressure")) || (rc = check_align_vec(P, dvdt_viscosity, "dvdt_viscosity")))
         return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_monaghan_rhs<KF, D, G_HEAVY, ST><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>(
+    WSPH_DISPATCH_KDS(*p, (k_monaghan_rhs<KF, D, G_HEAVY><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>(
                               (int)n, P, x, H, m, rho, v, u, c, alpha, Pr, omega, offs, cnt, list, dvdt_out, dudt_out, dEdt_out,
                               dvdt_pressure, dvdt_viscosity, dudt_pdv, dudt_conductivity, dudt_heating)));
     return check_launch("sph_monaghan_rhs");

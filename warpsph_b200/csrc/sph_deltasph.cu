@@ -35,10 +35,10 @@ int sph_deltasph_rhs(const SphParams* p, const SphWcParams* wc, int64_t n, const
     float* gL = scratch;
     float* Pr = scratch + n * P.dim;
     count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_ds_passA<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, W, x, H, m, rho, offs, cnt,
+    WSPH_DISPATCH_KDS(*p, (k_ds_passA<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, W, x, H, m, rho, offs, cnt,
                                                                                                      list, gL, Pr)));
     count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_ds_passB<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, W, x, H, m, rho, v,
+    WSPH_DISPATCH_KDS(*p, (k_ds_passB<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, W, x, H, m, rho, v,
                                                                                                      gL, Pr, offs, cnt, list,
                                                                                                      dvdt_out, drhodt_out)));
     return check_launch("sph_deltasph_rhs");

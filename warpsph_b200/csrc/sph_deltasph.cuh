@@ -93,7 +93,7 @@ template <int D> __device__ __forceinline__ Vec<D> renormalise(const Mat<D>& M, 
 }
 
 // Per-lane partial sums of pass A for particle i.
-template <int KF, int D, int G, int ST, bool CG = false>
+template <int KF, int D, int G, bool CG = false>
 __device__ __forceinline__ void passA_partial(int i, int lane, const DevParams& P, const float* x,
                                               const float* __restrict__ H, const float* __restrict__ m,
                                               const float* rho, const int32_t* __restrict__ offs,
@@ -103,7 +103,7 @@ __device__ __forceinline__ void passA_partial(int i, int lane, const DevParams& 
     const float Hi = H[i], rhoi = ldf<CG>(rho + i);
     const int b = offs[i], e = b + cnt[i];
     for (int q = b + lane; q < e; q += G) {
-        int j, k; entry<ST>(list, q, j, k);
+        int j, k; entry(list, q, j, k);
         const Vec<D> xij = dist_vec<D>(xi, ldv<D, CG>(x, j), P.dom);
         const float r = safe_sqrt(dot<D>(xij, xij));
         float W; Vec<D> gW;
@@ -131,7 +131,7 @@ template <int D, int G> __device__ __forceinline__ void passA_reduce(Mat<D>& M, 
 
 // Per-lane partial sums of pass B for particle i: cont = sum V (v_j - v_i).gW,
 // dd = sum V psi.gW, pf = sum V p_ij gW, visc = sum V mu f gW / rho_bar.
-template <int KF, int D, int G, int ST, bool CG = false>
+template <int KF, int D, int G, bool CG = false>
 __device__ __forceinline__ void passB_partial(int i, int lane, const DevParams& P, const WcDev& W, const float* x,
                                               const float* __restrict__ H, const float* __restrict__ m, const float* rho,
                                               const float* v, const float* gL, const float* Pr,
@@ -143,7 +143,7 @@ __device__ __forceinline__ void passB_partial(int i, int lane, const DevParams& 
     const float factor = W.inviscid ? W.alpha * W.c0 * Hi / W.xi : W.visc_nu;
     const int b = offs[i], e = b + cnt[i];
     for (int q = b + lane; q < e; q += G) {
-        int j, k; entry<ST>(list, q, j, k);
+        int j, k; entry(list, q, j, k);
         const Vec<D> xij = dist_vec<D>(xi, ldv<D, CG>(x, j), P.dom);
         const float r2 = dot<D>(xij, xij);
         const float r = safe_sqrt(r2);
@@ -211,7 +211,7 @@ template <int D> __device__ __forceinline__ void passB_finish(const WcDev& W, fl
 }
 
 // Pass A: gradRhoL [n, D] and the EOS pressure P [n].
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_ds_passA(int n, DevParams P, WcDev W, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
            const float* __restrict__ rho, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
@@ -219,7 +219,7 @@ k_ds_passA(int n, DevParams P, WcDev W, const float* __restrict__ x, const float
     Grp<G> g(n);
     Mat<D> M = mzero<D>();
     Vec<D> s = vzero<D>();
-    if (g.valid) passA_partial<KF, D, G, ST>(g.i, g.lane, P, x, H, m, rho, offs, cnt, list, M, s);
+    if (g.valid) passA_partial<KF, D, G>(g.i, g.lane, P, x, H, m, rho, offs, cnt, list, M, s);
     passA_reduce<D, G>(M, s);
     if (g.valid && g.lane == 0) {
         store_vec<D>(gL, g.i, renormalise<D>(M, s));
@@ -227,7 +227,7 @@ k_ds_passA(int n, DevParams P, WcDev W, const float* __restrict__ x, const float
     }
 }
 
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_ds_passB(int n, DevParams P, WcDev W, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
            const float* __restrict__ rho, const float* __restrict__ v, const float* __restrict__ gL, const float* __restrict__ Pr,
@@ -236,7 +236,7 @@ k_ds_passB(int n, DevParams P, WcDev W, const float* __restrict__ x, const float
     Grp<G> g(n);
     float cont = 0.f, dd = 0.f;
     Vec<D> pf = vzero<D>(), visc = vzero<D>();
-    if (g.valid) passB_partial<KF, D, G, ST>(g.i, g.lane, P, W, x, H, m, rho, v, gL, Pr, offs, cnt, list, cont, dd, pf, visc);
+    if (g.valid) passB_partial<KF, D, G>(g.i, g.lane, P, W, x, H, m, rho, v, gL, Pr, offs, cnt, list, cont, dd, pf, visc);
     cont = gsum<G>(cont); dd = gsum<G>(dd);
     #pragma unroll
     for (int a = 0; a < D; ++a) { pf.v[a] = gsum<G>(pf.v[a]); visc.v[a] = gsum<G>(visc.v[a]); }

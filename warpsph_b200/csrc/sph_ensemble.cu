@@ -206,7 +206,7 @@ k_ens_step(EnsArgs a) {
             const bool valid = i < a.n;
             Mat<D> M = mzero<D>();
             Vec<D> s = vzero<D>();
-            if (valid) passA_partial<KF, D, G, 1, true>(i, lane, a.P, xs, a.H, a.m, rs, a.offs, a.cnt, a.list, M, s);
+            if (valid) passA_partial<KF, D, G, true>(i, lane, a.P, xs, a.H, a.m, rs, a.offs, a.cnt, a.list, M, s);
             passA_reduce<D, G>(M, s);
             if (valid && lane == 0) {
                 store_vec<D>(a.gL, i, renormalise<D>(M, s));
@@ -220,7 +220,7 @@ k_ens_step(EnsArgs a) {
             const bool valid = i < a.n;
             float cont = 0.f, dd = 0.f;
             Vec<D> pf = vzero<D>(), visc = vzero<D>();
-            if (valid) passB_partial<KF, D, G, 1, true>(i, lane, a.P, a.W, xs, a.H, a.m, rs, vs, a.gL, a.Pr, a.offs, a.cnt, a.list,
+            if (valid) passB_partial<KF, D, G, true>(i, lane, a.P, a.W, xs, a.H, a.m, rs, vs, a.gL, a.Pr, a.offs, a.cnt, a.list,
                                                         cont, dd, pf, visc);
             cont = gsum<G>(cont); dd = gsum<G>(dd);
             #pragma unroll

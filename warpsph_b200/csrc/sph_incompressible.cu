@@ -60,7 +60,7 @@ template <int D> __device__ __forceinline__ Vec<D> load_vec_cg(const float* p, i
 // ---------------------------------------------------------------- per-lane partial sums
 // Pressure acceleration, modules/pressure/iisph.py:7-24 with the symmetric gradient
 // rho_i sum_j m_j (q_i/rho_i^2 + q_j/rho_j^2) gradW(x_ij, H_j).  p_j = praw_j - mu.
-template <int KF, int D, int G, int ST, bool CG>
+template <int KF, int D, int G, bool CG>
 __device__ __forceinline__ Vec<D> accel_partial(int i, int lane, const DevParams& P, const float* __restrict__ x,
                                                 const float* __restrict__ H, const float* __restrict__ m,
                                                 const float* __restrict__ rho, const float* praw, float mu, float qi,
@@ -70,7 +70,7 @@ __device__ __forceinline__ Vec<D> accel_partial(int i, int lane, const DevParams
     const Vec<D> xi = load_vec<D>(x, i);
     const int b = offs[i], e = b + cnt[i];
     for (int q = b + lane; q < e; q += G) {
-        int j, k; entry<ST>(list, q, j, k);
+        int j, k; entry(list, q, j, k);
         const Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
         const float r = safe_sqrt(dot<D>(xij, xij));
         float W; Vec<D> g;
@@ -85,7 +85,7 @@ __device__ __forceinline__ Vec<D> accel_partial(int i, int lane, const DevParams
 }
 
 // Pressure shift, modules/incompressible/drift.py:38-57: -sum_j V_j (a_j - a_i).gradW(x_ij, H_j).
-template <int KF, int D, int G, int ST, bool CG>
+template <int KF, int D, int G, bool CG>
 __device__ __forceinline__ float shift_partial(int i, int lane, const DevParams& P, const float* __restrict__ x,
                                                const float* __restrict__ H, const float* __restrict__ m,
                                                const float* __restrict__ rho, const float* acc, const Vec<D>& ai,
@@ -95,7 +95,7 @@ __device__ __forceinline__ float shift_partial(int i, int lane, const DevParams&
     const Vec<D> xi = load_vec<D>(x, i);
     const int b = offs[i], e = b + cnt[i];
     for (int q = b + lane; q < e; q += G) {
-        int j, k; entry<ST>(list, q, j, k);
+        int j, k; entry(list, q, j, k);
         const Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
         const float r = safe_sqrt(dot<D>(xij, xij));
         float W; Vec<D> g;
@@ -111,7 +111,7 @@ __device__ __forceinline__ float shift_partial(int i, int lane, const DevParams&
 
 // ---------------------------------------------------------------- prep: divergence, alpha, source, diagonal
 // mode -1: standalone (div_out and/or alpha_out); 0: divergence-free solve; 1: density solve.
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_dfsph_prep(int n, DevParams P, int mode, float rho0, const float* __restrict__ x, const float* __restrict__ H,
              const float* __restrict__ m, const float* __restrict__ rho, const float* __restrict__ v,
@@ -136,7 +136,7 @@ k_dfsph_prep(int n, DevParams P, int mode, float rho0, const float* __restrict__
         }
         const int b = offs[i], e = b + cnt[i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             const Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             const float r = safe_sqrt(dot<D>(xij, xij));
             const float Hj = __ldg(H + j), mj = __ldg(m + j);
@@ -190,7 +190,7 @@ k_dfsph_prep(int n, DevParams P, int mode, float rho0, const float* __restrict__
 }
 
 // ---------------------------------------------------------------- standalone accel / shift passes
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_iisph_accel(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
               const float* __restrict__ rho, const float* __restrict__ pr, const int32_t* __restrict__ offs,
@@ -200,7 +200,7 @@ k_iisph_accel(int n, DevParams P, const float* __restrict__ x, const float* __re
     float rhoi = 1.f;
     if (g.valid) {
         rhoi = rho[g.i];
-        s = accel_partial<KF, D, G, ST, false>(g.i, g.lane, P, x, H, m, rho, pr, 0.f, pr[g.i] / (rhoi * rhoi), offs, cnt, list);
+        s = accel_partial<KF, D, G, false>(g.i, g.lane, P, x, H, m, rho, pr, 0.f, pr[g.i] / (rhoi * rhoi), offs, cnt, list);
     }
     #pragma unroll
     for (int a = 0; a < D; ++a) s.v[a] = gsum<G>(s.v[a]);
@@ -210,14 +210,14 @@ k_iisph_accel(int n, DevParams P, const float* __restrict__ x, const float* __re
     store_vec<D>(acc, g.i, s);
 }
 
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_iisph_shift(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
               const float* __restrict__ rho, const float* __restrict__ acc, const int32_t* __restrict__ offs,
               const int32_t* __restrict__ cnt, const int32_t* __restrict__ list, float* __restrict__ shift) {
     Grp<G> g(n);
     float s = 0.f;
-    if (g.valid) s = shift_partial<KF, D, G, ST, false>(g.i, g.lane, P, x, H, m, rho, acc, load_vec<D>(acc, g.i), offs, cnt, list);
+    if (g.valid) s = shift_partial<KF, D, G, false>(g.i, g.lane, P, x, H, m, rho, acc, load_vec<D>(acc, g.i), offs, cnt, list);
     s = gsum<G>(s);
     if (g.valid && g.lane == 0) shift[g.i] = -s;
 }
@@ -254,7 +254,7 @@ __device__ __forceinline__ unsigned int warp_max_u(unsigned int v) {
     return v;
 }
 
-template <int KF, int D, int ST>
+template <int KF, int D>
 __global__ void __launch_bounds__(JAC_BLOCK)
 k_jacobi(JacobiArgs a) {
     constexpr int G = JAC_G;
@@ -287,7 +287,7 @@ k_jacobi(JacobiArgs a) {
             if (valid) {
                 pi = __ldcg(a.praw + i) - mu;
                 rhoi = __ldg(a.rho + i);
-                s = accel_partial<KF, D, G, ST, true>(i, lane, a.P, a.x, a.H, a.m, a.rho, a.praw, mu, pi / (rhoi * rhoi),
+                s = accel_partial<KF, D, G, true>(i, lane, a.P, a.x, a.H, a.m, a.rho, a.praw, mu, pi / (rhoi * rhoi),
                                                       a.offs, a.cnt, a.list);
             }
             #pragma unroll
@@ -309,7 +309,7 @@ k_jacobi(JacobiArgs a) {
             const int i = (rd * (int)gridDim.x + (int)blockIdx.x) * JAC_PPB + (int)threadIdx.x / G;
             const bool valid = i < n;
             float s = 0.f;
-            if (valid) s = shift_partial<KF, D, G, ST, true>(i, lane, a.P, a.x, a.H, a.m, a.rho, a.acc, load_vec_cg<D>(a.acc, i),
+            if (valid) s = shift_partial<KF, D, G, true>(i, lane, a.P, a.x, a.H, a.m, a.rho, a.acc, load_vec_cg<D>(a.acc, i),
                                                              a.offs, a.cnt, a.list);
             s = gsum<G>(s);
             if (valid && lane == 0) {
@@ -384,7 +384,7 @@ static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 static int64_t dfsph_ws_bytes(int64_t n) { return (int64_t)(kCtlBytes + 3 * align256((size_t)n * sizeof(float))); }
 
-template <int KF, int D, int ST>
+template <int KF, int D>
 static int launch_jacobi(JacobiArgs& a, cudaStream_t s) {
     static std::mutex mu;
     static int cached_dev = -1, blocks_per_sm = 0, num_sms = 0;
@@ -399,7 +399,7 @@ static int launch_jacobi(JacobiArgs& a, cudaStream_t s) {
             if (e != cudaSuccess || !coop) return set_error(SPH_ERR_UNSUPPORTED, "jacobi: device %d has no cooperative launch", dev);
             e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
             if (e != cudaSuccess) return set_error(SPH_ERR_CUDA, "jacobi: SM count: %s", cudaGetErrorString(e));
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jacobi<KF, D, ST>, JAC_BLOCK, 0);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jacobi<KF, D>, JAC_BLOCK, 0);
             if (e != cudaSuccess || blocks_per_sm < 1) return set_error(SPH_ERR_CUDA, "jacobi: occupancy query failed");
             cached_dev = dev;
         }
@@ -408,7 +408,7 @@ static int launch_jacobi(JacobiArgs& a, cudaStream_t s) {
     const int grid = (int)std::min<int64_t>(need, (int64_t)blocks_per_sm * num_sms);
     void* args[] = {&a};
     count_launch();
-    e = cudaLaunchCooperativeKernel((const void*)k_jacobi<KF, D, ST>, dim3(grid), dim3(JAC_BLOCK), args, 0, s);
+    e = cudaLaunchCooperativeKernel((const void*)k_jacobi<KF, D>, dim3(grid), dim3(JAC_BLOCK), args, 0, s);
     if (e != cudaSuccess) return set_error(SPH_ERR_CUDA, "jacobi: cooperative launch: %s", cudaGetErrorString(e));
     return SPH_OK;
 }
@@ -444,7 +444,7 @@ static int dfsph_solve(int mode, const SphParams* p, const SphJacobiConfig* cfg,
     if (e != cudaSuccess) return set_error(SPH_ERR_CUDA, "jacobi: memset: %s", cudaGetErrorString(e));
     const float rho0 = (float)cfg->rest_density;
     count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_dfsph_prep<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
+    WSPH_DISPATCH_KDS(*p, (k_dfsph_prep<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
         (int)n, P, mode, rho0, x, H, m, rho, v, dvdt, dt, offs, cnt, list, nullptr, nullptr, p_init, cfg->init_mode, src, diag, praw)));
     if ((rc = check_launch("jacobi prep"))) return rc;
     JacobiArgs a;
@@ -455,13 +455,7 @@ static int dfsph_solve(int mode, const SphParams* p, const SphJacobiConfig* cfg,
     a.praw = praw; a.p_out = p_out; a.acc = accel_out; a.hist = history;
     a.iters_out = iterations; a.status_out = status; a.ctl = ctl;
     rc = SPH_ERR_UNSUPPORTED;
-    if (p->list_stride == 2) {
-        constexpr int ST = 2;
-        WSPH_DISPATCH_KD(P.kernel, P.dim, (rc = launch_jacobi<KF, D, ST>(a, s)));
-    } else {
-        constexpr int ST = 1;
-        WSPH_DISPATCH_KD(P.kernel, P.dim, (rc = launch_jacobi<KF, D, ST>(a, s)));
-    }
+    WSPH_DISPATCH_KD(P.kernel, P.dim, (rc = launch_jacobi<KF, D>(a, s)));
     return rc;
 }
 
@@ -492,7 +486,7 @@ __global__ void k_feature_sums(int n, const float* __restrict__ src, const float
 //   6  cnt_i / mean(cnt) - 1
 //   7  diag_i / mean(diag) - 1
 // with P = mean_i |p_jac_i| (written to scale_out[0]); a network output y maps to p = y P.
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_features(int n, DevParams P, float rho0, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
            const float* __restrict__ rho, const float* __restrict__ src, const float* __restrict__ diag,
@@ -509,7 +503,7 @@ k_features(int n, DevParams P, float rho0, const float* __restrict__ x, const fl
         const float Hi = H[i];
         const int b = offs[i], e = b + cnt[i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             const Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             const float w = __ldg(m + j) / __ldg(rho + j) * kernelW<KF, D>(safe_sqrt(dot<D>(xij, xij)), Hi);
             s0 += w;
@@ -549,7 +543,7 @@ int sph_dfsph_alpha(const SphParams* p, int64_t n, const float* x, const float* 
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     // v is only read for the divergence; x stands in as a valid vector array
     count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_dfsph_prep<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
+    WSPH_DISPATCH_KDS(*p, (k_dfsph_prep<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
         (int)n, P, -1, 0.f, x, H, m, rho, x, nullptr, nullptr, offs, cnt, list, nullptr, alpha_out, nullptr, 0, nullptr, nullptr, nullptr)));
     return check_launch("sph_dfsph_alpha");
 }
@@ -562,7 +556,7 @@ int sph_incompressible_divergence(const SphParams* p, int64_t n, double rest_den
     if (dvdt && !dt) return set_error(SPH_ERR_BAD_ARG, "sph_incompressible_divergence: dvdt given without dt");
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v")) || (rc = check_align_vec(P, dvdt, "dvdt"))) return rc;
     count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_dfsph_prep<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
+    WSPH_DISPATCH_KDS(*p, (k_dfsph_prep<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
         (int)n, P, -1, (float)rest_density, x, H, m, rho, v, dvdt, dt, offs, cnt, list, div_out, nullptr, nullptr, 0, nullptr, nullptr,
         nullptr)));
     return check_launch("sph_incompressible_divergence");
@@ -576,7 +570,7 @@ int sph_pressure_accel_iisph(const SphParams* p, int64_t n, const float* x, cons
     CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, accel_out, "accel_out"))) return rc;
     count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_iisph_accel<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
+    WSPH_DISPATCH_KDS(*p, (k_iisph_accel<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
         (int)n, P, x, H, m, rho, pressure, offs, cnt, list, accel_out)));
     return check_launch("sph_pressure_accel_iisph");
 }
@@ -589,7 +583,7 @@ int sph_pressure_shift_iisph(const SphParams* p, int64_t n, const float* x, cons
     CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, accel, "accel"))) return rc;
     count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_iisph_shift<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
+    WSPH_DISPATCH_KDS(*p, (k_iisph_shift<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
         (int)n, P, x, H, m, rho, accel, offs, cnt, list, shift_out)));
     return check_launch("sph_pressure_shift_iisph");
 }
@@ -616,14 +610,14 @@ int sph_dfsph_features(const SphParams* p, const SphJacobiConfig* cfg, int32_t m
     cudaError_t e = cudaMemsetAsync(sums3, 0, 3 * sizeof(double), s);
     if (e != cudaSuccess) return set_error(SPH_ERR_CUDA, "sph_dfsph_features: memset: %s", cudaGetErrorString(e));
     count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_dfsph_prep<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
+    WSPH_DISPATCH_KDS(*p, (k_dfsph_prep<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
         (int)n, P, mode, (float)cfg->rest_density, x, H, m, rho, v, dvdt, dt, offs, cnt, list, nullptr, nullptr, p_prev, 1, src, diag, p0)));
     int rb = grid_for(n, 256);
     if (rb > 148 * 4) rb = 148 * 4;
     count_launch();
     k_feature_sums<<<rb, 256, 0, s>>>((int)n, src, diag, cnt, sums3);
     count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_features<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
+    WSPH_DISPATCH_KDS(*p, (k_features<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>(
         (int)n, P, (float)cfg->rest_density, x, H, m, rho, src, diag, p_prev, offs, cnt, list, sums3, feats_out, scale_out)));
     return check_launch("sph_dfsph_features");
 }

@@ -252,18 +252,15 @@ __global__ void k_minmax(const float* __restrict__ a, int64_t n, float* out2) {
         float v = a[i];
         lo = fminf(lo, v); hi = fmaxf(hi, v);
     }
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    }
-    if ((threadIdx.x & 31) == 0) { atomic_min_float(out2, lo); atomic_max_float(out2 + 1, hi); }
+    lo = block_reduce(lo, __int_as_float(0x7f800000), OpMinF());
+    hi = block_reduce(hi, -__int_as_float(0x7f800000), OpMaxF());
+    if (threadIdx.x == 0) { atomic_min_float(out2, lo); atomic_max_float(out2 + 1, hi); }
 }
 
 int launch_minmax(int64_t n, const float* a, float* out2, cudaStream_t s) {
     wsph::count_launch(); k_minmax_init<<<1, 1, 0, s>>>(out2);
-    int blocks = (int)((n + 255) / 256);
-    if (blocks > 148 * 8) blocks = 148 * 8;
+    int blocks = (int)((n + 1023) / 1024);        // about four elements per thread
+    if (blocks > 148 * 4) blocks = 148 * 4;
     if (blocks < 1) blocks = 1;
     wsph::count_launch(); k_minmax<<<blocks, 256, 0, s>>>(a, n, out2);
     return check_launch("sph_minmax");
@@ -316,9 +313,8 @@ __global__ void k_hmax(const float* __restrict__ H, int64_t n, float* out, int32
         float h = H[i];
         if (!(h > 0.f) || isinf(h)) bad = true; else hi = fmaxf(hi, h);
     }
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int*>(out), __float_as_int(hi));
+    hi = block_reduce(hi, 0.f, OpMaxF());
+    if (threadIdx.x == 0) atomicMax(reinterpret_cast<int*>(out), __float_as_int(hi));
     if (bad) atomicOr(status, SPH_STATUS_NONFINITE);
 }
 
@@ -465,37 +461,44 @@ __device__ __forceinline__ int stencil_keys(const int* c, const GridDev& g, cons
 // owning sorted position start+l.  All lanes share the cell and hence the 3^d stencil
 // and every loop bound (no divergence).  Candidate records of each stencil cell are
 // staged through shared memory 32 at a time (one coalesced load, broadcast reads).
-// A Verlet entry needs r^2 < (verlet_scale*max(H_i,H_j))^2.  The fill pass also
-// marks the interacting subset used by the pair kernels -- fl(sqrt(r^2))/max(H_i,H_j)
-// < 1, exactly when some support scheme gives W != 0 (band test on r^2, exact
-// evaluation only inside the band) -- storing it inside the row's own Verlet range.
-// Rows are staged in shared memory (VS entries per lane) and flushed by the warp
-// cooperatively (VS lanes per row segment), so they are written with contiguous
-// stores.  Row order: stencil cells in offset order, candidates by sorted position.
+// A Verlet entry needs r^2 < (verlet_scale*max(H_i,H_j))^2.
+//
+// Row layout (when interacting counts are requested): the interacting entries --
+// fl(sqrt(r^2))/max(H_i,H_j) < 1, exactly the pairs some support scheme gives W != 0 --
+// come first, then the rest of the Verlet entries, each part in walk order (stencil
+// cells in offset order, candidates by sorted position).  The pair passes walk only
+// the prefix [offset, offset + interacting count): plain int32 indices, and pairwise
+// outputs written contiguously at their Verlet entry.  The count pass counts both
+// parts, so the fill pass knows where each row's tail starts.  Rows are staged in
+// shared memory (VS entries per lane and part) and flushed by the warp cooperatively,
+// so they are written with contiguous stores.
 constexpr int VW_WARPS = 4;
 constexpr int VW_BLOCK = 32 * VW_WARPS;
 constexpr int VS = 16;
 
-__device__ __forceinline__ void verlet_flush(int lane, int wib, int& nb, int& nib, int& written, int& iwritten, int row,
-                                             int32_t (*sbuf)[32][VS], int2 (*sibuf)[32][VS],
-                                             int32_t* __restrict__ list, int2* __restrict__ ilist, bool want_inter) {
-    __syncwarp();
+// fl(sqrt(r2)) / Hm < 1, with the square root only inside a narrow band around r = Hm
+// (outside it the comparison of r2 with Hm^2 decides the same way).
+__device__ __forceinline__ bool interacting_pair(float r2, float Hm) {
+    const float h2 = Hm * Hm;
+    if (r2 < 0.9998f * h2) return true;
+    if (!(r2 < 1.0002f * h2)) return false;
+    return __fdiv_rn(sqrtf(r2), Hm) < 1.f;
+}
+
+// Writes every lane's staged entries of one part: lanes pair up per owner row (16
+// entries per half warp), base_o + e for the owner's base.
+__device__ __forceinline__ void verlet_flush_part(int lane, int wib, int& nb, int& written, int base,
+                                                  int32_t (*buf)[32][VS], int32_t* __restrict__ list) {
     const int half = lane >> 4, e = lane & 15;
     #pragma unroll 4
     for (int r = 0; r < 32; r += 2) {
         const int owner = r + half;
         const int n_o = __shfl_sync(0xffffffffu, nb, owner);
-        const int b_o = __shfl_sync(0xffffffffu, row + written, owner);
-        if (e < n_o) list[b_o + e] = sbuf[wib][owner][e];
-        if (want_inter) {
-            const int ni_o = __shfl_sync(0xffffffffu, nib, owner);
-            const int ib_o = __shfl_sync(0xffffffffu, row + iwritten, owner);
-            if (e < ni_o) ilist[ib_o + e] = sibuf[wib][owner][e];
-        }
+        const int b_o = __shfl_sync(0xffffffffu, base + written, owner);
+        if (e < n_o) list[b_o + e] = buf[wib][owner][e];
     }
-    __syncwarp();
-    written += nb; iwritten += nib;
-    nb = 0; nib = 0;
+    written += nb;
+    nb = 0;
 }
 
 template <int D, bool FILL>
@@ -503,14 +506,13 @@ __global__ void __launch_bounds__(VW_BLOCK)
 k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_keys, const int32_t* __restrict__ tasks,
          const int32_t* __restrict__ ntasks, const GridDev* __restrict__ gp, DevParams P,
          const int32_t* __restrict__ sort_index, const int32_t* __restrict__ cell_begin, const int32_t* __restrict__ cell_end,
-         int32_t* __restrict__ counts, const int32_t* __restrict__ offsets, int32_t* __restrict__ ioffsets,
-         int32_t* __restrict__ icounts, int32_t* __restrict__ list, int2* __restrict__ ilist, long long* __restrict__ innz,
-         const long long* __restrict__ nnz, long long capacity) {
+         int32_t* __restrict__ counts, int32_t* __restrict__ icounts, const int32_t* __restrict__ offsets,
+         int32_t* __restrict__ list, long long* __restrict__ innz, const long long* __restrict__ nnz, long long capacity) {
     __shared__ float4 srec[VW_WARPS][32];
     __shared__ int32_t sidx[FILL ? VW_WARPS : 1][32];
-    __shared__ int32_t sbuf[FILL ? VW_WARPS : 1][32][VS];
-    __shared__ int2 sibuf[FILL ? VW_WARPS : 1][32][VS];
-    const bool want_inter = FILL && ilist != nullptr;
+    __shared__ int32_t sbuf[FILL ? VW_WARPS : 1][32][VS];     // rest of the row
+    __shared__ int32_t sibuf[FILL ? VW_WARPS : 1][32][VS];    // interacting prefix
+    const bool part = icounts != nullptr;
     if (FILL && *nnz > capacity) return;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -519,6 +521,7 @@ k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_ke
     const GridDev g = *gp;
     const DomainF dom = P.dom;
     const float vs = P.verlet_scale;
+    long long itotal = 0;
     for (int task = warp; task < nt; task += nwarps) {
         const int start = tasks[task];
         const uint32_t ckey = sorted_keys[start];
@@ -535,9 +538,12 @@ k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_ke
         const int nk = stencil_keys<D>(c, g, dom, keys, shifts);
         const bool min_image = grid_needs_min_image<D>(g, dom);     // uniform over the grid
         const int i = active ? sort_index[t] : 0;
-        int cnt = 0;
-        int row = 0, nb = 0, nib = 0, written = 0, iwritten = 0;
-        if (FILL && active) row = offsets[i];
+        int cnt = 0, icnt = 0;
+        int row = 0, tail = 0, nb = 0, nib = 0, written = 0, iwritten = 0;
+        if (FILL && active) {
+            row = offsets[i];
+            tail = row + (part ? icounts[i] : 0);
+        }
         for (int q = 0; q < nk; ++q) {
             const int b = cell_begin[keys[q]], e = cell_end[keys[q]];
             float sh[3] = {shifts[3 * q], shifts[3 * q + 1], shifts[3 * q + 2]};
@@ -550,9 +556,13 @@ k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_ke
                 __syncwarp();
                 const int mcount = min(32, e - k0);
                 for (int u0 = 0; u0 < mcount; u0 += 8) {
-                    // room for the next 8 candidates in every lane's buffer
-                    if (FILL && __any_sync(0xffffffffu, nb > VS - 8))
-                        verlet_flush(lane, wib, nb, nib, written, iwritten, row, sbuf, sibuf, list, ilist, want_inter);
+                    // room for the next 8 candidates in every lane's buffers
+                    if (FILL && __any_sync(0xffffffffu, nb > VS - 8 || nib > VS - 8)) {
+                        __syncwarp();
+                        verlet_flush_part(lane, wib, nib, iwritten, row, sibuf, list);
+                        verlet_flush_part(lane, wib, nb, written, tail, sbuf, list);
+                        __syncwarp();
+                    }
                     #pragma unroll
                     for (int du = 0; du < 8; ++du) {
                         const int u = u0 + du;
@@ -576,41 +586,38 @@ k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_ke
                         }
                         const float r2 = dist2_rn<D>(dv);
                         const bool hit = active & (u < mcount) & (r2 < __fmul_rn(R, R));
+                        const bool inter = part && hit && interacting_pair(r2, Hm);
                         if (FILL) {
-                            bool inter = false;
-                            if (want_inter) {
-                                const float h2 = Hm * Hm;
-                                inter = hit & (r2 < 0.9998f * h2);
-                                const bool band = hit & !inter & (r2 < 1.0002f * h2);
-                                if (__any_sync(0xffffffffu, band)) {     // rare: exact test near r = H
-                                    if (band) inter = __fdiv_rn(sqrtf(r2), Hm) < 1.f;
-                                }
-                            }
                             if (hit) {
                                 const int j = sidx[wib][u];
-                                if (inter) sibuf[wib][lane][nib++] = make_int2(j, row + written + nb);
-                                sbuf[wib][lane][nb++] = j;
+                                if (inter) sibuf[wib][lane][nib++] = j;
+                                else sbuf[wib][lane][nb++] = j;
                             }
                         } else {
                             cnt += hit;
+                            icnt += inter;
                         }
                     }
                 }
             }
         }
         if (FILL) {
-            if (__any_sync(0xffffffffu, nb > 0 || nib > 0))
-                verlet_flush(lane, wib, nb, nib, written, iwritten, row, sbuf, sibuf, list, ilist, want_inter);
-            if (want_inter) {
-                if (active) { ioffsets[i] = row; icounts[i] = iwritten; }
-                int tot = active ? iwritten : 0;
-                #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-                if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long*>(innz), (unsigned long long)tot);
+            if (__any_sync(0xffffffffu, nb > 0 || nib > 0)) {
+                __syncwarp();
+                verlet_flush_part(lane, wib, nib, iwritten, row, sibuf, list);
+                verlet_flush_part(lane, wib, nb, written, tail, sbuf, list);
+                __syncwarp();
             }
         } else if (active) {
             counts[i] = cnt;
+            if (part) icounts[i] = icnt;
+            itotal += icnt;
         }
+    }
+    if (!FILL && part) {
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) itotal += __shfl_xor_sync(0xffffffffu, itotal, o);
+        if (lane == 0 && itotal) atomicAdd(reinterpret_cast<unsigned long long*>(innz), (unsigned long long)itotal);
     }
 }
 
@@ -702,13 +709,10 @@ __global__ void k_refresh_check(const float* __restrict__ x, const float* __rest
         hmax = h0 > hmax ? h0 : hmax;
     }
     unsigned int e0 = ord_enc(dmax), e1 = ord_enc(amax), e2 = ord_enc(hmax);
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        e0 = max(e0, __shfl_xor_sync(0xffffffffu, e0, o));
-        e1 = max(e1, __shfl_xor_sync(0xffffffffu, e1, o));
-        e2 = max(e2, __shfl_xor_sync(0xffffffffu, e2, o));
-    }
-    if ((threadIdx.x & 31) == 0) { atomicMax(acc3 + 0, e0); atomicMax(acc3 + 1, e1); atomicMax(acc3 + 2, e2); }
+    e0 = block_reduce(e0, 0u, OpMaxU());
+    e1 = block_reduce(e1, 0u, OpMaxU());
+    e2 = block_reduce(e2, 0u, OpMaxU());
+    if (threadIdx.x == 0) { atomicMax(acc3 + 0, e0); atomicMax(acc3 + 1, e1); atomicMax(acc3 + 2, e2); }
 }
 
 __device__ __forceinline__ bool refresh_valid(const unsigned int* acc3) {
@@ -716,15 +720,17 @@ __device__ __forceinline__ bool refresh_valid(const unsigned int* acc3) {
     return amax + 2.0002f * dmax + 1e-5f * hmax <= 0.f;   // false for NaN
 }
 
-// Eight lanes per row, four rows per warp: the interacting entries
-// (fl(sqrt(r^2)) / max(H_i, H_j) < 1, the test the list builder applies) of the row's
-// Verlet range, compacted in Verlet order as (j, entry) with a ballot per 8-entry chunk.
+// Eight lanes per row, four rows per warp: the kept Verlet row rewritten into list_out
+// with the interacting entries (fl(sqrt(r^2)) / max(H_i, H_j) < 1 at the new positions,
+// the test the list builder applies) first, in the kept order, and the rest after them
+// in reverse kept order (filled from the row's end, so one pass suffices); a ballot
+// per 8-entry chunk compacts both parts.
 constexpr int RF_G = 8;
 template <int D>
 __global__ void k_refilter(const float* __restrict__ x, const float* __restrict__ H, int n, DevParams P,
                            const unsigned int* __restrict__ acc3, const int32_t* __restrict__ offs,
                            const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
-                           int32_t* __restrict__ ioffs, int32_t* __restrict__ icnt, int2* __restrict__ ilist,
+                           int32_t* __restrict__ list_out, int32_t* __restrict__ icnt,
                            unsigned long long* __restrict__ innz, int32_t* __restrict__ status) {
     if (!refresh_valid(acc3)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, SPH_STATUS_LIST_STALE);
@@ -733,6 +739,7 @@ __global__ void k_refilter(const float* __restrict__ x, const float* __restrict_
     const int lane = threadIdx.x & 31;
     const int sub = lane & (RF_G - 1);
     const int gshift = lane & ~(RF_G - 1);                 // first lane of this row's group
+    const unsigned int below = (1u << sub) - 1u;
     const int64_t ii = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / RF_G;
     const bool valid = ii < n;
     const int i = valid ? (int)ii : 0;
@@ -740,23 +747,26 @@ __global__ void k_refilter(const float* __restrict__ x, const float* __restrict_
     float Hi = 1.f;
     int b = 0, c = 0;
     if (valid) { xi = load_vec<D>(x, i); Hi = H[i]; b = offs[i]; c = cnt[i]; }
-    int w = 0;
+    int w = 0, rw = 0;
     for (int base = 0; __any_sync(0xffffffffu, base < c); base += RF_G) {
-        const int k = b + base + sub;
+        const bool in_row = base + sub < c;
         bool keep = false;
         int j = 0;
-        if (base + sub < c) {
-            j = list[k];
+        if (in_row) {
+            j = list[b + base + sub];
             const Vec<D> d = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             const float Hm = fmaxf(Hi, __ldg(H + j));
             keep = __fdiv_rn(sqrtf(dist2_rn<D>(d)), Hm) < 1.f;
         }
-        const unsigned int bits = (__ballot_sync(0xffffffffu, keep) >> gshift) & ((1u << RF_G) - 1u);
-        if (keep) ilist[b + w + __popc(bits & ((1u << sub) - 1u))] = make_int2(j, k);
-        w += __popc(bits);
+        const unsigned int kb = (__ballot_sync(0xffffffffu, keep) >> gshift) & ((1u << RF_G) - 1u);
+        const unsigned int rb = (__ballot_sync(0xffffffffu, in_row && !keep) >> gshift) & ((1u << RF_G) - 1u);
+        if (keep) list_out[b + w + __popc(kb & below)] = j;
+        else if (in_row) list_out[b + c - 1 - (rw + __popc(rb & below))] = j;
+        w += __popc(kb);
+        rw += __popc(rb);
     }
     unsigned long long t = (valid && sub == 0) ? (unsigned long long)w : 0ull;
-    if (valid && sub == 0) { ioffs[i] = b; icnt[i] = w; }
+    if (valid && sub == 0) icnt[i] = w;
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
     if (lane == 0 && t) atomicAdd(innz, t);
@@ -801,8 +811,7 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
                         int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
                         int32_t* neighbor_offsets, int32_t* num_neighbors,
                         int32_t* neighbor_list, int64_t list_capacity, int64_t* nnz_out,
-                        int32_t* inter_offsets, int32_t* inter_counts, int32_t* inter_list,
-                        int64_t inter_capacity, int64_t* inter_nnz_out,
+                        int32_t* inter_counts, int64_t* inter_nnz_out,
                         int32_t* status, void* stream) {
     DevParams P;
     int rc = params_to_dev(p, &P);
@@ -810,32 +819,28 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
     if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_build: n out of range");
     if (cell_capacity < 1) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_build: cell_capacity < 1");
     WSPH_CHECK_PTR(nnz_out); WSPH_CHECK_PTR(status); WSPH_CHECK_PTR(grid_out);
-    const bool inter = inter_list != nullptr || inter_counts != nullptr;
-    if (inter) { WSPH_CHECK_PTR(inter_offsets); WSPH_CHECK_PTR(inter_counts); WSPH_CHECK_PTR(inter_nnz_out); }
+    const bool part = inter_counts != nullptr;
+    if (part) WSPH_CHECK_PTR(inter_nnz_out);
     cudaStream_t s = WSPH_STREAM(stream);
     if (n == 0) {
         cudaMemsetAsync(nnz_out, 0, sizeof(int64_t), s);
-        if (inter) cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
+        if (part) cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
         return check_launch("sph_neighbors_build");
     }
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(workspace); WSPH_CHECK_PTR(sort_index);
     WSPH_CHECK_PTR(sorted_keys); WSPH_CHECK_PTR(cell_begin); WSPH_CHECK_PTR(cell_end);
     WSPH_CHECK_PTR(neighbor_offsets); WSPH_CHECK_PTR(num_neighbors);
     if (list_capacity > 0) WSPH_CHECK_PTR(neighbor_list);
-    if (inter && inter_capacity > 0) WSPH_CHECK_PTR(inter_list);
     if (P.dim == 2 && (reinterpret_cast<uintptr_t>(x) & 7)) return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
-    if (inter && (reinterpret_cast<uintptr_t>(inter_list) & 7)) return set_error(SPH_ERR_BAD_ARG, "inter_list must be 8-byte aligned");
-    if (inter && inter_capacity < list_capacity)
-        return set_error(SPH_ERR_BAD_ARG, "inter_capacity (%lld pairs) must be >= list_capacity (%lld)", (long long)inter_capacity, (long long)list_capacity);
     NbWs w = carve(reinterpret_cast<char*>(workspace), n, cell_capacity);
     if (workspace_bytes < w.bytes) return set_error(SPH_ERR_WORKSPACE, "neighbour workspace too small: %lld < %lld", (long long)workspace_bytes, (long long)w.bytes);
     int mb = max_bits_for(P.dim, cell_capacity);
     int64_t ncells = (int64_t)1 << (mb * P.dim);
-    long long* innz = inter ? reinterpret_cast<long long*>(inter_nnz_out) : nullptr;
+    long long* innz = part ? reinterpret_cast<long long*>(inter_nnz_out) : nullptr;
 
     cudaMemsetAsync(w.hmax, 0, sizeof(float), s);
-    int rblocks = grid_for(n, 256);
-    if (rblocks > 148 * 8) rblocks = 148 * 8;
+    int rblocks = (int)((n + 1023) / 1024);
+    if (rblocks > 148 * 4) rblocks = 148 * 4;
     wsph::count_launch(); k_hmax<<<rblocks, 256, 0, s>>>(H, n, w.hmax, status);
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, k_grid<D><<<1, 1, 0, s>>>(w.hmax, P, mb, w.grid, grid_out));
     cudaMemsetAsync(w.counts, 0, ncells * sizeof(int32_t), s);
@@ -848,30 +853,29 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
                                                                                                  sort_index, sorted_keys, w.recs, w.tasks, w.ntasks)));
     int vblocks = grid_for(n, VW_BLOCK);          // >= one warp per 32 particles; warps stride over the work items
     if (vblocks > 148 * 32) vblocks = 148 * 32;
+    if (part) cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, false><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
-                                                                                 cell_begin, cell_end, num_neighbors, nullptr, nullptr, nullptr,
-                                                                                 nullptr, nullptr, nullptr, nullptr, 0)));
+                                                                                 cell_begin, cell_end, num_neighbors, inter_counts, nullptr,
+                                                                                 nullptr, innz, nullptr, 0)));
     exclusive_scan_i32(num_neighbors, neighbor_offsets, n, w.scan, reinterpret_cast<long long*>(nnz_out), s);
     wsph::count_launch(); k_check_capacity<<<1, 1, 0, s>>>(reinterpret_cast<long long*>(nnz_out), list_capacity, status);
-    if (inter) cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, true><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
-                                                                                cell_begin, cell_end, nullptr, neighbor_offsets,
-                                                                                inter ? inter_offsets : nullptr, inter ? inter_counts : nullptr,
-                                                                                neighbor_list, inter ? reinterpret_cast<int2*>(inter_list) : nullptr,
-                                                                                innz, reinterpret_cast<long long*>(nnz_out), list_capacity)));
+                                                                                cell_begin, cell_end, nullptr, inter_counts, neighbor_offsets,
+                                                                                neighbor_list, nullptr, reinterpret_cast<long long*>(nnz_out),
+                                                                                list_capacity)));
     return check_launch("sph_neighbors_build");
 }
 
 int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const float* H, const float* x0, const float* H0,
                           const int32_t* neighbor_offsets, const int32_t* num_neighbors, const int32_t* neighbor_list,
-                          int32_t* inter_offsets, int32_t* inter_counts, int32_t* inter_list, uint32_t* scratch,
+                          int32_t* list_out, int32_t* inter_counts, uint32_t* scratch,
                           int64_t* inter_nnz_out, int32_t* status, void* stream) {
     DevParams P;
     int rc = params_to_dev(p, &P);
     if (rc) return rc;
     if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_refresh: n out of range");
     WSPH_CHECK_PTR(scratch); WSPH_CHECK_PTR(status);
-    const bool filter = inter_list != nullptr;
+    const bool filter = list_out != nullptr;
     cudaStream_t s = WSPH_STREAM(stream);
     if (filter) {
         WSPH_CHECK_PTR(inter_nnz_out);
@@ -881,23 +885,22 @@ int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const f
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(x0); WSPH_CHECK_PTR(H0);
     if (filter) {
         WSPH_CHECK_PTR(neighbor_offsets); WSPH_CHECK_PTR(num_neighbors); WSPH_CHECK_PTR(neighbor_list);
-        WSPH_CHECK_PTR(inter_offsets); WSPH_CHECK_PTR(inter_counts);
-        if (reinterpret_cast<uintptr_t>(inter_list) & 7) return set_error(SPH_ERR_BAD_ARG, "inter_list must be 8-byte aligned");
+        WSPH_CHECK_PTR(inter_counts);
+        if (list_out == neighbor_list) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_refresh: list_out must not alias neighbor_list");
     }
     if (P.dim == 2 && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(x0)) & 7))
         return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
     cudaMemsetAsync(scratch, 0, 3 * sizeof(uint32_t), s);
-    int cblocks = grid_for(n, 256);
-    if (cblocks > 148 * 8) cblocks = 148 * 8;
+    int cblocks = (int)((n + 1023) / 1024);
+    if (cblocks > 148 * 4) cblocks = 148 * 4;
     wsph::count_launch();
     WSPH_DISPATCH_DIM(P.dim, (k_refresh_check<D><<<cblocks, 256, 0, s>>>(x, H, x0, H0, (int)n, P, scratch)));
-    // without list buffers only the verdict is written (no rows are filtered)
+    // without an output list only the verdict is written (no rows are rewritten)
     const int64_t rows = filter ? n : 0;
     const int64_t rblocks = filter ? (n * RF_G + 255) / 256 : 1;   // RF_G lanes per row, 256 threads per block
     wsph::count_launch();
     WSPH_DISPATCH_DIM(P.dim, (k_refilter<D><<<(int)rblocks, 256, 0, s>>>(x, H, (int)rows, P, scratch, neighbor_offsets, num_neighbors,
-                                                                        neighbor_list, inter_offsets, inter_counts,
-                                                                        reinterpret_cast<int2*>(inter_list),
+                                                                        neighbor_list, list_out, inter_counts,
                                                                         reinterpret_cast<unsigned long long*>(inter_nnz_out), status)));
     return check_launch("sph_neighbors_refresh");
 }

@@ -1,5 +1,5 @@
 // Shared pieces of the pair passes: G lanes of a warp per particle, row-entry
-// decoding for the Verlet (stride 1) and interacting (stride 2) lists, kernel
+// decoding (Verlet rows or their interacting prefixes), kernel
 // evaluation with a precomputed 1/H, group reductions, and the host-side argument
 // checks and template dispatch of the pair entry points.
 #pragma once
@@ -31,13 +31,10 @@ template <int G> __device__ __forceinline__ float gmaxw(float v) {
     for (int o = G / 2; o > 0; o >>= 1) v = wmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
-template <int ST> __device__ __forceinline__ void entry(const int32_t* __restrict__ list, int q, int& j, int& k) {
-    if constexpr (ST == 2) {
-        int2 e = __ldg(reinterpret_cast<const int2*>(list) + q);
-        j = e.x; k = e.y;
-    } else {
-        j = __ldg(list + q); k = q;
-    }
+// Row entry q: neighbour j and the Verlet entry index k that pairwise arrays use (the
+// rows a pass walks are Verlet rows or their interacting prefixes, so k = q).
+__device__ __forceinline__ void entry(const int32_t* __restrict__ list, int q, int& j, int& k) {
+    j = __ldg(list + q); k = q;
 }
 template <int G> __host__ __forceinline__ int grid_g(int64_t n) { return (int)((n * G + PAIR_BLOCK - 1) / PAIR_BLOCK); }
 
@@ -76,25 +73,20 @@ struct KSum {
 #define G_HEAVY 8
 #define G_CRK 4
 
-#define WSPH_DISPATCH_KDS(params, ...)                                                    \
-    if ((params).list_stride == 2) { constexpr int ST = 2; WSPH_DISPATCH_KD(P.kernel, P.dim, __VA_ARGS__) } \
-    else { constexpr int ST = 1; WSPH_DISPATCH_KD(P.kernel, P.dim, __VA_ARGS__) }
-#define WSPH_DISPATCH_DS(params, ...)                                                     \
-    if ((params).list_stride == 2) { constexpr int ST = 2; WSPH_DISPATCH_DIM(P.dim, __VA_ARGS__) } \
-    else { constexpr int ST = 1; WSPH_DISPATCH_DIM(P.dim, __VA_ARGS__) }
+#define WSPH_DISPATCH_KDS(params, ...) WSPH_DISPATCH_KD(P.kernel, P.dim, __VA_ARGS__)
+#define WSPH_DISPATCH_DS(params, ...) WSPH_DISPATCH_DIM(P.dim, __VA_ARGS__)
 
 #define PAIR_PRELUDE()                                                        \
     DevParams P;                                                              \
     int rc = params_to_dev(p, &P);                                            \
     if (rc) return rc;                                                        \
     if (n < 0 || n > 0x3fffffff) return set_error(SPH_ERR_BAD_ARG, "%s: n out of range", __func__); \
-    if (p->list_stride < 0 || p->list_stride > 2) return set_error(SPH_ERR_BAD_ARG, "%s: list_stride must be 1 or 2", __func__); \
+    if (p->list_stride < 0 || p->list_stride > 1) return set_error(SPH_ERR_BAD_ARG, "%s: list_stride must be 1 (rows are Verlet rows or their interacting prefixes)", __func__); \
     if (n == 0) return SPH_OK;                                                \
     cudaStream_t s = WSPH_STREAM(stream);                                     \
     (void)s;
 
-#define CHECK_CSR() do { WSPH_CHECK_PTR(offs); WSPH_CHECK_PTR(cnt); WSPH_CHECK_PTR(list); \
-    if (p->list_stride == 2 && (reinterpret_cast<uintptr_t>(list) & 7)) return set_error(SPH_ERR_BAD_ARG, "%s: interacting list must be 8-byte aligned", __func__); } while (0)
+#define CHECK_CSR() do { WSPH_CHECK_PTR(offs); WSPH_CHECK_PTR(cnt); WSPH_CHECK_PTR(list); } while (0)
 
 inline int check_align_vec(const DevParams& P, const void* ptr, const char* name) {
     if (P.dim == 2 && ptr && (reinterpret_cast<uintptr_t>(ptr) & 7))

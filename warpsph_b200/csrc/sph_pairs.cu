@@ -3,11 +3,11 @@
 // Layout: G lanes of a warp cooperate on one particle i.  Lane l walks the entries
 // b+l, b+l+G, ... of i's neighbour row, so the G lanes read G consecutive entries
 // (coalesced index loads and pair-array stores), accumulate per-lane partial sums,
-// and reduce them with warp shuffles inside the group.  Rows are either the Verlet
-// list (stride 1, entry index = position in the list) or the interacting list
-// (stride 2, (j, Verlet entry index) pairs holding only r < max(H_i, H_j)), which
-// removes the beyond-support entries -- about half of a Verlet row -- from every
-// pass that only needs W != 0.
+// and reduce them with warp shuffles inside the group.  A row is either a whole Verlet
+// row or its interacting prefix (the list builder stores the entries with
+// r < max(H_i, H_j) first), which removes the beyond-support entries -- about half of
+// a Verlet row -- from every pass that only needs W != 0.  The entry index of a pair
+// is its position in the Verlet list in both cases.
 //
 // Arithmetic restates the reference (file:line at each kernel); divisions by the
 // same quantity are replaced by multiplications with a reciprocal, so results
@@ -20,7 +20,7 @@
 namespace wsph {
 
 // ---------------------------------------------------------------- density (modules/density/density.py:16-28)
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_density(int n, int mode, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
           const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
@@ -32,7 +32,7 @@ k_density(int n, int mode, DevParams P, const float* __restrict__ x, const float
         float Hi = H[g.i];
         int b = offs[g.i], e = b + cnt[g.i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             s += __ldg(m + j) * kernelW_mode<KF, D>(r, Hi, __ldg(H + j), mode);
@@ -52,7 +52,7 @@ template <int D> __device__ __forceinline__ float volume_to_support(float V, flo
 
 // One Newton iteration of modules/adaptiveSupport/optimalSupportMonaghan.py:87-125
 // with Omega of modules/adaptiveSupport/wp_omega.py:40-60 (gather support).
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_adaptive_h(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
              const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
@@ -64,7 +64,7 @@ k_adaptive_h(int n, DevParams P, const float* __restrict__ x, const float* __res
         Hi = H[g.i];
         int b = offs[g.i], e = b + cnt[g.i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W, dWdH;
@@ -94,7 +94,7 @@ k_adaptive_h(int n, DevParams P, const float* __restrict__ x, const float* __res
 }
 
 // ---------------------------------------------------------------- CRK volume (scatter support)
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_crk_volume(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H,
              const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
@@ -105,7 +105,7 @@ k_crk_volume(int n, DevParams P, const float* __restrict__ x, const float* __res
         Vec<D> xi = load_vec<D>(x, g.i);
         int b = offs[g.i], e = b + cnt[g.i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             s += kW_inv<KF, D>(r, 1.f / __ldg(H + j));
@@ -152,7 +152,7 @@ template <int D> __device__ __forceinline__ double inv_sym(const double (&a)[D][
 template <int D> struct CrkAcc {
     float m0, s0, m1[D], s1[D], dm0[D], m2[D][D], dm1[D][D], dm2[D][D][D];
 };
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_crk_factors(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
               const float* __restrict__ V, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
@@ -169,7 +169,7 @@ k_crk_factors(int n, DevParams P, const float* __restrict__ x, const float* __re
         Vec<D> xi = load_vec<D>(x, g.i);
         int b = offs[g.i], e = b + cnt[g.i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W; Vec<D> gW;
@@ -296,7 +296,7 @@ __global__ void k_eos(int n, float gamma, const float* __restrict__ u, const flo
 // ---------------------------------------------------------------- CRK velocity gradient (+ Cullen div, v_sig)
 // schemes/crkSPH.py:158-172 (difference form, scatter support, CRK kernel, .mT),
 // CullenDehnen2010.py:246-257 (super-symmetric divergence), wp_vsig.py:55-90.
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_grad_v(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
          const float* __restrict__ rho, const float* __restrict__ V, const float* __restrict__ A, const float* __restrict__ B,
@@ -316,7 +316,7 @@ k_grad_v(int n, DevParams P, const float* __restrict__ x, const float* __restric
         float ci = want_vs ? c[i] : 0.f;
         int b = offs[i], e = b + cnt[i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float Hj = __ldg(H + j);
@@ -376,7 +376,7 @@ k_grad_v(int n, DevParams P, const float* __restrict__ x, const float* __restric
 // R (CullenDehnen2010.py:121-164, gather interpolation of rho_j sgn(div_j) / rho_j * m_j),
 // v_sig over the Verlet set when not supplied (wp_vsig.py:55-90), Xi (:166-191) and the
 // alpha / alpha0 update (:281-314).
-template <int KF, int D, int G, int ST>
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
          const float* __restrict__ rho, const float* __restrict__ div, const float* __restrict__ div_prev,
@@ -397,7 +397,7 @@ k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restric
         float ci = want_vs ? c[i] : 0.f;
         int b = offs[i], e = b + cnt[i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W = kW_inv<KF, D>(r, invHi);   // gather support
@@ -492,20 +492,31 @@ __device__ __forceinline__ float van_leer(const Vec<D>& xij_, const Mat<D>& Gi, 
     return limiter_vl(wmin(ri, rj));
 }
 
+// Zero pairwise outputs of the entries [offs + cnt, offs + vcnt) of a row: the Verlet
+// entries after the interacting prefix, which carry no interaction (contiguous stores).
+template <int D, int G>
+__device__ __forceinline__ void zero_row_tail(int lane, int e, int te, float* __restrict__ ap, float* __restrict__ av) {
+    for (int q = e + lane; q < te; q += G) {
+        if (ap) store_vec<D>(ap, q, vzero<D>());
+        if (av) store_vec<D>(av, q, vzero<D>());
+    }
+}
+
 // modules/crk/accel.py:65-250 and modules/crk/dudt.py:62-229 in one pass.  The
 // unused computePi_actual calls of the reference (accel.py:143-168, dudt.py:128-153)
-// have no effect on the outputs and are not evaluated.  With the interacting list
-// (stride 2) the ap_ij / av_ij entries of non-interacting Verlet pairs are not
-// written (the caller provides zero-filled arrays).
-template <int KF, int D, int G, int ST>
+// have no effect on the outputs and are not evaluated.  dE/dt = m v.dv/dt + m du/dt
+// (schemes/crkSPH.py:330) is written per particle.  Walking the interacting prefix of
+// each Verlet row (cnt = interacting counts) with vcnt = the Verlet counts, the
+// ap_ij / av_ij entries of the rest of the row are written as zeros.
+template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
                  const float* __restrict__ rho, const float* __restrict__ V, const float* __restrict__ A,
                  const float* __restrict__ B, const float* __restrict__ gA, const float* __restrict__ gB,
                  const float* __restrict__ v, const float* __restrict__ c, const float* __restrict__ Pr,
                  const float* __restrict__ DvDx, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
-                 const int32_t* __restrict__ list, float* __restrict__ dvdt, float* __restrict__ dudt,
-                 float* __restrict__ ap, float* __restrict__ av) {
+                 const int32_t* __restrict__ list, const int32_t* __restrict__ vcnt, float* __restrict__ dvdt,
+                 float* __restrict__ dudt, float* __restrict__ dEdt, float* __restrict__ ap, float* __restrict__ av) {
     Grp<G> g(n);
     const bool comp = P.kahan != 0;
     KSum acc[D], du;
@@ -527,17 +538,15 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
         const float eps_i = 1.0e-7f * sm_i * sm_i;
         int b = offs[i], e = b + cnt[i];
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry<ST>(list, q, j, k);
+            int j, k; entry(list, q, j, k);
             Vec<D> xj = load_vec<D>(x, j);
             Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r2 = dot<D>(xij, xij);
             float Hj = __ldg(H + j);
             float Hm = wmax(Hi, Hj);
             if (!(r2 < Hm * Hm)) {
-                if (ST == 1) {
-                    if (ap) store_vec<D>(ap, k, vzero<D>());
-                    if (av) store_vec<D>(av, k, vzero<D>());
-                }
+                if (ap) store_vec<D>(ap, k, vzero<D>());
+                if (av) store_vec<D>(av, k, vzero<D>());
                 continue;
             }
             float r = safe_sqrt(r2);
@@ -610,19 +619,23 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
             // dudt.py:208-226
             du.add((Pj + 0.5f * Qd) * dotu * w, comp);
         }
+        if (vcnt && (ap || av)) zero_row_tail<D, G>(g.lane, e, b + __ldg(vcnt + i), ap, av);
     }
     float o[D], od;
     #pragma unroll
     for (int a = 0; a < D; ++a) o[a] = gsum<G>(acc[a].s) + gsum<G>(acc[a].c);
     od = gsum<G>(du.s) + gsum<G>(du.c);
     if (!g.valid || g.lane != 0) return;
-    if (dvdt) {
-        Vec<D> ov;
-        #pragma unroll
-        for (int a = 0; a < D; ++a) ov.v[a] = o[a];
-        store_vec<D>(dvdt, g.i, ov);
-    }
+    Vec<D> ov;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) ov.v[a] = o[a];
+    if (dvdt) store_vec<D>(dvdt, g.i, ov);
     if (dudt) dudt[g.i] = od;
+    if (dEdt) {
+        const Vec<D> vi = load_vec<D>(v, g.i);
+        const float mi = m[g.i];
+        dEdt[g.i] = mi * dot<D>(vi, ov) + mi * od;
+    }
 }
 
 // ---------------------------------------------------------------- energy partition f_ij (modules/compSPH/balance.py:62-154)
@@ -644,7 +657,7 @@ __global__ void k_balance_prep(int n, DevParams P, const float* __restrict__ rho
     sarr[i] = Pr[i] / powf(rho[i], P.gamma);
 }
 
-template <int D, int G, int ST>
+template <int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restrict__ rho, const float* __restrict__ Pr,
           const float* __restrict__ u, const float* __restrict__ vh, const float* __restrict__ sarr, const float* __restrict__ dtp,
@@ -659,7 +672,7 @@ k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restri
     const int scheme = P.energy_scheme;
     int b = offs[i], e = b + cnt[i];
     for (int q = b + g.lane; q < e; q += G) {
-        int j, k; entry<ST>(list, q, j, k);
+        int j, k; entry(list, q, j, k);
         Vec<D> vj = load_vec<D>(vh, j);
         Vec<D> apk = load_vec<D>(ap, k), avk = load_vec<D>(av, k);
         float dE = 0.f;
@@ -709,12 +722,9 @@ __global__ void k_cfl_reduce(int n, float gamma, const float* __restrict__ H, co
         hmin = fminf(hmin, H[i]);
         cmax = fmaxf(cmax, sqrtf(fabsf(u[i]) * gamma * (gamma - 1.f)));
     }
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        hmin = fminf(hmin, __shfl_xor_sync(0xffffffffu, hmin, o));
-        cmax = fmaxf(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
+    hmin = block_reduce(hmin, __int_as_float(0x7f800000), OpMinF());
+    cmax = block_reduce(cmax, 0.f, OpMaxF());
+    if (threadIdx.x == 0) {
         atomicMin(reinterpret_cast<int*>(red), __float_as_int(hmin));
         atomicMax(reinterpret_cast<int*>(red + 1), __float_as_int(cmax));
     }
@@ -776,7 +786,7 @@ __global__ void k_vhalf(int n, int ns, StagePtrs S, const float* __restrict__ dt
         vh[(size_t)i * D + a] = v0[(size_t)i * D + a] + 0.5f * fa * dt;
     }
 }
-template <int D, int G, int ST>
+template <int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_finalize(int n, int ns, StagePtrs S, int pdv, const float* __restrict__ dtp, const float* __restrict__ vh,
            const float* __restrict__ u0, float* __restrict__ u_out, float* __restrict__ du_out) {
@@ -793,7 +803,7 @@ k_finalize(int n, int ns, StagePtrs S, int pdv, const float* __restrict__ dtp, c
             int b = S.offs[s][g.i], e = b + S.cnt[s][g.i];
             float acc = 0.f;
             for (int q = b + g.lane; q < e; q += G) {
-                int j, k; entry<ST>(lst, q, j, k);
+                int j, k; entry(lst, q, j, k);
                 Vec<D> vj = load_vec<D>(vh, j);
                 Vec<D> a1 = load_vec<D>(ap, k), a2 = load_vec<D>(av, k);
                 float fk = __ldg(f + k);
@@ -882,7 +892,7 @@ int sph_density_gather(const SphParams* p, int64_t n, int32_t support_mode, cons
     if (support_mode < 0 || support_mode > 4) return set_error(SPH_ERR_BAD_ARG, "bad support mode %d", support_mode);
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_density<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, support_mode, P, x, H, m, offs, cnt, list, rho_out)));
+    WSPH_DISPATCH_KDS(*p, (k_density<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, support_mode, P, x, H, m, offs, cnt, list, rho_out)));
     return check_launch("sph_density_gather");
 }
 
@@ -894,7 +904,7 @@ int sph_adaptive_h_iter(const SphParams* p, int64_t n, int32_t support_mode, con
     if (support_mode != SPH_SUPPORT_GATHER) return set_error(SPH_ERR_UNSUPPORTED, "adaptive support: only the gather scheme is implemented");
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_adaptive_h<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, offs, cnt, list, hbounds, rho_out, H_out, ratio_out)));
+    WSPH_DISPATCH_KDS(*p, (k_adaptive_h<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, offs, cnt, list, hbounds, rho_out, H_out, ratio_out)));
     return check_launch("sph_adaptive_h_iter");
 }
 
@@ -904,7 +914,7 @@ int sph_crk_volume(const SphParams* p, int64_t n, const float* x, const float* H
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(V_out); CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_crk_volume<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, offs, cnt, list, V_out)));
+    WSPH_DISPATCH_KDS(*p, (k_crk_volume<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, offs, cnt, list, V_out)));
     return check_launch("sph_crk_volume");
 }
 
@@ -916,7 +926,7 @@ int sph_crk_factors(const SphParams* p, int64_t n, const float* x, const float* 
     WSPH_CHECK_PTR(A); WSPH_CHECK_PTR(B); WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_crk_factors<KF, D, G_CRK, ST><<<grid_g<G_CRK>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out)));
+    WSPH_DISPATCH_KDS(*p, (k_crk_factors<KF, D, G_CRK><<<grid_g<G_CRK>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out)));
     return check_launch("sph_crk_factors");
 }
 
@@ -941,7 +951,7 @@ int sph_grad_v(const SphParams* p, int64_t n, const float* x, const float* H, co
         (rc = check_align_vec(P, gradA, "gradA")))
         return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_grad_v<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
+    WSPH_DISPATCH_KDS(*p, (k_grad_v<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
                                                                                                   offs, cnt, list, DvDx_out, drhodt_out, div_out, vsig_out)));
     return check_launch("sph_grad_v");
 }
@@ -953,13 +963,10 @@ int sph_switch_cullen(const SphParams* p, int64_t n, const float* x, const float
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(div); WSPH_CHECK_PTR(div_prev);
     WSPH_CHECK_PTR(alpha0_prev); WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(alpha_out); CHECK_CSR();
-    if (!vsig) {
-        WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(c);
-        if (p->list_stride == 2) return set_error(SPH_ERR_BAD_ARG, "sph_switch_cullen: computing v_sig needs the Verlet list (stride 1)");
-    }
+    if (!vsig) { WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(c); }   // v_sig needs the whole Verlet rows
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_cullen<KF, D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div, div_prev, vsig, v, c,
+    WSPH_DISPATCH_KDS(*p, (k_cullen<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div, div_prev, vsig, v, c,
                                                                                                   alpha0_prev, dt, offs, cnt, list, alpha_out, R_out, vsig_out)));
     return check_launch("sph_switch_cullen");
 }
@@ -974,8 +981,8 @@ int sph_switch_balsara(const SphParams* p, int64_t n, const float* DvDx, const f
 int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
                        const float* V, const float* A, const float* B, const float* gradA, const float* gradB,
                        const float* v, const float* c, const float* Pr, const float* DvDx, const int32_t* offs,
-                       const int32_t* cnt, const int32_t* list, float* dvdt_out, float* dudt_out, float* ap_ij,
-                       float* av_ij, void* stream) {
+                       const int32_t* cnt, const int32_t* list, const int32_t* verlet_cnt, float* dvdt_out, float* dudt_out,
+                       float* dEdt_out, float* ap_ij, float* av_ij, void* stream) {
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(V); WSPH_CHECK_PTR(A);
     WSPH_CHECK_PTR(B); WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(c); WSPH_CHECK_PTR(Pr);
@@ -985,25 +992,26 @@ int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const floa
         (rc = check_align_vec(P, ap_ij, "ap_ij")) || (rc = check_align_vec(P, av_ij, "av_ij")))
         return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_crk_accel_dudt<KF, D, G_HEAVY, ST><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
-                                                                                                          Pr, DvDx, offs, cnt, list, dvdt_out, dudt_out, ap_ij, av_ij)));
+    WSPH_DISPATCH_KDS(*p, (k_crk_accel_dudt<KF, D, G_HEAVY><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
+                                                                                                          Pr, DvDx, offs, cnt, list, verlet_cnt, dvdt_out,
+                                                                                                          dudt_out, dEdt_out, ap_ij, av_ij)));
     return check_launch("sph_crk_accel_dudt");
 }
 
 int sph_crk_accel(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
                   const float* V, const float* A, const float* B, const float* gradA, const float* gradB, const float* v,
                   const float* c, const float* P, const float* DvDx, const int32_t* offs, const int32_t* cnt,
-                  const int32_t* list, float* dvdt_out, float* ap_ij, float* av_ij, void* stream) {
-    return sph_crk_accel_dudt(p, n, x, H, m, rho, V, A, B, gradA, gradB, v, c, P, DvDx, offs, cnt, list, dvdt_out, nullptr,
-                              ap_ij, av_ij, stream);
+                  const int32_t* list, const int32_t* verlet_cnt, float* dvdt_out, float* ap_ij, float* av_ij, void* stream) {
+    return sph_crk_accel_dudt(p, n, x, H, m, rho, V, A, B, gradA, gradB, v, c, P, DvDx, offs, cnt, list, verlet_cnt, dvdt_out,
+                              nullptr, nullptr, ap_ij, av_ij, stream);
 }
 
 int sph_crk_dudt(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
                  const float* V, const float* A, const float* B, const float* gradA, const float* gradB, const float* v,
                  const float* c, const float* P, const float* DvDx, const int32_t* offs, const int32_t* cnt,
                  const int32_t* list, float* dudt_out, void* stream) {
-    return sph_crk_accel_dudt(p, n, x, H, m, rho, V, A, B, gradA, gradB, v, c, P, DvDx, offs, cnt, list, nullptr, dudt_out,
-                              nullptr, nullptr, stream);
+    return sph_crk_accel_dudt(p, n, x, H, m, rho, V, A, B, gradA, gradB, v, c, P, DvDx, offs, cnt, list, nullptr, nullptr, dudt_out,
+                              nullptr, nullptr, nullptr, stream);
 }
 
 int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const float* rho, const float* Pr, const float* u,
@@ -1021,7 +1029,7 @@ int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const flo
     float* sarr = scratch + n * P.dim;
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_balance_prep<D><<<grid_for(n, 256), 256, 0, s>>>((int)n, P, rho, Pr, v, dvdt, dt, vh, sarr)));
     wsph::count_launch();
-    WSPH_DISPATCH_DS(*p, (k_balance<D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, m, rho, Pr, u, vh, sarr, dt, offs, cnt, list, ap_ij, av_ij, f_ij_out)));
+    WSPH_DISPATCH_DS(*p, (k_balance<D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, m, rho, Pr, u, vh, sarr, dt, offs, cnt, list, ap_ij, av_ij, f_ij_out)));
     return check_launch("sph_compsph_balance");
 }
 
@@ -1059,7 +1067,7 @@ int sph_cfl_dt(const SphParams* p, int64_t n, const float* H, const float* u, co
     cudaStream_t s = WSPH_STREAM(stream);
     float* red = dt_out + 1;
     wsph::count_launch(); k_cfl_init<<<1, 1, 0, s>>>(red);
-    int blocks = grid_for(n, 256);
+    int blocks = (int)((n + 1023) / 1024);
     if (blocks > 148 * 4) blocks = 148 * 4;
     wsph::count_launch(); k_cfl_reduce<<<blocks, 256, 0, s>>>((int)n, P.gamma, H, u, red);
     wsph::count_launch(); k_cfl_final<<<1, 1, 0, s>>>(P, red, dt_prev, dt_out);
@@ -1099,8 +1107,6 @@ int sph_finalize_compatible_energy(const SphParams* p, int64_t n, int32_t nstage
     for (int q = 0; q < nstages; ++q) {
         if (!dvdt_s[q] || !offs_s[q] || !cnt_s[q] || !list_s[q] || !f_ij_s[q] || !ap_ij_s[q] || !av_ij_s[q])
             return set_error(SPH_ERR_BAD_ARG, "finalize: null array for stage %d", q);
-        if (p->list_stride == 2 && (reinterpret_cast<uintptr_t>(list_s[q]) & 7))
-            return set_error(SPH_ERR_BAD_ARG, "finalize: interacting list of stage %d must be 8-byte aligned", q);
         S.dvdt[q] = dvdt_s[q]; S.offs[q] = offs_s[q]; S.cnt[q] = cnt_s[q]; S.list[q] = list_s[q];
         S.f[q] = f_ij_s[q]; S.ap[q] = ap_ij_s[q]; S.av[q] = av_ij_s[q]; S.w[q] = (float)weights[q];
     }
@@ -1109,7 +1115,7 @@ int sph_finalize_compatible_energy(const SphParams* p, int64_t n, int32_t nstage
     int pdv = P.energy_scheme == SPH_ENERGY_PDV;
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_vhalf<D><<<grid_for(n, 256), 256, 0, s>>>((int)n, nstages, S, dt, v0, vh)));
     wsph::count_launch();
-    WSPH_DISPATCH_DS(*p, (k_finalize<D, G_LIGHT, ST><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, nstages, S, pdv, dt, vh, u0, u_out, du_out)));
+    WSPH_DISPATCH_DS(*p, (k_finalize<D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, nstages, S, pdv, dt, vh, u0, u_out, du_out)));
     return check_launch("sph_finalize_compatible_energy");
 }
 

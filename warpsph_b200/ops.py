@@ -151,7 +151,7 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
         flags = torch.zeros(4, dtype=torch.int64, device=dev)   # [-, status (low half), scratch (2 words)]
         with _timed("neighbors_refresh"):
             check(L.sph_neighbors_refresh(_p(params), n, ptr(x), ptr(H), ptr(prior._x0), ptr(prior._h0), None, None, None, None,
-                                          None, None, flags.data_ptr() + 16, None, flags.data_ptr() + 8, stream_ptr(dev)),
+                                          None, flags.data_ptr() + 16, None, flags.data_ptr() + 8, stream_ptr(dev)),
                   "sph_neighbors_refresh")
         if not (int(flags[1].item()) & 0xffffffff) & _capi.STATUS_LIST_STALE:
             adj = AdjacencyList(neighborOffsets=prior.neighborOffsets, numNeighbors=prior.numNeighbors,
@@ -178,21 +178,17 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
     cb = torch.empty(cap, dtype=torch.int32, device=dev)
     ce = torch.empty(cap, dtype=torch.int32, device=dev)
     grid = torch.empty(8, dtype=torch.int32, device=dev)
-    ioffs = torch.empty(n, dtype=torch.int32, device=dev)
     icnt = torch.empty(n, dtype=torch.int32, device=dev)
     flags = torch.zeros(3, dtype=torch.int64, device=dev)   # [nnz, status (int32 in the low half), interacting nnz]
     hint = _nb_cache.cap_hint.get((dev.index, n, dim))
     list_cap = hint if hint is not None else max(n * 64, 1024)
     for attempt in range(2):
         lst = torch.empty(max(list_cap, 1), dtype=torch.int32, device=dev)
-        ilst = torch.empty(2 * max(list_cap, 1), dtype=torch.int32, device=dev)
-        inter_cap = list_cap
         flags.zero_()
         with _timed("neighbors_build"):
             rc = L.sph_neighbors_build(_p(params), n, ptr(x), ptr(H), ptr(ws), wsb.value, cap, ptr(si), ptr(sk), ptr(cb), ptr(ce),
                                        ptr(grid), ptr(offs), ptr(cnt), ptr(lst), list_cap, flags.data_ptr(),
-                                       ptr(ioffs), ptr(icnt), ptr(ilst), inter_cap, flags.data_ptr() + 16,
-                                       flags.data_ptr() + 8, stream_ptr(dev))
+                                       ptr(icnt), flags.data_ptr() + 16, flags.data_ptr() + 8, stream_ptr(dev))
         check(rc, "sph_neighbors_build")
         f = flags.cpu()
         nnz, status, innz = int(f[0]), int(f[1]) & 0xffffffff, int(f[2])
@@ -208,7 +204,7 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
     adj = AdjacencyList(neighborOffsets=offs, numNeighbors=cnt, neighborList=lst[:nnz], numRows=n, numCols=n, nnz=nnz,
                         sortIndex=si if keep_sort else None, sortedKeys=sk if keep_sort else None, grid=grid,
                         queryPositions=x, querySupports=H, verletScale=float(verletScale),
-                        interOffsets=ioffs, interCounts=icnt, interList=ilst[:2 * nnz], interNnz=innz)
+                        interCounts=icnt, interNnz=innz)
     adj._x_version = _version(x)
     adj._h_version = _version(H)
     adj._x0, adj._h0, adj._dim = x.clone(), H.clone(), dim   # build-time state for the validity check
@@ -230,33 +226,34 @@ def _csr(adj: AdjacencyList):
 
 
 def _materialize_inter(adj: AdjacencyList) -> None:
-    """Filters the interacting sublist of a kept prior list (sph_neighbors_refresh)."""
+    """Rewrites the rows of a kept prior list with the interacting entries for the
+    current positions first (sph_neighbors_refresh).  The rows go to a new tensor:
+    earlier stages keep the old order their pairwise arrays are indexed by."""
     params = adj._pending
     n, dev = adj.numRows, adj.neighborList.device
-    ioffs = torch.empty(n, dtype=torch.int32, device=dev)
     icnt = torch.empty(n, dtype=torch.int32, device=dev)
-    ilst = torch.empty(2 * max(adj.nnz, 1), dtype=torch.int32, device=dev)
+    lst = torch.empty(max(adj.nnz, 1), dtype=torch.int32, device=dev)
     flags = torch.zeros(4, dtype=torch.int64, device=dev)   # [inter nnz, status (low half), scratch (2 words)]
     with _timed("neighbors_refresh"):
         check(_capi.lib().sph_neighbors_refresh(_p(params), n, ptr(adj.queryPositions), ptr(adj.querySupports), ptr(adj._x0),
                                                 ptr(adj._h0), ptr(adj.neighborOffsets), ptr(adj.numNeighbors), ptr(adj.neighborList),
-                                                ptr(ioffs), ptr(icnt), ptr(ilst), flags.data_ptr() + 16, flags.data_ptr(),
+                                                ptr(lst), ptr(icnt), flags.data_ptr() + 16, flags.data_ptr(),
                                                 flags.data_ptr() + 8, stream_ptr(dev)), "sph_neighbors_refresh")
-    adj.interOffsets, adj.interCounts, adj.interList = ioffs, icnt, ilst[:2 * adj.nnz]
+    adj.neighborList, adj.interCounts = lst[: adj.nnz], icnt
+    adj._ij = None
     adj._inter_nnz_dev = flags[:1]
     adj._pending = None
 
 
 def _lists(params, adj: AdjacencyList, interacting: bool):
-    """Selects the row lists a pass walks: the interacting subset (r < max(H_i, H_j),
-    stride 2) when available and sufficient, else the Verlet list (stride 1).  A kept
-    prior list filters its interacting subset here, on first use."""
+    """Selects the rows a pass walks: the interacting prefixes (r < max(H_i, H_j)) when
+    available and sufficient, else the whole Verlet rows.  A kept prior list has its
+    rows reordered here, on first use."""
+    params.list_stride = 1
     if interacting and adj._pending is not None:
         _materialize_inter(adj)
-    if interacting and adj.interList is not None:
-        params.list_stride = 2
-        return iptr(adj.interOffsets), iptr(adj.interCounts), iptr(adj.interList)
-    params.list_stride = 1
+    if interacting and adj.interCounts is not None:
+        return iptr(adj.neighborOffsets), iptr(adj.interCounts), iptr(adj.neighborList)
     return _csr(adj)
 
 
@@ -352,21 +349,23 @@ def switch_balsara(params, DvDx, c):
     return al
 
 
-def crk_accel_dudt(params, x, H, m, rho, V, crk: CRKState, v, c, P, DvDx, adj: AdjacencyList, pair_arrays: bool = True):
-    """Fused CRK momentum and energy RHS over the interacting list; the pairwise
-    accelerations are returned in Verlet-entry order (zeros beyond the support)."""
+def crk_accel_dudt(params, x, H, m, rho, V, crk: CRKState, v, c, P, DvDx, adj: AdjacencyList, pair_arrays: bool = True,
+                   want_dEdt: bool = False):
+    """Fused CRK momentum and energy RHS over the interacting prefixes; the pairwise
+    accelerations are returned in Verlet-entry order (zeros for the rest of each row).
+    Returns (dvdt, dudt, ap, av), and dE/dt last when ``want_dEdt``."""
     n, d = H.shape[0], int(params.dim)
     dvdt, dudt = _empty((n, d), H), _empty(n, H)
-    inter = adj.interList is not None
-    alloc = torch.zeros if inter else torch.empty
-    ap = alloc((adj.nnz, d), device=H.device, dtype=torch.float32) if pair_arrays else None
-    av = alloc((adj.nnz, d), device=H.device, dtype=torch.float32) if pair_arrays else None
+    dEdt = _empty(n, H) if want_dEdt else None
+    ap = _empty((adj.nnz, d), H) if pair_arrays else None
+    av = _empty((adj.nnz, d), H) if pair_arrays else None
     with _timed("crk_accel_dudt"):
+        rows = _lists(params, adj, True)
         check(_capi.lib().sph_crk_accel_dudt(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(V), fptr(crk.A), fptr(crk.B),
-                                             fptr(crk.gradA), fptr(crk.gradB), fptr(v), fptr(c), fptr(P), fptr(DvDx),
-                                             *_lists(params, adj, True), ptr(dvdt), ptr(dudt), ptr(ap), ptr(av),
+                                             fptr(crk.gradA), fptr(crk.gradB), fptr(v), fptr(c), fptr(P), fptr(DvDx), *rows,
+                                             iptr(adj.numNeighbors), ptr(dvdt), ptr(dudt), ptr(dEdt), ptr(ap), ptr(av),
                                              stream_ptr(H.device)), "sph_crk_accel_dudt")
-    return dvdt, dudt, ap, av
+    return (dvdt, dudt, ap, av, dEdt) if want_dEdt else (dvdt, dudt, ap, av)
 
 
 def compsph_prep(params, x, H, m, rho, v, adj: AdjacencyList, grad_h: bool = True, want_div: bool = True,
@@ -390,13 +389,13 @@ def compsph_accel_dudt(params, x, H, m, rho, v, c, alpha, P, omega, adj: Adjacen
     n, d = H.shape[0], int(params.dim)
     dvdt, dudt = _empty((n, d), H), _empty(n, H)
     dEdt = _empty(n, H) if want_dEdt else None
-    alloc = torch.zeros if adj.interList is not None else torch.empty
-    ap = alloc((adj.nnz, d), device=H.device, dtype=torch.float32) if pair_arrays else None
-    av = alloc((adj.nnz, d), device=H.device, dtype=torch.float32) if pair_arrays else None
+    ap = _empty((adj.nnz, d), H) if pair_arrays else None
+    av = _empty((adj.nnz, d), H) if pair_arrays else None
     with _timed("compsph_accel_dudt"):
+        rows = _lists(params, adj, True)
         check(_capi.lib().sph_compsph_accel_dudt(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(v), fptr(c), fptr(alpha),
-                                                 fptr(P), fptr(omega), *_lists(params, adj, True), ptr(dvdt), ptr(dudt), ptr(dEdt),
-                                                 ptr(ap), ptr(av), stream_ptr(H.device)), "sph_compsph_accel_dudt")
+                                                 fptr(P), fptr(omega), *rows, iptr(adj.numNeighbors), ptr(dvdt), ptr(dudt),
+                                                 ptr(dEdt), ptr(ap), ptr(av), stream_ptr(H.device)), "sph_compsph_accel_dudt")
     return dvdt, dudt, dEdt, ap, av
 
 
@@ -459,12 +458,13 @@ def finalize_compatible_energy(params, weights, dt, v0, u0, stages):
     u = _empty(n, u0)
     scratch = _empty(n * (1 + d), u0)
     ns = len(stages)
-    inter = all(s[1].interList is not None for s in stages)
-    params.list_stride = 2 if inter else 1
+    # each stage's pairwise arrays are zero beyond the interacting prefix of its rows
+    inter = all(s[1].interCounts is not None and s[1]._pending is None for s in stages)
+    params.list_stride = 1
     arrs = [_capi.ptr_array([fptr(s[0]) for s in stages]),
-            _capi.ptr_array([iptr(s[1].interOffsets if inter else s[1].neighborOffsets) for s in stages]),
+            _capi.ptr_array([iptr(s[1].neighborOffsets) for s in stages]),
             _capi.ptr_array([iptr(s[1].interCounts if inter else s[1].numNeighbors) for s in stages]),
-            _capi.ptr_array([iptr(s[1].interList if inter else s[1].neighborList) for s in stages]),
+            _capi.ptr_array([iptr(s[1].neighborList) for s in stages]),
             _capi.ptr_array([fptr(s[2]) for s in stages]),
             _capi.ptr_array([fptr(s[3]) for s in stages]),
             _capi.ptr_array([fptr(s[4]) for s in stages])]

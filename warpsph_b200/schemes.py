@@ -10,7 +10,7 @@ every SPH operation executed by libwarpsph_b200 kernels:
   ideal-gas EOS                       crkSPH.py:95  -> sph_eos_ideal_gas
   CRK velocity gradient               crkSPH.py:158 -> sph_grad_v (also the Cullen divergence)
   viscosity switch                    crkSPH.py:195 -> sph_switch_cullen (R and v_sig) / sph_switch_balsara
-  momentum + energy RHS               crkSPH.py:241,263 -> sph_crk_accel_dudt (one fused pass)
+  momentum + energy RHS, dE/dt        crkSPH.py:241,263,330 -> sph_crk_accel_dudt (one fused pass)
   energy partition f_ij               crkSPH.py:343 -> sph_compsph_balance
 """
 from __future__ import annotations
@@ -132,12 +132,12 @@ def crkSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams:
     elif switch != ViscositySwitch.NoneSwitch:
         raise ValueError(f"Unsupported viscosity switch scheme: {switch}")
     # crkSPH.py:241-284
-    dvdt, dudt, S.ap_ij, S.av_ij = ops.crk_accel_dudt(params, S.positions, S.supports, S.masses, S.densities, V, crk, S.velocities,
-                                                      S.soundspeeds, S.pressures, DvDx, adjacency)
+    # (dE/dt = m v.dv/dt + m du/dt of crkSPH.py:330 is written by the same pass)
+    dvdt, dudt, S.ap_ij, S.av_ij, dEdt = ops.crk_accel_dudt(params, S.positions, S.supports, S.masses, S.densities, V, crk,
+                                                            S.velocities, S.soundspeeds, S.pressures, DvDx, adjacency,
+                                                            want_dEdt=True)
     # crkSPH.py:324-337
     S.divergence = -drhodt / S.densities
-    # the reference's einsum("ij,ij->i", v, dvdt) as a fused row dot (einsum lowers to a GEMV here)
-    dEdt = S.masses * (S.velocities * dvdt).sum(-1) + S.masses * dudt
     update = CompressibleSystemUpdate(dxdt=S.velocities, dvdt=dvdt, dudt=dudt, drhodt=drhodt, dEdt=dEdt, passive=None)
     # crkSPH.py:341-363
     S.f_ij = ops.compsph_balance(params, S.masses, S.densities, S.pressures, S.internalEnergies, S.velocities, dvdt, dt, adjacency,
