@@ -24,7 +24,7 @@ import torch
 from . import ops
 from .configurations import CompressibleSPHConfig, CompSPHConfig, SimulationConfig, make_params
 from .core import SupportScheme
-from .enumTypes import ViscositySwitch
+from .enumTypes import AdaptiveSupportScheme, ViscositySwitch
 from .schemes import evaluateOptimalSupport
 from .systems import CompressibleSystemUpdate, CompSPHSystem
 
@@ -44,13 +44,16 @@ def compSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams
     params = make_params(config, compParams)
     S = system.state
     # compSPH.py:36-47
-    rho_opt, h_opt, system.adjacency, *_ = evaluateOptimalSupport(S, config, compParams, SupportScheme.Gather, system.adjacency)
+    rho_opt, h_opt, adj_opt, *_ = evaluateOptimalSupport(S, config, compParams, SupportScheme.Gather, system.adjacency)
     S.supports = h_opt
     S.densities = rho_opt
-    adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, system.adjacency)
+    adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, adj_opt)
     system.adjacency = adjacency
-    # compSPH.py:57-66 (gather density)
-    S.densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
+    # compSPH.py:57-66: the gather density at the optimal supports.  When the adaptive
+    # support ran and the list is the one it ended with, that is the density it returned
+    # (the same pass over the same rows, so the same values) and is not recomputed.
+    if adjacency is not adj_opt or compParams.adaptiveSupportScheme == AdaptiveSupportScheme.NoScheme:
+        S.densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
     if S.divergence is None:
         _, _, dr0 = ops.compsph_prep(params, S.positions, S.supports, S.masses, S.densities, S.velocities, adjacency,
                                      grad_h=False, want_div=False)

@@ -509,7 +509,7 @@ __device__ __forceinline__ void zero_row_tail(int lane, int e, int te, float* __
 // each Verlet row (cnt = interacting counts) with vcnt = the Verlet counts, the
 // ap_ij / av_ij entries of the rest of the row are written as zeros.
 template <int KF, int D, int G>
-__global__ void __launch_bounds__(PAIR_BLOCK)
+__global__ void __launch_bounds__(PAIR_BLOCK, (D == 3 ? 5 : 8))
 k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
                  const float* __restrict__ rho, const float* __restrict__ V, const float* __restrict__ A,
                  const float* __restrict__ B, const float* __restrict__ gA, const float* __restrict__ gB,

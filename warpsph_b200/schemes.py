@@ -31,11 +31,13 @@ from .systems import CompressibleState, CompressibleSystem, CompressibleSystemUp
 # ------------------------------------------------------------------ adaptive support
 def evaluateOptimalSupport(particleState, config: SimulationConfig, compParams: CompressibleSPHConfig,
                            supportScheme: SupportScheme = SupportScheme.Scatter, adjacency: Optional[AdjacencyList] = None,
-                           iterations: Optional[int] = None, threshold: Optional[float] = None):
+                           iterations: Optional[int] = None, threshold: Optional[float] = None, final_density: bool = True):
     """modules/adaptiveSupport/optimalSupport.py:12-43 and optimalSupportMonaghan.py:62-150.
 
     Returns (densities, supports, adjacency, None, None).  The Owen LUT scheme is not
-    on this path; NoScheme returns the state unchanged."""
+    on this path; NoScheme returns the state unchanged.  With ``final_density=False``
+    the closing gather density at the new supports is not evaluated and the densities
+    of the last Newton iteration are returned (for callers that overwrite them)."""
     scheme = compParams.adaptiveSupportScheme
     if scheme == AdaptiveSupportScheme.NoScheme:
         return particleState.densities, particleState.supports, adjacency, None, None
@@ -57,6 +59,8 @@ def evaluateOptimalSupport(particleState, config: SimulationConfig, compParams: 
         if it < nIter - 1 and float((ratio - 1).abs().max()) < hThreshold:
             break
     adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, adjacency)
+    if not final_density:
+        return S.densities, S.supports, adjacency, None, None
     densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
     return densities, S.supports, adjacency, None, None
 
@@ -105,8 +109,10 @@ def crkSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams:
         raise NotImplementedError("boundary conditions are outside the GPU hot path")
     params = make_params(config, compParams)
     S = system.state
-    # crkSPH.py:40-42
-    rho_opt, h_opt, system.adjacency, *_ = evaluateOptimalSupport(S, config, compParams, SupportScheme.Gather, system.adjacency)
+    # crkSPH.py:40-42 (the densities are replaced by the CRK densities at crkSPH.py:61 before
+    # anything reads them, so the closing density pass is skipped)
+    rho_opt, h_opt, system.adjacency, *_ = evaluateOptimalSupport(S, config, compParams, SupportScheme.Gather, system.adjacency,
+                                                                  final_density=False)
     S.supports = h_opt
     S.densities = rho_opt
     # crkSPH.py:54-59
