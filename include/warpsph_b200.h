@@ -202,6 +202,21 @@ int sph_density_gather(const SphParams* p, int64_t n, int32_t support_mode,
                        const int32_t* offs, const int32_t* cnt, const int32_t* list,
                        float* rho_out, void* stream);
 
+/* One iteration of the Owen adaptive support (modules/adaptiveSupport/optimalSupportOwen.py:
+ * 70-108; replaces computePsi0Warp, wp_psi0.py:173, and the table lookup and update):
+ * psi0 and psi0H of wp_psi0.py:46-98 (gather support, W and |grad W| scaled by h^d and
+ * h^(d+1), each sum to the power 1/d), n_h from the table (lut_psiH[nlut] ascending ->
+ * lut_nh[nlut], device FP64; owenLUT.py:6-12), then H_new = (1 - a + a s) H with
+ * s = target_nh / n_h and a = 0.4 (1 + s^-3) (s >= 1) or 0.4 (1 + s^2)
+ * (optimalSupportOwen.py:27-33), clamped to [hbounds[0]/4, 4*hbounds[1]].  psi0_out,
+ * psiH_out and ratio_out (= H_new/H) may be null.  The rows must cover every pair within
+ * H_i (Verlet rows, or interacting prefixes for the current supports). */
+int sph_owen_iter(const SphParams* p, int64_t n, const float* x, const float* H,
+                  const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                  const double* lut_nh, const double* lut_psiH, int32_t nlut, double target_nh,
+                  const float* hbounds, float* psi0_out, float* psiH_out, float* H_out,
+                  float* ratio_out, void* stream);
+
 /* One Monaghan Newton iteration of the adaptive support
  * (modules/adaptiveSupport/optimalSupportMonaghan.py:87-125 with the Omega kernel
  * modules/adaptiveSupport/wp_omega.py:10-60): gather density, Omega = dF/dh,

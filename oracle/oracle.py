@@ -93,6 +93,7 @@ class Oracle:
         L.oracle_pressure_accel_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pressure_shift_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_deltasph_rhs.argtypes = [P, P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rp]
+        L.oracle_owen_iter.argtypes = [P, i64, rp, rp, _i32p, _i32p, _i32p, _f64p, _f64p, C.c_int, C.c_double, rp, rpn, rpn, rp, rpn]
         L.oracle_vsig.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pi_pairs.argtypes = [P, i64, rp, rp, rp, rp, rpn, rpn, rp, _i32p, _i32p, _i32p, C.c_int, C.c_int, rp]
         L.oracle_compsph_prep.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rpn, rpn, rpn]
@@ -285,6 +286,15 @@ class Oracle:
         self.lib.oracle_deltasph_rhs(self._p(params), C.c_void_p(C.addressof(wc)), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho),
                                      self.arr(v), nb["offsets"], nb["counts"], nb["list"], gL, P, dv, dr)
         return dv, dr, gL, P
+
+    def owen_iter(self, params, x, H, nb, lut_nh, lut_psiH, target, hb):
+        """(psi0, psiH, H_new, ratio) of one Owen support iteration."""
+        n = len(H)
+        psi0, psiH, Hn, ratio = (np.zeros(n, self.dtype) for _ in range(4))
+        self.lib.oracle_owen_iter(self._p(params), n, self.arr(x), self.arr(H), nb["offsets"], nb["counts"], nb["list"],
+                                  np.ascontiguousarray(lut_nh, np.float64), np.ascontiguousarray(lut_psiH, np.float64), len(lut_nh),
+                                  float(target), self.arr(hb), psi0, psiH, Hn, ratio)
+        return psi0, psiH, Hn, ratio
 
     def vsig(self, params, x, H, v, c, nb):
         out = np.zeros(len(H), self.dtype)

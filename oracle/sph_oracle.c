@@ -410,6 +410,48 @@ int oracle_adaptive_h_iter(const SphParams* p, int64_t n, const real* x, const r
 /* ------------------------------------------------------------------ CRK volume and coefficients
  * warpSPHCore crk_volume / crk_moments / crk_density (called via computeCRKFactors,
  * schemes/crkSPH.py:61), restated from Frontiere, Raskin & Owen 2017. */
+/* Owen adaptive support, one iteration (modules/adaptiveSupport/optimalSupportOwen.py:70-108,
+ * wp_psi0.py:46-98 gather support, owenLUT.py:6-12 lookup in FP64, the update of :27-33). */
+int oracle_owen_iter(const SphParams* p, int64_t n, const real* x, const real* H, const int32_t* offs, const int32_t* cnt,
+                     const int32_t* list, const double* lut_nh, const double* lut_psiH, int nlut, double target, const real* hb,
+                     real* psi0_out, real* psiH_out, real* H_out, real* ratio_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real hi = H[i];
+        real hsW = (real)1 / POW(hi, -(real)D), hsG = (real)1 / POW(hi, -(real)(D + 1));
+        real sW = 0, sG = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG(&o, d, rsqrt_safe(dotD(d, d, D)), hi, &W, g);
+            sW += hsW * W;
+            sG += hsG * rsqrt_safe(dotD(g, g, D));
+        }
+        real psi0 = POW(sW, (real)1 / (real)D), psiH = POW(sG, (real)1 / (real)D);
+        double xv = (double)psiH;
+        int cntle = 0;                                   /* searchsorted(right=True) */
+        while (cntle < nlut && lut_psiH[cntle] <= xv) ++cntle;
+        int il = cntle - 1;
+        il = il < 0 ? 0 : (il > nlut - 2 ? nlut - 2 : il);
+        double alpha = (xv - lut_psiH[il]) / (lut_psiH[il + 1] - lut_psiH[il]);
+        alpha = alpha < 0 ? 0 : (alpha > 1 ? 1 : alpha);
+        real nh = (real)(lut_nh[il] * (1 - alpha) + lut_nh[il + 1] * alpha);
+        real sv = (real)target / nh;
+        real a = sv >= 1 ? (real)0.4 * (1 + POW(sv, (real)-3)) : (real)0.4 * (1 + POW(sv, (real)2));
+        real hn = (1 - a + a * sv) * hi;
+        real lo = hb[0] * (real)0.25, up = hb[1] * (real)4;
+        hn = hn < lo ? lo : (hn > up ? up : hn);
+        if (psi0_out) psi0_out[i] = psi0;
+        if (psiH_out) psiH_out[i] = psiH;
+        H_out[i] = hn;
+        if (ratio_out) ratio_out[i] = hn / hi;
+    }
+    return 0;
+}
+
 int oracle_crk_volume(const SphParams* p, int64_t n, const real* x, const real* H, const int32_t* offs, const int32_t* cnt,
                       const int32_t* list, real* V) {
     OP o = op_from(p);

@@ -34,7 +34,7 @@ def cell_capacity_for(n: int, dim: int) -> int:
 
 class CRKSPHOracle:
     def __init__(self, params, precision: str = "f32", adaptive_iterations: int = 1, adaptive_threshold: float = 1e-3,
-                 switch: int = SWITCH_CULLEN, compatible_energy: bool = True, adaptive: bool = True):
+                 switch: int = SWITCH_CULLEN, compatible_energy: bool = True, adaptive: bool = True, owen_table=None):
         self.o = _oracle.get(precision)
         self.p = params
         self.dt_ = self.o.dtype
@@ -43,6 +43,7 @@ class CRKSPHOracle:
         self.switch = switch
         self.compatible = compatible_energy
         self.adaptive = adaptive
+        self.owen = owen_table          # (n_h, psi_H) table: the Owen scheme instead of Monaghan's
         self.dim = int(params.dim)
 
     # --------------------------------------------------------------- helpers
@@ -80,6 +81,15 @@ class CRKSPHOracle:
         hb = np.array([H.min(), H.max()], dtype=self.dt_)
         for it in range(self.iters):
             nb = self.nb(x, H)
+            if self.owen is not None:       # modules/adaptiveSupport/optimalSupportOwen.py:70-114
+                target = ((2.0 if self.dim == 1 else (np.pi if self.dim == 2 else 4 / 3 * np.pi)) / float(p.target_neighbors)) \
+                    ** (-1.0 / self.dim)
+                _, _, Hn, ratio = o.owen_iter(p, x, H, nb, self.owen[0], self.owen[1], target, hb)
+                hb = np.array([Hn.min(), Hn.max()], dtype=self.dt_)
+                H = Hn
+                if it < self.iters - 1 and np.abs(ratio - 1).max() < self.thr:
+                    break
+                continue
             rho, Hn, ratio = o.adaptive_h_iter(p, x, H, m, nb, hb)
             hb = np.array([Hn.min(), Hn.max()], dtype=self.dt_)
             H = Hn

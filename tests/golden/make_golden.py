@@ -734,10 +734,108 @@ def run_reference_compsph(ref: Path, case: dict) -> dict:
     return out
 
 
+# ---------------------------------------------------------------- Owen adaptive support
+def _eval_C_d(dim, kernel):
+    return kernel_C(int(kernel), int(dim))
+
+
+def _eval_k(q, dim, kernel):
+    q = F(q)
+    if not (q < F(1)):
+        return F(0)
+    return F(kernel_kp(int(kernel), int(dim), q)[0])
+
+
+def _eval_dkdq(q, dim, kernel):
+    q = F(q)
+    if not (q < F(1)):
+        return F(0)
+    return F(-(q * kernel_kp(int(kernel), int(dim), q)[1]))
+
+
+def run_reference_owen(ref: Path) -> dict:
+    """The reference's table generator (wp_psi.py computePsi, its per-entry body run with
+    wp.tid() set to the entry), the psi0 pair body (wp_psi0.py computePsi0_Func_i, gather
+    support), the table lookup (owenLUT.py interpolateLUT) and the support update
+    (optimalSupportOwen.py computeNewSupport), with this project's Wendland restatement
+    for the absent warpSPHCore kernel functions."""
+    from oracle import oracle
+    from oracle.steps import cell_capacity_for
+    from tests.cases import make_params, make_particles
+    import warpsph_b200 as ws
+    from warpsph_b200.owen import owen_table
+    psi_ns = load(ref, "modules/adaptiveSupport/wp_psi.py", dict(eval_k=_eval_k, eval_dkdq=_eval_dkdq, eval_C_d=_eval_C_d,
+                                                                  math=__import__("math")))
+    out = {}
+    rng = np.random.default_rng(11)
+    for (kern, dim, nsel) in ((1, 1, 64), (2, 2, 48), (2, 3, 4)):
+        nlut = 2 ** 12
+        sel = np.sort(rng.choice(nlut, nsel, replace=False))
+        n_out, psi, psiH, NH = (np.zeros(nlut, F) for _ in range(4))
+        for i in sel:
+            wp.tid = (lambda k: (lambda: int(k)))(i)
+            with np.errstate(all="ignore"):
+                psi_ns["computePsi"](kern, dim, F(2.0), F(6.0), nlut, n_out, psi, psiH, NH)
+        out[f"owen_lut_sel_k{kern}_d{dim}"] = sel
+        out[f"owen_lut_nh_k{kern}_d{dim}"] = n_out[sel].astype(np.float64)
+        out[f"owen_lut_psiH_k{kern}_d{dim}"] = psiH[sel].astype(np.float64)
+    wp.tid = lambda: 0
+    # per-particle iteration, 2D Wendland C4
+    Ctx.kernel, Ctx.dim = 2, 2
+    cfg, sch, p = make_params(2, kernel=ws.KernelFunctions.Wendland4)
+    P = make_particles(2, 16, seed=21, jitter=0.4, h_spread=0.15)
+    x, H, m = P["positions"], P["supports"], P["masses"]
+    n = len(H)
+    o = oracle.get("f32")
+    nb = o.neighbors(p, x, H, cell_capacity_for(n, 2))
+    offs, cnt, lst = nb["offsets"], nb["counts"], nb["list"].astype(np.int64)
+    rho = o.density(p, 0, x, H, m, nb)
+    state = SoA(positions=x, supports=H, masses=m, densities=rho, kinds=np.zeros(n, np.int32))
+
+    def sphKernel(xi, xj, hi, hj, kp, dom):
+        d = computeDistanceVec(xi, xj)
+        return kWG(d, safe_sqrt(wp.dot(d, d)), hi)[0]
+
+    def sphKernelGradient(xi, xj, hi, hj, kp, dom):
+        d = computeDistanceVec(xi, xj)
+        return kWG(d, safe_sqrt(wp.dot(d, d)), hi)[1]
+
+    psi0_ns = load(ref, "modules/adaptiveSupport/wp_psi0.py", dict(sphKernel=sphKernel, sphKernelGradient=sphKernelGradient,
+                                                                    dim_t=None))
+    psi0 = np.zeros(n, F)
+    psi0H = np.zeros(n, F)
+    kp = SoA(operationMode=0, kernelFunction=2, supportMode="gather")
+    with np.errstate(all="ignore"):
+        for i in range(n):
+            a, b = call(psi0_ns["computePsi0_Func_i"], i=i, dim=2, xi=x[i], hi=F(H[i]), mi=F(m[i]), rhoi=F(rho[i]),
+                        referenceState=state, domainState=SoA(dim=2), kernelProperties=kp, beginIndex=int(offs[i]),
+                        numIndices=int(cnt[i]), offsetArray=lst, ki=0, referenceKinds=state.kinds,
+                        useGradientRenormalization=False, Li=None, useGradHTerms=False, omega_i=F(1), referenceOmegas=None,
+                        useVolume=False, Vi=F(0), referenceVolumes=None, useCRK=False, Ai=F(1), Bi=np.zeros(2, F),
+                        gradAi=np.zeros(2, F), gradBi=np.zeros((2, 2), F))
+            psi0[i], psi0H[i] = a, b
+    lut_ns = load(ref, "modules/adaptiveSupport/owenLUT.py", dict(generatePSILut_warp=None))
+    nh_tab, psiH_tab = owen_table(ws.KernelFunctions.Wendland4, 2)
+    LUT = [torch.from_numpy(nh_tab), [torch.from_numpy(psiH_tab)], [torch.from_numpy(psiH_tab)], [torch.from_numpy(nh_tab)]]
+    n_h = lut_ns["interpolateLUT"](LUT, 2, which="n_h", psiH=torch.from_numpy(psi0H).to(torch.float64)).to(torch.float32)
+    own_ns = load(ref, "modules/adaptiveSupport/optimalSupportOwen.py", dict(computePsi0Warp=None, computeOwen=None,
+                                                                             interpolateLUT=None, CompressibleState=None,
+                                                                             SimulationConfig=None, CompressibleSPHConfig=None,
+                                                                             KernelFunctions=None, AdjacencyList=None,
+                                                                             CompactHashMap=None, SupportScheme=None))
+    target = own_ns["nH_to_n_h"](float(p.target_neighbors), 2)
+    Ht = torch.from_numpy(H)
+    h = own_ns["computeNewSupport"](target, n_h, Ht)
+    h = h.clamp(min=Ht.min() * 0.25, max=Ht.max() * 4.0)
+    out.update(owen_x=x, owen_H=H, owen_m=m, owen_offsets=offs, owen_counts=cnt, owen_list=nb["list"], owen_psi0=psi0,
+               owen_psi0H=psi0H, owen_nh=n_h.numpy(), owen_Hnew=h.numpy(), owen_target=np.array([target]))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph"], default="all")
+    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph", "owen"], default="all")
     a = ap.parse_args()
     ref = Path(a.reference)
     if a.which in ("all", "crk"):
@@ -768,6 +866,10 @@ def main():
                             P=case["P"], c=case["c"], offsets=nb["offsets"], counts=nb["counts"], list=nb["list"],
                             pi_sel=case["pi_sel"], pi_variants=PI_VARIANTS, pi_coeffs=PI_COEFFS, **out)
         print("wrote", Path(__file__).parent / "compsph_golden.npz", "particles", case["n"], "pairs", len(nb["list"]))
+    if a.which in ("all", "owen"):
+        out = run_reference_owen(ref)
+        np.savez_compressed(Path(__file__).parent / "owen_golden.npz", **out)
+        print("wrote", Path(__file__).parent / "owen_golden.npz")
 
 
 if __name__ == "__main__":

@@ -104,6 +104,7 @@ _PROTOS = {
     "sph_density_gather": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_adaptive_h_iter": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_minmax": [_I64, _P, _P, _P],
+    "sph_owen_iter": [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _I32, C.c_double, _P, _P, _P, _P, _P, _P],
     "sph_crk_volume": [_P, _I64, _P, _P, _P, _P, _P, _P, _P],
     "sph_crk_factors": [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_eos_ideal_gas": [_P, _I64, _P, _P, _P, _P, _P, _P],

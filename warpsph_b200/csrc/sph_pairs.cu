@@ -93,6 +93,72 @@ k_adaptive_h(int n, DevParams P, const float* __restrict__ x, const float* __res
     if (ratio) ratio[g.i] = hn / (Hi + 1e-6f);
 }
 
+// ---------------------------------------------------------------- Owen adaptive support
+// One iteration of modules/adaptiveSupport/optimalSupportOwen.py:70-108 for every particle:
+//   psi0_i  = (sum_j h_i^d W(r_ij, h_i))^(1/d), psi0H_i = (sum_j h_i^(d+1) |grad W(r_ij, h_i)|)^(1/d)
+//             (wp_psi0.py:46-98, gather support; h^k taken as 1 / h^-k as there),
+//   n_h_i   = the (psiH -> n_h) table linearly interpolated at psi0H_i in FP64 (owenLUT.py:6-12,
+//             64-67: index of the last entry <= psi0H, clamped to the table, weight clamped to [0, 1]),
+//   s = target / n_h_i, a = 0.4 (1 + s^-3) if s >= 1 else 0.4 (1 + s^2), h_new = (1 - a + a s) h
+//             (optimalSupportOwen.py:27-33), clamped to [hbounds[0] / 4, 4 hbounds[1]] (:96);
+//   ratio   = h_new / h (:100).
+__device__ __forceinline__ float owen_nh(const double* __restrict__ lut_nh, const double* __restrict__ lut_psiH, int nlut, float psiH) {
+    const double x = (double)psiH;
+    int lo = 0, hi = nlut;                       // first index with lut_psiH[idx] > x
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(lut_psiH + mid) <= x) lo = mid + 1; else hi = mid;
+    }
+    int il = lo - 1;
+    il = il < 0 ? 0 : (il > nlut - 2 ? nlut - 2 : il);
+    const double xl = __ldg(lut_psiH + il), xr = __ldg(lut_psiH + il + 1);
+    double alpha = (x - xl) / (xr - xl);
+    alpha = alpha < 0.0 ? 0.0 : (alpha > 1.0 ? 1.0 : alpha);
+    return (float)(__ldg(lut_nh + il) * (1.0 - alpha) + __ldg(lut_nh + il + 1) * alpha);
+}
+
+template <int KF, int D, int G>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_owen(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H,
+       const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+       const double* __restrict__ lut_nh, const double* __restrict__ lut_psiH, int nlut, float target,
+       const float* __restrict__ hb, float* __restrict__ psi0_out, float* __restrict__ psiH_out,
+       float* __restrict__ H_out, float* __restrict__ ratio) {
+    Grp<G> g(n);
+    float sW = 0.f, sG = 0.f, Hi = 1.f;
+    if (g.valid) {
+        const int i = g.i;
+        Vec<D> xi = load_vec<D>(x, i);
+        Hi = H[i];
+        const float invHi = 1.f / Hi;
+        const float hsW = 1.f / powf(Hi, -(float)D), hsG = 1.f / powf(Hi, -(float)(D + 1));
+        int b = offs[i], e = b + cnt[i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry(list, q, j, k);
+            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float r = safe_sqrt(dot<D>(xij, xij));
+            float W; Vec<D> gW;
+            kWG_inv<KF, D>(xij, r, invHi, W, gW);
+            sW += hsW * W;
+            sG += hsG * safe_sqrt(dot<D>(gW, gW));
+        }
+    }
+    sW = gsum<G>(sW);
+    sG = gsum<G>(sG);
+    if (!g.valid || g.lane != 0) return;
+    const int i = g.i;
+    const float psi0 = powf(sW, 1.f / (float)D), psiH = powf(sG, 1.f / (float)D);
+    const float nh = owen_nh(lut_nh, lut_psiH, nlut, psiH);
+    const float s = target / nh;
+    const float a = s >= 1.f ? 0.4f * (1.f + powf(s, -3.f)) : 0.4f * (1.f + powf(s, 2.f));
+    float hn = (1.f - a + a * s) * Hi;
+    hn = fminf(fmaxf(hn, hb[0] * 0.25f), hb[1] * 4.f);
+    if (psi0_out) psi0_out[i] = psi0;
+    if (psiH_out) psiH_out[i] = psiH;
+    H_out[i] = hn;
+    if (ratio) ratio[i] = hn / Hi;
+}
+
 // ---------------------------------------------------------------- CRK volume (scatter support)
 template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
@@ -906,6 +972,22 @@ int sph_adaptive_h_iter(const SphParams* p, int64_t n, int32_t support_mode, con
     wsph::count_launch();
     WSPH_DISPATCH_KDS(*p, (k_adaptive_h<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, offs, cnt, list, hbounds, rho_out, H_out, ratio_out)));
     return check_launch("sph_adaptive_h_iter");
+}
+
+int sph_owen_iter(const SphParams* p, int64_t n, const float* x, const float* H, const int32_t* offs, const int32_t* cnt,
+                  const int32_t* list, const double* lut_nh, const double* lut_psiH, int32_t nlut, double target_nh,
+                  const float* hbounds, float* psi0_out, float* psiH_out, float* H_out, float* ratio_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(lut_nh); WSPH_CHECK_PTR(lut_psiH); WSPH_CHECK_PTR(hbounds);
+    WSPH_CHECK_PTR(H_out); CHECK_CSR();
+    if (nlut < 2) return set_error(SPH_ERR_BAD_ARG, "sph_owen_iter: the table needs at least 2 entries");
+    if (!(target_nh > 0.0)) return set_error(SPH_ERR_BAD_ARG, "sph_owen_iter: target n_h must be positive");
+    if ((rc = check_align_vec(P, x, "x"))) return rc;
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_owen<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, offs, cnt, list, lut_nh, lut_psiH,
+                                                                                             (int)nlut, (float)target_nh, hbounds, psi0_out,
+                                                                                             psiH_out, H_out, ratio_out)));
+    return check_launch("sph_owen_iter");
 }
 
 int sph_crk_volume(const SphParams* p, int64_t n, const float* x, const float* H, const int32_t* offs, const int32_t* cnt,

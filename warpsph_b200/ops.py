@@ -274,6 +274,22 @@ def minmax(a: torch.Tensor) -> torch.Tensor:
     return out
 
 
+def owen_iter(params, x, H, adj: AdjacencyList, lut_nh: torch.Tensor, lut_psiH: torch.Tensor, target_nh: float,
+              hbounds: torch.Tensor, want_psi0: bool = False):
+    """One Owen support iteration (psi0 pair sums, table lookup, update): (psiH, H_new,
+    ratio), and psi0 last when ``want_psi0``."""
+    n = H.shape[0]
+    psiH, Hn, ratio = _empty(n, H), _empty(n, H), _empty(n, H)
+    psi0 = _empty(n, H) if want_psi0 else None
+    if lut_nh.dtype != torch.float64 or lut_psiH.dtype != torch.float64:
+        raise RuntimeError("the Owen table is FP64")
+    with _timed("owen_iter"):
+        check(_capi.lib().sph_owen_iter(_p(params), n, fptr(x), fptr(H), *_lists(params, adj, True), ptr(lut_nh), ptr(lut_psiH),
+                                        int(lut_nh.shape[0]), float(target_nh), fptr(hbounds), ptr(psi0), ptr(psiH), ptr(Hn),
+                                        ptr(ratio), stream_ptr(H.device)), "sph_owen_iter")
+    return (psiH, Hn, ratio, psi0) if want_psi0 else (psiH, Hn, ratio)
+
+
 def adaptive_h_iter(params, x, H, m, adj: AdjacencyList, hbounds: torch.Tensor):
     n = H.shape[0]
     rho, Hn, ratio = _empty(n, H), _empty(n, H), _empty(n, H)

@@ -34,15 +34,18 @@ def evaluateOptimalSupport(particleState, config: SimulationConfig, compParams: 
                            iterations: Optional[int] = None, threshold: Optional[float] = None, final_density: bool = True):
     """modules/adaptiveSupport/optimalSupport.py:12-43 and optimalSupportMonaghan.py:62-150.
 
-    Returns (densities, supports, adjacency, None, None).  The Owen LUT scheme is not
-    on this path; NoScheme returns the state unchanged.  With ``final_density=False``
+    Returns (densities, supports, adjacency, None, None); the Owen scheme
+    (optimalSupportOwen.py:35-127, ``owen.py``) returns its psi and support histories in
+    the last two.  NoScheme returns the state unchanged.  With ``final_density=False``
     the closing gather density at the new supports is not evaluated and the densities
     of the last Newton iteration are returned (for callers that overwrite them)."""
     scheme = compParams.adaptiveSupportScheme
     if scheme == AdaptiveSupportScheme.NoScheme:
         return particleState.densities, particleState.supports, adjacency, None, None
     if scheme == AdaptiveSupportScheme.Owen:
-        raise NotImplementedError("the Owen LUT adaptive-support scheme is not implemented on the GPU path; use Monaghan")
+        from .owen import evaluateOptimalSupportOwen
+        return evaluateOptimalSupportOwen(particleState, config, compParams, kernel_=config.kernel, adjacency=adjacency,
+                                          supportScheme=supportScheme)
     if supportScheme != SupportScheme.Gather:
         raise NotImplementedError("adaptive support is implemented for the gather support scheme")
     params = make_params(config, compParams)
