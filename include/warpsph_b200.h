@@ -108,7 +108,10 @@ typedef struct SphParams {
     /* DiffusionParameters.c_s: the sound speed of the viscosity terms when no per-particle
      * sound speeds are passed (diffusionParameters.py:24) */
     double c_s;
-    double reserved_d[7];
+    /* ViscositySwitchConfig.beta_c, beta_d of the Cullen-Hopkins switch
+     * (viscositySwitchParameters.py:21-22) */
+    double beta_c, beta_d;
+    double reserved_d[5];
     /* integers */
     int32_t dim;                      /* 1, 2 or 3 */
     int32_t kernel;                   /* SPH_KERNEL_* */
@@ -278,6 +281,29 @@ int sph_switch_cullen(const SphParams* p, int64_t n, const float* x, const float
                       const float* alpha0_prev, const float* dt,
                       const int32_t* offs, const int32_t* cnt, const int32_t* list,
                       float* alpha_out, float* R_out, float* vsig_out, void* stream);
+
+/* Cullen-Hopkins switch, first part (modules/shockCapturing/CullenHopkins.py:7-45,
+ * computeHopkinsTerms without the optional velocity-gradient correction): the gather
+ * difference velocity gradient, its divergence (div_out) and tr(S S^T) of its traceless
+ * symmetric part (shear2_out), then R (gather, CullenDehnen2010.py:121-164), Xi with the
+ * shear term (:166-191) and alpha_out = max(Xi alpha0, alpha_min).  The rows must cover
+ * the pairs within H_i.  R_out may be null. */
+int sph_switch_hopkins_terms(const SphParams* p, int64_t n, const float* x, const float* H,
+                             const float* m, const float* rho, const float* v, const float* alpha0,
+                             const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                             float* div_out, float* shear2_out, float* alpha_out, float* R_out,
+                             void* stream);
+/* Cullen-Hopkins switch, second part (computeHopkinsUpdate, CullenHopkins.py:48-149):
+ * v_sig over the Verlet rows (pass whole rows), d(div)/dt = (div - div_prev)/dt,
+ * alpha_tmp = alpha_max |d div/dt| / (|d div/dt| + beta_c c^2 / (h/xi)^2 + 1e-14), zero
+ * where d div/dt > 0 or div > 0, and alpha0_out = alpha_tmp where alpha_tmp >= alpha0,
+ * else alpha_tmp + (alpha0 - alpha_tmp) exp(-beta_d dt v_sig / (2 h/xi)).  dt is a
+ * device float; vsig_out may be null. */
+int sph_switch_hopkins_update(const SphParams* p, int64_t n, const float* x, const float* H,
+                              const float* v, const float* c, const float* div, const float* div_prev,
+                              const float* alpha0, const float* dt,
+                              const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                              float* alpha0_out, float* vsig_out, void* stream);
 
 /* Balsara 1995 switch alpha = clamp(|div v| / (|div v| + |curl v| + 1e-4 c), 0, 1)
  * with CRK difference-form divergence and curl (formula restated from the comment

@@ -94,6 +94,8 @@ class Oracle:
         L.oracle_pressure_shift_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_deltasph_rhs.argtypes = [P, P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rp]
         L.oracle_owen_iter.argtypes = [P, i64, rp, rp, _i32p, _i32p, _i32p, _f64p, _f64p, C.c_int, C.c_double, rp, rpn, rpn, rp, rpn]
+        L.oracle_switch_hopkins_terms.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rpn]
+        L.oracle_switch_hopkins_update.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, rp, real_c, _i32p, _i32p, _i32p, rp, rpn]
         L.oracle_vsig.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pi_pairs.argtypes = [P, i64, rp, rp, rp, rp, rpn, rpn, rp, _i32p, _i32p, _i32p, C.c_int, C.c_int, rp]
         L.oracle_compsph_prep.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rpn, rpn, rpn]
@@ -295,6 +297,23 @@ class Oracle:
                                   np.ascontiguousarray(lut_nh, np.float64), np.ascontiguousarray(lut_psiH, np.float64), len(lut_nh),
                                   float(target), self.arr(hb), psi0, psiH, Hn, ratio)
         return psi0, psiH, Hn, ratio
+
+    def switch_hopkins_terms(self, params, x, H, m, rho, v, alpha0, nb):
+        """(alphas, div, |S|^2, R)"""
+        n = len(H)
+        al, div, s2, R = (np.zeros(n, self.dtype) for _ in range(4))
+        self.lib.oracle_switch_hopkins_terms(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(v),
+                                             self.arr(alpha0), nb["offsets"], nb["counts"], nb["list"], div, s2, al, R)
+        return al, div, s2, R
+
+    def switch_hopkins_update(self, params, x, H, v, c, div, div_prev, alpha0, dt, nb):
+        """(alpha0_next, v_sig) over whole Verlet rows."""
+        n = len(H)
+        a0 = np.zeros(n, self.dtype); vs = np.zeros(n, self.dtype)
+        self.lib.oracle_switch_hopkins_update(self._p(params), n, self.arr(x), self.arr(H), self.arr(v), self.arr(c), self.arr(div),
+                                              self.arr(div_prev), self.arr(alpha0), float(dt), nb["offsets"], nb["counts"], nb["list"],
+                                              a0, vs)
+        return a0, vs
 
     def vsig(self, params, x, H, v, c, nb):
         out = np.zeros(len(H), self.dtype)

@@ -67,7 +67,7 @@ typedef struct {
     real target_neighbors;
     real cfl, min_dt, max_dt, dt_growth;
     real kscale, kxi;
-    real Cu_l, Cu_q, c_s;
+    real Cu_l, Cu_q, c_s, beta_c, beta_d;
     int visc_term, cond_term, mswitch, correct_xi, scale_beta;
 } OP;
 
@@ -99,6 +99,7 @@ static OP op_from(const SphParams* p) {
     o.kscale = (real)kscale_tab(p->kernel, p->dim);
     o.kxi = o.kscale;
     o.Cu_l = (real)p->Cu_l; o.Cu_q = (real)p->Cu_q; o.c_s = (real)p->c_s;
+    o.beta_c = (real)p->beta_c; o.beta_d = (real)p->beta_d;
     o.visc_term = p->viscosity_term; o.cond_term = p->conductivity_term;
     o.mswitch = p->monaghan_switch; o.correct_xi = p->correct_xi; o.scale_beta = p->scale_beta;
     return o;
@@ -690,6 +691,83 @@ int oracle_vsig(const SphParams* p, int64_t n, const real* x, const real* H, con
         }
         vsig_out[i] = FABS(vsig);
     }
+    return 0;
+}
+
+/* Cullen-Hopkins switch (modules/shockCapturing/CullenHopkins.py:7-149 without the optional
+ * gradient correction).  The velocity gradient is warpSPHCore's difference gradient with
+ * gather support, restated as sum_j m_j/rho_j (v_j - v_i) (x) grad W(r_ij, H_i). */
+int oracle_switch_hopkins_terms(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                                const real* v, const real* alpha0, const int32_t* offs, const int32_t* cnt,
+                                const int32_t* list, real* div_out, real* shear2_out, real* alpha_out, real* R_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real G[9] = {0};
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG(&o, d, rsqrt_safe(dotD(d, d, D)), H[i], &W, g);
+            if (W == 0) continue;
+            real Vj = m[j] / rho[j];
+            for (int a = 0; a < D; ++a)
+                for (int b = 0; b < D; ++b) G[a * D + b] += Vj * (v[(int64_t)j * D + a] - v[i * D + a]) * g[b];
+        }
+        real tr = 0, s2 = 0;
+        for (int a = 0; a < D; ++a) tr += G[a * D + a];
+        for (int a = 0; a < D; ++a)
+            for (int b = 0; b < D; ++b) {
+                real sv = (G[a * D + b] + G[b * D + a]) / 2 - (a == b ? tr / (real)D : 0);
+                s2 += sv * sv;
+            }
+        div_out[i] = tr;
+        shear2_out[i] = s2;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real s = 0, Hi = H[i];
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real W = kW(&o, rsqrt_safe(dotD(d, d, D)), Hi);
+            if (W == 0) continue;
+            real sg = div_out[j] > 0 ? 1 : (div_out[j] < 0 ? -1 : 0);
+            s += m[j] / rho[j] * (rho[j] * sg) * W;
+        }
+        real R = 1 / rho[i] * s;
+        real omr = 1 - R, omr2 = omr * omr;
+        real nom = o.beta_xi * (omr2 * omr2) * div_out[i];
+        real Xi = o.limit_xi ? (nom * nom + (real)1e-14 * Hi) / (nom * nom + shear2_out[i] + (real)1e-14 * Hi)
+                             : (nom * nom) / (nom * nom + shear2_out[i] + (real)1e-14 * Hi);
+        real al = Xi * alpha0[i];
+        alpha_out[i] = al < o.alpha_min ? o.alpha_min : al;
+        if (R_out) R_out[i] = R;
+    }
+    return 0;
+}
+
+int oracle_switch_hopkins_update(const SphParams* p, int64_t n, const real* x, const real* H, const real* v, const real* c,
+                                 const real* div, const real* div_prev, const real* alpha0, real dt,
+                                 const int32_t* offs, const int32_t* cnt, const int32_t* list, real* alpha0_out,
+                                 real* vsig_out) {
+    OP o = op_from(p);
+    real* vs = (real*)malloc(sizeof(real) * (size_t)(n > 0 ? n : 1));
+    oracle_vsig(p, n, x, H, v, c, offs, cnt, list, vs);
+    real f_kern = 1 / o.kxi;
+    for (int64_t i = 0; i < n; ++i) {
+        real ddiv = (div[i] - div_prev[i]) / dt;
+        real ad = FABS(ddiv);
+        real fh = f_kern * H[i];
+        real at = o.alpha_max * ad / (ad + o.beta_c * (c[i] * c[i]) / (fh * fh) + (real)1e-14);
+        if (ddiv > 0 || div[i] > 0) at = 0;
+        real nxt = at + (alpha0[i] - at) * EXP(-o.beta_d * dt * vs[i] / (2 * f_kern * H[i]));
+        alpha0_out[i] = at >= alpha0[i] ? at : nxt;
+        if (vsig_out) vsig_out[i] = vs[i];
+    }
+    free(vs);
     return 0;
 }
 

@@ -21,7 +21,7 @@ TABLEAUX = {
     "rungeKutta4": ([[], [0.5], [0.0, 0.5], [0.0, 0.0, 1.0]], [1 / 6, 1 / 3, 1 / 3, 1 / 6], [0.0, 0.5, 0.5, 1.0]),
 }
 
-SWITCH_NONE, SWITCH_CULLEN, SWITCH_BALSARA = 0, 1, 2
+SWITCH_NONE, SWITCH_CULLEN, SWITCH_BALSARA, SWITCH_HOPKINS = 0, 1, 2, 3
 
 
 def cell_capacity_for(n: int, dim: int) -> int:
@@ -177,9 +177,13 @@ class CompSPHOracle(CRKSPHOracle):
         if self.switch == SWITCH_CULLEN:
             vs = o.vsig(p, x, H, v, c, nb)
             st["alphas"], _ = o.switch_cullen(p, x, H, m, rho, div, st["divergence"], vs, st["alpha0s"], dt, nb)
+        elif self.switch == SWITCH_HOPKINS:       # modules/shockCapturing/CullenHopkins.py:7-45
+            st["alphas"], hdiv, _, _ = o.switch_hopkins_terms(p, x, H, m, rho, v, st["alpha0s"], nb)
         dvdt, dudt, dEdt, ap, av = o.compsph_accel_dudt(p, x, H, m, rho, v, c, st.get("alphas"), P, om, nb)
         if self.switch == SWITCH_CULLEN:
             st["alpha0s"] = st["alphas"]
+        elif self.switch == SWITCH_HOPKINS:       # CullenHopkins.py:48-149, before the divergence is replaced
+            st["alpha0s"], _ = o.switch_hopkins_update(p, x, H, v, c, hdiv, st["divergence"], st["alpha0s"], dt, nb)
         st["divergence"] = (-drho / rho).astype(self.dt_)
         st["ap_ij"], st["av_ij"] = ap, av
         st["f_ij"] = o.balance(p, m, rho, P, u, v, dvdt, dt, nb, ap, av)

@@ -734,6 +734,95 @@ def run_reference_compsph(ref: Path, case: dict) -> dict:
     return out
 
 
+# ---------------------------------------------------------------- Cullen-Hopkins switch
+def run_reference_hopkins(ref: Path, g: dict) -> dict:
+    """computeHopkinsTerms and computeHopkinsUpdate (modules/shockCapturing/CullenHopkins.py)
+    run unmodified on the CompSPH fixture's particles, with computeR / computeXi /
+    computeShearTensor from CullenDehnen2010.py and common.py, v_sig from the wp_vsig.py
+    pair body, and warpSPHCore's generic gather operations restated in numpy (difference
+    gradient sum_j V_j (q_j - q_i) (x) grad W(H_i); interpolation sum_j V_j q_j W(H_i))."""
+    Ctx.kernel, Ctx.dim = 2, 2
+    x, H, m, rho, v, c = (g[k] for k in ("x", "H", "m", "rho", "v", "c"))
+    offs, cnt, lst = g["offsets"], g["counts"], g["list"].astype(np.int64)
+    n = len(H)
+    rng = np.random.default_rng(17)
+    alpha0 = (0.1 + 1.5 * rng.random(n)).astype(F)
+    dt = F(2e-3)
+    dvdt = (0.5 * rng.standard_normal((n, 2))).astype(F)
+    pairs = []
+    for i in range(n):
+        for k in range(offs[i], offs[i] + cnt[i]):
+            j = lst[k]
+            d = computeDistanceVec(x[i], x[j])
+            W, gW = kWG(d, safe_sqrt(wp.dot(d, d)), H[i])
+            pairs.append((i, j, W, gW))
+
+    def warpOperation(state, props, domain=None, adjacency=None, queryValues=None, **kw):
+        q = queryValues.numpy().astype(F) if isinstance(queryValues, torch.Tensor) else np.asarray(queryValues, F)
+        if props.operation == "Gradient":
+            outv = np.zeros((n, 2, 2), F)
+            for i, j, W, gW in pairs:
+                if W == 0:
+                    continue
+                Vj = F(m[j] / rho[j])
+                for a in range(2):
+                    dq = F(Vj * (q[j, a] - q[i, a]))
+                    for b in range(2):
+                        outv[i, a, b] = F(outv[i, a, b] + dq * gW[b])
+            return torch.from_numpy(outv)
+        if props.operation == "Interpolate":
+            outv = np.zeros(n, F)
+            for i, j, W, gW in pairs:
+                if W == 0:
+                    continue
+                outv[i] = F(outv[i] + m[j] / rho[j] * q[j] * W)
+            return torch.from_numpy(outv)
+        if props.operation == "Divergence":
+            return torch.zeros(n)          # used only by computeSecondOrderV, whose result is discarded
+        raise NotImplementedError(props.operation)
+
+    class OperationProperties:
+        def __init__(self, kernel=None, operation=None, supportMode=None, gradientMode=None):
+            self.operation = operation
+
+    vs_ns = load(ref, "modules/shockCapturing/wp_vsig.py")
+    state = SoA(positions=x, supports=H, masses=m, densities=rho, kinds=np.zeros(n, np.int32))
+    vsig = np.zeros(n, F)
+    kp = SoA(operationMode=0, kernelFunction=2)
+    with np.errstate(all="ignore"):
+        for i in range(n):
+            vsig[i] = call(vs_ns["computeVsig_Func_i"], i=i, dim=2, xi=x[i], hi=F(H[i]), mi=F(m[i]), rhoi=F(rho[i]),
+                           referenceState=state, domainState=SoA(dim=2), kernelProperties=kp, beginIndex=int(offs[i]),
+                           numIndices=int(cnt[i]), offsetArray=lst, ki=0, referenceKinds=state.kinds,
+                           useGradientRenormalization=False, Li=None, useGradHTerms=False, Viscosity_i=F(1),
+                           referenceViscositys=None, useVolume=False, Vi=F(0), referenceVolumes=None, useCRK=False, Ai=F(1),
+                           Bi=None, gradAi=None, gradBi=None, vel_i=v[i], referenceVelocities=v, individual_cs=True,
+                           cs_i=F(c[i]), referenceCs=c, outputValue=F(0))
+    names = dict(warpOperation=warpOperation, OperationProperties=OperationProperties,
+                 WarpOperation=types.SimpleNamespace(Divergence="Divergence", Interpolate="Interpolate", Gradient="Gradient"),
+                 GradientScheme=types.SimpleNamespace(Difference=1), SupportScheme=types.SimpleNamespace(Gather=0, SuperSymmetric=3),
+                 ViscositySwitchState=lambda **kw: SoA(**kw), CompressibleState=None, SimulationConfig=None,
+                 CompressibleSPHConfig=None, AdjacencyList=None, CompactHashMap=None, computeMWarp=None,
+                 computeVsigWarp=lambda *a, **k: torch.from_numpy(vsig), Union=Union, Tuple=Tuple, Dict=dict, Optional=Optional)
+    common = load(ref, "modules/shockCapturing/common.py", names)
+    names.update({k: common[k] for k in ("computeM", "computeShearTensor")})
+    cd_ns = load(ref, "modules/shockCapturing/CullenDehnen2010.py", names)
+    names.update({k: cd_ns[k] for k in ("computeR", "computeXi", "computeSecondOrderV", "compute_vsig")})
+    hop = load(ref, "modules/shockCapturing/CullenHopkins.py", names)
+    div_prev = (0.3 * rng.standard_normal(n)).astype(F)
+    ps = SoA(positions=torch.from_numpy(x), supports=torch.from_numpy(H), densities=torch.from_numpy(rho),
+             divergence=torch.from_numpy(div_prev), alpha0s=torch.from_numpy(alpha0), velocities=torch.from_numpy(v),
+             soundspeeds=torch.from_numpy(c))
+    swc = SoA(alpha_min=0.02, alpha_max=2.0, beta_xi=2.0, limitXi=False, correctVelocityGradient=False, beta_c=0.7, beta_d=0.05)
+    sim = SoA(kernel=types.SimpleNamespace(value=2), supportMode=3, domain=None)
+    sch = SoA(viscositySwitchParams=swc)
+    alphas, st = hop["computeHopkinsTerms"](float(dt), ps, sim, sch, None, None)
+    a0n, st2 = hop["computeHopkinsUpdate"](st, float(dt), torch.from_numpy(dvdt), ps, sim, sch, None, None)
+    return dict(hopkins_alpha0=alpha0, hopkins_div_prev=div_prev, hopkins_dt=np.array([dt], F),
+                hopkins_alphas=alphas.numpy().astype(F), hopkins_div=st.div.numpy().astype(F), hopkins_R=st.R.numpy().astype(F),
+                hopkins_Xi=st.Xi.numpy().astype(F), hopkins_alpha0_next=a0n.numpy().astype(F), hopkins_vsig=np.abs(vsig))
+
+
 # ---------------------------------------------------------------- Owen adaptive support
 def _eval_C_d(dim, kernel):
     return kernel_C(int(kernel), int(dim))
@@ -835,7 +924,7 @@ def run_reference_owen(ref: Path) -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph", "owen"], default="all")
+    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph", "owen", "hopkins"], default="all")
     a = ap.parse_args()
     ref = Path(a.reference)
     if a.which in ("all", "crk"):
@@ -866,6 +955,11 @@ def main():
                             P=case["P"], c=case["c"], offsets=nb["offsets"], counts=nb["counts"], list=nb["list"],
                             pi_sel=case["pi_sel"], pi_variants=PI_VARIANTS, pi_coeffs=PI_COEFFS, **out)
         print("wrote", Path(__file__).parent / "compsph_golden.npz", "particles", case["n"], "pairs", len(nb["list"]))
+    if a.which in ("all", "hopkins"):
+        g = dict(np.load(Path(__file__).parent / "compsph_golden.npz"))
+        out = run_reference_hopkins(ref, g)
+        np.savez_compressed(Path(__file__).parent / "hopkins_golden.npz", **out)
+        print("wrote", Path(__file__).parent / "hopkins_golden.npz")
     if a.which in ("all", "owen"):
         out = run_reference_owen(ref)
         np.savez_compressed(Path(__file__).parent / "owen_golden.npz", **out)

@@ -14,7 +14,7 @@ import torch
 
 import warpsph_b200 as ws
 from oracle import oracle
-from oracle.steps import SWITCH_CULLEN, SWITCH_NONE, CompSPHOracle, MonaghanOracle, cell_capacity_for, state_to_numpy
+from oracle.steps import SWITCH_CULLEN, SWITCH_HOPKINS, SWITCH_NONE, CompSPHOracle, MonaghanOracle, cell_capacity_for, state_to_numpy
 from tests.cases import assert_close, make_params, make_particles
 from warpsph_b200 import core, ops
 from warpsph_b200.core import AdjacencyList
@@ -185,13 +185,16 @@ def sedov(nx, dev, scheme_name="compSPH", switch=ws.ViscositySwitch.CullenDehnen
     return cfg, sch, integrator, step, system
 
 
-@pytest.mark.parametrize("switch", [ws.ViscositySwitch.CullenDehnen2010, ws.ViscositySwitch.NoneSwitch])
+SWITCHES = {ws.ViscositySwitch.CullenDehnen2010: SWITCH_CULLEN, ws.ViscositySwitch.CullenHopkins: SWITCH_HOPKINS,
+            ws.ViscositySwitch.NoneSwitch: SWITCH_NONE}
+
+
+@pytest.mark.parametrize("switch", list(SWITCHES))
 def test_compsph_step_matches_oracle(cuda, switch):
     cfg, sch, integ, step, system = sedov(32, cuda, "compSPH", switch)
     dt = 2e-4
     st = state_to_numpy(system.state)
-    orc = CompSPHOracle(ws.make_params(cfg, sch), "f32", switch=SWITCH_CULLEN if switch == ws.ViscositySwitch.CullenDehnen2010
-                        else SWITCH_NONE)
+    orc = CompSPHOracle(ws.make_params(cfg, sch), "f32", switch=SWITCHES[switch])
     for k in range(3):
         system = integ.function(state=system, f=step, dt=dt, config=cfg, compParams=sch).state
         st, _, _ = orc.step(st, dt, "rungeKutta2")
@@ -202,7 +205,27 @@ def test_compsph_step_matches_oracle(cuda, switch):
         assert_close(S.internalEnergies.cpu().numpy(), st["internalEnergies"], tol, tol, f"u step {k}")
         assert_close(S.densities.cpu().numpy(), st["densities"], 1e-5, 1e-5, f"rho step {k}")
         assert_close(S.alphas.cpu().numpy(), st["alphas"], 1e-3, 1e-3, f"alpha step {k}")
+        assert_close(S.alpha0s.cpu().numpy(), st["alpha0s"], 1e-3, 1e-3, f"alpha0 step {k}")
     assert np.abs(st["velocities"]).max() > 0.1
+
+
+def test_gpu_hopkins_switch_matches_reference(G):
+    """The Cullen-Hopkins kernels against the reference's CullenHopkins.py (golden)."""
+    t, g = G
+    h = dict(np.load(GOLD.parent / "hopkins_golden.npz"))
+    p = params_for(g)
+    p.alpha_min, p.alpha_max, p.beta_xi, p.limit_xi, p.beta_c, p.beta_d = 0.02, 2.0, 2.0, 0, 0.7, 0.05
+    a0 = torch.from_numpy(h["hopkins_alpha0"]).to(t["x"].device)
+    for adj in (verlet_adjacency(t), built_adjacency(p, t["x"], t["H"])):
+        al, div, s2, R = ops.switch_hopkins_terms(p, t["x"], t["H"], t["m"], t["rho"], t["v"], a0, adj)
+        assert_close(div.cpu().numpy(), h["hopkins_div"], 1e-4, 1e-5, "divergence (GPU)")
+        assert_close(R.cpu().numpy(), h["hopkins_R"], 1e-4, 1e-5, "R (GPU)")
+        assert_close(al.cpu().numpy(), h["hopkins_alphas"], 1e-3, 1e-4, "alphas (GPU)")
+        nxt, vs = ops.switch_hopkins_update(p, t["x"], t["H"], t["v"], t["c"], div,
+                                            torch.from_numpy(h["hopkins_div_prev"]).to(a0.device), a0, float(h["hopkins_dt"][0]),
+                                            adj, want_vsig=True)
+        assert_close(vs.cpu().numpy(), h["hopkins_vsig"], 1e-5, 1e-6, "v_sig (GPU)")
+        assert_close(nxt.cpu().numpy(), h["hopkins_alpha0_next"], 1e-3, 1e-4, "alpha0 update (GPU)")
 
 
 def test_monaghan_step_matches_oracle(cuda):

@@ -44,7 +44,8 @@ class SphParams(C.Structure):
         ("target_neighbors", C.c_double),
         ("cfl", C.c_double), ("min_dt", C.c_double), ("max_dt", C.c_double), ("dt_growth", C.c_double),
         ("c_s", C.c_double),
-        ("reserved_d", C.c_double * 7),
+        ("beta_c", C.c_double), ("beta_d", C.c_double),
+        ("reserved_d", C.c_double * 5),
         ("dim", C.c_int32),
         ("kernel", C.c_int32),
         ("periodic", C.c_int32 * 3),
@@ -111,6 +112,8 @@ _PROTOS = {
     "sph_grad_v": [_P, _I64] + [_P] * 19,
     "sph_switch_cullen": [_P, _I64] + [_P] * 18,
     "sph_switch_balsara": [_P, _I64, _P, _P, _P, _P],
+    "sph_switch_hopkins_terms": [_P, _I64] + [_P] * 14,
+    "sph_switch_hopkins_update": [_P, _I64] + [_P] * 14,
     "sph_crk_accel_dudt": [_P, _I64] + [_P] * 23,
     "sph_crk_accel": [_P, _I64] + [_P] * 21,
     "sph_crk_dudt": [_P, _I64] + [_P] * 18,

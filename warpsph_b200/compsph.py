@@ -34,6 +34,11 @@ def _no_boundaries(compParams) -> None:
         raise NotImplementedError("boundary conditions are outside the GPU hot path")
 
 
+def _hopkins_supported(compParams) -> None:
+    if compParams.viscositySwitchParams.correctVelocityGradient:
+        raise NotImplementedError("the Cullen-Hopkins switch with correctVelocityGradient is not implemented on the GPU path")
+
+
 def compSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams: CompSPHConfig, verbose: bool = False):
     """schemes/compSPH.py:22-215 on the GPU.  Returns (update, adjacency, state).
 
@@ -65,19 +70,29 @@ def compSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams
     cullen = switch == ViscositySwitch.CullenDehnen2010
     omega, div, drhodt = ops.compsph_prep(params, S.positions, S.supports, S.masses, S.densities, S.velocities, adjacency,
                                           grad_h=bool(compParams.adaptiveSupportCorrections), want_div=cullen)
-    # compSPH.py:105-110 (computeCullenTerms returns the updated alpha0 as the alphas)
+    # compSPH.py:105-110 (computeCullenTerms returns the updated alpha0 as the alphas;
+    # computeHopkinsTerms returns max(Xi alpha0, alpha_min))
+    hopkins = switch == ViscositySwitch.CullenHopkins
     if cullen:
         alphas, _, _ = ops.switch_cullen(params, S.positions, S.supports, S.masses, S.densities, div, S.divergence, None,
                                          S.alpha0s, dt, adjacency, v=S.velocities, c=S.soundspeeds)
         S.alphas = alphas
+    elif hopkins:
+        _hopkins_supported(compParams)
+        S.alphas, hop_div, _, _ = ops.switch_hopkins_terms(params, S.positions, S.supports, S.masses, S.densities, S.velocities,
+                                                           S.alpha0s, adjacency)
     elif switch != ViscositySwitch.NoneSwitch:
         raise NotImplementedError(f"viscosity switch {switch} is not implemented on the GPU path")
     # compSPH.py:113-149 and :170
     dvdt, dudt, dEdt, S.ap_ij, S.av_ij = ops.compsph_accel_dudt(params, S.positions, S.supports, S.masses, S.densities, S.velocities,
                                                                 S.soundspeeds, S.alphas, S.pressures, omega, adjacency)
-    # compSPH.py:153-159 (computeCullenUpdate hands back the same alpha0)
+    # compSPH.py:153-159 (computeCullenUpdate hands back the same alpha0; computeHopkinsUpdate
+    # relaxes alpha0 with the divergence of the previous step, CullenHopkins.py:48-149)
     if cullen:
         S.alpha0s = S.alphas
+    elif hopkins:
+        S.alpha0s, _ = ops.switch_hopkins_update(params, S.positions, S.supports, S.velocities, S.soundspeeds, hop_div, S.divergence,
+                                                 S.alpha0s, dt, adjacency)
     # compSPH.py:169
     S.divergence = -drhodt / S.densities
     update = CompressibleSystemUpdate(dxdt=S.velocities.clone(), dvdt=dvdt, dudt=dudt, drhodt=drhodt, dEdt=dEdt,

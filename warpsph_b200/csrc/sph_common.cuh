@@ -30,6 +30,7 @@ struct DevParams {
     float target_neighbors;
     float cfl, min_dt, max_dt, dt_growth;
     float c_s;      // sound speed of the viscosity terms without per-particle sound speeds
+    float beta_c, beta_d;
     int conductivity_term;
     float kscale;   // H / h  (kernel scale)
     float kxi;      // the kernel "xi" used by CFL, viscosity and switches

@@ -92,6 +92,7 @@ int params_to_dev(const SphParams* p, DevParams* o) {
     o->target_neighbors = (float)p->target_neighbors;
     o->cfl = (float)p->cfl; o->min_dt = (float)p->min_dt; o->max_dt = (float)p->max_dt; o->dt_growth = (float)p->dt_growth;
     o->c_s = (float)p->c_s;
+    o->beta_c = (float)p->beta_c; o->beta_d = (float)p->beta_d;
     o->conductivity_term = p->conductivity_term;
     if (p->viscosity_term < SPH_VISC_DEFAULT || p->viscosity_term > SPH_VISC_DELTASPH)
         return set_error(SPH_ERR_BAD_ARG, "viscosity_term %d out of range", p->viscosity_term);

@@ -515,6 +515,149 @@ k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restric
     if (R_out) R_out[i] = R;
 }
 
+// ---------------------------------------------------------------- Cullen-Hopkins switch
+// modules/shockCapturing/CullenHopkins.py:7-45 (computeHopkinsTerms, without the optional
+// velocity-gradient correction): the gather difference gradient
+// V_i = sum_j m_j/rho_j (v_j - v_i) (x) grad W(r_ij, H_i) (computeShearTensor, common.py:30-58),
+// its trace (the divergence) and |S|^2 = tr(S S^T) of the traceless symmetric part S.
+template <int KF, int D, int G>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_hopkins_grad(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+               const float* __restrict__ rho, const float* __restrict__ v,
+               const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+               float* __restrict__ div_out, float* __restrict__ shear2_out) {
+    Grp<G> g(n);
+    Mat<D> Gm = mzero<D>();
+    if (g.valid) {
+        const int i = g.i;
+        Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
+        const float invHi = 1.f / H[i];
+        int b = offs[i], e = b + cnt[i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry(list, q, j, k);
+            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float r = safe_sqrt(dot<D>(xij, xij));
+            float W; Vec<D> gW;
+            kWG_inv<KF, D>(xij, r, invHi, W, gW);
+            if (W == 0.f) continue;
+            const float Vj = __ldg(m + j) / __ldg(rho + j);
+            Vec<D> vj = load_vec<D>(v, j);
+            #pragma unroll
+            for (int a = 0; a < D; ++a) {
+                const float dv = Vj * (vj.v[a] - vi.v[a]);
+                #pragma unroll
+                for (int w = 0; w < D; ++w) Gm.m[a][w] += dv * gW.v[w];
+            }
+        }
+    }
+    #pragma unroll
+    for (int a = 0; a < D; ++a)
+        #pragma unroll
+        for (int w = 0; w < D; ++w) Gm.m[a][w] = gsum<G>(Gm.m[a][w]);
+    if (!g.valid || g.lane != 0) return;
+    float tr = Gm.m[0][0];
+    #pragma unroll
+    for (int a = 1; a < D; ++a) tr += Gm.m[a][a];
+    float s2 = 0.f;
+    #pragma unroll
+    for (int a = 0; a < D; ++a)
+        #pragma unroll
+        for (int w = 0; w < D; ++w) {
+            float sv = (Gm.m[a][w] + Gm.m[w][a]) / 2.f - (a == w ? tr / (float)D : 0.f);
+            s2 += sv * sv;
+        }
+    div_out[g.i] = tr;
+    shear2_out[g.i] = s2;
+}
+
+// R (CullenDehnen2010.py:121-164, gather), Xi with the shear term (:166-191) and
+// alpha = max(Xi alpha0, alpha_min) (CullenHopkins.py:25).
+template <int KF, int D, int G>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_hopkins_alpha(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+                const float* __restrict__ rho, const float* __restrict__ div, const float* __restrict__ shear2,
+                const float* __restrict__ alpha0, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
+                const int32_t* __restrict__ list, float* __restrict__ alpha_out, float* __restrict__ R_out) {
+    Grp<G> g(n);
+    float s = 0.f;
+    if (g.valid) {
+        const int i = g.i;
+        Vec<D> xi = load_vec<D>(x, i);
+        const float invHi = 1.f / H[i];
+        int b = offs[i], e = b + cnt[i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry(list, q, j, k);
+            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float W = kW_inv<KF, D>(safe_sqrt(dot<D>(xij, xij)), invHi);
+            if (W == 0.f) continue;
+            float dj = __ldg(div + j);
+            float sg = dj > 0.f ? 1.f : (dj < 0.f ? -1.f : 0.f);
+            s += __ldg(m + j) * sg * W;
+        }
+    }
+    s = gsum<G>(s);
+    if (!g.valid || g.lane != 0) return;
+    const int i = g.i;
+    const float Hi = H[i];
+    const float R = 1.f / rho[i] * s;
+    const float omr = 1.f - R, omr2 = omr * omr;
+    const float nom = P.beta_xi * (omr2 * omr2) * div[i];
+    const float Xi = P.limit_xi ? (nom * nom + 1e-14f * Hi) / (nom * nom + shear2[i] + 1e-14f * Hi)
+                                : (nom * nom) / (nom * nom + shear2[i] + 1e-14f * Hi);
+    alpha_out[i] = fmaxf(Xi * alpha0[i], P.alpha_min);
+    if (R_out) R_out[i] = R;
+}
+
+// computeHopkinsUpdate (CullenHopkins.py:48-149): v_sig over the Verlet rows
+// (wp_vsig.py:55-90), d(div)/dt = (div - div_prev) / dt, the local alpha_tmp and the
+// relaxation of alpha0 towards it.
+template <int D, int G>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_hopkins_update(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ v,
+                 const float* __restrict__ c, const float* __restrict__ div, const float* __restrict__ div_prev,
+                 const float* __restrict__ alpha0, const float* __restrict__ dtp,
+                 const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+                 float* __restrict__ alpha0_out, float* __restrict__ vsig_out) {
+    Grp<G> g(n);
+    float vsig = 0.f;
+    if (g.valid) {
+        const int i = g.i;
+        Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
+        const float Hi = H[i], ci = c[i];
+        int b = offs[i], e = b + cnt[i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry(list, q, j, k);
+            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float r = safe_sqrt(dot<D>(xij, xij));
+            if (!(r < P.verlet_scale * wmax(Hi, __ldg(H + j)))) continue;
+            Vec<D> vj = load_vec<D>(v, j);
+            float mu = 0.f;
+            #pragma unroll
+            for (int a = 0; a < D; ++a) mu += (vi.v[a] - vj.v[a]) * xij.v[a];
+            mu = mu / (r + 1e-14f * Hi);
+            float vsv = 0.5f * (ci + __ldg(c + j)) - mu;
+            if (mu > 0.f) vsv = 0.f;
+            vsig = wmax(vsig, vsv);
+        }
+    }
+    vsig = gmaxw<G>(vsig);
+    if (!g.valid || g.lane != 0) return;
+    const int i = g.i;
+    const float vs = fabsf(vsig);
+    const float dt = *dtp;
+    const float Hi = H[i], ci = c[i], dv = div[i];
+    const float f_kern = 1.f / P.kxi;
+    const float ddiv = (dv - div_prev[i]) / dt;
+    const float ad = fabsf(ddiv);
+    const float fh = f_kern * Hi;
+    float at = P.alpha_max * ad / (ad + P.beta_c * (ci * ci) / (fh * fh) + 1e-14f);
+    if (ddiv > 0.f || dv > 0.f) at = 0.f;
+    const float a0 = alpha0[i];
+    const float next = at + (a0 - at) * expf(-P.beta_d * dt * vs / (2.f * f_kern * Hi));
+    alpha0_out[i] = at >= a0 ? at : next;
+    if (vsig_out) vsig_out[i] = vs;
+}
+
 // Balsara switch from the velocity gradient (schemes/crkSPH.py:132-133 comment).
 template <int D>
 __global__ void k_balsara(int n, const float* __restrict__ DvDx, const float* __restrict__ c, float* __restrict__ alpha) {
@@ -1051,6 +1194,37 @@ int sph_switch_cullen(const SphParams* p, int64_t n, const float* x, const float
     WSPH_DISPATCH_KDS(*p, (k_cullen<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div, div_prev, vsig, v, c,
                                                                                                   alpha0_prev, dt, offs, cnt, list, alpha_out, R_out, vsig_out)));
     return check_launch("sph_switch_cullen");
+}
+
+int sph_switch_hopkins_terms(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
+                             const float* v, const float* alpha0, const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                             float* div_out, float* shear2_out, float* alpha_out, float* R_out, void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(alpha0);
+    WSPH_CHECK_PTR(div_out); WSPH_CHECK_PTR(shear2_out); WSPH_CHECK_PTR(alpha_out); CHECK_CSR();
+    if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v"))) return rc;
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_hopkins_grad<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, v, offs, cnt, list,
+                                                                                                       div_out, shear2_out)));
+    if ((rc = check_launch("sph_switch_hopkins_terms"))) return rc;
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_hopkins_alpha<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div_out, shear2_out,
+                                                                                                        alpha0, offs, cnt, list, alpha_out, R_out)));
+    return check_launch("sph_switch_hopkins_terms");
+}
+
+int sph_switch_hopkins_update(const SphParams* p, int64_t n, const float* x, const float* H, const float* v, const float* c,
+                              const float* div, const float* div_prev, const float* alpha0, const float* dt,
+                              const int32_t* offs, const int32_t* cnt, const int32_t* list, float* alpha0_out, float* vsig_out,
+                              void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(c); WSPH_CHECK_PTR(div); WSPH_CHECK_PTR(div_prev);
+    WSPH_CHECK_PTR(alpha0); WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(alpha0_out); CHECK_CSR();
+    if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v"))) return rc;
+    wsph::count_launch();
+    WSPH_DISPATCH_DS(*p, (k_hopkins_update<D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, v, c, div, div_prev, alpha0, dt,
+                                                                                                  offs, cnt, list, alpha0_out, vsig_out)));
+    return check_launch("sph_switch_hopkins_update");
 }
 
 int sph_switch_balsara(const SphParams* p, int64_t n, const float* DvDx, const float* c, float* alpha_out, void* stream) {

@@ -358,6 +358,29 @@ def switch_cullen(params, x, H, m, rho, div, div_prev, vsig, alpha0, dt, adj: Ad
     return al, R, vs_out
 
 
+def switch_hopkins_terms(params, x, H, m, rho, v, alpha0, adj: AdjacencyList):
+    """Cullen-Hopkins switch terms: (alphas, div, |S|^2, R)."""
+    n = H.shape[0]
+    al, div, s2, R = _empty(n, H), _empty(n, H), _empty(n, H), _empty(n, H)
+    with _timed("switch_hopkins_terms"):
+        check(_capi.lib().sph_switch_hopkins_terms(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(v), fptr(_f32(alpha0)),
+                                                   *_lists(params, adj, True), ptr(div), ptr(s2), ptr(al), ptr(R),
+                                                   stream_ptr(H.device)), "sph_switch_hopkins_terms")
+    return al, div, s2, R
+
+
+def switch_hopkins_update(params, x, H, v, c, div, div_prev, alpha0, dt, adj: AdjacencyList, want_vsig: bool = False):
+    """Cullen-Hopkins alpha0 update (v_sig over the Verlet rows); (alpha0, v_sig or None)."""
+    n = H.shape[0]
+    a0 = _empty(n, H)
+    vs = _empty(n, H) if want_vsig else None
+    with _timed("switch_hopkins_update"):
+        check(_capi.lib().sph_switch_hopkins_update(_p(params), n, fptr(x), fptr(H), fptr(v), fptr(c), fptr(div), fptr(_f32(div_prev)),
+                                                    fptr(_f32(alpha0)), fptr(dt_tensor(dt, H.device)), *_lists(params, adj, False),
+                                                    ptr(a0), ptr(vs), stream_ptr(H.device)), "sph_switch_hopkins_update")
+    return a0, vs
+
+
 def switch_balsara(params, DvDx, c):
     n = c.shape[0]
     al = _empty(n, c)
