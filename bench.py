@@ -53,6 +53,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched delta-SPH ensemble")
     ap.add_argument("--no-compsph", action="store_true", help="skip the CompSPH Sedov 2D throughput")
     ap.add_argument("--no-sedov3d", action="store_true", help="skip the CRKSPH Sedov 3D (128^3) throughput")
+    ap.add_argument("--no-mlp", action="store_true", help="skip the warm-start MLP forward throughput")
     return ap.parse_args(argv)
 
 
@@ -287,6 +288,37 @@ def ensemble_throughput(dev, chunks: int = 6) -> dict:
             "status": E.status(), "wall_s": time.perf_counter() - t0}
 
 
+def mlp_forward_throughput(dev, n: int = 1 << 24, reps: int = 20) -> dict:
+    """The warm-start network's forward pass on n feature rows (n x 32 B, larger than L2)
+    through both tensor-core kernels: tcgen05 (TMEM accumulators) and mma.sync."""
+    import torch
+    from warpsph_b200 import learned, ops
+    peaks = load_peaks()
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    theta = learned.WarmStartMLP(dev, seed=7).theta
+    feats = torch.randn((n, 8), device=dev, generator=g)
+    flops = 2.0 * (8 * 64 + 2 * 64 * 64 + 64)     # per sample, without the K padding
+    out = {"samples": n, "flop_per_sample": flops, "peak_bf16_tflops": peaks["bf16_tflops"], "peak_source": peaks["source"]}
+    for tc in ("tcgen05", "mma"):
+        for _ in range(3):
+            ops.mlp_forward(theta, feats, tensor_cores=tc)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            ops.mlp_forward(theta, feats, tensor_cores=tc)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        tf = n * flops / (ms * 1e-3) / 1e12
+        out[tc] = {"ms": ms, "samples_per_s": n / (ms * 1e-3), "tflops": tf, "frac": tf / peaks["bf16_tflops"]}
+    st = int(ops.mlp_status(dev).item())
+    if st:
+        raise RuntimeError(f"sph_mlp_forward_tc reported status {st:#x}")
+    return out
+
+
 def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, steps: int, warmup: int, kahan: bool = False,
                       timed_kernel: str = None, bytes_per_particle: float = None) -> dict:
     """particle-steps/s of one compressible scheme on the Sedov blast (device-resident,
@@ -490,6 +522,9 @@ def gpu_arm(args, rank: int, world: int):
     if rank == 0 and world == 1 and not args.no_ensemble:
         ens = ensemble_throughput(dev)
 
+    mlp = None
+    if rank == 0 and world == 1 and not args.no_mlp:
+        mlp = mlp_forward_throughput(dev)
     comp = None
     if rank == 0 and world == 1 and not args.no_compsph:
         d, K = 2, 32.0
@@ -513,7 +548,7 @@ def gpu_arm(args, rank: int, world: int):
                 "config": {"workload": WORKLOAD, "particles": n, "nx": args.nx, "parallelism": f"replicas x{world}",
                            "l2": "working set larger than L2 (pair arrays ~0.7 GB per step), no flush needed"},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
-                "dfsph_warm_start": dfsph, "ensemble": ens, "compsph": comp, "sedov3d": s3}
+                "dfsph_warm_start": dfsph, "ensemble": ens, "compsph": comp, "sedov3d": s3, "mlp_forward": mlp}
         if breakdown is not None:
             line["breakdown_ms"] = {k: round(v["total_ms"] / 3, 4) for k, v in breakdown.items()}
         print(json.dumps(line), flush=True)

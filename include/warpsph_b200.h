@@ -623,6 +623,14 @@ int sph_dfsph_features(const SphParams* p, const SphJacobiConfig* cfg, int32_t m
 int sph_mlp_forward(const float* params, int64_t n, const float* feats, const float* scale,
                     float* out, void* stream);
 
+/* The same network on the Blackwell tensor cores (tcgen05.mma kind::f16, accumulators in
+ * TMEM): 128 samples per CTA tile, the same BF16 rounding points as sph_mlp_forward.
+ * feats must be 16-byte aligned.  If a tensor-core chain does not complete within about
+ * a second the kernel gives up: the samples it had not finished get NaN and
+ * SPH_STATUS_TIMEOUT is or-ed into *status (device int32; may be null). */
+int sph_mlp_forward_tc(const float* params, int64_t n, const float* feats, const float* scale,
+                       float* out, int32_t* status, void* stream);
+
 /* Gradient of the mean squared error (1/n) sum_i (MLP(feats_i) - target_i)^2 with
  * respect to the parameters: grad [SPH_MLP_PARAM_COUNT] is overwritten, *loss receives
  * sum_i (MLP(feats_i) - target_i)^2 (device double). */

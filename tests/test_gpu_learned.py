@@ -35,18 +35,51 @@ def random_net(seed):
     return th.astype(np.float32)
 
 
-@pytest.mark.parametrize("n", [1, 37, 1000, 20000])
-def test_mlp_forward_matches_oracle(cuda, n):
+@pytest.mark.parametrize("tensor_cores", ["tcgen05", "mma"])
+@pytest.mark.parametrize("n", [1, 37, 128, 129, 1000, 20000, 200003])
+def test_mlp_forward_matches_oracle(cuda, n, tensor_cores):
+    """Both forward kernels against the oracle; 200003 samples give the tcgen05 kernel
+    several 128-sample tiles per CTA and a ragged last tile."""
     rng = np.random.default_rng(n)
     th = random_net(1)
     x = rng.standard_normal((n, 8)).astype(np.float32)
     ref, _ = omlp.forward(th, x)
-    out = ops.mlp_forward(torch.from_numpy(th).to(cuda), torch.from_numpy(x).to(cuda))
-    assert_close(out.cpu().numpy(), ref, 1e-2, 1e-2, "MLP forward vs oracle")
+    st = ops.mlp_status(cuda)
+    st.zero_()
+    out = ops.mlp_forward(torch.from_numpy(th).to(cuda), torch.from_numpy(x).to(cuda), tensor_cores=tensor_cores)
+    assert int(st.item()) == 0
+    assert_close(out.cpu().numpy(), ref, 1e-2, 1e-2, f"MLP forward ({tensor_cores}) vs oracle")
     assert np.median(np.abs(out.cpu().numpy() - ref)) <= 1e-3 * np.abs(ref).max()
     sc = torch.tensor([2.5], device=cuda)
-    out2 = ops.mlp_forward(torch.from_numpy(th).to(cuda), torch.from_numpy(x).to(cuda), sc)
+    out2 = ops.mlp_forward(torch.from_numpy(th).to(cuda), torch.from_numpy(x).to(cuda), sc, tensor_cores=tensor_cores)
     assert torch.allclose(out2, 2.5 * out, rtol=1e-6, atol=0)
+    assert int(st.item()) == 0
+
+
+def test_mlp_forward_tcgen05_matches_mma(cuda):
+    """The two tensor-core paths round at the same points; they differ only in the FP32
+    accumulation order, which can flip a BF16 activation now and then."""
+    rng = np.random.default_rng(5)
+    th = torch.from_numpy(random_net(3)).to(cuda)
+    x = torch.from_numpy(rng.standard_normal((50000, 8)).astype(np.float32)).to(cuda)
+    a = ops.mlp_forward(th, x, tensor_cores="tcgen05")
+    b = ops.mlp_forward(th, x, tensor_cores="mma")
+    d = (a - b).abs()
+    scale = b.abs().max()
+    assert float(d.max()) <= 1e-2 * float(scale)
+    assert float(d.median()) <= 1e-4 * float(scale)
+
+
+def test_mlp_forward_tc_rejects_misaligned_features(cuda):
+    th = torch.from_numpy(random_net(1)).to(cuda)
+    buf = torch.zeros(8 * 64 + 2, device=cuda)
+    feats = buf[2:].view(64, 8)
+    out = torch.empty(64, device=cuda)
+    rc = _capi.lib().sph_mlp_forward_tc(th.data_ptr(), 64, feats.data_ptr(), None, out.data_ptr(), None, None)
+    assert rc == _capi.SPH_ERR_BAD_ARG
+    # the Python wrapper copies such a view to an aligned buffer
+    ref = ops.mlp_forward(th, feats.clone())
+    assert torch.equal(ops.mlp_forward(th, feats), ref)
 
 
 @pytest.mark.parametrize("n", [16, 333, 5000])

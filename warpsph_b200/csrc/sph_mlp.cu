@@ -19,6 +19,7 @@
 #include <cstdint>
 #include <mutex>
 #include "sph_common.cuh"
+#include "sph_tcgen05.cuh"
 
 namespace wsph {
 
@@ -348,6 +349,184 @@ __global__ void k_mlp_adam(float* __restrict__ prm, const float* __restrict__ gr
     }
 }
 
+// ---------------------------------------------------------------- inference on tcgen05
+// One CTA of 4 warps takes 128 samples per tile.  Each layer is one chain of
+//   D[128 x 64] (TMEM, FP32) = A[128 x K] (shared, BF16) x W[64 x K]^T (shared, BF16)
+// of K/16 tcgen05.mma kind::f16 instructions, issued by one thread and completed through
+// tcgen05.commit on an mbarrier.  Warp w then reads TMEM lanes 32w..32w+31 (one sample
+// per thread, tcgen05.ld 32x32b), applies ReLU while rounding to BF16 (cvt.rn.relu) and
+// writes the operand of the next layer back to shared memory; the 64 -> 1 output layer
+// is an FP32 dot product in registers.
+//
+// The biases ride in the contraction: A carries two constant-one columns after its real K
+// columns (X columns 8, 9; H columns 64, 65) and W the bias split into BF16 hi + lo parts
+// in the matching columns, so the FP32 accumulator receives b_hi + b_lo, which equals the
+// FP32 bias to about 2^-17 relative.  The hidden layers thus run K = 80 (five k-steps).
+// Rounding points otherwise match k_mlp_forward: BF16 features, weights and hidden
+// activations, FP32 accumulation, FP32 output layer.
+constexpr int TC_M = 128, TC_THREADS = 128, TC_TMEM_COLS = 64, TC_CTAS_PER_SM = 4;
+constexpr int TC_K2 = MLP_H + 16;   // hidden-layer K with the bias columns
+constexpr uint32_t TC_IDESC = umma_idesc_bf16_f32<TC_M, MLP_H>();
+static_assert(TC_IDESC == 0x08100490u, "kind::f16 descriptor: BF16 x BF16 -> FP32, M = 128, N = 64, K-major");
+constexpr long long TC_WAIT_CYCLES = 1ll << 31;   // about a second at B200 clocks
+
+struct MlpTcSmem {
+    __nv_bfloat16 W1[MLP_H * K1];      // [64 x 16]: W1 | b1 hi | b1 lo | 0
+    __nv_bfloat16 W2[MLP_H * TC_K2];   // [64 x 80]: W2 | b2 hi | b2 lo | 0
+    __nv_bfloat16 W3[MLP_H * TC_K2];
+    __nv_bfloat16 X[TC_M * K1];        // [128 x 16]: features | 1 | 1 | 0
+    __nv_bfloat16 H[TC_M * TC_K2];     // [128 x 80]: activations | 1 | 1 | 0
+    float w4[MLP_H];
+    unsigned long long bar;
+    float b4;
+    uint32_t tmem_base;
+    int abort;
+};
+static_assert((sizeof(__nv_bfloat16) * MLP_H * K1) % 128 == 0 && (sizeof(__nv_bfloat16) * MLP_H * TC_K2) % 128 == 0 &&
+              (sizeof(__nv_bfloat16) * TC_M * K1) % 128 == 0 && (sizeof(__nv_bfloat16) * TC_M * TC_K2) % 128 == 0,
+              "128 B aligned operands");
+// 4 CTAs fit in shared memory per SM; their TMEM columns must fit in the SM's 512.
+static_assert(4 * TC_TMEM_COLS <= 512 && 5 * sizeof(MlpTcSmem) > 228 * 1024, "TMEM columns of the resident CTAs");
+
+// relu of (lo, hi) rounded to BF16 and packed, lo in the low half
+__device__ __forceinline__ uint32_t relu_bf16x2(uint32_t lo, uint32_t hi) {
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(__uint_as_float(hi)), "f"(__uint_as_float(lo)));
+    return d;
+}
+// Column `part` of the bias block: 0 -> BF16 hi part of b, 1 -> BF16 lo part
+// (hi + lo reproduces b to about 2^-17 relative), 2.. -> 0.
+__device__ __forceinline__ __nv_bfloat16 bias_part(float b, int part) {
+    const __nv_bfloat16 hi = __float2bfloat16_rn(b);
+    return part == 0 ? hi : part == 1 ? __float2bfloat16_rn(b - __bfloat162float(hi)) : __float2bfloat16_rn(0.f);
+}
+
+__global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM)
+k_mlp_forward_tc(const float* __restrict__ prm, int64_t n, const float* __restrict__ feats, const float* __restrict__ scale,
+                 float* __restrict__ out, int32_t* __restrict__ status) {
+    __shared__ __align__(128) MlpTcSmem s;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (warp == 0) {
+        tmem_alloc(smem_u32(&s.tmem_base), TC_TMEM_COLS);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(smem_u32(&s.bar), 1);
+        s.abort = 0;
+        fence_mbar_init();
+    }
+    // weights in the K-major core-matrix layout (B operands: rows = output units)
+    for (int t = tid; t < MLP_H * K1; t += TC_THREADS) {
+        const int r = t / K1, k = t % K1;
+        s.W1[umma_k_index(r, k, MLP_H)] = k < MLP_IN ? __float2bfloat16_rn(prm[OFF_W1 + r * MLP_IN + k])
+                                                     : bias_part(prm[OFF_B1 + r], k - MLP_IN);
+    }
+    for (int t = tid; t < MLP_H * TC_K2; t += TC_THREADS) {
+        const int r = t / TC_K2, k = t % TC_K2;
+        const bool w = k < MLP_H;
+        s.W2[umma_k_index(r, k, MLP_H)] = w ? __float2bfloat16_rn(prm[OFF_W2 + r * MLP_H + k]) : bias_part(prm[OFF_B2 + r], k - MLP_H);
+        s.W3[umma_k_index(r, k, MLP_H)] = w ? __float2bfloat16_rn(prm[OFF_W3 + r * MLP_H + k]) : bias_part(prm[OFF_B3 + r], k - MLP_H);
+    }
+    if (tid < MLP_H) s.w4[tid] = prm[OFF_W4 + tid];
+    if (tid == 0) s.b4 = prm[OFF_B4];
+    {   // the constant columns of this thread's rows of X and H, the same for every tile
+        const uint4 ones = make_uint4(pack_bf16(1.f, 1.f), 0u, 0u, 0u), zero = make_uint4(0u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(s.X + umma_k_index(tid, MLP_IN, TC_M)) = ones;
+        *reinterpret_cast<uint4*>(s.H + umma_k_index(tid, MLP_H, TC_M)) = ones;
+        *reinterpret_cast<uint4*>(s.H + umma_k_index(tid, MLP_H + 8, TC_M)) = zero;
+    }
+    fence_proxy_async_smem();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+
+    const uint32_t tbase = s.tmem_base;
+    const uint32_t tlane = tbase + (static_cast<uint32_t>(warp * 32) << 16);
+    const uint32_t bar = smem_u32(&s.bar);
+    const uint32_t aX = smem_u32(s.X), aH = smem_u32(s.H), aW1 = smem_u32(s.W1), aW2 = smem_u32(s.W2), aW3 = smem_u32(s.W3);
+    const uint32_t LBO_A = TC_M * 16, LBO_B = MLP_H * 16, SBO = 128;
+    const float sc = scale ? *scale : 1.f;
+    const int64_t ntiles = (n + TC_M - 1) / TC_M;
+    uint32_t phase = 0;
+    int64_t tile = blockIdx.x;
+    for (; tile < ntiles; tile += gridDim.x) {
+        const int64_t row = tile * TC_M + tid;
+        {   // layer-1 operand: this thread's sample, 8 features -> 8 BF16 (16 B)
+            float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f), f1 = f0;
+            if (row < n) {
+                f0 = __ldg(reinterpret_cast<const float4*>(feats + row * MLP_IN));
+                f1 = __ldg(reinterpret_cast<const float4*>(feats + row * MLP_IN) + 1);
+            }
+            *reinterpret_cast<uint4*>(s.X + umma_k_index(tid, 0, TC_M)) =
+                make_uint4(pack_bf16(f0.x, f0.y), pack_bf16(f0.z, f0.w), pack_bf16(f1.x, f1.y), pack_bf16(f1.z, f1.w));
+        }
+        fence_proxy_async_smem();
+        tc_fence_before_sync();
+        __syncthreads();
+        float y = 0.f;
+        #pragma unroll 1
+        for (int layer = 0; layer < 3; ++layer) {
+            if (tid == 0) {
+                tc_fence_after_sync();
+                if (layer == 0) {
+                    umma_bf16_ss(tbase, umma_desc_kmajor(aX, LBO_A, SBO), umma_desc_kmajor(aW1, LBO_B, SBO), TC_IDESC, 0u);
+                } else {
+                    const uint32_t aW = layer == 1 ? aW2 : aW3;
+                    #pragma unroll
+                    for (int ks = 0; ks < TC_K2 / 16; ++ks)
+                        umma_bf16_ss(tbase, umma_desc_kmajor(aH + ks * 2 * LBO_A, LBO_A, SBO), umma_desc_kmajor(aW + ks * 2 * LBO_B, LBO_B, SBO),
+                                     TC_IDESC, ks > 0 ? 1u : 0u);
+                }
+                umma_commit(bar);
+            }
+            const bool done = mbar_wait_bounded(bar, phase, TC_WAIT_CYCLES);
+            phase ^= 1u;
+            if (!done) s.abort = 1;
+            __syncthreads();
+            if (s.abort) break;
+            tc_fence_after_sync();
+            #pragma unroll
+            for (int cb = 0; cb < MLP_H; cb += 32) {
+                uint32_t v[32];
+                tmem_ld_32x32b_x32(tlane + cb, v);
+                tmem_ld_wait(v);
+                if (layer < 2) {
+                    #pragma unroll
+                    for (int g8 = 0; g8 < 4; ++g8) {
+                        const uint32_t* vb = v + 8 * g8;
+                        *reinterpret_cast<uint4*>(s.H + umma_k_index(tid, cb + 8 * g8, TC_M)) =
+                            make_uint4(relu_bf16x2(vb[0], vb[1]), relu_bf16x2(vb[2], vb[3]), relu_bf16x2(vb[4], vb[5]), relu_bf16x2(vb[6], vb[7]));
+                    }
+                } else {
+                    #pragma unroll
+                    for (int j = 0; j < 32; ++j) y = fmaf(fmaxf(__uint_as_float(v[j]), 0.f), s.w4[cb + j], y);
+                }
+            }
+            if (layer < 2) {
+                fence_proxy_async_smem();
+                tc_fence_before_sync();
+                __syncthreads();
+            }
+        }
+        if (s.abort) break;
+        if (row < n) out[row] = (y + s.b4) * sc;
+    }
+    if (s.abort) {
+        // a chain did not complete in time: the samples of this and later tiles get NaN
+        for (; tile < ntiles; tile += gridDim.x) {
+            const int64_t row = tile * TC_M + tid;
+            if (row < n) out[row] = __int_as_float(0x7fc00000);
+        }
+        if (tid == 0 && status) atomicOr(status, SPH_STATUS_TIMEOUT);
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after_sync();
+        tmem_dealloc(tbase, TC_TMEM_COLS);
+    }
+}
+
 static int train_smem_bytes() { return (int)sizeof(MlpSmemTrain); }
 
 }  // namespace wsph
@@ -368,6 +547,20 @@ int sph_mlp_forward(const float* params, int64_t n, const float* feats, const fl
     count_launch();
     k_mlp_forward<<<grid, MLP_THREADS, 0, WSPH_STREAM(stream)>>>(params, n, feats, scale, out);
     return check_launch("sph_mlp_forward");
+}
+
+int sph_mlp_forward_tc(const float* params, int64_t n, const float* feats, const float* scale, float* out, int32_t* status,
+                       void* stream) {
+    if (n < 0) return set_error(SPH_ERR_BAD_ARG, "sph_mlp_forward_tc: n < 0");
+    if (n == 0) return SPH_OK;
+    WSPH_CHECK_PTR(params); WSPH_CHECK_PTR(feats); WSPH_CHECK_PTR(out);
+    if (reinterpret_cast<uintptr_t>(feats) & 15) return set_error(SPH_ERR_BAD_ARG, "sph_mlp_forward_tc: feats must be 16-byte aligned");
+    const int64_t tiles = (n + TC_M - 1) / TC_M;
+    const int64_t cap = 148 * TC_CTAS_PER_SM;
+    const int grid = (int)(tiles < cap ? tiles : cap);
+    count_launch();
+    k_mlp_forward_tc<<<grid, TC_THREADS, 0, WSPH_STREAM(stream)>>>(params, n, feats, scale, out, status);
+    return check_launch("sph_mlp_forward_tc");
 }
 
 int sph_mlp_grad(const float* params, int64_t n, const float* feats, const float* target, float* grad, double* loss, void* stream) {

@@ -617,11 +617,36 @@ def dfsph_features(params, mode: int, cfg, x, H, m, rho, v, dvdt, p_prev, dt, ad
     return feats, scale
 
 
-def mlp_forward(theta, feats, scale=None) -> torch.Tensor:
+_mlp_status: dict = {}
+
+
+def mlp_status(device) -> torch.Tensor:
+    """The device int32 word into which sph_mlp_forward_tc ors SPH_STATUS_TIMEOUT."""
+    dev = torch.device(device)
+    st = _mlp_status.get(dev.index)
+    if st is None:
+        st = torch.zeros(1, dtype=torch.int32, device=dev)
+        _mlp_status[dev.index] = st
+    return st
+
+
+def mlp_forward(theta, feats, scale=None, tensor_cores: str = "tcgen05") -> torch.Tensor:
+    """MLP(feats) * scale.  tensor_cores "tcgen05" runs sph_mlp_forward_tc (TMEM
+    accumulators, 128-sample tiles); "mma" runs sph_mlp_forward (warp-level mma.sync)."""
     out = torch.empty(feats.shape[0], device=feats.device, dtype=torch.float32)
-    with _timed("mlp_forward"):
-        check(_capi.lib().sph_mlp_forward(fptr(theta), feats.shape[0], fptr(feats.contiguous()), ptr(scale), ptr(out),
-                                          stream_ptr(feats.device)), "sph_mlp_forward")
+    f = feats.contiguous()
+    if tensor_cores == "tcgen05":
+        if f.data_ptr() % 16:
+            f = f.clone()
+        with _timed("mlp_forward"):
+            check(_capi.lib().sph_mlp_forward_tc(fptr(theta), f.shape[0], fptr(f), ptr(scale), ptr(out), ptr(mlp_status(f.device)),
+                                                 stream_ptr(f.device)), "sph_mlp_forward_tc")
+    elif tensor_cores == "mma":
+        with _timed("mlp_forward"):
+            check(_capi.lib().sph_mlp_forward(fptr(theta), f.shape[0], fptr(f), ptr(scale), ptr(out), stream_ptr(f.device)),
+                  "sph_mlp_forward")
+    else:
+        raise ValueError(f"tensor_cores must be 'tcgen05' or 'mma', not {tensor_cores!r}")
     return out
 
 
