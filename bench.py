@@ -54,6 +54,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-compsph", action="store_true", help="skip the CompSPH Sedov 2D throughput")
     ap.add_argument("--no-sedov3d", action="store_true", help="skip the CRKSPH Sedov 3D (128^3) throughput")
     ap.add_argument("--no-mlp", action="store_true", help="skip the warm-start MLP forward throughput")
+    ap.add_argument("--nx3d", type=int, default=128, help="lattice size of the CRKSPH Sedov 3D section (nx^3 particles)")
     return ap.parse_args(argv)
 
 
@@ -320,7 +321,7 @@ def mlp_forward_throughput(dev, n: int = 1 << 24, reps: int = 20) -> dict:
 
 
 def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, steps: int, warmup: int, kahan: bool = False,
-                      timed_kernel: str = None, bytes_per_particle: float = None) -> dict:
+                      timed_kernel: str = None, bytes_per_particle: float = None, breakdown: bool = False) -> dict:
     """particle-steps/s of one compressible scheme on the Sedov blast (device-resident,
     CUDA events, CFL dt on the device every step), the total-energy drift over the timed
     steps from the FP64 conservation sums, and the dominant pair kernel's average launch
@@ -377,6 +378,14 @@ def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, step
             out["kernel"] = {"name": timed_kernel, "avg_launch_ms": k["avg_ms"], "launches": k["launches"],
                              "algorithmic_bytes_per_particle": bytes_per_particle, "achieved_gbs": ach,
                              "frac_of_measured_hbm": ach / peaks["hbm_gbs"]}
+    if breakdown:
+        # one more step with CUDA events around every library call (after the timed region)
+        bt = ops.KernelTimer()
+        ops.TIMER = bt
+        one_step()
+        torch.cuda.synchronize()
+        ops.TIMER = None
+        out["breakdown_ms_one_step"] = {k: round(v["total_ms"], 3) for k, v in sorted(bt.summary().items(), key=lambda kv: -kv[1]["total_ms"])}
     out["wall_s"] = time.perf_counter() - t0
     return out
 
@@ -533,9 +542,10 @@ def gpu_arm(args, rank: int, world: int):
         comp["workload"] = f"Sedov 2D CompSPH {args.nx}x{args.nx}, Wendland C4, 32 neighbours, Cullen-Dehnen, RK2, compatible energy"
     s3 = None
     if rank == 0 and world == 1 and not args.no_sedov3d:
-        s3 = scheme_throughput(dev, "crkSPH", 3, 128, 128, steps=3, warmup=2, kahan=True, timed_kernel="crk_accel_dudt",
-                               bytes_per_particle=bytes_accel_dudt(3, 128.0))
-        s3["workload"] = "Sedov 3D CRKSPH 128^3 (2,097,152 particles), Wendland C4, 128 neighbours, Cullen-Dehnen, RK2, Kahan sums"
+        s3 = scheme_throughput(dev, "crkSPH", 3, args.nx3d, 128, steps=3, warmup=2, kahan=True, timed_kernel="crk_accel_dudt",
+                               bytes_per_particle=bytes_accel_dudt(3, 128.0), breakdown=True)
+        s3["workload"] = (f"Sedov 3D CRKSPH {args.nx3d}^3 ({args.nx3d ** 3:,} particles), Wendland C4, 128 neighbours, Cullen-Dehnen, RK2, "
+                          "Kahan sums")
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -157,6 +157,8 @@ def computeKernelGradientCRK(xi, xj, hi, hj, kernelProperties, domainState, useC
     mode = getattr(kernelProperties, "supportMode", None)
     if mode == "gather":
         W, gW = kWG(x, r, hi)
+    elif mode == "superSymmetric":
+        W, gW = kWG(x, r, wp.max(hi, hj))
     elif mode == "kernelMeanSymmetric":
         Wi, gi = kWG(x, r, hi)
         Wj, gj = kWG(x, r, hj)
@@ -921,10 +923,90 @@ def run_reference_owen(ref: Path) -> dict:
     return out
 
 
+# ---------------------------------------------------------------- delta-SPH pair bodies
+WC_COEFFS = np.array([0.05, 10.0, 1e-3], np.float64)   # inviscid alpha, c_s, viscid nu
+
+
+def make_deltasph_case(seed=9, n_side=16):
+    """Periodic unit box, varied supports (the super-symmetric support max(H_i, H_j)),
+    a compressive + shearing flow, densities from the gather sum perturbed by a few
+    per cent, and the renormalised density gradient and stiff-Tait pressure of the
+    oracle's first delta-SPH pass (warpSPHCore quantities in the reference)."""
+    from oracle import oracle
+    from oracle.steps import cell_capacity_for
+    from tests.cases import make_params, make_particles
+    import warpsph_b200 as ws
+    from warpsph_b200.configurations import WeaklyCompressibleSPHConfig, wc_params
+    cfg, sch, p = make_params(2, kernel=ws.KernelFunctions.Wendland4)
+    P = make_particles(2, n_side, seed=seed, jitter=0.3, flow=1.0, h_spread=0.15)
+    n = len(P["masses"])
+    rng = np.random.default_rng(seed + 400)
+    x, H, m = P["positions"], P["supports"], P["masses"]
+    v = (P["velocities"] - 1.2 * x + 0.3 * rng.standard_normal(x.shape)).astype(F)
+    o = oracle.get("f32")
+    nb = o.neighbors(p, x, H, cell_capacity_for(n, 2))
+    rho0 = o.density(p, 0, x, H, m, nb)
+    rho = (rho0 * (1.0 + 0.03 * rng.standard_normal(n))).astype(F)
+    wc = wc_params(WeaklyCompressibleSPHConfig())
+    _, _, gL, Pr = o.deltasph_rhs(p, wc, x, H, m, rho, v, nb)
+    return dict(params=p, x=x, H=H, m=m, v=v, rho=rho, gL=gL.astype(F), P=Pr.astype(F), nb=nb, n=n)
+
+
+def run_reference_deltasph(ref: Path, case: dict) -> dict:
+    """Executes, per particle and unmodified, the delta-SPH pair bodies under the
+    super-symmetric support: computeVelocityDiffusionDeltaSPH_Func_i
+    (modules/deltaSPH/wp_viscosityDelta.py; inviscid and viscid), 
+    computeDensityDiffusionDeltaSPH_Func_i (modules/deltaSPH/wp_densityDelta.py; the
+    deltaSPH, densityOnly and deltaOnly schemes) and computePressureSurfaceAware_Func_i
+    (modules/pressure/wp_surfaceAware.py; every pressure term, no surface mask)."""
+    p = case["params"]
+    n, nb = case["n"], case["nb"]
+    offs, cnt, lst = nb["offsets"], nb["counts"], nb["list"].astype(np.int64)
+    x, H, m, v, rho, gL, Pr = (case[k] for k in ("x", "H", "m", "v", "rho", "gL", "P"))
+    state = SoA(positions=x, supports=H, masses=m, densities=rho, kinds=np.zeros(n, np.int32))
+    dom = SoA(dim=2)
+    enums = load(ref, "enumTypes.py")
+    extra = dict(DensityDiffusionScheme=enums["DensityDiffusionScheme"], PressureForceScheme=enums["PressureForceScheme"])
+    vis = load(ref, "modules/deltaSPH/wp_viscosityDelta.py", extra)
+    den = load(ref, "modules/deltaSPH/wp_densityDelta.py", extra)
+    prs = load(ref, "modules/pressure/wp_surfaceAware.py", extra)
+    kp = SoA(operationMode=0, kernelFunction=int(p.kernel), supportMode="superSymmetric")
+    alpha, c_s, nu = (F(a) for a in WC_COEFFS)
+
+    def base(i):
+        return dict(i=i, dim=2, xi=x[i], hi=F(H[i]), mi=F(m[i]), rhoi=F(rho[i]), referenceState=state, domainState=dom,
+                    kernelProperties=kp, beginIndex=int(offs[i]), numIndices=int(cnt[i]), offsetArray=lst, ki=0,
+                    referenceKinds=state.kinds, useGradientRenormalization=False, Li=None, useGradHTerms=False, omega_i=F(1),
+                    referenceOmegas=None, useVolume=False, Vi=F(0), referenceVolumes=None, useCRK=False, Ai=F(1),
+                    Bi=np.zeros(2, F), gradAi=np.zeros(2, F), gradBi=np.zeros((2, 2), F), vel_i=v[i], referenceVelocities=v,
+                    alpha=alpha, c_s=c_s, nu=nu, n=2, gradRho_i=np.zeros(2, F), referenceGradRho=np.zeros((n, 2), F),
+                    gradRhoL_i=gL[i], referenceGradRhoL=gL, P_i=F(Pr[i]), referencePressures=Pr, mask_i=0,
+                    referenceSurfaceMask=np.zeros(n, np.int32), PressureSurfaceAware_i=F(0), referencePressureSurfaceAwares=None,
+                    outputValue=np.zeros(2, F))
+
+    out = {"visc_inviscid": np.zeros((n, 2), F), "visc_viscid": np.zeros((n, 2), F),
+           "dd": np.zeros((3, n), F), "pf": np.zeros((6, n, 2), F)}
+    schemes = [enums["DensityDiffusionScheme"].deltaSPH.value, enums["DensityDiffusionScheme"].densityOnly.value,
+               enums["DensityDiffusionScheme"].deltaOnly.value]
+    with np.errstate(all="ignore"):
+        for i in range(n):
+            b = base(i)
+            out["visc_inviscid"][i] = call(vis["computeVelocityDiffusionDeltaSPH_Func_i"], inviscid=True, **b)
+            out["visc_viscid"][i] = call(vis["computeVelocityDiffusionDeltaSPH_Func_i"], inviscid=False, **b)
+            for s_, sch in enumerate(schemes):
+                bb = dict(b, outputValue=F(0))
+                out["dd"][s_, i] = call(den["computeDensityDiffusionDeltaSPH_Func_i"], densityScheme=sch, **bb)
+            for t in range(6):
+                out["pf"][t, i] = call(prs["computePressureSurfaceAware_Func_i"], pressureTerm=t, **b)
+    out["dd_schemes"] = np.array(schemes, np.int32)
+    out["wc_coeffs"] = WC_COEFFS
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph", "owen", "hopkins"], default="all")
+    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph", "owen", "hopkins", "deltasph"], default="all")
     a = ap.parse_args()
     ref = Path(a.reference)
     if a.which in ("all", "crk"):
@@ -960,6 +1042,14 @@ def main():
         out = run_reference_hopkins(ref, g)
         np.savez_compressed(Path(__file__).parent / "hopkins_golden.npz", **out)
         print("wrote", Path(__file__).parent / "hopkins_golden.npz")
+    if a.which in ("all", "deltasph"):
+        case = make_deltasph_case()
+        out = run_reference_deltasph(ref, case)
+        nb = case["nb"]
+        np.savez_compressed(Path(__file__).parent / "deltasph_golden.npz",
+                            x=case["x"], H=case["H"], m=case["m"], v=case["v"], rho=case["rho"], gL=case["gL"], P=case["P"],
+                            offsets=nb["offsets"], counts=nb["counts"], list=nb["list"], **out)
+        print("wrote", Path(__file__).parent / "deltasph_golden.npz", "particles", case["n"], "pairs", len(nb["list"]))
     if a.which in ("all", "owen"):
         out = run_reference_owen(ref)
         np.savez_compressed(Path(__file__).parent / "owen_golden.npz", **out)
