@@ -597,6 +597,30 @@ int sph_ensemble_step(const SphParams* p, const SphWcParams* wc, int64_t n, cons
 /* weaklyCompressibleEOS (modules/eos/weaklyCompressible.py:21-44). */
 int sph_wc_eos(const SphWcParams* wc, int64_t n, const float* rho, float* P_out, void* stream);
 
+/* Velocity diffusion and continuity of the DFSPH step (schemes/dfsph.py:100-109:
+ * computeVelocityDiffusion, modules/deltaSPH/velocityDissipation.py:18-36 with
+ * wp_viscosityDelta.py:14-108, and computeMomentum, modules/momentum/inconsistent.py:16-31),
+ * one pass, super-symmetric support max(H_i, H_j): dvdt_out [n, dim] = the delta-SPH
+ * velocity diffusion, drhodt_out [n] = -rho_i sum_j V_j (v_j - v_i).gradW_ij.  Bit for
+ * bit the dvdt / drhodt of sph_deltasph_rhs with zero pressure and density_delta = 0. */
+int sph_wc_visc_continuity(const SphParams* p, const SphWcParams* wc, int64_t n, const float* x,
+                           const float* H, const float* m, const float* rho, const float* v,
+                           const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                           float* dvdt_out, float* drhodt_out, void* stream);
+
+/* One delta-plus shift (modules/shifting/delta.py:6-47 with sample/wp_deltaShift.py:57-126,
+ * gather support H_i): shift_out [n, dim] = -cfl Ma 2 (H_i / xi)^2 sum_j
+ * (1 + R (W_ij / W0_j)^nexp) m_j / (2 (rho_i + rho_j)) gradW_ij, with W0_j the kernel at
+ * (m_j / rho0)^(1/dim) / xi, Ma = max_i |v_i| / c0 over the finite magnitudes (0.1 when
+ * below 1e-6) and zero shift for kinds[i] != 0 (kinds may be null: all fluid).
+ * scratch: 2 device words (the max reduction).  The reference passes R = 0.25,
+ * nexp = 4 and rho0 = 1. */
+int sph_delta_shift(const SphParams* p, int64_t n, const float* x, const float* H, const float* m,
+                    const float* rho, const float* v, const int32_t* kinds,
+                    const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                    float cfl, float c0, float R, int32_t nexp, float rho0,
+                    uint32_t* scratch, float* shift_out, void* stream);
+
 /* ---------------------------------------------------------------- learned warm start
  * No counterpart in the reference: a per-particle MLP predicts the initial pressure of
  * the Jacobi solves (replacing 0.75 p_prev at divergenceFree.py:72 and 0 at

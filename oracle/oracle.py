@@ -93,6 +93,8 @@ class Oracle:
         L.oracle_pressure_accel_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pressure_shift_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_deltasph_rhs.argtypes = [P, P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rp]
+        L.oracle_delta_shift.argtypes = [P, i64, rp, rp, rp, rp, rp, C.c_void_p, _i32p, _i32p, _i32p, real_c, real_c, real_c, C.c_int,
+                                         real_c, rp]
         L.oracle_owen_iter.argtypes = [P, i64, rp, rp, _i32p, _i32p, _i32p, _f64p, _f64p, C.c_int, C.c_double, rp, rpn, rpn, rp, rpn]
         L.oracle_switch_hopkins_terms.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rpn]
         L.oracle_switch_hopkins_update.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, rp, real_c, _i32p, _i32p, _i32p, rp, rpn]
@@ -288,6 +290,26 @@ class Oracle:
         self.lib.oracle_deltasph_rhs(self._p(params), C.c_void_p(C.addressof(wc)), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho),
                                      self.arr(v), nb["offsets"], nb["counts"], nb["list"], gL, P, dv, dr)
         return dv, dr, gL, P
+
+    def visc_continuity(self, params, wc, x, H, m, rho, v, nb):
+        """(dvdt, drhodt) of the DFSPH step's velocity diffusion and continuity: the
+        delta-SPH right-hand side with zero pressure (Tait, kappa 0) and no density
+        diffusion."""
+        import copy
+        w = copy.copy(wc)
+        w.eos, w.kappa, w.density_delta = 1, 0.0, 0.0
+        dv, dr, _, _ = self.deltasph_rhs(params, w, x, H, m, rho, v, nb)
+        return dv, dr
+
+    def delta_shift(self, params, x, H, m, rho, v, nb, cfl, c0, kinds=None, R=0.25, nexp=4, rho0=1.0):
+        """One delta-plus shift [n, dim] (modules/shifting/delta.py, sample/wp_deltaShift.py)."""
+        n, d = len(H), params.dim
+        out = np.zeros((n, d), self.dtype)
+        kp = None if kinds is None else np.ascontiguousarray(kinds, np.int32)
+        self.lib.oracle_delta_shift(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(v),
+                                    None if kp is None else kp.ctypes.data, nb["offsets"], nb["counts"], nb["list"], cfl, c0, R,
+                                    int(nexp), rho0, out)
+        return out
 
     def owen_iter(self, params, x, H, nb, lut_nh, lut_psiH, target, hb):
         """(psi0, psiH, H_new, ratio) of one Owen support iteration."""

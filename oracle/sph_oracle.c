@@ -1308,6 +1308,54 @@ int oracle_deltasph_rhs(const SphParams* p, const SphWcParams* w, int64_t n, con
     return 0;
 }
 
+/* delta-plus shift: modules/shifting/delta.py:6-47 (the scaling -CFL Ma 2 h^2, Ma from the
+ * finite max |v| / c0, 0.1 below 1e-6) with the pair sum of sample/wp_deltaShift.py:57-126
+ * under the gather support: sum_j (1 + R (W_ij / W0)^nexp) m_j / (2 (rho_i + rho_j)) gradW_ij,
+ * W0 = eval_k(q0) C_d / H_i^d at q0 = ((m_j / rho0)^(1/d) / xi) / H_i.  Zero for kinds != 0
+ * (modules/shifting/wrapper.py:100). */
+int oracle_delta_shift(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho, const real* v,
+                       const int32_t* kinds, const int32_t* offs, const int32_t* cnt, const int32_t* list, real cfl, real c0,
+                       real R, int nexp, real rho0, real* shift) {
+    OP o = op_from(p);
+    int D = o.dim;
+    real vmax = 0;
+    int finite = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        real s2 = 0;
+        for (int a = 0; a < D; ++a) s2 += v[i * D + a] * v[i * D + a];
+        real mag = SQRT(s2);
+        if (isfinite(mag)) { vmax = mag > vmax ? mag : vmax; finite = 1; }
+    }
+    real cmax = finite ? vmax / c0 : (real)NAN;
+    real Ma = cmax < (real)1e-6 ? (real)0.1 : cmax;
+    real xi = o.kxi;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real acc[3] = {0, 0, 0};
+        real Hi = H[i], rhoi = rho[i];
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, gw[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG(&o, d, rsqrt_safe(dotD(d, d, D)), Hi, &W, gw);
+            real dxs = POW(m[j] / rho0, (real)1 / (real)D) / xi;
+            real q0 = dxs / Hi, k0 = 0, p0;
+            if (q0 < 1) kernel_kp(o.kernel, D, q0, &k0, &p0);
+            real hd = D == 1 ? Hi : (D == 2 ? Hi * Hi : Hi * Hi * Hi);
+            real W0 = k0 * kernel_C(o.kernel, D) / hd;
+            real term = 1 + R * POW(W / W0, (real)nexp);
+            real dterm = (real)0.5 * m[j] / (rhoi + rho[j]);
+            real sc = term * dterm;
+            for (int a = 0; a < D; ++a) acc[a] += sc * gw[a];
+        }
+        real h = Hi / xi;
+        real scale = -cfl * Ma * (real)2 * (h * h);
+        int moving = kinds == NULL || kinds[i] == 0;
+        for (int a = 0; a < D; ++a) shift[i * D + a] = moving ? acc[a] * scale : 0;
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------------------ artificial viscosity Pi_ij
  * modules/dissipation/pi.py:11-161 (computePi_actual) with util.py:6-38 (compute_mu_ij) and
  * util.py:42-134 (compute_bars).  ux = (v_i - v_j).x_ij, x_ij = x_i - x_j.  Returns Pi_ij

@@ -1000,6 +1000,47 @@ def run_reference_deltasph(ref: Path, case: dict) -> dict:
                 out["pf"][t, i] = call(prs["computePressureSurfaceAware_Func_i"], pressureTerm=t, **b)
     out["dd_schemes"] = np.array(schemes, np.int32)
     out["wc_coeffs"] = WC_COEFFS
+
+    # delta-plus shift: computeDeltaShift (modules/shifting/delta.py) unmodified, with the
+    # Warp launch wrapper replaced by the per-particle body computeDeltaShift_Func_i
+    # (sample/wp_deltaShift.py) under the gather support
+    def eval_k(q, dim, kf):
+        return kernel_kp(int(kf), int(dim), F(q))[0] if F(q) < F(1) else F(0)
+
+    def computeKernelCRK(xi_, xj_, hi_, hj_, kernelProperties, domainState, useCRK, A, B):
+        d = computeDistanceVec(xi_, xj_, domainState)
+        return kWG(d, safe_sqrt(wp.dot(d, d)), hi_)[0]
+
+    sh_names = dict(computeKernelCRK=computeKernelCRK, computePairwiseSupport=lambda hi_, hj_, mode: hi_, eval_k=eval_k,
+                    eval_C_d=lambda dim, kf: kernel_C(int(kf), int(dim)), eval_dkdq=None)
+    ds = load(ref, "sample/wp_deltaShift.py", sh_names)
+    kp_g = SoA(operationMode=0, kernelFunction=int(p.kernel), supportMode="gather")
+
+    def computeDeltaShiftWarp(state_, operationProperties=None, referenceParticles=None, domain=None, adjacency=None, CFL=0.0,
+                              computeMach=True, c_max=0.0, rho0=1.0, dx=0.0, R=0.25, n=4):
+        xs = state_.positions.numpy().astype(F)
+        outv = np.zeros((len(xs), 2), F)
+        st = SoA(positions=xs, supports=H, masses=m, densities=rho, kinds=np.zeros(len(xs), np.int32))
+        with np.errstate(all="ignore"):
+            for i in range(len(xs)):
+                b = base(i)
+                b.update(xi=xs[i], referenceState=st, kernelProperties=kp_g, correctionData=None, outputValue=np.zeros(2, F))
+                b.pop("n")   # the viscosity bodies' dimension argument; here n is the exponent
+                outv[i] = call(ds["computeDeltaShift_Func_i"], R=R, n=n, CFL=CFL, computeMach=computeMach, c_max=c_max, rho0=rho0,
+                               dx=dx, **b)
+        return torch.from_numpy(outv)
+
+    dl = load(ref, "modules/shifting/delta.py", dict(computeDeltaShiftWarp=computeDeltaShiftWarp, OperationProperties=lambda **k: None,
+                                                     WarpOperation=SoA(Density=0), SupportScheme=SoA(Gather=0),
+                                                     sphKernelScale=sphKernelScale))
+    cfl, c0 = F(0.3), F(10.0)
+    st = SoA(positions=torch.from_numpy(x.copy()), velocities=torch.from_numpy(v), supports=torch.from_numpy(H),
+             densities=torch.from_numpy(rho), masses=torch.from_numpy(m))
+    conf = SoA(dt=1e-3, dx=0.0625, kernel=SoA(value=int(p.kernel)), dim=2)
+    sconf = SoA(shiftProperties=SoA(iterations=1, CFL=float(cfl), computeMach=True), fluid=SoA(fixedSoundSpeed=float(c0)))
+    delta, _ = dl["computeDeltaShift"](st, conf, sconf, None, None, iters=1)
+    out["shift"] = delta.numpy().astype(F)
+    out["shift_coeffs"] = np.array([cfl, c0], np.float64)
     return out
 
 

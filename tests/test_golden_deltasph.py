@@ -75,3 +75,19 @@ def test_golden_density_diffusion(gold, s):
     xi = float(core.sphKernelScale(core.KernelFunctions.Wendland4, 2))
     dd = (d1.astype(np.float64) - d0) / (gold["H"].astype(np.float64) / xi * c0)
     assert_close(dd, gold["dd"][s], 1e-4, 1e-4, f"density diffusion {scheme}")
+
+
+def test_golden_delta_shift(gold):
+    """computeDeltaShift (modules/shifting/delta.py) with the reference's pair body: the
+    oracle agrees to 5e-5 of the field's scale (the (W/W0)^4 factor and the torch norm
+    behind Ma amplify FP32 rounding a little)."""
+    _, _, p = make_params(2, kernel=core.KernelFunctions.Wendland4)
+    nb = dict(offsets=gold["offsets"], counts=gold["counts"], list=gold["list"])
+    cfl, c0 = gold["shift_coeffs"]
+    s = oracle.get("f32").delta_shift(p, gold["x"], gold["H"], gold["m"], gold["rho"], gold["v"], nb, float(cfl), float(c0))
+    assert_close(s, gold["shift"], 5e-5, 5e-5, "delta-plus shift")
+    # boundary particles (kind != 0) do not move
+    kinds = np.zeros(len(gold["H"]), np.int32)
+    kinds[::7] = 1
+    s2 = oracle.get("f32").delta_shift(p, gold["x"], gold["H"], gold["m"], gold["rho"], gold["v"], nb, float(cfl), float(c0), kinds=kinds)
+    assert np.all(s2[::7] == 0) and np.array_equal(s2[kinds == 0], s[kinds == 0])

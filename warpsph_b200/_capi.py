@@ -144,6 +144,8 @@ _PROTOS = {
     "sph_ensemble_step": [_P, _P, _I64] + [_P] * 12 + [_I64, _I32, _I32, _P, _P, _P],
     "sph_mlp_forward": [_P, _I64, _P, _P, _P, _P],
     "sph_mlp_forward_tc": [_P, _I64, _P, _P, _P, _P, _P],
+    "sph_wc_visc_continuity": [_P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "sph_delta_shift": [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_float, _P, _P, _P],
     "sph_mlp_grad": [_P, _I64, _P, _P, _P, _P, _P],
     "sph_mlp_adam": [_P, _P, _P, _P, _I64, C.c_float, C.c_float, C.c_float, C.c_float, _I64, _P],
     "sph_dfsph_div_solve": [_P, _P, _I64] + [_P] * 12 + [_I64] + [_P] * 6,

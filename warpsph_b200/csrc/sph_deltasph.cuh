@@ -130,15 +130,18 @@ template <int D, int G> __device__ __forceinline__ void passA_reduce(Mat<D>& M, 
 }
 
 // Per-lane partial sums of pass B for particle i: cont = sum V (v_j - v_i).gW,
-// dd = sum V psi.gW, pf = sum V p_ij gW, visc = sum V mu f gW / rho_bar.
-template <int KF, int D, int G, bool CG = false>
+// dd = sum V psi.gW, pf = sum V p_ij gW, visc = sum V mu f gW / rho_bar.  With FULL
+// false only cont and visc are formed (gL and Pr are not read): the velocity diffusion
+// and continuity of the DFSPH step.
+template <int KF, int D, int G, bool CG = false, bool FULL = true>
 __device__ __forceinline__ void passB_partial(int i, int lane, const DevParams& P, const WcDev& W, const float* x,
                                               const float* __restrict__ H, const float* __restrict__ m, const float* rho,
                                               const float* v, const float* gL, const float* Pr,
                                               const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
                                               const int32_t* __restrict__ list, float& cont, float& dd, Vec<D>& pf, Vec<D>& visc) {
-    const Vec<D> xi = ldv<D, CG>(x, i), vi = ldv<D, CG>(v, i), gLi = ldv<D, CG>(gL, i);
-    const float Hi = H[i], rhoi = ldf<CG>(rho + i), Pi = ldf<CG>(Pr + i);
+    const Vec<D> xi = ldv<D, CG>(x, i), vi = ldv<D, CG>(v, i);
+    const Vec<D> gLi = FULL ? ldv<D, CG>(gL, i) : vzero<D>();
+    const float Hi = H[i], rhoi = ldf<CG>(rho + i), Pi = FULL ? ldf<CG>(Pr + i) : 0.f;
     const float eps = 1.0e-14f * Hi;
     const float factor = W.inviscid ? W.alpha * W.c0 * Hi / W.xi : W.visc_nu;
     const int b = offs[i], e = b + cnt[i];
@@ -158,7 +161,7 @@ __device__ __forceinline__ void passB_partial(int i, int lane, const DevParams& 
         for (int a = 0; a < D; ++a) t += (vj.v[a] - vi.v[a]) * gW.v[a];
         cont += Vj * t;
         // density diffusion (wp_densityDelta.py:88-117)
-        {
+        if constexpr (FULL) {
             const Vec<D> gLj = ldv<D, CG>(gL, j);
             const float inv = 1.f / (r + eps);
             const float s = 2.f * (rj - rhoi) * inv * inv;      // 2 (rho_j - rho_i) n_ij / (r + eps), n_ij = x_ij / (r + eps)
@@ -174,7 +177,7 @@ __device__ __forceinline__ void passB_partial(int i, int lane, const DevParams& 
             dd += Vj * pd;
         }
         // pressure (wp_surfaceAware.py:48-63); no free-surface mask on this path
-        {
+        if constexpr (FULL) {
             const float Pj = ldf<CG>(Pr + j);
             float pij;
             switch (W.pressure_term) {
@@ -245,6 +248,104 @@ k_ds_passB(int n, DevParams P, WcDev W, const float* __restrict__ x, const float
     passB_finish<D>(W, rho[g.i], H[g.i], cont, dd, pf, visc, dr, dv);
     drhodt[g.i] = dr;
     store_vec<D>(dvdt, g.i, dv);
+}
+
+// Velocity diffusion and continuity alone (dfsph.py:100-109): dvdt = visc,
+// drhodt = -rho cont, bit for bit what pass B gives with P = 0 and delta = 0.
+template <int KF, int D, int G>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_visc_cont(int n, DevParams P, WcDev W, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+            const float* __restrict__ rho, const float* __restrict__ v, const int32_t* __restrict__ offs,
+            const int32_t* __restrict__ cnt, const int32_t* __restrict__ list, float* __restrict__ dvdt, float* __restrict__ drhodt) {
+    Grp<G> g(n);
+    float cont = 0.f, dd = 0.f;
+    Vec<D> pf = vzero<D>(), visc = vzero<D>();
+    if (g.valid) passB_partial<KF, D, G, false, false>(g.i, g.lane, P, W, x, H, m, rho, v, nullptr, nullptr, offs, cnt, list, cont, dd, pf, visc);
+    cont = gsum<G>(cont);
+    #pragma unroll
+    for (int a = 0; a < D; ++a) visc.v[a] = gsum<G>(visc.v[a]);
+    if (!g.valid || g.lane != 0) return;
+    const float rhoi = rho[g.i];
+    drhodt[g.i] = -rhoi * cont + 0.f * dd;
+    Vec<D> dv;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) dv.v[a] = -pf.v[a] + visc.v[a];
+    store_vec<D>(dvdt, g.i, dv);
+}
+
+// ---------------------------------------------------------------- delta-plus shift
+// max_i |v_i| over the finite magnitudes (shifting/delta.py:10-17): red[0] holds the
+// float bits of the running maximum (non-negative, so integer order is float order),
+// red[1] counts finite magnitudes.
+template <int D>
+__global__ void k_vmax(int n, const float* __restrict__ v, unsigned int* __restrict__ red) {
+    float vmax = 0.f;
+    unsigned int finite = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        #pragma unroll
+        for (int a = 0; a < D; ++a) { const float c = v[(size_t)i * D + a]; s += c * c; }
+        const float mag = sqrtf(s);
+        if (isfinite(mag)) { vmax = fmaxf(vmax, mag); finite = 1u; }
+    }
+    vmax = block_reduce(vmax, 0.f, OpMaxF());
+    finite = block_reduce(finite, 0u, OpMaxU());
+    if (threadIdx.x == 0) {
+        atomicMax(red, __float_as_uint(vmax));
+        if (finite) atomicOr(red + 1, 1u);
+    }
+}
+
+// shift_i = -CFL Ma 2 (H_i / xi)^2 sum_j (1 + R (W_ij / W_0)^n) m_j / (2 (rho_i + rho_j)) gradW_ij
+// (sample/wp_deltaShift.py:57-126 and shifting/delta.py:18-45), gather support H_i,
+// W_0 = W((m_j / rho0)^(1/d) / xi, H_i), Ma = max|v| / c0 (0.1 below 1e-6), zero for
+// particles of kind != 0 (shifting/wrapper.py:100).
+template <int KF, int D, int G>
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_delta_shift(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+              const float* __restrict__ rho, const int32_t* __restrict__ kinds, const int32_t* __restrict__ offs,
+              const int32_t* __restrict__ cnt, const int32_t* __restrict__ list, float cfl, float c0, float R, int nexp, float rho0,
+              const unsigned int* __restrict__ red, float* __restrict__ shift) {
+    Grp<G> g(n);
+    Vec<D> s = vzero<D>();
+    if (g.valid) {
+        const int i = g.i;
+        const Vec<D> xi = load_vec<D>(x, i);
+        const float Hi = H[i], rhoi = rho[i];
+        const float xi_k = P.kscale;
+        const int b = offs[i], e = b + cnt[i];
+        for (int q = b + g.lane; q < e; q += G) {
+            int j, k; entry(list, q, j, k);
+            const Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            const float r = safe_sqrt(dot<D>(xij, xij));
+            float Wij; Vec<D> gW;
+            kernelWG<KF, D>(xij, r, Hi, Wij, gW);
+            const float mj = __ldg(m + j);
+            const float dxs = powf(mj / rho0, 1.f / (float)D) / xi_k;
+            const float q0 = dxs / Hi;
+            float k0 = 0.f, p0;
+            if (q0 < 1.f) kernel_kp<KF, D>(q0, k0, p0);
+            const float W0 = k0 * KernelTraits<KF, D>::C / ipow<D>(Hi);   // eval_k * eval_C_d / h^d
+            const float term = 1.f + R * powf(Wij / W0, (float)nexp);
+            const float dterm = 0.5f * mj / (rhoi + __ldg(rho + j));
+            const float sc = term * dterm;
+            #pragma unroll
+            for (int a = 0; a < D; ++a) s.v[a] += sc * gW.v[a];
+        }
+    }
+    #pragma unroll
+    for (int a = 0; a < D; ++a) s.v[a] = gsum<G>(s.v[a]);
+    if (!g.valid || g.lane != 0) return;
+    const int i = g.i;
+    float cmax = red[1] ? __uint_as_float(red[0]) / c0 : __int_as_float(0x7fc00000);
+    const float Ma = cmax < 1e-6f ? 0.1f : cmax;
+    const float h = H[i] / P.kscale;
+    const float scale = -cfl * Ma * 2.f * (h * h);
+    Vec<D> o;
+    const bool moving = kinds == nullptr || kinds[i] == 0;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) o.v[a] = moving ? s.v[a] * scale : 0.f;
+    store_vec<D>(shift, i, o);
 }
 
 }  // namespace wsph
