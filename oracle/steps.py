@@ -218,6 +218,121 @@ class MonaghanOracle(CRKSPHOracle):
         return upd, nb, st, dict(omega=om)
 
 
+class DFSPHOracle(CRKSPHOracle):
+    """schemes/dfsph.py:13-218 for a fluid-only system, with the finalize of
+    systems/incompressible.py:71-277: gather density (unless integrated), velocity
+    diffusion and continuity, gravity, the divergence-free Jacobi solve; after the stages
+    the gather density at the new positions and the density solve, whose acceleration
+    moves the particles by dt^2 a_p.  Positions, velocities and densities are integrated."""
+
+    def __init__(self, params, wc, df_cfg, rho_cfg, gravity=None, integrate_rho: bool = False, precision: str = "f32"):
+        super().__init__(params, precision, adaptive=False, compatible_energy=False)
+        self.wc, self.df_cfg, self.rho_cfg = wc, df_cfg, rho_cfg
+        self.g = None if gravity is None else np.asarray(gravity, self.dt_)
+        self.integrate_rho = integrate_rho
+
+    def gravity(self, n):
+        return np.zeros((n, self.dim), self.dt_) if self.g is None else np.tile(self.g, (n, 1)).astype(self.dt_)
+
+    def rhs(self, st, dt):
+        o, p = self.o, self.p
+        st = dict(st)
+        x, H, m, v = st["positions"], st["supports"], st["masses"], st["velocities"]
+        nb = self.nb(x, H)
+        if st.get("densities") is None or not self.integrate_rho:
+            st["densities"] = o.density(p, 0, x, H, m, nb)
+        rho = st["densities"]
+        dvdt_diss, drhodt = o.visc_continuity(p, self.wc, x, H, m, rho, v, nb)
+        dvdt = self.gravity(len(H))
+        p0 = st.get("pressures")
+        p0 = np.zeros(len(H), self.dt_) if p0 is None else p0
+        src = (dvdt + dvdt_diss).astype(self.dt_)
+        pr, acc, hist, it = o.jacobi_solve(p, 0, self.df_cfg, x, H, m, rho, v, src, p0, dt, nb)
+        st["pressures"] = pr
+        upd = dict(dxdt=v, dvdt=(src + acc).astype(self.dt_), drhodt=drhodt)
+        return upd, nb, st, dict(errors=hist[:, 0].copy(), iterations=it)
+
+    def step(self, st0, dt, scheme: str = "explicitEuler"):
+        a, b, _c = TABLEAUX[scheme]
+        updates, rvs = [], []
+        prev = dict(st0)
+        fields = (("positions", "dxdt", True), ("velocities", "dvdt", False), ("densities", "drhodt", False))
+        for s in range(len(b)):
+            Ss = dict(prev)
+            if s > 0:
+                for name, der, wr in fields:
+                    if st0.get(name) is not None:
+                        Ss[name] = self.combine(st0[name], [u[der] for u in updates], a[s], dt, wrap=wr)
+            upd, nb, Sout, ex = self.rhs(Ss, dt)
+            updates.append(upd)
+            rvs.append((nb, Sout, ex))
+            prev = Sout
+        Sf = dict(prev)
+        for name, der, wr in fields:
+            if st0.get(name) is not None:
+                Sf[name] = self.combine(st0[name], [u[der] for u in updates], b, dt, wrap=wr)
+        self.finalize(Sf, st0, dt, updates, rvs)
+        return Sf, updates, rvs
+
+    def finalize(self, Sf, st0, dt, updates, rvs):
+        o, p = self.o, self.p
+        last = rvs[-1][1]
+        Sf["pressures"] = last["pressures"]
+        x, H, m, v = Sf["positions"], Sf["supports"], Sf["masses"], Sf["velocities"]
+        nb = self.nb(x, H)
+        rho = o.density(p, 0, x, H, m, nb)
+        Sf["densities"] = rho
+        zero = np.zeros_like(v)
+        pr, acc, hist, it = o.jacobi_solve(p, 1, self.rho_cfg, x, H, m, rho, v, zero, Sf["pressures"], dt, nb)
+        k = (self.dt_(self.dt_(dt) * self.dt_(dt)) * acc).astype(self.dt_)
+        Sf["positions"] = self.combine(x, [k], [1.0], 1.0, wrap=True)
+        Sf["density_solve_iterations"] = it
+
+
+class DeltaSPHOracle(DFSPHOracle):
+    """schemes/deltaSPH.py:11-208 for a fluid-only system with the finalize of
+    systems/weaklyCompressible.py:73-200: the delta-SPH right-hand side plus gravity; after
+    the stages the delta-plus shift (when active) at the integrated state, the exponential
+    density update from the last stage, and the shift added to the positions."""
+
+    def __init__(self, params, wc, gravity=None, shift=None, precision: str = "f32"):
+        CRKSPHOracle.__init__(self, params, precision, adaptive=False, compatible_energy=False)
+        self.wc = wc
+        self.g = None if gravity is None else np.asarray(gravity, self.dt_)
+        self.shift = shift      # None or dict(cfl=, c0=, iterations=)
+
+    def rhs(self, st, dt):
+        o, p = self.o, self.p
+        st = dict(st)
+        x, H, m, v = st["positions"], st["supports"], st["masses"], st["velocities"]
+        nb = self.nb(x, H)
+        if st.get("densities") is None:
+            st["densities"] = o.density(p, 0, x, H, m, nb)
+        dv, dr, _, P = o.deltasph_rhs(p, self.wc, x, H, m, st["densities"], v, nb)
+        st["pressures"] = P
+        upd = dict(dxdt=v, dvdt=(dv + self.gravity(len(H))).astype(self.dt_), drhodt=dr)
+        return upd, nb, st, {}
+
+    def finalize(self, Sf, st0, dt, updates, rvs):
+        o, p, f = self.o, self.p, self.dt_
+        last = rvs[-1][1]
+        Sf["pressures"] = last["pressures"]
+        dx = None
+        if self.shift is not None:
+            x = Sf["positions"]
+            dx = np.zeros_like(x)
+            for _ in range(int(self.shift.get("iterations", 1))):
+                nb = self.nb(x, Sf["supports"])
+                upd = o.delta_shift(p, x, Sf["supports"], Sf["masses"], Sf["densities"], Sf["velocities"], nb, self.shift["cfl"],
+                                    self.shift["c0"])
+                dx = (dx + upd).astype(f)
+                x = self.combine(x, [upd], [1.0], 1.0, wrap=True)
+        t = ((f(dt) * updates[-1]["drhodt"]).astype(f) / last["densities"]).astype(f)
+        Sf["densities"] = (st0["densities"] * np.exp(t).astype(f)).astype(f)
+        if dx is not None:
+            Sf["positions"] = self.combine(Sf["positions"], [dx], [1.0], 1.0, wrap=True)
+
+
 def state_to_numpy(state, dtype=np.float32) -> dict:
     """Copies the tensors of a CompSPHState-like object into numpy arrays."""
     out = {}

@@ -1,0 +1,98 @@
+"""Host-side logic of the DFSPH and delta-SPH step functions (no GPU): the scheme
+builder entries, configuration round trips, the enum forms the reference passes, gravity,
+and the cases the GPU path refuses (boundary and ghost particles, boundary conditions,
+rigid bodies, active surface detection), which raise before any device work."""
+import numpy as np
+import pytest
+import torch
+
+import warpsph_b200 as ws
+from warpsph_b200 import configurations as cf
+from warpsph_b200.enumTypes import IncompressibleSPHScheme, WeaklyCompressibleSPHScheme
+from warpsph_b200.systems import IncompressibleState, IncompressibleSystem, WeaklyCompressibleSystem
+from warpsph_b200.wcsph import computeGravity, deltaSPH_step, dfsph_step
+
+
+@pytest.mark.parametrize("name,system,step", [("deltaSPH", WeaklyCompressibleSystem, deltaSPH_step),
+                                              (WeaklyCompressibleSPHScheme.deltaSPH, WeaklyCompressibleSystem, deltaSPH_step),
+                                              ("divergenceFree", IncompressibleSystem, dfsph_step),
+                                              ("dfsph", IncompressibleSystem, dfsph_step),
+                                              (IncompressibleSPHScheme.divergenceFree, IncompressibleSystem, dfsph_step)])
+def test_build_scheme_entries(name, system, step):
+    t = ws.buildScheme(name)
+    assert len(t) == 7 and t[0] is system and t[4] is step
+    cfg = t[2]()
+    assert t[6](t[5](cfg)) == cfg
+
+
+def test_defaults_follow_the_reference():
+    i, w = cf.IncompressibleSPHConfig(), cf.WeaklyCompressibleSPHConfig()
+    for c in (i, w):
+        assert c.shiftProperties.active and c.shiftProperties.iterations == 1 and c.shiftProperties.CFL == 0.3
+        assert not c.gravityConfig.active and c.gravityConfig.magnitude == 9.81
+        assert not c.surfaceDetectionConfig.active
+        assert c.diffusionParams.inviscid and c.diffusionParams.inviscidAlpha == 0.01
+    assert i.solverConfig.divergenceFreeSolver.maxIterations == 32 and i.solverConfig.pressureSolver.maxIterations == 64
+
+
+def test_wc_params_accepts_reference_enums():
+    from enum import Enum
+
+    class PressureForceScheme(Enum):
+        conservative = 0
+        Antuono = 2
+
+    class DensityDiffusionScheme(Enum):
+        densityOnly = 2
+
+    class EquationOfState(Enum):
+        Tait = "Tait"
+
+    c = cf.WeaklyCompressibleSPHConfig()
+    c.pressureForceTerm = PressureForceScheme.conservative
+    c.diffusionParams.densityDiffusionTerm = DensityDiffusionScheme.densityOnly
+    c.fluid.eosType = EquationOfState.Tait
+    w = cf.wc_params(c)
+    assert (w.pressure_term, w.density_scheme, w.eos) == (0, 2, 1)
+
+
+def cpu_state(n=16, kinds=None):
+    x = torch.rand(n, 2) - 0.5
+    return IncompressibleState(positions=x, velocities=torch.zeros(n, 2), supports=torch.full((n,), 0.2), masses=torch.ones(n),
+                               kinds=torch.zeros(n, dtype=torch.int32) if kinds is None else kinds)
+
+
+@pytest.mark.parametrize("step,cfgcls", [(dfsph_step, cf.IncompressibleSPHConfig), (deltaSPH_step, cf.WeaklyCompressibleSPHConfig)])
+def test_unsupported_inputs_raise(step, cfgcls):
+    config = cf.SimulationConfig()
+    k = torch.zeros(16, dtype=torch.int32)
+    k[3] = 1
+    with pytest.raises(NotImplementedError, match="mDBC"):
+        step(IncompressibleSystem(state=cpu_state(kinds=k)), 1e-3, config, cfgcls())
+    for attr, val, msg in (("boundaryConditions", [object()], "boundary conditions"), ("rigidBodies", [object()], "rigid bodies")):
+        c = cfgcls()
+        setattr(c, attr, val)
+        with pytest.raises(NotImplementedError, match=msg):
+            step(IncompressibleSystem(state=cpu_state()), 1e-3, config, c)
+    c = cfgcls()
+    c.surfaceDetectionConfig.active = True
+    with pytest.raises(NotImplementedError, match="surface"):
+        step(IncompressibleSystem(state=cpu_state()), 1e-3, config, c)
+
+
+def test_gravity_forms():
+    S = cpu_state()
+    c = cf.IncompressibleSPHConfig()
+    assert torch.equal(computeGravity(S, None, c), torch.zeros(16, 2))
+    c.gravityConfig.active = True
+    g = computeGravity(S, None, c)
+    assert g.shape == (16, 2) and torch.allclose(g, torch.tensor([0.0, -9.81]).expand(16, 2))
+    c.gravityConfig.type = cf.GravityType.PointSource
+    c.gravityConfig.origin = [0.1, 0.2]
+    g = computeGravity(S, None, c)
+    d = torch.tensor([0.1, 0.2]) - S.positions
+    assert g.shape == (16, 2)
+    assert torch.allclose(g, d / (d.norm(dim=1, keepdim=True) + 1e-8) * 9.81)
+    c.gravityConfig.type = cf.GravityType.PotentialField
+    with pytest.raises(NotImplementedError):
+        computeGravity(S, None, c)

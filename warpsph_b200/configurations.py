@@ -10,6 +10,7 @@ CRKViscosity / CRKSPHConfig (crkSPH.py:16-80), with the *ToDict / dictTo* round 
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass, field
 from enum import Enum
 from typing import Any, Dict, List, Optional
@@ -352,11 +353,82 @@ def buildDefaultIncompressibleSolverConfig() -> IncompressibleSolverConfig:
 
 @dataclass
 class fluidProperties:
-    """moduleConfigurations/fluidProperties.py:9-30 (the fields the solves read)."""
+    """moduleConfigurations/fluidProperties.py:9-30 (the fields the solves read).  eosType
+    None defers to the scheme configuration's own eosType."""
     restDensity: float = 1.0
     polytropicExponent: Optional[float] = 7.0
     kappa: Optional[float] = 1.3
     fixedSoundSpeed: Optional[float] = 10.0
+    eosType: Optional[Any] = None
+
+
+# ------------------------------------------------------------------ gravity, surface detection, shifting
+class GravityType(Enum):
+    """moduleConfigurations/gravity.py:7-10."""
+    Directional = 0
+    PointSource = 1
+    PotentialField = 2
+
+
+@dataclass
+class gravityConfiguration:
+    """moduleConfigurations/gravity.py:18-27 (same defaults: inactive, 9.81 along -y)."""
+    active: bool = False
+    type: GravityType = GravityType.Directional
+    magnitude: float = 9.81
+    direction: List[float] = field(default_factory=lambda: [0.0, -1.0])
+    origin: List[float] = field(default_factory=lambda: [0.0, 0.0])
+
+
+def buildDefaultGravityConfiguration() -> gravityConfiguration:
+    return gravityConfiguration()
+
+
+class SurfaceDetectionScheme(Enum):
+    ColorField = 0
+    ColorFieldGrad = 1
+    Barecasco = 2
+    Maronne = 3
+
+
+@dataclass
+class SurfaceDetectionConfig:
+    """moduleConfigurations/surfaceDetection.py:22-35; the schemes' default config is
+    inactive (buildDefaultSurfaceDetectionConfig, :38-48)."""
+    active: bool = False
+    colorFieldThreshold: float = 0.75
+    colorFieldGradThreshold: float = 10.0
+    barecascoThreshold: float = math.pi / 3
+    expansionIterations: int = 1
+    scheme: SurfaceDetectionScheme = SurfaceDetectionScheme.Barecasco
+
+
+def buildDefaultSurfaceDetectionConfig() -> SurfaceDetectionConfig:
+    return SurfaceDetectionConfig()
+
+
+@dataclass
+class ShiftProperties:
+    """moduleConfigurations/shifting.py:18-37 with the defaults of
+    buildDefaultShiftProperties (:40-53): one delta-plus iteration, CFL 0.3, active."""
+    iterations: int = 1
+    CFL: float = 0.3
+    computeMach: bool = True
+    maxC: float = 0.3
+    active: bool = True
+    scheme: str = "deltaSPH"
+    projectionScheme: str = "mat"
+    summationDensity: bool = False
+    surfaceScaling: float = 0.1
+    threshold: float = 0.5
+    projectQuantities: bool = False
+    correctdrhodt: bool = False
+    correctdvdt: bool = False
+    reuseNormals: bool = True
+
+
+def buildDefaultShiftProperties() -> ShiftProperties:
+    return ShiftProperties()
 
 
 def buildDefaultFluidProperties() -> fluidProperties:
@@ -364,10 +436,34 @@ def buildDefaultFluidProperties() -> fluidProperties:
 
 
 @dataclass
+class WeaklyCompressibleDiffusionParams:
+    """configurations/moduleConfigurations/weaklyCompressibleDiffusionParams.py:10-26."""
+    inviscid: bool = True
+    inviscidAlpha: float = 0.01
+    viscidNu: float = 1e-3
+    densityDelta: float = 0.1
+    densityDiffusionTerm: Any = "deltaSPH"
+
+
+@dataclass
 class IncompressibleSPHConfig:
-    """configurations/incompressible.py:32-68, restricted to the fields the pressure
-    solves use (fluid, solverConfig)."""
+    """configurations/incompressible.py:32-68: the fields dfsph_step and its finalize read.
+    Boundary conditions, regions and rigid bodies are accepted as the reference declares
+    them and rejected by the step when non-empty."""
     fluid: fluidProperties = field(default_factory=buildDefaultFluidProperties)
+    adaptiveSupportScheme: Any = None
+    adaptiveSupportIterations: int = 1
+    adaptiveSupportThreshold: float = 1e-3
+    adaptiveSupportCorrections: bool = True
+    diffusionParams: WeaklyCompressibleDiffusionParams = field(default_factory=WeaklyCompressibleDiffusionParams)
+    schemeName: str = "Compressible SPH"
+    boundaryConditions: List[Any] = field(default_factory=list)
+    pressureForceTerm: Any = "Antuono"
+    shiftProperties: ShiftProperties = field(default_factory=buildDefaultShiftProperties)
+    regions: List[Any] = field(default_factory=list)
+    rigidBodies: List[Any] = field(default_factory=list)
+    surfaceDetectionConfig: SurfaceDetectionConfig = field(default_factory=buildDefaultSurfaceDetectionConfig)
+    gravityConfig: gravityConfiguration = field(default_factory=buildDefaultGravityConfiguration)
     solverConfig: IncompressibleSolverConfig = field(default_factory=buildDefaultIncompressibleSolverConfig)
 
 
@@ -385,24 +481,25 @@ def jacobi_config(solver: RelaxedJacobiSolverConfig, restDensity: float, learned
 
 # ------------------------------------------------------------------ weakly compressible (delta-SPH)
 @dataclass
-class WeaklyCompressibleDiffusionParams:
-    """configurations/moduleConfigurations/weaklyCompressibleDiffusionParams.py:10-26."""
-    inviscid: bool = True
-    inviscidAlpha: float = 0.01
-    viscidNu: float = 1e-3
-    densityDelta: float = 0.1
-    densityDiffusionTerm: str = "deltaSPH"
-
-
-@dataclass
 class WeaklyCompressibleSPHConfig:
-    """configurations/weaklyCompressible.py:35-57, restricted to the fields of the periodic
-    delta-SPH right-hand side (fluid, diffusionParams, pressureForceTerm)."""
+    """configurations/weaklyCompressible.py:35-65: the fields deltaSPH_step and its
+    finalize read.  eosType here is used when fluid.eosType is None."""
     fluid: fluidProperties = field(default_factory=lambda: fluidProperties(restDensity=1.0, polytropicExponent=7.0, kappa=1.3,
                                                                            fixedSoundSpeed=10.0))
-    eosType: str = "stiffTait"
+    eosType: Any = "stiffTait"
+    adaptiveSupportScheme: Any = None
+    adaptiveSupportIterations: int = 1
+    adaptiveSupportThreshold: float = 1e-3
+    adaptiveSupportCorrections: bool = True
     diffusionParams: WeaklyCompressibleDiffusionParams = field(default_factory=WeaklyCompressibleDiffusionParams)
-    pressureForceTerm: str = "Antuono"
+    schemeName: str = "Compressible SPH"
+    boundaryConditions: List[Any] = field(default_factory=list)
+    pressureForceTerm: Any = "Antuono"
+    shiftProperties: ShiftProperties = field(default_factory=buildDefaultShiftProperties)
+    regions: List[Any] = field(default_factory=list)
+    rigidBodies: List[Any] = field(default_factory=list)
+    surfaceDetectionConfig: SurfaceDetectionConfig = field(default_factory=buildDefaultSurfaceDetectionConfig)
+    gravityConfig: gravityConfiguration = field(default_factory=buildDefaultGravityConfiguration)
 
 
 _EOS = {"stiffTait": 0, "Tait": 1, "isoThermal": 2, "polytropic": 3, "murnaghan": 4}
@@ -410,17 +507,24 @@ _DDIFF = {"deltaSPH": 0, "densityOnly": 2, "deltaOnly": 3}
 _PTERM = {"conservative": 0, "nonConservative": 1, "Antuono": 2, "i": 3, "j": 4, "symmetric": 5}
 
 
-def wc_params(cfg: WeaklyCompressibleSPHConfig) -> _capi.SphWcParams:
-    """Packs a WeaklyCompressibleSPHConfig into the C ABI's SphWcParams."""
+def _name(v) -> str:
+    """An enum member's name or the string itself (the reference passes enums)."""
+    return v.name if isinstance(v, Enum) else str(v)
+
+
+def wc_params(cfg) -> _capi.SphWcParams:
+    """Packs a WeaklyCompressibleSPHConfig (or IncompressibleSPHConfig) into the C ABI's
+    SphWcParams."""
     w = _capi.SphWcParams()
     f, d = cfg.fluid, cfg.diffusionParams
-    w.rest_density, w.sound_speed = float(f.restDensity), float(f.fixedSoundSpeed)
+    w.rest_density, w.sound_speed = float(f.restDensity), float(f.fixedSoundSpeed if f.fixedSoundSpeed is not None else 1.0)
     w.polytropic_exponent, w.kappa = float(f.polytropicExponent), float(f.kappa)
     w.density_delta, w.viscosity_nu, w.inviscid_alpha = float(d.densityDelta), float(d.viscidNu), float(d.inviscidAlpha)
     w.inviscid = int(bool(d.inviscid))
-    w.density_scheme = _DDIFF[d.densityDiffusionTerm]
-    w.pressure_term = _PTERM[cfg.pressureForceTerm]
-    w.eos = _EOS[cfg.eosType]
+    w.density_scheme = _DDIFF[_name(d.densityDiffusionTerm)]
+    w.pressure_term = _PTERM[_name(cfg.pressureForceTerm)]
+    eos = f.eosType if getattr(f, "eosType", None) is not None else getattr(cfg, "eosType", "isoThermal")
+    w.eos = _EOS[_name(eos)]
     return w
 
 
@@ -468,3 +572,54 @@ def make_params(config: SimulationConfig, scheme: Optional[CompressibleSPHConfig
             p.force_vanleer_off = int(bool(cv.forceVanLeerOff))
             p.force_vanleer_on = int(bool(cv.forceVanLeerOn))
     return p
+
+
+# ------------------------------------------------------------------ dict round trips of the WC / DFSPH configs
+def _to_dict(obj) -> Any:
+    import dataclasses
+    if dataclasses.is_dataclass(obj):
+        return {f.name: _to_dict(getattr(obj, f.name)) for f in dataclasses.fields(obj)}
+    if isinstance(obj, Enum):
+        return obj.name
+    if isinstance(obj, torch.Tensor):
+        return obj.detach().cpu().tolist()
+    if isinstance(obj, (list, tuple)):
+        return [_to_dict(v) for v in obj]
+    return obj
+
+
+def _from_dict(cls, d: Dict[str, Any]):
+    import dataclasses
+    import typing
+    hints = typing.get_type_hints(cls)
+    kw = {}
+    defaults = cls()
+    for f in dataclasses.fields(cls):
+        if f.name not in d:
+            continue
+        v, cur = d[f.name], getattr(defaults, f.name)
+        if dataclasses.is_dataclass(cur) and isinstance(v, dict):
+            v = _from_dict(type(cur), v)
+        elif isinstance(cur, Enum) and isinstance(v, str):
+            v = type(cur)[v]
+        kw[f.name] = v
+    return cls(**kw)
+
+
+def weaklyCompressibleConfigToDict(config: WeaklyCompressibleSPHConfig) -> Dict[str, Any]:
+    """configurations/weaklyCompressible.py (weaklyCompressibleConfigToDict): enums by name."""
+    return _to_dict(config)
+
+
+def dictToWeaklyCompressibleConfig(d: Dict[str, Any]) -> WeaklyCompressibleSPHConfig:
+    return _from_dict(WeaklyCompressibleSPHConfig, d)
+
+
+def incompressibleConfigToDict(config: IncompressibleSPHConfig) -> Dict[str, Any]:
+    """configurations/incompressible.py:71-130 (incompressibleConfigToDict): enums by name."""
+    return _to_dict(config)
+
+
+def dictToIncompressibleSPHConfig(d: Dict[str, Any]) -> IncompressibleSPHConfig:
+    return _from_dict(IncompressibleSPHConfig, d)
+

@@ -8,8 +8,11 @@ Tableaux (restated; the package's own choice is not visible):
   rungeKutta2 (Heun)  c=[0,1],        a21=1,                    b=[1/2,1/2]
   rungeKutta4         c=[0,1/2,1/2,1], a21=a32=1/2, a43=1,       b=[1/6,1/3,1/3,1/6]
 Stage s starts from a copy of stage s-1's state (so non-integrated fields such as
-the supports carry over), with positions, velocities and internal energies set to
-y0 + dt * sum_k a_sk K_k; periodic positions are wrapped into the domain.  After
+the supports carry over), with the system's integrated fields (positions, velocities
+and internal energies, or densities for the incompressible and weakly compressible
+systems) set to y0 + dt * sum_k a_sk K_k; periodic positions are wrapped into the
+domain.  Step functions may return more than (update, adjacency, state); the extra
+values are kept in the stage's return values for ``finalize``.  After
 the last stage the integrated fields are y0 + dt * sum_s b_s K_s and the system's
 ``finalize`` runs (compatible energy).
 """
@@ -43,6 +46,11 @@ _TABLEAUX = {
 }
 
 
+# (state field, update field, wrap periodic positions) of the compressible systems;
+# other systems declare their own table as INTEGRATED
+_COMPRESSIBLE_FIELDS = (("positions", "dxdt", True), ("velocities", "dvdt", False), ("internalEnergies", "dudt", False))
+
+
 class RungeKuttaIntegrator:
     def __init__(self, scheme: IntegrationSchemeType):
         if scheme not in _TABLEAUX:
@@ -63,23 +71,28 @@ class RungeKuttaIntegrator:
         updates, returnValues = [], []
         prev = S0
         adjacency = sys0.adjacency
+        fields = getattr(type(sys0), "INTEGRATED", _COMPRESSIBLE_FIELDS)
+
+        def advance(Ss, weights):
+            for name, deriv, wrap in fields:
+                y0 = getattr(S0, name)
+                if y0 is None:
+                    continue
+                setattr(Ss, name, self._combine(params, y0, [getattr(u, deriv) for u in updates], weights, dt, dim if wrap else 0))
+
         for s in range(len(self.b)):
             Ss = prev.initializeNewState()
             if s > 0:
-                aw = self.a[s]
-                Ss.positions = self._combine(params, S0.positions, [u.dxdt for u in updates], aw, dt, dim)
-                Ss.velocities = self._combine(params, S0.velocities, [u.dvdt for u in updates], aw, dt, 0)
-                Ss.internalEnergies = self._combine(params, S0.internalEnergies, [u.dudt for u in updates], aw, dt, 0)
+                advance(Ss, self.a[s])
             t_s = sys0.t + self.c[s] * (float(dt) if not isinstance(dt, torch.Tensor) else 0.0)
             sys_s = type(sys0)(state=Ss, adjacency=adjacency, domain=sys0.domain, t=t_s)
-            update, adjacency, Sout = f(sys_s, dt, config, compParams, verbose=verbose)
+            out = f(sys_s, dt, config, compParams, verbose=verbose)
+            update, adjacency, Sout = out[0], out[1], out[2]
             updates.append(update)
-            returnValues.append((adjacency, Sout))
+            returnValues.append(tuple(out[1:]))
             prev = Sout
         Sf = prev.initializeNewState()
-        Sf.positions = self._combine(params, S0.positions, [u.dxdt for u in updates], self.b, dt, dim)
-        Sf.velocities = self._combine(params, S0.velocities, [u.dvdt for u in updates], self.b, dt, 0)
-        Sf.internalEnergies = self._combine(params, S0.internalEnergies, [u.dudt for u in updates], self.b, dt, 0)
+        advance(Sf, self.b)
         new_sys = type(sys0)(state=Sf, adjacency=adjacency, domain=sys0.domain, t=sys0.t)
         new_sys.finalize(sys0, dt, returnValues, updates, self.b, config, compParams)
         new_sys.t = sys0.t + (float(dt) if not isinstance(dt, torch.Tensor) else 0.0)

@@ -678,6 +678,31 @@ def deltasph_rhs(params, wc, x, H, m, rho, v, adj: AdjacencyList):
     return dvdt, drhodt, scratch[: n * d].view(n, d), scratch[n * d:]
 
 
+def wc_visc_continuity(params, wc, x, H, m, rho, v, adj: AdjacencyList):
+    """Velocity diffusion and continuity of the DFSPH step: (dvdt_diss [n, dim], drhodt [n])."""
+    n, d = m.shape[0], int(params.dim)
+    dvdt, drhodt = _empty((n, d), m), _empty(n, m)
+    with _timed("wc_visc_continuity"):
+        check(_capi.lib().sph_wc_visc_continuity(_p(params), C.cast(C.pointer(wc), C.c_void_p), n, fptr(x), fptr(H), fptr(m), fptr(rho),
+                                                 fptr(v), *_lists(params, adj, True), ptr(dvdt), ptr(drhodt), stream_ptr(m.device)),
+              "sph_wc_visc_continuity")
+    return dvdt, drhodt
+
+
+def delta_shift(params, x, H, m, rho, v, kinds, adj: AdjacencyList, cfl: float, c0: float, R: float = 0.25, nexp: int = 4,
+                rho0: float = 1.0) -> torch.Tensor:
+    """One delta-plus shift [n, dim] (zero for kinds != 0; kinds may be None)."""
+    n, d = m.shape[0], int(params.dim)
+    out = _empty((n, d), m)
+    scratch = torch.empty(2, dtype=torch.int32, device=m.device)
+    k = None if kinds is None else kinds.to(torch.int32).contiguous()
+    with _timed("delta_shift"):
+        check(_capi.lib().sph_delta_shift(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(_f32(v)), iptr(k),
+                                          *_lists(params, adj, True), float(cfl), float(c0), float(R), int(nexp), float(rho0),
+                                          ptr(scratch), ptr(out), stream_ptr(m.device)), "sph_delta_shift")
+    return out
+
+
 def wc_eos(wc, rho) -> torch.Tensor:
     out = torch.empty_like(rho)
     check(_capi.lib().sph_wc_eos(C.cast(C.pointer(wc), C.c_void_p), rho.shape[0], fptr(rho), ptr(out), stream_ptr(rho.device)),

@@ -24,7 +24,7 @@ from .configurations import (CompSPHConfig, CompressibleSPHConfig, CRKSPHConfig,
                              compSPHConfigToDict, crkSPHConfigToDict, dictToCompressibleConfig, dictToCompSPHConfig,
                              dictToCRKSPHConfig, make_params)
 from .core import AdjacencyList, SupportScheme, sphKernel_xi, volumeToSupportHelper
-from .enumTypes import AdaptiveSupportScheme, CompressibleSPHScheme, ViscositySwitch
+from .enumTypes import AdaptiveSupportScheme, CompressibleSPHScheme, IncompressibleSPHScheme, ViscositySwitch, WeaklyCompressibleSPHScheme
 from .systems import CompressibleState, CompressibleSystem, CompressibleSystemUpdate, CompSPHState, CompSPHSystem
 
 
@@ -173,4 +173,16 @@ def buildScheme(schemeName: Union[str, CompressibleSPHScheme]):
         from .compsph import compressibleSPH_Monaghan
         return (CompressibleSystem, CompressibleState, CompressibleSPHConfig, CompressibleSystemUpdate, compressibleSPH_Monaghan,
                 compressibleConfigToDict, dictToCompressibleConfig)
+    if (isinstance(schemeName, str) and schemeName == "deltaSPH") or schemeName == WeaklyCompressibleSPHScheme.deltaSPH:
+        from .configurations import WeaklyCompressibleSPHConfig, dictToWeaklyCompressibleConfig, weaklyCompressibleConfigToDict
+        from .systems import WeaklyCompressibleState, WeaklyCompressibleSystem, WeaklyCompressibleSystemUpdate
+        from .wcsph import deltaSPH_step
+        return (WeaklyCompressibleSystem, WeaklyCompressibleState, WeaklyCompressibleSPHConfig, WeaklyCompressibleSystemUpdate,
+                deltaSPH_step, weaklyCompressibleConfigToDict, dictToWeaklyCompressibleConfig)
+    if (isinstance(schemeName, str) and schemeName in ("divergenceFree", "dfsph")) or schemeName == IncompressibleSPHScheme.divergenceFree:
+        from .configurations import IncompressibleSPHConfig, dictToIncompressibleSPHConfig, incompressibleConfigToDict
+        from .systems import IncompressibleState, IncompressibleSystem, IncompressibleSystemUpdate
+        from .wcsph import dfsph_step
+        return (IncompressibleSystem, IncompressibleState, IncompressibleSPHConfig, IncompressibleSystemUpdate, dfsph_step,
+                incompressibleConfigToDict, dictToIncompressibleSPHConfig)
     raise ValueError(f"Scheme {schemeName} not recognized.")

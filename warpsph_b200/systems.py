@@ -100,3 +100,84 @@ class CompSPHSystem:
 
 
 CompressibleSystem = CompSPHSystem
+
+
+# ------------------------------------------------------------------ incompressible and weakly compressible
+@dataclass
+class IncompressibleState:
+    """systems/incompressible.py:15-35: positions, velocities and densities are integrated
+    (dxdt, dvdt, drhodt); the rest is recomputed by the step function."""
+    positions: torch.Tensor
+    velocities: torch.Tensor
+    supports: torch.Tensor
+    masses: torch.Tensor
+    densities: Optional[torch.Tensor] = None
+    kinds: Optional[torch.Tensor] = None
+    materials: Optional[torch.Tensor] = None
+    UIDs: Optional[torch.Tensor] = None
+    UIDcounter: int = 0
+    pressures: Optional[torch.Tensor] = None
+    soundspeeds: Optional[torch.Tensor] = None
+    surfaceIndicators: Optional[torch.Tensor] = None
+    surfaceNormals: Optional[torch.Tensor] = None
+    surfaceLambdas: Optional[torch.Tensor] = None
+    ghostIndices: Optional[torch.Tensor] = None
+    ghostOffsets: Optional[torch.Tensor] = None
+
+    def initializeNewState(self):
+        return dataclasses.replace(self)
+
+    def clone(self):
+        kw = {}
+        for f in dataclasses.fields(self):
+            v = getattr(self, f.name)
+            kw[f.name] = v.clone() if isinstance(v, torch.Tensor) else v
+        return type(self)(**kw)
+
+
+@dataclass
+class IncompressibleSystemUpdate:
+    """systems/incompressible.py:37-42."""
+    dxdt: torch.Tensor
+    dvdt: torch.Tensor
+    drhodt: torch.Tensor
+    passive: Optional[torch.Tensor] = None
+
+
+_DENSITY_FIELDS = (("positions", "dxdt", True), ("velocities", "dvdt", False), ("densities", "drhodt", False))
+_LAST_STAGE_FIELDS = ("supports", "pressures", "soundspeeds", "surfaceIndicators", "surfaceNormals", "surfaceLambdas")
+
+
+@dataclass
+class IncompressibleSystem:
+    """systems/incompressible.py:47-277.  ``finalize`` copies the last stage's fields,
+    rebuilds the Verlet list, recomputes the gather density and moves the particles by
+    dt^2 times the density solve's pressure acceleration (:213-256)."""
+    state: IncompressibleState
+    adjacency: Optional[AdjacencyList] = None
+    domain: Optional[DomainDescription] = None
+    t: float = 0.0
+    INTEGRATED = _DENSITY_FIELDS
+
+    def initializeNewState(self, *args, verbose=False, **kwargs):
+        return type(self)(state=self.state.initializeNewState(), adjacency=self.adjacency, t=self.t, domain=self.domain)
+
+    def finalize(self, initialState, dt, returnValues, updateValues, weights, config, schemeConfig, *args, **kwargs):
+        from . import wcsph
+        return wcsph.finalize_incompressible(self, initialState, dt, returnValues, updateValues, config, schemeConfig)
+
+
+WeaklyCompressibleState = IncompressibleState   # systems/weaklyCompressible.py:14-35 declares the same fields
+WeaklyCompressibleSystemUpdate = IncompressibleSystemUpdate
+
+
+@dataclass
+class WeaklyCompressibleSystem(IncompressibleSystem):
+    """systems/weaklyCompressible.py:43-200.  ``finalize`` copies the last stage's fields,
+    applies the delta-plus shift when shiftProperties.active (computed before the density
+    update, added to the positions after it) and sets the density by the exponential
+    update rho0 exp(dt drhodt_last / rho_last) of the last stage (:179-186)."""
+
+    def finalize(self, initialState, dt, returnValues, updateValues, weights, config, schemeConfig, *args, **kwargs):
+        from . import wcsph
+        return wcsph.finalize_weakly_compressible(self, initialState, dt, returnValues, updateValues, config, schemeConfig)

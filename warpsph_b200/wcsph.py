@@ -1,0 +1,196 @@
+"""DFSPH and delta-SPH step functions on the GPU, with the finalize steps of their systems.
+
+``dfsph_step`` follows src/warpSPH/schemes/dfsph.py:13-218 and ``deltaSPH_step``
+follows schemes/deltaSPH.py:11-208, call for call, for fluid-only systems:
+
+  Verlet list (super-symmetric rows)      dfsph.py:27     -> sph_neighbors_build / refresh
+  gather density                          dfsph.py:36-40  -> sph_density_gather
+  mDBC density, boundary velocities,      dfsph.py:48-59, -> identities without boundary particles
+  Dirichlet conditions, forcing, no-pen.  :106-126           (the reference's own early returns)
+  free-surface detection                  dfsph.py:72-77  -> inactive by default: zero indicators
+  velocity diffusion + continuity         dfsph.py:100-109 -> sph_wc_visc_continuity (one pass)
+  gravity                                 dfsph.py:117-120 -> computeGravity (elementwise)
+  divergence-free solve                   dfsph.py:132-140 -> sph_dfsph_div_solve (persistent kernel)
+
+  delta-SPH right-hand side               deltaSPH.py:52-98 -> sph_deltasph_rhs (EOS, renormalised
+                                                               density gradient, density and
+                                                               velocity diffusion, continuity,
+                                                               pressure force in two passes)
+
+Systems with boundary (kind 1) or ghost (kind 2) particles, boundary conditions, rigid
+bodies or active surface detection need the mDBC, boundary-condition and surface passes,
+which are not on the GPU path; the steps raise NotImplementedError for them.
+"""
+from __future__ import annotations
+
+from typing import Any
+
+import torch
+
+from . import ops
+from .configurations import GravityType, make_params, wc_params
+from .core import SupportScheme
+from .incompressible import solveDivergenceFree, solveIncompressible
+from .systems import _LAST_STAGE_FIELDS, IncompressibleSystemUpdate, WeaklyCompressibleSystemUpdate
+
+_KINDS_CHECKED: dict = {}
+
+
+def _check_supported(state, schemeConfig) -> None:
+    if getattr(schemeConfig, "boundaryConditions", None):
+        raise NotImplementedError("boundary conditions are not on the GPU path")
+    if getattr(schemeConfig, "rigidBodies", None):
+        raise NotImplementedError("rigid bodies are not on the GPU path")
+    sd = getattr(schemeConfig, "surfaceDetectionConfig", None)
+    if sd is not None and sd.active:
+        raise NotImplementedError("free-surface detection is not on the GPU path (it is inactive by default)")
+    k = state.kinds
+    if k is not None:
+        key = (id(k), k._version)
+        if _KINDS_CHECKED.get(id(k)) != key:
+            if bool((k != 0).any()):
+                raise NotImplementedError("boundary and ghost particles (kinds != 0) need the mDBC passes, which are not on the GPU path")
+            _KINDS_CHECKED.clear()
+            _KINDS_CHECKED[id(k)] = key
+
+
+def computeGravity(currentState: Any, config: Any, schemeConfig: Any, adjacency=None) -> torch.Tensor:
+    """modules/gravity/wrapper.py:20-34.  Directional (directional.py:12-22): the constant
+    magnitude * direction.  Point source (pointGravity.py:13-29): magnitude times the unit
+    vector towards the origin, per particle (the reference's trailing .repeat(n, 1) turns
+    that [n, d] field into an [n^2, d] tensor, which no caller can use; the per-particle
+    field is returned here)."""
+    g = schemeConfig.gravityConfig
+    v = currentState.velocities
+    if not g.active:
+        return torch.zeros_like(v)
+    d = v.shape[1]
+    if g.type == GravityType.Directional:
+        direction = torch.as_tensor(g.direction, dtype=v.dtype, device=v.device)[:d]
+        return (direction * g.magnitude).expand(v.shape[0], d).contiguous()
+    if g.type == GravityType.PointSource:
+        origin = torch.as_tensor(g.origin, dtype=v.dtype, device=v.device)[:d]
+        direction = origin - currentState.positions
+        norm = torch.linalg.vector_norm(direction, dim=1, keepdim=True)
+        return direction / (norm + 1e-8) * g.magnitude
+    raise NotImplementedError(f"gravity type {g.type} is not on the GPU path")
+
+
+def _zero_surface(S) -> None:
+    """detectFreeSurface with an inactive configuration (surfaceDetection/wrapper.py:93-96)."""
+    S.surfaceIndicators = torch.zeros(S.positions.shape[0], dtype=torch.int32, device=S.positions.device)
+    S.surfaceNormals = torch.zeros_like(S.positions)
+    S.surfaceLambdas = None
+
+
+def _passive(S) -> torch.Tensor:
+    return torch.zeros(S.densities.shape, device=S.densities.device, dtype=torch.bool)
+
+
+def dfsph_step(system, dt, config, schemeConfig, verbose: bool = False):
+    """schemes/dfsph.py:13-218 on the GPU.  Returns (update, adjacency, state, (errors, pressures))."""
+    S = system.state
+    _check_supported(S, schemeConfig)
+    params = make_params(config)
+    adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, system.adjacency)
+    system.adjacency = adjacency
+    if S.densities is None or not schemeConfig.solverConfig.integrateRho:
+        S.densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
+    _zero_surface(S)
+    dvdt_diss, drhodt = ops.wc_visc_continuity(params, wc_params(schemeConfig), S.positions, S.supports, S.masses, S.densities,
+                                               S.velocities, adjacency)
+    dvdt = computeGravity(S, config, schemeConfig, adjacency)
+    if S.pressures is None:
+        S.pressures = torch.zeros_like(S.densities)
+    dvdt_pressure, pressure, errors, pressures = solveDivergenceFree(S, config, schemeConfig, adjacency, dvdt + dvdt_diss, dt)
+    S.pressures = pressure
+    update = IncompressibleSystemUpdate(dxdt=S.velocities.clone(), dvdt=dvdt + dvdt_diss + dvdt_pressure, drhodt=drhodt,
+                                        passive=_passive(S))
+    return update, adjacency, S, (errors, pressures)
+
+
+def deltaSPH_step(system, dt, config, schemeConfig, verbose: bool = False):
+    """schemes/deltaSPH.py:11-208 on the GPU.  Returns (update, adjacency, state)."""
+    S = system.state
+    _check_supported(S, schemeConfig)
+    params = make_params(config)
+    adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, system.adjacency)
+    system.adjacency = adjacency
+    if S.densities is None:
+        S.densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
+    _zero_surface(S)
+    dvdt_rhs, drhodt, _, P = ops.deltasph_rhs(params, wc_params(schemeConfig), S.positions, S.supports, S.masses, S.densities,
+                                              S.velocities, adjacency)
+    S.pressures = P
+    update = WeaklyCompressibleSystemUpdate(dxdt=S.velocities.clone(), dvdt=dvdt_rhs + computeGravity(S, config, schemeConfig, adjacency),
+                                            drhodt=drhodt, passive=_passive(S))
+    return update, adjacency, S
+
+
+def _add_positions(params, x, dx, dim) -> torch.Tensor:
+    """x + dx, wrapped into the periodic axes of the domain."""
+    return ops.rk_combine(params, x, [dx.contiguous()], [1.0], 1.0, dim)
+
+
+def solveShifting(state, config, schemeConfig, adjacency, dt):
+    """modules/shifting/wrapper.py:20-135 for a domain without free surface: per iteration
+    the Verlet list at the shifted positions and one delta-plus shift
+    (modules/shifting/delta.py), zero for kinds != 0.  Returns (dx, adjacency): the summed
+    shift, the state itself left unchanged."""
+    sp = schemeConfig.shiftProperties
+    params = make_params(config)
+    dim = int(config.dim)
+    c0 = schemeConfig.fluid.fixedSoundSpeed if schemeConfig.fluid.fixedSoundSpeed is not None else 1.0
+    x = state.positions
+    dx = torch.zeros_like(x)
+    for _ in range(int(sp.iterations)):
+        adjacency = ops.buildVerletList(x, state.supports, params, config.verletScale, adjacency)
+        rho = (ops.density(params, x, state.supports, state.masses, adjacency, SupportScheme.Gather) if sp.summationDensity
+               else state.densities)
+        upd = ops.delta_shift(params, x, state.supports, state.masses, rho, state.velocities, state.kinds, adjacency, sp.CFL, c0)
+        dx = dx + upd
+        x = _add_positions(params, x, upd, dim)
+    return dx, adjacency
+
+
+def finalize_incompressible(system, initialState, dt, returnValues, updateValues, config, schemeConfig):
+    """systems/incompressible.py:71-277.  The delta-plus shift the reference computes when
+    shiftProperties.active (:134-209) is not applied anywhere (the lines that would apply
+    it, :262-267, are commented out), so it is not evaluated here."""
+    last = returnValues[-1][1]
+    S = system.state
+    for name in _LAST_STAGE_FIELDS + ("densities",):
+        setattr(S, name, getattr(last, name))
+    params = make_params(config)
+    adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, returnValues[-1][0])
+    S.densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
+    zero = torch.zeros_like(S.velocities)
+    dvdt_incomp, _, errors_incomp, pressures_incomp = solveIncompressible(S, config, schemeConfig, adjacency, zero, dt)
+    # positions += dt^2 a_p of the density solve (:250-255)
+    S.positions = _add_positions(params, S.positions, (dt * dt) * dvdt_incomp, int(config.dim))
+    system.adjacency = adjacency
+    returnValues[-1] = tuple(returnValues[-1][:3]) + ((errors_incomp, pressures_incomp),)
+    return system
+
+
+def finalize_weakly_compressible(system, initialState, dt, returnValues, updateValues, config, schemeConfig):
+    """systems/weaklyCompressible.py:73-200: the last stage's fields, the delta-plus shift
+    (computed before the density update, added after it), and the exponential density
+    update rho0 exp(dt drhodt / rho) from the last stage (:179-186)."""
+    last = returnValues[-1][1]
+    S = system.state
+    for name in _LAST_STAGE_FIELDS:
+        setattr(S, name, getattr(last, name))
+    sp = schemeConfig.shiftProperties
+    adjacency = returnValues[-1][0]
+    dx = None
+    if sp.active:
+        if sp.correctdrhodt or sp.correctdvdt:
+            raise NotImplementedError("the shift corrections of drho/dt and dv/dt are not on the GPU path (off by default)")
+        dx, adjacency = solveShifting(S, config, schemeConfig, adjacency, dt)
+    rho_mid = last.densities
+    S.densities = initialState.state.densities * torch.exp(dt * updateValues[-1].drhodt / rho_mid)
+    if dx is not None:
+        S.positions = _add_positions(make_params(config), S.positions, dx, int(config.dim))
+    system.adjacency = adjacency
+    return system
