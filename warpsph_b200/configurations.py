@@ -547,7 +547,9 @@ def make_params(config: SimulationConfig, scheme: Optional[CompressibleSPHConfig
     p.min_dt = float(config.minDt if config.minDt is not None else 0.0)
     p.max_dt = float(config.maxDt if config.maxDt is not None else 1e30)
     p.dt_growth = float(config.dtGrowthFactor if config.dtGrowthFactor is not None else 1e30)
-    if scheme is not None:
+    # the weakly compressible and incompressible configurations carry their parameters in
+    # SphWcParams / SphJacobiConfig (wc_params, jacobi_config)
+    if isinstance(scheme, CompressibleSPHConfig):
         dp = scheme.diffusionParams
         p.C_l, p.C_q, p.Cu_l, p.Cu_q, p.K = float(dp.C_l), float(dp.C_q), float(dp.Cu_l), float(dp.Cu_q), float(dp.K)
         p.viscosity_term = _term_value(dp.viscosityTerm)
