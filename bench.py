@@ -54,6 +54,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-compsph", action="store_true", help="skip the CompSPH Sedov 2D throughput")
     ap.add_argument("--no-sedov3d", action="store_true", help="skip the CRKSPH Sedov 3D (128^3) throughput")
     ap.add_argument("--no-mlp", action="store_true", help="skip the warm-start MLP forward throughput")
+    ap.add_argument("--mlp-samples", type=int, default=1 << 24, help="feature rows of the MLP forward section")
     ap.add_argument("--nx3d", type=int, default=128, help="lattice size of the CRKSPH Sedov 3D section (nx^3 particles)")
     return ap.parse_args(argv)
 
@@ -533,7 +534,7 @@ def gpu_arm(args, rank: int, world: int):
 
     mlp = None
     if rank == 0 and world == 1 and not args.no_mlp:
-        mlp = mlp_forward_throughput(dev)
+        mlp = mlp_forward_throughput(dev, n=args.mlp_samples)
     comp = None
     if rank == 0 and world == 1 and not args.no_compsph:
         d, K = 2, 32.0

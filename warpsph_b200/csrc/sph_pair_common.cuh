@@ -68,10 +68,16 @@ struct KSum {
     }
 };
 
-// group sizes (lanes per particle) of the pair passes
+// group sizes (lanes per particle) of the pair passes (a build may override them)
+#ifndef G_LIGHT
 #define G_LIGHT 8
+#endif
+#ifndef G_HEAVY
 #define G_HEAVY 8
+#endif
+#ifndef G_CRK
 #define G_CRK 4
+#endif
 
 #define WSPH_DISPATCH_KDS(params, ...) WSPH_DISPATCH_KD(P.kernel, P.dim, __VA_ARGS__)
 #define WSPH_DISPATCH_DS(params, ...) WSPH_DISPATCH_DIM(P.dim, __VA_ARGS__)
