@@ -543,7 +543,7 @@ def gpu_arm(args, rank: int, world: int):
         comp["workload"] = f"Sedov 2D CompSPH {args.nx}x{args.nx}, Wendland C4, 32 neighbours, Cullen-Dehnen, RK2, compatible energy"
     s3 = None
     if rank == 0 and world == 1 and not args.no_sedov3d:
-        s3 = scheme_throughput(dev, "crkSPH", 3, args.nx3d, 128, steps=3, warmup=2, kahan=True, timed_kernel="crk_accel_dudt",
+        s3 = scheme_throughput(dev, "crkSPH", 3, args.nx3d, 128, steps=5, warmup=3, kahan=True, timed_kernel="crk_accel_dudt",
                                bytes_per_particle=bytes_accel_dudt(3, 128.0), breakdown=True)
         s3["workload"] = (f"Sedov 3D CRKSPH {args.nx3d}^3 ({args.nx3d ** 3:,} particles), Wendland C4, 128 neighbours, Cullen-Dehnen, RK2, "
                           "Kahan sums")

@@ -1113,7 +1113,7 @@ int sph_adaptive_h_iter(const SphParams* p, int64_t n, int32_t support_mode, con
     if (support_mode != SPH_SUPPORT_GATHER) return set_error(SPH_ERR_UNSUPPORTED, "adaptive support: only the gather scheme is implemented");
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_adaptive_h<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, offs, cnt, list, hbounds, rho_out, H_out, ratio_out)));
+    WSPH_DISPATCH_KDS(*p, (k_adaptive_h<KF, D, G_SCAN(D)><<<grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, offs, cnt, list, hbounds, rho_out, H_out, ratio_out)));
     return check_launch("sph_adaptive_h_iter");
 }
 
@@ -1139,7 +1139,7 @@ int sph_crk_volume(const SphParams* p, int64_t n, const float* x, const float* H
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(V_out); CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_crk_volume<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, offs, cnt, list, V_out)));
+    WSPH_DISPATCH_KDS(*p, (k_crk_volume<KF, D, G_SCAN(D)><<<grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, offs, cnt, list, V_out)));
     return check_launch("sph_crk_volume");
 }
 
@@ -1176,7 +1176,7 @@ int sph_grad_v(const SphParams* p, int64_t n, const float* x, const float* H, co
         (rc = check_align_vec(P, gradA, "gradA")))
         return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_grad_v<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
+    WSPH_DISPATCH_KDS(*p, (k_grad_v<KF, D, G_SCAN(D)><<<grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
                                                                                                   offs, cnt, list, DvDx_out, drhodt_out, div_out, vsig_out)));
     return check_launch("sph_grad_v");
 }
@@ -1191,7 +1191,7 @@ int sph_switch_cullen(const SphParams* p, int64_t n, const float* x, const float
     if (!vsig) { WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(c); }   // v_sig needs the whole Verlet rows
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_cullen<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div, div_prev, vsig, v, c,
+    WSPH_DISPATCH_KDS(*p, (k_cullen<KF, D, G_SCAN(D)><<<grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div, div_prev, vsig, v, c,
                                                                                                   alpha0_prev, dt, offs, cnt, list, alpha_out, R_out, vsig_out)));
     return check_launch("sph_switch_cullen");
 }
