@@ -499,23 +499,52 @@ def gpu_arm(args, rank: int, world: int):
         fields = ["positions", "velocities", "internalEnergies", "supports", "masses", "densities", "alpha0s", "alphas", "divergence"]
         S = state["system"].state
         host_in = {f: getattr(S, f).detach().cpu().pin_memory() for f in fields}
-        host_out = {f: torch.empty_like(host_in[f]).pin_memory() for f in fields}
+        # two pinned result buffers: step k's download may still run while step k+1 computes
+        host_out = [{f: torch.empty_like(host_in[f]).pin_memory() for f in fields} for _ in range(2)]
         h2d = sum(t.numel() * t.element_size() for t in host_in.values())
         d2h = h2d
         e2e_steps = max(3, args.steps // 2)
+        comp = torch.cuda.current_stream(dev)
+        copy = torch.cuda.Stream(dev)
+        # two device input sets: step k+1's inputs land in one while step k reads the other
+        d_in = [{f: torch.empty_like(getattr(S, f)) for f in fields} for _ in range(2)]
+
+        def upload(k):
+            """Copies step k's inputs from pinned host memory on the copy stream."""
+            with torch.cuda.stream(copy):
+                for f in fields:
+                    d_in[k % 2][f].copy_(host_in[f], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(copy)
+            return ev
+
+        def run(steps):
+            ev = upload(0)
+            for k in range(steps):
+                comp.wait_event(ev)
+                S = state["system"].state
+                for f in fields:
+                    setattr(S, f, d_in[k % 2][f])
+                if k + 1 < steps:
+                    ev = upload(k + 1)      # the next step's inputs cross while this step computes
+                one_step()
+                done = torch.cuda.Event()
+                done.record(comp)
+                copy.wait_event(done)
+                S = state["system"].state
+                with torch.cuda.stream(copy):   # this step's result crosses while the next step computes
+                    for f in fields:
+                        t = getattr(S, f)
+                        t.record_stream(copy)
+                        host_out[k % 2][f].copy_(t, non_blocking=True)
+            comp.wait_stream(copy)
+
+        run(2)   # untimed: settles the allocator's pools for this pattern
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(e2e_steps):
-            S = state["system"].state
-            for f in fields:
-                setattr(S, f, host_in[f].to(dev, non_blocking=True))
-            one_step()
-            S = state["system"].state
-            for f in fields:
-                host_out[f].copy_(getattr(S, f), non_blocking=True)
-            torch.cuda.current_stream().synchronize()
+        run(e2e_steps)
         e1.record()
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1)

@@ -364,7 +364,13 @@ __global__ void k_mlp_adam(float* __restrict__ prm, const float* __restrict__ gr
 // FP32 bias to about 2^-17 relative.  The hidden layers thus run K = 80 (five k-steps).
 // Rounding points otherwise match k_mlp_forward: BF16 features, weights and hidden
 // activations, FP32 accumulation, FP32 output layer.
-constexpr int TC_M = 128, TC_THREADS = 128, TC_TMEM_COLS = 64, TC_CTAS_PER_SM = 4;
+//
+// The layer-1 operand X [128 x 16] lives inside H: its features take H columns 56..63
+// (free until layer 1's epilogue writes them, after the first MMA has read them) and its
+// constant columns are H's bias block (columns 64..71 hold 1, 1, 0, ...; the same pattern
+// X needs in its columns 8..15).  That keeps a CTA at 43 KB of shared memory, 5 per SM.
+constexpr int TC_M = 128, TC_THREADS = 128, TC_TMEM_COLS = 64, TC_CTAS_PER_SM = 5;
+constexpr int TC_X_COL = 56;        // H column of X's first (feature) column
 constexpr int TC_K2 = MLP_H + 16;   // hidden-layer K with the bias columns
 constexpr uint32_t TC_IDESC = umma_idesc_bf16_f32<TC_M, MLP_H>();
 static_assert(TC_IDESC == 0x08100490u, "kind::f16 descriptor: BF16 x BF16 -> FP32, M = 128, N = 64, K-major");
@@ -374,7 +380,6 @@ struct MlpTcSmem {
     __nv_bfloat16 W1[MLP_H * K1];      // [64 x 16]: W1 | b1 hi | b1 lo | 0
     __nv_bfloat16 W2[MLP_H * TC_K2];   // [64 x 80]: W2 | b2 hi | b2 lo | 0
     __nv_bfloat16 W3[MLP_H * TC_K2];
-    __nv_bfloat16 X[TC_M * K1];        // [128 x 16]: features | 1 | 1 | 0
     __nv_bfloat16 H[TC_M * TC_K2];     // [128 x 80]: activations | 1 | 1 | 0
     float w4[MLP_H];
     unsigned long long bar;
@@ -383,10 +388,13 @@ struct MlpTcSmem {
     int abort;
 };
 static_assert((sizeof(__nv_bfloat16) * MLP_H * K1) % 128 == 0 && (sizeof(__nv_bfloat16) * MLP_H * TC_K2) % 128 == 0 &&
-              (sizeof(__nv_bfloat16) * TC_M * K1) % 128 == 0 && (sizeof(__nv_bfloat16) * TC_M * TC_K2) % 128 == 0,
+              (sizeof(__nv_bfloat16) * TC_M * TC_K2) % 128 == 0,
               "128 B aligned operands");
-// 4 CTAs fit in shared memory per SM; their TMEM columns must fit in the SM's 512.
-static_assert(4 * TC_TMEM_COLS <= 512 && 5 * sizeof(MlpTcSmem) > 228 * 1024, "TMEM columns of the resident CTAs");
+// 5 CTAs fit in shared memory per SM (with 1 KB reserved each), and no more; their TMEM
+// columns must fit in the SM's 512.
+static_assert(5 * (sizeof(MlpTcSmem) + 1024) <= 228 * 1024 && 6 * (sizeof(MlpTcSmem) + 1024) > 228 * 1024 &&
+              5 * TC_TMEM_COLS <= 512, "shared memory and TMEM of the resident CTAs");
+static_assert(TC_X_COL % 8 == 0 && TC_X_COL + 8 == MLP_H, "X's feature block sits just before H's bias block");
 
 // relu of (lo, hi) rounded to BF16 and packed, lo in the low half
 __device__ __forceinline__ uint32_t relu_bf16x2(uint32_t lo, uint32_t hi) {
@@ -431,7 +439,6 @@ k_mlp_forward_tc(const float* __restrict__ prm, int64_t n, const float* __restri
     if (tid == 0) s.b4 = prm[OFF_B4];
     {   // the constant columns of this thread's rows of X and H, the same for every tile
         const uint4 ones = make_uint4(pack_bf16(1.f, 1.f), 0u, 0u, 0u), zero = make_uint4(0u, 0u, 0u, 0u);
-        *reinterpret_cast<uint4*>(s.X + umma_k_index(tid, MLP_IN, TC_M)) = ones;
         *reinterpret_cast<uint4*>(s.H + umma_k_index(tid, MLP_H, TC_M)) = ones;
         *reinterpret_cast<uint4*>(s.H + umma_k_index(tid, MLP_H + 8, TC_M)) = zero;
     }
@@ -443,7 +450,7 @@ k_mlp_forward_tc(const float* __restrict__ prm, int64_t n, const float* __restri
     const uint32_t tbase = s.tmem_base;
     const uint32_t tlane = tbase + (static_cast<uint32_t>(warp * 32) << 16);
     const uint32_t bar = smem_u32(&s.bar);
-    const uint32_t aX = smem_u32(s.X), aH = smem_u32(s.H), aW1 = smem_u32(s.W1), aW2 = smem_u32(s.W2), aW3 = smem_u32(s.W3);
+    const uint32_t aX = smem_u32(s.H + umma_k_index(0, TC_X_COL, TC_M)), aH = smem_u32(s.H), aW1 = smem_u32(s.W1), aW2 = smem_u32(s.W2), aW3 = smem_u32(s.W3);
     const uint32_t LBO_A = TC_M * 16, LBO_B = MLP_H * 16, SBO = 128;
     const float sc = scale ? *scale : 1.f;
     const int64_t ntiles = (n + TC_M - 1) / TC_M;
@@ -457,7 +464,7 @@ k_mlp_forward_tc(const float* __restrict__ prm, int64_t n, const float* __restri
                 f0 = __ldg(reinterpret_cast<const float4*>(feats + row * MLP_IN));
                 f1 = __ldg(reinterpret_cast<const float4*>(feats + row * MLP_IN) + 1);
             }
-            *reinterpret_cast<uint4*>(s.X + umma_k_index(tid, 0, TC_M)) =
+            *reinterpret_cast<uint4*>(s.H + umma_k_index(tid, TC_X_COL, TC_M)) =
                 make_uint4(pack_bf16(f0.x, f0.y), pack_bf16(f0.z, f0.w), pack_bf16(f1.x, f1.y), pack_bf16(f1.z, f1.w));
         }
         fence_proxy_async_smem();
