@@ -1251,7 +1251,7 @@ int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const floa
         (rc = check_align_vec(P, ap_ij, "ap_ij")) || (rc = check_align_vec(P, av_ij, "av_ij")))
         return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_crk_accel_dudt<KF, D, G_HEAVY><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
+    WSPH_DISPATCH_KDS(*p, (k_crk_accel_dudt<KF, D, G_ACCEL><<<grid_g<G_ACCEL>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
                                                                                                           Pr, DvDx, offs, cnt, list, verlet_cnt, dvdt_out,
                                                                                                           dudt_out, dEdt_out, ap_ij, av_ij)));
     return check_launch("sph_crk_accel_dudt");
