@@ -140,7 +140,7 @@ def bytes_accel_dudt(d: int, K: float) -> float:
 # DRAM bytes (read + write) of one k_crk_accel_dudt launch from an ncu capture of the
 # 384^2 case (profiles/k_crk_accel_dudt_sedov2d_384.md), scaled to a launch of n
 # particles by particle count (the pass is per particle, so traffic grows with n).
-ACCEL_TRAFFIC_BYTES_PER_PARTICLE = (56.95e6 + 111.43e6) / 147456
+ACCEL_TRAFFIC_BYTES_PER_PARTICLE = (67.91e6 + 119.07e6) / 147456
 
 
 def load_peaks() -> dict:
