@@ -351,12 +351,15 @@ __global__ void k_mlp_adam(float* __restrict__ prm, const float* __restrict__ gr
 
 // ---------------------------------------------------------------- inference on tcgen05
 // One CTA of 4 warps takes 128 samples per tile.  Each layer is one chain of
-//   D[128 x 64] (TMEM, FP32) = A[128 x K] (shared, BF16) x W[64 x K]^T (shared, BF16)
-// of K/16 tcgen05.mma kind::f16 instructions, issued by one thread and completed through
-// tcgen05.commit on an mbarrier.  Warp w then reads TMEM lanes 32w..32w+31 (one sample
-// per thread, tcgen05.ld 32x32b), applies ReLU while rounding to BF16 (cvt.rn.relu) and
-// writes the operand of the next layer back to shared memory; the 64 -> 1 output layer
-// is an FP32 dot product in registers.
+//   D[128 x 64] (TMEM, FP32) = A[128 x K] (TMEM, BF16) x W[64 x K]^T (shared, BF16)
+// of K/16 tcgen05.mma kind::f16 instructions with A read from tensor memory, issued by one
+// thread and completed through tcgen05.commit on an mbarrier.  Warp w then reads TMEM
+// lanes 32w..32w+31 of D (one sample per thread, tcgen05.ld 32x32b), applies ReLU while
+// rounding to BF16 (cvt.rn.relu) and stores the packed pairs straight back into the A
+// columns of the next layer (tcgen05.st 32x32b).  Activations never pass through shared
+// memory, which holds only the weights: with A in shared memory every MMA re-read its
+// activations from there (about 98 KB of shared-memory traffic per tile, the limit).
+// The 64 -> 1 output layer is an FP32 dot product in registers.
 //
 // The biases ride in the contraction: A carries two constant-one columns after its real K
 // columns (X columns 8, 9; H columns 64, 65) and W the bias split into BF16 hi + lo parts
@@ -365,36 +368,36 @@ __global__ void k_mlp_adam(float* __restrict__ prm, const float* __restrict__ gr
 // Rounding points otherwise match k_mlp_forward: BF16 features, weights and hidden
 // activations, FP32 accumulation, FP32 output layer.
 //
-// The layer-1 operand X [128 x 16] lives inside H: its features take H columns 56..63
-// (free until layer 1's epilogue writes them, after the first MMA has read them) and its
-// constant columns are H's bias block (columns 64..71 hold 1, 1, 0, ...; the same pattern
-// X needs in its columns 8..15).  That keeps a CTA at 43 KB of shared memory, 5 per SM.
-constexpr int TC_M = 128, TC_THREADS = 128, TC_TMEM_COLS = 64, TC_CTAS_PER_SM = 5;
-constexpr int TC_X_COL = 56;        // H column of X's first (feature) column
+// TMEM columns of a CTA (128 allocated, 32-bit each):
+//   0..63    D, the FP32 accumulator
+//   64..103  H, the hidden-layer A operand: 64 BF16 activations (64..95), then 1, 1, 0... (96..103)
+//   104..111 X, the layer-1 A operand: 8 BF16 features (104..107), then 1, 1, 0... (108..111)
+constexpr int TC_M = 128, TC_THREADS = 128, TC_TMEM_COLS = 128, TC_CTAS_PER_SM = 4;
 constexpr int TC_K2 = MLP_H + 16;   // hidden-layer K with the bias columns
+constexpr uint32_t TC_COL_D = 0, TC_COL_H = 64, TC_COL_X = 104;
 constexpr uint32_t TC_IDESC = umma_idesc_bf16_f32<TC_M, MLP_H>();
 static_assert(TC_IDESC == 0x08100490u, "kind::f16 descriptor: BF16 x BF16 -> FP32, M = 128, N = 64, K-major");
+static_assert(TC_COL_H >= TC_COL_D + MLP_H && TC_COL_X >= TC_COL_H + TC_K2 / 2 && TC_COL_X + K1 / 2 <= TC_TMEM_COLS,
+              "TMEM column plan");
 constexpr long long TC_WAIT_CYCLES = 1ll << 31;   // about a second at B200 clocks
 
 struct MlpTcSmem {
     __nv_bfloat16 W1[MLP_H * K1];      // [64 x 16]: W1 | b1 hi | b1 lo | 0
     __nv_bfloat16 W2[MLP_H * TC_K2];   // [64 x 80]: W2 | b2 hi | b2 lo | 0
     __nv_bfloat16 W3[MLP_H * TC_K2];
-    __nv_bfloat16 H[TC_M * TC_K2];     // [128 x 80]: activations | 1 | 1 | 0
     float w4[MLP_H];
     unsigned long long bar;
     float b4;
     uint32_t tmem_base;
     int abort;
+    // keeps the CTA above a fifth of the SM's shared memory, so that no more than the 4
+    // CTAs whose 128 TMEM columns fit in 512 are resident on one SM
+    unsigned char occupancy_pad[24 * 1024];
 };
-static_assert((sizeof(__nv_bfloat16) * MLP_H * K1) % 128 == 0 && (sizeof(__nv_bfloat16) * MLP_H * TC_K2) % 128 == 0 &&
-              (sizeof(__nv_bfloat16) * TC_M * TC_K2) % 128 == 0,
+static_assert((sizeof(__nv_bfloat16) * MLP_H * K1) % 128 == 0 && (sizeof(__nv_bfloat16) * MLP_H * TC_K2) % 128 == 0,
               "128 B aligned operands");
-// 5 CTAs fit in shared memory per SM (with 1 KB reserved each), and no more; their TMEM
-// columns must fit in the SM's 512.
-static_assert(5 * (sizeof(MlpTcSmem) + 1024) <= 228 * 1024 && 6 * (sizeof(MlpTcSmem) + 1024) > 228 * 1024 &&
-              5 * TC_TMEM_COLS <= 512, "shared memory and TMEM of the resident CTAs");
-static_assert(TC_X_COL % 8 == 0 && TC_X_COL + 8 == MLP_H, "X's feature block sits just before H's bias block");
+static_assert(4 * (sizeof(MlpTcSmem) + 1024) <= 228 * 1024 && 5 * (sizeof(MlpTcSmem) + 1024) > 228 * 1024 &&
+              4 * TC_TMEM_COLS <= 512, "4 resident CTAs per SM, within the SM's TMEM columns");
 
 // relu of (lo, hi) rounded to BF16 and packed, lo in the low half
 __device__ __forceinline__ uint32_t relu_bf16x2(uint32_t lo, uint32_t hi) {
@@ -437,37 +440,39 @@ k_mlp_forward_tc(const float* __restrict__ prm, int64_t n, const float* __restri
     }
     if (tid < MLP_H) s.w4[tid] = prm[OFF_W4 + tid];
     if (tid == 0) s.b4 = prm[OFF_B4];
-    {   // the constant columns of this thread's rows of X and H, the same for every tile
-        const uint4 ones = make_uint4(pack_bf16(1.f, 1.f), 0u, 0u, 0u), zero = make_uint4(0u, 0u, 0u, 0u);
-        *reinterpret_cast<uint4*>(s.H + umma_k_index(tid, MLP_H, TC_M)) = ones;
-        *reinterpret_cast<uint4*>(s.H + umma_k_index(tid, MLP_H + 8, TC_M)) = zero;
-    }
     fence_proxy_async_smem();
     tc_fence_before_sync();
     __syncthreads();
     tc_fence_after_sync();
 
     const uint32_t tbase = s.tmem_base;
-    const uint32_t tlane = tbase + (static_cast<uint32_t>(warp * 32) << 16);
+    const uint32_t tlane = tbase + (static_cast<uint32_t>(warp * 32) << 16);   // this warp's 32 lanes
+    {   // the constant columns of this thread's row of H and X, the same for every tile
+        const uint32_t one2 = pack_bf16(1.f, 1.f);
+        const uint32_t hb[8] = {one2, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        tmem_st_32x32b_x8(tlane + TC_COL_H + MLP_H / 2, hb);
+        tmem_st_32x32b_x4(tlane + TC_COL_X + MLP_IN / 2, one2, 0u, 0u, 0u);
+        tmem_st_wait();
+    }
     const uint32_t bar = smem_u32(&s.bar);
-    const uint32_t aX = smem_u32(s.H + umma_k_index(0, TC_X_COL, TC_M)), aH = smem_u32(s.H), aW1 = smem_u32(s.W1), aW2 = smem_u32(s.W2), aW3 = smem_u32(s.W3);
-    const uint32_t LBO_A = TC_M * 16, LBO_B = MLP_H * 16, SBO = 128;
+    const uint32_t aW1 = smem_u32(s.W1), aW2 = smem_u32(s.W2), aW3 = smem_u32(s.W3);
+    const uint32_t LBO_B = MLP_H * 16, SBO = 128;
     const float sc = scale ? *scale : 1.f;
     const int64_t ntiles = (n + TC_M - 1) / TC_M;
     uint32_t phase = 0;
     int64_t tile = blockIdx.x;
     for (; tile < ntiles; tile += gridDim.x) {
         const int64_t row = tile * TC_M + tid;
-        {   // layer-1 operand: this thread's sample, 8 features -> 8 BF16 (16 B)
+        {   // layer-1 operand: this thread's sample, 8 features -> 4 packed BF16 pairs
             float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f), f1 = f0;
             if (row < n) {
                 f0 = __ldg(reinterpret_cast<const float4*>(feats + row * MLP_IN));
                 f1 = __ldg(reinterpret_cast<const float4*>(feats + row * MLP_IN) + 1);
             }
-            *reinterpret_cast<uint4*>(s.H + umma_k_index(tid, TC_X_COL, TC_M)) =
-                make_uint4(pack_bf16(f0.x, f0.y), pack_bf16(f0.z, f0.w), pack_bf16(f1.x, f1.y), pack_bf16(f1.z, f1.w));
+            tmem_st_32x32b_x4(tlane + TC_COL_X, pack_bf16(f0.x, f0.y), pack_bf16(f0.z, f0.w), pack_bf16(f1.x, f1.y),
+                              pack_bf16(f1.z, f1.w));
+            tmem_st_wait();
         }
-        fence_proxy_async_smem();
         tc_fence_before_sync();
         __syncthreads();
         float y = 0.f;
@@ -476,12 +481,12 @@ k_mlp_forward_tc(const float* __restrict__ prm, int64_t n, const float* __restri
             if (tid == 0) {
                 tc_fence_after_sync();
                 if (layer == 0) {
-                    umma_bf16_ss(tbase, umma_desc_kmajor(aX, LBO_A, SBO), umma_desc_kmajor(aW1, LBO_B, SBO), TC_IDESC, 0u);
+                    umma_bf16_ts(tbase + TC_COL_D, tbase + TC_COL_X, umma_desc_kmajor(aW1, LBO_B, SBO), TC_IDESC, 0u);
                 } else {
                     const uint32_t aW = layer == 1 ? aW2 : aW3;
                     #pragma unroll
                     for (int ks = 0; ks < TC_K2 / 16; ++ks)
-                        umma_bf16_ss(tbase, umma_desc_kmajor(aH + ks * 2 * LBO_A, LBO_A, SBO), umma_desc_kmajor(aW + ks * 2 * LBO_B, LBO_B, SBO),
+                        umma_bf16_ts(tbase + TC_COL_D, tbase + TC_COL_H + ks * 8, umma_desc_kmajor(aW + ks * 2 * LBO_B, LBO_B, SBO),
                                      TC_IDESC, ks > 0 ? 1u : 0u);
                 }
                 umma_commit(bar);
@@ -495,22 +500,23 @@ k_mlp_forward_tc(const float* __restrict__ prm, int64_t n, const float* __restri
             #pragma unroll
             for (int cb = 0; cb < MLP_H; cb += 32) {
                 uint32_t v[32];
-                tmem_ld_32x32b_x32(tlane + cb, v);
+                tmem_ld_32x32b_x32(tlane + TC_COL_D + cb, v);
                 tmem_ld_wait(v);
                 if (layer < 2) {
+                    uint32_t h[16];
                     #pragma unroll
-                    for (int g8 = 0; g8 < 4; ++g8) {
-                        const uint32_t* vb = v + 8 * g8;
-                        *reinterpret_cast<uint4*>(s.H + umma_k_index(tid, cb + 8 * g8, TC_M)) =
-                            make_uint4(relu_bf16x2(vb[0], vb[1]), relu_bf16x2(vb[2], vb[3]), relu_bf16x2(vb[4], vb[5]), relu_bf16x2(vb[6], vb[7]));
-                    }
+                    for (int j = 0; j < 16; ++j) h[j] = relu_bf16x2(v[2 * j], v[2 * j + 1]);
+                    const uint32_t (&h0)[8] = *reinterpret_cast<const uint32_t(*)[8]>(h);
+                    const uint32_t (&h1)[8] = *reinterpret_cast<const uint32_t(*)[8]>(h + 8);
+                    tmem_st_32x32b_x8(tlane + TC_COL_H + cb / 2, h0);
+                    tmem_st_32x32b_x8(tlane + TC_COL_H + cb / 2 + 8, h1);
                 } else {
                     #pragma unroll
                     for (int j = 0; j < 32; ++j) y = fmaf(fmaxf(__uint_as_float(v[j]), 0.f), s.w4[cb + j], y);
                 }
             }
             if (layer < 2) {
-                fence_proxy_async_smem();
+                tmem_st_wait();
                 tc_fence_before_sync();
                 __syncthreads();
             }
