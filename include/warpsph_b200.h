@@ -414,11 +414,15 @@ int sph_monaghan_rhs(const SphParams* p, int64_t n, const float* x, const float*
 /* Pairwise energy-partition fraction f_ij (modules/compSPH/balance.py:17-154) for
  * the six energy schemes, evaluated at v_half = v + dt/2 dvdt (schemes/crkSPH.py:341-363).
  * scratch: device memory of n*(dim+1) floats (half-step velocities and P/rho^gamma).
- * f_ij is written for every entry of `list` (pass the Verlet list to fill all of it). */
+ * f_ij is written for every entry of `list` (pass the Verlet list to fill all of it).
+ * inter_counts (may be null): per row, the length of the interacting prefix of a list
+ * whose rows hold their interacting entries first (sph_neighbors_build / refresh); the
+ * entries after it have ap_ij = av_ij = 0, and their pair arrays are not read. */
 int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const float* rho,
                         const float* P, const float* u, const float* v, const float* dvdt,
                         const float* dt, const int32_t* offs, const int32_t* cnt,
-                        const int32_t* list, const float* ap_ij, const float* av_ij,
+                        const int32_t* list, const int32_t* inter_counts,
+                        const float* ap_ij, const float* av_ij,
                         float* scratch, float* f_ij_out, void* stream);
 
 /* sph_compsph_balance without a scratch argument: no counterpart in the reference,

@@ -3,6 +3,8 @@
 Integer/indexing work is compared bit for bit; floating-point outputs with the
 tolerances written at each assertion (FP32 GPU vs FP32 oracle: differences come
 only from FMA contraction and operation order; vs the FP64 oracle: FP32 rounding)."""
+import ctypes as C
+
 import numpy as np
 import pytest
 import torch
@@ -10,7 +12,7 @@ import torch
 from oracle import oracle
 from oracle.steps import cell_capacity_for
 from tests.cases import assert_close, make_params, make_particles
-from warpsph_b200 import core, ops
+from warpsph_b200 import _capi, core, ops
 from warpsph_b200.enumTypes import EnergyScheme
 
 pytestmark = pytest.mark.gpu
@@ -225,6 +227,19 @@ def test_crk_pipeline(cuda, dim, n_side):
         mism = np.mean(np.abs(fg - rf) > 1e-4)
         # the partition is discontinuous in sign(dE); entries where dE rounds across zero may flip
         assert mism < 2e-3, (es, mism)
+        # skipping the entries past each row's interacting prefix (ap = av = 0 there) gives the
+        # same f_ij, bit for bit, as reading them
+        assert adj.interCounts is not None and adj._pending is None
+        f_full = torch.empty_like(f)
+        scratch = torch.empty(G["masses"].shape[0] * (int(p.dim) + 1), device=cuda)
+        dtt = torch.tensor([1e-3], device=cuda)
+        rc = _capi.lib().sph_compsph_balance(C.byref(p), G["masses"].shape[0], G["masses"].data_ptr(), rho.data_ptr(), Pr.data_ptr(),
+                                             G["internalEnergies"].data_ptr(), G["velocities"].data_ptr(), dvdt.data_ptr(),
+                                             dtt.data_ptr(), adj.neighborOffsets.data_ptr(), adj.numNeighbors.data_ptr(),
+                                             adj.neighborList.data_ptr(), None, ap.data_ptr(), av.data_ptr(), scratch.data_ptr(),
+                                             f_full.data_ptr(), _capi.stream_ptr(cuda))
+        assert rc == 0
+        assert torch.equal(f_full, f), es
 
 
 def test_kahan_option_matches(cuda):

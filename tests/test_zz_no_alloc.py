@@ -45,7 +45,7 @@ def call(p, t, adj, dt, noalloc):
         rc = L.sph_compsph_balance_noalloc(*common, ptr(f), stream_ptr(t["m"].device))
     else:
         scratch = torch.empty(n * (d + 1), dtype=torch.float32, device=t["m"].device)
-        rc = L.sph_compsph_balance(*common, ptr(scratch), ptr(f), stream_ptr(t["m"].device))
+        rc = L.sph_compsph_balance(*common[:12], None, *common[12:], ptr(scratch), ptr(f), stream_ptr(t["m"].device))
         f.scratch = scratch   # keep the caller scratch alive until the launch completes
     _capi.check(rc, "balance")
     return f

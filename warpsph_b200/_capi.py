@@ -123,7 +123,7 @@ _PROTOS = {
     "sph_compsph_accel": [_P, _I64] + [_P] * 17,
     "sph_compsph_dudt": [_P, _I64] + [_P] * 14,
     "sph_monaghan_rhs": [_P, _I64] + [_P] * 22,
-    "sph_compsph_balance": [_P, _I64] + [_P] * 15,
+    "sph_compsph_balance": [_P, _I64] + [_P] * 16,
     "sph_compsph_balance_noalloc": [_P, _I64] + [_P] * 14,
     "sph_cfl_dt": [_P, _I64, _P, _P, _P, _P, _P, _P],
     "sph_rk_combine": [_P, _I64, _P, _I32, _P, _P, _P, _I32, _P, _P],

@@ -874,7 +874,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK)
 k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restrict__ rho, const float* __restrict__ Pr,
           const float* __restrict__ u, const float* __restrict__ vh, const float* __restrict__ sarr, const float* __restrict__ dtp,
           const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
-          const float* __restrict__ ap, const float* __restrict__ av, float* __restrict__ fout) {
+          const int32_t* __restrict__ icnt, const float* __restrict__ ap, const float* __restrict__ av, float* __restrict__ fout) {
     Grp<G> g(n);
     if (!g.valid) return;
     const int i = g.i;
@@ -883,13 +883,18 @@ k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restri
     const float mi = m[i], rhoi = rho[i], Pi = Pr[i], ui = u[i], si = sarr[i];
     const int scheme = P.energy_scheme;
     int b = offs[i], e = b + cnt[i];
+    // entries past the interacting prefix carry ap = av = 0, so their dE is 0 (the same
+    // value the loads would give) and their pair arrays and half-step velocities are not read
+    const int ie = icnt ? b + icnt[i] : e;
     for (int q = b + g.lane; q < e; q += G) {
         int j, k; entry(list, q, j, k);
-        Vec<D> vj = load_vec<D>(vh, j);
-        Vec<D> apk = load_vec<D>(ap, k), avk = load_vec<D>(av, k);
         float dE = 0.f;
-        #pragma unroll
-        for (int a = 0; a < D; ++a) dE += (vj.v[a] - vi.v[a]) * (apk.v[a] + avk.v[a]);
+        if (q < ie) {
+            Vec<D> vj = load_vec<D>(vh, j);
+            Vec<D> apk = load_vec<D>(ap, k), avk = load_vec<D>(av, k);
+            #pragma unroll
+            for (int a = 0; a < D; ++a) dE += (vj.v[a] - vi.v[a]) * (apk.v[a] + avk.v[a]);
+        }
         dE = mi * dE * dt;
         float f = 0.5f;
         if (scheme == SPH_ENERGY_CRK) {
@@ -1275,8 +1280,8 @@ int sph_crk_dudt(const SphParams* p, int64_t n, const float* x, const float* H, 
 
 int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const float* rho, const float* Pr, const float* u,
                         const float* v, const float* dvdt, const float* dt, const int32_t* offs, const int32_t* cnt,
-                        const int32_t* list, const float* ap_ij, const float* av_ij, float* scratch, float* f_ij_out,
-                        void* stream) {
+                        const int32_t* list, const int32_t* inter_counts, const float* ap_ij, const float* av_ij, float* scratch,
+                        float* f_ij_out, void* stream) {
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(Pr); WSPH_CHECK_PTR(u); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(dvdt);
     WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(ap_ij); WSPH_CHECK_PTR(av_ij); WSPH_CHECK_PTR(scratch); WSPH_CHECK_PTR(f_ij_out); CHECK_CSR();
@@ -1288,7 +1293,7 @@ int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const flo
     float* sarr = scratch + n * P.dim;
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_balance_prep<D><<<grid_for(n, 256), 256, 0, s>>>((int)n, P, rho, Pr, v, dvdt, dt, vh, sarr)));
     wsph::count_launch();
-    WSPH_DISPATCH_DS(*p, (k_balance<D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, m, rho, Pr, u, vh, sarr, dt, offs, cnt, list, ap_ij, av_ij, f_ij_out)));
+    WSPH_DISPATCH_DS(*p, (k_balance<D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, m, rho, Pr, u, vh, sarr, dt, offs, cnt, list, inter_counts, ap_ij, av_ij, f_ij_out)));
     return check_launch("sph_compsph_balance");
 }
 
@@ -1308,11 +1313,11 @@ int sph_compsph_balance_noalloc(const SphParams* p, int64_t n, const float* m, c
     if (n > 0 && n * (int64_t)(p->dim + 1) > (int64_t)SPH_BALANCE_NOALLOC_MAX_FLOATS)
         return set_error(SPH_ERR_BAD_ARG, "sph_compsph_balance_noalloc: n*(dim+1) = %lld exceeds the fixed scratch of %d floats",
                          (long long)(n * (p->dim + 1)), SPH_BALANCE_NOALLOC_MAX_FLOATS);
-    if (n <= 0) return sph_compsph_balance(p, n, m, rho, Pr, u, v, dvdt, dt, offs, cnt, list, ap_ij, av_ij, nullptr, f_ij_out, stream);
+    if (n <= 0) return sph_compsph_balance(p, n, m, rho, Pr, u, v, dvdt, dt, offs, cnt, list, nullptr, ap_ij, av_ij, nullptr, f_ij_out, stream);
     float* scratch = nullptr;
     int rc = balance_scratch_on_current_device(&scratch);
     if (rc) return rc;
-    return sph_compsph_balance(p, n, m, rho, Pr, u, v, dvdt, dt, offs, cnt, list, ap_ij, av_ij, scratch, f_ij_out, stream);
+    return sph_compsph_balance(p, n, m, rho, Pr, u, v, dvdt, dt, offs, cnt, list, nullptr, ap_ij, av_ij, scratch, f_ij_out, stream);
 }
 
 int sph_cfl_dt(const SphParams* p, int64_t n, const float* H, const float* u, const float* rho, const float* dt_prev,

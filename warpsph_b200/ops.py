@@ -463,7 +463,8 @@ def compsph_balance(params, m, rho, P, u, v, dvdt, dt, adj: AdjacencyList, ap, a
     scratch = _empty(n * (d + 1), m)
     with _timed("compsph_balance"):
         check(_capi.lib().sph_compsph_balance(_p(params), n, fptr(m), fptr(rho), fptr(P), fptr(u), fptr(v), fptr(dvdt),
-                                              fptr(dt_tensor(dt, m.device)), *_lists(params, adj, False), fptr(ap), fptr(av),
+                                              fptr(dt_tensor(dt, m.device)), *_lists(params, adj, False),
+                                              iptr(adj.interCounts) if adj._pending is None else None, fptr(ap), fptr(av),
                                               ptr(scratch), ptr(f), stream_ptr(m.device)), "sph_compsph_balance")
     return f
 
