@@ -83,6 +83,13 @@ class ClockSampler:
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
 
+    def wait_ready(self, timeout: float = 5.0) -> None:
+        """Returns once nvidia-smi has printed its first sample (its driver start-up done), so
+        that the start-up does not overlap the timed region; gives up after `timeout` s."""
+        t0 = time.perf_counter()
+        while self.proc is not None and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.01)
+
     def _read(self):
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
@@ -433,6 +440,7 @@ def gpu_arm(args, rank: int, world: int):
 
     clocks = ClockSampler(dev.index)
     clocks.start()
+    clocks.wait_ready()
     for _ in range(max(args.warmup, 0)):
         one_step()
     torch.cuda.synchronize()

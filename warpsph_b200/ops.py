@@ -126,6 +126,43 @@ def cell_capacity_for(n: int, dim: int) -> int:
 REUSE_PRIOR = True
 
 
+def speculative_refresh(x: torch.Tensor, H: torch.Tensor, params, verletScale: float, prior: Optional[AdjacencyList]):
+    """Launches the validity check of `prior`'s Verlet rows for (x, H) (sph_neighbors_refresh,
+    verdict only) and returns (the list kept for (x, H), its device status word) without
+    reading the verdict, or None when `prior` cannot be kept whatever the verdict (none,
+    another size, scale, device or dimension).  The kept list is only valid once
+    verdicts_stale() says it is not stale; it filters its interacting rows on first use."""
+    x = _f32(x)
+    H = _f32(H)
+    n = int(H.shape[0])
+    dim = int(params.dim)
+    dev = x.device
+    if not (REUSE_PRIOR and prior is not None and prior._x0 is not None and prior.numRows == n and
+            prior.verletScale == float(verletScale) and prior._x0.device == dev and prior._dim == dim):
+        return None
+    params.verlet_scale = float(verletScale)
+    flags = torch.zeros(4, dtype=torch.int64, device=dev)   # [-, status (low half), scratch (2 words)]
+    with _timed("neighbors_refresh"):
+        check(_capi.lib().sph_neighbors_refresh(_p(params), n, ptr(x), ptr(H), ptr(prior._x0), ptr(prior._h0), None, None, None,
+                                                None, None, flags.data_ptr() + 16, None, flags.data_ptr() + 8, stream_ptr(dev)),
+              "sph_neighbors_refresh")
+    adj = AdjacencyList(neighborOffsets=prior.neighborOffsets, numNeighbors=prior.numNeighbors,
+                        neighborList=prior.neighborList, numRows=n, numCols=n, nnz=prior.nnz, sortIndex=prior.sortIndex,
+                        sortedKeys=prior.sortedKeys, grid=prior.grid, queryPositions=x, querySupports=H,
+                        verletScale=float(verletScale))
+    adj._x_version, adj._h_version = _version(x), _version(H)
+    adj._x0, adj._h0, adj._dim = prior._x0, prior._h0, dim
+    adj._pending = _capi.SphParams.from_buffer_copy(params)   # interacting sublist filtered on first use
+    return adj, flags
+
+
+def verdicts_stale(flags_list) -> list:
+    """Reads the verdicts of several speculative_refresh calls in one host read: True where
+    the kept list is stale (a particle left the Verlet skin) and must be rebuilt."""
+    words = flags_list[0][1:2] if len(flags_list) == 1 else torch.stack([f[1] for f in flags_list])
+    return [bool((int(w) & 0xffffffff) & _capi.STATUS_LIST_STALE) for w in words.cpu().tolist()]
+
+
 def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float,
                     priorNeighborhood: Optional[AdjacencyList] = None, keep_sort: bool = True) -> AdjacencyList:
     """Replaces warpSPHCore buildVerletList (schemes/crkSPH.py:54-58).
@@ -146,21 +183,10 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
     dev = x.device
     L = _capi.lib()
     prior = priorNeighborhood
-    if REUSE_PRIOR and prior is not None and prior._x0 is not None and prior.numRows == n and \
-            prior.verletScale == float(verletScale) and prior._x0.device == dev and prior._dim == dim:
-        flags = torch.zeros(4, dtype=torch.int64, device=dev)   # [-, status (low half), scratch (2 words)]
-        with _timed("neighbors_refresh"):
-            check(L.sph_neighbors_refresh(_p(params), n, ptr(x), ptr(H), ptr(prior._x0), ptr(prior._h0), None, None, None, None,
-                                          None, flags.data_ptr() + 16, None, flags.data_ptr() + 8, stream_ptr(dev)),
-                  "sph_neighbors_refresh")
-        if not (int(flags[1].item()) & 0xffffffff) & _capi.STATUS_LIST_STALE:
-            adj = AdjacencyList(neighborOffsets=prior.neighborOffsets, numNeighbors=prior.numNeighbors,
-                                neighborList=prior.neighborList, numRows=n, numCols=n, nnz=prior.nnz, sortIndex=prior.sortIndex,
-                                sortedKeys=prior.sortedKeys, grid=prior.grid, queryPositions=x, querySupports=H,
-                                verletScale=float(verletScale))
-            adj._x_version, adj._h_version = _version(x), _version(H)
-            adj._x0, adj._h0, adj._dim = prior._x0, prior._h0, dim
-            adj._pending = _capi.SphParams.from_buffer_copy(params)   # interacting sublist filtered on first use
+    spec = speculative_refresh(x, H, params, verletScale, prior)
+    if spec is not None:
+        adj, flags = spec
+        if not verdicts_stale([flags])[0]:
             return adj
     cap = cell_capacity_for(n, dim)
     wsb = C.c_int64(0)

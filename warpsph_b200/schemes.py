@@ -53,6 +53,25 @@ def evaluateOptimalSupport(particleState, config: SimulationConfig, compParams: 
     hThreshold = compParams.adaptiveSupportThreshold if threshold is None else threshold
     S = particleState
     hb = ops.minmax(S.supports)
+    if nIter == 1:
+        # One Newton iteration on a list kept from the previous stage: its validity for the
+        # moved positions and for the new supports is checked by two launches whose verdicts
+        # are read together, after the iteration has run on the kept rows.  When the first
+        # verdict says stale the iteration is discarded and the path below runs as usual.
+        spec = ops.speculative_refresh(S.positions, S.supports, params, config.verletScale, adjacency)
+        if spec is not None:
+            adj1, f1 = spec
+            rho, h_new, _ = ops.adaptive_h_iter(params, S.positions, S.supports, S.masses, adj1, hb)
+            spec2 = ops.speculative_refresh(S.positions, h_new, params, config.verletScale, adj1)
+            stale1, stale2 = ops.verdicts_stale([f1, spec2[1]])
+            if not stale1:
+                S.densities, S.supports = rho, h_new
+                adjacency = (spec2[0] if not stale2
+                             else ops.buildVerletList(S.positions, S.supports, params, config.verletScale, adj1))
+                if not final_density:
+                    return S.densities, S.supports, adjacency, None, None
+                densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
+                return densities, S.supports, adjacency, None, None
     for it in range(nIter):
         adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, adjacency)
         rho, h_new, ratio = ops.adaptive_h_iter(params, S.positions, S.supports, S.masses, adjacency, hb)
