@@ -126,6 +126,16 @@ def cell_capacity_for(n: int, dim: int) -> int:
 REUSE_PRIOR = True
 
 
+_LIST_GRANULE = 1 << 22   # entries (16 MB)
+
+
+def _list_capacity(entries: int) -> int:
+    """List capacity rounded up to a whole number of granules.  Rebuilds then request the
+    same few sizes, and the caching allocator reuses the freed blocks instead of going to
+    cudaMalloc, which synchronises the device."""
+    return max(-(-int(entries) // _LIST_GRANULE) * _LIST_GRANULE, _LIST_GRANULE)
+
+
 def speculative_refresh(x: torch.Tensor, H: torch.Tensor, params, verletScale: float, prior: Optional[AdjacencyList]):
     """Launches the validity check of `prior`'s Verlet rows for (x, H) (sph_neighbors_refresh,
     verdict only) and returns (the list kept for (x, H), its device status word) without
@@ -207,7 +217,7 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
     icnt = torch.empty(n, dtype=torch.int32, device=dev)
     flags = torch.zeros(3, dtype=torch.int64, device=dev)   # [nnz, status (int32 in the low half), interacting nnz]
     hint = _nb_cache.cap_hint.get((dev.index, n, dim))
-    list_cap = hint if hint is not None else max(n * 64, 1024)
+    list_cap = hint if hint is not None else _list_capacity(n * 64)
     for attempt in range(2):
         lst = torch.empty(max(list_cap, 1), dtype=torch.int32, device=dev)
         flags.zero_()
@@ -221,12 +231,12 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
         if status & _capi.STATUS_NONFINITE:
             raise RuntimeError("buildVerletList: supports must be finite and positive")
         if status & _capi.STATUS_LIST_OVERFLOW:
-            list_cap = max(list_cap, int(nnz * 1.15) + 1024)
+            list_cap = max(list_cap, _list_capacity(int(nnz * 1.15) + 1024))
             continue
         break
     else:  # pragma: no cover
         raise RuntimeError("buildVerletList: list capacity could not be satisfied")
-    _nb_cache.cap_hint[(dev.index, n, dim)] = int(nnz * 1.15) + 1024
+    _nb_cache.cap_hint[(dev.index, n, dim)] = max(_list_capacity(int(nnz * 1.15) + 1024), hint or 0)
     adj = AdjacencyList(neighborOffsets=offs, numNeighbors=cnt, neighborList=lst[:nnz], numRows=n, numCols=n, nnz=nnz,
                         sortIndex=si if keep_sort else None, sortedKeys=sk if keep_sort else None, grid=grid,
                         queryPositions=x, querySupports=H, verletScale=float(verletScale),
