@@ -450,6 +450,7 @@ def gpu_arm(args, rank: int, world: int):
     barrier()
     torch.cuda.synchronize()
     tw0 = time.time()
+    mem0 = torch.cuda.memory_stats(dev)
     launches0 = L.sph_launch_count()
     ops.TIMER = timer
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -460,6 +461,10 @@ def gpu_arm(args, rank: int, world: int):
     torch.cuda.synchronize()
     ops.TIMER = None
     launches = L.sph_launch_count() - launches0
+    mem1 = torch.cuda.memory_stats(dev)
+    # device allocations by torch's caching allocator inside the timed region (each one a
+    # cudaMalloc / cudaFree, which synchronise the device)
+    allocator = {k: int(mem1.get(k, 0) - mem0.get(k, 0)) for k in ("num_device_alloc", "num_device_free", "num_alloc_retries")}
     tw1 = time.time()
     barrier()
     clocks.stop()
@@ -596,6 +601,7 @@ def gpu_arm(args, rank: int, world: int):
                 "config": {"workload": WORKLOAD, "particles": n, "nx": args.nx, "parallelism": f"replicas x{world}",
                            "l2": "working set larger than L2 (pair arrays ~0.7 GB per step), no flush needed"},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
+                "allocator_in_timed_region": allocator,
                 "dfsph_warm_start": dfsph, "ensemble": ens, "compsph": comp, "sedov3d": s3, "mlp_forward": mlp}
         if breakdown is not None:
             line["breakdown_ms"] = {k: round(v["total_ms"] / 3, 4) for k, v in breakdown.items()}

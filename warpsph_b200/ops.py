@@ -136,6 +136,15 @@ def _list_capacity(entries: int) -> int:
     return max(-(-int(entries) // _LIST_GRANULE) * _LIST_GRANULE, _LIST_GRANULE)
 
 
+def _pair_empty(nnz: int, d: int, like: torch.Tensor) -> torch.Tensor:
+    """An uninitialised per-entry array of nnz rows (d columns, or a vector for d = 0) cut
+    from storage rounded up to whole list granules, so that successive steps request the
+    same few sizes from the caching allocator."""
+    cap = _list_capacity(nnz)
+    base = torch.empty((cap, d) if d else cap, dtype=like.dtype, device=like.device)
+    return base[:nnz]
+
+
 def speculative_refresh(x: torch.Tensor, H: torch.Tensor, params, verletScale: float, prior: Optional[AdjacencyList]):
     """Launches the validity check of `prior`'s Verlet rows for (x, H) (sph_neighbors_refresh,
     verdict only) and returns (the list kept for (x, H), its device status word) without
@@ -268,7 +277,7 @@ def _materialize_inter(adj: AdjacencyList) -> None:
     params = adj._pending
     n, dev = adj.numRows, adj.neighborList.device
     icnt = torch.empty(n, dtype=torch.int32, device=dev)
-    lst = torch.empty(max(adj.nnz, 1), dtype=torch.int32, device=dev)
+    lst = torch.empty(_list_capacity(adj.nnz), dtype=torch.int32, device=dev)
     flags = torch.zeros(4, dtype=torch.int64, device=dev)   # [inter nnz, status (low half), scratch (2 words)]
     with _timed("neighbors_refresh"):
         check(_capi.lib().sph_neighbors_refresh(_p(params), n, ptr(adj.queryPositions), ptr(adj.querySupports), ptr(adj._x0),
@@ -432,8 +441,8 @@ def crk_accel_dudt(params, x, H, m, rho, V, crk: CRKState, v, c, P, DvDx, adj: A
     n, d = H.shape[0], int(params.dim)
     dvdt, dudt = _empty((n, d), H), _empty(n, H)
     dEdt = _empty(n, H) if want_dEdt else None
-    ap = _empty((adj.nnz, d), H) if pair_arrays else None
-    av = _empty((adj.nnz, d), H) if pair_arrays else None
+    ap = _pair_empty(adj.nnz, d, H) if pair_arrays else None
+    av = _pair_empty(adj.nnz, d, H) if pair_arrays else None
     with _timed("crk_accel_dudt"):
         rows = _lists(params, adj, True)
         check(_capi.lib().sph_crk_accel_dudt(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(V), fptr(crk.A), fptr(crk.B),
@@ -464,8 +473,8 @@ def compsph_accel_dudt(params, x, H, m, rho, v, c, alpha, P, omega, adj: Adjacen
     n, d = H.shape[0], int(params.dim)
     dvdt, dudt = _empty((n, d), H), _empty(n, H)
     dEdt = _empty(n, H) if want_dEdt else None
-    ap = _empty((adj.nnz, d), H) if pair_arrays else None
-    av = _empty((adj.nnz, d), H) if pair_arrays else None
+    ap = _pair_empty(adj.nnz, d, H) if pair_arrays else None
+    av = _pair_empty(adj.nnz, d, H) if pair_arrays else None
     with _timed("compsph_accel_dudt"):
         rows = _lists(params, adj, True)
         check(_capi.lib().sph_compsph_accel_dudt(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(v), fptr(c), fptr(alpha),
@@ -495,7 +504,7 @@ def monaghan_rhs(params, x, H, m, rho, v, u, c, alpha, P, omega, adj: AdjacencyL
 def compsph_balance(params, m, rho, P, u, v, dvdt, dt, adj: AdjacencyList, ap, av):
     """Energy partition f_ij for every Verlet entry."""
     n, d = m.shape[0], int(params.dim)
-    f = _empty(adj.nnz, m)
+    f = _pair_empty(adj.nnz, 0, m)
     scratch = _empty(n * (d + 1), m)
     with _timed("compsph_balance"):
         check(_capi.lib().sph_compsph_balance(_p(params), n, fptr(m), fptr(rho), fptr(P), fptr(u), fptr(v), fptr(dvdt),
