@@ -191,6 +191,18 @@ int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const f
                           const int32_t* neighbor_list, int32_t* list_out, int32_t* inter_counts,
                           uint32_t* scratch, int64_t* inter_nnz_out, int32_t* status, void* stream);
 
+/* sph_neighbors_refresh with list_out set, fused with the CRK volume of the rewritten
+ * rows (computeCRKFactors, schemes/crkSPH.py:61: V_i = 1 / sum_j W(r_ij, H_j), the
+ * scatter support): V_out [n] receives the volumes that sph_crk_volume gives on the
+ * rewritten rows, summed in the row's original order.  The other arguments are those
+ * of sph_neighbors_refresh; list_out, inter_counts and inter_nnz_out are required. */
+int sph_neighbors_refresh_volume(const SphParams* p, int64_t n, const float* x, const float* H,
+                                 const float* x0, const float* H0,
+                                 const int32_t* neighbor_offsets, const int32_t* num_neighbors,
+                                 const int32_t* neighbor_list, int32_t* list_out,
+                                 int32_t* inter_counts, uint32_t* scratch, int64_t* inter_nnz_out,
+                                 int32_t* status, float* V_out, void* stream);
+
 /* Expands CSR rows into the reference's AdjacencyList.i / .j int64 arrays
  * (io.py:8-20 field names). */
 int sph_neighbors_expand(int64_t n, const int32_t* neighbor_offsets, const int32_t* num_neighbors,

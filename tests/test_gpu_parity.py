@@ -305,3 +305,31 @@ def test_prior_list_refresh(cuda, dim, n_side):
     ref = oracle.get("f32").neighbors(p, x2, H, cell_capacity_for(len(H), dim))
     assert np.array_equal(adj2.neighborList.cpu().numpy(), ref["list"])
     assert np.array_equal(adj2.interCounts.cpu().numpy(), ref["inter_counts"])
+
+
+@pytest.mark.parametrize("dim,n_side", CASES)
+def test_prior_list_rewrite_fused_with_volume(cuda, dim, n_side):
+    """The CRK volume of a kept list whose rows await their rewrite comes from the fused
+    pass (sph_neighbors_refresh_volume): the rewritten rows and interacting counts equal
+    the plain rewrite's bit for bit, and the volumes equal the standalone volume pass on
+    those rows to FP32 rounding (the fused sum runs in the row's original order)."""
+    cfg, sch, p = make_params(dim)
+    P = make_particles(dim, n_side, seed=70 + dim)
+    G = to_gpu(P, cuda)
+    adj0 = ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale)
+    rng = np.random.default_rng(8)
+    H = P["supports"]
+    x1 = (P["positions"] + (0.02 * H[:, None] * rng.standard_normal(P["positions"].shape)).astype(np.float32)).astype(np.float32)
+    x1 = torch.from_numpy(((x1 + 0.5) % 1.0 - 0.5).astype(np.float32)).to(cuda)
+    H1 = torch.from_numpy((H * (1 + 0.05 * (rng.random(len(H)) - 0.5))).astype(np.float32)).to(cuda)
+    fused = ops.buildVerletList(x1, H1, p, p.verlet_scale, adj0)
+    plain = ops.buildVerletList(x1, H1, p, p.verlet_scale, adj0)
+    assert fused._pending is not None and plain._pending is not None
+    V_fused = ops.crk_volume(p, x1, H1, fused)
+    assert fused._pending is None
+    ops._lists(p, plain, True)
+    V_plain = ops.crk_volume(p, x1, H1, plain)
+    assert torch.equal(fused.neighborList, plain.neighborList)
+    assert torch.equal(fused.interCounts, plain.interCounts)
+    assert int(fused._inter_nnz_dev.item()) == int(plain._inter_nnz_dev.item())
+    assert torch.allclose(V_fused, V_plain, rtol=2e-6, atol=0)

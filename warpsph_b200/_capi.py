@@ -101,6 +101,7 @@ _PROTOS = {
     "sph_neighbors_build": [_P, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _P,
                             _P, _P, _P, _P],
     "sph_neighbors_refresh": [_P, _I64] + [_P] * 13,
+    "sph_neighbors_refresh_volume": [_P, _I64] + [_P] * 14,
     "sph_neighbors_expand": [_I64, _P, _P, _P, _I64, _P, _P, _P],
     "sph_density_gather": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_adaptive_h_iter": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],

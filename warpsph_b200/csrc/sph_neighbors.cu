@@ -21,6 +21,7 @@
 #include <atomic>
 #include <cuda_runtime.h>
 #include "sph_common.cuh"
+#include "sph_pair_common.cuh"
 
 namespace wsph {
 
@@ -773,6 +774,65 @@ __global__ void k_refilter(const float* __restrict__ x, const float* __restrict_
     if (lane == 0 && t) atomicAdd(innz, t);
 }
 
+// k_refilter fused with the CRK volume of the rewritten rows (modules/crk, computeCRKFactors:
+// V_i = 1 / sum_j W(r_ij, H_j), the scatter support): the rewrite already gathers every
+// Verlet neighbour's position and support, and W(r_ij, H_j) is zero past the interacting
+// prefix (r >= max(H_i, H_j) >= H_j), so the whole row can be summed.  The sum runs in
+// the row's original order, 8 lanes per row.
+template <int KF, int D>
+__global__ void k_refilter_volume(const float* __restrict__ x, const float* __restrict__ H, int n, DevParams P,
+                                  const unsigned int* __restrict__ acc3, const int32_t* __restrict__ offs,
+                                  const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
+                                  int32_t* __restrict__ list_out, int32_t* __restrict__ icnt,
+                                  unsigned long long* __restrict__ innz, int32_t* __restrict__ status, float* __restrict__ V) {
+    if (!refresh_valid(acc3)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, SPH_STATUS_LIST_STALE);
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & (RF_G - 1);
+    const int gshift = lane & ~(RF_G - 1);
+    const unsigned int below = (1u << sub) - 1u;
+    const int64_t ii = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / RF_G;
+    const bool valid = ii < n;
+    const int i = valid ? (int)ii : 0;
+    Vec<D> xi;
+    float Hi = 1.f;
+    int b = 0, c = 0;
+    if (valid) { xi = load_vec<D>(x, i); Hi = H[i]; b = offs[i]; c = cnt[i]; }
+    int w = 0, rw = 0;
+    float wsum = 0.f;
+    for (int base = 0; __any_sync(0xffffffffu, base < c); base += RF_G) {
+        const bool in_row = base + sub < c;
+        bool keep = false;
+        int j = 0;
+        if (in_row) {
+            j = list[b + base + sub];
+            const Vec<D> d = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            const float Hj = __ldg(H + j);
+            const float Hm = fmaxf(Hi, Hj);
+            keep = __fdiv_rn(sqrtf(dist2_rn<D>(d)), Hm) < 1.f;
+            wsum += kW_inv<KF, D>(safe_sqrt(dot<D>(d, d)), 1.f / Hj);
+        }
+        const unsigned int kb = (__ballot_sync(0xffffffffu, keep) >> gshift) & ((1u << RF_G) - 1u);
+        const unsigned int rb = (__ballot_sync(0xffffffffu, in_row && !keep) >> gshift) & ((1u << RF_G) - 1u);
+        if (keep) list_out[b + w + __popc(kb & below)] = j;
+        else if (in_row) list_out[b + c - 1 - (rw + __popc(rb & below))] = j;
+        w += __popc(kb);
+        rw += __popc(rb);
+    }
+    #pragma unroll
+    for (int o = 1; o < RF_G; o <<= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+    unsigned long long t = (valid && sub == 0) ? (unsigned long long)w : 0ull;
+    if (valid && sub == 0) {
+        icnt[i] = w;
+        V[i] = 1.f / wsum;
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0 && t) atomicAdd(innz, t);
+}
+
 }  // namespace wsph
 
 using namespace wsph;
@@ -904,6 +964,39 @@ int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const f
                                                                         neighbor_list, list_out, inter_counts,
                                                                         reinterpret_cast<unsigned long long*>(inter_nnz_out), status)));
     return check_launch("sph_neighbors_refresh");
+}
+
+int sph_neighbors_refresh_volume(const SphParams* p, int64_t n, const float* x, const float* H, const float* x0, const float* H0,
+                                 const int32_t* neighbor_offsets, const int32_t* num_neighbors, const int32_t* neighbor_list,
+                                 int32_t* list_out, int32_t* inter_counts, uint32_t* scratch, int64_t* inter_nnz_out,
+                                 int32_t* status, float* V_out, void* stream) {
+    DevParams P;
+    int rc = params_to_dev(p, &P);
+    if (rc) return rc;
+    if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_refresh_volume: n out of range");
+    WSPH_CHECK_PTR(scratch); WSPH_CHECK_PTR(status); WSPH_CHECK_PTR(inter_nnz_out);
+    cudaStream_t s = WSPH_STREAM(stream);
+    cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
+    if (n == 0) return check_launch("sph_neighbors_refresh_volume");
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(x0); WSPH_CHECK_PTR(H0); WSPH_CHECK_PTR(V_out);
+    WSPH_CHECK_PTR(neighbor_offsets); WSPH_CHECK_PTR(num_neighbors); WSPH_CHECK_PTR(neighbor_list); WSPH_CHECK_PTR(list_out);
+    WSPH_CHECK_PTR(inter_counts);
+    if (list_out == neighbor_list) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_refresh_volume: list_out must not alias neighbor_list");
+    if (P.dim == 2 && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(x0)) & 7))
+        return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
+    cudaMemsetAsync(scratch, 0, 3 * sizeof(uint32_t), s);
+    int cblocks = (int)((n + 1023) / 1024);
+    if (cblocks > 148 * 4) cblocks = 148 * 4;
+    wsph::count_launch();
+    WSPH_DISPATCH_DIM(P.dim, (k_refresh_check<D><<<cblocks, 256, 0, s>>>(x, H, x0, H0, (int)n, P, scratch)));
+    const int rblocks = (int)((n * RF_G + 255) / 256);
+    wsph::count_launch();
+    WSPH_DISPATCH_KD(P.kernel, P.dim, (k_refilter_volume<KF, D><<<rblocks, 256, 0, s>>>(x, H, (int)n, P, scratch, neighbor_offsets,
+                                                                                       num_neighbors, neighbor_list, list_out,
+                                                                                       inter_counts,
+                                                                                       reinterpret_cast<unsigned long long*>(inter_nnz_out),
+                                                                                       status, V_out)));
+    return check_launch("sph_neighbors_refresh_volume");
 }
 
 int sph_neighbors_expand(int64_t n, const int32_t* neighbor_offsets, const int32_t* num_neighbors,

@@ -270,20 +270,24 @@ def _csr(adj: AdjacencyList):
     return iptr(adj.neighborOffsets), iptr(adj.numNeighbors), iptr(adj.neighborList)
 
 
-def _materialize_inter(adj: AdjacencyList) -> None:
+def _materialize_inter(adj: AdjacencyList, V_out: Optional[torch.Tensor] = None) -> None:
     """Rewrites the rows of a kept prior list with the interacting entries for the
     current positions first (sph_neighbors_refresh).  The rows go to a new tensor:
-    earlier stages keep the old order their pairwise arrays are indexed by."""
+    earlier stages keep the old order their pairwise arrays are indexed by.  With V_out
+    the CRK volumes of the rewritten rows are computed in the same pass."""
     params = adj._pending
     n, dev = adj.numRows, adj.neighborList.device
     icnt = torch.empty(n, dtype=torch.int32, device=dev)
     lst = torch.empty(_list_capacity(adj.nnz), dtype=torch.int32, device=dev)
     flags = torch.zeros(4, dtype=torch.int64, device=dev)   # [inter nnz, status (low half), scratch (2 words)]
+    args = (_p(params), n, ptr(adj.queryPositions), ptr(adj.querySupports), ptr(adj._x0), ptr(adj._h0), ptr(adj.neighborOffsets),
+            ptr(adj.numNeighbors), ptr(adj.neighborList), ptr(lst), ptr(icnt), flags.data_ptr() + 16, flags.data_ptr(),
+            flags.data_ptr() + 8)
     with _timed("neighbors_refresh"):
-        check(_capi.lib().sph_neighbors_refresh(_p(params), n, ptr(adj.queryPositions), ptr(adj.querySupports), ptr(adj._x0),
-                                                ptr(adj._h0), ptr(adj.neighborOffsets), ptr(adj.numNeighbors), ptr(adj.neighborList),
-                                                ptr(lst), ptr(icnt), flags.data_ptr() + 16, flags.data_ptr(),
-                                                flags.data_ptr() + 8, stream_ptr(dev)), "sph_neighbors_refresh")
+        if V_out is None:
+            check(_capi.lib().sph_neighbors_refresh(*args, stream_ptr(dev)), "sph_neighbors_refresh")
+        else:   # the rewrite fused with the CRK volume sum of the rewritten rows
+            check(_capi.lib().sph_neighbors_refresh_volume(*args, fptr(V_out), stream_ptr(dev)), "sph_neighbors_refresh_volume")
     adj.neighborList, adj.interCounts = lst[: adj.nnz], icnt
     adj._ij = None
     adj._inter_nnz_dev = flags[:1]
@@ -348,8 +352,13 @@ def adaptive_h_iter(params, x, H, m, adj: AdjacencyList, hbounds: torch.Tensor):
 
 
 def crk_volume(params, x, H, adj: AdjacencyList) -> torch.Tensor:
+    """V_i = 1 / sum_j W(r_ij, H_j).  A kept list whose rows still await their rewrite for
+    (x, H) gets it here, fused with the volume sum (sph_neighbors_refresh_volume)."""
     n = H.shape[0]
     V = _empty(n, H)
+    if adj is not None and adj._pending is not None and adj.queryPositions is x and adj.querySupports is H:
+        _materialize_inter(adj, V_out=V)
+        return V
     with _timed("crk_volume"):
         check(_capi.lib().sph_crk_volume(_p(params), n, fptr(x), fptr(H), *_lists(params, adj, True), ptr(V), stream_ptr(H.device)), "sph_crk_volume")
     return V
