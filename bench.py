@@ -20,6 +20,7 @@ run N independent replicas; value = total particle-steps/s, time = max over rank
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -449,6 +450,10 @@ def gpu_arm(args, rank: int, world: int):
     timer = ops.KernelTimer(names={"crk_accel_dudt"})
     barrier()
     torch.cuda.synchronize()
+    # as timeit does: one collection before the timed region and none inside it, so a
+    # generation-2 sweep of the interpreter heap does not land between two launches
+    gc.collect()
+    gc.disable()
     tw0 = time.time()
     mem0 = torch.cuda.memory_stats(dev)
     launches0 = L.sph_launch_count()
@@ -461,6 +466,7 @@ def gpu_arm(args, rank: int, world: int):
     torch.cuda.synchronize()
     ops.TIMER = None
     launches = L.sph_launch_count() - launches0
+    gc.enable()
     mem1 = torch.cuda.memory_stats(dev)
     # device allocations by torch's caching allocator inside the timed region (each one a
     # cudaMalloc / cudaFree, which synchronise the device)
@@ -555,11 +561,14 @@ def gpu_arm(args, rank: int, world: int):
         run(2)   # untimed: settles the allocator's pools for this pattern
         barrier()
         torch.cuda.synchronize()
+        gc.collect()
+        gc.disable()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         run(e2e_steps)
         e1.record()
         torch.cuda.synchronize()
+        gc.enable()
         ems = e0.elapsed_time(e1)
         te = torch.tensor([ems], device=dev, dtype=torch.float64)
         if world > 1:
