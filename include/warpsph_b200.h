@@ -130,7 +130,11 @@ typedef struct SphParams {
     /* DiffusionParameters.thermalConducitiyTerm (SPH_VISC_*): the signal-velocity form of
      * the artificial conductivity (diffusionParameters.py:33, pi.py:63) */
     int32_t conductivity_term;
-    int32_t reserved_i[6];
+    /* ViscositySwitchParameters.correctVelocityGradient (CullenHopkins.py:19-34): the
+     * Cullen-Hopkins velocity gradient is multiplied by pinv(M) of the CRKSPH moment matrix
+     * M_i = -sum_j m_j x_ij (x) grad W(r_ij, H_i) (common.py:10-25, wp_computeM.py:55-86) */
+    int32_t correct_velocity_gradient;
+    int32_t reserved_i[5];
 } SphParams;
 
 /* ---------------------------------------------------------------- library */

@@ -96,7 +96,8 @@ class Oracle:
         L.oracle_delta_shift.argtypes = [P, i64, rp, rp, rp, rp, rp, C.c_void_p, _i32p, _i32p, _i32p, real_c, real_c, real_c, C.c_int,
                                          real_c, rp]
         L.oracle_owen_iter.argtypes = [P, i64, rp, rp, _i32p, _i32p, _i32p, _f64p, _f64p, C.c_int, C.c_double, rp, rpn, rpn, rp, rpn]
-        L.oracle_switch_hopkins_terms.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rpn]
+        L.oracle_switch_hopkins_terms.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rpn, rp, rp, rp, rpn]
+        L.oracle_moment_matrix.argtypes = [P, i64, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_switch_hopkins_update.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, rp, real_c, _i32p, _i32p, _i32p, rp, rpn]
         L.oracle_vsig.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pi_pairs.argtypes = [P, i64, rp, rp, rp, rp, rpn, rpn, rp, _i32p, _i32p, _i32p, C.c_int, C.c_int, rp]
@@ -320,12 +321,31 @@ class Oracle:
                                   float(target), self.arr(hb), psi0, psiH, Hn, ratio)
         return psi0, psiH, Hn, ratio
 
+    def moment_matrix(self, params, x, H, m, nb):
+        """M_i = -sum_j m_j x_ij (x) grad W(r_ij, H_i), shape (n, D, D)."""
+        n, D = len(H), int(params.dim)
+        M = np.zeros((n, D, D), self.dtype)
+        self.lib.oracle_moment_matrix(self._p(params), n, self.arr(x), self.arr(H), self.arr(m),
+                                      nb["offsets"], nb["counts"], nb["list"], M)
+        return M
+
+    @staticmethod
+    def moment_pinv(M):
+        """torch.linalg.pinv's default for a float32 input (CullenHopkins.py:27): singular
+        values at or below D * eps_float32 * sigma_max are dropped.  LAPACK's SVD in float64."""
+        D = M.shape[-1]
+        return np.linalg.pinv(np.asarray(M, np.float64), rcond=D * float(np.finfo(np.float32).eps))
+
     def switch_hopkins_terms(self, params, x, H, m, rho, v, alpha0, nb):
-        """(alphas, div, |S|^2, R)"""
+        """(alphas, div, |S|^2, R); with params.correct_velocity_gradient the gradient is
+        pinv(M) V (CullenHopkins.py:24-34)."""
         n = len(H)
         al, div, s2, R = (np.zeros(n, self.dtype) for _ in range(4))
+        Minv = None
+        if int(getattr(params, "correct_velocity_gradient", 0)):
+            Minv = self.arr(self.moment_pinv(self.moment_matrix(params, x, H, m, nb)))
         self.lib.oracle_switch_hopkins_terms(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(v),
-                                             self.arr(alpha0), nb["offsets"], nb["counts"], nb["list"], div, s2, al, R)
+                                             self.arr(alpha0), nb["offsets"], nb["counts"], nb["list"], Minv, div, s2, al, R)
         return al, div, s2, R
 
     def switch_hopkins_update(self, params, x, H, v, c, div, div_prev, alpha0, dt, nb):

@@ -62,7 +62,7 @@ typedef struct {
     real eta_crit, eta_fold;
     int crk_lim, vl, vl_off, vl_on;
     real gamma;
-    int energy_scheme, limit_xi, kahan;
+    int energy_scheme, limit_xi, kahan, correct_grad_v;
     real alpha_min, alpha_max, beta_xi;
     real target_neighbors;
     real cfl, min_dt, max_dt, dt_growth;
@@ -93,6 +93,7 @@ static OP op_from(const SphParams* p) {
     o.eta_crit = (real)p->eta_crit; o.eta_fold = (real)p->eta_fold;
     o.crk_lim = p->enable_crk_limiter; o.vl = p->enable_vanleer_limiter; o.vl_off = p->force_vanleer_off; o.vl_on = p->force_vanleer_on;
     o.gamma = (real)p->gamma; o.energy_scheme = p->energy_scheme; o.limit_xi = p->limit_xi; o.kahan = p->kahan;
+    o.correct_grad_v = p->correct_velocity_gradient;
     o.alpha_min = (real)p->alpha_min; o.alpha_max = (real)p->alpha_max; o.beta_xi = (real)p->beta_xi;
     o.target_neighbors = (real)p->target_neighbors;
     o.cfl = (real)p->cfl; o.min_dt = (real)p->min_dt; o.max_dt = (real)p->max_dt; o.dt_growth = (real)p->dt_growth;
@@ -694,12 +695,38 @@ int oracle_vsig(const SphParams* p, int64_t n, const real* x, const real* H, con
     return 0;
 }
 
-/* Cullen-Hopkins switch (modules/shockCapturing/CullenHopkins.py:7-149 without the optional
- * gradient correction).  The velocity gradient is warpSPHCore's difference gradient with
- * gather support, restated as sum_j m_j/rho_j (v_j - v_i) (x) grad W(r_ij, H_i). */
+/* CRKSPH moment matrix of the velocity-gradient correction (common.py:10-25 negating
+ * wp_computeM.py:55-86): M_i = -sum_j m_j x_ij (x) grad W(r_ij, H_i), gather support,
+ * row-major D x D per particle. */
+int oracle_moment_matrix(const SphParams* p, int64_t n, const real* x, const real* H, const real* m,
+                         const int32_t* offs, const int32_t* cnt, const int32_t* list, real* M_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real M[9] = {0};
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG(&o, d, rsqrt_safe(dotD(d, d, D)), H[i], &W, g);
+            for (int a = 0; a < D; ++a)
+                for (int b = 0; b < D; ++b) M[a * D + b] += m[j] * d[a] * g[b];
+        }
+        for (int a = 0; a < D * D; ++a) M_out[i * D * D + a] = -M[a];
+    }
+    return 0;
+}
+
+/* Cullen-Hopkins switch (modules/shockCapturing/CullenHopkins.py:7-149).  The velocity
+ * gradient is warpSPHCore's difference gradient with gather support, restated as
+ * sum_j m_j/rho_j (v_j - v_i) (x) grad W(r_ij, H_i).  With correctVelocityGradient the
+ * caller passes Minv = pinv(M) (row-major D x D per particle) and the gradient becomes
+ * Minv V before its trace and shear are taken (common.py:76-78); NULL leaves it as is. */
 int oracle_switch_hopkins_terms(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
                                 const real* v, const real* alpha0, const int32_t* offs, const int32_t* cnt,
-                                const int32_t* list, real* div_out, real* shear2_out, real* alpha_out, real* R_out) {
+                                const int32_t* list, const real* Minv, real* div_out, real* shear2_out, real* alpha_out,
+                                real* R_out) {
     OP o = op_from(p);
     int D = o.dim;
 #pragma omp parallel for schedule(static)
@@ -714,6 +741,14 @@ int oracle_switch_hopkins_terms(const SphParams* p, int64_t n, const real* x, co
             real Vj = m[j] / rho[j];
             for (int a = 0; a < D; ++a)
                 for (int b = 0; b < D; ++b) G[a * D + b] += Vj * (v[(int64_t)j * D + a] - v[i * D + a]) * g[b];
+        }
+        if (Minv) {
+            const real* Mi = Minv + i * D * D;
+            real C[9] = {0};
+            for (int a = 0; a < D; ++a)
+                for (int b = 0; b < D; ++b)
+                    for (int c = 0; c < D; ++c) C[a * D + b] += Mi[a * D + c] * G[c * D + b];
+            for (int a = 0; a < D * D; ++a) G[a] = C[a];
         }
         real tr = 0, s2 = 0;
         for (int a = 0; a < D; ++a) tr += G[a * D + a];

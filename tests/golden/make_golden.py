@@ -57,6 +57,7 @@ wp = types.SimpleNamespace(
     min=lambda a, b: a if a < b else b, max=lambda a, b: a if a > b else b,
     abs=lambda x: abs(x), exp=lambda x: F(np.exp(F(x))), pow=lambda a, b: F(np.power(F(a), F(b))),
     sqrt=lambda x: F(np.sqrt(F(x))),
+    outer=lambda a, b: np.outer(np.asarray(a, F), np.asarray(b, F)).astype(F),
     int32=int, int64=int, bool=bool, float32=F, array=lambda *a, **k: None, tid=lambda: 0,
 )
 vector = matrix = lambda *a, **k: None
@@ -742,7 +743,10 @@ def run_reference_hopkins(ref: Path, g: dict) -> dict:
     run unmodified on the CompSPH fixture's particles, with computeR / computeXi /
     computeShearTensor from CullenDehnen2010.py and common.py, v_sig from the wp_vsig.py
     pair body, and warpSPHCore's generic gather operations restated in numpy (difference
-    gradient sum_j V_j (q_j - q_i) (x) grad W(H_i); interpolation sum_j V_j q_j W(H_i))."""
+    gradient sum_j V_j (q_j - q_i) (x) grad W(H_i); interpolation sum_j V_j q_j W(H_i)).
+    A second run sets correctVelocityGradient: computeM (common.py) then negates the
+    reference's own moment-matrix pair body (wp_computeM.py computeM_Func_i, gather support)
+    and torch.linalg.pinv inverts it, as CullenHopkins.py does; its results carry "cvg"."""
     Ctx.kernel, Ctx.dim = 2, 2
     x, H, m, rho, v, c = (g[k] for k in ("x", "H", "m", "rho", "v", "c"))
     offs, cnt, lst = g["offsets"], g["counts"], g["list"].astype(np.int64)
@@ -800,11 +804,25 @@ def run_reference_hopkins(ref: Path, g: dict) -> dict:
                            referenceViscositys=None, useVolume=False, Vi=F(0), referenceVolumes=None, useCRK=False, Ai=F(1),
                            Bi=None, gradAi=None, gradBi=None, vel_i=v[i], referenceVelocities=v, individual_cs=True,
                            cs_i=F(c[i]), referenceCs=c, outputValue=F(0))
+    m_ns = load(ref, "modules/shockCapturing/wp_computeM.py")
+    kpm = SoA(operationMode=OperationDirection.TrueAllToToAll.value, supportMode="gather")
+
+    def computeMWarp(*a, **kw):
+        outm = np.zeros((n, 2, 2), F)
+        for i in range(n):
+            outm[i] = call(m_ns["computeM_Func_i"], i=i, dim=2, xi=x[i], hi=F(H[i]), mi=F(m[i]), rhoi=F(rho[i]),
+                           referenceState=state, domainState=None, kernelProperties=kpm, beginIndex=int(offs[i]),
+                           numIndices=int(cnt[i]), offsetArray=lst, ki=0, referenceKinds=state.kinds,
+                           useGradientRenormalization=False, Li=None, useGradHTerms=False, Viscosity_i=F(1),
+                           referenceViscositys=None, useVolume=False, Vi=F(0), referenceVolumes=None, useCRK=False, Ai=F(1),
+                           Bi=None, gradAi=None, gradBi=None, outputValue=np.zeros((2, 2), F))
+        return torch.from_numpy(outm)
+
     names = dict(warpOperation=warpOperation, OperationProperties=OperationProperties,
                  WarpOperation=types.SimpleNamespace(Divergence="Divergence", Interpolate="Interpolate", Gradient="Gradient"),
                  GradientScheme=types.SimpleNamespace(Difference=1), SupportScheme=types.SimpleNamespace(Gather=0, SuperSymmetric=3),
                  ViscositySwitchState=lambda **kw: SoA(**kw), CompressibleState=None, SimulationConfig=None,
-                 CompressibleSPHConfig=None, AdjacencyList=None, CompactHashMap=None, computeMWarp=None,
+                 CompressibleSPHConfig=None, AdjacencyList=None, CompactHashMap=None, computeMWarp=computeMWarp,
                  computeVsigWarp=lambda *a, **k: torch.from_numpy(vsig), Union=Union, Tuple=Tuple, Dict=dict, Optional=Optional)
     common = load(ref, "modules/shockCapturing/common.py", names)
     names.update({k: common[k] for k in ("computeM", "computeShearTensor")})
@@ -815,14 +833,19 @@ def run_reference_hopkins(ref: Path, g: dict) -> dict:
     ps = SoA(positions=torch.from_numpy(x), supports=torch.from_numpy(H), densities=torch.from_numpy(rho),
              divergence=torch.from_numpy(div_prev), alpha0s=torch.from_numpy(alpha0), velocities=torch.from_numpy(v),
              soundspeeds=torch.from_numpy(c))
-    swc = SoA(alpha_min=0.02, alpha_max=2.0, beta_xi=2.0, limitXi=False, correctVelocityGradient=False, beta_c=0.7, beta_d=0.05)
-    sim = SoA(kernel=types.SimpleNamespace(value=2), supportMode=3, domain=None)
-    sch = SoA(viscositySwitchParams=swc)
-    alphas, st = hop["computeHopkinsTerms"](float(dt), ps, sim, sch, None, None)
-    a0n, st2 = hop["computeHopkinsUpdate"](st, float(dt), torch.from_numpy(dvdt), ps, sim, sch, None, None)
-    return dict(hopkins_alpha0=alpha0, hopkins_div_prev=div_prev, hopkins_dt=np.array([dt], F),
-                hopkins_alphas=alphas.numpy().astype(F), hopkins_div=st.div.numpy().astype(F), hopkins_R=st.R.numpy().astype(F),
-                hopkins_Xi=st.Xi.numpy().astype(F), hopkins_alpha0_next=a0n.numpy().astype(F), hopkins_vsig=np.abs(vsig))
+    out = dict(hopkins_alpha0=alpha0, hopkins_div_prev=div_prev, hopkins_dt=np.array([dt], F), hopkins_vsig=np.abs(vsig))
+    for tag, correct in (("hopkins", False), ("hopkins_cvg", True)):
+        swc = SoA(alpha_min=0.02, alpha_max=2.0, beta_xi=2.0, limitXi=False, correctVelocityGradient=correct, beta_c=0.7,
+                  beta_d=0.05)
+        sim = SoA(kernel=types.SimpleNamespace(value=2), supportMode=3, domain=None)
+        sch = SoA(viscositySwitchParams=swc)
+        alphas, st = hop["computeHopkinsTerms"](float(dt), ps, sim, sch, None, None)
+        a0n, st2 = hop["computeHopkinsUpdate"](st, float(dt), torch.from_numpy(dvdt), ps, sim, sch, None, None)
+        out.update({f"{tag}_alphas": alphas.numpy().astype(F), f"{tag}_div": st.div.numpy().astype(F),
+                    f"{tag}_R": st.R.numpy().astype(F), f"{tag}_Xi": st.Xi.numpy().astype(F),
+                    f"{tag}_alpha0_next": a0n.numpy().astype(F)})
+    out["hopkins_cvg_M"] = common["computeM"](ps, sim, sch, None, None).numpy().astype(F)
+    return out
 
 
 # ---------------------------------------------------------------- Owen adaptive support

@@ -35,3 +35,43 @@ def test_hopkins_switch_matches_reference():
     # both branches of the update occur
     assert (h["hopkins_alpha0_next"] != h["hopkins_alpha0"]).mean() > 0.3
     assert h["hopkins_alphas"].min() == np.float32(0.02) and h["hopkins_alphas"].max() > 0.5
+
+
+def test_moment_matrix_matches_reference():
+    """M_i = -sum_j m_j x_ij (x) grad W(r_ij, H_i) against the reference's computeM
+    (common.py negating the wp_computeM.py pair body)."""
+    g, h = dict(np.load(HERE / "compsph_golden.npz")), dict(np.load(HERE / "hopkins_golden.npz"))
+    p = hopkins_params()
+    nb = dict(offsets=g["offsets"], counts=g["counts"], list=g["list"])
+    for precision in ("f32", "f64"):
+        M = oracle.get(precision).moment_matrix(p, g["x"], g["H"], g["m"], nb)
+        assert_close(M, h["hopkins_cvg_M"], 1e-5, 1e-6, f"moment matrix ({precision}) vs reference wp_computeM.py")
+
+
+def test_hopkins_corrected_gradient_matches_reference():
+    """correctVelocityGradient: the gradient is pinv(M) V before its trace and shear
+    (CullenHopkins.py:24-34, common.py:76-78)."""
+    g, h = dict(np.load(HERE / "compsph_golden.npz")), dict(np.load(HERE / "hopkins_golden.npz"))
+    p = hopkins_params()
+    p.correct_velocity_gradient = 1
+    nb = dict(offsets=g["offsets"], counts=g["counts"], list=g["list"])
+    for precision, tol in (("f32", 1e-5), ("f64", 1e-5)):
+        o = oracle.get(precision)
+        al, div, s2, R = o.switch_hopkins_terms(p, g["x"], g["H"], g["m"], g["rho"], g["v"], h["hopkins_alpha0"], nb)
+        assert_close(div, h["hopkins_cvg_div"], tol, tol, f"corrected divergence ({precision})")
+        assert_close(R, h["hopkins_cvg_R"], tol, tol, f"R from the corrected divergence ({precision})")
+        assert_close(al, h["hopkins_cvg_alphas"], 1e-4, 1e-5, f"alphas, corrected gradient ({precision})")
+        a0, _ = o.switch_hopkins_update(p, g["x"], g["H"], g["v"], g["c"], div, h["hopkins_div_prev"], h["hopkins_alpha0"],
+                                        h["hopkins_dt"][0], nb)
+        assert_close(a0, h["hopkins_cvg_alpha0_next"], 1e-4, 1e-5, f"alpha0 update, corrected gradient ({precision})")
+    # the correction changes the result by more than the tolerance
+    assert np.abs(h["hopkins_cvg_div"] - h["hopkins_div"]).max() > 0.05 * np.abs(h["hopkins_div"]).max()
+
+
+def test_moment_pinv_drops_singular_directions():
+    """torch.linalg.pinv's default cutoff for float32: singular values at or below
+    D * eps_float32 * sigma_max are dropped."""
+    M = np.array([[[2.0, 0.0], [0.0, 1e-9]], [[1.0, 1.0], [1.0, 1.0]], [[0.0, 0.0], [0.0, 0.0]], [[0.0, 2.0], [-4.0, 0.0]]])
+    P = oracle.get("f64").moment_pinv(M)
+    want = np.array([[[0.5, 0.0], [0.0, 0.0]], [[0.25, 0.25], [0.25, 0.25]], [[0.0, 0.0], [0.0, 0.0]], [[0.0, -0.25], [0.5, 0.0]]])
+    assert np.allclose(P, want, rtol=1e-12, atol=1e-12)

@@ -228,6 +228,25 @@ def test_gpu_hopkins_switch_matches_reference(G):
         assert_close(nxt.cpu().numpy(), h["hopkins_alpha0_next"], 1e-3, 1e-4, "alpha0 update (GPU)")
 
 
+def test_gpu_hopkins_corrected_gradient_matches_reference(G):
+    """correctVelocityGradient on the GPU (moment matrix and FP64 Jacobi pseudo-inverse in
+    the gradient pass) against the reference's CullenHopkins.py with torch.linalg.pinv."""
+    t, g = G
+    h = dict(np.load(GOLD.parent / "hopkins_golden.npz"))
+    p = params_for(g)
+    p.alpha_min, p.alpha_max, p.beta_xi, p.limit_xi, p.beta_c, p.beta_d = 0.02, 2.0, 2.0, 0, 0.7, 0.05
+    p.correct_velocity_gradient = 1
+    a0 = torch.from_numpy(h["hopkins_alpha0"]).to(t["x"].device)
+    for adj in (verlet_adjacency(t), built_adjacency(p, t["x"], t["H"])):
+        al, div, s2, R = ops.switch_hopkins_terms(p, t["x"], t["H"], t["m"], t["rho"], t["v"], a0, adj)
+        assert_close(div.cpu().numpy(), h["hopkins_cvg_div"], 1e-4, 1e-5, "corrected divergence (GPU)")
+        assert_close(R.cpu().numpy(), h["hopkins_cvg_R"], 1e-4, 1e-5, "R (GPU, corrected)")
+        assert_close(al.cpu().numpy(), h["hopkins_cvg_alphas"], 1e-3, 1e-4, "alphas (GPU, corrected)")
+        nxt, _ = ops.switch_hopkins_update(p, t["x"], t["H"], t["v"], t["c"], div,
+                                           torch.from_numpy(h["hopkins_div_prev"]).to(a0.device), a0, float(h["hopkins_dt"][0]), adj)
+        assert_close(nxt.cpu().numpy(), h["hopkins_cvg_alpha0_next"], 1e-3, 1e-4, "alpha0 update (GPU, corrected)")
+
+
 def test_monaghan_step_matches_oracle(cuda):
     cfg, sch, integ, step, system = sedov(32, cuda, "MonaghanCompressibleSPH", ws.ViscositySwitch.NoneSwitch)
     dt = 2e-4

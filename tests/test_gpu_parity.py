@@ -333,3 +333,52 @@ def test_prior_list_rewrite_fused_with_volume(cuda, dim, n_side):
     assert torch.equal(fused.interCounts, plain.interCounts)
     assert int(fused._inter_nnz_dev.item()) == int(plain._inter_nnz_dev.item())
     assert torch.allclose(V_fused, V_plain, rtol=2e-6, atol=0)
+
+
+def _hopkins_both(p, P, G, adj, dev):
+    nb = nb_numpy(adj)
+    rho = ops.density(p, G["positions"], G["supports"], G["masses"], adj, core.SupportScheme.Gather)
+    n = rho.shape[0]
+    a0 = np.linspace(0.2, 1.5, n).astype(np.float32)
+    gpu = ops.switch_hopkins_terms(p, G["positions"], G["supports"], G["masses"], rho, G["velocities"],
+                                   torch.from_numpy(a0).to(dev), adj)
+    ref = oracle.get("f64").switch_hopkins_terms(p, P["positions"], P["supports"], P["masses"], rho.cpu().numpy(),
+                                                 P["velocities"], a0, nb)
+    return [t.cpu().numpy() for t in gpu], ref
+
+
+@pytest.mark.parametrize("dim,n_side", CASES)
+def test_hopkins_corrected_gradient(cuda, dim, n_side):
+    """correctVelocityGradient: moment matrix and FP64 one-sided Jacobi pseudo-inverse on
+    the GPU against the FP64 oracle (LAPACK SVD pseudo-inverse, the same cutoff)."""
+    cfg, sch, p, P, G, adj = pipeline_inputs(dim, n_side, cuda)
+    (al0, div0, s20, _), _ = _hopkins_both(p, P, G, adj, cuda)
+    p.correct_velocity_gradient = 1
+    (al, div, s2, R), (r_al, r_div, r_s2, r_R) = _hopkins_both(p, P, G, adj, cuda)
+    assert_close(div, r_div, 2e-4, 2e-5, f"corrected divergence {dim}D")
+    assert_close(s2, r_s2, 1e-3, 1e-5, f"corrected |S|^2 {dim}D")
+    assert_close(R, r_R, 2e-4, 2e-5, f"R {dim}D")
+    assert_close(al, r_al, 1e-3, 1e-4, f"alphas {dim}D")
+    assert np.abs(div - div0).max() > 1e-3 * np.abs(div0).max(), "the flag did not reach the kernel"
+
+
+def test_hopkins_corrected_gradient_rank_deficient(cuda):
+    """Particles on the x axis of a 2D domain: M has an exactly zero singular value, which
+    the pseudo-inverse drops, so only the xx component of the gradient survives."""
+    cfg, sch, p = make_params(2, periodic=False)
+    n, dx = 256, 1.0 / 256
+    x = np.zeros((n, 2), np.float32)
+    x[:, 0] = ((np.arange(n) + 0.5) * dx - 0.5).astype(np.float32)
+    rng = np.random.default_rng(3)
+    v = np.stack([np.sin(2 * np.pi * x[:, 0]), np.cos(2 * np.pi * x[:, 0])], 1).astype(np.float32)
+    v += (0.05 * rng.standard_normal(v.shape)).astype(np.float32)
+    P = dict(positions=x, supports=np.full(n, 4 * dx, np.float32), masses=np.full(n, dx, np.float32), velocities=v)
+    G = to_gpu(P, cuda)
+    adj = ops.buildVerletList(G["positions"], G["supports"], p, p.verlet_scale)
+    p.correct_velocity_gradient = 1
+    (al, div, s2, R), (r_al, r_div, r_s2, r_R) = _hopkins_both(p, P, G, adj, cuda)
+    assert np.isfinite(div).all() and np.isfinite(s2).all()
+    assert_close(div, r_div, 2e-4, 2e-5, "corrected divergence on a line")
+    assert_close(s2, r_s2, 1e-3, 1e-5, "corrected |S|^2 on a line")
+    # traceless symmetric part of diag(g, 0): |S|^2 = g^2 / 2 with g the divergence
+    assert_close(s2, 0.5 * div.astype(np.float64) ** 2, 1e-4, 1e-6, "|S|^2 of a rank-one gradient")

@@ -58,7 +58,8 @@ class SphParams(C.Structure):
         ("kahan", C.c_int32),
         ("list_stride", C.c_int32),
         ("conductivity_term", C.c_int32),
-        ("reserved_i", C.c_int32 * 6),
+        ("correct_velocity_gradient", C.c_int32),
+        ("reserved_i", C.c_int32 * 5),
     ]
 
 

@@ -34,11 +34,6 @@ def _no_boundaries(compParams) -> None:
         raise NotImplementedError("boundary conditions are outside the GPU hot path")
 
 
-def _hopkins_supported(compParams) -> None:
-    if compParams.viscositySwitchParams.correctVelocityGradient:
-        raise NotImplementedError("the Cullen-Hopkins switch with correctVelocityGradient is not implemented on the GPU path")
-
-
 def compSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams: CompSPHConfig, verbose: bool = False):
     """schemes/compSPH.py:22-215 on the GPU.  Returns (update, adjacency, state).
 
@@ -78,7 +73,6 @@ def compSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams
                                          S.alpha0s, dt, adjacency, v=S.velocities, c=S.soundspeeds)
         S.alphas = alphas
     elif hopkins:
-        _hopkins_supported(compParams)
         S.alphas, hop_div, _, _ = ops.switch_hopkins_terms(params, S.positions, S.supports, S.masses, S.densities, S.velocities,
                                                            S.alpha0s, adjacency)
     elif switch != ViscositySwitch.NoneSwitch:

@@ -563,6 +563,7 @@ def make_params(config: SimulationConfig, scheme: Optional[CompressibleSPHConfig
         p.alpha_min, p.alpha_max, p.beta_xi = float(sw.alpha_min), float(sw.alpha_max), float(sw.beta_xi)
         p.beta_c, p.beta_d = float(sw.beta_c), float(sw.beta_d)
         p.limit_xi = int(bool(sw.limitXi))
+        p.correct_velocity_gradient = int(bool(sw.correctVelocityGradient))
         p.kahan = int(bool(getattr(scheme, "compensatedSums", False)))
         es = getattr(scheme, "energyScheme", EnergyScheme.CRK)
         p.energy_scheme = int(es.value)

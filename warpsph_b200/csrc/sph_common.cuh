@@ -25,7 +25,7 @@ struct DevParams {
     float eta_crit, eta_fold;
     int enable_crk_limiter, enable_vanleer, force_vl_off, force_vl_on;
     float gamma;
-    int energy_scheme, limit_xi, kahan;
+    int energy_scheme, limit_xi, kahan, correct_grad_v;
     float alpha_min, alpha_max, beta_xi;
     float target_neighbors;
     float cfl, min_dt, max_dt, dt_growth;

@@ -89,6 +89,7 @@ int params_to_dev(const SphParams* p, DevParams* o) {
     o->force_vl_off = p->force_vanleer_off; o->force_vl_on = p->force_vanleer_on;
     o->gamma = (float)p->gamma;
     o->energy_scheme = p->energy_scheme; o->limit_xi = p->limit_xi; o->kahan = p->kahan;
+    o->correct_grad_v = p->correct_velocity_gradient;
     o->alpha_min = (float)p->alpha_min; o->alpha_max = (float)p->alpha_max; o->beta_xi = (float)p->beta_xi;
     o->target_neighbors = (float)p->target_neighbors;
     o->cfl = (float)p->cfl; o->min_dt = (float)p->min_dt; o->max_dt = (float)p->max_dt; o->dt_growth = (float)p->dt_growth;

@@ -13,6 +13,7 @@
 // same quantity are replaced by multiplications with a reciprocal, so results
 // differ from the CPU oracle by rounding only.
 #include <cuda_runtime.h>
+#include <cfloat>
 #include <atomic>
 #include <mutex>
 #include "sph_pair_common.cuh"
@@ -516,10 +517,72 @@ k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restric
 }
 
 // ---------------------------------------------------------------- Cullen-Hopkins switch
-// modules/shockCapturing/CullenHopkins.py:7-45 (computeHopkinsTerms, without the optional
-// velocity-gradient correction): the gather difference gradient
-// V_i = sum_j m_j/rho_j (v_j - v_i) (x) grad W(r_ij, H_i) (computeShearTensor, common.py:30-58),
-// its trace (the divergence) and |S|^2 = tr(S S^T) of the traceless symmetric part S.
+// Moore-Penrose inverse of a D x D matrix in FP64 by one-sided (Hestenes) Jacobi: column
+// rotations make A V = U orthogonal-columned, sigma_k = |U_k|, and
+// pinv(A) = sum_k v_k U_k^T / sigma_k^2 over sigma_k > rtol * sigma_max.  With
+// rtol = D * FLT_EPSILON this is torch.linalg.pinv's default cutoff for a float32 input
+// (CullenHopkins.py:27).  The sweep count is bounded; D <= 3 converges in a few sweeps.
+template <int D>
+__device__ __forceinline__ void pinv_jacobi(const double (&A)[D][D], double (&P)[D][D], double rtol) {
+    double U[D][D], V[D][D];
+    #pragma unroll
+    for (int a = 0; a < D; ++a)
+        #pragma unroll
+        for (int b = 0; b < D; ++b) { U[a][b] = A[a][b]; V[a][b] = a == b ? 1.0 : 0.0; }
+    for (int sweep = 0; sweep < 16; ++sweep) {
+        bool rotated = false;
+        #pragma unroll
+        for (int p = 0; p < D - 1; ++p)
+            #pragma unroll
+            for (int q = p + 1; q < D; ++q) {
+                double al = 0.0, be = 0.0, ga = 0.0;
+                #pragma unroll
+                for (int r = 0; r < D; ++r) { al += U[r][p] * U[r][p]; be += U[r][q] * U[r][q]; ga += U[r][p] * U[r][q]; }
+                if (!(fabs(ga) > 1e-15 * sqrt(al * be))) continue;
+                rotated = true;
+                const double zeta = (be - al) / (2.0 * ga);
+                const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                const double c = 1.0 / sqrt(1.0 + t * t), sn = c * t;
+                #pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    const double up = U[r][p], uq = U[r][q];
+                    U[r][p] = c * up - sn * uq; U[r][q] = sn * up + c * uq;
+                    const double vp = V[r][p], vq = V[r][q];
+                    V[r][p] = c * vp - sn * vq; V[r][q] = sn * vp + c * vq;
+                }
+            }
+        if (!rotated) break;
+    }
+    double s2[D], smax = 0.0;
+    #pragma unroll
+    for (int k = 0; k < D; ++k) {
+        s2[k] = 0.0;
+        #pragma unroll
+        for (int r = 0; r < D; ++r) s2[k] += U[r][k] * U[r][k];
+        smax = fmax(smax, sqrt(s2[k]));
+    }
+    const double cut = rtol * smax;
+    #pragma unroll
+    for (int a = 0; a < D; ++a)
+        #pragma unroll
+        for (int b = 0; b < D; ++b) P[a][b] = 0.0;
+    #pragma unroll
+    for (int k = 0; k < D; ++k) {
+        if (!(sqrt(s2[k]) > cut)) continue;
+        const double inv = 1.0 / s2[k];
+        #pragma unroll
+        for (int a = 0; a < D; ++a)
+            #pragma unroll
+            for (int b = 0; b < D; ++b) P[a][b] += V[a][k] * U[b][k] * inv;
+    }
+}
+
+// modules/shockCapturing/CullenHopkins.py:7-45 (computeHopkinsTerms): the gather difference
+// gradient V_i = sum_j m_j/rho_j (v_j - v_i) (x) grad W(r_ij, H_i) (computeShearTensor,
+// common.py:41-85), its trace (the divergence) and |S|^2 = tr(S S^T) of the traceless
+// symmetric part S.  With correctVelocityGradient the same pass accumulates the moment
+// matrix M_i = -sum_j m_j x_ij (x) grad W(r_ij, H_i) (common.py:10-25, wp_computeM.py:55-86)
+// and the gradient becomes pinv(M_i) V_i (common.py:76-78).
 template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_hopkins_grad(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
@@ -527,7 +590,8 @@ k_hopkins_grad(int n, DevParams P, const float* __restrict__ x, const float* __r
                const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
                float* __restrict__ div_out, float* __restrict__ shear2_out) {
     Grp<G> g(n);
-    Mat<D> Gm = mzero<D>();
+    Mat<D> Gm = mzero<D>(), Mm = mzero<D>();
+    const bool corr = P.correct_grad_v != 0;
     if (g.valid) {
         const int i = g.i;
         Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
@@ -540,7 +604,8 @@ k_hopkins_grad(int n, DevParams P, const float* __restrict__ x, const float* __r
             float W; Vec<D> gW;
             kWG_inv<KF, D>(xij, r, invHi, W, gW);
             if (W == 0.f) continue;
-            const float Vj = __ldg(m + j) / __ldg(rho + j);
+            const float mj = __ldg(m + j);
+            const float Vj = mj / __ldg(rho + j);
             Vec<D> vj = load_vec<D>(v, j);
             #pragma unroll
             for (int a = 0; a < D; ++a) {
@@ -548,13 +613,44 @@ k_hopkins_grad(int n, DevParams P, const float* __restrict__ x, const float* __r
                 #pragma unroll
                 for (int w = 0; w < D; ++w) Gm.m[a][w] += dv * gW.v[w];
             }
+            if (corr) {
+                #pragma unroll
+                for (int a = 0; a < D; ++a)
+                    #pragma unroll
+                    for (int w = 0; w < D; ++w) Mm.m[a][w] -= mj * xij.v[a] * gW.v[w];
+            }
         }
     }
     #pragma unroll
     for (int a = 0; a < D; ++a)
         #pragma unroll
         for (int w = 0; w < D; ++w) Gm.m[a][w] = gsum<G>(Gm.m[a][w]);
+    if (corr) {
+        #pragma unroll
+        for (int a = 0; a < D; ++a)
+            #pragma unroll
+            for (int w = 0; w < D; ++w) Mm.m[a][w] = gsum<G>(Mm.m[a][w]);
+    }
     if (!g.valid || g.lane != 0) return;
+    if (corr) {
+        double Md[D][D], Pd[D][D];
+        #pragma unroll
+        for (int a = 0; a < D; ++a)
+            #pragma unroll
+            for (int w = 0; w < D; ++w) Md[a][w] = (double)Mm.m[a][w];
+        pinv_jacobi<D>(Md, Pd, (double)D * (double)FLT_EPSILON);
+        Mat<D> C;
+        #pragma unroll
+        for (int a = 0; a < D; ++a)
+            #pragma unroll
+            for (int w = 0; w < D; ++w) {
+                double acc = 0.0;
+                #pragma unroll
+                for (int c = 0; c < D; ++c) acc += Pd[a][c] * (double)Gm.m[c][w];
+                C.m[a][w] = (float)acc;
+            }
+        Gm = C;
+    }
     float tr = Gm.m[0][0];
     #pragma unroll
     for (int a = 1; a < D; ++a) tr += Gm.m[a][a];

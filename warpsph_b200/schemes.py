@@ -159,8 +159,6 @@ def crkSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams:
         S.alphas = ops.switch_balsara(params, DvDx, S.soundspeeds)
     elif switch == ViscositySwitch.CullenHopkins:
         # crkSPH.py:195-200 (the alpha0 update of crkSPH.py:308-314 is commented out there)
-        if compParams.viscositySwitchParams.correctVelocityGradient:
-            raise NotImplementedError("the Cullen-Hopkins switch with correctVelocityGradient is not implemented on the GPU path")
         S.alphas, _, _, _ = ops.switch_hopkins_terms(params, S.positions, S.supports, S.masses, S.densities, S.velocities, S.alpha0s,
                                                      adjacency)
     elif switch != ViscositySwitch.NoneSwitch:
