@@ -641,6 +641,36 @@ int sph_delta_shift(const SphParams* p, int64_t n, const float* x, const float* 
                     float cfl, float c0, float R, int32_t nexp, float rho0,
                     uint32_t* scratch, float* shift_out, void* stream);
 
+/* ---------------------------------------------------------------- free-surface detection
+ * detectFreeSurface with the colour-field scheme (modules/surfaceDetection/wrapper.py:84-149).
+ * Rows are the interacting prefixes (every pair with r < max(H_i, H_j)).
+ *
+ * Colour field (colorFieldCompute.py:11-45, first half): color_out[i] =
+ * sum_j m_j/rho_j W(r_ij, H_i). */
+int sph_surface_color_field(const SphParams* p, int64_t n, const float* x, const float* H, const float* m,
+                            const float* rho, const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                            float* color_out, void* stream);
+
+/* detectFreeSurfaceColorField (colorFieldDetection.py:16-73) in one pass, with the gradient
+ * of colorFieldCompute.py:33-44 and the counts and sums of util/wp_numNeighbors.py and
+ * util/wp_sum.py (pairs with W(r_ij, max(H_i, H_j)) > 0, self included):
+ *   fs_out[i] = 1 if color[i] < S_i / N_i and N_i < neighbor_limit, else 0
+ *     (neighbor_limit = targetNeighbors * colorFieldThreshold);
+ *   normals_out [n, dim] (may be null) = normal_sign * grad c_i / max(|grad c_i|, 1e-12),
+ *     with grad c_i = sum_j m_j/rho_j (c_j - c_i) grad W(r_ij, H_i).  normal_sign is -1 for
+ *     NormalSource.ColorFieldGrad (wrapper.py:54-61) and +1 for the scheme's own normals;
+ *   num_neighbors_out (may be null) = N_i. */
+int sph_surface_detect_color_field(const SphParams* p, int64_t n, const float* x, const float* H, const float* m,
+                                   const float* rho, const float* color, const int32_t* offs, const int32_t* cnt,
+                                   const int32_t* list, float neighbor_limit, float normal_sign, float* fs_out,
+                                   float* normals_out, float* num_neighbors_out, void* stream);
+
+/* One dilation iteration (wp_dilate.py:14-89): fs_out[i] = sum_j fs_in[j] over the pairs
+ * with W(r_ij, max(H_i, H_j)) > 0.  The reference keeps the sum (a count, not a 0/1 mask);
+ * so does this.  fs_in and fs_out must not alias. */
+int sph_surface_dilate(const SphParams* p, int64_t n, const float* x, const float* H, const float* fs_in,
+                       const int32_t* offs, const int32_t* cnt, const int32_t* list, float* fs_out, void* stream);
+
 /* ---------------------------------------------------------------- learned warm start
  * No counterpart in the reference: a per-particle MLP predicts the initial pressure of
  * the Jacobi solves (replacing 0.75 p_prev at divergenceFree.py:72 and 0 at

@@ -98,6 +98,9 @@ class Oracle:
         L.oracle_owen_iter.argtypes = [P, i64, rp, rp, _i32p, _i32p, _i32p, _f64p, _f64p, C.c_int, C.c_double, rp, rpn, rpn, rp, rpn]
         L.oracle_switch_hopkins_terms.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rpn, rp, rp, rp, rpn]
         L.oracle_moment_matrix.argtypes = [P, i64, rp, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_surface_color_field.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_surface_detect.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, real_c, real_c, rp, rp, rp]
+        L.oracle_surface_dilate.argtypes = [P, i64, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_switch_hopkins_update.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, rp, real_c, _i32p, _i32p, _i32p, rp, rpn]
         L.oracle_vsig.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pi_pairs.argtypes = [P, i64, rp, rp, rp, rp, rpn, rpn, rp, _i32p, _i32p, _i32p, C.c_int, C.c_int, rp]
@@ -335,6 +338,27 @@ class Oracle:
         values at or below D * eps_float32 * sigma_max are dropped.  LAPACK's SVD in float64."""
         D = M.shape[-1]
         return np.linalg.pinv(np.asarray(M, np.float64), rcond=D * float(np.finfo(np.float32).eps))
+
+    def surface_color_field(self, params, x, H, m, rho, nb):
+        n = len(H)
+        c = np.zeros(n, self.dtype)
+        self.lib.oracle_surface_color_field(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho),
+                                            nb["offsets"], nb["counts"], nb["list"], c)
+        return c
+
+    def surface_detect(self, params, x, H, m, rho, c, nb, limit, normal_sign=-1.0):
+        """(fs mask, normals [n, D], neighbour counts)"""
+        n, D = len(H), int(params.dim)
+        fs, nn, nrm = np.zeros(n, self.dtype), np.zeros(n, self.dtype), np.zeros((n, D), self.dtype)
+        self.lib.oracle_surface_detect(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(c),
+                                       nb["offsets"], nb["counts"], nb["list"], float(limit), float(normal_sign), fs, nrm, nn)
+        return fs, nrm, nn
+
+    def surface_dilate(self, params, x, H, fs, nb):
+        out = np.zeros(len(H), self.dtype)
+        self.lib.oracle_surface_dilate(self._p(params), len(H), self.arr(x), self.arr(H), self.arr(fs),
+                                       nb["offsets"], nb["counts"], nb["list"], out)
+        return out
 
     def switch_hopkins_terms(self, params, x, H, m, rho, v, alpha0, nb):
         """(alphas, div, |S|^2, R); with params.correct_velocity_gradient the gradient is

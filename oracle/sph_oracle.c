@@ -784,6 +784,74 @@ int oracle_switch_hopkins_terms(const SphParams* p, int64_t n, const real* x, co
     return 0;
 }
 
+/* Free-surface detection, colour-field scheme (modules/surfaceDetection/colorFieldCompute.py,
+ * colorFieldDetection.py, util/wp_numNeighbors.py, util/wp_sum.py, wp_dilate.py).  The
+ * super-symmetric tests are W(r_ij, max(H_i, H_j)) > 0 as in the reference pair bodies. */
+int oracle_surface_color_field(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                               const int32_t* offs, const int32_t* cnt, const int32_t* list, real* c_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real s = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real W = kW(&o, rsqrt_safe(dotD(d, d, D)), H[i]);
+            if (W == 0) continue;
+            s += m[j] / rho[j] * W;
+        }
+        c_out[i] = s;
+    }
+    return 0;
+}
+
+int oracle_surface_detect(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                          const real* c, const int32_t* offs, const int32_t* cnt, const int32_t* list, real limit,
+                          real normal_sign, real* fs_out, real* normals_out, real* nn_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real gc[3] = {0, 0, 0}, nn = 0, cs = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real r = rsqrt_safe(dotD(d, d, D));
+            kWG(&o, d, r, H[i], &W, g);
+            if (W != 0)
+                for (int a = 0; a < D; ++a) gc[a] += m[j] / rho[j] * (c[j] - c[i]) * g[a];
+            if (kW(&o, r, H[i] > H[j] ? H[i] : H[j]) > 0) { nn += 1; cs += c[j]; }
+        }
+        fs_out[i] = (c[i] < cs / nn && nn < limit) ? 1 : 0;
+        nn_out[i] = nn;
+        real nrm = SQRT(dotD(gc, gc, D));
+        if (nrm < (real)1e-12) nrm = (real)1e-12;
+        for (int a = 0; a < D; ++a) normals_out[i * D + a] = normal_sign * (gc[a] / nrm);
+    }
+    return 0;
+}
+
+int oracle_surface_dilate(const SphParams* p, int64_t n, const real* x, const real* H, const real* fs, const int32_t* offs,
+                          const int32_t* cnt, const int32_t* list, real* out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real s = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            if (kW(&o, rsqrt_safe(dotD(d, d, D)), H[i] > H[j] ? H[i] : H[j]) > 0) s += fs[j];
+        }
+        out[i] = s;
+    }
+    return 0;
+}
+
 int oracle_switch_hopkins_update(const SphParams* p, int64_t n, const real* x, const real* H, const real* v, const real* c,
                                  const real* div, const real* div_prev, const real* alpha0, real dt,
                                  const int32_t* offs, const int32_t* cnt, const int32_t* list, real* alpha0_out,

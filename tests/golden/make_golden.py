@@ -66,6 +66,7 @@ vector = matrix = lambda *a, **k: None
 # ---------------------------------------------------------------- warpSPHCore restatement (ours)
 class OperationDirection(Enum):
     TrueAllToToAll = 0
+    AllToAll = 1
 
 
 KSCALE = {(1, 1): 1.620185175, (1, 2): 1.897366596, (1, 3): 1.936491673,
@@ -179,6 +180,15 @@ def computeKernelGradientCRK(xi, xj, hi, hj, kernelProperties, domainState, useC
     return out
 
 
+def computeKernelCRK(xi, xj, hi, hj, kernelProperties, domainState, useCRK, A, B):
+    # the kernel value under the operation's support scheme (no CRK call site here)
+    x = computeDistanceVec(xi, xj, domainState)
+    r = safe_sqrt(wp.dot(x, x))
+    mode = getattr(kernelProperties, "supportMode", None)
+    h = hi if mode == "gather" else (wp.max(hi, hj) if mode == "superSymmetric" else hj)
+    return kWG(x, r, h)[0]
+
+
 def sphKernelDkDh(xi, xj, hi, hj, kernelProperties, domainState):
     # gather support (the only call site, wp_omega.py:71, runs under SupportScheme.Gather)
     x = computeDistanceVec(xi, xj, domainState)
@@ -241,7 +251,7 @@ CORE = dict(scalar_t=F, vector=vector, matrix=matrix, Any=Any, OperationDirectio
             computeDistanceVec=computeDistanceVec, safe_sqrt=safe_sqrt, computeKernelGradientCRK=computeKernelGradientCRK,
             sphKernelScale=sphKernelScale, sphKernel_xi=sphKernel_xi, zero_like_warp=zero_like_warp, matmul=matmul,
             getParticle=getParticle, getVolume_j=getVolume_j, getCRK_j=getCRK_j, checkDirectionality_j=checkDirectionality_j,
-            sphKernelDkDh=sphKernelDkDh, iPow=iPow,
+            sphKernelDkDh=sphKernelDkDh, iPow=iPow, computeKernelCRK=computeKernelCRK,
             domainData=None, kernelState=None, adjacencyData=None, gridData=None)
 
 
@@ -265,6 +275,7 @@ def load(ref: Path, rel: str, extra: dict | None = None) -> dict:
               Enum=Enum, record_function=torch.profiler.record_function, __name__="ref_" + rel.replace("/", "_"))
     if extra:
         ns.update(extra)
+    sys.modules.setdefault(ns["__name__"], types.ModuleType(ns["__name__"]))   # dataclasses look their module up
     exec(compile("\n".join(out), str(ref / "src" / "warpSPH" / rel), "exec"), ns)
     return ns
 
@@ -848,6 +859,121 @@ def run_reference_hopkins(ref: Path, g: dict) -> dict:
     return out
 
 
+# ---------------------------------------------------------------- free-surface detection
+def make_surface_case(seed=21, nx=22, ny=12):
+    """A jittered 2D block of fluid in the lower half of a closed unit box: a free surface on
+    top and three walls without boundary particles, so the block's edges are surface."""
+    rng = np.random.default_rng(seed)
+    dx = 1.0 / 32
+    gx, gy = np.meshgrid((np.arange(nx) + 0.5) * dx - 0.5, (np.arange(ny) + 0.5) * dx - 0.5, indexing="xy")
+    x = np.stack([gx.ravel(), gy.ravel()], 1) + 0.2 * dx * (rng.random((nx * ny, 2)) - 0.5)
+    x = x.astype(F)
+    n = len(x)
+    H = (dx * np.sqrt(32 / np.pi) * (1 + 0.05 * (2 * rng.random(n) - 1))).astype(F)
+    m = np.full(n, dx * dx, F)
+    Ctx.kernel, Ctx.dim = 2, 2
+    rows = []
+    for i in range(n):
+        d = x[i] - x
+        r = np.sqrt((d.astype(np.float64) ** 2).sum(1))
+        rows.append(np.nonzero(r < 1.5 * np.maximum(H[i], H))[0].astype(np.int32))
+    counts = np.array([len(r) for r in rows], np.int32)
+    offsets = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int32)
+    lst = np.concatenate(rows).astype(np.int32)
+    rho = np.zeros(n, F)
+    for i in range(n):
+        for j in rows[i]:
+            d = computeDistanceVec(x[i], x[j])
+            rho[i] = F(rho[i] + m[j] * kWG(d, safe_sqrt(wp.dot(d, d)), H[i])[0])
+    return dict(x=x, H=H, m=m, rho=rho, offsets=offsets, counts=counts, list=lst)
+
+
+def run_reference_surface(ref: Path, case: dict) -> dict:
+    """detectFreeSurface (surfaceDetection/wrapper.py) with the SurfaceDetectionConfig
+    dataclass defaults (colour-field scheme, colour-field-gradient normals, one dilation),
+    run unmodified with computeColorField (colorFieldCompute.py), detectFreeSurfaceColorField
+    (colorFieldDetection.py) and dilateSurface (dilation.py).  The pair bodies of
+    countNeighborsWarp (util/wp_numNeighbors.py), warpSum (util/wp_sum.py) and
+    dilateSurfaceMaskWarp (wp_dilate.py) are the reference's own, run per particle under
+    super-symmetric support; warpSPHCore's gather interpolation and difference gradient are
+    restated in numpy as for the switches."""
+    Ctx.kernel, Ctx.dim = 2, 2
+    x, H, m, rho = (case[k] for k in ("x", "H", "m", "rho"))
+    offs, cnt, lst = case["offsets"], case["counts"], case["list"].astype(np.int64)
+    n = len(H)
+    state = SoA(positions=x, supports=H, masses=m, densities=rho, kinds=np.zeros(n, np.int32))
+
+    def warpOperation(st, props, domain=None, adjacency=None, queryValues=None, **kw):
+        q = queryValues.numpy().astype(F) if isinstance(queryValues, torch.Tensor) else np.asarray(queryValues, F)
+        outv = np.zeros((n, 2) if props.operation == "Gradient" else n, F)
+        for i in range(n):
+            for k in range(offs[i], offs[i] + cnt[i]):
+                j = lst[k]
+                d = computeDistanceVec(x[i], x[j])
+                W, gW = kWG(d, safe_sqrt(wp.dot(d, d)), H[i])
+                if W == 0:
+                    continue
+                Vj = F(m[j] / rho[j])
+                if props.operation == "Interpolate":
+                    outv[i] = F(outv[i] + Vj * q[j] * W)
+                else:
+                    outv[i] = (outv[i] + F(Vj * (q[j] - q[i])) * gW).astype(F)
+        return torch.from_numpy(outv)
+
+    class OperationProperties:
+        def __init__(self, kernel=None, operation=None, supportMode=None, gradientMode=None, operationMode=None):
+            self.operation = operation
+
+    kp = SoA(operationMode=OperationDirection.TrueAllToToAll.value, supportMode="superSymmetric")
+    common_args = dict(dim=2, referenceState=state, domainState=None, kernelProperties=kp, offsetArray=lst, ki=0,
+                       referenceKinds=state.kinds, useGradientRenormalization=False, Li=None, useGradHTerms=False,
+                       omega_i=F(1), referenceOmegas=None, Viscosity_i=F(1), referenceViscositys=None, useVolume=False, Vi=F(0),
+                       referenceVolumes=None, useCRK=False, Ai=F(1), Bi=None, gradAi=None, gradBi=None, outputValue=F(0))
+
+    def per_particle(fn, **extra):
+        out = np.zeros(n, F)
+        for i in range(n):
+            out[i] = call(fn, i=i, xi=x[i], hi=F(H[i]), mi=F(m[i]), rhoi=F(rho[i]), beginIndex=int(offs[i]),
+                          numIndices=int(cnt[i]), **common_args, **extra)
+        return torch.from_numpy(out)
+
+    nn_ns = load(ref, "modules/util/wp_numNeighbors.py")
+    sum_ns = load(ref, "modules/util/wp_sum.py")
+    dil_ns = load(ref, "modules/surfaceDetection/wp_dilate.py")
+    fnames = [k for k in nn_ns if k.endswith("_Func_i")]
+    count_fn = nn_ns[fnames[0]]
+    sum_fn = sum_ns["warpSum_Func_i"]
+    dil_fn = dil_ns["dilateSurfaceMask_Func_i"]
+    countNeighborsWarp = lambda *a, **k: per_particle(count_fn)
+    warpSum = lambda *a, queryValues=None, **k: per_particle(sum_fn, queryValues=np.asarray(queryValues, F))
+    dilateSurfaceMaskWarp = lambda *a, freeSurfaceMask=None, **k: per_particle(dil_fn, freeSurfaceMask=np.asarray(freeSurfaceMask, F))
+    names = dict(warpOperation=warpOperation, OperationProperties=OperationProperties,
+                 WarpOperation=types.SimpleNamespace(Interpolate="Interpolate", Gradient="Gradient"),
+                 GradientScheme=types.SimpleNamespace(Difference=1, Naive=0),
+                 SupportScheme=types.SimpleNamespace(Gather=0, SuperSymmetric=3), SimulationConfig=None,
+                 SurfaceDetectionConfig=None, AdjacencyList=None, CompactHashMap=None, RenormalizationState=None,
+                 countNeighborsWarp=countNeighborsWarp, warpSum=warpSum, dilateSurfaceMaskWarp=dilateSurfaceMaskWarp)
+    cfg_ns = load(ref, "configurations/moduleConfigurations/surfaceDetection.py")
+    names.update(SurfaceDetectionScheme=cfg_ns["SurfaceDetectionScheme"], NormalSource=cfg_ns["NormalSource"])
+    cf_ns = load(ref, "modules/surfaceDetection/colorFieldCompute.py", names)
+    names["computeColorField"] = cf_ns["computeColorField"]
+    det_ns = load(ref, "modules/surfaceDetection/colorFieldDetection.py", names)
+    names["detectFreeSurfaceColorField"] = det_ns["detectFreeSurfaceColorField"]
+    dl_ns = load(ref, "modules/surfaceDetection/dilation.py", names)
+    names["dilateSurface"] = dl_ns["dilateSurface"]
+    wr_ns = load(ref, "modules/surfaceDetection/wrapper.py", names)
+    sd = cfg_ns["SurfaceDetectionConfig"]()
+    ps = SoA(positions=torch.from_numpy(x))
+    sim = SoA(kernel=types.SimpleNamespace(value=2), domain=None, targetNeighbors=32.0)
+    fsm, fs, normals, _, _ = wr_ns["detectFreeSurface"](ps, sim, None, sd, None, returnNormals=True)
+    c, gc = cf_ns["computeColorField"](ps, sim, None, None)
+    nnb = per_particle(count_fn)
+    return dict(surface_color=c.numpy().astype(F), surface_color_grad=gc.numpy().astype(F), surface_num_neighbors=nnb.numpy(),
+                surface_fsm=fsm.numpy().astype(F), surface_fs=fs.numpy().astype(F), surface_normals=normals.numpy().astype(F),
+                surface_target_neighbors=np.array([32.0], F), surface_threshold=np.array([sd.colorFieldThreshold], F),
+                surface_expansion=np.array([sd.expansionIterations], np.int32))
+
+
 # ---------------------------------------------------------------- Owen adaptive support
 def _eval_C_d(dim, kernel):
     return kernel_C(int(kernel), int(dim))
@@ -1070,7 +1196,7 @@ def run_reference_deltasph(ref: Path, case: dict) -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph", "owen", "hopkins", "deltasph"], default="all")
+    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph", "owen", "hopkins", "deltasph", "surface"], default="all")
     a = ap.parse_args()
     ref = Path(a.reference)
     if a.which in ("all", "crk"):
@@ -1106,6 +1232,11 @@ def main():
         out = run_reference_hopkins(ref, g)
         np.savez_compressed(Path(__file__).parent / "hopkins_golden.npz", **out)
         print("wrote", Path(__file__).parent / "hopkins_golden.npz")
+    if a.which in ("all", "surface"):
+        case = make_surface_case()
+        out = run_reference_surface(ref, case)
+        np.savez_compressed(Path(__file__).parent / "surface_golden.npz", **case, **out)
+        print("wrote", Path(__file__).parent / "surface_golden.npz", "particles", len(case["H"]), "surface", int(out["surface_fsm"].sum()))
     if a.which in ("all", "deltasph"):
         case = make_deltasph_case()
         out = run_reference_deltasph(ref, case)

@@ -74,10 +74,18 @@ def test_unsupported_inputs_raise(step, cfgcls):
         setattr(c, attr, val)
         with pytest.raises(NotImplementedError, match=msg):
             step(IncompressibleSystem(state=cpu_state()), 1e-3, config, c)
-    c = cfgcls()
-    c.surfaceDetectionConfig.active = True
-    with pytest.raises(NotImplementedError, match="surface"):
-        step(IncompressibleSystem(state=cpu_state()), 1e-3, config, c)
+    # the colour-field scheme is built; the others raise before any pass runs
+    from warpsph_b200 import surface
+    from warpsph_b200.configurations import NormalSource, SurfaceDetectionScheme
+    st = cpu_state()
+    for scheme, normals in ((SurfaceDetectionScheme.Barecasco, NormalSource.ColorFieldGrad),
+                            (SurfaceDetectionScheme.Maronne, NormalSource.ColorFieldGrad),
+                            (SurfaceDetectionScheme.ColorField, NormalSource.LambdaGrad)):
+        sd = ws.configurations.SurfaceDetectionConfig(scheme=scheme, normalSource=normals)
+        with pytest.raises(NotImplementedError, match="surface detection scheme|normal source"):
+            surface.detectFreeSurface(st, config, cfgcls(), sd, None)
+    fsm, fs, n, _, _ = surface.detectFreeSurface(st, config, cfgcls(), ws.configurations.buildDefaultSurfaceDetectionConfig(), None)
+    assert not fsm.any() and not fs.any() and not n.any()
 
 
 def test_gravity_forms():

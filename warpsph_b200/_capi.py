@@ -147,6 +147,9 @@ _PROTOS = {
     "sph_mlp_forward": [_P, _I64, _P, _P, _P, _P],
     "sph_mlp_forward_tc": [_P, _I64, _P, _P, _P, _P, _P],
     "sph_wc_visc_continuity": [_P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "sph_surface_color_field": [_P, _I64] + [_P] * 9,
+    "sph_surface_detect_color_field": [_P, _I64] + [_P] * 8 + [C.c_float, C.c_float] + [_P] * 4,
+    "sph_surface_dilate": [_P, _I64] + [_P] * 8,
     "sph_delta_shift": [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_float, _P, _P, _P],
     "sph_mlp_grad": [_P, _I64, _P, _P, _P, _P, _P],
     "sph_mlp_adam": [_P, _P, _P, _P, _I64, C.c_float, C.c_float, C.c_float, C.c_float, _I64, _P],

@@ -391,20 +391,31 @@ class SurfaceDetectionScheme(Enum):
     Maronne = 3
 
 
+class NormalSource(Enum):
+    Native = 0
+    ColorFieldGrad = 1
+    LambdaGrad = 2
+    Maronne = 3
+
+
 @dataclass
 class SurfaceDetectionConfig:
-    """moduleConfigurations/surfaceDetection.py:22-35; the schemes' default config is
-    inactive (buildDefaultSurfaceDetectionConfig, :38-48)."""
-    active: bool = False
+    """moduleConfigurations/surfaceDetection.py:22-35 (the dataclass defaults: active,
+    colour-field scheme, colour-field-gradient normals).  The schemes take the inactive
+    buildDefaultSurfaceDetectionConfig (:38-48)."""
+    active: bool = True
     colorFieldThreshold: float = 0.75
     colorFieldGradThreshold: float = 10.0
-    barecascoThreshold: float = math.pi / 3
+    barecascoThreshold: float = 1.5
     expansionIterations: int = 1
-    scheme: SurfaceDetectionScheme = SurfaceDetectionScheme.Barecasco
+    scheme: SurfaceDetectionScheme = SurfaceDetectionScheme.ColorField
+    normalSource: NormalSource = NormalSource.ColorFieldGrad
 
 
 def buildDefaultSurfaceDetectionConfig() -> SurfaceDetectionConfig:
-    return SurfaceDetectionConfig()
+    return SurfaceDetectionConfig(active=False, colorFieldThreshold=0.75, colorFieldGradThreshold=10.0,
+                                  barecascoThreshold=math.pi / 3, expansionIterations=1,
+                                  scheme=SurfaceDetectionScheme.Barecasco, normalSource=NormalSource.LambdaGrad)
 
 
 @dataclass

@@ -423,6 +423,38 @@ def switch_hopkins_terms(params, x, H, m, rho, v, alpha0, adj: AdjacencyList):
     return al, div, s2, R
 
 
+def surface_color_field(params, x, H, m, rho, adj: AdjacencyList):
+    """Colour field c_i = sum_j m_j/rho_j W(r_ij, H_i) (colorFieldCompute.py:11-31)."""
+    c = _empty(H.shape[0], H)
+    with _timed("surface_color_field"):
+        check(_capi.lib().sph_surface_color_field(_p(params), H.shape[0], fptr(x), fptr(H), fptr(m), fptr(rho),
+                                                  *_lists(params, adj, True), ptr(c), stream_ptr(H.device)),
+              "sph_surface_color_field")
+    return c
+
+
+def surface_detect_color_field(params, x, H, m, rho, color, adj: AdjacencyList, neighbor_limit: float, normal_sign: float = -1.0):
+    """detectFreeSurfaceColorField (colorFieldDetection.py:16-73): (mask, normals, counts)."""
+    n, d = H.shape[0], x.shape[1]
+    fs, nn = _empty(n, H), _empty(n, H)
+    normals = torch.empty((n, d), device=H.device, dtype=torch.float32)
+    with _timed("surface_detect"):
+        check(_capi.lib().sph_surface_detect_color_field(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(color),
+                                                         *_lists(params, adj, True), float(neighbor_limit), float(normal_sign),
+                                                         ptr(fs), ptr(normals), ptr(nn), stream_ptr(H.device)),
+              "sph_surface_detect_color_field")
+    return fs, normals, nn
+
+
+def surface_dilate(params, x, H, fs, adj: AdjacencyList):
+    """One dilation iteration (wp_dilate.py:14-89): the sum of fs_j over the super-symmetric pairs."""
+    out = _empty(H.shape[0], H)
+    with _timed("surface_dilate"):
+        check(_capi.lib().sph_surface_dilate(_p(params), H.shape[0], fptr(x), fptr(H), fptr(_f32(fs)),
+                                             *_lists(params, adj, True), ptr(out), stream_ptr(H.device)), "sph_surface_dilate")
+    return out
+
+
 def switch_hopkins_update(params, x, H, v, c, div, div_prev, alpha0, dt, adj: AdjacencyList, want_vsig: bool = False):
     """Cullen-Hopkins alpha0 update (v_sig over the Verlet rows); (alpha0, v_sig or None)."""
     n = H.shape[0]

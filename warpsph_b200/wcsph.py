@@ -7,7 +7,7 @@ follows schemes/deltaSPH.py:11-208, call for call, for fluid-only systems:
   gather density                          dfsph.py:36-40  -> sph_density_gather
   mDBC density, boundary velocities,      dfsph.py:48-59, -> identities without boundary particles
   Dirichlet conditions, forcing, no-pen.  :106-126           (the reference's own early returns)
-  free-surface detection                  dfsph.py:72-77  -> inactive by default: zero indicators
+  free-surface detection                  dfsph.py:72-77  -> surface.detectFreeSurface (colour-field scheme)
   velocity diffusion + continuity         dfsph.py:100-109 -> sph_wc_visc_continuity (one pass)
   gravity                                 dfsph.py:117-120 -> computeGravity (elementwise)
   divergence-free solve                   dfsph.py:132-140 -> sph_dfsph_div_solve (persistent kernel)
@@ -17,9 +17,9 @@ follows schemes/deltaSPH.py:11-208, call for call, for fluid-only systems:
                                                                velocity diffusion, continuity,
                                                                pressure force in two passes)
 
-Systems with boundary (kind 1) or ghost (kind 2) particles, boundary conditions, rigid
-bodies or active surface detection need the mDBC, boundary-condition and surface passes,
-which are not on the GPU path; the steps raise NotImplementedError for them.
+Systems with boundary (kind 1) or ghost (kind 2) particles, boundary conditions or rigid
+bodies need the mDBC and boundary-condition passes, which are not on the GPU path; the
+steps raise NotImplementedError for them, as does the surface-aware shift.
 """
 from __future__ import annotations
 
@@ -31,6 +31,7 @@ from . import ops
 from .configurations import GravityType, make_params, wc_params
 from .core import SupportScheme
 from .incompressible import solveDivergenceFree, solveIncompressible
+from .surface import detectFreeSurface
 from .systems import _LAST_STAGE_FIELDS, IncompressibleSystemUpdate, WeaklyCompressibleSystemUpdate
 
 _KINDS_CHECKED: dict = {}
@@ -41,9 +42,6 @@ def _check_supported(state, schemeConfig) -> None:
         raise NotImplementedError("boundary conditions are not on the GPU path")
     if getattr(schemeConfig, "rigidBodies", None):
         raise NotImplementedError("rigid bodies are not on the GPU path")
-    sd = getattr(schemeConfig, "surfaceDetectionConfig", None)
-    if sd is not None and sd.active:
-        raise NotImplementedError("free-surface detection is not on the GPU path (it is inactive by default)")
     k = state.kinds
     if k is not None:
         key = (id(k), k._version)
@@ -83,6 +81,18 @@ def _zero_surface(S) -> None:
     S.surfaceLambdas = None
 
 
+def _surface(S, config, schemeConfig, adjacency) -> None:
+    """Step 8 of dfsph.py:72-77 / deltaSPH.py:86-91: indicators = (dilated mask > 0.5)."""
+    sd = getattr(schemeConfig, "surfaceDetectionConfig", None)
+    if sd is None or not sd.active:
+        _zero_surface(S)
+        return
+    fsm, fs, n, _, lmin = detectFreeSurface(S, config, schemeConfig, sd, adjacency, returnNormals=True)
+    S.surfaceIndicators = (fs > 0.5).to(torch.int32)
+    S.surfaceNormals = n
+    S.surfaceLambdas = lmin
+
+
 def _passive(S) -> torch.Tensor:
     return torch.zeros(S.densities.shape, device=S.densities.device, dtype=torch.bool)
 
@@ -96,7 +106,7 @@ def dfsph_step(system, dt, config, schemeConfig, verbose: bool = False):
     system.adjacency = adjacency
     if S.densities is None or not schemeConfig.solverConfig.integrateRho:
         S.densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
-    _zero_surface(S)
+    _surface(S, config, schemeConfig, adjacency)
     dvdt_diss, drhodt = ops.wc_visc_continuity(params, wc_params(schemeConfig), S.positions, S.supports, S.masses, S.densities,
                                                S.velocities, adjacency)
     dvdt = computeGravity(S, config, schemeConfig, adjacency)
@@ -118,7 +128,7 @@ def deltaSPH_step(system, dt, config, schemeConfig, verbose: bool = False):
     system.adjacency = adjacency
     if S.densities is None:
         S.densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
-    _zero_surface(S)
+    _surface(S, config, schemeConfig, adjacency)
     dvdt_rhs, drhodt, _, P = ops.deltasph_rhs(params, wc_params(schemeConfig), S.positions, S.supports, S.masses, S.densities,
                                               S.velocities, adjacency)
     S.pressures = P
@@ -138,6 +148,9 @@ def solveShifting(state, config, schemeConfig, adjacency, dt):
     (modules/shifting/delta.py), zero for kinds != 0.  Returns (dx, adjacency): the summed
     shift, the state itself left unchanged."""
     sp = schemeConfig.shiftProperties
+    sd = getattr(schemeConfig, "surfaceDetectionConfig", None)
+    if sd is not None and sd.active:
+        raise NotImplementedError("the free-surface treatment of the shift (shifting/wrapper.py:71-120) is not on the GPU path")
     params = make_params(config)
     dim = int(config.dim)
     c0 = schemeConfig.fluid.fixedSoundSpeed if schemeConfig.fluid.fixedSoundSpeed is not None else 1.0
