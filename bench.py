@@ -366,11 +366,16 @@ def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, step
     timer = ops.KernelTimer(names={timed_kernel}) if timed_kernel else None
     ops.TIMER = timer
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(steps):
-        one_step()
-    e1.record()
-    torch.cuda.synchronize()
+    gc.collect()
+    gc.disable()
+    try:
+        e0.record()
+        for _ in range(steps):
+            one_step()
+        e1.record()
+        torch.cuda.synchronize()
+    finally:
+        gc.enable()
     ops.TIMER = None
     ms = e0.elapsed_time(e1)
     S = box["system"].state
