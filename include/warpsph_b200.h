@@ -572,17 +572,21 @@ typedef struct SphWcParams {
     int32_t reserved_i[4];
 } SphWcParams;
 
-/* One delta-SPH right-hand side (schemes/deltaSPH.py:97-171 for a periodic fluid with
- * no boundaries, forcing or surface detection): pass A computes the renormalised
- * density gradient (modules/density/gradRhoL.py) and the EOS pressure into scratch
- * [n*(dim+1)] floats; pass B writes dvdt [n, dim] = pressure force
- * (modules/pressure/wp_surfaceAware.py) + velocity diffusion (wp_viscosityDelta.py) and
- * drhodt [n] = continuity (modules/momentum/inconsistent.py) + density diffusion
- * (modules/deltaSPH/densityDiffusion.py).  Kernel support max(H_i, H_j). */
+/* One delta-SPH right-hand side (schemes/deltaSPH.py:97-171 for a fluid with no
+ * boundaries or forcing): pass A computes the renormalised density gradient
+ * (modules/density/gradRhoL.py) and the EOS pressure into scratch [n*(dim+1)] floats;
+ * pass B writes dvdt [n, dim] = pressure force -sum_j V_j p_ij gradW_ij / rho_i
+ * (modules/pressure/wp_surfaceAware.py:207-218) + velocity diffusion (wp_viscosityDelta.py)
+ * and drhodt [n] = continuity (modules/momentum/inconsistent.py) + density diffusion
+ * (modules/deltaSPH/densityDiffusion.py).  Kernel support max(H_i, H_j).
+ * surface_mask [n] int32 (nullable = no free surface): the state's surfaceIndicators;
+ * the Antuono term takes P_j + P_i for a particle whose indicator is 1
+ * (wp_surfaceAware.py:89-92). */
 int sph_deltasph_rhs(const SphParams* p, const SphWcParams* wc, int64_t n, const float* x,
                      const float* H, const float* m, const float* rho, const float* v,
-                     const int32_t* offs, const int32_t* cnt, const int32_t* list,
-                     float* scratch, float* dvdt_out, float* drhodt_out, void* stream);
+                     const int32_t* surface_mask, const int32_t* offs, const int32_t* cnt,
+                     const int32_t* list, float* scratch, float* dvdt_out, float* drhodt_out,
+                     void* stream);
 
 /* Batched ensemble of independent periodic boxes (no counterpart in the reference, which
  * runs one simulation per process).  Particles of every box share one set of arrays;

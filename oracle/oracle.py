@@ -92,7 +92,7 @@ class Oracle:
         L.oracle_dfsph_alpha.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pressure_accel_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pressure_shift_iisph.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
-        L.oracle_deltasph_rhs.argtypes = [P, P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp, rp, rp]
+        L.oracle_deltasph_rhs.argtypes = [P, P, i64, rp, rp, rp, rp, rp, _nullable(_i32p), _i32p, _i32p, _i32p, rp, rp, rp, rp]
         L.oracle_delta_shift.argtypes = [P, i64, rp, rp, rp, rp, rp, C.c_void_p, _i32p, _i32p, _i32p, real_c, real_c, real_c, C.c_int,
                                          real_c, rp]
         L.oracle_owen_iter.argtypes = [P, i64, rp, rp, _i32p, _i32p, _i32p, _f64p, _f64p, C.c_int, C.c_double, rp, rpn, rpn, rp, rpn]
@@ -286,13 +286,15 @@ class Oracle:
         return p, acc, hist[: it.value], it.value
 
     # ------------------------------------------------------------------ weakly compressible delta-SPH
-    def deltasph_rhs(self, params, wc, x, H, m, rho, v, nb):
-        """(dvdt, drhodt, gradRhoL, P); wc is a warpsph_b200._capi.SphWcParams."""
+    def deltasph_rhs(self, params, wc, x, H, m, rho, v, nb, surface_mask=None):
+        """(dvdt, drhodt, gradRhoL, P); wc is a warpsph_b200._capi.SphWcParams; surface_mask
+        the int32 free-surface indicators or None."""
         n, d = len(H), params.dim
         gL = np.zeros((n, d), self.dtype); P = np.zeros(n, self.dtype)
         dv = np.zeros((n, d), self.dtype); dr = np.zeros(n, self.dtype)
+        sm = None if surface_mask is None else np.ascontiguousarray(surface_mask, np.int32)
         self.lib.oracle_deltasph_rhs(self._p(params), C.c_void_p(C.addressof(wc)), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho),
-                                     self.arr(v), nb["offsets"], nb["counts"], nb["list"], gL, P, dv, dr)
+                                     self.arr(v), sm, nb["offsets"], nb["counts"], nb["list"], gL, P, dv, dr)
         return dv, dr, gL, P
 
     def visc_continuity(self, params, wc, x, H, m, rho, v, nb):

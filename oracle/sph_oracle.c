@@ -1324,8 +1324,8 @@ static real wc_eos(const SphWcParams* w, real rho) {
 }
 
 int oracle_deltasph_rhs(const SphParams* p, const SphWcParams* w, int64_t n, const real* x, const real* H, const real* m,
-                        const real* rho, const real* v, const int32_t* offs, const int32_t* cnt, const int32_t* list, real* gL,
-                        real* Pr, real* dvdt, real* drhodt) {
+                        const real* rho, const real* v, const int32_t* smask, const int32_t* offs, const int32_t* cnt,
+                        const int32_t* list, real* gL, real* Pr, real* dvdt, real* drhodt) {
     OP o = op_from(p);
     int D = o.dim;
 #pragma omp parallel for schedule(static)
@@ -1368,6 +1368,7 @@ int oracle_deltasph_rhs(const SphParams* p, const SphWcParams* w, int64_t n, con
     for (int64_t i = 0; i < n; ++i) {
         real cont = 0, dd = 0, pf[3] = {0, 0, 0}, vs[3] = {0, 0, 0};
         real Hi = H[i], rhoi = rho[i], Pi = Pr[i], eps = (real)1.0e-14 * Hi;
+        int surf_i = smask != NULL && smask[i] == 1;   /* wp_surfaceAware.py:89-92: mask_i == 1 */
         real factor = w->inviscid ? (real)w->inviscid_alpha * (real)w->sound_speed * Hi / xi : visc_nu;
         for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
             int32_t j = list[k];
@@ -1392,7 +1393,7 @@ int oracle_deltasph_rhs(const SphParams* p, const SphWcParams* w, int64_t n, con
             switch (w->pressure_term) {
                 case SPH_PRESSURE_CONSERVATIVE: pij = Pj - Pi; break;
                 case SPH_PRESSURE_NONCONSERVATIVE: pij = Pj + Pi; break;
-                case SPH_PRESSURE_ANTUONO: pij = (Pi >= 0 || Pj >= 0) ? Pj + Pi : Pj - Pi; break;
+                case SPH_PRESSURE_ANTUONO: pij = (Pi >= 0 || Pj >= 0 || surf_i) ? Pj + Pi : Pj - Pi; break;
                 case SPH_PRESSURE_I: pij = Pi; break;
                 case SPH_PRESSURE_J: pij = Pj; break;
                 default: pij = (Pj / (rj * rj) + Pi / (rhoi * rhoi)) * rj; break;
@@ -1406,7 +1407,8 @@ int oracle_deltasph_rhs(const SphParams* p, const SphWcParams* w, int64_t n, con
             for (int a = 0; a < D; ++a) vs[a] += ww * gw[a];
         }
         drhodt[i] = -rhoi * cont + (real)w->density_delta * Hi / xi * (real)w->sound_speed * dd;
-        for (int a = 0; a < D; ++a) dvdt[i * D + a] = -pf[a] + vs[a];
+        /* the pressure force is divided by the particle's own density (wp_surfaceAware.py:207-218) */
+        for (int a = 0; a < D; ++a) dvdt[i * D + a] = -pf[a] / rhoi + vs[a];
     }
     return 0;
 }

@@ -293,11 +293,15 @@ class DeltaSPHOracle(DFSPHOracle):
     """schemes/deltaSPH.py:11-208 for a fluid-only system with the finalize of
     systems/weaklyCompressible.py:73-200: the delta-SPH right-hand side plus gravity; after
     the stages the delta-plus shift (when active) at the integrated state, the exponential
-    density update from the last stage, and the shift added to the positions."""
+    density update from the last stage, and the shift added to the positions.  With
+    ``surface`` (dict limit=, iterations=) the colour-field free-surface detection of
+    deltaSPH.py:86-91 runs before the right-hand side and its dilated indicators
+    (> 0.5) enter the Antuono pressure term."""
 
-    def __init__(self, params, wc, gravity=None, shift=None, precision: str = "f32"):
+    def __init__(self, params, wc, gravity=None, shift=None, precision: str = "f32", surface=None):
         CRKSPHOracle.__init__(self, params, precision, adaptive=False, compatible_energy=False)
         self.wc = wc
+        self.surface = surface
         self.g = None if gravity is None else np.asarray(gravity, self.dt_)
         self.shift = shift      # None or dict(cfl=, c0=, iterations=)
 
@@ -308,7 +312,16 @@ class DeltaSPHOracle(DFSPHOracle):
         nb = self.nb(x, H)
         if st.get("densities") is None:
             st["densities"] = o.density(p, 0, x, H, m, nb)
-        dv, dr, _, P = o.deltasph_rhs(p, self.wc, x, H, m, st["densities"], v, nb)
+        mask = None
+        if self.surface is not None:
+            rho = st["densities"]
+            c = o.surface_color_field(p, x, H, m, rho, nb)
+            fs = o.surface_detect(p, x, H, m, rho, c, nb, self.surface["limit"])[0]
+            for _ in range(int(self.surface.get("iterations", 1))):
+                fs = o.surface_dilate(p, x, H, fs, nb)
+            mask = (fs > 0.5).astype(np.int32)
+            st["surfaceIndicators"] = mask
+        dv, dr, _, P = o.deltasph_rhs(p, self.wc, x, H, m, st["densities"], v, nb, mask)
         st["pressures"] = P
         upd = dict(dxdt=v, dvdt=(dv + self.gravity(len(H))).astype(self.dt_), drhodt=dr)
         return upd, nb, st, {}

@@ -21,7 +21,7 @@ can feed identical inputs to the oracle or the GPU and compare with the referenc
 own results.
 
 Usage (in a container that has the reference checkout):
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference checkout> [--which ...]
 """
 from __future__ import annotations
 
@@ -1107,7 +1107,8 @@ def run_reference_deltasph(ref: Path, case: dict) -> dict:
     (modules/deltaSPH/wp_viscosityDelta.py; inviscid and viscid), 
     computeDensityDiffusionDeltaSPH_Func_i (modules/deltaSPH/wp_densityDelta.py; the
     deltaSPH, densityOnly and deltaOnly schemes) and computePressureSurfaceAware_Func_i
-    (modules/pressure/wp_surfaceAware.py; every pressure term, no surface mask)."""
+    (modules/pressure/wp_surfaceAware.py; every pressure term without a surface mask, and
+    the Antuono term with every third particle marked as free surface)."""
     p = case["params"]
     n, nb = case["n"], case["nb"]
     offs, cnt, lst = nb["offsets"], nb["counts"], nb["list"].astype(np.int64)
@@ -1147,6 +1148,15 @@ def run_reference_deltasph(ref: Path, case: dict) -> dict:
                 out["dd"][s_, i] = call(den["computeDensityDiffusionDeltaSPH_Func_i"], densityScheme=sch, **bb)
             for t in range(6):
                 out["pf"][t, i] = call(prs["computePressureSurfaceAware_Func_i"], pressureTerm=t, **b)
+    # the Antuono switch with free-surface particles (mask_i == 1 forces P_j + P_i)
+    smask = (np.arange(n) % 3 == 0).astype(np.int32)
+    antuono = enums["PressureForceScheme"].Antuono.value
+    out["pf_antuono_mask"] = np.zeros((n, 2), F)
+    with np.errstate(all="ignore"):
+        for i in range(n):
+            b = dict(base(i), mask_i=int(smask[i]), referenceSurfaceMask=smask)
+            out["pf_antuono_mask"][i] = call(prs["computePressureSurfaceAware_Func_i"], pressureTerm=antuono, **b)
+    out["surface_mask"] = smask
     out["dd_schemes"] = np.array(schemes, np.int32)
     out["wc_coeffs"] = WC_COEFFS
 
@@ -1195,7 +1205,7 @@ def run_reference_deltasph(ref: Path, case: dict) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the reference checkout (wi-re/warpSPH)")
     ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph", "owen", "hopkins", "deltasph", "surface"], default="all")
     a = ap.parse_args()
     ref = Path(a.reference)

@@ -7,7 +7,7 @@ The fixture holds the reference's (x, rho, u, p) profile and wave positions for 
 states (left rho=1, p=1, v=0; right rho=0.125, p=0.1, v=0; gamma=1.4) at t = 0.2 on
 [-0.5, 0.5] with the interface at 0.  tests/test_sod.py checks oracle/riemann.py against it.
 
-Usage:  python tests/golden/make_sod_exact.py [--reference /root/reference]
+Usage:  python tests/golden/make_sod_exact.py --reference <reference checkout>
 """
 from __future__ import annotations
 
@@ -20,7 +20,7 @@ import numpy as np
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the reference checkout (wi-re/warpSPH)")
     a = ap.parse_args()
     path = Path(a.reference) / "src" / "warpSPH" / "caseUtils" / "compressible" / "sod" / "sodSolution.py"
     spec = importlib.util.spec_from_file_location("ref_sodSolution", path)

@@ -3,8 +3,10 @@ reference's own pair bodies (tests/golden/make_golden.py --which deltasph runs
 modules/deltaSPH/wp_viscosityDelta.py, modules/deltaSPH/wp_densityDelta.py and
 modules/pressure/wp_surfaceAware.py unmodified, under the super-symmetric support).
 
-The oracle combines the terms (dv/dt = -pressure + viscosity, drho/dt = -rho continuity +
-delta (H / xi) c0 diffusion); each term is isolated by a parameter choice: a Tait EOS
+The oracle combines the terms (dv/dt = -pressure / rho_i + viscosity, the division being
+the one the reference's kernel wrapper applies at wp_surfaceAware.py:207-218; drho/dt =
+-rho continuity + delta (H / xi) c0 diffusion); each term is isolated by a parameter
+choice: a Tait EOS
 with kappa = 0 gives P = 0 (no pressure term), inviscid alpha = 0 gives no viscosity,
 and two densityDelta values separate the diffusion from the continuity.  Tolerances are
 a few FP32 ulps of each field's scale (1e-5 relative; 1e-4 where a difference of two
@@ -29,7 +31,7 @@ def gold():
     return dict(np.load(GOLD))
 
 
-def run(g, **kw):
+def run(g, surface_mask=None, **kw):
     _, _, p = make_params(2, kernel=core.KernelFunctions.Wendland4)
     cfg = WeaklyCompressibleSPHConfig()
     for k, v in kw.items():
@@ -40,7 +42,7 @@ def run(g, **kw):
         else:
             setattr(cfg, k, v)
     nb = dict(offsets=g["offsets"], counts=g["counts"], list=g["list"])
-    return oracle.get("f32").deltasph_rhs(p, wc_params(cfg), g["x"], g["H"], g["m"], g["rho"], g["v"], nb)
+    return oracle.get("f32").deltasph_rhs(p, wc_params(cfg), g["x"], g["H"], g["m"], g["rho"], g["v"], nb, surface_mask)
 
 
 def test_golden_inputs_reproduced(gold):
@@ -63,7 +65,20 @@ def test_golden_velocity_diffusion(gold, inviscid):
 def test_golden_pressure_force(gold, t):
     dv, _, _, P = run(gold, inviscid=True, inviscidAlpha=0.0, pressureForceTerm=PTERMS[t])
     assert np.array_equal(P, gold["P"])
-    assert_close(-dv, gold["pf"][t], 1e-5, 1e-5, f"pressure force {PTERMS[t]}")
+    want = -gold["pf"][t] / gold["rho"][:, None]      # the wrapper's -sum / rho_i
+    assert_close(dv, want, 1e-5, 1e-5, f"pressure force {PTERMS[t]}")
+
+
+def test_golden_pressure_force_surface_mask(gold):
+    """The Antuono term with free-surface particles: mask_i == 1 selects P_j + P_i even
+    where both pressures are negative (wp_surfaceAware.py:89-92)."""
+    mask = gold["surface_mask"]
+    assert np.any((mask == 1) & (gold["P"] < 0))
+    dv, _, _, _ = run(gold, surface_mask=mask, inviscid=True, inviscidAlpha=0.0, pressureForceTerm="Antuono")
+    assert_close(dv, -gold["pf_antuono_mask"] / gold["rho"][:, None], 1e-5, 1e-5, "Antuono pressure force with surface mask")
+    # without the mask the masked particles with negative pressure differ
+    dv0, _, _, _ = run(gold, inviscid=True, inviscidAlpha=0.0, pressureForceTerm="Antuono")
+    assert not np.allclose(dv0, dv)
 
 
 @pytest.mark.parametrize("s", range(3))

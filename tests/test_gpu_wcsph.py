@@ -130,3 +130,58 @@ def test_visc_continuity_and_shift_match_oracle(cuda):
     rs = o.delta_shift(p, x, H, m, rho, v, nb, 0.3, 10.0, kinds=kinds.cpu().numpy())
     assert_close(s.cpu().numpy(), rs, 1e-5, 1e-5, "delta-plus shift")
     assert bool((s[::5] == 0).all())
+
+
+def test_deltasph_rhs_surface_mask_matches_reference(cuda):
+    """The Antuono pressure force with free-surface particles on the GPU against the
+    reference's own pair body (golden vectors), divided by rho_i as the reference's
+    kernel wrapper does (wp_surfaceAware.py:207-218)."""
+    from pathlib import Path
+    g = dict(np.load(Path(__file__).resolve().parent / "golden" / "deltasph_golden.npz"))
+    cfg, _, p = make_params(2, kernel=core.KernelFunctions.Wendland4)
+    sch = WeaklyCompressibleSPHConfig()
+    sch.diffusionParams.inviscid = True
+    sch.diffusionParams.inviscidAlpha = 0.0
+    sch.pressureForceTerm = "Antuono"
+    t = {k: torch.from_numpy(np.ascontiguousarray(g[k])).to(cuda) for k in ("x", "H", "m", "rho", "v", "offsets", "counts", "list",
+                                                                              "surface_mask")}
+    n = len(g["H"])
+    adj = core.AdjacencyList(neighborOffsets=t["offsets"], numNeighbors=t["counts"], neighborList=t["list"], numRows=n, numCols=n,
+                             nnz=int(g["list"].shape[0]))
+    dv, _, _, P = ws.ops.deltasph_rhs(p, wc_params(sch), t["x"], t["H"], t["m"], t["rho"], t["v"], adj, t["surface_mask"])
+    assert_close(P.cpu().numpy(), g["P"], 1e-5, 1e-5, "stiff Tait pressure")
+    assert_close(dv.cpu().numpy(), -g["pf_antuono_mask"] / g["rho"][:, None], 1e-4, 1e-4, "Antuono force with surface mask")
+    dv0, _, _, _ = ws.ops.deltasph_rhs(p, wc_params(sch), t["x"], t["H"], t["m"], t["rho"], t["v"], adj)
+    assert_close(dv0.cpu().numpy(), -g["pf"][2] / g["rho"][:, None], 1e-4, 1e-4, "Antuono force without surface mask")
+
+
+def test_deltasph_step_free_surface_matches_oracle(cuda):
+    """deltaSPH_step with colour-field surface detection active on a block of fluid with
+    free edges: the dilated indicators switch the Antuono term of the surface particles."""
+    cfg, p, st = fluid_box(n_side=20, seed=7, kernel=core.KernelFunctions.Wendland4)
+    # squeeze the lattice into the middle of the periodic box: free surfaces on all sides
+    st = dict(st, positions=(st["positions"] * 0.5).astype(np.float32), masses=(st["masses"] * 0.25).astype(np.float32),
+              supports=(st["supports"] * 0.5).astype(np.float32))
+    System, State, Config, Update, step, *_ = ws.buildScheme("deltaSPH")
+    sch = Config()
+    sch.shiftProperties.active = False
+    sch.surfaceDetectionConfig.active = True
+    sch.pressureForceTerm = "Antuono"
+    dt = 5e-4
+    rng = np.random.default_rng(5)
+    rho = (1.0 + 0.01 * rng.standard_normal(len(st["masses"]))).astype(np.float32)
+    system = gpu_system(System, State, st, cuda, densities=rho)
+    res = getIntegrator(core.IntegrationSchemeType.rungeKutta2).function(state=system, f=step, dt=dt, config=cfg, compParams=sch)
+    sd = sch.surfaceDetectionConfig
+    orc = DeltaSPHOracle(p, wc_params(sch), surface=dict(limit=float(cfg.targetNeighbors) * float(sd.colorFieldThreshold),
+                                                         iterations=int(sd.expansionIterations)))
+    want, _, rvs = orc.step(dict(st, densities=rho, pressures=None), dt, "rungeKutta2")
+    S = res.state.state
+    mask = S.surfaceIndicators.cpu().numpy()
+    assert 0 < mask.sum() < len(mask)
+    assert np.array_equal(mask, rvs[-1][1]["surfaceIndicators"])
+    d = S.positions.cpu().numpy() - want["positions"]
+    d = d - np.round(d)
+    assert np.abs(d).max() < 2e-6, f"positions differ by {np.abs(d).max():.3g}"
+    for name in ("velocities", "densities", "pressures"):
+        assert_close(getattr(S, name).cpu().numpy(), want[name], 2e-4, 2e-4, f"delta-SPH free surface {name}")

@@ -1,7 +1,8 @@
 """Host-side logic of the DFSPH and delta-SPH step functions (no GPU): the scheme
 builder entries, configuration round trips, the enum forms the reference passes, gravity,
 and the cases the GPU path refuses (boundary and ghost particles, boundary conditions,
-rigid bodies, active surface detection), which raise before any device work."""
+rigid bodies, surface detection schemes other than the colour field), which raise before
+any device work."""
 import numpy as np
 import pytest
 import torch
@@ -21,6 +22,10 @@ from warpsph_b200.wcsph import computeGravity, deltaSPH_step, dfsph_step
 def test_build_scheme_entries(name, system, step):
     t = ws.buildScheme(name)
     assert len(t) == 7 and t[0] is system and t[4] is step
+    # builder.py:26-29 pairs deltaSPH with CompressibleSystemUpdate
+    if step is deltaSPH_step:
+        from warpsph_b200.systems import CompressibleSystemUpdate
+        assert t[3] is CompressibleSystemUpdate
     cfg = t[2]()
     assert t[6](t[5](cfg)) == cfg
 

@@ -1,12 +1,13 @@
 // Weakly compressible delta-SPH right-hand side (schemes/deltaSPH.py:11-208 without
-// boundaries, forcing, gravity, surface detection and shifting -- the periodic-box case):
+// boundaries, forcing, gravity and shifting; the free-surface indicators enter the Antuono
+// pressure term when the caller passes them):
 //
 //   pass A  L_i = (sum_j V_j gradW_ij (x) (x_j - x_i))^-1      renormalisation matrix
 //           gradRhoL_i = L_i sum_j V_j (rho_j - rho_i) gradW_ij (modules/density/gradRhoL.py:33-56)
 //   pass B  drhodt_i   = -rho_i sum_j V_j (v_j - v_i).gradW_ij  (modules/momentum/inconsistent.py:16-31)
 //                      + delta (H_i / xi) c0 sum_j V_j psi_ij.gradW_ij
 //                        (modules/deltaSPH/densityDiffusion.py:17-35, wp_densityDelta.py:14-118)
-//           dvdt_i     = -sum_j V_j p_ij gradW_ij               (modules/pressure/wp_surfaceAware.py:10-64, :207)
+//           dvdt_i     = -sum_j V_j p_ij gradW_ij / rho_i       (modules/pressure/wp_surfaceAware.py:10-102, :207)
 //                      + sum_j V_j mu_ij f gradW_ij / ((rho_i + rho_j) / 2)
 //                        (modules/deltaSPH/wp_viscosityDelta.py:14-108)
 // with V_j = m_j / rho_j, gradW_ij = grad_i W(x_i - x_j, max(H_i, H_j)) (super-symmetric
@@ -22,8 +23,8 @@ using namespace wsph;
 extern "C" {
 
 int sph_deltasph_rhs(const SphParams* p, const SphWcParams* wc, int64_t n, const float* x, const float* H, const float* m,
-                     const float* rho, const float* v, const int32_t* offs, const int32_t* cnt, const int32_t* list,
-                     float* scratch, float* dvdt_out, float* drhodt_out, void* stream) {
+                     const float* rho, const float* v, const int32_t* surface_mask, const int32_t* offs, const int32_t* cnt,
+                     const int32_t* list, float* scratch, float* dvdt_out, float* drhodt_out, void* stream) {
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(wc); WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(v);
     WSPH_CHECK_PTR(scratch); WSPH_CHECK_PTR(dvdt_out); WSPH_CHECK_PTR(drhodt_out); CHECK_CSR();
@@ -39,8 +40,8 @@ int sph_deltasph_rhs(const SphParams* p, const SphWcParams* wc, int64_t n, const
                                                                                                      list, gL, Pr)));
     count_launch();
     WSPH_DISPATCH_KDS(*p, (k_ds_passB<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, W, x, H, m, rho, v,
-                                                                                                     gL, Pr, offs, cnt, list,
-                                                                                                     dvdt_out, drhodt_out)));
+                                                                                                     gL, Pr, surface_mask, offs, cnt,
+                                                                                                     list, dvdt_out, drhodt_out)));
     return check_launch("sph_deltasph_rhs");
 }
 

@@ -132,16 +132,19 @@ template <int D, int G> __device__ __forceinline__ void passA_reduce(Mat<D>& M, 
 // Per-lane partial sums of pass B for particle i: cont = sum V (v_j - v_i).gW,
 // dd = sum V psi.gW, pf = sum V p_ij gW, visc = sum V mu f gW / rho_bar.  With FULL
 // false only cont and visc are formed (gL and Pr are not read): the velocity diffusion
-// and continuity of the DFSPH step.
+// and continuity of the DFSPH step.  smask (nullable) is the free-surface indicator of
+// each particle; the Antuono pressure term takes P_j + P_i when P_i >= 0, P_j >= 0 or
+// particle i lies on the free surface (wp_surfaceAware.py:89-92).
 template <int KF, int D, int G, bool CG = false, bool FULL = true>
 __device__ __forceinline__ void passB_partial(int i, int lane, const DevParams& P, const WcDev& W, const float* x,
                                               const float* __restrict__ H, const float* __restrict__ m, const float* rho,
-                                              const float* v, const float* gL, const float* Pr,
+                                              const float* v, const float* gL, const float* Pr, const int32_t* __restrict__ smask,
                                               const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
                                               const int32_t* __restrict__ list, float& cont, float& dd, Vec<D>& pf, Vec<D>& visc) {
     const Vec<D> xi = ldv<D, CG>(x, i), vi = ldv<D, CG>(v, i);
     const Vec<D> gLi = FULL ? ldv<D, CG>(gL, i) : vzero<D>();
     const float Hi = H[i], rhoi = ldf<CG>(rho + i), Pi = FULL ? ldf<CG>(Pr + i) : 0.f;
+    const bool surf_i = FULL && smask != nullptr && smask[i] == 1;
     const float eps = 1.0e-14f * Hi;
     const float factor = W.inviscid ? W.alpha * W.c0 * Hi / W.xi : W.visc_nu;
     const int b = offs[i], e = b + cnt[i];
@@ -176,14 +179,14 @@ __device__ __forceinline__ void passB_partial(int i, int lane, const DevParams& 
             }
             dd += Vj * pd;
         }
-        // pressure (wp_surfaceAware.py:48-63); no free-surface mask on this path
+        // pressure (wp_surfaceAware.py:48-102)
         if constexpr (FULL) {
             const float Pj = ldf<CG>(Pr + j);
             float pij;
             switch (W.pressure_term) {
                 case SPH_PRESSURE_CONSERVATIVE: pij = Pj - Pi; break;
                 case SPH_PRESSURE_NONCONSERVATIVE: pij = Pj + Pi; break;
-                case SPH_PRESSURE_ANTUONO: pij = (Pi >= 0.f || Pj >= 0.f) ? Pj + Pi : Pj - Pi; break;
+                case SPH_PRESSURE_ANTUONO: pij = (Pi >= 0.f || Pj >= 0.f || surf_i) ? Pj + Pi : Pj - Pi; break;
                 case SPH_PRESSURE_I: pij = Pi; break;
                 case SPH_PRESSURE_J: pij = Pj; break;
                 default: pij = (Pj / (rj * rj) + Pi / (rhoi * rhoi)) * rj; break;
@@ -205,12 +208,13 @@ __device__ __forceinline__ void passB_partial(int i, int lane, const DevParams& 
     }
 }
 
-// pass B output: drhodt = -rho cont + delta (H / xi) c0 dd, dvdt = -pf + visc.
+// pass B output: drhodt = -rho cont + delta (H / xi) c0 dd, dvdt = -pf / rho_i + visc
+// (the pressure force is divided by the particle's own density, wp_surfaceAware.py:207-218).
 template <int D> __device__ __forceinline__ void passB_finish(const WcDev& W, float rhoi, float Hi, float cont, float dd, const Vec<D>& pf,
                                                                const Vec<D>& visc, float& drho, Vec<D>& dv) {
     drho = -rhoi * cont + W.delta * Hi / W.xi * W.c0 * dd;
     #pragma unroll
-    for (int a = 0; a < D; ++a) dv.v[a] = -pf.v[a] + visc.v[a];
+    for (int a = 0; a < D; ++a) dv.v[a] = -pf.v[a] / rhoi + visc.v[a];
 }
 
 // Pass A: gradRhoL [n, D] and the EOS pressure P [n].
@@ -234,12 +238,12 @@ template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_ds_passB(int n, DevParams P, WcDev W, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
            const float* __restrict__ rho, const float* __restrict__ v, const float* __restrict__ gL, const float* __restrict__ Pr,
-           const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
-           float* __restrict__ dvdt, float* __restrict__ drhodt) {
+           const int32_t* __restrict__ smask, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
+           const int32_t* __restrict__ list, float* __restrict__ dvdt, float* __restrict__ drhodt) {
     Grp<G> g(n);
     float cont = 0.f, dd = 0.f;
     Vec<D> pf = vzero<D>(), visc = vzero<D>();
-    if (g.valid) passB_partial<KF, D, G>(g.i, g.lane, P, W, x, H, m, rho, v, gL, Pr, offs, cnt, list, cont, dd, pf, visc);
+    if (g.valid) passB_partial<KF, D, G>(g.i, g.lane, P, W, x, H, m, rho, v, gL, Pr, smask, offs, cnt, list, cont, dd, pf, visc);
     cont = gsum<G>(cont); dd = gsum<G>(dd);
     #pragma unroll
     for (int a = 0; a < D; ++a) { pf.v[a] = gsum<G>(pf.v[a]); visc.v[a] = gsum<G>(visc.v[a]); }
@@ -260,7 +264,8 @@ k_visc_cont(int n, DevParams P, WcDev W, const float* __restrict__ x, const floa
     Grp<G> g(n);
     float cont = 0.f, dd = 0.f;
     Vec<D> pf = vzero<D>(), visc = vzero<D>();
-    if (g.valid) passB_partial<KF, D, G, false, false>(g.i, g.lane, P, W, x, H, m, rho, v, nullptr, nullptr, offs, cnt, list, cont, dd, pf, visc);
+    if (g.valid) passB_partial<KF, D, G, false, false>(g.i, g.lane, P, W, x, H, m, rho, v, nullptr, nullptr, nullptr, offs, cnt, list, cont, dd, pf,
+                                                       visc);
     cont = gsum<G>(cont);
     #pragma unroll
     for (int a = 0; a < D; ++a) visc.v[a] = gsum<G>(visc.v[a]);

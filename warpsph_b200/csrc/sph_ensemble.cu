@@ -220,8 +220,8 @@ k_ens_step(EnsArgs a) {
             const bool valid = i < a.n;
             float cont = 0.f, dd = 0.f;
             Vec<D> pf = vzero<D>(), visc = vzero<D>();
-            if (valid) passB_partial<KF, D, G, true>(i, lane, a.P, a.W, xs, a.H, a.m, rs, vs, a.gL, a.Pr, a.offs, a.cnt, a.list,
-                                                        cont, dd, pf, visc);
+            if (valid) passB_partial<KF, D, G, true>(i, lane, a.P, a.W, xs, a.H, a.m, rs, vs, a.gL, a.Pr, nullptr, a.offs, a.cnt,
+                                                        a.list, cont, dd, pf, visc);
             cont = gsum<G>(cont); dd = gsum<G>(dd);
             #pragma unroll
             for (int c = 0; c < D; ++c) { pf.v[c] = gsum<G>(pf.v[c]); visc.v[c] = gsum<G>(visc.v[c]); }

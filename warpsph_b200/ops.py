@@ -753,14 +753,16 @@ def mlp_adam(theta, grad, m1, m2, step: int, lr: float, beta1=0.9, beta2=0.999, 
 
 
 # ------------------------------------------------------------------ weakly compressible delta-SPH
-def deltasph_rhs(params, wc, x, H, m, rho, v, adj: AdjacencyList):
-    """One delta-SPH right-hand side: (dvdt [n, dim], drhodt [n], gradRhoL [n, dim], P [n])."""
+def deltasph_rhs(params, wc, x, H, m, rho, v, adj: AdjacencyList, surface_mask=None):
+    """One delta-SPH right-hand side: (dvdt [n, dim], drhodt [n], gradRhoL [n, dim], P [n]).
+    surface_mask: the int32 free-surface indicators (None: no free surface)."""
     n, d = m.shape[0], int(params.dim)
     scratch = _empty(n * (d + 1), m)
     dvdt, drhodt = _empty((n, d), m), _empty(n, m)
+    sm = None if surface_mask is None else surface_mask.to(torch.int32).contiguous()
     with _timed("deltasph_rhs"):
         check(_capi.lib().sph_deltasph_rhs(_p(params), C.cast(C.pointer(wc), C.c_void_p), n, fptr(x), fptr(H), fptr(m), fptr(rho),
-                                           fptr(v), *_lists(params, adj, True), ptr(scratch), ptr(dvdt), ptr(drhodt),
+                                           fptr(v), iptr(sm), *_lists(params, adj, True), ptr(scratch), ptr(dvdt), ptr(drhodt),
                                            stream_ptr(m.device)), "sph_deltasph_rhs")
     return dvdt, drhodt, scratch[: n * d].view(n, d), scratch[n * d:]
 

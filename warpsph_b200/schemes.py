@@ -192,9 +192,11 @@ def buildScheme(schemeName: Union[str, CompressibleSPHScheme]):
                 compressibleConfigToDict, dictToCompressibleConfig)
     if (isinstance(schemeName, str) and schemeName == "deltaSPH") or schemeName == WeaklyCompressibleSPHScheme.deltaSPH:
         from .configurations import WeaklyCompressibleSPHConfig, dictToWeaklyCompressibleConfig, weaklyCompressibleConfigToDict
-        from .systems import WeaklyCompressibleState, WeaklyCompressibleSystem, WeaklyCompressibleSystemUpdate
+        from .systems import WeaklyCompressibleState, WeaklyCompressibleSystem
         from .wcsph import deltaSPH_step
-        return (WeaklyCompressibleSystem, WeaklyCompressibleState, WeaklyCompressibleSPHConfig, WeaklyCompressibleSystemUpdate,
+        # the reference's builder hands out CompressibleSystemUpdate here (builder.py:26-29),
+        # although deltaSPH_step itself builds WeaklyCompressibleSystemUpdate
+        return (WeaklyCompressibleSystem, WeaklyCompressibleState, WeaklyCompressibleSPHConfig, CompressibleSystemUpdate,
                 deltaSPH_step, weaklyCompressibleConfigToDict, dictToWeaklyCompressibleConfig)
     if (isinstance(schemeName, str) and schemeName in ("divergenceFree", "dfsph")) or schemeName == IncompressibleSPHScheme.divergenceFree:
         from .configurations import IncompressibleSPHConfig, dictToIncompressibleSPHConfig, incompressibleConfigToDict

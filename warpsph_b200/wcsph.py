@@ -15,7 +15,9 @@ follows schemes/deltaSPH.py:11-208, call for call, for fluid-only systems:
   delta-SPH right-hand side               deltaSPH.py:52-98 -> sph_deltasph_rhs (EOS, renormalised
                                                                density gradient, density and
                                                                velocity diffusion, continuity,
-                                                               pressure force in two passes)
+                                                               pressure force in two passes; the
+                                                               surface indicators enter the
+                                                               Antuono pressure term)
 
 Systems with boundary (kind 1) or ghost (kind 2) particles, boundary conditions or rigid
 bodies need the mDBC and boundary-condition passes, which are not on the GPU path; the
@@ -130,7 +132,7 @@ def deltaSPH_step(system, dt, config, schemeConfig, verbose: bool = False):
         S.densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
     _surface(S, config, schemeConfig, adjacency)
     dvdt_rhs, drhodt, _, P = ops.deltasph_rhs(params, wc_params(schemeConfig), S.positions, S.supports, S.masses, S.densities,
-                                              S.velocities, adjacency)
+                                              S.velocities, adjacency, S.surfaceIndicators)
     S.pressures = P
     update = WeaklyCompressibleSystemUpdate(dxdt=S.velocities.clone(), dvdt=dvdt_rhs + computeGravity(S, config, schemeConfig, adjacency),
                                             drhodt=drhodt, passive=_passive(S))
