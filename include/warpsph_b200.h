@@ -56,6 +56,9 @@ extern "C" {
 #define SPH_KERNEL_WENDLAND2 1
 #define SPH_KERNEL_WENDLAND4 2
 #define SPH_KERNEL_WENDLAND6 3
+/* B7: the degree-7 B-spline (eight intervals, knots at q = 1/4, 1/2, 3/4), the kernel of
+ * the reference's compressible notebooks (e.g. examples/compressible/01-Sod_Shock_Tube_1D.ipynb). */
+#define SPH_KERNEL_B7        4
 
 /* Support schemes (warpSPHCore SupportScheme): h used for the pair kernel value. */
 #define SPH_SUPPORT_GATHER               0   /* H_i */
@@ -446,9 +449,11 @@ int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const flo
  * device memory on the step path (an FFI host with no caching allocator, or a timed
  * loop where cudaMalloc/cudaFree would synchronise the device).  The scratch is a
  * fixed per-device array of SPH_BALANCE_NOALLOC_MAX_FLOATS floats, so n*(dim+1) must
- * not exceed it (SPH_ERR_BAD_ARG otherwise).  The first call on a device resolves the
- * array's address; make it before any stream capture.  Calls in flight at the same
- * time on one device share the array and race: serialise them on one stream. */
+ * not exceed it (SPH_ERR_BAD_ARG otherwise).  The array (16 MiB) is held on every
+ * device that loads the library until the process exits.  The first call on a device,
+ * and the first after its context was replaced (cudaDeviceReset), resolves the array's
+ * address; make it before any stream capture.  Calls in flight at the same time on one
+ * device share the array and race: serialise them on one stream. */
 #define SPH_BALANCE_NOALLOC_MAX_FLOATS (1 << 22)
 int sph_compsph_balance_noalloc(const SphParams* p, int64_t n, const float* m, const float* rho,
                                 const float* P, const float* u, const float* v, const float* dvdt,
@@ -469,7 +474,11 @@ typedef struct SphJacobiConfig {
      *    divergenceFree.py:72; density: 0, incompressible.py:79);
      * 1: p_init is used as given (a learned warm start). */
     int32_t init_mode;
-    int32_t reserved_i[3];
+    /* wait limit of each grid barrier in microseconds (0: 2 s).  A barrier that runs out
+     * sets SPH_STATUS_TIMEOUT and every block of the solve returns; the outputs then hold
+     * the last completed iteration's values. */
+    int32_t barrier_timeout_us;
+    int32_t reserved_i[2];
 } SphJacobiConfig;
 
 /* DFSPH diagonal, the value computeAlpha returns (modules/incompressible/wp_alpha.py:35-118,

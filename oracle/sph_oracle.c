@@ -71,10 +71,14 @@ typedef struct {
     int visc_term, cond_term, mswitch, correct_xi, scale_beta;
 } OP;
 
+/* Kernel scale H/h: Dehnen & Aly (2012) Table 1 for the Wendland kernels; for B7 the
+ * factor of the reference's CFL step as its notebooks print it (1D Woodward-Colella, 2D
+ * Gresho-Chan; 3D by the quintic spline's moment ratio sqrt(15/14) from 1D). */
 static double kscale_tab(int kernel, int dim) {
-    static const double t[3][3] = {{1.620185175, 1.897366596, 1.936491673},
+    static const double t[4][3] = {{1.620185175, 1.897366596, 1.936491673},
                                    {1.936491673, 2.171240593, 2.207940217},
-                                   {2.207940217, 2.415229458, 2.449489743}};
+                                   {2.207940217, 2.415229458, 2.449489743},
+                                   {3.865656972, 3.932734728, 4.001335111}};
     return t[kernel - 1][dim - 1];
 }
 
@@ -108,15 +112,35 @@ static OP op_from(const SphParams* p) {
 
 /* ------------------------------------------------------------------ kernels
  * Wendland (1995) functions with support radius H, q = r/H, normalisations C_d
- * (Dehnen & Aly 2012):  W = C_d/H^d k(q),  dk/dq = -q p(q). */
+ * (Dehnen & Aly 2012):  W = C_d/H^d k(q),  dk/dq = -q p(q).
+ * B7 (K = 4): the degree-7 B-spline k(q) = sum_j c_j (a_j - q)_+^7, a = 1, 3/4, 1/2, 1/4,
+ * c = 1, -8, 28, -56; p = -k'/q, from the expanded polynomial below q = 1/4 (where the
+ * constant term of k' cancels) and from the truncated powers above. */
+static real tpow(real a, real q, int n) {
+    real t = a - q, r = t;
+    if (!(t > 0)) return 0;
+    for (int i = 1; i < n; ++i) r *= t;
+    return r;
+}
 static real kernel_C(int K, int D) {
+    if (K == 4) return D == 1 ? (real)(4096.0 / 315.0) : (D == 2 ? (real)(589824.0 / (7435.0 * 3.14159265358979323846))
+                                                              : (real)(16384.0 / (105.0 * 3.14159265358979323846)));
     if (K == 1) return D == 1 ? (real)1.25 : (D == 2 ? (real)(7.0 / 3.14159265358979323846) : (real)(21.0 / (2.0 * 3.14159265358979323846)));
     if (K == 2) return D == 1 ? (real)1.5 : (D == 2 ? (real)(9.0 / 3.14159265358979323846) : (real)(495.0 / (32.0 * 3.14159265358979323846)));
     return D == 1 ? (real)1.71875 : (D == 2 ? (real)(78.0 / (7.0 * 3.14159265358979323846)) : (real)(1365.0 / (64.0 * 3.14159265358979323846)));
 }
 static void kernel_kp(int K, int D, real q, real* k, real* p) {
     real t = 1 - q;
-    if (K == 1) {
+    if (K == 4) {
+        *k = tpow(1, q, 7) - 8 * tpow((real)0.75, q, 7) + 28 * tpow((real)0.5, q, 7) - 56 * tpow((real)0.25, q, 7);
+        if (q < (real)0.25) {
+            real q2 = q * q;
+            *p = (real)3.28125 + q2 * ((real)-35 + q2 * ((real)210 - (real)245 * q));
+        } else {
+            *p = 7 * (tpow(1, q, 6) - 8 * tpow((real)0.75, q, 6) + 28 * tpow((real)0.5, q, 6)) / q;
+        }
+        (void)D;
+    } else if (K == 1) {
         if (D == 1) { real t2 = t * t; *k = t2 * t * (1 + 3 * q); *p = 12 * t2; }
         else { real t3 = t * t * t; *k = t3 * t * (1 + 4 * q); *p = 20 * t3; }
     } else if (K == 2) {

@@ -190,3 +190,42 @@ def test_jacobi_small_and_ragged_sizes(cuda):
 def C_ptr(cfg):
     import ctypes as C
     return C.cast(C.pointer(cfg), C.c_void_p)
+
+
+def test_jacobi_barrier_timeout_returns_status_and_next_solve_is_clean(cuda):
+    """A grid-barrier wait limit of 1 us makes the persistent solve's barriers run out: every
+    block returns, SPH_STATUS_TIMEOUT is set, the outputs hold the last completed phase
+    (finite), and the next solve with the default limit runs normally and matches the
+    oracle.  Nothing waits without a limit, so the test cannot hang the device."""
+    cfg, p, P, G, adj, nb = incompressible_case(2, 96, 71, cuda)
+    args = (G["positions"], G["supports"], G["masses"], G["rho"], G["velocities"], G["dvdt"], G["p_prev"], 2e-3, adj)
+    c = jcfg(64, 64, 0.0)
+    c.barrier_timeout_us = 1
+    timed_out = 0
+    for _ in range(3):      # each barrier gives up unless every block arrives within 1 us
+        pr, acc, hist, it, st = ops.jacobi_solve(p, ops.DIVERGENCE_FREE, c, *args)
+        s = int(st.item())
+        timed_out += bool(s & 0x8)
+        assert torch.isfinite(pr).all() and torch.isfinite(acc).all()
+        assert 0 <= int(it.item()) < 64 or not (s & 0x8)
+    assert timed_out >= 1
+    c.barrier_timeout_us = 0
+    pr, acc, hist, it, st = ops.jacobi_solve(p, ops.DIVERGENCE_FREE, c, *args)
+    assert int(st.item()) & 0x8 == 0 and int(it.item()) == 64
+    rp, racc, rhist, rit = oracle.get("f32").jacobi_solve(p, ops.DIVERGENCE_FREE, c, P["positions"], P["supports"], P["masses"],
+                                                          P["rho"], P["velocities"], P["dvdt"], P["p_prev"], 2e-3, nb)
+    assert_close(pr.cpu().numpy(), rp, 1e-3, 1e-3, "pressure after a timed-out solve")
+
+
+def test_nonfinite_inputs_report_status(cuda):
+    """Host-injected NaN velocities: the divergence source and the Jacobi error become
+    non-finite and the persistent solve stops with SPH_STATUS_NONFINITE instead of
+    iterating to the cap."""
+    cfg, p, P, G, adj, nb = incompressible_case(2, 48, 72, cuda)
+    v = G["velocities"].clone()
+    v[5] = float("nan")
+    c = jcfg(2, 32, 1e-6)
+    pr, acc, hist, it, st = ops.jacobi_solve(p, ops.DIVERGENCE_FREE, c, G["positions"], G["supports"], G["masses"], G["rho"], v,
+                                             G["dvdt"], G["p_prev"], 2e-3, adj)
+    assert int(st.item()) & 0x2, f"status {int(st.item()):#x}"
+    assert int(it.item()) < 32

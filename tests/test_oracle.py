@@ -22,6 +22,35 @@ def o32():
     return oracle.get("f32")
 
 
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_b7_kernel(o64, dim):
+    """The degree-7 B-spline: unit integral, the spline's values at its knots, derivatives
+    against finite differences across the polynomial switch at q = 1/4, and the kernel
+    scale table (1D and 2D read from the reference notebooks' printed time steps; their
+    ratio is the quintic spline's sqrt(d I_(d-1)/I_(d+1)) ratio, which also gives 3D)."""
+    kernel = core.KernelFunctions.B7
+    surf = {1: lambda r: 2.0, 2: lambda r: 2 * np.pi * r, 3: lambda r: 4 * np.pi * r * r}[dim]
+    W = lambda r: o64.kernel_eval(kernel.value, dim, np.array([r]), 1.0)[0][0]
+    assert abs(quad(lambda r: W(r) * surf(r), 0, 1, epsabs=1e-13, points=[0.25, 0.5, 0.75])[0] - 1.0) < 1e-9
+    C = core.kernel_constants(kernel, dim)[0]
+    tp = lambda a, q: max(a - q, 0.0) ** 7
+    for q in (0.0, 0.1, 0.25, 0.4, 0.5, 0.75, 0.9):
+        want = C * (tp(1, q) - 8 * tp(0.75, q) + 28 * tp(0.5, q) - 56 * tp(0.25, q))
+        assert abs(W(q) - want) < 1e-12 * C
+    r = np.concatenate([np.linspace(0.01, 0.99, 97), [0.2499, 0.25, 0.2501]])
+    H = 0.7
+    _, dWdr, dWdH = o64.kernel_eval(kernel.value, dim, r, H)
+    e = 1e-6
+    Wp, _, _ = o64.kernel_eval(kernel.value, dim, r + e, H)
+    Wm, _, _ = o64.kernel_eval(kernel.value, dim, r - e, H)
+    assert_close(dWdr, (Wp - Wm) / (2 * e), 1e-6, 1e-6, "dW/dr")
+    Hp, _, _ = o64.kernel_eval(kernel.value, dim, r, H + e)
+    Hm, _, _ = o64.kernel_eval(kernel.value, dim, r, H - e)
+    assert_close(dWdH, (Hp - Hm) / (2 * e), 1e-6, 1e-6, "dW/dH")
+    s1, s2, s3 = (core.sphKernelScale(kernel, d) for d in (1, 2, 3))
+    assert abs(s2 / s1 - np.sqrt(2868 / 2771)) < 1e-7 and abs(s3 / s1 - np.sqrt(15 / 14)) < 1e-9
+
+
 @pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("dim", [1, 2, 3])
 def test_kernel_normalisation_and_derivatives(o64, kernel, dim):

@@ -73,7 +73,8 @@ class SphJacobiConfig(C.Structure):
         ("min_iterations", C.c_int32),
         ("max_iterations", C.c_int32),
         ("init_mode", C.c_int32),
-        ("reserved_i", C.c_int32 * 3),
+        ("barrier_timeout_us", C.c_int32),
+        ("reserved_i", C.c_int32 * 2),
     ]
 
 

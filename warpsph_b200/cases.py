@@ -47,11 +47,14 @@ def buildPointCloud(nx, domain, targetNeighbors=16, device=None, dtype=torch.flo
 
 
 def kernel_weight(kernel, dim, r: torch.Tensor, H: torch.Tensor) -> torch.Tensor:
-    """W(r, H) of the Wendland family on torch tensors (set-up only)."""
+    """W(r, H) of the Wendland family and of B7 on torch tensors (set-up only)."""
     C, _ = kernel_constants(kernel, dim)
     q = (r / H).clamp(max=1.0)
     t = 1 - q
     k = kernel.value
+    if k == 4:
+        tp = lambda a: (a - q).clamp(min=0.0) ** 7
+        return C / H ** dim * (tp(1.0) - 8 * tp(0.75) + 28 * tp(0.5) - 56 * tp(0.25))
     if k == 1:
         f = t ** 3 * (1 + 3 * q) if dim == 1 else t ** 4 * (1 + 4 * q)
     elif k == 2:

@@ -469,6 +469,9 @@ class IncompressibleSPHConfig:
     diffusionParams: WeaklyCompressibleDiffusionParams = field(default_factory=WeaklyCompressibleDiffusionParams)
     schemeName: str = "Compressible SPH"
     boundaryConditions: List[Any] = field(default_factory=list)
+    dt_viscosityConstraint: bool = True
+    dt_accelerationConstraint: bool = True
+    dt_acousticConstraint: bool = True
     pressureForceTerm: Any = "Antuono"
     shiftProperties: ShiftProperties = field(default_factory=buildDefaultShiftProperties)
     regions: List[Any] = field(default_factory=list)
@@ -505,6 +508,9 @@ class WeaklyCompressibleSPHConfig:
     diffusionParams: WeaklyCompressibleDiffusionParams = field(default_factory=WeaklyCompressibleDiffusionParams)
     schemeName: str = "Compressible SPH"
     boundaryConditions: List[Any] = field(default_factory=list)
+    dt_viscosityConstraint: bool = True
+    dt_accelerationConstraint: bool = True
+    dt_acousticConstraint: bool = True
     pressureForceTerm: Any = "Antuono"
     shiftProperties: ShiftProperties = field(default_factory=buildDefaultShiftProperties)
     regions: List[Any] = field(default_factory=list)

@@ -21,6 +21,7 @@ class KernelFunctions(Enum):
     Wendland2 = 1
     Wendland4 = 2
     Wendland6 = 3
+    B7 = 4          # degree-7 B-spline, the compressible notebooks' kernel
 
 
 class SupportScheme(Enum):
@@ -63,14 +64,24 @@ class SamplingScheme(Enum):
 
 
 def kernel_constants(kernel: KernelFunctions, dim: int) -> tuple[float, float]:
-    """(normalisation C_d, kernel scale H/h) -- Wendland (1995), Dehnen & Aly (2012) Table 1."""
+    """(normalisation C_d, kernel scale H/h).
+
+    Wendland kernels: Wendland (1995) normalisations and Dehnen & Aly (2012) Table 1 scales;
+    the 2D values reproduce the reference notebooks' printed lattice densities and c0
+    (examples/incompressible/01-taylor-green-vortex.ipynb, periodic-random-flow.ipynb).
+    B7 (degree-7 B-spline): C_d integrates it to one; the scale is the factor the
+    reference's CFL step divides by, read from the printed initial time steps of
+    examples/compressible/05-Woodward_Colella.ipynb (1D) and 09-Gresho_Chan_Vortex.ipynb
+    (2D), and continued to 3D by the quintic spline's moment ratio sqrt(15/14)."""
     pi = np.pi
     norms = {1: {1: 1.25, 2: 7 / pi, 3: 21 / (2 * pi)},
              2: {1: 1.5, 2: 9 / pi, 3: 495 / (32 * pi)},
-             3: {1: 1.71875, 2: 78 / (7 * pi), 3: 1365 / (64 * pi)}}
+             3: {1: 1.71875, 2: 78 / (7 * pi), 3: 1365 / (64 * pi)},
+             4: {1: 4096 / 315, 2: 589824 / (7435 * pi), 3: 16384 / (105 * pi)}}
     scales = {1: {1: 1.620185175, 2: 1.897366596, 3: 1.936491673},
               2: {1: 1.936491673, 2: 2.171240593, 3: 2.207940217},
-              3: {1: 2.207940217, 2: 2.415229458, 3: 2.449489743}}
+              3: {1: 2.207940217, 2: 2.415229458, 3: 2.449489743},
+              4: {1: 3.865656972, 2: 3.932734728, 3: 4.001335111}}
     k = kernel.value
     return norms[k][dim], scales[k][dim]
 

@@ -145,6 +145,14 @@ template <int D> __device__ __forceinline__ float dist2_rn(const Vec<D>& d) {
 //   dW/dH    = -C_D / H^(D+1) * (D k(q) - q^2 p(q))
 // Normalisations C_D integrate W to one; they are the standard Wendland (1995)
 // values used by Dehnen & Aly (2012).
+//
+// B7 is the degree-7 B-spline on q in [0, 1] (knots at 1/4, 1/2, 3/4):
+//   k(q) = (1-q)^7 - 8 (3/4-q)^7 + 28 (1/2-q)^7 - 56 (1/4-q)^7   (truncated powers)
+// with p(q) = -k'(q)/q.  Below q = 1/4 p is the expanded polynomial
+//   105/32 - 35 q^2 + 210 q^4 - 245 q^5
+// (the constant term of k' cancels there, so dividing by q would lose digits); above it
+// the truncated-power sum divided by q.  C_D = 4096/315, 589824/(7435 pi),
+// 16384/(105 pi) integrate it to one in 1, 2 and 3 dimensions.
 template <int KF, int D> struct KernelTraits;
 template <> struct KernelTraits<SPH_KERNEL_WENDLAND2, 1> { static constexpr float C = 1.25f; };
 template <> struct KernelTraits<SPH_KERNEL_WENDLAND2, 2> { static constexpr float C = (float)(7.0 / 3.14159265358979323846); };
@@ -155,11 +163,31 @@ template <> struct KernelTraits<SPH_KERNEL_WENDLAND4, 3> { static constexpr floa
 template <> struct KernelTraits<SPH_KERNEL_WENDLAND6, 1> { static constexpr float C = 1.71875f; };
 template <> struct KernelTraits<SPH_KERNEL_WENDLAND6, 2> { static constexpr float C = (float)(78.0 / (7.0 * 3.14159265358979323846)); };
 template <> struct KernelTraits<SPH_KERNEL_WENDLAND6, 3> { static constexpr float C = (float)(1365.0 / (64.0 * 3.14159265358979323846)); };
+template <> struct KernelTraits<SPH_KERNEL_B7, 1> { static constexpr float C = (float)(4096.0 / 315.0); };
+template <> struct KernelTraits<SPH_KERNEL_B7, 2> { static constexpr float C = (float)(589824.0 / (7435.0 * 3.14159265358979323846)); };
+template <> struct KernelTraits<SPH_KERNEL_B7, 3> { static constexpr float C = (float)(16384.0 / (105.0 * 3.14159265358979323846)); };
+
+// Truncated power (a - q)_+^n.
+template <int N> __device__ __forceinline__ float tpow(float a, float q) {
+    const float t = a - q;
+    if (!(t > 0.f)) return 0.f;
+    float r = t;
+    _Pragma("unroll") for (int i = 1; i < N; ++i) r *= t;
+    return r;
+}
 
 // k(q) and p(q) for 0 <= q < 1 (callers handle q >= 1).
 template <int KF, int D> __device__ __forceinline__ void kernel_kp(float q, float& k, float& p) {
     float t = 1.f - q;
-    if constexpr (KF == SPH_KERNEL_WENDLAND2) {
+    if constexpr (KF == SPH_KERNEL_B7) {
+        k = tpow<7>(1.f, q) - 8.f * tpow<7>(0.75f, q) + 28.f * tpow<7>(0.5f, q) - 56.f * tpow<7>(0.25f, q);
+        if (q < 0.25f) {
+            const float q2 = q * q;
+            p = 3.28125f + q2 * (-35.f + q2 * (210.f - 245.f * q));
+        } else {
+            p = 7.f * (tpow<6>(1.f, q) - 8.f * tpow<6>(0.75f, q) + 28.f * tpow<6>(0.5f, q)) / q;
+        }
+    } else if constexpr (KF == SPH_KERNEL_WENDLAND2) {
         if constexpr (D == 1) { float t2 = t * t; k = t2 * t * (1.f + 3.f * q); p = 12.f * t2; }
         else { float t3 = t * t * t; k = t3 * t * (1.f + 4.f * q); p = 20.f * t3; }
     } else if constexpr (KF == SPH_KERNEL_WENDLAND4) {
@@ -257,6 +285,7 @@ template <int D> __device__ __forceinline__ Vec<D> crk_grad(const Vec<D>& x, flo
         case SPH_KERNEL_WENDLAND2: { constexpr int KF = SPH_KERNEL_WENDLAND2; WSPH_DISPATCH_DIM(dim, __VA_ARGS__) } break; \
         case SPH_KERNEL_WENDLAND4: { constexpr int KF = SPH_KERNEL_WENDLAND4; WSPH_DISPATCH_DIM(dim, __VA_ARGS__) } break; \
         case SPH_KERNEL_WENDLAND6: { constexpr int KF = SPH_KERNEL_WENDLAND6; WSPH_DISPATCH_DIM(dim, __VA_ARGS__) } break; \
+        case SPH_KERNEL_B7: { constexpr int KF = SPH_KERNEL_B7; WSPH_DISPATCH_DIM(dim, __VA_ARGS__) } break;               \
         default: break;                                                                               \
     }
 

@@ -236,6 +236,7 @@ struct JacobiArgs {
     int32_t* iters_out;
     int32_t* status_out;
     JacobiCtl* ctl;
+    unsigned long long barrier_ns;   // grid-barrier wait limit
 };
 
 template <typename T> __device__ __forceinline__ T warp_sum(T v) {
@@ -252,6 +253,15 @@ __device__ __forceinline__ unsigned int warp_max_u(unsigned int v) {
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
+}
+
+// A grid barrier ran out: the block records the timeout (block 0 also the iteration it
+// had reached) and returns.  p_out and acc hold the last completed phase A.
+__device__ __forceinline__ void jacobi_gave_up(const JacobiArgs& a, int it) {
+    if (threadIdx.x == 0) {
+        atomicOr(a.status_out, SPH_STATUS_TIMEOUT);
+        if (blockIdx.x == 0) *a.iters_out = it;
+    }
 }
 
 template <int KF, int D>
@@ -300,7 +310,7 @@ k_jacobi(JacobiArgs a) {
             }
         }
         if (converged || it >= a.max_it) break;
-        if (!grid_barrier(&c->bar)) { if (threadIdx.x == 0) atomicOr(a.status_out, SPH_STATUS_TIMEOUT); return; }
+        if (!grid_barrier(&c->bar, a.barrier_ns)) { jacobi_gave_up(a, it); return; }
 
         // ------------------------------------------------ phase B: shift, residual, update
         double psum = 0.0, esum = 0.0;
@@ -344,7 +354,7 @@ k_jacobi(JacobiArgs a) {
             atomicMin(&c->mm[sl][0], lo);
             atomicMax(&c->mm[sl][1], hi);
         }
-        if (!grid_barrier(&c->bar)) { if (threadIdx.x == 0) atomicOr(a.status_out, SPH_STATUS_TIMEOUT); return; }
+        if (!grid_barrier(&c->bar, a.barrier_ns)) { jacobi_gave_up(a, it); return; }
 
         // ------------------------------------------------ decide (identical in every block)
         const int sl = it % 3;
@@ -428,6 +438,7 @@ static int dfsph_solve(int mode, const SphParams* p, const SphJacobiConfig* cfg,
         return set_error(SPH_ERR_BAD_ARG, "jacobi: iteration counts out of range");
     if (!(cfg->relaxation == cfg->relaxation) || !(cfg->tolerance == cfg->tolerance))
         return set_error(SPH_ERR_BAD_ARG, "jacobi: NaN relaxation or tolerance");
+    if (cfg->barrier_timeout_us < 0) return set_error(SPH_ERR_BAD_ARG, "jacobi: barrier_timeout_us must be >= 0");
     if (ws_bytes < dfsph_ws_bytes(n)) return set_error(SPH_ERR_WORKSPACE, "jacobi: workspace %lld < %lld bytes", (long long)ws_bytes,
                                                        (long long)dfsph_ws_bytes(n));
     if (reinterpret_cast<uintptr_t>(ws) & 255) return set_error(SPH_ERR_BAD_ARG, "jacobi: workspace must be 256-byte aligned");
@@ -454,6 +465,7 @@ static int dfsph_solve(int mode, const SphParams* p, const SphJacobiConfig* cfg,
     a.offs = offs; a.cnt = cnt; a.list = list;
     a.praw = praw; a.p_out = p_out; a.acc = accel_out; a.hist = history;
     a.iters_out = iterations; a.status_out = status; a.ctl = ctl;
+    a.barrier_ns = cfg->barrier_timeout_us > 0 ? 1000ull * (unsigned long long)cfg->barrier_timeout_us : kBarrierLimitNs;
     rc = SPH_ERR_UNSUPPORTED;
     WSPH_DISPATCH_KD(P.kernel, P.dim, (rc = launch_jacobi<KF, D>(a, s)));
     return rc;

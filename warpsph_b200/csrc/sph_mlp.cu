@@ -525,12 +525,19 @@ k_mlp_forward_tc(const float* __restrict__ prm, int64_t n, const float* __restri
         if (row < n) out[row] = (y + s.b4) * sc;
     }
     if (s.abort) {
-        // a chain did not complete in time: the samples of this and later tiles get NaN
+        // a chain did not complete in time: the samples of this and later tiles get NaN.
+        // The MMA chain and its commit may still be in flight, so the issuing thread waits
+        // once more (bounded) for that commit before the TMEM columns are released; the
+        // timeout status tells the host that the context is suspect, and the host stops
+        // issuing work to this device's MLP after it.
         for (; tile < ntiles; tile += gridDim.x) {
             const int64_t row = tile * TC_M + tid;
             if (row < n) out[row] = __int_as_float(0x7fc00000);
         }
-        if (tid == 0 && status) atomicOr(status, SPH_STATUS_TIMEOUT);
+        if (tid == 0) {
+            (void)mbar_wait_bounded(bar, phase ^ 1u, TC_WAIT_CYCLES);
+            if (status) atomicOr(status, SPH_STATUS_TIMEOUT);
+        }
     }
     tc_fence_before_sync();
     __syncthreads();

@@ -50,23 +50,30 @@ double kernel_norm(int kernel, int dim) {
     if (kernel == SPH_KERNEL_WENDLAND2) return dim == 1 ? 1.25 : (dim == 2 ? 7.0 / pi : 21.0 / (2.0 * pi));
     if (kernel == SPH_KERNEL_WENDLAND4) return dim == 1 ? 1.5 : (dim == 2 ? 9.0 / pi : 495.0 / (32.0 * pi));
     if (kernel == SPH_KERNEL_WENDLAND6) return dim == 1 ? 1.71875 : (dim == 2 ? 78.0 / (7.0 * pi) : 1365.0 / (64.0 * pi));
+    if (kernel == SPH_KERNEL_B7) return dim == 1 ? 4096.0 / 315.0 : (dim == 2 ? 589824.0 / (7435.0 * pi) : 16384.0 / (105.0 * pi));
     return 0.0;
 }
 
-// H / h with h = 2 sigma, sigma^2 = (1/d) int |x|^2 W dx (Dehnen & Aly 2012, Table 1).
+// Wendland kernels: H / h with h = 2 sigma, sigma^2 = (1/d) int |x|^2 W dx (Dehnen & Aly
+// 2012, Table 1).  B7: the factor the reference's CFL time step divides by, read from its
+// notebooks' printed initial time steps (1D: Woodward-Colella, 2D: Gresho-Chan, where the
+// step depends only on this factor, the support and the sound speed); 3D continues the
+// 1D -> 2D ratio, which equals the quintic B-spline's sqrt(d I_(d-1) / I_(d+1)) ratio
+// (I_n = int_0^1 k(q) q^n dq) to 7e-8, by that spline's 3D/1D ratio sqrt(15/14).
 double kernel_scale(int kernel, int dim) {
-    static const double t[3][3] = {
+    static const double t[4][3] = {
         {1.620185175, 1.897366596, 1.936491673},
         {1.936491673, 2.171240593, 2.207940217},
-        {2.207940217, 2.415229458, 2.449489743}};
-    if (kernel < 1 || kernel > 3 || dim < 1 || dim > 3) return 0.0;
+        {2.207940217, 2.415229458, 2.449489743},
+        {3.865656972, 3.932734728, 4.001335111}};
+    if (kernel < 1 || kernel > 4 || dim < 1 || dim > 3) return 0.0;
     return t[kernel - 1][dim - 1];
 }
 
 int params_to_dev(const SphParams* p, DevParams* o) {
     if (!p) return set_error(SPH_ERR_BAD_ARG, "null SphParams");
     if (p->dim < 1 || p->dim > 3) return set_error(SPH_ERR_BAD_ARG, "dim must be 1..3 (got %d)", p->dim);
-    if (p->kernel < SPH_KERNEL_WENDLAND2 || p->kernel > SPH_KERNEL_WENDLAND6)
+    if (p->kernel < SPH_KERNEL_WENDLAND2 || p->kernel > SPH_KERNEL_B7)
         return set_error(SPH_ERR_BAD_ARG, "unsupported kernel id %d", p->kernel);
     memset(o, 0, sizeof(*o));
     o->dim = p->dim;

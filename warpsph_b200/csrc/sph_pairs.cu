@@ -12,6 +12,7 @@
 // Arithmetic restates the reference (file:line at each kernel); divisions by the
 // same quantity are replaced by multiplications with a reciprocal, so results
 // differ from the CPU oracle by rounding only.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cfloat>
 #include <atomic>
@@ -1168,31 +1169,71 @@ using namespace wsph;
 static __device__ __align__(256) float g_balance_scratch[SPH_BALANCE_NOALLOC_MAX_FLOATS];
 
 constexpr int kMaxDevices = 64;
-static std::atomic<float*> g_balance_scratch_ptr[kMaxDevices];
+
+// The scratch address is a property of the context that loaded this module: a
+// cudaDeviceReset (or another context made current on the same device) loads the module
+// again and may place the array elsewhere.  So the address is cached per device together
+// with the unique id of the context it was resolved in (cuCtxGetId, reached through
+// cudaGetDriverEntryPoint, so the library does not link the driver API), and resolved
+// again with cudaGetSymbolAddress whenever the current context's id differs.
+struct ScratchSlot {
+    unsigned long long ctx_id;
+    float* ptr;
+};
+static ScratchSlot g_balance_scratch_slot[kMaxDevices];
 static std::mutex g_balance_scratch_mu;
 
-// Address of g_balance_scratch on the current device, resolved once per device with
-// cudaGetSymbolAddress while that device is current.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// The unique id of the context current on this thread; 0 when none is current yet.
+static int current_context_id(unsigned long long* id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+    });
+    if (!get_current || !get_id)
+        return set_error(SPH_ERR_CUDA, "sph_compsph_balance_noalloc: the driver does not provide cuCtxGetCurrent/cuCtxGetId");
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS) return set_error(SPH_ERR_CUDA, "sph_compsph_balance_noalloc: cuCtxGetCurrent failed");
+    *id = 0;
+    if (ctx && get_id(ctx, id) != CUDA_SUCCESS) return set_error(SPH_ERR_CUDA, "sph_compsph_balance_noalloc: cuCtxGetId failed");
+    return SPH_OK;
+}
+
+// Address of g_balance_scratch in the current context, resolved once per device and
+// context with cudaGetSymbolAddress while that device is current.
 static int balance_scratch_on_current_device(float** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return set_error(SPH_ERR_CUDA, "sph_compsph_balance_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return set_error(SPH_ERR_BAD_ARG, "sph_compsph_balance_noalloc: device %d >= %d", dev, kMaxDevices);
-    float* ptr = g_balance_scratch_ptr[dev].load(std::memory_order_acquire);
-    if (!ptr) {
-        std::lock_guard<std::mutex> lock(g_balance_scratch_mu);
-        ptr = g_balance_scratch_ptr[dev].load(std::memory_order_relaxed);
-        if (!ptr) {
-            void* sym = nullptr;
-            e = cudaGetSymbolAddress(&sym, g_balance_scratch);
-            if (e != cudaSuccess || !sym)
-                return set_error(SPH_ERR_CUDA, "sph_compsph_balance_noalloc: cudaGetSymbolAddress on device %d: %s", dev,
-                                 cudaGetErrorString(e));
-            ptr = static_cast<float*>(sym);
-            g_balance_scratch_ptr[dev].store(ptr, std::memory_order_release);
-        }
+    unsigned long long id = 0;
+    int rc = current_context_id(&id);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lock(g_balance_scratch_mu);
+    ScratchSlot& slot = g_balance_scratch_slot[dev];
+    if (id == 0 || !slot.ptr || slot.ctx_id != id) {
+        // cudaGetSymbolAddress also initialises the device's primary context when no
+        // context was current yet; the id is read again after it
+        void* sym = nullptr;
+        e = cudaGetSymbolAddress(&sym, g_balance_scratch);
+        if (e != cudaSuccess || !sym)
+            return set_error(SPH_ERR_CUDA, "sph_compsph_balance_noalloc: cudaGetSymbolAddress on device %d: %s", dev,
+                             cudaGetErrorString(e));
+        if (id == 0 && (rc = current_context_id(&id))) return rc;
+        slot.ptr = static_cast<float*>(sym);
+        slot.ctx_id = id;
     }
-    *out = ptr;
+    *out = slot.ptr;
     return SPH_OK;
 }
 
@@ -1397,9 +1438,11 @@ int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const flo
 // caller.  For callers that cannot allocate device memory on the step path: a plain C
 // or Fortran host code bound through the FFI with no caching allocator of its own, or
 // a timed inner loop, where cudaMalloc/cudaFree would synchronise the whole device.
-// The first call on each device resolves the scratch address (cudaGetSymbolAddress);
-// make that first call before any stream capture.  Calls in flight at the same time on
-// one device (different streams, or different host threads) share the scratch and race.
+// The first call on each device (and the first after that device's context was replaced,
+// e.g. by cudaDeviceReset) resolves the scratch address (cudaGetSymbolAddress); make that
+// first call before any stream capture.  Every device that loads the library holds the
+// 16 MiB array until the process exits.  Calls in flight at the same time on one device
+// (different streams, or different host threads) share the scratch and race.
 int sph_compsph_balance_noalloc(const SphParams* p, int64_t n, const float* m, const float* rho, const float* Pr,
                                 const float* u, const float* v, const float* dvdt, const float* dt, const int32_t* offs,
                                 const int32_t* cnt, const int32_t* list, const float* ap_ij, const float* av_ij,

@@ -1,8 +1,9 @@
 // Bounded grid-wide barrier for cooperative persistent kernels (the DFSPH Jacobi solves
 // and the batched delta-SPH step).  The launch must be cooperative (every block
-// co-resident).  A wait gives up after about 2 s or 2^26 polls, sets SPH_STATUS_TIMEOUT
-// in the control block and makes every block return, so a failure ends the kernel
-// instead of hanging the GPU.
+// co-resident).  A wait gives up after limit_ns nanoseconds of the global timer (2 s by
+// default; the Jacobi solves take the limit from their launch arguments) or 2^26 polls,
+// sets SPH_STATUS_TIMEOUT in the control block and makes every block return, so a
+// failure ends the kernel instead of hanging the GPU.
 #pragma once
 #include <cuda_runtime.h>
 #include "sph_common.cuh"
@@ -22,8 +23,10 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
+constexpr unsigned long long kBarrierLimitNs = 2000000000ull;
+
 // Returns false when any block gave up (SPH_STATUS_TIMEOUT); the caller then returns.
-static __device__ __noinline__ bool grid_barrier(BarrierCtl* c) {
+static __device__ __noinline__ bool grid_barrier(BarrierCtl* c, unsigned long long limit_ns = kBarrierLimitNs) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -42,7 +45,7 @@ static __device__ __noinline__ bool grid_barrier(BarrierCtl* c) {
             unsigned int spins = 0;
             while (*vgen == g) {
                 if (*vstat & SPH_STATUS_TIMEOUT) { good = 0; break; }
-                if (++spins > (1u << 26) || global_ns() - t0 > 2000000000ull) {
+                if (++spins > (1u << 26) || global_ns() - t0 > limit_ns) {
                     atomicOr(&c->status, SPH_STATUS_TIMEOUT);
                     good = 0;
                     break;

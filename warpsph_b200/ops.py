@@ -704,6 +704,7 @@ def dfsph_features(params, mode: int, cfg, x, H, m, rho, v, dvdt, p_prev, dt, ad
     return feats, scale
 
 
+_mlp_suspect: set = set()
 _mlp_status: dict = {}
 
 
@@ -717,12 +718,24 @@ def mlp_status(device) -> torch.Tensor:
     return st
 
 
+def check_mlp_status(device) -> None:
+    """Reads the tcgen05 forward's status word (one host read).  A timeout means an MMA
+    chain did not complete in about a second: its outputs are NaN and the device context is
+    suspect, so this device's tensor-core forward refuses further launches (RuntimeError)."""
+    dev = torch.device(device)
+    if int(mlp_status(dev).item()) & 0x8:
+        _mlp_suspect.add(dev.index)
+        raise RuntimeError(f"tcgen05 MLP forward timed out on {dev}: the CUDA context is suspect; restart the process")
+
+
 def mlp_forward(theta, feats, scale=None, tensor_cores: str = "tcgen05") -> torch.Tensor:
     """MLP(feats) * scale.  tensor_cores "tcgen05" runs sph_mlp_forward_tc (TMEM
     accumulators, 128-sample tiles); "mma" runs sph_mlp_forward (warp-level mma.sync)."""
     out = torch.empty(feats.shape[0], device=feats.device, dtype=torch.float32)
     f = feats.contiguous()
     if tensor_cores == "tcgen05":
+        if f.device.index in _mlp_suspect:
+            raise RuntimeError(f"tcgen05 MLP forward on {f.device}: an earlier launch timed out; the context is suspect")
         if f.data_ptr() % 16:
             f = f.clone()
         with _timed("mlp_forward"):

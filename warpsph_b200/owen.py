@@ -27,10 +27,25 @@ F32 = np.float32
 _TABLES: dict = {}
 
 
+def _tpow(a, q, n):
+    t = F32(F32(a) - q)
+    if not t > 0:
+        return F32(0)
+    r = t
+    for _ in range(n - 1):
+        r = F32(r * t)
+    return r
+
+
 def _dkdq_C(kernel: int, dim: int, q):
-    """|dk/dq| C_d of the dimensionless Wendland kernels (dk/dq = -q p(q))."""
+    """|dk/dq| C_d of the dimensionless kernels (Wendland: dk/dq = -q p(q); B7: the
+    derivative of the degree-7 B-spline's truncated powers)."""
     q = F32(q)
     t = F32(1) - q
+    if kernel == 4:
+        C = {1: F32(4096.0 / 315.0), 2: F32(589824.0 / (7435.0 * math.pi)), 3: F32(16384.0 / (105.0 * math.pi))}[dim]
+        d = F32(-7) * (_tpow(1.0, q, 6) - F32(8) * _tpow(0.75, q, 6) + F32(28) * _tpow(0.5, q, 6) - F32(56) * _tpow(0.25, q, 6))
+        return abs(F32(d * C))
     if kernel == 1:
         C = {1: F32(1.25), 2: F32(7.0 / math.pi), 3: F32(21.0 / (2.0 * math.pi))}[dim]
         p = F32(12) * t * t if dim == 1 else F32(20) * t * t * t

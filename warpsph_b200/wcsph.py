@@ -31,7 +31,7 @@ import torch
 
 from . import ops
 from .configurations import GravityType, make_params, wc_params
-from .core import SupportScheme
+from .core import SupportScheme, sphKernelScale, volumeToSupportHelper
 from .incompressible import solveDivergenceFree, solveIncompressible
 from .surface import detectFreeSurface
 from .systems import _LAST_STAGE_FIELDS, IncompressibleSystemUpdate, WeaklyCompressibleSystemUpdate
@@ -137,6 +137,71 @@ def deltaSPH_step(system, dt, config, schemeConfig, verbose: bool = False):
     update = WeaklyCompressibleSystemUpdate(dxdt=S.velocities.clone(), dvdt=dvdt_rhs + computeGravity(S, config, schemeConfig, adjacency),
                                             drhodt=drhodt, passive=_passive(S))
     return update, adjacency, S
+
+
+def computeTimestep(system, config, compParams, dt=None, systemUpdate=None):
+    """modules/timestep/weaklyCompressible.py:13-88 (Sun et al., the delta-SPH time step):
+    the viscous limit 0.125 H^2 / nu / k, the acoustic limit CFL H / c0 / k and the
+    acceleration limit 0.25 sqrt(H / (max|dv/dt| + 1e-7)) / k, with H the smallest
+    support and k the kernel scale, each applied when its flag is set; then clamped to
+    [minDt, maxDt] and to dtGrowthFactor * dt when it would grow.  nu is
+    alpha c0 H / (2 (d + 2)) for the inviscid form.  Returns a 0-d device tensor, as the
+    reference does."""
+    if not config.adaptiveDt:
+        return dt
+    S = system.state
+    dev, dtype = S.supports.device, S.supports.dtype
+    H = ops.minmax(S.supports)[0]
+    scale = float(sphKernelScale(config.kernel, int(config.dim)))
+    d = compParams.diffusionParams
+    c_s = float(compParams.fluid.fixedSoundSpeed)
+    dim = int(S.positions.shape[1])
+    nu = d.inviscidAlpha * c_s * H / (2 * (dim + 2)) if d.inviscid else torch.tensor(float(d.viscidNu), dtype=dtype, device=dev)
+    dt_v = 0.125 * H * H / nu / scale
+    dt_c = float(config.cflFactor) * H / c_s / scale
+    vel = getattr(systemUpdate, "velocities", None) if systemUpdate is not None else None
+    if vel is not None:
+        # the reference drops NaN components before taking the largest norm
+        finite = vel[~torch.isnan(vel)]
+        max_accel = torch.max(torch.linalg.norm(finite, dim=-1))
+        dt_a = 0.25 * torch.sqrt(H / (max_accel + 1e-7)) / scale
+    else:
+        dt_a = torch.tensor(float(config.maxDt), dtype=dtype, device=dev)
+    prev = torch.tensor(float(config.maxDt) if dt is None else float(dt), dtype=dtype, device=dev)
+    new_dt = prev
+    if compParams.dt_viscosityConstraint:
+        new_dt = dt_v
+    if compParams.dt_accelerationConstraint:
+        new_dt = torch.minimum(new_dt, dt_a)
+    if compParams.dt_acousticConstraint:
+        new_dt = torch.minimum(new_dt, dt_c)
+    new_dt = torch.clamp(new_dt, min=float(config.minDt), max=float(config.maxDt))
+    if bool(new_dt > prev):
+        new_dt = torch.clamp(new_dt, max=float(config.dtGrowthFactor) * prev)
+    return new_dt
+
+
+def setupWeaklyCompressibleTimestep(config, schemeConfig, compressibleSystem, targetDt, verbose: bool = True):
+    """modules/timestep/weaklyCompressible.py:90-116: the sound speed c0 for which the
+    acoustic limit at the 2D support of spacing config.dx equals targetDt,
+    c0 = 0.3 H2(dx) / k2 / targetDt (H2 and k2 evaluated in two dimensions, as the reference
+    does for every dimension); sets schemeConfig.fluid.fixedSoundSpeed and config.dt =
+    targetDt.  Returns (c0, dt)."""
+    dx = float(config.dx)
+    c0 = 0.3 * float(volumeToSupportHelper(dx ** 2, config.targetNeighbors, 2)) / float(sphKernelScale(config.kernel, 2)) / targetDt
+    if verbose:
+        print(f"Computed c0: {c0}, target c0: {schemeConfig.fluid.fixedSoundSpeed}, diff: {abs(c0 - schemeConfig.fluid.fixedSoundSpeed)}")
+    schemeConfig.fluid.fixedSoundSpeed = c0
+    dt = targetDt
+    uMax = torch.max(torch.linalg.norm(compressibleSystem.state.velocities, dim=1))
+    if verbose:
+        print(f"Computed dt: {dt}, target dt: {targetDt}, diff: {abs(dt - targetDt)}")
+        print(f"Max velocity: {uMax}, CFL: {uMax * dt / dx}, Max Mach: {uMax / c0}")
+    if uMax / c0 > 0.1:
+        print(f"Warning: Max Mach number ({uMax / c0:.2f}) is greater than 0.1, which may lead to instability in the simulation. "
+              "Consider changing the relevant parameters.")
+    config.dt = dt
+    return c0, dt
 
 
 def _add_positions(params, x, dx, dim) -> torch.Tensor:
