@@ -18,5 +18,6 @@ from .systems import CompressibleState, CompressibleSystem, CompressibleSystemUp
 from .integrators import IntegrationResult, getIntegrator
 from .schemes import buildScheme, computeCRKFactors, computeTimestep, crkSPH_step, evaluateOptimalSupport, idealGasEOS
 from .cases import buildPointCloud, buildSedov, buildSod1D, sodInitialState
+from .io import exportSimulationSystem, importConfigs, importSimulationSystem, prepExport
 
 __version__ = "0.1.0"
