@@ -461,6 +461,40 @@ int sph_compsph_balance_noalloc(const SphParams* p, int64_t n, const float* m, c
                                 const int32_t* list, const float* ap_ij, const float* av_ij,
                                 float* f_ij_out, void* stream);
 
+/* ---------------------------------------------------------------- mDBC wall particles */
+/* Particle kinds: 0 fluid, 1 wall (boundary), 2 ghost point of a wall particle (the
+ * reference's kinds, initializers/weaklyCompressible.py:145 and
+ * rigidBody/ghostParticles.py:71).  ghost_indices: a wall particle's ghost and a ghost's
+ * wall particle (-1 for fluid); ghost_offsets [n, dim]: x_wall - x_ghost for a wall
+ * particle, its negative for the ghost. */
+
+/* computeMdbcDensity (modules/mdbc/density2025.py:20-85) with interpolateLiuLiu
+ * (modules/liu/interp.py:9-37) and the moment sums of computeLiuMatrices_Func_i
+ * (modules/liu/wp_mat.py:9-135): rho_out = rho, except for each wall particle, whose
+ * density comes from the Liu-Liu interpolation of the fluid densities at its ghost point
+ * (scatter support H_j; the FP64 pseudo-inverse of the (dim+1)^2 moment matrix when more
+ * than 4 fluid neighbours lie inside their supports), projected back to the wall by the
+ * first-order term (more than 9 neighbours) or else the hydrostatic Shepard estimate
+ * max(rho0, rho0 + (c_s^2 (rho_sh - rho0) + rho0 (n.g)(r.n)) / c_s^2).  The rows are Verlet
+ * rows of a list built over every particle, ghosts included.  gravity [3] (nullable = none)
+ * is the acceleration vector.  ghost_neighbors_out [n] (nullable) gets the ghosts'
+ * neighbour counts.  rho_out may alias rho. */
+int sph_mdbc_density(const SphParams* p, int64_t n, const float* x, const float* H, const float* m,
+                     const float* rho, const int32_t* kinds, const int32_t* ghost_indices,
+                     const float* ghost_offsets, const int32_t* offs, const int32_t* cnt,
+                     const int32_t* list, double rest_density, double sound_speed,
+                     const double* gravity, float* rho_out, int32_t* ghost_neighbors_out,
+                     void* stream);
+
+/* computeMdbcNoPenShift (modules/mdbc/wp_nopenshift.py:187-307, :400-420, :493-511): for
+ * each fluid particle the wall neighbours under the gather support, the wall normal from
+ * the wall particle's ghost offset, and per axis the no-penetration terms of the pairs
+ * that qualify, averaged over their count; shift_out [n, dim] (zero for non-fluid). */
+int sph_mdbc_nopen_shift(const SphParams* p, int64_t n, const float* x, const float* H,
+                         const float* m, const float* v, const int32_t* kinds,
+                         const float* ghost_offsets, const int32_t* offs, const int32_t* cnt,
+                         const int32_t* list, float* shift_out, void* stream);
+
 /* ---------------------------------------------------------------- (c) incompressible (DFSPH) */
 /* Relaxed Jacobi solver settings (configurations/moduleConfigurations/solver.py:8-28
  * RelaxedJacobiSolverConfig) plus the rest density (fluidProperties.restDensity). */

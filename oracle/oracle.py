@@ -111,6 +111,8 @@ class Oracle:
                                           rpn, rpn, rpn, rpn]
         L.oracle_jacobi_solve.argtypes = [P, C.c_int, P, i64, rp, rp, rp, rp, rp, rpn, rp, real_c, _i32p, _i32p, _i32p, rp, rp,
                                           _f64p, C.POINTER(C.c_int)]
+        L.oracle_liu_moments.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, _i32p, rp, rp, _i32p]
+        L.oracle_mdbc_nopen_shift.argtypes = [P, i64, rp, rp, rp, rp, _i32p, rp, _i32p, _i32p, _i32p, rp]
 
     # ------------------------------------------------------------------ helpers
     def arr(self, a) -> np.ndarray:
@@ -360,6 +362,56 @@ class Oracle:
         out = np.zeros(len(H), self.dtype)
         self.lib.oracle_surface_dilate(self._p(params), len(H), self.arr(x), self.arr(H), self.arr(fs),
                                        nb["offsets"], nb["counts"], nb["list"], out)
+        return out
+
+    # ------------------------------------------------------------------ mDBC
+    def liu_moments(self, params, x, H, m, rho, kinds, nb):
+        """(b [n, D+1], A [n, D+1, D+1], neighbour counts [n]) at the ghost rows."""
+        n, D = len(H), int(params.dim)
+        b = np.zeros((n, D + 1), self.dtype)
+        A = np.zeros((n, D + 1, D + 1), self.dtype)
+        nbrs = np.zeros(n, np.int32)
+        self.lib.oracle_liu_moments(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho),
+                                    np.ascontiguousarray(kinds, np.int32), nb["offsets"], nb["counts"], nb["list"], b, A, nbrs)
+        return b, A, nbrs
+
+    def mdbc_density(self, params, x, H, m, rho, kinds, ghost_indices, ghost_offsets, nb, rho0, c_s, g):
+        """modules/mdbc/density2025.py:20-85 with the Liu-Liu interpolation of liu/interp.py:
+        the moments from the C restatement, the pseudo-inverse by LAPACK's SVD (numpy, the
+        rtol torch.linalg.pinv uses for float32) and the density formula in numpy."""
+        D = int(params.dim)
+        b, A, nbrs = self.liu_moments(params, x, H, m, rho, kinds, nb)
+        ghost = np.nonzero(np.asarray(kinds) == 2)[0]
+        f = self.dtype
+        out = np.array(rho, f, copy=True)
+        # the pseudo-inverse and product at the oracle's precision (the reference's torch
+        # pinv runs at the moments' float32)
+        bg, Ag, ng = b[ghost], A[ghost], nbrs[ghost]
+        res = np.zeros_like(bg)
+        for k in range(len(ghost)):
+            if ng[k] > 4:
+                res[k] = (np.linalg.pinv(Ag[k], rcond=(D + 1) * np.finfo(np.float32).eps) @ bg[k]).astype(f)
+        res = res.astype(f)
+        rho0, cs2 = f(rho0), f(c_s * c_s)
+        shep = np.where(Ag[:, 0, 0] > 0, (bg[:, 0] / np.where(Ag[:, 0, 0] > 0, Ag[:, 0, 0], 1)).astype(f), rho0).astype(f)
+        rho_g = np.where(ng > 1, shep, rho0).astype(f)
+        P_g = (cs2 * (rho_g - rho0)).astype(f)
+        rel = (-np.asarray(ghost_offsets, f)[ghost]).astype(f)
+        nrm = (rel / np.maximum(np.linalg.norm(rel, axis=1, keepdims=True), 1e-12)).astype(f)
+        gv = np.asarray(g, f)[:D]
+        dot = (nrm * gv).sum(1).astype(f)
+        dot2 = (rel * nrm).sum(1).astype(f)
+        rho_b = np.maximum((rho0 + (P_g + rho0 * (dot * dot2)) / cs2).astype(f), rho0)
+        rho_proj = (res[:, 0] - (rel * res[:, 1:]).sum(1)).astype(f)
+        out[np.asarray(ghost_indices)[ghost]] = np.where(ng > 9, rho_proj, rho_b)
+        return out, nbrs
+
+    def mdbc_nopen_shift(self, params, x, H, m, v, kinds, ghost_offsets, nb):
+        n, D = len(H), int(params.dim)
+        out = np.zeros((n, D), self.dtype)
+        self.lib.oracle_mdbc_nopen_shift(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(v),
+                                         np.ascontiguousarray(kinds, np.int32), self.arr(ghost_offsets), nb["offsets"], nb["counts"],
+                                         nb["list"], out)
         return out
 
     def switch_hopkins_terms(self, params, x, H, m, rho, v, alpha0, nb):

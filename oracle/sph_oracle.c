@@ -1761,3 +1761,92 @@ int64_t oracle_params_layout(int which) {
         default: return -1;
     }
 }
+
+/* ------------------------------------------------------------------ mDBC (wall particles)
+ * Liu-Liu moments at the ghost points, modules/liu/wp_mat.py:9-135 (computeLiuMatrices_Func_i)
+ * under the scatter support H_j and the FluidToGhost direction (fluid neighbours only):
+ *   b = sum_j V_j rho_j [W, grad W],  A = sum_j V_j [[W, -x_gj W], [grad W, -x_gj (x) grad W]],
+ * nbrs = #{j : r < H_j}.  Rows of particles that are not ghosts (kind != 2) are zero.  The
+ * pseudo-inverse and the density formula of density2025.py are in oracle.py. */
+int oracle_liu_moments(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                       const int32_t* kinds, const int32_t* offs, const int32_t* cnt, const int32_t* list, real* b_out,
+                       real* A_out, int32_t* nbrs_out) {
+    OP o = op_from(p);
+    int D = o.dim, E = D + 1;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real b[4] = {0, 0, 0, 0}, A[4][4];
+        for (int a = 0; a < 4; ++a)
+            for (int c = 0; c < 4; ++c) A[a][c] = 0;
+        int nb = 0;
+        if (kinds[i] == 2) {
+            for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+                int32_t j = list[k];
+                if (kinds[j] != 0) continue;
+                real d[3], W, gw[3];
+                dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+                real r = rsqrt_safe(dotD(d, d, D));
+                kWG(&o, d, r, H[j], &W, gw);
+                real Vj = m[j] / rho[j];
+                real VQ = Vj * rho[j];
+                b[0] += VQ * W;
+                A[0][0] += Vj * W;
+                for (int a = 0; a < D; ++a) {
+                    b[a + 1] += VQ * gw[a];
+                    A[a + 1][0] += Vj * gw[a];
+                    A[0][a + 1] += -Vj * d[a] * W;
+                    for (int c = 0; c < D; ++c) A[a + 1][c + 1] += -Vj * d[a] * gw[c];
+                }
+                if (r < H[j]) ++nb;
+            }
+        }
+        for (int a = 0; a < E; ++a) {
+            b_out[i * E + a] = b[a];
+            for (int c = 0; c < E; ++c) A_out[(i * E + a) * E + c] = A[a][c];
+        }
+        nbrs_out[i] = nb;
+    }
+    return 0;
+}
+
+/* No-penetration shift, modules/mdbc/wp_nopenshift.py:187-307 (computeMdbcNoPenShift_Func_i)
+ * and its kernel's per-axis average (:400-420): fluid query particles, wall neighbours
+ * (BoundaryToFluid), gather support.  Rows that are not fluid are zero. */
+int oracle_mdbc_nopen_shift(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* v,
+                            const int32_t* kinds, const real* ghost_off, const int32_t* offs, const int32_t* cnt,
+                            const int32_t* list, real* out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real acc[3] = {0, 0, 0}, ctr[3] = {0, 0, 0};
+        if (kinds[i] == 0) {
+            real dp = POW(m[i], (real)1 / (real)D);
+            for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+                int32_t j = list[k];
+                if (kinds[j] != 1) continue;
+                real d[3];
+                dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+                real r = rsqrt_safe(dotD(d, d, D));
+                if (!(kW(&o, r, H[i]) > 0)) continue;
+                real on = 0, nj[3], normDist = 0;
+                for (int a = 0; a < D; ++a) on += ghost_off[(int64_t)j * D + a] * ghost_off[(int64_t)j * D + a];
+                real norm_j = rsqrt_safe(on) + (real)1e-12;
+                for (int a = 0; a < D; ++a) { nj[a] = -ghost_off[(int64_t)j * D + a] / norm_j; normDist += d[a] * nj[a]; }
+                int cab = (r < (real)1.25 * dp) && (FABS(normDist) < (real)0.75 * norm_j && norm_j < (real)1.75 * dp);
+                for (int a = 0; a < D; ++a) {
+                    real dv = v[i * D + a] - v[(int64_t)j * D + a], nrm = nj[a], dr = d[a];
+                    int mask = cab && (dr * nrm < (real)0.75) && (FABS(nrm) > (real)0.001 * dp);
+                    real vfc = dv * nrm;
+                    real ratio = FABS(dr / nrm);
+                    ratio = ratio < (real)0.25 ? (real)0.25 : (ratio > 1 ? 1 : ratio);
+                    real factor = (real)-4 * ratio + 3;
+                    real term = -factor * dv * nrm * nrm;
+                    if (mask && vfc < 0) { acc[a] += term; ctr[a] += 1; }
+                }
+            }
+        }
+        for (int a = 0; a < D; ++a) out[i * D + a] = acc[a] / (ctr[a] + (real)1e-12);
+    }
+    return 0;
+}

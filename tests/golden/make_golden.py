@@ -57,6 +57,7 @@ wp = types.SimpleNamespace(
     min=lambda a, b: a if a < b else b, max=lambda a, b: a if a > b else b,
     abs=lambda x: abs(x), exp=lambda x: F(np.exp(F(x))), pow=lambda a, b: F(np.power(F(a), F(b))),
     sqrt=lambda x: F(np.sqrt(F(x))),
+    clamp=lambda x, lo, hi: (lo if x < lo else (hi if x > hi else x)),
     outer=lambda a, b: np.outer(np.asarray(a, F), np.asarray(b, F)).astype(F),
     int32=int, int64=int, bool=bool, float32=F, array=lambda *a, **k: None, tid=lambda: 0,
 )
@@ -67,6 +68,8 @@ vector = matrix = lambda *a, **k: None
 class OperationDirection(Enum):
     TrueAllToToAll = 0
     AllToAll = 1
+    FluidToGhost = 2
+    BoundaryToFluid = 3
 
 
 KSCALE = {(1, 1): 1.620185175, (1, 2): 1.897366596, (1, 3): 1.936491673,
@@ -1203,10 +1206,115 @@ def run_reference_deltasph(ref: Path, case: dict) -> dict:
     return out
 
 
+# ---------------------------------------------------------------- mDBC (wall particles)
+def make_mdbc_case(seed=11):
+    """A 2D fluid block resting on a wall of three particle layers, with one ghost point per
+    wall particle mirrored across the wall surface y = 0 (the layout addBoundaryGhostParticles
+    builds, rigidBody/ghostParticles.py:6-79: fluid, wall, ghosts; a wall particle's ghost
+    offset is x_b - x_g, its ghost's the negative).  The lowest fluid row is pressed against
+    the wall and moves into it, so the no-penetration shift acts; densities are perturbed
+    by a few per cent; gravity points down."""
+    from oracle import oracle
+    from oracle.steps import cell_capacity_for
+    from tests.cases import make_params
+    import warpsph_b200 as ws
+    cfg, sch, p = make_params(2, kernel=ws.KernelFunctions.Wendland4)
+    rng = np.random.default_rng(seed)
+    dx = F(1 / 32)
+    fx, fy = np.meshgrid((np.arange(16) + 0.5) * dx - F(0.25), (np.arange(8) + 0.5) * dx, indexing="xy")
+    fluid = np.stack([fx.ravel(), fy.ravel()], 1) + F(0.15) * dx * (rng.random((128, 2)) - F(0.5))
+    fluid[:16, 1] = F(0.2) * dx
+    bx, by = np.meshgrid((np.arange(20) + 0.5) * dx - F(0.3125), -(np.arange(3) + 0.5) * dx, indexing="xy")
+    wall = np.stack([bx.ravel(), by.ravel()], 1)
+    ghost = wall * np.array([1, -1], F)
+    x = np.concatenate([fluid, wall, ghost]).astype(F)
+    nf, nw = len(fluid), len(wall)
+    n = len(x)
+    kinds = np.concatenate([np.zeros(nf), np.ones(nw), np.full(nw, 2)]).astype(np.int32)
+    gidx = np.full(n, -1, np.int32)
+    gidx[nf:nf + nw] = np.arange(nf + nw, n)
+    gidx[nf + nw:] = np.arange(nf, nf + nw)
+    goff = np.zeros((n, 2), F)
+    goff[nf:nf + nw] = (wall - ghost).astype(F)
+    goff[nf + nw:] = -goff[nf:nf + nw]
+    H = np.full(n, ws.volumeToSupportHelper(float(dx) ** 2, cfg.targetNeighbors, 2), F)
+    m = np.full(n, float(dx) ** 2, F)
+    o = oracle.get("f32")
+    nb = o.neighbors(p, x, H, cell_capacity_for(n, 2))
+    rho = (o.density(p, 0, x, H, m, nb) * (1 + 0.02 * rng.standard_normal(n))).astype(F)
+    v = (0.3 * rng.standard_normal((n, 2))).astype(F)
+    v[:16, 1] = -np.abs(v[:16, 1]) - F(0.1)
+    v[kinds != 0] = 0
+    return dict(params=p, x=x, H=H, m=m, rho=rho, v=v, kinds=kinds, ghost_indices=gidx, ghost_offsets=goff, nb=nb, n=n,
+                rho0=np.array([1.0]), c_s=np.array([10.0]), gravity=np.array([0.0, -9.81]))
+
+
+def run_reference_mdbc(ref: Path, case: dict) -> dict:
+    """Executes the reference's mDBC code unmodified: the Liu-Liu moment body
+    computeLiuMatrices_Func_i (modules/liu/wp_mat.py) for every ghost point, interpolateLiuLiu
+    (modules/liu/interp.py; torch.linalg.pinv) over those moments, computeMdbcDensity
+    (modules/mdbc/density2025.py) on top, and the no-penetration body
+    computeMdbcNoPenShift_Func_i (modules/mdbc/wp_nopenshift.py) for every fluid particle with
+    its kernel's per-axis average (:413-415, restated: a @wp.kernel body)."""
+    p = case["params"]
+    n, nb = case["n"], case["nb"]
+    offs, cnt, lst = nb["offsets"], nb["counts"], nb["list"].astype(np.int64)
+    x, H, m, rho, v, kinds = (case[k] for k in ("x", "H", "m", "rho", "v", "kinds"))
+    goff, gidx = case["ghost_offsets"], case["ghost_indices"]
+    state = SoA(positions=x, supports=H, masses=m, densities=rho, kinds=kinds)
+    dom = SoA(dim=2)
+    ghosts = np.nonzero(kinds == 2)[0]
+    mat = load(ref, "modules/liu/wp_mat.py", dict(checkDirectionality_j=lambda k, mode: k == 0))
+    kp = SoA(operationMode=OperationDirection.FluidToGhost.value, kernelFunction=int(p.kernel), supportMode="scatter")
+    cd = SoA(V=(m / rho).astype(F))
+    shep, bs, As, nbrs = [], [], [], []
+    with np.errstate(all="ignore"):
+        for i in ghosts:
+            r = call(mat["computeLiuMatrices_Func_i"], i=int(i), dim=2, xi=x[i], referenceState=state, correctionData=cd, domainState=dom,
+                     kernelProperties=kp, beginIndex=int(offs[i]), numIndices=int(cnt[i]), offsetArray=lst, referenceKinds=kinds,
+                     useGradientRenormalization=False, Li=None, useGradHTerms=False, omega_i=F(1), useVolume=False, Vi=F(0),
+                     useCRK=False, Ai=F(1), Bi=np.zeros(2, F), gradAi=np.zeros(2, F), gradBi=np.zeros((2, 2), F),
+                     referenceQuantities=rho, vector_out=np.zeros(3, F), matrix_out=np.zeros((3, 3), F), shep_out=F(0))
+            shep.append(F(r[0])); bs.append(np.asarray(r[1], F)); As.append(np.asarray(r[2], F)); nbrs.append(int(r[3]))
+    moments = (torch.tensor(np.array(shep, F)), torch.tensor(np.array(bs, F)), torch.tensor(np.array(As, F)),
+               torch.tensor(np.array(nbrs, np.int32)))
+
+    def computeLiuMatricesWarp(queryPositions, referenceParticles, referenceQuantities, operationProperties, domain, adjacency=None):
+        return moments
+
+    interp = load(ref, "modules/liu/interp.py", dict(computeLiuMatricesWarp=computeLiuMatricesWarp, OperationProperties=lambda **k: SoA(**k),
+                                                    SupportScheme=SoA(Scatter="scatter"), AdjacencyList=type("AdjacencyList", (), {}),
+                                                    SimulationConfig=object))
+    dens = load(ref, "modules/mdbc/density2025.py", dict(interpolateLiuLiu=interp["interpolateLiuLiu"],
+                                                          AdjacencyList=type("AdjacencyList", (), {}), CompactHashMap=object,
+                                                          SimulationConfig=object))
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a))
+    st = SoA(positions=T(x), supports=T(H), masses=T(m), densities=T(rho), velocities=T(v), kinds=T(kinds), ghostIndices=T(gidx),
+             ghostOffsets=T(goff))
+    rho0, c_s = float(case["rho0"][0]), float(case["c_s"][0])
+    sc = SoA(fluid=SoA(restDensity=rho0, fixedSoundSpeed=c_s), gravityConfig=SoA(direction=[0.0, -1.0], magnitude=9.81, active=True))
+    out = {"mdbc_density": dens["computeMdbcDensity"](st, SoA(kernel=None, domain=None), sc, None).numpy().astype(F),
+           "liu_b": np.array(bs, F), "liu_A": np.array(As, F), "liu_nbrs": np.array(nbrs, np.int32)}
+    nps = load(ref, "modules/mdbc/wp_nopenshift.py", dict(checkDirectionality_j=lambda k, mode: k == 1))
+    kpg = SoA(operationMode=OperationDirection.BoundaryToFluid.value, kernelFunction=int(p.kernel), supportMode="gather")
+    shift = np.zeros((n, 2), F)
+    with np.errstate(all="ignore"):
+        for i in np.nonzero(kinds == 0)[0]:
+            o_, c_ = call(nps["computeMdbcNoPenShift_Func_i"], i=int(i), dim=2, xi=x[i], hi=F(H[i]), mi=F(m[i]), rhoi=F(rho[i]),
+                          referenceState=state, domainState=dom, kernelProperties=kpg, beginIndex=int(offs[i]), numIndices=int(cnt[i]),
+                          offsetArray=lst, ki=0, referenceKinds=kinds, useGradientRenormalization=False, Li=None, useGradHTerms=False,
+                          omega_i=F(1), referenceOmegas=None, useVolume=False, Vi=F(0), referenceVolumes=None, useCRK=False, Ai=F(1),
+                          Bi=np.zeros(2, F), gradAi=np.zeros(2, F), gradBi=np.zeros((2, 2), F), vel_i=v[i], referenceVelocities=v,
+                          ghostOffset_i=goff[i], referenceGhostOffsets=goff, outCtr=np.zeros(2, np.int32))
+            shift[i] = [F(o_[d]) / (F(c_[d]) + F(1e-12)) for d in range(2)]
+    out["nopen_shift"] = shift
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the reference checkout (wi-re/warpSPH)")
-    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph", "owen", "hopkins", "deltasph", "surface"], default="all")
+    ap.add_argument("--which", choices=["all", "crk", "dfsph", "compsph", "owen", "hopkins", "deltasph", "surface", "mdbc"], default="all")
     a = ap.parse_args()
     ref = Path(a.reference)
     if a.which in ("all", "crk"):
@@ -1255,6 +1363,16 @@ def main():
                             x=case["x"], H=case["H"], m=case["m"], v=case["v"], rho=case["rho"], gL=case["gL"], P=case["P"],
                             offsets=nb["offsets"], counts=nb["counts"], list=nb["list"], **out)
         print("wrote", Path(__file__).parent / "deltasph_golden.npz", "particles", case["n"], "pairs", len(nb["list"]))
+    if a.which in ("all", "mdbc"):
+        case = make_mdbc_case()
+        out = run_reference_mdbc(ref, case)
+        nb = case["nb"]
+        keep = ("x", "H", "m", "rho", "v", "kinds", "ghost_indices", "ghost_offsets", "rho0", "c_s", "gravity")
+        np.savez_compressed(Path(__file__).parent / "mdbc_golden.npz", **{k: case[k] for k in keep}, offsets=nb["offsets"],
+                            counts=nb["counts"], list=nb["list"], **out)
+        print("wrote", Path(__file__).parent / "mdbc_golden.npz", "particles", case["n"], "pairs", len(nb["list"]),
+              "ghost neighbours", out["liu_nbrs"].min(), out["liu_nbrs"].max(),
+              "shifted", int((np.abs(out["nopen_shift"]).sum(1) > 0).sum()))
     if a.which in ("all", "owen"):
         out = run_reference_owen(ref)
         np.savez_compressed(Path(__file__).parent / "owen_golden.npz", **out)

@@ -139,6 +139,8 @@ _PROTOS = {
     "sph_dfsph_workspace_size": [_I64, _I32],
     "sph_dfsph_features": [_P, _P, _I32, _I64] + [_P] * 12 + [_I64] + [_P] * 3,
     "sph_mlp_param_count": [],
+    "sph_mdbc_density": [_P, _I64] + [_P] * 10 + [C.c_double, C.c_double] + [_P] * 4,
+    "sph_mdbc_nopen_shift": [_P, _I64] + [_P] * 11,
     "sph_deltasph_rhs": [_P, _P, _I64] + [_P] * 13,
     "sph_wc_eos": [_P, _I64, _P, _P, _P],
     "sph_ensemble_neighbors_workspace_size": [_I64, _I64],

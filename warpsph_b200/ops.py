@@ -810,3 +810,36 @@ def wc_eos(wc, rho) -> torch.Tensor:
     check(_capi.lib().sph_wc_eos(C.cast(C.pointer(wc), C.c_void_p), rho.shape[0], fptr(rho), ptr(out), stream_ptr(rho.device)),
           "sph_wc_eos")
     return out
+
+
+# ------------------------------------------------------------------ mDBC wall particles
+def mdbc_density(params, x, H, m, rho, kinds, ghost_indices, ghost_offsets, adj: AdjacencyList, rest_density: float,
+                 sound_speed: float, gravity=None, want_neighbors: bool = False):
+    """computeMdbcDensity on the GPU: the densities with the wall particles' replaced
+    (sph_mdbc_density).  adj is a list over every particle, ghosts included.  Returns the
+    densities, and the ghosts' neighbour counts with want_neighbors."""
+    n = m.shape[0]
+    out = _empty(n, m)
+    nb = torch.zeros(n, dtype=torch.int32, device=m.device) if want_neighbors else None
+    g = None
+    if gravity is not None:
+        gv = [float(a) for a in gravity] + [0.0] * (3 - len(gravity))
+        g = (C.c_double * 3)(*gv[:3])
+    with _timed("mdbc_density"):
+        check(_capi.lib().sph_mdbc_density(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), iptr(kinds.to(torch.int32).contiguous()),
+                                           iptr(ghost_indices.to(torch.int32).contiguous()), fptr(_f32(ghost_offsets)),
+                                           *_csr(adj), float(rest_density), float(sound_speed),
+                                           None if g is None else C.cast(g, C.c_void_p), ptr(out), ptr(nb), stream_ptr(m.device)),
+              "sph_mdbc_density")
+    return (out, nb) if want_neighbors else out
+
+
+def mdbc_nopen_shift(params, x, H, m, v, kinds, ghost_offsets, adj: AdjacencyList) -> torch.Tensor:
+    """computeMdbcNoPenShift on the GPU: the no-penetration shift [n, dim] (zero for non-fluid)."""
+    n, d = m.shape[0], int(params.dim)
+    out = _empty((n, d), m)
+    with _timed("mdbc_nopen_shift"):
+        check(_capi.lib().sph_mdbc_nopen_shift(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(_f32(v)), iptr(kinds.to(torch.int32).contiguous()),
+                                               fptr(_f32(ghost_offsets)), *_csr(adj), ptr(out), stream_ptr(m.device)),
+              "sph_mdbc_nopen_shift")
+    return out
