@@ -289,6 +289,69 @@ class DFSPHOracle(CRKSPHOracle):
         Sf["density_solve_iterations"] = it
 
 
+class DFSPHWallOracle(DFSPHOracle):
+    """dfsph_step with wall particles and their ghost points (schemes/dfsph.py:27-126,
+    170-186) and the incompressible finalize, in the library's arrangement: the first nfw
+    particles (fluid and walls) take part in every pass, the ghosts only in the mDBC wall
+    density (modules/mdbc/density2025.py), whose sums use a list over every particle; wall
+    velocities are zero (mdbc/velocity.py, zeros walls); the no-penetration shift
+    (mdbc/wp_nopenshift.py) enters dv/dt divided by dt; updates and the finalize's position
+    shift are zero for walls and ghosts."""
+
+    def __init__(self, params, wc, df_cfg, rho_cfg, walls: dict, gravity=None, precision: str = "f32"):
+        super().__init__(params, wc, df_cfg, rho_cfg, gravity=gravity, precision=precision)
+        self.w = walls      # kinds, ghost_indices, ghost_offsets, nfw, rho0, c_s
+
+    def rhs(self, st, dt):
+        o, p, w, f = self.o, self.p, self.w, self.dt_
+        st = dict(st)
+        nfw, kinds = w["nfw"], w["kinds"]
+        x, H, m, v = st["positions"], st["supports"], st["masses"], st["velocities"]
+        nb = self.nb(x[:nfw], H[:nfw])
+        nb_all = self.nb(x, H)
+        r = o.density(p, 0, x[:nfw], H[:nfw], m[:nfw], nb)
+        rho_prev = st.get("densities")
+        tail = rho_prev[nfw:] if rho_prev is not None else np.full(len(H) - nfw, w["rho0"], f)
+        rho = np.concatenate([r, tail]).astype(f)
+        g = [0.0] * self.dim if self.g is None else list(self.g)
+        rho, _ = o.mdbc_density(p, x, H, m, rho, kinds, w["ghost_indices"], w["ghost_offsets"], nb_all, w["rho0"], w["c_s"], g)
+        st["densities"] = rho
+        v = np.where((kinds == 1)[:, None], f(0), v).astype(f)
+        st["velocities"] = v
+        xh, Hh, mh, rh, vh = x[:nfw], H[:nfw], m[:nfw], rho[:nfw], v[:nfw]
+        dvdt_diss, drhodt = o.visc_continuity(p, self.wc, xh, Hh, mh, rh, vh, nb)
+        dvdt = self.gravity(nfw)
+        nopen = o.mdbc_nopen_shift(p, xh, Hh, mh, vh, kinds[:nfw], w["ghost_offsets"][:nfw], nb)
+        dvdt = (dvdt + nopen / f(dt)).astype(f)
+        p0 = st.get("pressures")
+        p0 = np.zeros(nfw, f) if p0 is None else p0[:nfw]
+        src = (dvdt + dvdt_diss).astype(f)
+        pr, acc, hist, it = o.jacobi_solve(p, 0, self.df_cfg, xh, Hh, mh, rh, vh, src, p0, dt, nb)
+        n = len(H)
+        pad = lambda a: np.concatenate([a, np.zeros((n - nfw,) + a.shape[1:], f)]).astype(f)
+        st["pressures"] = pad(pr)
+        fluid = kinds[:nfw] == 0
+        upd = dict(dxdt=pad(np.where(fluid[:, None], vh, f(0))), dvdt=pad(np.where(fluid[:, None], (src + acc).astype(f), f(0))),
+                   drhodt=pad(np.where(fluid, drhodt, f(0))))
+        return upd, nb, st, dict(errors=hist[:, 0].copy(), iterations=it)
+
+    def finalize(self, Sf, st0, dt, updates, rvs):
+        o, p, w, f = self.o, self.p, self.w, self.dt_
+        nfw, kinds = w["nfw"], w["kinds"]
+        last = rvs[-1][1]
+        Sf["pressures"] = last["pressures"]
+        x, H, m, v = Sf["positions"], Sf["supports"], Sf["masses"], Sf["velocities"]
+        nb = self.nb(x[:nfw], H[:nfw])
+        rho = o.density(p, 0, x[:nfw], H[:nfw], m[:nfw], nb)
+        Sf["densities"] = np.concatenate([rho, Sf["densities"][nfw:]]).astype(f)
+        zero = np.zeros_like(v[:nfw])
+        pr, acc, hist, it = o.jacobi_solve(p, 1, self.rho_cfg, x[:nfw], H[:nfw], m[:nfw], rho, v[:nfw], zero, Sf["pressures"][:nfw],
+                                           dt, nb)
+        k = np.where((kinds[:nfw] == 0)[:, None], (f(f(dt) * f(dt)) * acc).astype(f), f(0)).astype(f)
+        Sf["positions"] = np.concatenate([self.combine(x[:nfw], [k], [1.0], 1.0, wrap=True), x[nfw:]]).astype(f)
+        Sf["density_solve_iterations"] = it
+
+
 class DeltaSPHOracle(DFSPHOracle):
     """schemes/deltaSPH.py:11-208 for a fluid-only system with the finalize of
     systems/weaklyCompressible.py:73-200: the delta-SPH right-hand side plus gravity; after

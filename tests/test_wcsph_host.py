@@ -1,8 +1,9 @@
 """Host-side logic of the DFSPH and delta-SPH step functions (no GPU): the scheme
 builder entries, configuration round trips, the enum forms the reference passes, gravity,
-and the cases the GPU path refuses (boundary and ghost particles, boundary conditions,
-rigid bodies, surface detection schemes other than the colour field), which raise before
-any device work."""
+the wall-particle layout check and boundary velocities, and the cases the GPU path
+refuses (walls in deltaSPH_step or without ghost points, boundary conditions, rigid
+bodies, surface detection schemes other than the colour field), which raise before any
+device work."""
 import numpy as np
 import pytest
 import torch
@@ -72,8 +73,18 @@ def test_unsupported_inputs_raise(step, cfgcls):
     config = cf.SimulationConfig()
     k = torch.zeros(16, dtype=torch.int32)
     k[3] = 1
-    with pytest.raises(NotImplementedError, match="mDBC"):
+    # a wall particle without a ghost point after the fluid and walls
+    with pytest.raises(NotImplementedError, match="ghost point" if step is dfsph_step else "wall"):
         step(IncompressibleSystem(state=cpu_state(kinds=k)), 1e-3, config, cfgcls())
+    k[14], k[15] = 1, 2
+    k[3] = 0
+    st = cpu_state(kinds=k)
+    if step is dfsph_step:      # walls with ghosts are accepted, but need their ghost fields
+        with pytest.raises(ValueError, match="ghostIndices"):
+            step(IncompressibleSystem(state=st), 1e-3, config, cfgcls())
+    else:
+        with pytest.raises(NotImplementedError, match="dfsph_step only"):
+            step(IncompressibleSystem(state=st), 1e-3, config, cfgcls())
     for attr, val, msg in (("boundaryConditions", [object()], "boundary conditions"), ("rigidBodies", [object()], "rigid bodies")):
         c = cfgcls()
         setattr(c, attr, val)
@@ -109,3 +120,26 @@ def test_gravity_forms():
     c.gravityConfig.type = cf.GravityType.PotentialField
     with pytest.raises(NotImplementedError):
         computeGravity(S, None, c)
+
+
+def test_boundary_velocities_and_wall_layout():
+    from warpsph_b200.wcsph import _wall_layout, computeBoundaryVelocities
+    k = torch.tensor([0, 0, 0, 1, 1, 2, 2], dtype=torch.int32)
+    st = cpu_state(7, kinds=k)
+    st.velocities = torch.ones(7, 2)
+    st.ghostIndices = torch.tensor([-1, -1, -1, 5, 6, 3, 4], dtype=torch.int32)
+    st.ghostOffsets = torch.zeros(7, 2)
+    assert _wall_layout(st, True) == 5 and _wall_layout(cpu_state(7), True) is None
+    v = computeBoundaryVelocities(st, cf.SimulationConfig(), cf.IncompressibleSPHConfig())
+    assert torch.equal(v[3:5], torch.zeros(2, 2)) and torch.equal(v[:3], torch.ones(3, 2)) and torch.equal(v[5:], torch.ones(2, 2))
+    # per-region types: material 0 a zeros wall, material 1 a constant wall
+    import types
+    Z, Cn, B = (types.SimpleNamespace(name=s_) for s_ in ("zeros", "constant", "Boundary"))
+    config = cf.SimulationConfig()
+    config.regions = [types.SimpleNamespace(type=B, kind=Z), types.SimpleNamespace(type=B, kind=Cn)]
+    st.materials = torch.tensor([0, 0, 0, 0, 1, 0, 1], dtype=torch.int32)
+    v = computeBoundaryVelocities(st, config, cf.IncompressibleSPHConfig())
+    assert torch.equal(v[3], torch.zeros(2)) and torch.equal(v[4], torch.ones(2))
+    config.regions[1].kind = types.SimpleNamespace(name="noSlip")
+    with pytest.raises(NotImplementedError, match="noSlip"):
+        computeBoundaryVelocities(st, config, cf.IncompressibleSPHConfig())

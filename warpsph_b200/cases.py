@@ -19,11 +19,12 @@ from __future__ import annotations
 import math
 from typing import NamedTuple
 
+import numpy as np
 import torch
 
 from . import ops
 from .configurations import CompressibleSPHConfig, SimulationConfig, make_params
-from .core import SupportScheme, buildDomainDescription, kernel_constants, volumeToSupportHelper
+from .core import DomainDescription, SupportScheme, buildDomainDescription, kernel_constants, volumeToSupportHelper
 from .enumTypes import AdaptiveSupportScheme
 from .schemes import computeTimestep, evaluateOptimalSupport
 
@@ -187,3 +188,79 @@ def buildSod1D(SimulationSystem, SimulationState, samplingRatio: int, leftState:
     config.dx = float(masses.min())
     config.dt = computeTimestep(system, config, compParams, dt=None)
     return system
+
+
+def tank_particles(dim: int, dx: float, column, tank, layers: int = 3, jitter: float = 0.0, seed: int = 0):
+    """The particles of a dam break in an open-topped box tank (numpy, FP32).
+
+    The tank's interior is [0, tank[a]] along every axis; axis 1 is vertical and the top is
+    open.  The fluid column fills [0, column[a]] in the corner at the origin on the
+    cell-centred lattice of spacing dx (optionally jittered by jitter * dx).  The walls are
+    `layers` lattice layers outside the floor and the side walls, up to the tank's height.
+    Each wall particle has one ghost point, its mirror image through the closest point of
+    the interior box: x_g = 2 c(x_b) - x_b, which for the reference's SDF construction
+    (rigidBody/ghostParticles.py:30-54, offset = (d - min(-d, 1.5 H)) n) is the same point
+    whenever the wall depth is below 1.5 supports.  Returns (fluid [nf, d], walls [nw, d],
+    ghosts [nw, d])."""
+    rng = np.random.default_rng(seed)
+    col = [int(round(c / dx)) for c in column]
+    axes = [(np.arange(c) + 0.5) * dx for c in col]
+    grids = np.meshgrid(*axes, indexing="ij")
+    fluid = np.stack([g.ravel() for g in grids], 1)
+    if jitter > 0:
+        fluid = fluid + jitter * dx * (rng.random(fluid.shape) - 0.5)
+    ncell = [int(round(t / dx)) for t in tank]
+    waxes = []
+    for a in range(dim):
+        hi = ncell[a] if a == 1 else ncell[a] + layers
+        waxes.append((np.arange(-layers, hi) + 0.5) * dx)
+    wg = np.meshgrid(*waxes, indexing="ij")
+    pts = np.stack([g.ravel() for g in wg], 1)
+    lo = np.zeros(dim)
+    hi = np.asarray(tank[:dim], dtype=np.float64)
+    outside = np.any((pts < lo) | (pts > hi), axis=1)
+    walls = pts[outside]
+    closest = np.clip(walls, lo, hi)
+    ghosts = 2 * closest - walls
+    return fluid.astype(np.float32), walls.astype(np.float32), ghosts.astype(np.float32)
+
+
+def buildDamBreak(SimulationSystem, SimulationState, config: SimulationConfig, dx: float, column=(0.5, 1.0, 0.5),
+                  tank=(1.6, 1.2, 0.6), layers: int = 3, rho0: float = 1.0, jitter: float = 0.0, seed: int = 0, device=None,
+                  dtype=torch.float32):
+    """A dam break with mDBC walls in the layout of the reference's
+    initializeSimulation / addBoundaryGhostParticles (initializers/weaklyCompressible.py:230,
+    rigidBody/ghostParticles.py:6-79): fluid (kind 0), then walls (kind 1), then one ghost
+    point per wall particle (kind 2); ghostIndices link a wall particle and its ghost,
+    ghostOffsets hold x_wall - x_ghost for the wall particle and the negative for its ghost.
+    Masses rho0 dx^d, supports from config.targetNeighbors, densities rho0, at rest.  Sets
+    config.domain to a non-periodic box around the tank (open above the tank's top)."""
+    dim = int(config.dim)
+    device = device or config.device
+    fluid, walls, ghosts = tank_particles(dim, dx, column[:dim], tank[:dim], layers, jitter, seed)
+    nf, nw = len(fluid), len(walls)
+    x = np.concatenate([fluid, walls, ghosts])
+    n = len(x)
+    kinds = np.concatenate([np.zeros(nf), np.ones(nw), np.full(nw, 2)]).astype(np.int32)
+    gidx = np.full(n, -1, np.int64)
+    gidx[nf:nf + nw] = np.arange(nf + nw, n)
+    gidx[nf + nw:] = np.arange(nf, nf + nw)
+    goff = np.zeros_like(x)
+    goff[nf:nf + nw] = walls - ghosts
+    goff[nf + nw:] = ghosts - walls
+    pad = (layers + 2) * dx
+    lo = [-pad] * dim
+    hi = [t + pad for t in tank[:dim]]
+    hi[1] = tank[1] + 2.0 * tank[1]          # room for the splash above the open top
+    config.domain = DomainDescription(torch.tensor(lo, device=device, dtype=dtype), torch.tensor(hi, device=device, dtype=dtype),
+                                      torch.zeros(dim, dtype=torch.bool, device=device), dim)
+    H = float(volumeToSupportHelper(dx ** dim, config.targetNeighbors, dim))
+    t = lambda a, dt_=dtype: torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dt_)
+    state = SimulationState(positions=t(x), velocities=torch.zeros((n, dim), device=device, dtype=dtype),
+                            supports=torch.full((n,), H, device=device, dtype=dtype),
+                            masses=torch.full((n,), rho0 * dx ** dim, device=device, dtype=dtype),
+                            densities=torch.full((n,), rho0, device=device, dtype=dtype), kinds=t(kinds, torch.int32),
+                            materials=torch.zeros(n, dtype=torch.int32, device=device),
+                            UIDs=torch.arange(n, dtype=torch.int64, device=device), UIDcounter=n,
+                            ghostIndices=t(gidx, torch.int64), ghostOffsets=t(goff))
+    return SimulationSystem(state=state, adjacency=None, domain=config.domain)

@@ -5,8 +5,10 @@ follows schemes/deltaSPH.py:11-208, call for call, for fluid-only systems:
 
   Verlet list (super-symmetric rows)      dfsph.py:27     -> sph_neighbors_build / refresh
   gather density                          dfsph.py:36-40  -> sph_density_gather
-  mDBC density, boundary velocities,      dfsph.py:48-59, -> identities without boundary particles
-  Dirichlet conditions, forcing, no-pen.  :106-126           (the reference's own early returns)
+  mDBC density, boundary velocities,      dfsph.py:48-59, -> sph_mdbc_density, computeBoundaryVelocities,
+  no-penetration shift                    :120-126           sph_mdbc_nopen_shift (identities without walls,
+                                                             the reference's own early returns)
+  Dirichlet conditions, forcing           :57, :110-113     -> none (no boundary conditions on this path)
   free-surface detection                  dfsph.py:72-77  -> surface.detectFreeSurface (colour-field scheme)
   velocity diffusion + continuity         dfsph.py:100-109 -> sph_wc_visc_continuity (one pass)
   gravity                                 dfsph.py:117-120 -> computeGravity (elementwise)
@@ -19,13 +21,15 @@ follows schemes/deltaSPH.py:11-208, call for call, for fluid-only systems:
                                                                surface indicators enter the
                                                                Antuono pressure term)
 
-Systems with boundary (kind 1) or ghost (kind 2) particles, boundary conditions or rigid
-bodies need the mDBC and boundary-condition passes, which are not on the GPU path; the
-steps raise NotImplementedError for them, as does the surface-aware shift.
+dfsph_step also runs systems with wall particles (kind 1) and their ghost points (kind 2):
+the mDBC wall density (sph_mdbc_density), the wall velocities and the no-penetration
+shift (sph_mdbc_nopen_shift), see _dfsph_step_walls.  Boundary conditions, rigid bodies,
+walls in deltaSPH_step and the surface-aware shift raise NotImplementedError.
 """
 from __future__ import annotations
 
-from typing import Any
+import dataclasses
+from typing import Any, Optional
 
 import torch
 
@@ -37,21 +41,99 @@ from .surface import detectFreeSurface
 from .systems import _LAST_STAGE_FIELDS, IncompressibleSystemUpdate, WeaklyCompressibleSystemUpdate
 
 _KINDS_CHECKED: dict = {}
+# the last list over every particle (ghost points included) per (device, particle count):
+# the prior that the next mDBC density pass's list build validates and keeps or rebuilds
+_GHOST_LISTS: dict = {}
 
 
-def _check_supported(state, schemeConfig) -> None:
+def _wall_layout(state, allow_walls: bool) -> Optional[int]:
+    """None for a fluid-only system.  With wall particles (kind 1) and their ghost points
+    (kind 2): the number of fluid and wall particles, which come first, followed by the
+    ghosts, as addBoundaryGhostParticles lays them out (rigidBody/ghostParticles.py:61-79).
+    One host read each time the kinds tensor changes."""
+    k = state.kinds
+    if k is None:
+        return None
+    key = (id(k), k._version, k.data_ptr(), tuple(k.shape))
+    hit = _KINDS_CHECKED.get(id(k))
+    if hit is not None and hit[0] == key:
+        nfw = hit[1]
+    else:
+        n = int(k.shape[0])
+        nf, nw, ng = (int(c) for c in torch.stack([(k == 0).sum(), (k == 1).sum(), (k == 2).sum()]).tolist())
+        if nw == 0 and ng == 0 and nf == n:
+            nfw = None
+        else:
+            if nf + nw + ng != n:
+                raise ValueError("particle kinds must be 0 (fluid), 1 (wall) or 2 (ghost)")
+            if ng != nw or not bool((k[nf + nw:] == 2).all()):
+                raise NotImplementedError("wall particles need one ghost point each, the ghosts after every fluid and wall particle "
+                                          "(the layout of addBoundaryGhostParticles)")
+            nfw = nf + nw
+        _KINDS_CHECKED.clear()
+        _KINDS_CHECKED[id(k)] = (key, nfw)
+    if nfw is not None:
+        if not allow_walls:
+            raise NotImplementedError("wall and ghost particles are on the GPU path of dfsph_step only")
+        if state.ghostIndices is None or state.ghostOffsets is None:
+            raise ValueError("wall particles need the state's ghostIndices and ghostOffsets")
+    return nfw
+
+
+def _check_supported(state, schemeConfig, allow_walls: bool = False) -> Optional[int]:
+    """Raises for what the GPU path does not cover; returns the wall layout (_wall_layout)."""
     if getattr(schemeConfig, "boundaryConditions", None):
         raise NotImplementedError("boundary conditions are not on the GPU path")
     if getattr(schemeConfig, "rigidBodies", None):
         raise NotImplementedError("rigid bodies are not on the GPU path")
-    k = state.kinds
-    if k is not None:
-        key = (id(k), k._version)
-        if _KINDS_CHECKED.get(id(k)) != key:
-            if bool((k != 0).any()):
-                raise NotImplementedError("boundary and ghost particles (kinds != 0) need the mDBC passes, which are not on the GPU path")
-            _KINDS_CHECKED.clear()
-            _KINDS_CHECKED[id(k)] = key
+    return _wall_layout(state, allow_walls)
+
+
+def _head(state, n: int):
+    """The first n particles of every per-particle field (views, no copies)."""
+    N = state.positions.shape[0]
+    kw = {}
+    for f in dataclasses.fields(state):
+        v = getattr(state, f.name)
+        kw[f.name] = v[:n] if isinstance(v, torch.Tensor) and v.dim() >= 1 and v.shape[0] == N else v
+    return type(state)(**kw)
+
+
+def _pad(t: Optional[torch.Tensor], n: int) -> Optional[torch.Tensor]:
+    """t with zero rows appended up to n rows (the ghost points' rows)."""
+    if t is None or t.shape[0] == n:
+        return t
+    return torch.cat([t, t.new_zeros((n - t.shape[0],) + tuple(t.shape[1:]))])
+
+
+def _gravity_vector(schemeConfig, dim: int):
+    g = schemeConfig.gravityConfig
+    if not g.active or g.type != GravityType.Directional:
+        return None
+    return [float(a) * float(g.magnitude) for a in list(g.direction)[:dim]]
+
+
+def computeBoundaryVelocities(currentState: Any, config: Any, schemeConfig: Any, adjacency=None) -> torch.Tensor:
+    """modules/mdbc/velocity.py:167-268 for walls with the zeros and constant boundary
+    types (BCType, moduleConfigurations/boundaryConditions.py:8-13): a wall particle of a
+    zeros region gets zero velocity, a constant region keeps its own.  The wall regions are
+    config.regions' boundary regions in order (a wall particle's material indexes them);
+    without regions every wall is a zeros wall.  The interpolated types (noSlip, freeSlip,
+    extended) raise NotImplementedError."""
+    k, v = currentState.kinds, currentState.velocities
+    if k is None:
+        return v
+    regions = [r for r in (getattr(config, "regions", None) or []) if getattr(getattr(r, "type", None), "name", "") == "Boundary"]
+    kinds_bc = [getattr(getattr(r, "kind", None), "name", "zeros") for r in regions]
+    bad = sorted(set(kinds_bc) - {"zeros", "constant"})
+    if bad:
+        raise NotImplementedError(f"boundary velocity types {bad} are not on the GPU path")
+    wall = k == 1
+    if regions:
+        zero_of_material = torch.tensor([b == "zeros" for b in kinds_bc], device=v.device)
+        mat = currentState.materials.long().clamp(0, len(kinds_bc) - 1)
+        wall = wall & zero_of_material[mat]
+    return torch.where(wall[:, None], torch.zeros_like(v), v)
 
 
 def computeGravity(currentState: Any, config: Any, schemeConfig: Any, adjacency=None) -> torch.Tensor:
@@ -102,7 +184,9 @@ def _passive(S) -> torch.Tensor:
 def dfsph_step(system, dt, config, schemeConfig, verbose: bool = False):
     """schemes/dfsph.py:13-218 on the GPU.  Returns (update, adjacency, state, (errors, pressures))."""
     S = system.state
-    _check_supported(S, schemeConfig)
+    nfw = _check_supported(S, schemeConfig, allow_walls=True)
+    if nfw is not None:
+        return _dfsph_step_walls(system, dt, config, schemeConfig, nfw)
     params = make_params(config)
     adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, system.adjacency)
     system.adjacency = adjacency
@@ -117,6 +201,58 @@ def dfsph_step(system, dt, config, schemeConfig, verbose: bool = False):
     dvdt_pressure, pressure, errors, pressures = solveDivergenceFree(S, config, schemeConfig, adjacency, dvdt + dvdt_diss, dt)
     S.pressures = pressure
     update = IncompressibleSystemUpdate(dxdt=S.velocities.clone(), dvdt=dvdt + dvdt_diss + dvdt_pressure, drhodt=drhodt,
+                                        passive=_passive(S))
+    return update, adjacency, S, (errors, pressures)
+
+
+def _dfsph_step_walls(system, dt, config, schemeConfig, nfw: int):
+    """dfsph_step with wall particles and their ghost points (dfsph.py:27-126, 170-186).
+
+    The fluid and wall particles (the first nfw) form the particle set of every pass
+    that the reference runs over fluid and walls; the ghost points take part only in the
+    mDBC density, whose Liu-Liu sums run over a second list built over every particle.
+    Steps: gather density; mDBC wall density (density2025.py); wall velocities
+    (mdbc/velocity.py); surface detection; velocity diffusion and continuity; gravity; the
+    no-penetration shift over dt (wp_nopenshift.py); the divergence-free solve, in which
+    the walls take part with their mDBC densities and zero velocities; and the update,
+    zero for walls and ghosts (dfsph.py:183-186)."""
+    S = system.state
+    n = int(S.positions.shape[0])
+    params = make_params(config)
+    vs = config.verletScale
+    adjacency = ops.buildVerletList(S.positions[:nfw], S.supports[:nfw], params, vs, system.adjacency)
+    key = (S.positions.device.index, n)
+    full = ops.buildVerletList(S.positions, S.supports, params, vs, _GHOST_LISTS.get(key))
+    _GHOST_LISTS.clear()
+    _GHOST_LISTS[key] = full
+    system.adjacency = adjacency
+    rho0 = float(schemeConfig.fluid.restDensity)
+    if S.densities is None or not schemeConfig.solverConfig.integrateRho:
+        rho = ops.density(params, S.positions[:nfw], S.supports[:nfw], S.masses[:nfw], adjacency, SupportScheme.Gather)
+        tail = S.densities[nfw:] if S.densities is not None else torch.full((n - nfw,), rho0, device=rho.device, dtype=rho.dtype)
+        S.densities = torch.cat([rho, tail])
+    S.densities = ops.mdbc_density(params, S.positions, S.supports, S.masses, S.densities, S.kinds, S.ghostIndices, S.ghostOffsets,
+                                   full, rho0, float(schemeConfig.fluid.fixedSoundSpeed), _gravity_vector(schemeConfig, int(config.dim)))
+    S.velocities = computeBoundaryVelocities(S, config, schemeConfig, adjacency)
+    Hd = _head(S, nfw)
+    _surface(Hd, config, schemeConfig, adjacency)
+    S.surfaceIndicators, S.surfaceNormals = _pad(Hd.surfaceIndicators, n), _pad(Hd.surfaceNormals, n)
+    S.surfaceLambdas = _pad(Hd.surfaceLambdas, n)
+    dvdt_diss, drhodt = ops.wc_visc_continuity(params, wc_params(schemeConfig), Hd.positions, Hd.supports, Hd.masses, Hd.densities,
+                                               Hd.velocities, adjacency)
+    dvdt = computeGravity(Hd, config, schemeConfig, adjacency)
+    nopen = ops.mdbc_nopen_shift(params, Hd.positions, Hd.supports, Hd.masses, Hd.velocities, Hd.kinds, Hd.ghostOffsets, adjacency)
+    dvdt = dvdt + nopen / dt
+    if S.pressures is None:
+        S.pressures = torch.zeros_like(S.densities)
+    Hd.pressures = S.pressures[:nfw]
+    dvdt_pressure, pressure, errors, pressures = solveDivergenceFree(Hd, config, schemeConfig, adjacency, dvdt + dvdt_diss, dt)
+    S.pressures = _pad(pressure, n)
+    fluid = (Hd.kinds == 0)[:, None]
+    zero_v = torch.zeros_like(Hd.velocities)
+    update = IncompressibleSystemUpdate(dxdt=_pad(torch.where(fluid, Hd.velocities, zero_v), n),
+                                        dvdt=_pad(torch.where(fluid, dvdt + dvdt_diss + dvdt_pressure, zero_v), n),
+                                        drhodt=_pad(torch.where(fluid[:, 0], drhodt, torch.zeros_like(drhodt)), n),
                                         passive=_passive(S))
     return update, adjacency, S, (errors, pressures)
 
@@ -236,12 +372,29 @@ def solveShifting(state, config, schemeConfig, adjacency, dt):
 def finalize_incompressible(system, initialState, dt, returnValues, updateValues, config, schemeConfig):
     """systems/incompressible.py:71-277.  The delta-plus shift the reference computes when
     shiftProperties.active (:134-209) is not applied anywhere (the lines that would apply
-    it, :262-267, are commented out), so it is not evaluated here."""
+    it, :262-267, are commented out), so it is not evaluated here.  With wall particles the
+    density solve runs over the fluid and wall particles and only fluid particles move:
+    the reference moves every particle by dt^2 a_p (:250-255), walls included, which would
+    carry the tank's walls along with the solve."""
     last = returnValues[-1][1]
     S = system.state
     for name in _LAST_STAGE_FIELDS + ("densities",):
         setattr(S, name, getattr(last, name))
     params = make_params(config)
+    nfw = _wall_layout(S, True)
+    if nfw is not None:
+        n = int(S.positions.shape[0])
+        adjacency = ops.buildVerletList(S.positions[:nfw], S.supports[:nfw], params, config.verletScale, returnValues[-1][0])
+        rho = ops.density(params, S.positions[:nfw], S.supports[:nfw], S.masses[:nfw], adjacency, SupportScheme.Gather)
+        S.densities = torch.cat([rho, S.densities[nfw:]])
+        Hd = _head(S, nfw)
+        zero = torch.zeros_like(Hd.velocities)
+        dvdt_incomp, _, errors_incomp, pressures_incomp = solveIncompressible(Hd, config, schemeConfig, adjacency, zero, dt)
+        shift = torch.where((Hd.kinds == 0)[:, None], (dt * dt) * dvdt_incomp, zero)
+        S.positions = torch.cat([_add_positions(params, Hd.positions, shift, int(config.dim)), S.positions[nfw:]])
+        system.adjacency = adjacency
+        returnValues[-1] = tuple(returnValues[-1][:3]) + ((errors_incomp, pressures_incomp),)
+        return system
     adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, returnValues[-1][0])
     S.densities = ops.density(params, S.positions, S.supports, S.masses, adjacency, SupportScheme.Gather)
     zero = torch.zeros_like(S.velocities)
