@@ -244,6 +244,152 @@ class DamBreak2D:
         self.t += self.dt
 
 
+@dataclass
+class DamBreakMDBC:
+    """The dam break of the learned warm start with the reference's mDBC walls, in 2D or 3D:
+    a column[:dim] fluid block in the corner of an open tank[:dim] tank (axis 1 vertical),
+    three wall layers with one mirrored ghost point per wall particle (cases.tank_particles).
+
+    Each step: the gather density of fluid and walls; the mDBC wall densities
+    (sph_mdbc_density, the Liu-Liu sums at the ghost points over a list of every particle);
+    the no-penetration shift (sph_mdbc_nopen_shift) added to gravity over dt; the density
+    solve; the divergence-free solve on the predicted velocity; symplectic Euler for the
+    fluid.  The walls take part in both solves with their mDBC densities and zero
+    velocities and never move.  rho0 = 1 for the reason DamBreak2D gives; masses are set so
+    that an interior fluid particle of the lattice sums to rho0.  ``collect`` and
+    ``compare`` work as in DamBreak2D."""
+    dim: int = 3
+    column: tuple = (0.5, 1.0, 0.5)
+    tank: tuple = (1.6, 1.2, 0.6)
+    dx: float = 0.02
+    rho0: float = 1.0
+    sound_speed: float = 10.0
+    g: float = -9.81
+    dt: float = 1e-3
+    target_neighbors: float = 40.0
+    device: str = "cuda"
+    kernel: KernelFunctions = KernelFunctions.Wendland2
+    layers: int = 3
+    seed: int = 0
+    jitter: float = 0.02
+    state: dict = field(default_factory=dict)
+
+    def __post_init__(self):
+        from .cases import tank_particles
+        dev = torch.device(self.device)
+        d, dx = self.dim, self.dx
+        fluid, walls, ghosts = tank_particles(d, dx, self.column[:d], self.tank[:d], self.layers, self.jitter, self.seed)
+        self.n_fluid, self.n_wall = len(fluid), len(walls)
+        self.nfw = self.n_fluid + self.n_wall
+        x = np.concatenate([fluid, walls, ghosts]).astype(np.float32)
+        self.n = len(x)
+        pad = (self.layers + 2) * dx
+        hi = [t + pad for t in self.tank[:d]]
+        hi[1] = 3.0 * self.tank[1]
+        self.domain = DomainDescription(torch.full((d,), -pad, device=dev), torch.tensor(hi, device=dev, dtype=torch.float32),
+                                        torch.zeros(d, dtype=torch.bool, device=dev), d)
+        from .configurations import SimulationConfig
+        self.config = SimulationConfig(device=dev, domain=self.domain, dim=d, kernel=self.kernel, verletScale=2.0 ** (1.0 / d),
+                                       targetNeighbors=self.target_neighbors)
+        self.params = make_params(self.config)
+        S = self.state
+        S["x"] = torch.from_numpy(x).to(dev)
+        S["H"] = torch.full((self.n,), float(volumeToSupportHelper(dx ** d, self.target_neighbors, d)), device=dev)
+        S["m"] = torch.ones(self.n, device=dev)
+        kinds = np.concatenate([np.zeros(self.n_fluid), np.ones(self.n_wall), np.full(self.n_wall, 2)]).astype(np.int32)
+        gidx = np.full(self.n, -1, np.int32)
+        gidx[self.n_fluid:self.nfw] = np.arange(self.nfw, self.n)
+        gidx[self.nfw:] = np.arange(self.n_fluid, self.nfw)
+        goff = np.zeros_like(x)
+        goff[self.n_fluid:self.nfw] = walls - ghosts
+        goff[self.nfw:] = ghosts - walls
+        S["kinds"] = torch.from_numpy(kinds).to(dev)
+        S["gidx"] = torch.from_numpy(gidx).to(dev)
+        S["goff"] = torch.from_numpy(goff).to(dev)
+        adj = ops.buildVerletList(S["x"][: self.nfw], S["H"][: self.nfw], self.params, self.config.verletScale)
+        rho_unit = ops.density(self.params, S["x"][: self.nfw], S["H"][: self.nfw], S["m"][: self.nfw], adj)
+        c = np.asarray(self.column[:d]) * 0.5
+        interior = int(np.argmin(np.linalg.norm(fluid - c, axis=1)))
+        S["m"] *= self.rho0 / float(rho_unit[interior].item())
+        S["v"] = torch.zeros((self.nfw, d), device=dev)
+        S["p_rho"] = torch.zeros(self.nfw, device=dev)
+        S["p_df"] = torch.zeros(self.nfw, device=dev)
+        self.fluid = torch.zeros(self.nfw, dtype=torch.bool, device=dev)
+        self.fluid[: self.n_fluid] = True
+        self.gvec = torch.zeros((self.nfw, d), device=dev)
+        self.gvec[: self.n_fluid, 1] = self.g
+        self.gravity = [0.0] * d
+        self.gravity[1] = self.g
+        self.adj = None
+        self.full = None
+        self.t = 0.0
+
+    def _solve(self, mode, cfg, v, dvdt, p_init, rho):
+        S, k = self.state, self.nfw
+        return ops.jacobi_solve(self.params, mode, cfg, S["x"][:k], S["H"][:k], S["m"][:k], rho, v, dvdt, p_init, self.dt, self.adj)
+
+    def _arm(self, mode, solver: RelaxedJacobiSolverConfig, v, dvdt, p_prev, rho, net: Optional[WarmStartMLP]) -> SolveStats:
+        S, k = self.state, self.nfw
+        cfg = jacobi_config(solver, self.rho0, learned_init=net is not None)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        p0 = p_prev
+        if net is not None:
+            p0 = net.initial_pressure(self.params, mode, cfg, S["x"][:k], S["H"][:k], S["m"][:k], rho, v, dvdt, p_prev, self.dt, self.adj)
+        pr, acc, hist, it, st = self._solve(mode, cfg, v, dvdt, p0, rho)
+        ev1.record()
+        torch.cuda.synchronize()
+        n_it = int(it.item())
+        err = float(hist[n_it - 1, 0].item()) if n_it > 0 else float("nan")
+        return SolveStats(mode, n_it, ev0.elapsed_time(ev1), err, (int(st.item()) & _capi.STATUS_NOT_CONVERGED) == 0)
+
+    def densities(self) -> torch.Tensor:
+        """Gather density of fluid and walls with the walls' replaced by the mDBC pass."""
+        S, k = self.state, self.nfw
+        self.adj = ops.buildVerletList(S["x"][:k], S["H"][:k], self.params, self.config.verletScale, self.adj)
+        self.full = ops.buildVerletList(S["x"], S["H"], self.params, self.config.verletScale, self.full)
+        r = ops.density(self.params, S["x"][:k], S["H"][:k], S["m"][:k], self.adj)
+        r_all = torch.cat([r, torch.full((self.n - k,), self.rho0, device=r.device)])
+        r_all = ops.mdbc_density(self.params, S["x"], S["H"], S["m"], r_all, S["kinds"], S["gidx"], S["goff"], self.full, self.rho0,
+                                 self.sound_speed, self.gravity)
+        return r_all[:k].contiguous()
+
+    def step(self, driver: tuple, collect: Optional[dict] = None, compare: Optional[dict] = None):
+        S, k = self.state, self.nfw
+        rho = self.densities()
+        zero = torch.zeros_like(S["v"])
+        nopen = ops.mdbc_nopen_shift(self.params, S["x"][:k], S["H"][:k], S["m"][:k], S["v"], S["kinds"][:k], S["goff"][:k], self.adj)
+        ext = (self.gvec + nopen / self.dt).contiguous()
+        out = {}
+        for mode, key in ((ops.DENSITY, "p_rho"), (ops.DIVERGENCE_FREE, "p_df")):
+            if mode == ops.DENSITY:
+                v, dvdt = S["v"], ext
+            else:
+                v = torch.where(self.fluid[:, None], S["v"] + self.dt * (ext + out[ops.DENSITY]), zero).contiguous()
+                dvdt = zero
+                vstar = v
+            solver = driver[0] if mode == ops.DENSITY else driver[1]
+            dcfg = jacobi_config(solver, self.rho0, learned_init=True)
+            if compare is not None:
+                ev = compare["solvers"][0] if mode == ops.DENSITY else compare["solvers"][1]
+                net = compare["nets"][0] if mode == ops.DENSITY else compare["nets"][1]
+                compare["stats"].append(("plain", self._arm(mode, ev, v, dvdt, S[key], rho, None)))
+                compare["stats"].append(("learned", self._arm(mode, ev, v, dvdt, S[key], rho, net)))
+            if collect is not None:
+                f, sc = ops.dfsph_features(self.params, mode, dcfg, S["x"][:k], S["H"][:k], S["m"][:k], rho, v, dvdt, S[key], self.dt,
+                                           self.adj)
+            pr, acc, hist, it, st = self._solve(mode, dcfg, v, dvdt, S[key], rho)
+            out[mode] = acc
+            if collect is not None:
+                collect.setdefault(("feats", mode), []).append(f)
+                collect.setdefault(("target", mode), []).append(pr / sc)
+            S[key] = pr
+        v = torch.where(self.fluid[:, None], vstar + self.dt * out[ops.DIVERGENCE_FREE], zero)
+        S["x"] = torch.cat([S["x"][: self.n_fluid] + self.dt * v[: self.n_fluid], S["x"][self.n_fluid:]]).contiguous()
+        S["v"] = v.contiguous()
+        self.t += self.dt
+
+
 def solver_configs(rho0: float, density_tol_frac: float = 1e-4, div_tol_frac: float = 1e-3, max_iterations: int = 400):
     """The reference's relaxed-Jacobi settings (solver.py:15-28) with the tolerances of
     a 0.01 % density error and a 0.1 % divergence error, both normalised by rho0."""
@@ -264,15 +410,25 @@ def driver_configs(rho0: float):
     return rho, df
 
 
-def generate_samples(geometries, steps: int, device="cuda", dx: float = 0.02, dt: float = 1e-3):
+def dam_break_2d(w, h, seed, dx, dt, device):
+    return DamBreak2D(width=w, height=h, dx=dx, dt=dt, device=device, seed=seed)
+
+
+def dam_break_mdbc_3d(w, h, seed, dx, dt, device):
+    """The 3D mDBC dam break with a w x h x w column (the 1.6 x 1.2 x 0.6 m tank)."""
+    return DamBreakMDBC(dim=3, column=(w, h, w), dx=dx, dt=dt, device=device, seed=seed)
+
+
+def generate_samples(geometries, steps: int, device="cuda", dx: float = 0.02, dt: float = 1e-3, make_case=dam_break_2d,
+                     collect_every: int = 1):
     """(features, targets) per solve mode from dam-break trajectories; ``geometries`` is a
-    list of (width, height, seed)."""
+    list of (width, height, seed); samples are collected every ``collect_every`` steps."""
     collect: dict = {}
     for (w, h, seed) in geometries:
-        case = DamBreak2D(width=w, height=h, dx=dx, dt=dt, device=device, seed=seed)
+        case = make_case(w, h, seed, dx, dt, device)
         drv = driver_configs(case.rho0)
-        for _ in range(steps):
-            case.step(drv, collect=collect)
+        for s_ in range(steps):
+            case.step(drv, collect=collect if (s_ + 1) % collect_every == 0 else None)
     out = {}
     for mode in (0, 1):
         out[mode] = (torch.cat(collect[("feats", mode)]).contiguous(), torch.cat(collect[("target", mode)]).contiguous())
@@ -280,7 +436,7 @@ def generate_samples(geometries, steps: int, device="cuda", dx: float = 0.02, dt
 
 
 def compare_warm_starts(geometries, steps: int, nets, device="cuda", dx: float = 0.02, dt: float = 1e-3, skip: int = 2,
-                        max_iterations: int = 2000, df_budget: int = 32):
+                        max_iterations: int = 2000, df_budget: int = 32, make_case=dam_break_2d):
     """Plain against learned initial pressure on the same states, after the first ``skip``
     steps of each trajectory:
       density solve: summed iterations and GPU ms to the 0.01 % tolerance (cap
@@ -290,7 +446,7 @@ def compare_warm_starts(geometries, steps: int, nets, device="cuda", dx: float =
     tot = {"density": {"plain": [0, 0.0, 0], "learned": [0, 0.0, 0]},
            "divergence_free": {"plain": [0.0, 0.0, 0], "learned": [0.0, 0.0, 0]}}
     for (w, h, seed) in geometries:
-        case = DamBreak2D(width=w, height=h, dx=dx, dt=dt, device=device, seed=seed)
+        case = make_case(w, h, seed, dx, dt, device)
         drv = driver_configs(case.rho0)
         rho_ev, df_ev = solver_configs(case.rho0, max_iterations=max_iterations)
         df_ev = RelaxedJacobiSolverConfig(minIterations=df_budget, maxIterations=df_budget, tolerance=0.0,
