@@ -346,6 +346,20 @@ int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const floa
                        const int32_t* offs, const int32_t* cnt, const int32_t* list,
                        const int32_t* verlet_cnt, float* dvdt_out, float* dudt_out,
                        float* dEdt_out, float* ap_ij, float* av_ij, void* stream);
+/* The same pass over packed particle records: a first launch copies the fields the pass
+ * reads into records [n, R] (R = sph_crk_record_floats(dim) floats per particle: 12, 24
+ * and 36 in 1D, 2D and 3D; 16-byte aligned, caller-owned scratch), and the pair launch
+ * gathers each neighbour as R/4 128-bit loads from that one record.  Outputs and
+ * arguments otherwise as sph_crk_accel_dudt. */
+int sph_crk_record_floats(int32_t dim);
+int sph_crk_accel_dudt_packed(const SphParams* p, int64_t n, const float* x, const float* H,
+                              const float* m, const float* rho, const float* V,
+                              const float* A, const float* B, const float* gradA, const float* gradB,
+                              const float* v, const float* c, const float* P, const float* DvDx,
+                              const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                              const int32_t* verlet_cnt, float* dvdt_out, float* dudt_out,
+                              float* dEdt_out, float* ap_ij, float* av_ij, float* records,
+                              void* stream);
 /* Same pass, separate names for callers that bind the reference's two wrappers
  * computeCrkSPHAccelWarp (modules/crk/accel.py:391) and computeCrkSPHdudtWarp
  * (modules/crk/dudt.py:364). */

@@ -14,8 +14,8 @@ import warpsph_b200 as ws
 from oracle.steps import DeltaSPHOracle, DFSPHOracle
 from tests.cases import assert_close, make_params
 from warpsph_b200 import core
-from warpsph_b200.configurations import (IncompressibleSPHConfig, RelaxedJacobiSolverConfig, WeaklyCompressibleSPHConfig,
-                                         jacobi_config, wc_params)
+from warpsph_b200.configurations import (IncompressibleSPHConfig, NormalSource, RelaxedJacobiSolverConfig,
+                                         SurfaceDetectionScheme, WeaklyCompressibleSPHConfig, jacobi_config, wc_params)
 from warpsph_b200.integrators import getIntegrator
 
 pytestmark = pytest.mark.gpu
@@ -166,6 +166,8 @@ def test_deltasph_step_free_surface_matches_oracle(cuda):
     sch = Config()
     sch.shiftProperties.active = False
     sch.surfaceDetectionConfig.active = True
+    sch.surfaceDetectionConfig.scheme = SurfaceDetectionScheme.ColorField
+    sch.surfaceDetectionConfig.normalSource = NormalSource.ColorFieldGrad
     sch.pressureForceTerm = "Antuono"
     dt = 5e-4
     rng = np.random.default_rng(5)

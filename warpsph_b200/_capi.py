@@ -118,6 +118,8 @@ _PROTOS = {
     "sph_switch_hopkins_terms": [_P, _I64] + [_P] * 14,
     "sph_switch_hopkins_update": [_P, _I64] + [_P] * 14,
     "sph_crk_accel_dudt": [_P, _I64] + [_P] * 23,
+    "sph_crk_record_floats": [_I32],
+    "sph_crk_accel_dudt_packed": [_P, _I64] + [_P] * 24,
     "sph_crk_accel": [_P, _I64] + [_P] * 21,
     "sph_crk_dudt": [_P, _I64] + [_P] * 18,
     "sph_compsph_prep": [_P, _I64] + [_P] * 12,

@@ -79,7 +79,8 @@ def compSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams
         raise NotImplementedError(f"viscosity switch {switch} is not implemented on the GPU path")
     # compSPH.py:113-149 and :170
     dvdt, dudt, dEdt, S.ap_ij, S.av_ij = ops.compsph_accel_dudt(params, S.positions, S.supports, S.masses, S.densities, S.velocities,
-                                                                S.soundspeeds, S.alphas, S.pressures, omega, adjacency)
+                                                                S.soundspeeds, S.alphas, S.pressures, omega, adjacency,
+                                                                reference_layout=False)
     # compSPH.py:153-159 (computeCullenUpdate hands back the same alpha0; computeHopkinsUpdate
     # relaxes alpha0 with the divergence of the previous step, CullenHopkins.py:48-149)
     if cullen:

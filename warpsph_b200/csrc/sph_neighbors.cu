@@ -485,6 +485,10 @@ __device__ __forceinline__ int stencil_keys(const int* c, const GridDev& g, cons
 constexpr int VW_WARPS = 4;
 constexpr int VW_BLOCK = 32 * VW_WARPS;
 constexpr int VS = 16;
+// Row pitch of the staging buffers: one word more than VS, so that the 32 lanes'
+// stores of their next entry fall in 32 different banks (with a pitch of 16 words the
+// even and the odd lanes would each share one bank, a 16-way conflict per store).
+constexpr int VP = VS + 1;
 
 // fl(sqrt(r2)) / Hm < 1, with the square root only inside a narrow band around r = Hm
 // (outside it the comparison of r2 with Hm^2 decides the same way).
@@ -498,7 +502,7 @@ __device__ __forceinline__ bool interacting_pair(float r2, float Hm) {
 // Writes every lane's staged entries of one part: lanes pair up per owner row (16
 // entries per half warp), base_o + e for the owner's base.
 __device__ __forceinline__ void verlet_flush_part(int lane, int wib, int& nb, int& written, int base,
-                                                  int32_t (*buf)[32][VS], int32_t* __restrict__ list) {
+                                                  int32_t (*buf)[32][VP], int32_t* __restrict__ list) {
     const int half = lane >> 4, e = lane & 15;
     #pragma unroll 4
     for (int r = 0; r < 32; r += 2) {
@@ -520,8 +524,8 @@ k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_ke
          int32_t* __restrict__ list, long long* __restrict__ innz, const long long* __restrict__ nnz, long long capacity) {
     __shared__ float4 srec[VW_WARPS][32];
     __shared__ int32_t sidx[FILL ? VW_WARPS : 1][32];
-    __shared__ int32_t sbuf[FILL ? VW_WARPS : 1][32][VS];     // rest of the row
-    __shared__ int32_t sibuf[FILL ? VW_WARPS : 1][32][VS];    // interacting prefix
+    __shared__ int32_t sbuf[FILL ? VW_WARPS : 1][32][VP];     // rest of the row
+    __shared__ int32_t sibuf[FILL ? VW_WARPS : 1][32][VP];    // interacting prefix
     const bool part = icounts != nullptr;
     if (FILL && *nnz > capacity) return;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;

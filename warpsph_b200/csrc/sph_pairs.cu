@@ -749,6 +749,96 @@ __device__ __forceinline__ void zero_row_tail(int lane, int e, int te, float* __
     }
 }
 
+// Packed per-particle record of the CRK accel pass: every field a pair reads from
+// particle j (and the pass reads from particle i) in one block of R floats, R a multiple
+// of 4, so a pair's neighbour gather is R/4 128-bit loads from adjacent sectors instead
+// of 2D^2+4D+6 scalar loads from as many arrays (D = 2: 6 loads and 3 sectors instead of
+// 22 loads and 22 sectors).  The fields are in the order the pair body first uses them,
+// and the body loads them in three groups of 16-byte granules: position and support
+// (before the distance test), velocity, gradient, sound speed and pressure (the limiter
+// and Q), and the rest (the corrected gradient of W_ji), which keeps fewer of them live.
+template <int D> struct CrkRec {
+    static constexpr int X = 0, H = D, RHO = D + 1, V = D + 2, G = 2 * D + 2, C = 2 * D + 2 + D * D, P = C + 1,
+                         VOL = C + 2, A = C + 3, B = C + 4, GA = B + D, GB = GA + D, END = GB + D * D,
+                         R = (END + 3) / 4 * 4;
+    static constexpr int K1 = (H + 1 + 3) / 4;      // granules of the first group
+    static constexpr int K2 = (P + 1 + 3) / 4;      // ... of the first two groups
+    static constexpr int K3 = R / 4;
+};
+template <int D, int K0, int K1>
+__device__ __forceinline__ void rec_granules(const float4* __restrict__ src, float (&r)[CrkRec<D>::R]) {
+    #pragma unroll
+    for (int k = K0; k < K1; ++k) {
+        float4 t = __ldg(src + k);
+        r[4 * k] = t.x; r[4 * k + 1] = t.y; r[4 * k + 2] = t.z; r[4 * k + 3] = t.w;
+    }
+}
+
+template <int D>
+__global__ void k_crk_pack(int n, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ rho,
+                           const float* __restrict__ V, const float* __restrict__ A, const float* __restrict__ B,
+                           const float* __restrict__ gA, const float* __restrict__ gB, const float* __restrict__ v,
+                           const float* __restrict__ c, const float* __restrict__ Pr, const float* __restrict__ DvDx,
+                           float* __restrict__ rec) {
+    using L = CrkRec<D>;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float r[L::R];
+    #pragma unroll
+    for (int a = 0; a < D; ++a) {
+        r[L::X + a] = x[(size_t)i * D + a];
+        r[L::V + a] = v[(size_t)i * D + a];
+        r[L::B + a] = B[(size_t)i * D + a];
+        r[L::GA + a] = gA[(size_t)i * D + a];
+    }
+    #pragma unroll
+    for (int a = 0; a < D * D; ++a) {
+        r[L::GB + a] = gB[(size_t)i * D * D + a];
+        r[L::G + a] = DvDx[(size_t)i * D * D + a];
+    }
+    r[L::H] = H[i]; r[L::RHO] = rho[i]; r[L::VOL] = V[i]; r[L::C] = c[i]; r[L::P] = Pr[i]; r[L::A] = A[i];
+    #pragma unroll
+    for (int a = L::END; a < L::R; ++a) r[a] = 0.f;
+    float4* dst = reinterpret_cast<float4*>(rec + (size_t)i * L::R);
+    #pragma unroll
+    for (int k = 0; k < L::R / 4; ++k) dst[k] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
+}
+
+// The fields of one particle as the accel pass uses them.
+template <int D> struct CrkPart {
+    Vec<D> x, v, B, gA;
+    Mat<D> gB, G;
+    float H, rho, V, c, P, A;
+};
+// Group 1: position and support; group 2: velocity, velocity gradient, density, sound
+// speed, pressure; group 3: volume and the CRK correction fields.
+template <int D> __device__ __forceinline__ void crk_unpack1(const float (&r)[CrkRec<D>::R], CrkPart<D>& o) {
+    using L = CrkRec<D>;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) o.x.v[a] = r[L::X + a];
+    o.H = r[L::H];
+}
+template <int D> __device__ __forceinline__ void crk_unpack2(const float (&r)[CrkRec<D>::R], CrkPart<D>& o) {
+    using L = CrkRec<D>;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) o.v.v[a] = r[L::V + a];
+    #pragma unroll
+    for (int a = 0; a < D; ++a)
+        #pragma unroll
+        for (int b = 0; b < D; ++b) o.G.m[a][b] = r[L::G + a * D + b];
+    o.rho = r[L::RHO]; o.c = r[L::C]; o.P = r[L::P];
+}
+template <int D> __device__ __forceinline__ void crk_unpack3(const float (&r)[CrkRec<D>::R], CrkPart<D>& o) {
+    using L = CrkRec<D>;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) { o.B.v[a] = r[L::B + a]; o.gA.v[a] = r[L::GA + a]; }
+    #pragma unroll
+    for (int a = 0; a < D; ++a)
+        #pragma unroll
+        for (int b = 0; b < D; ++b) o.gB.m[a][b] = r[L::GB + a * D + b];
+    o.V = r[L::VOL]; o.A = r[L::A];
+}
+
 // modules/crk/accel.py:65-250 and modules/crk/dudt.py:62-229 in one pass.  The pair
 // body's quotients (Van Leer ratios, 1/H_j, the mu_ij denominators) use the fast FP32
 // divide (about 2 ulp): about a tenth of the pass's time, well inside the pass's parity
@@ -758,15 +848,19 @@ __device__ __forceinline__ void zero_row_tail(int lane, int e, int te, float* __
 // (schemes/crkSPH.py:330) is written per particle.  Walking the interacting prefix of
 // each Verlet row (cnt = interacting counts) with vcnt = the Verlet counts, the
 // ap_ij / av_ij entries of the rest of the row are written as zeros.
-template <int KF, int D, int G>
-__global__ void __launch_bounds__(PAIR_BLOCK, (D == 3 ? 5 : 8))
+#ifndef CRK_REC_BLOCKS
+#define CRK_REC_BLOCKS 7
+#endif
+template <int KF, int D, int G, bool REC>
+__global__ void __launch_bounds__(PAIR_BLOCK, (D == 3 ? 5 : (REC ? CRK_REC_BLOCKS : 8)))
 k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
                  const float* __restrict__ rho, const float* __restrict__ V, const float* __restrict__ A,
                  const float* __restrict__ B, const float* __restrict__ gA, const float* __restrict__ gB,
                  const float* __restrict__ v, const float* __restrict__ c, const float* __restrict__ Pr,
-                 const float* __restrict__ DvDx, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
-                 const int32_t* __restrict__ list, const int32_t* __restrict__ vcnt, float* __restrict__ dvdt,
-                 float* __restrict__ dudt, float* __restrict__ dEdt, float* __restrict__ ap, float* __restrict__ av) {
+                 const float* __restrict__ DvDx, const float* __restrict__ rec, const int32_t* __restrict__ offs,
+                 const int32_t* __restrict__ cnt, const int32_t* __restrict__ list, const int32_t* __restrict__ vcnt,
+                 float* __restrict__ dvdt, float* __restrict__ dudt, float* __restrict__ dEdt, float* __restrict__ ap,
+                 float* __restrict__ av) {
     Grp<G> g(n);
     const bool comp = P.kahan != 0;
     KSum acc[D], du;
@@ -775,13 +869,19 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
     du.init();
     if (g.valid) {
         const int i = g.i;
-        Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
-        const float Hi = H[i], rhoi = rho[i], ci = c[i], Pi = Pr[i];
+        CrkPart<D> pi;
+        if constexpr (REC) {
+            float r[CrkRec<D>::R];
+            rec_granules<D, 0, CrkRec<D>::K3>(reinterpret_cast<const float4*>(rec + (size_t)i * CrkRec<D>::R), r);
+            crk_unpack1<D>(r, pi); crk_unpack2<D>(r, pi); crk_unpack3<D>(r, pi);
+        } else {
+            pi.x = load_vec<D>(x, i); pi.v = load_vec<D>(v, i); pi.B = load_vec<D>(B, i); pi.gA = load_vec<D>(gA, i);
+            pi.gB = load_mat<D>(gB, i); pi.G = load_mat<D>(DvDx, i);
+            pi.H = H[i]; pi.rho = rho[i]; pi.V = V[i]; pi.c = c[i]; pi.P = Pr[i]; pi.A = A[i];
+        }
+        const float Hi = pi.H, rhoi = pi.rho, ci = pi.c, Pi = pi.P;
         const float invHi = 1.f / Hi;
-        const float Vi_m = V[i] / m[i];          // V_i / m_i
-        const float Ai = A[i];
-        Vec<D> Bi = load_vec<D>(B, i), gAi = load_vec<D>(gA, i);
-        Mat<D> gBi = load_mat<D>(gB, i), Gi = load_mat<D>(DvDx, i);
+        const float Vi_m = pi.V / m[i];          // V_i / m_i
         const float ks = P.kscale;
         const float inv_smooth_i = ks * invHi;   // 1 / (H_i / ks)
         const float sm_i = Hi / ks;
@@ -789,21 +889,30 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
         int b = offs[i], e = b + cnt[i];
         for (int q = b + g.lane; q < e; q += G) {
             int j, k; entry(list, q, j, k);
-            Vec<D> xj = load_vec<D>(x, j);
-            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
+            CrkPart<D> pj;
+            float rj[CrkRec<D>::R];
+            const float4* sj = REC ? reinterpret_cast<const float4*>(rec + (size_t)j * CrkRec<D>::R) : nullptr;
+            if constexpr (REC) { rec_granules<D, 0, CrkRec<D>::K1>(sj, rj); crk_unpack1<D>(rj, pj); }
+            else { pj.x = load_vec<D>(x, j); pj.H = __ldg(H + j); }
+            Vec<D> xij = dist_vec<D>(pi.x, pj.x, P.dom);
             float r2 = dot<D>(xij, xij);
-            float Hj = __ldg(H + j);
+            const float Hj = pj.H;
             float Hm = wmax(Hi, Hj);
             if (!(r2 < Hm * Hm)) {
                 if (ap) store_vec<D>(ap, k, vzero<D>());
                 if (av) store_vec<D>(av, k, vzero<D>());
                 continue;
             }
+            if constexpr (REC) {
+                rec_granules<D, CrkRec<D>::K1, CrkRec<D>::K2>(sj, rj); crk_unpack2<D>(rj, pj);
+            } else {
+                pj.v = load_vec<D>(v, j);
+                pj.rho = __ldg(rho + j); pj.c = __ldg(c + j); pj.P = __ldg(Pr + j);
+                pj.G = load_mat<D>(DvDx, j);
+            }
             float r = safe_sqrt(r2);
             const float invHj = __fdividef(1.f, Hj);
-            Vec<D> vj = load_vec<D>(v, j);
-            float rhoj = __ldg(rho + j), Vj = __ldg(V + j), cj = __ldg(c + j), Pj = __ldg(Pr + j);
-            Mat<D> Gj = load_mat<D>(DvDx, j);
+            const float rhoj = pj.rho, cj = pj.c, Pj = pj.P;
             // CRK limiter (limiter.py:89-128), eta measured in supports
             float factor = 1.f;
             if (P.enable_crk_limiter) {
@@ -811,33 +920,36 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
                 if (eta < P.eta_crit) { float t = (eta - P.eta_crit) / P.eta_fold; factor = expf(-(t * t)); }
             }
             float phi = 0.f;
-            if (P.enable_vanleer) phi = van_leer<D>(xij, Gi, Gj) * factor;
+            if (P.enable_vanleer) phi = van_leer<D>(xij, pi.G, pj.G) * factor;
             if (P.force_vl_off) phi = 0.f;
             if (P.force_vl_on) phi = 1.f;
             phi = wmax(wmin(phi, 1.f), 0.f);
-            Vec<D> Gix = matvec<D>(Gi, xij), Gjx = matvec<D>(Gj, xij);
+            Vec<D> Gix = matvec<D>(pi.G, xij), Gjx = matvec<D>(pj.G, xij);
             float hp = 0.5f * phi;
             // v_dot_i - v_dot_j (accel.py:137-141; dudt.py:122-126 uses gradV_j . (-x_ij))
             Vec<D> da, dd;
             #pragma unroll
             for (int a = 0; a < D; ++a) {
-                float vdi = vi.v[a] - hp * Gix.v[a];
-                da.v[a] = vdi - (vj.v[a] + hp * Gjx.v[a]);
-                dd.v[a] = vdi - (vj.v[a] - hp * Gjx.v[a]);
+                float vdi = pi.v.v[a] - hp * Gix.v[a];
+                da.v[a] = vdi - (pj.v.v[a] + hp * Gjx.v[a]);
+                dd.v[a] = vdi - (pj.v.v[a] - hp * Gjx.v[a]);
             }
             // corrected gradients (accel.py:170-187, dudt.py:155-170)
             float Wi; Vec<D> gWi;
             kWG_inv<KF, D>(xij, r, invHj, Wi, gWi);
-            Vec<D> gradw_i = crk_grad<D>(xij, Wi, gWi, Ai, Bi, gAi, gBi);
-            float Aj = __ldg(A + j);
-            Vec<D> Bj = load_vec<D>(B, j), gAj = load_vec<D>(gA, j);
-            Mat<D> gBj = load_mat<D>(gB, j);
+            Vec<D> gradw_i = crk_grad<D>(xij, Wi, gWi, pi.A, pi.B, pi.gA, pi.gB);
+            if constexpr (REC) {
+                rec_granules<D, CrkRec<D>::K2, CrkRec<D>::K3>(sj, rj); crk_unpack3<D>(rj, pj);
+            } else {
+                pj.V = __ldg(V + j);
+                pj.A = __ldg(A + j); pj.B = load_vec<D>(B, j); pj.gA = load_vec<D>(gA, j); pj.gB = load_mat<D>(gB, j);
+            }
             Vec<D> xji;
             #pragma unroll
             for (int a = 0; a < D; ++a) xji.v[a] = -xij.v[a];
             float Wj; Vec<D> gWj;
             kWG_inv<KF, D>(xji, r, invHi, Wj, gWj);
-            Vec<D> gradw_j = crk_grad<D>(xji, Wj, gWj, Aj, Bj, gAj, gBj);
+            Vec<D> gradw_j = crk_grad<D>(xji, Wj, gWj, pj.A, pj.B, pj.gA, pj.gB);
             Vec<D> gij;
             #pragma unroll
             for (int a = 0; a < D; ++a) gij.v[a] = 0.5f * (gradw_i.v[a] - gradw_j.v[a]);
@@ -854,7 +966,7 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
             float Qa = rhoi * (-P.C_l * ci * mia + P.C_q * mia * mia) + rhoj * (-P.C_l * cj * mja + P.C_q * mja * mja);
             float Qd = rhoi * (-P.C_l * ci * mid + P.C_q * mid * mid) + rhoj * (-P.C_l * cj * mjd + P.C_q * mjd * mjd);
             // accel.py:228-249 (mu_ij = 1 there)
-            const float w = Vj * Vi_m;   // V_i V_j / m_i
+            const float w = pj.V * Vi_m;   // V_i V_j / m_i
             Vec<D> pt, vt;
             float dotu = 0.f;
             #pragma unroll
@@ -862,7 +974,7 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
                 pt.v[a] = -(Pi + Pj) * gij.v[a] * w;
                 vt.v[a] = -Qa * gij.v[a] * w;
                 acc[a].add(pt.v[a] + vt.v[a], comp);
-                dotu += (vi.v[a] - vj.v[a]) * gij.v[a];
+                dotu += (pi.v.v[a] - pj.v.v[a]) * gij.v[a];
             }
             if (ap) store_vec<D>(ap, k, pt);
             if (av) store_vec<D>(av, k, vt);
@@ -882,8 +994,14 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
     if (dvdt) store_vec<D>(dvdt, g.i, ov);
     if (dudt) dudt[g.i] = od;
     if (dEdt) {
-        const Vec<D> vi = load_vec<D>(v, g.i);
         const float mi = m[g.i];
+        Vec<D> vi;
+        if constexpr (REC) {
+            #pragma unroll
+            for (int a = 0; a < D; ++a) vi.v[a] = __ldg(rec + (size_t)g.i * CrkRec<D>::R + CrkRec<D>::V + a);
+        } else {
+            vi = load_vec<D>(v, g.i);
+        }
         dEdt[g.i] = mi * dot<D>(vi, ov) + mi * od;
     }
 }
@@ -1320,11 +1438,12 @@ int sph_switch_balsara(const SphParams* p, int64_t n, const float* DvDx, const f
     return check_launch("sph_switch_balsara");
 }
 
-int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
-                       const float* V, const float* A, const float* B, const float* gradA, const float* gradB,
-                       const float* v, const float* c, const float* Pr, const float* DvDx, const int32_t* offs,
-                       const int32_t* cnt, const int32_t* list, const int32_t* verlet_cnt, float* dvdt_out, float* dudt_out,
-                       float* dEdt_out, float* ap_ij, float* av_ij, void* stream) {
+static int crk_accel_dudt_impl(const SphParams* p, int64_t n, const float* x, const float* H, const float* m,
+                               const float* rho, const float* V, const float* A, const float* B, const float* gradA,
+                               const float* gradB, const float* v, const float* c, const float* Pr, const float* DvDx,
+                               const int32_t* offs, const int32_t* cnt, const int32_t* list, const int32_t* verlet_cnt,
+                               float* dvdt_out, float* dudt_out, float* dEdt_out, float* ap_ij, float* av_ij, float* records,
+                               void* stream, const char* name) {
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(V); WSPH_CHECK_PTR(A);
     WSPH_CHECK_PTR(B); WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(c); WSPH_CHECK_PTR(Pr);
@@ -1333,11 +1452,46 @@ int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const floa
         (rc = check_align_vec(P, gradA, "gradA")) || (rc = check_align_vec(P, dvdt_out, "dvdt")) ||
         (rc = check_align_vec(P, ap_ij, "ap_ij")) || (rc = check_align_vec(P, av_ij, "av_ij")))
         return rc;
-    wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_crk_accel_dudt<KF, D, G_ACCEL><<<grid_g<G_ACCEL>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
-                                                                                                          Pr, DvDx, offs, cnt, list, verlet_cnt, dvdt_out,
-                                                                                                          dudt_out, dEdt_out, ap_ij, av_ij)));
-    return check_launch("sph_crk_accel_dudt");
+    if (records && (reinterpret_cast<uintptr_t>(records) & 15))
+        return set_error(SPH_ERR_BAD_ARG, "%s: records must be 16-byte aligned", name);
+    if (records) {
+        wsph::count_launch();
+        WSPH_DISPATCH_DS(*p, (k_crk_pack<D><<<(unsigned)((n + 255) / 256), 256, 0, s>>>((int)n, x, H, rho, V, A, B, gradA, gradB, v, c,
+                                                                                       Pr, DvDx, records)));
+        wsph::count_launch();
+        WSPH_DISPATCH_KDS(*p, (k_crk_accel_dudt<KF, D, G_ACCEL, true><<<grid_g<G_ACCEL>(n), PAIR_BLOCK, 0, s>>>(
+                                  (int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c, Pr, DvDx, records, offs, cnt, list,
+                                  verlet_cnt, dvdt_out, dudt_out, dEdt_out, ap_ij, av_ij)));
+    } else {
+        wsph::count_launch();
+        WSPH_DISPATCH_KDS(*p, (k_crk_accel_dudt<KF, D, G_ACCEL, false><<<grid_g<G_ACCEL>(n), PAIR_BLOCK, 0, s>>>(
+                                  (int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c, Pr, DvDx, nullptr, offs, cnt, list,
+                                  verlet_cnt, dvdt_out, dudt_out, dEdt_out, ap_ij, av_ij)));
+    }
+    return check_launch(name);
+}
+
+int sph_crk_accel_dudt(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
+                       const float* V, const float* A, const float* B, const float* gradA, const float* gradB,
+                       const float* v, const float* c, const float* Pr, const float* DvDx, const int32_t* offs,
+                       const int32_t* cnt, const int32_t* list, const int32_t* verlet_cnt, float* dvdt_out, float* dudt_out,
+                       float* dEdt_out, float* ap_ij, float* av_ij, void* stream) {
+    return crk_accel_dudt_impl(p, n, x, H, m, rho, V, A, B, gradA, gradB, v, c, Pr, DvDx, offs, cnt, list, verlet_cnt, dvdt_out,
+                               dudt_out, dEdt_out, ap_ij, av_ij, nullptr, stream, "sph_crk_accel_dudt");
+}
+
+int sph_crk_record_floats(int32_t dim) {
+    return dim == 1 ? CrkRec<1>::R : dim == 2 ? CrkRec<2>::R : dim == 3 ? CrkRec<3>::R : 0;
+}
+
+int sph_crk_accel_dudt_packed(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
+                              const float* V, const float* A, const float* B, const float* gradA, const float* gradB,
+                              const float* v, const float* c, const float* Pr, const float* DvDx, const int32_t* offs,
+                              const int32_t* cnt, const int32_t* list, const int32_t* verlet_cnt, float* dvdt_out,
+                              float* dudt_out, float* dEdt_out, float* ap_ij, float* av_ij, float* records, void* stream) {
+    WSPH_CHECK_PTR(records);
+    return crk_accel_dudt_impl(p, n, x, H, m, rho, V, A, B, gradA, gradB, v, c, Pr, DvDx, offs, cnt, list, verlet_cnt, dvdt_out,
+                               dudt_out, dEdt_out, ap_ij, av_ij, records, stream, "sph_crk_accel_dudt_packed");
 }
 
 int sph_crk_accel(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,

@@ -10,9 +10,10 @@ namespace wsph {
 // pinv(A) = sum_k v_k U_k^T / sigma_k^2 over sigma_k > rtol * sigma_max.  With
 // rtol = D * FLT_EPSILON this is torch.linalg.pinv's default cutoff for a float32 input
 // (CullenHopkins.py:27, liu/interp.py:31).  The sweep count is bounded; D <= 4 converges in a few
-// sweeps.
+// sweeps.  With smin_out the smallest singular value is written there (for a symmetric A, its
+// smallest |eigenvalue|).
 template <int D>
-__device__ __forceinline__ void pinv_jacobi(const double (&A)[D][D], double (&P)[D][D], double rtol) {
+__device__ __forceinline__ void pinv_jacobi(const double (&A)[D][D], double (&P)[D][D], double rtol, double* smin_out = nullptr) {
     double U[D][D], V[D][D];
     #pragma unroll
     for (int a = 0; a < D; ++a)
@@ -49,6 +50,12 @@ __device__ __forceinline__ void pinv_jacobi(const double (&A)[D][D], double (&P)
         #pragma unroll
         for (int r = 0; r < D; ++r) s2[k] += U[r][k] * U[r][k];
         smax = fmax(smax, sqrt(s2[k]));
+    }
+    if (smin_out) {
+        double smin = sqrt(s2[0]);
+        #pragma unroll
+        for (int k = 1; k < D; ++k) smin = fmin(smin, sqrt(s2[k]));
+        *smin_out = smin;
     }
     const double cut = rtol * smax;
     #pragma unroll

@@ -30,6 +30,7 @@ from typing import Any, Optional
 import numpy as np
 import torch
 
+from . import ops
 from .core import AdjacencyList
 from .enumTypes import CompressibleSPHScheme, IncompressibleSPHScheme, WeaklyCompressibleSPHScheme
 from .integrators import StageRecord
@@ -183,13 +184,20 @@ def dumpAdjacency(adjacency: AdjacencyList, adjacencyGroup) -> None:
     adjacencyGroup.attrs["dim"] = int(adjacency._dim)
 
 
-def dumpState(state, stateGroup) -> None:
+_PAIR_FIELDS = ("ap_ij", "av_ij")
+
+
+def dumpState(state, stateGroup, adjacency: Optional[AdjacencyList] = None) -> None:
     """io.py:22-33: tensors as datasets, None as the attribute 'None', other values as
-    attributes."""
+    attributes.  Pairwise arrays that the step wrote over the interacting prefixes of
+    ``adjacency``'s rows are written in the reference's layout (zeros past them)."""
     for fieldName in state.__dict__.keys():
         if fieldName.startswith("_"):
             continue
         fieldValue = getattr(state, fieldName)
+        if fieldName in _PAIR_FIELDS and isinstance(fieldValue, torch.Tensor) and adjacency is not None and \
+                fieldValue.shape[0] == adjacency.nnz:
+            fieldValue, = ops.pair_reference_layout(adjacency, fieldValue)
         if isinstance(fieldValue, torch.Tensor):
             stateGroup.create_dataset(fieldName, data=_np(fieldValue))
         elif fieldValue is None:
@@ -202,12 +210,13 @@ def dumpStage(stage, stageGroups, index: int, SimulationState, exportStagesAdjac
     """io.py:35-58."""
     stageGroups[index].attrs["index"] = index
     auxGroup = stageGroups[index].create_group("aux")
+    stageAdjacency = next((a for a in stage.aux if isinstance(a, AdjacencyList)), None)
     for auxIndex, aux in enumerate(stage.aux):
         if isinstance(aux, AdjacencyList):
             if exportStagesAdjacency:
                 dumpAdjacency(aux, auxGroup.create_group(f"{auxIndex}_adjacency"))
         elif isinstance(aux, SimulationState):
-            dumpState(aux, auxGroup.create_group(f"{auxIndex}_state"))
+            dumpState(aux, auxGroup.create_group(f"{auxIndex}_state"), stageAdjacency)
         else:
             print(f"Unsupported aux type: {type(aux)}")
     for updateKey, updateValue in stage.update.__dict__.items():
@@ -230,7 +239,7 @@ def exportSimulationSystem(exportPath, tag, scheme, system: Any, exportAdjacency
     out.attrs["time"] = system.t if isinstance(system.t, float) else float(system.t)
     if system.adjacency is not None:
         dumpAdjacency(system.adjacency, out.create_group("adjacency"))
-    dumpState(system.state, out.create_group("state"))
+    dumpState(system.state, out.create_group("state"), system.adjacency)
     if stages is not None:
         stageGroups = out.create_group("stages")
         groups = []

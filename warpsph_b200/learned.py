@@ -11,8 +11,10 @@ gradient and ``sph_mlp_adam`` for the update.  The solve then iterates from that
 to the same tolerance, so it remains both the fallback and the judge of the network's
 error (init_mode 1 of the solver).
 
-``DamBreak2D`` is a small incompressible dam break run entirely by the library's
-kernels. Its parts:
+``DamBreakMDBC`` is the dam break of the warm start in 3D (or 2D) with the reference's
+mDBC wall particles and its DFSPH step order (the divergence-free solve in the step, the
+density solve in the finalize).  ``DamBreak2D`` is the earlier small 2D stand-in, run
+entirely by the library's kernels. Its parts:
   * Fluid column: the column sits in a tank lined with three layers of fixed boundary
     particles. These take part in every sum and are solved like fluid, but never move.
   * Step: the density solve, then the divergence-free solve on the predicted
@@ -250,14 +252,16 @@ class DamBreakMDBC:
     a column[:dim] fluid block in the corner of an open tank[:dim] tank (axis 1 vertical),
     three wall layers with one mirrored ghost point per wall particle (cases.tank_particles).
 
-    Each step: the gather density of fluid and walls; the mDBC wall densities
-    (sph_mdbc_density, the Liu-Liu sums at the ghost points over a list of every particle);
-    the no-penetration shift (sph_mdbc_nopen_shift) added to gravity over dt; the density
-    solve; the divergence-free solve on the predicted velocity; symplectic Euler for the
-    fluid.  The walls take part in both solves with their mDBC densities and zero
-    velocities and never move.  rho0 = 1 for the reason DamBreak2D gives; masses are set so
-    that an interior fluid particle of the lattice sums to rho0.  ``collect`` and
-    ``compare`` work as in DamBreak2D."""
+    Each step follows the reference's DFSPH (``step``): the gather density of fluid and
+    walls with the walls' replaced by the mDBC pass (sph_mdbc_density, the Liu-Liu sums at
+    the ghost points over a list of every particle); the no-penetration shift
+    (sph_mdbc_nopen_shift) added to gravity over dt; the divergence-free solve; explicit
+    Euler for the fluid; then the finalize's density solve at the new positions, whose
+    acceleration shifts the fluid by dt^2 a_p.  The walls take part in both solves with
+    their mDBC densities and zero velocities and never move.  rho0 = 1 for the reason
+    DamBreak2D gives; masses are set so that an interior fluid particle of the lattice sums
+    to rho0.  The kinematic viscosity of water (1e-6 m^2/s) is left out: its force, of
+    order nu |v| / dx^2, is below 0.5 % of gravity at the spacings used here."""
     dim: int = 3
     column: tuple = (0.5, 1.0, 0.5)
     tank: tuple = (1.6, 1.2, 0.6)
@@ -328,9 +332,13 @@ class DamBreakMDBC:
         S, k = self.state, self.nfw
         return ops.jacobi_solve(self.params, mode, cfg, S["x"][:k], S["H"][:k], S["m"][:k], rho, v, dvdt, p_init, self.dt, self.adj)
 
-    def _arm(self, mode, solver: RelaxedJacobiSolverConfig, v, dvdt, p_prev, rho, net: Optional[WarmStartMLP]) -> SolveStats:
+    def _arm(self, mode, solver: RelaxedJacobiSolverConfig, v, dvdt, p_prev, rho, net: Optional[WarmStartMLP],
+             previous: bool = False) -> SolveStats:
+        """One solve of the current state from the plain guess (the reference's rule), the
+        learned guess (``net``) or, with ``previous``, the previous step's pressure as it is;
+        timed on the GPU including the guess."""
         S, k = self.state, self.nfw
-        cfg = jacobi_config(solver, self.rho0, learned_init=net is not None)
+        cfg = jacobi_config(solver, self.rho0, learned_init=net is not None or previous)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         p0 = p_prev
@@ -354,48 +362,74 @@ class DamBreakMDBC:
                                  self.sound_speed, self.gravity)
         return r_all[:k].contiguous()
 
-    def step(self, driver: tuple, collect: Optional[dict] = None, compare: Optional[dict] = None):
+    def driver(self):
+        """Solves that advance the case: the density solve to a tenth of the evaluation
+        tolerance (3000 iterations at most), the divergence-free solve to half of its
+        per-step tolerance in at most 200 iterations (run much longer, the reference's
+        divergence-free Jacobi iteration, which has no free-surface condition and a
+        zero-mean pressure gauge, grows again in a free-surface column)."""
+        rho, df = solver_configs(self.rho0, 1e-5, 5e-4, 3000, dt=self.dt)
+        df.maxIterations = 200
+        return rho, df
+
+    def _solve_mode(self, mode, key, v, dvdt, rho, solver, collect, compare):
+        """Compare arms (``compare``), features (``collect``), then the driver solve from the
+        previous pressure; stores the pressure under ``key`` and returns the acceleration."""
         S, k = self.state, self.nfw
+        dcfg = jacobi_config(solver, self.rho0, learned_init=True)
+        if compare is not None:
+            ev = compare["solvers"][0] if mode == ops.DENSITY else compare["solvers"][1]
+            net = compare["nets"][0] if mode == ops.DENSITY else compare["nets"][1]
+            compare["stats"].append(("plain", self._arm(mode, ev, v, dvdt, S[key], rho, None)))
+            compare["stats"].append(("learned", self._arm(mode, ev, v, dvdt, S[key], rho, net)))
+            if compare.get("previous"):
+                compare["stats"].append(("previous", self._arm(mode, ev, v, dvdt, S[key], rho, None, previous=True)))
+        if collect is not None:
+            f, sc = ops.dfsph_features(self.params, mode, dcfg, S["x"][:k], S["H"][:k], S["m"][:k], rho, v, dvdt, S[key], self.dt,
+                                       self.adj)
+        pr, acc, hist, it, st = self._solve(mode, dcfg, v, dvdt, S[key], rho)
+        # a solve whose source vanishes (a column at rest) has no pressure scale and teaches nothing
+        if collect is not None and float(sc.item()) > 1e-20:
+            collect.setdefault(("feats", mode), []).append(f[: self.n_fluid])
+            collect.setdefault(("target", mode), []).append((pr / sc)[: self.n_fluid])
+        S[key] = pr
+        return acc
+
+    def step(self, driver: tuple, collect: Optional[dict] = None, compare: Optional[dict] = None):
+        """One explicit-Euler step of the reference's DFSPH with mDBC walls: the step of
+        schemes/dfsph.py:27-186 (wall densities, zero wall velocities, no-penetration
+        shift over dt added to gravity, the divergence-free solve on v + dt dv/dt, the
+        update with zero wall rows) and the finalize of systems/incompressible.py:212-249
+        (the density at the new positions, the density solve with dv/dt = 0, and the
+        position shift dt^2 a_p; velocities keep the step's values).  ``driver``,
+        ``collect`` and ``compare`` as in DamBreak2D; samples are taken of fluid
+        particles only."""
+        S, k, nf = self.state, self.nfw, self.n_fluid
         rho = self.densities()
         zero = torch.zeros_like(S["v"])
         nopen = ops.mdbc_nopen_shift(self.params, S["x"][:k], S["H"][:k], S["m"][:k], S["v"], S["kinds"][:k], S["goff"][:k], self.adj)
         ext = (self.gvec + nopen / self.dt).contiguous()
-        out = {}
-        for mode, key in ((ops.DENSITY, "p_rho"), (ops.DIVERGENCE_FREE, "p_df")):
-            if mode == ops.DENSITY:
-                v, dvdt = S["v"], ext
-            else:
-                v = torch.where(self.fluid[:, None], S["v"] + self.dt * (ext + out[ops.DENSITY]), zero).contiguous()
-                dvdt = zero
-                vstar = v
-            solver = driver[0] if mode == ops.DENSITY else driver[1]
-            dcfg = jacobi_config(solver, self.rho0, learned_init=True)
-            if compare is not None:
-                ev = compare["solvers"][0] if mode == ops.DENSITY else compare["solvers"][1]
-                net = compare["nets"][0] if mode == ops.DENSITY else compare["nets"][1]
-                compare["stats"].append(("plain", self._arm(mode, ev, v, dvdt, S[key], rho, None)))
-                compare["stats"].append(("learned", self._arm(mode, ev, v, dvdt, S[key], rho, net)))
-            if collect is not None:
-                f, sc = ops.dfsph_features(self.params, mode, dcfg, S["x"][:k], S["H"][:k], S["m"][:k], rho, v, dvdt, S[key], self.dt,
-                                           self.adj)
-            pr, acc, hist, it, st = self._solve(mode, dcfg, v, dvdt, S[key], rho)
-            out[mode] = acc
-            if collect is not None:
-                collect.setdefault(("feats", mode), []).append(f)
-                collect.setdefault(("target", mode), []).append(pr / sc)
-            S[key] = pr
-        v = torch.where(self.fluid[:, None], vstar + self.dt * out[ops.DIVERGENCE_FREE], zero)
-        S["x"] = torch.cat([S["x"][: self.n_fluid] + self.dt * v[: self.n_fluid], S["x"][self.n_fluid:]]).contiguous()
-        S["v"] = v.contiguous()
+        a_df = self._solve_mode(ops.DIVERGENCE_FREE, "p_df", S["v"], ext, rho, driver[1], collect, compare)
+        v = torch.where(self.fluid[:, None], S["v"] + self.dt * (ext + a_df), zero).contiguous()
+        S["v"] = v
+        S["x"] = torch.cat([S["x"][:nf] + self.dt * v[:nf], S["x"][nf:]]).contiguous()
+        rho = self.densities()
+        a_rho = self._solve_mode(ops.DENSITY, "p_rho", v, zero, rho, driver[0], collect, compare)
+        S["x"] = torch.cat([S["x"][:nf] + (self.dt * self.dt) * a_rho[:nf], S["x"][nf:]]).contiguous()
         self.t += self.dt
 
 
-def solver_configs(rho0: float, density_tol_frac: float = 1e-4, div_tol_frac: float = 1e-3, max_iterations: int = 400):
+def solver_configs(rho0: float, density_tol_frac: float = 1e-4, div_tol_frac: float = 1e-3, max_iterations: int = 400,
+                   dt: Optional[float] = None):
     """The reference's relaxed-Jacobi settings (solver.py:15-28) with the tolerances of
-    a 0.01 % density error and a 0.1 % divergence error, both normalised by rho0."""
+    a 0.01 % density error and a 0.1 % divergence error, both normalised by rho0.  The
+    divergence-free solve's residual is a density rate (rho0 div v, in rho0 per second);
+    with ``dt`` its tolerance is the 0.1 % per time step of Bender and Koschier's DFSPH
+    (IEEE TVCG 2017), div_tol_frac rho0 / dt, else div_tol_frac rho0 per second."""
     return (RelaxedJacobiSolverConfig(minIterations=2, maxIterations=max_iterations, tolerance=density_tol_frac * rho0,
                                       relaxationFactor=0.3),
-            RelaxedJacobiSolverConfig(minIterations=2, maxIterations=max_iterations, tolerance=div_tol_frac * rho0,
+            RelaxedJacobiSolverConfig(minIterations=2, maxIterations=max_iterations,
+                                      tolerance=div_tol_frac * rho0 / (dt if dt else 1.0),
                                       relaxationFactor=0.3))
 
 
@@ -419,45 +453,67 @@ def dam_break_mdbc_3d(w, h, seed, dx, dt, device):
     return DamBreakMDBC(dim=3, column=(w, h, w), dx=dx, dt=dt, device=device, seed=seed)
 
 
+def _driver(case):
+    return case.driver() if hasattr(case, "driver") else driver_configs(case.rho0)
+
+
 def generate_samples(geometries, steps: int, device="cuda", dx: float = 0.02, dt: float = 1e-3, make_case=dam_break_2d,
-                     collect_every: int = 1):
+                     collect_every: int = 1, max_samples: Optional[int] = None, seed: int = 0):
     """(features, targets) per solve mode from dam-break trajectories; ``geometries`` is a
-    list of (width, height, seed); samples are collected every ``collect_every`` steps."""
+    list of (width, height, seed); samples are collected every ``collect_every`` steps;
+    rows with a non-finite feature or target are dropped, and with ``max_samples`` a
+    seeded random subset of that many rows is kept per mode."""
     collect: dict = {}
-    for (w, h, seed) in geometries:
-        case = make_case(w, h, seed, dx, dt, device)
-        drv = driver_configs(case.rho0)
+    for (w, h, gseed) in geometries:
+        case = make_case(w, h, gseed, dx, dt, device)
+        drv = _driver(case)
         for s_ in range(steps):
             case.step(drv, collect=collect if (s_ + 1) % collect_every == 0 else None)
     out = {}
+    gen = torch.Generator(device="cpu").manual_seed(seed)
     for mode in (0, 1):
-        out[mode] = (torch.cat(collect[("feats", mode)]).contiguous(), torch.cat(collect[("target", mode)]).contiguous())
+        f, t = torch.cat(collect[("feats", mode)]), torch.cat(collect[("target", mode)])
+        ok = torch.isfinite(f).all(dim=1) & torch.isfinite(t)
+        if not bool(ok.all()):
+            f, t = f[ok], t[ok]
+        if max_samples is not None and f.shape[0] > max_samples:
+            keep = torch.randperm(f.shape[0], generator=gen)[:max_samples].to(f.device)
+            f, t = f[keep], t[keep]
+        out[mode] = (f.contiguous(), t.contiguous())
     return out
 
 
 def compare_warm_starts(geometries, steps: int, nets, device="cuda", dx: float = 0.02, dt: float = 1e-3, skip: int = 2,
-                        max_iterations: int = 2000, df_budget: int = 32, make_case=dam_break_2d):
-    """Plain against learned initial pressure on the same states, after the first ``skip``
-    steps of each trajectory:
+                        max_iterations: int = 2000, df_budget: Optional[int] = 32, make_case=dam_break_2d,
+                        compare_every: int = 1, cases: Optional[list] = None, previous: bool = False):
+    """Plain against learned initial pressure on the same states, every ``compare_every``
+    steps after the first ``skip`` steps of each trajectory:
       density solve: summed iterations and GPU ms to the 0.01 % tolerance (cap
         ``max_iterations``), and how many solves missed it;
-      divergence-free solve: the error after the reference's budget of ``df_budget``
-        iterations (solver.py:22-28, maxIterations 32), summed, and the GPU ms."""
-    tot = {"density": {"plain": [0, 0.0, 0], "learned": [0, 0.0, 0]},
-           "divergence_free": {"plain": [0.0, 0.0, 0], "learned": [0.0, 0.0, 0]}}
-    for (w, h, seed) in geometries:
-        case = make_case(w, h, seed, dx, dt, device)
-        drv = driver_configs(case.rho0)
-        rho_ev, df_ev = solver_configs(case.rho0, max_iterations=max_iterations)
-        df_ev = RelaxedJacobiSolverConfig(minIterations=df_budget, maxIterations=df_budget, tolerance=0.0,
-                                          relaxationFactor=df_ev.relaxationFactor)
+      divergence-free solve: with ``df_budget`` the error after the reference's budget of
+        that many iterations (solver.py:22-28, maxIterations 32), summed, and the GPU ms;
+        with ``df_budget`` None as the density solve, to the 0.1 % per-step tolerance.
+    ``cases`` may hold prebuilt cases (one per geometry) instead of building them; with
+    ``previous`` (cases that support it) a third arm starts from the previous step's
+    pressure as it is.  Returns the sums and the per-solve statistics."""
+    tot = {"density": {"plain": [0, 0.0, 0], "learned": [0, 0.0, 0], "previous": [0, 0.0, 0]},
+           "divergence_free": {"plain": [0.0, 0.0, 0], "learned": [0.0, 0.0, 0], "previous": [0.0, 0.0, 0]}, "solves": []}
+    for gi, (w, h, seed) in enumerate(geometries):
+        case = cases[gi] if cases is not None else make_case(w, h, seed, dx, dt, device)
+        drv = _driver(case)
+        rho_ev, df_ev = solver_configs(case.rho0, max_iterations=max_iterations, dt=None if df_budget else case.dt)
+        if df_budget:
+            df_ev = RelaxedJacobiSolverConfig(minIterations=df_budget, maxIterations=df_budget, tolerance=0.0,
+                                              relaxationFactor=df_ev.relaxationFactor)
         for k in range(steps):
-            cmp = {"solvers": (rho_ev, df_ev), "nets": nets, "stats": []} if k >= skip else None
+            on = k >= skip and (k - skip) % compare_every == 0
+            cmp = {"solvers": (rho_ev, df_ev), "nets": nets, "stats": [], "previous": previous} if on else None
             case.step(drv, compare=cmp)
             if cmp is not None:
                 for arm, st in cmp["stats"]:
-                    if st.mode == ops.DENSITY:
-                        t = tot["density"][arm]
+                    tot["solves"].append((gi, k, arm, st))
+                    if st.mode == ops.DENSITY or not df_budget:
+                        t = tot["density" if st.mode == ops.DENSITY else "divergence_free"][arm]
                         t[0] += st.iterations; t[1] += st.ms; t[2] += int(not st.converged)
                     else:
                         t = tot["divergence_free"][arm]

@@ -475,22 +475,56 @@ def switch_balsara(params, DvDx, c):
 
 
 def crk_accel_dudt(params, x, H, m, rho, V, crk: CRKState, v, c, P, DvDx, adj: AdjacencyList, pair_arrays: bool = True,
-                   want_dEdt: bool = False):
-    """Fused CRK momentum and energy RHS over the interacting prefixes; the pairwise
-    accelerations are returned in Verlet-entry order (zeros for the rest of each row).
+                   want_dEdt: bool = False, reference_layout: bool = True):
+    """Fused CRK momentum and energy RHS over the interacting prefixes, gathering each
+    neighbour from a packed per-particle record (sph_crk_accel_dudt_packed).  The
+    pairwise accelerations are returned in Verlet-entry order.  With
+    ``reference_layout`` the rest of each row is written as zeros, the reference's
+    layout; without it only the interacting prefix is written and the rest is left
+    unspecified (what the library's own readers of these arrays need: the energy
+    partition and the compatible-energy finalize read the prefix only).
     Returns (dvdt, dudt, ap, av), and dE/dt last when ``want_dEdt``."""
     n, d = H.shape[0], int(params.dim)
     dvdt, dudt = _empty((n, d), H), _empty(n, H)
     dEdt = _empty(n, H) if want_dEdt else None
     ap = _pair_empty(adj.nnz, d, H) if pair_arrays else None
     av = _pair_empty(adj.nnz, d, H) if pair_arrays else None
+    recs = _empty(n * crk_record_floats(d), H)
     with _timed("crk_accel_dudt"):
         rows = _lists(params, adj, True)
-        check(_capi.lib().sph_crk_accel_dudt(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(V), fptr(crk.A), fptr(crk.B),
-                                             fptr(crk.gradA), fptr(crk.gradB), fptr(v), fptr(c), fptr(P), fptr(DvDx), *rows,
-                                             iptr(adj.numNeighbors), ptr(dvdt), ptr(dudt), ptr(dEdt), ptr(ap), ptr(av),
-                                             stream_ptr(H.device)), "sph_crk_accel_dudt")
+        check(_capi.lib().sph_crk_accel_dudt_packed(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(V), fptr(crk.A),
+                                                    fptr(crk.B), fptr(crk.gradA), fptr(crk.gradB), fptr(v), fptr(c), fptr(P),
+                                                    fptr(DvDx), *rows, iptr(adj.numNeighbors) if reference_layout else None,
+                                                    ptr(dvdt), ptr(dudt), ptr(dEdt), ptr(ap), ptr(av), ptr(recs),
+                                                    stream_ptr(H.device)), "sph_crk_accel_dudt_packed")
     return (dvdt, dudt, ap, av, dEdt) if want_dEdt else (dvdt, dudt, ap, av)
+
+
+def crk_record_floats(dim: int) -> int:
+    """Floats per particle of the packed record of the CRK accel pass."""
+    return int(_capi.lib().sph_crk_record_floats(int(dim)))
+
+
+def pair_reference_layout(adj: AdjacencyList, *arrays):
+    """Copies of per-entry arrays with the entries past each row's interacting prefix set
+    to zero: the reference's layout of ap_ij / av_ij, for arrays written over the
+    prefixes only.  Arrays of lists without interacting prefixes are returned as is."""
+    if adj is None or adj.interCounts is None or getattr(adj, "_pending", None) is not None:
+        return arrays
+    n = adj.numRows
+    dev = adj.neighborOffsets.device
+    rows = torch.repeat_interleave(torch.arange(n, device=dev), adj.numNeighbors.long(), output_size=adj.nnz)
+    pos = torch.arange(adj.nnz, device=dev) - adj.neighborOffsets.long()[rows]
+    tail = pos >= adj.interCounts.long()[rows]
+    out = []
+    for a in arrays:
+        if a is None:
+            out.append(None)
+            continue
+        b = a[: adj.nnz].clone()
+        b[tail] = 0
+        out.append(b)
+    return tuple(out)
 
 
 def compsph_prep(params, x, H, m, rho, v, adj: AdjacencyList, grad_h: bool = True, want_div: bool = True,
@@ -508,9 +542,11 @@ def compsph_prep(params, x, H, m, rho, v, adj: AdjacencyList, grad_h: bool = Tru
 
 
 def compsph_accel_dudt(params, x, H, m, rho, v, c, alpha, P, omega, adj: AdjacencyList, pair_arrays: bool = True,
-                       want_dEdt: bool = True):
+                       want_dEdt: bool = True, reference_layout: bool = True):
     """Fused CompSPH momentum and energy RHS; returns (dvdt, dudt, dEdt, ap_ij, av_ij) with
-    the pairwise accelerations in Verlet-entry order (zeros beyond the support)."""
+    the pairwise accelerations in Verlet-entry order: zeros beyond the support with
+    ``reference_layout``, else written over the interacting prefixes only (as
+    crk_accel_dudt)."""
     n, d = H.shape[0], int(params.dim)
     dvdt, dudt = _empty((n, d), H), _empty(n, H)
     dEdt = _empty(n, H) if want_dEdt else None
@@ -519,7 +555,7 @@ def compsph_accel_dudt(params, x, H, m, rho, v, c, alpha, P, omega, adj: Adjacen
     with _timed("compsph_accel_dudt"):
         rows = _lists(params, adj, True)
         check(_capi.lib().sph_compsph_accel_dudt(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(v), fptr(c), fptr(alpha),
-                                                 fptr(P), fptr(omega), *rows, iptr(adj.numNeighbors), ptr(dvdt), ptr(dudt),
+                                                 fptr(P), fptr(omega), *rows, iptr(adj.numNeighbors) if reference_layout else None, ptr(dvdt), ptr(dudt),
                                                  ptr(dEdt), ptr(ap), ptr(av), stream_ptr(H.device)), "sph_compsph_accel_dudt")
     return dvdt, dudt, dEdt, ap, av
 
@@ -584,12 +620,13 @@ def finalize_compatible_energy(params, weights, dt, v0, u0, stages):
     u = _empty(n, u0)
     scratch = _empty(n * (1 + d), u0)
     ns = len(stages)
-    # each stage's pairwise arrays are zero beyond the interacting prefix of its rows
-    inter = all(s[1].interCounts is not None and s[1]._pending is None for s in stages)
+    # a stage whose list has interacting prefixes is walked over them (its pairwise
+    # arrays carry no interaction past them, and may be left unwritten there)
+    inter = [s[1].interCounts is not None and s[1]._pending is None for s in stages]
     params.list_stride = 1
     arrs = [_capi.ptr_array([fptr(s[0]) for s in stages]),
             _capi.ptr_array([iptr(s[1].neighborOffsets) for s in stages]),
-            _capi.ptr_array([iptr(s[1].interCounts if inter else s[1].numNeighbors) for s in stages]),
+            _capi.ptr_array([iptr(s[1].interCounts if it else s[1].numNeighbors) for s, it in zip(stages, inter)]),
             _capi.ptr_array([iptr(s[1].neighborList) for s in stages]),
             _capi.ptr_array([fptr(s[2]) for s in stages]),
             _capi.ptr_array([fptr(s[3]) for s in stages]),

@@ -167,7 +167,7 @@ def crkSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams:
     # (dE/dt = m v.dv/dt + m du/dt of crkSPH.py:330 is written by the same pass)
     dvdt, dudt, S.ap_ij, S.av_ij, dEdt = ops.crk_accel_dudt(params, S.positions, S.supports, S.masses, S.densities, V, crk,
                                                             S.velocities, S.soundspeeds, S.pressures, DvDx, adjacency,
-                                                            want_dEdt=True)
+                                                            want_dEdt=True, reference_layout=False)
     # crkSPH.py:324-337
     S.divergence = -drhodt / S.densities
     update = CompressibleSystemUpdate(dxdt=S.velocities, dvdt=dvdt, dudt=dudt, drhodt=drhodt, dEdt=dEdt, passive=None)
