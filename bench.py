@@ -145,10 +145,11 @@ def bytes_accel_dudt(d: int, K: float) -> float:
     return (16 * d + 40 + 8 * d * d) + 4 * d + 4 + K * (4 + 8 * d)
 
 
-# DRAM bytes (read + write) of one k_crk_accel_dudt launch from an ncu capture of the
-# 384^2 case (profiles/k_crk_accel_dudt_sedov2d_384.md), scaled to a launch of n
-# particles by particle count (the pass is per particle, so traffic grows with n).
-ACCEL_TRAFFIC_BYTES_PER_PARTICLE = (67.91e6 + 119.07e6) / 147456
+# DRAM bytes (read + write) of one accel pass on this bench's own workload (512^2), from an
+# ncu capture of dram__bytes_read.sum + dram__bytes_write.sum: k_crk_accel_dudt 131.6 MB
+# read + 132.5 MB written, and the k_crk_pack launch before it 23.1 MB read (its records
+# stay in L2 for the accel launch).  Other sizes are scaled by particle count.
+ACCEL_TRAFFIC_BYTES_PER_PARTICLE = (131.64e6 + 132.50e6 + 23.08e6) / 262144
 
 
 def load_peaks() -> dict:
@@ -255,7 +256,9 @@ def dfsph_dambreak_3d(dev, eval_dx: float = 0.005, train_dx: float = 0.025, trai
         f, tg = data[mode]
         net = learned.WarmStartMLP(dev, seed=mode)
         losses = net.fit(f, tg, epochs=25, batch=4096, lr=2e-3)
-        fit[mode] = {"samples": int(f.shape[0]), "final_mse": losses[-1], "target_variance": float(tg.var())}
+        q = torch.quantile(tg.abs().float(), torch.tensor([0.5, 0.99], device=tg.device)).tolist()
+        fit[mode] = {"samples": int(f.shape[0]), "final_mse": losses[-1], "target_variance": float(tg.var()),
+                     "target_abs_p50": q[0], "target_abs_p99": q[1]}
         nets[mode] = net
     t_fit = time.perf_counter() - t0 - t_data
     case = learned.DamBreakMDBC(dim=3, column=(0.5, 1.0, 0.5), dx=eval_dx, dt=0.1 * eval_dx, device=dev, seed=7)
@@ -521,7 +524,7 @@ def gpu_arm(args, rank: int, world: int):
     achieved = per_particle * n / (ksum["avg_ms"] / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": ACCEL_TRAFFIC_BYTES_PER_PARTICLE * n / 1e9,
-                "traffic_unit": "GB per launch (ncu dram__bytes_read+write, 384^2 capture scaled by particle count)",
+                "traffic_unit": "GB per launch of the pack + accel pass (ncu dram__bytes_read+write on this 512^2 workload)",
                 "kernel": "k_crk_accel_dudt",
                 "algorithmic_bytes_per_particle": per_particle, "model_K": 32, "measured_interacting_per_particle": K_meas,
                 "verlet_entries_per_particle": nnz_per, "avg_launch_ms": ksum["avg_ms"], "launches_timed": ksum["launches"],
@@ -541,35 +544,45 @@ def gpu_arm(args, rank: int, world: int):
     e2e = None
     if not args.no_e2e:
         fields = ["positions", "velocities", "internalEnergies", "supports", "masses", "densities", "alpha0s", "alphas", "divergence"]
+        e2e_steps = max(3, args.steps // 2)
+        # the inputs of 2 + e2e_steps consecutive steps of the run, recorded into pinned host
+        # memory beforehand: every step of the end-to-end leg uploads the state that step
+        # really starts from, so its neighbour lists are kept or rebuilt as in the
+        # device-resident run
+        traj = []
+        for _ in range(2 + e2e_steps):
+            S = state["system"].state
+            traj.append({f: getattr(S, f).detach().cpu().pin_memory() for f in fields})
+            one_step()
+        torch.cuda.synchronize()
         S = state["system"].state
-        host_in = {f: getattr(S, f).detach().cpu().pin_memory() for f in fields}
+        host_in = traj[0]
         # two pinned result buffers: step k's download may still run while step k+1 computes
         host_out = [{f: torch.empty_like(host_in[f]).pin_memory() for f in fields} for _ in range(2)]
         h2d = sum(t.numel() * t.element_size() for t in host_in.values())
         d2h = h2d
-        e2e_steps = max(3, args.steps // 2)
         comp = torch.cuda.current_stream(dev)
         copy = torch.cuda.Stream(dev)
         # two device input sets: step k+1's inputs land in one while step k reads the other
         d_in = [{f: torch.empty_like(getattr(S, f)) for f in fields} for _ in range(2)]
 
         def upload(k):
-            """Copies step k's inputs from pinned host memory on the copy stream."""
+            """Copies step k's recorded inputs from pinned host memory on the copy stream."""
             with torch.cuda.stream(copy):
                 for f in fields:
-                    d_in[k % 2][f].copy_(host_in[f], non_blocking=True)
+                    d_in[k % 2][f].copy_(traj[k][f], non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(copy)
             return ev
 
-        def run(steps):
-            ev = upload(0)
-            for k in range(steps):
+        def run(k0, steps):
+            ev = upload(k0)
+            for k in range(k0, k0 + steps):
                 comp.wait_event(ev)
                 S = state["system"].state
                 for f in fields:
                     setattr(S, f, d_in[k % 2][f])
-                if k + 1 < steps:
+                if k + 1 < k0 + steps:
                     ev = upload(k + 1)      # the next step's inputs cross while this step computes
                 one_step()
                 done = torch.cuda.Event()
@@ -583,14 +596,14 @@ def gpu_arm(args, rank: int, world: int):
                         host_out[k % 2][f].copy_(t, non_blocking=True)
             comp.wait_stream(copy)
 
-        run(2)   # untimed: settles the allocator's pools for this pattern
+        run(0, 2)   # untimed: settles the allocator's pools for this pattern
         barrier()
         torch.cuda.synchronize()
         gc.collect()
         gc.disable()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        run(e2e_steps)
+        run(2, e2e_steps)
         e1.record()
         torch.cuda.synchronize()
         gc.enable()
@@ -599,7 +612,8 @@ def gpu_arm(args, rank: int, world: int):
         if world > 1:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         e2e = {"value": n * e2e_steps * world / (float(te.item()) / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "steps": e2e_steps}
+               "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+               "inputs": "each step uploads the state it starts from, recorded from the same run beforehand"}
 
     dfsph = None
     if rank == 0 and world == 1 and not args.no_dfsph:

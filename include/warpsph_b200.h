@@ -731,6 +731,45 @@ int sph_surface_detect_color_field(const SphParams* p, int64_t n, const float* x
  * so does this.  fs_in and fs_out must not alias. */
 int sph_surface_dilate(const SphParams* p, int64_t n, const float* x, const float* H, const float* fs_in,
                        const int32_t* offs, const int32_t* cnt, const int32_t* list, float* fs_out, void* stream);
+/* Barecasco detection (wp_barecasco.py:36-453, barecascoDetection.py:22-43): the cover
+ * vector c_i = sum_j x_ij / (r_ij + 1e-14 H_i) over the pairs with W(r, max(H_i, H_j)) > 0,
+ * normals_out = c_i / |c_i| (0 for c_i = 0), count_out = the pairs with W > 0 whose
+ * acos(-n_ij . c^_i) <= threshold / 2 (j != i), or every pair when |c^_i| <= 0.5; fs_out =
+ * 1 where the count is below 0.5.  normals_out and count_out may be null. */
+int sph_surface_barecasco(const SphParams* p, int64_t n, const float* x, const float* H,
+                          const int32_t* offs, const int32_t* cnt, const int32_t* list, float threshold,
+                          float* fs_out, float* normals_out, float* count_out, void* stream);
+/* Maronne detection (wp_maronne.py:57-332, maronneDetection.py:20-80) with the given
+ * normals [n, dim]: fs_out = 1 where no neighbour j != i with r_ij < H_j lies in the
+ * circle of radius H_j / xi around T_i = x_i + n_i H_i / xi (r_ij >= sqrt(2) H_j / xi) or in
+ * the square |n_i.(x_j - T_i)| + |tau_i.(x_j - T_i)| < H_j / xi (r_ij < sqrt(2) H_j / xi),
+ * for |n_i| > 0.5; xi = p's kernel xi.  count_out (may be null) gets the count. */
+int sph_surface_maronne(const SphParams* p, int64_t n, const float* x, const float* H, const float* normals,
+                        const int32_t* offs, const int32_t* cnt, const int32_t* list, float* fs_out,
+                        float* count_out, void* stream);
+/* Colour-field-gradient detection (colorFieldGradientDetection.py:18-56): the gather
+ * difference gradient g_i of the colour field, fs_out = [|g_i| > threshold H_i / xi] and
+ * normals_out = -g_i / max(|g_i|, 1e-12) (may be null). */
+int sph_surface_detect_color_gradient(const SphParams* p, int64_t n, const float* x, const float* H,
+                                      const float* m, const float* rho, const float* color,
+                                      const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                                      float threshold, float* fs_out, float* normals_out, void* stream);
+/* Renormalisation matrices, standing in for warpSPHCore's computeRenormalizationMatrices
+ * (called at surfaceDetection/wrapper.py:21-33): M_i = sum_j V_j (x_j - x_i) (x)
+ * grad_i W(r_ij, max(H_i, H_j)), V_j = m_j / rho_j; L_out [n, dim, dim] = pinv(M_i) (FP64,
+ * cutoff dim * FLT_EPSILON * sigma_max), lambda_out [n] = the smallest |eigenvalue| of M_i.
+ * Either output may be null, not both. */
+int sph_surface_renormalization(const SphParams* p, int64_t n, const float* x, const float* H,
+                                const float* m, const float* rho, const int32_t* offs, const int32_t* cnt,
+                                const int32_t* list, float* L_out, float* lambda_out, void* stream);
+/* Normals from the renormalised gradients, normals_out = -g_i / max(|g_i|, 1e-12) with
+ * g_i = L_i sum_j V_j q_ij grad W(r_ij, H_j) (scatter support): mode 0, the lambda gradient
+ * of lambdaGrad.py:46-83 (q_ij = lambda_j - lambda_i); mode 1, Maronne's normals of
+ * maronneNormals.py:16-62 (q_ij = 1; lambdas may be null).  grad_out (may be null) gets g. */
+int sph_surface_renormalized_normals(const SphParams* p, int64_t n, int32_t mode, const float* x,
+                                     const float* H, const float* m, const float* rho, const float* L,
+                                     const float* lambdas, const int32_t* offs, const int32_t* cnt,
+                                     const int32_t* list, float* normals_out, float* grad_out, void* stream);
 
 /* ---------------------------------------------------------------- learned warm start
  * No counterpart in the reference: a per-particle MLP predicts the initial pressure of

@@ -101,6 +101,11 @@ class Oracle:
         L.oracle_surface_color_field.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_surface_detect.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, real_c, real_c, rp, rp, rp]
         L.oracle_surface_dilate.argtypes = [P, i64, rp, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_surface_barecasco.argtypes = [P, i64, rp, rp, _i32p, _i32p, _i32p, real_c, rp, rp, rp]
+        L.oracle_surface_maronne.argtypes = [P, i64, rp, rp, rp, _i32p, _i32p, _i32p, rp, rp]
+        L.oracle_surface_color_gradient.argtypes = [P, i64, rp, rp, rp, rp, rp, _i32p, _i32p, _i32p, real_c, rp, rp]
+        L.oracle_surface_moments.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
+        L.oracle_surface_renorm_normals.argtypes = [P, i64, C.c_int, rp, rp, rp, rp, rp, rpn, _i32p, _i32p, _i32p, rp, rpn]
         L.oracle_switch_hopkins_update.argtypes = [P, i64, rp, rp, rp, rp, rp, rp, rp, real_c, _i32p, _i32p, _i32p, rp, rpn]
         L.oracle_vsig.argtypes = [P, i64, rp, rp, rp, rp, _i32p, _i32p, _i32p, rp]
         L.oracle_pi_pairs.argtypes = [P, i64, rp, rp, rp, rp, rpn, rpn, rp, _i32p, _i32p, _i32p, C.c_int, C.c_int, rp]
@@ -363,6 +368,51 @@ class Oracle:
         self.lib.oracle_surface_dilate(self._p(params), len(H), self.arr(x), self.arr(H), self.arr(fs),
                                        nb["offsets"], nb["counts"], nb["list"], out)
         return out
+
+    def surface_barecasco(self, params, x, H, nb, threshold):
+        """(mask, normalised cover vectors [n, D], cone counts)"""
+        n, D = len(H), int(params.dim)
+        fs, cnt, nrm = np.zeros(n, self.dtype), np.zeros(n, self.dtype), np.zeros((n, D), self.dtype)
+        self.lib.oracle_surface_barecasco(self._p(params), n, self.arr(x), self.arr(H), nb["offsets"], nb["counts"], nb["list"],
+                                          float(threshold), fs, nrm, cnt)
+        return fs, nrm, cnt
+
+    def surface_maronne(self, params, x, H, normals, nb):
+        """(mask, counts)"""
+        n = len(H)
+        fs, cnt = np.zeros(n, self.dtype), np.zeros(n, self.dtype)
+        self.lib.oracle_surface_maronne(self._p(params), n, self.arr(x), self.arr(H), self.arr(normals), nb["offsets"], nb["counts"],
+                                        nb["list"], fs, cnt)
+        return fs, cnt
+
+    def surface_color_gradient(self, params, x, H, m, rho, c, nb, threshold):
+        """(mask, normals)"""
+        n, D = len(H), int(params.dim)
+        fs, nrm = np.zeros(n, self.dtype), np.zeros((n, D), self.dtype)
+        self.lib.oracle_surface_color_gradient(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), self.arr(c),
+                                               nb["offsets"], nb["counts"], nb["list"], float(threshold), fs, nrm)
+        return fs, nrm
+
+    def surface_renormalization(self, params, x, H, m, rho, nb):
+        """(L = pinv(M) [n, D, D] by LAPACK in FP64 with torch's FP32 cutoff, the smallest
+        |eigenvalue| of the symmetric M [n], M [n, D, D])"""
+        n, D = len(H), int(params.dim)
+        M = np.zeros((n, D, D), self.dtype)
+        self.lib.oracle_surface_moments(self._p(params), n, self.arr(x), self.arr(H), self.arr(m), self.arr(rho), nb["offsets"],
+                                        nb["counts"], nb["list"], M)
+        M64 = M.astype(np.float64)
+        L = np.linalg.pinv(M64, rcond=D * np.finfo(np.float32).eps).astype(self.dtype)
+        lam = np.abs(np.linalg.eigvalsh(0.5 * (M64 + M64.transpose(0, 2, 1)))).min(axis=1).astype(self.dtype)
+        return L, lam, M
+
+    def surface_renorm_normals(self, params, mode, x, H, m, rho, L, lam, nb):
+        """(normals, renormalised gradient)"""
+        n, D = len(H), int(params.dim)
+        nrm, g = np.zeros((n, D), self.dtype), np.zeros((n, D), self.dtype)
+        self.lib.oracle_surface_renorm_normals(self._p(params), n, int(mode), self.arr(x), self.arr(H), self.arr(m), self.arr(rho),
+                                               self.arr(L), None if lam is None else self.arr(lam), nb["offsets"], nb["counts"],
+                                               nb["list"], nrm, g)
+        return nrm, g
 
     # ------------------------------------------------------------------ mDBC
     def liu_moments(self, params, x, H, m, rho, kinds, nb):

@@ -44,12 +44,14 @@ static inline real rsqrt_safe(real x) { return (real)sqrt((double)(x > 0 ? x : 0
 #define POW powf
 #define FABS fabsf
 #define FLOOR floorf
+#define ACOS acosf
 #else
 #define SQRT sqrt
 #define EXP exp
 #define POW pow
 #define FABS fabs
 #define FLOOR floor
+#define ACOS acos
 #endif
 
 /* ------------------------------------------------------------------ parameters */
@@ -872,6 +874,165 @@ int oracle_surface_dilate(const SphParams* p, int64_t n, const real* x, const re
             if (kW(&o, rsqrt_safe(dotD(d, d, D)), H[i] > H[j] ? H[i] : H[j]) > 0) s += fs[j];
         }
         out[i] = s;
+    }
+    return 0;
+}
+
+/* Barecasco detection (modules/surfaceDetection/wp_barecasco.py:36-113, 120-236, 338-355;
+ * barecascoDetection.py:22-43): cover vector over the pairs with W(r, max(H_i, H_j)) > 0,
+ * Warp's normalize (zero for a zero vector), the cone count, mask = count < 0.5. */
+int oracle_surface_barecasco(const SphParams* p, int64_t n, const real* x, const real* H, const int32_t* offs, const int32_t* cnt,
+                             const int32_t* list, real threshold, real* fs_out, real* normals_out, real* count_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real c[3] = {0, 0, 0};
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real r = rsqrt_safe(dotD(d, d, D));
+            if (!(kW(&o, r, H[i] > H[j] ? H[i] : H[j]) > 0)) continue;
+            for (int a = 0; a < D; ++a) c[a] += d[a] / (r + (real)1e-14 * H[i]);
+        }
+        real l = SQRT(dotD(c, c, D));
+        real ch[3] = {0, 0, 0};
+        for (int a = 0; a < D; ++a) ch[a] = l > 0 ? c[a] / l : 0;
+        int degenerate = SQRT(dotD(ch, ch, D)) <= (real)0.5;
+        real count = 0;
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real r = rsqrt_safe(dotD(d, d, D));
+            if (!(kW(&o, r, H[i] > H[j] ? H[i] : H[j]) > 0)) continue;
+            real den = r + (real)1e-14 * H[i], dt = 0;
+            for (int a = 0; a < D; ++a) dt += -(d[a] / den) * ch[a];
+            if (dt > 1) dt = 1;
+            if (dt < -1) dt = -1;
+            real angle = ACOS(dt);
+            if ((angle <= threshold / 2 && j != i) || degenerate) count += 1;
+        }
+        fs_out[i] = count < (real)0.5 ? 1 : 0;
+        count_out[i] = count;
+        for (int a = 0; a < D; ++a) normals_out[i * D + a] = ch[a];
+    }
+    return 0;
+}
+
+/* Maronne detection (modules/surfaceDetection/wp_maronne.py:57-161) with given normals. */
+int oracle_surface_maronne(const SphParams* p, int64_t n, const real* x, const real* H, const real* normals, const int32_t* offs,
+                           const int32_t* cnt, const int32_t* list, real* fs_out, real* count_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+    real xk = (real)o.kxi;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        const real* ni = normals + i * D;
+        real T[3] = {0, 0, 0}, tau[3] = {0, 0, 0};
+        for (int a = 0; a < D; ++a) T[a] = x[i * D + a] + ni[a] * H[i] / xk;
+        if (D == 2) { tau[0] = -ni[1]; tau[1] = ni[0]; }
+        if (D == 3) { tau[0] = ni[1] * ni[2]; tau[1] = -ni[0] * ni[2]; tau[2] = ni[0] * ni[1]; }
+        int long_normal = rsqrt_safe(dotD(ni, ni, D)) > (real)0.5;
+        real count = 0, s2 = SQRT((real)2);
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], dt[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            real rij = rsqrt_safe(dotD(d, d, D)), hij = H[j];
+            if (rij >= hij) continue;
+            dist_vec(&o, x + (int64_t)j * D, T, dt);
+            real rjt = rsqrt_safe(dotD(dt, dt, D)), lim = hij / xk;
+            int A = rij >= s2 * hij / xk && rjt <= lim && j != i;
+            int B = rij < s2 * hij / xk && FABS(dotD(ni, dt, D)) + FABS(dotD(tau, dt, D)) < lim && j != i;
+            if ((A || B) && long_normal) count += 1;
+        }
+        fs_out[i] = count < (real)0.5 ? 1 : 0;
+        count_out[i] = count;
+    }
+    return 0;
+}
+
+/* Colour-field-gradient detection (colorFieldGradientDetection.py:18-56). */
+int oracle_surface_color_gradient(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                                  const real* c, const int32_t* offs, const int32_t* cnt, const int32_t* list, real threshold,
+                                  real* fs_out, real* normals_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real gc[3] = {0, 0, 0};
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG(&o, d, rsqrt_safe(dotD(d, d, D)), H[i], &W, g);
+            if (W == 0) continue;
+            for (int a = 0; a < D; ++a) gc[a] += m[j] / rho[j] * (c[j] - c[i]) * g[a];
+        }
+        real l = SQRT(dotD(gc, gc, D));
+        fs_out[i] = l > threshold * H[i] / (real)o.kxi ? 1 : 0;
+        real den = l < (real)1e-12 ? (real)1e-12 : l;
+        for (int a = 0; a < D; ++a) normals_out[i * D + a] = -(gc[a] / den);
+    }
+    return 0;
+}
+
+/* The moment matrix of the renormalisation, M_i = sum_j V_j (x_j - x_i) (x) grad_i W(r,
+ * max(H_i, H_j)) (M_out row-major D x D per particle); the caller inverts it. */
+int oracle_surface_moments(const SphParams* p, int64_t n, const real* x, const real* H, const real* m, const real* rho,
+                           const int32_t* offs, const int32_t* cnt, const int32_t* list, real* M_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real M[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG(&o, d, rsqrt_safe(dotD(d, d, D)), H[i] > H[j] ? H[i] : H[j], &W, g);
+            if (W == 0) continue;
+            real Vj = m[j] / rho[j];
+            for (int a = 0; a < D; ++a)
+                for (int b = 0; b < D; ++b) M[a * D + b] += Vj * (-d[a]) * g[b];
+        }
+        for (int a = 0; a < D * D; ++a) M_out[i * D * D + a] = M[a];
+    }
+    return 0;
+}
+
+/* Normals from the renormalised gradients: mode 0 (lambdaGrad.py) sum_j V_j (lambda_j -
+ * lambda_i) grad W(r, H_j), mode 1 (maronneNormals.py) sum_j V_j grad W(r, H_j); g = L_i times
+ * the sum, normals = -g / max(|g|, 1e-12). */
+int oracle_surface_renorm_normals(const SphParams* p, int64_t n, int mode, const real* x, const real* H, const real* m,
+                                  const real* rho, const real* L, const real* lam, const int32_t* offs, const int32_t* cnt,
+                                  const int32_t* list, real* normals_out, real* grad_out) {
+    OP o = op_from(p);
+    int D = o.dim;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        real s[3] = {0, 0, 0};
+        for (int32_t k = offs[i]; k < offs[i] + cnt[i]; ++k) {
+            int32_t j = list[k];
+            real d[3], W, g[3];
+            dist_vec(&o, x + i * D, x + (int64_t)j * D, d);
+            kWG(&o, d, rsqrt_safe(dotD(d, d, D)), H[j], &W, g);
+            if (W == 0) continue;
+            real Vj = m[j] / rho[j];
+            real w = mode == 0 ? Vj * (lam[j] - lam[i]) : Vj;
+            for (int a = 0; a < D; ++a) s[a] += w * g[a];
+        }
+        real v[3] = {0, 0, 0};
+        for (int a = 0; a < D; ++a)
+            for (int b = 0; b < D; ++b) v[a] += L[i * D * D + a * D + b] * s[b];
+        real l = SQRT(dotD(v, v, D));
+        if (l < (real)1e-12) l = (real)1e-12;
+        for (int a = 0; a < D; ++a) {
+            normals_out[i * D + a] = -(v[a] / l);
+            if (grad_out) grad_out[i * D + a] = v[a];
+        }
     }
     return 0;
 }

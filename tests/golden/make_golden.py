@@ -59,6 +59,9 @@ wp = types.SimpleNamespace(
     sqrt=lambda x: F(np.sqrt(F(x))),
     clamp=lambda x, lo, hi: (lo if x < lo else (hi if x > hi else x)),
     outer=lambda a, b: np.outer(np.asarray(a, F), np.asarray(b, F)).astype(F),
+    acos=lambda x: F(np.arccos(np.clip(F(x), F(-1), F(1)))),     # Warp clamps the argument
+    normalize=lambda v: (np.asarray(v, F) / F(np.sqrt(F(np.dot(np.asarray(v, F), np.asarray(v, F)))))).astype(F)
+    if F(np.dot(np.asarray(v, F), np.asarray(v, F))) > 0 else np.zeros_like(np.asarray(v, F)),
     int32=int, int64=int, bool=bool, float32=F, array=lambda *a, **k: None, tid=lambda: 0,
 )
 vector = matrix = lambda *a, **k: None
@@ -977,6 +980,67 @@ def run_reference_surface(ref: Path, case: dict) -> dict:
                 surface_expansion=np.array([sd.expansionIterations], np.int32))
 
 
+def run_reference_surface_schemes(ref: Path, case: dict, base: dict) -> dict:
+    """The other detection schemes on the surface case, with the reference's own bodies:
+    Barecasco (wp_barecasco.py computeBarecascoSurfaceDetection_Func_i_first / _second and
+    the kernel's normalisation, barecascoDetection.py's mask) at the buildDefault threshold
+    pi/3 and the dataclass default 1.5; Maronne (wp_maronne.py
+    computeMaronneSurfaceDetection_Func_i and computeMaronneSurfaceDetection's mask) with two
+    normal fields, the colour-field normals and the Barecasco cover directions; and the
+    colour-field-gradient scheme (colorFieldGradientDetection.py), run unmodified on the
+    restated colour field.  All under super-symmetric support."""
+    import math
+    Ctx.kernel, Ctx.dim = 2, 2
+    x, H, m, rho = (case[k] for k in ("x", "H", "m", "rho"))
+    offs, cnt, lst = case["offsets"], case["counts"], case["list"].astype(np.int64)
+    n = len(H)
+    state = SoA(positions=x, supports=H, masses=m, densities=rho, kinds=np.zeros(n, np.int32))
+    kp = SoA(operationMode=OperationDirection.TrueAllToToAll.value, supportMode="superSymmetric", kernelFunction=2)
+    common = dict(dim=2, referenceState=state, domainState=None, kernelProperties=kp, offsetArray=lst, ki=0,
+                  referenceKinds=state.kinds, useGradientRenormalization=False, Li=None, useGradHTerms=False, omega_i=F(1),
+                  referenceOmegas=None, useVolume=False, Vi=F(0), referenceVolumes=None, useCRK=False, Ai=F(1), Bi=None, gradAi=None,
+                  gradBi=None)
+    out = {}
+    bc = load(ref, "modules/surfaceDetection/wp_barecasco.py")
+    first, second = bc["computeBarecascoSurfaceDetection_Func_i_first"], bc["computeBarecascoSurfaceDetection_Func_i_second"]
+    for tag, theta in (("pi3", F(math.pi / 3)), ("1p5", F(1.5))):
+        nrm = np.zeros((n, 2), F)
+        count = np.zeros(n, F)
+        for i in range(n):
+            pi_ = dict(i=i, xi=x[i], hi=F(H[i]), mi=F(m[i]), rhoi=F(rho[i]), beginIndex=int(offs[i]), numIndices=int(cnt[i]))
+            cv = call(first, **pi_, **common)
+            ch = wp.normalize(cv)
+            nrm[i] = ch
+            count[i] = call(second, **pi_, **common, coverVector=ch, threshold=theta)
+        out[f"barecasco_{tag}_normals"] = nrm
+        out[f"barecasco_{tag}_count"] = count
+        out[f"barecasco_{tag}_fsm"] = (count < 0.5).astype(F)
+        out[f"barecasco_{tag}_threshold"] = np.array([theta], F)
+    mr = load(ref, "modules/surfaceDetection/wp_maronne.py")
+    mfn = mr["computeMaronneSurfaceDetection_Func_i"]
+    for tag, normals in (("colour", base["surface_normals"]), ("cover", out["barecasco_pi3_normals"])):
+        count = np.zeros(n, F)
+        for i in range(n):
+            count[i] = call(mfn, i=i, xi=x[i], hi=F(H[i]), mi=F(m[i]), rhoi=F(rho[i]), beginIndex=int(offs[i]),
+                            numIndices=int(cnt[i]), **common, normals=np.asarray(normals, F))
+        out[f"maronne_{tag}_normals"] = np.asarray(normals, F)
+        out[f"maronne_{tag}_count"] = count
+        out[f"maronne_{tag}_fsm"] = (count < 0.5).astype(F)
+    # colour-field-gradient scheme, unmodified, on the colour field of run_reference_surface
+    names = dict(SimulationConfig=None, SurfaceDetectionConfig=None, AdjacencyList=None, CompactHashMap=None,
+                 computeColorField=lambda *a, **k: (torch.from_numpy(base["surface_color"]), torch.from_numpy(base["surface_color_grad"])))
+    cg = load(ref, "modules/surfaceDetection/colorFieldGradientDetection.py", names)
+    cfg_ns = load(ref, "configurations/moduleConfigurations/surfaceDetection.py")
+    sd = cfg_ns["SurfaceDetectionConfig"]()
+    ps = SoA(positions=torch.from_numpy(x), supports=torch.from_numpy(H))
+    sim = SoA(kernel=types.SimpleNamespace(value=2), dim=2)
+    fs, nrm = cg["detectFreeSurfaceColorFieldGradient"](ps, sim, None, sd, None, returnNormals=True)
+    out["cfgrad_fsm"] = fs.numpy().astype(F)
+    out["cfgrad_normals"] = nrm.numpy().astype(F)
+    out["cfgrad_threshold"] = np.array([sd.colorFieldGradThreshold], F)
+    return out
+
+
 # ---------------------------------------------------------------- Owen adaptive support
 def _eval_C_d(dim, kernel):
     return kernel_C(int(kernel), int(dim))
@@ -1355,6 +1419,10 @@ def main():
         out = run_reference_surface(ref, case)
         np.savez_compressed(Path(__file__).parent / "surface_golden.npz", **case, **out)
         print("wrote", Path(__file__).parent / "surface_golden.npz", "particles", len(case["H"]), "surface", int(out["surface_fsm"].sum()))
+        out2 = run_reference_surface_schemes(ref, case, out)
+        np.savez_compressed(Path(__file__).parent / "surface_schemes_golden.npz", **out2)
+        print("wrote", Path(__file__).parent / "surface_schemes_golden.npz",
+              {k: int(v.sum()) for k, v in out2.items() if k.endswith("_fsm")})
     if a.which in ("all", "deltasph"):
         case = make_deltasph_case()
         out = run_reference_deltasph(ref, case)

@@ -2,7 +2,7 @@
 builder entries, configuration round trips, the enum forms the reference passes, gravity,
 the wall-particle layout check and boundary velocities, and the cases the GPU path
 refuses (walls in deltaSPH_step or without ghost points, boundary conditions, rigid
-bodies, surface detection schemes other than the colour field), which raise before any
+bodies, unknown surface detection schemes and normal sources), which raise before any
 device work."""
 import numpy as np
 import pytest
@@ -10,6 +10,7 @@ import torch
 
 import warpsph_b200 as ws
 from warpsph_b200 import configurations as cf
+from warpsph_b200.configurations import NormalSource, SurfaceDetectionScheme
 from warpsph_b200.enumTypes import IncompressibleSPHScheme, WeaklyCompressibleSPHScheme
 from warpsph_b200.systems import IncompressibleState, IncompressibleSystem, WeaklyCompressibleSystem
 from warpsph_b200.wcsph import computeGravity, deltaSPH_step, dfsph_step
@@ -90,15 +91,12 @@ def test_unsupported_inputs_raise(step, cfgcls):
         setattr(c, attr, val)
         with pytest.raises(NotImplementedError, match=msg):
             step(IncompressibleSystem(state=cpu_state()), 1e-3, config, c)
-    # the colour-field scheme is built; the others raise before any pass runs
+    # every scheme and normal source of the reference is built; unknown ones raise before any pass runs
     from warpsph_b200 import surface
-    from warpsph_b200.configurations import NormalSource, SurfaceDetectionScheme
     st = cpu_state()
-    for scheme, normals in ((SurfaceDetectionScheme.Barecasco, NormalSource.ColorFieldGrad),
-                            (SurfaceDetectionScheme.Maronne, NormalSource.ColorFieldGrad),
-                            (SurfaceDetectionScheme.ColorField, NormalSource.LambdaGrad)):
+    for scheme, normals in (("NoSuchScheme", NormalSource.ColorFieldGrad), (SurfaceDetectionScheme.Barecasco, "NoSuchSource")):
         sd = ws.configurations.SurfaceDetectionConfig(scheme=scheme, normalSource=normals)
-        with pytest.raises(NotImplementedError, match="surface detection scheme|normal source"):
+        with pytest.raises(ValueError, match="Unknown"):
             surface.detectFreeSurface(st, config, cfgcls(), sd, None)
     fsm, fs, n, _, _ = surface.detectFreeSurface(st, config, cfgcls(), ws.configurations.buildDefaultSurfaceDetectionConfig(), None)
     assert not fsm.any() and not fs.any() and not n.any()

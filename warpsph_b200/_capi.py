@@ -155,6 +155,11 @@ _PROTOS = {
     "sph_surface_color_field": [_P, _I64] + [_P] * 9,
     "sph_surface_detect_color_field": [_P, _I64] + [_P] * 8 + [C.c_float, C.c_float] + [_P] * 4,
     "sph_surface_dilate": [_P, _I64] + [_P] * 8,
+    "sph_surface_barecasco": [_P, _I64] + [_P] * 5 + [C.c_float] + [_P] * 4,
+    "sph_surface_maronne": [_P, _I64] + [_P] * 9,
+    "sph_surface_detect_color_gradient": [_P, _I64] + [_P] * 8 + [C.c_float] + [_P] * 3,
+    "sph_surface_renormalization": [_P, _I64] + [_P] * 10,
+    "sph_surface_renormalized_normals": [_P, _I64, _I32] + [_P] * 12,
     "sph_delta_shift": [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_float, _P, _P, _P],
     "sph_mlp_grad": [_P, _I64, _P, _P, _P, _P, _P],
     "sph_mlp_adam": [_P, _P, _P, _P, _I64, C.c_float, C.c_float, C.c_float, C.c_float, _I64, _P],

@@ -458,10 +458,11 @@ def _driver(case):
 
 
 def generate_samples(geometries, steps: int, device="cuda", dx: float = 0.02, dt: float = 1e-3, make_case=dam_break_2d,
-                     collect_every: int = 1, max_samples: Optional[int] = None, seed: int = 0):
+                     collect_every: int = 1, max_samples: Optional[int] = None, seed: int = 0, max_target: float = 1e3):
     """(features, targets) per solve mode from dam-break trajectories; ``geometries`` is a
     list of (width, height, seed); samples are collected every ``collect_every`` steps;
-    rows with a non-finite feature or target are dropped, and with ``max_samples`` a
+    rows with a non-finite feature or a target of magnitude max_target or more (solves
+    whose pressure scale is a rounding residue) are dropped, and with ``max_samples`` a
     seeded random subset of that many rows is kept per mode."""
     collect: dict = {}
     for (w, h, gseed) in geometries:
@@ -473,7 +474,7 @@ def generate_samples(geometries, steps: int, device="cuda", dx: float = 0.02, dt
     gen = torch.Generator(device="cpu").manual_seed(seed)
     for mode in (0, 1):
         f, t = torch.cat(collect[("feats", mode)]), torch.cat(collect[("target", mode)])
-        ok = torch.isfinite(f).all(dim=1) & torch.isfinite(t)
+        ok = torch.isfinite(f).all(dim=1) & torch.isfinite(t) & (t.abs() < max_target)
         if not bool(ok.all()):
             f, t = f[ok], t[ok]
         if max_samples is not None and f.shape[0] > max_samples:

@@ -455,6 +455,65 @@ def surface_dilate(params, x, H, fs, adj: AdjacencyList):
     return out
 
 
+def surface_barecasco(params, x, H, adj: AdjacencyList, threshold: float):
+    """Barecasco detection (wp_barecasco.py, barecascoDetection.py): (mask, normalised cover
+    vectors, cone counts)."""
+    n, d = H.shape[0], x.shape[1]
+    fs, cnt = _empty(n, H), _empty(n, H)
+    normals = torch.empty((n, d), device=H.device, dtype=torch.float32)
+    with _timed("surface_barecasco"):
+        check(_capi.lib().sph_surface_barecasco(_p(params), n, fptr(x), fptr(H), *_lists(params, adj, True), float(threshold),
+                                                ptr(fs), ptr(normals), ptr(cnt), stream_ptr(H.device)), "sph_surface_barecasco")
+    return fs, normals, cnt
+
+
+def surface_maronne(params, x, H, normals, adj: AdjacencyList):
+    """Maronne detection with the given normals (wp_maronne.py, maronneDetection.py): (mask, counts)."""
+    n = H.shape[0]
+    fs, cnt = _empty(n, H), _empty(n, H)
+    with _timed("surface_maronne"):
+        check(_capi.lib().sph_surface_maronne(_p(params), n, fptr(x), fptr(H), fptr(normals), *_lists(params, adj, True), ptr(fs),
+                                              ptr(cnt), stream_ptr(H.device)), "sph_surface_maronne")
+    return fs, cnt
+
+
+def surface_detect_color_gradient(params, x, H, m, rho, color, adj: AdjacencyList, threshold: float):
+    """Colour-field-gradient detection (colorFieldGradientDetection.py): (mask, normals)."""
+    n, d = H.shape[0], x.shape[1]
+    fs = _empty(n, H)
+    normals = torch.empty((n, d), device=H.device, dtype=torch.float32)
+    with _timed("surface_detect"):
+        check(_capi.lib().sph_surface_detect_color_gradient(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(color),
+                                                            *_lists(params, adj, True), float(threshold), ptr(fs), ptr(normals),
+                                                            stream_ptr(H.device)), "sph_surface_detect_color_gradient")
+    return fs, normals
+
+
+def surface_renormalization(params, x, H, m, rho, adj: AdjacencyList):
+    """Renormalisation matrices L = pinv(M) [n, d, d] and the smallest |eigenvalue| of M [n]."""
+    n, d = H.shape[0], x.shape[1]
+    L = torch.empty((n, d, d), device=H.device, dtype=torch.float32)
+    lam = _empty(n, H)
+    with _timed("surface_renormalization"):
+        check(_capi.lib().sph_surface_renormalization(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), *_lists(params, adj, True),
+                                                      ptr(L), ptr(lam), stream_ptr(H.device)), "sph_surface_renormalization")
+    return L, lam
+
+
+def surface_renormalized_normals(params, mode: int, x, H, m, rho, L, lambdas, adj: AdjacencyList, want_grad: bool = False):
+    """Normals from the renormalised lambda gradient (mode 0) or Maronne's (mode 1); with
+    ``want_grad`` also the renormalised gradient."""
+    n, d = H.shape[0], x.shape[1]
+    normals = torch.empty((n, d), device=H.device, dtype=torch.float32)
+    g = torch.empty((n, d), device=H.device, dtype=torch.float32) if want_grad else None
+    with _timed("surface_normals"):
+        check(_capi.lib().sph_surface_renormalized_normals(_p(params), n, int(mode), fptr(x), fptr(H), fptr(m), fptr(rho), fptr(L),
+                                                           fptr(lambdas) if lambdas is not None else None,
+                                                           *_lists(params, adj, True), ptr(normals), ptr(g), stream_ptr(H.device)),
+              "sph_surface_renormalized_normals")
+    return (normals, g) if want_grad else normals
+
+
 def switch_hopkins_update(params, x, H, v, c, div, div_prev, alpha0, dt, adj: AdjacencyList, want_vsig: bool = False):
     """Cullen-Hopkins alpha0 update (v_sig over the Verlet rows); (alpha0, v_sig or None)."""
     n = H.shape[0]
