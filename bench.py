@@ -295,7 +295,8 @@ def ensemble_throughput(dev, chunks: int = 6) -> dict:
     """The batched weakly compressible delta-SPH ensemble: 256 periodic 2D unit boxes with
     particle counts log-uniform in [4096, 65536] (seed 0), divergence-free E(k) ~ k^-5/3
     velocity fields at U_max = 1, stiff Tait EOS c0 = 10, delta = 0.1, nu = 1e-3, Wendland
-    C2 with the reference's default 50 neighbours, Heun RK2 at dt = 0.3 h / c0 per box.
+    C2 with the reference's default 50 neighbours, Heun RK2 at the weakly compressible step
+    rule per box (viscous and acoustic limits; the acoustic 0.3 h / c0 / k decides).
     One cooperative launch per step for all boxes, steps replayed from a CUDA graph,
     lists rebuilt when the Verlet skin requires it (included in the time)."""
     import torch

@@ -141,3 +141,17 @@ def test_boundary_velocities_and_wall_layout():
     config.regions[1].kind = types.SimpleNamespace(name="noSlip")
     with pytest.raises(NotImplementedError, match="noSlip"):
         computeBoundaryVelocities(st, config, cf.IncompressibleSPHConfig())
+
+
+def test_weakly_compressible_step_limit():
+    """The weakly compressible time-step rule (timestep/weaklyCompressible.py:13-88) as the
+    ensemble applies it per box: the smallest enabled limit."""
+    from warpsph_b200.wcsph import weaklyCompressibleStepLimit
+    c = cf.WeaklyCompressibleSPHConfig()
+    H, c0, nu, k = 0.05, 10.0, 1e-3, 1.9
+    v, a = 0.125 * H * H / nu / k, 0.3 * H / c0 / k
+    assert weaklyCompressibleStepLimit(H, c0, nu, k, 0.3, c) == min(v, a)
+    acc = 0.25 * (H / (1e4 + 1e-7)) ** 0.5 / k
+    assert weaklyCompressibleStepLimit(H, c0, nu, k, 0.3, c, max_accel=1e4) == min(v, a, acc)
+    c.dt_acousticConstraint = False
+    assert weaklyCompressibleStepLimit(H, 1.0, 1.0, k, 0.3, c) == 0.125 * H * H / 1.0 / k

@@ -515,13 +515,201 @@ __device__ __forceinline__ void verlet_flush_part(int lane, int wib, int& nb, in
     nb = 0;
 }
 
+// One work item of the walk (32 particles of one cell against its stencil).  MI: the grid
+// has fewer than three cells along a periodic axis, and every pair takes its minimum image
+// (rare, tiny grids; kept out of line so the common loop stays compact).  Candidate slots
+// past the end of a cell hold a record at 3e38, which no test accepts, so the unrolled
+// candidate loop needs no bound check.
+//
+// Acceptance bits (masks non-null, not MI): the count pass reserves 32 words per candidate
+// chunk of its work item from a bounded pool and stores each lane's 32 acceptance bits per
+// chunk; the fill pass then visits only the accepted candidates, in the same order, and
+// repeats the distance arithmetic only to split them into the interacting prefix and the
+// rest.  A work item that found the pool exhausted tests every candidate again.
+template <int D, bool MI>
+__device__ __forceinline__ void verlet_pair(const Vec<D>& xi, float Hi, const float4& rj, const float* sh, const DomainF& dom,
+                                            float vs, float& r2, float& Hm, float& R) {
+    Hm = fmaxf(Hi, rj.w);
+    R = __fmul_rn(vs, Hm);
+    Vec<D> dv;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) {
+        const float xj = a == 0 ? rj.x : (a == 1 ? rj.y : rj.z);
+        if (MI) {
+            float d = __fsub_rn(xi.v[a], xj);
+            if (dom.periodic[a]) {
+                if (d > dom.halfL[a]) d = __fsub_rn(d, dom.L[a]);
+                else if (d < -dom.halfL[a]) d = __fadd_rn(d, dom.L[a]);
+            }
+            dv.v[a] = d;
+        } else {
+            dv.v[a] = __fsub_rn(__fsub_rn(xi.v[a], xj), sh[a]);
+        }
+    }
+    r2 = dist2_rn<D>(dv);
+}
+
+template <int D, bool FILL, bool MI>
+__device__ __forceinline__ void verlet_task(int task, int lane, int wib, const float4* __restrict__ recs,
+                                            const uint32_t* __restrict__ sorted_keys, const int32_t* __restrict__ tasks,
+                                            const GridDev& g, const DevParams& P, const int32_t* __restrict__ sort_index,
+                                            const int32_t* __restrict__ cell_begin, const int32_t* __restrict__ cell_end,
+                                            int32_t* __restrict__ counts, int32_t* __restrict__ icounts,
+                                            const int32_t* __restrict__ offsets, int32_t* __restrict__ list, long long& itotal,
+                                            float4 (*srec)[32], int32_t (*sidx)[32], int32_t (*sbuf)[32][VP],
+                                            int32_t (*sibuf)[32][VP], uint32_t* __restrict__ masks,
+                                            int32_t* __restrict__ mask_base, unsigned long long* __restrict__ mask_cursor,
+                                            long long mask_words) {
+    const bool part = icounts != nullptr;
+    const DomainF& dom = P.dom;
+    const float vs = P.verlet_scale;
+    const int start = tasks[task];
+    const uint32_t ckey = sorted_keys[start];
+    const int stop = min(start + 32, cell_end[ckey]);
+    const int t = start + lane;
+    const bool active = t < stop;
+    const float4 ri = recs[active ? t : start];
+    const Vec<D> xi = rec_pos<D>(ri);
+    const float Hi = ri.w;
+    int c[3];
+    cell_coords<D>(rec_pos<D>(recs[start]), g, dom, c);
+    uint32_t keys[D == 1 ? 3 : (D == 2 ? 9 : 27)];
+    float shifts[3 * (D == 1 ? 3 : (D == 2 ? 9 : 27))];
+    const int nk = stencil_keys<D>(c, g, dom, keys, shifts);
+    const int i = active ? sort_index[t] : 0;
+    int cnt = 0, icnt = 0;
+    int row = 0, tail = 0, nb = 0, nib = 0, written = 0, iwritten = 0;
+    if (FILL && active) {
+        row = offsets[i];
+        tail = row + (part ? icounts[i] : 0);
+    }
+    // the work item's slice of the acceptance-bit pool
+    int mbase = -1;
+    if (!MI && masks != nullptr) {
+        if (!FILL) {
+            int nch = 0;
+            for (int q = 0; q < nk; ++q) nch += (cell_end[keys[q]] - cell_begin[keys[q]] + 31) >> 5;
+            if (lane == 0) {
+                const unsigned long long need = 32ull * (unsigned long long)nch;
+                const unsigned long long o = atomicAdd(mask_cursor, need);
+                mbase = o + need <= (unsigned long long)mask_words ? (int)o : -1;
+                mask_base[task] = mbase;
+            }
+            mbase = __shfl_sync(0xffffffffu, mbase, 0);
+        } else {
+            mbase = mask_base[task];
+        }
+    }
+    const float4 far = make_float4(3e38f, 3e38f, 3e38f, 0.f);
+    int ch = 0;
+    for (int q = 0; q < nk; ++q) {
+        const int b = cell_begin[keys[q]], e = cell_end[keys[q]];
+        const float sh[3] = {shifts[3 * q], shifts[3 * q + 1], shifts[3 * q + 2]};
+        for (int k0 = b; k0 < e; k0 += 32, ++ch) {
+            uint32_t m = 0;
+            if (FILL && mbase >= 0) {
+                m = active ? masks[mbase + 32 * ch + lane] : 0u;
+                if (!__any_sync(0xffffffffu, m != 0u)) continue;
+            }
+            __syncwarp();
+            const bool real = k0 + lane < e;
+            srec[wib][lane] = real ? recs[k0 + lane] : far;
+            if (FILL && real) sidx[wib][lane] = sort_index[k0 + lane];
+            __syncwarp();
+            if (FILL && mbase >= 0) {
+                // accepted candidates only, lowest bit (candidate order) first, up to 8 per
+                // lane between two flushes
+                while (__any_sync(0xffffffffu, m != 0u)) {
+                    if (__any_sync(0xffffffffu, nb > VS - 8 || nib > VS - 8)) {
+                        __syncwarp();
+                        verlet_flush_part(lane, wib, nib, iwritten, row, sibuf, list);
+                        verlet_flush_part(lane, wib, nb, written, tail, sbuf, list);
+                        __syncwarp();
+                    }
+                    #pragma unroll
+                    for (int r = 0; r < 8; ++r) {
+                        if (m != 0u) {
+                            const int u = __ffs(m) - 1;
+                            m &= m - 1u;
+                            float r2, Hm, R;
+                            verlet_pair<D, MI>(xi, Hi, srec[wib][u], sh, dom, vs, r2, Hm, R);
+                            const int j = sidx[wib][u];
+                            if (part && interacting_pair(r2, Hm)) sibuf[wib][lane][nib++] = j;
+                            else sbuf[wib][lane][nb++] = j;
+                        }
+                    }
+                }
+                continue;
+            }
+            const int mcount = min(32, e - k0);
+            uint32_t hm = 0;
+            for (int u0 = 0; u0 < mcount; u0 += 8) {
+                // room for the next 8 candidates in every lane's buffers
+                if (FILL && __any_sync(0xffffffffu, nb > VS - 8 || nib > VS - 8)) {
+                    __syncwarp();
+                    verlet_flush_part(lane, wib, nib, iwritten, row, sibuf, list);
+                    verlet_flush_part(lane, wib, nb, written, tail, sbuf, list);
+                    __syncwarp();
+                }
+                #pragma unroll
+                for (int du = 0; du < 8; ++du) {
+                    const int u = u0 + du;
+                    float r2, Hm, R;
+                    verlet_pair<D, MI>(xi, Hi, srec[wib][u], sh, dom, vs, r2, Hm, R);
+                    const bool hit = active & (r2 < __fmul_rn(R, R));
+                    const bool inter = part && hit && interacting_pair(r2, Hm);
+                    if (FILL) {
+                        if (hit) {
+                            const int j = sidx[wib][u];
+                            if (inter) sibuf[wib][lane][nib++] = j;
+                            else sbuf[wib][lane][nb++] = j;
+                        }
+                    } else {
+                        cnt += hit;
+                        icnt += inter;
+                        hm |= (uint32_t)hit << u;
+                    }
+                }
+            }
+            if (!FILL && mbase >= 0) masks[mbase + 32 * ch + lane] = hm;
+        }
+    }
+    if (FILL) {
+        if (__any_sync(0xffffffffu, nb > 0 || nib > 0)) {
+            __syncwarp();
+            verlet_flush_part(lane, wib, nib, iwritten, row, sibuf, list);
+            verlet_flush_part(lane, wib, nb, written, tail, sbuf, list);
+            __syncwarp();
+        }
+    } else if (active) {
+        counts[i] = cnt;
+        if (part) icounts[i] = icnt;
+        itotal += icnt;
+    }
+}
+
+template <int D, bool FILL>
+__device__ __noinline__ void verlet_task_min_image(int task, int lane, int wib, const float4* __restrict__ recs,
+                                                   const uint32_t* __restrict__ sorted_keys, const int32_t* __restrict__ tasks,
+                                                   const GridDev& g, const DevParams& P, const int32_t* __restrict__ sort_index,
+                                                   const int32_t* __restrict__ cell_begin, const int32_t* __restrict__ cell_end,
+                                                   int32_t* __restrict__ counts, int32_t* __restrict__ icounts,
+                                                   const int32_t* __restrict__ offsets, int32_t* __restrict__ list, long long& itotal,
+                                                   float4 (*srec)[32], int32_t (*sidx)[32], int32_t (*sbuf)[32][VP],
+                                                   int32_t (*sibuf)[32][VP]) {
+    verlet_task<D, FILL, true>(task, lane, wib, recs, sorted_keys, tasks, g, P, sort_index, cell_begin, cell_end, counts, icounts,
+                               offsets, list, itotal, srec, sidx, sbuf, sibuf, nullptr, nullptr, nullptr, 0);
+}
+
 template <int D, bool FILL>
 __global__ void __launch_bounds__(VW_BLOCK)
 k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_keys, const int32_t* __restrict__ tasks,
          const int32_t* __restrict__ ntasks, const GridDev* __restrict__ gp, DevParams P,
          const int32_t* __restrict__ sort_index, const int32_t* __restrict__ cell_begin, const int32_t* __restrict__ cell_end,
          int32_t* __restrict__ counts, int32_t* __restrict__ icounts, const int32_t* __restrict__ offsets,
-         int32_t* __restrict__ list, long long* __restrict__ innz, const long long* __restrict__ nnz, long long capacity) {
+         int32_t* __restrict__ list, long long* __restrict__ innz, const long long* __restrict__ nnz, long long capacity,
+         uint32_t* __restrict__ masks, int32_t* __restrict__ mask_base, unsigned long long* __restrict__ mask_cursor,
+         long long mask_words) {
     __shared__ float4 srec[VW_WARPS][32];
     __shared__ int32_t sidx[FILL ? VW_WARPS : 1][32];
     __shared__ int32_t sbuf[FILL ? VW_WARPS : 1][32][VP];     // rest of the row
@@ -533,100 +721,17 @@ k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_ke
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nt = *ntasks;
     const GridDev g = *gp;
-    const DomainF dom = P.dom;
-    const float vs = P.verlet_scale;
+    const bool min_image = grid_needs_min_image<D>(g, P.dom);     // uniform over the grid
     long long itotal = 0;
     for (int task = warp; task < nt; task += nwarps) {
-        const int start = tasks[task];
-        const uint32_t ckey = sorted_keys[start];
-        const int stop = min(start + 32, cell_end[ckey]);
-        const int t = start + lane;
-        const bool active = t < stop;
-        const float4 ri = recs[active ? t : start];
-        const Vec<D> xi = rec_pos<D>(ri);
-        const float Hi = ri.w;
-        int c[3];
-        cell_coords<D>(rec_pos<D>(recs[start]), g, dom, c);
-        uint32_t keys[D == 1 ? 3 : (D == 2 ? 9 : 27)];
-        float shifts[3 * (D == 1 ? 3 : (D == 2 ? 9 : 27))];
-        const int nk = stencil_keys<D>(c, g, dom, keys, shifts);
-        const bool min_image = grid_needs_min_image<D>(g, dom);     // uniform over the grid
-        const int i = active ? sort_index[t] : 0;
-        int cnt = 0, icnt = 0;
-        int row = 0, tail = 0, nb = 0, nib = 0, written = 0, iwritten = 0;
-        if (FILL && active) {
-            row = offsets[i];
-            tail = row + (part ? icounts[i] : 0);
-        }
-        for (int q = 0; q < nk; ++q) {
-            const int b = cell_begin[keys[q]], e = cell_end[keys[q]];
-            float sh[3] = {shifts[3 * q], shifts[3 * q + 1], shifts[3 * q + 2]};
-            for (int k0 = b; k0 < e; k0 += 32) {
-                __syncwarp();
-                if (k0 + lane < e) {
-                    srec[wib][lane] = recs[k0 + lane];
-                    if (FILL) sidx[wib][lane] = sort_index[k0 + lane];
-                }
-                __syncwarp();
-                const int mcount = min(32, e - k0);
-                for (int u0 = 0; u0 < mcount; u0 += 8) {
-                    // room for the next 8 candidates in every lane's buffers
-                    if (FILL && __any_sync(0xffffffffu, nb > VS - 8 || nib > VS - 8)) {
-                        __syncwarp();
-                        verlet_flush_part(lane, wib, nib, iwritten, row, sibuf, list);
-                        verlet_flush_part(lane, wib, nb, written, tail, sbuf, list);
-                        __syncwarp();
-                    }
-                    #pragma unroll
-                    for (int du = 0; du < 8; ++du) {
-                        const int u = u0 + du;
-                        const float4 rj = srec[wib][u < mcount ? u : 0];
-                        const float Hm = fmaxf(Hi, rj.w);
-                        const float R = __fmul_rn(vs, Hm);
-                        Vec<D> dv;
-                        #pragma unroll
-                        for (int a = 0; a < D; ++a) {
-                            const float xj = a == 0 ? rj.x : (a == 1 ? rj.y : rj.z);
-                            if (min_image) {
-                                float d = __fsub_rn(xi.v[a], xj);
-                                if (dom.periodic[a]) {
-                                    if (d > dom.halfL[a]) d = __fsub_rn(d, dom.L[a]);
-                                    else if (d < -dom.halfL[a]) d = __fadd_rn(d, dom.L[a]);
-                                }
-                                dv.v[a] = d;
-                            } else {
-                                dv.v[a] = __fsub_rn(__fsub_rn(xi.v[a], xj), sh[a]);
-                            }
-                        }
-                        const float r2 = dist2_rn<D>(dv);
-                        const bool hit = active & (u < mcount) & (r2 < __fmul_rn(R, R));
-                        const bool inter = part && hit && interacting_pair(r2, Hm);
-                        if (FILL) {
-                            if (hit) {
-                                const int j = sidx[wib][u];
-                                if (inter) sibuf[wib][lane][nib++] = j;
-                                else sbuf[wib][lane][nb++] = j;
-                            }
-                        } else {
-                            cnt += hit;
-                            icnt += inter;
-                        }
-                    }
-                }
-            }
-        }
-        if (FILL) {
-            if (__any_sync(0xffffffffu, nb > 0 || nib > 0)) {
-                __syncwarp();
-                verlet_flush_part(lane, wib, nib, iwritten, row, sibuf, list);
-                verlet_flush_part(lane, wib, nb, written, tail, sbuf, list);
-                __syncwarp();
-            }
-        } else if (active) {
-            counts[i] = cnt;
-            if (part) icounts[i] = icnt;
-            itotal += icnt;
-        }
+        if (min_image)
+            verlet_task_min_image<D, FILL>(task, lane, wib, recs, sorted_keys, tasks, g, P, sort_index, cell_begin, cell_end, counts,
+                                           icounts, offsets, list, itotal, srec, FILL ? sidx : nullptr, FILL ? sbuf : nullptr,
+                                           FILL ? sibuf : nullptr);
+        else
+            verlet_task<D, FILL, false>(task, lane, wib, recs, sorted_keys, tasks, g, P, sort_index, cell_begin, cell_end, counts,
+                                        icounts, offsets, list, itotal, srec, FILL ? sidx : nullptr, FILL ? sbuf : nullptr,
+                                        FILL ? sibuf : nullptr, masks, mask_base, mask_cursor, mask_words);
     }
     if (!FILL && part) {
         #pragma unroll
@@ -662,8 +767,19 @@ struct NbWs {
     int32_t* tasks;
     int32_t* ntasks;
     char* scan;
+    uint32_t* masks;                  // acceptance bits of the count pass, 32 words per candidate chunk
+    int32_t* mask_base;               // per work item: first mask word, or -1 (none kept)
+    unsigned long long* mask_cursor;
+    int64_t mask_words;
     int64_t bytes;
 };
+// Acceptance-bit budget: 64 words per particle (the 3D walk needs about 58: 27 stencil cells
+// of about two 32-candidate chunks per 32 particles), at most 2^28 words.  Work items past the
+// budget test their candidates again in the fill pass.
+static int64_t mask_budget(int64_t n) {
+    int64_t w = n * 64;
+    return w < ((int64_t)1 << 28) ? w : ((int64_t)1 << 28);
+}
 static int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
 static NbWs carve(char* base, int64_t n, int64_t cap) {
     NbWs w;
@@ -680,6 +796,10 @@ static NbWs carve(char* base, int64_t n, int64_t cap) {
     w.scan = base + off;
     int64_t sb = scan_ws_bytes(cap > n ? cap : n);
     off += align256(sb);
+    w.mask_words = mask_budget(n);
+    w.masks = reinterpret_cast<uint32_t*>(base + off); off += align256(w.mask_words * 4);
+    w.mask_base = reinterpret_cast<int32_t*>(base + off); off += align256(n * 4);
+    w.mask_cursor = reinterpret_cast<unsigned long long*>(base + off); off += 256;
     w.bytes = off;
     return w;
 }
@@ -927,15 +1047,18 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
     int vblocks = grid_for(n, VW_BLOCK);          // >= one warp per 32 particles; warps stride over the work items
     if (vblocks > 148 * 32) vblocks = 148 * 32;
     if (part) cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
+    cudaMemsetAsync(w.mask_cursor, 0, sizeof(unsigned long long), s);
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, false><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
                                                                                  cell_begin, cell_end, num_neighbors, inter_counts, nullptr,
-                                                                                 nullptr, innz, nullptr, 0)));
+                                                                                 nullptr, innz, nullptr, 0, w.masks, w.mask_base,
+                                                                                 w.mask_cursor, (long long)w.mask_words)));
     exclusive_scan_i32(num_neighbors, neighbor_offsets, n, w.scan, reinterpret_cast<long long*>(nnz_out), s);
     wsph::count_launch(); k_check_capacity<<<1, 1, 0, s>>>(reinterpret_cast<long long*>(nnz_out), list_capacity, status);
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, true><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
                                                                                 cell_begin, cell_end, nullptr, inter_counts, neighbor_offsets,
                                                                                 neighbor_list, nullptr, reinterpret_cast<long long*>(nnz_out),
-                                                                                list_capacity)));
+                                                                                list_capacity, w.masks, w.mask_base, w.mask_cursor,
+                                                                                (long long)w.mask_words)));
     return check_launch("sph_neighbors_build");
 }
 

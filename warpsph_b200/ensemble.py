@@ -19,8 +19,10 @@ The case (``build_boxes``) is a set of periodic unit boxes:
     |A(k)|^2 ~ |k|^-5/3 / |k| (the 2D shell of E(k) ~ k^-5/3), phases from the box's
     seed, scaled to U_max = 1.
   * Physics: stiff Tait EOS with c0 = 10 U_max, rho0 = 1, delta = 0.1, nu = 1e-3.
-  * Time step: the rule of modules/timestep/weaklyCompressible.py:90-116,
-    dt = 0.3 h / c0 per box.
+  * Time step: per box, the weakly compressible rule of
+    modules/timestep/weaklyCompressible.py:13-88 (wcsph.weaklyCompressibleStepLimit): the
+    smaller of the viscous limit 0.125 h^2 / nu / k and the acoustic limit CFL h / c0 / k
+    (CFL 0.3), fixed at set-up; for these boxes the acoustic limit decides.
 
 No counterpart in the reference, which runs one simulation per process.
 """
@@ -38,6 +40,7 @@ from . import _capi, ops
 from ._capi import check, ptr
 from .configurations import SimulationConfig, WeaklyCompressibleSPHConfig, make_params, wc_params
 from .core import AdjacencyList, KernelFunctions, buildDomainDescription, n_h_to_nH, sphKernelScale, volumeToSupportHelper
+from .wcsph import weaklyCompressibleStepLimit
 
 TILE_CANDIDATES = [(4, 128), (4, 256), (8, 128), (8, 256), (16, 128), (16, 256)]
 
@@ -115,7 +118,8 @@ class Ensemble:
             box_of.append(torch.full((nx * nx,), b, dtype=torch.int32, device=dev))
             H.append(torch.full((nx * nx,), hb, device=dev))
             m.append(torch.full((nx * nx,), float(self.scheme.fluid.restDensity) * dx * dx, device=dev))
-            dts.append(0.3 * hb / kscale / c0)
+            nu = float(self.scheme.diffusionParams.viscidNu)
+            dts.append(weaklyCompressibleStepLimit(hb, c0, nu, kscale, float(self.config.cflFactor), self.scheme))
             G = int(math.floor(1.0 / (self.config.verletScale * hb * (1 + 1e-5))))
             if G < 3:
                 raise ValueError(f"box {b}: support {hb:.4g} too large for a 3-cell periodic grid")

@@ -28,6 +28,8 @@ walls in deltaSPH_step and the surface-aware shift raise NotImplementedError.
 """
 from __future__ import annotations
 
+import math
+
 import dataclasses
 from typing import Any, Optional
 
@@ -273,6 +275,22 @@ def deltaSPH_step(system, dt, config, schemeConfig, verbose: bool = False):
     update = WeaklyCompressibleSystemUpdate(dxdt=S.velocities.clone(), dvdt=dvdt_rhs + computeGravity(S, config, schemeConfig, adjacency),
                                             drhodt=drhodt, passive=_passive(S))
     return update, adjacency, S
+
+
+def weaklyCompressibleStepLimit(H: float, c_s: float, nu: float, kernel_scale: float, cfl: float, compParams,
+                                max_accel: Optional[float] = None, max_dt: float = float("inf")) -> float:
+    """The limit of modules/timestep/weaklyCompressible.py:13-88 for one simulation as host
+    floats: min over the enabled constraints of 0.125 H^2 / nu / k (viscous), cfl H / c_s / k
+    (acoustic) and, when max_accel is given, 0.25 sqrt(H / (max_accel + 1e-7)) / k, with H
+    the smallest support and k the kernel scale (computeTimestep's rule before its clamps)."""
+    new_dt = max_dt
+    if compParams.dt_viscosityConstraint:
+        new_dt = 0.125 * H * H / nu / kernel_scale
+    if compParams.dt_accelerationConstraint and max_accel is not None:
+        new_dt = min(new_dt, 0.25 * math.sqrt(H / (max_accel + 1e-7)) / kernel_scale)
+    if compParams.dt_acousticConstraint:
+        new_dt = min(new_dt, cfl * H / c_s / kernel_scale)
+    return new_dt
 
 
 def computeTimestep(system, config, compParams, dt=None, systemUpdate=None):
