@@ -810,6 +810,12 @@ int sph_mlp_forward_tc(const float* params, int64_t n, const float* feats, const
  * sum_i (MLP(feats_i) - target_i)^2 (device double). */
 int sph_mlp_grad(const float* params, int64_t n, const float* feats, const float* target,
                  float* grad, double* loss, void* stream);
+/* The same gradient with every GEMM on tcgen05 (one CTA per SM, the weight gradients
+ * accumulated in tensor memory; feats 16-byte aligned).  Rounding points as sph_mlp_grad,
+ * except that the bias gradients are summed from the BF16 dZ.  A tensor-core wait that
+ * runs out ors SPH_STATUS_TIMEOUT into *status (may be null) and leaves grad incomplete. */
+int sph_mlp_grad_tc(const float* params, int64_t n, const float* feats, const float* target,
+                    float* grad, double* loss, int32_t* status, void* stream);
 
 /* One Adam step (Kingma & Ba 2015, bias-corrected; step counts from 1). */
 int sph_mlp_adam(float* params, const float* grad, float* m1, float* m2, int64_t count,

@@ -82,16 +82,21 @@ def test_mlp_forward_tc_rejects_misaligned_features(cuda):
     assert torch.equal(ops.mlp_forward(th, feats), ref)
 
 
-@pytest.mark.parametrize("n", [16, 333, 5000])
-def test_mlp_gradient_matches_oracle(cuda, n):
+@pytest.mark.parametrize("tc", ["tcgen05", "mma"])
+@pytest.mark.parametrize("n", [16, 333, 5000, 70000])
+def test_mlp_gradient_matches_oracle(cuda, n, tc):
     """The gradient check: every parameter block of the kernel's MSE gradient against the
-    oracle's analytic gradient (itself checked against finite differences on the CPU)."""
+    oracle's analytic gradient (itself checked against finite differences on the CPU), for
+    the tcgen05 kernel (n = 70000 spreads the tiles over every SM, several per CTA) and the
+    mma.sync one."""
     rng = np.random.default_rng(10 + n)
     th = random_net(2)
     x = rng.standard_normal((n, 8)).astype(np.float32)
     t = rng.standard_normal(n).astype(np.float32)
     gref, lref = omlp.grad(th, x, t)
-    g, loss = ops.mlp_grad(torch.from_numpy(th).to(cuda), torch.from_numpy(x).to(cuda), torch.from_numpy(t).to(cuda))
+    g, loss = ops.mlp_grad(torch.from_numpy(th).to(cuda), torch.from_numpy(x).to(cuda), torch.from_numpy(t).to(cuda),
+                           tensor_cores=tc)
+    assert int(ops.mlp_status(cuda).item()) == 0
     g = g.cpu().numpy()
     assert abs(float(loss.item()) - lref) <= 1e-2 * lref
     for name, a, b in BLOCKS:

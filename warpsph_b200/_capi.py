@@ -162,6 +162,7 @@ _PROTOS = {
     "sph_surface_renormalized_normals": [_P, _I64, _I32] + [_P] * 12,
     "sph_delta_shift": [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_float, _P, _P, _P],
     "sph_mlp_grad": [_P, _I64, _P, _P, _P, _P, _P],
+    "sph_mlp_grad_tc": [_P, _I64, _P, _P, _P, _P, _P, _P],
     "sph_mlp_adam": [_P, _P, _P, _P, _I64, C.c_float, C.c_float, C.c_float, C.c_float, _I64, _P],
     "sph_dfsph_div_solve": [_P, _P, _I64] + [_P] * 12 + [_I64] + [_P] * 6,
     "sph_dfsph_density_solve": [_P, _P, _I64] + [_P] * 12 + [_I64] + [_P] * 6,

@@ -547,6 +547,353 @@ k_mlp_forward_tc(const float* __restrict__ prm, int64_t n, const float* __restri
     }
 }
 
+// ---------------------------------------------------------------- training on tcgen05
+// The gradient of the mean squared error with every GEMM on the tensor cores.  One CTA per
+// SM (4 warps, one sample per thread and TMEM lane) loops over 128-sample tiles:
+//   forward   the three hidden layers as in k_mlp_forward_tc (TS form, biases in the
+//             contraction), keeping each layer's BF16 input transposed in shared memory
+//             (XT, H1T, H2T: rows = input unit, K = sample) and the ReLU masks in registers;
+//   output    y = h3 . w4 + b4 in FP32, dy = 2 (y - t) / n; the w4 and b4 gradients are
+//             warp-reduced FP32 sums;
+//   backward  dZ3 = dy w4 * [z3 > 0]; then per layer l = 3, 2, 1 two MMA chains:
+//               G_l (+)= H_{l-1}^T dZ_l^T   (SS form, M = 128 input rows, N = 64 outputs,
+//                                           K = 128 samples; accumulated in TMEM over the
+//                                           CTA's tiles; the ones row of H^T gives db_l)
+//               dH_{l-1} = dZ_l W_l          (TS form, A = dZ_l in TMEM, B = W_l^T)
+//             and dZ_{l-1} = dH_{l-1} * [z_{l-1} > 0] in the epilogue.
+// At the end each thread adds its TMEM lane of G_1..G_3 (one input unit, all outputs) to the
+// global gradient with FP32 atomics.  Rounding points: BF16 inputs, weights, activations and
+// dZ, FP32 accumulation, as the oracle's BF16 gradient (oracle/mlp.py); the bias gradients
+// come from the BF16 dZ, which the oracle sums unrounded.
+//
+// TMEM columns (512, one CTA per SM):
+//   0..63     D: layer outputs in the forward pass, dH in the backward pass (FP32)
+//   64..103   H: the hidden A operand; in the backward pass columns 64..95 hold dZ (BF16)
+//   104..111  X: the layer-1 A operand
+//   128..191, 192..255, 256..319   G_1, G_2, G_3 (lane = input unit, column = output unit)
+constexpr int GT_TMEM_COLS = 512;
+constexpr uint32_t GT_COL_G1 = 128, GT_COL_G2 = 192, GT_COL_G3 = 256;
+
+struct MlpGradTcSmem {
+    __nv_bfloat16 W1[MLP_H * K1];      // B of layer 1 [64 x 16]: W1 | b1 hi | b1 lo | 0
+    __nv_bfloat16 W2[MLP_H * TC_K2];   // B of layer 2 [64 x 80]
+    __nv_bfloat16 W3[MLP_H * TC_K2];
+    __nv_bfloat16 W2T[MLP_H * MLP_H];  // B of dH1 = dZ2 W2: rows = input unit, K = output unit
+    __nv_bfloat16 W3T[MLP_H * MLP_H];
+    __nv_bfloat16 XT[TC_M * TC_M];     // A of the weight GEMMs: rows = input unit (+ a ones row), K = sample
+    __nv_bfloat16 H1T[TC_M * TC_M];
+    __nv_bfloat16 H2T[TC_M * TC_M];
+    __nv_bfloat16 DZT[MLP_H * TC_M];   // B of the weight GEMMs: rows = output unit, K = sample
+    float w4[MLP_H];
+    float gw4[MLP_H];
+    float gb4;
+    float b4;
+    double loss;
+    unsigned long long bar;
+    uint32_t tmem_base;
+    int abort;
+};
+static_assert(sizeof(MlpGradTcSmem) + 128 <= 227 * 1024, "one CTA per SM");
+
+__device__ __forceinline__ float bf16_lo(uint32_t p) { return __uint_as_float(p << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t p) { return __uint_as_float(p & 0xffff0000u); }
+__device__ __forceinline__ __nv_bfloat16 bf16_bits(uint32_t b) { return __ushort_as_bfloat16(static_cast<unsigned short>(b)); }
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+k_mlp_grad_tc(const float* __restrict__ prm, int64_t n, const float* __restrict__ feats, const float* __restrict__ target,
+              float* __restrict__ grad, double* __restrict__ loss_out, int32_t* __restrict__ status) {
+    extern __shared__ unsigned char gt_dyn[];
+    MlpGradTcSmem& s = *reinterpret_cast<MlpGradTcSmem*>((reinterpret_cast<uintptr_t>(gt_dyn) + 127) & ~static_cast<uintptr_t>(127));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) {
+        tmem_alloc(smem_u32(&s.tmem_base), GT_TMEM_COLS);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(smem_u32(&s.bar), 1);
+        s.abort = 0;
+        s.gb4 = 0.f;
+        s.loss = 0.0;
+        fence_mbar_init();
+    }
+    for (int t = tid; t < MLP_H * K1; t += TC_THREADS) {
+        const int r = t / K1, k = t % K1;
+        s.W1[umma_k_index(r, k, MLP_H)] = k < MLP_IN ? __float2bfloat16_rn(prm[OFF_W1 + r * MLP_IN + k])
+                                                     : bias_part(prm[OFF_B1 + r], k - MLP_IN);
+    }
+    for (int t = tid; t < MLP_H * TC_K2; t += TC_THREADS) {
+        const int r = t / TC_K2, k = t % TC_K2;
+        const bool w = k < MLP_H;
+        s.W2[umma_k_index(r, k, MLP_H)] = w ? __float2bfloat16_rn(prm[OFF_W2 + r * MLP_H + k]) : bias_part(prm[OFF_B2 + r], k - MLP_H);
+        s.W3[umma_k_index(r, k, MLP_H)] = w ? __float2bfloat16_rn(prm[OFF_W3 + r * MLP_H + k]) : bias_part(prm[OFF_B3 + r], k - MLP_H);
+    }
+    for (int t = tid; t < MLP_H * MLP_H; t += TC_THREADS) {
+        const int o = t / MLP_H, i = t % MLP_H;      // W[o][i]
+        s.W2T[umma_k_index(i, o, MLP_H)] = __float2bfloat16_rn(prm[OFF_W2 + t]);
+        s.W3T[umma_k_index(i, o, MLP_H)] = __float2bfloat16_rn(prm[OFF_W3 + t]);
+    }
+    {   // the ones rows of the transposed inputs (row MLP_IN of XT, row MLP_H of H1T and H2T)
+        const __nv_bfloat16 one = __float2bfloat16_rn(1.f);
+        s.XT[umma_k_index(MLP_IN, tid, TC_M)] = one;
+        s.H1T[umma_k_index(MLP_H, tid, TC_M)] = one;
+        s.H2T[umma_k_index(MLP_H, tid, TC_M)] = one;
+    }
+    if (tid < MLP_H) { s.w4[tid] = prm[OFF_W4 + tid]; s.gw4[tid] = 0.f; }
+    if (tid == 0) s.b4 = prm[OFF_B4];
+    fence_proxy_async_smem();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+
+    const uint32_t tbase = s.tmem_base;
+    const uint32_t tlane = tbase + (static_cast<uint32_t>(warp * 32) << 16);
+    {
+        const uint32_t one2 = pack_bf16(1.f, 1.f);
+        const uint32_t hb[8] = {one2, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        tmem_st_32x32b_x8(tlane + TC_COL_H + MLP_H / 2, hb);
+        tmem_st_32x32b_x4(tlane + TC_COL_X + MLP_IN / 2, one2, 0u, 0u, 0u);
+        tmem_st_wait();
+    }
+    const uint32_t bar = smem_u32(&s.bar);
+    const uint32_t aW1 = smem_u32(s.W1), aW2 = smem_u32(s.W2), aW3 = smem_u32(s.W3), aW2T = smem_u32(s.W2T),
+                   aW3T = smem_u32(s.W3T), aXT = smem_u32(s.XT), aH1T = smem_u32(s.H1T), aH2T = smem_u32(s.H2T),
+                   aDZT = smem_u32(s.DZT);
+    constexpr uint32_t LBO_64 = MLP_H * 16, LBO_128 = TC_M * 16, SBO = 128;
+    const float inv_n = 2.f / static_cast<float>(n);
+    const int64_t ntiles = (n + TC_M - 1) / TC_M;
+    uint32_t phase = 0;
+    bool first = true;
+    int64_t tile = blockIdx.x;
+
+    // one MMA phase: issue (thread 0), commit, bounded wait, then every thread may read TMEM
+    auto sync_mma = [&](auto issue) -> bool {
+        if (tid == 0) {
+            tc_fence_after_sync();
+            issue();
+            umma_commit(bar);
+        }
+        const bool done = mbar_wait_bounded(bar, phase, TC_WAIT_CYCLES);
+        phase ^= 1u;
+        if (!done) s.abort = 1;
+        __syncthreads();
+        tc_fence_after_sync();
+        return s.abort == 0;
+    };
+    // this thread's BF16 value of input unit c for sample tid into a transposed operand
+    auto put_t = [&](__nv_bfloat16* dstT, int rows, int c, __nv_bfloat16 v) { dstT[umma_k_index(c, tid, rows)] = v; };
+    auto finish_epilogue = [&]() {
+        tmem_st_wait();
+        fence_proxy_async_smem();
+        tc_fence_before_sync();
+        __syncthreads();
+    };
+
+    for (; tile < ntiles; tile += gridDim.x) {
+        const int64_t row = tile * TC_M + tid;
+        const bool valid = row < n;
+        {
+            float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f), f1 = f0;
+            if (valid) {
+                f0 = __ldg(reinterpret_cast<const float4*>(feats + row * MLP_IN));
+                f1 = __ldg(reinterpret_cast<const float4*>(feats + row * MLP_IN) + 1);
+            }
+            const uint32_t x01 = pack_bf16(f0.x, f0.y), x23 = pack_bf16(f0.z, f0.w), x45 = pack_bf16(f1.x, f1.y),
+                           x67 = pack_bf16(f1.z, f1.w);
+            tmem_st_32x32b_x4(tlane + TC_COL_X, x01, x23, x45, x67);
+            const uint32_t xp[4] = {x01, x23, x45, x67};
+            #pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                put_t(s.XT, TC_M, 2 * j, bf16_bits(xp[j]));
+                put_t(s.XT, TC_M, 2 * j + 1, bf16_bits(xp[j] >> 16));
+            }
+            finish_epilogue();
+        }
+        // ---- forward
+        uint32_t mask[2][2] = {{0u, 0u}, {0u, 0u}};     // [layer][32-column half]: z > 0
+        float dy = 0.f;
+        #pragma unroll 1
+        for (int layer = 0; layer < 3; ++layer) {
+            const bool ok = sync_mma([&] {
+                if (layer == 0) {
+                    umma_bf16_ts(tbase + TC_COL_D, tbase + TC_COL_X, umma_desc_kmajor(aW1, LBO_64, SBO), TC_IDESC, 0u);
+                } else {
+                    const uint32_t aW = layer == 1 ? aW2 : aW3;
+                    #pragma unroll
+                    for (int ks = 0; ks < TC_K2 / 16; ++ks)
+                        umma_bf16_ts(tbase + TC_COL_D, tbase + TC_COL_H + ks * 8, umma_desc_kmajor(aW + ks * 2 * LBO_64, LBO_64, SBO),
+                                     TC_IDESC, ks > 0 ? 1u : 0u);
+                }
+            });
+            if (!ok) break;
+            float y = 0.f;
+            #pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const int cb = 32 * half;
+                uint32_t v[32];
+                tmem_ld_32x32b_x32(tlane + TC_COL_D + cb, v);
+                tmem_ld_wait(v);
+                if (layer < 2) {
+                    uint32_t h[16], m = 0u;
+                    #pragma unroll
+                    for (int j = 0; j < 16; ++j) h[j] = relu_bf16x2(v[2 * j], v[2 * j + 1]);
+                    #pragma unroll
+                    for (int j = 0; j < 32; ++j) m |= (__uint_as_float(v[j]) > 0.f ? 1u : 0u) << j;
+                    mask[layer][half] = m;
+                    const uint32_t (&h0)[8] = *reinterpret_cast<const uint32_t(*)[8]>(h);
+                    const uint32_t (&h1)[8] = *reinterpret_cast<const uint32_t(*)[8]>(h + 8);
+                    tmem_st_32x32b_x8(tlane + TC_COL_H + cb / 2, h0);
+                    tmem_st_32x32b_x8(tlane + TC_COL_H + cb / 2 + 8, h1);
+                    __nv_bfloat16* dstT = layer == 0 ? s.H1T : s.H2T;
+                    #pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        put_t(dstT, TC_M, cb + 2 * j, bf16_bits(h[j]));
+                        put_t(dstT, TC_M, cb + 2 * j + 1, bf16_bits(h[j] >> 16));
+                    }
+                } else {
+                    #pragma unroll
+                    for (int j = 0; j < 32; ++j) y = fmaf(fmaxf(__uint_as_float(v[j]), 0.f), s.w4[cb + j], y);
+                }
+            }
+            if (layer < 2) {
+                finish_epilogue();
+            } else {
+                // ---- output layer and dZ3
+                y += s.b4;
+                const float e = valid ? y - __ldg(target + row) : 0.f;
+                dy = e * inv_n;
+                double le = static_cast<double>(e) * static_cast<double>(e);
+                float gb = dy;
+                #pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    le += __shfl_xor_sync(0xffffffffu, le, o);
+                    gb += __shfl_xor_sync(0xffffffffu, gb, o);
+                }
+                if (lane == 0) { atomicAdd(&s.loss, le); atomicAdd(&s.gb4, gb); }
+                #pragma unroll
+                for (int half = 0; half < 2; ++half) {
+                    const int cb = 32 * half;
+                    uint32_t v[32];      // z3 of this half, read again now that dy is known
+                    tmem_ld_32x32b_x32(tlane + TC_COL_D + cb, v);
+                    tmem_ld_wait(v);
+                    uint32_t p[16];
+                    #pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        float g = dy * fmaxf(__uint_as_float(v[j]), 0.f);      // d loss / d w4_j
+                        #pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
+                        if (lane == 0) atomicAdd(&s.gw4[cb + j], g);
+                    }
+                    #pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const float d0 = __uint_as_float(v[2 * j]) > 0.f ? dy * s.w4[cb + 2 * j] : 0.f;
+                        const float d1 = __uint_as_float(v[2 * j + 1]) > 0.f ? dy * s.w4[cb + 2 * j + 1] : 0.f;
+                        p[j] = pack_bf16(d0, d1);
+                        put_t(s.DZT, MLP_H, cb + 2 * j, bf16_bits(p[j]));
+                        put_t(s.DZT, MLP_H, cb + 2 * j + 1, bf16_bits(p[j] >> 16));
+                    }
+                    const uint32_t (&p0)[8] = *reinterpret_cast<const uint32_t(*)[8]>(p);
+                    const uint32_t (&p1)[8] = *reinterpret_cast<const uint32_t(*)[8]>(p + 8);
+                    tmem_st_32x32b_x8(tlane + TC_COL_H + cb / 2, p0);
+                    tmem_st_32x32b_x8(tlane + TC_COL_H + cb / 2 + 8, p1);
+                }
+                finish_epilogue();
+            }
+        }
+        if (s.abort) break;
+        // ---- backward: l = 3, 2, 1
+        #pragma unroll 1
+        for (int l = 3; l >= 1; --l) {
+            const uint32_t aA = l == 3 ? aH2T : (l == 2 ? aH1T : aXT);
+            const uint32_t colG = l == 3 ? GT_COL_G3 : (l == 2 ? GT_COL_G2 : GT_COL_G1);
+            const uint32_t aWT = l == 3 ? aW3T : aW2T;
+            const bool acc0 = !first;
+            const bool ok = sync_mma([&] {
+                #pragma unroll
+                for (int ks = 0; ks < TC_M / 16; ++ks)
+                    umma_bf16_ss(tbase + colG, umma_desc_kmajor(aA + ks * 2 * LBO_128, LBO_128, SBO),
+                                 umma_desc_kmajor(aDZT + ks * 2 * LBO_64, LBO_64, SBO), TC_IDESC, (acc0 || ks > 0) ? 1u : 0u);
+                if (l > 1) {
+                    #pragma unroll
+                    for (int ks = 0; ks < MLP_H / 16; ++ks)
+                        umma_bf16_ts(tbase + TC_COL_D, tbase + TC_COL_H + ks * 8, umma_desc_kmajor(aWT + ks * 2 * LBO_64, LBO_64, SBO),
+                                     TC_IDESC, ks > 0 ? 1u : 0u);
+                }
+            });
+            if (!ok) break;
+            if (l == 1) break;
+            // dZ_{l-1} = dH_{l-1} * [z_{l-1} > 0]
+            #pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const int cb = 32 * half;
+                const uint32_t m = mask[l - 2][half];
+                uint32_t v[32];
+                tmem_ld_32x32b_x32(tlane + TC_COL_D + cb, v);
+                tmem_ld_wait(v);
+                uint32_t p[16];
+                #pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const float d0 = ((m >> (2 * j)) & 1u) ? __uint_as_float(v[2 * j]) : 0.f;
+                    const float d1 = ((m >> (2 * j + 1)) & 1u) ? __uint_as_float(v[2 * j + 1]) : 0.f;
+                    p[j] = pack_bf16(d0, d1);
+                    put_t(s.DZT, MLP_H, cb + 2 * j, bf16_bits(p[j]));
+                    put_t(s.DZT, MLP_H, cb + 2 * j + 1, bf16_bits(p[j] >> 16));
+                }
+                if (l == 3) {     // dZ2 is the A operand of dH1 = dZ2 W2
+                    const uint32_t (&p0)[8] = *reinterpret_cast<const uint32_t(*)[8]>(p);
+                    const uint32_t (&p1)[8] = *reinterpret_cast<const uint32_t(*)[8]>(p + 8);
+                    tmem_st_32x32b_x8(tlane + TC_COL_H + cb / 2, p0);
+                    tmem_st_32x32b_x8(tlane + TC_COL_H + cb / 2 + 8, p1);
+                }
+            }
+            finish_epilogue();
+        }
+        if (s.abort) break;
+        first = false;
+    }
+    if (s.abort) {
+        if (tid == 0) {
+            (void)mbar_wait_bounded(bar, phase ^ 1u, TC_WAIT_CYCLES);
+            if (status) atomicOr(status, SPH_STATUS_TIMEOUT);
+        }
+    } else if (!first) {
+        // this thread's TMEM lane of G_1..G_3: input unit r = tid, every output unit
+        const int r = tid;
+        #pragma unroll 1
+        for (int l = 1; l <= 3; ++l) {
+            const uint32_t colG = l == 3 ? GT_COL_G3 : (l == 2 ? GT_COL_G2 : GT_COL_G1);
+            const int nin = l == 1 ? MLP_IN : MLP_H;
+            const int offW = l == 1 ? OFF_W1 : (l == 2 ? OFF_W2 : OFF_W3), offB = l == 1 ? OFF_B1 : (l == 2 ? OFF_B2 : OFF_B3);
+            #pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                uint32_t v[32];
+                tmem_ld_32x32b_x32(tlane + colG + 32 * half, v);
+                tmem_ld_wait(v);
+                if (r < nin) {
+                    #pragma unroll 4
+                    for (int j = 0; j < 32; ++j) atomicAdd(&grad[offW + (32 * half + j) * nin + r], __uint_as_float(v[j]));
+                } else if (r == nin) {
+                    #pragma unroll 4
+                    for (int j = 0; j < 32; ++j) atomicAdd(&grad[offB + 32 * half + j], __uint_as_float(v[j]));
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < MLP_H) atomicAdd(&grad[OFF_W4 + tid], s.gw4[tid]);
+        if (tid == 0) {
+            atomicAdd(&grad[OFF_B4], s.gb4);
+            atomicAdd(loss_out, s.loss);
+        }
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after_sync();
+        tmem_dealloc(tbase, GT_TMEM_COLS);
+    }
+}
+
+static int grad_tc_smem_bytes() { return (int)sizeof(MlpGradTcSmem) + 128; }
+
 static int train_smem_bytes() { return (int)sizeof(MlpSmemTrain); }
 
 }  // namespace wsph
@@ -602,6 +949,30 @@ int sph_mlp_grad(const float* params, int64_t n, const float* feats, const float
     count_launch();
     k_mlp_grad<<<grid, MLP_THREADS, train_smem_bytes(), s>>>(params, n, feats, target, grad, loss);
     return check_launch("sph_mlp_grad");
+}
+
+int sph_mlp_grad_tc(const float* params, int64_t n, const float* feats, const float* target, float* grad, double* loss,
+                    int32_t* status, void* stream) {
+    if (n < 0) return set_error(SPH_ERR_BAD_ARG, "sph_mlp_grad_tc: n < 0");
+    WSPH_CHECK_PTR(params); WSPH_CHECK_PTR(grad); WSPH_CHECK_PTR(loss);
+    cudaStream_t s = WSPH_STREAM(stream);
+    cudaMemsetAsync(grad, 0, sizeof(float) * MLP_NPARAM, s);
+    cudaMemsetAsync(loss, 0, sizeof(double), s);
+    if (n == 0) return check_launch("sph_mlp_grad_tc");
+    WSPH_CHECK_PTR(feats); WSPH_CHECK_PTR(target);
+    if (reinterpret_cast<uintptr_t>(feats) & 15) return set_error(SPH_ERR_BAD_ARG, "sph_mlp_grad_tc: feats must be 16-byte aligned");
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(k_mlp_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, grad_tc_smem_bytes());
+    });
+    if (attr_err != cudaSuccess)
+        return set_error(SPH_ERR_CUDA, "sph_mlp_grad_tc: shared memory opt-in: %s", cudaGetErrorString(attr_err));
+    const int64_t tiles = (n + TC_M - 1) / TC_M;
+    const int grid = (int)(tiles < 148 ? tiles : 148);
+    count_launch();
+    k_mlp_grad_tc<<<grid, TC_THREADS, grad_tc_smem_bytes(), s>>>(params, n, feats, target, grad, loss, status);
+    return check_launch("sph_mlp_grad_tc");
 }
 
 int sph_mlp_adam(float* params, const float* grad, float* m1, float* m2, int64_t count, float lr, float beta1, float beta2, float eps,

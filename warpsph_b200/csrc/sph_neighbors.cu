@@ -521,12 +521,13 @@ __device__ __forceinline__ void verlet_flush_part(int lane, int wib, int& nb, in
 // past the end of a cell hold a record at 3e38, which no test accepts, so the unrolled
 // candidate loop needs no bound check.
 //
-// Acceptance bits (masks non-null, not MI): the count pass reserves 32 words per candidate
-// chunk of its work item from a bounded pool and stores each lane's 32 acceptance bits per
-// chunk; the fill pass then visits only the accepted candidates, in the same order, and
-// repeats the distance arithmetic only to split them into the interacting prefix and the
-// rest.  A work item that found the pool exhausted tests every candidate again.
-template <int D, bool MI>
+// Acceptance bits (masks non-null, not MI): the count pass reserves 64 words per candidate
+// chunk of its work item from a bounded pool and stores each lane's 32 acceptance bits and 32
+// interacting bits per chunk; the fill pass then walks the candidates that some lane accepted,
+// in the same order, and files each into the interacting prefix or the rest from the bits,
+// without distance arithmetic.  A work item that found the pool exhausted tests every
+// candidate again.
+template <int D, bool MI, bool SH = true>
 __device__ __forceinline__ void verlet_pair(const Vec<D>& xi, float Hi, const float4& rj, const float* sh, const DomainF& dom,
                                             float vs, float& r2, float& Hm, float& R) {
     Hm = fmaxf(Hi, rj.w);
@@ -542,11 +543,32 @@ __device__ __forceinline__ void verlet_pair(const Vec<D>& xi, float Hi, const fl
                 else if (d < -dom.halfL[a]) d = __fadd_rn(d, dom.L[a]);
             }
             dv.v[a] = d;
-        } else {
+        } else if (SH) {
             dv.v[a] = __fsub_rn(__fsub_rn(xi.v[a], xj), sh[a]);
+        } else {
+            dv.v[a] = __fsub_rn(xi.v[a], xj);     // equal to the above with sh = 0 (x - 0 = x exactly)
         }
     }
     r2 = dist2_rn<D>(dv);
+}
+
+// The count pass over one staged chunk: acceptance and interacting bits of the lane's
+// particle against the (up to 32) staged candidates; padded slots never match.
+template <int D, bool MI, bool SH>
+__device__ __forceinline__ void verlet_count_chunk(const Vec<D>& xi, float Hi, bool active, bool part, const float4* __restrict__ sr,
+                                                   const float* sh, const DomainF& dom, float vs, int mcount, uint32_t& hm,
+                                                   uint32_t& im) {
+    for (int u0 = 0; u0 < mcount; u0 += 8) {
+        #pragma unroll
+        for (int du = 0; du < 8; ++du) {
+            const int u = u0 + du;
+            float r2, Hm, R;
+            verlet_pair<D, MI, SH>(xi, Hi, sr[u], sh, dom, vs, r2, Hm, R);
+            const bool hit = active & (r2 < __fmul_rn(R, R));
+            hm |= hit ? (1u << u) : 0u;
+            if (part) im |= (hit && interacting_pair(r2, Hm)) ? (1u << u) : 0u;
+        }
+    }
 }
 
 template <int D, bool FILL, bool MI>
@@ -590,7 +612,7 @@ __device__ __forceinline__ void verlet_task(int task, int lane, int wib, const f
             int nch = 0;
             for (int q = 0; q < nk; ++q) nch += (cell_end[keys[q]] - cell_begin[keys[q]] + 31) >> 5;
             if (lane == 0) {
-                const unsigned long long need = 32ull * (unsigned long long)nch;
+                const unsigned long long need = 64ull * (unsigned long long)nch;
                 const unsigned long long o = atomicAdd(mask_cursor, need);
                 mbase = o + need <= (unsigned long long)mask_words ? (int)o : -1;
                 mask_base[task] = mbase;
@@ -606,43 +628,52 @@ __device__ __forceinline__ void verlet_task(int task, int lane, int wib, const f
         const int b = cell_begin[keys[q]], e = cell_end[keys[q]];
         const float sh[3] = {shifts[3 * q], shifts[3 * q + 1], shifts[3 * q + 2]};
         for (int k0 = b; k0 < e; k0 += 32, ++ch) {
-            uint32_t m = 0;
             if (FILL && mbase >= 0) {
-                m = active ? masks[mbase + 32 * ch + lane] : 0u;
-                if (!__any_sync(0xffffffffu, m != 0u)) continue;
+                const uint32_t m = active ? masks[mbase + 64 * ch + lane] : 0u;
+                const uint32_t im = active ? masks[mbase + 64 * ch + 32 + lane] : 0u;
+                uint32_t U = __reduce_or_sync(0xffffffffu, m);
+                if (U == 0u) continue;
+                __syncwarp();
+                if (k0 + lane < e) sidx[wib][lane] = sort_index[k0 + lane];
+                __syncwarp();
+                // the candidates some lane accepted, in candidate order; each lane files at
+                // most one entry per candidate, so 8 candidates fit between two flushes
+                for (int r = 0; U != 0u; ++r) {
+                    if ((r & 7) == 0 && __any_sync(0xffffffffu, nb > VS - 8 || nib > VS - 8)) {
+                        __syncwarp();
+                        verlet_flush_part(lane, wib, nib, iwritten, row, sibuf, list);
+                        verlet_flush_part(lane, wib, nb, written, tail, sbuf, list);
+                        __syncwarp();
+                    }
+                    const int u = __ffs(U) - 1;
+                    U &= U - 1u;
+                    if ((m >> u) & 1u) {
+                        const int j = sidx[wib][u];
+                        if ((im >> u) & 1u) sibuf[wib][lane][nib++] = j;
+                        else sbuf[wib][lane][nb++] = j;
+                    }
+                }
+                continue;
             }
             __syncwarp();
             const bool real = k0 + lane < e;
             srec[wib][lane] = real ? recs[k0 + lane] : far;
             if (FILL && real) sidx[wib][lane] = sort_index[k0 + lane];
             __syncwarp();
-            if (FILL && mbase >= 0) {
-                // accepted candidates only, lowest bit (candidate order) first, up to 8 per
-                // lane between two flushes
-                while (__any_sync(0xffffffffu, m != 0u)) {
-                    if (__any_sync(0xffffffffu, nb > VS - 8 || nib > VS - 8)) {
-                        __syncwarp();
-                        verlet_flush_part(lane, wib, nib, iwritten, row, sibuf, list);
-                        verlet_flush_part(lane, wib, nb, written, tail, sbuf, list);
-                        __syncwarp();
-                    }
-                    #pragma unroll
-                    for (int r = 0; r < 8; ++r) {
-                        if (m != 0u) {
-                            const int u = __ffs(m) - 1;
-                            m &= m - 1u;
-                            float r2, Hm, R;
-                            verlet_pair<D, MI>(xi, Hi, srec[wib][u], sh, dom, vs, r2, Hm, R);
-                            const int j = sidx[wib][u];
-                            if (part && interacting_pair(r2, Hm)) sibuf[wib][lane][nib++] = j;
-                            else sbuf[wib][lane][nb++] = j;
-                        }
-                    }
-                }
-                continue;
-            }
             const int mcount = min(32, e - k0);
-            uint32_t hm = 0;
+            if constexpr (!FILL) {
+                uint32_t hm = 0, im = 0;
+                if (!MI && sh[0] == 0.f && sh[1] == 0.f && sh[2] == 0.f)
+                    verlet_count_chunk<D, MI, false>(xi, Hi, active, part, srec[wib], sh, dom, vs, mcount, hm, im);
+                else
+                    verlet_count_chunk<D, MI, true>(xi, Hi, active, part, srec[wib], sh, dom, vs, mcount, hm, im);
+                cnt += __popc(hm);
+                icnt += __popc(im);
+                if (mbase >= 0) {
+                    masks[mbase + 64 * ch + lane] = hm;
+                    masks[mbase + 64 * ch + 32 + lane] = im;
+                }
+            } else {
             for (int u0 = 0; u0 < mcount; u0 += 8) {
                 // room for the next 8 candidates in every lane's buffers
                 if (FILL && __any_sync(0xffffffffu, nb > VS - 8 || nib > VS - 8)) {
@@ -658,20 +689,14 @@ __device__ __forceinline__ void verlet_task(int task, int lane, int wib, const f
                     verlet_pair<D, MI>(xi, Hi, srec[wib][u], sh, dom, vs, r2, Hm, R);
                     const bool hit = active & (r2 < __fmul_rn(R, R));
                     const bool inter = part && hit && interacting_pair(r2, Hm);
-                    if (FILL) {
-                        if (hit) {
-                            const int j = sidx[wib][u];
-                            if (inter) sibuf[wib][lane][nib++] = j;
-                            else sbuf[wib][lane][nb++] = j;
-                        }
-                    } else {
-                        cnt += hit;
-                        icnt += inter;
-                        hm |= (uint32_t)hit << u;
+                    if (hit) {
+                        const int j = sidx[wib][u];
+                        if (inter) sibuf[wib][lane][nib++] = j;
+                        else sbuf[wib][lane][nb++] = j;
                     }
                 }
             }
-            if (!FILL && mbase >= 0) masks[mbase + 32 * ch + lane] = hm;
+            }
         }
     }
     if (FILL) {
@@ -773,11 +798,12 @@ struct NbWs {
     int64_t mask_words;
     int64_t bytes;
 };
-// Acceptance-bit budget: 64 words per particle (the 3D walk needs about 58: 27 stencil cells
-// of about two 32-candidate chunks per 32 particles), at most 2^28 words.  Work items past the
-// budget test their candidates again in the fill pass.
+// Acceptance-bit budget: 128 words per particle (the 3D walk needs about 116: 27 stencil
+// cells of about two 32-candidate chunks per 32 particles, two words per lane and chunk), at
+// most 2^28 words (1 GiB).  Work items past the budget test their candidates again in the
+// fill pass.
 static int64_t mask_budget(int64_t n) {
-    int64_t w = n * 64;
+    int64_t w = n * 128;
     return w < ((int64_t)1 << 28) ? w : ((int64_t)1 << 28);
 }
 static int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }

@@ -805,7 +805,7 @@ _mlp_status: dict = {}
 
 
 def mlp_status(device) -> torch.Tensor:
-    """The device int32 word into which sph_mlp_forward_tc ors SPH_STATUS_TIMEOUT."""
+    """The device int32 word into which sph_mlp_forward_tc and sph_mlp_grad_tc or SPH_STATUS_TIMEOUT."""
     dev = torch.device(device)
     st = _mlp_status.get(dev.index)
     if st is None:
@@ -846,13 +846,28 @@ def mlp_forward(theta, feats, scale=None, tensor_cores: str = "tcgen05") -> torc
     return out
 
 
-def mlp_grad(theta, feats, target):
-    """(grad [P] float32, loss [1] float64 = sum of squared errors) of the MSE."""
+def mlp_grad(theta, feats, target, tensor_cores: str = "tcgen05"):
+    """(grad [P] float32, loss [1] float64 = sum of squared errors) of the MSE.
+    tensor_cores "tcgen05" runs sph_mlp_grad_tc (every GEMM on tcgen05, the weight
+    gradients accumulated in TMEM); "mma" runs sph_mlp_grad (warp-level mma.sync)."""
     g = torch.empty_like(theta)
     loss = torch.empty(1, device=theta.device, dtype=torch.float64)
-    with _timed("mlp_grad"):
-        check(_capi.lib().sph_mlp_grad(fptr(theta), feats.shape[0], fptr(feats.contiguous()), fptr(target.contiguous()), ptr(g),
-                                       ptr(loss), stream_ptr(theta.device)), "sph_mlp_grad")
+    f = feats.contiguous()
+    t = target.contiguous()
+    if tensor_cores == "tcgen05":
+        if f.device.index in _mlp_suspect:
+            raise RuntimeError(f"tcgen05 MLP gradient on {f.device}: an earlier launch timed out; the context is suspect")
+        if f.data_ptr() % 16:
+            f = f.clone()
+        with _timed("mlp_grad"):
+            check(_capi.lib().sph_mlp_grad_tc(fptr(theta), f.shape[0], fptr(f), fptr(t), ptr(g), ptr(loss), ptr(mlp_status(f.device)),
+                                              stream_ptr(theta.device)), "sph_mlp_grad_tc")
+    elif tensor_cores == "mma":
+        with _timed("mlp_grad"):
+            check(_capi.lib().sph_mlp_grad(fptr(theta), f.shape[0], fptr(f), fptr(t), ptr(g), ptr(loss), stream_ptr(theta.device)),
+                  "sph_mlp_grad")
+    else:
+        raise ValueError(f"tensor_cores must be 'tcgen05' or 'mma', not {tensor_cores!r}")
     return g, loss
 
 
