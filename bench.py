@@ -324,7 +324,8 @@ def ensemble_throughput(dev, chunks: int = 6) -> dict:
 
 def mlp_forward_throughput(dev, n: int = 1 << 24, reps: int = 20) -> dict:
     """The warm-start network's forward pass on n feature rows (n x 32 B, larger than L2)
-    through both tensor-core kernels: tcgen05 (TMEM accumulators) and mma.sync."""
+    through both tensor-core kernels, tcgen05 (TMEM accumulators) and mma.sync, and the
+    training gradient on min(n, 2^22) rows through both."""
     import torch
     from warpsph_b200 import learned, ops
     peaks = load_peaks()
@@ -347,9 +348,29 @@ def mlp_forward_throughput(dev, n: int = 1 << 24, reps: int = 20) -> dict:
         ms = e0.elapsed_time(e1) / reps
         tf = n * flops / (ms * 1e-3) / 1e12
         out[tc] = {"ms": ms, "samples_per_s": n / (ms * 1e-3), "tflops": tf, "frac": tf / peaks["bf16_tflops"]}
+    # the training gradient (forward with kept activations, then the backward GEMMs): per
+    # sample the forward's FLOPs, the two data-gradient GEMMs (2 x 2 x 64 x 64) and the three
+    # weight-gradient GEMMs (2 x (2 x 64 x 64 + 64 x 8))
+    gflops = flops + 2 * (2 * 64 * 64) + 2 * (2 * 64 * 64 + 64 * 8)
+    ng = min(n, 1 << 22)
+    fg, tg = feats[:ng].contiguous(), torch.randn(ng, device=dev, generator=g)
+    out["grad"] = {"samples": ng, "flop_per_sample": gflops}
+    for tc in ("tcgen05", "mma"):
+        for _ in range(3):
+            ops.mlp_grad(theta, fg, tg, tensor_cores=tc)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            ops.mlp_grad(theta, fg, tg, tensor_cores=tc)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        tf = ng * gflops / (ms * 1e-3) / 1e12
+        out["grad"][tc] = {"ms": ms, "samples_per_s": ng / (ms * 1e-3), "tflops": tf, "frac": tf / peaks["bf16_tflops"]}
     st = int(ops.mlp_status(dev).item())
     if st:
-        raise RuntimeError(f"sph_mlp_forward_tc reported status {st:#x}")
+        raise RuntimeError(f"tcgen05 MLP kernels reported status {st:#x}")
     return out
 
 
