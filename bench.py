@@ -46,7 +46,7 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nx", type=int, default=512)
-    ap.add_argument("--cpu-steps", type=int, default=1, help="steps of the CPU baseline sample")
+    ap.add_argument("--cpu-steps", type=int, default=8, help="steps of the CPU baseline sample (about 1 s each on 16 cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--breakdown", action="store_true", help="print a per-kernel time breakdown to stderr")
@@ -57,6 +57,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-mlp", action="store_true", help="skip the warm-start MLP forward throughput")
     ap.add_argument("--mlp-samples", type=int, default=1 << 24, help="feature rows of the MLP forward section")
     ap.add_argument("--nx3d", type=int, default=128, help="lattice size of the CRKSPH Sedov 3D section (nx^3 particles)")
+    ap.add_argument("--list-build-only", type=int, default=0, metavar="NX",
+                    help="only time three neighbour-list builds of a periodic NX^3 lattice (128 neighbours) and exit")
     return ap.parse_args(argv)
 
 
@@ -408,11 +410,12 @@ def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, step
     torch.cuda.synchronize()
     S = box["system"].state
     c0 = ops.conservation_sums(params, S.masses, S.velocities, S.internalEnergies).cpu().numpy()
-    timer = ops.KernelTimer(names={timed_kernel}) if timed_kernel else None
+    timer = ops.KernelTimer(names={timed_kernel, "neighbors_build"}) if timed_kernel else None
     ops.TIMER = timer
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     gc.collect()
     gc.disable()
+    a0 = torch.cuda.memory_stats(dev)
     try:
         e0.record()
         for _ in range(steps):
@@ -421,6 +424,7 @@ def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, step
         torch.cuda.synchronize()
     finally:
         gc.enable()
+    a1 = torch.cuda.memory_stats(dev)
     ops.TIMER = None
     ms = e0.elapsed_time(e1)
     S = box["system"].state
@@ -428,8 +432,12 @@ def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, step
     out = {"particles": int(n), "neighbours": neighbours, "steps": steps, "ms_per_step": ms / steps,
            "value": n * steps / (ms / 1e3), "unit": UNIT, "compensated_sums": kahan,
            "energy_drift_timed_steps": float(abs(c1[3] - c0[3]) / c0[3]),
-           "verlet_entries_per_particle": box["system"].adjacency.nnz / n}
+           "verlet_entries_per_particle": box["system"].adjacency.nnz / n,
+           "allocator_in_timed_region": {key: int(a1.get(key, 0) - a0.get(key, 0)) for key in
+                                         ("num_device_alloc", "num_device_free", "num_alloc_retries")}}
     if timer is not None:
+        nb = timer.summary().get("neighbors_build")
+        out["list_builds_timed"] = nb["launches"] if nb else 0
         k = timer.summary().get(timed_kernel)
         if k:
             peaks = load_peaks()
@@ -679,8 +687,34 @@ def gpu_arm(args, rank: int, world: int):
     return 0
 
 
+def list_build_only(nx: int) -> int:
+    """Three full neighbour-list builds (sph_neighbors_build through ops.buildVerletList)
+    of a periodic nx^3 lattice with Wendland C4 supports for 128 neighbours; prints one JSON
+    line with the wall time of each build."""
+    import torch
+    import warpsph_b200 as ws
+    from warpsph_b200 import ops
+    dev = torch.device("cuda")
+    dom = ws.buildDomainDescription(1.0, 3, True, dev)
+    cfg, _ = ws.buildConfig(dim=3, domain=dom, kernel=ws.KernelFunctions.Wendland4, targetNeighbors=128, device=dev)
+    x, H, _, _ = ws.buildPointCloud(nx, dom, cfg.targetNeighbors, device=dev)
+    p = ws.make_params(cfg)
+    ms, entries = [], 0.0
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        adj = ops.buildVerletList(x, H, p, cfg.verletScale)
+        torch.cuda.synchronize()
+        ms.append(1e3 * (time.perf_counter() - t0))
+        entries = adj.nnz / x.shape[0]
+    print(json.dumps({"list_build": {"particles": int(x.shape[0]), "verlet_entries_per_particle": entries, "ms": ms}}), flush=True)
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
+    if args.list_build_only:
+        return list_build_only(args.list_build_only)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -414,6 +414,18 @@ int sph_compsph_accel_dudt(const SphParams* p, int64_t n, const float* x, const 
                            const int32_t* offs, const int32_t* cnt, const int32_t* list,
                            const int32_t* verlet_cnt, float* dvdt_out, float* dudt_out,
                            float* dEdt_out, float* ap_ij, float* av_ij, void* stream);
+/* The same pass over packed particle records: a first launch copies the fields the pass
+ * reads into records [n, R] (R = sph_compsph_record_floats(dim) floats per particle: 12, 12
+ * and 16 in 1D, 2D and 3D; 16-byte aligned, caller-owned scratch; null c, alpha, omega take
+ * their defaults there), and the pair launch gathers each neighbour from that one record.
+ * Outputs and arguments otherwise as sph_compsph_accel_dudt. */
+int sph_compsph_record_floats(int32_t dim);
+int sph_compsph_accel_dudt_packed(const SphParams* p, int64_t n, const float* x, const float* H,
+                                  const float* m, const float* rho, const float* v, const float* c,
+                                  const float* alpha, const float* P, const float* omega,
+                                  const int32_t* offs, const int32_t* cnt, const int32_t* list,
+                                  const int32_t* verlet_cnt, float* dvdt_out, float* dudt_out,
+                                  float* dEdt_out, float* ap_ij, float* av_ij, float* records, void* stream);
 /* The same pass under the reference's two wrapper names. */
 int sph_compsph_accel(const SphParams* p, int64_t n, const float* x, const float* H,
                       const float* m, const float* rho, const float* v, const float* c,

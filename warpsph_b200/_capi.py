@@ -125,6 +125,8 @@ _PROTOS = {
     "sph_compsph_prep": [_P, _I64] + [_P] * 12,
     "sph_grad_h_omega": [_P, _I64] + [_P] * 9,
     "sph_compsph_accel_dudt": [_P, _I64] + [_P] * 19,
+    "sph_compsph_record_floats": [_I32],
+    "sph_compsph_accel_dudt_packed": [_P, _I64] + [_P] * 20,
     "sph_compsph_accel": [_P, _I64] + [_P] * 17,
     "sph_compsph_dudt": [_P, _I64] + [_P] * 14,
     "sph_monaghan_rhs": [_P, _I64] + [_P] * 22,

@@ -89,11 +89,51 @@ k_compsph_prep(int n, DevParams P, const float* __restrict__ x, const float* __r
 // (accel.py:195-198).  Walking the interacting prefix of each Verlet row (cnt =
 // interacting counts) with vcnt = the Verlet counts, the ap_ij / av_ij entries of the
 // rest of the row are written as zeros.
-template <int KF, int D, int G>
+// Packed per-particle record of the CompSPH accel pass: position and support first (read
+// before the distance test), then velocity, mass, density, pressure, sound speed, switch
+// and grad-h factor, in one block of R floats (16-byte granules), so a neighbour is R/4
+// 128-bit loads from one record instead of 2D + 8 scalar loads from as many arrays.  The
+// optional fields take their defaults at pack time (sound speed c_s, switch 1, Omega 1).
+template <int D> struct CompRec {
+    static constexpr int X = 0, H = D, V = D + 1, M = 2 * D + 1, RHO = M + 1, P = M + 2, C = M + 3, AL = M + 4, OM = M + 5,
+                         END = M + 6, R = (END + 3) / 4 * 4, K1 = (H + 1 + 3) / 4, K2 = R / 4;
+};
+
+template <int D>
+__global__ void k_compsph_pack(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
+                               const float* __restrict__ rho, const float* __restrict__ v, const float* __restrict__ c,
+                               const float* __restrict__ alpha, const float* __restrict__ Pr, const float* __restrict__ omega,
+                               float* __restrict__ rec) {
+    using L = CompRec<D>;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float r[L::R];
+    #pragma unroll
+    for (int a = 0; a < D; ++a) { r[L::X + a] = x[(size_t)i * D + a]; r[L::V + a] = v[(size_t)i * D + a]; }
+    r[L::H] = H[i]; r[L::M] = m[i]; r[L::RHO] = rho[i]; r[L::P] = Pr[i];
+    r[L::C] = c ? c[i] : P.c_s; r[L::AL] = alpha ? alpha[i] : 1.f; r[L::OM] = omega ? omega[i] : 1.f;
+    #pragma unroll
+    for (int a = L::END; a < L::R; ++a) r[a] = 0.f;
+    float4* dst = reinterpret_cast<float4*>(rec + (size_t)i * L::R);
+    #pragma unroll
+    for (int k = 0; k < L::R / 4; ++k) dst[k] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
+}
+
+template <int D, int K0, int K1>
+__device__ __forceinline__ void comp_granules(const float4* __restrict__ src, float (&r)[CompRec<D>::R]) {
+    #pragma unroll
+    for (int k = K0; k < K1; ++k) {
+        const float4 t = __ldg(src + k);
+        r[4 * k] = t.x; r[4 * k + 1] = t.y; r[4 * k + 2] = t.z; r[4 * k + 3] = t.w;
+    }
+}
+
+template <int KF, int D, int G, bool REC>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
                      const float* __restrict__ rho, const float* __restrict__ v, const float* __restrict__ c,
                      const float* __restrict__ alpha, const float* __restrict__ Pr, const float* __restrict__ omega,
+                     const float* __restrict__ rec,
                      const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
                      const int32_t* __restrict__ vcnt, float* __restrict__ dvdt, float* __restrict__ dudt,
                      float* __restrict__ dEdt, float* __restrict__ ap, float* __restrict__ av) {
@@ -105,17 +145,40 @@ k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const floa
     du.init();
     if (g.valid) {
         const int i = g.i;
-        Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
-        const float Hi = H[i], rhoi = rho[i], Pi = Pr[i];
-        const float ci = c ? c[i] : P.c_s, ai = alpha ? alpha[i] : 1.f, omi = omega ? omega[i] : 1.f;
+        using L = CompRec<D>;
+        Vec<D> xi, vi;
+        float Hi, rhoi, Pi, ci, ai, omi;
+        if constexpr (REC) {
+            float r[L::R];
+            comp_granules<D, 0, L::K2>(reinterpret_cast<const float4*>(rec + (size_t)i * L::R), r);
+            #pragma unroll
+            for (int a = 0; a < D; ++a) { xi.v[a] = r[L::X + a]; vi.v[a] = r[L::V + a]; }
+            Hi = r[L::H]; rhoi = r[L::RHO]; Pi = r[L::P]; ci = r[L::C]; ai = r[L::AL]; omi = r[L::OM];
+        } else {
+            xi = load_vec<D>(x, i); vi = load_vec<D>(v, i);
+            Hi = H[i]; rhoi = rho[i]; Pi = Pr[i];
+            ci = c ? c[i] : P.c_s; ai = alpha ? alpha[i] : 1.f; omi = omega ? omega[i] : 1.f;
+        }
         const float invHi = 1.f / Hi;
         const float pTi = Pi / (rhoi * rhoi) / omi;
         int b = offs[i], e = b + cnt[i];
         for (int q = b + g.lane; q < e; q += G) {
             int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            float rj[L::R];
+            const float4* sj = REC ? reinterpret_cast<const float4*>(rec + (size_t)j * L::R) : nullptr;
+            Vec<D> xj;
+            float Hj;
+            if constexpr (REC) {
+                comp_granules<D, 0, L::K1>(sj, rj);
+                #pragma unroll
+                for (int a = 0; a < D; ++a) xj.v[a] = rj[L::X + a];
+                Hj = rj[L::H];
+            } else {
+                xj = load_vec<D>(x, j);
+                Hj = __ldg(H + j);
+            }
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r2 = dot<D>(xij, xij);
-            float Hj = __ldg(H + j);
             float Hm = wmax(Hi, Hj);
             if (!(r2 < Hm * Hm)) {
                 if (ap) store_vec<D>(ap, k, vzero<D>());
@@ -123,9 +186,18 @@ k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const floa
                 continue;
             }
             float r = safe_sqrt(r2);
-            Vec<D> vj = load_vec<D>(v, j);
-            const float mj = __ldg(m + j), rhoj = __ldg(rho + j), Pj = __ldg(Pr + j);
-            const float cj = c ? __ldg(c + j) : P.c_s, aj = alpha ? __ldg(alpha + j) : 1.f, omj = omega ? __ldg(omega + j) : 1.f;
+            Vec<D> vj;
+            float mj, rhoj, Pj, cj, aj, omj;
+            if constexpr (REC) {
+                comp_granules<D, L::K1, L::K2>(sj, rj);
+                #pragma unroll
+                for (int a = 0; a < D; ++a) vj.v[a] = rj[L::V + a];
+                mj = rj[L::M]; rhoj = rj[L::RHO]; Pj = rj[L::P]; cj = rj[L::C]; aj = rj[L::AL]; omj = rj[L::OM];
+            } else {
+                vj = load_vec<D>(v, j);
+                mj = __ldg(m + j); rhoj = __ldg(rho + j); Pj = __ldg(Pr + j);
+                cj = c ? __ldg(c + j) : P.c_s; aj = alpha ? __ldg(alpha + j) : 1.f; omj = omega ? __ldg(omega + j) : 1.f;
+            }
             const float Vj = mj / rhoj;
             const float rho_bar = 0.5f * (rhoi + rhoj);
             float ux = 0.f;
@@ -175,8 +247,16 @@ k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const floa
     if (dvdt) store_vec<D>(dvdt, i, ov);
     if (dudt) dudt[i] = od;
     if (dEdt) {
-        Vec<D> vi = load_vec<D>(v, i);
-        const float mi = m[i];
+        Vec<D> vi;
+        float mi;
+        if constexpr (REC) {
+            #pragma unroll
+            for (int a = 0; a < D; ++a) vi.v[a] = __ldg(rec + (size_t)i * CompRec<D>::R + CompRec<D>::V + a);
+            mi = __ldg(rec + (size_t)i * CompRec<D>::R + CompRec<D>::M);
+        } else {
+            vi = load_vec<D>(v, i);
+            mi = m[i];
+        }
         dEdt[i] = mi * dot<D>(vi, ov) + mi * od;
     }
 }
@@ -326,10 +406,37 @@ int sph_compsph_accel_dudt(const SphParams* p, int64_t n, const float* x, const 
         (rc = check_align_vec(P, ap_ij, "ap_ij")) || (rc = check_align_vec(P, av_ij, "av_ij")))
         return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_compsph_accel_dudt<KF, D, G_HEAVY><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>(
-                              (int)n, P, x, H, m, rho, v, c, alpha, Pr, omega, offs, cnt, list, verlet_cnt, dvdt_out, dudt_out, dEdt_out,
-                              ap_ij, av_ij)));
+    WSPH_DISPATCH_KDS(*p, (k_compsph_accel_dudt<KF, D, G_HEAVY, false><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>(
+                              (int)n, P, x, H, m, rho, v, c, alpha, Pr, omega, nullptr, offs, cnt, list, verlet_cnt, dvdt_out, dudt_out,
+                              dEdt_out, ap_ij, av_ij)));
     return check_launch("sph_compsph_accel_dudt");
+}
+
+int sph_compsph_record_floats(int32_t dim) {
+    return dim == 1 ? CompRec<1>::R : dim == 2 ? CompRec<2>::R : dim == 3 ? CompRec<3>::R : 0;
+}
+
+int sph_compsph_accel_dudt_packed(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,
+                                  const float* v, const float* c, const float* alpha, const float* Pr, const float* omega,
+                                  const int32_t* offs, const int32_t* cnt, const int32_t* list, const int32_t* verlet_cnt,
+                                  float* dvdt_out, float* dudt_out, float* dEdt_out, float* ap_ij, float* av_ij, float* records,
+                                  void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(rho); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(Pr);
+    WSPH_CHECK_PTR(records);
+    CHECK_CSR();
+    if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v")) || (rc = check_align_vec(P, dvdt_out, "dvdt")) ||
+        (rc = check_align_vec(P, ap_ij, "ap_ij")) || (rc = check_align_vec(P, av_ij, "av_ij")))
+        return rc;
+    if (reinterpret_cast<uintptr_t>(records) & 15) return set_error(SPH_ERR_BAD_ARG, "sph_compsph_accel_dudt_packed: records must be 16-byte aligned");
+    wsph::count_launch();
+    WSPH_DISPATCH_DS(*p, (k_compsph_pack<D><<<(unsigned)((n + 255) / 256), 256, 0, s>>>((int)n, P, x, H, m, rho, v, c, alpha, Pr, omega,
+                                                                                        records)));
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_compsph_accel_dudt<KF, D, G_HEAVY, true><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>(
+                              (int)n, P, x, H, m, rho, v, c, alpha, Pr, omega, records, offs, cnt, list, verlet_cnt, dvdt_out, dudt_out,
+                              dEdt_out, ap_ij, av_ij)));
+    return check_launch("sph_compsph_accel_dudt_packed");
 }
 
 int sph_compsph_accel(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* rho,

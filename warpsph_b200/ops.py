@@ -602,7 +602,8 @@ def compsph_prep(params, x, H, m, rho, v, adj: AdjacencyList, grad_h: bool = Tru
 
 def compsph_accel_dudt(params, x, H, m, rho, v, c, alpha, P, omega, adj: AdjacencyList, pair_arrays: bool = True,
                        want_dEdt: bool = True, reference_layout: bool = True):
-    """Fused CompSPH momentum and energy RHS; returns (dvdt, dudt, dEdt, ap_ij, av_ij) with
+    """Fused CompSPH momentum and energy RHS over packed particle records
+    (sph_compsph_accel_dudt_packed); returns (dvdt, dudt, dEdt, ap_ij, av_ij) with
     the pairwise accelerations in Verlet-entry order: zeros beyond the support with
     ``reference_layout``, else written over the interacting prefixes only (as
     crk_accel_dudt)."""
@@ -611,11 +612,14 @@ def compsph_accel_dudt(params, x, H, m, rho, v, c, alpha, P, omega, adj: Adjacen
     dEdt = _empty(n, H) if want_dEdt else None
     ap = _pair_empty(adj.nnz, d, H) if pair_arrays else None
     av = _pair_empty(adj.nnz, d, H) if pair_arrays else None
+    recs = _empty(n * int(_capi.lib().sph_compsph_record_floats(d)), H)
     with _timed("compsph_accel_dudt"):
         rows = _lists(params, adj, True)
-        check(_capi.lib().sph_compsph_accel_dudt(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(v), fptr(c), fptr(alpha),
-                                                 fptr(P), fptr(omega), *rows, iptr(adj.numNeighbors) if reference_layout else None, ptr(dvdt), ptr(dudt),
-                                                 ptr(dEdt), ptr(ap), ptr(av), stream_ptr(H.device)), "sph_compsph_accel_dudt")
+        check(_capi.lib().sph_compsph_accel_dudt_packed(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(rho), fptr(v), fptr(c),
+                                                        fptr(alpha), fptr(P), fptr(omega), *rows,
+                                                        iptr(adj.numNeighbors) if reference_layout else None, ptr(dvdt), ptr(dudt),
+                                                        ptr(dEdt), ptr(ap), ptr(av), ptr(recs), stream_ptr(H.device)),
+              "sph_compsph_accel_dudt_packed")
     return dvdt, dudt, dEdt, ap, av
 
 
