@@ -227,16 +227,16 @@ def check(rc: int, what: str) -> None:
 
 
 def ptr(t) -> int | None:
-    """Device pointer of a CUDA tensor (None for None)."""
+    """Device pointer of a contiguous CUDA tensor (None for None); anything else raises."""
     if t is None:
         return None
+    if isinstance(t, torch.Tensor) and t.is_cuda and t.is_contiguous():
+        return t.data_ptr()
     if not isinstance(t, torch.Tensor):
         raise TypeError(f"expected a torch.Tensor, got {type(t)}")
     if not t.is_cuda:
         raise RuntimeError("warpsph_b200 operates on CUDA tensors only (no CPU fallback)")
-    if not t.is_contiguous():
-        raise RuntimeError("warpsph_b200 requires contiguous tensors")
-    return t.data_ptr()
+    raise RuntimeError("warpsph_b200 requires contiguous tensors")
 
 
 def fptr(t) -> int | None:
@@ -251,7 +251,22 @@ def iptr(t) -> int | None:
     return ptr(t)
 
 
+try:   # the raw handle of the current stream without building a Stream object per call
+    from torch._C import _cuda_getCurrentRawStream as _raw_stream
+except ImportError:   # pragma: no cover
+    _raw_stream = None
+
+
 def stream_ptr(device=None) -> int:
+    """cudaStream_t of the current stream of `device` (a torch.device, an index or None for
+    the current device), as an int."""
+    if _raw_stream is not None:
+        if isinstance(device, str):
+            device = torch.device(device)
+        idx = device.index if isinstance(device, torch.device) else device
+        if idx is None:
+            idx = torch.cuda.current_device()
+        return _raw_stream(idx)
     return torch.cuda.current_stream(device).cuda_stream
 
 

@@ -776,12 +776,22 @@ k_mlp_grad_tc(const float* __restrict__ prm, int64_t n, const float* __restrict_
                     tmem_ld_32x32b_x32(tlane + TC_COL_D + cb, v);
                     tmem_ld_wait(v);
                     uint32_t p[16];
-                    #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        float g = dy * fmaxf(__uint_as_float(v[j]), 0.f);      // d loss / d w4_j
+                    {   // d loss / d w4_j summed over the warp's samples: a butterfly that
+                        // halves the values per lane each round leaves lane l with column l
+                        float g[32];
                         #pragma unroll
-                        for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
-                        if (lane == 0) atomicAdd(&s.gw4[cb + j], g);
+                        for (int j = 0; j < 32; ++j) g[j] = dy * fmaxf(__uint_as_float(v[j]), 0.f);
+                        #pragma unroll
+                        for (int off = 16; off >= 1; off >>= 1) {
+                            const bool upper = (lane & off) != 0;
+                            #pragma unroll
+                            for (int t = 0; t < off; ++t) {
+                                const float send = upper ? g[t] : g[t + off];
+                                const float keep = upper ? g[t + off] : g[t];
+                                g[t] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+                            }
+                        }
+                        atomicAdd(&s.gw4[cb + lane], g[0]);
                     }
                     #pragma unroll
                     for (int j = 0; j < 16; ++j) {

@@ -5,9 +5,10 @@ The plain solves start from the reference's guesses: 0.75 p_prev for the
 divergence-free solve (modules/incompressible/divergenceFree.py:72) and 0 for the
 density solve (modules/incompressible/incompressible.py:79).  ``WarmStartMLP``
 predicts the initial pressure per particle from eight local features
-(``sph_dfsph_features``).  The prediction is an 8 -> 64 -> 64 -> 64 -> 1 ReLU network
-trained by the library's own BF16 tensor-core kernels: ``sph_mlp_grad`` for the
-gradient and ``sph_mlp_adam`` for the update.  The solve then iterates from that guess
+(``sph_dfsph_features``) as P MLP(features), with P the features' pressure scale.  The
+network is 8 -> 64 -> 64 -> 64 -> 1 with ReLU, trained by the library's own BF16
+tensor-core kernels: ``sph_mlp_grad_tc`` (tcgen05) for the gradient and
+``sph_mlp_adam`` for the update.  The solve then iterates from that guess
 to the same tolerance, so it remains both the fallback and the judge of the network's
 error (init_mode 1 of the solver).
 
@@ -89,6 +90,7 @@ class WarmStartMLP:
 
     # -------------------------------------------------------------- inference
     def initial_pressure(self, params, mode: int, cfg, x, H, m, rho, v, dvdt, p_prev, dt, adj: AdjacencyList) -> torch.Tensor:
+        """P MLP(features), with P the features' pressure scale."""
         feats, scale = ops.dfsph_features(params, mode, cfg, x, H, m, rho, v, dvdt, p_prev, dt, adj)
         return ops.mlp_forward(self.theta, feats, scale)
 
