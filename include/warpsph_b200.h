@@ -210,6 +210,41 @@ int sph_neighbors_refresh_volume(const SphParams* p, int64_t n, const float* x, 
                                  int32_t* inter_counts, uint32_t* scratch, int64_t* inter_nnz_out,
                                  int32_t* status, float* V_out, void* stream);
 
+/* Device-decided list update for a stepping loop that never reads the device: replaces
+ * the host-side keep-or-rebuild decision of buildVerletList (schemes/crkSPH.py:54-58 in the
+ * reference rebuilds every call).  The Verlet rows (neighbor_offsets, num_neighbors,
+ * neighbor_list, nnz) are kept across calls together with the positions x0 [n, dim] and
+ * supports H0 [n] they were built from.  One call checks them for (x, H) as
+ * sph_neighbors_refresh does (verdict: 3 words of scratch) and, when a particle has left the
+ * Verlet skin, rebuilds them in place on the GPU (every build launch returns at once when
+ * the rows are kept) and copies x, H into x0, H0.  Initialise H0 with zeros (or anything
+ * non-finite) to force the first build.  The rows are in no particular order:
+ * sph_neighbors_rewrite gives the interacting prefixes.  When a rebuild needs more than
+ * list_capacity entries the status word gets SPH_STATUS_LIST_OVERFLOW and every row is cut
+ * to fit (the results of the walks that follow are then wrong but stay in bounds): read the
+ * status word at some later point and redo the work from a saved state with a larger list.
+ * Zero-fill neighbor_list once at allocation. */
+int sph_neighbors_update(const SphParams* p, int64_t n, const float* x, const float* H,
+                         float* x0, float* H0, void* workspace, int64_t workspace_bytes,
+                         int64_t cell_capacity, int32_t* sort_index, uint32_t* sorted_keys,
+                         int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
+                         int32_t* neighbor_offsets, int32_t* num_neighbors, int32_t* neighbor_list,
+                         int64_t list_capacity, int64_t* nnz, uint32_t* verdict, int32_t* status,
+                         void* stream);
+
+/* Rewrites the rows of a list valid for (x, H) into list_out (same offsets, capacity of the
+ * input list) with the interacting entries (fl(sqrt(r^2)) / max(H_i, H_j) < 1) first, in row
+ * order, and the rest after them, as sph_neighbors_refresh does, with no validity check.
+ * offsets_out / counts_out [n] receive copies of the rows' offsets and lengths (so that a
+ * later rebuild of the input rows leaves this list intact), inter_counts [n] the prefix
+ * lengths, inter_nnz_out their sum.  With V_out the CRK volumes of the rows are computed in
+ * the same pass, as in sph_neighbors_refresh_volume. */
+int sph_neighbors_rewrite(const SphParams* p, int64_t n, const float* x, const float* H,
+                          const int32_t* neighbor_offsets, const int32_t* num_neighbors,
+                          const int32_t* neighbor_list, int32_t* list_out, int32_t* offsets_out,
+                          int32_t* counts_out, int32_t* inter_counts, int64_t* inter_nnz_out,
+                          float* V_out, int32_t* status, void* stream);
+
 /* Expands CSR rows into the reference's AdjacencyList.i / .j int64 arrays
  * (io.py:8-20 field names). */
 int sph_neighbors_expand(int64_t n, const int32_t* neighbor_offsets, const int32_t* num_neighbors,

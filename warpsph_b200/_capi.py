@@ -104,6 +104,8 @@ _PROTOS = {
                             _P, _P, _P, _P],
     "sph_neighbors_refresh": [_P, _I64] + [_P] * 13,
     "sph_neighbors_refresh_volume": [_P, _I64] + [_P] * 14,
+    "sph_neighbors_update": [_P, _I64, _P, _P, _P, _P, _P, _I64, _I64] + [_P] * 8 + [_I64] + [_P] * 4,
+    "sph_neighbors_rewrite": [_P, _I64] + [_P] * 13,
     "sph_neighbors_expand": [_I64, _P, _P, _P, _I64, _P, _P, _P],
     "sph_density_gather": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_adaptive_h_iter": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],

@@ -181,6 +181,8 @@ class AdjacencyList:
     # SphParams of a kept prior list whose interacting subset is filtered on first use
     _pending: Optional[object] = field(default=None, repr=False)
     _inter_nnz_dev: Optional[torch.Tensor] = field(default=None, repr=False)
+    # rows kept in fixed buffers and updated on the GPU (ops.DeviceLists): nnz is the capacity
+    _device_rows: bool = field(default=False, repr=False)
 
     @property
     def edgeOffsets(self) -> torch.Tensor:

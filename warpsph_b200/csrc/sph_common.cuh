@@ -301,7 +301,8 @@ inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block
 
 // Exclusive scan of int32 values with a device int64 total (sph_neighbors.cu), and the
 // bytes of workspace it needs for n values.
-void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, char* ws, long long* total, cudaStream_t s);
+void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, char* ws, long long* total, cudaStream_t s,
+                        const unsigned int* gate = nullptr);
 int64_t scan_ws_bytes(int64_t n);
 
 }  // namespace wsph

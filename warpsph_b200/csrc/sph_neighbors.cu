@@ -112,6 +112,26 @@ int params_to_dev(const SphParams* p, DevParams* o) {
     return SPH_OK;
 }
 
+// ---------------------------------------------------------------- list verdict
+// Ordered encoding of floats into unsigned words (atomicMax on the words is a max on the
+// floats), and the validity verdict of a kept Verlet list (k_refresh_check below reduces
+// the three words).
+__device__ __forceinline__ unsigned int ord_enc(float f) {
+    const unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord_dec(unsigned int o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+__device__ __forceinline__ bool refresh_valid(const unsigned int* acc3) {
+    const float dmax = ord_dec(acc3[0]), amax = ord_dec(acc3[1]), hmax = ord_dec(acc3[2]);
+    return amax + 2.0002f * dmax + 1e-5f * hmax <= 0.f;   // false for NaN
+}
+// Gate of the device-decided list update (sph_neighbors_update): a build kernel given
+// the verdict words returns at once when they say the kept list is still valid, so the
+// rebuild is decided on the GPU with no host read.  A null gate always runs.
+__device__ __forceinline__ bool gate_closed(const unsigned int* gate) { return gate != nullptr && refresh_valid(gate); }
+
 // ---------------------------------------------------------------- scan
 // Exclusive scan of int32 values with an int64 grand total.  Block-level scans of
 // 2048 items (256 threads x 8), recursive over block sums.
@@ -147,7 +167,8 @@ __device__ __forceinline__ long long block_exclusive_scan(long long v, long long
 
 // in -> out (exclusive, local to tile), tile totals -> sums
 __global__ void k_scan_tiles(const int32_t* __restrict__ in, int64_t n, long long* __restrict__ out_ll,
-                             int32_t* __restrict__ out32, long long* __restrict__ sums) {
+                             int32_t* __restrict__ out32, long long* __restrict__ sums, const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate)) return;
     __shared__ long long sw[SCAN_THREADS / 32];
     int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
     long long vals[SCAN_ITEMS];
@@ -171,7 +192,9 @@ __global__ void k_scan_tiles(const int32_t* __restrict__ in, int64_t n, long lon
     if (threadIdx.x == 0) sums[blockIdx.x] = total;
 }
 // in and out may alias (in-place scan of tile sums): no __restrict__ here.
-__global__ void k_scan_tiles_ll(const long long* in, int64_t n, long long* out, long long* __restrict__ sums) {
+__global__ void k_scan_tiles_ll(const long long* in, int64_t n, long long* out, long long* __restrict__ sums,
+                                const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate)) return;
     __shared__ long long sw[SCAN_THREADS / 32];
     int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
     long long vals[SCAN_ITEMS];
@@ -193,7 +216,8 @@ __global__ void k_scan_tiles_ll(const long long* in, int64_t n, long long* out, 
     if (threadIdx.x == 0) sums[blockIdx.x] = total;
 }
 __global__ void k_scan_add(long long* __restrict__ out_ll, int32_t* __restrict__ out32, int64_t n,
-                           const long long* __restrict__ tile_off) {
+                           const long long* __restrict__ tile_off, const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate)) return;
     int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
     long long o = tile_off[idx / SCAN_TILE];
@@ -213,34 +237,50 @@ int64_t scan_ws_bytes(int64_t n) {
     return bytes + 256;
 }
 
-// Scans a level of long long values in place (exclusive) and writes the total to *total.
-static void scan_ll_inplace(long long* data, int64_t n, char* ws, long long* total, cudaStream_t s) {
-    int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
-    if (tiles < 1) tiles = 1;
-    long long* sums = reinterpret_cast<long long*>(ws);
-    char* next = ws + ((tiles * 8 + 255) / 256) * 256 * 2;
-    wsph::count_launch(); k_scan_tiles_ll<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(data, n, data, sums);
-    if (tiles == 1) {
-        cudaMemcpyAsync(total, sums, sizeof(long long), cudaMemcpyDeviceToDevice, s);
-        return;
-    }
-    scan_ll_inplace(sums, tiles, next, total, s);
-    wsph::count_launch(); k_scan_add<<<grid_for(n, 256), 256, 0, s>>>(data, nullptr, n, sums);
+__global__ void k_copy_total(long long* __restrict__ total, const long long* __restrict__ sums, const unsigned int* __restrict__ gate) {
+    if (!gate_closed(gate)) *total = *sums;
 }
 
-// Exclusive scan int32 -> int32, total (int64, device).
-void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, char* ws, long long* total, cudaStream_t s) {
+// The single-tile total: a device copy, or under a gate a one-thread kernel (a copy
+// cannot be skipped by the GPU).
+static void copy_total(long long* total, const long long* sums, const unsigned int* gate, cudaStream_t s) {
+    if (gate) {
+        wsph::count_launch(); k_copy_total<<<1, 1, 0, s>>>(total, sums, gate);
+    } else {
+        cudaMemcpyAsync(total, sums, sizeof(long long), cudaMemcpyDeviceToDevice, s);
+    }
+}
+
+// Scans a level of long long values in place (exclusive) and writes the total to *total.
+static void scan_ll_inplace(long long* data, int64_t n, char* ws, long long* total, cudaStream_t s, const unsigned int* gate) {
     int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (tiles < 1) tiles = 1;
     long long* sums = reinterpret_cast<long long*>(ws);
     char* next = ws + ((tiles * 8 + 255) / 256) * 256 * 2;
-    wsph::count_launch(); k_scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, nullptr, out, sums);
+    wsph::count_launch(); k_scan_tiles_ll<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(data, n, data, sums, gate);
     if (tiles == 1) {
-        cudaMemcpyAsync(total, sums, sizeof(long long), cudaMemcpyDeviceToDevice, s);
+        copy_total(total, sums, gate, s);
         return;
     }
-    scan_ll_inplace(sums, tiles, next, total, s);
-    wsph::count_launch(); k_scan_add<<<grid_for(n, 256), 256, 0, s>>>(nullptr, out, n, sums);
+    scan_ll_inplace(sums, tiles, next, total, s, gate);
+    wsph::count_launch(); k_scan_add<<<grid_for(n, 256), 256, 0, s>>>(data, nullptr, n, sums, gate);
+}
+
+// Exclusive scan int32 -> int32, total (int64, device).  Under a gate every launch
+// returns at once when the gate is closed, leaving out and total as they were.
+void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, char* ws, long long* total, cudaStream_t s,
+                        const unsigned int* gate) {
+    int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (tiles < 1) tiles = 1;
+    long long* sums = reinterpret_cast<long long*>(ws);
+    char* next = ws + ((tiles * 8 + 255) / 256) * 256 * 2;
+    wsph::count_launch(); k_scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, nullptr, out, sums, gate);
+    if (tiles == 1) {
+        copy_total(total, sums, gate, s);
+        return;
+    }
+    scan_ll_inplace(sums, tiles, next, total, s, gate);
+    wsph::count_launch(); k_scan_add<<<grid_for(n, 256), 256, 0, s>>>(nullptr, out, n, sums, gate);
 }
 
 // ---------------------------------------------------------------- min / max
@@ -316,7 +356,8 @@ template <int D> __device__ __forceinline__ void cell_coords(const Vec<D>& x, co
     }
 }
 
-__global__ void k_hmax(const float* __restrict__ H, int64_t n, float* out, int32_t* status) {
+__global__ void k_hmax(const float* __restrict__ H, int64_t n, float* out, int32_t* status, const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate)) return;
     float hi = 0.f;
     bool bad = false;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -330,7 +371,8 @@ __global__ void k_hmax(const float* __restrict__ H, int64_t n, float* out, int32
 
 // One thread: derive the grid from max H and the cell-table capacity.
 template <int D>
-__global__ void k_grid(const float* hmax, DevParams P, int max_bits, GridDev* g, int32_t* grid_out) {
+__global__ void k_grid(const float* hmax, DevParams P, int max_bits, GridDev* g, int32_t* grid_out, const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate)) return;
     float h = *hmax;
     float Lmax = 0.f;
     for (int a = 0; a < D; ++a) Lmax = fmaxf(Lmax, P.dom.L[a]);
@@ -357,9 +399,9 @@ __global__ void k_grid(const float* hmax, DevParams P, int max_bits, GridDev* g,
 
 template <int D>
 __global__ void k_keys(const float* __restrict__ x, int n, const GridDev* __restrict__ gp, DomainF dom,
-                       uint32_t* __restrict__ keys, int32_t* __restrict__ counts) {
+                       uint32_t* __restrict__ keys, int32_t* __restrict__ counts, const unsigned int* __restrict__ gate) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || gate_closed(gate)) return;
     GridDev g = *gp;
     int c[3];
     cell_coords<D>(load_vec<D>(x, i), g, dom, c);
@@ -368,9 +410,10 @@ __global__ void k_keys(const float* __restrict__ x, int n, const GridDev* __rest
     atomicAdd(counts + key, 1);
 }
 
-__global__ void k_scatter(const uint32_t* __restrict__ keys, int n, int32_t* __restrict__ cursor, int32_t* __restrict__ sort_index) {
+__global__ void k_scatter(const uint32_t* __restrict__ keys, int n, int32_t* __restrict__ cursor, int32_t* __restrict__ sort_index,
+                          const unsigned int* __restrict__ gate) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || gate_closed(gate)) return;
     int pos = atomicAdd(cursor + keys[i], 1);
     sort_index[pos] = i;
 }
@@ -385,9 +428,9 @@ __global__ void k_rank_sort(const int32_t* __restrict__ tmp, const uint32_t* __r
                             const int32_t* __restrict__ begin, const int32_t* __restrict__ end, int n,
                             const float* __restrict__ x, const float* __restrict__ H,
                             int32_t* __restrict__ sort_index, uint32_t* __restrict__ sorted_keys, float4* __restrict__ recs,
-                            int32_t* __restrict__ tasks, int32_t* __restrict__ ntasks) {
+                            int32_t* __restrict__ tasks, int32_t* __restrict__ ntasks, const unsigned int* __restrict__ gate) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+    if (k >= n || gate_closed(gate)) return;
     int i = tmp[k];
     uint32_t c = keys[i];
     int b = begin[c], e = end[c];
@@ -734,7 +777,8 @@ k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_ke
          int32_t* __restrict__ counts, int32_t* __restrict__ icounts, const int32_t* __restrict__ offsets,
          int32_t* __restrict__ list, long long* __restrict__ innz, const long long* __restrict__ nnz, long long capacity,
          uint32_t* __restrict__ masks, int32_t* __restrict__ mask_base, unsigned long long* __restrict__ mask_cursor,
-         long long mask_words) {
+         long long mask_words, const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate)) return;
     __shared__ float4 srec[VW_WARPS][32];
     __shared__ int32_t sidx[FILL ? VW_WARPS : 1][32];
     __shared__ int32_t sbuf[FILL ? VW_WARPS : 1][32][VP];     // rest of the row
@@ -765,8 +809,34 @@ k_verlet(const float4* __restrict__ recs, const uint32_t* __restrict__ sorted_ke
     }
 }
 
-__global__ void k_check_capacity(const long long* nnz, long long capacity, int32_t* status) {
+__global__ void k_check_capacity(const long long* nnz, long long capacity, int32_t* status, const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate)) return;
     if (*nnz > capacity) atomicOr(status, SPH_STATUS_LIST_OVERFLOW);
+}
+
+// After a gated rebuild that overflowed the list (the fill pass wrote nothing), each row
+// is cut to the part that lies inside the list, so that every walk of the rows stays in
+// bounds; the overflow bit is already in the status word for the host to read.
+__global__ void k_clamp_rows(const long long* __restrict__ nnz, long long capacity, const int32_t* __restrict__ offs,
+                             int32_t* __restrict__ cnt, int n, const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate) || *nnz <= capacity) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long room = capacity - (long long)offs[i];
+    if ((long long)cnt[i] > room) cnt[i] = room > 0 ? (int32_t)room : 0;
+}
+
+// After a gated rebuild: the positions and supports the rows were built from, kept for
+// the next validity check.
+template <int D>
+__global__ void k_keep_state(const float* __restrict__ x, const float* __restrict__ H, float* __restrict__ x0,
+                             float* __restrict__ H0, int n, const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    #pragma unroll
+    for (int a = 0; a < D; ++a) x0[(int64_t)i * D + a] = x[(int64_t)i * D + a];
+    H0[i] = H[i];
 }
 
 __global__ void k_expand(const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
@@ -847,13 +917,6 @@ static int max_bits_for(int dim, int64_t cap) {
 // three ordered-encoded words; k_refilter evaluates the criterion (with a relative
 // margin for rounding) and, when it holds, rebuilds the interacting sublist in place of
 // a full neighbour search.
-__device__ __forceinline__ unsigned int ord_enc(float f) {
-    const unsigned int u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float ord_dec(unsigned int o) {
-    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
-}
 
 template <int D>
 __global__ void k_refresh_check(const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ x0,
@@ -863,10 +926,11 @@ __global__ void k_refresh_check(const float* __restrict__ x, const float* __rest
         const Vec<D> d = dist_vec<D>(load_vec<D>(x, i), load_vec<D>(x0, i), P.dom);
         const float disp = sqrtf(dist2_rn<D>(d));
         const float h = H[i], h0 = P.verlet_scale * H0[i];
-        // a NaN keeps itself (both comparisons fail afterwards) and forces a rebuild
-        dmax = (disp > dmax || disp != disp) ? disp : dmax;
-        amax = (h - h0 > amax || h != h) ? h - h0 : amax;
-        hmax = h0 > hmax ? h0 : hmax;
+        // a NaN anywhere makes the displacement bound infinite, which forces a rebuild
+        const bool bad = isnan(disp) || isnan(h) || isnan(h0);
+        dmax = bad ? __int_as_float(0x7f800000) : fmaxf(dmax, disp);
+        amax = fmaxf(amax, h - h0);
+        hmax = fmaxf(hmax, h0);
     }
     unsigned int e0 = ord_enc(dmax), e1 = ord_enc(amax), e2 = ord_enc(hmax);
     e0 = block_reduce(e0, 0u, OpMaxU());
@@ -875,10 +939,6 @@ __global__ void k_refresh_check(const float* __restrict__ x, const float* __rest
     if (threadIdx.x == 0) { atomicMax(acc3 + 0, e0); atomicMax(acc3 + 1, e1); atomicMax(acc3 + 2, e2); }
 }
 
-__device__ __forceinline__ bool refresh_valid(const unsigned int* acc3) {
-    const float dmax = ord_dec(acc3[0]), amax = ord_dec(acc3[1]), hmax = ord_dec(acc3[2]);
-    return amax + 2.0002f * dmax + 1e-5f * hmax <= 0.f;   // false for NaN
-}
 
 // Eight lanes per row, four rows per warp: the kept Verlet row rewritten into list_out
 // with the interacting entries (fl(sqrt(r^2)) / max(H_i, H_j) < 1 at the new positions,
@@ -891,8 +951,9 @@ __global__ void k_refilter(const float* __restrict__ x, const float* __restrict_
                            const unsigned int* __restrict__ acc3, const int32_t* __restrict__ offs,
                            const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
                            int32_t* __restrict__ list_out, int32_t* __restrict__ icnt,
-                           unsigned long long* __restrict__ innz, int32_t* __restrict__ status) {
-    if (!refresh_valid(acc3)) {
+                           unsigned long long* __restrict__ innz, int32_t* __restrict__ status,
+                           int32_t* __restrict__ offs_out, int32_t* __restrict__ cnt_out) {
+    if (acc3 != nullptr && !refresh_valid(acc3)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, SPH_STATUS_LIST_STALE);
         return;
     }
@@ -926,7 +987,10 @@ __global__ void k_refilter(const float* __restrict__ x, const float* __restrict_
         rw += __popc(rb);
     }
     unsigned long long t = (valid && sub == 0) ? (unsigned long long)w : 0ull;
-    if (valid && sub == 0) icnt[i] = w;
+    if (valid && sub == 0) {
+        icnt[i] = w;
+        if (offs_out) { offs_out[i] = b; cnt_out[i] = c; }
+    }
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
     if (lane == 0 && t) atomicAdd(innz, t);
@@ -942,8 +1006,9 @@ __global__ void k_refilter_volume(const float* __restrict__ x, const float* __re
                                   const unsigned int* __restrict__ acc3, const int32_t* __restrict__ offs,
                                   const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
                                   int32_t* __restrict__ list_out, int32_t* __restrict__ icnt,
-                                  unsigned long long* __restrict__ innz, int32_t* __restrict__ status, float* __restrict__ V) {
-    if (!refresh_valid(acc3)) {
+                                  unsigned long long* __restrict__ innz, int32_t* __restrict__ status, float* __restrict__ V,
+                                  int32_t* __restrict__ offs_out, int32_t* __restrict__ cnt_out) {
+    if (acc3 != nullptr && !refresh_valid(acc3)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, SPH_STATUS_LIST_STALE);
         return;
     }
@@ -985,10 +1050,55 @@ __global__ void k_refilter_volume(const float* __restrict__ x, const float* __re
     if (valid && sub == 0) {
         icnt[i] = w;
         V[i] = 1.f / wsum;
+        if (offs_out) { offs_out[i] = b; cnt_out[i] = c; }
     }
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
     if (lane == 0 && t) atomicAdd(innz, t);
+}
+
+// The list build (grid, counting sort, count pass, scan, fill pass) on the stream.  With a
+// gate every launch returns at once when the gate's verdict says the kept rows are still
+// valid; the clears of workspace words stay unconditional (they touch the workspace only).
+static void build_rows(const DevParams& P, int64_t n, const float* x, const float* H, const NbWs& w, int64_t cell_capacity,
+                       int32_t* sort_index, uint32_t* sorted_keys, int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
+                       int32_t* neighbor_offsets, int32_t* num_neighbors, int32_t* neighbor_list, int64_t list_capacity,
+                       int64_t* nnz_out, int32_t* inter_counts, int64_t* inter_nnz_out, int32_t* status,
+                       const unsigned int* gate, cudaStream_t s) {
+    const bool part = inter_counts != nullptr;
+    int mb = max_bits_for(P.dim, cell_capacity);
+    int64_t ncells = (int64_t)1 << (mb * P.dim);
+    long long* innz = part ? reinterpret_cast<long long*>(inter_nnz_out) : nullptr;
+
+    cudaMemsetAsync(w.hmax, 0, sizeof(float), s);
+    int rblocks = (int)((n + 1023) / 1024);
+    if (rblocks > 148 * 4) rblocks = 148 * 4;
+    wsph::count_launch(); k_hmax<<<rblocks, 256, 0, s>>>(H, n, w.hmax, status, gate);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, k_grid<D><<<1, 1, 0, s>>>(w.hmax, P, mb, w.grid, grid_out, gate));
+    cudaMemsetAsync(w.counts, 0, ncells * sizeof(int32_t), s);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, k_keys<D><<<grid_for(n, 256), 256, 0, s>>>(x, (int)n, w.grid, P.dom, w.keys, w.counts, gate));
+    exclusive_scan_i32(w.counts, cell_begin, ncells, w.scan, w.total, s, gate);
+    cudaMemcpyAsync(cell_end, cell_begin, ncells * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+    wsph::count_launch(); k_scatter<<<grid_for(n, 256), 256, 0, s>>>(w.keys, (int)n, cell_end, w.tmp, gate);
+    cudaMemsetAsync(w.ntasks, 0, sizeof(int32_t), s);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_rank_sort<D><<<grid_for(n, 256), 256, 0, s>>>(w.tmp, w.keys, cell_begin, cell_end, (int)n, x, H,
+                                                                                                 sort_index, sorted_keys, w.recs, w.tasks, w.ntasks,
+                                                                                                 gate)));
+    int vblocks = grid_for(n, VW_BLOCK);          // >= one warp per 32 particles; warps stride over the work items
+    if (vblocks > 148 * 32) vblocks = 148 * 32;
+    if (part) cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
+    cudaMemsetAsync(w.mask_cursor, 0, sizeof(unsigned long long), s);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, false><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
+                                                                                 cell_begin, cell_end, num_neighbors, inter_counts, nullptr,
+                                                                                 nullptr, innz, nullptr, 0, w.masks, w.mask_base,
+                                                                                 w.mask_cursor, (long long)w.mask_words, gate)));
+    exclusive_scan_i32(num_neighbors, neighbor_offsets, n, w.scan, reinterpret_cast<long long*>(nnz_out), s, gate);
+    wsph::count_launch(); k_check_capacity<<<1, 1, 0, s>>>(reinterpret_cast<long long*>(nnz_out), list_capacity, status, gate);
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, true><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
+                                                                                cell_begin, cell_end, nullptr, inter_counts, neighbor_offsets,
+                                                                                neighbor_list, nullptr, reinterpret_cast<long long*>(nnz_out),
+                                                                                list_capacity, w.masks, w.mask_base, w.mask_cursor,
+                                                                                (long long)w.mask_words, gate)));
 }
 
 }  // namespace wsph
@@ -1053,38 +1163,8 @@ int sph_neighbors_build(const SphParams* p, int64_t n, const float* x, const flo
     if (P.dim == 2 && (reinterpret_cast<uintptr_t>(x) & 7)) return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
     NbWs w = carve(reinterpret_cast<char*>(workspace), n, cell_capacity);
     if (workspace_bytes < w.bytes) return set_error(SPH_ERR_WORKSPACE, "neighbour workspace too small: %lld < %lld", (long long)workspace_bytes, (long long)w.bytes);
-    int mb = max_bits_for(P.dim, cell_capacity);
-    int64_t ncells = (int64_t)1 << (mb * P.dim);
-    long long* innz = part ? reinterpret_cast<long long*>(inter_nnz_out) : nullptr;
-
-    cudaMemsetAsync(w.hmax, 0, sizeof(float), s);
-    int rblocks = (int)((n + 1023) / 1024);
-    if (rblocks > 148 * 4) rblocks = 148 * 4;
-    wsph::count_launch(); k_hmax<<<rblocks, 256, 0, s>>>(H, n, w.hmax, status);
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, k_grid<D><<<1, 1, 0, s>>>(w.hmax, P, mb, w.grid, grid_out));
-    cudaMemsetAsync(w.counts, 0, ncells * sizeof(int32_t), s);
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, k_keys<D><<<grid_for(n, 256), 256, 0, s>>>(x, (int)n, w.grid, P.dom, w.keys, w.counts));
-    exclusive_scan_i32(w.counts, cell_begin, ncells, w.scan, w.total, s);
-    cudaMemcpyAsync(cell_end, cell_begin, ncells * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
-    wsph::count_launch(); k_scatter<<<grid_for(n, 256), 256, 0, s>>>(w.keys, (int)n, cell_end, w.tmp);
-    cudaMemsetAsync(w.ntasks, 0, sizeof(int32_t), s);
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_rank_sort<D><<<grid_for(n, 256), 256, 0, s>>>(w.tmp, w.keys, cell_begin, cell_end, (int)n, x, H,
-                                                                                                 sort_index, sorted_keys, w.recs, w.tasks, w.ntasks)));
-    int vblocks = grid_for(n, VW_BLOCK);          // >= one warp per 32 particles; warps stride over the work items
-    if (vblocks > 148 * 32) vblocks = 148 * 32;
-    if (part) cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
-    cudaMemsetAsync(w.mask_cursor, 0, sizeof(unsigned long long), s);
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, false><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
-                                                                                 cell_begin, cell_end, num_neighbors, inter_counts, nullptr,
-                                                                                 nullptr, innz, nullptr, 0, w.masks, w.mask_base,
-                                                                                 w.mask_cursor, (long long)w.mask_words)));
-    exclusive_scan_i32(num_neighbors, neighbor_offsets, n, w.scan, reinterpret_cast<long long*>(nnz_out), s);
-    wsph::count_launch(); k_check_capacity<<<1, 1, 0, s>>>(reinterpret_cast<long long*>(nnz_out), list_capacity, status);
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, true><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
-                                                                                cell_begin, cell_end, nullptr, inter_counts, neighbor_offsets,
-                                                                                neighbor_list, nullptr, reinterpret_cast<long long*>(nnz_out),
-                                                                                list_capacity, w.masks, w.mask_base, w.mask_cursor,
-                                                                                (long long)w.mask_words)));
+    build_rows(P, n, x, H, w, cell_capacity, sort_index, sorted_keys, cell_begin, cell_end, grid_out, neighbor_offsets, num_neighbors,
+               neighbor_list, list_capacity, nnz_out, inter_counts, inter_nnz_out, status, nullptr, s);
     return check_launch("sph_neighbors_build");
 }
 
@@ -1123,7 +1203,8 @@ int sph_neighbors_refresh(const SphParams* p, int64_t n, const float* x, const f
     wsph::count_launch();
     WSPH_DISPATCH_DIM(P.dim, (k_refilter<D><<<(int)rblocks, 256, 0, s>>>(x, H, (int)rows, P, scratch, neighbor_offsets, num_neighbors,
                                                                         neighbor_list, list_out, inter_counts,
-                                                                        reinterpret_cast<unsigned long long*>(inter_nnz_out), status)));
+                                                                        reinterpret_cast<unsigned long long*>(inter_nnz_out), status,
+                                                                        nullptr, nullptr)));
     return check_launch("sph_neighbors_refresh");
 }
 
@@ -1156,8 +1237,81 @@ int sph_neighbors_refresh_volume(const SphParams* p, int64_t n, const float* x, 
                                                                                        num_neighbors, neighbor_list, list_out,
                                                                                        inter_counts,
                                                                                        reinterpret_cast<unsigned long long*>(inter_nnz_out),
-                                                                                       status, V_out)));
+                                                                                       status, V_out, nullptr, nullptr)));
     return check_launch("sph_neighbors_refresh_volume");
+}
+
+int sph_neighbors_update(const SphParams* p, int64_t n, const float* x, const float* H, float* x0, float* H0,
+                         void* workspace, int64_t workspace_bytes, int64_t cell_capacity,
+                         int32_t* sort_index, uint32_t* sorted_keys, int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
+                         int32_t* neighbor_offsets, int32_t* num_neighbors, int32_t* neighbor_list, int64_t list_capacity,
+                         int64_t* nnz, uint32_t* verdict, int32_t* status, void* stream) {
+    DevParams P;
+    int rc = params_to_dev(p, &P);
+    if (rc) return rc;
+    if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_update: n out of range");
+    if (cell_capacity < 1) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_update: cell_capacity < 1");
+    if (list_capacity < 1) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_update: list_capacity < 1");
+    WSPH_CHECK_PTR(nnz); WSPH_CHECK_PTR(verdict); WSPH_CHECK_PTR(status); WSPH_CHECK_PTR(grid_out);
+    cudaStream_t s = WSPH_STREAM(stream);
+    if (n == 0) {
+        cudaMemsetAsync(nnz, 0, sizeof(int64_t), s);
+        return check_launch("sph_neighbors_update");
+    }
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(x0); WSPH_CHECK_PTR(H0); WSPH_CHECK_PTR(workspace);
+    WSPH_CHECK_PTR(sort_index); WSPH_CHECK_PTR(sorted_keys); WSPH_CHECK_PTR(cell_begin); WSPH_CHECK_PTR(cell_end);
+    WSPH_CHECK_PTR(neighbor_offsets); WSPH_CHECK_PTR(num_neighbors); WSPH_CHECK_PTR(neighbor_list);
+    if (P.dim == 2 && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(x0)) & 7))
+        return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
+    NbWs w = carve(reinterpret_cast<char*>(workspace), n, cell_capacity);
+    if (workspace_bytes < w.bytes) return set_error(SPH_ERR_WORKSPACE, "neighbour workspace too small: %lld < %lld", (long long)workspace_bytes, (long long)w.bytes);
+    cudaMemsetAsync(verdict, 0, 3 * sizeof(uint32_t), s);
+    int cblocks = (int)((n + 1023) / 1024);
+    if (cblocks > 148 * 4) cblocks = 148 * 4;
+    wsph::count_launch();
+    WSPH_DISPATCH_DIM(P.dim, (k_refresh_check<D><<<cblocks, 256, 0, s>>>(x, H, x0, H0, (int)n, P, verdict)));
+    build_rows(P, n, x, H, w, cell_capacity, sort_index, sorted_keys, cell_begin, cell_end, grid_out, neighbor_offsets, num_neighbors,
+               neighbor_list, list_capacity, nnz, nullptr, nullptr, status, verdict, s);
+    wsph::count_launch();
+    k_clamp_rows<<<grid_for(n, 256), 256, 0, s>>>(reinterpret_cast<const long long*>(nnz), list_capacity, neighbor_offsets, num_neighbors,
+                                                 (int)n, verdict);
+    wsph::count_launch();
+    WSPH_DISPATCH_DIM(P.dim, (k_keep_state<D><<<grid_for(n, 256), 256, 0, s>>>(x, H, x0, H0, (int)n, verdict)));
+    return check_launch("sph_neighbors_update");
+}
+
+int sph_neighbors_rewrite(const SphParams* p, int64_t n, const float* x, const float* H,
+                          const int32_t* neighbor_offsets, const int32_t* num_neighbors, const int32_t* neighbor_list,
+                          int32_t* list_out, int32_t* offsets_out, int32_t* counts_out, int32_t* inter_counts,
+                          int64_t* inter_nnz_out, float* V_out, int32_t* status, void* stream) {
+    DevParams P;
+    int rc = params_to_dev(p, &P);
+    if (rc) return rc;
+    if (n < 0 || n > 0x7fffffff) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_rewrite: n out of range");
+    WSPH_CHECK_PTR(inter_nnz_out); WSPH_CHECK_PTR(status);
+    cudaStream_t s = WSPH_STREAM(stream);
+    cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
+    if (n == 0) return check_launch("sph_neighbors_rewrite");
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(neighbor_offsets); WSPH_CHECK_PTR(num_neighbors);
+    WSPH_CHECK_PTR(neighbor_list); WSPH_CHECK_PTR(list_out); WSPH_CHECK_PTR(offsets_out); WSPH_CHECK_PTR(counts_out);
+    WSPH_CHECK_PTR(inter_counts);
+    if (list_out == neighbor_list) return set_error(SPH_ERR_BAD_ARG, "sph_neighbors_rewrite: list_out must not alias neighbor_list");
+    if (P.dim == 2 && (reinterpret_cast<uintptr_t>(x) & 7)) return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
+    const int rblocks = (int)((n * RF_G + 255) / 256);
+    wsph::count_launch();
+    if (V_out) {
+        WSPH_DISPATCH_KD(P.kernel, P.dim, (k_refilter_volume<KF, D><<<rblocks, 256, 0, s>>>(x, H, (int)n, P, nullptr, neighbor_offsets,
+                                                                                           num_neighbors, neighbor_list, list_out,
+                                                                                           inter_counts,
+                                                                                           reinterpret_cast<unsigned long long*>(inter_nnz_out),
+                                                                                           status, V_out, offsets_out, counts_out)));
+    } else {
+        WSPH_DISPATCH_DIM(P.dim, (k_refilter<D><<<rblocks, 256, 0, s>>>(x, H, (int)n, P, nullptr, neighbor_offsets, num_neighbors,
+                                                                         neighbor_list, list_out, inter_counts,
+                                                                         reinterpret_cast<unsigned long long*>(inter_nnz_out), status,
+                                                                         offsets_out, counts_out)));
+    }
+    return check_launch("sph_neighbors_rewrite");
 }
 
 int sph_neighbors_expand(int64_t n, const int32_t* neighbor_offsets, const int32_t* num_neighbors,

@@ -6,6 +6,7 @@ Errors from the library raise RuntimeError; there is no CPU path.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 from typing import Optional
 
@@ -156,6 +157,8 @@ def speculative_refresh(x: torch.Tensor, H: torch.Tensor, params, verletScale: f
     n = int(H.shape[0])
     dim = int(params.dim)
     dev = x.device
+    if _DEVICE_LISTS[0]:   # the device-decided update below keeps or rebuilds the rows itself
+        return None
     if not (REUSE_PRIOR and prior is not None and prior._x0 is not None and prior.numRows == n and
             prior.verletScale == float(verletScale) and prior._x0.device == dev and prior._dim == dim):
         return None
@@ -196,6 +199,8 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
     if priorNeighborhood is not None and priorNeighborhood._x_version == _version(x) and \
             priorNeighborhood._h_version == _version(H) and priorNeighborhood.verletScale == float(verletScale):
         return priorNeighborhood
+    if _DEVICE_LISTS[0]:
+        return device_lists_for(x, H, params, verletScale).update(x, H, params)
     n = int(H.shape[0])
     dim = int(params.dim)
     params.verlet_scale = float(verletScale)
@@ -258,10 +263,11 @@ def buildVerletList(x: torch.Tensor, H: torch.Tensor, params, verletScale: float
 
 def expand_adjacency(adj: AdjacencyList):
     dev = adj.neighborList.device
-    i = torch.empty(adj.nnz, dtype=torch.int64, device=dev)
-    j = torch.empty(adj.nnz, dtype=torch.int64, device=dev)
+    nnz = list_entries(adj)
+    i = torch.empty(nnz, dtype=torch.int64, device=dev)
+    j = torch.empty(nnz, dtype=torch.int64, device=dev)
     check(_capi.lib().sph_neighbors_expand(adj.numRows, ptr(adj.neighborOffsets), ptr(adj.numNeighbors),
-                                           ptr(adj.neighborList), adj.nnz, ptr(i), ptr(j), stream_ptr(dev)),
+                                           ptr(adj.neighborList), nnz, ptr(i), ptr(j), stream_ptr(dev)),
           "sph_neighbors_expand")
     return i, j
 
@@ -275,6 +281,9 @@ def _materialize_inter(adj: AdjacencyList, V_out: Optional[torch.Tensor] = None)
     current positions first (sph_neighbors_refresh).  The rows go to a new tensor:
     earlier stages keep the old order their pairwise arrays are indexed by.  With V_out
     the CRK volumes of the rewritten rows are computed in the same pass."""
+    if isinstance(adj._pending, _DevicePending):
+        adj._pending.rewrite(adj, V_out)
+        return
     params = adj._pending
     n, dev = adj.numRows, adj.neighborList.device
     icnt = torch.empty(n, dtype=torch.int32, device=dev)
@@ -292,6 +301,148 @@ def _materialize_inter(adj: AdjacencyList, V_out: Optional[torch.Tensor] = None)
     adj._ij = None
     adj._inter_nnz_dev = flags[:1]
     adj._pending = None
+
+
+# ------------------------------------------------------------------ device-decided lists
+# A stepping loop that must not read the device (a CUDA graph replays it, or the host runs
+# ahead of the GPU) keeps its Verlet rows in fixed buffers and lets the GPU decide between
+# keeping and rebuilding them (sph_neighbors_update); pair passes walk per-call rewrites of
+# the rows (sph_neighbors_rewrite).  Lists then report their capacity as nnz (per-entry
+# arrays are allocated that long; entries past the rows are never read) and
+# ``list_entries`` reads the true count.
+_DEVICE_LISTS = [0]
+_device_lists: dict = {}
+DEVICE_LIST_HEADROOM = 1.3   # list capacity over the entries of the sizing build
+
+
+@contextlib.contextmanager
+def device_decided_lists():
+    """Within this context buildVerletList neither reads the device nor allocates its rows:
+    see DeviceLists."""
+    _DEVICE_LISTS[0] += 1
+    try:
+        yield
+    finally:
+        _DEVICE_LISTS[0] -= 1
+
+
+class DeviceLists:
+    """The kept Verlet rows of one particle set (n, dim, verlet scale, device) for
+    device-decided updates.  The list capacity is DEVICE_LIST_HEADROOM times the entries of
+    one ordinary build at creation; a rebuild that needs more sets the overflow bit of the
+    status word, which ``check()`` (one host read) turns into an error."""
+
+    def __init__(self, x: torch.Tensor, H: torch.Tensor, params, verletScale: float):
+        n, dim, dev = int(H.shape[0]), int(params.dim), x.device
+        self.n, self.dim, self.verletScale = n, dim, float(verletScale)
+        sizing = _capi.SphParams.from_buffer_copy(params)
+        with _suspend_device_lists():
+            probe = buildVerletList(x, H, sizing, verletScale, None, keep_sort=False)
+        self.capacity = int(probe.nnz * DEVICE_LIST_HEADROOM) + 4096
+        self.cell_capacity = cell_capacity_for(n, dim)
+        wsb = C.c_int64(0)
+        check(_capi.lib().sph_neighbors_workspace_size(_p(sizing), n, self.cell_capacity, C.byref(wsb)), "sph_neighbors_workspace_size")
+        self.ws_bytes = wsb.value
+        self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=dev)
+        i32 = dict(dtype=torch.int32, device=dev)
+        self.sort_index, self.sorted_keys = torch.empty(n, **i32), torch.empty(n, **i32)
+        self.cell_begin, self.cell_end = torch.empty(self.cell_capacity, **i32), torch.empty(self.cell_capacity, **i32)
+        self.grid = torch.zeros(8, **i32)
+        self.offsets, self.counts = torch.zeros(n, **i32), torch.zeros(n, **i32)
+        self.rows = torch.zeros(self.capacity, **i32)     # zero-filled: a cut row never names a bad index
+        self.nnz = torch.zeros(1, dtype=torch.int64, device=dev)
+        # zero build-time supports fail every validity check: the first update builds
+        self.x0 = x.detach().clone()
+        self.h0 = torch.zeros_like(H)
+        self.verdict = torch.zeros(4, **i32)
+        self.status = torch.zeros(1, **i32)
+        self.generation = 0
+
+    def update(self, x: torch.Tensor, H: torch.Tensor, params) -> AdjacencyList:
+        x, H = _f32(x), _f32(H)
+        params.verlet_scale = self.verletScale
+        with _timed("neighbors_update"):
+            check(_capi.lib().sph_neighbors_update(_p(params), self.n, ptr(x), ptr(H), ptr(self.x0), ptr(self.h0), ptr(self.ws),
+                                                   self.ws_bytes, self.cell_capacity, ptr(self.sort_index), ptr(self.sorted_keys),
+                                                   ptr(self.cell_begin), ptr(self.cell_end), ptr(self.grid), ptr(self.offsets),
+                                                   ptr(self.counts), ptr(self.rows), self.capacity, ptr(self.nnz), ptr(self.verdict),
+                                                   ptr(self.status), stream_ptr(x.device)), "sph_neighbors_update")
+        self.generation += 1
+        adj = AdjacencyList(neighborOffsets=self.offsets, numNeighbors=self.counts, neighborList=self.rows, numRows=self.n,
+                            numCols=self.n, nnz=self.capacity, grid=self.grid, queryPositions=x, querySupports=H,
+                            verletScale=self.verletScale)
+        adj._x_version, adj._h_version, adj._dim = _version(x), _version(H), self.dim
+        adj._pending = _DevicePending(self, _capi.SphParams.from_buffer_copy(params), self.generation)
+        adj._device_rows = True
+        return adj
+
+    def check(self) -> None:
+        """Raises when a rebuild since creation overflowed the list or met a non-finite or
+        non-positive support (one host read)."""
+        st = int(self.status.item()) & 0xffffffff
+        if st & _capi.STATUS_NONFINITE:
+            raise RuntimeError("device-decided neighbour list: supports must be finite and positive")
+        if st & _capi.STATUS_LIST_OVERFLOW:
+            raise RuntimeError(f"device-decided neighbour list: a rebuild needed more than {self.capacity} entries; "
+                               "raise DEVICE_LIST_HEADROOM and start again from a saved state")
+
+
+class _DevicePending:
+    """The interacting rewrite of a device-decided list, done on first use."""
+
+    def __init__(self, lists: DeviceLists, params, generation: int):
+        self.lists, self.params, self.generation = lists, params, generation
+
+    def rewrite(self, adj: AdjacencyList, V_out: Optional[torch.Tensor]) -> None:
+        nb = self.lists
+        if nb.generation != self.generation:
+            raise RuntimeError("a device-decided list was used after a later update of the same rows")
+        n, dev = nb.n, nb.rows.device
+        lst = torch.empty(nb.capacity, dtype=torch.int32, device=dev)
+        offs, cnt, icnt = (torch.empty(n, dtype=torch.int32, device=dev) for _ in range(3))
+        innz = torch.empty(1, dtype=torch.int64, device=dev)
+        with _timed("neighbors_rewrite"):
+            check(_capi.lib().sph_neighbors_rewrite(_p(self.params), n, ptr(adj.queryPositions), ptr(adj.querySupports),
+                                                    ptr(nb.offsets), ptr(nb.counts), ptr(nb.rows), ptr(lst), ptr(offs), ptr(cnt),
+                                                    ptr(icnt), ptr(innz), fptr(V_out) if V_out is not None else None,
+                                                    ptr(nb.status), stream_ptr(dev)), "sph_neighbors_rewrite")
+        adj.neighborOffsets, adj.numNeighbors, adj.neighborList, adj.interCounts = offs, cnt, lst, icnt
+        adj._inter_nnz_dev = innz
+        adj._ij = None
+        adj._pending = None
+
+
+@contextlib.contextmanager
+def _suspend_device_lists():
+    saved = _DEVICE_LISTS[0]
+    _DEVICE_LISTS[0] = 0
+    try:
+        yield
+    finally:
+        _DEVICE_LISTS[0] = saved
+
+
+def device_lists_for(x: torch.Tensor, H: torch.Tensor, params, verletScale: float) -> DeviceLists:
+    """The DeviceLists of this particle set, created (with one sizing build) on first use."""
+    key = (x.device.index, int(H.shape[0]), int(params.dim), float(verletScale))
+    nb = _device_lists.get(key)
+    if nb is None:
+        nb = DeviceLists(x, H, params, verletScale)
+        _device_lists[key] = nb
+    return nb
+
+
+def release_device_lists() -> None:
+    """Drops every DeviceLists (their buffers return to the caching allocator)."""
+    _device_lists.clear()
+
+
+def list_entries(adj: AdjacencyList) -> int:
+    """Entries in the rows of `adj`: its nnz, or for a device-decided list (whose nnz is the
+    capacity) the true count, read from the device."""
+    if not getattr(adj, "_device_rows", False) or adj.numRows == 0:
+        return adj.nnz
+    return int((adj.neighborOffsets[-1].long() + adj.numNeighbors[-1].long()).item())
 
 
 def _lists(params, adj: AdjacencyList, interacting: bool):
@@ -571,16 +722,17 @@ def pair_reference_layout(adj: AdjacencyList, *arrays):
     if adj is None or adj.interCounts is None or getattr(adj, "_pending", None) is not None:
         return arrays
     n = adj.numRows
+    nnz = list_entries(adj)
     dev = adj.neighborOffsets.device
-    rows = torch.repeat_interleave(torch.arange(n, device=dev), adj.numNeighbors.long(), output_size=adj.nnz)
-    pos = torch.arange(adj.nnz, device=dev) - adj.neighborOffsets.long()[rows]
+    rows = torch.repeat_interleave(torch.arange(n, device=dev), adj.numNeighbors.long(), output_size=nnz)
+    pos = torch.arange(nnz, device=dev) - adj.neighborOffsets.long()[rows]
     tail = pos >= adj.interCounts.long()[rows]
     out = []
     for a in arrays:
         if a is None:
             out.append(None)
             continue
-        b = a[: adj.nnz].clone()
+        b = a[:nnz].clone()
         b[tail] = 0
         out.append(b)
     return tuple(out)
