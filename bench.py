@@ -49,6 +49,8 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-steps", type=int, default=8, help="steps of the CPU baseline sample (about 1 s each on 16 cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--eager", action="store_true",
+                    help="time the step as issued from Python every step instead of as a replayed CUDA graph")
     ap.add_argument("--breakdown", action="store_true", help="print a per-kernel time breakdown to stderr")
     ap.add_argument("--no-dfsph", action="store_true", help="skip the DFSPH warm-start comparison")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched delta-SPH ensemble")
@@ -472,6 +474,78 @@ def build_workload(nx, dev):
     return cfg, sch, integrator, step, system
 
 
+E2E_FIELDS = ["positions", "velocities", "internalEnergies", "supports", "masses", "densities", "alpha0s", "alphas", "divergence"]
+
+
+def e2e_graph(sg, steps: int, world: int, barrier) -> dict:
+    """particle-steps/s through the recorded step with host buffers: every step copies the
+    state it starts from (recorded beforehand from the same run) from pinned host memory
+    into the graph's inputs, replays the step and copies the resulting state back to
+    pinned host memory.  The uploads and downloads run on a copy stream, overlapped with
+    the neighbouring steps; the time is the whole sequence on the device clock."""
+    import torch
+    import torch.distributed as dist
+    dev = sg.device
+    n = sg.n
+    traj = []
+    for _ in range(2 + steps):
+        S = sg.inputs.state
+        traj.append({f: getattr(S, f).detach().cpu().pin_memory() for f in E2E_FIELDS})
+        sg.replay(1)
+    torch.cuda.synchronize()
+    h2d = sum(t.numel() * t.element_size() for t in traj[0].values())
+    host_out = [{f: torch.empty_like(traj[0][f]).pin_memory() for f in E2E_FIELDS} for _ in range(2)]
+    comp = torch.cuda.current_stream(dev)
+    copy = torch.cuda.Stream(dev)
+    d_in = [{f: torch.empty_like(getattr(sg.inputs.state, f)) for f in E2E_FIELDS} for _ in range(2)]
+    d_out = [{f: torch.empty_like(getattr(sg.inputs.state, f)) for f in E2E_FIELDS} for _ in range(2)]
+
+    def upload(k):
+        with torch.cuda.stream(copy):
+            for f in E2E_FIELDS:
+                d_in[k % 2][f].copy_(traj[k][f], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(copy)
+        return ev
+
+    def run(k0, count):
+        ev = upload(k0)
+        for k in range(k0, k0 + count):
+            comp.wait_event(ev)
+            sg.load_state(d_in[k % 2])
+            if k + 1 < k0 + count:
+                ev = upload(k + 1)        # the next step's inputs cross while this step computes
+            sg.replay(1)
+            S = sg.system.state
+            for f in E2E_FIELDS:          # the result leaves the graph's buffers before the next replay
+                d_out[k % 2][f].copy_(getattr(S, f), non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(comp)
+            copy.wait_event(done)
+            with torch.cuda.stream(copy):   # and crosses to the host while the next step computes
+                for f in E2E_FIELDS:
+                    host_out[k % 2][f].copy_(d_out[k % 2][f], non_blocking=True)
+        comp.wait_stream(copy)
+
+    run(0, 2)
+    barrier()
+    torch.cuda.synchronize()
+    gc.collect()
+    gc.disable()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run(2, steps)
+    e1.record()
+    torch.cuda.synchronize()
+    gc.enable()
+    te = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    return {"value": n * steps * world / (float(te.item()) / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": h2d, "steps": steps, "path": "recorded step (CUDA graph)",
+            "inputs": "each step uploads the state it starts from, recorded from the same run beforehand"}
+
+
 def gpu_arm(args, rank: int, world: int):
     import torch
     import torch.distributed as dist
@@ -504,7 +578,7 @@ def gpu_arm(args, rank: int, world: int):
         one_step()
     torch.cuda.synchronize()
 
-    # ------------------------------------------------ device-resident timed region
+    # ------------------------------------------------ the step issued from Python (eager)
     timer = ops.KernelTimer(names={"crk_accel_dudt"})
     barrier()
     torch.cuda.synchronize()
@@ -530,15 +604,60 @@ def gpu_arm(args, rank: int, world: int):
     # cudaMalloc / cudaFree, which synchronise the device)
     allocator = {k: int(mem1.get(k, 0) - mem0.get(k, 0)) for k in ("num_device_alloc", "num_device_free", "num_alloc_retries")}
     tw1 = time.time()
+
+    # ------------------------------------------------ the step recorded once as a CUDA graph
+    # (device-decided neighbour lists: no step reads the device; one graph launch per step)
+    sg = None
+    graph_info = None
+    if not args.eager:
+        from warpsph_b200.stepgraph import StepGraph
+        t_cap = time.perf_counter()
+        sg = StepGraph(state["system"], integ, step, cfg, sch, dt=state["dt"], warmup=3)
+        torch.cuda.synchronize()
+        t_cap = time.perf_counter() - t_cap
+        sg.replay(max(args.warmup, 3))
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        gc.collect()
+        gc.disable()
+        rb0 = sg.rebuilds()
+        gw0 = time.time()
+        gmem0 = torch.cuda.memory_stats(dev)
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record()
+        sg.replay(args.steps)
+        g1.record()
+        torch.cuda.synchronize()
+        gc.enable()
+        gmem1 = torch.cuda.memory_stats(dev)
+        gw1 = time.time()
+        barrier()
+        sg.check()
+        g_ms = g0.elapsed_time(g1)
+        rebuilds = sg.rebuilds() - rb0
+        graph_info = {"ms": g_ms, "wall": (gw0, gw1),
+                      "launches": sg.launches_per_step * args.steps + sg.launches_per_rebuild * rebuilds,
+                      "launches_per_step": sg.launches_per_step, "launches_per_list_rebuild": sg.launches_per_rebuild,
+                      "list_rebuilds_timed": rebuilds, "capture_s": round(t_cap, 3),
+                      "list_capacity": sg.lists[0].capacity if sg.lists else None,
+                      "allocator": {k: int(gmem1.get(k, 0) - gmem0.get(k, 0))
+                                    for k in ("num_device_alloc", "num_device_free", "num_alloc_retries")}}
+
     barrier()
     clocks.stop()
-    clock_info = clocks.summarise(tw0, tw1)
-    ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    clock_info = clocks.summarise(tw0, graph_info["wall"][1] if graph_info else tw1)
+    eager_ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([graph_info["ms"] if graph_info else eager_ms, eager_ms], device=dev, dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max, eager_ms_max = float(t[0].item()), float(t[1].item())
     value = n * args.steps * world / (ms_max / 1e3)
+    eager = {"value": n * args.steps * world / (eager_ms_max / 1e3), "ms_per_step": eager_ms_max / args.steps,
+             "launches_per_step": launches / max(args.steps, 1), "allocator_in_timed_region": allocator}
+    if graph_info:
+        launches = graph_info["launches"]
+        allocator = graph_info["allocator"]
     ksum = timer.summary().get("crk_accel_dudt", {"launches": 0, "avg_ms": float("nan")})
 
     # roofline of the dominant kernel
@@ -572,8 +691,10 @@ def gpu_arm(args, rank: int, world: int):
 
     # ------------------------------------------------ end-to-end through the API with host buffers
     e2e = None
-    if not args.no_e2e:
-        fields = ["positions", "velocities", "internalEnergies", "supports", "masses", "densities", "alpha0s", "alphas", "divergence"]
+    if not args.no_e2e and sg is not None:
+        e2e = e2e_graph(sg, max(3, args.steps // 2), world, barrier)
+    elif not args.no_e2e:
+        fields = E2E_FIELDS
         e2e_steps = max(3, args.steps // 2)
         # the inputs of 2 + e2e_steps consecutive steps of the run, recorded into pinned host
         # memory beforehand: every step of the end-to-end leg uploads the state that step
@@ -680,6 +801,10 @@ def gpu_arm(args, rank: int, world: int):
                            "l2": "working set larger than L2 (pair arrays ~0.7 GB per step), no flush needed"},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
                 "allocator_in_timed_region": allocator,
+                "step_path": ("one CUDA graph launch per step (StepGraph), device-decided neighbour lists" if graph_info
+                              else "issued from Python every step"),
+                "graph": ({k: v for k, v in graph_info.items() if k not in ("wall", "ms", "allocator")} if graph_info else None),
+                "eager": eager,
                 "dfsph_dambreak_3d": dfsph, "ensemble": ens, "compsph": comp, "sedov3d": s3, "mlp_forward": mlp}
         if breakdown is not None:
             line["breakdown_ms"] = {k: round(v["total_ms"] / 3, 4) for k, v in breakdown.items()}

@@ -143,8 +143,12 @@ typedef struct SphParams {
 /* ---------------------------------------------------------------- library */
 const char* sph_version(void);
 const char* sph_last_error_string(void);
-/* Number of CUDA kernels this library has launched in the process (all threads). */
+/* Number of CUDA kernels this library has launched in the process (all threads); a launch
+ * recorded into a CUDA graph counts once, when it is recorded. */
 int64_t sph_launch_count(void);
+/* Of those, the launches recorded into the rebuild bodies of graph conditional nodes
+ * (sph_neighbors_update during a capture): a replay runs them only when it rebuilds. */
+int64_t sph_launch_count_conditional(void);
 /* Kernel-function constants used by the library (normalisation C_d, kernel scale
  * H/h = 1/(2 sigma), Dehnen & Aly 2012 Table 1). Host-only, no GPU needed. */
 int sph_kernel_constants(int32_t kernel, int32_t dim, double* norm_out, double* scale_out);
@@ -223,14 +227,19 @@ int sph_neighbors_refresh_volume(const SphParams* p, int64_t n, const float* x, 
  * list_capacity entries the status word gets SPH_STATUS_LIST_OVERFLOW and every row is cut
  * to fit (the results of the walks that follow are then wrong but stay in bounds): read the
  * status word at some later point and redo the work from a saved state with a larger list.
- * Zero-fill neighbor_list once at allocation. */
+ * Zero-fill neighbor_list once at allocation.  rebuilds (optional, one int64 on the device) is
+ * incremented by every rebuild.  Called on a stream that is being captured into a CUDA graph,
+ * the rebuild is recorded as the body of an IF conditional node whose condition the GPU sets
+ * from the verdict, so a replay that keeps the rows skips it; its body is captured on a
+ * private stream per device, created by the first call outside a capture (make one before
+ * capturing; without it the gated launches are recorded instead). */
 int sph_neighbors_update(const SphParams* p, int64_t n, const float* x, const float* H,
                          float* x0, float* H0, void* workspace, int64_t workspace_bytes,
                          int64_t cell_capacity, int32_t* sort_index, uint32_t* sorted_keys,
                          int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
                          int32_t* neighbor_offsets, int32_t* num_neighbors, int32_t* neighbor_list,
                          int64_t list_capacity, int64_t* nnz, uint32_t* verdict, int32_t* status,
-                         void* stream);
+                         int64_t* rebuilds, void* stream);
 
 /* Rewrites the rows of a list valid for (x, H) into list_out (same offsets, capacity of the
  * input list) with the interacting entries (fl(sqrt(r^2)) / max(H_i, H_j) < 1) first, in row

@@ -153,3 +153,39 @@ def test_device_list_overflow_reported(cuda):
             nb.check()
     finally:
         ops.DEVICE_LIST_HEADROOM = old
+
+
+def test_recorded_update_rebuilds_only_when_stale(cuda):
+    """sph_neighbors_update recorded in a CUDA graph (the rebuild is a conditional node):
+    a replay after a move across the skin rebuilds the rows, one after a small move keeps
+    them, and the rewritten interacting rows equal a fresh build's in both cases."""
+    cfg, sch, _, _, system = sedov(64, cuda)
+    params = ws.make_params(cfg, sch)
+    S = system.state
+    n = S.positions.shape[0]
+    x, H = S.positions.clone(), S.supports.clone()
+    nb = ops.device_lists_for(x, H, params, cfg.verletScale)
+    device_pairs(nb, x, H, params)                      # the first call (outside a recording) builds
+    side = torch.cuda.Stream(cuda)
+    side.wait_stream(torch.cuda.current_stream(cuda))
+    with torch.cuda.stream(side):
+        device_pairs(nb, x, H, params)
+    torch.cuda.current_stream(cuda).wait_stream(side)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        adj = nb.update(x, H, params)
+        ops._lists(params, adj, True)
+    gen = torch.Generator(device=cuda).manual_seed(5)
+    skin = float((cfg.verletScale - 1.0) * H.min())
+    for scale, rebuilt in ((4.0, True), (0.05, False), (4.0, True)):
+        x_prev0 = nb.x0.clone()
+        x.copy_(wrap(x + scale * skin * (torch.rand(x.shape, generator=gen, device=cuda) - 0.5)))
+        g.replay()
+        torch.cuda.synchronize()
+        if rebuilt:
+            assert torch.equal(nb.x0, x), "a replay after a move across the skin must rebuild"
+        else:
+            assert torch.equal(nb.x0, x_prev0), "a replay after a small move must keep the rows"
+        assert np.array_equal(interacting_pairs(adj, n), fresh_pairs(x, H, params, cfg.verletScale, n))
+    nb.check()

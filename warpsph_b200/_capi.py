@@ -98,13 +98,14 @@ _PROTOS = {
     "sph_version": [],
     "sph_last_error_string": [],
     "sph_launch_count": [],
+    "sph_launch_count_conditional": [],
     "sph_kernel_constants": [_I32, _I32, _P, _P],
     "sph_neighbors_workspace_size": [_P, _I64, _I64, _P],
     "sph_neighbors_build": [_P, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _P,
                             _P, _P, _P, _P],
     "sph_neighbors_refresh": [_P, _I64] + [_P] * 13,
     "sph_neighbors_refresh_volume": [_P, _I64] + [_P] * 14,
-    "sph_neighbors_update": [_P, _I64, _P, _P, _P, _P, _P, _I64, _I64] + [_P] * 8 + [_I64] + [_P] * 4,
+    "sph_neighbors_update": [_P, _I64, _P, _P, _P, _P, _P, _I64, _I64] + [_P] * 8 + [_I64] + [_P] * 5,
     "sph_neighbors_rewrite": [_P, _I64] + [_P] * 13,
     "sph_neighbors_expand": [_I64, _P, _P, _P, _I64, _P, _P, _P],
     "sph_density_gather": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P],
@@ -171,7 +172,7 @@ _PROTOS = {
     "sph_dfsph_div_solve": [_P, _P, _I64] + [_P] * 12 + [_I64] + [_P] * 6,
     "sph_dfsph_density_solve": [_P, _P, _I64] + [_P] * 12 + [_I64] + [_P] * 6,
 }
-_RESTYPE = {"sph_version": C.c_char_p, "sph_last_error_string": C.c_char_p, "sph_launch_count": C.c_int64,
+_RESTYPE = {"sph_version": C.c_char_p, "sph_last_error_string": C.c_char_p, "sph_launch_count": C.c_int64, "sph_launch_count_conditional": C.c_int64,
             "sph_dfsph_workspace_size": C.c_int64,
             "sph_mlp_param_count": C.c_int64, "sph_ensemble_neighbors_workspace_size": C.c_int64,
             "sph_ensemble_step_workspace_size": C.c_int64}

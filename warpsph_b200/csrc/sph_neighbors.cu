@@ -38,6 +38,8 @@ int set_error(int code, const char* fmt, ...) {
 
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+// launches recorded into the rebuild bodies of graph conditionals (they run only on a rebuild)
+static std::atomic<long long> g_conditional_launches{0};
 
 int check_launch(const char* what) {
     cudaError_t e = cudaGetLastError();
@@ -830,9 +832,11 @@ __global__ void k_clamp_rows(const long long* __restrict__ nnz, long long capaci
 // the next validity check.
 template <int D>
 __global__ void k_keep_state(const float* __restrict__ x, const float* __restrict__ H, float* __restrict__ x0,
-                             float* __restrict__ H0, int n, const unsigned int* __restrict__ gate) {
+                             float* __restrict__ H0, int n, const unsigned int* __restrict__ gate,
+                             unsigned long long* __restrict__ rebuilds) {
     if (gate_closed(gate)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && rebuilds) *rebuilds += 1ull;
     if (i >= n) return;
     #pragma unroll
     for (int a = 0; a < D; ++a) x0[(int64_t)i * D + a] = x[(int64_t)i * D + a];
@@ -1057,9 +1061,24 @@ __global__ void k_refilter_volume(const float* __restrict__ x, const float* __re
     if (lane == 0 && t) atomicAdd(innz, t);
 }
 
+// Word fill and copy for the gated build (a memset or a copy cannot be skipped by the GPU).
+__global__ void k_fill_gated(uint32_t* __restrict__ p, int64_t count, uint32_t v, const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate)) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ void k_copy_gated(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, int64_t count,
+                             const unsigned int* __restrict__ gate) {
+    if (gate_closed(gate)) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) dst[i] = src[i];
+}
+static int word_blocks(int64_t words) {
+    int64_t b = (words + 255) / 256;
+    return (int)(b < 1 ? 1 : (b > 148 * 8 ? 148 * 8 : b));
+}
+
 // The list build (grid, counting sort, count pass, scan, fill pass) on the stream.  With a
-// gate every launch returns at once when the gate's verdict says the kept rows are still
-// valid; the clears of workspace words stay unconditional (they touch the workspace only).
+// gate every launch (the clears and copies included) returns at once when the gate's verdict
+// says the kept rows are still valid.
 static void build_rows(const DevParams& P, int64_t n, const float* x, const float* H, const NbWs& w, int64_t cell_capacity,
                        int32_t* sort_index, uint32_t* sorted_keys, int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
                        int32_t* neighbor_offsets, int32_t* num_neighbors, int32_t* neighbor_list, int64_t list_capacity,
@@ -1069,25 +1088,39 @@ static void build_rows(const DevParams& P, int64_t n, const float* x, const floa
     int mb = max_bits_for(P.dim, cell_capacity);
     int64_t ncells = (int64_t)1 << (mb * P.dim);
     long long* innz = part ? reinterpret_cast<long long*>(inter_nnz_out) : nullptr;
+    auto clear = [&](void* ptr, int64_t bytes) {          // bytes: a multiple of 4
+        if (gate) {
+            wsph::count_launch();
+            k_fill_gated<<<word_blocks(bytes / 4), 256, 0, s>>>(reinterpret_cast<uint32_t*>(ptr), bytes / 4, 0u, gate);
+        } else {
+            cudaMemsetAsync(ptr, 0, bytes, s);
+        }
+    };
 
-    cudaMemsetAsync(w.hmax, 0, sizeof(float), s);
+    clear(w.hmax, sizeof(float));
     int rblocks = (int)((n + 1023) / 1024);
     if (rblocks > 148 * 4) rblocks = 148 * 4;
     wsph::count_launch(); k_hmax<<<rblocks, 256, 0, s>>>(H, n, w.hmax, status, gate);
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, k_grid<D><<<1, 1, 0, s>>>(w.hmax, P, mb, w.grid, grid_out, gate));
-    cudaMemsetAsync(w.counts, 0, ncells * sizeof(int32_t), s);
+    clear(w.counts, ncells * sizeof(int32_t));
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, k_keys<D><<<grid_for(n, 256), 256, 0, s>>>(x, (int)n, w.grid, P.dom, w.keys, w.counts, gate));
     exclusive_scan_i32(w.counts, cell_begin, ncells, w.scan, w.total, s, gate);
-    cudaMemcpyAsync(cell_end, cell_begin, ncells * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+    if (gate) {
+        wsph::count_launch();
+        k_copy_gated<<<word_blocks(ncells), 256, 0, s>>>(reinterpret_cast<uint32_t*>(cell_end), reinterpret_cast<const uint32_t*>(cell_begin),
+                                                          ncells, gate);
+    } else {
+        cudaMemcpyAsync(cell_end, cell_begin, ncells * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+    }
     wsph::count_launch(); k_scatter<<<grid_for(n, 256), 256, 0, s>>>(w.keys, (int)n, cell_end, w.tmp, gate);
-    cudaMemsetAsync(w.ntasks, 0, sizeof(int32_t), s);
+    clear(w.ntasks, sizeof(int32_t));
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_rank_sort<D><<<grid_for(n, 256), 256, 0, s>>>(w.tmp, w.keys, cell_begin, cell_end, (int)n, x, H,
                                                                                                  sort_index, sorted_keys, w.recs, w.tasks, w.ntasks,
                                                                                                  gate)));
     int vblocks = grid_for(n, VW_BLOCK);          // >= one warp per 32 particles; warps stride over the work items
     if (vblocks > 148 * 32) vblocks = 148 * 32;
-    if (part) cudaMemsetAsync(inter_nnz_out, 0, sizeof(int64_t), s);
-    cudaMemsetAsync(w.mask_cursor, 0, sizeof(unsigned long long), s);
+    if (part) clear(inter_nnz_out, sizeof(int64_t));
+    clear(w.mask_cursor, sizeof(unsigned long long));
     wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_verlet<D, false><<<vblocks, VW_BLOCK, 0, s>>>(w.recs, sorted_keys, w.tasks, w.ntasks, w.grid, P, sort_index,
                                                                                  cell_begin, cell_end, num_neighbors, inter_counts, nullptr,
                                                                                  nullptr, innz, nullptr, 0, w.masks, w.mask_base,
@@ -1101,6 +1134,85 @@ static void build_rows(const DevParams& P, int64_t n, const float* x, const floa
                                                                                 (long long)w.mask_words, gate)));
 }
 
+// ---------------------------------------------------------------- rebuild as a graph conditional
+// While a stream is being captured into a CUDA graph, the rebuild of sph_neighbors_update
+// goes into the body of an IF conditional node: one kernel turns the verdict into the
+// node's condition, and a replay whose rows are kept skips the whole body instead of
+// launching ~20 kernels that return at once.  The body is captured on a private stream per
+// device, created by the first call made outside a capture (a call during a capture with no
+// such stream yet falls back to the gated launches).
+__global__ void k_set_rebuild(const unsigned int* __restrict__ verdict, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, refresh_valid(verdict) ? 0u : 1u);
+}
+
+constexpr int MAX_DEVICES = 64;
+static cudaStream_t g_body_stream[MAX_DEVICES] = {};
+static std::atomic<int> g_body_lock{0};
+
+static cudaStream_t body_stream(bool create) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return nullptr;
+    if (g_body_stream[dev] || !create) return g_body_stream[dev];
+    int expected = 0;
+    while (!g_body_lock.compare_exchange_weak(expected, 1)) expected = 0;
+    if (!g_body_stream[dev]) {
+        cudaStream_t st = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess) g_body_stream[dev] = st;
+        else cudaGetLastError();
+    }
+    g_body_lock.store(0);
+    return g_body_stream[dev];
+}
+
+#define WSPH_CK_GRAPH(call)                                                                                  \
+    do {                                                                                                    \
+        cudaError_t e_ = (call);                                                                            \
+        if (e_ != cudaSuccess) return set_error(SPH_ERR_CUDA, "sph_neighbors_update: %s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// The rebuild (the gated build of build_rows with the clamp and the build-state copy) as an
+// IF node on the capturing stream s; bs: the private body stream.
+static int rebuild_conditional(const DevParams& P, int64_t n, const float* x, const float* H, float* x0, float* H0, const NbWs& w,
+                               int64_t cell_capacity, int32_t* sort_index, uint32_t* sorted_keys, int32_t* cell_begin,
+                               int32_t* cell_end, int32_t* grid_out, int32_t* offs, int32_t* cnt, int32_t* list,
+                               int64_t list_capacity, int64_t* nnz, const unsigned int* verdict, int32_t* status,
+                               int64_t* rebuilds, cudaStream_t s, cudaStream_t bs) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    WSPH_CK_GRAPH(cudaStreamGetCaptureInfo(s, &st, nullptr, &graph, &deps, &ndeps));
+    cudaGraphConditionalHandle h;
+    WSPH_CK_GRAPH(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    wsph::count_launch();
+    k_set_rebuild<<<1, 1, 0, s>>>(verdict, h);
+    WSPH_CK_GRAPH(cudaGetLastError());
+    WSPH_CK_GRAPH(cudaStreamGetCaptureInfo(s, &st, nullptr, &graph, &deps, &ndeps));
+    alignas(cudaGraphNodeParams) unsigned char np_bytes[sizeof(cudaGraphNodeParams)] = {};   // zeroed, as the API wants
+    cudaGraphNodeParams& np = *reinterpret_cast<cudaGraphNodeParams*>(np_bytes);
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    WSPH_CK_GRAPH(cudaGraphAddNode(&node, graph, deps, ndeps, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    WSPH_CK_GRAPH(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    WSPH_CK_GRAPH(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    const long long l0 = g_launches.load();
+    build_rows(P, n, x, H, w, cell_capacity, sort_index, sorted_keys, cell_begin, cell_end, grid_out, offs, cnt, list, list_capacity,
+               nnz, nullptr, nullptr, status, verdict, bs);
+    wsph::count_launch();
+    k_clamp_rows<<<grid_for(n, 256), 256, 0, bs>>>(reinterpret_cast<const long long*>(nnz), list_capacity, offs, cnt, (int)n, verdict);
+    wsph::count_launch();
+    WSPH_DISPATCH_DIM(P.dim, (k_keep_state<D><<<grid_for(n, 256), 256, 0, bs>>>(x, H, x0, H0, (int)n, verdict,
+                                                                                reinterpret_cast<unsigned long long*>(rebuilds))));
+    g_conditional_launches.fetch_add(g_launches.load() - l0);
+    cudaGraph_t captured = nullptr;
+    WSPH_CK_GRAPH(cudaStreamEndCapture(bs, &captured));
+    return SPH_OK;
+}
+
 }  // namespace wsph
 
 using namespace wsph;
@@ -1110,6 +1222,7 @@ extern "C" {
 const char* sph_version(void) { return "warpsph_b200 0.1.0 (sm_100a)"; }
 const char* sph_last_error_string(void) { return g_err; }
 int64_t sph_launch_count(void) { return g_launches.load(); }
+int64_t sph_launch_count_conditional(void) { return g_conditional_launches.load(); }
 
 int sph_kernel_constants(int32_t kernel, int32_t dim, double* norm_out, double* scale_out) {
     double c = kernel_norm(kernel, dim), s = kernel_scale(kernel, dim);
@@ -1245,7 +1358,7 @@ int sph_neighbors_update(const SphParams* p, int64_t n, const float* x, const fl
                          void* workspace, int64_t workspace_bytes, int64_t cell_capacity,
                          int32_t* sort_index, uint32_t* sorted_keys, int32_t* cell_begin, int32_t* cell_end, int32_t* grid_out,
                          int32_t* neighbor_offsets, int32_t* num_neighbors, int32_t* neighbor_list, int64_t list_capacity,
-                         int64_t* nnz, uint32_t* verdict, int32_t* status, void* stream) {
+                         int64_t* nnz, uint32_t* verdict, int32_t* status, int64_t* rebuilds, void* stream) {
     DevParams P;
     int rc = params_to_dev(p, &P);
     if (rc) return rc;
@@ -1265,18 +1378,28 @@ int sph_neighbors_update(const SphParams* p, int64_t n, const float* x, const fl
         return set_error(SPH_ERR_BAD_ARG, "positions must be 8-byte aligned in 2D");
     NbWs w = carve(reinterpret_cast<char*>(workspace), n, cell_capacity);
     if (workspace_bytes < w.bytes) return set_error(SPH_ERR_WORKSPACE, "neighbour workspace too small: %lld < %lld", (long long)workspace_bytes, (long long)w.bytes);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return check_launch("sph_neighbors_update");
+    cudaStream_t bs = body_stream(cs == cudaStreamCaptureStatusNone);
     cudaMemsetAsync(verdict, 0, 3 * sizeof(uint32_t), s);
     int cblocks = (int)((n + 1023) / 1024);
     if (cblocks > 148 * 4) cblocks = 148 * 4;
     wsph::count_launch();
     WSPH_DISPATCH_DIM(P.dim, (k_refresh_check<D><<<cblocks, 256, 0, s>>>(x, H, x0, H0, (int)n, P, verdict)));
+    if (cs == cudaStreamCaptureStatusActive && bs != nullptr && bs != s) {
+        rc = rebuild_conditional(P, n, x, H, x0, H0, w, cell_capacity, sort_index, sorted_keys, cell_begin, cell_end, grid_out,
+                                 neighbor_offsets, num_neighbors, neighbor_list, list_capacity, nnz, verdict, status, rebuilds, s, bs);
+        if (rc) return rc;
+        return check_launch("sph_neighbors_update");
+    }
     build_rows(P, n, x, H, w, cell_capacity, sort_index, sorted_keys, cell_begin, cell_end, grid_out, neighbor_offsets, num_neighbors,
                neighbor_list, list_capacity, nnz, nullptr, nullptr, status, verdict, s);
     wsph::count_launch();
     k_clamp_rows<<<grid_for(n, 256), 256, 0, s>>>(reinterpret_cast<const long long*>(nnz), list_capacity, neighbor_offsets, num_neighbors,
                                                  (int)n, verdict);
     wsph::count_launch();
-    WSPH_DISPATCH_DIM(P.dim, (k_keep_state<D><<<grid_for(n, 256), 256, 0, s>>>(x, H, x0, H0, (int)n, verdict)));
+    WSPH_DISPATCH_DIM(P.dim, (k_keep_state<D><<<grid_for(n, 256), 256, 0, s>>>(x, H, x0, H0, (int)n, verdict,
+                                                                               reinterpret_cast<unsigned long long*>(rebuilds))));
     return check_launch("sph_neighbors_update");
 }
 

@@ -356,6 +356,7 @@ class DeviceLists:
         self.h0 = torch.zeros_like(H)
         self.verdict = torch.zeros(4, **i32)
         self.status = torch.zeros(1, **i32)
+        self.rebuilds = torch.zeros(1, dtype=torch.int64, device=dev)   # counted on the device
         self.generation = 0
 
     def update(self, x: torch.Tensor, H: torch.Tensor, params) -> AdjacencyList:
@@ -366,7 +367,7 @@ class DeviceLists:
                                                    self.ws_bytes, self.cell_capacity, ptr(self.sort_index), ptr(self.sorted_keys),
                                                    ptr(self.cell_begin), ptr(self.cell_end), ptr(self.grid), ptr(self.offsets),
                                                    ptr(self.counts), ptr(self.rows), self.capacity, ptr(self.nnz), ptr(self.verdict),
-                                                   ptr(self.status), stream_ptr(x.device)), "sph_neighbors_update")
+                                                   ptr(self.status), ptr(self.rebuilds), stream_ptr(x.device)), "sph_neighbors_update")
         self.generation += 1
         adj = AdjacencyList(neighborOffsets=self.offsets, numNeighbors=self.counts, neighborList=self.rows, numRows=self.n,
                             numCols=self.n, nnz=self.capacity, grid=self.grid, queryPositions=x, querySupports=H,

@@ -107,7 +107,9 @@ class StepGraph:
         self.dt = dt_t.clone()
 
         self.graph = torch.cuda.CUDAGraph()
-        launches0 = _capi.lib().sph_launch_count()
+        lib = _capi.lib()
+        launches0, cond0 = lib.sph_launch_count(), lib.sph_launch_count_conditional()
+        gen0 = [nb.generation for nb in self.lists]
         with ops.device_decided_lists(), torch.cuda.graph(self.graph):
             out, dt_new = self._advance(self.inputs, self.dt)
             static = dict(_per_particle(self.inputs.state, n))
@@ -120,8 +122,12 @@ class StepGraph:
             self.dt.copy_(dt_new)
             if isinstance(getattr(out, "t_device", None), torch.Tensor) and isinstance(getattr(self.inputs, "t_device", None), torch.Tensor):
                 self.inputs.t_device.copy_(out.t_device)
-        # launches of this library's kernels in one recorded step
-        self.launches_per_step = _capi.lib().sph_launch_count() - launches0
+        # this library's kernels in one recorded step: those every replay runs, and those of
+        # one neighbour-list rebuild (the bodies of the rebuild conditionals)
+        cond = lib.sph_launch_count_conditional() - cond0
+        updates = sum(nb.generation - g for nb, g in zip(self.lists, gen0))
+        self.launches_per_step = lib.sph_launch_count() - launches0 - cond
+        self.launches_per_rebuild = cond // updates if updates and cond else 0
         self.out = out
         self.steps = 0
 
@@ -146,6 +152,10 @@ class StepGraph:
         buffers, on the current stream; the next replay starts from them."""
         for name, v in fields.items():
             getattr(self.inputs.state, name).copy_(v, non_blocking=True)
+
+    def rebuilds(self) -> int:
+        """Neighbour-list rebuilds so far (counted on the device; one host read per list)."""
+        return sum(int(nb.rebuilds.item()) for nb in self.lists)
 
     def check(self) -> None:
         """Raises if a neighbour-list rebuild since the start overflowed the list or met a
