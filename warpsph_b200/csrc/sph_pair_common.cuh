@@ -36,6 +36,31 @@ template <int G> __device__ __forceinline__ float gmaxw(float v) {
 __device__ __forceinline__ void entry(const int32_t* __restrict__ list, int q, int& j, int& k) {
     j = __ldg(list + q); k = q;
 }
+// One lane's walk over a row (entries q0, q0 + step, ... < e) with the neighbour index loaded
+// two entries ahead and the neighbour's D-vector from `src` one entry ahead: the dependent
+// global loads of an entry are in flight while the entry before it is computed.  Past the
+// row's end the prefetches read index 0 (a valid particle whenever a row is walked).
+template <int D> struct RowPipe {
+    const int32_t* __restrict__ list;
+    const float* __restrict__ src;
+    int e, step, j1, j2;
+    Vec<D> v1;
+    __device__ __forceinline__ RowPipe(const int32_t* __restrict__ l, const float* __restrict__ s, int q0, int e_, int st)
+        : list(l), src(s), e(e_), step(st) {
+        j1 = q0 < e_ ? __ldg(l + q0) : 0;
+        j2 = q0 + st < e_ ? __ldg(l + q0 + st) : 0;
+        v1 = load_vec<D>(s, j1);
+    }
+    // the entry at q (the caller's loop index, q0 + k * step): its neighbour and vector
+    __device__ __forceinline__ void take(int q, int& j, Vec<D>& vj) {
+        j = j1;
+        vj = v1;
+        j1 = j2;
+        v1 = load_vec<D>(src, j1);
+        j2 = q + 2 * step < e ? __ldg(list + q + 2 * step) : 0;
+    }
+};
+
 template <int G> __host__ __forceinline__ int grid_g(int64_t n) { return (int)((n * G + PAIR_BLOCK - 1) / PAIR_BLOCK); }
 
 // W and grad_i W with a precomputed 1/H.

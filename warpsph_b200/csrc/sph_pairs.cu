@@ -34,9 +34,10 @@ k_density(int n, int mode, DevParams P, const float* __restrict__ x, const float
         Vec<D> xi = load_vec<D>(x, g.i);
         float Hi = H[g.i];
         int b = offs[g.i], e = b + cnt[g.i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             s += __ldg(m + j) * kernelW_mode<KF, D>(r, Hi, __ldg(H + j), mode);
         }
@@ -66,9 +67,10 @@ k_adaptive_h(int n, DevParams P, const float* __restrict__ x, const float* __res
         Vec<D> xi = load_vec<D>(x, g.i);
         Hi = H[g.i];
         int b = offs[g.i], e = b + cnt[g.i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W, dWdH;
             kernelWdH<KF, D>(r, Hi, W, dWdH);
@@ -136,9 +138,10 @@ k_owen(int n, DevParams P, const float* __restrict__ x, const float* __restrict_
         const float invHi = 1.f / Hi;
         const float hsW = 1.f / powf(Hi, -(float)D), hsG = 1.f / powf(Hi, -(float)(D + 1));
         int b = offs[i], e = b + cnt[i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W; Vec<D> gW;
             kWG_inv<KF, D>(xij, r, invHi, W, gW);
@@ -173,9 +176,10 @@ k_crk_volume(int n, DevParams P, const float* __restrict__ x, const float* __res
     if (g.valid) {
         Vec<D> xi = load_vec<D>(x, g.i);
         int b = offs[g.i], e = b + cnt[g.i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             s += kW_inv<KF, D>(r, 1.f / __ldg(H + j));
         }
@@ -237,9 +241,10 @@ k_crk_factors(int n, DevParams P, const float* __restrict__ x, const float* __re
     if (g.valid) {
         Vec<D> xi = load_vec<D>(x, g.i);
         int b = offs[g.i], e = b + cnt[g.i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W; Vec<D> gW;
             kWG_inv<KF, D>(xij, r, 1.f / __ldg(H + j), W, gW);
@@ -384,9 +389,10 @@ k_grad_v(int n, DevParams P, const float* __restrict__ x, const float* __restric
         Mat<D> gBi = load_mat<D>(gB, i);
         float ci = want_vs ? c[i] : 0.f;
         int b = offs[i], e = b + cnt[i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float Hj = __ldg(H + j);
             Vec<D> vj = load_vec<D>(v, j);
@@ -465,9 +471,10 @@ k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restric
         Vec<D> vi = want_vs ? load_vec<D>(v, i) : vzero<D>();
         float ci = want_vs ? c[i] : 0.f;
         int b = offs[i], e = b + cnt[i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W = kW_inv<KF, D>(r, invHi);   // gather support
             if (W != 0.f) {
@@ -539,9 +546,10 @@ k_hopkins_grad(int n, DevParams P, const float* __restrict__ x, const float* __r
         Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
         const float invHi = 1.f / H[i];
         int b = offs[i], e = b + cnt[i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W; Vec<D> gW;
             kWG_inv<KF, D>(xij, r, invHi, W, gW);
@@ -623,9 +631,10 @@ k_hopkins_alpha(int n, DevParams P, const float* __restrict__ x, const float* __
         Vec<D> xi = load_vec<D>(x, i);
         const float invHi = 1.f / H[i];
         int b = offs[i], e = b + cnt[i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float W = kW_inv<KF, D>(safe_sqrt(dot<D>(xij, xij)), invHi);
             if (W == 0.f) continue;
             float dj = __ldg(div + j);
@@ -663,9 +672,10 @@ k_hopkins_update(int n, DevParams P, const float* __restrict__ x, const float* _
         Vec<D> xi = load_vec<D>(x, i), vi = load_vec<D>(v, i);
         const float Hi = H[i], ci = c[i];
         int b = offs[i], e = b + cnt[i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             if (!(r < P.verlet_scale * wmax(Hi, __ldg(H + j)))) continue;
             Vec<D> vj = load_vec<D>(v, j);
