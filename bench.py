@@ -379,7 +379,8 @@ def mlp_forward_throughput(dev, n: int = 1 << 24, reps: int = 20) -> dict:
 
 
 def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, steps: int, warmup: int, kahan: bool = False,
-                      timed_kernel: str = None, bytes_per_particle: float = None, breakdown: bool = False) -> dict:
+                      timed_kernel: str = None, bytes_per_particle: float = None, breakdown: bool = False,
+                      graph: bool = True) -> dict:
     """particle-steps/s of one compressible scheme on the Sedov blast (device-resident,
     CUDA events, CFL dt on the device every step), the total-energy drift over the timed
     steps from the FP64 conservation sums, and the dominant pair kernel's average launch
@@ -417,6 +418,7 @@ def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, step
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     gc.collect()
     gc.disable()
+    torch.cuda.reset_peak_memory_stats(dev)
     a0 = torch.cuda.memory_stats(dev)
     try:
         e0.record()
@@ -437,6 +439,40 @@ def scheme_throughput(dev, scheme: str, dim: int, nx: int, neighbours: int, step
            "verlet_entries_per_particle": box["system"].adjacency.nnz / n,
            "allocator_in_timed_region": {key: int(a1.get(key, 0) - a0.get(key, 0)) for key in
                                          ("num_device_alloc", "num_device_free", "num_alloc_retries")}}
+    if graph:
+        # the same steps recorded once as a CUDA graph (device-decided lists), when the device
+        # has room for a second step's worth of buffers (the graph keeps its own)
+        torch.cuda.empty_cache()
+        free, _ = torch.cuda.mem_get_info(dev)
+        need = 2 * max(a1.get("allocated_bytes.all.peak", 0) - a0.get("allocated_bytes.all.current", 0), 1)
+        if free < need:
+            out["graph"] = {"skipped": f"{free / 2**30:.1f} GiB free, about {need / 2**30:.1f} GiB needed"}
+        else:
+            from warpsph_b200.stepgraph import StepGraph
+            sg = StepGraph(box["system"], integ, step, cfg, sch, dt=box["dt"], warmup=3)
+            sg.replay(2)
+            torch.cuda.synchronize()
+            gc.collect()
+            gc.disable()
+            try:
+                rb0 = sg.rebuilds()
+                g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                g0.record()
+                sg.replay(steps)
+                g1.record()
+                torch.cuda.synchronize()
+            finally:
+                gc.enable()
+            sg.check()
+            gms = g0.elapsed_time(g1)
+            out["eager_value"], out["eager_ms_per_step"] = out["value"], out["ms_per_step"]
+            out["value"], out["ms_per_step"] = n * steps / (gms / 1e3), gms / steps
+            out["graph"] = {"launches_per_step": sg.launches_per_step, "launches_per_list_rebuild": sg.launches_per_rebuild,
+                            "list_rebuilds_timed": sg.rebuilds() - rb0}
+            sg.release()
+            del sg
+            ops.release_device_lists()
+            torch.cuda.empty_cache()
     if timer is not None:
         nb = timer.summary().get("neighbors_build")
         out["list_builds_timed"] = nb["launches"] if nb else 0
