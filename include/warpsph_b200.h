@@ -313,6 +313,15 @@ int sph_crk_factors(const SphParams* p, int64_t n, const float* x, const float* 
                     float* A, float* B, float* gradA, float* gradB, float* rho_out,
                     void* stream);
 
+/* sph_crk_factors with the ideal-gas EOS of its density fused into the same pass
+ * (modules/eos/idealGas.py:16-36, as sph_eos_ideal_gas computes it): from u [n] it writes
+ * entropy_out, P_out and c_out [n] (each optional), gamma from p. */
+int sph_crk_factors_eos(const SphParams* p, int64_t n, const float* x, const float* H,
+                        const float* m, const float* V, const int32_t* offs, const int32_t* cnt,
+                        const int32_t* list, float* A, float* B, float* gradA, float* gradB,
+                        float* rho_out, const float* u, float* entropy_out, float* P_out,
+                        float* c_out, void* stream);
+
 /* Ideal-gas EOS (modules/eos/idealGas.py:6-38 with u and rho given). */
 int sph_eos_ideal_gas(const SphParams* p, int64_t n, const float* u, const float* rho,
                       float* A_out, float* P_out, float* c_out, void* stream);
@@ -891,6 +900,15 @@ int sph_cfl_dt(const SphParams* p, int64_t n, const float* H, const float* u, co
 int sph_rk_combine(const SphParams* p, int64_t count, const float* y0, int32_t nk,
                    const float* const* k_ptrs, const double* weights, const float* dt,
                    int32_t wrap_dim, float* y_out, void* stream);
+
+/* sph_rk_combine over up to 4 fields in one launch (the stage update of positions,
+ * velocities and energies together): field f has counts[f] floats y0s[f] -> y_outs[f],
+ * wrap_dims[f] as wrap_dim above, and derivatives k_ptrs[f * nk + q]; the weights are
+ * shared.  Each element is computed as sph_rk_combine computes it. */
+int sph_rk_combine_fields(const SphParams* p, int32_t nfields, const int64_t* counts,
+                          const float* const* y0s, float* const* y_outs, const int32_t* wrap_dims,
+                          int32_t nk, const float* const* k_ptrs, const double* weights,
+                          const float* dt, void* stream);
 
 /* Compatible-energy finalize (systems/compSPH.py:100-111 and
  * modules/compSPH/multistep.py:52-94): v_half = v0 + dt/2 sum_s b_s dvdt_s,

@@ -107,6 +107,8 @@ _PROTOS = {
     "sph_neighbors_refresh_volume": [_P, _I64] + [_P] * 14,
     "sph_neighbors_update": [_P, _I64, _P, _P, _P, _P, _P, _I64, _I64] + [_P] * 8 + [_I64] + [_P] * 5,
     "sph_neighbors_rewrite": [_P, _I64] + [_P] * 13,
+    "sph_rk_combine_fields": [_P, _I32, _P, _P, _P, _P, _I32, _P, _P, _P, _P],
+    "sph_crk_factors_eos": [_P, _I64] + [_P] * 17,
     "sph_neighbors_expand": [_I64, _P, _P, _P, _I64, _P, _P, _P],
     "sph_density_gather": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P],
     "sph_adaptive_h_iter": [_P, _I64, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],

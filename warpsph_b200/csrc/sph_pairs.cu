@@ -225,12 +225,22 @@ template <int D> __device__ __forceinline__ double inv_sym(const double (&a)[D][
 template <int D> struct CrkAcc {
     float m0, s0, m1[D], s1[D], dm0[D], m2[D][D], dm1[D][D], dm2[D][D][D];
 };
+// The ideal-gas EOS of one particle (modules/eos/idealGas.py:16-36), as k_eos computes it:
+// fused into the epilogue of the pass that produces the density.
+struct EosOut { const float* u; float* A; float* P; float* c; float gamma; };
+__device__ __forceinline__ void eos_ideal_gas_at(int i, const EosOut& eo, float r) {
+    const float gamma = eo.gamma, ui = eo.u[i];
+    if (eo.c) eo.c[i] = sqrtf(fabsf(ui) * gamma * (gamma - 1.f));
+    if (eo.P) eo.P[i] = (gamma - 1.f) * r * ui;
+    if (eo.A) eo.A[i] = ui * (gamma - 1.f) * powf(r, 1.f - gamma);
+}
+
 template <int KF, int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_crk_factors(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
               const float* __restrict__ V, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
               const int32_t* __restrict__ list, float* __restrict__ Aout, float* __restrict__ Bout,
-              float* __restrict__ gAout, float* __restrict__ gBout, float* __restrict__ rho_out) {
+              float* __restrict__ gAout, float* __restrict__ gBout, float* __restrict__ rho_out, EosOut eo) {
     Grp<G> g(n);
     CrkAcc<D> a;
     {
@@ -354,6 +364,7 @@ k_crk_factors(int n, DevParams P, const float* __restrict__ x, const float* __re
         for (int c = 0; c < D; ++c) gBout[(size_t)i * D * D + u * D + c] = (float)gB[u][c];
     }
     if (rho_out) rho_out[i] = (float)rho;
+    if (eo.u) eos_ideal_gas_at(i, eo, (float)rho);
 }
 
 // ---------------------------------------------------------------- EOS (modules/eos/idealGas.py:16-36)
@@ -1145,6 +1156,39 @@ __global__ void k_rk_combine(int64_t count, const float* __restrict__ y0, int nk
     y[idx] = val;
 }
 
+// Several fields combined in one launch (the integrator's positions, velocities and
+// energies of one stage): the same arithmetic as k_rk_combine per element.
+constexpr int RKF_MAX = 4;
+struct FieldPtrs {
+    const float* y0[RKF_MAX];
+    float* y[RKF_MAX];
+    const float* k[RKF_MAX][8];
+    int64_t end[RKF_MAX];        // cumulative element counts
+    int wrap[RKF_MAX];
+    float w[8];
+};
+__global__ void k_rk_combine_fields(int nf, int nk, FieldPtrs F, const float* __restrict__ dtp, DomainF dom) {
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= F.end[nf - 1]) return;
+    int f = 0;
+    #pragma unroll
+    for (int q = 0; q < RKF_MAX - 1; ++q) f += (q < nf - 1 && g >= F.end[q]) ? 1 : 0;
+    const int64_t idx = g - (f > 0 ? F.end[f - 1] : 0);
+    const float dt = *dtp;
+    float s = 0.f;
+    for (int q = 0; q < nk; ++q) s = __fadd_rn(s, __fmul_rn(F.w[q], F.k[f][q][idx]));
+    float val = __fadd_rn(F.y0[f][idx], __fmul_rn(dt, s));
+    const int wd = F.wrap[f];
+    if (wd > 0) {
+        int a = (int)(idx % wd);
+        if (dom.periodic[a]) {
+            if (val >= dom.max[a]) val = __fsub_rn(val, dom.L[a]);
+            else if (val < dom.min[a]) val = __fadd_rn(val, dom.L[a]);
+        }
+    }
+    F.y[f][idx] = val;
+}
+
 // ---------------------------------------------------------------- compatible energy
 // modules/compSPH/multistep.py:52-94 and systems/compSPH.py:100-111
 struct StagePtrs {
@@ -1365,8 +1409,24 @@ int sph_crk_factors(const SphParams* p, int64_t n, const float* x, const float* 
     WSPH_CHECK_PTR(A); WSPH_CHECK_PTR(B); WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_crk_factors<KF, D, G_CRK><<<grid_g<G_CRK>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out)));
+    WSPH_DISPATCH_KDS(*p, (k_crk_factors<KF, D, G_CRK><<<grid_g<G_CRK>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out,
+                                                                                                   EosOut{nullptr, nullptr, nullptr, nullptr, 0.f})));
     return check_launch("sph_crk_factors");
+}
+
+int sph_crk_factors_eos(const SphParams* p, int64_t n, const float* x, const float* H, const float* m, const float* V,
+                        const int32_t* offs, const int32_t* cnt, const int32_t* list, float* A, float* B, float* gradA,
+                        float* gradB, float* rho_out, const float* u, float* entropy_out, float* P_out, float* c_out,
+                        void* stream) {
+    PAIR_PRELUDE();
+    WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(V);
+    WSPH_CHECK_PTR(A); WSPH_CHECK_PTR(B); WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); WSPH_CHECK_PTR(rho_out); WSPH_CHECK_PTR(u);
+    CHECK_CSR();
+    if ((rc = check_align_vec(P, x, "x"))) return rc;
+    wsph::count_launch();
+    WSPH_DISPATCH_KDS(*p, (k_crk_factors<KF, D, G_CRK><<<grid_g<G_CRK>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out,
+                                                                                                   EosOut{u, entropy_out, P_out, c_out, P.gamma})));
+    return check_launch("sph_crk_factors_eos");
 }
 
 int sph_eos_ideal_gas(const SphParams* p, int64_t n, const float* u, const float* rho, float* A_out, float* P_out,
@@ -1599,6 +1659,39 @@ int sph_rk_combine(const SphParams* p, int64_t count, const float* y0, int32_t n
     }
     wsph::count_launch(); k_rk_combine<<<grid_for(count, 256), 256, 0, WSPH_STREAM(stream)>>>(count, y0, nk, K, dt, wrap_dim, P.dom, y_out);
     return check_launch("sph_rk_combine");
+}
+
+int sph_rk_combine_fields(const SphParams* p, int32_t nfields, const int64_t* counts, const float* const* y0s,
+                          float* const* y_outs, const int32_t* wrap_dims, int32_t nk, const float* const* k_ptrs,
+                          const double* weights, const float* dt, void* stream) {
+    DevParams P;
+    int rc = params_to_dev(p, &P);
+    if (rc) return rc;
+    if (nfields < 1 || nfields > RKF_MAX) return set_error(SPH_ERR_BAD_ARG, "sph_rk_combine_fields: nfields must be in [1, %d]", RKF_MAX);
+    if (nk < 0 || nk > 8) return set_error(SPH_ERR_BAD_ARG, "sph_rk_combine_fields: nk must be in [0, 8]");
+    WSPH_CHECK_PTR(counts); WSPH_CHECK_PTR(y0s); WSPH_CHECK_PTR(y_outs); WSPH_CHECK_PTR(wrap_dims); WSPH_CHECK_PTR(dt);
+    if (nk > 0) { WSPH_CHECK_PTR(k_ptrs); WSPH_CHECK_PTR(weights); }
+    FieldPtrs F;
+    memset(&F, 0, sizeof(F));
+    int64_t total = 0;
+    for (int f = 0; f < nfields; ++f) {
+        if (counts[f] < 0) return set_error(SPH_ERR_BAD_ARG, "sph_rk_combine_fields: count %d < 0", f);
+        if (counts[f] > 0 && (!y0s[f] || !y_outs[f])) return set_error(SPH_ERR_BAD_ARG, "sph_rk_combine_fields: null field %d", f);
+        if (wrap_dims[f] < 0 || wrap_dims[f] > 3) return set_error(SPH_ERR_BAD_ARG, "sph_rk_combine_fields: wrap_dim %d out of range", f);
+        F.y0[f] = y0s[f]; F.y[f] = y_outs[f]; F.wrap[f] = wrap_dims[f];
+        for (int q = 0; q < nk; ++q) {
+            if (counts[f] > 0 && !k_ptrs[f * nk + q])
+                return set_error(SPH_ERR_BAD_ARG, "sph_rk_combine_fields: null derivative %d of field %d", q, f);
+            F.k[f][q] = k_ptrs[f * nk + q];
+        }
+        total += counts[f];
+        F.end[f] = total;
+    }
+    for (int q = 0; q < nk; ++q) F.w[q] = (float)weights[q];
+    if (total == 0) return SPH_OK;
+    wsph::count_launch();
+    k_rk_combine_fields<<<grid_for(total, 256), 256, 0, WSPH_STREAM(stream)>>>(nfields, nk, F, dt, P.dom);
+    return check_launch("sph_rk_combine_fields");
 }
 
 int sph_finalize_compatible_energy(const SphParams* p, int64_t n, int32_t nstages, const double* weights, const float* dt,

@@ -74,11 +74,19 @@ class RungeKuttaIntegrator:
         fields = getattr(type(sys0), "INTEGRATED", _COMPRESSIBLE_FIELDS)
 
         def advance(Ss, weights):
-            for name, deriv, wrap in fields:
-                y0 = getattr(S0, name)
-                if y0 is None:
-                    continue
-                setattr(Ss, name, self._combine(params, y0, [getattr(u, deriv) for u in updates], weights, dt, dim if wrap else 0))
+            # every integrated field in one launch (sph_rk_combine_fields), same arithmetic as
+            # one rk_combine per field
+            keep = [q for q, w in enumerate(weights) if w != 0.0]
+            todo = [(name, getattr(S0, name), [getattr(updates[q], deriv) for q in keep], dim if wrap else 0)
+                    for name, deriv, wrap in fields if getattr(S0, name) is not None]
+            if len(todo) > 4 or any(k is None for _, _, ks, _ in todo for k in ks):
+                for name, y0, _, wrap_dim in todo:
+                    deriv = next(d for nm, d, _ in fields if nm == name)
+                    setattr(Ss, name, self._combine(params, y0, [getattr(u, deriv) for u in updates], weights, dt, wrap_dim))
+                return
+            outs = ops.rk_combine_fields(params, [(y0, ks, wrap_dim) for _, y0, ks, wrap_dim in todo], [weights[q] for q in keep], dt)
+            for (name, _, _, _), y in zip(todo, outs):
+                setattr(Ss, name, y)
 
         for s in range(len(self.b)):
             Ss = prev.initializeNewState()

@@ -525,6 +525,19 @@ def crk_factors(params, x, H, m, V, adj: AdjacencyList):
     return CRKState(A=A, B=B, gradA=gA, gradB=gB), rho
 
 
+def crk_factors_eos(params, x, H, m, V, adj: AdjacencyList, u):
+    """crk_factors with the ideal-gas EOS of the CRK density in the same pass
+    (sph_crk_factors_eos): (crk, rho, entropy, P, c)."""
+    n, d = H.shape[0], int(params.dim)
+    A, B, gA, gB, rho = _empty(n, H), _empty((n, d), H), _empty((n, d), H), _empty((n, d, d), H), _empty(n, H)
+    Ae, P, c = _empty(n, H), _empty(n, H), _empty(n, H)
+    with _timed("crk_factors"):
+        check(_capi.lib().sph_crk_factors_eos(_p(params), n, fptr(x), fptr(H), fptr(m), fptr(V), *_lists(params, adj, True), ptr(A), ptr(B),
+                                              ptr(gA), ptr(gB), ptr(rho), fptr(u), ptr(Ae), ptr(P), ptr(c), stream_ptr(H.device)),
+              "sph_crk_factors_eos")
+    return CRKState(A=A, B=B, gradA=gA, gradB=gB), rho, Ae, P, c
+
+
 def eos_ideal_gas(params, u, rho):
     n = u.shape[0]
     A, P, c = _empty(n, u), _empty(n, u), _empty(n, u)
@@ -828,6 +841,37 @@ def rk_combine(params, y0: torch.Tensor, ks, weights, dt, wrap_dim: int = 0, out
                                          C.cast(w, C.c_void_p) if w is not None else None, fptr(dt_tensor(dt, y0.device)), wrap_dim,
                                          ptr(y), stream_ptr(y0.device)), "sph_rk_combine")
     return y
+
+
+def rk_combine_fields(params, fields, weights, dt):
+    """rk_combine over up to 4 fields in one launch (sph_rk_combine_fields).  fields: list of
+    (y0, [K_1..K_nk], wrap_dim); returns the new arrays in order."""
+    if not fields:
+        return []
+    if len(fields) > 4:
+        raise ValueError("rk_combine_fields: at most 4 fields per launch")
+    nk = len(weights)
+    y0s = [_f32(y0) for y0, _, _ in fields]
+    outs = [torch.empty_like(y) for y in y0s]
+    ks = []
+    for (_, kf, _), y in zip(fields, y0s):
+        if len(kf) != nk:
+            raise ValueError("rk_combine_fields: every field needs one derivative per weight")
+        ks += [fptr(_f32(k)) for k in kf]
+    counts = (C.c_int64 * len(fields))(*[y.numel() for y in y0s])
+    wraps = (C.c_int32 * len(fields))(*[int(w) for _, _, w in fields])
+    karr = _capi.ptr_array(ks) if ks else None
+    w = _capi.double_array(weights) if nk else None
+    dev = y0s[0].device
+    with _timed("rk_combine"):
+        check(_capi.lib().sph_rk_combine_fields(_p(params), len(fields), C.cast(counts, C.c_void_p),
+                                                C.cast(_capi.ptr_array([ptr(y) for y in y0s]), C.c_void_p),
+                                                C.cast(_capi.ptr_array([ptr(y) for y in outs]), C.c_void_p),
+                                                C.cast(wraps, C.c_void_p), nk,
+                                                C.cast(karr, C.c_void_p) if karr is not None else None,
+                                                C.cast(w, C.c_void_p) if w is not None else None,
+                                                fptr(dt_tensor(dt, dev)), stream_ptr(dev)), "sph_rk_combine_fields")
+    return outs
 
 
 def finalize_compatible_energy(params, weights, dt, v0, u0, stages):

@@ -6,8 +6,8 @@ every SPH operation executed by libwarpsph_b200 kernels:
 
   adaptive support (Monaghan Newton)  crkSPH.py:40  -> sph_adaptive_h_iter + sph_density_gather
   Verlet list                         crkSPH.py:54  -> sph_neighbors_build (unchanged prior reused)
-  CRK volume / coefficients / rho     crkSPH.py:61  -> sph_crk_volume + sph_crk_factors
-  ideal-gas EOS                       crkSPH.py:95  -> sph_eos_ideal_gas
+  CRK volume / coefficients / rho     crkSPH.py:61  -> sph_crk_volume + sph_crk_factors_eos
+  ideal-gas EOS                       crkSPH.py:95  -> the epilogue of sph_crk_factors_eos
   CRK velocity gradient               crkSPH.py:158 -> sph_grad_v (also the Cullen divergence)
   viscosity switch                    crkSPH.py:195 -> sph_switch_cullen (R and v_sig) / sph_switch_balsara
   momentum + energy RHS, dE/dt        crkSPH.py:241,263,330 -> sph_crk_accel_dudt (one fused pass)
@@ -76,9 +76,11 @@ def evaluateOptimalSupport(particleState, config: SimulationConfig, compParams: 
         adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, adjacency)
         rho, h_new, ratio = ops.adaptive_h_iter(params, S.positions, S.supports, S.masses, adjacency, hb)
         S.densities = rho
-        hb = ops.minmax(h_new)
         S.supports = h_new
-        if it < nIter - 1 and float((ratio - 1).abs().max()) < hThreshold:
+        if it == nIter - 1:
+            break
+        hb = ops.minmax(h_new)      # the support bounds of the next iteration
+        if float((ratio - 1).abs().max()) < hThreshold:
             break
     adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, adjacency)
     if not final_density:
@@ -140,12 +142,13 @@ def crkSPH_step(system: CompSPHSystem, dt, config: SimulationConfig, compParams:
     # crkSPH.py:54-59
     adjacency = ops.buildVerletList(S.positions, S.supports, params, config.verletScale, system.adjacency)
     system.adjacency = adjacency
-    # crkSPH.py:61
-    V, S.densities, crk = computeCRKFactors(S, config, adjacency, params)
+    # crkSPH.py:61 (computeCRKFactors) with crkSPH.py:95-101 (the ideal-gas EOS of the CRK
+    # density) in the epilogue of the same pass
+    V = ops.crk_volume(params, S.positions, S.supports, adjacency)
+    crk, S.densities, S.entropies, S.pressures, S.soundspeeds = ops.crk_factors_eos(params, S.positions, S.supports, S.masses, V,
+                                                                                   adjacency, S.internalEnergies)
     if S.divergence is None:
         S.divergence = torch.zeros_like(S.densities)
-    # crkSPH.py:95-101
-    S.entropies, S.pressures, S.soundspeeds = ops.eos_ideal_gas(params, S.internalEnergies, S.densities)
     switch = compParams.viscositySwitchParams.scheme
     cullen = switch == ViscositySwitch.CullenDehnen2010
     # crkSPH.py:158-172 (+ the Cullen divergence in the same pass)

@@ -113,12 +113,16 @@ class StepGraph:
         with ops.device_decided_lists(), torch.cuda.graph(self.graph):
             out, dt_new = self._advance(self.inputs, self.dt)
             static = dict(_per_particle(self.inputs.state, n))
+            dsts, srcs = [], []
             for name, v in _per_particle(out.state, n):
                 dst = static.get(name)
                 if dst is None:
                     raise RuntimeError(f"StepGraph: the step produces state field {name!r} that the warm-up state lacks")
                 if dst is not v:
-                    dst.copy_(v)
+                    dsts.append(dst)
+                    srcs.append(v)
+            if dsts:
+                torch._foreach_copy_(dsts, srcs)     # the copies in one or a few multi-tensor launches
             self.dt.copy_(dt_new)
             if isinstance(getattr(out, "t_device", None), torch.Tensor) and isinstance(getattr(self.inputs, "t_device", None), torch.Tensor):
                 self.inputs.t_device.copy_(out.t_device)
