@@ -219,9 +219,9 @@ int sph_neighbors_refresh_volume(const SphParams* p, int64_t n, const float* x, 
  * reference rebuilds every call).  The Verlet rows (neighbor_offsets, num_neighbors,
  * neighbor_list, nnz) are kept across calls together with the positions x0 [n, dim] and
  * supports H0 [n] they were built from.  One call checks them for (x, H) as
- * sph_neighbors_refresh does (verdict: 3 words of scratch) and, when a particle has left the
- * Verlet skin, rebuilds them in place on the GPU (every build launch returns at once when
- * the rows are kept) and copies x, H into x0, H0.  Initialise H0 with zeros (or anything
+ * sph_neighbors_refresh does (verdict: 4 words, zeroed once at allocation) and, when a
+ * particle has left the Verlet skin, rebuilds them in place on the GPU (every build launch
+ * returns at once when the rows are kept) and copies x, H into x0, H0.  Initialise H0 with zeros (or anything
  * non-finite) to force the first build.  The rows are in no particular order:
  * sph_neighbors_rewrite gives the interacting prefixes.  When a rebuild needs more than
  * list_capacity entries the status word gets SPH_STATUS_LIST_OVERFLOW and every row is cut
@@ -229,8 +229,9 @@ int sph_neighbors_refresh_volume(const SphParams* p, int64_t n, const float* x, 
  * status word at some later point and redo the work from a saved state with a larger list.
  * Zero-fill neighbor_list once at allocation.  rebuilds (optional, one int64 on the device) is
  * incremented by every rebuild.  Called on a stream that is being captured into a CUDA graph,
- * the rebuild is recorded as the body of an IF conditional node whose condition the GPU sets
- * from the verdict, so a replay that keeps the rows skips it; its body is captured on a
+ * the rebuild is recorded as the body of an IF conditional node whose condition the last block
+ * of the validity check sets from the verdict (and zeroes the verdict words for the next
+ * replay), so a replay that keeps the rows skips it; its body is captured on a
  * private stream per device, created by the first call outside a capture (make one before
  * capturing; without it the gated launches are recorded instead). */
 int sph_neighbors_update(const SphParams* p, int64_t n, const float* x, const float* H,

@@ -943,6 +943,46 @@ __global__ void k_refresh_check(const float* __restrict__ x, const float* __rest
     if (threadIdx.x == 0) { atomicMax(acc3 + 0, e0); atomicMax(acc3 + 1, e1); atomicMax(acc3 + 2, e2); }
 }
 
+// k_refresh_check for a recorded update: the last block to finish (acc[3] counts the blocks)
+// turns the verdict into the condition of the rebuild node and zeroes acc[0..3] for the
+// next replay, so the update needs neither a memset nor a separate condition kernel.
+// acc holds zeros before the first launch.
+template <int D>
+__global__ void k_refresh_check_cond(const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ x0,
+                                     const float* __restrict__ H0, int n, DevParams P, unsigned int* __restrict__ acc,
+                                     cudaGraphConditionalHandle h) {
+    float dmax = 0.f, amax = -__int_as_float(0x7f800000), hmax = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Vec<D> d = dist_vec<D>(load_vec<D>(x, i), load_vec<D>(x0, i), P.dom);
+        const float disp = sqrtf(dist2_rn<D>(d));
+        const float hh = H[i], h0 = P.verlet_scale * H0[i];
+        const bool bad = isnan(disp) || isnan(hh) || isnan(h0);
+        dmax = bad ? __int_as_float(0x7f800000) : fmaxf(dmax, disp);
+        amax = fmaxf(amax, hh - h0);
+        hmax = fmaxf(hmax, h0);
+    }
+    unsigned int e0 = ord_enc(dmax), e1 = ord_enc(amax), e2 = ord_enc(hmax);
+    e0 = block_reduce(e0, 0u, OpMaxU());
+    e1 = block_reduce(e1, 0u, OpMaxU());
+    e2 = block_reduce(e2, 0u, OpMaxU());
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        atomicMax(acc + 0, e0); atomicMax(acc + 1, e1); atomicMax(acc + 2, e2);
+        __threadfence();
+        last = atomicAdd(acc + 3, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        unsigned int v[3];
+        #pragma unroll
+        for (int q = 0; q < 3; ++q) v[q] = atomicAdd(acc + q, 0u);     // coherent reads of the merged words
+        cudaGraphSetConditional(h, refresh_valid(v) ? 0u : 1u);
+        #pragma unroll
+        for (int q = 0; q < 4; ++q) atomicExch(acc + q, 0u);
+    }
+}
+
 
 // Eight lanes per row, four rows per warp: the kept Verlet row rewritten into list_out
 // with the interacting entries (fl(sqrt(r^2)) / max(H_i, H_j) < 1 at the new positions,
@@ -1136,14 +1176,11 @@ static void build_rows(const DevParams& P, int64_t n, const float* x, const floa
 
 // ---------------------------------------------------------------- rebuild as a graph conditional
 // While a stream is being captured into a CUDA graph, the rebuild of sph_neighbors_update
-// goes into the body of an IF conditional node: one kernel turns the verdict into the
-// node's condition, and a replay whose rows are kept skips the whole body instead of
+// goes into the body of an IF conditional node: the validity check's last block turns the
+// verdict into the node's condition, and a replay whose rows are kept skips the whole body instead of
 // launching ~20 kernels that return at once.  The body is captured on a private stream per
 // device, created by the first call made outside a capture (a call during a capture with no
 // such stream yet falls back to the gated launches).
-__global__ void k_set_rebuild(const unsigned int* __restrict__ verdict, cudaGraphConditionalHandle h) {
-    cudaGraphSetConditional(h, refresh_valid(verdict) ? 0u : 1u);
-}
 
 constexpr int MAX_DEVICES = 64;
 static cudaStream_t g_body_stream[MAX_DEVICES] = {};
@@ -1175,7 +1212,7 @@ static cudaStream_t body_stream(bool create) {
 static int rebuild_conditional(const DevParams& P, int64_t n, const float* x, const float* H, float* x0, float* H0, const NbWs& w,
                                int64_t cell_capacity, int32_t* sort_index, uint32_t* sorted_keys, int32_t* cell_begin,
                                int32_t* cell_end, int32_t* grid_out, int32_t* offs, int32_t* cnt, int32_t* list,
-                               int64_t list_capacity, int64_t* nnz, const unsigned int* verdict, int32_t* status,
+                               int64_t list_capacity, int64_t* nnz, unsigned int* verdict, int32_t* status,
                                int64_t* rebuilds, cudaStream_t s, cudaStream_t bs) {
     cudaStreamCaptureStatus st;
     cudaGraph_t graph = nullptr;
@@ -1184,8 +1221,10 @@ static int rebuild_conditional(const DevParams& P, int64_t n, const float* x, co
     WSPH_CK_GRAPH(cudaStreamGetCaptureInfo(s, &st, nullptr, &graph, &deps, &ndeps));
     cudaGraphConditionalHandle h;
     WSPH_CK_GRAPH(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    int cblocks = (int)((n + 1023) / 1024);
+    if (cblocks > 148 * 4) cblocks = 148 * 4;
     wsph::count_launch();
-    k_set_rebuild<<<1, 1, 0, s>>>(verdict, h);
+    WSPH_DISPATCH_DIM(P.dim, (k_refresh_check_cond<D><<<cblocks, 256, 0, s>>>(x, H, x0, H0, (int)n, P, verdict, h)));
     WSPH_CK_GRAPH(cudaGetLastError());
     WSPH_CK_GRAPH(cudaStreamGetCaptureInfo(s, &st, nullptr, &graph, &deps, &ndeps));
     alignas(cudaGraphNodeParams) unsigned char np_bytes[sizeof(cudaGraphNodeParams)] = {};   // zeroed, as the API wants
@@ -1200,12 +1239,13 @@ static int rebuild_conditional(const DevParams& P, int64_t n, const float* x, co
     WSPH_CK_GRAPH(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
     WSPH_CK_GRAPH(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     const long long l0 = g_launches.load();
+    // the body runs only on a rebuild: its launches are ungated
     build_rows(P, n, x, H, w, cell_capacity, sort_index, sorted_keys, cell_begin, cell_end, grid_out, offs, cnt, list, list_capacity,
-               nnz, nullptr, nullptr, status, verdict, bs);
+               nnz, nullptr, nullptr, status, nullptr, bs);
     wsph::count_launch();
-    k_clamp_rows<<<grid_for(n, 256), 256, 0, bs>>>(reinterpret_cast<const long long*>(nnz), list_capacity, offs, cnt, (int)n, verdict);
+    k_clamp_rows<<<grid_for(n, 256), 256, 0, bs>>>(reinterpret_cast<const long long*>(nnz), list_capacity, offs, cnt, (int)n, nullptr);
     wsph::count_launch();
-    WSPH_DISPATCH_DIM(P.dim, (k_keep_state<D><<<grid_for(n, 256), 256, 0, bs>>>(x, H, x0, H0, (int)n, verdict,
+    WSPH_DISPATCH_DIM(P.dim, (k_keep_state<D><<<grid_for(n, 256), 256, 0, bs>>>(x, H, x0, H0, (int)n, nullptr,
                                                                                 reinterpret_cast<unsigned long long*>(rebuilds))));
     g_conditional_launches.fetch_add(g_launches.load() - l0);
     cudaGraph_t captured = nullptr;
@@ -1381,17 +1421,17 @@ int sph_neighbors_update(const SphParams* p, int64_t n, const float* x, const fl
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return check_launch("sph_neighbors_update");
     cudaStream_t bs = body_stream(cs == cudaStreamCaptureStatusNone);
-    cudaMemsetAsync(verdict, 0, 3 * sizeof(uint32_t), s);
-    int cblocks = (int)((n + 1023) / 1024);
-    if (cblocks > 148 * 4) cblocks = 148 * 4;
-    wsph::count_launch();
-    WSPH_DISPATCH_DIM(P.dim, (k_refresh_check<D><<<cblocks, 256, 0, s>>>(x, H, x0, H0, (int)n, P, verdict)));
     if (cs == cudaStreamCaptureStatusActive && bs != nullptr && bs != s) {
         rc = rebuild_conditional(P, n, x, H, x0, H0, w, cell_capacity, sort_index, sorted_keys, cell_begin, cell_end, grid_out,
                                  neighbor_offsets, num_neighbors, neighbor_list, list_capacity, nnz, verdict, status, rebuilds, s, bs);
         if (rc) return rc;
         return check_launch("sph_neighbors_update");
     }
+    cudaMemsetAsync(verdict, 0, 3 * sizeof(uint32_t), s);
+    int cblocks = (int)((n + 1023) / 1024);
+    if (cblocks > 148 * 4) cblocks = 148 * 4;
+    wsph::count_launch();
+    WSPH_DISPATCH_DIM(P.dim, (k_refresh_check<D><<<cblocks, 256, 0, s>>>(x, H, x0, H0, (int)n, P, verdict)));
     build_rows(P, n, x, H, w, cell_capacity, sort_index, sorted_keys, cell_begin, cell_end, grid_out, neighbor_offsets, num_neighbors,
                neighbor_list, list_capacity, nnz, nullptr, nullptr, status, verdict, s);
     wsph::count_launch();
