@@ -536,12 +536,14 @@ constexpr int VS = 16;
 constexpr int VP = VS + 1;
 
 // fl(sqrt(r2)) / Hm < 1, with the square root only inside a narrow band around r = Hm
-// (outside it the comparison of r2 with Hm^2 decides the same way).
+// (outside it the comparison of r2 with Hm^2 decides the same way).  For positive finite
+// a and b, fl(a / b) < 1 exactly when a < b (a < b gives a / b <= 1 - 2^-24, the float
+// next below 1, so a / b never rounds up to 1), so the test is fl(sqrt(r2)) < Hm.
 __device__ __forceinline__ bool interacting_pair(float r2, float Hm) {
     const float h2 = Hm * Hm;
     if (r2 < 0.9998f * h2) return true;
     if (!(r2 < 1.0002f * h2)) return false;
-    return __fdiv_rn(sqrtf(r2), Hm) < 1.f;
+    return sqrtf(r2) < Hm;
 }
 
 // Writes every lane's staged entries of one part: lanes pair up per owner row (16
@@ -1021,7 +1023,7 @@ __global__ void k_refilter(const float* __restrict__ x, const float* __restrict_
             j = list[b + base + sub];
             const Vec<D> d = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             const float Hm = fmaxf(Hi, __ldg(H + j));
-            keep = __fdiv_rn(sqrtf(dist2_rn<D>(d)), Hm) < 1.f;
+            keep = interacting_pair(dist2_rn<D>(d), Hm);
         }
         const unsigned int kb = (__ballot_sync(0xffffffffu, keep) >> gshift) & ((1u << RF_G) - 1u);
         const unsigned int rb = (__ballot_sync(0xffffffffu, in_row && !keep) >> gshift) & ((1u << RF_G) - 1u);
@@ -1078,7 +1080,7 @@ __global__ void k_refilter_volume(const float* __restrict__ x, const float* __re
             const Vec<D> d = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
             const float Hj = __ldg(H + j);
             const float Hm = fmaxf(Hi, Hj);
-            keep = __fdiv_rn(sqrtf(dist2_rn<D>(d)), Hm) < 1.f;
+            keep = interacting_pair(dist2_rn<D>(d), Hm);
             wsum += kW_inv<KF, D>(safe_sqrt(dot<D>(d, d)), 1.f / Hj);
         }
         const unsigned int kb = (__ballot_sync(0xffffffffu, keep) >> gshift) & ((1u << RF_G) - 1u);
