@@ -127,7 +127,7 @@ __device__ __forceinline__ float ord_dec(unsigned int o) {
 }
 __device__ __forceinline__ bool refresh_valid(const unsigned int* acc3) {
     const float dmax = ord_dec(acc3[0]), amax = ord_dec(acc3[1]), hmax = ord_dec(acc3[2]);
-    return amax + 2.0002f * dmax + 1e-5f * hmax <= 0.f;   // false for NaN
+    return amax + 1.0002f * dmax + 1e-5f * hmax <= 0.f;   // false for NaN
 }
 // Gate of the device-decided list update (sph_neighbors_update): a build kernel given
 // the verdict words returns at once when they say the kept list is still valid, so the
@@ -917,9 +917,10 @@ static int max_bits_for(int dim, int64_t cap) {
 // ---------------------------------------------------------------- prior-list refresh
 // Validity of a Verlet list built at (x0, H0): every pair with |x_i - x_j| < max(H_i, H_j)
 // at (x, H) is in the list when, for every particle k,
-//     H_k + 2 max_l |x_l - x0_l| <= vs H0_k
-// (triangle inequality: r0 <= r + |dx_i| + |dx_j| < H_i + 2 dmax <= vs H0_i <= vs max(H0_i, H0_j)).
-// k_refresh_check reduces max_k |x_k - x0_k|, max_k (H_k - vs H0_k) and max_k vs H0_k into
+//     H_k + |x_k - x0_k| + max_l |x_l - x0_l| <= vs H0_k
+// (triangle inequality, H_i the larger current support of the pair:
+//  r0 <= r + |dx_i| + |dx_j| < H_i + |dx_i| + dmax <= vs H0_i <= vs max(H0_i, H0_j)).
+// k_refresh_check reduces max_k |x_k - x0_k|, max_k (H_k - vs H0_k + |x_k - x0_k|) and max_k vs H0_k into
 // three ordered-encoded words; k_refilter evaluates the criterion (with a relative
 // margin for rounding) and, when it holds, rebuilds the interacting sublist in place of
 // a full neighbour search.
@@ -935,7 +936,7 @@ __global__ void k_refresh_check(const float* __restrict__ x, const float* __rest
         // a NaN anywhere makes the displacement bound infinite, which forces a rebuild
         const bool bad = isnan(disp) || isnan(h) || isnan(h0);
         dmax = bad ? __int_as_float(0x7f800000) : fmaxf(dmax, disp);
-        amax = fmaxf(amax, h - h0);
+        amax = fmaxf(amax, h - h0 + disp);
         hmax = fmaxf(hmax, h0);
     }
     unsigned int e0 = ord_enc(dmax), e1 = ord_enc(amax), e2 = ord_enc(hmax);
@@ -960,7 +961,7 @@ __global__ void k_refresh_check_cond(const float* __restrict__ x, const float* _
         const float hh = H[i], h0 = P.verlet_scale * H0[i];
         const bool bad = isnan(disp) || isnan(hh) || isnan(h0);
         dmax = bad ? __int_as_float(0x7f800000) : fmaxf(dmax, disp);
-        amax = fmaxf(amax, hh - h0);
+        amax = fmaxf(amax, hh - h0 + disp);
         hmax = fmaxf(hmax, h0);
     }
     unsigned int e0 = ord_enc(dmax), e1 = ord_enc(amax), e2 = ord_enc(hmax);
