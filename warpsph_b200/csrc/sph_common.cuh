@@ -289,6 +289,16 @@ template <int D> __device__ __forceinline__ Vec<D> crk_grad(const Vec<D>& x, flo
         default: break;                                                                               \
     }
 
+// ---------------------------------------------------------------- programmatic dependent launch
+// A kernel launched by launch_pdl (host side, sph_pair_common.cuh) starts with pdl_entry():
+// it lets the next kernel of the stream begin launching once every block of this one has
+// started (its blocks then wait on the SMs instead of behind a launch), and waits until the
+// kernel before it has completed and its writes are visible before touching memory.
+__device__ __forceinline__ void pdl_entry() {
+    cudaTriggerProgrammaticLaunchCompletion();
+    cudaGridDependencySynchronize();
+}
+
 // ---------------------------------------------------------------- host side
 int set_error(int code, const char* fmt, ...);
 int check_launch(const char* what);

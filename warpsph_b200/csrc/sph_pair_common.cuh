@@ -3,6 +3,7 @@
 // evaluation with a precomputed 1/H, group reductions, and the host-side argument
 // checks and template dispatch of the pair entry points.
 #pragma once
+#include <cstring>
 #include <cuda_runtime.h>
 #include "sph_common.cuh"
 
@@ -116,6 +117,24 @@ struct KSum {
 
 #define WSPH_DISPATCH_KDS(params, ...) WSPH_DISPATCH_KD(P.kernel, P.dim, __VA_ARGS__)
 #define WSPH_DISPATCH_DS(params, ...) WSPH_DISPATCH_DIM(P.dim, __VA_ARGS__)
+
+// Launch with programmatic stream serialization (the kernel must begin with pdl_entry()).
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    memset(at, 0, sizeof(at));
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    (void)cudaLaunchKernelEx(&cfg, kern, args...);
+}
 
 #define PAIR_PRELUDE()                                                        \
     DevParams P;                                                              \

@@ -28,6 +28,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK)
 k_density(int n, int mode, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
           const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
           float* __restrict__ rho) {
+    pdl_entry();
     Grp<G> g(n);
     float s = 0.f;
     if (g.valid) {
@@ -61,6 +62,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK)
 k_adaptive_h(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H, const float* __restrict__ m,
              const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
              const float* __restrict__ hb, float* __restrict__ rho_out, float* __restrict__ H_out, float* __restrict__ ratio) {
+    pdl_entry();
     Grp<G> g(n);
     float rs = 0.f, ds = 0.f, Hi = 1.f;
     if (g.valid) {
@@ -129,6 +131,7 @@ k_owen(int n, DevParams P, const float* __restrict__ x, const float* __restrict_
        const double* __restrict__ lut_nh, const double* __restrict__ lut_psiH, int nlut, float target,
        const float* __restrict__ hb, float* __restrict__ psi0_out, float* __restrict__ psiH_out,
        float* __restrict__ H_out, float* __restrict__ ratio) {
+    pdl_entry();
     Grp<G> g(n);
     float sW = 0.f, sG = 0.f, Hi = 1.f;
     if (g.valid) {
@@ -171,6 +174,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK)
 k_crk_volume(int n, DevParams P, const float* __restrict__ x, const float* __restrict__ H,
              const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
              float* __restrict__ V) {
+    pdl_entry();
     Grp<G> g(n);
     float s = 0.f;
     if (g.valid) {
@@ -241,6 +245,7 @@ k_crk_factors(int n, DevParams P, const float* __restrict__ x, const float* __re
               const float* __restrict__ V, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
               const int32_t* __restrict__ list, float* __restrict__ Aout, float* __restrict__ Bout,
               float* __restrict__ gAout, float* __restrict__ gBout, float* __restrict__ rho_out, EosOut eo) {
+    pdl_entry();
     Grp<G> g(n);
     CrkAcc<D> a;
     {
@@ -370,6 +375,7 @@ k_crk_factors(int n, DevParams P, const float* __restrict__ x, const float* __re
 // ---------------------------------------------------------------- EOS (modules/eos/idealGas.py:16-36)
 __global__ void k_eos(int n, float gamma, const float* __restrict__ u, const float* __restrict__ rho,
                       float* __restrict__ Aout, float* __restrict__ Pout, float* __restrict__ cout) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float ui = u[i], r = rho[i];
@@ -388,6 +394,7 @@ k_grad_v(int n, DevParams P, const float* __restrict__ x, const float* __restric
          const float* __restrict__ gA, const float* __restrict__ gB, const float* __restrict__ v, const float* __restrict__ c,
          const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
          float* __restrict__ DvDx, float* __restrict__ drhodt, float* __restrict__ div_out, float* __restrict__ vsig_out) {
+    pdl_entry();
     Grp<G> g(n);
     const bool want_div = div_out != nullptr, want_vs = vsig_out != nullptr;
     Mat<D> Gm = mzero<D>();
@@ -470,6 +477,7 @@ k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restric
          const float* __restrict__ alpha0_prev, const float* __restrict__ dtp,
          const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
          float* __restrict__ alpha_out, float* __restrict__ R_out, float* __restrict__ vsig_out) {
+    pdl_entry();
     Grp<G> g(n);
     const bool want_vs = vsig_in == nullptr;
     float s = 0.f, vsig = 0.f;
@@ -549,6 +557,7 @@ k_hopkins_grad(int n, DevParams P, const float* __restrict__ x, const float* __r
                const float* __restrict__ rho, const float* __restrict__ v,
                const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
                float* __restrict__ div_out, float* __restrict__ shear2_out) {
+    pdl_entry();
     Grp<G> g(n);
     Mat<D> Gm = mzero<D>(), Mm = mzero<D>();
     const bool corr = P.correct_grad_v != 0;
@@ -635,6 +644,7 @@ k_hopkins_alpha(int n, DevParams P, const float* __restrict__ x, const float* __
                 const float* __restrict__ rho, const float* __restrict__ div, const float* __restrict__ shear2,
                 const float* __restrict__ alpha0, const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt,
                 const int32_t* __restrict__ list, float* __restrict__ alpha_out, float* __restrict__ R_out) {
+    pdl_entry();
     Grp<G> g(n);
     float s = 0.f;
     if (g.valid) {
@@ -676,6 +686,7 @@ k_hopkins_update(int n, DevParams P, const float* __restrict__ x, const float* _
                  const float* __restrict__ alpha0, const float* __restrict__ dtp,
                  const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
                  float* __restrict__ alpha0_out, float* __restrict__ vsig_out) {
+    pdl_entry();
     Grp<G> g(n);
     float vsig = 0.f;
     if (g.valid) {
@@ -720,6 +731,7 @@ k_hopkins_update(int n, DevParams P, const float* __restrict__ x, const float* _
 // Balsara switch from the velocity gradient (schemes/crkSPH.py:132-133 comment).
 template <int D>
 __global__ void k_balsara(int n, const float* __restrict__ DvDx, const float* __restrict__ c, float* __restrict__ alpha) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Mat<D> Gm = load_mat<D>(DvDx, i);
@@ -801,6 +813,7 @@ __global__ void k_crk_pack(int n, const float* __restrict__ x, const float* __re
                            const float* __restrict__ gA, const float* __restrict__ gB, const float* __restrict__ v,
                            const float* __restrict__ c, const float* __restrict__ Pr, const float* __restrict__ DvDx,
                            float* __restrict__ rec) {
+    pdl_entry();
     using L = CrkRec<D>;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -882,6 +895,7 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
                  const int32_t* __restrict__ cnt, const int32_t* __restrict__ list, const int32_t* __restrict__ vcnt,
                  float* __restrict__ dvdt, float* __restrict__ dudt, float* __restrict__ dEdt, float* __restrict__ ap,
                  float* __restrict__ av) {
+    pdl_entry();
     Grp<G> g(n);
     const bool comp = P.kahan != 0;
     KSum acc[D], du;
@@ -1036,6 +1050,7 @@ template <int D>
 __global__ void k_balance_prep(int n, DevParams P, const float* __restrict__ rho, const float* __restrict__ Pr,
                                const float* __restrict__ v, const float* __restrict__ dvdt, const float* __restrict__ dtp,
                                float* __restrict__ vh, float* __restrict__ sarr) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float hdt = 0.5f * (*dtp);
@@ -1052,6 +1067,7 @@ k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restri
           const float* __restrict__ u, const float* __restrict__ vh, const float* __restrict__ sarr, const float* __restrict__ dtp,
           const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
           const int32_t* __restrict__ icnt, const float* __restrict__ ap, const float* __restrict__ av, float* __restrict__ fout) {
+    pdl_entry();
     Grp<G> g(n);
     if (!g.valid) return;
     const int i = g.i;
@@ -1111,6 +1127,7 @@ k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restri
 // ---------------------------------------------------------------- CFL dt (modules/timestep/compressible.py:18-61)
 __global__ void k_cfl_reduce(int n, float gamma, const float* __restrict__ H, const float* __restrict__ u,
                              float* __restrict__ red /* [0]=min H, [1]=max c */) {
+    pdl_entry();
     float hmin = __int_as_float(0x7f800000), cmax = 0.f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         hmin = fminf(hmin, H[i]);
@@ -1123,8 +1140,10 @@ __global__ void k_cfl_reduce(int n, float gamma, const float* __restrict__ H, co
         atomicMax(reinterpret_cast<int*>(red + 1), __float_as_int(cmax));
     }
 }
-__global__ void k_cfl_init(float* red) { red[0] = __int_as_float(0x7f800000); red[1] = 0.f; }
+__global__ void k_cfl_init(float* red) {
+    pdl_entry(); red[0] = __int_as_float(0x7f800000); red[1] = 0.f; }
 __global__ void k_cfl_final(DevParams P, const float* __restrict__ red, const float* __restrict__ dt_prev, float* __restrict__ dt_out) {
+    pdl_entry();
     // min_i cfl*h/(c_i*xi) is attained at max_i c_i (the map c -> cfl*h/(c*xi) is monotone)
     float dt = P.cfl * red[0] / (red[1] * P.kxi);
     dt = fminf(fmaxf(dt, P.min_dt), P.max_dt);
@@ -1139,6 +1158,7 @@ __global__ void k_cfl_final(DevParams P, const float* __restrict__ red, const fl
 struct KPtrs { const float* k[8]; float w[8]; };
 __global__ void k_rk_combine(int64_t count, const float* __restrict__ y0, int nk, KPtrs K, const float* __restrict__ dtp,
                              int wrap_dim, DomainF dom, float* __restrict__ y) {
+    pdl_entry();
     int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= count) return;
     float dt = *dtp;
@@ -1168,6 +1188,7 @@ struct FieldPtrs {
     float w[8];
 };
 __global__ void k_rk_combine_fields(int nf, int nk, FieldPtrs F, const float* __restrict__ dtp, DomainF dom) {
+    pdl_entry();
     int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= F.end[nf - 1]) return;
     int f = 0;
@@ -1203,6 +1224,7 @@ struct StagePtrs {
 };
 template <int D>
 __global__ void k_vhalf(int n, int ns, StagePtrs S, const float* __restrict__ dtp, const float* __restrict__ v0, float* __restrict__ vh) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float dt = *dtp;
@@ -1217,6 +1239,7 @@ template <int D, int G>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_finalize(int n, int ns, StagePtrs S, int pdv, const float* __restrict__ dtp, const float* __restrict__ vh,
            const float* __restrict__ u0, float* __restrict__ u_out, float* __restrict__ du_out) {
+    pdl_entry();
     Grp<G> g(n);
     float du = 0.f;
     if (g.valid) {
@@ -1252,6 +1275,7 @@ k_finalize(int n, int ns, StagePtrs S, int pdv, const float* __restrict__ dtp, c
 // ---------------------------------------------------------------- conservation sums (FP64)
 template <int D>
 __global__ void k_cons(int n, const float* __restrict__ m, const float* __restrict__ v, const float* __restrict__ u, double* out) {
+    pdl_entry();
     double M = 0, KE = 0, IE = 0, p[3] = {0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double mi = m[i];
@@ -1359,7 +1383,7 @@ int sph_density_gather(const SphParams* p, int64_t n, int32_t support_mode, cons
     if (support_mode < 0 || support_mode > 4) return set_error(SPH_ERR_BAD_ARG, "bad support mode %d", support_mode);
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_density<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, support_mode, P, x, H, m, offs, cnt, list, rho_out)));
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_density<KF, D, G_LIGHT>, grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s, (int)n, support_mode, P, x, H, m, offs, cnt, list, rho_out)));
     return check_launch("sph_density_gather");
 }
 
@@ -1371,7 +1395,7 @@ int sph_adaptive_h_iter(const SphParams* p, int64_t n, int32_t support_mode, con
     if (support_mode != SPH_SUPPORT_GATHER) return set_error(SPH_ERR_UNSUPPORTED, "adaptive support: only the gather scheme is implemented");
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_adaptive_h<KF, D, G_SCAN(D)><<<grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, offs, cnt, list, hbounds, rho_out, H_out, ratio_out)));
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_adaptive_h<KF, D, G_SCAN(D)>, grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, offs, cnt, list, hbounds, rho_out, H_out, ratio_out)));
     return check_launch("sph_adaptive_h_iter");
 }
 
@@ -1385,7 +1409,7 @@ int sph_owen_iter(const SphParams* p, int64_t n, const float* x, const float* H,
     if (!(target_nh > 0.0)) return set_error(SPH_ERR_BAD_ARG, "sph_owen_iter: target n_h must be positive");
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_owen<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, offs, cnt, list, lut_nh, lut_psiH,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_owen<KF, D, G_LIGHT>, grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, offs, cnt, list, lut_nh, lut_psiH,
                                                                                              (int)nlut, (float)target_nh, hbounds, psi0_out,
                                                                                              psiH_out, H_out, ratio_out)));
     return check_launch("sph_owen_iter");
@@ -1397,7 +1421,7 @@ int sph_crk_volume(const SphParams* p, int64_t n, const float* x, const float* H
     WSPH_CHECK_PTR(x); WSPH_CHECK_PTR(H); WSPH_CHECK_PTR(V_out); CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_crk_volume<KF, D, G_SCAN(D)><<<grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, offs, cnt, list, V_out)));
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_crk_volume<KF, D, G_SCAN(D)>, grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, offs, cnt, list, V_out)));
     return check_launch("sph_crk_volume");
 }
 
@@ -1409,7 +1433,7 @@ int sph_crk_factors(const SphParams* p, int64_t n, const float* x, const float* 
     WSPH_CHECK_PTR(A); WSPH_CHECK_PTR(B); WSPH_CHECK_PTR(gradA); WSPH_CHECK_PTR(gradB); CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_crk_factors<KF, D, G_CRK><<<grid_g<G_CRK>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_crk_factors<KF, D, G_CRK>, grid_g<G_CRK>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out,
                                                                                                    EosOut{nullptr, nullptr, nullptr, nullptr, 0.f})));
     return check_launch("sph_crk_factors");
 }
@@ -1424,7 +1448,7 @@ int sph_crk_factors_eos(const SphParams* p, int64_t n, const float* x, const flo
     CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_crk_factors<KF, D, G_CRK><<<grid_g<G_CRK>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_crk_factors<KF, D, G_CRK>, grid_g<G_CRK>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, V, offs, cnt, list, A, B, gradA, gradB, rho_out,
                                                                                                    EosOut{u, entropy_out, P_out, c_out, P.gamma})));
     return check_launch("sph_crk_factors_eos");
 }
@@ -1433,7 +1457,7 @@ int sph_eos_ideal_gas(const SphParams* p, int64_t n, const float* u, const float
                       float* c_out, void* stream) {
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(u); WSPH_CHECK_PTR(rho);
-    wsph::count_launch(); k_eos<<<grid_for(n, 256), 256, 0, s>>>((int)n, P.gamma, u, rho, A_out, P_out, c_out);
+    wsph::count_launch(); launch_pdl(k_eos, grid_for(n, 256), 256, 0, s, (int)n, P.gamma, u, rho, A_out, P_out, c_out);
     return check_launch("sph_eos_ideal_gas");
 }
 
@@ -1450,7 +1474,7 @@ int sph_grad_v(const SphParams* p, int64_t n, const float* x, const float* H, co
         (rc = check_align_vec(P, gradA, "gradA")))
         return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_grad_v<KF, D, G_SCAN(D)><<<grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_grad_v<KF, D, G_SCAN(D)>, grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c,
                                                                                                   offs, cnt, list, DvDx_out, drhodt_out, div_out, vsig_out)));
     return check_launch("sph_grad_v");
 }
@@ -1465,7 +1489,7 @@ int sph_switch_cullen(const SphParams* p, int64_t n, const float* x, const float
     if (!vsig) { WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(c); }   // v_sig needs the whole Verlet rows
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_cullen<KF, D, G_SCAN(D)><<<grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div, div_prev, vsig, v, c,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_cullen<KF, D, G_SCAN(D)>, grid_g<G_SCAN(D)>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, rho, div, div_prev, vsig, v, c,
                                                                                                   alpha0_prev, dt, offs, cnt, list, alpha_out, R_out, vsig_out)));
     return check_launch("sph_switch_cullen");
 }
@@ -1478,11 +1502,11 @@ int sph_switch_hopkins_terms(const SphParams* p, int64_t n, const float* x, cons
     WSPH_CHECK_PTR(div_out); WSPH_CHECK_PTR(shear2_out); WSPH_CHECK_PTR(alpha_out); CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_hopkins_grad<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, v, offs, cnt, list,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_hopkins_grad<KF, D, G_LIGHT>, grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, rho, v, offs, cnt, list,
                                                                                                        div_out, shear2_out)));
     if ((rc = check_launch("sph_switch_hopkins_terms"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_hopkins_alpha<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, div_out, shear2_out,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_hopkins_alpha<KF, D, G_LIGHT>, grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, rho, div_out, shear2_out,
                                                                                                         alpha0, offs, cnt, list, alpha_out, R_out)));
     return check_launch("sph_switch_hopkins_terms");
 }
@@ -1496,7 +1520,7 @@ int sph_switch_hopkins_update(const SphParams* p, int64_t n, const float* x, con
     WSPH_CHECK_PTR(alpha0); WSPH_CHECK_PTR(dt); WSPH_CHECK_PTR(alpha0_out); CHECK_CSR();
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_DS(*p, (k_hopkins_update<D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, v, c, div, div_prev, alpha0, dt,
+    WSPH_DISPATCH_DS(*p, (launch_pdl(k_hopkins_update<D, G_LIGHT>, grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, v, c, div, div_prev, alpha0, dt,
                                                                                                   offs, cnt, list, alpha0_out, vsig_out)));
     return check_launch("sph_switch_hopkins_update");
 }
@@ -1504,7 +1528,7 @@ int sph_switch_hopkins_update(const SphParams* p, int64_t n, const float* x, con
 int sph_switch_balsara(const SphParams* p, int64_t n, const float* DvDx, const float* c, float* alpha_out, void* stream) {
     PAIR_PRELUDE();
     WSPH_CHECK_PTR(DvDx); WSPH_CHECK_PTR(c); WSPH_CHECK_PTR(alpha_out);
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_balsara<D><<<grid_for(n, 256), 256, 0, s>>>((int)n, DvDx, c, alpha_out)));
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (launch_pdl(k_balsara<D>, grid_for(n, 256), 256, 0, s, (int)n, DvDx, c, alpha_out)));
     return check_launch("sph_switch_balsara");
 }
 
@@ -1526,16 +1550,14 @@ static int crk_accel_dudt_impl(const SphParams* p, int64_t n, const float* x, co
         return set_error(SPH_ERR_BAD_ARG, "%s: records must be 16-byte aligned", name);
     if (records) {
         wsph::count_launch();
-        WSPH_DISPATCH_DS(*p, (k_crk_pack<D><<<(unsigned)((n + 255) / 256), 256, 0, s>>>((int)n, x, H, rho, V, A, B, gradA, gradB, v, c,
+        WSPH_DISPATCH_DS(*p, (launch_pdl(k_crk_pack<D>, (unsigned)((n + 255) / 256), 256, 0, s, (int)n, x, H, rho, V, A, B, gradA, gradB, v, c,
                                                                                        Pr, DvDx, records)));
         wsph::count_launch();
-        WSPH_DISPATCH_KDS(*p, (k_crk_accel_dudt<KF, D, G_ACCEL, true><<<grid_g<G_ACCEL>(n), PAIR_BLOCK, 0, s>>>(
-                                  (int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c, Pr, DvDx, records, offs, cnt, list,
+        WSPH_DISPATCH_KDS(*p, (launch_pdl(k_crk_accel_dudt<KF, D, G_ACCEL, true>, grid_g<G_ACCEL>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c, Pr, DvDx, records, offs, cnt, list,
                                   verlet_cnt, dvdt_out, dudt_out, dEdt_out, ap_ij, av_ij)));
     } else {
         wsph::count_launch();
-        WSPH_DISPATCH_KDS(*p, (k_crk_accel_dudt<KF, D, G_ACCEL, false><<<grid_g<G_ACCEL>(n), PAIR_BLOCK, 0, s>>>(
-                                  (int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c, Pr, DvDx, nullptr, offs, cnt, list,
+        WSPH_DISPATCH_KDS(*p, (launch_pdl(k_crk_accel_dudt<KF, D, G_ACCEL, false>, grid_g<G_ACCEL>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, rho, V, A, B, gradA, gradB, v, c, Pr, DvDx, nullptr, offs, cnt, list,
                                   verlet_cnt, dvdt_out, dudt_out, dEdt_out, ap_ij, av_ij)));
     }
     return check_launch(name);
@@ -1593,9 +1615,9 @@ int sph_compsph_balance(const SphParams* p, int64_t n, const float* m, const flo
         return rc;
     float* vh = scratch;
     float* sarr = scratch + n * P.dim;
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_balance_prep<D><<<grid_for(n, 256), 256, 0, s>>>((int)n, P, rho, Pr, v, dvdt, dt, vh, sarr)));
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (launch_pdl(k_balance_prep<D>, grid_for(n, 256), 256, 0, s, (int)n, P, rho, Pr, v, dvdt, dt, vh, sarr)));
     wsph::count_launch();
-    WSPH_DISPATCH_DS(*p, (k_balance<D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, m, rho, Pr, u, vh, sarr, dt, offs, cnt, list, inter_counts, ap_ij, av_ij, f_ij_out)));
+    WSPH_DISPATCH_DS(*p, (launch_pdl(k_balance<D, G_LIGHT>, grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s, (int)n, P, m, rho, Pr, u, vh, sarr, dt, offs, cnt, list, inter_counts, ap_ij, av_ij, f_ij_out)));
     return check_launch("sph_compsph_balance");
 }
 
@@ -1634,11 +1656,11 @@ int sph_cfl_dt(const SphParams* p, int64_t n, const float* H, const float* u, co
     (void)rho;
     cudaStream_t s = WSPH_STREAM(stream);
     float* red = dt_out + 1;
-    wsph::count_launch(); k_cfl_init<<<1, 1, 0, s>>>(red);
+    wsph::count_launch(); launch_pdl(k_cfl_init, 1, 1, 0, s, red);
     int blocks = (int)((n + 1023) / 1024);
     if (blocks > 148 * 4) blocks = 148 * 4;
-    wsph::count_launch(); k_cfl_reduce<<<blocks, 256, 0, s>>>((int)n, P.gamma, H, u, red);
-    wsph::count_launch(); k_cfl_final<<<1, 1, 0, s>>>(P, red, dt_prev, dt_out);
+    wsph::count_launch(); launch_pdl(k_cfl_reduce, blocks, 256, 0, s, (int)n, P.gamma, H, u, red);
+    wsph::count_launch(); launch_pdl(k_cfl_final, 1, 1, 0, s, P, red, dt_prev, dt_out);
     return check_launch("sph_cfl_dt");
 }
 
@@ -1657,7 +1679,7 @@ int sph_rk_combine(const SphParams* p, int64_t count, const float* y0, int32_t n
         if (!k_ptrs || !k_ptrs[q] || !weights) return set_error(SPH_ERR_BAD_ARG, "sph_rk_combine: null derivative %d", q);
         K.k[q] = k_ptrs[q]; K.w[q] = (float)weights[q];
     }
-    wsph::count_launch(); k_rk_combine<<<grid_for(count, 256), 256, 0, WSPH_STREAM(stream)>>>(count, y0, nk, K, dt, wrap_dim, P.dom, y_out);
+    wsph::count_launch(); launch_pdl(k_rk_combine, grid_for(count, 256), 256, 0, WSPH_STREAM(stream), count, y0, nk, K, dt, wrap_dim, P.dom, y_out);
     return check_launch("sph_rk_combine");
 }
 
@@ -1690,7 +1712,7 @@ int sph_rk_combine_fields(const SphParams* p, int32_t nfields, const int64_t* co
     for (int q = 0; q < nk; ++q) F.w[q] = (float)weights[q];
     if (total == 0) return SPH_OK;
     wsph::count_launch();
-    k_rk_combine_fields<<<grid_for(total, 256), 256, 0, WSPH_STREAM(stream)>>>(nfields, nk, F, dt, P.dom);
+    launch_pdl(k_rk_combine_fields, grid_for(total, 256), 256, 0, WSPH_STREAM(stream), nfields, nk, F, dt, P.dom);
     return check_launch("sph_rk_combine_fields");
 }
 
@@ -1714,9 +1736,9 @@ int sph_finalize_compatible_energy(const SphParams* p, int64_t n, int32_t nstage
     if (!du_out) return set_error(SPH_ERR_BAD_ARG, "finalize: du_out must hold n*(1+dim) floats (du and v_half scratch)");
     float* vh = du_out + n;
     int pdv = P.energy_scheme == SPH_ENERGY_PDV;
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_vhalf<D><<<grid_for(n, 256), 256, 0, s>>>((int)n, nstages, S, dt, v0, vh)));
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (launch_pdl(k_vhalf<D>, grid_for(n, 256), 256, 0, s, (int)n, nstages, S, dt, v0, vh)));
     wsph::count_launch();
-    WSPH_DISPATCH_DS(*p, (k_finalize<D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, nstages, S, pdv, dt, vh, u0, u_out, du_out)));
+    WSPH_DISPATCH_DS(*p, (launch_pdl(k_finalize<D, G_LIGHT>, grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s, (int)n, nstages, S, pdv, dt, vh, u0, u_out, du_out)));
     return check_launch("sph_finalize_compatible_energy");
 }
 
@@ -1732,7 +1754,7 @@ int sph_conservation_sums(const SphParams* p, int64_t n, const float* m, const f
     WSPH_CHECK_PTR(m); WSPH_CHECK_PTR(v); WSPH_CHECK_PTR(u);
     int blocks = grid_for(n, 256);
     if (blocks > 148 * 4) blocks = 148 * 4;
-    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (k_cons<D><<<blocks, 256, 0, s>>>((int)n, m, v, u, out)));
+    wsph::count_launch(); WSPH_DISPATCH_DIM(P.dim, (launch_pdl(k_cons<D>, blocks, 256, 0, s, (int)n, m, v, u, out)));
     return check_launch("sph_conservation_sums");
 }
 
