@@ -31,6 +31,7 @@ k_compsph_prep(int n, DevParams P, const float* __restrict__ x, const float* __r
                const float* __restrict__ rho, const float* __restrict__ v,
                const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
                float* __restrict__ omega, float* __restrict__ div, float* __restrict__ drhodt) {
+    pdl_entry();
     Grp<G> g(n);
     const bool want_om = omega != nullptr, want_div = div != nullptr, want_con = drhodt != nullptr;
     float sdh = 0.f, sdiv = 0.f, scon = 0.f;
@@ -104,6 +105,7 @@ __global__ void k_compsph_pack(int n, DevParams P, const float* __restrict__ x, 
                                const float* __restrict__ rho, const float* __restrict__ v, const float* __restrict__ c,
                                const float* __restrict__ alpha, const float* __restrict__ Pr, const float* __restrict__ omega,
                                float* __restrict__ rec) {
+    pdl_entry();
     using L = CompRec<D>;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -137,6 +139,7 @@ k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const floa
                      const int32_t* __restrict__ offs, const int32_t* __restrict__ cnt, const int32_t* __restrict__ list,
                      const int32_t* __restrict__ vcnt, float* __restrict__ dvdt, float* __restrict__ dudt,
                      float* __restrict__ dEdt, float* __restrict__ ap, float* __restrict__ av) {
+    pdl_entry();
     Grp<G> g(n);
     const bool comp = P.kahan != 0;
     KSum acc[D], du;
@@ -285,6 +288,7 @@ k_monaghan_rhs(int n, DevParams P, const float* __restrict__ x, const float* __r
                float* __restrict__ dvdt, float* __restrict__ dudt, float* __restrict__ dEdt,
                float* __restrict__ dvdt_p, float* __restrict__ dvdt_visc, float* __restrict__ dudt_pdv,
                float* __restrict__ dudt_cond, float* __restrict__ dudt_heat) {
+    pdl_entry();
     Grp<G> g(n);
     const bool comp = P.kahan != 0;
     KSum sp[D], sv[D], spdv, scond, sheat;
@@ -384,7 +388,7 @@ int sph_compsph_prep(const SphParams* p, int64_t n, const float* x, const float*
     if (!omega_out && !div_out && !drhodt_out) return SPH_OK;
     if ((rc = check_align_vec(P, x, "x")) || (rc = check_align_vec(P, v, "v"))) return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_compsph_prep<KF, D, G_LIGHT><<<grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s>>>((int)n, P, x, H, m, rho, v, offs, cnt, list,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_compsph_prep<KF, D, G_LIGHT>, grid_g<G_LIGHT>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, rho, v, offs, cnt, list,
                                                                                                         omega_out, div_out, drhodt_out)));
     return check_launch("sph_compsph_prep");
 }
@@ -406,8 +410,7 @@ int sph_compsph_accel_dudt(const SphParams* p, int64_t n, const float* x, const 
         (rc = check_align_vec(P, ap_ij, "ap_ij")) || (rc = check_align_vec(P, av_ij, "av_ij")))
         return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_compsph_accel_dudt<KF, D, G_HEAVY, false><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>(
-                              (int)n, P, x, H, m, rho, v, c, alpha, Pr, omega, nullptr, offs, cnt, list, verlet_cnt, dvdt_out, dudt_out,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_compsph_accel_dudt<KF, D, G_HEAVY, false>, grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, rho, v, c, alpha, Pr, omega, nullptr, offs, cnt, list, verlet_cnt, dvdt_out, dudt_out,
                               dEdt_out, ap_ij, av_ij)));
     return check_launch("sph_compsph_accel_dudt");
 }
@@ -430,11 +433,10 @@ int sph_compsph_accel_dudt_packed(const SphParams* p, int64_t n, const float* x,
         return rc;
     if (reinterpret_cast<uintptr_t>(records) & 15) return set_error(SPH_ERR_BAD_ARG, "sph_compsph_accel_dudt_packed: records must be 16-byte aligned");
     wsph::count_launch();
-    WSPH_DISPATCH_DS(*p, (k_compsph_pack<D><<<(unsigned)((n + 255) / 256), 256, 0, s>>>((int)n, P, x, H, m, rho, v, c, alpha, Pr, omega,
+    WSPH_DISPATCH_DS(*p, (launch_pdl(k_compsph_pack<D>, (unsigned)((n + 255) / 256), 256, 0, s, (int)n, P, x, H, m, rho, v, c, alpha, Pr, omega,
                                                                                         records)));
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_compsph_accel_dudt<KF, D, G_HEAVY, true><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>(
-                              (int)n, P, x, H, m, rho, v, c, alpha, Pr, omega, records, offs, cnt, list, verlet_cnt, dvdt_out, dudt_out,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_compsph_accel_dudt<KF, D, G_HEAVY, true>, grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, rho, v, c, alpha, Pr, omega, records, offs, cnt, list, verlet_cnt, dvdt_out, dudt_out,
                               dEdt_out, ap_ij, av_ij)));
     return check_launch("sph_compsph_accel_dudt_packed");
 }
@@ -466,8 +468,7 @@ int sph_monaghan_rhs(const SphParams* p, int64_t n, const float* x, const float*
         (rc = check_align_vec(P, dvdt_pressure, "dvdt_pressure")) || (rc = check_align_vec(P, dvdt_viscosity, "dvdt_viscosity")))
         return rc;
     wsph::count_launch();
-    WSPH_DISPATCH_KDS(*p, (k_monaghan_rhs<KF, D, G_HEAVY><<<grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s>>>(
-                              (int)n, P, x, H, m, rho, v, u, c, alpha, Pr, omega, offs, cnt, list, dvdt_out, dudt_out, dEdt_out,
+    WSPH_DISPATCH_KDS(*p, (launch_pdl(k_monaghan_rhs<KF, D, G_HEAVY>, grid_g<G_HEAVY>(n), PAIR_BLOCK, 0, s, (int)n, P, x, H, m, rho, v, u, c, alpha, Pr, omega, offs, cnt, list, dvdt_out, dudt_out, dEdt_out,
                               dvdt_pressure, dvdt_viscosity, dudt_pdv, dudt_conductivity, dudt_heating)));
     return check_launch("sph_monaghan_rhs");
 }
