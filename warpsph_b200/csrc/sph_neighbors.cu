@@ -993,6 +993,35 @@ __global__ void k_refresh_check_cond(const float* __restrict__ x, const float* _
 // in reverse kept order (filled from the row's end, so one pass suffices); a ballot
 // per 8-entry chunk compacts both parts.
 constexpr int RF_G = 8;
+
+// One lane's entries of a row in the rewrite (q = b + sub, b + sub + RF_G, ... < b + c):
+// the neighbour index is loaded two entries ahead and its position and support one entry
+// ahead, so the gathers of an entry are in flight while the previous one is tested.  Past
+// the row's end the prefetches read particle 0.
+template <int D> struct RewritePipe {
+    const int32_t* __restrict__ list;
+    const float* __restrict__ x;
+    const float* __restrict__ H;
+    int q2, e, j1, j2;
+    Vec<D> x1;
+    float H1;
+    __device__ __forceinline__ RewritePipe(const int32_t* __restrict__ l, const float* __restrict__ x_, const float* __restrict__ H_,
+                                           int q0, int e_)
+        : list(l), x(x_), H(H_), q2(q0 + 2 * RF_G), e(e_) {
+        j1 = q0 < e_ ? l[q0] : 0;
+        j2 = q0 + RF_G < e_ ? l[q0 + RF_G] : 0;
+        x1 = load_vec<D>(x_, j1);
+        H1 = __ldg(H_ + j1);
+    }
+    __device__ __forceinline__ void take(int& j, Vec<D>& xj, float& Hj) {
+        j = j1; xj = x1; Hj = H1;
+        j1 = j2;
+        x1 = load_vec<D>(x, j1);
+        H1 = __ldg(H + j1);
+        j2 = q2 < e ? list[q2] : 0;
+        q2 += RF_G;
+    }
+};
 template <int D>
 __global__ void k_refilter(const float* __restrict__ x, const float* __restrict__ H, int n, DevParams P,
                            const unsigned int* __restrict__ acc3, const int32_t* __restrict__ offs,
@@ -1016,14 +1045,17 @@ __global__ void k_refilter(const float* __restrict__ x, const float* __restrict_
     int b = 0, c = 0;
     if (valid) { xi = load_vec<D>(x, i); Hi = H[i]; b = offs[i]; c = cnt[i]; }
     int w = 0, rw = 0;
+    RewritePipe<D> pipe(list, x, H, b + sub, b + c);
     for (int base = 0; __any_sync(0xffffffffu, base < c); base += RF_G) {
         const bool in_row = base + sub < c;
         bool keep = false;
-        int j = 0;
+        int j;
+        Vec<D> xj;
+        float Hj;
+        pipe.take(j, xj, Hj);
         if (in_row) {
-            j = list[b + base + sub];
-            const Vec<D> d = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
-            const float Hm = fmaxf(Hi, __ldg(H + j));
+            const Vec<D> d = dist_vec<D>(xi, xj, P.dom);
+            const float Hm = fmaxf(Hi, Hj);
             keep = interacting_pair(dist2_rn<D>(d), Hm);
         }
         const unsigned int kb = (__ballot_sync(0xffffffffu, keep) >> gshift) & ((1u << RF_G) - 1u);
@@ -1072,14 +1104,16 @@ __global__ void k_refilter_volume(const float* __restrict__ x, const float* __re
     if (valid) { xi = load_vec<D>(x, i); Hi = H[i]; b = offs[i]; c = cnt[i]; }
     int w = 0, rw = 0;
     float wsum = 0.f;
+    RewritePipe<D> pipe(list, x, H, b + sub, b + c);
     for (int base = 0; __any_sync(0xffffffffu, base < c); base += RF_G) {
         const bool in_row = base + sub < c;
         bool keep = false;
-        int j = 0;
+        int j;
+        Vec<D> xj;
+        float Hj;
+        pipe.take(j, xj, Hj);
         if (in_row) {
-            j = list[b + base + sub];
-            const Vec<D> d = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
-            const float Hj = __ldg(H + j);
+            const Vec<D> d = dist_vec<D>(xi, xj, P.dom);
             const float Hm = fmaxf(Hi, Hj);
             keep = interacting_pair(dist2_rn<D>(d), Hm);
             wsum += kW_inv<KF, D>(safe_sqrt(dot<D>(d, d)), 1.f / Hj);
