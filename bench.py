@@ -552,9 +552,8 @@ def e2e_graph(sg, steps: int, world: int, barrier) -> dict:
             if k + 1 < k0 + count:
                 ev = upload(k + 1)        # the next step's inputs cross while this step computes
             sg.replay(1)
-            S = sg.system.state
-            for f in E2E_FIELDS:          # the result leaves the graph's buffers before the next replay
-                d_out[k % 2][f].copy_(getattr(S, f), non_blocking=True)
+            S = sg.system.state            # the result leaves the graph's buffers before the next replay
+            torch._foreach_copy_([d_out[k % 2][f] for f in E2E_FIELDS], [getattr(S, f) for f in E2E_FIELDS], non_blocking=True)
             done = torch.cuda.Event()
             done.record(comp)
             copy.wait_event(done)

@@ -154,8 +154,14 @@ class StepGraph:
     def load_state(self, fields: dict) -> None:
         """Copies tensors (device or pinned host, by state field name) into the graph's input
         buffers, on the current stream; the next replay starts from them."""
-        for name, v in fields.items():
-            getattr(self.inputs.state, name).copy_(v, non_blocking=True)
+        names = list(fields)
+        dsts = [getattr(self.inputs.state, name) for name in names]
+        srcs = [fields[name] for name in names]
+        if all(t.is_cuda for t in srcs):
+            torch._foreach_copy_(dsts, srcs, non_blocking=True)   # one multi-tensor launch
+        else:
+            for d, v in zip(dsts, srcs):
+                d.copy_(v, non_blocking=True)
 
     def rebuilds(self) -> int:
         """Neighbour-list rebuilds so far (counted on the device; one host read per list)."""
