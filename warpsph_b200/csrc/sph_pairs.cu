@@ -493,23 +493,25 @@ k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restric
         RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
             int j; Vec<D> xj; rp.take(q, j, xj);
+            // every gather of the entry issued together, ahead of the tests that select them
+            const float dj = __ldg(div + j), mj = __ldg(m + j);
+            const float Hj = want_vs ? __ldg(H + j) : 0.f, cj = want_vs ? __ldg(c + j) : 0.f;
+            const Vec<D> vj = want_vs ? load_vec<D>(v, j) : vzero<D>();
             Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W = kW_inv<KF, D>(r, invHi);   // gather support
             if (W != 0.f) {
-                float dj = __ldg(div + j);
                 float sg = dj > 0.f ? 1.f : (dj < 0.f ? -1.f : 0.f);
-                s += __ldg(m + j) * sg * W;
+                s += mj * sg * W;
             }
             if (want_vs) {
-                float Hs = wmax(Hi, __ldg(H + j));
+                float Hs = wmax(Hi, Hj);
                 if (r < P.verlet_scale * Hs) {
-                    Vec<D> vj = load_vec<D>(v, j);
                     float mu = 0.f;
                     #pragma unroll
                     for (int a = 0; a < D; ++a) mu += (vi.v[a] - vj.v[a]) * xij.v[a];
                     mu = mu / (r + 1e-14f * Hi);
-                    float vsv = 0.5f * (ci + __ldg(c + j)) - mu;
+                    float vsv = 0.5f * (ci + cj) - mu;
                     if (mu > 0.f) vsv = 0.f;
                     vsig = wmax(vsig, vsv);
                 }
@@ -757,14 +759,13 @@ __device__ __forceinline__ float limiter_vl(float x) {
 }
 __device__ __forceinline__ float sgn_pos(float x) { return x >= 0.f ? 1.f : -1.f; }
 
-// modules/crk/limiter.py:27-86 (quadratic-form Van Leer)
+// modules/crk/limiter.py:27-86 (quadratic-form Van Leer) with g = (G h).h, h = x_ij / 2,
+// from the products G_i x_ij and G_j x_ij the pass needs anyway: halving is exact in
+// floating point, so (G h).h = (G x_ij).x_ij / 4 (outside the subnormal range).
 template <int D>
-__device__ __forceinline__ float van_leer(const Vec<D>& xij_, const Mat<D>& Gi, const Mat<D>& Gj) {
-    Vec<D> h;
-    #pragma unroll
-    for (int a = 0; a < D; ++a) h.v[a] = 0.5f * xij_.v[a];
-    float gi = dot<D>(matvec<D>(Gi, h), h);
-    float gj = dot<D>(matvec<D>(Gj, h), h);
+__device__ __forceinline__ float van_leer(const Vec<D>& xij_, const Vec<D>& Gix, const Vec<D>& Gjx) {
+    float gi = 0.25f * dot<D>(Gix, xij_);
+    float gj = 0.25f * dot<D>(Gjx, xij_);
     float ri = __fdividef(gi, sgn_pos(gj) * fabsf(gj));
     float rj = __fdividef(gj, sgn_pos(gi) * fabsf(gi));
     if (ri != ri) ri = 1.f;
@@ -954,12 +955,12 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
                 float eta = r * wmin(invHi, invHj);
                 if (eta < P.eta_crit) { float t = (eta - P.eta_crit) / P.eta_fold; factor = expf(-(t * t)); }
             }
+            Vec<D> Gix = matvec<D>(pi.G, xij), Gjx = matvec<D>(pj.G, xij);
             float phi = 0.f;
-            if (P.enable_vanleer) phi = van_leer<D>(xij, pi.G, pj.G) * factor;
+            if (P.enable_vanleer) phi = van_leer<D>(xij, Gix, Gjx) * factor;
             if (P.force_vl_off) phi = 0.f;
             if (P.force_vl_on) phi = 1.f;
             phi = wmax(wmin(phi, 1.f), 0.f);
-            Vec<D> Gix = matvec<D>(pi.G, xij), Gjx = matvec<D>(pj.G, xij);
             float hp = 0.5f * phi;
             // v_dot_i - v_dot_j (accel.py:137-141; dudt.py:122-126 uses gradV_j . (-x_ij))
             Vec<D> da, dd;
