@@ -72,11 +72,11 @@ k_adaptive_h(int n, DevParams P, const float* __restrict__ x, const float* __res
         RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
             int j; Vec<D> xj; rp.take(q, j, xj);
+            const float mj = __ldg(m + j);
             Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W, dWdH;
             kernelWdH<KF, D>(r, Hi, W, dWdH);
-            float mj = __ldg(m + j);
             rs += mj * W;
             ds += mj * dWdH;
         }
@@ -259,12 +259,12 @@ k_crk_factors(int n, DevParams P, const float* __restrict__ x, const float* __re
         RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
             int j; Vec<D> xj; rp.take(q, j, xj);
+            const float Hj = __ldg(H + j), Vj = __ldg(V + j), mj = __ldg(m + j);   // gathers issued together
             Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W; Vec<D> gW;
-            kWG_inv<KF, D>(xij, r, 1.f / __ldg(H + j), W, gW);
+            kWG_inv<KF, D>(xij, r, 1.f / Hj, W, gW);
             if (W == 0.f) continue;
-            float Vj = __ldg(V + j), mj = __ldg(m + j);
             float VW = Vj * W, mW = mj * W;
             a.m0 += VW;
             a.s0 += mW;
@@ -410,15 +410,15 @@ k_grad_v(int n, DevParams P, const float* __restrict__ x, const float* __restric
         RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
             int j; Vec<D> xj; rp.take(q, j, xj);
+            const float Hj = __ldg(H + j), Vj = __ldg(V + j);   // gathers issued together
+            const float mj = want_div ? __ldg(m + j) : 0.f, rhoj = want_div ? __ldg(rho + j) : 1.f;
+            const Vec<D> vj = load_vec<D>(v, j);
             Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
-            float Hj = __ldg(H + j);
-            Vec<D> vj = load_vec<D>(v, j);
             float W; Vec<D> gW;
             kWG_inv<KF, D>(xij, r, 1.f / Hj, W, gW);
             if (W != 0.f) {
                 Vec<D> gR = crk_grad<D>(xij, W, gW, Ai, Bi, gAi, gBi);
-                float Vj = __ldg(V + j);
                 #pragma unroll
                 for (int a = 0; a < D; ++a) {
                     float dv = Vj * (vj.v[a] - vi.v[a]);
@@ -430,7 +430,7 @@ k_grad_v(int n, DevParams P, const float* __restrict__ x, const float* __restric
             if (want_div && r < Hs) {
                 float W2; Vec<D> g2;
                 kWG_inv<KF, D>(xij, r, 1.f / Hs, W2, g2);
-                float vol = __ldg(m + j) / __ldg(rho + j);
+                float vol = mj / rhoj;
                 float s = 0.f;
                 #pragma unroll
                 for (int a = 0; a < D; ++a) s += (vj.v[a] - vi.v[a]) * g2.v[a];
@@ -1082,6 +1082,7 @@ k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restri
     const int ie = icnt ? b + icnt[i] : e;
     for (int q = b + g.lane; q < e; q += G) {
         int j, k; entry(list, q, j, k);
+        const float sj_crk = scheme == SPH_ENERGY_CRK ? __ldg(sarr + j) : 0.f;   // issued with the entry's other gathers
         float dE = 0.f;
         if (q < ie) {
             Vec<D> vj = load_vec<D>(vh, j);
@@ -1092,7 +1093,7 @@ k_balance(int n, DevParams P, const float* __restrict__ m, const float* __restri
         dE = mi * dE * dt;
         float f = 0.5f;
         if (scheme == SPH_ENERGY_CRK) {
-            float sj = __ldg(sarr + j);
+            const float sj = sj_crk;
             float smin = wmin(fabsf(si), fabsf(sj)), smax = wmax(fabsf(si), fabsf(sj));
             bool mA = fabsf(si - sj) == 0.f;
             bool mB = (dE >= 0.f && si >= sj) || (dE < 0.f && si < sj);
