@@ -41,14 +41,18 @@ k_compsph_prep(int n, DevParams P, const float* __restrict__ x, const float* __r
         Vec<D> vi = (want_div || want_con) ? load_vec<D>(v, i) : vzero<D>();
         const float Hi = H[i];
         int b = offs[i], e = b + cnt[i];
+        RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
-            int j, k; entry(list, q, j, k);
-            Vec<D> xij = dist_vec<D>(xi, load_vec<D>(x, j), P.dom);
+            int j; Vec<D> xj; rp.take(q, j, xj);
+            // every gather of the entry issued together, ahead of the tests that select them
+            const float Hj = __ldg(H + j), mj = __ldg(m + j);
+            const float rhoj = want_div ? __ldg(rho + j) : 1.f;
+            const Vec<D> vj = (want_div || want_con) ? load_vec<D>(v, j) : vzero<D>();
+            Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r2 = dot<D>(xij, xij);
-            float Hs = wmax(Hi, __ldg(H + j));
+            float Hs = wmax(Hi, Hj);
             if (!(r2 < Hs * Hs)) continue;
             float r = safe_sqrt(r2);
-            float mj = __ldg(m + j);
             if (want_om && r < Hi) {
                 float W, dWdH;
                 kernelWdH<KF, D>(r, Hi, W, dWdH);
@@ -57,11 +61,10 @@ k_compsph_prep(int n, DevParams P, const float* __restrict__ x, const float* __r
             if (want_div || want_con) {
                 float W; Vec<D> gS;
                 kWG_inv<KF, D>(xij, r, 1.f / Hs, W, gS);
-                Vec<D> vj = load_vec<D>(v, j);
                 float s = 0.f;
                 #pragma unroll
                 for (int a = 0; a < D; ++a) s += (vj.v[a] - vi.v[a]) * gS.v[a];
-                if (want_div) sdiv += mj / __ldg(rho + j) * s;
+                if (want_div) sdiv += mj / rhoj * s;
                 scon += mj * s;
             }
         }
