@@ -175,7 +175,9 @@ k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const floa
             Vec<D> xj;
             float Hj;
             if constexpr (REC) {
-                comp_granules<D, 0, L::K1>(sj, rj);
+                // the first two groups issued together (walked rows are interacting prefixes, so
+                // the range test below almost never discards the second)
+                comp_granules<D, 0, L::K2>(sj, rj);
                 #pragma unroll
                 for (int a = 0; a < D; ++a) xj.v[a] = rj[L::X + a];
                 Hj = rj[L::H];
@@ -195,7 +197,6 @@ k_compsph_accel_dudt(int n, DevParams P, const float* __restrict__ x, const floa
             Vec<D> vj;
             float mj, rhoj, Pj, cj, aj, omj;
             if constexpr (REC) {
-                comp_granules<D, L::K1, L::K2>(sj, rj);
                 #pragma unroll
                 for (int a = 0; a < D; ++a) vj.v[a] = rj[L::V + a];
                 mj = rj[L::M]; rhoj = rj[L::RHO]; Pj = rj[L::P]; cj = rj[L::C]; aj = rj[L::AL]; omj = rj[L::OM];

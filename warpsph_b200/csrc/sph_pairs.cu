@@ -928,7 +928,12 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
             CrkPart<D> pj;
             float rj[CrkRec<D>::R];
             const float4* sj = REC ? reinterpret_cast<const float4*>(rec + (size_t)j * CrkRec<D>::R) : nullptr;
-            if constexpr (REC) { rec_granules<D, 0, CrkRec<D>::K1>(sj, rj); crk_unpack1<D>(rj, pj); }
+            if constexpr (REC) {
+                // the first two groups issued together (walked rows are interacting prefixes, so
+                // the range test below almost never discards the second)
+                rec_granules<D, 0, CrkRec<D>::K2>(sj, rj);
+                crk_unpack1<D>(rj, pj);
+            }
             else { pj.x = load_vec<D>(x, j); pj.H = __ldg(H + j); }
             Vec<D> xij = dist_vec<D>(pi.x, pj.x, P.dom);
             float r2 = dot<D>(xij, xij);
@@ -940,7 +945,7 @@ k_crk_accel_dudt(int n, DevParams P, const float* __restrict__ x, const float* _
                 continue;
             }
             if constexpr (REC) {
-                rec_granules<D, CrkRec<D>::K1, CrkRec<D>::K2>(sj, rj); crk_unpack2<D>(rj, pj);
+                crk_unpack2<D>(rj, pj);
             } else {
                 pj.v = load_vec<D>(v, j);
                 pj.rho = __ldg(rho + j); pj.c = __ldg(c + j); pj.P = __ldg(Pr + j);
