@@ -728,7 +728,7 @@ def gpu_arm(args, rank: int, world: int):
     # ------------------------------------------------ end-to-end through the API with host buffers
     e2e = None
     if not args.no_e2e and sg is not None:
-        e2e = e2e_graph(sg, max(3, args.steps // 2), world, barrier)
+        e2e = e2e_graph(sg, max(3, args.steps), world, barrier)
     elif not args.no_e2e:
         fields = E2E_FIELDS
         e2e_steps = max(3, args.steps // 2)
