@@ -93,3 +93,31 @@ def test_energy_momentum_conservation_and_symmetry(cuda, nx):
     ke = 0.5 * S.masses.cpu().numpy() * np.sum(S.velocities.cpu().numpy().astype(np.float64) ** 2, 1)
     left, right = ke[x[:, 0] < 0].sum(), ke[x[:, 0] > 0].sum()
     assert abs(left - right) / (left + right) < 1e-3
+
+
+def test_fused_entries_equal_separate_calls(cuda):
+    """The launch-saving entries give the separate calls' results bit for bit:
+    sph_crk_factors_eos against sph_crk_factors + sph_eos_ideal_gas, and
+    sph_rk_combine_fields against one sph_rk_combine per field."""
+    from warpsph_b200 import ops
+    cfg, sch, integ, step, system = sedov(48, cuda)
+    params = ws.make_params(cfg, sch)
+    S = system.state
+    adj = ops.buildVerletList(S.positions, S.supports, params, cfg.verletScale, None)
+    V = ops.crk_volume(params, S.positions, S.supports, adj)
+    crk1, rho1 = ops.crk_factors(params, S.positions, S.supports, S.masses, V, adj)
+    A1, P1, c1 = ops.eos_ideal_gas(params, S.internalEnergies, rho1)
+    crk2, rho2, A2, P2, c2 = ops.crk_factors_eos(params, S.positions, S.supports, S.masses, V, adj, S.internalEnergies)
+    for a, b in ((crk1.A, crk2.A), (crk1.B, crk2.B), (crk1.gradA, crk2.gradA), (crk1.gradB, crk2.gradB), (rho1, rho2),
+                 (A1, A2), (P1, P2), (c1, c2)):
+        assert torch.equal(a, b)
+    g = torch.Generator(device=cuda).manual_seed(11)
+    n, d = S.positions.shape
+    ks = [[torch.randn(S.positions.shape, generator=g, device=cuda) for _ in range(2)],
+          [torch.randn(S.velocities.shape, generator=g, device=cuda) for _ in range(2)],
+          [torch.randn(S.internalEnergies.shape, generator=g, device=cuda) for _ in range(2)]]
+    fields = [(S.positions, ks[0], d), (S.velocities, ks[1], 0), (S.internalEnergies, ks[2], 0)]
+    w, dt = [0.5, 0.5], torch.tensor([3e-3], device=cuda)
+    fused = ops.rk_combine_fields(params, fields, w, dt)
+    for (y0, kf, wrap), y in zip(fields, fused):
+        assert torch.equal(ops.rk_combine(params, y0, kf, w, dt, wrap), y)
