@@ -110,7 +110,9 @@ class StepGraph:
         lib = _capi.lib()
         launches0, cond0 = lib.sph_launch_count(), lib.sph_launch_count_conditional()
         gen0 = [nb.generation for nb in self.lists]
-        with ops.device_decided_lists(), torch.cuda.graph(self.graph):
+        # thread-local capture: other threads of the process (a process group's watchdog, for
+        # one) may keep making CUDA calls while this thread records
+        with ops.device_decided_lists(), torch.cuda.graph(self.graph, capture_error_mode="thread_local"):
             out, dt_new = self._advance(self.inputs, self.dt)
             static = dict(_per_particle(self.inputs.state, n))
             dsts, srcs = [], []
