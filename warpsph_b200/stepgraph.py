@@ -20,6 +20,10 @@ Usage::
     sg.check()                     # one host read: list overflow / bad supports
     state = sg.system.state        # tensors the next replay overwrites (clone to keep)
 
+The neighbour list has a fixed capacity, 1.3 times the entries of one build at the start
+(``ops.DEVICE_LIST_HEADROOM``); a workload whose neighbour counts grow past it makes
+``check()`` raise, and is recorded again with a larger headroom from a saved state.
+
 Each step's time step is ``next_dt(system, dt_prev)`` (a device scalar); the default is
 the CFL step of the compressible schemes (modules/timestep/compressible.py:12-66) when
 ``config.adaptiveDt`` is set, else the fixed dt.  The step function must not read the
