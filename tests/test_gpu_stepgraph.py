@@ -189,3 +189,39 @@ def test_recorded_update_rebuilds_only_when_stale(cuda):
             assert torch.equal(nb.x0, x_prev0), "a replay after a small move must keep the rows"
         assert np.array_equal(interacting_pairs(adj, n), fresh_pairs(x, H, params, cfg.verletScale, n))
     nb.check()
+
+
+def _graph_vs_device_eager(cuda, cfg, sch, integ, step, sys_a, sys_b, warm, steps, rtol, atol):
+    """Replays of a recorded step against the same steps issued eagerly with device-decided
+    lists, from the same initial state."""
+    dt0 = torch.tensor([cfg.dt], device=cuda, dtype=torch.float32)
+    sg = StepGraph(sys_a, integ, step, cfg, sch, dt=dt0, warmup=warm)
+    sg.replay(steps)
+    torch.cuda.synchronize()
+    sg.check()
+    A = sg.system.state
+    ops.release_device_lists()
+    params = ws.make_params(cfg, sch)
+    dt = dt0.clone()
+    with ops.device_decided_lists():
+        for _ in range(warm + steps):
+            dt = ops.cfl_dt(params, sys_b.state.supports, sys_b.state.internalEnergies, dt_prev=dt)
+            sys_b = integ.function(state=sys_b, f=step, dt=dt, config=cfg, compParams=sch).state
+    B = sys_b.state
+    for name in ("positions", "velocities", "internalEnergies", "densities", "supports"):
+        assert_close(getattr(A, name).cpu().numpy(), getattr(B, name).cpu().numpy(), rtol, atol, name)
+    sg.release()
+
+
+def test_graph_replay_3d(cuda):
+    from tests.test_gpu_sedov3d import sedov3d
+    cfg, sch, integ, step, sys_a = sedov3d(16, cuda)
+    *_, sys_b = sedov3d(16, cuda)
+    _graph_vs_device_eager(cuda, cfg, sch, integ, step, sys_a, sys_b, 2, 3, 1e-5, 1e-6)
+
+
+def test_graph_replay_rk4(cuda):
+    cfg, sch, integ, step, sys_a = sedov(32, cuda)
+    *_, sys_b = sedov(32, cuda)
+    integ4 = ws.getIntegrator(ws.IntegrationSchemeType.rungeKutta4)
+    _graph_vs_device_eager(cuda, cfg, sch, integ4, step, sys_a, sys_b, 2, 3, 1e-5, 1e-6)
