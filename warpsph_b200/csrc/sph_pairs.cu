@@ -493,14 +493,18 @@ k_cullen(int n, DevParams P, const float* __restrict__ x, const float* __restric
         RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
             int j; Vec<D> xj; rp.take(q, j, xj);
-            // every gather of the entry issued together, ahead of the tests that select them
-            const float dj = __ldg(div + j), mj = __ldg(m + j);
+            // every gather of the entry issued together, ahead of the tests that select them;
+            // in 3D, where about two thirds of a Verlet row lie outside the support, the
+            // divergence and the mass are loaded only for the entries inside it (measured:
+            // 11.3 against 12.8 ms per step at 128^3; in 2D loading them ahead wins)
+            const float dj_ahead = D < 3 ? __ldg(div + j) : 0.f, mj_ahead = D < 3 ? __ldg(m + j) : 0.f;
             const float Hj = want_vs ? __ldg(H + j) : 0.f, cj = want_vs ? __ldg(c + j) : 0.f;
             const Vec<D> vj = want_vs ? load_vec<D>(v, j) : vzero<D>();
             Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W = kW_inv<KF, D>(r, invHi);   // gather support
             if (W != 0.f) {
+                const float dj = D < 3 ? dj_ahead : __ldg(div + j), mj = D < 3 ? mj_ahead : __ldg(m + j);
                 float sg = dj > 0.f ? 1.f : (dj < 0.f ? -1.f : 0.f);
                 s += mj * sg * W;
             }
