@@ -72,11 +72,14 @@ k_adaptive_h(int n, DevParams P, const float* __restrict__ x, const float* __res
         RowPipe<D> rp(list, x, b + g.lane, e, G);
         for (int q = b + g.lane; q < e; q += G) {
             int j; Vec<D> xj; rp.take(q, j, xj);
-            const float mj = __ldg(m + j);
+            // the mass ahead of the kernel evaluation in 1D and 2D; in 3D most Verlet entries
+            // lie outside the support, whose kernel values are 0 (the load is skipped for them)
+            const float mj_ahead = D < 3 ? __ldg(m + j) : 0.f;
             Vec<D> xij = dist_vec<D>(xi, xj, P.dom);
             float r = safe_sqrt(dot<D>(xij, xij));
             float W, dWdH;
             kernelWdH<KF, D>(r, Hi, W, dWdH);
+            const float mj = D < 3 ? mj_ahead : (W != 0.f || dWdH != 0.f ? __ldg(m + j) : 0.f);
             rs += mj * W;
             ds += mj * dWdH;
         }
